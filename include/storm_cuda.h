@@ -1,0 +1,326 @@
+/*
+ * storm_cuda.h -- C ABI of the B200 Implicit Monte Carlo (IMC) transport engine.
+ *
+ * This is the host->device crossing of the drop-in replacement for STORM's
+ * serial manager.  In STORM the whole time step is
+ *
+ *     std::vector<Particle> MonteCarloManagerSerial<T,Grid>::step(std::vector<Particle>&&, dt_t)
+ *     (manager/MonteCarloManagerSerial.hpp:44, 386-469)
+ *
+ * which calls RadiationIMC::preStep (radiation/RadiationIMC.hpp:1618-1694), the
+ * per-particle RadiationIMC::step (radiation/RadiationIMC.hpp:1700-1881) until
+ * census/escape/absorption, CombPopulationControl::activate
+ * (population/CombPopulationControl.hpp:79-253) and RadiationIMC::postStep
+ * (radiation/RadiationIMC.hpp:1887-2029).  Here the same step runs on one GPU
+ * behind an opaque handle.  Everything is plain C: pointers, sizes, int status.
+ *
+ * Error convention: every entry point returns an int status (0 = STORM_OK).  No
+ * exception crosses the ABI.  A nonzero status carries the class below; the
+ * device error word (STORM_DERR_*) that a kernel raised is read with
+ * storm_cuda_last_error().  The C++ host template (storm/MonteCarloManagerCUDA.hpp)
+ * converts a nonzero status into STORM::StormError, matching the reference's
+ * "report and rethrow" behaviour (manager/MonteCarloManagerSerial.hpp:458-462).
+ *
+ * Threading: one CUDA stream per handle; calls on one handle must be serialised
+ * by the caller (the reference manager is single-threaded and not reentrant,
+ * manager/MonteCarloManagerSerial.hpp:269-270).  Different handles are
+ * independent.
+ */
+#ifndef STORM_CUDA_H
+#define STORM_CUDA_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define STORM_CUDA_ABI_VERSION 1
+
+/* ---------------------------------------------------------------- status */
+enum StormStatus {
+    STORM_OK = 0,
+    STORM_ERR_INVALID_ARG = 1,   /* bad descriptor / argument (host-side check) */
+    STORM_ERR_CUDA = 2,          /* a CUDA runtime call failed */
+    STORM_ERR_OOM = 3,           /* device allocation failed */
+    STORM_ERR_DEVICE = 4,        /* a kernel raised a STORM_DERR_* error word */
+    STORM_ERR_CAPACITY = 5,      /* particle bank capacity exceeded */
+    STORM_ERR_UNSUPPORTED = 6,   /* option not supported by this engine */
+    STORM_ERR_NO_DEVICE = 7      /* no CUDA device visible */
+};
+
+/* Device error words (first error wins, recorded with cell / particle index).
+ * Each corresponds to a StormError the reference throws. */
+enum StormDeviceError {
+    STORM_DERR_NONE = 0,
+    STORM_DERR_NO_FACE = 1,          /* particle/Particle.hpp:257-278 "no face intersection found" */
+    STORM_DERR_NOT_ON_BOUNDARY = 2,  /* boundary/RigidBoundary.hpp:66-68, SideTemperature.hpp:110-111 */
+    STORM_DERR_FLECK = 3,            /* radiation/RadiationIMC.hpp:1650-1661 invalid Fleck factor */
+    STORM_DERR_NEGATIVE_ENERGY = 4,  /* radiation/RadiationIMC.hpp:771-817 */
+    STORM_DERR_COMB_OUTSIDE = 5,     /* population/CombPopulationControl.hpp:110-121 */
+    STORM_DERR_COMB_WEIGHT = 6,      /* population/CombPopulationControl.hpp:122-135 (non-finite or negative) */
+    STORM_DERR_RW_SHRINK = 7,        /* RW shrink-to-inside loop exceeded its iteration limit */
+    STORM_DERR_HISTORY_CAP = 8,      /* a history exceeded max_rounds * segments_per_visit segments */
+    STORM_DERR_BANK_OVERFLOW = 9,    /* more particles than bank capacity */
+    STORM_DERR_TAPE_EXHAUSTED = 10,  /* replay: uniform tape too short */
+    STORM_DERR_COMB_TOTAL = 11       /* population/CombPopulationControl.hpp:147-153 total weight not finite */
+};
+
+/* ---------------------------------------------------------------- enums */
+enum StormPrecision {
+    STORM_PRECISION_FP64 = 0,        /* all-FP64 tracking (reference arithmetic) */
+    STORM_PRECISION_FP32_TRACK = 1   /* cell index + FP32 cell-local offset, FP32 direction/distance;
+                                        weights, time, tallies and material update in FP64 */
+};
+
+enum StormFaceAction {
+    STORM_FACE_REFLECT = 0,          /* BoundaryCondition::reflectParticleOnBoxFace (boundary/BoundaryCondition.hpp:87-108) */
+    STORM_FACE_ESCAPE = 1            /* particle removed, its weight tallied as escaped */
+};
+
+enum StormOpacityKind {
+    /* sigma_a[cell], sigma_s[cell] given per cell (temperature independent) */
+    STORM_OPACITY_CELL_TABLE = 0,
+    /* sigma_a = min(kP0 * (kev_kelvin / max(T, t_floor))^alpha * rho^beta, cap)
+       sigma_s = max(kR0 * f - kP0 * f, 0) with the same factors f.
+       Marshak form: examples/marshak_wave/MarshakOpacity.hpp:30-46 (cap = +inf there). */
+    STORM_OPACITY_POWER_LAW = 1
+};
+
+enum StormEosKind {
+    /* dT2cv = cv_per_mass ; de2T = e / cv_per_mass   (examples/densmore2012/main.cpp:56-77) */
+    STORM_EOS_LINEAR = 0,
+    /* e_vol = f * T^beta * rho^(1-mu)   (examples/marshak_wave/MarshakCommon.hpp:138-155, 162-183) */
+    STORM_EOS_POWER_LAW = 1
+};
+
+/* ---------------------------------------------------------------- descriptor */
+
+/* One of the six faces of the bounding box, in GetBoxFaces() order:
+ * 0 x-low, 1 x-high, 2 y-low, 3 y-high, 4 z-low, 5 z-high. */
+typedef struct StormBoxFace {
+    int32_t action;              /* StormFaceAction */
+    int32_t pad_;
+    double source_temperature;   /* K; > 0 makes this face a Planck surface source */
+    uint64_t packets_per_face;   /* packets per boundary cell-face per step (SideTemperature::Npercell) */
+} StormBoxFace;
+
+typedef struct StormProblemDesc {
+    uint32_t abi_version;        /* must be STORM_CUDA_ABI_VERSION */
+    int32_t precision;           /* StormPrecision */
+
+    /* ---- rectilinear mesh (the Cartesian Grid of the reference examples).
+     * Cell index = i + nx*(j + ny*k).  Edges strictly increasing. */
+    uint32_t nx, ny, nz;
+    const double *x_edges;       /* nx+1 */
+    const double *y_edges;       /* ny+1 */
+    const double *z_edges;       /* nz+1 */
+
+    /* ---- per-cell material state (host arrays, Ncells each).  Units as in
+     * radiation/RadiationCell.hpp:6-19: temperature [K], mass [g],
+     * internal_energy = extensive material energy [erg]. */
+    const double *temperature;
+    const double *mass;
+    const double *internal_energy;
+    const double *cell_internal_energy;  /* RadiationCell::internalEnergy (positivity floor); NULL = internal_energy */
+
+    /* ---- opacity plug-in lowered to a device descriptor */
+    int32_t opacity_kind;        /* StormOpacityKind */
+    int32_t eos_kind;            /* StormEosKind */
+    const double *sigma_a;       /* CELL_TABLE: absorption (Planck) opacity [1/cm], Ncells */
+    const double *sigma_s;       /* CELL_TABLE: scattering opacity [1/cm], Ncells (NULL = 0) */
+    double kP0, kR0, alpha, beta, t_floor, cap;   /* POWER_LAW parameters */
+    const double *density_factor;               /* POWER_LAW: rho^beta per cell (NULL = 1) */
+
+    /* ---- EOS */
+    double cv_per_mass;          /* LINEAR */
+    double eos_f, eos_beta, eos_mu;  /* POWER_LAW */
+
+    /* ---- boundary plug-in lowered to per-box-face actions */
+    StormBoxFace faces[6];
+    int32_t escape_without_check;    /* VacuumBoundary::apply removes without a closeness test (boundary/Vacuum.hpp:18-22) */
+    int32_t pad0_;
+
+    /* ---- RadiationIMCParameters<1> (radiation/RadiationIMCParameters.hpp:13-56) */
+    uint64_t new_photons_per_cell;
+    int32_t with_random_walk;
+    int32_t no_hydro_feedback;
+    double rw_min_cell_optical_depth;
+    double rw_min_particle_optical_depth;
+
+    /* ---- CombPopulationControl(grid, Nmin, factor) (population/CombPopulationControl.hpp:21-31) */
+    int32_t comb_enabled;
+    int32_t pad1_;
+    uint64_t comb_nmin;
+    double comb_factor;
+
+    /* ---- physical constants, taken from the caller's `units` so that host and
+     * device agree with whatever constants the caller's physics uses. */
+    double clight, arad, sigma_sb, kev_kelvin;
+
+    /* ---- engine settings (MonteCarloConfig-like) */
+    uint64_t seed;
+    uint64_t capacity;               /* max particles in flight (0 = automatic) */
+    uint32_t segments_per_visit;     /* segments a thread runs per bank visit (0 = automatic) */
+    uint32_t max_rounds;             /* bank visits per step before STORM_DERR_HISTORY_CAP (0 = automatic) */
+    int32_t per_cell_segment_counters;   /* fill GetCellsStepsCounters() (costs one atomic per segment) */
+    int32_t device;                  /* CUDA device ordinal */
+} StormProblemDesc;
+
+/* Particle arrays, struct-of-arrays.  Mirrors the fields of
+ * Particle<T,Grid> (particle/Particle.hpp:67-85) that the gray path uses.
+ * Host or device pointers depending on the call. */
+typedef struct StormParticlesSoA {
+    double *x, *y, *z;           /* location [cm] */
+    double *vx, *vy, *vz;        /* velocity = c * direction [cm/s] */
+    double *time_left;           /* [s] */
+    double *weight;              /* [erg] */
+    double *initial_weight;      /* [erg] */
+    uint32_t *cell;              /* cellIndex */
+    uint64_t *id;                /* particle id within the step (may be NULL on input) */
+    uint64_t count;
+} StormParticlesSoA;
+
+typedef struct StormStepStats {
+    uint64_t census_in;          /* particles handed to the step (GetInitialParticleCount) */
+    uint64_t emitted_cells;      /* cell-source packets (RadiationIMC::generateParticles) */
+    uint64_t emitted_faces;      /* boundary-source packets */
+    uint64_t census_out_pre_comb;/* DONE particles before population control */
+    uint64_t census_out;         /* particles after population control (GetEndParticleCount) */
+    uint64_t segments;           /* sum of GetCellsStepsCounters() */
+    uint64_t rw_steps;           /* getRandomWalkStepCount() */
+    uint64_t escaped;            /* particles removed at the boundary */
+    uint64_t cutoff;             /* particles removed by the weight cutoff */
+    uint64_t rounds;             /* bank visits used by transport */
+    double energy_census_in;     /* sum of census weights at step start */
+    double energy_emitted;       /* cell + face source energy */
+    double energy_deposited;     /* sum of material deposits during transport (incl. cutoff) */
+    double energy_escaped;       /* weight that left through ESCAPE faces */
+    double energy_census_pre_comb;
+    double energy_census_out;
+    double energy_emission_debit;/* material energy removed by cell emission */
+    double transport_ms;         /* device time of transport (CUDA events) */
+    double step_ms;              /* device time of the whole step */
+} StormStepStats;
+
+/* Replay of single segments against a recorded uniform tape: the parity
+ * entry point.  Each item is one call of RadiationIMC::step plus the manager's
+ * face/boundary handling (manager/MonteCarloManagerSerial.hpp:318-369). */
+typedef struct StormReplayBatch {
+    uint64_t n;
+    /* inputs, n each (host) */
+    const double *x, *y, *z, *vx, *vy, *vz, *time_left, *weight, *initial_weight;
+    const uint32_t *cell;
+    const uint64_t *tape_offset;     /* into tape */
+    const uint32_t *tape_length;
+    const double *tape;              /* raw std::uniform_real_distribution draws */
+    /* outputs, n each (host) */
+    double *phys_x, *phys_y, *phys_z, *phys_vx, *phys_vy, *phys_vz, *phys_time_left, *phys_weight;
+    int32_t *phys_status;            /* ParticleStatus of RadiationIMC::step (particle/ParticleStatus.hpp:8-15) */
+    uint32_t *phys_next_cell;        /* StepResult::nextCellIndex (face crossings), else UINT32_MAX */
+    double *dep_material;            /* sum added to extensives[cell].internal_energy */
+    double *dep_erad;                /* sum added to Erad_time_avg_[cell] */
+    double *mgr_x, *mgr_y, *mgr_z, *mgr_vx, *mgr_vy, *mgr_vz; /* after the manager's nudge / boundary */
+    uint32_t *mgr_cell;
+    int32_t *mgr_status;             /* 0 continue, 1 census, 2 removed (cutoff), 3 escaped */
+    uint32_t *draws_used;
+    int32_t *used_random_walk;
+} StormReplayBatch;
+
+typedef struct StormHandle StormHandle;
+
+/* ---------------------------------------------------------------- lifecycle */
+
+/* Replaces constructing MonteCarloManagerSerial(grid, physics, populationControl,
+ * boundaryCondition) (manager/MonteCarloManagerSerial.hpp:38-40, 120-129) and the
+ * RadiationIMC constructor (radiation/RadiationIMC.hpp:562-640). */
+int storm_cuda_create(const StormProblemDesc *desc, StormHandle **out);
+/* Replaces ~MonteCarloManagerSerial (manager/MonteCarloManagerSerial.hpp:186-195). */
+int storm_cuda_destroy(StormHandle *h);
+
+/* ---------------------------------------------------------------- the step */
+
+/* One full time step on the device-resident census: MonteCarloManagerSerial::step
+ * (manager/MonteCarloManagerSerial.hpp:386-469).  stats may be NULL. */
+int storm_cuda_step(StormHandle *h, double dt, StormStepStats *stats);
+
+/* The phases of storm_cuda_step, callable one at a time (parity tests):
+ *   prestep   -> RadiationIMC::preStep minus emission (RadiationIMC.hpp:1618-1672)
+ *   emit      -> generateParticles + boundary->generateNewBoundaryParticles (RadiationIMC.hpp:1674-1692, 2035-2510)
+ *   transport -> the HandleAll loop (MonteCarloManagerSerial.hpp:267-383, 436-456)
+ *   comb      -> populationControl->activate (MonteCarloManagerSerial.hpp:464)
+ *   poststep  -> physics->postStep (MonteCarloManagerSerial.hpp:466) */
+int storm_cuda_phase_prestep(StormHandle *h, double dt);
+int storm_cuda_phase_emit(StormHandle *h, double dt);
+int storm_cuda_phase_transport(StormHandle *h);
+int storm_cuda_phase_comb(StormHandle *h);
+int storm_cuda_phase_poststep(StormHandle *h, double dt);
+/* statistics gathered by the phases since the last storm_cuda_phase_begin / storm_cuda_step */
+int storm_cuda_phase_begin(StormHandle *h, double dt);
+int storm_cuda_phase_stats(StormHandle *h, StormStepStats *stats);
+
+/* ---------------------------------------------------------------- state in/out */
+
+/* Replace the census with host particles (the std::vector<Particle>&& argument
+ * of step()).  Copies host -> device. */
+int storm_cuda_set_census(StormHandle *h, const StormParticlesSoA *host_in);
+/* Copy the census (the vector step() returns) device -> host.  host_out arrays
+ * must hold `capacity` entries; *count receives the census size. */
+int storm_cuda_get_census(StormHandle *h, StormParticlesSoA *host_out, uint64_t capacity, uint64_t *count);
+int storm_cuda_census_count(StormHandle *h, uint64_t *count);
+
+/* Per-cell arrays (host, Ncells each; any pointer may be NULL):
+ * temperature [K], internal_energy [erg], erad_time_avg (getEradTimeAvg(),
+ * RadiationIMC.hpp:431), erad_census (SimpleExtensives::Erad), sigma_a
+ * (getPlanckOpacities), fleck (getFactorFleck), segment counters
+ * (GetCellsStepsCounters, MonteCarloManagerSerial.hpp:74). */
+int storm_cuda_get_cell_arrays(StormHandle *h, double *temperature, double *internal_energy,
+                               double *erad_time_avg, double *erad_census,
+                               double *sigma_a, double *fleck, uint64_t *segment_counters);
+/* Overwrite the material state (e.g. after the caller's hydro step). */
+int storm_cuda_set_cell_state(StormHandle *h, const double *temperature, const double *internal_energy,
+                              const double *cell_internal_energy);
+/* Overwrite the per-cell physics tables prestep would compute (sigma_a,
+ * sigma_s, Fleck factor).  Replay parity uses the reference's own tables. */
+int storm_cuda_set_cell_physics(StormHandle *h, const double *sigma_a, const double *sigma_s,
+                                const double *fleck);
+/* MarshakBoundary::SetTemperature / SideTemperature::SetTemperature. */
+int storm_cuda_set_face_temperature(StormHandle *h, int face, double temperature);
+
+/* Source counts per cell of the last emission (getLastSourcePhotonsPerCell,
+ * RadiationIMC.hpp:437) and the emission energy per cell. */
+int storm_cuda_get_emission(StormHandle *h, uint64_t *photons_per_cell, double *energy_per_cell);
+
+/* ---------------------------------------------------------------- parity */
+
+/* Run each replay item as one segment fed by its uniform tape. Uses the
+ * handle's mesh, per-cell tables and Random Walk tables. */
+int storm_cuda_replay_segments(StormHandle *h, StormReplayBatch *batch);
+
+/* The Random Walk tables (radiation/RandomWalk.hpp:23-79), 1024 tau values,
+ * 1024 survival values, 1024*256 radius values; host buffers. */
+int storm_cuda_get_random_walk_tables(StormHandle *h, double *tau, double *survival, double *radius);
+/* Evaluate RandomWalk::sampleLeakTime / sampleRadius on the device for n inputs. */
+int storm_cuda_random_walk_sample(StormHandle *h, uint64_t n, const double *xi_leak, const double *tau,
+                                  const double *xi_radius, double *leak_out, double *radius_out);
+
+/* ---------------------------------------------------------------- diagnostics */
+
+/* First device error word, the cell and particle it was raised for, and a message. */
+int storm_cuda_last_error(StormHandle *h, int32_t *derr, uint64_t *cell, uint64_t *particle,
+                          char *msg, size_t msg_len);
+/* Bytes of device memory the handle holds (GetHandlerMemoryBytes). */
+int storm_cuda_memory_bytes(StormHandle *h, uint64_t *bytes);
+/* Kernel launches issued by the handle since creation (for launch accounting). */
+int storm_cuda_launch_count(StormHandle *h, uint64_t *launches);
+/* Segment-per-visit override (autotuner hook). */
+int storm_cuda_set_segments_per_visit(StormHandle *h, uint32_t k);
+const char *storm_cuda_status_string(int status);
+int storm_cuda_abi_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* STORM_CUDA_H */

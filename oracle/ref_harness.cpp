@@ -1,0 +1,656 @@
+// Test infrastructure only (the oracle's reference build).  Nothing in the
+// product links, loads or runs this file.
+//
+// Builds STORM's own serial path -- MonteCarloManagerSerial + RadiationIMC +
+// CombPopulationControl + boundary plug-ins, compiled unmodified from the
+// reference sources -- against the project-written stand-ins in oracle/shims
+// for the dependencies the reference does not vendor (Boost pieces, `units`,
+// `planck_integral`, a MadCart-compatible Cartesian grid).  It exposes a C API
+// so the tests can:
+//   * run full reference time steps on the same problem descriptor the CUDA
+//     engine takes (CPU baseline and statistical parity),
+//   * record, for every RadiationIMC::step call, the particle before/after,
+//     the tallies before/after and the exact uniforms the call drew from the
+//     reference's private std::mt19937_64 (replay parity),
+//   * probe single components (RandomWalk samplers, the in-cell and on-face
+//     position samplers, isotropic directions, comb) with recorded draws.
+//
+// The engine is reached through the opacity plug-in: RadiationIMC passes its
+// private engine by reference to getRandomVelocity (radiation/RadiationIMC.hpp:2543),
+// so the harness opacity model keeps the address on first use.  Engine states
+// compare with ==, so the draws of one step are counted by advancing a copy
+// taken before the call, and replayed through a second copy to log the doubles.
+#include <cassert>
+#include <chrono>
+#include <cstdint>
+#include <cstring>
+#include <fstream>
+#include <iostream>
+#include <memory>
+#include <random>
+#include <sstream>
+#include <string>
+#include <vector>
+
+#include "examples/Vector3D.hpp"
+#include "MadCart/CartesianMesh3D.hpp"
+#include <units/units.hpp>
+#include "radiation/RadiationIMC.hpp"
+#include "radiation/RadiationCell.hpp"
+#include "radiation/RandomWalk.hpp"
+#include "population/CombPopulationControl.hpp"
+#include "population/NoPopulationControl.hpp"
+#include "boundary/RigidBoundary.hpp"
+#include "boundary/Vacuum.hpp"
+#include "boundary/SideTemperature.hpp"
+#include "boundary/TwoSidesTemperature.hpp"
+#include "manager/MonteCarloManagerSerial.hpp"
+#include "utils/RandomInCell.hpp"
+#include "utils/RandomOnFace.hpp"
+
+#include "storm_cuda.h"
+
+using Grid = MadCart::CartesianMesh3D<Vector3D>;
+using Cell = STORM::RadiationCell;
+using Ext = STORM::SimpleExtensives;
+using MCParticle = STORM::Particle<Vector3D, Grid>;
+
+namespace {
+
+// ------------------------------------------------------------------ EOS
+// Linear EOS as examples/densmore2012/main.cpp:56-77; power law as
+// examples/marshak_wave/MarshakCommon.hpp:138-155, 162-183.
+struct HarnessEOS {
+    int kind = STORM_EOS_LINEAR;
+    double cvPerMass = 1.0, f = 1.0, beta = 1.0, mu = 0.0;
+    double dT2cv(double density, double temperature, const std::vector<double> &, const std::vector<std::string> &) const {
+        if (kind == STORM_EOS_LINEAR) return cvPerMass;
+        double cvVol = f * beta * std::pow(std::max(temperature, 1.0), beta - 1.0) * std::pow(density, 1.0 - mu);
+        return cvVol / density;
+    }
+    double de2T(double density, double specificEnergy, const std::vector<double> &, const std::vector<std::string> &) const {
+        if (kind == STORM_EOS_LINEAR) return (cvPerMass > 0.0) ? specificEnergy / cvPerMass : 0.0;
+        double energyPerVolume = specificEnergy * density;
+        double rhoFactor = std::pow(density, 1.0 - mu);
+        double ratio = std::max(energyPerVolume, 0.0) / (f * rhoFactor);
+        return std::pow(std::max(ratio, 0.0), 1.0 / beta);
+    }
+};
+
+// ------------------------------------------------------------------ opacity
+class HarnessOpacity : public STORM::RadiationOpacityModel<Vector3D, Grid, Cell, 1> {
+public:
+    using Base = STORM::RadiationOpacityModel<Vector3D, Grid, Cell, 1>;
+    int kind = STORM_OPACITY_CELL_TABLE;
+    std::vector<double> sigA, sigS, rhoFactor;
+    double kP0 = 0, kR0 = 0, alpha = 0, tFloor = 1.0, cap = 0, kevKelvin = units::kev_kelvin;
+    const std::vector<Cell> *cells = nullptr;
+    std::mt19937_64 *captured = nullptr;
+
+    double CalcPlanckOpacity(const Cell &cell) override {
+        std::size_t i = index(cell);
+        if (kind == STORM_OPACITY_CELL_TABLE) return sigA[i];
+        double tf = std::pow(kevKelvin / std::max(cell.temperature, tFloor), alpha);
+        double k = kP0 * tf * rf(i);
+        return (cap > 0.0) ? std::min(k, cap) : k;
+    }
+    double CalcScatteringOpacity(const Cell &cell) override {
+        std::size_t i = index(cell);
+        if (kind == STORM_OPACITY_CELL_TABLE) return sigS.empty() ? 0.0 : sigS[i];
+        if (!(kR0 > 0.0)) return 0.0;
+        double tf = std::pow(kevKelvin / std::max(cell.temperature, tFloor), alpha);
+        double kR = kR0 * tf * rf(i);
+        double kP = kP0 * tf * rf(i);
+        return std::max(kR - kP, 0.0);
+    }
+    Vector3D getRandomVelocity(const Cell &cell, std::mt19937_64 &rng, std::uniform_real_distribution<double> &dist) override {
+        captured = &rng;
+        return Base::getRandomVelocity(cell, rng, dist);
+    }
+    static Vector3D isotropic(std::mt19937_64 &rng, std::uniform_real_distribution<double> &dist) {
+        return Base::isotropicVelocity(rng, dist);
+    }
+
+private:
+    std::size_t index(const Cell &cell) const { return static_cast<std::size_t>(&cell - cells->data()); }
+    double rf(std::size_t i) const { return rhoFactor.empty() ? 1.0 : rhoFactor[i]; }
+};
+
+// ------------------------------------------------------------------ boundary
+// A per-box-face boundary plug-in written against STORM's BoundaryCondition
+// API (the same shape as examples/marshak_wave/MarshakBoundary.hpp): faces
+// either escape or reflect with the reference's own reflectParticleOnBoxFace;
+// faces with a source temperature emit Planck surface packets like
+// SideTemperature::generateNewBoundaryParticles (boundary/SideTemperature.hpp:114-163),
+// including TwoSidesTemperature's outside-box repair (boundary/TwoSidesTemperature.hpp:178-189).
+class HarnessBoundary : public STORM::BoundaryCondition<Vector3D, Grid> {
+public:
+    StormBoxFace faces[6];
+    bool escapeNoCheck = false;
+    double sigmaSB = units::sigma_sb, clight = units::clight;
+    double escaped = 0.0;
+    std::mt19937_64 re{0};
+
+    explicit HarnessBoundary(const Grid &g) : STORM::BoundaryCondition<Vector3D, Grid>(g) { std::memset(faces, 0, sizeof(faces)); }
+
+    STORM::ParticleStatus apply(MCParticle &particle) override {
+        if (escapeNoCheck) {
+            escaped += particle.weight;
+            return STORM::ParticleStatus::REMOVE;
+        }
+        STORM::ParticleStatus status = STORM::ParticleStatus::DONE;
+        const auto &bfs = this->grid.GetBoxFaces();
+        for (std::size_t f = 0; f < bfs.size(); ++f) {
+            Vector3D normal;
+            double faceScale = 0.0;
+            if (this->getInwardBoxFaceNormalIfClose(bfs[f], particle.location, normal, faceScale)) {
+                if (faces[f].action == STORM_FACE_ESCAPE) {
+                    escaped += particle.weight;
+                    return STORM::ParticleStatus::REMOVE;
+                }
+                if (this->reflectParticleOnBoxFace(particle, bfs[f])) status = STORM::ParticleStatus::REFLECT;
+            }
+        }
+        if (status == STORM::ParticleStatus::REFLECT) return status;
+        STORM::StormError eo("Particle is not on any boundary");
+        eo.addEntry("Particle", particle);
+        throw eo;
+    }
+
+    std::vector<MCParticle> generateNewBoundaryParticles(double fullDt) override {
+        std::uniform_real_distribution<double> unif(0, 1);
+        std::vector<MCParticle> out;
+        std::size_t N = this->grid.GetPointNo();
+        for (std::size_t i = 0; i < N; ++i) {
+            const Vector3D &point = this->grid.GetMeshPoint(i);
+            for (const std::size_t &faceIdx : this->grid.GetCellFaces(i)) {
+                const auto &nb = this->grid.GetFaceNeighbors(faceIdx);
+                std::size_t nbIdx = (nb.first == i) ? nb.second : nb.first;
+                if (!(nbIdx >= N && this->grid.IsPointOutsideBox(nbIdx))) continue;
+                Vector3D out_n = STORM::fallback::normalize(this->grid.GetMeshPoint(nbIdx) - point);
+                int bf = -1, axis = 0;
+                double sgn = 1.0;
+                if (out_n.x < -0.99) { bf = 0; axis = 0; sgn = 1.0; }
+                else if (out_n.x > 0.99) { bf = 1; axis = 0; sgn = -1.0; }
+                else if (out_n.y < -0.99) { bf = 2; axis = 1; sgn = 1.0; }
+                else if (out_n.y > 0.99) { bf = 3; axis = 1; sgn = -1.0; }
+                else if (out_n.z < -0.99) { bf = 4; axis = 2; sgn = 1.0; }
+                else if (out_n.z > 0.99) { bf = 5; axis = 2; sgn = -1.0; }
+                if (bf < 0 || !(faces[bf].source_temperature > 0.0) || faces[bf].packets_per_face == 0) continue;
+                const std::size_t Np = faces[bf].packets_per_face;
+                const double T4 = boost::math::pow<4>(faces[bf].source_temperature);
+                double energyToProduce = sigmaSB * T4 * this->grid.GetArea(faceIdx) * fullDt / Np;
+                for (std::size_t j = 0; j < Np; ++j) {
+                    out.emplace_back();
+                    MCParticle &p = out.back();
+                    p.location = STORM::RandomPointOnFace<Vector3D, Grid>(this->grid, faceIdx);
+                    double mu = std::sqrt(unif(re));
+                    double v[3];
+                    v[axis] = sgn * mu;
+                    double _1mmu = std::sqrt(1 - mu * mu);
+                    double theta = 2 * M_PI * unif(re);
+                    v[(axis + 1) % 3] = _1mmu * std::cos(theta);
+                    v[(axis + 2) % 3] = _1mmu * std::sin(theta);
+                    p.velocity = Vector3D(v[0], v[1], v[2]);
+                    p.velocity *= clight;
+                    p.frequency = 0;
+                    p.weight = energyToProduce;
+                    p.initialWeight = p.weight;
+                    p.timeLeft = fullDt * unif(re);
+                    p.cellIndex = i;
+                    if (this->grid.IsPointOutsideBox(p.location)) {
+                        Vector3D original = p.location;
+                        Vector3D direction = point - original;
+                        double t = 1e-8;
+                        while (this->grid.IsPointOutsideBox(p.location) && t < 1.0) {
+                            p.location = original + t * direction;
+                            t *= 2;
+                        }
+                        p.location = p.location + 1e-8 * (point - p.location);
+                    }
+                }
+            }
+        }
+        return out;
+    }
+};
+
+// ------------------------------------------------------------------ recording IMC
+struct Record {
+    uint64_t id;
+    uint32_t cell;
+    double before[9];   // x y z vx vy vz timeLeft weight initialWeight
+    double after[8];    // x y z vx vy vz timeLeft weight
+    int32_t status;
+    uint64_t nextCell;
+    double ematBefore, ematAfter, eradBefore, eradAfter;
+    uint64_t tapeOffset;
+    uint32_t tapeLength;
+    int32_t usedRW;
+};
+
+using IMCBase = STORM::RadiationIMC<Vector3D, Grid, Cell, Ext, HarnessEOS, 1>;
+
+class RecordingIMC : public IMCBase {
+public:
+    using IMCBase::IMCBase;
+    HarnessOpacity *opac = nullptr;
+    std::vector<Ext> *ext = nullptr;
+    bool recording = false;
+    std::size_t maxRecords = 0;
+    std::vector<Record> records;
+    std::vector<double> tape;
+
+    Functionality step(MCParticle &p, std::vector<MCParticle> &add) override {
+        if (!recording || opac == nullptr || opac->captured == nullptr || records.size() >= maxRecords)
+            return IMCBase::step(p, add);
+        Record r{};
+        r.id = p.id;
+        r.cell = static_cast<uint32_t>(p.cellIndex);
+        const std::size_t c = p.cellIndex;
+        double b[9] = {p.location.x, p.location.y, p.location.z, p.velocity.x, p.velocity.y, p.velocity.z,
+                       p.timeLeft, p.weight, p.initialWeight};
+        std::memcpy(r.before, b, sizeof(b));
+        r.eradBefore = this->getEradTimeAvg()[c];
+        r.ematBefore = (*ext)[c].internal_energy;
+        std::mt19937_64 snap = *opac->captured;
+        std::size_t rwBefore = this->getRandomWalkStepCount();
+        Functionality res = IMCBase::step(p, add);
+        std::mt19937_64 counter = snap;
+        uint32_t n = 0;
+        while (!(counter == *opac->captured)) {
+            counter.discard(1);
+            if (++n > 4096) throw STORM::StormError("recording: could not match the engine state");
+        }
+        std::uniform_real_distribution<double> dist(0.0, 1.0);
+        r.tapeOffset = tape.size();
+        r.tapeLength = n;
+        for (uint32_t k = 0; k < n; ++k) tape.push_back(dist(snap));
+        double a[8] = {p.location.x, p.location.y, p.location.z, p.velocity.x, p.velocity.y, p.velocity.z,
+                       p.timeLeft, p.weight};
+        std::memcpy(r.after, a, sizeof(a));
+        r.status = static_cast<int32_t>(res.change);
+        r.nextCell = res.nextCellIndex;
+        r.eradAfter = this->getEradTimeAvg()[c];
+        r.ematAfter = (*ext)[c].internal_energy;
+        r.usedRW = this->getRandomWalkStepCount() != rwBefore;
+        records.push_back(r);
+        return res;
+    }
+};
+
+class NullBuf : public std::streambuf {
+protected:
+    int overflow(int c) override { return c; }
+};
+
+} // namespace
+
+// ------------------------------------------------------------------ handle
+struct RefHandle {
+    std::vector<double> xe, ye, ze;
+    std::unique_ptr<Grid> grid;
+    std::vector<Cell> cells;
+    std::vector<Ext> ext;
+    std::shared_ptr<HarnessEOS> eos;
+    std::shared_ptr<HarnessOpacity> opacity;
+    std::shared_ptr<STORM::BoundaryCondition<Vector3D, Grid>> boundary;
+    HarnessBoundary *harnessBoundary = nullptr;
+    std::shared_ptr<RecordingIMC> physics;
+    std::shared_ptr<STORM::PopulationControl<Vector3D, Grid>> pop;
+    std::unique_ptr<STORM::MonteCarloManagerSerial<Vector3D, Grid>> manager;
+    std::vector<MCParticle> census;
+    std::string lastError;
+};
+
+extern "C" {
+
+typedef struct RefStepOut {
+    uint64_t initial, prestep, start, end, segments, rw_steps;
+    double wall_seconds;
+    double escaped_energy;
+} RefStepOut;
+
+// boundary_kind: 0 per-face descriptor (HarnessBoundary), 1 RigidBoundary,
+// 2 VacuumBoundary, 3 SideTemperature(faces[0]), 4 TwoSidesTemperature(faces[0], faces[1]).
+RefHandle *ref_create(const StormProblemDesc *d, int boundary_kind, char *err, size_t errlen) {
+    try {
+        auto h = std::make_unique<RefHandle>();
+        std::vector<double> xe(d->x_edges, d->x_edges + d->nx + 1), ye(d->y_edges, d->y_edges + d->ny + 1),
+            ze(d->z_edges, d->z_edges + d->nz + 1);
+        h->xe = xe; h->ye = ye; h->ze = ze;
+        h->grid = std::make_unique<Grid>(xe, ye, ze);
+        const std::size_t N = h->grid->GetPointNo();
+        h->cells.resize(N);
+        h->ext.resize(N);
+        for (std::size_t i = 0; i < N; ++i) {
+            h->cells[i].temperature = d->temperature[i];
+            h->cells[i].internalEnergy = d->cell_internal_energy ? d->cell_internal_energy[i] : d->internal_energy[i];
+            h->ext[i].mass = d->mass[i];
+            h->ext[i].internal_energy = d->internal_energy[i];
+        }
+        h->eos = std::make_shared<HarnessEOS>();
+        h->eos->kind = d->eos_kind;
+        h->eos->cvPerMass = d->cv_per_mass;
+        h->eos->f = d->eos_f;
+        h->eos->beta = d->eos_beta;
+        h->eos->mu = d->eos_mu;
+        h->opacity = std::make_shared<HarnessOpacity>();
+        auto &op = *h->opacity;
+        op.kind = d->opacity_kind;
+        op.cells = &h->cells;
+        if (d->opacity_kind == STORM_OPACITY_CELL_TABLE) {
+            op.sigA.assign(d->sigma_a, d->sigma_a + N);
+            if (d->sigma_s) op.sigS.assign(d->sigma_s, d->sigma_s + N);
+        } else {
+            op.kP0 = d->kP0; op.kR0 = d->kR0; op.alpha = d->alpha; op.tFloor = d->t_floor; op.cap = d->cap;
+            op.kevKelvin = d->kev_kelvin;
+            if (d->density_factor) op.rhoFactor.assign(d->density_factor, d->density_factor + N);
+        }
+        switch (boundary_kind) {
+        case 0: {
+            auto b = std::make_shared<HarnessBoundary>(*h->grid);
+            std::memcpy(b->faces, d->faces, sizeof(b->faces));
+            b->escapeNoCheck = d->escape_without_check != 0;
+            b->sigmaSB = d->sigma_sb;
+            b->clight = d->clight;
+            h->harnessBoundary = b.get();
+            h->boundary = b;
+            break;
+        }
+        case 1: h->boundary = std::make_shared<STORM::RigidBoundary<Vector3D, Grid>>(*h->grid); break;
+        case 2: h->boundary = std::make_shared<STORM::VacuumBoundary<Vector3D, Grid>>(*h->grid); break;
+        case 3:
+            h->boundary = std::make_shared<STORM::SideTemperature<Vector3D, Grid>>(*h->grid, d->faces[0].source_temperature,
+                                                                                   d->faces[0].packets_per_face);
+            break;
+        case 4:
+            h->boundary = std::make_shared<STORM::TwoSidesTemperature<Vector3D, Grid>>(
+                *h->grid, d->faces[0].source_temperature, d->faces[1].source_temperature, d->faces[0].packets_per_face);
+            break;
+        default: throw STORM::StormError("unknown boundary kind");
+        }
+        STORM::RadiationIMCParameters<1> p;
+        p.newPhotonsPerCell = d->new_photons_per_cell;
+        p.withRandomWalk = d->with_random_walk != 0;
+        p.rwMinCellOpticalDepth = d->rw_min_cell_optical_depth;
+        p.rwMinParticleOpticalDepth = d->rw_min_particle_optical_depth;
+        p.noHydroFeedback = d->no_hydro_feedback != 0;
+        h->physics = std::make_shared<RecordingIMC>(*h->grid, h->boundary, h->cells, h->ext, h->eos, h->opacity, p,
+                                                    STORM::DirectRadiationIMCTraits<Vector3D, Cell, Ext, 1>(),
+                                                    RandomInCellPositionSampler<Vector3D, Grid>(), d->seed);
+        h->physics->opac = h->opacity.get();
+        h->physics->ext = &h->ext;
+        if (d->comb_enabled)
+            h->pop = std::make_shared<STORM::CombPopulationControl<Vector3D, Grid>>(*h->grid, d->comb_nmin, d->comb_factor);
+        else
+            h->pop = std::make_shared<STORM::NoPopulationControl<Vector3D, Grid>>(*h->grid);
+        h->manager = std::make_unique<STORM::MonteCarloManagerSerial<Vector3D, Grid>>(*h->grid, h->physics, h->pop, h->boundary);
+        return h.release();
+    } catch (const std::exception &e) {
+        if (err && errlen) std::snprintf(err, errlen, "%s", e.what());
+        return nullptr;
+    }
+}
+
+void ref_destroy(RefHandle *h) { delete h; }
+
+const char *ref_last_error(RefHandle *h) { return h->lastError.c_str(); }
+
+int ref_step(RefHandle *h, double dt, RefStepOut *out) {
+    NullBuf nb;
+    std::streambuf *old = std::cout.rdbuf(&nb);
+    try {
+        if (h->harnessBoundary) h->harnessBoundary->escaped = 0.0;
+        auto t0 = std::chrono::steady_clock::now();
+        h->census = h->manager->step(std::move(h->census), dt);
+        auto t1 = std::chrono::steady_clock::now();
+        std::cout.rdbuf(old);
+        if (out) {
+            out->initial = h->manager->GetInitialParticleCount();
+            out->prestep = h->manager->GetPreStepParticleCount();
+            out->start = h->manager->GetStartParticleCount();
+            out->end = h->manager->GetEndParticleCount();
+            uint64_t s = 0;
+            for (auto c : h->manager->GetCellsStepsCounters()) s += c;
+            out->segments = s;
+            out->rw_steps = h->physics->getRandomWalkStepCount();
+            out->wall_seconds = std::chrono::duration<double>(t1 - t0).count();
+            out->escaped_energy = h->harnessBoundary ? h->harnessBoundary->escaped : 0.0;
+        }
+        return 0;
+    } catch (const std::exception &e) {
+        std::cout.rdbuf(old);
+        h->lastError = e.what();
+        return 1;
+    }
+}
+
+// Calls physics->preStep(dt) alone (emission included); the emitted particles
+// replace the census buffer so the tests can inspect them.
+int ref_prestep_only(RefHandle *h, double dt, uint64_t *emitted) {
+    try {
+        h->physics->updateGridData();
+        h->census = h->physics->preStep(dt);
+        if (emitted) *emitted = h->census.size();
+        return 0;
+    } catch (const std::exception &e) {
+        h->lastError = e.what();
+        return 1;
+    }
+}
+
+uint64_t ref_census_count(RefHandle *h) { return h->census.size(); }
+
+int ref_get_census(RefHandle *h, StormParticlesSoA *o) {
+    for (std::size_t k = 0; k < h->census.size() && k < o->count; ++k) {
+        const MCParticle &p = h->census[k];
+        o->x[k] = p.location.x; o->y[k] = p.location.y; o->z[k] = p.location.z;
+        o->vx[k] = p.velocity.x; o->vy[k] = p.velocity.y; o->vz[k] = p.velocity.z;
+        o->time_left[k] = p.timeLeft; o->weight[k] = p.weight; o->initial_weight[k] = p.initialWeight;
+        o->cell[k] = static_cast<uint32_t>(p.cellIndex);
+        if (o->id) o->id[k] = p.id;
+    }
+    return 0;
+}
+
+int ref_set_census(RefHandle *h, const StormParticlesSoA *in) {
+    h->census.clear();
+    for (uint64_t k = 0; k < in->count; ++k) {
+        MCParticle p;
+        p.location = Vector3D(in->x[k], in->y[k], in->z[k]);
+        p.velocity = Vector3D(in->vx[k], in->vy[k], in->vz[k]);
+        p.timeLeft = in->time_left[k];
+        p.weight = in->weight[k];
+        p.initialWeight = in->initial_weight[k];
+        p.cellIndex = in->cell[k];
+        p.frequency = 0;
+        p.id = in->id ? in->id[k] : std::numeric_limits<std::size_t>::max();
+        h->census.push_back(p);
+    }
+    return 0;
+}
+
+int ref_get_cells(RefHandle *h, double *T, double *eint, double *eradAvg, double *eradCensus, double *sigA, double *fleck,
+                  uint64_t *segs) {
+    const std::size_t N = h->grid->GetPointNo();
+    const auto &ea = h->physics->getEradTimeAvg();
+    const auto &sa = h->physics->getPlanckOpacities();
+    const auto &ff = h->physics->getFactorFleck();
+    const auto &sc = h->manager->GetCellsStepsCounters();
+    for (std::size_t i = 0; i < N; ++i) {
+        if (T) T[i] = h->cells[i].temperature;
+        if (eint) eint[i] = h->ext[i].internal_energy;
+        if (eradAvg) eradAvg[i] = i < ea.size() ? ea[i] : 0.0;
+        if (eradCensus) eradCensus[i] = h->ext[i].Erad;
+        if (sigA) sigA[i] = i < sa.size() ? sa[i] : 0.0;
+        if (fleck) fleck[i] = i < ff.size() ? ff[i] : 0.0;
+        if (segs) segs[i] = i < sc.size() ? sc[i] : 0;
+    }
+    return 0;
+}
+
+int ref_get_emission(RefHandle *h, uint64_t *photons) {
+    const auto &v = h->physics->getLastSourcePhotonsPerCell();
+    for (std::size_t i = 0; i < v.size(); ++i) photons[i] = v[i];
+    return 0;
+}
+
+// ---------------- recording
+int ref_record_begin(RefHandle *h, uint64_t maxRecords) {
+    h->physics->records.clear();
+    h->physics->tape.clear();
+    h->physics->maxRecords = maxRecords;
+    h->physics->recording = true;
+    return 0;
+}
+int ref_record_end(RefHandle *h) {
+    h->physics->recording = false;
+    return 0;
+}
+uint64_t ref_record_count(RefHandle *h) { return h->physics->records.size(); }
+uint64_t ref_record_tape_size(RefHandle *h) { return h->physics->tape.size(); }
+
+// Copies the records out as parallel arrays.  before: 9n, after: 8n,
+// tallies: 4n (emat before/after, erad before/after), tape: tape_size.
+int ref_record_get(RefHandle *h, uint64_t *id, uint32_t *cell, double *before, double *after, int32_t *status,
+                   uint64_t *nextCell, double *tallies, uint64_t *tapeOffset, uint32_t *tapeLength, int32_t *usedRW,
+                   double *tape) {
+    const auto &R = h->physics->records;
+    for (std::size_t k = 0; k < R.size(); ++k) {
+        id[k] = R[k].id;
+        cell[k] = R[k].cell;
+        std::memcpy(before + 9 * k, R[k].before, sizeof(R[k].before));
+        std::memcpy(after + 8 * k, R[k].after, sizeof(R[k].after));
+        status[k] = R[k].status;
+        nextCell[k] = R[k].nextCell;
+        tallies[4 * k + 0] = R[k].ematBefore;
+        tallies[4 * k + 1] = R[k].ematAfter;
+        tallies[4 * k + 2] = R[k].eradBefore;
+        tallies[4 * k + 3] = R[k].eradAfter;
+        tapeOffset[k] = R[k].tapeOffset;
+        tapeLength[k] = R[k].tapeLength;
+        usedRW[k] = R[k].usedRW;
+    }
+    std::memcpy(tape, h->physics->tape.data(), h->physics->tape.size() * sizeof(double));
+    return 0;
+}
+
+// ---------------- component probes
+int ref_rw_sample(uint64_t n, const double *xiLeak, const double *tau, const double *xiRad, double *leak, double *rad) {
+    static STORM::RandomWalk rw;
+    for (uint64_t k = 0; k < n; ++k) {
+        if (xiLeak) leak[k] = rw.sampleLeakTime(xiLeak[k]);
+        if (tau && xiRad) rad[k] = rw.sampleRadius(tau[k], xiRad[k]);
+    }
+    return 0;
+}
+int ref_rw_functions(uint64_t n, const double *tau, const double *x, double *survival, double *cdf) {
+    static STORM::RandomWalk rw;
+    for (uint64_t k = 0; k < n; ++k) {
+        if (survival) survival[k] = rw.computeSurvival(tau[k]);
+        if (cdf) cdf[k] = rw.computeRadialCDF(x[k], tau[k]);
+    }
+    return 0;
+}
+
+// RandomInCellPositionSampler (utils/RandomInCell.hpp:11-67) driven by a
+// seeded std::mt19937_64; the draws each call consumed are logged (tape, 4 per call).
+int ref_sample_in_cell(RefHandle *h, uint64_t n, const uint32_t *cells, uint64_t seed, double *pos, double *tape,
+                       uint32_t *ndraws) {
+    std::mt19937_64 eng(seed);
+    std::uniform_real_distribution<double> dist(0.0, 1.0);
+    RandomInCellPositionSampler<Vector3D, Grid> sampler;
+    uint64_t t = 0;
+    for (uint64_t k = 0; k < n; ++k) {
+        std::mt19937_64 snap = eng;
+        Vector3D p = sampler(*h->grid, cells[k], eng, dist);
+        pos[3 * k] = p.x; pos[3 * k + 1] = p.y; pos[3 * k + 2] = p.z;
+        std::mt19937_64 cnt = snap;
+        uint32_t m = 0;
+        while (!(cnt == eng)) { cnt.discard(1); ++m; }
+        ndraws[k] = m;
+        for (uint32_t q = 0; q < m; ++q) tape[t++] = dist(snap);
+    }
+    return 0;
+}
+
+// RadiationOpacityModel::isotropicVelocity (radiation/RadiationOpacityModel.hpp:139-150), 2 draws per call.
+int ref_isotropic(uint64_t n, uint64_t seed, double *vel, double *tape) {
+    std::mt19937_64 eng(seed);
+    std::uniform_real_distribution<double> dist(0.0, 1.0);
+    for (uint64_t k = 0; k < n; ++k) {
+        std::mt19937_64 snap = eng;
+        Vector3D v = HarnessOpacity::isotropic(eng, dist);
+        vel[3 * k] = v.x; vel[3 * k + 1] = v.y; vel[3 * k + 2] = v.z;
+        tape[2 * k] = dist(snap);
+        tape[2 * k + 1] = dist(snap);
+    }
+    return 0;
+}
+
+// RandomPointOnFace (utils/RandomOnFace.hpp:15-66) keeps a function-static
+// std::mt19937(0).  A distinct grid type gives this probe its own template
+// instance, hence its own fresh engine, which a mirror engine here tracks
+// draw for draw (3 doubles per call).
+namespace {
+struct ProbeGrid : public Grid {
+    using Grid::Grid;
+};
+} // namespace
+int ref_point_on_face(RefHandle *h, uint64_t n, const uint64_t *faces, double *pos, double *tape) {
+    static std::unique_ptr<ProbeGrid> pg;
+    static std::mt19937 mirror(0);
+    static std::uniform_real_distribution<double> mdist(0.0, 1.0);
+    pg = std::make_unique<ProbeGrid>(h->xe, h->ye, h->ze);
+    for (uint64_t k = 0; k < n; ++k) {
+        Vector3D p = STORM::RandomPointOnFace<Vector3D, ProbeGrid>(*pg, faces[k]);
+        pos[3 * k] = p.x; pos[3 * k + 1] = p.y; pos[3 * k + 2] = p.z;
+        tape[3 * k] = mdist(mirror);
+        tape[3 * k + 1] = mdist(mirror);
+        tape[3 * k + 2] = mdist(mirror);
+    }
+    return 0;
+}
+
+// CombPopulationControl::activate on a given particle list (invariant tests).
+int ref_comb(RefHandle *h, const StormParticlesSoA *in, StormParticlesSoA *out, uint64_t *outCount) {
+    try {
+        std::vector<MCParticle> v;
+        for (uint64_t k = 0; k < in->count; ++k) {
+            MCParticle p;
+            p.location = Vector3D(in->x[k], in->y[k], in->z[k]);
+            p.velocity = Vector3D(in->vx[k], in->vy[k], in->vz[k]);
+            p.timeLeft = in->time_left[k];
+            p.weight = in->weight[k];
+            p.initialWeight = in->initial_weight[k];
+            p.cellIndex = in->cell[k];
+            p.id = in->id ? in->id[k] : k;
+            v.push_back(p);
+        }
+        std::vector<MCParticle> r = h->pop->activate(v);
+        *outCount = r.size();
+        for (std::size_t k = 0; k < r.size() && k < out->count; ++k) {
+            out->x[k] = r[k].location.x; out->y[k] = r[k].location.y; out->z[k] = r[k].location.z;
+            out->vx[k] = r[k].velocity.x; out->vy[k] = r[k].velocity.y; out->vz[k] = r[k].velocity.z;
+            out->time_left[k] = r[k].timeLeft; out->weight[k] = r[k].weight; out->initial_weight[k] = r[k].initialWeight;
+            out->cell[k] = static_cast<uint32_t>(r[k].cellIndex);
+            if (out->id) out->id[k] = r[k].id;
+        }
+        return 0;
+    } catch (const std::exception &e) {
+        h->lastError = e.what();
+        return 1;
+    }
+}
+
+// The unit constants this build of the reference was compiled with.
+int ref_units(double *out) {
+    out[0] = units::clight; out[1] = units::arad; out[2] = units::sigma_sb; out[3] = units::kev_kelvin;
+    out[4] = units::k_boltz; out[5] = units::kev;
+    return 0;
+}
+
+double ref_planck_integral(double a, double b) { return planck_integral::planck_integral(a, b); }
+
+} // extern "C"

@@ -1,0 +1,216 @@
+"""Problem descriptors: the mesh, material, opacity/EOS plug-ins, boundary faces,
+IMC parameters and comb settings of one IMC problem, packed into the C ABI's
+StormProblemDesc.
+
+The builders at the bottom produce the synthetic workloads the engine is
+measured on (seeded, no external data):
+
+* ``gray_slab``  -- 100x1x1 slab on [0,1]x[0,0.01]^2, x=0 face at 1 keV,
+  vacuum at x=1, reflecting y/z, kappa_a = min(10 T_keV^-3, 1e6), constant cv.
+* ``step_cube``  -- 64^3 unit cube, kappa_a = 1 (x<0.5) / 1000 (x>=0.5) 1/cm,
+  hot face x=0 at 1 keV, vacuum elsewhere, Random Walk where kappa*dx > 10.
+"""
+from dataclasses import dataclass, field
+import numpy as np
+
+from . import _abi as A
+from .units import UNITS
+
+
+@dataclass
+class BoxFace:
+    action: int = A.FACE_REFLECT
+    source_temperature: float = 0.0     # K
+    packets_per_face: int = 0
+
+
+@dataclass
+class Problem:
+    x_edges: np.ndarray
+    y_edges: np.ndarray
+    z_edges: np.ndarray
+    temperature: np.ndarray             # K, per cell
+    mass: np.ndarray                    # g
+    internal_energy: np.ndarray         # erg (extensive)
+    cell_internal_energy: np.ndarray = None
+    opacity_kind: int = A.OPACITY_CELL_TABLE
+    sigma_a: np.ndarray = None
+    sigma_s: np.ndarray = None
+    kP0: float = 0.0
+    kR0: float = 0.0
+    alpha: float = 0.0
+    beta: float = 0.0
+    t_floor: float = 1.0
+    cap: float = 0.0
+    density_factor: np.ndarray = None
+    eos_kind: int = A.EOS_LINEAR
+    cv_per_mass: float = 1.0
+    eos_f: float = 1.0
+    eos_beta: float = 1.0
+    eos_mu: float = 0.0
+    faces: list = field(default_factory=lambda: [BoxFace() for _ in range(6)])
+    escape_without_check: bool = False
+    new_photons_per_cell: int = 1
+    with_random_walk: bool = False
+    no_hydro_feedback: bool = False
+    rw_min_cell_optical_depth: float = 25.0      # RadiationIMCParameters defaults
+    rw_min_particle_optical_depth: float = 5.0
+    comb_enabled: bool = True
+    comb_nmin: int = 20
+    comb_factor: float = 2.0
+    seed: int = 42
+    precision: int = A.PRECISION_FP64
+    capacity: int = 0
+    segments_per_visit: int = 0
+    max_rounds: int = 0
+    per_cell_segment_counters: bool = True
+    device: int = 0
+    dt: float = 1e-11
+    name: str = "problem"
+
+    @property
+    def shape(self):
+        return (len(self.x_edges) - 1, len(self.y_edges) - 1, len(self.z_edges) - 1)
+
+    @property
+    def ncells(self):
+        nx, ny, nz = self.shape
+        return nx * ny * nz
+
+    def cell_centers(self):
+        """Cell centres with the grid's own arithmetic: 0.5*(e_i + e_{i+1})."""
+        xc = 0.5 * (self.x_edges[:-1] + self.x_edges[1:])
+        yc = 0.5 * (self.y_edges[:-1] + self.y_edges[1:])
+        zc = 0.5 * (self.z_edges[:-1] + self.z_edges[1:])
+        Z, Y, X = np.meshgrid(zc, yc, xc, indexing="ij")
+        return X.ravel(), Y.ravel(), Z.ravel()
+
+    def volumes(self):
+        dx = np.diff(self.x_edges)
+        dy = np.diff(self.y_edges)
+        dz = np.diff(self.z_edges)
+        Z, Y, X = np.meshgrid(dz, dy, dx, indexing="ij")
+        return ((X * Y) * Z).ravel()
+
+    def to_desc(self):
+        """Pack into a ctypes StormProblemDesc.  The returned object keeps the
+        numpy arrays it points to alive (attribute ``_keep``)."""
+        keep = []
+
+        def arr(a, dtype=np.float64):
+            if a is None:
+                return None
+            a = np.ascontiguousarray(a, dtype=dtype)
+            keep.append(a)
+            return A.ptr(a)
+
+        d = A.StormProblemDesc()
+        d.abi_version = A.ABI_VERSION
+        d.precision = self.precision
+        nx, ny, nz = self.shape
+        d.nx, d.ny, d.nz = nx, ny, nz
+        d.x_edges = arr(self.x_edges)
+        d.y_edges = arr(self.y_edges)
+        d.z_edges = arr(self.z_edges)
+        d.temperature = arr(self.temperature)
+        d.mass = arr(self.mass)
+        d.internal_energy = arr(self.internal_energy)
+        d.cell_internal_energy = arr(self.cell_internal_energy)
+        d.opacity_kind = self.opacity_kind
+        d.eos_kind = self.eos_kind
+        d.sigma_a = arr(self.sigma_a)
+        d.sigma_s = arr(self.sigma_s)
+        d.kP0, d.kR0, d.alpha, d.beta, d.t_floor, d.cap = self.kP0, self.kR0, self.alpha, self.beta, self.t_floor, self.cap
+        d.density_factor = arr(self.density_factor)
+        d.cv_per_mass = self.cv_per_mass
+        d.eos_f, d.eos_beta, d.eos_mu = self.eos_f, self.eos_beta, self.eos_mu
+        for k, f in enumerate(self.faces):
+            d.faces[k].action = f.action
+            d.faces[k].source_temperature = f.source_temperature
+            d.faces[k].packets_per_face = f.packets_per_face
+        d.escape_without_check = int(self.escape_without_check)
+        d.new_photons_per_cell = self.new_photons_per_cell
+        d.with_random_walk = int(self.with_random_walk)
+        d.no_hydro_feedback = int(self.no_hydro_feedback)
+        d.rw_min_cell_optical_depth = self.rw_min_cell_optical_depth
+        d.rw_min_particle_optical_depth = self.rw_min_particle_optical_depth
+        d.comb_enabled = int(self.comb_enabled)
+        d.comb_nmin = self.comb_nmin
+        d.comb_factor = self.comb_factor
+        d.clight, d.arad, d.sigma_sb, d.kev_kelvin = (UNITS["clight"], UNITS["arad"], UNITS["sigma_sb"],
+                                                      UNITS["kev_kelvin"])
+        d.seed = self.seed
+        d.capacity = self.capacity
+        d.segments_per_visit = self.segments_per_visit
+        d.max_rounds = self.max_rounds
+        d.per_cell_segment_counters = int(self.per_cell_segment_counters)
+        d.device = self.device
+        d._keep = keep
+        return d
+
+
+def uniform_edges(a, b, n):
+    """a + (b - a) * i / n with the last edge exactly b (the grid's own rule)."""
+    e = np.array([a + (b - a) * i / n for i in range(n + 1)], dtype=np.float64)
+    e[n] = b
+    return e
+
+
+def _material(p, T0, cv_per_volume, density=1.0):
+    vol = p.volumes()
+    n = p.ncells
+    p.temperature = np.full(n, T0)
+    p.mass = density * vol
+    p.internal_energy = cv_per_volume * T0 * vol
+    p.cell_internal_energy = p.internal_energy.copy()
+    p.cv_per_mass = cv_per_volume / density
+    p.eos_kind = A.EOS_LINEAR
+
+
+# Densmore's volumetric heat capacity, 1e15 erg/cm^3/keV
+# (examples/densmore2012/main.cpp:142).
+CV_PER_VOLUME = 1e15 / UNITS["kev_kelvin"]
+
+
+def gray_slab(nx=100, new_photons_per_cell=50, face_packets=50000, comb_nmin=500, comb_factor=2.0,
+              seed=42, dt=1e-11, precision=A.PRECISION_FP64):
+    """Plain gray FP64 IMC slab (the reference's CPU-runnable case)."""
+    keV = UNITS["kev_kelvin"]
+    empty = np.zeros(1)
+    p = Problem(uniform_edges(0.0, 1.0, nx), uniform_edges(0.0, 0.01, 1), uniform_edges(0.0, 0.01, 1),
+                empty, empty, empty)
+    _material(p, 1e-3 * keV, CV_PER_VOLUME)
+    p.opacity_kind = A.OPACITY_POWER_LAW
+    p.kP0, p.alpha, p.cap, p.t_floor, p.kR0 = 10.0, 3.0, 1e6, 1.0, 0.0
+    p.faces = [BoxFace(A.FACE_ESCAPE, 1.0 * keV, face_packets), BoxFace(A.FACE_ESCAPE)] + \
+              [BoxFace(A.FACE_REFLECT) for _ in range(4)]
+    p.new_photons_per_cell = new_photons_per_cell
+    p.with_random_walk = False
+    p.comb_enabled = True
+    p.comb_nmin, p.comb_factor = comb_nmin, comb_factor
+    p.seed, p.dt, p.precision, p.name = seed, dt, precision, "gray_slab"
+    return p
+
+
+def step_cube(n=64, new_photons_per_cell=3, face_packets=450, comb_nmin=20, comb_factor=2.0, seed=42,
+              dt=1e-11, precision=A.PRECISION_FP64, with_random_walk=True):
+    """Two-material step-opacity cube with Random Walk."""
+    keV = UNITS["kev_kelvin"]
+    empty = np.zeros(1)
+    e = uniform_edges(0.0, 1.0, n)
+    p = Problem(e, e.copy(), e.copy(), empty, empty, empty)
+    _material(p, 0.01 * keV, CV_PER_VOLUME)
+    xc, _, _ = p.cell_centers()
+    p.opacity_kind = A.OPACITY_CELL_TABLE
+    p.sigma_a = np.where(xc < 0.5, 1.0, 1000.0)
+    p.sigma_s = np.zeros(p.ncells)
+    p.faces = [BoxFace(A.FACE_ESCAPE, 1.0 * keV, face_packets)] + [BoxFace(A.FACE_ESCAPE) for _ in range(5)]
+    p.new_photons_per_cell = new_photons_per_cell
+    p.with_random_walk = with_random_walk
+    # mean chord 4V/S = 2 dx / 3 for a cube cell: kappa*dx > 10 <=> kappa*chord > 20/3
+    p.rw_min_cell_optical_depth = 20.0 / 3.0
+    p.rw_min_particle_optical_depth = 5.0
+    p.comb_enabled = True
+    p.comb_nmin, p.comb_factor = comb_nmin, comb_factor
+    p.seed, p.dt, p.precision, p.name = seed, dt, precision, "step_cube"
+    return p
