@@ -269,6 +269,11 @@ int storm_cuda_set_census(StormHandle *h, const StormParticlesSoA *host_in);
  * must hold `capacity` entries; *count receives the census size. */
 int storm_cuda_get_census(StormHandle *h, StormParticlesSoA *host_out, uint64_t capacity, uint64_t *count);
 int storm_cuda_census_count(StormHandle *h, uint64_t *count);
+/* populationControl->activate(particles) on host particles: the result becomes
+ * the handle's census (CombPopulationControl::activate,
+ * population/CombPopulationControl.hpp:79-253; with comb disabled the
+ * particles pass unchanged, NoPopulationControl.hpp:25-28). */
+int storm_cuda_population_control(StormHandle *h, const StormParticlesSoA *host_in);
 
 /* Per-cell arrays (host, Ncells each; any pointer may be NULL):
  * temperature [K], internal_energy [erg], erad_time_avg (getEradTimeAvg(),
@@ -314,6 +319,12 @@ int storm_cuda_last_error(StormHandle *h, int32_t *derr, uint64_t *cell, uint64_
 int storm_cuda_memory_bytes(StormHandle *h, uint64_t *bytes);
 /* Kernel launches issued by the handle since creation (for launch accounting). */
 int storm_cuda_launch_count(StormHandle *h, uint64_t *launches);
+/* Per-launch CUDA-event timing of the transport kernel (off by default). When
+ * on, each transport launch is bracketed by events on the handle's stream and
+ * storm_cuda_transport_timing() returns the summed kernel time, the number of
+ * launches and the segments they ran since the last reset. */
+int storm_cuda_set_profiling(StormHandle *h, int on);
+int storm_cuda_transport_timing(StormHandle *h, double *kernel_ms, uint64_t *launches, uint64_t *segments, int reset);
 /* Segment-per-visit override (autotuner hook). */
 int storm_cuda_set_segments_per_visit(StormHandle *h, uint32_t k);
 const char *storm_cuda_status_string(int status);

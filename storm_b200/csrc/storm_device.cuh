@@ -1,0 +1,510 @@
+// Device-side building blocks of the IMC engine: counter-based random streams,
+// the per-cell / mesh context, and the FP64 segment (one RadiationIMC::step call
+// plus the serial manager's face and boundary handling).
+//
+// This translation unit is compiled with --fmad=false: every plain expression
+// rounds like the reference's x86-64 build (no contraction), and expressions keep
+// the reference's association, so on the same uniforms a segment reproduces the
+// reference bit for bit except where CUDA's log1p / expm1 / sin / cos / exp / log
+// differ from glibc by an ulp.
+#pragma once
+
+#include <cstdint>
+#include <cfloat>
+#include <math_constants.h>
+
+#include "storm_cuda.h"
+
+namespace storm {
+
+// ParticleStatus (particle/ParticleStatus.hpp:8-15)
+enum : int { NO_CELL_MOVE = 0, CELL_MOVE = 1, DONE = 2, REMOVE = 3, REFLECT = 4 };
+// outcome of a segment after the manager's handling
+enum : int { OUT_CONTINUE = 0, OUT_CENSUS = 1, OUT_CUTOFF = 2, OUT_ESCAPE = 3, OUT_ERROR = -1 };
+// random stream tags
+enum : uint32_t { TAG_TRANSPORT = 1, TAG_CELL_EMIT = 2, TAG_FACE_EMIT = 3, TAG_COMB = 4 };
+
+constexpr uint32_t OUTSIDE = 0xffffffffu;
+constexpr double EPSILON_FACE = 1e-12;       // particle/Particle.hpp:17
+constexpr double MONTECARLO_EPS = 1e-8;      // manager/MonteCarloConfig.hpp:11
+constexpr double RW_NUDGE = 1e-6;            // radiation/RadiationIMC.hpp:1211
+constexpr double RW_PI = 3.14159265358979323846;
+constexpr double TWO_PI_ISO = 6.283185307179586476925286766559;   // radiation/RadiationOpacityModel.hpp:143
+constexpr double ONE_BELOW = 0x1.fffffffffffffp-1;                  // std::nextafter(1.0, 0.0)
+constexpr int RW_TABLE = 1024;
+constexpr int RW_RADIUS = 256;
+constexpr int RW_XGRID = 512;
+constexpr int RW_SHRINK_CAP = 100000;
+
+// One box face as the host precomputes it from BoundaryCondition's helpers
+// (boundary/BoundaryCondition.hpp:61-108) with the reference's arithmetic.
+struct BoxFaceDev {
+    double raw[3];      // CrossProduct(v1 - v0, v2 - v0)
+    double unit[3];     // raw * (1 / |raw|), oriented toward the box centre
+    double on[3];       // vertices[0]
+    double thresh;      // EPSILON * faceScale^3
+    double nudge;       // 1e-6 * faceScale
+    int32_t action;     // StormFaceAction
+    int32_t valid;      // the helper's finiteness / non-degeneracy checks
+};
+
+struct RwTables {
+    const double *tau, *logTau, *surv, *radius;
+    double logMin, logMax;   // std::log(1e-8), std::log(64) as the host computes them
+};
+
+// Everything a kernel needs, passed by value.
+struct Ctx {
+    uint32_t nx, ny, nz, ncells;
+    const double *xe, *ye, *ze, *xc, *yc, *zc;
+    double X0, X1, Y0, Y1, Z0, Z1;
+    BoxFaceDev bf[6];
+    int32_t escapeNoCheck;
+    int32_t withRW;
+    int32_t noFeedback;
+    int32_t perCellCounters;
+    double clight, arad, sigmaSB, kevKelvin;
+    double rwMinParticle, rwMinCell;
+    double sourceT[6];       // source temperature of each box face [K]
+    uint32_t seedLo, seedHi, step;
+    // per-cell arrays
+    const double *sigA, *sigS, *fleck, *rwSigT;
+    const uint8_t *rwElig;
+    double *eint, *eradAvg;
+    uint32_t *segs;
+    RwTables rw;
+    int32_t *err;            // [0] code, [1] cell lo, [2] particle lo
+};
+
+// ------------------------------------------------------------------ errors
+__device__ __forceinline__ void raise_error(const Ctx &C, int code, uint32_t cell, uint32_t particle) {
+    if (atomicCAS(C.err, 0, code) == 0) {
+        C.err[1] = static_cast<int32_t>(cell);
+        C.err[2] = static_cast<int32_t>(particle);
+    }
+}
+
+// ------------------------------------------------------------------ Philox4x32-10
+// Salmon, Moraes, Dror, Shaw, "Parallel random numbers: as easy as 1, 2, 3" (SC'11).
+__device__ __forceinline__ void philox4x32_10(uint32_t c0, uint32_t c1, uint32_t c2, uint32_t c3, uint32_t k0,
+                                              uint32_t k1, uint32_t out[4]) {
+#pragma unroll
+    for (int r = 0; r < 10; ++r) {
+        uint32_t hi0 = __umulhi(0xD2511F53u, c0), lo0 = 0xD2511F53u * c0;
+        uint32_t hi1 = __umulhi(0xCD9E8D57u, c2), lo1 = 0xCD9E8D57u * c2;
+        uint32_t n0 = hi1 ^ c1 ^ k0, n2 = hi0 ^ c3 ^ k1;
+        c0 = n0; c1 = lo1; c2 = n2; c3 = lo0;
+        k0 += 0x9E3779B9u;
+        k1 += 0xBB67AE85u;
+    }
+    out[0] = c0; out[1] = c1; out[2] = c2; out[3] = c3;
+}
+
+// 52-bit uniform on the open interval: (m + 0.5) * 2^-52.
+__device__ __forceinline__ double u52(uint32_t a, uint32_t b) {
+    uint64_t m = (static_cast<uint64_t>(a >> 6) << 26) | static_cast<uint64_t>(b >> 6);
+    return (static_cast<double>(m) + 0.5) * 0x1p-52;
+}
+
+__device__ __forceinline__ double stream_uniform(uint32_t k0, uint32_t k1, uint32_t tag, uint32_t step, uint32_t pid,
+                                                 uint32_t draw) {
+    uint32_t o[4];
+    philox4x32_10(draw >> 1, pid, step, tag, k0, k1, o);
+    return (draw & 1u) ? u52(o[2], o[3]) : u52(o[0], o[1]);
+}
+
+// The engine's per-particle stream: counter (draw >> 1, pid, step, tag).
+struct PhiloxRng {
+    uint32_t k0, k1, tag, step, pid, draw;
+    uint32_t block;
+    double c0, c1;
+    __device__ __forceinline__ void init(uint32_t kk0, uint32_t kk1, uint32_t t, uint32_t s, uint32_t p, uint32_t d) {
+        k0 = kk0; k1 = kk1; tag = t; step = s; pid = p; draw = d; block = 0xffffffffu;
+    }
+    __device__ __forceinline__ double raw() {
+        uint32_t b = draw >> 1;
+        if (b != block) {
+            uint32_t o[4];
+            philox4x32_10(b, pid, step, tag, k0, k1, o);
+            c0 = u52(o[0], o[1]);
+            c1 = u52(o[2], o[3]);
+            block = b;
+        }
+        double u = (draw & 1u) ? c1 : c0;
+        ++draw;
+        return u;
+    }
+    // RadiationIMC::randomUnitOpen (radiation/RadiationIMC.hpp:700-713); a no-op on
+    // these uniforms, kept for the shared code path.
+    __device__ __forceinline__ double open() {
+        double v = raw();
+        return v <= 0.0 ? DBL_MIN : (v >= 1.0 ? ONE_BELOW : v);
+    }
+    __device__ __forceinline__ bool exhausted() const { return false; }
+};
+
+// Replay of a recorded tape of the reference's draws.
+struct TapeRng {
+    const double *tape;
+    uint32_t len, pos;
+    bool over;
+    __device__ __forceinline__ double raw() {
+        if (pos >= len) { over = true; return 0.5; }
+        return tape[pos++];
+    }
+    __device__ __forceinline__ double open() {
+        double v = raw();
+        return v <= 0.0 ? DBL_MIN : (v >= 1.0 ? ONE_BELOW : v);
+    }
+    __device__ __forceinline__ bool exhausted() const { return over; }
+};
+
+// ------------------------------------------------------------------ particle in registers
+struct PartReg {
+    double x, y, z, vx, vy, vz, t, w, w0;
+    uint32_t cell;
+};
+
+__device__ __forceinline__ void cell_ijk(const Ctx &C, uint32_t c, uint32_t &i, uint32_t &j, uint32_t &k) {
+    i = c % C.nx;
+    uint32_t r = c / C.nx;
+    j = r % C.ny;
+    k = r / C.ny;
+}
+
+// STORM::fallback::abs (elementary/PointOps.hpp:71)
+__device__ __forceinline__ double vnorm(double x, double y, double z) { return sqrt(x * x + y * y + z * z); }
+
+// ------------------------------------------------------------------ Random Walk samplers (radiation/RandomWalk.hpp:81-137)
+__device__ __forceinline__ double clampd(double v, double lo, double hi) { return v < lo ? lo : (hi < v ? hi : v); }
+
+__device__ inline double rw_sample_leak(const RwTables &T, double xi) {
+    double target = 1.0 - xi;
+    if (target >= T.surv[0]) return T.tau[0];
+    if (target <= T.surv[RW_TABLE - 1]) return T.tau[RW_TABLE - 1];
+    // std::lower_bound with comp(a, b) = a > b on the non-increasing survival table
+    uint32_t first = 0, count = RW_TABLE;
+    while (count > 0) {
+        uint32_t step = count >> 1, it = first + step;
+        if (T.surv[it] > target) { first = it + 1; count -= step + 1; } else count = step;
+    }
+    if (first == 0) return T.tau[0];
+    if (first == RW_TABLE) return T.tau[RW_TABLE - 1];
+    double S0 = T.surv[first - 1], S1 = T.surv[first];
+    double frac = (S0 - target) / (S0 - S1);
+    double l0 = T.logTau[first - 1], l1 = T.logTau[first];
+    double logT = l0 + frac * (l1 - l0);
+    return exp(logT);
+}
+
+__device__ inline double rw_sample_radius(const RwTables &T, double tau, double xi) {
+    double logTau = log(clampd(tau, 1e-8, 64.0));
+    double tauPos = (logTau - T.logMin) / (T.logMax - T.logMin) * static_cast<double>(RW_TABLE - 1);
+    uint32_t tauIdx = static_cast<uint32_t>(tauPos);
+    if (tauIdx > RW_TABLE - 2) tauIdx = RW_TABLE - 2;
+    double tauFrac = tauPos - static_cast<double>(tauIdx);
+    double xiC = clampd(xi, 0.0, 1.0);
+    double xiPos = xiC * static_cast<double>(RW_RADIUS - 1);
+    uint32_t xiIdx = static_cast<uint32_t>(xiPos);
+    if (xiIdx > RW_RADIUS - 2) xiIdx = RW_RADIUS - 2;
+    double xiFrac = xiPos - static_cast<double>(xiIdx);
+    const double *r0p = T.radius + static_cast<size_t>(tauIdx) * RW_RADIUS + xiIdx;
+    const double *r1p = r0p + RW_RADIUS;
+    double r00 = r0p[0], r01 = r0p[1], r10 = r1p[0], r11 = r1p[1];
+    double r0 = r00 + xiFrac * (r01 - r00);
+    double r1 = r10 + xiFrac * (r11 - r10);
+    return clampd(r0 + tauFrac * (r1 - r0), 0.0, 1.0);
+}
+
+// ------------------------------------------------------------------ isotropic direction
+// RadiationOpacityModel::isotropicVelocity (radiation/RadiationOpacityModel.hpp:139-150)
+template <class RNG>
+__device__ __forceinline__ void isotropic(RNG &rng, double c, double &vx, double &vy, double &vz) {
+    double theta = TWO_PI_ISO * rng.raw();
+    double cosTheta = 2.0 * rng.raw() - 1.0;
+    double s2 = 1.0 - cosTheta * cosTheta;
+    double sinTheta = sqrt(s2 > 0.0 ? s2 : 0.0);
+    double st, ct;
+    sincos(theta, &st, &ct);
+    vx = sinTheta * ct * c;
+    vy = sinTheta * st * c;
+    vz = cosTheta * c;
+}
+
+// ------------------------------------------------------------------ tallies
+// Sink for the two per-cell tallies a segment writes: the material energy
+// (extensives[cell].internal_energy) and the time-integrated radiation energy
+// (Erad_time_avg_[cell]).
+struct AtomicTally {
+    double *eint, *erad;
+    double depSum;
+    __device__ __forceinline__ void mat(uint32_t c, double v) { atomicAdd(eint + c, v); depSum += v; }
+    __device__ __forceinline__ void rad(uint32_t c, double v) { atomicAdd(erad + c, v); }
+};
+struct LocalTally {
+    double mat_, rad_;
+    __device__ __forceinline__ void mat(uint32_t, double v) { mat_ += v; }
+    __device__ __forceinline__ void rad(uint32_t, double v) { rad_ += v; }
+};
+
+// ------------------------------------------------------------------ Random Walk jump
+// RadiationIMC::tryRandomWalkStep (radiation/RadiationIMC.hpp:1065-1276), gray.
+// Returns -1 when the walk is not taken (no draws consumed), else a ParticleStatus.
+template <class RNG, class TALLY>
+__device__ inline int try_random_walk(const Ctx &C, PartReg &p, RNG &rng, TALLY &tal, double xl, double xh, double yl,
+                                      double yh, double zl, double zh, double cx, double cy, double cz) {
+    const uint32_t cell = p.cell;
+    // computeMinDistanceToFaces (:956-969) in GetCellFaces order
+    double d[6] = {p.x - xl, xh - p.x, p.y - yl, yh - p.y, p.z - zl, zh - p.z};
+    double Ro = DBL_MAX;
+#pragma unroll
+    for (int s = 0; s < 6; ++s) Ro = (d[s] < Ro) ? d[s] : Ro;
+    Ro = (Ro > 0.0) ? Ro : 0.0;
+    const double c = C.clight;
+    double sigmaT = C.rwSigT[cell];
+    double sigmaAeff = C.sigA[cell];
+    double Dphys = (sigmaT > 0.0) ? c / (3.0 * sigmaT) : 0.0;
+    bool doRW = (Ro > 0.0 && sigmaT > 0.0 && Dphys > 0.0 && Ro * sigmaT >= C.rwMinParticle);
+    if (!doRW) return -1;
+    double f = C.fleck[cell];
+    double tauLeak = rw_sample_leak(C.rw, rng.open());
+    double tLeak = tauLeak * Ro * Ro / Dphys;
+    double tCensus = p.t;
+    int ev;
+    double dt;
+    if (tLeak <= tCensus && tLeak <= DBL_MAX) { ev = 0; dt = tLeak; }
+    else if (tCensus <= DBL_MAX) { ev = 1; dt = tCensus; }
+    else { ev = 2; dt = DBL_MAX; }
+    double rate = sigmaAeff * f * c;
+    double rwExp = expm1(-dt * rate);
+    if (!C.noFeedback) tal.mat(cell, -rwExp * p.w);
+    if (rate > 0.0) tal.rad(cell, p.w * rwExp * (-1.0 / rate));
+    p.w *= 1.0 + rwExp;
+    p.t -= dt;
+    if (fabs(p.w) < p.w0 * 1e-4) {
+        if (!C.noFeedback) tal.mat(cell, p.w);
+        return REMOVE;
+    }
+    double cosTheta = 2.0 * rng.open() - 1.0;
+    double s2 = 1.0 - cosTheta * cosTheta;
+    double sinTheta = sqrt(s2 > 0.0 ? s2 : 0.0);
+    double phi = 2.0 * RW_PI * rng.open();
+    double sp, cp;
+    sincos(phi, &sp, &cp);
+    double dx = sinTheta * cp, dy = sinTheta * sp, dz = cosTheta;
+    double disp;
+    if (ev == 0) disp = Ro;
+    else {
+        double tauPos = Dphys * dt / (Ro * Ro);
+        disp = Ro * rw_sample_radius(C.rw, tauPos, rng.open());
+    }
+    if (disp > Ro * (1.0 + 1e-12)) disp = Ro;
+    const double ox = p.x, oy = p.y, oz = p.z;
+    double lx = ox + disp * dx, ly = oy + disp * dy, lz = oz + disp * dz;
+    lx = lx * (1.0 - RW_NUDGE) + RW_NUDGE * cx;
+    ly = ly * (1.0 - RW_NUDGE) + RW_NUDGE * cy;
+    lz = lz * (1.0 - RW_NUDGE) + RW_NUDGE * cz;
+    // shrink until inside every face plane (:1216-1228)
+    int guard = 0;
+    for (int s = 0; s < 6; ++s) {
+        double q;
+        switch (s) {
+        case 0: q = lx - xl; break;
+        case 1: q = xh - lx; break;
+        case 2: q = ly - yl; break;
+        case 3: q = yh - ly; break;
+        case 4: q = lz - zl; break;
+        default: q = zh - lz; break;
+        }
+        if (q < 0.0) {
+            disp *= 0.99;
+            lx = ox + disp * dx;
+            ly = oy + disp * dy;
+            lz = oz + disp * dz;
+            s = -1;
+            if (++guard > RW_SHRINK_CAP) return -2;
+        }
+    }
+    p.x = lx; p.y = ly; p.z = lz;
+    isotropic(rng, c, p.vx, p.vy, p.vz);
+    return (ev == 1) ? DONE : NO_CELL_MOVE;
+}
+
+// ------------------------------------------------------------------ physics step
+struct PhysOut {
+    int status;        // ParticleStatus or -1 error code in errCode
+    uint32_t next;     // neighbour cell or OUTSIDE (face crossings)
+    uint32_t ghost;    // Ncells + global face index when next is OUTSIDE
+    int usedRW;
+    int errCode;
+};
+
+// global face index of side s of cell (i,j,k) (the grid's face numbering)
+__device__ __forceinline__ uint32_t face_index(const Ctx &C, uint32_t i, uint32_t j, uint32_t k, int s) {
+    uint32_t nx = C.nx, ny = C.ny, nz = C.nz;
+    uint32_t nxf = (nx + 1) * ny * nz, nyf = nx * (ny + 1) * nz;
+    switch (s) {
+    case 0: return i + (nx + 1) * (j + ny * k);
+    case 1: return (i + 1) + (nx + 1) * (j + ny * k);
+    case 2: return nxf + i + nx * (j + (ny + 1) * k);
+    case 3: return nxf + i + nx * ((j + 1) + (ny + 1) * k);
+    case 4: return nxf + nyf + i + nx * (j + ny * k);
+    default: return nxf + nyf + i + nx * (j + ny * (k + 1));
+    }
+}
+
+// RadiationIMC::step (radiation/RadiationIMC.hpp:1700-1881), gray, without hydro,
+// including the face search of Particle::distanceToNearestFace
+// (particle/Particle.hpp:188-279).  For an axis-aligned cell the inward normals
+// are exact +-unit vectors, so (p_f - x).n and n.v reduce exactly to one
+// coordinate difference and one velocity component.
+template <class RNG, class TALLY>
+__device__ inline PhysOut physics_step(const Ctx &C, PartReg &p, RNG &rng, TALLY &tal) {
+    PhysOut o;
+    o.status = NO_CELL_MOVE;
+    o.next = OUTSIDE;
+    o.ghost = 0;
+    o.usedRW = 0;
+    o.errCode = 0;
+    const uint32_t cell = p.cell;
+    uint32_t i, j, k;
+    cell_ijk(C, cell, i, j, k);
+    const double xl = C.xe[i], xh = C.xe[i + 1], yl = C.ye[j], yh = C.ye[j + 1], zl = C.ze[k], zh = C.ze[k + 1];
+    const double speed = vnorm(p.vx, p.vy, p.vz);
+    const double thr = EPSILON_FACE * speed;
+    double minA = DBL_MAX;
+    int minF = -1;
+    double a;
+    if (p.vx < -thr) { a = (xl - p.x) / p.vx; if (a < minA && a > 0) { minA = a; minF = 0; } }
+    if (p.vx > thr) { a = (xh - p.x) / p.vx; if (a < minA && a > 0) { minA = a; minF = 1; } }
+    if (p.vy < -thr) { a = (yl - p.y) / p.vy; if (a < minA && a > 0) { minA = a; minF = 2; } }
+    if (p.vy > thr) { a = (yh - p.y) / p.vy; if (a < minA && a > 0) { minA = a; minF = 3; } }
+    if (p.vz < -thr) { a = (zl - p.z) / p.vz; if (a < minA && a > 0) { minA = a; minF = 4; } }
+    if (p.vz > thr) { a = (zh - p.z) / p.vz; if (a < minA && a > 0) { minA = a; minF = 5; } }
+    if (minF < 0) { o.errCode = STORM_DERR_NO_FACE; return o; }
+    uint32_t next = OUTSIDE;
+    switch (minF) {
+    case 0: next = (i > 0) ? cell - 1 : OUTSIDE; break;
+    case 1: next = (i + 1 < C.nx) ? cell + 1 : OUTSIDE; break;
+    case 2: next = (j > 0) ? cell - C.nx : OUTSIDE; break;
+    case 3: next = (j + 1 < C.ny) ? cell + C.nx : OUTSIDE; break;
+    case 4: next = (k > 0) ? cell - C.nx * C.ny : OUTSIDE; break;
+    default: next = (k + 1 < C.nz) ? cell + C.nx * C.ny : OUTSIDE; break;
+    }
+    const double tFace = minA;
+
+    if (C.withRW && C.rwElig[cell]) {
+        int r = try_random_walk(C, p, rng, tal, xl, xh, yl, yh, zl, zh, C.xc[i], C.yc[j], C.zc[k]);
+        if (r == -2) { o.errCode = STORM_DERR_RW_SHRINK; return o; }
+        if (r >= 0) { o.status = r; o.usedRW = 1; return o; }
+    }
+
+    const double c = C.clight;
+    const double absorptionOpacity = C.sigA[cell];
+    const double f = C.fleck[cell];
+    const double effectiveAbsorptionOpacity = (1.0 - f) * absorptionOpacity;
+    const double eventOpacity = C.sigS[cell] + effectiveAbsorptionOpacity;
+    const double scatteringLength = (eventOpacity > 0.0) ? 1.0 / eventOpacity : CUDART_INF;
+    const double lp = -log1p(rng.open() - 1.0);
+    const double scatteringDistance = scatteringLength * lp;
+    const double timeScattering = isfinite(scatteringDistance) ? scatteringDistance / speed : CUDART_INF;
+    // std::min_element over {face, scatter, census}: first smallest wins
+    int best = 0;
+    double dt = tFace;
+    if (timeScattering < dt) { best = 1; dt = timeScattering; }
+    if (p.t < dt) { best = 2; dt = p.t; }
+    p.t -= dt;
+    const double tmp2 = absorptionOpacity * f * c;
+    const double tmp = -dt * tmp2;
+    const double e1 = expm1(tmp);
+    double integrated = p.w * dt;
+    if (fabs(tmp2 * dt) >= 1e-12) integrated = p.w * e1 * (-1.0 / tmp2);
+    p.x += p.vx * dt;
+    p.y += p.vy * dt;
+    p.z += p.vz * dt;
+    if (!C.noFeedback) tal.mat(cell, -e1 * p.w);
+    tal.rad(cell, integrated);
+    p.w *= 1.0 + e1;
+    if (fabs(p.w) < p.w0 * 1e-3) {
+        if (!C.noFeedback) tal.mat(cell, p.w);
+        o.status = REMOVE;
+        return o;
+    }
+    if (best == 0) {
+        o.status = CELL_MOVE;
+        o.next = next;
+        if (next == OUTSIDE) o.ghost = C.ncells + face_index(C, i, j, k, minF);
+    } else if (best == 1) {
+        (void)rng.open();   // event-type draw; both branches re-scatter isotropically
+        isotropic(rng, c, p.vx, p.vy, p.vz);
+        o.status = NO_CELL_MOVE;
+    } else {
+        o.status = DONE;
+    }
+    return o;
+}
+
+// ------------------------------------------------------------------ boundary
+// BoundaryCondition::getInwardBoxFaceNormalIfClose (:61-85) with host-precomputed face data.
+__device__ __forceinline__ bool box_face_close(const BoxFaceDev &F, double x, double y, double z) {
+    if (!F.valid) return false;
+    double pd = F.raw[0] * (x - F.on[0]) + F.raw[1] * (y - F.on[1]) + F.raw[2] * (z - F.on[2]);
+    return fabs(pd) < F.thresh;
+}
+// reflectParticleOnBoxFace (:87-108)
+__device__ __forceinline__ void box_face_reflect(const BoxFaceDev &F, PartReg &p) {
+    double sd = (p.x - F.on[0]) * F.unit[0] + (p.y - F.on[1]) * F.unit[1] + (p.z - F.on[2]) * F.unit[2];
+    p.x -= sd * F.unit[0];
+    p.y -= sd * F.unit[1];
+    p.z -= sd * F.unit[2];
+    p.x += F.nudge * F.unit[0];
+    p.y += F.nudge * F.unit[1];
+    p.z += F.nudge * F.unit[2];
+    double vn = p.vx * F.unit[0] + p.vy * F.unit[1] + p.vz * F.unit[2];
+    if (vn < 0.0) {
+        double s2 = 2.0 * vn;
+        p.vx -= s2 * F.unit[0];
+        p.vy -= s2 * F.unit[1];
+        p.vz -= s2 * F.unit[2];
+    }
+}
+
+// The serial manager's handling of one RadiationIMC::step result
+// (manager/MonteCarloManagerSerial.hpp:318-369), with BoundaryCondition::apply
+// for the per-face descriptor (VacuumBoundary, RigidBoundary, SideTemperature,
+// TwoSidesTemperature all lower to it).
+__device__ __forceinline__ int manager_handle(const Ctx &C, PartReg &p, const PhysOut &o) {
+    if (o.status == CELL_MOVE) {
+        if (o.next != OUTSIDE) {
+            uint32_t i, j, k;
+            cell_ijk(C, o.next, i, j, k);
+            p.x = (1 - MONTECARLO_EPS) * p.x + MONTECARLO_EPS * C.xc[i];
+            p.y = (1 - MONTECARLO_EPS) * p.y + MONTECARLO_EPS * C.yc[j];
+            p.z = (1 - MONTECARLO_EPS) * p.z + MONTECARLO_EPS * C.zc[k];
+            p.cell = o.next;
+            return OUT_CONTINUE;
+        }
+        if (C.escapeNoCheck) return OUT_ESCAPE;
+        bool reflected = false;
+#pragma unroll
+        for (int f = 0; f < 6; ++f) {
+            if (box_face_close(C.bf[f], p.x, p.y, p.z)) {
+                if (C.bf[f].action == STORM_FACE_ESCAPE) return OUT_ESCAPE;
+                box_face_reflect(C.bf[f], p);
+                reflected = true;
+            }
+        }
+        if (!reflected) return OUT_ERROR;
+        uint32_t i, j, k;
+        cell_ijk(C, p.cell, i, j, k);
+        p.x = (1 - MONTECARLO_EPS) * p.x + MONTECARLO_EPS * C.xc[i];
+        p.y = (1 - MONTECARLO_EPS) * p.y + MONTECARLO_EPS * C.yc[j];
+        p.z = (1 - MONTECARLO_EPS) * p.z + MONTECARLO_EPS * C.zc[k];
+        return OUT_CONTINUE;
+    }
+    if (o.status == REMOVE) return OUT_CUTOFF;
+    if (o.status == DONE) return OUT_CENSUS;
+    return OUT_CONTINUE;
+}
+
+}  // namespace storm

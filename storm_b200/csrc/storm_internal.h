@@ -1,0 +1,105 @@
+// Internal interface between the host runtime (storm_runtime.cu) and the kernels
+// (storm_kernels.cu).  Not part of the C ABI.
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "storm_device.cuh"
+
+namespace storm {
+
+// Particle bank, struct of arrays.  pid keys the particle's random stream for the
+// step; draw counts the uniforms it has consumed.
+struct Bank {
+    double *x, *y, *z, *vx, *vy, *vz, *t, *w, *w0;
+    uint32_t *cell, *pid, *draw;
+};
+
+struct CellArrays {
+    double *T, *mass, *vol, *eint, *ceint;
+    double *sigA, *sigS, *fleck, *rwSigT, *eradAvg, *eradCensus, *emitE;
+    uint8_t *rwElig;
+    uint64_t *photons;
+};
+
+struct OpacityEos {
+    int32_t opacityKind, eosKind;
+    const double *tabA, *tabS, *rhoF;
+    double kP0, kR0, alpha, tFloor, cap;
+    double cvPerMass, eosF, eosBeta, eosMu;
+};
+
+// Boundary cell-faces that emit, in (cell, GetCellFaces side) order, with the
+// packet prefix offset[0..count].
+struct FaceSources {
+    const uint32_t *cell;
+    const int32_t *side;
+    const uint64_t *offset;
+    uint32_t count;
+};
+
+struct CombParams {
+    uint64_t ntotal, nmin;
+};
+
+struct DevStats {
+    unsigned long long segments, rwSteps, escaped, cutoff, census;
+    double eCensusIn, eEmitted, eDeposited, eEscaped, eCensusPre, eCensusOut, eDebit;
+};
+
+struct ReplayDev {
+    const double *in[9];
+    const uint32_t *cell;
+    const uint64_t *tapeOffset;
+    const uint32_t *tapeLength;
+    const double *tape;
+    double *phys[8];
+    int32_t *physStatus;
+    uint32_t *physNext;
+    double *dep[2];
+    double *mgr[6];
+    uint32_t *mgrCell;
+    int32_t *mgrStatus;
+    uint32_t *draws;
+    int32_t *usedRW;
+};
+
+void launch_begin(cudaStream_t s, const Bank &b, uint32_t n, double dt, DevStats *st);
+void launch_prestep(cudaStream_t s, const Ctx &C, const CellArrays &A, const OpacityEos &M, double dt);
+void launch_rw_eligibility(cudaStream_t s, const Ctx &C, const CellArrays &A);
+void launch_emission_energy(cudaStream_t s, const Ctx &C, const CellArrays &A, double dt);
+void launch_sequential_sum(cudaStream_t s, const double *v, uint32_t n, double *out);
+void launch_allocate(cudaStream_t s, const Ctx &C, const CellArrays &A, const double *total, uint64_t newPerCell);
+void launch_emission_debit(cudaStream_t s, const Ctx &C, const CellArrays &A, DevStats *st);
+void launch_scan_u64(cudaStream_t s, const uint64_t *in, uint32_t n, uint64_t *out, uint64_t *tileSums, uint64_t *total);
+void launch_emit_cells(cudaStream_t s, const Ctx &C, const CellArrays &A, const uint64_t *offsets, uint64_t total,
+                       const Bank &b, uint32_t bankBase, double dt, DevStats *st);
+void launch_emit_faces(cudaStream_t s, const Ctx &C, const FaceSources &F, uint64_t total, const Bank &b,
+                       uint32_t bankBase, double dt, DevStats *st);
+void launch_transport(cudaStream_t s, uint32_t grid, const Ctx &C, const Bank &in, const uint32_t *nIn, const Bank &out,
+                      uint32_t *nOut, const Bank &cen, uint32_t *nCen, uint32_t K, DevStats *st);
+void launch_comb_keys(cudaStream_t s, const Ctx &C, const Bank &cen, uint32_t n, uint64_t *keys, uint32_t *vals,
+                      uint32_t combKey);
+int launch_radix_sort(cudaStream_t s, uint64_t *keys, uint32_t *vals, uint64_t *keysAlt, uint32_t *valsAlt, uint32_t n,
+                      int bits, uint32_t *tileHist);
+uint32_t radix_tile_count(uint32_t n);
+void launch_comb_ranges(cudaStream_t s, const uint64_t *keys, uint32_t n, uint32_t ncells, uint32_t *start);
+void launch_comb_cell_sums(cudaStream_t s, const Bank &cen, const uint32_t *idx, const uint32_t *start, uint32_t ncells,
+                           double *W);
+void launch_blocked_sum(cudaStream_t s, const double *v, uint32_t n, double *out);
+void launch_comb_count(cudaStream_t s, const Ctx &C, const CombParams &P, const Bank &cen, const uint32_t *idx,
+                       const uint32_t *start, const double *W, const double *Wtot, uint64_t *outCount);
+void launch_comb_write(cudaStream_t s, const Ctx &C, const CombParams &P, const Bank &cen, const uint32_t *idx,
+                       const uint32_t *start, const double *W, const double *Wtot, const uint64_t *outOffset,
+                       const Bank &out, double *eradCensus, DevStats *st);
+void launch_census_keys_pid(cudaStream_t s, const Bank &cen, uint32_t n, uint64_t *keys, uint32_t *vals);
+void launch_gather(cudaStream_t s, const Bank &src, const uint32_t *idx, uint32_t n, const Bank &dst, double *eradCensus,
+                   DevStats *st);
+void launch_poststep(cudaStream_t s, const Ctx &C, const CellArrays &A, const OpacityEos &M, double dt);
+void launch_replay(cudaStream_t s, const Ctx &C, const ReplayDev &R, uint32_t n);
+void launch_rw_radius(cudaStream_t s, const double *tau, const double *surv, double *radius);
+void launch_rw_sample(cudaStream_t s, const RwTables &T, uint32_t n, const double *xiLeak, const double *tau,
+                      const double *xiRad, double *leak, double *rad);
+
+}  // namespace storm

@@ -1,0 +1,1038 @@
+// sm_100a kernels of the IMC time step.  Compiled with --fmad=false (see
+// storm_device.cuh).  Each kernel names the reference lines it implements.
+#include <cuda_runtime.h>
+#include <math_constants.h>
+
+#include "storm_device.cuh"
+#include "storm_internal.h"
+
+namespace storm {
+
+constexpr unsigned FULL = 0xffffffffu;
+
+__device__ __forceinline__ unsigned lanemask_lt() {
+    unsigned m;
+    asm("mov.u32 %0, %%lanemask_lt;" : "=r"(m));
+    return m;
+}
+
+template <class T>
+__device__ __forceinline__ T warp_sum(T v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(FULL, v, o);
+    return v;
+}
+
+// ------------------------------------------------------------------ bank access
+__device__ __forceinline__ void load_part(const Bank &b, uint32_t q, PartReg &p) {
+    p.x = b.x[q]; p.y = b.y[q]; p.z = b.z[q];
+    p.vx = b.vx[q]; p.vy = b.vy[q]; p.vz = b.vz[q];
+    p.t = b.t[q]; p.w = b.w[q]; p.w0 = b.w0[q];
+    p.cell = b.cell[q];
+}
+__device__ __forceinline__ void store_part(const Bank &b, uint32_t q, const PartReg &p, uint32_t pid, uint32_t draw) {
+    b.x[q] = p.x; b.y[q] = p.y; b.z[q] = p.z;
+    b.vx[q] = p.vx; b.vy[q] = p.vy; b.vz[q] = p.vz;
+    b.t[q] = p.t; b.w[q] = p.w; b.w0[q] = p.w0;
+    b.cell[q] = p.cell; b.pid[q] = pid; b.draw[q] = draw;
+}
+
+// ------------------------------------------------------------------ step start
+// manager step() (manager/MonteCarloManagerSerial.hpp:393-405): census particles
+// get timeLeft = dt, initialWeight = |w|; they take pids 0..n-1.
+__global__ void k_begin(Bank b, uint32_t n, double dt, DevStats *st) {
+    double e = 0.0;
+    for (uint32_t q = blockIdx.x * blockDim.x + threadIdx.x; q < n; q += gridDim.x * blockDim.x) {
+        double w = b.w[q];
+        b.t[q] = dt;
+        b.w0[q] = fabs(w);
+        b.pid[q] = q;
+        b.draw[q] = 0;
+        e += w;
+    }
+    e = warp_sum(e);
+    if ((threadIdx.x & 31) == 0 && e != 0.0) atomicAdd(&st->eCensusIn, e);
+}
+
+// ------------------------------------------------------------------ prestep
+// RadiationIMC::preStep (radiation/RadiationIMC.hpp:1618-1661) per cell, the opacity
+// plug-in (CalcPlanckOpacity / CalcScatteringOpacity) and precomputeRandomWalkData
+// (:982-1006, gray branch); clears Erad_time_avg_.
+__global__ void k_prestep(Ctx C, CellArrays A, OpacityEos M, double dt) {
+    for (uint32_t c = blockIdx.x * blockDim.x + threadIdx.x; c < C.ncells; c += gridDim.x * blockDim.x) {
+        double sa, ss;
+        const double T = A.T[c];
+        if (M.opacityKind == STORM_OPACITY_CELL_TABLE) {
+            sa = M.tabA[c];
+            ss = M.tabS ? M.tabS[c] : 0.0;
+        } else {
+            double tmax = T < M.tFloor ? M.tFloor : T;   // std::max(T, floor)
+            double tf = pow(C.kevKelvin / tmax, M.alpha);
+            double rf = M.rhoF ? M.rhoF[c] : 1.0;
+            double kk = M.kP0 * tf * rf;
+            sa = (M.cap > 0.0) ? (M.cap < kk ? M.cap : kk) : kk;
+            if (M.kR0 > 0.0) {
+                double kR = M.kR0 * tf * rf, kP = M.kP0 * tf * rf;
+                double sd = kR - kP;
+                ss = sd > 0.0 ? sd : 0.0;   // std::max(kR - kP, 0)
+            } else {
+                ss = 0.0;
+            }
+        }
+        A.sigA[c] = sa;
+        A.sigS[c] = ss;
+        A.eradAvg[c] = 0.0;
+        double cv;
+        if (M.eosKind == STORM_EOS_LINEAR) {
+            cv = M.cvPerMass;
+        } else {
+            double rho = A.mass[c] / A.vol[c];
+            double Tm = T < 1.0 ? 1.0 : T;
+            cv = M.eosF * M.eosBeta * pow(Tm, M.eosBeta - 1.0) * pow(rho, 1.0 - M.eosMu) / rho;
+        }
+        double T3 = (T * T) * T;   // boost::math::pow<3>
+        double f = 1.0 / (1.0 + (4.0 * C.arad * T3 * sa * C.clight * dt * 1.0) / cv);
+        A.fleck[c] = f;
+        if (f < 0.0 || f > 1.0) raise_error(C, STORM_DERR_FLECK, c, 0);
+        if (C.withRW) {
+            double sigmaT = sa + ss;
+            A.rwSigT[c] = sigmaT;
+            uint32_t i, j, k;
+            cell_ijk(C, c, i, j, k);
+            double dx = C.xe[i + 1] - C.xe[i], dy = C.ye[j + 1] - C.ye[j], dz = C.ze[k + 1] - C.ze[k];
+            double ax = dy * dz, ay = dz * dx, az = dx * dy;
+            double S = 0.0;   // computeCellSurfaceArea (:971-980) in GetCellFaces order
+            S += ax; S += ax; S += ay; S += ay; S += az; S += az;
+            double chord = (S > 0.0) ? 4.0 * A.vol[c] / S : 0.0;
+            A.rwElig[c] = (sigmaT * chord >= C.rwMinCell) ? 1 : 0;
+        }
+    }
+}
+
+// RW eligibility from externally supplied tables (storm_cuda_set_cell_physics).
+__global__ void k_rw_eligibility(Ctx C, CellArrays A) {
+    for (uint32_t c = blockIdx.x * blockDim.x + threadIdx.x; c < C.ncells; c += gridDim.x * blockDim.x) {
+        double sigmaT = A.sigA[c] + A.sigS[c];
+        A.rwSigT[c] = sigmaT;
+        uint32_t i, j, k;
+        cell_ijk(C, c, i, j, k);
+        double dx = C.xe[i + 1] - C.xe[i], dy = C.ye[j + 1] - C.ye[j], dz = C.ze[k + 1] - C.ze[k];
+        double ax = dy * dz, ay = dz * dx, az = dx * dy;
+        double S = 0.0;
+        S += ax; S += ax; S += ay; S += ay; S += az; S += az;
+        double chord = (S > 0.0) ? 4.0 * A.vol[c] / S : 0.0;
+        A.rwElig[c] = (sigmaT * chord >= C.rwMinCell) ? 1 : 0;
+    }
+}
+
+// ------------------------------------------------------------------ emission allocation
+// generateParticles (radiation/RadiationIMC.hpp:2047-2059): energy per cell.
+__global__ void k_emission_energy(Ctx C, CellArrays A, double dt) {
+    for (uint32_t c = blockIdx.x * blockDim.x + threadIdx.x; c < C.ncells; c += gridDim.x * blockDim.x) {
+        double T = A.T[c];
+        double T4 = (T * T) * (T * T);   // boost::math::pow<4>
+        A.emitE[c] = A.fleck[c] * A.vol[c] * C.arad * T4 * A.sigA[c] * dt * C.clight;
+    }
+}
+
+// localTotalEnergy += energyToCreateVec[i] (:2058-2059) in the reference's order:
+// one thread adds the cells left to right so the allocation below floors against
+// the same total, bit for bit.  A warp streams the values through shared memory.
+__global__ void k_sequential_sum(const double *v, uint32_t n, double *out) {
+    __shared__ double buf[1024];
+    double s = 0.0;
+    for (uint32_t base = 0; base < n; base += 1024) {
+        for (uint32_t q = threadIdx.x; q < 1024 && base + q < n; q += blockDim.x) buf[q] = v[base + q];
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            uint32_t m = (n - base) < 1024 ? (n - base) : 1024;
+            for (uint32_t q = 0; q < m; ++q) s += buf[q];
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) *out = s;
+}
+
+// nPhotonsVec (:2071-2087)
+__global__ void k_allocate(Ctx C, CellArrays A, const double *total, uint64_t newPerCell) {
+    const double tot = *total;
+    const uint64_t totalParticles = static_cast<uint64_t>(C.ncells) * newPerCell * 10;
+    for (uint32_t c = blockIdx.x * blockDim.x + threadIdx.x; c < C.ncells; c += gridDim.x * blockDim.x) {
+        double E = A.emitE[c];
+        uint64_t share = (tot > 0) ? static_cast<uint64_t>(E / tot * static_cast<double>(totalParticles)) : newPerCell;
+        uint64_t cap = newPerCell * 20;
+        uint64_t m = share < cap ? share : cap;
+        A.photons[c] = (E > 0.0) ? (m > newPerCell ? m : newPerCell) : 0;
+    }
+}
+
+// material debit (:2193-2195)
+__global__ void k_emission_debit(Ctx C, CellArrays A, DevStats *st) {
+    double deb = 0.0;
+    for (uint32_t c = blockIdx.x * blockDim.x + threadIdx.x; c < C.ncells; c += gridDim.x * blockDim.x) {
+        if (A.photons[c] == 0) continue;
+        double E = A.emitE[c];
+        if (!C.noFeedback) A.eint[c] -= E;
+        deb += E;
+    }
+    deb = warp_sum(deb);
+    if ((threadIdx.x & 31) == 0 && deb != 0.0) atomicAdd(&st->eDebit, deb);
+}
+
+// ------------------------------------------------------------------ exclusive scan (uint64)
+// Three phases: per-block inclusive scan of 1024-element tiles, scan of the tile
+// totals by one block, add-back.  Output out[0..n] with out[n] = total.
+__device__ __forceinline__ uint64_t block_scan_incl(uint64_t v, uint64_t *sh) {
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        uint64_t y = __shfl_up_sync(FULL, v, o);
+        if (lane >= o) v += y;
+    }
+    if (lane == 31) sh[wid] = v;
+    __syncthreads();
+    if (wid == 0) {
+        uint64_t s = (lane < (blockDim.x >> 5)) ? sh[lane] : 0;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            uint64_t y = __shfl_up_sync(FULL, s, o);
+            if (lane >= o) s += y;
+        }
+        sh[lane] = s;
+    }
+    __syncthreads();
+    if (wid > 0) v += sh[wid - 1];
+    __syncthreads();
+    return v;
+}
+__global__ void k_scan_tiles(const uint64_t *in, uint32_t n, uint64_t *out, uint64_t *tileSums) {
+    __shared__ uint64_t sh[32];
+    uint32_t q = blockIdx.x * blockDim.x + threadIdx.x;
+    uint64_t v = q < n ? in[q] : 0;
+    uint64_t inc = block_scan_incl(v, sh);
+    if (q < n) out[q] = inc - v;
+    if (threadIdx.x == blockDim.x - 1) tileSums[blockIdx.x] = inc;
+}
+__global__ void k_scan_sums(uint64_t *tileSums, uint32_t ntiles, uint64_t *total) {
+    __shared__ uint64_t sh[32];
+    __shared__ uint64_t last;
+    uint64_t carry = 0;
+    for (uint32_t base = 0; base < ntiles; base += blockDim.x) {
+        uint32_t q = base + threadIdx.x;
+        uint64_t v = q < ntiles ? tileSums[q] : 0;
+        uint64_t inc = block_scan_incl(v, sh);
+        if (q < ntiles) tileSums[q] = carry + inc - v;
+        if (threadIdx.x == blockDim.x - 1) last = inc;
+        __syncthreads();
+        carry += last;
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) *total = carry;
+}
+__global__ void k_scan_add(uint64_t *out, uint32_t n, const uint64_t *tileSums, const uint64_t *total) {
+    uint32_t q = blockIdx.x * blockDim.x + threadIdx.x;
+    if (q < n) out[q] += tileSums[blockIdx.x];
+    if (q == 0) out[n] = *total;
+}
+
+// ------------------------------------------------------------------ samplers
+// Vertex coordinates of side s of cell (i,j,k) in the grid's GetPointsInFace order.
+__device__ __forceinline__ void face_vertices(const Ctx &C, uint32_t i, uint32_t j, uint32_t k, int s, double q[4][3]) {
+    int axis = s >> 1, hi = s & 1;
+    if (axis == 0) {
+        double X = C.xe[i + hi];
+        double y0 = C.ye[j], y1 = C.ye[j + 1], z0 = C.ze[k], z1 = C.ze[k + 1];
+        q[0][0] = X; q[0][1] = y0; q[0][2] = z0;
+        q[1][0] = X; q[1][1] = y1; q[1][2] = z0;
+        q[2][0] = X; q[2][1] = y1; q[2][2] = z1;
+        q[3][0] = X; q[3][1] = y0; q[3][2] = z1;
+    } else if (axis == 1) {
+        double Y = C.ye[j + hi];
+        double x0 = C.xe[i], x1 = C.xe[i + 1], z0 = C.ze[k], z1 = C.ze[k + 1];
+        q[0][0] = x0; q[0][1] = Y; q[0][2] = z0;
+        q[1][0] = x0; q[1][1] = Y; q[1][2] = z1;
+        q[2][0] = x1; q[2][1] = Y; q[2][2] = z1;
+        q[3][0] = x1; q[3][1] = Y; q[3][2] = z0;
+    } else {
+        double Z = C.ze[k + hi];
+        double x0 = C.xe[i], x1 = C.xe[i + 1], y0 = C.ye[j], y1 = C.ye[j + 1];
+        q[0][0] = x0; q[0][1] = y0; q[0][2] = Z;
+        q[1][0] = x1; q[1][1] = y0; q[1][2] = Z;
+        q[2][0] = x1; q[2][1] = y1; q[2][2] = Z;
+        q[3][0] = x0; q[3][1] = y1; q[3][2] = Z;
+    }
+}
+
+// RandomInCellPositionSampler::operator() (utils/RandomInCell.hpp:11-67): pick one
+// of the 12 fan tetrahedra by volume, then a uniform point in it.
+template <class RNG>
+__device__ inline void sample_in_cell(const Ctx &C, uint32_t cell, RNG &rng, double &px, double &py, double &pz) {
+    uint32_t i, j, k;
+    cell_ijk(C, cell, i, j, k);
+    const double cx = C.xc[i], cy = C.yc[j], cz = C.zc[k];
+    double cum[12];
+    double total = 0.0;
+#pragma unroll
+    for (int s = 0; s < 6; ++s) {
+        double q[4][3];
+        face_vertices(C, i, j, k, s, q);
+#pragma unroll
+        for (int t = 1; t < 3; ++t) {
+            double ax = q[0][0] - cx, ay = q[0][1] - cy, az = q[0][2] - cz;
+            double bx = q[t][0] - cx, by = q[t][1] - cy, bz = q[t][2] - cz;
+            double ex = q[t + 1][0] - cx, ey = q[t + 1][1] - cy, ez = q[t + 1][2] - cz;
+            double crx = by * ez - bz * ey, cry = bz * ex - bx * ez, crz = bx * ey - by * ex;
+            double vol = fabs(ax * crx + ay * cry + az * crz);
+            total += vol;
+            cum[2 * s + (t - 1)] = total;
+        }
+    }
+    double r = rng.raw() * total;
+    // std::lower_bound over the 12 cumulative volumes
+    uint32_t first = 0, count = 12;
+    while (count > 0) {
+        uint32_t step = count >> 1, it = first + step;
+        if (cum[it] < r) { first = it + 1; count -= step + 1; } else count = step;
+    }
+    if (first >= 12) first = 11;
+    double s = rng.raw(), t = rng.raw(), u = rng.raw(), tmp;
+    if (s > t) { tmp = s; s = t; t = tmp; }
+    if (t > u) { tmp = t; t = u; u = tmp; }
+    if (s > t) { tmp = s; s = t; t = tmp; }
+    const int side = first >> 1, tri = (first & 1) + 1;
+    double q[4][3];
+    face_vertices(C, i, j, k, side, q);
+    const double a0 = s, a1 = t - s, a2 = u - t, a3 = 1 - u;
+    px = a0 * q[0][0] + a1 * q[tri][0] + a2 * q[tri + 1][0] + a3 * cx;
+    py = a0 * q[0][1] + a1 * q[tri][1] + a2 * q[tri + 1][1] + a3 * cy;
+    pz = a0 * q[0][2] + a1 * q[tri][2] + a2 * q[tri + 1][2] + a3 * cz;
+}
+
+// RandomPointOnFace (utils/RandomOnFace.hpp:15-66) for a quad face.
+template <class RNG>
+__device__ inline void point_on_face(const double q[4][3], RNG &rng, double &px, double &py, double &pz) {
+    double cum[2];
+    double total = 0;
+#pragma unroll
+    for (int t = 1; t < 3; ++t) {
+        double ux = q[t][0] - q[0][0], uy = q[t][1] - q[0][1], uz = q[t][2] - q[0][2];
+        double vx = q[t + 1][0] - q[0][0], vy = q[t + 1][1] - q[0][1], vz = q[t + 1][2] - q[0][2];
+        double cx = uy * vz - uz * vy, cy = uz * vx - ux * vz, cz = ux * vy - uy * vx;
+        total += sqrt(cx * cx + cy * cy + cz * cz);
+        cum[t - 1] = total;
+    }
+    double r = rng.raw() * total;
+    int idx = (cum[0] < r) ? 1 : 0;   // lower_bound over two entries
+    if (idx == 1 && cum[1] < r) idx = 2;
+    if (idx >= 2) idx = 1;
+    double r1 = rng.raw(), r2 = rng.raw();
+    if (r1 + r2 > 1) { r1 = 1 - r1; r2 = 1 - r2; }
+    const double a0 = 1 - r1 - r2;
+    px = a0 * q[0][0] + r1 * q[idx + 1][0] + r2 * q[idx + 2][0];
+    py = a0 * q[0][1] + r1 * q[idx + 1][1] + r2 * q[idx + 2][1];
+    pz = a0 * q[0][2] + r1 * q[idx + 1][2] + r2 * q[idx + 2][2];
+}
+
+__device__ __forceinline__ bool outside_box(const Ctx &C, double x, double y, double z) {
+    return x < C.X0 || x > C.X1 || y < C.Y0 || y > C.Y1 || z < C.Z0 || z > C.Z1;
+}
+
+// outside-box repair of generateSingleParticle (radiation/RadiationIMC.hpp:2528-2541)
+// and TwoSidesTemperature (boundary/TwoSidesTemperature.hpp:178-189)
+__device__ __forceinline__ void repair_outside(const Ctx &C, double &x, double &y, double &z, double mx, double my,
+                                               double mz) {
+    if (!outside_box(C, x, y, z)) return;
+    const double ox = x, oy = y, oz = z, dx = mx - ox, dy = my - oy, dz = mz - oz;
+    double t = 1e-8;
+    int guard = 0;
+    while (outside_box(C, x, y, z) && t < 1.0 && guard++ < 64) {
+        x = ox + t * dx; y = oy + t * dy; z = oz + t * dz;
+        t *= 2;
+    }
+    x = x + 1e-8 * (mx - x);
+    y = y + 1e-8 * (my - y);
+    z = z + 1e-8 * (mz - z);
+}
+
+// ------------------------------------------------------------------ cell emission
+// generateParticles per-photon loop (radiation/RadiationIMC.hpp:2405-2506) with
+// generateSingleParticle (:2516-2553).  Packet e of cell c draws from stream
+// (TAG_CELL_EMIT, step, e): 4 position, 2 direction, 1 time.
+__global__ void k_emit_cells(Ctx C, CellArrays A, const uint64_t *offsets, uint64_t total, Bank b, uint32_t bankBase,
+                             double dt, DevStats *st) {
+    double esum = 0.0;
+    for (uint64_t e = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; e < total; e += (uint64_t)gridDim.x * blockDim.x) {
+        // last cell whose offset <= e
+        uint32_t lo = 0, hi = C.ncells;   // offsets has ncells + 1 entries
+        while (lo < hi) {
+            uint32_t mid = (lo + hi) >> 1;
+            if (offsets[mid] <= e) lo = mid + 1; else hi = mid;
+        }
+        const uint32_t c = lo - 1;
+        const uint64_t np = A.photons[c];
+        const double energyPerPhoton = A.emitE[c] * 1.0 / static_cast<double>(np);
+        PhiloxRng rng;
+        rng.init(C.seedLo, C.seedHi, TAG_CELL_EMIT, C.step, static_cast<uint32_t>(e), 0);
+        PartReg p;
+        p.cell = c;
+        sample_in_cell(C, c, rng, p.x, p.y, p.z);
+        uint32_t i, j, k;
+        cell_ijk(C, c, i, j, k);
+        repair_outside(C, p.x, p.y, p.z, C.xc[i], C.yc[j], C.zc[k]);
+        isotropic(rng, C.clight, p.vx, p.vy, p.vz);
+        p.t = dt * rng.open();
+        p.w = energyPerPhoton;
+        p.w0 = fabs(p.w);
+        store_part(b, bankBase + static_cast<uint32_t>(e), p, bankBase + static_cast<uint32_t>(e), 0);
+        esum += p.w;
+    }
+    esum = warp_sum(esum);
+    if ((threadIdx.x & 31) == 0 && esum != 0.0) atomicAdd(&st->eEmitted, esum);
+}
+
+// ------------------------------------------------------------------ face emission
+// SideTemperature / TwoSidesTemperature::generateNewBoundaryParticles
+// (boundary/SideTemperature.hpp:114-163, TwoSidesTemperature.hpp:126-199) for the
+// per-face descriptor.  Face packet f draws from (TAG_FACE_EMIT, step, f):
+// 3 position, mu, theta, time.
+__global__ void k_emit_faces(Ctx C, FaceSources F, uint64_t total, Bank b, uint32_t bankBase, double dt,
+                             DevStats *st) {
+    double esum = 0.0;
+    for (uint64_t f = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; f < total; f += (uint64_t)gridDim.x * blockDim.x) {
+        uint32_t lo = 0, hi = F.count;
+        while (lo < hi) {
+            uint32_t mid = (lo + hi) >> 1;
+            if (F.offset[mid] <= f) lo = mid + 1; else hi = mid;
+        }
+        const uint32_t q = lo - 1;
+        const uint32_t c = F.cell[q];
+        const int side = F.side[q];
+        const int axis = side >> 1;
+        const double sgn = (side & 1) ? -1.0 : 1.0;
+        const uint64_t Np = F.offset[q + 1] - F.offset[q];
+        const double Tf = C.sourceT[side];
+        const double T4 = (Tf * Tf) * (Tf * Tf);
+        uint32_t i, j, k;
+        cell_ijk(C, c, i, j, k);
+        const double dx = C.xe[i + 1] - C.xe[i], dy = C.ye[j + 1] - C.ye[j], dz = C.ze[k + 1] - C.ze[k];
+        const double area = axis == 0 ? dy * dz : (axis == 1 ? dz * dx : dx * dy);
+        const double energy = C.sigmaSB * T4 * area * dt / static_cast<double>(Np);
+        PhiloxRng rng;
+        rng.init(C.seedLo, C.seedHi, TAG_FACE_EMIT, C.step, static_cast<uint32_t>(f), 0);
+        double qv[4][3];
+        face_vertices(C, i, j, k, side, qv);
+        PartReg p;
+        point_on_face(qv, rng, p.x, p.y, p.z);
+        const double mu = sqrt(rng.raw());
+        double v[3];
+        v[axis] = sgn * mu;
+        const double one_m = sqrt(1 - mu * mu);
+        const double theta = 2 * 3.14159265358979323846 * rng.raw();
+        double stt, ctt;
+        sincos(theta, &stt, &ctt);
+        v[(axis + 1) % 3] = one_m * ctt;
+        v[(axis + 2) % 3] = one_m * stt;
+        p.vx = v[0] * C.clight; p.vy = v[1] * C.clight; p.vz = v[2] * C.clight;
+        p.w = energy;
+        p.t = dt * rng.raw();
+        p.cell = c;
+        repair_outside(C, p.x, p.y, p.z, C.xc[i], C.yc[j], C.zc[k]);
+        p.w0 = fabs(p.w);
+        const uint32_t slot = bankBase + static_cast<uint32_t>(f);
+        store_part(b, slot, p, slot, 0);
+        esum += p.w;
+    }
+    esum = warp_sum(esum);
+    if ((threadIdx.x & 31) == 0 && esum != 0.0) atomicAdd(&st->eEmitted, esum);
+}
+
+// ------------------------------------------------------------------ transport
+// One bank visit of the HandleAll loop (manager/MonteCarloManagerSerial.hpp:267-383):
+// every active particle runs up to K segments in registers; survivors are
+// compacted into the next bank and census particles appended to the census bank
+// (warp ballot + one atomic per warp).
+__global__ void __launch_bounds__(256) k_transport(Ctx C, Bank in, const uint32_t *nIn, Bank out, uint32_t *nOut,
+                                                   Bank cen, uint32_t *nCen, uint32_t K, DevStats *st) {
+    const uint32_t n = *nIn;
+    const unsigned lane = threadIdx.x & 31;
+    unsigned long long segs = 0, rw = 0, esc = 0, cut = 0, ncen = 0;
+    double dep = 0.0, eEsc = 0.0, eCen = 0.0;
+    for (uint32_t base = blockIdx.x * blockDim.x; base < n; base += gridDim.x * blockDim.x) {
+        const uint32_t idx = base + threadIdx.x;
+        const bool active = idx < n;
+        PartReg p;
+        uint32_t pid = 0, draw = 0;
+        int outcome = OUT_CONTINUE;
+        if (active) {
+            load_part(in, idx, p);
+            pid = in.pid[idx];
+            draw = in.draw[idx];
+            PhiloxRng rng;
+            rng.init(C.seedLo, C.seedHi, TAG_TRANSPORT, C.step, pid, draw);
+            AtomicTally tal{C.eint, C.eradAvg, 0.0};
+            for (uint32_t s = 0; s < K; ++s) {
+                if (C.perCellCounters) atomicAdd(C.segs + p.cell, 1u);
+                ++segs;
+                const uint32_t cell0 = p.cell;
+                PhysOut o = physics_step(C, p, rng, tal);
+                if (o.errCode) {
+                    raise_error(C, o.errCode, cell0, pid);
+                    outcome = OUT_ERROR;
+                    break;
+                }
+                rw += o.usedRW;
+                outcome = manager_handle(C, p, o);
+                if (outcome != OUT_CONTINUE) {
+                    if (outcome == OUT_ERROR) raise_error(C, STORM_DERR_NOT_ON_BOUNDARY, cell0, pid);
+                    break;
+                }
+            }
+            draw = rng.draw;
+            dep += tal.depSum;
+            if (outcome == OUT_ESCAPE) { ++esc; eEsc += p.w; }
+            else if (outcome == OUT_CUTOFF) { ++cut; }
+            else if (outcome == OUT_CENSUS) { ++ncen; eCen += p.w; }
+        }
+        const bool keep = active && outcome == OUT_CONTINUE;
+        const bool cens = active && outcome == OUT_CENSUS;
+        const unsigned mK = __ballot_sync(FULL, keep), mC = __ballot_sync(FULL, cens);
+        uint32_t bK = 0, bC = 0;
+        if (lane == 0) {
+            if (mK) bK = atomicAdd(nOut, __popc(mK));
+            if (mC) bC = atomicAdd(nCen, __popc(mC));
+        }
+        bK = __shfl_sync(FULL, bK, 0);
+        bC = __shfl_sync(FULL, bC, 0);
+        const unsigned lt = lanemask_lt();
+        if (keep) store_part(out, bK + __popc(mK & lt), p, pid, draw);
+        if (cens) store_part(cen, bC + __popc(mC & lt), p, pid, draw);
+    }
+    segs = warp_sum(segs); rw = warp_sum(rw); esc = warp_sum(esc); cut = warp_sum(cut); ncen = warp_sum(ncen);
+    dep = warp_sum(dep); eEsc = warp_sum(eEsc); eCen = warp_sum(eCen);
+    if (lane == 0) {
+        if (segs) atomicAdd(&st->segments, segs);
+        if (rw) atomicAdd(&st->rwSteps, rw);
+        if (esc) atomicAdd(&st->escaped, esc);
+        if (cut) atomicAdd(&st->cutoff, cut);
+        if (ncen) atomicAdd(&st->census, ncen);
+        if (dep != 0.0) atomicAdd(&st->eDeposited, dep);
+        if (eEsc != 0.0) atomicAdd(&st->eEscaped, eEsc);
+        if (eCen != 0.0) atomicAdd(&st->eCensusPre, eCen);
+    }
+}
+
+// ------------------------------------------------------------------ comb
+// CombPopulationControl::activate (population/CombPopulationControl.hpp:79-253).
+// Sort key = (cell << 32) | bijective hash of the particle's pid: a pseudo-random
+// order inside each cell (the reference sorts by id then std::shuffles) that does
+// not depend on the order particles reached census.  Zero-weight particles get
+// cell = Ncells and sort last (they are skipped, :136-137).
+__device__ __forceinline__ uint32_t fmix32(uint32_t h) {
+    h ^= h >> 16; h *= 0x85ebca6bu; h ^= h >> 13; h *= 0xc2b2ae35u; h ^= h >> 16;
+    return h;
+}
+__global__ void k_comb_keys(Ctx C, Bank cen, uint32_t n, uint64_t *keys, uint32_t *vals, uint32_t combKey) {
+    for (uint32_t q = blockIdx.x * blockDim.x + threadIdx.x; q < n; q += gridDim.x * blockDim.x) {
+        const double x = cen.x[q], y = cen.y[q], z = cen.z[q], w = cen.w[q];
+        const uint32_t pid = cen.pid[q];
+        uint32_t cell = cen.cell[q];
+        if (outside_box(C, x, y, z)) raise_error(C, STORM_DERR_COMB_OUTSIDE, cell, pid);
+        if (!isfinite(w) || w < 0.0) raise_error(C, STORM_DERR_COMB_WEIGHT, cell, pid);
+        if (w == 0.0) cell = C.ncells;
+        keys[q] = (static_cast<uint64_t>(cell) << 32) | fmix32(pid ^ combKey);
+        vals[q] = q;
+    }
+}
+
+// LSD radix sort, 8-bit digits: per-tile histograms, scan, stable scatter.
+constexpr int RS_THREADS = 256, RS_WARPS = 8, RS_PER_WARP = 512, RS_TILE = RS_WARPS * RS_PER_WARP;
+
+__global__ void __launch_bounds__(RS_THREADS) k_rs_hist(const uint64_t *keys, uint32_t n, int shift, uint32_t *tileHist,
+                                                        uint32_t ntiles) {
+    __shared__ uint32_t h[256];
+    h[threadIdx.x] = 0;
+    __syncthreads();
+    const uint32_t base = blockIdx.x * RS_TILE;
+    for (int it = 0; it < RS_TILE / RS_THREADS; ++it) {
+        uint32_t q = base + it * RS_THREADS + threadIdx.x;
+        if (q < n) atomicAdd(&h[(keys[q] >> shift) & 255u], 1u);
+    }
+    __syncthreads();
+    tileHist[threadIdx.x * ntiles + blockIdx.x] = h[threadIdx.x];
+}
+
+// exclusive scan of the digit-major tile histogram (256 * ntiles) by one block
+__global__ void k_rs_scan(uint32_t *tileHist, uint32_t len) {
+    __shared__ uint64_t sh[32];
+    __shared__ uint64_t last;
+    uint64_t carry = 0;
+    for (uint32_t base = 0; base < len; base += blockDim.x) {
+        uint32_t q = base + threadIdx.x;
+        uint64_t v = q < len ? tileHist[q] : 0;
+        uint64_t inc = block_scan_incl(v, sh);
+        if (q < len) tileHist[q] = static_cast<uint32_t>(carry + inc - v);
+        if (threadIdx.x == blockDim.x - 1) last = inc;
+        __syncthreads();
+        carry += last;
+        __syncthreads();
+    }
+}
+
+__global__ void __launch_bounds__(RS_THREADS) k_rs_scatter(const uint64_t *kin, const uint32_t *vin, uint64_t *kout,
+                                                           uint32_t *vout, uint32_t n, int shift,
+                                                           const uint32_t *tileOff, uint32_t ntiles) {
+    __shared__ uint32_t wc[RS_WARPS][257];
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    for (int d = lane; d < 257; d += 32) wc[wid][d] = 0;
+    __syncwarp();
+    const uint32_t start = blockIdx.x * RS_TILE + wid * RS_PER_WARP;
+    for (int it = 0; it < RS_PER_WARP / 32; ++it) {
+        uint32_t q = start + it * 32 + lane;
+        uint32_t d = (q < n) ? static_cast<uint32_t>((kin[q] >> shift) & 255u) : 256u;
+        unsigned m = __match_any_sync(FULL, d);
+        if ((__ffs(m) - 1) == lane) wc[wid][d] += __popc(m);
+        __syncwarp();
+    }
+    __syncthreads();
+    {
+        const uint32_t d = threadIdx.x;   // 256 threads, one digit each
+        uint32_t run = tileOff[d * ntiles + blockIdx.x];
+        for (int w = 0; w < RS_WARPS; ++w) {
+            uint32_t c = wc[w][d];
+            wc[w][d] = run;
+            run += c;
+        }
+    }
+    __syncthreads();
+    const unsigned lt = lanemask_lt();
+    for (int it = 0; it < RS_PER_WARP / 32; ++it) {
+        uint32_t q = start + it * 32 + lane;
+        const bool valid = q < n;
+        uint64_t key = valid ? kin[q] : 0;
+        uint32_t d = valid ? static_cast<uint32_t>((key >> shift) & 255u) : 256u;
+        unsigned m = __match_any_sync(FULL, d);
+        uint32_t pos = wc[wid][d] + __popc(m & lt);
+        __syncwarp();
+        if (valid) {
+            kout[pos] = key;
+            vout[pos] = vin[q];
+            if ((__ffs(m) - 1) == lane) wc[wid][d] += __popc(m);
+        }
+        __syncwarp();
+    }
+}
+
+// first sorted position of each cell (lower_bound of cell << 32), cells 0..N
+__global__ void k_comb_ranges(const uint64_t *keys, uint32_t n, uint32_t ncells, uint32_t *start) {
+    for (uint32_t c = blockIdx.x * blockDim.x + threadIdx.x; c <= ncells; c += gridDim.x * blockDim.x) {
+        const uint64_t v = static_cast<uint64_t>(c) << 32;
+        uint32_t first = 0, count = n;
+        while (count > 0) {
+            uint32_t step = count >> 1, it = first + step;
+            if (keys[it] < v) { first = it + 1; count -= step + 1; } else count = step;
+        }
+        start[c] = first;
+    }
+}
+
+// weights[cell] (:136-141), summed in sorted order
+__global__ void k_comb_cell_sums(Bank cen, const uint32_t *idx, const uint32_t *start, uint32_t ncells, double *W) {
+    for (uint32_t c = blockIdx.x * blockDim.x + threadIdx.x; c < ncells; c += gridDim.x * blockDim.x) {
+        double s = 0.0;
+        for (uint32_t q = start[c]; q < start[c + 1]; ++q) s += cen.w[idx[q]];
+        W[c] = s;
+    }
+}
+
+// Deterministic total: 1024 contiguous chunks left to right, then a pairwise tree.
+__global__ void k_blocked_sum(const double *v, uint32_t n, double *out) {
+    __shared__ double part[1024];
+    const uint32_t chunk = (n + 1023) / 1024;
+    const uint32_t a = threadIdx.x * chunk;
+    double s = 0.0;
+    for (uint32_t q = a; q < a + chunk && q < n; ++q) s += v[q];
+    part[threadIdx.x] = s;
+    __syncthreads();
+    for (uint32_t w = 512; w >= 1; w >>= 1) {
+        if (threadIdx.x < w) part[threadIdx.x] = part[threadIdx.x] + part[threadIdx.x + w];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) *out = part[0];
+}
+
+struct CombCell {
+    uint64_t nin;
+    double w_ideal;   // split path
+    double e;         // comb path: new_energy
+    double r;
+    int mode;         // 0 keep/split, 1 comb
+};
+
+__device__ __forceinline__ CombCell comb_cell_params(const Ctx &C, const CombParams &P, uint32_t c, uint32_t cnt,
+                                                     double Wc, double Wtot) {
+    CombCell cc;
+    uint64_t share = static_cast<uint64_t>(static_cast<double>(P.ntotal) * Wc / Wtot);
+    uint64_t lo = share > P.nmin ? share : P.nmin;
+    cc.nin = (P.nmin * 20 < lo) ? P.nmin * 20 : lo;
+    cc.mode = (cnt <= cc.nin) ? 0 : 1;
+    cc.w_ideal = Wc / static_cast<double>(cc.nin);
+    cc.e = cc.w_ideal;
+    cc.r = cc.mode ? stream_uniform(C.seedLo, C.seedHi, TAG_COMB, C.step, c, 0) : 0.0;
+    return cc;
+}
+
+// output count per cell (:161-226)
+__global__ void k_comb_count(Ctx C, CombParams P, Bank cen, const uint32_t *idx, const uint32_t *start, const double *W,
+                             const double *Wtot, uint64_t *outCount) {
+    const double tot = *Wtot;
+    if (!isfinite(tot)) {
+        if (blockIdx.x == 0 && threadIdx.x == 0) raise_error(C, STORM_DERR_COMB_TOTAL, 0, 0);
+    }
+    for (uint32_t c = blockIdx.x * blockDim.x + threadIdx.x; c < C.ncells; c += gridDim.x * blockDim.x) {
+        const uint32_t a = start[c], b = start[c + 1];
+        if (tot == 0.0 || !isfinite(tot) || a == b) { outCount[c] = 0; continue; }
+        CombCell cc = comb_cell_params(C, P, c, b - a, W[c], tot);
+        uint64_t m = 0;
+        if (cc.mode == 0) {
+            for (uint32_t q = a; q < b; ++q) {
+                double w = cen.w[idx[q]];
+                m += (w > 2 * cc.w_ideal) ? static_cast<uint64_t>(ceil(w / cc.w_ideal)) : 1;
+            }
+        } else {
+            uint64_t k = 0;
+            double cum = 0;
+            for (uint32_t q = a; q < b; ++q) {
+                double w = cen.w[idx[q]];
+                while ((cum + w) > (static_cast<double>(k) + cc.r) * cc.e) ++k;
+                cum += w;
+            }
+            m = k;
+        }
+        outCount[c] = m;
+    }
+}
+
+// write the combed census into the next step's bank; per-cell census radiation
+// energy (RadiationIMC::postStep :1989-2028) summed in output order.
+__global__ void k_comb_write(Ctx C, CombParams P, Bank cen, const uint32_t *idx, const uint32_t *start, const double *W,
+                             const double *Wtot, const uint64_t *outOffset, Bank out, double *eradCensus,
+                             DevStats *st) {
+    const double tot = *Wtot;
+    double eOut = 0.0;
+    for (uint32_t c = blockIdx.x * blockDim.x + threadIdx.x; c < C.ncells; c += gridDim.x * blockDim.x) {
+        const uint32_t a = start[c], b = start[c + 1];
+        double ecell = 0.0;
+        if (!(tot == 0.0 || !isfinite(tot) || a == b)) {
+            CombCell cc = comb_cell_params(C, P, c, b - a, W[c], tot);
+            uint64_t o = outOffset[c];
+            uint32_t i, j, k;
+            cell_ijk(C, c, i, j, k);
+            const double mx = C.xc[i], my = C.yc[j], mz = C.zc[k];
+            auto emit = [&](uint32_t src, double w, bool reweight) {
+                PartReg p;
+                load_part(cen, src, p);
+                if (reweight) { p.w = w; p.w0 = w; p.t = 0; }
+                p.cell = c;
+                if (outside_box(C, p.x, p.y, p.z)) {   // :228-250
+                    const double ox = p.x, oy = p.y, oz = p.z, dx = mx - ox, dy = my - oy, dz = mz - oz;
+                    double t = 1e-6;
+                    while (outside_box(C, p.x, p.y, p.z) && t < 1.0) {
+                        p.x = ox + t * dx; p.y = oy + t * dy; p.z = oz + t * dz;
+                        t *= 2;
+                    }
+                    if (outside_box(C, p.x, p.y, p.z)) { p.x = mx; p.y = my; p.z = mz; }
+                }
+                store_part(out, static_cast<uint32_t>(o), p, static_cast<uint32_t>(o), 0);
+                ecell += p.w;
+                ++o;
+            };
+            if (cc.mode == 0) {
+                for (uint32_t q = a; q < b; ++q) {
+                    const uint32_t src = idx[q];
+                    const double w = cen.w[src];
+                    if (w > 2 * cc.w_ideal) {
+                        const uint64_t ns = static_cast<uint64_t>(ceil(w / cc.w_ideal));
+                        const double ws = w / static_cast<double>(ns);
+                        for (uint64_t s = 0; s < ns; ++s) emit(src, ws, true);
+                    } else {
+                        emit(src, w, false);
+                    }
+                }
+            } else {
+                uint64_t k2 = 0;
+                double cum = 0;
+                for (uint32_t q = a; q < b; ++q) {
+                    const uint32_t src = idx[q];
+                    const double w = cen.w[src];
+                    while ((cum + w) > (static_cast<double>(k2) + cc.r) * cc.e) {
+                        ++k2;
+                        emit(src, cc.e, true);
+                    }
+                    cum += w;
+                }
+            }
+        }
+        eradCensus[c] = ecell;
+        eOut += ecell;
+    }
+    eOut = warp_sum(eOut);
+    if ((threadIdx.x & 31) == 0 && eOut != 0.0) atomicAdd(&st->eCensusOut, eOut);
+}
+
+// census kept as is (no population control): order by pid for a deterministic bank
+__global__ void k_census_keys_pid(Bank cen, uint32_t n, uint64_t *keys, uint32_t *vals) {
+    for (uint32_t q = blockIdx.x * blockDim.x + threadIdx.x; q < n; q += gridDim.x * blockDim.x) {
+        keys[q] = cen.pid[q];
+        vals[q] = q;
+    }
+}
+__global__ void k_gather(Bank src, const uint32_t *idx, uint32_t n, Bank dst, double *eradCensus, DevStats *st) {
+    double e = 0.0;
+    for (uint32_t q = blockIdx.x * blockDim.x + threadIdx.x; q < n; q += gridDim.x * blockDim.x) {
+        PartReg p;
+        load_part(src, idx[q], p);
+        store_part(dst, q, p, q, 0);
+        atomicAdd(eradCensus + p.cell, p.w);
+        e += p.w;
+    }
+    e = warp_sum(e);
+    if ((threadIdx.x & 31) == 0 && e != 0.0) atomicAdd(&st->eCensusOut, e);
+}
+
+// ------------------------------------------------------------------ poststep
+// RadiationIMC::postStep (radiation/RadiationIMC.hpp:1887-2029), gray, no hydro.
+__global__ void k_poststep(Ctx C, CellArrays A, OpacityEos M, double dt) {
+    for (uint32_t c = blockIdx.x * blockDim.x + threadIdx.x; c < C.ncells; c += gridDim.x * blockDim.x) {
+        A.eradAvg[c] /= (dt * A.vol[c]);
+        if (C.noFeedback) continue;
+        double E = A.eint[c];
+        if (E < 0.0) {   // throwIfNegativeInternalEnergy (:771-817)
+            double thermalScale = C.arad * pow(A.T[c], 4.0) * A.vol[c];
+            if (thermalScale < 1e-30) thermalScale = 1e-30;
+            double ratio = fabs(E) / thermalScale;
+            if (ratio < 0.1) {
+                double fl = A.ceint[c];
+                E = fl > 0.0 ? fl : 0.0;
+                A.eint[c] = E;
+            } else {
+                raise_error(C, STORM_DERR_NEGATIVE_ENERGY, c, 0);
+            }
+        }
+        // synchronizeMaterialCell (:830-866)
+        const double spec = E / A.mass[c];
+        A.ceint[c] = E;
+        const double rho = A.mass[c] / A.vol[c];
+        double T;
+        if (M.eosKind == STORM_EOS_LINEAR) {
+            T = (M.cvPerMass > 0.0) ? spec / M.cvPerMass : 0.0;
+        } else {
+            double ev = spec * rho;
+            double rf = pow(rho, 1.0 - M.eosMu);
+            double ratio = (ev > 0.0 ? ev : 0.0) / (M.eosF * rf);
+            T = pow(ratio > 0.0 ? ratio : 0.0, 1.0 / M.eosBeta);
+        }
+        A.T[c] = T;
+    }
+}
+
+// ------------------------------------------------------------------ replay
+__global__ void k_replay(Ctx C, ReplayDev R, uint32_t n) {
+    for (uint32_t q = blockIdx.x * blockDim.x + threadIdx.x; q < n; q += gridDim.x * blockDim.x) {
+        PartReg p;
+        p.x = R.in[0][q]; p.y = R.in[1][q]; p.z = R.in[2][q];
+        p.vx = R.in[3][q]; p.vy = R.in[4][q]; p.vz = R.in[5][q];
+        p.t = R.in[6][q]; p.w = R.in[7][q]; p.w0 = R.in[8][q];
+        p.cell = R.cell[q];
+        TapeRng rng{R.tape + R.tapeOffset[q], R.tapeLength[q], 0, false};
+        LocalTally tal{0.0, 0.0};
+        PhysOut o = physics_step(C, p, rng, tal);
+        R.phys[0][q] = p.x; R.phys[1][q] = p.y; R.phys[2][q] = p.z;
+        R.phys[3][q] = p.vx; R.phys[4][q] = p.vy; R.phys[5][q] = p.vz;
+        R.phys[6][q] = p.t; R.phys[7][q] = p.w;
+        R.physStatus[q] = o.errCode ? -1 : o.status;
+        R.physNext[q] = (o.status == CELL_MOVE && !o.errCode) ? (o.next != OUTSIDE ? o.next : o.ghost) : OUTSIDE;
+        R.dep[0][q] = tal.mat_;
+        R.dep[1][q] = tal.rad_;
+        R.usedRW[q] = o.usedRW;
+        R.draws[q] = rng.pos;
+        int m = o.errCode ? OUT_ERROR : manager_handle(C, p, o);
+        R.mgr[0][q] = p.x; R.mgr[1][q] = p.y; R.mgr[2][q] = p.z;
+        R.mgr[3][q] = p.vx; R.mgr[4][q] = p.vy; R.mgr[5][q] = p.vz;
+        R.mgrCell[q] = p.cell;
+        R.mgrStatus[q] = rng.exhausted() ? -2 : m;
+    }
+}
+
+// ------------------------------------------------------------------ Random Walk tables
+// RandomWalk::RandomWalk radius table (radiation/RandomWalk.hpp:41-78): one block
+// per tau row; the 512-point radial CDF lives in shared memory.
+__device__ double rw_radial_cdf(double x, double tau, double S) {   // computeRadialCDF :152-167
+    if (tau <= 0.0) return (x > 0.0) ? 1.0 : 0.0;
+    if (x <= 0.0) return 0.0;
+    if (x >= 1.0) return 1.0;
+    if (tau < 0.01) {   // radialCdfFreeSpace :194-206
+        double a = x / (2.0 * sqrt(tau));
+        return clampd(erf(a) - 2.0 * a * exp(-a * a) / sqrt(RW_PI), 0.0, 1.0);
+    }
+    if (S < 1e-30) return 1.0;   // radialCdfEigen :208-237
+    double sum = 0.0;
+    for (int m = 1; m <= 500; ++m) {
+        double arg = -static_cast<double>(m * m) * RW_PI * RW_PI * tau;
+        if (arg < -700.0) break;
+        double npi = static_cast<double>(m) * RW_PI;
+        double npx = npi * x;
+        double sn, cs;
+        sincos(npx, &sn, &cs);
+        sum += exp(arg) * (sn / npi - x * cs);
+    }
+    return clampd(2.0 * sum / S, 0.0, 1.0);
+}
+__global__ void k_rw_radius(const double *tau, const double *surv, double *radius) {
+    __shared__ double g[RW_XGRID];
+    const uint32_t row = blockIdx.x;
+    const double t = tau[row];
+    double S = t <= 0.0 || t < 1e-4 ? 1.0 : surv[row];
+    // the eigen CDF normalises by computeSurvival(tau), which equals the table entry
+    for (int k = threadIdx.x; k < RW_XGRID; k += blockDim.x)
+        g[k] = rw_radial_cdf(static_cast<double>(k) / static_cast<double>(RW_XGRID - 1), t, S);
+    __syncthreads();
+    for (int j = threadIdx.x; j < RW_RADIUS; j += blockDim.x) {
+        double xi = static_cast<double>(j) / static_cast<double>(RW_RADIUS - 1);
+        double r;
+        if (xi <= g[0]) r = 0.0;
+        else if (xi >= g[RW_XGRID - 1]) r = 1.0;
+        else {
+            uint32_t first = 0, count = RW_XGRID;
+            while (count > 0) {
+                uint32_t step = count >> 1, it = first + step;
+                if (g[it] < xi) { first = it + 1; count -= step + 1; } else count = step;
+            }
+            if (first == 0) first = 1;
+            double g0 = g[first - 1], g1 = g[first];
+            double x0 = static_cast<double>(first - 1) / static_cast<double>(RW_XGRID - 1);
+            double x1 = static_cast<double>(first) / static_cast<double>(RW_XGRID - 1);
+            double f = (g1 > g0) ? (xi - g0) / (g1 - g0) : 0.5;
+            r = x0 + f * (x1 - x0);
+        }
+        radius[static_cast<size_t>(row) * RW_RADIUS + j] = r;
+    }
+}
+__global__ void k_rw_sample(RwTables T, uint32_t n, const double *xiLeak, const double *tau, const double *xiRad,
+                            double *leak, double *rad) {
+    for (uint32_t q = blockIdx.x * blockDim.x + threadIdx.x; q < n; q += gridDim.x * blockDim.x) {
+        if (xiLeak) leak[q] = rw_sample_leak(T, xiLeak[q]);
+        if (tau && xiRad) rad[q] = rw_sample_radius(T, tau[q], xiRad[q]);
+    }
+}
+
+// ------------------------------------------------------------------ launchers
+static inline uint32_t grid_for(uint64_t n, uint32_t block, uint32_t cap) {
+    uint64_t g = (n + block - 1) / block;
+    if (g == 0) g = 1;
+    return static_cast<uint32_t>(g < cap ? g : cap);
+}
+
+void launch_begin(cudaStream_t s, const Bank &b, uint32_t n, double dt, DevStats *st) {
+    k_begin<<<grid_for(n, 256, 4096), 256, 0, s>>>(b, n, dt, st);
+}
+void launch_prestep(cudaStream_t s, const Ctx &C, const CellArrays &A, const OpacityEos &M, double dt) {
+    k_prestep<<<grid_for(C.ncells, 256, 8192), 256, 0, s>>>(C, A, M, dt);
+}
+void launch_rw_eligibility(cudaStream_t s, const Ctx &C, const CellArrays &A) {
+    k_rw_eligibility<<<grid_for(C.ncells, 256, 8192), 256, 0, s>>>(C, A);
+}
+void launch_emission_energy(cudaStream_t s, const Ctx &C, const CellArrays &A, double dt) {
+    k_emission_energy<<<grid_for(C.ncells, 256, 8192), 256, 0, s>>>(C, A, dt);
+}
+void launch_sequential_sum(cudaStream_t s, const double *v, uint32_t n, double *out) {
+    k_sequential_sum<<<1, 256, 0, s>>>(v, n, out);
+}
+void launch_allocate(cudaStream_t s, const Ctx &C, const CellArrays &A, const double *total, uint64_t newPerCell) {
+    k_allocate<<<grid_for(C.ncells, 256, 8192), 256, 0, s>>>(C, A, total, newPerCell);
+}
+void launch_emission_debit(cudaStream_t s, const Ctx &C, const CellArrays &A, DevStats *st) {
+    k_emission_debit<<<grid_for(C.ncells, 256, 8192), 256, 0, s>>>(C, A, st);
+}
+void launch_scan_u64(cudaStream_t s, const uint64_t *in, uint32_t n, uint64_t *out, uint64_t *tileSums, uint64_t *total) {
+    const uint32_t tiles = (n + 1023) / 1024 ? (n + 1023) / 1024 : 1;
+    k_scan_tiles<<<tiles, 1024, 0, s>>>(in, n, out, tileSums);
+    k_scan_sums<<<1, 1024, 0, s>>>(tileSums, tiles, total);
+    k_scan_add<<<tiles, 1024, 0, s>>>(out, n, tileSums, total);
+}
+void launch_emit_cells(cudaStream_t s, const Ctx &C, const CellArrays &A, const uint64_t *offsets, uint64_t total,
+                       const Bank &b, uint32_t bankBase, double dt, DevStats *st) {
+    if (!total) return;
+    k_emit_cells<<<grid_for(total, 256, 148 * 16), 256, 0, s>>>(C, A, offsets, total, b, bankBase, dt, st);
+}
+void launch_emit_faces(cudaStream_t s, const Ctx &C, const FaceSources &F, uint64_t total, const Bank &b,
+                       uint32_t bankBase, double dt, DevStats *st) {
+    if (!total) return;
+    k_emit_faces<<<grid_for(total, 256, 148 * 16), 256, 0, s>>>(C, F, total, b, bankBase, dt, st);
+}
+void launch_transport(cudaStream_t s, uint32_t grid, const Ctx &C, const Bank &in, const uint32_t *nIn, const Bank &out,
+                      uint32_t *nOut, const Bank &cen, uint32_t *nCen, uint32_t K, DevStats *st) {
+    k_transport<<<grid, 256, 0, s>>>(C, in, nIn, out, nOut, cen, nCen, K, st);
+}
+void launch_comb_keys(cudaStream_t s, const Ctx &C, const Bank &cen, uint32_t n, uint64_t *keys, uint32_t *vals,
+                      uint32_t combKey) {
+    k_comb_keys<<<grid_for(n, 256, 8192), 256, 0, s>>>(C, cen, n, keys, vals, combKey);
+}
+int launch_radix_sort(cudaStream_t s, uint64_t *keys, uint32_t *vals, uint64_t *keysAlt, uint32_t *valsAlt, uint32_t n,
+                      int bits, uint32_t *tileHist) {
+    // returns 1 when the sorted data ends in the Alt buffers
+    const uint32_t ntiles = (n + RS_TILE - 1) / RS_TILE ? (n + RS_TILE - 1) / RS_TILE : 1;
+    int passes = (bits + 7) / 8;
+    uint64_t *ka = keys, *kb = keysAlt;
+    uint32_t *va = vals, *vb = valsAlt;
+    for (int p = 0; p < passes; ++p) {
+        k_rs_hist<<<ntiles, RS_THREADS, 0, s>>>(ka, n, 8 * p, tileHist, ntiles);
+        k_rs_scan<<<1, 1024, 0, s>>>(tileHist, 256 * ntiles);
+        k_rs_scatter<<<ntiles, RS_THREADS, 0, s>>>(ka, va, kb, vb, n, 8 * p, tileHist, ntiles);
+        uint64_t *tk = ka; ka = kb; kb = tk;
+        uint32_t *tv = va; va = vb; vb = tv;
+    }
+    return passes & 1;
+}
+uint32_t radix_tile_count(uint32_t n) { return (n + RS_TILE - 1) / RS_TILE ? (n + RS_TILE - 1) / RS_TILE : 1; }
+void launch_comb_ranges(cudaStream_t s, const uint64_t *keys, uint32_t n, uint32_t ncells, uint32_t *start) {
+    k_comb_ranges<<<grid_for(ncells + 1, 256, 8192), 256, 0, s>>>(keys, n, ncells, start);
+}
+void launch_comb_cell_sums(cudaStream_t s, const Bank &cen, const uint32_t *idx, const uint32_t *start, uint32_t ncells,
+                           double *W) {
+    k_comb_cell_sums<<<grid_for(ncells, 128, 8192), 128, 0, s>>>(cen, idx, start, ncells, W);
+}
+void launch_blocked_sum(cudaStream_t s, const double *v, uint32_t n, double *out) {
+    k_blocked_sum<<<1, 1024, 0, s>>>(v, n, out);
+}
+void launch_comb_count(cudaStream_t s, const Ctx &C, const CombParams &P, const Bank &cen, const uint32_t *idx,
+                       const uint32_t *start, const double *W, const double *Wtot, uint64_t *outCount) {
+    k_comb_count<<<grid_for(C.ncells, 128, 8192), 128, 0, s>>>(C, P, cen, idx, start, W, Wtot, outCount);
+}
+void launch_comb_write(cudaStream_t s, const Ctx &C, const CombParams &P, const Bank &cen, const uint32_t *idx,
+                       const uint32_t *start, const double *W, const double *Wtot, const uint64_t *outOffset,
+                       const Bank &out, double *eradCensus, DevStats *st) {
+    k_comb_write<<<grid_for(C.ncells, 128, 8192), 128, 0, s>>>(C, P, cen, idx, start, W, Wtot, outOffset, out, eradCensus,
+                                                                st);
+}
+void launch_census_keys_pid(cudaStream_t s, const Bank &cen, uint32_t n, uint64_t *keys, uint32_t *vals) {
+    k_census_keys_pid<<<grid_for(n, 256, 8192), 256, 0, s>>>(cen, n, keys, vals);
+}
+void launch_gather(cudaStream_t s, const Bank &src, const uint32_t *idx, uint32_t n, const Bank &dst, double *eradCensus,
+                   DevStats *st) {
+    k_gather<<<grid_for(n, 256, 8192), 256, 0, s>>>(src, idx, n, dst, eradCensus, st);
+}
+void launch_poststep(cudaStream_t s, const Ctx &C, const CellArrays &A, const OpacityEos &M, double dt) {
+    k_poststep<<<grid_for(C.ncells, 256, 8192), 256, 0, s>>>(C, A, M, dt);
+}
+void launch_replay(cudaStream_t s, const Ctx &C, const ReplayDev &R, uint32_t n) {
+    k_replay<<<grid_for(n, 128, 8192), 128, 0, s>>>(C, R, n);
+}
+void launch_rw_radius(cudaStream_t s, const double *tau, const double *surv, double *radius) {
+    k_rw_radius<<<RW_TABLE, 256, 0, s>>>(tau, surv, radius);
+}
+void launch_rw_sample(cudaStream_t s, const RwTables &T, uint32_t n, const double *xiLeak, const double *tau,
+                      const double *xiRad, double *leak, double *rad) {
+    k_rw_sample<<<grid_for(n, 256, 4096), 256, 0, s>>>(T, n, xiLeak, tau, xiRad, leak, rad);
+}
+
+}  // namespace storm

@@ -1,0 +1,1097 @@
+// Host runtime of the C ABI (include/storm_cuda.h): handle lifecycle, device
+// memory, the order of kernels in a time step, and state transfer.  One CUDA
+// stream per handle; every kernel launch goes through this file.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "storm_cuda.h"
+#include "storm_internal.h"
+
+using namespace storm;
+
+namespace {
+
+template <class T>
+struct DBuf {
+    T *p = nullptr;
+    size_t n = 0;
+};
+
+struct BankBuf {
+    Bank b{};
+    size_t cap = 0;
+};
+
+}  // namespace
+
+struct StormHandle {
+    StormProblemDesc desc{};
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    cudaEvent_t evStart = nullptr, evTransport0 = nullptr, evTransport1 = nullptr, evEnd = nullptr;
+    uint32_t nx = 0, ny = 0, nz = 0, N = 0;
+    std::vector<double> hxe, hye, hze, hxc, hyc, hzc;
+    // device mesh + cells
+    double *xe = nullptr, *ye = nullptr, *ze = nullptr, *xc = nullptr, *yc = nullptr, *zc = nullptr;
+    CellArrays A{};
+    double *tabA = nullptr, *tabS = nullptr, *rhoF = nullptr;
+    uint32_t *segs = nullptr;
+    OpacityEos M{};
+    Ctx C{};
+    // random walk tables
+    double *rwTau = nullptr, *rwLogTau = nullptr, *rwSurv = nullptr, *rwRadius = nullptr;
+    // face sources
+    uint32_t *fsCell = nullptr;
+    int32_t *fsSide = nullptr;
+    uint64_t *fsOffset = nullptr;
+    uint32_t fsCount = 0;
+    uint64_t fsTotal = 0;
+    // banks
+    size_t cap = 0;
+    Bank bankA{}, bankB{}, bankC{};
+    uint64_t *keys = nullptr, *keysAlt = nullptr;
+    uint32_t *vals = nullptr, *valsAlt = nullptr, *tileHist = nullptr;
+    size_t tileHistLen = 0;
+    // scratch
+    uint64_t *offsets = nullptr, *tileSums = nullptr, *dTotalU64 = nullptr;
+    double *dTotalE = nullptr, *combW = nullptr, *combWtot = nullptr;
+    uint32_t *combStart = nullptr;
+    uint64_t *combCount = nullptr;
+    uint32_t *counts = nullptr;      // transport round counters (maxRounds + 1) + census counter
+    DevStats *dStats = nullptr;
+    int32_t *dErr = nullptr;
+    // host state
+    uint64_t nCensus = 0;            // particles at the head of bankA
+    uint64_t nBank = 0;              // particles in bankA after emission
+    uint32_t step = 0;
+    uint32_t K = 8, maxRounds = 4096;
+    uint64_t launches = 0;
+    uint64_t memBytes = 0;
+    StormStepStats stats{};
+    std::vector<uint64_t> lastPhotons;
+    double lastTransportMs = 0.0, lastStepMs = 0.0;
+    // transport kernel timing
+    bool profiling = false;
+    std::vector<cudaEvent_t> evPool;
+    double profMs = 0.0;
+    uint64_t profLaunches = 0, profSegments = 0;
+    int32_t errCode = 0;
+    uint64_t errCell = 0, errParticle = 0;
+    std::string errMsg;
+};
+
+namespace {
+
+int cuda_fail(StormHandle *h, cudaError_t e, const char *what) {
+    if (h) {
+        h->errMsg = std::string(what) + ": " + cudaGetErrorString(e);
+    }
+    return e == cudaErrorMemoryAllocation ? STORM_ERR_OOM : STORM_ERR_CUDA;
+}
+
+#define CK(call)                                              \
+    do {                                                      \
+        cudaError_t e_ = (call);                              \
+        if (e_ != cudaSuccess) return cuda_fail(h, e_, #call); \
+    } while (0)
+
+template <class T>
+cudaError_t dalloc(StormHandle *h, T **p, size_t n) {
+    size_t bytes = sizeof(T) * (n ? n : 1);
+    cudaError_t e = cudaMalloc(reinterpret_cast<void **>(p), bytes);
+    if (e == cudaSuccess) h->memBytes += bytes;
+    return e;
+}
+template <class T>
+void dfree(StormHandle *h, T *&p, size_t n) {
+    if (p) {
+        cudaFree(p);
+        h->memBytes -= sizeof(T) * (n ? n : 1);
+        p = nullptr;
+    }
+}
+
+cudaError_t bank_alloc(StormHandle *h, Bank &b, size_t n) {
+    double **d[] = {&b.x, &b.y, &b.z, &b.vx, &b.vy, &b.vz, &b.t, &b.w, &b.w0};
+    for (double **q : d) {
+        cudaError_t e = dalloc(h, q, n);
+        if (e != cudaSuccess) return e;
+    }
+    uint32_t **u[] = {&b.cell, &b.pid, &b.draw};
+    for (uint32_t **q : u) {
+        cudaError_t e = dalloc(h, q, n);
+        if (e != cudaSuccess) return e;
+    }
+    return cudaSuccess;
+}
+void bank_free(StormHandle *h, Bank &b, size_t n) {
+    double **d[] = {&b.x, &b.y, &b.z, &b.vx, &b.vy, &b.vz, &b.t, &b.w, &b.w0};
+    for (double **q : d) dfree(h, *q, n);
+    uint32_t **u[] = {&b.cell, &b.pid, &b.draw};
+    for (uint32_t **q : u) dfree(h, *q, n);
+}
+cudaError_t bank_copy(cudaStream_t s, const Bank &dst, const Bank &src, size_t n) {
+    if (!n) return cudaSuccess;
+    const double *sd[] = {src.x, src.y, src.z, src.vx, src.vy, src.vz, src.t, src.w, src.w0};
+    double *dd[] = {dst.x, dst.y, dst.z, dst.vx, dst.vy, dst.vz, dst.t, dst.w, dst.w0};
+    for (int q = 0; q < 9; ++q) {
+        cudaError_t e = cudaMemcpyAsync(dd[q], sd[q], n * sizeof(double), cudaMemcpyDeviceToDevice, s);
+        if (e != cudaSuccess) return e;
+    }
+    const uint32_t *su[] = {src.cell, src.pid, src.draw};
+    uint32_t *du[] = {dst.cell, dst.pid, dst.draw};
+    for (int q = 0; q < 3; ++q) {
+        cudaError_t e = cudaMemcpyAsync(du[q], su[q], n * sizeof(uint32_t), cudaMemcpyDeviceToDevice, s);
+        if (e != cudaSuccess) return e;
+    }
+    return cudaSuccess;
+}
+
+// (Re)allocate every per-particle buffer for capacity n, keeping the first
+// `keep` particles of bank A.
+int ensure_capacity(StormHandle *h, size_t n, size_t keep) {
+    if (n <= h->cap) return STORM_OK;
+    if (n > 0xF0000000ull) {
+        h->errMsg = "particle count exceeds the 32-bit bank index range";
+        return STORM_ERR_CAPACITY;
+    }
+    size_t nc = std::max<size_t>(n + n / 4, 1u << 16);
+    Bank na{};
+    CK(bank_alloc(h, na, nc));
+    if (keep) CK(bank_copy(h->stream, na, h->bankA, keep));
+    CK(cudaStreamSynchronize(h->stream));
+    bank_free(h, h->bankA, h->cap);
+    bank_free(h, h->bankB, h->cap);
+    bank_free(h, h->bankC, h->cap);
+    dfree(h, h->keys, h->cap); dfree(h, h->keysAlt, h->cap);
+    dfree(h, h->vals, h->cap); dfree(h, h->valsAlt, h->cap);
+    dfree(h, h->tileHist, h->tileHistLen);
+    h->bankA = na;
+    CK(bank_alloc(h, h->bankB, nc));
+    CK(bank_alloc(h, h->bankC, nc));
+    CK(dalloc(h, &h->keys, nc)); CK(dalloc(h, &h->keysAlt, nc));
+    CK(dalloc(h, &h->vals, nc)); CK(dalloc(h, &h->valsAlt, nc));
+    h->tileHistLen = 256ull * radix_tile_count(static_cast<uint32_t>(nc));
+    CK(dalloc(h, &h->tileHist, h->tileHistLen));
+    h->cap = nc;
+    return STORM_OK;
+}
+
+// Box-face data from BoundaryCondition::getInwardBoxFaceNormalIfClose
+// (boundary/BoundaryCondition.hpp:61-85) evaluated once with the same arithmetic.
+void box_faces(StormHandle *h) {
+    const double X0 = h->hxe.front(), X1 = h->hxe.back(), Y0 = h->hye.front(), Y1 = h->hye.back(), Z0 = h->hze.front(),
+                 Z1 = h->hze.back();
+    double V[6][3][3] = {
+        {{X0, Y0, Z0}, {X0, Y1, Z0}, {X0, Y1, Z1}}, {{X1, Y0, Z0}, {X1, Y1, Z0}, {X1, Y1, Z1}},
+        {{X0, Y0, Z0}, {X0, Y0, Z1}, {X1, Y0, Z1}}, {{X0, Y1, Z0}, {X0, Y1, Z1}, {X1, Y1, Z1}},
+        {{X0, Y0, Z0}, {X1, Y0, Z0}, {X1, Y1, Z0}}, {{X0, Y0, Z1}, {X1, Y0, Z1}, {X1, Y1, Z1}},
+    };
+    const double bc[3] = {0.5 * (X0 + X1), 0.5 * (Y0 + Y1), 0.5 * (Z0 + Z1)};
+    for (int f = 0; f < 6; ++f) {
+        BoxFaceDev &F = h->C.bf[f];
+        double u[3], v[3];
+        for (int a = 0; a < 3; ++a) {
+            u[a] = V[f][1][a] - V[f][0][a];
+            v[a] = V[f][2][a] - V[f][0][a];
+            F.on[a] = V[f][0][a];
+        }
+        F.raw[0] = u[1] * v[2] - u[2] * v[1];
+        F.raw[1] = u[2] * v[0] - u[0] * v[2];
+        F.raw[2] = u[0] * v[1] - u[1] * v[0];
+        double au = std::sqrt(u[0] * u[0] + u[1] * u[1] + u[2] * u[2]);
+        double av = std::sqrt(v[0] * v[0] + v[1] * v[1] + v[2] * v[2]);
+        double fs = std::min(au, av);
+        double nn = std::sqrt(F.raw[0] * F.raw[0] + F.raw[1] * F.raw[1] + F.raw[2] * F.raw[2]);
+        F.valid = (nn > 0.0) && std::isfinite(nn) && (fs > 0.0) && std::isfinite(fs);
+        F.thresh = 1e-12 * fs * fs * fs;
+        F.nudge = 1e-6 * fs;
+        double inv = 1.0 / nn;
+        double n[3] = {F.raw[0] * inv, F.raw[1] * inv, F.raw[2] * inv};
+        double tc = n[0] * (bc[0] - F.on[0]) + n[1] * (bc[1] - F.on[1]) + n[2] * (bc[2] - F.on[2]);
+        if (tc < 0.0) {
+            n[0] *= -1.0; n[1] *= -1.0; n[2] *= -1.0;
+        }
+        F.unit[0] = n[0]; F.unit[1] = n[1]; F.unit[2] = n[2];
+        F.action = h->desc.faces[f].action;
+        h->C.sourceT[f] = h->desc.faces[f].source_temperature;
+    }
+}
+
+// Boundary cell-faces with a source, cells in index order and sides in
+// GetCellFaces order (the order generateNewBoundaryParticles visits them).
+int build_face_sources(StormHandle *h) {
+    std::vector<uint32_t> cell;
+    std::vector<int32_t> side;
+    std::vector<uint64_t> off(1, 0);
+    const uint32_t nx = h->nx, ny = h->ny, nz = h->nz;
+    for (uint32_t c = 0; c < h->N; ++c) {
+        uint32_t i = c % nx, j = (c / nx) % ny, k = c / (nx * ny);
+        bool bnd[6] = {i == 0, i + 1 == nx, j == 0, j + 1 == ny, k == 0, k + 1 == nz};
+        for (int s = 0; s < 6; ++s) {
+            if (!bnd[s]) continue;
+            const StormBoxFace &bf = h->desc.faces[s];
+            if (!(bf.source_temperature > 0.0) || bf.packets_per_face == 0) continue;
+            cell.push_back(c);
+            side.push_back(s);
+            off.push_back(off.back() + bf.packets_per_face);
+        }
+    }
+    dfree(h, h->fsCell, h->fsCount);
+    dfree(h, h->fsSide, h->fsCount);
+    dfree(h, h->fsOffset, h->fsCount + 1);
+    h->fsCount = static_cast<uint32_t>(cell.size());
+    h->fsTotal = off.back();
+    CK(dalloc(h, &h->fsCell, cell.size()));
+    CK(dalloc(h, &h->fsSide, side.size()));
+    CK(dalloc(h, &h->fsOffset, off.size()));
+    if (!cell.empty()) {
+        CK(cudaMemcpy(h->fsCell, cell.data(), cell.size() * sizeof(uint32_t), cudaMemcpyHostToDevice));
+        CK(cudaMemcpy(h->fsSide, side.data(), side.size() * sizeof(int32_t), cudaMemcpyHostToDevice));
+    }
+    CK(cudaMemcpy(h->fsOffset, off.data(), off.size() * sizeof(uint64_t), cudaMemcpyHostToDevice));
+    return STORM_OK;
+}
+
+// RandomWalk tables (radiation/RandomWalk.hpp:23-79): tau and survival on the
+// host with the reference's arithmetic, the 1024x256 radius inverse on the device.
+double rw_survival(double tau) {
+    if (tau <= 0.0 || tau < 1e-4) return 1.0;
+    double sum = 0.0;
+    const double PI = 3.14159265358979323846;
+    for (int n = 1; n <= 500; ++n) {
+        double arg = -static_cast<double>(n * n) * PI * PI * tau;
+        if (arg < -700.0) break;
+        double term = std::exp(arg);
+        sum += (n % 2 == 1) ? term : -term;
+    }
+    double s = 2.0 * sum;
+    return s < 0.0 ? 0.0 : (1.0 < s ? 1.0 : s);
+}
+int build_rw_tables(StormHandle *h) {
+    std::vector<double> tau(RW_TABLE), ltau(RW_TABLE), surv(RW_TABLE);
+    const double logMin = std::log(1e-8), logMax = std::log(64.0);
+    for (int i = 0; i < RW_TABLE; ++i) {
+        double frac = static_cast<double>(i) / static_cast<double>(RW_TABLE - 1);
+        tau[i] = std::exp(logMin + frac * (logMax - logMin));
+        ltau[i] = std::log(tau[i]);
+        surv[i] = rw_survival(tau[i]);
+    }
+    CK(dalloc(h, &h->rwTau, RW_TABLE));
+    CK(dalloc(h, &h->rwLogTau, RW_TABLE));
+    CK(dalloc(h, &h->rwSurv, RW_TABLE));
+    CK(dalloc(h, &h->rwRadius, static_cast<size_t>(RW_TABLE) * RW_RADIUS));
+    CK(cudaMemcpy(h->rwTau, tau.data(), RW_TABLE * sizeof(double), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(h->rwLogTau, ltau.data(), RW_TABLE * sizeof(double), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(h->rwSurv, surv.data(), RW_TABLE * sizeof(double), cudaMemcpyHostToDevice));
+    launch_rw_radius(h->stream, h->rwTau, h->rwSurv, h->rwRadius);
+    ++h->launches;
+    CK(cudaGetLastError());
+    CK(cudaStreamSynchronize(h->stream));
+    h->C.rw.tau = h->rwTau;
+    h->C.rw.logTau = h->rwLogTau;
+    h->C.rw.surv = h->rwSurv;
+    h->C.rw.radius = h->rwRadius;
+    h->C.rw.logMin = logMin;
+    h->C.rw.logMax = logMax;
+    return STORM_OK;
+}
+
+int check_device_error(StormHandle *h) {
+    int32_t e[3] = {0, 0, 0};
+    CK(cudaMemcpyAsync(e, h->dErr, sizeof(e), cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    if (e[0] != 0) {
+        h->errCode = e[0];
+        h->errCell = static_cast<uint32_t>(e[1]);
+        h->errParticle = static_cast<uint32_t>(e[2]);
+        char buf[160];
+        std::snprintf(buf, sizeof(buf), "device error %d at cell %u particle %u", e[0], static_cast<uint32_t>(e[1]),
+                      static_cast<uint32_t>(e[2]));
+        h->errMsg = buf;
+        return STORM_ERR_DEVICE;
+    }
+    return STORM_OK;
+}
+
+void refresh_ctx(StormHandle *h) {
+    h->C.step = h->step;
+}
+
+uint32_t grid_transport(uint64_t n) {
+    uint64_t g = (n + 255) / 256;
+    const uint64_t cap = 148ull * 8;
+    if (g < 1) g = 1;
+    return static_cast<uint32_t>(g < cap ? g : cap);
+}
+
+}  // namespace
+
+// ====================================================================== C ABI
+extern "C" {
+
+int storm_cuda_abi_version(void) { return STORM_CUDA_ABI_VERSION; }
+
+const char *storm_cuda_status_string(int s) {
+    switch (s) {
+    case STORM_OK: return "ok";
+    case STORM_ERR_INVALID_ARG: return "invalid argument";
+    case STORM_ERR_CUDA: return "CUDA runtime error";
+    case STORM_ERR_OOM: return "device out of memory";
+    case STORM_ERR_DEVICE: return "device error word raised";
+    case STORM_ERR_CAPACITY: return "particle capacity exceeded";
+    case STORM_ERR_UNSUPPORTED: return "unsupported option";
+    case STORM_ERR_NO_DEVICE: return "no CUDA device";
+    default: return "unknown status";
+    }
+}
+
+int storm_cuda_create(const StormProblemDesc *d, StormHandle **out) {
+    if (!d || !out) return STORM_ERR_INVALID_ARG;
+    *out = nullptr;
+    if (d->abi_version != STORM_CUDA_ABI_VERSION) return STORM_ERR_INVALID_ARG;
+    if (d->nx == 0 || d->ny == 0 || d->nz == 0 || !d->x_edges || !d->y_edges || !d->z_edges) return STORM_ERR_INVALID_ARG;
+    if (!d->temperature || !d->mass || !d->internal_energy) return STORM_ERR_INVALID_ARG;
+    if (d->new_photons_per_cell == 0) return STORM_ERR_INVALID_ARG;   // RadiationIMC.hpp:584-588
+    if (d->opacity_kind == STORM_OPACITY_CELL_TABLE && !d->sigma_a) return STORM_ERR_INVALID_ARG;
+    if (d->opacity_kind != STORM_OPACITY_CELL_TABLE && d->opacity_kind != STORM_OPACITY_POWER_LAW)
+        return STORM_ERR_UNSUPPORTED;
+    if (d->eos_kind != STORM_EOS_LINEAR && d->eos_kind != STORM_EOS_POWER_LAW) return STORM_ERR_UNSUPPORTED;
+    if (d->precision != STORM_PRECISION_FP64) return STORM_ERR_UNSUPPORTED;
+    uint64_t N64 = static_cast<uint64_t>(d->nx) * d->ny * d->nz;
+    if (N64 >= 0x7fffffffull) return STORM_ERR_INVALID_ARG;
+    for (int a = 0; a < 3; ++a) {
+        const double *e = a == 0 ? d->x_edges : (a == 1 ? d->y_edges : d->z_edges);
+        uint32_t n = a == 0 ? d->nx : (a == 1 ? d->ny : d->nz);
+        for (uint32_t q = 0; q < n; ++q)
+            if (!(e[q + 1] > e[q])) return STORM_ERR_INVALID_ARG;
+    }
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return STORM_ERR_NO_DEVICE;
+    if (d->device < 0 || d->device >= ndev) return STORM_ERR_INVALID_ARG;
+
+    StormHandle *h = new StormHandle();
+    h->desc = *d;
+    h->device = d->device;
+    h->nx = d->nx; h->ny = d->ny; h->nz = d->nz;
+    h->N = static_cast<uint32_t>(N64);
+    const uint32_t N = h->N;
+    auto fail = [&](int rc) {
+        storm_cuda_destroy(h);
+        return rc;
+    };
+    if (cudaSetDevice(h->device) != cudaSuccess) return fail(STORM_ERR_CUDA);
+    if (cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking) != cudaSuccess) return fail(STORM_ERR_CUDA);
+    cudaEventCreate(&h->evStart);
+    cudaEventCreate(&h->evTransport0);
+    cudaEventCreate(&h->evTransport1);
+    cudaEventCreate(&h->evEnd);
+
+    h->hxe.assign(d->x_edges, d->x_edges + d->nx + 1);
+    h->hye.assign(d->y_edges, d->y_edges + d->ny + 1);
+    h->hze.assign(d->z_edges, d->z_edges + d->nz + 1);
+    h->hxc.resize(d->nx); h->hyc.resize(d->ny); h->hzc.resize(d->nz);
+    for (uint32_t i = 0; i < d->nx; ++i) h->hxc[i] = 0.5 * (h->hxe[i] + h->hxe[i + 1]);
+    for (uint32_t j = 0; j < d->ny; ++j) h->hyc[j] = 0.5 * (h->hye[j] + h->hye[j + 1]);
+    for (uint32_t k = 0; k < d->nz; ++k) h->hzc[k] = 0.5 * (h->hze[k] + h->hze[k + 1]);
+
+#define ALLOC(ptr, n) do { if (dalloc(h, &(ptr), (n)) != cudaSuccess) return fail(STORM_ERR_OOM); } while (0)
+#define H2D(dst, src, n) do { if (cudaMemcpy((dst), (src), sizeof(*(dst)) * (n), cudaMemcpyHostToDevice) != cudaSuccess) return fail(STORM_ERR_CUDA); } while (0)
+    ALLOC(h->xe, d->nx + 1); ALLOC(h->ye, d->ny + 1); ALLOC(h->ze, d->nz + 1);
+    ALLOC(h->xc, d->nx); ALLOC(h->yc, d->ny); ALLOC(h->zc, d->nz);
+    H2D(h->xe, h->hxe.data(), d->nx + 1); H2D(h->ye, h->hye.data(), d->ny + 1); H2D(h->ze, h->hze.data(), d->nz + 1);
+    H2D(h->xc, h->hxc.data(), d->nx); H2D(h->yc, h->hyc.data(), d->ny); H2D(h->zc, h->hzc.data(), d->nz);
+
+    CellArrays &A = h->A;
+    double **cd[] = {&A.T, &A.mass, &A.vol, &A.eint, &A.ceint, &A.sigA, &A.sigS, &A.fleck, &A.rwSigT, &A.eradAvg,
+                     &A.eradCensus, &A.emitE};
+    for (double **q : cd) ALLOC(*q, N);
+    ALLOC(A.rwElig, N);
+    ALLOC(A.photons, N);
+    ALLOC(h->segs, N);
+    std::vector<double> vol(N);
+    for (uint32_t c = 0; c < N; ++c) {
+        uint32_t i = c % d->nx, j = (c / d->nx) % d->ny, k = c / (d->nx * d->ny);
+        vol[c] = (h->hxe[i + 1] - h->hxe[i]) * (h->hye[j + 1] - h->hye[j]) * (h->hze[k + 1] - h->hze[k]);
+    }
+    H2D(A.vol, vol.data(), N);
+    H2D(A.T, d->temperature, N);
+    H2D(A.mass, d->mass, N);
+    H2D(A.eint, d->internal_energy, N);
+    H2D(A.ceint, d->cell_internal_energy ? d->cell_internal_energy : d->internal_energy, N);
+    if (cudaMemset(A.eradAvg, 0, N * sizeof(double)) != cudaSuccess) return fail(STORM_ERR_CUDA);
+    if (cudaMemset(A.eradCensus, 0, N * sizeof(double)) != cudaSuccess) return fail(STORM_ERR_CUDA);
+    if (cudaMemset(A.sigS, 0, N * sizeof(double)) != cudaSuccess) return fail(STORM_ERR_CUDA);
+    if (cudaMemset(A.rwElig, 0, N) != cudaSuccess) return fail(STORM_ERR_CUDA);
+    if (cudaMemset(A.photons, 0, N * sizeof(uint64_t)) != cudaSuccess) return fail(STORM_ERR_CUDA);
+    if (cudaMemset(h->segs, 0, N * sizeof(uint32_t)) != cudaSuccess) return fail(STORM_ERR_CUDA);
+    std::vector<double> ones(N, 1.0);
+    H2D(A.fleck, ones.data(), N);
+
+    OpacityEos &M = h->M;
+    M.opacityKind = d->opacity_kind;
+    M.eosKind = d->eos_kind;
+    if (d->opacity_kind == STORM_OPACITY_CELL_TABLE) {
+        ALLOC(h->tabA, N);
+        H2D(h->tabA, d->sigma_a, N);
+        if (d->sigma_s) {
+            ALLOC(h->tabS, N);
+            H2D(h->tabS, d->sigma_s, N);
+        }
+    }
+    if (d->density_factor) {
+        ALLOC(h->rhoF, N);
+        H2D(h->rhoF, d->density_factor, N);
+    }
+    M.tabA = h->tabA; M.tabS = h->tabS; M.rhoF = h->rhoF;
+    M.kP0 = d->kP0; M.kR0 = d->kR0; M.alpha = d->alpha; M.tFloor = d->t_floor; M.cap = d->cap;
+    M.cvPerMass = d->cv_per_mass; M.eosF = d->eos_f; M.eosBeta = d->eos_beta; M.eosMu = d->eos_mu;
+
+    ALLOC(h->offsets, N + 1);
+    ALLOC(h->tileSums, (N + 1023) / 1024 + 1);
+    ALLOC(h->dTotalU64, 2);
+    ALLOC(h->dTotalE, 2);
+    ALLOC(h->combW, N);
+    ALLOC(h->combWtot, 2);
+    ALLOC(h->combStart, N + 2);
+    ALLOC(h->combCount, N + 1);
+    h->maxRounds = d->max_rounds ? d->max_rounds : 16384;
+    ALLOC(h->counts, h->maxRounds + 2);
+    ALLOC(h->dStats, 1);
+    ALLOC(h->dErr, 4);
+    if (cudaMemset(h->dErr, 0, 4 * sizeof(int32_t)) != cudaSuccess) return fail(STORM_ERR_CUDA);
+    h->K = d->segments_per_visit ? d->segments_per_visit : 8;
+
+    Ctx &C = h->C;
+    C.nx = d->nx; C.ny = d->ny; C.nz = d->nz; C.ncells = N;
+    C.xe = h->xe; C.ye = h->ye; C.ze = h->ze; C.xc = h->xc; C.yc = h->yc; C.zc = h->zc;
+    C.X0 = h->hxe.front(); C.X1 = h->hxe.back();
+    C.Y0 = h->hye.front(); C.Y1 = h->hye.back();
+    C.Z0 = h->hze.front(); C.Z1 = h->hze.back();
+    box_faces(h);
+    C.escapeNoCheck = d->escape_without_check;
+    C.withRW = d->with_random_walk;
+    C.noFeedback = d->no_hydro_feedback;
+    C.perCellCounters = d->per_cell_segment_counters;
+    C.clight = d->clight; C.arad = d->arad; C.sigmaSB = d->sigma_sb; C.kevKelvin = d->kev_kelvin;
+    C.rwMinParticle = d->rw_min_particle_optical_depth;
+    C.rwMinCell = d->rw_min_cell_optical_depth;
+    C.seedLo = static_cast<uint32_t>(d->seed);
+    C.seedHi = static_cast<uint32_t>(d->seed >> 32);
+    C.step = 0;
+    C.sigA = A.sigA; C.sigS = A.sigS; C.fleck = A.fleck; C.rwSigT = A.rwSigT; C.rwElig = A.rwElig;
+    C.eint = A.eint; C.eradAvg = A.eradAvg; C.segs = h->segs;
+    C.err = h->dErr;
+
+    if (build_face_sources(h) != STORM_OK) return fail(STORM_ERR_CUDA);
+    if (build_rw_tables(h) != STORM_OK) return fail(STORM_ERR_CUDA);
+    size_t cap0 = d->capacity ? d->capacity : std::max<size_t>(1u << 20, N * d->new_photons_per_cell * 4 + h->fsTotal * 2);
+    int rc = ensure_capacity(h, cap0, 0);
+    if (rc != STORM_OK) return fail(rc);
+    // clear the desc's borrowed pointers: the caller may free them after create
+    h->desc.x_edges = h->desc.y_edges = h->desc.z_edges = nullptr;
+    h->desc.temperature = h->desc.mass = h->desc.internal_energy = h->desc.cell_internal_energy = nullptr;
+    h->desc.sigma_a = h->desc.sigma_s = h->desc.density_factor = nullptr;
+#undef ALLOC
+#undef H2D
+    *out = h;
+    return STORM_OK;
+}
+
+int storm_cuda_destroy(StormHandle *h) {
+    if (!h) return STORM_OK;
+    cudaSetDevice(h->device);
+    if (h->stream) cudaStreamSynchronize(h->stream);
+    bank_free(h, h->bankA, h->cap);
+    bank_free(h, h->bankB, h->cap);
+    bank_free(h, h->bankC, h->cap);
+    void *ps[] = {h->xe, h->ye, h->ze, h->xc, h->yc, h->zc, h->A.T, h->A.mass, h->A.vol, h->A.eint, h->A.ceint,
+                  h->A.sigA, h->A.sigS, h->A.fleck, h->A.rwSigT, h->A.eradAvg, h->A.eradCensus, h->A.emitE,
+                  h->A.rwElig, h->A.photons, h->segs, h->tabA, h->tabS, h->rhoF, h->rwTau, h->rwLogTau, h->rwSurv,
+                  h->rwRadius, h->fsCell, h->fsSide, h->fsOffset, h->keys, h->keysAlt, h->vals, h->valsAlt,
+                  h->tileHist, h->offsets, h->tileSums, h->dTotalU64, h->dTotalE, h->combW, h->combWtot,
+                  h->combStart, h->combCount, h->counts, h->dStats, h->dErr};
+    for (void *p : ps)
+        if (p) cudaFree(p);
+    cudaEvent_t evs[] = {h->evStart, h->evTransport0, h->evTransport1, h->evEnd};
+    for (cudaEvent_t e : evs)
+        if (e) cudaEventDestroy(e);
+    for (cudaEvent_t e : h->evPool)
+        if (e) cudaEventDestroy(e);
+    if (h->stream) cudaStreamDestroy(h->stream);
+    delete h;
+    return STORM_OK;
+}
+
+int storm_cuda_phase_begin(StormHandle *h, double dt) {
+    if (!h || !(dt > 0.0)) return STORM_ERR_INVALID_ARG;
+    CK(cudaSetDevice(h->device));
+    h->errCode = 0;
+    h->stats = StormStepStats{};
+    CK(cudaMemsetAsync(h->dStats, 0, sizeof(DevStats), h->stream));
+    CK(cudaMemsetAsync(h->dErr, 0, 4 * sizeof(int32_t), h->stream));
+    refresh_ctx(h);
+    h->stats.census_in = h->nCensus;
+    if (h->nCensus) {
+        launch_begin(h->stream, h->bankA, static_cast<uint32_t>(h->nCensus), dt, h->dStats);
+        ++h->launches;
+    }
+    h->nBank = h->nCensus;
+    CK(cudaGetLastError());
+    return STORM_OK;
+}
+
+int storm_cuda_phase_prestep(StormHandle *h, double dt) {
+    if (!h) return STORM_ERR_INVALID_ARG;
+    refresh_ctx(h);
+    launch_prestep(h->stream, h->C, h->A, h->M, dt);
+    ++h->launches;
+    CK(cudaGetLastError());
+    return STORM_OK;
+}
+
+int storm_cuda_phase_emit(StormHandle *h, double dt) {
+    if (!h) return STORM_ERR_INVALID_ARG;
+    refresh_ctx(h);
+    const uint32_t N = h->N;
+    launch_emission_energy(h->stream, h->C, h->A, dt);
+    launch_sequential_sum(h->stream, h->A.emitE, N, h->dTotalE);
+    launch_allocate(h->stream, h->C, h->A, h->dTotalE, h->desc.new_photons_per_cell);
+    launch_emission_debit(h->stream, h->C, h->A, h->dStats);
+    launch_scan_u64(h->stream, h->A.photons, N, h->offsets, h->tileSums, h->dTotalU64);
+    h->launches += 7;
+    CK(cudaGetLastError());
+    uint64_t ne = 0;
+    CK(cudaMemcpyAsync(&ne, h->dTotalU64, sizeof(uint64_t), cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    const uint64_t nf = h->fsTotal;
+    const uint64_t total = h->nCensus + ne + nf;
+    int rc = ensure_capacity(h, total, h->nCensus);
+    if (rc != STORM_OK) return rc;
+    launch_emit_cells(h->stream, h->C, h->A, h->offsets, ne, h->bankA, static_cast<uint32_t>(h->nCensus), dt, h->dStats);
+    FaceSources F{h->fsCell, h->fsSide, h->fsOffset, h->fsCount};
+    launch_emit_faces(h->stream, h->C, F, nf, h->bankA, static_cast<uint32_t>(h->nCensus + ne), dt, h->dStats);
+    h->launches += (ne ? 1 : 0) + (nf ? 1 : 0);
+    CK(cudaGetLastError());
+    h->stats.emitted_cells = ne;
+    h->stats.emitted_faces = nf;
+    h->nBank = total;
+    return STORM_OK;
+}
+
+int storm_cuda_phase_transport(StormHandle *h) {
+    if (!h) return STORM_ERR_INVALID_ARG;
+    refresh_ctx(h);
+    const uint64_t n0 = h->nBank;
+    CK(cudaEventRecord(h->evTransport0, h->stream));
+    CK(cudaMemsetAsync(h->counts, 0, sizeof(uint32_t) * (h->maxRounds + 2), h->stream));
+    if (h->desc.per_cell_segment_counters) CK(cudaMemsetAsync(h->segs, 0, sizeof(uint32_t) * h->N, h->stream));
+    uint32_t n32 = static_cast<uint32_t>(n0);
+    CK(cudaMemcpyAsync(h->counts, &n32, sizeof(uint32_t), cudaMemcpyHostToDevice, h->stream));
+    uint32_t *nCen = h->counts + h->maxRounds + 1;
+    const uint32_t grid = grid_transport(n0);
+    uint32_t r = 0;
+    bool done = (n0 == 0);
+    const uint32_t pollEvery = 4;
+    uint32_t remaining = n32;
+    if (h->profiling && h->evPool.empty()) {
+        h->evPool.resize(2 * pollEvery);
+        for (auto &e : h->evPool) CK(cudaEventCreate(&e));
+    }
+    uint32_t inWindow = 0;
+    while (!done && r < h->maxRounds) {
+        const Bank &in = (r & 1) ? h->bankB : h->bankA;
+        const Bank &out = (r & 1) ? h->bankA : h->bankB;
+        if (h->profiling) CK(cudaEventRecord(h->evPool[2 * inWindow], h->stream));
+        launch_transport(h->stream, grid, h->C, in, h->counts + r, out, h->counts + r + 1, h->bankC, nCen, h->K,
+                         h->dStats);
+        if (h->profiling) CK(cudaEventRecord(h->evPool[2 * inWindow + 1], h->stream));
+        ++inWindow;
+        ++h->launches;
+        ++r;
+        if (r % pollEvery == 0 || r == h->maxRounds) {
+            CK(cudaGetLastError());
+            CK(cudaMemcpyAsync(&remaining, h->counts + r, sizeof(uint32_t), cudaMemcpyDeviceToHost, h->stream));
+            CK(cudaStreamSynchronize(h->stream));
+            if (h->profiling) {
+                for (uint32_t q = 0; q < inWindow; ++q) {
+                    float ms = 0.f;
+                    CK(cudaEventElapsedTime(&ms, h->evPool[2 * q], h->evPool[2 * q + 1]));
+                    h->profMs += ms;
+                }
+                h->profLaunches += inWindow;
+            }
+            inWindow = 0;
+            if (remaining == 0) done = true;
+            int32_t e0 = 0;
+            CK(cudaMemcpy(&e0, h->dErr, sizeof(int32_t), cudaMemcpyDeviceToHost));
+            if (e0) break;
+        }
+    }
+    CK(cudaEventRecord(h->evTransport1, h->stream));
+    h->stats.rounds = r;
+    int rc = check_device_error(h);
+    if (rc != STORM_OK) return rc;
+    if (!done) {
+        h->errCode = STORM_DERR_HISTORY_CAP;
+        h->errMsg = "transport did not finish within max_rounds bank visits";
+        return STORM_ERR_DEVICE;
+    }
+    uint32_t nc = 0;
+    CK(cudaMemcpy(&nc, nCen, sizeof(uint32_t), cudaMemcpyDeviceToHost));
+    h->stats.census_out_pre_comb = nc;
+    if (h->profiling) {
+        DevStats d{};
+        CK(cudaMemcpy(&d, h->dStats, sizeof(d), cudaMemcpyDeviceToHost));
+        h->profSegments += d.segments;
+    }
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, h->evTransport0, h->evTransport1);
+    h->lastTransportMs = ms;
+    h->nBank = 0;
+    return STORM_OK;
+}
+
+int storm_cuda_phase_comb(StormHandle *h) {
+    if (!h) return STORM_ERR_INVALID_ARG;
+    refresh_ctx(h);
+    const uint32_t n = static_cast<uint32_t>(h->stats.census_out_pre_comb);
+    const uint32_t N = h->N;
+    CK(cudaMemsetAsync(h->A.eradCensus, 0, sizeof(double) * N, h->stream));
+    if (n == 0) {
+        h->nCensus = 0;
+        h->stats.census_out = 0;
+        return STORM_OK;
+    }
+    if (!h->desc.comb_enabled) {
+        // NoPopulationControl (population/NoPopulationControl.hpp:25-28): the census
+        // passes unchanged; order it by pid so the next step's streams are reproducible.
+        launch_census_keys_pid(h->stream, h->bankC, n, h->keys, h->vals);
+        int alt = launch_radix_sort(h->stream, h->keys, h->vals, h->keysAlt, h->valsAlt, n, 32, h->tileHist);
+        const uint32_t *idx = alt ? h->valsAlt : h->vals;
+        launch_gather(h->stream, h->bankC, idx, n, h->bankA, h->A.eradCensus, h->dStats);
+        h->launches += 2 + 3 * 4;
+        CK(cudaGetLastError());
+        h->nCensus = n;
+        h->stats.census_out = n;
+        return check_device_error(h);
+    }
+    // CombPopulationControl::activate
+    const uint32_t combKey = [&] {
+        auto fm = [](uint32_t x) {
+            x ^= x >> 16; x *= 0x85ebca6bu; x ^= x >> 13; x *= 0xc2b2ae35u; x ^= x >> 16;
+            return x;
+        };
+        return fm(static_cast<uint32_t>(h->desc.seed) ^ fm(h->step * 0x9E3779B9u + static_cast<uint32_t>(h->desc.seed >> 32)));
+    }();
+    launch_comb_keys(h->stream, h->C, h->bankC, n, h->keys, h->vals, combKey);
+    int cellBits = 0;
+    while ((1ull << cellBits) <= N) ++cellBits;
+    int alt = launch_radix_sort(h->stream, h->keys, h->vals, h->keysAlt, h->valsAlt, n, 32 + cellBits, h->tileHist);
+    const uint64_t *skeys = alt ? h->keysAlt : h->keys;
+    const uint32_t *idx = alt ? h->valsAlt : h->vals;
+    const int passes = (32 + cellBits + 7) / 8;
+    launch_comb_ranges(h->stream, skeys, n, N, h->combStart);
+    launch_comb_cell_sums(h->stream, h->bankC, idx, h->combStart, N, h->combW);
+    launch_blocked_sum(h->stream, h->combW, N, h->combWtot);
+    CombParams P;
+    P.nmin = h->desc.comb_nmin;
+    P.ntotal = static_cast<uint64_t>(static_cast<double>(static_cast<uint64_t>(N) * h->desc.comb_nmin) * h->desc.comb_factor);
+    launch_comb_count(h->stream, h->C, P, h->bankC, idx, h->combStart, h->combW, h->combWtot, h->combCount);
+    launch_scan_u64(h->stream, h->combCount, N, h->offsets, h->tileSums, h->dTotalU64);
+    h->launches += 1 + 3 * passes + 4 + 3;
+    CK(cudaGetLastError());
+    int rc = check_device_error(h);
+    if (rc != STORM_OK) return rc;
+    uint64_t total = 0;
+    CK(cudaMemcpy(&total, h->dTotalU64, sizeof(uint64_t), cudaMemcpyDeviceToHost));
+    // the write goes to bank A, which transport has finished with
+    if (total > h->cap) {
+        // grow: bank C (the census) must survive, so grow around it
+        size_t nc = total + total / 4;
+        Bank newA{}, newC{};
+        CK(bank_alloc(h, newA, nc));
+        CK(bank_alloc(h, newC, nc));
+        CK(bank_copy(h->stream, newC, h->bankC, n));
+        CK(cudaStreamSynchronize(h->stream));
+        bank_free(h, h->bankA, h->cap);
+        bank_free(h, h->bankB, h->cap);
+        bank_free(h, h->bankC, h->cap);
+        dfree(h, h->keys, h->cap); dfree(h, h->keysAlt, h->cap);
+        dfree(h, h->vals, h->cap); dfree(h, h->valsAlt, h->cap);
+        // keep the sorted indices: copy them into fresh buffers
+        uint32_t *idxNew = nullptr;
+        CK(dalloc(h, &idxNew, nc));
+        CK(cudaMemcpyAsync(idxNew, idx, sizeof(uint32_t) * n, cudaMemcpyDeviceToDevice, h->stream));
+        CK(cudaStreamSynchronize(h->stream));
+        h->bankA = newA;
+        h->bankC = newC;
+        CK(bank_alloc(h, h->bankB, nc));
+        CK(dalloc(h, &h->keys, nc)); CK(dalloc(h, &h->keysAlt, nc));
+        h->vals = idxNew;
+        CK(dalloc(h, &h->valsAlt, nc));
+        dfree(h, h->tileHist, h->tileHistLen);
+        h->tileHistLen = 256ull * radix_tile_count(static_cast<uint32_t>(nc));
+        CK(dalloc(h, &h->tileHist, h->tileHistLen));
+        h->cap = nc;
+        idx = h->vals;
+    }
+    launch_comb_write(h->stream, h->C, P, h->bankC, idx, h->combStart, h->combW, h->combWtot, h->offsets, h->bankA,
+                      h->A.eradCensus, h->dStats);
+    ++h->launches;
+    CK(cudaGetLastError());
+    h->nCensus = total;
+    h->stats.census_out = total;
+    return check_device_error(h);
+}
+
+int storm_cuda_phase_poststep(StormHandle *h, double dt) {
+    if (!h) return STORM_ERR_INVALID_ARG;
+    refresh_ctx(h);
+    launch_poststep(h->stream, h->C, h->A, h->M, dt);
+    ++h->launches;
+    CK(cudaGetLastError());
+    int rc = check_device_error(h);
+    ++h->step;
+    return rc;
+}
+
+int storm_cuda_phase_stats(StormHandle *h, StormStepStats *s) {
+    if (!h || !s) return STORM_ERR_INVALID_ARG;
+    DevStats d{};
+    CK(cudaMemcpyAsync(&d, h->dStats, sizeof(d), cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    *s = h->stats;
+    s->segments = d.segments;
+    s->rw_steps = d.rwSteps;
+    s->escaped = d.escaped;
+    s->cutoff = d.cutoff;
+    s->energy_census_in = d.eCensusIn;
+    s->energy_emitted = d.eEmitted;
+    s->energy_deposited = d.eDeposited;
+    s->energy_escaped = d.eEscaped;
+    s->energy_census_pre_comb = d.eCensusPre;
+    s->energy_census_out = d.eCensusOut;
+    s->energy_emission_debit = d.eDebit;
+    s->transport_ms = h->lastTransportMs;
+    s->step_ms = h->lastStepMs;
+    return STORM_OK;
+}
+
+int storm_cuda_step(StormHandle *h, double dt, StormStepStats *stats) {
+    if (!h) return STORM_ERR_INVALID_ARG;
+    CK(cudaSetDevice(h->device));
+    CK(cudaEventRecord(h->evStart, h->stream));
+    int rc = storm_cuda_phase_begin(h, dt);
+    if (rc == STORM_OK) rc = storm_cuda_phase_prestep(h, dt);
+    if (rc == STORM_OK) rc = storm_cuda_phase_emit(h, dt);
+    if (rc == STORM_OK) rc = storm_cuda_phase_transport(h);
+    if (rc == STORM_OK) rc = storm_cuda_phase_comb(h);
+    if (rc == STORM_OK) rc = storm_cuda_phase_poststep(h, dt);
+    CK(cudaEventRecord(h->evEnd, h->stream));
+    CK(cudaEventSynchronize(h->evEnd));
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, h->evStart, h->evEnd);
+    h->lastStepMs = ms;
+    if (stats) storm_cuda_phase_stats(h, stats);
+    return rc;
+}
+
+// ---------------------------------------------------------------- state in/out
+int storm_cuda_set_census(StormHandle *h, const StormParticlesSoA *in) {
+    if (!h || !in) return STORM_ERR_INVALID_ARG;
+    CK(cudaSetDevice(h->device));
+    const uint64_t n = in->count;
+    int rc = ensure_capacity(h, n, 0);
+    if (rc != STORM_OK) return rc;
+    const double *sd[] = {in->x, in->y, in->z, in->vx, in->vy, in->vz, in->time_left, in->weight, in->initial_weight};
+    double *dd[] = {h->bankA.x, h->bankA.y, h->bankA.z, h->bankA.vx, h->bankA.vy, h->bankA.vz, h->bankA.t, h->bankA.w,
+                    h->bankA.w0};
+    for (int q = 0; q < 9; ++q) {
+        if (!sd[q] && n) return STORM_ERR_INVALID_ARG;
+        if (n) CK(cudaMemcpyAsync(dd[q], sd[q], n * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+    }
+    if (n) {
+        if (!in->cell) return STORM_ERR_INVALID_ARG;
+        std::vector<uint32_t> cells(in->cell, in->cell + n);
+        for (uint32_t c : cells)
+            if (c >= h->N) return STORM_ERR_INVALID_ARG;
+        CK(cudaMemcpyAsync(h->bankA.cell, in->cell, n * sizeof(uint32_t), cudaMemcpyHostToDevice, h->stream));
+        CK(cudaStreamSynchronize(h->stream));
+    }
+    h->nCensus = n;
+    return STORM_OK;
+}
+
+int storm_cuda_population_control(StormHandle *h, const StormParticlesSoA *in) {
+    if (!h || !in) return STORM_ERR_INVALID_ARG;
+    CK(cudaSetDevice(h->device));
+    const uint64_t n = in->count;
+    int rc = ensure_capacity(h, n, 0);
+    if (rc != STORM_OK) return rc;
+    const double *sd[] = {in->x, in->y, in->z, in->vx, in->vy, in->vz, in->time_left, in->weight, in->initial_weight};
+    double *dd[] = {h->bankC.x, h->bankC.y, h->bankC.z, h->bankC.vx, h->bankC.vy, h->bankC.vz, h->bankC.t, h->bankC.w,
+                    h->bankC.w0};
+    if (n) {
+        for (int q = 0; q < 9; ++q) {
+            if (!sd[q]) return STORM_ERR_INVALID_ARG;
+            CK(cudaMemcpyAsync(dd[q], sd[q], n * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+        }
+        if (!in->cell) return STORM_ERR_INVALID_ARG;
+        for (uint64_t q = 0; q < n; ++q)
+            if (in->cell[q] >= h->N) return STORM_ERR_INVALID_ARG;
+        std::vector<uint32_t> pid(n);
+        for (uint64_t q = 0; q < n; ++q) pid[q] = static_cast<uint32_t>(q);
+        CK(cudaMemcpyAsync(h->bankC.cell, in->cell, n * sizeof(uint32_t), cudaMemcpyHostToDevice, h->stream));
+        CK(cudaMemcpyAsync(h->bankC.pid, pid.data(), n * sizeof(uint32_t), cudaMemcpyHostToDevice, h->stream));
+        CK(cudaStreamSynchronize(h->stream));
+    }
+    CK(cudaMemsetAsync(h->dStats, 0, sizeof(DevStats), h->stream));
+    CK(cudaMemsetAsync(h->dErr, 0, 4 * sizeof(int32_t), h->stream));
+    h->stats = StormStepStats{};
+    h->stats.census_out_pre_comb = n;
+    return storm_cuda_phase_comb(h);
+}
+
+int storm_cuda_census_count(StormHandle *h, uint64_t *count) {
+    if (!h || !count) return STORM_ERR_INVALID_ARG;
+    *count = h->nCensus;
+    return STORM_OK;
+}
+
+int storm_cuda_get_census(StormHandle *h, StormParticlesSoA *out, uint64_t capacity, uint64_t *count) {
+    if (!h || !out) return STORM_ERR_INVALID_ARG;
+    CK(cudaSetDevice(h->device));
+    const uint64_t n = std::min<uint64_t>(h->nCensus, capacity);
+    if (count) *count = h->nCensus;
+    const double *sd[] = {h->bankA.x, h->bankA.y, h->bankA.z, h->bankA.vx, h->bankA.vy, h->bankA.vz, h->bankA.t,
+                          h->bankA.w, h->bankA.w0};
+    double *dd[] = {out->x, out->y, out->z, out->vx, out->vy, out->vz, out->time_left, out->weight, out->initial_weight};
+    for (int q = 0; q < 9; ++q)
+        if (dd[q] && n) CK(cudaMemcpyAsync(dd[q], sd[q], n * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+    if (out->cell && n) CK(cudaMemcpyAsync(out->cell, h->bankA.cell, n * sizeof(uint32_t), cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    if (out->id)
+        for (uint64_t q = 0; q < n; ++q) out->id[q] = q;
+    out->count = n;
+    return STORM_OK;
+}
+
+int storm_cuda_get_cell_arrays(StormHandle *h, double *T, double *eint, double *eradAvg, double *eradCensus,
+                               double *sigA, double *fleck, uint64_t *segs) {
+    if (!h) return STORM_ERR_INVALID_ARG;
+    CK(cudaSetDevice(h->device));
+    const size_t N = h->N;
+    const double *src[] = {h->A.T, h->A.eint, h->A.eradAvg, h->A.eradCensus, h->A.sigA, h->A.fleck};
+    double *dst[] = {T, eint, eradAvg, eradCensus, sigA, fleck};
+    for (int q = 0; q < 6; ++q)
+        if (dst[q]) CK(cudaMemcpyAsync(dst[q], src[q], N * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+    std::vector<uint32_t> s32;
+    if (segs) {
+        s32.resize(N);
+        CK(cudaMemcpyAsync(s32.data(), h->segs, N * sizeof(uint32_t), cudaMemcpyDeviceToHost, h->stream));
+    }
+    CK(cudaStreamSynchronize(h->stream));
+    if (segs)
+        for (size_t q = 0; q < N; ++q) segs[q] = s32[q];
+    return STORM_OK;
+}
+
+int storm_cuda_set_cell_state(StormHandle *h, const double *T, const double *eint, const double *ceint) {
+    if (!h) return STORM_ERR_INVALID_ARG;
+    CK(cudaSetDevice(h->device));
+    const size_t N = h->N;
+    if (T) CK(cudaMemcpyAsync(h->A.T, T, N * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+    if (eint) CK(cudaMemcpyAsync(h->A.eint, eint, N * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+    if (ceint) CK(cudaMemcpyAsync(h->A.ceint, ceint, N * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    return STORM_OK;
+}
+
+int storm_cuda_set_cell_physics(StormHandle *h, const double *sigA, const double *sigS, const double *fleck) {
+    if (!h) return STORM_ERR_INVALID_ARG;
+    CK(cudaSetDevice(h->device));
+    const size_t N = h->N;
+    if (sigA) CK(cudaMemcpyAsync(h->A.sigA, sigA, N * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+    if (sigS) CK(cudaMemcpyAsync(h->A.sigS, sigS, N * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+    if (fleck) CK(cudaMemcpyAsync(h->A.fleck, fleck, N * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    if (h->desc.with_random_walk) {
+        launch_rw_eligibility(h->stream, h->C, h->A);
+        ++h->launches;
+        CK(cudaGetLastError());
+        CK(cudaStreamSynchronize(h->stream));
+    }
+    return STORM_OK;
+}
+
+int storm_cuda_set_face_temperature(StormHandle *h, int face, double T) {
+    if (!h || face < 0 || face > 5 || !(T >= 0.0)) return STORM_ERR_INVALID_ARG;
+    CK(cudaSetDevice(h->device));
+    const bool wasSource = h->desc.faces[face].source_temperature > 0.0;
+    h->desc.faces[face].source_temperature = T;
+    h->C.sourceT[face] = T;
+    if (wasSource != (T > 0.0)) return build_face_sources(h);
+    return STORM_OK;
+}
+
+int storm_cuda_get_emission(StormHandle *h, uint64_t *photons, double *energy) {
+    if (!h) return STORM_ERR_INVALID_ARG;
+    CK(cudaSetDevice(h->device));
+    if (photons) CK(cudaMemcpyAsync(photons, h->A.photons, h->N * sizeof(uint64_t), cudaMemcpyDeviceToHost, h->stream));
+    if (energy) CK(cudaMemcpyAsync(energy, h->A.emitE, h->N * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    return STORM_OK;
+}
+
+// ---------------------------------------------------------------- parity
+int storm_cuda_replay_segments(StormHandle *h, StormReplayBatch *b) {
+    if (!h || !b) return STORM_ERR_INVALID_ARG;
+    CK(cudaSetDevice(h->device));
+    const uint64_t n = b->n;
+    if (n == 0) return STORM_OK;
+    if (n > 0x7fffffffull) return STORM_ERR_INVALID_ARG;
+    uint64_t tapeLen = 0;
+    for (uint64_t q = 0; q < n; ++q) tapeLen = std::max<uint64_t>(tapeLen, b->tape_offset[q] + b->tape_length[q]);
+    CK(cudaStreamSynchronize(h->stream));
+    std::vector<void *> owned;
+    auto up = [&](const void *src, size_t bytes) -> void * {
+        void *p = nullptr;
+        if (cudaMalloc(&p, bytes ? bytes : 8) != cudaSuccess) return nullptr;
+        owned.push_back(p);
+        if (src && bytes) cudaMemcpy(p, src, bytes, cudaMemcpyHostToDevice);
+        return p;
+    };
+    ReplayDev R{};
+    const double *ins[9] = {b->x, b->y, b->z, b->vx, b->vy, b->vz, b->time_left, b->weight, b->initial_weight};
+    for (int q = 0; q < 9; ++q) R.in[q] = static_cast<const double *>(up(ins[q], n * sizeof(double)));
+    R.cell = static_cast<const uint32_t *>(up(b->cell, n * sizeof(uint32_t)));
+    R.tapeOffset = static_cast<const uint64_t *>(up(b->tape_offset, n * sizeof(uint64_t)));
+    R.tapeLength = static_cast<const uint32_t *>(up(b->tape_length, n * sizeof(uint32_t)));
+    R.tape = static_cast<const double *>(up(b->tape, tapeLen * sizeof(double)));
+    for (int q = 0; q < 8; ++q) R.phys[q] = static_cast<double *>(up(nullptr, n * sizeof(double)));
+    for (int q = 0; q < 2; ++q) R.dep[q] = static_cast<double *>(up(nullptr, n * sizeof(double)));
+    for (int q = 0; q < 6; ++q) R.mgr[q] = static_cast<double *>(up(nullptr, n * sizeof(double)));
+    R.physStatus = static_cast<int32_t *>(up(nullptr, n * sizeof(int32_t)));
+    R.physNext = static_cast<uint32_t *>(up(nullptr, n * sizeof(uint32_t)));
+    R.mgrCell = static_cast<uint32_t *>(up(nullptr, n * sizeof(uint32_t)));
+    R.mgrStatus = static_cast<int32_t *>(up(nullptr, n * sizeof(int32_t)));
+    R.draws = static_cast<uint32_t *>(up(nullptr, n * sizeof(uint32_t)));
+    R.usedRW = static_cast<int32_t *>(up(nullptr, n * sizeof(int32_t)));
+    bool ok = true;
+    for (void *p : owned) ok = ok && p;
+    int rc = STORM_OK;
+    if (!ok) rc = STORM_ERR_OOM;
+    if (rc == STORM_OK) {
+        refresh_ctx(h);
+        launch_replay(h->stream, h->C, R, static_cast<uint32_t>(n));
+        ++h->launches;
+        if (cudaGetLastError() != cudaSuccess || cudaStreamSynchronize(h->stream) != cudaSuccess) rc = STORM_ERR_CUDA;
+    }
+    if (rc == STORM_OK) {
+        double *ph[8] = {b->phys_x, b->phys_y, b->phys_z, b->phys_vx, b->phys_vy, b->phys_vz, b->phys_time_left,
+                         b->phys_weight};
+        for (int q = 0; q < 8; ++q) cudaMemcpy(ph[q], R.phys[q], n * sizeof(double), cudaMemcpyDeviceToHost);
+        double *mg[6] = {b->mgr_x, b->mgr_y, b->mgr_z, b->mgr_vx, b->mgr_vy, b->mgr_vz};
+        for (int q = 0; q < 6; ++q) cudaMemcpy(mg[q], R.mgr[q], n * sizeof(double), cudaMemcpyDeviceToHost);
+        cudaMemcpy(b->dep_material, R.dep[0], n * sizeof(double), cudaMemcpyDeviceToHost);
+        cudaMemcpy(b->dep_erad, R.dep[1], n * sizeof(double), cudaMemcpyDeviceToHost);
+        cudaMemcpy(b->phys_status, R.physStatus, n * sizeof(int32_t), cudaMemcpyDeviceToHost);
+        cudaMemcpy(b->phys_next_cell, R.physNext, n * sizeof(uint32_t), cudaMemcpyDeviceToHost);
+        cudaMemcpy(b->mgr_cell, R.mgrCell, n * sizeof(uint32_t), cudaMemcpyDeviceToHost);
+        cudaMemcpy(b->mgr_status, R.mgrStatus, n * sizeof(int32_t), cudaMemcpyDeviceToHost);
+        cudaMemcpy(b->draws_used, R.draws, n * sizeof(uint32_t), cudaMemcpyDeviceToHost);
+        cudaMemcpy(b->used_random_walk, R.usedRW, n * sizeof(int32_t), cudaMemcpyDeviceToHost);
+    }
+    for (void *p : owned)
+        if (p) cudaFree(p);
+    return rc;
+}
+
+int storm_cuda_get_random_walk_tables(StormHandle *h, double *tau, double *survival, double *radius) {
+    if (!h) return STORM_ERR_INVALID_ARG;
+    CK(cudaSetDevice(h->device));
+    CK(cudaStreamSynchronize(h->stream));
+    if (tau) CK(cudaMemcpy(tau, h->rwTau, RW_TABLE * sizeof(double), cudaMemcpyDeviceToHost));
+    if (survival) CK(cudaMemcpy(survival, h->rwSurv, RW_TABLE * sizeof(double), cudaMemcpyDeviceToHost));
+    if (radius)
+        CK(cudaMemcpy(radius, h->rwRadius, static_cast<size_t>(RW_TABLE) * RW_RADIUS * sizeof(double),
+                      cudaMemcpyDeviceToHost));
+    return STORM_OK;
+}
+
+int storm_cuda_random_walk_sample(StormHandle *h, uint64_t n, const double *xiLeak, const double *tau,
+                                  const double *xiRad, double *leakOut, double *radOut) {
+    if (!h || n == 0 || n > 0x7fffffffull) return STORM_ERR_INVALID_ARG;
+    CK(cudaSetDevice(h->device));
+    CK(cudaStreamSynchronize(h->stream));
+    double *d[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
+    for (int q = 0; q < 5; ++q) CK(cudaMalloc(&d[q], n * sizeof(double)));
+    if (xiLeak) CK(cudaMemcpy(d[0], xiLeak, n * sizeof(double), cudaMemcpyHostToDevice));
+    if (tau) CK(cudaMemcpy(d[1], tau, n * sizeof(double), cudaMemcpyHostToDevice));
+    if (xiRad) CK(cudaMemcpy(d[2], xiRad, n * sizeof(double), cudaMemcpyHostToDevice));
+    launch_rw_sample(h->stream, h->C.rw, static_cast<uint32_t>(n), xiLeak ? d[0] : nullptr, tau ? d[1] : nullptr,
+                     xiRad ? d[2] : nullptr, d[3], d[4]);
+    ++h->launches;
+    CK(cudaGetLastError());
+    CK(cudaStreamSynchronize(h->stream));
+    if (leakOut && xiLeak) CK(cudaMemcpy(leakOut, d[3], n * sizeof(double), cudaMemcpyDeviceToHost));
+    if (radOut && tau && xiRad) CK(cudaMemcpy(radOut, d[4], n * sizeof(double), cudaMemcpyDeviceToHost));
+    for (int q = 0; q < 5; ++q) cudaFree(d[q]);
+    return STORM_OK;
+}
+
+// ---------------------------------------------------------------- diagnostics
+int storm_cuda_last_error(StormHandle *h, int32_t *derr, uint64_t *cell, uint64_t *particle, char *msg, size_t len) {
+    if (!h) return STORM_ERR_INVALID_ARG;
+    if (derr) *derr = h->errCode;
+    if (cell) *cell = h->errCell;
+    if (particle) *particle = h->errParticle;
+    if (msg && len) std::snprintf(msg, len, "%s", h->errMsg.c_str());
+    return STORM_OK;
+}
+
+int storm_cuda_memory_bytes(StormHandle *h, uint64_t *bytes) {
+    if (!h || !bytes) return STORM_ERR_INVALID_ARG;
+    *bytes = h->memBytes;
+    return STORM_OK;
+}
+
+int storm_cuda_launch_count(StormHandle *h, uint64_t *launches) {
+    if (!h || !launches) return STORM_ERR_INVALID_ARG;
+    *launches = h->launches;
+    return STORM_OK;
+}
+
+int storm_cuda_set_profiling(StormHandle *h, int on) {
+    if (!h) return STORM_ERR_INVALID_ARG;
+    h->profiling = on != 0;
+    return STORM_OK;
+}
+
+int storm_cuda_transport_timing(StormHandle *h, double *ms, uint64_t *launches, uint64_t *segments, int reset) {
+    if (!h) return STORM_ERR_INVALID_ARG;
+    if (ms) *ms = h->profMs;
+    if (launches) *launches = h->profLaunches;
+    if (segments) *segments = h->profSegments;
+    if (reset) {
+        h->profMs = 0.0;
+        h->profLaunches = 0;
+        h->profSegments = 0;
+    }
+    return STORM_OK;
+}
+
+int storm_cuda_set_segments_per_visit(StormHandle *h, uint32_t k) {
+    if (!h || k == 0) return STORM_ERR_INVALID_ARG;
+    h->K = k;
+    return STORM_OK;
+}
+
+}  // extern "C"

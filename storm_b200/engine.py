@@ -1,0 +1,229 @@
+"""ctypes binding of libstorm_cuda.so (include/storm_cuda.h).
+
+The engine has no CPU fallback: loading fails loudly when the shared library is
+missing, and creating a handle fails with STORM_ERR_NO_DEVICE without a GPU.
+"""
+import ctypes as C
+import os
+import numpy as np
+
+from . import _abi as A
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libstorm_cuda.so")
+_lib = None
+
+
+class StormError(RuntimeError):
+    """Raised for a nonzero status; mirrors STORM::StormError (StormError.hpp:13-48)."""
+
+    def __init__(self, status, msg, derr=0, cell=0, particle=0):
+        self.status, self.derr, self.cell, self.particle = status, derr, cell, particle
+        super().__init__(f"{A.STATUS_NAMES.get(status, status)}: {msg} "
+                         f"(device error {A.DERR_NAMES.get(derr, derr)}, cell {cell}, particle {particle})")
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise RuntimeError(f"CUDA engine library not built: {LIB_PATH} (run python -m storm_b200.build)")
+        L = C.CDLL(LIB_PATH)
+        vp, dp = C.c_void_p, C.POINTER(C.c_double)
+        u64p, u32p, i32p = C.POINTER(C.c_uint64), C.POINTER(C.c_uint32), C.POINTER(C.c_int32)
+        L.storm_cuda_create.argtypes = [C.POINTER(A.StormProblemDesc), C.POINTER(vp)]
+        L.storm_cuda_destroy.argtypes = [vp]
+        L.storm_cuda_step.argtypes = [vp, C.c_double, C.POINTER(A.StormStepStats)]
+        for f in ("begin", "prestep", "emit", "poststep"):
+            getattr(L, "storm_cuda_phase_" + f).argtypes = [vp, C.c_double]
+        for f in ("transport", "comb"):
+            getattr(L, "storm_cuda_phase_" + f).argtypes = [vp]
+        L.storm_cuda_phase_stats.argtypes = [vp, C.POINTER(A.StormStepStats)]
+        L.storm_cuda_set_census.argtypes = [vp, C.POINTER(A.StormParticlesSoA)]
+        L.storm_cuda_get_census.argtypes = [vp, C.POINTER(A.StormParticlesSoA), C.c_uint64, u64p]
+        L.storm_cuda_census_count.argtypes = [vp, u64p]
+        L.storm_cuda_population_control.argtypes = [vp, C.POINTER(A.StormParticlesSoA)]
+        L.storm_cuda_get_cell_arrays.argtypes = [vp, dp, dp, dp, dp, dp, dp, u64p]
+        L.storm_cuda_set_cell_state.argtypes = [vp, dp, dp, dp]
+        L.storm_cuda_set_cell_physics.argtypes = [vp, dp, dp, dp]
+        L.storm_cuda_set_face_temperature.argtypes = [vp, C.c_int, C.c_double]
+        L.storm_cuda_get_emission.argtypes = [vp, u64p, dp]
+        L.storm_cuda_replay_segments.argtypes = [vp, C.POINTER(A.StormReplayBatch)]
+        L.storm_cuda_get_random_walk_tables.argtypes = [vp, dp, dp, dp]
+        L.storm_cuda_random_walk_sample.argtypes = [vp, C.c_uint64, dp, dp, dp, dp, dp]
+        L.storm_cuda_last_error.argtypes = [vp, i32p, u64p, u64p, C.c_char_p, C.c_size_t]
+        L.storm_cuda_memory_bytes.argtypes = [vp, u64p]
+        L.storm_cuda_launch_count.argtypes = [vp, u64p]
+        L.storm_cuda_set_segments_per_visit.argtypes = [vp, C.c_uint32]
+        L.storm_cuda_set_profiling.argtypes = [vp, C.c_int]
+        L.storm_cuda_transport_timing.argtypes = [vp, dp, u64p, u64p, C.c_int]
+        L.storm_cuda_status_string.restype = C.c_char_p
+        L.storm_cuda_status_string.argtypes = [C.c_int]
+        L.storm_cuda_abi_version.restype = C.c_int
+        _lib = L
+    return _lib
+
+
+class Particles:
+    """Host struct-of-arrays census (the fields of Particle<T,Grid> the gray path uses)."""
+    FIELDS = ("x", "y", "z", "vx", "vy", "vz", "time_left", "weight", "initial_weight")
+
+    def __init__(self, n=0):
+        for f in self.FIELDS:
+            setattr(self, f, np.zeros(n))
+        self.cell = np.zeros(n, np.uint32)
+        self.id = np.zeros(n, np.uint64)
+        self.n = n
+
+    def soa(self):
+        s = A.StormParticlesSoA()
+        for f in self.FIELDS:
+            setattr(s, f, A.ptr(getattr(self, f)))
+        s.cell = A.ptr(self.cell, C.c_uint32)
+        s.id = A.ptr(self.id, C.c_uint64)
+        s.count = self.n
+        return s
+
+    def __len__(self):
+        return self.n
+
+
+class Engine:
+    """One IMC problem on the GPU (a StormHandle)."""
+
+    def __init__(self, problem):
+        self.problem = problem
+        self.desc = problem.to_desc()
+        h = C.c_void_p()
+        self._check(lib().storm_cuda_create(C.byref(self.desc), C.byref(h)), handle=None)
+        self.h = h
+        self.n = problem.ncells
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().storm_cuda_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        self.close()
+
+    def _check(self, rc, handle="self"):
+        if rc == A.STORM_OK:
+            return
+        derr, cell, part = C.c_int32(), C.c_uint64(), C.c_uint64()
+        msg = C.create_string_buffer(512)
+        hh = self.h if handle == "self" else None
+        if hh:
+            lib().storm_cuda_last_error(hh, C.byref(derr), C.byref(cell), C.byref(part), msg, 512)
+        raise StormError(rc, msg.value.decode() or lib().storm_cuda_status_string(rc).decode(), derr.value,
+                         cell.value, part.value)
+
+    # ---------------------------------------------------------------- step
+    def step(self, dt=None):
+        st = A.StormStepStats()
+        self._check(lib().storm_cuda_step(self.h, self.problem.dt if dt is None else dt, C.byref(st)))
+        return st.as_dict()
+
+    def phase(self, name, dt=None):
+        dt = self.problem.dt if dt is None else dt
+        L = lib()
+        if name in ("begin", "prestep", "emit", "poststep"):
+            self._check(getattr(L, "storm_cuda_phase_" + name)(self.h, dt))
+        else:
+            self._check(getattr(L, "storm_cuda_phase_" + name)(self.h))
+
+    def stats(self):
+        st = A.StormStepStats()
+        self._check(lib().storm_cuda_phase_stats(self.h, C.byref(st)))
+        return st.as_dict()
+
+    # ---------------------------------------------------------------- state
+    def census_count(self):
+        n = C.c_uint64()
+        self._check(lib().storm_cuda_census_count(self.h, C.byref(n)))
+        return n.value
+
+    def census(self):
+        n = self.census_count()
+        p = Particles(n)
+        s = p.soa()
+        cnt = C.c_uint64()
+        self._check(lib().storm_cuda_get_census(self.h, C.byref(s), n, C.byref(cnt)))
+        return p
+
+    def set_census(self, p):
+        s = p.soa()
+        self._check(lib().storm_cuda_set_census(self.h, C.byref(s)))
+
+    def population_control(self, p):
+        """CombPopulationControl::activate on host particles; returns the new census."""
+        s = p.soa()
+        self._check(lib().storm_cuda_population_control(self.h, C.byref(s)))
+        return self.census()
+
+    def cells(self):
+        keys = ("temperature", "internal_energy", "erad_time_avg", "erad_census", "sigma_a", "fleck")
+        out = {k: np.zeros(self.n) for k in keys}
+        segs = np.zeros(self.n, np.uint64)
+        self._check(lib().storm_cuda_get_cell_arrays(self.h, *[A.ptr(out[k]) for k in keys], A.ptr(segs, C.c_uint64)))
+        out["segments"] = segs
+        return out
+
+    def set_cell_state(self, temperature=None, internal_energy=None, cell_internal_energy=None):
+        arr = [None if a is None else np.ascontiguousarray(a, float)
+               for a in (temperature, internal_energy, cell_internal_energy)]
+        self._check(lib().storm_cuda_set_cell_state(self.h, *[A.ptr(a) for a in arr]))
+
+    def set_cell_physics(self, sigma_a=None, sigma_s=None, fleck=None):
+        arr = [None if a is None else np.ascontiguousarray(a, float) for a in (sigma_a, sigma_s, fleck)]
+        self._check(lib().storm_cuda_set_cell_physics(self.h, *[A.ptr(a) for a in arr]))
+
+    def set_face_temperature(self, face, T):
+        self._check(lib().storm_cuda_set_face_temperature(self.h, face, T))
+
+    def emission(self):
+        c = np.zeros(self.n, np.uint64)
+        e = np.zeros(self.n)
+        self._check(lib().storm_cuda_get_emission(self.h, A.ptr(c, C.c_uint64), A.ptr(e)))
+        return c, e
+
+    # ---------------------------------------------------------------- parity
+    def replay(self, batch):
+        """batch: object with .struct (StormReplayBatch) and host arrays."""
+        self._check(lib().storm_cuda_replay_segments(self.h, C.byref(batch.struct)))
+        return batch
+
+    def rw_tables(self):
+        tau, s, r = np.zeros(1024), np.zeros(1024), np.zeros(1024 * 256)
+        self._check(lib().storm_cuda_get_random_walk_tables(self.h, A.ptr(tau), A.ptr(s), A.ptr(r)))
+        return tau, s, r.reshape(1024, 256)
+
+    def rw_sample(self, xi_leak, tau, xi_rad):
+        n = len(xi_leak)
+        leak, rad = np.zeros(n), np.zeros(n)
+        a = [np.ascontiguousarray(v, float) for v in (xi_leak, tau, xi_rad)]
+        self._check(lib().storm_cuda_random_walk_sample(self.h, n, A.ptr(a[0]), A.ptr(a[1]), A.ptr(a[2]),
+                                                        A.ptr(leak), A.ptr(rad)))
+        return leak, rad
+
+    # ---------------------------------------------------------------- diagnostics
+    def memory_bytes(self):
+        b = C.c_uint64()
+        self._check(lib().storm_cuda_memory_bytes(self.h, C.byref(b)))
+        return b.value
+
+    def launches(self):
+        b = C.c_uint64()
+        self._check(lib().storm_cuda_launch_count(self.h, C.byref(b)))
+        return b.value
+
+    def set_profiling(self, on=True):
+        self._check(lib().storm_cuda_set_profiling(self.h, int(on)))
+
+    def transport_timing(self, reset=False):
+        ms, n, s = C.c_double(), C.c_uint64(), C.c_uint64()
+        self._check(lib().storm_cuda_transport_timing(self.h, C.byref(ms), C.byref(n), C.byref(s), int(reset)))
+        return {"kernel_ms": ms.value, "launches": n.value, "segments": s.value}
+
+    def set_segments_per_visit(self, k):
+        self._check(lib().storm_cuda_set_segments_per_visit(self.h, k))

@@ -1,0 +1,118 @@
+"""Generate the golden fixtures in this directory from the reference build
+(oracle/_ref/libstormref.so: STORM's own serial path compiled from the reference
+sources against oracle/shims).  Run in a container where the reference sources
+are present:
+
+    make -C oracle && python tests/golden/make_golden.py
+
+Fixtures (numpy .npz):
+  replay_slab.npz     recorded RadiationIMC::step calls on the gray slab (boundary
+                      reflect / escape, face crossings, collisions, census, cutoff)
+  replay_cube_rw.npz  recorded calls on an 8^3 step-opacity cube with Random Walk
+  rw_samples.npz      RandomWalk::sampleLeakTime / sampleRadius at seeded points
+  samplers.npz        RandomInCellPositionSampler / isotropicVelocity /
+                      RandomPointOnFace outputs with the draws each consumed
+  allocation_slab.npz photon counts per cell (getLastSourcePhotonsPerCell) and the
+                      cell temperatures they were allocated from, several steps
+"""
+import os
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.dirname(os.path.dirname(HERE)))
+
+from oracle import ref  # noqa: E402
+from storm_b200 import problems  # noqa: E402
+
+
+def record(problem, warm_steps, max_records, take):
+    r = ref.Reference(problem)
+    for _ in range(warm_steps):
+        r.step()
+    c = r.cells()     # tables of the last step; the recorded step recomputes them
+    r.record_begin(max_records)
+    r.step()
+    r.record_end()
+    rec = r.records()
+    c = r.cells()
+    n = len(rec["cell"])
+    # keep a deterministic, representative subset: every k-th record plus all
+    # boundary interactions and Random Walk jumps
+    idx = np.arange(n)
+    special = (rec["status"] == 1) & (rec["next"] >= problem.ncells)
+    special |= rec["used_rw"] == 1
+    special |= rec["status"] == 3
+    sub = idx[(idx % max(1, n // take) == 0) | special]
+    if len(sub) > 3 * take:
+        sub = sub[np.linspace(0, len(sub) - 1, 3 * take).astype(int)]
+    tape_off = rec["tape_offset"][sub]
+    tape_len = rec["tape_length"][sub]
+    tape = np.concatenate([rec["tape"][o:o + l] for o, l in zip(tape_off, tape_len)]) if len(sub) else np.zeros(0)
+    new_off = np.concatenate([[0], np.cumsum(tape_len)[:-1]]).astype(np.uint64)
+    # chained successor (the same particle's next record) for the manager check
+    nxt_before = np.full((len(sub), 6), np.nan)
+    nxt_cell = np.full(len(sub), -1, np.int64)
+    for q, k in enumerate(sub):
+        if k + 1 < n and rec["id"][k + 1] == rec["id"][k]:
+            nxt_before[q] = rec["before"][k + 1][:6]
+            nxt_cell[q] = rec["cell"][k + 1]
+    return dict(before=rec["before"][sub], after=rec["after"][sub], status=rec["status"][sub],
+                next=rec["next"][sub].astype(np.int64), tallies=rec["tallies"][sub], cell=rec["cell"][sub],
+                used_rw=rec["used_rw"][sub], tape=tape, tape_offset=new_off, tape_length=tape_len,
+                next_before=nxt_before, next_cell=nxt_cell, sigma_a=c["sigma_a"], fleck=c["fleck"])
+
+
+def main():
+    slab = problems.gray_slab(new_photons_per_cell=5, face_packets=2000, comb_nmin=50)
+    np.savez_compressed(os.path.join(HERE, "replay_slab.npz"), **record(slab, 2, 400000, 1500))
+
+    cube = problems.step_cube(n=8, new_photons_per_cell=3, face_packets=40, comb_nmin=20)
+    np.savez_compressed(os.path.join(HERE, "replay_cube_rw.npz"), **record(cube, 1, 400000, 1500))
+
+    rng = np.random.default_rng(7)
+    xi_leak = np.concatenate([rng.random(3000), [1e-300, 1e-12, 0.5, 1 - 1e-12, np.nextafter(1, 0)]])
+    tau = np.concatenate([10 ** rng.uniform(-10, 2.5, 3000), [1e-9, 1e-8, 64.0, 100.0, 0.01]])
+    xi_rad = np.concatenate([rng.random(3000), [0.0, 1.0, 0.5, 1e-9, 1 - 1e-9]])
+    leak, rad = ref.rw_sample(xi_leak, tau, xi_rad)
+    t_grid = 10 ** np.linspace(-9, 2, 400)
+    x_grid = rng.random(400)
+    surv, cdf = ref.rw_functions(t_grid, x_grid)
+    np.savez_compressed(os.path.join(HERE, "rw_samples.npz"), xi_leak=xi_leak, tau=tau, xi_rad=xi_rad, leak=leak,
+                        radius=rad, t_grid=t_grid, x_grid=x_grid, survival=surv, cdf=cdf)
+
+    small = problems.step_cube(n=4)
+    rs = ref.Reference(small)
+    cells = rng.integers(0, small.ncells, 500).astype(np.uint32)
+    pos, ptape, nd = rs.sample_in_cell(cells, 12345)
+    vel, vtape = ref.isotropic(500, 99)
+    nxf = 5 * 4 * 4
+    faces = rng.integers(0, 3 * nxf, 300).astype(np.uint64)
+    fpos, ftape = rs.point_on_face(faces)
+    np.savez_compressed(os.path.join(HERE, "samplers.npz"), cells=cells, cell_pos=pos, cell_tape=ptape,
+                        cell_draws=nd, vel=vel, vel_tape=vtape, faces=faces, face_pos=fpos, face_tape=ftape,
+                        x_edges=small.x_edges, y_edges=small.y_edges, z_edges=small.z_edges)
+
+    slab2 = problems.gray_slab(new_photons_per_cell=5, face_packets=2000, comb_nmin=50)
+    r2 = ref.Reference(slab2)
+    T_before, counts, eint_before, sig, fl = [], [], [], [], []
+    for _ in range(4):
+        c = r2.cells()
+        T_before.append(c["temperature"])
+        eint_before.append(c["internal_energy"])
+        r2.step()
+        counts.append(r2.emission_counts())
+        c = r2.cells()
+        sig.append(c["sigma_a"])
+        fl.append(c["fleck"])
+    np.savez_compressed(os.path.join(HERE, "allocation_slab.npz"), temperature=np.array(T_before),
+                        internal_energy=np.array(eint_before), photons=np.array(counts), sigma_a=np.array(sig),
+                        fleck=np.array(fl))
+    for f in sorted(os.listdir(HERE)):
+        if f.endswith(".npz"):
+            print(f, os.path.getsize(os.path.join(HERE, f)))
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,91 @@
+"""The C-ABI library loads without a GPU, exports every entry point the header
+declares, and its struct layouts match the ctypes mirror."""
+import ctypes as C
+import os
+import re
+import subprocess
+import tempfile
+
+import pytest
+
+from conftest import ROOT
+from storm_b200 import _abi as A
+from storm_b200 import engine, problems
+
+HEADER = os.path.join(ROOT, "include", "storm_cuda.h")
+
+
+def declared_symbols():
+    text = open(HEADER).read()
+    return sorted(set(re.findall(r"\b(storm_cuda_[a-z0-9_]+)\s*\(", text)))
+
+
+def test_library_exports_header_symbols():
+    L = engine.lib()
+    syms = declared_symbols()
+    assert len(syms) >= 25
+    for s in syms:
+        assert hasattr(L, s), s
+    assert L.storm_cuda_abi_version() == A.ABI_VERSION
+
+
+def test_struct_layout_matches_header():
+    prog = r'''
+#include <stddef.h>
+#include <stdio.h>
+#include "storm_cuda.h"
+int main(void) {
+  printf("%zu %zu %zu %zu %zu\n", sizeof(StormProblemDesc), sizeof(StormParticlesSoA), sizeof(StormStepStats),
+         sizeof(StormReplayBatch), sizeof(StormBoxFace));
+  printf("%zu %zu %zu %zu\n", offsetof(StormProblemDesc, faces), offsetof(StormProblemDesc, seed),
+         offsetof(StormProblemDesc, device), offsetof(StormReplayBatch, used_random_walk));
+  return 0;
+}
+'''
+    with tempfile.TemporaryDirectory() as d:
+        src = os.path.join(d, "t.c")
+        exe = os.path.join(d, "t")
+        open(src, "w").write(prog)
+        r = subprocess.run(["gcc", "-I" + os.path.join(ROOT, "include"), src, "-o", exe], capture_output=True)
+        if r.returncode != 0:
+            pytest.skip("no C compiler")
+        out = subprocess.run([exe], capture_output=True, text=True).stdout.split()
+    sizes = [int(x) for x in out]
+    assert sizes[:5] == [C.sizeof(A.StormProblemDesc), C.sizeof(A.StormParticlesSoA), C.sizeof(A.StormStepStats),
+                         C.sizeof(A.StormReplayBatch), C.sizeof(A.StormBoxFace)]
+    assert sizes[5:] == [A.StormProblemDesc.faces.offset, A.StormProblemDesc.seed.offset,
+                         A.StormProblemDesc.device.offset, A.StormReplayBatch.used_random_walk.offset]
+
+
+def _create(desc):
+    h = C.c_void_p()
+    return engine.lib().storm_cuda_create(C.byref(desc), C.byref(h)), h
+
+
+def test_create_rejects_invalid_descriptors():
+    p = problems.gray_slab()
+    d = p.to_desc()
+    d.abi_version = 99
+    assert _create(d)[0] == 1
+    d = p.to_desc()
+    d.new_photons_per_cell = 0          # RadiationIMC requires newPhotonsPerCell > 0
+    assert _create(d)[0] == 1
+    d = p.to_desc()
+    d.nx = 0
+    assert _create(d)[0] == 1
+    d = p.to_desc()
+    d.opacity_kind = 9
+    assert _create(d)[0] == 6
+    e = p.x_edges.copy()
+    e[3] = e[2]                          # edges must increase strictly
+    p2 = problems.gray_slab()
+    p2.x_edges = e
+    assert _create(p2.to_desc())[0] == 1
+
+
+def test_create_without_device_fails_loudly():
+    import torch
+    if torch.cuda.is_available():
+        pytest.skip("a GPU is visible")
+    rc, _ = _create(problems.gray_slab().to_desc())
+    assert rc == 7   # STORM_ERR_NO_DEVICE: no CPU fallback
