@@ -537,8 +537,10 @@ __global__ void k_comb_keys(Ctx C, Bank cen, uint32_t n, uint64_t *keys, uint32_
         const uint32_t pid = cen.pid[q];
         uint32_t cell = cen.cell[q];
         if (outside_box(C, x, y, z)) raise_error(C, STORM_DERR_COMB_OUTSIDE, cell, pid);
-        if (!isfinite(w) || w < 0.0) raise_error(C, STORM_DERR_COMB_WEIGHT, cell, pid);
-        if (w == 0.0) cell = C.ncells;
+        const bool badWeight = !isfinite(w) || w < 0.0;
+        if (badWeight) raise_error(C, STORM_DERR_COMB_WEIGHT, cell, pid);
+        // zero, negative and non-finite weights never reach the per-cell loops
+        if (w == 0.0 || badWeight || cell >= C.ncells) cell = C.ncells;
         keys[q] = (static_cast<uint64_t>(cell) << 32) | fmix32(pid ^ combKey);
         vals[q] = q;
     }
