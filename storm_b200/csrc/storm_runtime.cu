@@ -711,41 +711,35 @@ int storm_cuda_phase_comb(StormHandle *h) {
     if (rc != STORM_OK) return rc;
     uint64_t total = 0;
     CK(cudaMemcpy(&total, h->dTotalU64, sizeof(uint64_t), cudaMemcpyDeviceToHost));
-    // the write goes to bank A, which transport has finished with
+    // The write goes to bank A, which transport has finished with.  When the
+    // combed census outgrows the banks, A and B are replaced first (their
+    // contents are dead); C and the sort buffers, which the write still reads,
+    // are replaced after it.
+    size_t grown = 0;
     if (total > h->cap) {
-        // grow: bank C (the census) must survive, so grow around it
-        size_t nc = total + total / 4;
-        Bank newA{}, newC{};
-        CK(bank_alloc(h, newA, nc));
-        CK(bank_alloc(h, newC, nc));
-        CK(bank_copy(h->stream, newC, h->bankC, n));
-        CK(cudaStreamSynchronize(h->stream));
+        grown = total + total / 4;
         bank_free(h, h->bankA, h->cap);
         bank_free(h, h->bankB, h->cap);
-        bank_free(h, h->bankC, h->cap);
-        dfree(h, h->keys, h->cap); dfree(h, h->keysAlt, h->cap);
-        dfree(h, h->vals, h->cap); dfree(h, h->valsAlt, h->cap);
-        // keep the sorted indices: copy them into fresh buffers
-        uint32_t *idxNew = nullptr;
-        CK(dalloc(h, &idxNew, nc));
-        CK(cudaMemcpyAsync(idxNew, idx, sizeof(uint32_t) * n, cudaMemcpyDeviceToDevice, h->stream));
-        CK(cudaStreamSynchronize(h->stream));
-        h->bankA = newA;
-        h->bankC = newC;
-        CK(bank_alloc(h, h->bankB, nc));
-        CK(dalloc(h, &h->keys, nc)); CK(dalloc(h, &h->keysAlt, nc));
-        h->vals = idxNew;
-        CK(dalloc(h, &h->valsAlt, nc));
-        dfree(h, h->tileHist, h->tileHistLen);
-        h->tileHistLen = 256ull * radix_tile_count(static_cast<uint32_t>(nc));
-        CK(dalloc(h, &h->tileHist, h->tileHistLen));
-        h->cap = nc;
-        idx = h->vals;
+        CK(bank_alloc(h, h->bankA, grown));
+        CK(bank_alloc(h, h->bankB, grown));
     }
     launch_comb_write(h->stream, h->C, P, h->bankC, idx, h->combStart, h->combW, h->combWtot, h->offsets, h->bankA,
                       h->A.eradCensus, h->dStats);
     ++h->launches;
     CK(cudaGetLastError());
+    if (grown) {
+        CK(cudaStreamSynchronize(h->stream));
+        bank_free(h, h->bankC, h->cap);
+        dfree(h, h->keys, h->cap); dfree(h, h->keysAlt, h->cap);
+        dfree(h, h->vals, h->cap); dfree(h, h->valsAlt, h->cap);
+        dfree(h, h->tileHist, h->tileHistLen);
+        CK(bank_alloc(h, h->bankC, grown));
+        CK(dalloc(h, &h->keys, grown)); CK(dalloc(h, &h->keysAlt, grown));
+        CK(dalloc(h, &h->vals, grown)); CK(dalloc(h, &h->valsAlt, grown));
+        h->tileHistLen = 256ull * radix_tile_count(static_cast<uint32_t>(grown));
+        CK(dalloc(h, &h->tileHist, h->tileHistLen));
+        h->cap = grown;
+    }
     h->nCensus = total;
     h->stats.census_out = total;
     return check_device_error(h);

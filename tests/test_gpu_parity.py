@@ -44,10 +44,16 @@ def _check_replay(b, g, ncells, near_tie_allowance=0.001):
     moved = ok & (g["status"] == 1)
     np.testing.assert_array_equal(b["phys_next_cell"][moved].astype(np.int64), g["next"][moved])
     names = ["phys_x", "phys_y", "phys_z", "phys_vx", "phys_vy", "phys_vz", "phys_time_left", "phys_weight"]
-    box = 1.0
     for k, nm in enumerate(names):
-        atol = 1e-13 * box if k < 3 else 0.0
-        good = close(b[nm][ok], g["after"][ok, k], atol=atol if k < 3 else 1e-300)
+        if k < 3:
+            atol = 1e-13                     # positions: cm, box size 1
+        elif k == 7:
+            # w *= 1 + expm1(-tau): for large tau the sum cancels, so an ulp of
+            # CUDA's expm1 is an ulp of the segment's starting weight
+            atol = 8e-16 * np.abs(g["before"][ok, 7])
+        else:
+            atol = 1e-300
+        good = close(b[nm][ok], g["after"][ok, k], atol=atol)
         assert good.all(), (nm, np.where(~good)[0][:5])
     dm = g["tallies"][:, 1] - g["tallies"][:, 0]
     de = g["tallies"][:, 3] - g["tallies"][:, 2]
@@ -122,6 +128,8 @@ def _pair(p):
 
 def _compare_census(ce, co):
     assert ce.n == co.n
+    if ce.n == 0:
+        return
     for f in ("x", "y", "z", "vx", "vy", "vz", "weight", "initial_weight"):
         ok = close(getattr(ce, f), getattr(co, f), 1e-12, atol=1e-300 if f[0] != "x" else 1e-14)
         assert ok.mean() > 0.999, (f, (~ok).sum())
