@@ -310,6 +310,31 @@ int storm_cuda_get_random_walk_tables(StormHandle *h, double *tau, double *survi
 int storm_cuda_random_walk_sample(StormHandle *h, uint64_t n, const double *xi_leak, const double *tau,
                                   const double *xi_radius, double *leak_out, double *radius_out);
 
+/* ---------------------------------------------------------------- allocation-free variant */
+
+/* Largest cell count storm_cuda_emission_allocation_noalloc accepts. */
+#define STORM_NOALLOC_MAX_CELLS (1u << 24)
+
+/* Photon counts per cell for an emission step (the per-cell counts
+ * storm_cuda_phase_emit computes and storm_cuda_get_emission returns), for
+ * callers that cannot allocate device memory while they run: code recording
+ * into a CUDA graph, a host framework whose allocator owns the device memory,
+ * a loop with a no-allocation rule.  This entry point has no counterpart in
+ * the reference; it calls no cudaMalloc / cudaFree and no allocating library
+ * routine.
+ *   d_energy   per-cell emission energy (device, ncells)
+ *   d_photons  out: photons per cell (device, ncells)
+ *   d_offsets  out: exclusive prefix sum of d_photons, d_offsets[ncells] = total (device, ncells + 1)
+ *   stream     cudaStream_t to run on (NULL = the legacy default stream)
+ * Its scratch is one fixed array inside the library (about 128 KiB per GPU
+ * that loads the library, held until exit).  The first call on a device looks
+ * up that array's device address; make the first call before any stream
+ * capture.  Calls whose work overlaps on the GPU share the array and race.
+ * ncells above STORM_NOALLOC_MAX_CELLS returns STORM_ERR_INVALID_ARG. */
+int storm_cuda_emission_allocation_noalloc(int device, const double *d_energy, uint32_t ncells,
+                                           uint64_t new_photons_per_cell, uint64_t *d_photons,
+                                           uint64_t *d_offsets, void *stream);
+
 /* ---------------------------------------------------------------- diagnostics */
 
 /* First device error word, the cell and particle it was raised for, and a message. */
