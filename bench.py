@@ -44,6 +44,8 @@ def parse():
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--segments-per-visit", type=int, default=0)
+    ap.add_argument("--min-blocks", type=int, default=0, help="transport occupancy variant (1-4)")
+    ap.add_argument("--waves", type=int, default=4)
     return ap.parse_args()
 
 
@@ -215,6 +217,8 @@ def run_storm(args, ws, rank, local, dist):
     eng = Engine(p)
     if args.segments_per_visit:
         eng.set_segments_per_visit(args.segments_per_visit)
+    if args.min_blocks:
+        eng.set_transport_variant(args.min_blocks, args.waves)
     eng.set_profiling(True)
     for _ in range(args.warmup):
         eng.step()

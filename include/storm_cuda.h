@@ -350,6 +350,10 @@ int storm_cuda_launch_count(StormHandle *h, uint64_t *launches);
  * launches and the segments they ran since the last reset. */
 int storm_cuda_set_profiling(StormHandle *h, int on);
 int storm_cuda_transport_timing(StormHandle *h, double *kernel_ms, uint64_t *launches, uint64_t *segments, int reset);
+/* Transport kernel variant (autotuner hook): the occupancy target of the
+ * kernel (__launch_bounds__ minimum blocks per SM, 1-4) and the grid size in
+ * waves of resident blocks. */
+int storm_cuda_set_transport_variant(StormHandle *h, int min_blocks_per_sm, int waves);
 /* Segment-per-visit override (autotuner hook). */
 int storm_cuda_set_segments_per_visit(StormHandle *h, uint32_t k);
 const char *storm_cuda_status_string(int status);

@@ -68,6 +68,7 @@ struct Ctx {
     double sourceT[6];       // source temperature of each box face [K]
     uint32_t seedLo, seedHi, step;
     // per-cell arrays
+    const double4 *phys;     // per-cell segment constants (CellPhys layout)
     const double *sigA, *sigS, *fleck, *rwSigT;
     const uint8_t *rwElig;
     double *eint, *eradAvg;
@@ -251,8 +252,9 @@ struct LocalTally {
 // RadiationIMC::tryRandomWalkStep (radiation/RadiationIMC.hpp:1065-1276), gray.
 // Returns -1 when the walk is not taken (no draws consumed), else a ParticleStatus.
 template <class RNG, class TALLY>
-__device__ inline int try_random_walk(const Ctx &C, PartReg &p, RNG &rng, TALLY &tal, double xl, double xh, double yl,
-                                      double yh, double zl, double zh, double cx, double cy, double cz) {
+__device__ inline int try_random_walk(const Ctx &C, PartReg &p, RNG &rng, TALLY &tal, const double4 &cp, double xl,
+                                      double xh, double yl, double yh, double zl, double zh, double cx, double cy,
+                                      double cz) {
     const uint32_t cell = p.cell;
     // computeMinDistanceToFaces (:956-969) in GetCellFaces order
     double d[6] = {p.x - xl, xh - p.x, p.y - yl, yh - p.y, p.z - zl, zh - p.z};
@@ -262,11 +264,9 @@ __device__ inline int try_random_walk(const Ctx &C, PartReg &p, RNG &rng, TALLY 
     Ro = (Ro > 0.0) ? Ro : 0.0;
     const double c = C.clight;
     double sigmaT = C.rwSigT[cell];
-    double sigmaAeff = C.sigA[cell];
-    double Dphys = (sigmaT > 0.0) ? c / (3.0 * sigmaT) : 0.0;
+    double Dphys = cp.w;
     bool doRW = (Ro > 0.0 && sigmaT > 0.0 && Dphys > 0.0 && Ro * sigmaT >= C.rwMinParticle);
     if (!doRW) return -1;
-    double f = C.fleck[cell];
     double tauLeak = rw_sample_leak(C.rw, rng.open());
     double tLeak = tauLeak * Ro * Ro / Dphys;
     double tCensus = p.t;
@@ -275,10 +275,10 @@ __device__ inline int try_random_walk(const Ctx &C, PartReg &p, RNG &rng, TALLY 
     if (tLeak <= tCensus && tLeak <= DBL_MAX) { ev = 0; dt = tLeak; }
     else if (tCensus <= DBL_MAX) { ev = 1; dt = tCensus; }
     else { ev = 2; dt = DBL_MAX; }
-    double rate = sigmaAeff * f * c;
+    const double rate = cp.y;   // sigma_a * f * c
     double rwExp = expm1(-dt * rate);
     if (!C.noFeedback) tal.mat(cell, -rwExp * p.w);
-    if (rate > 0.0) tal.rad(cell, p.w * rwExp * (-1.0 / rate));
+    if (rate > 0.0) tal.rad(cell, p.w * rwExp * cp.z);
     p.w *= 1.0 + rwExp;
     p.t -= dt;
     if (fabs(p.w) < p.w0 * 1e-4) {
@@ -289,9 +289,9 @@ __device__ inline int try_random_walk(const Ctx &C, PartReg &p, RNG &rng, TALLY 
     double s2 = 1.0 - cosTheta * cosTheta;
     double sinTheta = sqrt(s2 > 0.0 ? s2 : 0.0);
     double phi = 2.0 * RW_PI * rng.open();
-    double sp, cp;
-    sincos(phi, &sp, &cp);
-    double dx = sinTheta * cp, dy = sinTheta * sp, dz = cosTheta;
+    double sphi, cphi;
+    sincos(phi, &sphi, &cphi);
+    double dx = sinTheta * cphi, dy = sinTheta * sphi, dz = cosTheta;
     double disp;
     if (ev == 0) disp = Ro;
     else {
@@ -333,6 +333,7 @@ __device__ inline int try_random_walk(const Ctx &C, PartReg &p, RNG &rng, TALLY 
 // ------------------------------------------------------------------ physics step
 struct PhysOut {
     int status;        // ParticleStatus or -1 error code in errCode
+    int face;          // crossed side (GetCellFaces order) for CELL_MOVE
     uint32_t next;     // neighbour cell or OUTSIDE (face crossings)
     uint32_t ghost;    // Ncells + global face index when next is OUTSIDE
     int usedRW;
@@ -353,37 +354,76 @@ __device__ __forceinline__ uint32_t face_index(const Ctx &C, uint32_t i, uint32_
     }
 }
 
+// Per-cell constants of a segment, evaluated once per step with the same
+// operations the reference evaluates per segment, so the values are identical:
+//   x = scatteringLength = 1 / (sigma_s + (1 - f) sigma_a)  (+inf when that is <= 0)
+//   y = tmp2 = sigma_a * f * c  (also the Random Walk absorption rate)
+//   z = -1 / tmp2
+//   w = D = c / (3 sigma_T) for the Random Walk (0 when sigma_T <= 0)
+__device__ __forceinline__ double4 cell_phys(double sigA, double sigS, double f, double sigT, double c) {
+    const double eventOpacity = sigS + (1.0 - f) * sigA;
+    double4 r;
+    r.x = (eventOpacity > 0.0) ? 1.0 / eventOpacity : CUDART_INF;
+    r.y = sigA * f * c;
+    r.z = -1.0 / r.y;
+    r.w = (sigT > 0.0) ? c / (3.0 * sigT) : 0.0;
+    return r;
+}
+
+// A particle being tracked: its state plus the cell coordinates and speed kept
+// in registers between segments.
+struct Track {
+    PartReg p;
+    uint32_t i, j, k;
+    double speed;   // STORM::fallback::abs(velocity), recomputed when the velocity changes
+};
+
+__device__ __forceinline__ void track_begin(const Ctx &C, Track &T) {
+    cell_ijk(C, T.p.cell, T.i, T.j, T.k);
+    T.speed = vnorm(T.p.vx, T.p.vy, T.p.vz);
+}
+
 // RadiationIMC::step (radiation/RadiationIMC.hpp:1700-1881), gray, without hydro,
 // including the face search of Particle::distanceToNearestFace
 // (particle/Particle.hpp:188-279).  For an axis-aligned cell the inward normals
 // are exact +-unit vectors, so (p_f - x).n and n.v reduce exactly to one
-// coordinate difference and one velocity component.
+// coordinate difference and one velocity component, and each axis offers at
+// most one candidate face.  The candidates are ordered by comparing
+// |n_a| |v_b| with |n_b| |v_a| (no division), and only the winner's exit time
+// is divided out: that time is bit-identical to the reference's; the choice of
+// face can differ only when two exit times agree to within rounding.
 template <class RNG, class TALLY>
-__device__ inline PhysOut physics_step(const Ctx &C, PartReg &p, RNG &rng, TALLY &tal) {
+__device__ inline PhysOut physics_step(const Ctx &C, Track &T, RNG &rng, TALLY &tal) {
+    PartReg &p = T.p;
     PhysOut o;
     o.status = NO_CELL_MOVE;
+    o.face = -1;
     o.next = OUTSIDE;
     o.ghost = 0;
     o.usedRW = 0;
     o.errCode = 0;
     const uint32_t cell = p.cell;
-    uint32_t i, j, k;
-    cell_ijk(C, cell, i, j, k);
+    const uint32_t i = T.i, j = T.j, k = T.k;
     const double xl = C.xe[i], xh = C.xe[i + 1], yl = C.ye[j], yh = C.ye[j + 1], zl = C.ze[k], zh = C.ze[k + 1];
-    const double speed = vnorm(p.vx, p.vy, p.vz);
-    const double thr = EPSILON_FACE * speed;
-    double minA = DBL_MAX;
-    int minF = -1;
-    double a;
-    if (p.vx < -thr) { a = (xl - p.x) / p.vx; if (a < minA && a > 0) { minA = a; minF = 0; } }
-    if (p.vx > thr) { a = (xh - p.x) / p.vx; if (a < minA && a > 0) { minA = a; minF = 1; } }
-    if (p.vy < -thr) { a = (yl - p.y) / p.vy; if (a < minA && a > 0) { minA = a; minF = 2; } }
-    if (p.vy > thr) { a = (yh - p.y) / p.vy; if (a < minA && a > 0) { minA = a; minF = 3; } }
-    if (p.vz < -thr) { a = (zl - p.z) / p.vz; if (a < minA && a > 0) { minA = a; minF = 4; } }
-    if (p.vz > thr) { a = (zh - p.z) / p.vz; if (a < minA && a > 0) { minA = a; minF = 5; } }
-    if (minF < 0) { o.errCode = STORM_DERR_NO_FACE; return o; }
-    uint32_t next = OUTSIDE;
-    switch (minF) {
+    const double thr = EPSILON_FACE * T.speed;
+    // candidate face per axis: numerator (p_f - x) and velocity component
+    double nb = 0.0, vb = 1.0;
+    int face = -1;
+    {
+        double n;
+        bool ok;
+        if (p.vx < -thr) { n = xl - p.x; ok = n < 0.0; } else if (p.vx > thr) { n = xh - p.x; ok = n > 0.0; } else ok = false;
+        if (ok) { nb = n; vb = p.vx; face = p.vx > 0.0 ? 1 : 0; }
+        if (p.vy < -thr) { n = yl - p.y; ok = n < 0.0; } else if (p.vy > thr) { n = yh - p.y; ok = n > 0.0; } else ok = false;
+        if (ok && (face < 0 || fabs(n) * fabs(vb) < fabs(nb) * fabs(p.vy))) { nb = n; vb = p.vy; face = p.vy > 0.0 ? 3 : 2; }
+        if (p.vz < -thr) { n = zl - p.z; ok = n < 0.0; } else if (p.vz > thr) { n = zh - p.z; ok = n > 0.0; } else ok = false;
+        if (ok && (face < 0 || fabs(n) * fabs(vb) < fabs(nb) * fabs(p.vz))) { nb = n; vb = p.vz; face = p.vz > 0.0 ? 5 : 4; }
+    }
+    if (face < 0) { o.errCode = STORM_DERR_NO_FACE; return o; }
+    const double tFace = nb / vb;
+    if (!(tFace > 0.0)) { o.errCode = STORM_DERR_NO_FACE; return o; }
+    uint32_t next;
+    switch (face) {
     case 0: next = (i > 0) ? cell - 1 : OUTSIDE; break;
     case 1: next = (i + 1 < C.nx) ? cell + 1 : OUTSIDE; break;
     case 2: next = (j > 0) ? cell - C.nx : OUTSIDE; break;
@@ -391,34 +431,34 @@ __device__ inline PhysOut physics_step(const Ctx &C, PartReg &p, RNG &rng, TALLY
     case 4: next = (k > 0) ? cell - C.nx * C.ny : OUTSIDE; break;
     default: next = (k + 1 < C.nz) ? cell + C.nx * C.ny : OUTSIDE; break;
     }
-    const double tFace = minA;
+    const double4 cp = C.phys[cell];
 
     if (C.withRW && C.rwElig[cell]) {
-        int r = try_random_walk(C, p, rng, tal, xl, xh, yl, yh, zl, zh, C.xc[i], C.yc[j], C.zc[k]);
+        int r = try_random_walk(C, p, rng, tal, cp, xl, xh, yl, yh, zl, zh, C.xc[i], C.yc[j], C.zc[k]);
         if (r == -2) { o.errCode = STORM_DERR_RW_SHRINK; return o; }
-        if (r >= 0) { o.status = r; o.usedRW = 1; return o; }
+        if (r >= 0) {
+            o.status = r;
+            o.usedRW = 1;
+            T.speed = vnorm(p.vx, p.vy, p.vz);
+            return o;
+        }
     }
 
     const double c = C.clight;
-    const double absorptionOpacity = C.sigA[cell];
-    const double f = C.fleck[cell];
-    const double effectiveAbsorptionOpacity = (1.0 - f) * absorptionOpacity;
-    const double eventOpacity = C.sigS[cell] + effectiveAbsorptionOpacity;
-    const double scatteringLength = (eventOpacity > 0.0) ? 1.0 / eventOpacity : CUDART_INF;
     const double lp = -log1p(rng.open() - 1.0);
-    const double scatteringDistance = scatteringLength * lp;
-    const double timeScattering = isfinite(scatteringDistance) ? scatteringDistance / speed : CUDART_INF;
+    const double scatteringDistance = cp.x * lp;
+    const double timeScattering = isfinite(scatteringDistance) ? scatteringDistance / T.speed : CUDART_INF;
     // std::min_element over {face, scatter, census}: first smallest wins
     int best = 0;
     double dt = tFace;
     if (timeScattering < dt) { best = 1; dt = timeScattering; }
     if (p.t < dt) { best = 2; dt = p.t; }
     p.t -= dt;
-    const double tmp2 = absorptionOpacity * f * c;
+    const double tmp2 = cp.y;
     const double tmp = -dt * tmp2;
     const double e1 = expm1(tmp);
     double integrated = p.w * dt;
-    if (fabs(tmp2 * dt) >= 1e-12) integrated = p.w * e1 * (-1.0 / tmp2);
+    if (fabs(tmp2 * dt) >= 1e-12) integrated = p.w * e1 * cp.z;
     p.x += p.vx * dt;
     p.y += p.vy * dt;
     p.z += p.vz * dt;
@@ -432,11 +472,13 @@ __device__ inline PhysOut physics_step(const Ctx &C, PartReg &p, RNG &rng, TALLY
     }
     if (best == 0) {
         o.status = CELL_MOVE;
+        o.face = face;
         o.next = next;
-        if (next == OUTSIDE) o.ghost = C.ncells + face_index(C, i, j, k, minF);
+        if (next == OUTSIDE) o.ghost = C.ncells + face_index(C, i, j, k, face);
     } else if (best == 1) {
         (void)rng.open();   // event-type draw; both branches re-scatter isotropically
         isotropic(rng, c, p.vx, p.vy, p.vz);
+        T.speed = vnorm(p.vx, p.vy, p.vz);
         o.status = NO_CELL_MOVE;
     } else {
         o.status = DONE;
@@ -473,14 +515,21 @@ __device__ __forceinline__ void box_face_reflect(const BoxFaceDev &F, PartReg &p
 // (manager/MonteCarloManagerSerial.hpp:318-369), with BoundaryCondition::apply
 // for the per-face descriptor (VacuumBoundary, RigidBoundary, SideTemperature,
 // TwoSidesTemperature all lower to it).
-__device__ __forceinline__ int manager_handle(const Ctx &C, PartReg &p, const PhysOut &o) {
+__device__ __forceinline__ int manager_handle(const Ctx &C, Track &T, const PhysOut &o) {
+    PartReg &p = T.p;
     if (o.status == CELL_MOVE) {
         if (o.next != OUTSIDE) {
-            uint32_t i, j, k;
-            cell_ijk(C, o.next, i, j, k);
-            p.x = (1 - MONTECARLO_EPS) * p.x + MONTECARLO_EPS * C.xc[i];
-            p.y = (1 - MONTECARLO_EPS) * p.y + MONTECARLO_EPS * C.yc[j];
-            p.z = (1 - MONTECARLO_EPS) * p.z + MONTECARLO_EPS * C.zc[k];
+            switch (o.face) {
+            case 0: --T.i; break;
+            case 1: ++T.i; break;
+            case 2: --T.j; break;
+            case 3: ++T.j; break;
+            case 4: --T.k; break;
+            default: ++T.k; break;
+            }
+            p.x = (1 - MONTECARLO_EPS) * p.x + MONTECARLO_EPS * C.xc[T.i];
+            p.y = (1 - MONTECARLO_EPS) * p.y + MONTECARLO_EPS * C.yc[T.j];
+            p.z = (1 - MONTECARLO_EPS) * p.z + MONTECARLO_EPS * C.zc[T.k];
             p.cell = o.next;
             return OUT_CONTINUE;
         }
@@ -495,11 +544,10 @@ __device__ __forceinline__ int manager_handle(const Ctx &C, PartReg &p, const Ph
             }
         }
         if (!reflected) return OUT_ERROR;
-        uint32_t i, j, k;
-        cell_ijk(C, p.cell, i, j, k);
-        p.x = (1 - MONTECARLO_EPS) * p.x + MONTECARLO_EPS * C.xc[i];
-        p.y = (1 - MONTECARLO_EPS) * p.y + MONTECARLO_EPS * C.yc[j];
-        p.z = (1 - MONTECARLO_EPS) * p.z + MONTECARLO_EPS * C.zc[k];
+        T.speed = vnorm(p.vx, p.vy, p.vz);
+        p.x = (1 - MONTECARLO_EPS) * p.x + MONTECARLO_EPS * C.xc[T.i];
+        p.y = (1 - MONTECARLO_EPS) * p.y + MONTECARLO_EPS * C.yc[T.j];
+        p.z = (1 - MONTECARLO_EPS) * p.z + MONTECARLO_EPS * C.zc[T.k];
         return OUT_CONTINUE;
     }
     if (o.status == REMOVE) return OUT_CUTOFF;

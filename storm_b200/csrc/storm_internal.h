@@ -21,6 +21,7 @@ struct CellArrays {
     double *sigA, *sigS, *fleck, *rwSigT, *eradAvg, *eradCensus, *emitE;
     uint8_t *rwElig;
     uint64_t *photons;
+    double4 *phys;      // per-cell segment constants (cell_phys)
 };
 
 struct OpacityEos {
@@ -78,7 +79,8 @@ void launch_emit_cells(cudaStream_t s, const Ctx &C, const CellArrays &A, const 
 void launch_emit_faces(cudaStream_t s, const Ctx &C, const FaceSources &F, uint64_t total, const Bank &b,
                        uint32_t bankBase, double dt, DevStats *st);
 void launch_transport(cudaStream_t s, uint32_t grid, const Ctx &C, const Bank &in, const uint32_t *nIn, const Bank &out,
-                      uint32_t *nOut, const Bank &cen, uint32_t *nCen, uint32_t K, DevStats *st);
+                      uint32_t *nOut, const Bank &cen, uint32_t *nCen, uint32_t K, DevStats *st, int minBlocks);
+int transport_blocks_per_sm(int minBlocks);
 void launch_comb_keys(cudaStream_t s, const Ctx &C, const Bank &cen, uint32_t n, uint64_t *keys, uint32_t *vals,
                       uint32_t combKey);
 int launch_radix_sort(cudaStream_t s, uint64_t *keys, uint32_t *vals, uint64_t *keysAlt, uint32_t *valsAlt, uint32_t n,
@@ -88,11 +90,16 @@ void launch_comb_ranges(cudaStream_t s, const uint64_t *keys, uint32_t n, uint32
 void launch_comb_cell_sums(cudaStream_t s, const Bank &cen, const uint32_t *idx, const uint32_t *start, uint32_t ncells,
                            double *W);
 void launch_blocked_sum(cudaStream_t s, const double *v, uint32_t n, double *out);
-void launch_comb_count(cudaStream_t s, const Ctx &C, const CombParams &P, const Bank &cen, const uint32_t *idx,
-                       const uint32_t *start, const double *W, const double *Wtot, uint64_t *outCount);
-void launch_comb_write(cudaStream_t s, const Ctx &C, const CombParams &P, const Bank &cen, const uint32_t *idx,
-                       const uint32_t *start, const double *W, const double *Wtot, const uint64_t *outOffset,
-                       const Bank &out, double *eradCensus, DevStats *st);
+void launch_comb_plan(cudaStream_t s, const Ctx &C, const CombParams &P, const Bank &cen, const uint32_t *idx,
+                      const uint32_t *start, const double *W, const double *Wtot, uint32_t *pCount, double *pWeight,
+                      uint64_t *cellCount, double *eradCensus, DevStats *st);
+void launch_comb_emit(cudaStream_t s, const Ctx &C, const Bank &cen, const uint32_t *idx, const uint64_t *sortedKeys,
+                      uint32_t nValid, const uint32_t *pCount, const double *pWeight, const uint64_t *pOffset,
+                      const Bank &out);
+void launch_mask_count(cudaStream_t s, const uint32_t *pCount, uint32_t n, uint64_t *out);
+void launch_allocate_checked(cudaStream_t s, const Ctx &C, const CellArrays &A, const double *total,
+                             uint64_t newPerCell, double rel, int32_t *ambiguous);
+size_t radix_scratch_words(uint32_t n);
 void launch_census_keys_pid(cudaStream_t s, const Bank &cen, uint32_t n, uint64_t *keys, uint32_t *vals);
 void launch_gather(cudaStream_t s, const Bank &src, const uint32_t *idx, uint32_t n, const Bank &dst, double *eradCensus,
                    DevStats *st);

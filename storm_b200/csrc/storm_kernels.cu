@@ -94,6 +94,7 @@ __global__ void k_prestep(Ctx C, CellArrays A, OpacityEos M, double dt) {
         double f = 1.0 / (1.0 + (4.0 * C.arad * T3 * sa * C.clight * dt * 1.0) / cv);
         A.fleck[c] = f;
         if (f < 0.0 || f > 1.0) raise_error(C, STORM_DERR_FLECK, c, 0);
+        A.phys[c] = cell_phys(sa, ss, f, sa + ss, C.clight);
         if (C.withRW) {
             double sigmaT = sa + ss;
             A.rwSigT[c] = sigmaT;
@@ -109,10 +110,13 @@ __global__ void k_prestep(Ctx C, CellArrays A, OpacityEos M, double dt) {
     }
 }
 
-// RW eligibility from externally supplied tables (storm_cuda_set_cell_physics).
+// Segment constants and RW eligibility from externally supplied tables
+// (storm_cuda_set_cell_physics).
 __global__ void k_rw_eligibility(Ctx C, CellArrays A) {
     for (uint32_t c = blockIdx.x * blockDim.x + threadIdx.x; c < C.ncells; c += gridDim.x * blockDim.x) {
         double sigmaT = A.sigA[c] + A.sigS[c];
+        A.phys[c] = cell_phys(A.sigA[c], A.sigS[c], A.fleck[c], sigmaT, C.clight);
+        if (!C.withRW) continue;
         A.rwSigT[c] = sigmaT;
         uint32_t i, j, k;
         cell_ijk(C, c, i, j, k);
@@ -164,6 +168,33 @@ __global__ void k_allocate(Ctx C, CellArrays A, const double *total, uint64_t ne
         uint64_t m = share < cap ? share : cap;
         A.photons[c] = (E > 0.0) ? (m > newPerCell ? m : newPerCell) : 0;
     }
+}
+
+// The same counts from a fast deterministic total.  E_i >= 0, so the reference's
+// left-to-right total and this blocked total both lie within rel * total of the
+// exact sum (rel bounds the rounding of either order).  floor(fl(fl(E/S) * T)) is
+// monotone in S, so when it agrees at both ends of that interval it equals the
+// count the reference's total gives; otherwise the cell is flagged and the
+// caller recomputes everything with the exact sequential total.
+__global__ void k_allocate_checked(Ctx C, CellArrays A, const double *total, uint64_t newPerCell, double rel,
+                                   int32_t *ambiguous) {
+    const double tot = *total;
+    const uint64_t totalParticles = static_cast<uint64_t>(C.ncells) * newPerCell * 10;
+    const double lo = tot * (1.0 - rel), hi = tot * (1.0 + rel);
+    int amb = 0;
+    for (uint32_t c = blockIdx.x * blockDim.x + threadIdx.x; c < C.ncells; c += gridDim.x * blockDim.x) {
+        double E = A.emitE[c];
+        uint64_t share = (tot > 0) ? static_cast<uint64_t>(E / tot * static_cast<double>(totalParticles)) : newPerCell;
+        if (tot > 0 && E > 0.0) {
+            uint64_t a = static_cast<uint64_t>(E / lo * static_cast<double>(totalParticles));
+            uint64_t b = static_cast<uint64_t>(E / hi * static_cast<double>(totalParticles));
+            if (a != b) amb = 1;
+        }
+        uint64_t cap = newPerCell * 20;
+        uint64_t m = share < cap ? share : cap;
+        A.photons[c] = (E > 0.0) ? (m > newPerCell ? m : newPerCell) : 0;
+    }
+    if (__any_sync(FULL, amb) && (threadIdx.x & 31) == 0) atomicOr(ambiguous, 1);
 }
 
 // material debit (:2193-2195)
@@ -450,48 +481,62 @@ __global__ void k_emit_faces(Ctx C, FaceSources F, uint64_t total, Bank b, uint3
 // One bank visit of the HandleAll loop (manager/MonteCarloManagerSerial.hpp:267-383):
 // every active particle runs up to K segments in registers; survivors are
 // compacted into the next bank and census particles appended to the census bank
-// (warp ballot + one atomic per warp).
-__global__ void __launch_bounds__(256) k_transport(Ctx C, Bank in, const uint32_t *nIn, Bank out, uint32_t *nOut,
-                                                   Bank cen, uint32_t *nCen, uint32_t K, DevStats *st) {
+// (warp ballot + one atomic per warp).  Statistics go to per-block shared
+// counters when the event happens, so no thread holds accumulators.
+struct BlockStats {
+    unsigned long long segments, rwSteps, escaped, cutoff, census;
+    double eDeposited, eEscaped, eCensusPre;
+};
+
+template <int MINB>
+__global__ void __launch_bounds__(256, MINB) k_transport(Ctx C, Bank in, const uint32_t *nIn, Bank out,
+                                                          uint32_t *nOut, Bank cen, uint32_t *nCen, uint32_t K,
+                                                          DevStats *st) {
+    __shared__ BlockStats bs;
+    if (threadIdx.x == 0) bs = BlockStats{0, 0, 0, 0, 0, 0.0, 0.0, 0.0};
+    __syncthreads();
     const uint32_t n = *nIn;
     const unsigned lane = threadIdx.x & 31;
-    unsigned long long segs = 0, rw = 0, esc = 0, cut = 0, ncen = 0;
-    double dep = 0.0, eEsc = 0.0, eCen = 0.0;
     for (uint32_t base = blockIdx.x * blockDim.x; base < n; base += gridDim.x * blockDim.x) {
         const uint32_t idx = base + threadIdx.x;
         const bool active = idx < n;
-        PartReg p;
+        Track T;
+        PartReg &p = T.p;
         uint32_t pid = 0, draw = 0;
         int outcome = OUT_CONTINUE;
         if (active) {
             load_part(in, idx, p);
             pid = in.pid[idx];
             draw = in.draw[idx];
+            track_begin(C, T);
             PhiloxRng rng;
             rng.init(C.seedLo, C.seedHi, TAG_TRANSPORT, C.step, pid, draw);
             AtomicTally tal{C.eint, C.eradAvg, 0.0};
-            for (uint32_t s = 0; s < K; ++s) {
+            uint32_t s = 0, rw = 0;
+            for (; s < K;) {
                 if (C.perCellCounters) atomicAdd(C.segs + p.cell, 1u);
-                ++segs;
+                ++s;
                 const uint32_t cell0 = p.cell;
-                PhysOut o = physics_step(C, p, rng, tal);
+                PhysOut o = physics_step(C, T, rng, tal);
                 if (o.errCode) {
                     raise_error(C, o.errCode, cell0, pid);
                     outcome = OUT_ERROR;
                     break;
                 }
                 rw += o.usedRW;
-                outcome = manager_handle(C, p, o);
+                outcome = manager_handle(C, T, o);
                 if (outcome != OUT_CONTINUE) {
                     if (outcome == OUT_ERROR) raise_error(C, STORM_DERR_NOT_ON_BOUNDARY, cell0, pid);
                     break;
                 }
             }
             draw = rng.draw;
-            dep += tal.depSum;
-            if (outcome == OUT_ESCAPE) { ++esc; eEsc += p.w; }
-            else if (outcome == OUT_CUTOFF) { ++cut; }
-            else if (outcome == OUT_CENSUS) { ++ncen; eCen += p.w; }
+            atomicAdd(&bs.segments, static_cast<unsigned long long>(s));
+            if (rw) atomicAdd(&bs.rwSteps, static_cast<unsigned long long>(rw));
+            if (tal.depSum != 0.0) atomicAdd(&bs.eDeposited, tal.depSum);
+            if (outcome == OUT_ESCAPE) { atomicAdd(&bs.escaped, 1ull); atomicAdd(&bs.eEscaped, p.w); }
+            else if (outcome == OUT_CUTOFF) { atomicAdd(&bs.cutoff, 1ull); }
+            else if (outcome == OUT_CENSUS) { atomicAdd(&bs.census, 1ull); atomicAdd(&bs.eCensusPre, p.w); }
         }
         const bool keep = active && outcome == OUT_CONTINUE;
         const bool cens = active && outcome == OUT_CENSUS;
@@ -507,17 +552,16 @@ __global__ void __launch_bounds__(256) k_transport(Ctx C, Bank in, const uint32_
         if (keep) store_part(out, bK + __popc(mK & lt), p, pid, draw);
         if (cens) store_part(cen, bC + __popc(mC & lt), p, pid, draw);
     }
-    segs = warp_sum(segs); rw = warp_sum(rw); esc = warp_sum(esc); cut = warp_sum(cut); ncen = warp_sum(ncen);
-    dep = warp_sum(dep); eEsc = warp_sum(eEsc); eCen = warp_sum(eCen);
-    if (lane == 0) {
-        if (segs) atomicAdd(&st->segments, segs);
-        if (rw) atomicAdd(&st->rwSteps, rw);
-        if (esc) atomicAdd(&st->escaped, esc);
-        if (cut) atomicAdd(&st->cutoff, cut);
-        if (ncen) atomicAdd(&st->census, ncen);
-        if (dep != 0.0) atomicAdd(&st->eDeposited, dep);
-        if (eEsc != 0.0) atomicAdd(&st->eEscaped, eEsc);
-        if (eCen != 0.0) atomicAdd(&st->eCensusPre, eCen);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        if (bs.segments) atomicAdd(&st->segments, bs.segments);
+        if (bs.rwSteps) atomicAdd(&st->rwSteps, bs.rwSteps);
+        if (bs.escaped) atomicAdd(&st->escaped, bs.escaped);
+        if (bs.cutoff) atomicAdd(&st->cutoff, bs.cutoff);
+        if (bs.census) atomicAdd(&st->census, bs.census);
+        if (bs.eDeposited != 0.0) atomicAdd(&st->eDeposited, bs.eDeposited);
+        if (bs.eEscaped != 0.0) atomicAdd(&st->eEscaped, bs.eEscaped);
+        if (bs.eCensusPre != 0.0) atomicAdd(&st->eCensusPre, bs.eCensusPre);
     }
 }
 
@@ -561,6 +605,20 @@ __global__ void __launch_bounds__(RS_THREADS) k_rs_hist(const uint64_t *keys, ui
     }
     __syncthreads();
     tileHist[threadIdx.x * ntiles + blockIdx.x] = h[threadIdx.x];
+}
+
+// exclusive scan (in place) of the digit-major tile histogram, three phases
+__global__ void k_scan32_tiles(uint32_t *v, uint32_t n, uint64_t *tileSums) {
+    __shared__ uint64_t sh[32];
+    uint32_t q = blockIdx.x * blockDim.x + threadIdx.x;
+    uint64_t x = q < n ? v[q] : 0;
+    uint64_t inc = block_scan_incl(x, sh);
+    if (q < n) v[q] = static_cast<uint32_t>(inc - x);
+    if (threadIdx.x == blockDim.x - 1) tileSums[blockIdx.x] = inc;
+}
+__global__ void k_scan32_add(uint32_t *v, uint32_t n, const uint64_t *tileSums) {
+    uint32_t q = blockIdx.x * blockDim.x + threadIdx.x;
+    if (q < n) v[q] += static_cast<uint32_t>(tileSums[blockIdx.x]);
 }
 
 // exclusive scan of the digit-major tile histogram (256 * ntiles) by one block
@@ -683,102 +741,102 @@ __device__ __forceinline__ CombCell comb_cell_params(const Ctx &C, const CombPar
     return cc;
 }
 
-// output count per cell (:161-226)
-__global__ void k_comb_count(Ctx C, CombParams P, Bank cen, const uint32_t *idx, const uint32_t *start, const double *W,
-                             const double *Wtot, uint64_t *outCount) {
+// Per cell (:161-226): the number of copies of each sorted particle, the weight
+// of those copies, and the cell's census radiation energy summed in output order
+// (RadiationIMC::postStep :2013-2016).  pCount bit 31 marks a particle kept as is.
+constexpr uint32_t KEEP = 0x80000000u;
+__global__ void k_comb_plan(Ctx C, CombParams P, Bank cen, const uint32_t *idx, const uint32_t *start, const double *W,
+                            const double *Wtot, uint32_t *pCount, double *pWeight, uint64_t *cellCount,
+                            double *eradCensus, DevStats *st) {
     const double tot = *Wtot;
     if (!isfinite(tot)) {
         if (blockIdx.x == 0 && threadIdx.x == 0) raise_error(C, STORM_DERR_COMB_TOTAL, 0, 0);
     }
-    for (uint32_t c = blockIdx.x * blockDim.x + threadIdx.x; c < C.ncells; c += gridDim.x * blockDim.x) {
-        const uint32_t a = start[c], b = start[c + 1];
-        if (tot == 0.0 || !isfinite(tot) || a == b) { outCount[c] = 0; continue; }
-        CombCell cc = comb_cell_params(C, P, c, b - a, W[c], tot);
-        uint64_t m = 0;
-        if (cc.mode == 0) {
-            for (uint32_t q = a; q < b; ++q) {
-                double w = cen.w[idx[q]];
-                m += (w > 2 * cc.w_ideal) ? static_cast<uint64_t>(ceil(w / cc.w_ideal)) : 1;
-            }
-        } else {
-            uint64_t k = 0;
-            double cum = 0;
-            for (uint32_t q = a; q < b; ++q) {
-                double w = cen.w[idx[q]];
-                while ((cum + w) > (static_cast<double>(k) + cc.r) * cc.e) ++k;
-                cum += w;
-            }
-            m = k;
-        }
-        outCount[c] = m;
-    }
-}
-
-// write the combed census into the next step's bank; per-cell census radiation
-// energy (RadiationIMC::postStep :1989-2028) summed in output order.
-__global__ void k_comb_write(Ctx C, CombParams P, Bank cen, const uint32_t *idx, const uint32_t *start, const double *W,
-                             const double *Wtot, const uint64_t *outOffset, Bank out, double *eradCensus,
-                             DevStats *st) {
-    const double tot = *Wtot;
     double eOut = 0.0;
     for (uint32_t c = blockIdx.x * blockDim.x + threadIdx.x; c < C.ncells; c += gridDim.x * blockDim.x) {
         const uint32_t a = start[c], b = start[c + 1];
         double ecell = 0.0;
-        if (!(tot == 0.0 || !isfinite(tot) || a == b)) {
+        uint64_t m = 0;
+        if (tot == 0.0 || !isfinite(tot) || a == b) {
+            for (uint32_t q = a; q < b; ++q) pCount[q] = 0;
+        } else {
             CombCell cc = comb_cell_params(C, P, c, b - a, W[c], tot);
-            uint64_t o = outOffset[c];
-            uint32_t i, j, k;
-            cell_ijk(C, c, i, j, k);
-            const double mx = C.xc[i], my = C.yc[j], mz = C.zc[k];
-            auto emit = [&](uint32_t src, double w, bool reweight) {
-                PartReg p;
-                load_part(cen, src, p);
-                if (reweight) { p.w = w; p.w0 = w; p.t = 0; }
-                p.cell = c;
-                if (outside_box(C, p.x, p.y, p.z)) {   // :228-250
-                    const double ox = p.x, oy = p.y, oz = p.z, dx = mx - ox, dy = my - oy, dz = mz - oz;
-                    double t = 1e-6;
-                    while (outside_box(C, p.x, p.y, p.z) && t < 1.0) {
-                        p.x = ox + t * dx; p.y = oy + t * dy; p.z = oz + t * dz;
-                        t *= 2;
-                    }
-                    if (outside_box(C, p.x, p.y, p.z)) { p.x = mx; p.y = my; p.z = mz; }
-                }
-                store_part(out, static_cast<uint32_t>(o), p, static_cast<uint32_t>(o), 0);
-                ecell += p.w;
-                ++o;
-            };
             if (cc.mode == 0) {
                 for (uint32_t q = a; q < b; ++q) {
-                    const uint32_t src = idx[q];
-                    const double w = cen.w[src];
+                    const double w = cen.w[idx[q]];
                     if (w > 2 * cc.w_ideal) {
                         const uint64_t ns = static_cast<uint64_t>(ceil(w / cc.w_ideal));
                         const double ws = w / static_cast<double>(ns);
-                        for (uint64_t s = 0; s < ns; ++s) emit(src, ws, true);
+                        for (uint64_t k = 0; k < ns; ++k) ecell += ws;
+                        pCount[q] = static_cast<uint32_t>(ns);
+                        pWeight[q] = ws;
+                        m += ns;
                     } else {
-                        emit(src, w, false);
+                        ecell += w;
+                        pCount[q] = 1u | KEEP;
+                        pWeight[q] = w;
+                        m += 1;
                     }
                 }
             } else {
-                uint64_t k2 = 0;
+                uint64_t k = 0;
                 double cum = 0;
                 for (uint32_t q = a; q < b; ++q) {
-                    const uint32_t src = idx[q];
-                    const double w = cen.w[src];
-                    while ((cum + w) > (static_cast<double>(k2) + cc.r) * cc.e) {
-                        ++k2;
-                        emit(src, cc.e, true);
+                    const double w = cen.w[idx[q]];
+                    const uint64_t k0 = k;
+                    while ((cum + w) > (static_cast<double>(k) + cc.r) * cc.e) {
+                        ++k;
+                        ecell += cc.e;
                     }
                     cum += w;
+                    pCount[q] = static_cast<uint32_t>(k - k0);
+                    pWeight[q] = cc.e;
                 }
+                m = k;
             }
         }
+        cellCount[c] = m;
         eradCensus[c] = ecell;
         eOut += ecell;
     }
     eOut = warp_sum(eOut);
     if ((threadIdx.x & 31) == 0 && eOut != 0.0) atomicAdd(&st->eCensusOut, eOut);
+}
+
+// One thread per sorted particle writes its copies at its output offset.
+// The exclusive prefix of the copy counts over sorted particles is the output
+// position: cells are contiguous in sorted order and the output is cell-major.
+__global__ void k_comb_emit(Ctx C, Bank cen, const uint32_t *idx, const uint64_t *sortedKeys, uint32_t nValid,
+                            const uint32_t *pCount, const double *pWeight, const uint64_t *pOffset, Bank out) {
+    for (uint32_t q = blockIdx.x * blockDim.x + threadIdx.x; q < nValid; q += gridDim.x * blockDim.x) {
+        const uint32_t raw = pCount[q];
+        const uint32_t m = raw & ~KEEP;
+        if (m == 0) continue;
+        const uint32_t c = static_cast<uint32_t>(sortedKeys[q] >> 32);
+        PartReg p;
+        load_part(cen, idx[q], p);
+        if (!(raw & KEEP)) { p.w = pWeight[q]; p.w0 = p.w; p.t = 0; }
+        p.cell = c;
+        if (outside_box(C, p.x, p.y, p.z)) {   // :228-250
+            uint32_t i, j, k;
+            cell_ijk(C, c, i, j, k);
+            const double mx = C.xc[i], my = C.yc[j], mz = C.zc[k];
+            const double ox = p.x, oy = p.y, oz = p.z, dx = mx - ox, dy = my - oy, dz = mz - oz;
+            double t = 1e-6;
+            while (outside_box(C, p.x, p.y, p.z) && t < 1.0) {
+                p.x = ox + t * dx; p.y = oy + t * dy; p.z = oz + t * dz;
+                t *= 2;
+            }
+            if (outside_box(C, p.x, p.y, p.z)) { p.x = mx; p.y = my; p.z = mz; }
+        }
+        const uint64_t o = pOffset[q];
+        for (uint32_t k = 0; k < m; ++k) store_part(out, static_cast<uint32_t>(o + k), p, static_cast<uint32_t>(o + k), 0);
+    }
+}
+
+__global__ void k_mask_count(const uint32_t *pCount, uint32_t n, uint64_t *out) {
+    for (uint32_t q = blockIdx.x * blockDim.x + threadIdx.x; q < n; q += gridDim.x * blockDim.x)
+        out[q] = pCount[q] & ~KEEP;
 }
 
 // census kept as is (no population control): order by pid for a deterministic bank
@@ -840,14 +898,16 @@ __global__ void k_poststep(Ctx C, CellArrays A, OpacityEos M, double dt) {
 // ------------------------------------------------------------------ replay
 __global__ void k_replay(Ctx C, ReplayDev R, uint32_t n) {
     for (uint32_t q = blockIdx.x * blockDim.x + threadIdx.x; q < n; q += gridDim.x * blockDim.x) {
-        PartReg p;
+        Track T;
+        PartReg &p = T.p;
         p.x = R.in[0][q]; p.y = R.in[1][q]; p.z = R.in[2][q];
         p.vx = R.in[3][q]; p.vy = R.in[4][q]; p.vz = R.in[5][q];
         p.t = R.in[6][q]; p.w = R.in[7][q]; p.w0 = R.in[8][q];
         p.cell = R.cell[q];
+        track_begin(C, T);
         TapeRng rng{R.tape + R.tapeOffset[q], R.tapeLength[q], 0, false};
         LocalTally tal{0.0, 0.0};
-        PhysOut o = physics_step(C, p, rng, tal);
+        PhysOut o = physics_step(C, T, rng, tal);
         R.phys[0][q] = p.x; R.phys[1][q] = p.y; R.phys[2][q] = p.z;
         R.phys[3][q] = p.vx; R.phys[4][q] = p.vy; R.phys[5][q] = p.vz;
         R.phys[6][q] = p.t; R.phys[7][q] = p.w;
@@ -857,7 +917,7 @@ __global__ void k_replay(Ctx C, ReplayDev R, uint32_t n) {
         R.dep[1][q] = tal.rad_;
         R.usedRW[q] = o.usedRW;
         R.draws[q] = rng.pos;
-        int m = o.errCode ? OUT_ERROR : manager_handle(C, p, o);
+        int m = o.errCode ? OUT_ERROR : manager_handle(C, T, o);
         R.mgr[0][q] = p.x; R.mgr[1][q] = p.y; R.mgr[2][q] = p.z;
         R.mgr[3][q] = p.vx; R.mgr[4][q] = p.vy; R.mgr[5][q] = p.vz;
         R.mgrCell[q] = p.cell;
@@ -949,6 +1009,10 @@ void launch_emission_energy(cudaStream_t s, const Ctx &C, const CellArrays &A, d
 void launch_sequential_sum(cudaStream_t s, const double *v, uint32_t n, double *out) {
     k_sequential_sum<<<1, 256, 0, s>>>(v, n, out);
 }
+void launch_allocate_checked(cudaStream_t s, const Ctx &C, const CellArrays &A, const double *total,
+                             uint64_t newPerCell, double rel, int32_t *ambiguous) {
+    k_allocate_checked<<<grid_for(C.ncells, 256, 8192), 256, 0, s>>>(C, A, total, newPerCell, rel, ambiguous);
+}
 void launch_allocate(cudaStream_t s, const Ctx &C, const CellArrays &A, const double *total, uint64_t newPerCell) {
     k_allocate<<<grid_for(C.ncells, 256, 8192), 256, 0, s>>>(C, A, total, newPerCell);
 }
@@ -972,8 +1036,23 @@ void launch_emit_faces(cudaStream_t s, const Ctx &C, const FaceSources &F, uint6
     k_emit_faces<<<grid_for(total, 256, 148 * 16), 256, 0, s>>>(C, F, total, b, bankBase, dt, st);
 }
 void launch_transport(cudaStream_t s, uint32_t grid, const Ctx &C, const Bank &in, const uint32_t *nIn, const Bank &out,
-                      uint32_t *nOut, const Bank &cen, uint32_t *nCen, uint32_t K, DevStats *st) {
-    k_transport<<<grid, 256, 0, s>>>(C, in, nIn, out, nOut, cen, nCen, K, st);
+                      uint32_t *nOut, const Bank &cen, uint32_t *nCen, uint32_t K, DevStats *st, int minBlocks) {
+    switch (minBlocks) {
+    case 3: k_transport<3><<<grid, 256, 0, s>>>(C, in, nIn, out, nOut, cen, nCen, K, st); break;
+    case 4: k_transport<4><<<grid, 256, 0, s>>>(C, in, nIn, out, nOut, cen, nCen, K, st); break;
+    case 2: k_transport<2><<<grid, 256, 0, s>>>(C, in, nIn, out, nOut, cen, nCen, K, st); break;
+    default: k_transport<1><<<grid, 256, 0, s>>>(C, in, nIn, out, nOut, cen, nCen, K, st); break;
+    }
+}
+int transport_blocks_per_sm(int minBlocks) {
+    int nb = 0;
+    switch (minBlocks) {
+    case 3: cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_transport<3>, 256, 0); break;
+    case 4: cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_transport<4>, 256, 0); break;
+    case 2: cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_transport<2>, 256, 0); break;
+    default: cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_transport<1>, 256, 0); break;
+    }
+    return nb;
 }
 void launch_comb_keys(cudaStream_t s, const Ctx &C, const Bank &cen, uint32_t n, uint64_t *keys, uint32_t *vals,
                       uint32_t combKey) {
@@ -986,9 +1065,14 @@ int launch_radix_sort(cudaStream_t s, uint64_t *keys, uint32_t *vals, uint64_t *
     int passes = (bits + 7) / 8;
     uint64_t *ka = keys, *kb = keysAlt;
     uint32_t *va = vals, *vb = valsAlt;
+    const uint32_t len = 256 * ntiles;
+    const uint32_t stiles = (len + 1023) / 1024;
+    uint64_t *scanSums = reinterpret_cast<uint64_t *>(tileHist + len + (len & 1));
     for (int p = 0; p < passes; ++p) {
         k_rs_hist<<<ntiles, RS_THREADS, 0, s>>>(ka, n, 8 * p, tileHist, ntiles);
-        k_rs_scan<<<1, 1024, 0, s>>>(tileHist, 256 * ntiles);
+        k_scan32_tiles<<<stiles, 1024, 0, s>>>(tileHist, len, scanSums);
+        k_scan_sums<<<1, 1024, 0, s>>>(scanSums, stiles, scanSums + stiles);
+        k_scan32_add<<<stiles, 1024, 0, s>>>(tileHist, len, scanSums);
         k_rs_scatter<<<ntiles, RS_THREADS, 0, s>>>(ka, va, kb, vb, n, 8 * p, tileHist, ntiles);
         uint64_t *tk = ka; ka = kb; kb = tk;
         uint32_t *tv = va; va = vb; vb = tv;
@@ -996,6 +1080,12 @@ int launch_radix_sort(cudaStream_t s, uint64_t *keys, uint32_t *vals, uint64_t *
     return passes & 1;
 }
 uint32_t radix_tile_count(uint32_t n) { return (n + RS_TILE - 1) / RS_TILE ? (n + RS_TILE - 1) / RS_TILE : 1; }
+// 32-bit words the radix sort needs for its tile histogram and the scan's tile sums
+size_t radix_scratch_words(uint32_t n) {
+    size_t len = 256ull * radix_tile_count(n);
+    size_t stiles = (len + 1023) / 1024;
+    return len + (len & 1) + 2 * (stiles + 2);
+}
 void launch_comb_ranges(cudaStream_t s, const uint64_t *keys, uint32_t n, uint32_t ncells, uint32_t *start) {
     k_comb_ranges<<<grid_for(ncells + 1, 256, 8192), 256, 0, s>>>(keys, n, ncells, start);
 }
@@ -1006,15 +1096,21 @@ void launch_comb_cell_sums(cudaStream_t s, const Bank &cen, const uint32_t *idx,
 void launch_blocked_sum(cudaStream_t s, const double *v, uint32_t n, double *out) {
     k_blocked_sum<<<1, 1024, 0, s>>>(v, n, out);
 }
-void launch_comb_count(cudaStream_t s, const Ctx &C, const CombParams &P, const Bank &cen, const uint32_t *idx,
-                       const uint32_t *start, const double *W, const double *Wtot, uint64_t *outCount) {
-    k_comb_count<<<grid_for(C.ncells, 128, 8192), 128, 0, s>>>(C, P, cen, idx, start, W, Wtot, outCount);
+void launch_comb_plan(cudaStream_t s, const Ctx &C, const CombParams &P, const Bank &cen, const uint32_t *idx,
+                      const uint32_t *start, const double *W, const double *Wtot, uint32_t *pCount, double *pWeight,
+                      uint64_t *cellCount, double *eradCensus, DevStats *st) {
+    k_comb_plan<<<grid_for(C.ncells, 128, 8192), 128, 0, s>>>(C, P, cen, idx, start, W, Wtot, pCount, pWeight, cellCount,
+                                                               eradCensus, st);
 }
-void launch_comb_write(cudaStream_t s, const Ctx &C, const CombParams &P, const Bank &cen, const uint32_t *idx,
-                       const uint32_t *start, const double *W, const double *Wtot, const uint64_t *outOffset,
-                       const Bank &out, double *eradCensus, DevStats *st) {
-    k_comb_write<<<grid_for(C.ncells, 128, 8192), 128, 0, s>>>(C, P, cen, idx, start, W, Wtot, outOffset, out, eradCensus,
-                                                                st);
+void launch_comb_emit(cudaStream_t s, const Ctx &C, const Bank &cen, const uint32_t *idx, const uint64_t *sortedKeys,
+                      uint32_t nValid, const uint32_t *pCount, const double *pWeight, const uint64_t *pOffset,
+                      const Bank &out) {
+    if (!nValid) return;
+    k_comb_emit<<<grid_for(nValid, 256, 148 * 16), 256, 0, s>>>(C, cen, idx, sortedKeys, nValid, pCount, pWeight,
+                                                                pOffset, out);
+}
+void launch_mask_count(cudaStream_t s, const uint32_t *pCount, uint32_t n, uint64_t *out) {
+    k_mask_count<<<grid_for(n, 256, 8192), 256, 0, s>>>(pCount, n, out);
 }
 void launch_census_keys_pid(cudaStream_t s, const Bank &cen, uint32_t n, uint64_t *keys, uint32_t *vals) {
     k_census_keys_pid<<<grid_for(n, 256, 8192), 256, 0, s>>>(cen, n, keys, vals);

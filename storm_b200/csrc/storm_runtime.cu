@@ -58,6 +58,10 @@ struct StormHandle {
     uint64_t *keys = nullptr, *keysAlt = nullptr;
     uint32_t *vals = nullptr, *valsAlt = nullptr, *tileHist = nullptr;
     size_t tileHistLen = 0;
+    uint32_t *pCount = nullptr;      // comb: copies per sorted particle
+    double *pWeight = nullptr;       // comb: weight of those copies
+    uint64_t *pOff = nullptr, *pTiles = nullptr;   // comb: output positions, scan tile sums
+    int32_t *dAmbiguous = nullptr;
     // scratch
     uint64_t *offsets = nullptr, *tileSums = nullptr, *dTotalU64 = nullptr;
     double *dTotalE = nullptr, *combW = nullptr, *combWtot = nullptr;
@@ -71,7 +75,11 @@ struct StormHandle {
     uint64_t nBank = 0;              // particles in bankA after emission
     uint32_t step = 0;
     uint32_t K = 8, maxRounds = 4096;
+    int minBlocks = 2;               // transport occupancy variant (__launch_bounds__ min blocks)
+    int smCount = 148;
+    uint32_t transportGrid = 0;      // resident blocks of the chosen variant x SMs
     uint64_t launches = 0;
+    uint64_t exactSums = 0;          // steps whose allocation needed the left-to-right total
     uint64_t memBytes = 0;
     StormStepStats stats{};
     std::vector<uint64_t> lastPhotons;
@@ -153,6 +161,32 @@ cudaError_t bank_copy(cudaStream_t s, const Bank &dst, const Bank &src, size_t n
     return cudaSuccess;
 }
 
+// Buffers sized by particle capacity, other than the transport banks A and B.
+cudaError_t alloc_rest(StormHandle *h, size_t nc) {
+    cudaError_t e;
+    if ((e = bank_alloc(h, h->bankC, nc)) != cudaSuccess) return e;
+    if ((e = dalloc(h, &h->keys, nc)) != cudaSuccess) return e;
+    if ((e = dalloc(h, &h->keysAlt, nc)) != cudaSuccess) return e;
+    if ((e = dalloc(h, &h->vals, nc)) != cudaSuccess) return e;
+    if ((e = dalloc(h, &h->valsAlt, nc)) != cudaSuccess) return e;
+    h->tileHistLen = radix_scratch_words(static_cast<uint32_t>(nc));
+    if ((e = dalloc(h, &h->tileHist, h->tileHistLen)) != cudaSuccess) return e;
+    if ((e = dalloc(h, &h->pCount, nc)) != cudaSuccess) return e;
+    if ((e = dalloc(h, &h->pWeight, nc)) != cudaSuccess) return e;
+    if ((e = dalloc(h, &h->pOff, nc + 1)) != cudaSuccess) return e;
+    return dalloc(h, &h->pTiles, nc / 1024 + 4);
+}
+void free_rest(StormHandle *h, size_t nc) {
+    bank_free(h, h->bankC, nc);
+    dfree(h, h->keys, nc); dfree(h, h->keysAlt, nc);
+    dfree(h, h->vals, nc); dfree(h, h->valsAlt, nc);
+    dfree(h, h->tileHist, h->tileHistLen);
+    dfree(h, h->pCount, nc);
+    dfree(h, h->pWeight, nc);
+    dfree(h, h->pOff, nc + 1);
+    dfree(h, h->pTiles, nc / 1024 + 4);
+}
+
 // (Re)allocate every per-particle buffer for capacity n, keeping the first
 // `keep` particles of bank A.
 int ensure_capacity(StormHandle *h, size_t n, size_t keep) {
@@ -168,17 +202,10 @@ int ensure_capacity(StormHandle *h, size_t n, size_t keep) {
     CK(cudaStreamSynchronize(h->stream));
     bank_free(h, h->bankA, h->cap);
     bank_free(h, h->bankB, h->cap);
-    bank_free(h, h->bankC, h->cap);
-    dfree(h, h->keys, h->cap); dfree(h, h->keysAlt, h->cap);
-    dfree(h, h->vals, h->cap); dfree(h, h->valsAlt, h->cap);
-    dfree(h, h->tileHist, h->tileHistLen);
+    free_rest(h, h->cap);
     h->bankA = na;
     CK(bank_alloc(h, h->bankB, nc));
-    CK(bank_alloc(h, h->bankC, nc));
-    CK(dalloc(h, &h->keys, nc)); CK(dalloc(h, &h->keysAlt, nc));
-    CK(dalloc(h, &h->vals, nc)); CK(dalloc(h, &h->valsAlt, nc));
-    h->tileHistLen = 256ull * radix_tile_count(static_cast<uint32_t>(nc));
-    CK(dalloc(h, &h->tileHist, h->tileHistLen));
+    CK(alloc_rest(h, nc));
     h->cap = nc;
     return STORM_OK;
 }
@@ -324,9 +351,11 @@ void refresh_ctx(StormHandle *h) {
     h->C.step = h->step;
 }
 
-uint32_t grid_transport(uint64_t n) {
+// A persistent-style grid: the resident blocks of the variant on every SM (a
+// multiple of the SM count), or fewer when the bank is small.
+uint32_t grid_transport(uint64_t n, uint32_t resident) {
     uint64_t g = (n + 255) / 256;
-    const uint64_t cap = 148ull * 8;
+    const uint64_t cap = resident ? resident : 148ull * 8;
     if (g < 1) g = 1;
     return static_cast<uint32_t>(g < cap ? g : cap);
 }
@@ -414,6 +443,7 @@ int storm_cuda_create(const StormProblemDesc *d, StormHandle **out) {
     for (double **q : cd) ALLOC(*q, N);
     ALLOC(A.rwElig, N);
     ALLOC(A.photons, N);
+    ALLOC(A.phys, N);
     ALLOC(h->segs, N);
     std::vector<double> vol(N);
     for (uint32_t c = 0; c < N; ++c) {
@@ -464,9 +494,17 @@ int storm_cuda_create(const StormProblemDesc *d, StormHandle **out) {
     h->maxRounds = d->max_rounds ? d->max_rounds : 16384;
     ALLOC(h->counts, h->maxRounds + 2);
     ALLOC(h->dStats, 1);
+    ALLOC(h->dAmbiguous, 2);
     ALLOC(h->dErr, 4);
     if (cudaMemset(h->dErr, 0, 4 * sizeof(int32_t)) != cudaSuccess) return fail(STORM_ERR_CUDA);
     h->K = d->segments_per_visit ? d->segments_per_visit : 8;
+    {
+        cudaDeviceProp prop{};
+        cudaGetDeviceProperties(&prop, h->device);
+        int nb = transport_blocks_per_sm(h->minBlocks);
+        h->transportGrid = static_cast<uint32_t>(prop.multiProcessorCount) * static_cast<uint32_t>(nb > 0 ? nb : 1) * 4;
+        h->smCount = prop.multiProcessorCount;
+    }
 
     Ctx &C = h->C;
     C.nx = d->nx; C.ny = d->ny; C.nz = d->nz; C.ncells = N;
@@ -485,6 +523,7 @@ int storm_cuda_create(const StormProblemDesc *d, StormHandle **out) {
     C.seedLo = static_cast<uint32_t>(d->seed);
     C.seedHi = static_cast<uint32_t>(d->seed >> 32);
     C.step = 0;
+    C.phys = A.phys;
     C.sigA = A.sigA; C.sigS = A.sigS; C.fleck = A.fleck; C.rwSigT = A.rwSigT; C.rwElig = A.rwElig;
     C.eint = A.eint; C.eradAvg = A.eradAvg; C.segs = h->segs;
     C.err = h->dErr;
@@ -510,12 +549,11 @@ int storm_cuda_destroy(StormHandle *h) {
     if (h->stream) cudaStreamSynchronize(h->stream);
     bank_free(h, h->bankA, h->cap);
     bank_free(h, h->bankB, h->cap);
-    bank_free(h, h->bankC, h->cap);
+    free_rest(h, h->cap);
     void *ps[] = {h->xe, h->ye, h->ze, h->xc, h->yc, h->zc, h->A.T, h->A.mass, h->A.vol, h->A.eint, h->A.ceint,
                   h->A.sigA, h->A.sigS, h->A.fleck, h->A.rwSigT, h->A.eradAvg, h->A.eradCensus, h->A.emitE,
-                  h->A.rwElig, h->A.photons, h->segs, h->tabA, h->tabS, h->rhoF, h->rwTau, h->rwLogTau, h->rwSurv,
-                  h->rwRadius, h->fsCell, h->fsSide, h->fsOffset, h->keys, h->keysAlt, h->vals, h->valsAlt,
-                  h->tileHist, h->offsets, h->tileSums, h->dTotalU64, h->dTotalE, h->combW, h->combWtot,
+                  h->A.rwElig, h->A.photons, h->A.phys, h->segs, h->tabA, h->tabS, h->rhoF, h->rwTau, h->rwLogTau, h->rwSurv,
+                  h->rwRadius, h->fsCell, h->fsSide, h->fsOffset, h->dAmbiguous, h->offsets, h->tileSums, h->dTotalU64, h->dTotalE, h->combW, h->combWtot,
                   h->combStart, h->combCount, h->counts, h->dStats, h->dErr};
     for (void *p : ps)
         if (p) cudaFree(p);
@@ -560,16 +598,36 @@ int storm_cuda_phase_emit(StormHandle *h, double dt) {
     if (!h) return STORM_ERR_INVALID_ARG;
     refresh_ctx(h);
     const uint32_t N = h->N;
+    // The reference floors each cell's share against its left-to-right total
+    // (RadiationIMC.hpp:2058-2087).  A blocked total plus a rigorous interval
+    // settles almost every step; a flagged step recomputes with the exact
+    // left-to-right total.  Either way the counts equal the reference's.
     launch_emission_energy(h->stream, h->C, h->A, dt);
-    launch_sequential_sum(h->stream, h->A.emitE, N, h->dTotalE);
-    launch_allocate(h->stream, h->C, h->A, h->dTotalE, h->desc.new_photons_per_cell);
-    launch_emission_debit(h->stream, h->C, h->A, h->dStats);
+    launch_blocked_sum(h->stream, h->A.emitE, N, h->dTotalE);
+    CK(cudaMemsetAsync(h->dAmbiguous, 0, sizeof(int32_t), h->stream));
+    const double u = 0x1p-53;
+    const double rel = 4.0 * (static_cast<double>(N) + 1100.0) * u;   // both orders' rounding, with margin
+    launch_allocate_checked(h->stream, h->C, h->A, h->dTotalE, h->desc.new_photons_per_cell, rel, h->dAmbiguous);
     launch_scan_u64(h->stream, h->A.photons, N, h->offsets, h->tileSums, h->dTotalU64);
-    h->launches += 7;
+    h->launches += 6;
     CK(cudaGetLastError());
-    uint64_t ne = 0;
-    CK(cudaMemcpyAsync(&ne, h->dTotalU64, sizeof(uint64_t), cudaMemcpyDeviceToHost, h->stream));
+    struct { uint64_t total; int32_t amb; } back{};
+    CK(cudaMemcpyAsync(&back.total, h->dTotalU64, sizeof(uint64_t), cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaMemcpyAsync(&back.amb, h->dAmbiguous, sizeof(int32_t), cudaMemcpyDeviceToHost, h->stream));
     CK(cudaStreamSynchronize(h->stream));
+    if (back.amb) {
+        launch_sequential_sum(h->stream, h->A.emitE, N, h->dTotalE);
+        launch_allocate(h->stream, h->C, h->A, h->dTotalE, h->desc.new_photons_per_cell);
+        launch_scan_u64(h->stream, h->A.photons, N, h->offsets, h->tileSums, h->dTotalU64);
+        h->launches += 5;
+        ++h->exactSums;
+        CK(cudaGetLastError());
+        CK(cudaMemcpyAsync(&back.total, h->dTotalU64, sizeof(uint64_t), cudaMemcpyDeviceToHost, h->stream));
+        CK(cudaStreamSynchronize(h->stream));
+    }
+    launch_emission_debit(h->stream, h->C, h->A, h->dStats);
+    ++h->launches;
+    uint64_t ne = back.total;
     const uint64_t nf = h->fsTotal;
     const uint64_t total = h->nCensus + ne + nf;
     int rc = ensure_capacity(h, total, h->nCensus);
@@ -595,7 +653,7 @@ int storm_cuda_phase_transport(StormHandle *h) {
     uint32_t n32 = static_cast<uint32_t>(n0);
     CK(cudaMemcpyAsync(h->counts, &n32, sizeof(uint32_t), cudaMemcpyHostToDevice, h->stream));
     uint32_t *nCen = h->counts + h->maxRounds + 1;
-    const uint32_t grid = grid_transport(n0);
+    const uint32_t grid = grid_transport(n0, h->transportGrid);
     uint32_t r = 0;
     bool done = (n0 == 0);
     const uint32_t pollEvery = 4;
@@ -610,7 +668,7 @@ int storm_cuda_phase_transport(StormHandle *h) {
         const Bank &out = (r & 1) ? h->bankA : h->bankB;
         if (h->profiling) CK(cudaEventRecord(h->evPool[2 * inWindow], h->stream));
         launch_transport(h->stream, grid, h->C, in, h->counts + r, out, h->counts + r + 1, h->bankC, nCen, h->K,
-                         h->dStats);
+                         h->dStats, h->minBlocks);
         if (h->profiling) CK(cudaEventRecord(h->evPool[2 * inWindow + 1], h->stream));
         ++inWindow;
         ++h->launches;
@@ -703,9 +761,21 @@ int storm_cuda_phase_comb(StormHandle *h) {
     CombParams P;
     P.nmin = h->desc.comb_nmin;
     P.ntotal = static_cast<uint64_t>(static_cast<double>(static_cast<uint64_t>(N) * h->desc.comb_nmin) * h->desc.comb_factor);
-    launch_comb_count(h->stream, h->C, P, h->bankC, idx, h->combStart, h->combW, h->combWtot, h->combCount);
-    launch_scan_u64(h->stream, h->combCount, N, h->offsets, h->tileSums, h->dTotalU64);
-    h->launches += 1 + 3 * passes + 4 + 3;
+    launch_comb_plan(h->stream, h->C, P, h->bankC, idx, h->combStart, h->combW, h->combWtot, h->pCount, h->pWeight,
+                     h->combCount, h->A.eradCensus, h->dStats);
+    h->launches += 1 + 5 * passes + 4;
+    CK(cudaGetLastError());
+    uint32_t nValid = 0;
+    CK(cudaMemcpyAsync(&nValid, h->combStart + N, sizeof(uint32_t), cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    uint64_t *countU64 = alt ? h->keys : h->keysAlt;   // the sort's spare key buffer
+    if (nValid) {
+        launch_mask_count(h->stream, h->pCount, nValid, countU64);
+        launch_scan_u64(h->stream, countU64, nValid, h->pOff, h->pTiles, h->dTotalU64);
+        h->launches += 4;
+    } else {
+        CK(cudaMemsetAsync(h->dTotalU64, 0, sizeof(uint64_t), h->stream));
+    }
     CK(cudaGetLastError());
     int rc = check_device_error(h);
     if (rc != STORM_OK) return rc;
@@ -713,31 +783,24 @@ int storm_cuda_phase_comb(StormHandle *h) {
     CK(cudaMemcpy(&total, h->dTotalU64, sizeof(uint64_t), cudaMemcpyDeviceToHost));
     // The write goes to bank A, which transport has finished with.  When the
     // combed census outgrows the banks, A and B are replaced first (their
-    // contents are dead); C and the sort buffers, which the write still reads,
+    // contents are dead); C and the comb buffers, which the write still reads,
     // are replaced after it.
     size_t grown = 0;
     if (total > h->cap) {
+        if (total > 0xF0000000ull) return STORM_ERR_CAPACITY;
         grown = total + total / 4;
         bank_free(h, h->bankA, h->cap);
         bank_free(h, h->bankB, h->cap);
         CK(bank_alloc(h, h->bankA, grown));
         CK(bank_alloc(h, h->bankB, grown));
     }
-    launch_comb_write(h->stream, h->C, P, h->bankC, idx, h->combStart, h->combW, h->combWtot, h->offsets, h->bankA,
-                      h->A.eradCensus, h->dStats);
+    launch_comb_emit(h->stream, h->C, h->bankC, idx, skeys, nValid, h->pCount, h->pWeight, h->pOff, h->bankA);
     ++h->launches;
     CK(cudaGetLastError());
     if (grown) {
         CK(cudaStreamSynchronize(h->stream));
-        bank_free(h, h->bankC, h->cap);
-        dfree(h, h->keys, h->cap); dfree(h, h->keysAlt, h->cap);
-        dfree(h, h->vals, h->cap); dfree(h, h->valsAlt, h->cap);
-        dfree(h, h->tileHist, h->tileHistLen);
-        CK(bank_alloc(h, h->bankC, grown));
-        CK(dalloc(h, &h->keys, grown)); CK(dalloc(h, &h->keysAlt, grown));
-        CK(dalloc(h, &h->vals, grown)); CK(dalloc(h, &h->valsAlt, grown));
-        h->tileHistLen = 256ull * radix_tile_count(static_cast<uint32_t>(grown));
-        CK(dalloc(h, &h->tileHist, h->tileHistLen));
+        free_rest(h, h->cap);
+        CK(alloc_rest(h, grown));
         h->cap = grown;
     }
     h->nCensus = total;
@@ -916,12 +979,10 @@ int storm_cuda_set_cell_physics(StormHandle *h, const double *sigA, const double
     if (sigS) CK(cudaMemcpyAsync(h->A.sigS, sigS, N * sizeof(double), cudaMemcpyHostToDevice, h->stream));
     if (fleck) CK(cudaMemcpyAsync(h->A.fleck, fleck, N * sizeof(double), cudaMemcpyHostToDevice, h->stream));
     CK(cudaStreamSynchronize(h->stream));
-    if (h->desc.with_random_walk) {
-        launch_rw_eligibility(h->stream, h->C, h->A);
-        ++h->launches;
-        CK(cudaGetLastError());
-        CK(cudaStreamSynchronize(h->stream));
-    }
+    launch_rw_eligibility(h->stream, h->C, h->A);
+    ++h->launches;
+    CK(cudaGetLastError());
+    CK(cudaStreamSynchronize(h->stream));
     return STORM_OK;
 }
 
@@ -1079,6 +1140,14 @@ int storm_cuda_transport_timing(StormHandle *h, double *ms, uint64_t *launches, 
         h->profLaunches = 0;
         h->profSegments = 0;
     }
+    return STORM_OK;
+}
+
+int storm_cuda_set_transport_variant(StormHandle *h, int min_blocks_per_sm, int waves) {
+    if (!h || min_blocks_per_sm < 1 || min_blocks_per_sm > 4 || waves < 1 || waves > 64) return STORM_ERR_INVALID_ARG;
+    h->minBlocks = min_blocks_per_sm;
+    int nb = transport_blocks_per_sm(h->minBlocks);
+    h->transportGrid = static_cast<uint32_t>(h->smCount) * static_cast<uint32_t>(nb > 0 ? nb : 1) * waves;
     return STORM_OK;
 }
 

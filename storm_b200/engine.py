@@ -56,6 +56,7 @@ def lib():
         L.storm_cuda_launch_count.argtypes = [vp, u64p]
         L.storm_cuda_set_segments_per_visit.argtypes = [vp, C.c_uint32]
         L.storm_cuda_set_profiling.argtypes = [vp, C.c_int]
+        L.storm_cuda_set_transport_variant.argtypes = [vp, C.c_int, C.c_int]
         L.storm_cuda_transport_timing.argtypes = [vp, dp, u64p, u64p, C.c_int]
         L.storm_cuda_status_string.restype = C.c_char_p
         L.storm_cuda_status_string.argtypes = [C.c_int]
@@ -224,6 +225,9 @@ class Engine:
         ms, n, s = C.c_double(), C.c_uint64(), C.c_uint64()
         self._check(lib().storm_cuda_transport_timing(self.h, C.byref(ms), C.byref(n), C.byref(s), int(reset)))
         return {"kernel_ms": ms.value, "launches": n.value, "segments": s.value}
+
+    def set_transport_variant(self, min_blocks_per_sm, waves=4):
+        self._check(lib().storm_cuda_set_transport_variant(self.h, min_blocks_per_sm, waves))
 
     def set_segments_per_visit(self, k):
         self._check(lib().storm_cuda_set_segments_per_visit(self.h, k))
