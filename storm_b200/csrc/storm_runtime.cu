@@ -75,7 +75,7 @@ struct StormHandle {
     uint64_t nBank = 0;              // particles in bankA after emission
     uint32_t step = 0;
     uint32_t K = 8, maxRounds = 4096;
-    int minBlocks = 2;               // transport occupancy variant (__launch_bounds__ min blocks)
+    int minBlocks = 3;               // transport occupancy variant (__launch_bounds__ min blocks)
     int smCount = 148;
     uint32_t transportGrid = 0;      // resident blocks of the chosen variant x SMs
     uint64_t launches = 0;
@@ -497,7 +497,7 @@ int storm_cuda_create(const StormProblemDesc *d, StormHandle **out) {
     ALLOC(h->dAmbiguous, 2);
     ALLOC(h->dErr, 4);
     if (cudaMemset(h->dErr, 0, 4 * sizeof(int32_t)) != cudaSuccess) return fail(STORM_ERR_CUDA);
-    h->K = d->segments_per_visit ? d->segments_per_visit : 8;
+    h->K = d->segments_per_visit ? d->segments_per_visit : 16;
     {
         cudaDeviceProp prop{};
         cudaGetDeviceProperties(&prop, h->device);
