@@ -32,6 +32,9 @@ UNIT = "segments/s"
 # Algorithmic bytes per segment of the FP64 form: particle state read + write
 # (2 x 72 B), cell sigma_a and Fleck factor (16 B), two tallies (16 B).
 BYTES_PER_SEGMENT_FP64 = 176
+# FP32-tracking form: state 2 x 44 B (cell 4, offset 3x4, direction 3x4, weight 8,
+# time 8), cell constants 16 B, tallies 16 B.
+BYTES_PER_SEGMENT_FP32 = 120
 
 
 def parse():
@@ -206,13 +209,22 @@ def cpu_baseline(n, cores, steps=3):
 
 
 # ---------------------------------------------------------------------- storm arm
-def run_storm(args, ws, rank, local, dist):
-    import numpy as np
+def _peak():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        v = json.load(open(path)).get("hbm_gbs")
+        if v:
+            return float(v), "measured"
+    return 6650.0, "fallback"
+
+
+def run_form(args, precision, seed, local, dist, timed=True):
+    """Warm up, then time args.steps IMC steps of one form; returns its numbers."""
     import torch
-    from storm_b200.engine import Engine, Particles
-    torch.cuda.set_device(local)
-    p = workload(args.n, seed=42 + rank)
+    from storm_b200.engine import Engine
+    p = workload(args.n, seed=seed)
     p.device = local
+    p.precision = precision
     p.per_cell_segment_counters = False
     eng = Engine(p)
     if args.segments_per_visit:
@@ -224,115 +236,145 @@ def run_storm(args, ws, rank, local, dist):
         eng.step()
     torch.cuda.synchronize()
     barrier(dist, "storm")
-    clocks = Clocks(local)
-    clocks.start()
     eng.transport_timing(reset=True)
     l0 = eng.launches()
     step_ms, segs = [], 0
-    for _ in range(args.steps):
+    for _ in range(args.steps if timed else 0):
         st = eng.step()
         step_ms.append(st["step_ms"])
         segs += st["segments"]
     torch.cuda.synchronize()
     barrier(dist, "storm")
+    out = {"engine": eng, "problem": p, "step_ms": step_ms, "segments": segs, "launches": eng.launches() - l0,
+           "transport": eng.transport_timing(reset=True)}
+    return out
+
+
+def roofline(res, bytes_per_segment):
+    peak, src = _peak()
+    tt = res["transport"]
+    mean_ms = tt["kernel_ms"] / max(tt["launches"], 1)
+    bytes_per_launch = bytes_per_segment * tt["segments"] / max(tt["launches"], 1)
+    achieved = bytes_per_launch / (mean_ms / 1000.0) / 1e9
+    return {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+            "traffic": None, "kernel": "k_transport32" if bytes_per_segment == BYTES_PER_SEGMENT_FP32 else "k_transport",
+            "bytes_per_segment": bytes_per_segment, "mean_launch_ms": mean_ms, "launches": tt["launches"],
+            "peak_source": src, "note": "peak = measured copy bandwidth (" + src + ")"}
+
+
+def e2e_run(args, eng, p, dist):
+    """The same metric through the C ABI with host buffers: the census goes
+    host->device from pinned memory before each step and comes back with the
+    material temperatures after it."""
+    import numpy as np
+    import torch
+    from storm_b200.engine import Particles
+    cen = eng.census()
+    n = cen.n
+    cap = max(2 * n, 1)
+    pin = {f: torch.empty(cap, dtype=torch.float64, pin_memory=True).numpy() for f in Particles.FIELDS}
+    pin_cell = torch.empty(cap, dtype=torch.int32, pin_memory=True).numpy().view(np.uint32)
+    pin_T = torch.empty(p.ncells, dtype=torch.float64, pin_memory=True).numpy()
+    host = Particles(0)
+
+    def stage(src, m):
+        for f in Particles.FIELDS:
+            pin[f][:m] = getattr(src, f)[:m]
+            setattr(host, f, pin[f][:m])
+        pin_cell[:m] = src.cell[:m]
+        host.cell = pin_cell[:m]
+        host.id = np.zeros(m, np.uint64)
+        host.n = m
+
+    stage(cen, n)
+    torch.cuda.synchronize()
+    barrier(dist, "storm")
+    t0 = time.perf_counter()
+    segs, h2d, d2h = 0, 0, 0
+    for _ in range(args.e2e_steps):
+        eng.set_census(host)
+        h2d += host.n * (9 * 8 + 4)
+        st = eng.step()
+        segs += st["segments"]
+        out = eng.census()
+        d2h += out.n * (9 * 8 + 4)
+        pin_T[:] = eng.cells()["temperature"]
+        d2h += p.ncells * 8
+        if out.n > cap:
+            break
+        stage(out, out.n)
+    torch.cuda.synchronize()
+    wall = reduce(dist, time.perf_counter() - t0, "max", "storm")
+    allsegs = reduce(dist, segs, "sum", "storm")
+    return {"value": allsegs / wall, "unit": UNIT, "h2d_bytes_per_step": int(h2d / args.e2e_steps),
+            "d2h_bytes_per_step": int(d2h / args.e2e_steps), "steps": args.e2e_steps,
+            "note": "census + temperatures through storm_cuda_set_census / step / get_census / get_cell_arrays; "
+                    "host staging in pinned memory; copies inside the timed region"}
+
+
+def run_storm(args, ws, rank, local, dist):
+    import numpy as np
+    import torch
+    from storm_b200 import _abi as A
+    torch.cuda.set_device(local)
+    seed = 42 + rank
+    clocks = Clocks(local)
+    clocks.start()
+    f32 = run_form(args, A.PRECISION_FP32_TRACK, seed, local, dist)
+    f64 = run_form(args, A.PRECISION_FP64, seed, local, dist)
     ck = clocks.stop()
-    launches = eng.launches() - l0
-    tt = eng.transport_timing(reset=True)
-    total_ms = reduce(dist, sum(step_ms), "max", "storm")
-    all_segs = reduce(dist, segs, "sum", "storm")
-    value = all_segs / (total_ms / 1000.0)
+    e2e = e2e_run(args, f32["engine"], f32["problem"], dist) if args.e2e_steps > 0 else None
 
-    # dominant kernel: transport; algorithmic bytes per launch / mean launch time
-    peak = None
-    peaks_path = os.path.join(ROOT, "MEASURED_PEAKS.json")
-    peak_src = "fallback"
-    if os.path.exists(peaks_path):
-        peak = json.load(open(peaks_path)).get("hbm_gbs")
-        peak_src = "measured"
-    if not peak:
-        peak = 6650.0
-    mean_launch_ms = tt["kernel_ms"] / max(tt["launches"], 1)
-    bytes_per_launch = BYTES_PER_SEGMENT_FP64 * tt["segments"] / max(tt["launches"], 1)
-    achieved = bytes_per_launch / (mean_launch_ms / 1000.0) / 1e9
-    traffic = None
-    tpath = os.path.join(ROOT, "profiles", "transport_traffic.json")
-    if os.path.exists(tpath):
-        traffic = json.load(open(tpath)).get("dram_bytes_per_launch_fullsize")
+    def rate(res):
+        ms = reduce(dist, sum(res["step_ms"]), "max", "storm")
+        sg = reduce(dist, res["segments"], "sum", "storm")
+        return sg / (ms / 1000.0), ms
 
-    # end to end through the C ABI with host buffers
-    e2e = None
-    if args.e2e_steps > 0:
-        cen = eng.census()
-        n = cen.n
-        host = Particles(0)
-        pin = {}
-        for f in Particles.FIELDS:
-            pin[f] = torch.empty(max(n, 1) * 2, dtype=torch.float64, pin_memory=True).numpy()
-        pin_cell = torch.empty(max(n, 1) * 2, dtype=torch.int32, pin_memory=True).numpy().view(np.uint32)
-        host.n = n
-        for f in Particles.FIELDS:
-            getattr(pin[f], "__setitem__")(slice(0, n), getattr(cen, f))
-            setattr(host, f, pin[f][:n])
-        pin_cell[:n] = cen.cell
-        host.cell = pin_cell[:n]
-        host.id = np.zeros(n, np.uint64)
-        tempT = torch.empty(p.ncells, dtype=torch.float64, pin_memory=True).numpy()
-        torch.cuda.synchronize()
-        barrier(dist, "storm")
-        t0 = time.perf_counter()
-        e2e_segs, h2d, d2h = 0, 0, 0
-        for _ in range(args.e2e_steps):
-            eng.set_census(host)
-            h2d += host.n * (9 * 8 + 4)
-            st = eng.step()
-            e2e_segs += st["segments"]
-            out = eng.census()            # census back to the host
-            d2h += out.n * (9 * 8 + 4)
-            T = eng.cells()["temperature"]
-            tempT[:] = T
-            d2h += p.ncells * 8
-            nn = out.n
-            if nn > len(pin_cell):
-                break
-            for f in Particles.FIELDS:
-                pin[f][:nn] = getattr(out, f)
-                setattr(host, f, pin[f][:nn])
-            pin_cell[:nn] = out.cell
-            host.cell = pin_cell[:nn]
-            host.id = np.zeros(nn, np.uint64)
-            host.n = nn
-        torch.cuda.synchronize()
-        wall = time.perf_counter() - t0
-        wall = reduce(dist, wall, "max", "storm")
-        e2e_all = reduce(dist, e2e_segs, "sum", "storm")
-        e2e = {"value": e2e_all / wall, "unit": UNIT, "h2d_bytes_per_step": int(h2d / args.e2e_steps),
-               "d2h_bytes_per_step": int(d2h / args.e2e_steps), "steps": args.e2e_steps,
-               "note": "pageable->pinned staging in numpy; copies inside the timed region"}
-
+    v32, ms32 = rate(f32)
+    v64, ms64 = rate(f64)
+    # FP32 vs FP64 on the same Philox streams, against the seed-to-seed scatter of the FP64 form
+    dev = None
+    if rank == 0:
+        T32 = f32["engine"].cells()["temperature"]
+        T64 = f64["engine"].cells()["temperature"]
+        other = run_form(args, A.PRECISION_FP64, seed + 1000, local, None, timed=True)
+        T64b = other["engine"].cells()["temperature"]
+        hot = T64 > 2.0 * T64.min()
+        sigma = np.sqrt(np.mean((T64 - T64b)[hot] ** 2) / 2.0)
+        dev = {"quantity": "per-cell material temperature after warm-up + timed steps",
+               "rms_fp32_minus_fp64_over_sigma": float(np.sqrt(np.mean((T32 - T64)[hot] ** 2)) / sigma),
+               "max_abs_fp32_minus_fp64_over_sigma": float(np.max(np.abs(T32 - T64)[hot]) / sigma),
+               "sigma_estimate": "rms difference of two FP64 seeds / sqrt(2), hot cells", "cells": int(hot.sum())}
+        other["engine"].close()
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline(args.n, 1)
-
     if rank == 0:
-        lat = sorted(step_ms)
+        lat = sorted(f32["step_ms"])
         line = {
-            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded Philox streams)",
-            "config": workload_config(args.n) | {"parallelism": f"{ws} independent problem(s), one per GPU"},
+            "metric": METRIC, "value": v32, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms32 / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32-track/f64-tally",
+            "data": "synthetic (seeded Philox streams)",
+            "config": workload_config(args.n) | {"parallelism": f"{ws} independent problem(s), one per GPU",
+                                                 "form": "FP32 cell-local tracking, FP64 time/weights/tallies"},
             "latency_ms": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99))},
-            "segments_per_step": segs / args.steps,
-            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                         "traffic": traffic, "kernel": "k_transport",
-                         "bytes_per_segment": BYTES_PER_SEGMENT_FP64,
-                         "mean_launch_ms": mean_launch_ms, "launches": tt["launches"],
-                         "peak_source": peak_src},
-            "cpu_baseline": cpu, "e2e": e2e, "clocks": ck, "gpu_launches": launches,
-            "transport_share": tt["kernel_ms"] / max(sum(step_ms), 1e-9),
+            "segments_per_step": f32["segments"] / args.steps,
+            "roofline": roofline(f32, BYTES_PER_SEGMENT_FP32),
+            "fp64": {"value": v64, "ms_per_step": ms64 / args.steps, "dtype": "f64",
+                     "latency_ms": {"p50": float(np.percentile(f64["step_ms"], 50)),
+                                    "p99": float(np.percentile(f64["step_ms"], 99))},
+                     "segments_per_step": f64["segments"] / args.steps,
+                     "roofline": roofline(f64, BYTES_PER_SEGMENT_FP64)},
+            "fp32_over_fp64": v32 / v64,
+            "fp32_vs_fp64_deviation": dev,
+            "cpu_baseline": cpu, "e2e": e2e, "clocks": ck, "gpu_launches": f32["launches"],
+            "transport_share": f32["transport"]["kernel_ms"] / max(sum(f32["step_ms"]), 1e-9),
         }
         print(json.dumps(line), flush=True)
+    f32["engine"].close()
+    f64["engine"].close()
     if dist is not None:
-        eng.close()
         dist.destroy_process_group()
 
 

@@ -67,6 +67,12 @@ struct Ctx {
     double rwMinParticle, rwMinCell;
     double sourceT[6];       // source temperature of each box face [K]
     uint32_t seedLo, seedHi, step;
+    // FP32-tracking form
+    int32_t fp32;            // banks hold cell-local FP32 offsets and FP32 directions
+    const float *hx, *hy, *hz;   // half widths per axis
+    const float4 *phys32;    // x = 1/sigma_e (inf when none), y = sigma_a f [1/cm]
+    float reflNudge[6];      // 1e-6 * faceScale of each box face, capped at a quarter cell
+    double invC;             // 1 / c
     // per-cell arrays
     const double4 *phys;     // per-cell segment constants (CellPhys layout)
     const double *sigA, *sigS, *fleck, *rwSigT;
@@ -484,6 +490,135 @@ __device__ inline PhysOut physics_step(const Ctx &C, Track &T, RNG &rng, TALLY &
         o.status = DONE;
     }
     return o;
+}
+
+// ------------------------------------------------------------------ FP32-tracking form
+// A particle in the FP32-tracking form: cell index plus its offset from the cell
+// centre and its direction in FP32; time, weight and initial weight in FP64.
+struct Track32 {
+    float qx, qy, qz, ux, uy, uz;
+    double t, w, w0;
+    uint32_t cell, i, j, k;
+};
+
+__device__ __forceinline__ float clampf(float v, float h) { return fminf(fmaxf(v, -h), h); }
+
+// uniform in (0,1) as float that is never 0 or 1
+__device__ __forceinline__ float to_open_float(double u) { return fminf(fmaxf(static_cast<float>(u), 0x1p-40f), 0x1.fffffep-1f); }
+
+// One segment plus the manager's handling, in the FP32-tracking form.  Same
+// events, same draws per event and the same FP64 tally updates as the FP64
+// form; distances, the face search and the collision distance are FP32 in the
+// cell's own frame, so precision follows the cell size, not the domain.
+template <class RNG, class TALLY>
+__device__ inline int segment32(const Ctx &C, Track32 &T, RNG &rng, TALLY &tal, int &usedRW, int &err) {
+    const uint32_t cell = T.cell;
+    const float hx = C.hx[T.i], hy = C.hy[T.j], hz = C.hz[T.k];
+    float sF = CUDART_INF_F;
+    int face = -1;
+    if (T.ux != 0.0f) {
+        float s = fmaxf((copysignf(hx, T.ux) - T.qx) / T.ux, 0.0f);
+        if (s < sF) { sF = s; face = T.ux > 0.0f ? 1 : 0; }
+    }
+    if (T.uy != 0.0f) {
+        float s = fmaxf((copysignf(hy, T.uy) - T.qy) / T.uy, 0.0f);
+        if (s < sF) { sF = s; face = T.uy > 0.0f ? 3 : 2; }
+    }
+    if (T.uz != 0.0f) {
+        float s = fmaxf((copysignf(hz, T.uz) - T.qz) / T.uz, 0.0f);
+        if (s < sF) { sF = s; face = T.uz > 0.0f ? 5 : 4; }
+    }
+    if (face < 0) { err = STORM_DERR_NO_FACE; return OUT_ERROR; }
+    const double c = C.clight;
+
+    if (C.withRW && C.rwElig[cell]) {
+        // the Random Walk jump in FP64 on the particle's global coordinates
+        const double cx = C.xc[T.i], cy = C.yc[T.j], cz = C.zc[T.k];
+        PartReg p;
+        p.x = cx + static_cast<double>(T.qx); p.y = cy + static_cast<double>(T.qy); p.z = cz + static_cast<double>(T.qz);
+        p.vx = static_cast<double>(T.ux) * c; p.vy = static_cast<double>(T.uy) * c; p.vz = static_cast<double>(T.uz) * c;
+        p.t = T.t; p.w = T.w; p.w0 = T.w0; p.cell = cell;
+        const double4 cp = C.phys[cell];
+        int r = try_random_walk(C, p, rng, tal, cp, C.xe[T.i], C.xe[T.i + 1], C.ye[T.j], C.ye[T.j + 1], C.ze[T.k],
+                                C.ze[T.k + 1], cx, cy, cz);
+        if (r == -2) { err = STORM_DERR_RW_SHRINK; return OUT_ERROR; }
+        if (r >= 0) {
+            usedRW = 1;
+            T.t = p.t; T.w = p.w;
+            T.qx = clampf(static_cast<float>(p.x - cx), hx);
+            T.qy = clampf(static_cast<float>(p.y - cy), hy);
+            T.qz = clampf(static_cast<float>(p.z - cz), hz);
+            const double inv = C.invC;
+            T.ux = static_cast<float>(p.vx * inv); T.uy = static_cast<float>(p.vy * inv); T.uz = static_cast<float>(p.vz * inv);
+            if (r == REMOVE) return OUT_CUTOFF;
+            if (r == DONE) return OUT_CENSUS;
+            return OUT_CONTINUE;
+        }
+    }
+
+    const float4 cp = C.phys32[cell];
+    const float sC = cp.x * (-__logf(to_open_float(rng.open())));
+    const float sL = static_cast<float>(T.t * c);
+    int best = 0;
+    float ds = sF;
+    if (sC < ds) { best = 1; ds = sC; }
+    if (sL < ds) { best = 2; ds = sL; }
+    const double dt = (best == 2) ? T.t : static_cast<double>(ds) * C.invC;
+    T.t -= dt;
+    const float tau = cp.y * ds;
+    const double e1 = static_cast<double>(expm1f(-tau));
+    double integrated = T.w * dt;
+    if (tau >= 1e-12f) integrated = T.w * e1 * C.phys[cell].z;
+    T.qx = clampf(fmaf(T.ux, ds, T.qx), hx);
+    T.qy = clampf(fmaf(T.uy, ds, T.qy), hy);
+    T.qz = clampf(fmaf(T.uz, ds, T.qz), hz);
+    if (!C.noFeedback) tal.mat(cell, -e1 * T.w);
+    tal.rad(cell, integrated);
+    T.w *= 1.0 + e1;
+    if (fabs(T.w) < T.w0 * 1e-3) {
+        if (!C.noFeedback) tal.mat(cell, T.w);
+        return OUT_CUTOFF;
+    }
+    if (best == 2) return OUT_CENSUS;
+    if (best == 1) {
+        (void)rng.open();
+        const float theta = 6.2831853f * to_open_float(rng.raw());
+        const float cosT = 2.0f * static_cast<float>(rng.raw()) - 1.0f;
+        const float sinT = sqrtf(fmaxf(0.0f, 1.0f - cosT * cosT));
+        float st, ct;
+        __sincosf(theta, &st, &ct);
+        T.ux = sinT * ct; T.uy = sinT * st; T.uz = cosT;
+        return OUT_CONTINUE;
+    }
+    // face crossing
+    const int axis = face >> 1, hi = face & 1;
+    bool inside;
+    switch (face) {
+    case 0: inside = T.i > 0; break;
+    case 1: inside = T.i + 1 < C.nx; break;
+    case 2: inside = T.j > 0; break;
+    case 3: inside = T.j + 1 < C.ny; break;
+    case 4: inside = T.k > 0; break;
+    default: inside = T.k + 1 < C.nz; break;
+    }
+    if (inside) {
+        switch (face) {
+        case 0: --T.i; T.cell -= 1; T.qx = C.hx[T.i]; break;
+        case 1: ++T.i; T.cell += 1; T.qx = -C.hx[T.i]; break;
+        case 2: --T.j; T.cell -= C.nx; T.qy = C.hy[T.j]; break;
+        case 3: ++T.j; T.cell += C.nx; T.qy = -C.hy[T.j]; break;
+        case 4: --T.k; T.cell -= C.nx * C.ny; T.qz = C.hz[T.k]; break;
+        default: ++T.k; T.cell += C.nx * C.ny; T.qz = -C.hz[T.k]; break;
+        }
+        return OUT_CONTINUE;
+    }
+    // the box face this cell face lies on (GetBoxFaces order matches the side order)
+    if (C.escapeNoCheck || C.bf[face].action == STORM_FACE_ESCAPE) return OUT_ESCAPE;
+    const float sgn = hi ? 1.0f : -1.0f;
+    if (axis == 0) { T.ux = -T.ux; T.qx = sgn * (hx - fminf(C.reflNudge[face], 0.25f * hx)); }
+    else if (axis == 1) { T.uy = -T.uy; T.qy = sgn * (hy - fminf(C.reflNudge[face], 0.25f * hy)); }
+    else { T.uz = -T.uz; T.qz = sgn * (hz - fminf(C.reflNudge[face], 0.25f * hz)); }
+    return OUT_CONTINUE;
 }
 
 // ------------------------------------------------------------------ boundary

@@ -22,6 +22,7 @@ struct CellArrays {
     uint8_t *rwElig;
     uint64_t *photons;
     double4 *phys;      // per-cell segment constants (cell_phys)
+    float4 *phys32;     // FP32-tracking form: 1/sigma_e, sigma_a f
 };
 
 struct OpacityEos {
@@ -80,7 +81,9 @@ void launch_emit_faces(cudaStream_t s, const Ctx &C, const FaceSources &F, uint6
                        uint32_t bankBase, double dt, DevStats *st);
 void launch_transport(cudaStream_t s, uint32_t grid, const Ctx &C, const Bank &in, const uint32_t *nIn, const Bank &out,
                       uint32_t *nOut, const Bank &cen, uint32_t *nCen, uint32_t K, DevStats *st, int minBlocks);
-int transport_blocks_per_sm(int minBlocks);
+int transport_blocks_per_sm(int minBlocks, bool fp32);
+void launch_bank_to_local(cudaStream_t s, const Ctx &C, const Bank &src, const Bank &dst, uint32_t n);
+void launch_bank_to_global(cudaStream_t s, const Ctx &C, const Bank &src, const Bank &dst, uint32_t n);
 void launch_comb_keys(cudaStream_t s, const Ctx &C, const Bank &cen, uint32_t n, uint64_t *keys, uint32_t *vals,
                       uint32_t combKey);
 int launch_radix_sort(cudaStream_t s, uint64_t *keys, uint32_t *vals, uint64_t *keysAlt, uint32_t *valsAlt, uint32_t n,
@@ -101,8 +104,8 @@ void launch_allocate_checked(cudaStream_t s, const Ctx &C, const CellArrays &A, 
                              uint64_t newPerCell, double rel, int32_t *ambiguous);
 size_t radix_scratch_words(uint32_t n);
 void launch_census_keys_pid(cudaStream_t s, const Bank &cen, uint32_t n, uint64_t *keys, uint32_t *vals);
-void launch_gather(cudaStream_t s, const Bank &src, const uint32_t *idx, uint32_t n, const Bank &dst, double *eradCensus,
-                   DevStats *st);
+void launch_gather(cudaStream_t s, const Ctx &C, const Bank &src, const uint32_t *idx, uint32_t n, const Bank &dst,
+                   double *eradCensus, DevStats *st);
 void launch_poststep(cudaStream_t s, const Ctx &C, const CellArrays &A, const OpacityEos &M, double dt);
 void launch_replay(cudaStream_t s, const Ctx &C, const ReplayDev &R, uint32_t n);
 void launch_rw_radius(cudaStream_t s, const double *tau, const double *surv, double *radius);

@@ -37,6 +37,96 @@ __device__ __forceinline__ void store_part(const Bank &b, uint32_t q, const Part
     b.cell[q] = p.cell; b.pid[q] = pid; b.draw[q] = draw;
 }
 
+// FP32-tracking banks reuse the same buffers: x,y,z hold the cell-local
+// offsets and vx,vy,vz the direction, as floats in the first half of each buffer.
+__device__ __forceinline__ void load32(const Bank &b, uint32_t q, Track32 &T) {
+    T.qx = reinterpret_cast<const float *>(b.x)[q];
+    T.qy = reinterpret_cast<const float *>(b.y)[q];
+    T.qz = reinterpret_cast<const float *>(b.z)[q];
+    T.ux = reinterpret_cast<const float *>(b.vx)[q];
+    T.uy = reinterpret_cast<const float *>(b.vy)[q];
+    T.uz = reinterpret_cast<const float *>(b.vz)[q];
+    T.t = b.t[q]; T.w = b.w[q]; T.w0 = b.w0[q];
+    T.cell = b.cell[q];
+}
+__device__ __forceinline__ void store32(const Bank &b, uint32_t q, const Track32 &T, uint32_t pid, uint32_t draw) {
+    reinterpret_cast<float *>(b.x)[q] = T.qx;
+    reinterpret_cast<float *>(b.y)[q] = T.qy;
+    reinterpret_cast<float *>(b.z)[q] = T.qz;
+    reinterpret_cast<float *>(b.vx)[q] = T.ux;
+    reinterpret_cast<float *>(b.vy)[q] = T.uy;
+    reinterpret_cast<float *>(b.vz)[q] = T.uz;
+    b.t[q] = T.t; b.w[q] = T.w; b.w0[q] = T.w0;
+    b.cell[q] = T.cell; b.pid[q] = pid; b.draw[q] = draw;
+}
+// global FP64 particle -> FP32-tracking particle of its cell
+__device__ __forceinline__ void to_local(const Ctx &C, const PartReg &p, Track32 &T) {
+    cell_ijk(C, p.cell, T.i, T.j, T.k);
+    T.cell = p.cell;
+    T.qx = clampf(static_cast<float>(p.x - C.xc[T.i]), C.hx[T.i]);
+    T.qy = clampf(static_cast<float>(p.y - C.yc[T.j]), C.hy[T.j]);
+    T.qz = clampf(static_cast<float>(p.z - C.zc[T.k]), C.hz[T.k]);
+    const double sp = vnorm(p.vx, p.vy, p.vz);
+    const double inv = sp > 0.0 ? 1.0 / sp : 0.0;
+    T.ux = static_cast<float>(p.vx * inv); T.uy = static_cast<float>(p.vy * inv); T.uz = static_cast<float>(p.vz * inv);
+    T.t = p.t; T.w = p.w; T.w0 = p.w0;
+}
+__device__ __forceinline__ void to_global(const Ctx &C, const Track32 &T, PartReg &p) {
+    uint32_t i, j, k;
+    cell_ijk(C, T.cell, i, j, k);
+    p.x = C.xc[i] + static_cast<double>(T.qx);
+    p.y = C.yc[j] + static_cast<double>(T.qy);
+    p.z = C.zc[k] + static_cast<double>(T.qz);
+    p.vx = static_cast<double>(T.ux) * C.clight;
+    p.vy = static_cast<double>(T.uy) * C.clight;
+    p.vz = static_cast<double>(T.uz) * C.clight;
+    p.t = T.t; p.w = T.w; p.w0 = T.w0; p.cell = T.cell;
+}
+// store an FP64 particle in the bank's layout
+__device__ __forceinline__ void store_any(const Ctx &C, const Bank &b, uint32_t q, const PartReg &p, uint32_t pid,
+                                          uint32_t draw) {
+    if (C.fp32) {
+        Track32 T;
+        to_local(C, p, T);
+        store32(b, q, T, pid, draw);
+    } else {
+        store_part(b, q, p, pid, draw);
+    }
+}
+// copy one particle between banks of the same layout
+__device__ __forceinline__ void copy_any(const Ctx &C, const Bank &src, uint32_t qs, const Bank &dst, uint32_t qd,
+                                         uint32_t pid, uint32_t draw) {
+    if (C.fp32) {
+        Track32 T;
+        load32(src, qs, T);
+        store32(dst, qd, T, pid, draw);
+    } else {
+        PartReg p;
+        load_part(src, qs, p);
+        store_part(dst, qd, p, pid, draw);
+    }
+}
+
+// convert a bank between the FP64 (global) and FP32-tracking (local) layouts
+__global__ void k_bank_to_local(Ctx C, Bank src, Bank dst, uint32_t n) {
+    for (uint32_t q = blockIdx.x * blockDim.x + threadIdx.x; q < n; q += gridDim.x * blockDim.x) {
+        PartReg p;
+        load_part(src, q, p);
+        Track32 T;
+        to_local(C, p, T);
+        store32(dst, q, T, src.pid[q], src.draw[q]);
+    }
+}
+__global__ void k_bank_to_global(Ctx C, Bank src, Bank dst, uint32_t n) {
+    for (uint32_t q = blockIdx.x * blockDim.x + threadIdx.x; q < n; q += gridDim.x * blockDim.x) {
+        Track32 T;
+        load32(src, q, T);
+        PartReg p;
+        to_global(C, T, p);
+        store_part(dst, q, p, src.pid[q], src.draw[q]);
+    }
+}
+
 // ------------------------------------------------------------------ step start
 // manager step() (manager/MonteCarloManagerSerial.hpp:393-405): census particles
 // get timeLeft = dt, initialWeight = |w|; they take pids 0..n-1.
@@ -95,6 +185,11 @@ __global__ void k_prestep(Ctx C, CellArrays A, OpacityEos M, double dt) {
         A.fleck[c] = f;
         if (f < 0.0 || f > 1.0) raise_error(C, STORM_DERR_FLECK, c, 0);
         A.phys[c] = cell_phys(sa, ss, f, sa + ss, C.clight);
+        if (C.fp32) {
+            const double eventOpacity = ss + (1.0 - f) * sa;
+            A.phys32[c] = make_float4(eventOpacity > 0.0 ? static_cast<float>(1.0 / eventOpacity) : CUDART_INF_F,
+                                      static_cast<float>(sa * f), 0.0f, 0.0f);
+        }
         if (C.withRW) {
             double sigmaT = sa + ss;
             A.rwSigT[c] = sigmaT;
@@ -116,6 +211,11 @@ __global__ void k_rw_eligibility(Ctx C, CellArrays A) {
     for (uint32_t c = blockIdx.x * blockDim.x + threadIdx.x; c < C.ncells; c += gridDim.x * blockDim.x) {
         double sigmaT = A.sigA[c] + A.sigS[c];
         A.phys[c] = cell_phys(A.sigA[c], A.sigS[c], A.fleck[c], sigmaT, C.clight);
+        if (C.fp32) {
+            const double eventOpacity = A.sigS[c] + (1.0 - A.fleck[c]) * A.sigA[c];
+            A.phys32[c] = make_float4(eventOpacity > 0.0 ? static_cast<float>(1.0 / eventOpacity) : CUDART_INF_F,
+                                      static_cast<float>(A.sigA[c] * A.fleck[c]), 0.0f, 0.0f);
+        }
         if (!C.withRW) continue;
         A.rwSigT[c] = sigmaT;
         uint32_t i, j, k;
@@ -414,7 +514,7 @@ __global__ void k_emit_cells(Ctx C, CellArrays A, const uint64_t *offsets, uint6
         p.t = dt * rng.open();
         p.w = energyPerPhoton;
         p.w0 = fabs(p.w);
-        store_part(b, bankBase + static_cast<uint32_t>(e), p, bankBase + static_cast<uint32_t>(e), 0);
+        store_any(C, b, bankBase + static_cast<uint32_t>(e), p, bankBase + static_cast<uint32_t>(e), 0);
         esum += p.w;
     }
     esum = warp_sum(esum);
@@ -470,7 +570,7 @@ __global__ void k_emit_faces(Ctx C, FaceSources F, uint64_t total, Bank b, uint3
         repair_outside(C, p.x, p.y, p.z, C.xc[i], C.yc[j], C.zc[k]);
         p.w0 = fabs(p.w);
         const uint32_t slot = bankBase + static_cast<uint32_t>(f);
-        store_part(b, slot, p, slot, 0);
+        store_any(C, b, slot, p, slot, 0);
         esum += p.w;
     }
     esum = warp_sum(esum);
@@ -565,6 +665,78 @@ __global__ void __launch_bounds__(256, MINB) k_transport(Ctx C, Bank in, const u
     }
 }
 
+// The same bank visit in the FP32-tracking form.
+template <int MINB>
+__global__ void __launch_bounds__(256, MINB) k_transport32(Ctx C, Bank in, const uint32_t *nIn, Bank out,
+                                                            uint32_t *nOut, Bank cen, uint32_t *nCen, uint32_t K,
+                                                            DevStats *st) {
+    __shared__ BlockStats bs;
+    if (threadIdx.x == 0) bs = BlockStats{0, 0, 0, 0, 0, 0.0, 0.0, 0.0};
+    __syncthreads();
+    const uint32_t n = *nIn;
+    const unsigned lane = threadIdx.x & 31;
+    for (uint32_t base = blockIdx.x * blockDim.x; base < n; base += gridDim.x * blockDim.x) {
+        const uint32_t idx = base + threadIdx.x;
+        const bool active = idx < n;
+        Track32 T;
+        uint32_t pid = 0, draw = 0;
+        int outcome = OUT_CONTINUE;
+        if (active) {
+            load32(in, idx, T);
+            cell_ijk(C, T.cell, T.i, T.j, T.k);
+            pid = in.pid[idx];
+            draw = in.draw[idx];
+            PhiloxRng rng;
+            rng.init(C.seedLo, C.seedHi, TAG_TRANSPORT, C.step, pid, draw);
+            AtomicTally tal{C.eint, C.eradAvg, 0.0};
+            uint32_t s = 0, rw = 0;
+            for (; s < K;) {
+                if (C.perCellCounters) atomicAdd(C.segs + T.cell, 1u);
+                ++s;
+                const uint32_t cell0 = T.cell;
+                int usedRW = 0, err = 0;
+                outcome = segment32(C, T, rng, tal, usedRW, err);
+                rw += usedRW;
+                if (outcome != OUT_CONTINUE) {
+                    if (outcome == OUT_ERROR) raise_error(C, err ? err : STORM_DERR_NOT_ON_BOUNDARY, cell0, pid);
+                    break;
+                }
+            }
+            draw = rng.draw;
+            atomicAdd(&bs.segments, static_cast<unsigned long long>(s));
+            if (rw) atomicAdd(&bs.rwSteps, static_cast<unsigned long long>(rw));
+            if (tal.depSum != 0.0) atomicAdd(&bs.eDeposited, tal.depSum);
+            if (outcome == OUT_ESCAPE) { atomicAdd(&bs.escaped, 1ull); atomicAdd(&bs.eEscaped, T.w); }
+            else if (outcome == OUT_CUTOFF) { atomicAdd(&bs.cutoff, 1ull); }
+            else if (outcome == OUT_CENSUS) { atomicAdd(&bs.census, 1ull); atomicAdd(&bs.eCensusPre, T.w); }
+        }
+        const bool keep = active && outcome == OUT_CONTINUE;
+        const bool cens = active && outcome == OUT_CENSUS;
+        const unsigned mK = __ballot_sync(FULL, keep), mC = __ballot_sync(FULL, cens);
+        uint32_t bK = 0, bC = 0;
+        if (lane == 0) {
+            if (mK) bK = atomicAdd(nOut, __popc(mK));
+            if (mC) bC = atomicAdd(nCen, __popc(mC));
+        }
+        bK = __shfl_sync(FULL, bK, 0);
+        bC = __shfl_sync(FULL, bC, 0);
+        const unsigned lt = lanemask_lt();
+        if (keep) store32(out, bK + __popc(mK & lt), T, pid, draw);
+        if (cens) store32(cen, bC + __popc(mC & lt), T, pid, draw);
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        if (bs.segments) atomicAdd(&st->segments, bs.segments);
+        if (bs.rwSteps) atomicAdd(&st->rwSteps, bs.rwSteps);
+        if (bs.escaped) atomicAdd(&st->escaped, bs.escaped);
+        if (bs.cutoff) atomicAdd(&st->cutoff, bs.cutoff);
+        if (bs.census) atomicAdd(&st->census, bs.census);
+        if (bs.eDeposited != 0.0) atomicAdd(&st->eDeposited, bs.eDeposited);
+        if (bs.eEscaped != 0.0) atomicAdd(&st->eEscaped, bs.eEscaped);
+        if (bs.eCensusPre != 0.0) atomicAdd(&st->eCensusPre, bs.eCensusPre);
+    }
+}
+
 // ------------------------------------------------------------------ comb
 // CombPopulationControl::activate (population/CombPopulationControl.hpp:79-253).
 // Sort key = (cell << 32) | bijective hash of the particle's pid: a pseudo-random
@@ -577,10 +749,11 @@ __device__ __forceinline__ uint32_t fmix32(uint32_t h) {
 }
 __global__ void k_comb_keys(Ctx C, Bank cen, uint32_t n, uint64_t *keys, uint32_t *vals, uint32_t combKey) {
     for (uint32_t q = blockIdx.x * blockDim.x + threadIdx.x; q < n; q += gridDim.x * blockDim.x) {
-        const double x = cen.x[q], y = cen.y[q], z = cen.z[q], w = cen.w[q];
+        const double w = cen.w[q];
         const uint32_t pid = cen.pid[q];
         uint32_t cell = cen.cell[q];
-        if (outside_box(C, x, y, z)) raise_error(C, STORM_DERR_COMB_OUTSIDE, cell, pid);
+        // FP32-tracking particles are inside their cell by construction
+        if (!C.fp32 && outside_box(C, cen.x[q], cen.y[q], cen.z[q])) raise_error(C, STORM_DERR_COMB_OUTSIDE, cell, pid);
         const bool badWeight = !isfinite(w) || w < 0.0;
         if (badWeight) raise_error(C, STORM_DERR_COMB_WEIGHT, cell, pid);
         // zero, negative and non-finite weights never reach the per-cell loops
@@ -813,6 +986,15 @@ __global__ void k_comb_emit(Ctx C, Bank cen, const uint32_t *idx, const uint64_t
         const uint32_t m = raw & ~KEEP;
         if (m == 0) continue;
         const uint32_t c = static_cast<uint32_t>(sortedKeys[q] >> 32);
+        if (C.fp32) {
+            Track32 T;
+            load32(cen, idx[q], T);
+            if (!(raw & KEEP)) { T.w = pWeight[q]; T.w0 = T.w; T.t = 0; }
+            T.cell = c;
+            const uint64_t o = pOffset[q];
+            for (uint32_t k = 0; k < m; ++k) store32(out, static_cast<uint32_t>(o + k), T, static_cast<uint32_t>(o + k), 0);
+            continue;
+        }
         PartReg p;
         load_part(cen, idx[q], p);
         if (!(raw & KEEP)) { p.w = pWeight[q]; p.w0 = p.w; p.t = 0; }
@@ -846,14 +1028,14 @@ __global__ void k_census_keys_pid(Bank cen, uint32_t n, uint64_t *keys, uint32_t
         vals[q] = q;
     }
 }
-__global__ void k_gather(Bank src, const uint32_t *idx, uint32_t n, Bank dst, double *eradCensus, DevStats *st) {
+__global__ void k_gather(Ctx C, Bank src, const uint32_t *idx, uint32_t n, Bank dst, double *eradCensus, DevStats *st) {
     double e = 0.0;
     for (uint32_t q = blockIdx.x * blockDim.x + threadIdx.x; q < n; q += gridDim.x * blockDim.x) {
-        PartReg p;
-        load_part(src, idx[q], p);
-        store_part(dst, q, p, q, 0);
-        atomicAdd(eradCensus + p.cell, p.w);
-        e += p.w;
+        const uint32_t sq = idx[q];
+        copy_any(C, src, sq, dst, q, q, 0);
+        const double w = src.w[sq];
+        atomicAdd(eradCensus + src.cell[sq], w);
+        e += w;
     }
     e = warp_sum(e);
     if ((threadIdx.x & 31) == 0 && e != 0.0) atomicAdd(&st->eCensusOut, e);
@@ -1037,6 +1219,15 @@ void launch_emit_faces(cudaStream_t s, const Ctx &C, const FaceSources &F, uint6
 }
 void launch_transport(cudaStream_t s, uint32_t grid, const Ctx &C, const Bank &in, const uint32_t *nIn, const Bank &out,
                       uint32_t *nOut, const Bank &cen, uint32_t *nCen, uint32_t K, DevStats *st, int minBlocks) {
+    if (C.fp32) {
+        switch (minBlocks) {
+        case 3: k_transport32<3><<<grid, 256, 0, s>>>(C, in, nIn, out, nOut, cen, nCen, K, st); break;
+        case 4: k_transport32<4><<<grid, 256, 0, s>>>(C, in, nIn, out, nOut, cen, nCen, K, st); break;
+        case 2: k_transport32<2><<<grid, 256, 0, s>>>(C, in, nIn, out, nOut, cen, nCen, K, st); break;
+        default: k_transport32<1><<<grid, 256, 0, s>>>(C, in, nIn, out, nOut, cen, nCen, K, st); break;
+        }
+        return;
+    }
     switch (minBlocks) {
     case 3: k_transport<3><<<grid, 256, 0, s>>>(C, in, nIn, out, nOut, cen, nCen, K, st); break;
     case 4: k_transport<4><<<grid, 256, 0, s>>>(C, in, nIn, out, nOut, cen, nCen, K, st); break;
@@ -1044,8 +1235,17 @@ void launch_transport(cudaStream_t s, uint32_t grid, const Ctx &C, const Bank &i
     default: k_transport<1><<<grid, 256, 0, s>>>(C, in, nIn, out, nOut, cen, nCen, K, st); break;
     }
 }
-int transport_blocks_per_sm(int minBlocks) {
+int transport_blocks_per_sm(int minBlocks, bool fp32) {
     int nb = 0;
+    if (fp32) {
+        switch (minBlocks) {
+        case 3: cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_transport32<3>, 256, 0); break;
+        case 4: cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_transport32<4>, 256, 0); break;
+        case 2: cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_transport32<2>, 256, 0); break;
+        default: cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_transport32<1>, 256, 0); break;
+        }
+        return nb;
+    }
     switch (minBlocks) {
     case 3: cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_transport<3>, 256, 0); break;
     case 4: cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_transport<4>, 256, 0); break;
@@ -1115,9 +1315,15 @@ void launch_mask_count(cudaStream_t s, const uint32_t *pCount, uint32_t n, uint6
 void launch_census_keys_pid(cudaStream_t s, const Bank &cen, uint32_t n, uint64_t *keys, uint32_t *vals) {
     k_census_keys_pid<<<grid_for(n, 256, 8192), 256, 0, s>>>(cen, n, keys, vals);
 }
-void launch_gather(cudaStream_t s, const Bank &src, const uint32_t *idx, uint32_t n, const Bank &dst, double *eradCensus,
-                   DevStats *st) {
-    k_gather<<<grid_for(n, 256, 8192), 256, 0, s>>>(src, idx, n, dst, eradCensus, st);
+void launch_gather(cudaStream_t s, const Ctx &C, const Bank &src, const uint32_t *idx, uint32_t n, const Bank &dst,
+                   double *eradCensus, DevStats *st) {
+    k_gather<<<grid_for(n, 256, 8192), 256, 0, s>>>(C, src, idx, n, dst, eradCensus, st);
+}
+void launch_bank_to_local(cudaStream_t s, const Ctx &C, const Bank &src, const Bank &dst, uint32_t n) {
+    if (n) k_bank_to_local<<<grid_for(n, 256, 8192), 256, 0, s>>>(C, src, dst, n);
+}
+void launch_bank_to_global(cudaStream_t s, const Ctx &C, const Bank &src, const Bank &dst, uint32_t n) {
+    if (n) k_bank_to_global<<<grid_for(n, 256, 8192), 256, 0, s>>>(C, src, dst, n);
 }
 void launch_poststep(cudaStream_t s, const Ctx &C, const CellArrays &A, const OpacityEos &M, double dt) {
     k_poststep<<<grid_for(C.ncells, 256, 8192), 256, 0, s>>>(C, A, M, dt);

@@ -39,6 +39,8 @@ struct StormHandle {
     std::vector<double> hxe, hye, hze, hxc, hyc, hzc;
     // device mesh + cells
     double *xe = nullptr, *ye = nullptr, *ze = nullptr, *xc = nullptr, *yc = nullptr, *zc = nullptr;
+    float *hx = nullptr, *hy = nullptr, *hz = nullptr;   // FP32-tracking half widths
+    bool fp32 = false;
     CellArrays A{};
     double *tabA = nullptr, *tabS = nullptr, *rhoF = nullptr;
     uint32_t *segs = nullptr;
@@ -239,6 +241,7 @@ void box_faces(StormHandle *h) {
         F.valid = (nn > 0.0) && std::isfinite(nn) && (fs > 0.0) && std::isfinite(fs);
         F.thresh = 1e-12 * fs * fs * fs;
         F.nudge = 1e-6 * fs;
+        h->C.reflNudge[f] = static_cast<float>(F.nudge);
         double inv = 1.0 / nn;
         double n[3] = {F.raw[0] * inv, F.raw[1] * inv, F.raw[2] * inv};
         double tc = n[0] * (bc[0] - F.on[0]) + n[1] * (bc[1] - F.on[1]) + n[2] * (bc[2] - F.on[2]);
@@ -392,7 +395,7 @@ int storm_cuda_create(const StormProblemDesc *d, StormHandle **out) {
     if (d->opacity_kind != STORM_OPACITY_CELL_TABLE && d->opacity_kind != STORM_OPACITY_POWER_LAW)
         return STORM_ERR_UNSUPPORTED;
     if (d->eos_kind != STORM_EOS_LINEAR && d->eos_kind != STORM_EOS_POWER_LAW) return STORM_ERR_UNSUPPORTED;
-    if (d->precision != STORM_PRECISION_FP64) return STORM_ERR_UNSUPPORTED;
+    if (d->precision != STORM_PRECISION_FP64 && d->precision != STORM_PRECISION_FP32_TRACK) return STORM_ERR_UNSUPPORTED;
     uint64_t N64 = static_cast<uint64_t>(d->nx) * d->ny * d->nz;
     if (N64 >= 0x7fffffffull) return STORM_ERR_INVALID_ARG;
     for (int a = 0; a < 3; ++a) {
@@ -436,6 +439,15 @@ int storm_cuda_create(const StormProblemDesc *d, StormHandle **out) {
     ALLOC(h->xc, d->nx); ALLOC(h->yc, d->ny); ALLOC(h->zc, d->nz);
     H2D(h->xe, h->hxe.data(), d->nx + 1); H2D(h->ye, h->hye.data(), d->ny + 1); H2D(h->ze, h->hze.data(), d->nz + 1);
     H2D(h->xc, h->hxc.data(), d->nx); H2D(h->yc, h->hyc.data(), d->ny); H2D(h->zc, h->hzc.data(), d->nz);
+    h->fp32 = d->precision == STORM_PRECISION_FP32_TRACK;
+    {
+        std::vector<float> fx(d->nx), fy(d->ny), fz(d->nz);
+        for (uint32_t i = 0; i < d->nx; ++i) fx[i] = static_cast<float>(0.5 * (h->hxe[i + 1] - h->hxe[i]));
+        for (uint32_t j = 0; j < d->ny; ++j) fy[j] = static_cast<float>(0.5 * (h->hye[j + 1] - h->hye[j]));
+        for (uint32_t k = 0; k < d->nz; ++k) fz[k] = static_cast<float>(0.5 * (h->hze[k + 1] - h->hze[k]));
+        ALLOC(h->hx, d->nx); ALLOC(h->hy, d->ny); ALLOC(h->hz, d->nz);
+        H2D(h->hx, fx.data(), d->nx); H2D(h->hy, fy.data(), d->ny); H2D(h->hz, fz.data(), d->nz);
+    }
 
     CellArrays &A = h->A;
     double **cd[] = {&A.T, &A.mass, &A.vol, &A.eint, &A.ceint, &A.sigA, &A.sigS, &A.fleck, &A.rwSigT, &A.eradAvg,
@@ -444,6 +456,7 @@ int storm_cuda_create(const StormProblemDesc *d, StormHandle **out) {
     ALLOC(A.rwElig, N);
     ALLOC(A.photons, N);
     ALLOC(A.phys, N);
+    ALLOC(A.phys32, N);
     ALLOC(h->segs, N);
     std::vector<double> vol(N);
     for (uint32_t c = 0; c < N; ++c) {
@@ -501,7 +514,7 @@ int storm_cuda_create(const StormProblemDesc *d, StormHandle **out) {
     {
         cudaDeviceProp prop{};
         cudaGetDeviceProperties(&prop, h->device);
-        int nb = transport_blocks_per_sm(h->minBlocks);
+        int nb = transport_blocks_per_sm(h->minBlocks, h->fp32);
         h->transportGrid = static_cast<uint32_t>(prop.multiProcessorCount) * static_cast<uint32_t>(nb > 0 ? nb : 1) * 4;
         h->smCount = prop.multiProcessorCount;
     }
@@ -524,6 +537,10 @@ int storm_cuda_create(const StormProblemDesc *d, StormHandle **out) {
     C.seedHi = static_cast<uint32_t>(d->seed >> 32);
     C.step = 0;
     C.phys = A.phys;
+    C.phys32 = A.phys32;
+    C.fp32 = h->fp32 ? 1 : 0;
+    C.hx = h->hx; C.hy = h->hy; C.hz = h->hz;
+    C.invC = 1.0 / d->clight;
     C.sigA = A.sigA; C.sigS = A.sigS; C.fleck = A.fleck; C.rwSigT = A.rwSigT; C.rwElig = A.rwElig;
     C.eint = A.eint; C.eradAvg = A.eradAvg; C.segs = h->segs;
     C.err = h->dErr;
@@ -552,7 +569,7 @@ int storm_cuda_destroy(StormHandle *h) {
     free_rest(h, h->cap);
     void *ps[] = {h->xe, h->ye, h->ze, h->xc, h->yc, h->zc, h->A.T, h->A.mass, h->A.vol, h->A.eint, h->A.ceint,
                   h->A.sigA, h->A.sigS, h->A.fleck, h->A.rwSigT, h->A.eradAvg, h->A.eradCensus, h->A.emitE,
-                  h->A.rwElig, h->A.photons, h->A.phys, h->segs, h->tabA, h->tabS, h->rhoF, h->rwTau, h->rwLogTau, h->rwSurv,
+                  h->A.rwElig, h->A.photons, h->A.phys, h->A.phys32, h->hx, h->hy, h->hz, h->segs, h->tabA, h->tabS, h->rhoF, h->rwTau, h->rwLogTau, h->rwSurv,
                   h->rwRadius, h->fsCell, h->fsSide, h->fsOffset, h->dAmbiguous, h->offsets, h->tileSums, h->dTotalU64, h->dTotalE, h->combW, h->combWtot,
                   h->combStart, h->combCount, h->counts, h->dStats, h->dErr};
     for (void *p : ps)
@@ -733,7 +750,7 @@ int storm_cuda_phase_comb(StormHandle *h) {
         launch_census_keys_pid(h->stream, h->bankC, n, h->keys, h->vals);
         int alt = launch_radix_sort(h->stream, h->keys, h->vals, h->keysAlt, h->valsAlt, n, 32, h->tileHist);
         const uint32_t *idx = alt ? h->valsAlt : h->vals;
-        launch_gather(h->stream, h->bankC, idx, n, h->bankA, h->A.eradCensus, h->dStats);
+        launch_gather(h->stream, h->C, h->bankC, idx, n, h->bankA, h->A.eradCensus, h->dStats);
         h->launches += 2 + 3 * 4;
         CK(cudaGetLastError());
         h->nCensus = n;
@@ -867,19 +884,25 @@ int storm_cuda_set_census(StormHandle *h, const StormParticlesSoA *in) {
     const uint64_t n = in->count;
     int rc = ensure_capacity(h, n, 0);
     if (rc != STORM_OK) return rc;
+    const Bank &stage = h->fp32 ? h->bankB : h->bankA;   // FP32 form: stage FP64, then convert
     const double *sd[] = {in->x, in->y, in->z, in->vx, in->vy, in->vz, in->time_left, in->weight, in->initial_weight};
-    double *dd[] = {h->bankA.x, h->bankA.y, h->bankA.z, h->bankA.vx, h->bankA.vy, h->bankA.vz, h->bankA.t, h->bankA.w,
-                    h->bankA.w0};
+    double *dd[] = {stage.x, stage.y, stage.z, stage.vx, stage.vy, stage.vz, stage.t, stage.w, stage.w0};
+    if (n) {
+        if (!in->cell) return STORM_ERR_INVALID_ARG;
+        for (uint64_t q = 0; q < n; ++q)
+            if (in->cell[q] >= h->N) return STORM_ERR_INVALID_ARG;
+    }
     for (int q = 0; q < 9; ++q) {
         if (!sd[q] && n) return STORM_ERR_INVALID_ARG;
         if (n) CK(cudaMemcpyAsync(dd[q], sd[q], n * sizeof(double), cudaMemcpyHostToDevice, h->stream));
     }
     if (n) {
-        if (!in->cell) return STORM_ERR_INVALID_ARG;
-        std::vector<uint32_t> cells(in->cell, in->cell + n);
-        for (uint32_t c : cells)
-            if (c >= h->N) return STORM_ERR_INVALID_ARG;
-        CK(cudaMemcpyAsync(h->bankA.cell, in->cell, n * sizeof(uint32_t), cudaMemcpyHostToDevice, h->stream));
+        CK(cudaMemcpyAsync(stage.cell, in->cell, n * sizeof(uint32_t), cudaMemcpyHostToDevice, h->stream));
+        if (h->fp32) {
+            launch_bank_to_local(h->stream, h->C, h->bankB, h->bankA, static_cast<uint32_t>(n));
+            ++h->launches;
+            CK(cudaGetLastError());
+        }
         CK(cudaStreamSynchronize(h->stream));
     }
     h->nCensus = n;
@@ -892,9 +915,9 @@ int storm_cuda_population_control(StormHandle *h, const StormParticlesSoA *in) {
     const uint64_t n = in->count;
     int rc = ensure_capacity(h, n, 0);
     if (rc != STORM_OK) return rc;
+    const Bank &stage = h->fp32 ? h->bankB : h->bankC;
     const double *sd[] = {in->x, in->y, in->z, in->vx, in->vy, in->vz, in->time_left, in->weight, in->initial_weight};
-    double *dd[] = {h->bankC.x, h->bankC.y, h->bankC.z, h->bankC.vx, h->bankC.vy, h->bankC.vz, h->bankC.t, h->bankC.w,
-                    h->bankC.w0};
+    double *dd[] = {stage.x, stage.y, stage.z, stage.vx, stage.vy, stage.vz, stage.t, stage.w, stage.w0};
     if (n) {
         for (int q = 0; q < 9; ++q) {
             if (!sd[q]) return STORM_ERR_INVALID_ARG;
@@ -905,8 +928,14 @@ int storm_cuda_population_control(StormHandle *h, const StormParticlesSoA *in) {
             if (in->cell[q] >= h->N) return STORM_ERR_INVALID_ARG;
         std::vector<uint32_t> pid(n);
         for (uint64_t q = 0; q < n; ++q) pid[q] = static_cast<uint32_t>(q);
-        CK(cudaMemcpyAsync(h->bankC.cell, in->cell, n * sizeof(uint32_t), cudaMemcpyHostToDevice, h->stream));
-        CK(cudaMemcpyAsync(h->bankC.pid, pid.data(), n * sizeof(uint32_t), cudaMemcpyHostToDevice, h->stream));
+        CK(cudaMemcpyAsync(stage.cell, in->cell, n * sizeof(uint32_t), cudaMemcpyHostToDevice, h->stream));
+        CK(cudaMemcpyAsync(stage.pid, pid.data(), n * sizeof(uint32_t), cudaMemcpyHostToDevice, h->stream));
+        CK(cudaMemsetAsync(stage.draw, 0, n * sizeof(uint32_t), h->stream));
+        if (h->fp32) {
+            launch_bank_to_local(h->stream, h->C, h->bankB, h->bankC, static_cast<uint32_t>(n));
+            ++h->launches;
+            CK(cudaGetLastError());
+        }
         CK(cudaStreamSynchronize(h->stream));
     }
     CK(cudaMemsetAsync(h->dStats, 0, sizeof(DevStats), h->stream));
@@ -927,12 +956,17 @@ int storm_cuda_get_census(StormHandle *h, StormParticlesSoA *out, uint64_t capac
     CK(cudaSetDevice(h->device));
     const uint64_t n = std::min<uint64_t>(h->nCensus, capacity);
     if (count) *count = h->nCensus;
-    const double *sd[] = {h->bankA.x, h->bankA.y, h->bankA.z, h->bankA.vx, h->bankA.vy, h->bankA.vz, h->bankA.t,
-                          h->bankA.w, h->bankA.w0};
+    if (h->fp32 && n) {
+        launch_bank_to_global(h->stream, h->C, h->bankA, h->bankB, static_cast<uint32_t>(n));
+        ++h->launches;
+        CK(cudaGetLastError());
+    }
+    const Bank &src = h->fp32 ? h->bankB : h->bankA;
+    const double *sd[] = {src.x, src.y, src.z, src.vx, src.vy, src.vz, src.t, src.w, src.w0};
     double *dd[] = {out->x, out->y, out->z, out->vx, out->vy, out->vz, out->time_left, out->weight, out->initial_weight};
     for (int q = 0; q < 9; ++q)
         if (dd[q] && n) CK(cudaMemcpyAsync(dd[q], sd[q], n * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
-    if (out->cell && n) CK(cudaMemcpyAsync(out->cell, h->bankA.cell, n * sizeof(uint32_t), cudaMemcpyDeviceToHost, h->stream));
+    if (out->cell && n) CK(cudaMemcpyAsync(out->cell, src.cell, n * sizeof(uint32_t), cudaMemcpyDeviceToHost, h->stream));
     CK(cudaStreamSynchronize(h->stream));
     if (out->id)
         for (uint64_t q = 0; q < n; ++q) out->id[q] = q;
@@ -1146,7 +1180,7 @@ int storm_cuda_transport_timing(StormHandle *h, double *ms, uint64_t *launches, 
 int storm_cuda_set_transport_variant(StormHandle *h, int min_blocks_per_sm, int waves) {
     if (!h || min_blocks_per_sm < 1 || min_blocks_per_sm > 4 || waves < 1 || waves > 64) return STORM_ERR_INVALID_ARG;
     h->minBlocks = min_blocks_per_sm;
-    int nb = transport_blocks_per_sm(h->minBlocks);
+    int nb = transport_blocks_per_sm(h->minBlocks, h->fp32);
     h->transportGrid = static_cast<uint32_t>(h->smCount) * static_cast<uint32_t>(nb > 0 ? nb : 1) * waves;
     return STORM_OK;
 }
