@@ -49,6 +49,8 @@ def parse():
     ap.add_argument("--segments-per-visit", type=int, default=0)
     ap.add_argument("--min-blocks", type=int, default=0, help="transport occupancy variant (1-4)")
     ap.add_argument("--waves", type=int, default=4)
+    ap.add_argument("--refill", type=int, default=-1, help="1 persistent refill kernel, 0 bank visits")
+    ap.add_argument("--burst", type=int, default=4)
     return ap.parse_args()
 
 
@@ -231,6 +233,8 @@ def run_form(args, precision, seed, local, dist, timed=True):
         eng.set_segments_per_visit(args.segments_per_visit)
     if args.min_blocks:
         eng.set_transport_variant(args.min_blocks, args.waves)
+    if args.refill >= 0:
+        eng.set_transport_mode(bool(args.refill), args.burst)
     eng.set_profiling(True)
     for _ in range(args.warmup):
         eng.step()
@@ -323,7 +327,6 @@ def run_storm(args, ws, rank, local, dist):
     f32 = run_form(args, A.PRECISION_FP32_TRACK, seed, local, dist)
     f64 = run_form(args, A.PRECISION_FP64, seed, local, dist)
     ck = clocks.stop()
-    e2e = e2e_run(args, f32["engine"], f32["problem"], dist) if args.e2e_steps > 0 else None
 
     def rate(res):
         ms = reduce(dist, sum(res["step_ms"]), "max", "storm")
@@ -346,6 +349,7 @@ def run_storm(args, ws, rank, local, dist):
                "max_abs_fp32_minus_fp64_over_sigma": float(np.max(np.abs(T32 - T64)[hot]) / sigma),
                "sigma_estimate": "rms difference of two FP64 seeds / sqrt(2), hot cells", "cells": int(hot.sum())}
         other["engine"].close()
+    e2e = e2e_run(args, f32["engine"], f32["problem"], dist) if args.e2e_steps > 0 else None
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline(args.n, 1)

@@ -92,6 +92,12 @@ class Particles:
         self.n = n
 
     def soa(self):
+        """Struct of pointers; every field is made contiguous first (the C side
+        reads plain arrays)."""
+        for f in self.FIELDS:
+            setattr(self, f, np.ascontiguousarray(getattr(self, f), dtype=np.float64))
+        self.cell = np.ascontiguousarray(self.cell, dtype=np.uint32)
+        self.id = np.ascontiguousarray(self.id, dtype=np.uint64)
         s = A.StormParticlesSoA()
         for f in self.FIELDS:
             setattr(s, f, A.ptr(getattr(self, f)))

@@ -82,6 +82,10 @@ void launch_emit_faces(cudaStream_t s, const Ctx &C, const FaceSources &F, uint6
 void launch_transport(cudaStream_t s, uint32_t grid, const Ctx &C, const Bank &in, const uint32_t *nIn, const Bank &out,
                       uint32_t *nOut, const Bank &cen, uint32_t *nCen, uint32_t K, DevStats *st, int minBlocks);
 int transport_blocks_per_sm(int minBlocks, bool fp32);
+void launch_transport_refill(cudaStream_t s, uint32_t grid, int minBlocks, const Ctx &C, const Bank &in, uint32_t n,
+                             uint32_t *nextIdx, const Bank &cen, uint32_t *nCen, uint32_t burst, uint32_t maxSegs,
+                             DevStats *st);
+int refill_blocks_per_sm(int minBlocks, bool fp32);
 void launch_bank_to_local(cudaStream_t s, const Ctx &C, const Bank &src, const Bank &dst, uint32_t n);
 void launch_bank_to_global(cudaStream_t s, const Ctx &C, const Bank &src, const Bank &dst, uint32_t n);
 void launch_comb_keys(cudaStream_t s, const Ctx &C, const Bank &cen, uint32_t n, uint64_t *keys, uint32_t *vals,

@@ -737,6 +737,140 @@ __global__ void __launch_bounds__(256, MINB) k_transport32(Ctx C, Bank in, const
     }
 }
 
+// ------------------------------------------------------------------ persistent transport
+// Both forms behind one interface for the persistent kernel.
+struct Form64 {
+    using T = Track;
+    static __device__ __forceinline__ void load(const Ctx &C, const Bank &b, uint32_t q, T &t) {
+        load_part(b, q, t.p);
+        track_begin(C, t);
+    }
+    static __device__ __forceinline__ void store(const Bank &b, uint32_t q, const T &t, uint32_t pid, uint32_t draw) {
+        store_part(b, q, t.p, pid, draw);
+    }
+    template <class RNG, class TALLY>
+    static __device__ __forceinline__ int seg(const Ctx &C, T &t, RNG &rng, TALLY &tal, int &usedRW, int &err) {
+        PhysOut o = physics_step(C, t, rng, tal);
+        if (o.errCode) { err = o.errCode; return OUT_ERROR; }
+        usedRW = o.usedRW;
+        int m = manager_handle(C, t, o);
+        if (m == OUT_ERROR) err = STORM_DERR_NOT_ON_BOUNDARY;
+        return m;
+    }
+    static __device__ __forceinline__ uint32_t cell(const T &t) { return t.p.cell; }
+    static __device__ __forceinline__ double weight(const T &t) { return t.p.w; }
+};
+struct Form32 {
+    using T = Track32;
+    static __device__ __forceinline__ void load(const Ctx &C, const Bank &b, uint32_t q, T &t) {
+        load32(b, q, t);
+        cell_ijk(C, t.cell, t.i, t.j, t.k);
+    }
+    static __device__ __forceinline__ void store(const Bank &b, uint32_t q, const T &t, uint32_t pid, uint32_t draw) {
+        store32(b, q, t, pid, draw);
+    }
+    template <class RNG, class TALLY>
+    static __device__ __forceinline__ int seg(const Ctx &C, T &t, RNG &rng, TALLY &tal, int &usedRW, int &err) {
+        int m = segment32(C, t, rng, tal, usedRW, err);
+        if (m == OUT_ERROR && !err) err = STORM_DERR_NOT_ON_BOUNDARY;
+        return m;
+    }
+    static __device__ __forceinline__ uint32_t cell(const T &t) { return t.cell; }
+    static __device__ __forceinline__ double weight(const T &t) { return t.w; }
+};
+
+// The whole HandleAll loop in one launch.  Every lane holds one history; a lane
+// whose particle reaches census, escapes or is cut off writes it out and takes
+// the next unstarted particle (one atomic per warp for the lanes that need
+// one), so lanes do not idle behind the longest history of their warp.  A
+// history longer than maxSegs raises STORM_DERR_HISTORY_CAP and stops.
+template <class F, int MINB>
+__global__ void __launch_bounds__(256, MINB) k_transport_refill(Ctx C, Bank in, uint32_t n, uint32_t *nextIdx, Bank cen,
+                                                                 uint32_t *nCen, uint32_t burst, uint32_t maxSegs,
+                                                                 DevStats *st) {
+    __shared__ BlockStats bs;
+    if (threadIdx.x == 0) bs = BlockStats{0, 0, 0, 0, 0, 0.0, 0.0, 0.0};
+    __syncthreads();
+    const unsigned lane = threadIdx.x & 31;
+    const unsigned lt = lanemask_lt();
+    typename F::T t;
+    PhiloxRng rng;
+    uint32_t pid = 0, segsThis = 0;
+    bool has = false;
+    bool exhausted = false;   // warp-uniform: the counter has passed n, stop adding to it
+    double dep = 0.0;
+    unsigned long long segs = 0, rws = 0;
+    for (;;) {
+        // refill the empty lanes from the unstarted particles
+        const unsigned need = exhausted ? 0u : __ballot_sync(FULL, !has);
+        if (need) {
+            uint32_t base = 0;
+            if (lane == static_cast<unsigned>(__ffs(need) - 1)) base = atomicAdd(nextIdx, __popc(need));
+            base = __shfl_sync(FULL, base, __ffs(need) - 1);
+            if (base + __popc(need) >= n) exhausted = true;
+            if (!has) {
+                const uint32_t q = base + __popc(need & lt);
+                if (q < n) {
+                    F::load(C, in, q, t);
+                    pid = in.pid[q];
+                    rng.init(C.seedLo, C.seedHi, TAG_TRANSPORT, C.step, pid, in.draw[q]);
+                    segsThis = 0;
+                    has = true;
+                }
+            }
+        }
+        if (!__any_sync(FULL, has)) break;
+        int outcome = OUT_CONTINUE;
+        if (has) {
+            AtomicTally tal{C.eint, C.eradAvg, 0.0};
+            for (uint32_t b = 0; b < burst; ++b) {
+                const uint32_t cell0 = F::cell(t);
+                if (C.perCellCounters) atomicAdd(C.segs + cell0, 1u);
+                ++segs;
+                int usedRW = 0, err = 0;
+                outcome = F::seg(C, t, rng, tal, usedRW, err);
+                rws += usedRW;
+                if (outcome != OUT_CONTINUE) {
+                    if (outcome == OUT_ERROR) raise_error(C, err, cell0, pid);
+                    break;
+                }
+                if (++segsThis >= maxSegs) {
+                    raise_error(C, STORM_DERR_HISTORY_CAP, cell0, pid);
+                    outcome = OUT_ERROR;
+                    break;
+                }
+            }
+            dep += tal.depSum;
+            if (outcome == OUT_ESCAPE) { atomicAdd(&bs.escaped, 1ull); atomicAdd(&bs.eEscaped, F::weight(t)); }
+            else if (outcome == OUT_CUTOFF) { atomicAdd(&bs.cutoff, 1ull); }
+            else if (outcome == OUT_CENSUS) { atomicAdd(&bs.census, 1ull); atomicAdd(&bs.eCensusPre, F::weight(t)); }
+        }
+        const bool cens = has && outcome == OUT_CENSUS;
+        const unsigned mC = __ballot_sync(FULL, cens);
+        if (mC) {
+            uint32_t bC = 0;
+            if (lane == static_cast<unsigned>(__ffs(mC) - 1)) bC = atomicAdd(nCen, __popc(mC));
+            bC = __shfl_sync(FULL, bC, __ffs(mC) - 1);
+            if (cens) F::store(cen, bC + __popc(mC & lt), t, pid, rng.draw);
+        }
+        if (has && outcome != OUT_CONTINUE) has = false;
+    }
+    atomicAdd(&bs.segments, segs);
+    if (rws) atomicAdd(&bs.rwSteps, rws);
+    if (dep != 0.0) atomicAdd(&bs.eDeposited, dep);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        if (bs.segments) atomicAdd(&st->segments, bs.segments);
+        if (bs.rwSteps) atomicAdd(&st->rwSteps, bs.rwSteps);
+        if (bs.escaped) atomicAdd(&st->escaped, bs.escaped);
+        if (bs.cutoff) atomicAdd(&st->cutoff, bs.cutoff);
+        if (bs.census) atomicAdd(&st->census, bs.census);
+        if (bs.eDeposited != 0.0) atomicAdd(&st->eDeposited, bs.eDeposited);
+        if (bs.eEscaped != 0.0) atomicAdd(&st->eEscaped, bs.eEscaped);
+        if (bs.eCensusPre != 0.0) atomicAdd(&st->eCensusPre, bs.eCensusPre);
+    }
+}
+
 // ------------------------------------------------------------------ comb
 // CombPopulationControl::activate (population/CombPopulationControl.hpp:79-253).
 // Sort key = (cell << 32) | bijective hash of the particle's pid: a pseudo-random
@@ -1319,6 +1453,36 @@ void launch_gather(cudaStream_t s, const Ctx &C, const Bank &src, const uint32_t
                    double *eradCensus, DevStats *st) {
     k_gather<<<grid_for(n, 256, 8192), 256, 0, s>>>(C, src, idx, n, dst, eradCensus, st);
 }
+template <class F>
+static void refill_launch(cudaStream_t s, uint32_t grid, int minBlocks, const Ctx &C, const Bank &in, uint32_t n,
+                          uint32_t *nextIdx, const Bank &cen, uint32_t *nCen, uint32_t burst, uint32_t maxSegs,
+                          DevStats *st) {
+    switch (minBlocks) {
+    case 4: k_transport_refill<F, 4><<<grid, 256, 0, s>>>(C, in, n, nextIdx, cen, nCen, burst, maxSegs, st); break;
+    case 3: k_transport_refill<F, 3><<<grid, 256, 0, s>>>(C, in, n, nextIdx, cen, nCen, burst, maxSegs, st); break;
+    case 2: k_transport_refill<F, 2><<<grid, 256, 0, s>>>(C, in, n, nextIdx, cen, nCen, burst, maxSegs, st); break;
+    default: k_transport_refill<F, 1><<<grid, 256, 0, s>>>(C, in, n, nextIdx, cen, nCen, burst, maxSegs, st); break;
+    }
+}
+void launch_transport_refill(cudaStream_t s, uint32_t grid, int minBlocks, const Ctx &C, const Bank &in, uint32_t n,
+                             uint32_t *nextIdx, const Bank &cen, uint32_t *nCen, uint32_t burst, uint32_t maxSegs,
+                             DevStats *st) {
+    if (C.fp32) refill_launch<Form32>(s, grid, minBlocks, C, in, n, nextIdx, cen, nCen, burst, maxSegs, st);
+    else refill_launch<Form64>(s, grid, minBlocks, C, in, n, nextIdx, cen, nCen, burst, maxSegs, st);
+}
+template <class F>
+static int refill_occ(int minBlocks) {
+    int nb = 0;
+    switch (minBlocks) {
+    case 4: cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_transport_refill<F, 4>, 256, 0); break;
+    case 3: cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_transport_refill<F, 3>, 256, 0); break;
+    case 2: cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_transport_refill<F, 2>, 256, 0); break;
+    default: cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_transport_refill<F, 1>, 256, 0); break;
+    }
+    return nb;
+}
+int refill_blocks_per_sm(int minBlocks, bool fp32) { return fp32 ? refill_occ<Form32>(minBlocks) : refill_occ<Form64>(minBlocks); }
+
 void launch_bank_to_local(cudaStream_t s, const Ctx &C, const Bank &src, const Bank &dst, uint32_t n) {
     if (n) k_bank_to_local<<<grid_for(n, 256, 8192), 256, 0, s>>>(C, src, dst, n);
 }

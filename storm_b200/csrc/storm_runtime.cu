@@ -78,6 +78,8 @@ struct StormHandle {
     uint32_t step = 0;
     uint32_t K = 8, maxRounds = 4096;
     int minBlocks = 3;               // transport occupancy variant (__launch_bounds__ min blocks)
+    int refill = 0;                  // 1: persistent refill kernel, 0: bank visits of K segments
+    uint32_t burst = 4;              // refill kernel: segments between refills
     int smCount = 148;
     uint32_t transportGrid = 0;      // resident blocks of the chosen variant x SMs
     uint64_t launches = 0;
@@ -670,6 +672,51 @@ int storm_cuda_phase_transport(StormHandle *h) {
     uint32_t n32 = static_cast<uint32_t>(n0);
     CK(cudaMemcpyAsync(h->counts, &n32, sizeof(uint32_t), cudaMemcpyHostToDevice, h->stream));
     uint32_t *nCen = h->counts + h->maxRounds + 1;
+    if (h->refill) {
+        // one launch carries every history to census, escape or cutoff
+        const uint64_t maxSegs64 = static_cast<uint64_t>(h->maxRounds) * h->K;
+        const uint32_t maxSegs = static_cast<uint32_t>(std::min<uint64_t>(maxSegs64, 0xffffffffull));
+        int nb = refill_blocks_per_sm(h->minBlocks, h->fp32);
+        uint32_t grid = static_cast<uint32_t>(h->smCount) * static_cast<uint32_t>(nb > 0 ? nb : 1);
+        const uint32_t need = static_cast<uint32_t>((n0 + 255) / 256);
+        if (need < grid) grid = need ? need : 1;
+        if (n0) {
+            if (h->profiling && h->evPool.empty()) {
+                h->evPool.resize(8);
+                for (auto &e : h->evPool) CK(cudaEventCreate(&e));
+            }
+            if (h->profiling) CK(cudaEventRecord(h->evPool[0], h->stream));
+            launch_transport_refill(h->stream, grid, h->minBlocks, h->C, h->bankA, n32, h->counts + 1, h->bankC, nCen,
+                                    h->burst, maxSegs, h->dStats);
+            if (h->profiling) CK(cudaEventRecord(h->evPool[1], h->stream));
+            ++h->launches;
+        }
+        CK(cudaGetLastError());
+        CK(cudaEventRecord(h->evTransport1, h->stream));
+        CK(cudaStreamSynchronize(h->stream));
+        if (h->profiling && n0) {
+            float ms = 0.f;
+            CK(cudaEventElapsedTime(&ms, h->evPool[0], h->evPool[1]));
+            h->profMs += ms;
+            h->profLaunches += 1;
+        }
+        h->stats.rounds = n0 ? 1 : 0;
+        int rc = check_device_error(h);
+        if (rc != STORM_OK) return rc;
+        uint32_t nc = 0;
+        CK(cudaMemcpy(&nc, nCen, sizeof(uint32_t), cudaMemcpyDeviceToHost));
+        h->stats.census_out_pre_comb = nc;
+        if (h->profiling) {
+            DevStats d{};
+            CK(cudaMemcpy(&d, h->dStats, sizeof(d), cudaMemcpyDeviceToHost));
+            h->profSegments += d.segments;
+        }
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, h->evTransport0, h->evTransport1);
+        h->lastTransportMs = ms;
+        h->nBank = 0;
+        return STORM_OK;
+    }
     const uint32_t grid = grid_transport(n0, h->transportGrid);
     uint32_t r = 0;
     bool done = (n0 == 0);
@@ -1174,6 +1221,13 @@ int storm_cuda_transport_timing(StormHandle *h, double *ms, uint64_t *launches, 
         h->profLaunches = 0;
         h->profSegments = 0;
     }
+    return STORM_OK;
+}
+
+int storm_cuda_set_transport_mode(StormHandle *h, int refill, uint32_t burst) {
+    if (!h || burst == 0 || burst > 1024) return STORM_ERR_INVALID_ARG;
+    h->refill = refill != 0;
+    h->burst = burst;
     return STORM_OK;
 }
 

@@ -57,6 +57,7 @@ def lib():
         L.storm_cuda_set_segments_per_visit.argtypes = [vp, C.c_uint32]
         L.storm_cuda_set_profiling.argtypes = [vp, C.c_int]
         L.storm_cuda_set_transport_variant.argtypes = [vp, C.c_int, C.c_int]
+        L.storm_cuda_set_transport_mode.argtypes = [vp, C.c_int, C.c_uint32]
         L.storm_cuda_transport_timing.argtypes = [vp, dp, u64p, u64p, C.c_int]
         L.storm_cuda_status_string.restype = C.c_char_p
         L.storm_cuda_status_string.argtypes = [C.c_int]
@@ -77,6 +78,12 @@ class Particles:
         self.n = n
 
     def soa(self):
+        """Struct of pointers; every field is made contiguous first (the C side
+        reads plain arrays)."""
+        for f in self.FIELDS:
+            setattr(self, f, np.ascontiguousarray(getattr(self, f), dtype=np.float64))
+        self.cell = np.ascontiguousarray(self.cell, dtype=np.uint32)
+        self.id = np.ascontiguousarray(self.id, dtype=np.uint64)
         s = A.StormParticlesSoA()
         for f in self.FIELDS:
             setattr(s, f, A.ptr(getattr(self, f)))
@@ -228,6 +235,9 @@ class Engine:
 
     def set_transport_variant(self, min_blocks_per_sm, waves=4):
         self._check(lib().storm_cuda_set_transport_variant(self.h, min_blocks_per_sm, waves))
+
+    def set_transport_mode(self, refill=True, burst=4):
+        self._check(lib().storm_cuda_set_transport_mode(self.h, int(refill), burst))
 
     def set_segments_per_visit(self, k):
         self._check(lib().storm_cuda_set_segments_per_visit(self.h, k))

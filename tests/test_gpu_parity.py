@@ -223,7 +223,7 @@ def test_step_cube_statistics_vs_oracle(oracle_lib):
 
 def test_errors_are_reported():
     p = problems.gray_slab()
-    p.precision = 1   # FP32 tracking form is selected separately
+    p.precision = 7   # no such precision
     with pytest.raises(StormError):
         Engine(p)
     e = Engine(problems.gray_slab())
