@@ -1070,14 +1070,12 @@ int orc_phase_transport(Oracle *o) {
 }
 
 /* Deterministic reduction used by the engine for the comb's total weight:
- * 1024 contiguous chunks summed left to right, then a pairwise tree. */
+ * partial sum t adds v[t], v[t + 1024], ... in order, then a pairwise tree. */
 static double blocked_sum(const double *v, uint64_t n) {
     double part[1024];
-    uint64_t chunk = (n + 1023) / 1024;
     for (uint64_t t = 0; t < 1024; ++t) {
         double s = 0.0;
-        uint64_t a = t * chunk, b = a + chunk < n ? a + chunk : n;
-        for (uint64_t q = a; q < b; ++q) s += v[q];
+        for (uint64_t q = t; q < n; q += 1024) s += v[q];
         part[t] = s;
     }
     for (uint64_t w = 512; w >= 1; w >>= 1)

@@ -16,6 +16,13 @@ struct Bank {
     uint32_t *cell, *pid, *draw;
 };
 
+// Census bank: one record of 16-byte vectors per particle (96 B in the FP64
+// form, 64 B in the FP32-tracking form), so the comb's random-order gather reads
+// one record instead of twelve scattered array elements.
+struct CensusBank {
+    uint4 *rec;
+};
+
 struct CellArrays {
     double *T, *mass, *vol, *eint, *ceint;
     double *sigA, *sigS, *fleck, *rwSigT, *eradAvg, *eradCensus, *emitE;
@@ -80,36 +87,38 @@ void launch_emit_cells(cudaStream_t s, const Ctx &C, const CellArrays &A, const 
 void launch_emit_faces(cudaStream_t s, const Ctx &C, const FaceSources &F, uint64_t total, const Bank &b,
                        uint32_t bankBase, double dt, DevStats *st);
 void launch_transport(cudaStream_t s, uint32_t grid, const Ctx &C, const Bank &in, const uint32_t *nIn, const Bank &out,
-                      uint32_t *nOut, const Bank &cen, uint32_t *nCen, uint32_t K, DevStats *st, int minBlocks);
+                      uint32_t *nOut, const CensusBank &cen, uint32_t *nCen, uint32_t K, DevStats *st, int minBlocks);
 int transport_blocks_per_sm(int minBlocks, bool fp32);
 void launch_transport_refill(cudaStream_t s, uint32_t grid, int minBlocks, const Ctx &C, const Bank &in, uint32_t n,
-                             uint32_t *nextIdx, const Bank &cen, uint32_t *nCen, uint32_t burst, uint32_t maxSegs,
+                             uint32_t *nextIdx, const CensusBank &cen, uint32_t *nCen, uint32_t burst, uint32_t maxSegs,
                              DevStats *st);
 int refill_blocks_per_sm(int minBlocks, bool fp32);
 void launch_bank_to_local(cudaStream_t s, const Ctx &C, const Bank &src, const Bank &dst, uint32_t n);
 void launch_bank_to_global(cudaStream_t s, const Ctx &C, const Bank &src, const Bank &dst, uint32_t n);
-void launch_comb_keys(cudaStream_t s, const Ctx &C, const Bank &cen, uint32_t n, uint64_t *keys, uint32_t *vals,
+void launch_comb_keys(cudaStream_t s, const Ctx &C, const CensusBank &cen, uint32_t n, uint64_t *keys, uint32_t *vals,
                       uint32_t combKey);
 int launch_radix_sort(cudaStream_t s, uint64_t *keys, uint32_t *vals, uint64_t *keysAlt, uint32_t *valsAlt, uint32_t n,
                       int bits, uint32_t *tileHist);
 uint32_t radix_tile_count(uint32_t n);
 void launch_comb_ranges(cudaStream_t s, const uint64_t *keys, uint32_t n, uint32_t ncells, uint32_t *start);
-void launch_comb_cell_sums(cudaStream_t s, const Bank &cen, const uint32_t *idx, const uint32_t *start, uint32_t ncells,
-                           double *W);
+void launch_comb_cell_sums(cudaStream_t s, const Ctx &C, const CensusBank &cen, const uint32_t *idx,
+                           const uint32_t *start, uint32_t ncells, double *W);
 void launch_blocked_sum(cudaStream_t s, const double *v, uint32_t n, double *out);
-void launch_comb_plan(cudaStream_t s, const Ctx &C, const CombParams &P, const Bank &cen, const uint32_t *idx,
+void launch_comb_plan(cudaStream_t s, const Ctx &C, const CombParams &P, const CensusBank &cen, const uint32_t *idx,
                       const uint32_t *start, const double *W, const double *Wtot, uint32_t *pCount, double *pWeight,
                       uint64_t *cellCount, double *eradCensus, DevStats *st);
-void launch_comb_emit(cudaStream_t s, const Ctx &C, const Bank &cen, const uint32_t *idx, const uint64_t *sortedKeys,
+void launch_comb_emit(cudaStream_t s, const Ctx &C, const CensusBank &cen, const uint32_t *idx, const uint64_t *sortedKeys,
                       uint32_t nValid, const uint32_t *pCount, const double *pWeight, const uint64_t *pOffset,
                       const Bank &out);
 void launch_mask_count(cudaStream_t s, const uint32_t *pCount, uint32_t n, uint64_t *out);
 void launch_allocate_checked(cudaStream_t s, const Ctx &C, const CellArrays &A, const double *total,
                              uint64_t newPerCell, double rel, int32_t *ambiguous);
 size_t radix_scratch_words(uint32_t n);
-void launch_census_keys_pid(cudaStream_t s, const Bank &cen, uint32_t n, uint64_t *keys, uint32_t *vals);
-void launch_gather(cudaStream_t s, const Ctx &C, const Bank &src, const uint32_t *idx, uint32_t n, const Bank &dst,
+void launch_census_keys_pid(cudaStream_t s, const Ctx &C, const CensusBank &cen, uint32_t n, uint64_t *keys,
+                            uint32_t *vals);
+void launch_gather(cudaStream_t s, const Ctx &C, const CensusBank &src, const uint32_t *idx, uint32_t n, const Bank &dst,
                    double *eradCensus, DevStats *st);
+void launch_bank_to_census(cudaStream_t s, const Ctx &C, const Bank &src, const CensusBank &dst, uint32_t n);
 void launch_poststep(cudaStream_t s, const Ctx &C, const CellArrays &A, const OpacityEos &M, double dt);
 void launch_replay(cudaStream_t s, const Ctx &C, const ReplayDev &R, uint32_t n);
 void launch_rw_radius(cudaStream_t s, const double *tau, const double *surv, double *radius);

@@ -107,6 +107,71 @@ __device__ __forceinline__ void copy_any(const Ctx &C, const Bank &src, uint32_t
     }
 }
 
+// ---- census bank: array of records, gathered in random order by the comb.
+// FP64 form, 96 B: (x,y) (z,vx) (vy,vz) (t,w) (w0,[cell,pid]) ([draw,-,-,-])
+// FP32 form, 64 B: (qx,qy,qz,ux) (uy,uz,t) (w,w0) (cell,pid,draw,-)
+__device__ __forceinline__ uint4 two_doubles(double a, double b) {
+    const unsigned long long x = __double_as_longlong(a), y = __double_as_longlong(b);
+    return make_uint4(static_cast<uint32_t>(x), static_cast<uint32_t>(x >> 32), static_cast<uint32_t>(y),
+                      static_cast<uint32_t>(y >> 32));
+}
+__device__ __forceinline__ double lo_double(const uint4 &v) {
+    return __longlong_as_double((static_cast<unsigned long long>(v.y) << 32) | v.x);
+}
+__device__ __forceinline__ double hi_double(const uint4 &v) {
+    return __longlong_as_double((static_cast<unsigned long long>(v.w) << 32) | v.z);
+}
+__device__ __forceinline__ void census_store64(const CensusBank &c, uint32_t q, const PartReg &p, uint32_t pid,
+                                               uint32_t draw) {
+    uint4 *r = c.rec + static_cast<size_t>(q) * 6;
+    r[0] = two_doubles(p.x, p.y);
+    r[1] = two_doubles(p.z, p.vx);
+    r[2] = two_doubles(p.vy, p.vz);
+    r[3] = two_doubles(p.t, p.w);
+    const unsigned long long w0 = __double_as_longlong(p.w0);
+    r[4] = make_uint4(static_cast<uint32_t>(w0), static_cast<uint32_t>(w0 >> 32), p.cell, pid);
+    r[5] = make_uint4(draw, 0u, 0u, 0u);
+}
+__device__ __forceinline__ void census_load64(const CensusBank &c, uint32_t q, PartReg &p, uint32_t &pid,
+                                              uint32_t &draw) {
+    const uint4 *r = c.rec + static_cast<size_t>(q) * 6;
+    const uint4 a = r[0], b = r[1], d = r[2], e = r[3], f = r[4], g = r[5];
+    p.x = lo_double(a); p.y = hi_double(a);
+    p.z = lo_double(b); p.vx = hi_double(b);
+    p.vy = lo_double(d); p.vz = hi_double(d);
+    p.t = lo_double(e); p.w = hi_double(e);
+    p.w0 = lo_double(f);
+    p.cell = f.z; pid = f.w; draw = g.x;
+}
+__device__ __forceinline__ void census_store32(const CensusBank &c, uint32_t q, const Track32 &T, uint32_t pid,
+                                               uint32_t draw) {
+    uint4 *r = c.rec + static_cast<size_t>(q) * 4;
+    r[0] = make_uint4(__float_as_uint(T.qx), __float_as_uint(T.qy), __float_as_uint(T.qz), __float_as_uint(T.ux));
+    const unsigned long long t = __double_as_longlong(T.t);
+    r[1] = make_uint4(__float_as_uint(T.uy), __float_as_uint(T.uz), static_cast<uint32_t>(t), static_cast<uint32_t>(t >> 32));
+    r[2] = two_doubles(T.w, T.w0);
+    r[3] = make_uint4(T.cell, pid, draw, 0u);
+}
+__device__ __forceinline__ void census_load32(const CensusBank &c, uint32_t q, Track32 &T, uint32_t &pid,
+                                              uint32_t &draw) {
+    const uint4 *r = c.rec + static_cast<size_t>(q) * 4;
+    const uint4 a = r[0], b = r[1], d = r[2], e = r[3];
+    T.qx = __uint_as_float(a.x); T.qy = __uint_as_float(a.y); T.qz = __uint_as_float(a.z); T.ux = __uint_as_float(a.w);
+    T.uy = __uint_as_float(b.x); T.uz = __uint_as_float(b.y);
+    T.t = __longlong_as_double((static_cast<unsigned long long>(b.w) << 32) | b.z);
+    T.w = lo_double(d); T.w0 = hi_double(d);
+    T.cell = e.x; pid = e.y; draw = e.z;
+}
+// weight, cell and pid of census record q
+__device__ __forceinline__ double census_w(const Ctx &C, const CensusBank &c, uint32_t q) {
+    const uint4 v = c.rec[static_cast<size_t>(q) * (C.fp32 ? 4 : 6) + (C.fp32 ? 2 : 3)];
+    return C.fp32 ? lo_double(v) : hi_double(v);
+}
+__device__ __forceinline__ uint2 census_cell_pid(const Ctx &C, const CensusBank &c, uint32_t q) {
+    const uint4 v = c.rec[static_cast<size_t>(q) * (C.fp32 ? 4 : 6) + (C.fp32 ? 3 : 4)];
+    return C.fp32 ? make_uint2(v.x, v.y) : make_uint2(v.z, v.w);
+}
+
 // convert a bank between the FP64 (global) and FP32-tracking (local) layouts
 __global__ void k_bank_to_local(Ctx C, Bank src, Bank dst, uint32_t n) {
     for (uint32_t q = blockIdx.x * blockDim.x + threadIdx.x; q < n; q += gridDim.x * blockDim.x) {
@@ -115,6 +180,19 @@ __global__ void k_bank_to_local(Ctx C, Bank src, Bank dst, uint32_t n) {
         Track32 T;
         to_local(C, p, T);
         store32(dst, q, T, src.pid[q], src.draw[q]);
+    }
+}
+__global__ void k_bank_to_census(Ctx C, Bank src, CensusBank dst, uint32_t n) {
+    for (uint32_t q = blockIdx.x * blockDim.x + threadIdx.x; q < n; q += gridDim.x * blockDim.x) {
+        PartReg p;
+        load_part(src, q, p);
+        if (C.fp32) {
+            Track32 T;
+            to_local(C, p, T);
+            census_store32(dst, q, T, src.pid[q], src.draw[q]);
+        } else {
+            census_store64(dst, q, p, src.pid[q], src.draw[q]);
+        }
     }
 }
 __global__ void k_bank_to_global(Ctx C, Bank src, Bank dst, uint32_t n) {
@@ -590,7 +668,7 @@ struct BlockStats {
 
 template <int MINB>
 __global__ void __launch_bounds__(256, MINB) k_transport(Ctx C, Bank in, const uint32_t *nIn, Bank out,
-                                                          uint32_t *nOut, Bank cen, uint32_t *nCen, uint32_t K,
+                                                          uint32_t *nOut, CensusBank cen, uint32_t *nCen, uint32_t K,
                                                           DevStats *st) {
     __shared__ BlockStats bs;
     if (threadIdx.x == 0) bs = BlockStats{0, 0, 0, 0, 0, 0.0, 0.0, 0.0};
@@ -650,7 +728,7 @@ __global__ void __launch_bounds__(256, MINB) k_transport(Ctx C, Bank in, const u
         bC = __shfl_sync(FULL, bC, 0);
         const unsigned lt = lanemask_lt();
         if (keep) store_part(out, bK + __popc(mK & lt), p, pid, draw);
-        if (cens) store_part(cen, bC + __popc(mC & lt), p, pid, draw);
+        if (cens) census_store64(cen, bC + __popc(mC & lt), p, pid, draw);
     }
     __syncthreads();
     if (threadIdx.x == 0) {
@@ -668,7 +746,7 @@ __global__ void __launch_bounds__(256, MINB) k_transport(Ctx C, Bank in, const u
 // The same bank visit in the FP32-tracking form.
 template <int MINB>
 __global__ void __launch_bounds__(256, MINB) k_transport32(Ctx C, Bank in, const uint32_t *nIn, Bank out,
-                                                            uint32_t *nOut, Bank cen, uint32_t *nCen, uint32_t K,
+                                                            uint32_t *nOut, CensusBank cen, uint32_t *nCen, uint32_t K,
                                                             DevStats *st) {
     __shared__ BlockStats bs;
     if (threadIdx.x == 0) bs = BlockStats{0, 0, 0, 0, 0, 0.0, 0.0, 0.0};
@@ -722,7 +800,7 @@ __global__ void __launch_bounds__(256, MINB) k_transport32(Ctx C, Bank in, const
         bC = __shfl_sync(FULL, bC, 0);
         const unsigned lt = lanemask_lt();
         if (keep) store32(out, bK + __popc(mK & lt), T, pid, draw);
-        if (cens) store32(cen, bC + __popc(mC & lt), T, pid, draw);
+        if (cens) census_store32(cen, bC + __popc(mC & lt), T, pid, draw);
     }
     __syncthreads();
     if (threadIdx.x == 0) {
@@ -745,8 +823,9 @@ struct Form64 {
         load_part(b, q, t.p);
         track_begin(C, t);
     }
-    static __device__ __forceinline__ void store(const Bank &b, uint32_t q, const T &t, uint32_t pid, uint32_t draw) {
-        store_part(b, q, t.p, pid, draw);
+    static __device__ __forceinline__ void store(const CensusBank &b, uint32_t q, const T &t, uint32_t pid,
+                                                 uint32_t draw) {
+        census_store64(b, q, t.p, pid, draw);
     }
     template <class RNG, class TALLY>
     static __device__ __forceinline__ int seg(const Ctx &C, T &t, RNG &rng, TALLY &tal, int &usedRW, int &err) {
@@ -766,8 +845,9 @@ struct Form32 {
         load32(b, q, t);
         cell_ijk(C, t.cell, t.i, t.j, t.k);
     }
-    static __device__ __forceinline__ void store(const Bank &b, uint32_t q, const T &t, uint32_t pid, uint32_t draw) {
-        store32(b, q, t, pid, draw);
+    static __device__ __forceinline__ void store(const CensusBank &b, uint32_t q, const T &t, uint32_t pid,
+                                                 uint32_t draw) {
+        census_store32(b, q, t, pid, draw);
     }
     template <class RNG, class TALLY>
     static __device__ __forceinline__ int seg(const Ctx &C, T &t, RNG &rng, TALLY &tal, int &usedRW, int &err) {
@@ -785,7 +865,7 @@ struct Form32 {
 // one), so lanes do not idle behind the longest history of their warp.  A
 // history longer than maxSegs raises STORM_DERR_HISTORY_CAP and stops.
 template <class F, int MINB>
-__global__ void __launch_bounds__(256, MINB) k_transport_refill(Ctx C, Bank in, uint32_t n, uint32_t *nextIdx, Bank cen,
+__global__ void __launch_bounds__(256, MINB) k_transport_refill(Ctx C, Bank in, uint32_t n, uint32_t *nextIdx, CensusBank cen,
                                                                  uint32_t *nCen, uint32_t burst, uint32_t maxSegs,
                                                                  DevStats *st) {
     __shared__ BlockStats bs;
@@ -881,13 +961,17 @@ __device__ __forceinline__ uint32_t fmix32(uint32_t h) {
     h ^= h >> 16; h *= 0x85ebca6bu; h ^= h >> 13; h *= 0xc2b2ae35u; h ^= h >> 16;
     return h;
 }
-__global__ void k_comb_keys(Ctx C, Bank cen, uint32_t n, uint64_t *keys, uint32_t *vals, uint32_t combKey) {
+__global__ void k_comb_keys(Ctx C, CensusBank cen, uint32_t n, uint64_t *keys, uint32_t *vals, uint32_t combKey) {
     for (uint32_t q = blockIdx.x * blockDim.x + threadIdx.x; q < n; q += gridDim.x * blockDim.x) {
-        const double w = cen.w[q];
-        const uint32_t pid = cen.pid[q];
-        uint32_t cell = cen.cell[q];
+        const double w = census_w(C, cen, q);
+        const uint2 cp = census_cell_pid(C, cen, q);
+        const uint32_t pid = cp.y;
+        uint32_t cell = cp.x;
         // FP32-tracking particles are inside their cell by construction
-        if (!C.fp32 && outside_box(C, cen.x[q], cen.y[q], cen.z[q])) raise_error(C, STORM_DERR_COMB_OUTSIDE, cell, pid);
+        if (!C.fp32) {
+            const uint4 a = cen.rec[static_cast<size_t>(q) * 6], b = cen.rec[static_cast<size_t>(q) * 6 + 1];
+            if (outside_box(C, lo_double(a), hi_double(a), lo_double(b))) raise_error(C, STORM_DERR_COMB_OUTSIDE, cell, pid);
+        }
         const bool badWeight = !isfinite(w) || w < 0.0;
         if (badWeight) raise_error(C, STORM_DERR_COMB_WEIGHT, cell, pid);
         // zero, negative and non-finite weights never reach the per-cell loops
@@ -1003,21 +1087,21 @@ __global__ void k_comb_ranges(const uint64_t *keys, uint32_t n, uint32_t ncells,
 }
 
 // weights[cell] (:136-141), summed in sorted order
-__global__ void k_comb_cell_sums(Bank cen, const uint32_t *idx, const uint32_t *start, uint32_t ncells, double *W) {
+__global__ void k_comb_cell_sums(Ctx C, CensusBank cen, const uint32_t *idx, const uint32_t *start, uint32_t ncells,
+                                 double *W) {
     for (uint32_t c = blockIdx.x * blockDim.x + threadIdx.x; c < ncells; c += gridDim.x * blockDim.x) {
         double s = 0.0;
-        for (uint32_t q = start[c]; q < start[c + 1]; ++q) s += cen.w[idx[q]];
+        for (uint32_t q = start[c]; q < start[c + 1]; ++q) s += census_w(C, cen, idx[q]);
         W[c] = s;
     }
 }
 
-// Deterministic total: 1024 contiguous chunks left to right, then a pairwise tree.
+// Deterministic total: thread t adds v[t], v[t + 1024], ... in order (coalesced),
+// then a pairwise tree over the 1024 partial sums.
 __global__ void k_blocked_sum(const double *v, uint32_t n, double *out) {
     __shared__ double part[1024];
-    const uint32_t chunk = (n + 1023) / 1024;
-    const uint32_t a = threadIdx.x * chunk;
     double s = 0.0;
-    for (uint32_t q = a; q < a + chunk && q < n; ++q) s += v[q];
+    for (uint32_t q = threadIdx.x; q < n; q += 1024) s += v[q];
     part[threadIdx.x] = s;
     __syncthreads();
     for (uint32_t w = 512; w >= 1; w >>= 1) {
@@ -1052,7 +1136,7 @@ __device__ __forceinline__ CombCell comb_cell_params(const Ctx &C, const CombPar
 // of those copies, and the cell's census radiation energy summed in output order
 // (RadiationIMC::postStep :2013-2016).  pCount bit 31 marks a particle kept as is.
 constexpr uint32_t KEEP = 0x80000000u;
-__global__ void k_comb_plan(Ctx C, CombParams P, Bank cen, const uint32_t *idx, const uint32_t *start, const double *W,
+__global__ void k_comb_plan(Ctx C, CombParams P, CensusBank cen, const uint32_t *idx, const uint32_t *start, const double *W,
                             const double *Wtot, uint32_t *pCount, double *pWeight, uint64_t *cellCount,
                             double *eradCensus, DevStats *st) {
     const double tot = *Wtot;
@@ -1070,7 +1154,7 @@ __global__ void k_comb_plan(Ctx C, CombParams P, Bank cen, const uint32_t *idx, 
             CombCell cc = comb_cell_params(C, P, c, b - a, W[c], tot);
             if (cc.mode == 0) {
                 for (uint32_t q = a; q < b; ++q) {
-                    const double w = cen.w[idx[q]];
+                    const double w = census_w(C, cen, idx[q]);
                     if (w > 2 * cc.w_ideal) {
                         const uint64_t ns = static_cast<uint64_t>(ceil(w / cc.w_ideal));
                         const double ws = w / static_cast<double>(ns);
@@ -1089,7 +1173,7 @@ __global__ void k_comb_plan(Ctx C, CombParams P, Bank cen, const uint32_t *idx, 
                 uint64_t k = 0;
                 double cum = 0;
                 for (uint32_t q = a; q < b; ++q) {
-                    const double w = cen.w[idx[q]];
+                    const double w = census_w(C, cen, idx[q]);
                     const uint64_t k0 = k;
                     while ((cum + w) > (static_cast<double>(k) + cc.r) * cc.e) {
                         ++k;
@@ -1113,7 +1197,7 @@ __global__ void k_comb_plan(Ctx C, CombParams P, Bank cen, const uint32_t *idx, 
 // One thread per sorted particle writes its copies at its output offset.
 // The exclusive prefix of the copy counts over sorted particles is the output
 // position: cells are contiguous in sorted order and the output is cell-major.
-__global__ void k_comb_emit(Ctx C, Bank cen, const uint32_t *idx, const uint64_t *sortedKeys, uint32_t nValid,
+__global__ void k_comb_emit(Ctx C, CensusBank cen, const uint32_t *idx, const uint64_t *sortedKeys, uint32_t nValid,
                             const uint32_t *pCount, const double *pWeight, const uint64_t *pOffset, Bank out) {
     for (uint32_t q = blockIdx.x * blockDim.x + threadIdx.x; q < nValid; q += gridDim.x * blockDim.x) {
         const uint32_t raw = pCount[q];
@@ -1122,7 +1206,8 @@ __global__ void k_comb_emit(Ctx C, Bank cen, const uint32_t *idx, const uint64_t
         const uint32_t c = static_cast<uint32_t>(sortedKeys[q] >> 32);
         if (C.fp32) {
             Track32 T;
-            load32(cen, idx[q], T);
+            uint32_t pid_, draw_;
+            census_load32(cen, idx[q], T, pid_, draw_);
             if (!(raw & KEEP)) { T.w = pWeight[q]; T.w0 = T.w; T.t = 0; }
             T.cell = c;
             const uint64_t o = pOffset[q];
@@ -1130,7 +1215,8 @@ __global__ void k_comb_emit(Ctx C, Bank cen, const uint32_t *idx, const uint64_t
             continue;
         }
         PartReg p;
-        load_part(cen, idx[q], p);
+        uint32_t pid_, draw_;
+        census_load64(cen, idx[q], p, pid_, draw_);
         if (!(raw & KEEP)) { p.w = pWeight[q]; p.w0 = p.w; p.t = 0; }
         p.cell = c;
         if (outside_box(C, p.x, p.y, p.z)) {   // :228-250
@@ -1156,19 +1242,31 @@ __global__ void k_mask_count(const uint32_t *pCount, uint32_t n, uint64_t *out) 
 }
 
 // census kept as is (no population control): order by pid for a deterministic bank
-__global__ void k_census_keys_pid(Bank cen, uint32_t n, uint64_t *keys, uint32_t *vals) {
+__global__ void k_census_keys_pid(Ctx C, CensusBank cen, uint32_t n, uint64_t *keys, uint32_t *vals) {
     for (uint32_t q = blockIdx.x * blockDim.x + threadIdx.x; q < n; q += gridDim.x * blockDim.x) {
-        keys[q] = cen.pid[q];
+        keys[q] = census_cell_pid(C, cen, q).y;
         vals[q] = q;
     }
 }
-__global__ void k_gather(Ctx C, Bank src, const uint32_t *idx, uint32_t n, Bank dst, double *eradCensus, DevStats *st) {
+__global__ void k_gather(Ctx C, CensusBank src, const uint32_t *idx, uint32_t n, Bank dst, double *eradCensus,
+                         DevStats *st) {
     double e = 0.0;
     for (uint32_t q = blockIdx.x * blockDim.x + threadIdx.x; q < n; q += gridDim.x * blockDim.x) {
         const uint32_t sq = idx[q];
-        copy_any(C, src, sq, dst, q, q, 0);
-        const double w = src.w[sq];
-        atomicAdd(eradCensus + src.cell[sq], w);
+        double w;
+        uint32_t cell, pid_, draw_;
+        if (C.fp32) {
+            Track32 T;
+            census_load32(src, sq, T, pid_, draw_);
+            store32(dst, q, T, q, 0);
+            w = T.w; cell = T.cell;
+        } else {
+            PartReg p;
+            census_load64(src, sq, p, pid_, draw_);
+            store_part(dst, q, p, q, 0);
+            w = p.w; cell = p.cell;
+        }
+        atomicAdd(eradCensus + cell, w);
         e += w;
     }
     e = warp_sum(e);
@@ -1352,7 +1450,7 @@ void launch_emit_faces(cudaStream_t s, const Ctx &C, const FaceSources &F, uint6
     k_emit_faces<<<grid_for(total, 256, 148 * 16), 256, 0, s>>>(C, F, total, b, bankBase, dt, st);
 }
 void launch_transport(cudaStream_t s, uint32_t grid, const Ctx &C, const Bank &in, const uint32_t *nIn, const Bank &out,
-                      uint32_t *nOut, const Bank &cen, uint32_t *nCen, uint32_t K, DevStats *st, int minBlocks) {
+                      uint32_t *nOut, const CensusBank &cen, uint32_t *nCen, uint32_t K, DevStats *st, int minBlocks) {
     if (C.fp32) {
         switch (minBlocks) {
         case 3: k_transport32<3><<<grid, 256, 0, s>>>(C, in, nIn, out, nOut, cen, nCen, K, st); break;
@@ -1388,7 +1486,7 @@ int transport_blocks_per_sm(int minBlocks, bool fp32) {
     }
     return nb;
 }
-void launch_comb_keys(cudaStream_t s, const Ctx &C, const Bank &cen, uint32_t n, uint64_t *keys, uint32_t *vals,
+void launch_comb_keys(cudaStream_t s, const Ctx &C, const CensusBank &cen, uint32_t n, uint64_t *keys, uint32_t *vals,
                       uint32_t combKey) {
     k_comb_keys<<<grid_for(n, 256, 8192), 256, 0, s>>>(C, cen, n, keys, vals, combKey);
 }
@@ -1423,20 +1521,20 @@ size_t radix_scratch_words(uint32_t n) {
 void launch_comb_ranges(cudaStream_t s, const uint64_t *keys, uint32_t n, uint32_t ncells, uint32_t *start) {
     k_comb_ranges<<<grid_for(ncells + 1, 256, 8192), 256, 0, s>>>(keys, n, ncells, start);
 }
-void launch_comb_cell_sums(cudaStream_t s, const Bank &cen, const uint32_t *idx, const uint32_t *start, uint32_t ncells,
-                           double *W) {
-    k_comb_cell_sums<<<grid_for(ncells, 128, 8192), 128, 0, s>>>(cen, idx, start, ncells, W);
+void launch_comb_cell_sums(cudaStream_t s, const Ctx &C, const CensusBank &cen, const uint32_t *idx,
+                           const uint32_t *start, uint32_t ncells, double *W) {
+    k_comb_cell_sums<<<grid_for(ncells, 128, 8192), 128, 0, s>>>(C, cen, idx, start, ncells, W);
 }
 void launch_blocked_sum(cudaStream_t s, const double *v, uint32_t n, double *out) {
     k_blocked_sum<<<1, 1024, 0, s>>>(v, n, out);
 }
-void launch_comb_plan(cudaStream_t s, const Ctx &C, const CombParams &P, const Bank &cen, const uint32_t *idx,
+void launch_comb_plan(cudaStream_t s, const Ctx &C, const CombParams &P, const CensusBank &cen, const uint32_t *idx,
                       const uint32_t *start, const double *W, const double *Wtot, uint32_t *pCount, double *pWeight,
                       uint64_t *cellCount, double *eradCensus, DevStats *st) {
     k_comb_plan<<<grid_for(C.ncells, 128, 8192), 128, 0, s>>>(C, P, cen, idx, start, W, Wtot, pCount, pWeight, cellCount,
                                                                eradCensus, st);
 }
-void launch_comb_emit(cudaStream_t s, const Ctx &C, const Bank &cen, const uint32_t *idx, const uint64_t *sortedKeys,
+void launch_comb_emit(cudaStream_t s, const Ctx &C, const CensusBank &cen, const uint32_t *idx, const uint64_t *sortedKeys,
                       uint32_t nValid, const uint32_t *pCount, const double *pWeight, const uint64_t *pOffset,
                       const Bank &out) {
     if (!nValid) return;
@@ -1446,16 +1544,17 @@ void launch_comb_emit(cudaStream_t s, const Ctx &C, const Bank &cen, const uint3
 void launch_mask_count(cudaStream_t s, const uint32_t *pCount, uint32_t n, uint64_t *out) {
     k_mask_count<<<grid_for(n, 256, 8192), 256, 0, s>>>(pCount, n, out);
 }
-void launch_census_keys_pid(cudaStream_t s, const Bank &cen, uint32_t n, uint64_t *keys, uint32_t *vals) {
-    k_census_keys_pid<<<grid_for(n, 256, 8192), 256, 0, s>>>(cen, n, keys, vals);
+void launch_census_keys_pid(cudaStream_t s, const Ctx &C, const CensusBank &cen, uint32_t n, uint64_t *keys,
+                            uint32_t *vals) {
+    k_census_keys_pid<<<grid_for(n, 256, 8192), 256, 0, s>>>(C, cen, n, keys, vals);
 }
-void launch_gather(cudaStream_t s, const Ctx &C, const Bank &src, const uint32_t *idx, uint32_t n, const Bank &dst,
+void launch_gather(cudaStream_t s, const Ctx &C, const CensusBank &src, const uint32_t *idx, uint32_t n, const Bank &dst,
                    double *eradCensus, DevStats *st) {
     k_gather<<<grid_for(n, 256, 8192), 256, 0, s>>>(C, src, idx, n, dst, eradCensus, st);
 }
 template <class F>
 static void refill_launch(cudaStream_t s, uint32_t grid, int minBlocks, const Ctx &C, const Bank &in, uint32_t n,
-                          uint32_t *nextIdx, const Bank &cen, uint32_t *nCen, uint32_t burst, uint32_t maxSegs,
+                          uint32_t *nextIdx, const CensusBank &cen, uint32_t *nCen, uint32_t burst, uint32_t maxSegs,
                           DevStats *st) {
     switch (minBlocks) {
     case 4: k_transport_refill<F, 4><<<grid, 256, 0, s>>>(C, in, n, nextIdx, cen, nCen, burst, maxSegs, st); break;
@@ -1465,7 +1564,7 @@ static void refill_launch(cudaStream_t s, uint32_t grid, int minBlocks, const Ct
     }
 }
 void launch_transport_refill(cudaStream_t s, uint32_t grid, int minBlocks, const Ctx &C, const Bank &in, uint32_t n,
-                             uint32_t *nextIdx, const Bank &cen, uint32_t *nCen, uint32_t burst, uint32_t maxSegs,
+                             uint32_t *nextIdx, const CensusBank &cen, uint32_t *nCen, uint32_t burst, uint32_t maxSegs,
                              DevStats *st) {
     if (C.fp32) refill_launch<Form32>(s, grid, minBlocks, C, in, n, nextIdx, cen, nCen, burst, maxSegs, st);
     else refill_launch<Form64>(s, grid, minBlocks, C, in, n, nextIdx, cen, nCen, burst, maxSegs, st);
@@ -1485,6 +1584,9 @@ int refill_blocks_per_sm(int minBlocks, bool fp32) { return fp32 ? refill_occ<Fo
 
 void launch_bank_to_local(cudaStream_t s, const Ctx &C, const Bank &src, const Bank &dst, uint32_t n) {
     if (n) k_bank_to_local<<<grid_for(n, 256, 8192), 256, 0, s>>>(C, src, dst, n);
+}
+void launch_bank_to_census(cudaStream_t s, const Ctx &C, const Bank &src, const CensusBank &dst, uint32_t n) {
+    if (n) k_bank_to_census<<<grid_for(n, 256, 8192), 256, 0, s>>>(C, src, dst, n);
 }
 void launch_bank_to_global(cudaStream_t s, const Ctx &C, const Bank &src, const Bank &dst, uint32_t n) {
     if (n) k_bank_to_global<<<grid_for(n, 256, 8192), 256, 0, s>>>(C, src, dst, n);

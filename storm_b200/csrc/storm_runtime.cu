@@ -56,7 +56,8 @@ struct StormHandle {
     uint64_t fsTotal = 0;
     // banks
     size_t cap = 0;
-    Bank bankA{}, bankB{}, bankC{};
+    Bank bankA{}, bankB{};
+    CensusBank bankC{};              // census records (see CensusBank)
     uint64_t *keys = nullptr, *keysAlt = nullptr;
     uint32_t *vals = nullptr, *valsAlt = nullptr, *tileHist = nullptr;
     size_t tileHistLen = 0;
@@ -166,9 +167,11 @@ cudaError_t bank_copy(cudaStream_t s, const Bank &dst, const Bank &src, size_t n
 }
 
 // Buffers sized by particle capacity, other than the transport banks A and B.
+size_t census_words(const StormHandle *h) { return h->fp32 ? 4 : 6; }   // uint4 per record
+
 cudaError_t alloc_rest(StormHandle *h, size_t nc) {
     cudaError_t e;
-    if ((e = bank_alloc(h, h->bankC, nc)) != cudaSuccess) return e;
+    if ((e = dalloc(h, &h->bankC.rec, nc * census_words(h))) != cudaSuccess) return e;
     if ((e = dalloc(h, &h->keys, nc)) != cudaSuccess) return e;
     if ((e = dalloc(h, &h->keysAlt, nc)) != cudaSuccess) return e;
     if ((e = dalloc(h, &h->vals, nc)) != cudaSuccess) return e;
@@ -181,7 +184,7 @@ cudaError_t alloc_rest(StormHandle *h, size_t nc) {
     return dalloc(h, &h->pTiles, nc / 1024 + 4);
 }
 void free_rest(StormHandle *h, size_t nc) {
-    bank_free(h, h->bankC, nc);
+    dfree(h, h->bankC.rec, nc * census_words(h));
     dfree(h, h->keys, nc); dfree(h, h->keysAlt, nc);
     dfree(h, h->vals, nc); dfree(h, h->valsAlt, nc);
     dfree(h, h->tileHist, h->tileHistLen);
@@ -794,7 +797,7 @@ int storm_cuda_phase_comb(StormHandle *h) {
     if (!h->desc.comb_enabled) {
         // NoPopulationControl (population/NoPopulationControl.hpp:25-28): the census
         // passes unchanged; order it by pid so the next step's streams are reproducible.
-        launch_census_keys_pid(h->stream, h->bankC, n, h->keys, h->vals);
+        launch_census_keys_pid(h->stream, h->C, h->bankC, n, h->keys, h->vals);
         int alt = launch_radix_sort(h->stream, h->keys, h->vals, h->keysAlt, h->valsAlt, n, 32, h->tileHist);
         const uint32_t *idx = alt ? h->valsAlt : h->vals;
         launch_gather(h->stream, h->C, h->bankC, idx, n, h->bankA, h->A.eradCensus, h->dStats);
@@ -820,7 +823,7 @@ int storm_cuda_phase_comb(StormHandle *h) {
     const uint32_t *idx = alt ? h->valsAlt : h->vals;
     const int passes = (32 + cellBits + 7) / 8;
     launch_comb_ranges(h->stream, skeys, n, N, h->combStart);
-    launch_comb_cell_sums(h->stream, h->bankC, idx, h->combStart, N, h->combW);
+    launch_comb_cell_sums(h->stream, h->C, h->bankC, idx, h->combStart, N, h->combW);
     launch_blocked_sum(h->stream, h->combW, N, h->combWtot);
     CombParams P;
     P.nmin = h->desc.comb_nmin;
@@ -962,7 +965,7 @@ int storm_cuda_population_control(StormHandle *h, const StormParticlesSoA *in) {
     const uint64_t n = in->count;
     int rc = ensure_capacity(h, n, 0);
     if (rc != STORM_OK) return rc;
-    const Bank &stage = h->fp32 ? h->bankB : h->bankC;
+    const Bank &stage = h->bankB;   // staged in FP64 layout, then written as census records
     const double *sd[] = {in->x, in->y, in->z, in->vx, in->vy, in->vz, in->time_left, in->weight, in->initial_weight};
     double *dd[] = {stage.x, stage.y, stage.z, stage.vx, stage.vy, stage.vz, stage.t, stage.w, stage.w0};
     if (n) {
@@ -978,11 +981,9 @@ int storm_cuda_population_control(StormHandle *h, const StormParticlesSoA *in) {
         CK(cudaMemcpyAsync(stage.cell, in->cell, n * sizeof(uint32_t), cudaMemcpyHostToDevice, h->stream));
         CK(cudaMemcpyAsync(stage.pid, pid.data(), n * sizeof(uint32_t), cudaMemcpyHostToDevice, h->stream));
         CK(cudaMemsetAsync(stage.draw, 0, n * sizeof(uint32_t), h->stream));
-        if (h->fp32) {
-            launch_bank_to_local(h->stream, h->C, h->bankB, h->bankC, static_cast<uint32_t>(n));
-            ++h->launches;
-            CK(cudaGetLastError());
-        }
+        launch_bank_to_census(h->stream, h->C, h->bankB, h->bankC, static_cast<uint32_t>(n));
+        ++h->launches;
+        CK(cudaGetLastError());
         CK(cudaStreamSynchronize(h->stream));
     }
     CK(cudaMemsetAsync(h->dStats, 0, sizeof(DevStats), h->stream));
