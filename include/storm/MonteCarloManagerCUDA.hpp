@@ -1,0 +1,376 @@
+// MonteCarloManagerCUDA -- drop-in replacement for STORM's MonteCarloManagerSerial
+// (manager/MonteCarloManagerSerial.hpp:26-117) that runs the IMC time step on a
+// B200 through the C ABI in storm_cuda.h.
+//
+// Same constructor shape and the same step() contract:
+//     std::vector<Particle<T,Grid>> step(std::vector<Particle<T,Grid>> &&census, dt_t dt)
+// consumes the census and returns the post-comb census; the caller's cells and
+// extensives are updated in place exactly where RadiationIMC::postStep updates
+// them (radiation/RadiationIMC.hpp:1887-2029).  Getters mirror the serial
+// manager's (manager/MonteCarloManagerSerial.hpp:72-83).  Errors arrive as
+// STORM::StormError, after reportError, like the serial manager
+// (manager/MonteCarloManagerSerial.hpp:458-462).
+//
+// What the plug-ins keep private -- the opacity and EOS models, a boundary's
+// temperatures, the comb's Nmin / factor, the RNG seed, and the cell vectors
+// RadiationIMC holds by reference -- is handed over in a CudaIMCBinding.
+// bind_parameters() copies the public RadiationIMCParameters.  An unsupported
+// plug-in is rejected with StormError; there is no CPU fallback.
+//
+// Include after the reference headers (Particle, MonteCarloPhysics,
+// PopulationControl, BoundaryCondition, MonteCarloConfig, RadiationCell).
+#ifndef STORM_MONTE_CARLO_MANAGER_CUDA_HPP
+#define STORM_MONTE_CARLO_MANAGER_CUDA_HPP
+
+#include <algorithm>
+#include <array>
+#include <chrono>
+#include <cmath>
+#include <cstring>
+#include <functional>
+#include <iostream>
+#include <limits>
+#include <memory>
+#include <set>
+#include <string>
+#include <vector>
+
+#include "../storm_cuda.h"
+
+namespace STORM {
+
+template <typename CellT, typename ExtensivesT>
+struct CudaIMCBinding {
+    // the vectors RadiationIMC was constructed with (it mutates them in place)
+    std::vector<CellT> *cells = nullptr;
+    std::vector<ExtensivesT> *extensives = nullptr;
+    // opacity plug-in lowered to a device descriptor
+    int opacityKind = STORM_OPACITY_CELL_TABLE;
+    std::function<double(std::size_t)> planckOpacity;       // CELL_TABLE: sigma_a of cell i
+    std::function<double(std::size_t)> scatteringOpacity;   // CELL_TABLE: sigma_s of cell i (empty = 0)
+    double kP0 = 0, kR0 = 0, alpha = 0, beta = 0, tFloor = 1.0, cap = 0;
+    std::vector<double> densityFactor;                        // POWER_LAW: rho^beta per cell
+    // EOS plug-in
+    int eosKind = STORM_EOS_LINEAR;
+    double cvPerMass = 1.0, eosF = 1.0, eosBeta = 1.0, eosMu = 0.0;
+    // boundary plug-in as per-box-face actions, GetBoxFaces() order
+    std::array<StormBoxFace, 6> faces{};
+    bool escapeWithoutCheck = false;
+    // RadiationIMCParameters<1> (copy with bind_parameters)
+    std::size_t newPhotonsPerCell = 1;
+    bool withRandomWalk = false, noHydroFeedback = false;
+    double rwMinCellOpticalDepth = 25.0, rwMinParticleOpticalDepth = 5.0;
+    // CombPopulationControl(grid, Nmin, factor)
+    bool combEnabled = true;
+    std::size_t combNmin = 20;
+    double combFactor = 2.0;
+    // constants the caller's physics uses (units::*)
+    double clight = 0, arad = 0, sigmaSB = 0, kevKelvin = 0;
+    // engine
+    std::uint64_t seed = 42;
+    int precision = STORM_PRECISION_FP64;
+    int device = 0;
+    std::uint32_t segmentsPerVisit = 0;
+
+    template <typename ParametersT>
+    void bind_parameters(const ParametersT &p) {
+        newPhotonsPerCell = p.newPhotonsPerCell;
+        withRandomWalk = p.withRandomWalk;
+        noHydroFeedback = p.noHydroFeedback;
+        rwMinCellOpticalDepth = p.rwMinCellOpticalDepth;
+        rwMinParticleOpticalDepth = p.rwMinParticleOpticalDepth;
+        if (p.withHydro || p.withMultigroupOpacity || p.withDDMC || p.MMC || p.withCompton) {
+            StormError eo("MonteCarloManagerCUDA: RadiationIMC option not supported on the device path");
+            eo.addEntry("withHydro", p.withHydro);
+            eo.addEntry("withMultigroupOpacity", p.withMultigroupOpacity);
+            eo.addEntry("withDDMC", p.withDDMC);
+            throw eo;
+        }
+    }
+};
+
+namespace cuda_detail {
+
+inline void check(int rc, StormHandle *h, const char *what) {
+    if (rc == STORM_OK) return;
+    StormError eo(std::string("MonteCarloManagerCUDA: ") + what + " failed");
+    eo.addEntry("Status", storm_cuda_status_string(rc));
+    if (h) {
+        std::int32_t derr = 0;
+        std::uint64_t cell = 0, particle = 0;
+        char msg[256] = {0};
+        storm_cuda_last_error(h, &derr, &cell, &particle, msg, sizeof(msg));
+        eo.addEntry("Device error", derr);
+        eo.addEntry("Cell index", cell);
+        eo.addEntry("Particle", particle);
+        eo.addEntry("Message", msg);
+    }
+    throw eo;
+}
+
+// Rectilinear edges of a Cartesian Grid through the reference Grid API: every
+// face centroid lies on a plane x = const, y = const or z = const.
+template <typename Grid>
+std::array<std::vector<double>, 3> rectilinear_edges(const Grid &grid) {
+    std::array<std::set<double>, 3> planes;
+    const std::size_t N = grid.GetPointNo();
+    for (std::size_t c = 0; c < N; ++c) {
+        for (const std::size_t &f : grid.GetCellFaces(c)) {
+            auto n = grid.Normal(f);
+            auto cm = grid.FaceCM(f);
+            double a[3] = {std::fabs(n.x), std::fabs(n.y), std::fabs(n.z)};
+            int axis = (a[0] >= a[1] && a[0] >= a[2]) ? 0 : (a[1] >= a[2] ? 1 : 2);
+            planes[axis].insert(axis == 0 ? cm.x : (axis == 1 ? cm.y : cm.z));
+        }
+    }
+    std::array<std::vector<double>, 3> e;
+    for (int a = 0; a < 3; ++a) e[a].assign(planes[a].begin(), planes[a].end());
+    const std::size_t nx = e[0].size() - 1, ny = e[1].size() - 1, nz = e[2].size() - 1;
+    if (e[0].size() < 2 || e[1].size() < 2 || e[2].size() < 2 || nx * ny * nz != N) {
+        StormError eo("MonteCarloManagerCUDA: the grid is not a rectilinear Cartesian grid");
+        eo.addEntry("Cells", N);
+        throw eo;
+    }
+    for (std::size_t c = 0; c < N; ++c) {   // cell index = i + nx (j + ny k)
+        std::size_t i = c % nx, j = (c / nx) % ny, k = c / (nx * ny);
+        auto p = grid.GetMeshPoint(c);
+        if (!(p.x > e[0][i] && p.x < e[0][i + 1] && p.y > e[1][j] && p.y < e[1][j + 1] && p.z > e[2][k] &&
+              p.z < e[2][k + 1])) {
+            StormError eo("MonteCarloManagerCUDA: cell ordering is not i + nx*(j + ny*k)");
+            eo.addEntry("Cell", c);
+            throw eo;
+        }
+    }
+    return e;
+}
+
+}  // namespace cuda_detail
+
+template <typename T, typename Grid, typename CellT = RadiationCell, typename ExtensivesT = SimpleExtensives>
+class MonteCarloManagerCUDA {
+    using MCParticle = Particle<T, Grid>;
+
+public:
+    MonteCarloManagerCUDA(const Grid &grid, const std::shared_ptr<MonteCarloPhysics<T, Grid>> &physics,
+                          const std::shared_ptr<PopulationControl<T, Grid>> &populationControl,
+                          const std::shared_ptr<BoundaryCondition<T, Grid>> &boundaryCondition,
+                          const CudaIMCBinding<CellT, ExtensivesT> &binding,
+                          const MonteCarloConfig &config = MonteCarloConfig())
+        : grid_(grid), physics_(physics), populationControl_(populationControl), boundary_(boundaryCondition),
+          binding_(binding), config_(config) {
+        if (!physics_ || !populationControl_ || !boundary_)
+            throw StormError("MonteCarloManagerCUDA: physics, population control and boundary are required");
+        if (!binding_.cells || !binding_.extensives)
+            throw StormError("MonteCarloManagerCUDA: the binding needs the cells and extensives vectors");
+        create();
+    }
+    ~MonteCarloManagerCUDA() {
+        if (h_) storm_cuda_destroy(h_);
+    }
+    MonteCarloManagerCUDA(const MonteCarloManagerCUDA &) = delete;
+    MonteCarloManagerCUDA &operator=(const MonteCarloManagerCUDA &) = delete;
+
+    // MonteCarloManagerSerial::step (manager/MonteCarloManagerSerial.hpp:386-469)
+    std::vector<MCParticle> step(std::vector<MCParticle> &&particleList, dt_t fullDt) {
+        try {
+            auto t0 = std::chrono::steady_clock::now();
+            upload_cells();
+            upload_census(particleList);
+            std::vector<MCParticle>().swap(particleList);
+            StormStepStats st{};
+            cuda_detail::check(storm_cuda_step(h_, fullDt, &st), h_, "storm_cuda_step");
+            download_cells();
+            std::vector<MCParticle> out = download_census();
+            initialParticleCount_ = st.census_in;
+            preStepParticleCount_ = st.emitted_cells + st.emitted_faces;
+            startParticleCount_ = initialParticleCount_ + preStepParticleCount_;
+            endParticleCount_ = st.census_out;
+            pureComputeTime_ = st.step_ms * 1e-3;
+            wallTime_ = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+            return out;
+        } catch (const StormError &eo) {
+            reportError(eo);
+            throw;
+        }
+    }
+
+    inline const std::vector<std::size_t> &GetCellsStepsCounters(void) const { return cellsStepsCounters_; }
+    inline std::vector<std::size_t> &GetCellsStepsCounters(void) { return cellsStepsCounters_; }
+    inline std::size_t GetStartParticleCount(void) const { return startParticleCount_; }
+    inline std::size_t GetInitialParticleCount(void) const { return initialParticleCount_; }
+    inline std::size_t GetPreStepParticleCount(void) const { return preStepParticleCount_; }
+    inline std::size_t GetEndParticleCount(void) const { return endParticleCount_; }
+    inline double GetPureComputeTime(void) const { return pureComputeTime_; }
+    inline double GetWallTime(void) const { return wallTime_; }
+    inline std::size_t GetHandlerMemoryBytes(void) const {
+        std::uint64_t b = 0;
+        storm_cuda_memory_bytes(h_, &b);
+        return b;
+    }
+    // Erad_time_avg_ of the last step (RadiationIMC::getEradTimeAvg, radiation/RadiationIMC.hpp:431)
+    inline const std::vector<double> &getEradTimeAvg(void) const { return eradAvg_; }
+    inline const std::vector<double> &getPlanckOpacities(void) const { return sigmaA_; }
+    inline const std::vector<double> &getFactorFleck(void) const { return fleck_; }
+    // the boundary's drive temperature (MarshakBoundary::SetTemperature, SideTemperature::SetTemperature)
+    void SetFaceTemperature(int face, double temperature) {
+        cuda_detail::check(storm_cuda_set_face_temperature(h_, face, temperature), h_, "set_face_temperature");
+    }
+
+private:
+    void create() {
+        auto edges = cuda_detail::rectilinear_edges(grid_);
+        const std::size_t N = grid_.GetPointNo();
+        auto &cells = *binding_.cells;
+        auto &ext = *binding_.extensives;
+        if (cells.size() < N || ext.size() < N) throw StormError("MonteCarloManagerCUDA: cells/extensives too small");
+        std::vector<double> temp(N), mass(N), eint(N), ceint(N), sa, ss;
+        for (std::size_t i = 0; i < N; ++i) {
+            temp[i] = cells[i].temperature;
+            mass[i] = ext[i].mass;
+            eint[i] = ext[i].internal_energy;
+            ceint[i] = cells[i].internalEnergy;
+        }
+        StormProblemDesc d;
+        std::memset(&d, 0, sizeof(d));
+        d.abi_version = STORM_CUDA_ABI_VERSION;
+        d.precision = binding_.precision;
+        d.nx = static_cast<std::uint32_t>(edges[0].size() - 1);
+        d.ny = static_cast<std::uint32_t>(edges[1].size() - 1);
+        d.nz = static_cast<std::uint32_t>(edges[2].size() - 1);
+        d.x_edges = edges[0].data();
+        d.y_edges = edges[1].data();
+        d.z_edges = edges[2].data();
+        d.temperature = temp.data();
+        d.mass = mass.data();
+        d.internal_energy = eint.data();
+        d.cell_internal_energy = ceint.data();
+        d.opacity_kind = binding_.opacityKind;
+        if (binding_.opacityKind == STORM_OPACITY_CELL_TABLE) {
+            if (!binding_.planckOpacity) throw StormError("MonteCarloManagerCUDA: CELL_TABLE opacity needs planckOpacity");
+            sa.resize(N);
+            ss.assign(N, 0.0);
+            for (std::size_t i = 0; i < N; ++i) {
+                sa[i] = binding_.planckOpacity(i);
+                if (binding_.scatteringOpacity) ss[i] = binding_.scatteringOpacity(i);
+            }
+            d.sigma_a = sa.data();
+            d.sigma_s = ss.data();
+        }
+        d.kP0 = binding_.kP0; d.kR0 = binding_.kR0; d.alpha = binding_.alpha; d.beta = binding_.beta;
+        d.t_floor = binding_.tFloor;
+        d.cap = binding_.cap;
+        d.density_factor = binding_.densityFactor.empty() ? nullptr : binding_.densityFactor.data();
+        d.eos_kind = binding_.eosKind;
+        d.cv_per_mass = binding_.cvPerMass;
+        d.eos_f = binding_.eosF; d.eos_beta = binding_.eosBeta; d.eos_mu = binding_.eosMu;
+        for (int f = 0; f < 6; ++f) d.faces[f] = binding_.faces[f];
+        d.escape_without_check = binding_.escapeWithoutCheck;
+        d.new_photons_per_cell = binding_.newPhotonsPerCell;
+        d.with_random_walk = binding_.withRandomWalk;
+        d.no_hydro_feedback = binding_.noHydroFeedback;
+        d.rw_min_cell_optical_depth = binding_.rwMinCellOpticalDepth;
+        d.rw_min_particle_optical_depth = binding_.rwMinParticleOpticalDepth;
+        d.comb_enabled = binding_.combEnabled;
+        d.comb_nmin = binding_.combNmin;
+        d.comb_factor = binding_.combFactor;
+        d.clight = binding_.clight; d.arad = binding_.arad; d.sigma_sb = binding_.sigmaSB; d.kev_kelvin = binding_.kevKelvin;
+        d.seed = binding_.seed;
+        // MonteCarloConfig sizes the serial manager's buffer; here it seeds the bank capacity
+        d.capacity = config_.initialBufferSize > 5000 ? config_.initialBufferSize : 0;
+        d.segments_per_visit = binding_.segmentsPerVisit;
+        d.per_cell_segment_counters = 1;
+        d.device = binding_.device;
+        cuda_detail::check(storm_cuda_create(&d, &h_), nullptr, "storm_cuda_create");
+        N_ = N;
+        cellsStepsCounters_.assign(N, 0);
+    }
+
+    void upload_cells() {
+        auto &cells = *binding_.cells;
+        auto &ext = *binding_.extensives;
+        hostT_.resize(N_); hostE_.resize(N_); hostCE_.resize(N_);
+        for (std::size_t i = 0; i < N_; ++i) {
+            hostT_[i] = cells[i].temperature;
+            hostE_[i] = ext[i].internal_energy;
+            hostCE_[i] = cells[i].internalEnergy;
+        }
+        cuda_detail::check(storm_cuda_set_cell_state(h_, hostT_.data(), hostE_.data(), hostCE_.data()), h_,
+                           "set_cell_state");
+    }
+
+    void upload_census(const std::vector<MCParticle> &ps) {
+        const std::size_t n = ps.size();
+        std::vector<double> x(n), y(n), z(n), vx(n), vy(n), vz(n), t(n), w(n), w0(n);
+        std::vector<std::uint32_t> cell(n);
+        for (std::size_t q = 0; q < n; ++q) {
+            const MCParticle &p = ps[q];
+            x[q] = p.location.x; y[q] = p.location.y; z[q] = p.location.z;
+            vx[q] = p.velocity.x; vy[q] = p.velocity.y; vz[q] = p.velocity.z;
+            t[q] = p.timeLeft; w[q] = p.weight; w0[q] = p.initialWeight;
+            cell[q] = static_cast<std::uint32_t>(p.cellIndex);
+        }
+        StormParticlesSoA s{x.data(), y.data(), z.data(), vx.data(), vy.data(), vz.data(), t.data(), w.data(),
+                            w0.data(), cell.data(), nullptr, n};
+        cuda_detail::check(storm_cuda_set_census(h_, &s), h_, "set_census");
+    }
+
+    std::vector<MCParticle> download_census() {
+        std::uint64_t n = 0;
+        cuda_detail::check(storm_cuda_census_count(h_, &n), h_, "census_count");
+        std::vector<double> x(n), y(n), z(n), vx(n), vy(n), vz(n), t(n), w(n), w0(n);
+        std::vector<std::uint32_t> cell(n);
+        std::vector<std::uint64_t> id(n);
+        StormParticlesSoA s{x.data(), y.data(), z.data(), vx.data(), vy.data(), vz.data(), t.data(), w.data(),
+                            w0.data(), cell.data(), id.data(), n};
+        std::uint64_t got = 0;
+        cuda_detail::check(storm_cuda_get_census(h_, &s, n, &got), h_, "get_census");
+        std::vector<MCParticle> out(n);
+        for (std::size_t q = 0; q < n; ++q) {
+            MCParticle &p = out[q];
+            p.location = T(x[q], y[q], z[q]);
+            p.velocity = T(vx[q], vy[q], vz[q]);
+            p.timeLeft = t[q]; p.weight = w[q]; p.initialWeight = w0[q];
+            p.cellIndex = cell[q];
+            p.frequency = 0;
+            p.id = std::numeric_limits<std::size_t>::max();   // ids are reassigned at the next step, as comb copies are
+        }
+        return out;
+    }
+
+    // RadiationIMC::postStep's writes into the caller's state (:1887-2029)
+    void download_cells() {
+        std::vector<double> temp(N_), eint(N_), eradCensus(N_);
+        std::vector<std::uint64_t> segs(N_);
+        eradAvg_.resize(N_); sigmaA_.resize(N_); fleck_.resize(N_);
+        cuda_detail::check(storm_cuda_get_cell_arrays(h_, temp.data(), eint.data(), eradAvg_.data(), eradCensus.data(),
+                                                      sigmaA_.data(), fleck_.data(), segs.data()),
+                           h_, "get_cell_arrays");
+        auto &cells = *binding_.cells;
+        auto &ext = *binding_.extensives;
+        for (std::size_t i = 0; i < N_; ++i) {
+            cellsStepsCounters_[i] = segs[i];
+            ext[i].internal_energy = eint[i];
+            cells[i].temperature = temp[i];
+            if (!binding_.noHydroFeedback) cells[i].internalEnergy = eint[i];   // synchronizeMaterialCell, radiation/RadiationIMC.hpp:831-848
+            ext[i].Erad = eradCensus[i];
+            cells[i].Erad = ext[i].mass > 0.0 ? eradCensus[i] / ext[i].mass : 0.0;
+        }
+    }
+
+    const Grid &grid_;
+    std::shared_ptr<MonteCarloPhysics<T, Grid>> physics_;
+    std::shared_ptr<PopulationControl<T, Grid>> populationControl_;
+    std::shared_ptr<BoundaryCondition<T, Grid>> boundary_;
+    CudaIMCBinding<CellT, ExtensivesT> binding_;
+    MonteCarloConfig config_;
+    StormHandle *h_ = nullptr;
+    std::size_t N_ = 0;
+    std::vector<std::size_t> cellsStepsCounters_;
+    std::vector<double> hostT_, hostE_, hostCE_, eradAvg_, sigmaA_, fleck_;
+    std::size_t startParticleCount_ = 0, initialParticleCount_ = 0, preStepParticleCount_ = 0, endParticleCount_ = 0;
+    double pureComputeTime_ = 0.0, wallTime_ = 0.0;
+};
+
+}  // namespace STORM
+
+#endif

@@ -120,27 +120,46 @@ __device__ __forceinline__ double stream_uniform(uint32_t k0, uint32_t k1, uint3
     return (draw & 1u) ? u52(o[2], o[3]) : u52(o[0], o[1]);
 }
 
-// The engine's per-particle stream: counter (draw >> 1, pid, step, tag).
+// Float uniform on the open interval from the top 23 bits of a Philox word:
+// (w >> 9) * 2^-23 + 2^-24, built in the exponent-1 binade so no conversion
+// instruction is issued.  (1 + k 2^-23) - (1 - 2^-24) is exact (Sterbenz).
+__device__ __forceinline__ float u23(uint32_t w) {
+    return __uint_as_float(0x3f800000u | (w >> 9)) - 0x1.fffffep-1f;
+}
+
+// The engine's per-particle stream: counter (draw >> 1, pid, step, tag).  The
+// four words of the current Philox block are cached; a draw converts only the
+// pair it uses.  rawf() reads the same draw as raw() rounded to the 2^-23 bin
+// its high word selects, so the FP32 form follows the FP64 form's stream.
 struct PhiloxRng {
     uint32_t k0, k1, tag, step, pid, draw;
     uint32_t block;
-    double c0, c1;
+    uint32_t w[4];
     __device__ __forceinline__ void init(uint32_t kk0, uint32_t kk1, uint32_t t, uint32_t s, uint32_t p, uint32_t d) {
         k0 = kk0; k1 = kk1; tag = t; step = s; pid = p; draw = d; block = 0xffffffffu;
     }
-    __device__ __forceinline__ double raw() {
+    __device__ __forceinline__ void fetch() {
         uint32_t b = draw >> 1;
         if (b != block) {
-            uint32_t o[4];
-            philox4x32_10(b, pid, step, tag, k0, k1, o);
-            c0 = u52(o[0], o[1]);
-            c1 = u52(o[2], o[3]);
+            philox4x32_10(b, pid, step, tag, k0, k1, w);
             block = b;
         }
-        double u = (draw & 1u) ? c1 : c0;
+    }
+    __device__ __forceinline__ double raw() {
+        fetch();
+        const bool odd = draw & 1u;
+        const double u = u52(odd ? w[2] : w[0], odd ? w[3] : w[1]);
         ++draw;
         return u;
     }
+    __device__ __forceinline__ float rawf() {
+        fetch();
+        float u = u23((draw & 1u) ? w[2] : w[0]);
+        ++draw;
+        return u;
+    }
+    // a draw whose value is not used
+    __device__ __forceinline__ void skip() { ++draw; }
     // RadiationIMC::randomUnitOpen (radiation/RadiationIMC.hpp:700-713); a no-op on
     // these uniforms, kept for the shared code path.
     __device__ __forceinline__ double open() {
@@ -163,6 +182,10 @@ struct TapeRng {
         double v = raw();
         return v <= 0.0 ? DBL_MIN : (v >= 1.0 ? ONE_BELOW : v);
     }
+    __device__ __forceinline__ float rawf() {
+        return fminf(fmaxf(static_cast<float>(raw()), 0x1p-24f), 0x1.fffffep-1f);
+    }
+    __device__ __forceinline__ void skip() { (void)raw(); }
     __device__ __forceinline__ bool exhausted() const { return over; }
 };
 
@@ -241,17 +264,26 @@ __device__ __forceinline__ void isotropic(RNG &rng, double c, double &vx, double
 // ------------------------------------------------------------------ tallies
 // Sink for the two per-cell tallies a segment writes: the material energy
 // (extensives[cell].internal_energy) and the time-integrated radiation energy
-// (Erad_time_avg_[cell]).
-struct AtomicTally {
-    double *eint, *erad;
-    double depSum;
-    __device__ __forceinline__ void mat(uint32_t c, double v) { atomicAdd(eint + c, v); depSum += v; }
-    __device__ __forceinline__ void rad(uint32_t c, double v) { atomicAdd(erad + c, v); }
-};
+// (Erad_time_avg_[cell]).  LocalTally sums one segment's deposits (replay).
 struct LocalTally {
     double mat_, rad_;
     __device__ __forceinline__ void mat(uint32_t, double v) { mat_ += v; }
     __device__ __forceinline__ void rad(uint32_t, double v) { rad_ += v; }
+};
+// The transport kernels' tally: every segment adds its deposits to the cell with
+// fire-and-forget atomics (RED) and counts itself for the per-cell segment
+// counters.  (Summing a run of segments in one cell in registers first costs
+// more in register spills than it saves in atomics.)
+struct SegmentTally {
+    double *eint, *erad;
+    uint32_t *segs;        // NULL: no per-cell counters
+    double depSum;
+    __device__ __forceinline__ void init(double *e, double *a, uint32_t *sc) {
+        eint = e; erad = a; segs = sc; depSum = 0.0;
+    }
+    __device__ __forceinline__ void enter(uint32_t c) { if (segs) atomicAdd(segs + c, 1u); }
+    __device__ __forceinline__ void mat(uint32_t c, double v) { atomicAdd(eint + c, v); depSum += v; }
+    __device__ __forceinline__ void rad(uint32_t c, double v) { atomicAdd(erad + c, v); }
 };
 
 // ------------------------------------------------------------------ Random Walk jump
@@ -482,7 +514,7 @@ __device__ inline PhysOut physics_step(const Ctx &C, Track &T, RNG &rng, TALLY &
         o.next = next;
         if (next == OUTSIDE) o.ghost = C.ncells + face_index(C, i, j, k, face);
     } else if (best == 1) {
-        (void)rng.open();   // event-type draw; both branches re-scatter isotropically
+        rng.skip();   // event-type draw; both branches re-scatter isotropically
         isotropic(rng, c, p.vx, p.vy, p.vz);
         T.speed = vnorm(p.vx, p.vy, p.vz);
         o.status = NO_CELL_MOVE;
@@ -503,32 +535,29 @@ struct Track32 {
 
 __device__ __forceinline__ float clampf(float v, float h) { return fminf(fmaxf(v, -h), h); }
 
-// uniform in (0,1) as float that is never 0 or 1
-__device__ __forceinline__ float to_open_float(double u) { return fminf(fmaxf(static_cast<float>(u), 0x1p-40f), 0x1.fffffep-1f); }
-
 // One segment plus the manager's handling, in the FP32-tracking form.  Same
 // events, same draws per event and the same FP64 tally updates as the FP64
 // form; distances, the face search and the collision distance are FP32 in the
 // cell's own frame, so precision follows the cell size, not the domain.
+//
+// Face search: along each axis the exit plane is n_a = h_a - sign(u_a) q_a away
+// at speed |u_a|; the nearest exit is found by cross-multiplied comparisons
+// (n_a |u_b| < n_b |u_a|, first smallest wins, an axis with u_a = 0 never
+// wins) and only the winner is divided.
 template <class RNG, class TALLY>
 __device__ inline int segment32(const Ctx &C, Track32 &T, RNG &rng, TALLY &tal, int &usedRW, int &err) {
     const uint32_t cell = T.cell;
     const float hx = C.hx[T.i], hy = C.hy[T.j], hz = C.hz[T.k];
-    float sF = CUDART_INF_F;
-    int face = -1;
-    if (T.ux != 0.0f) {
-        float s = fmaxf((copysignf(hx, T.ux) - T.qx) / T.ux, 0.0f);
-        if (s < sF) { sF = s; face = T.ux > 0.0f ? 1 : 0; }
-    }
-    if (T.uy != 0.0f) {
-        float s = fmaxf((copysignf(hy, T.uy) - T.qy) / T.uy, 0.0f);
-        if (s < sF) { sF = s; face = T.uy > 0.0f ? 3 : 2; }
-    }
-    if (T.uz != 0.0f) {
-        float s = fmaxf((copysignf(hz, T.uz) - T.qz) / T.uz, 0.0f);
-        if (s < sF) { sF = s; face = T.uz > 0.0f ? 5 : 4; }
-    }
+    const float ax = fabsf(T.ux), ay = fabsf(T.uy), az = fabsf(T.uz);
+    const float nxp = ax > 0.0f ? fmaxf(hx - (T.ux > 0.0f ? T.qx : -T.qx), 0.0f) : 1.0f;
+    const float nyp = ay > 0.0f ? fmaxf(hy - (T.uy > 0.0f ? T.qy : -T.qy), 0.0f) : 1.0f;
+    const float nzp = az > 0.0f ? fmaxf(hz - (T.uz > 0.0f ? T.qz : -T.qz), 0.0f) : 1.0f;
+    float bn = nxp, bd = ax;
+    int face = ax > 0.0f ? (T.ux > 0.0f ? 1 : 0) : -1;
+    if (ay > 0.0f && (face < 0 || nyp * bd < bn * ay)) { bn = nyp; bd = ay; face = T.uy > 0.0f ? 3 : 2; }
+    if (az > 0.0f && (face < 0 || nzp * bd < bn * az)) { bn = nzp; bd = az; face = T.uz > 0.0f ? 5 : 4; }
     if (face < 0) { err = STORM_DERR_NO_FACE; return OUT_ERROR; }
+    const float sF = __fdividef(bn, bd);
     const double c = C.clight;
 
     if (C.withRW && C.rwElig[cell]) {
@@ -557,7 +586,7 @@ __device__ inline int segment32(const Ctx &C, Track32 &T, RNG &rng, TALLY &tal, 
     }
 
     const float4 cp = C.phys32[cell];
-    const float sC = cp.x * (-__logf(to_open_float(rng.open())));
+    const float sC = cp.x * (-__logf(rng.rawf()));
     const float sL = static_cast<float>(T.t * c);
     int best = 0;
     float ds = sF;
@@ -581,9 +610,9 @@ __device__ inline int segment32(const Ctx &C, Track32 &T, RNG &rng, TALLY &tal, 
     }
     if (best == 2) return OUT_CENSUS;
     if (best == 1) {
-        (void)rng.open();
-        const float theta = 6.2831853f * to_open_float(rng.raw());
-        const float cosT = 2.0f * static_cast<float>(rng.raw()) - 1.0f;
+        rng.skip();
+        const float theta = 6.2831853f * rng.rawf();
+        const float cosT = 2.0f * rng.rawf() - 1.0f;
         const float sinT = sqrtf(fmaxf(0.0f, 1.0f - cosT * cosT));
         float st, ct;
         __sincosf(theta, &st, &ct);

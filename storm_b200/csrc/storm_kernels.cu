@@ -656,80 +656,40 @@ __global__ void k_emit_faces(Ctx C, FaceSources F, uint64_t total, Bank b, uint3
 }
 
 // ------------------------------------------------------------------ transport
-// One bank visit of the HandleAll loop (manager/MonteCarloManagerSerial.hpp:267-383):
-// every active particle runs up to K segments in registers; survivors are
-// compacted into the next bank and census particles appended to the census bank
-// (warp ballot + one atomic per warp).  Statistics go to per-block shared
-// counters when the event happens, so no thread holds accumulators.
 struct BlockStats {
     unsigned long long segments, rwSteps, escaped, cutoff, census;
     double eDeposited, eEscaped, eCensusPre;
 };
 
-template <int MINB>
-__global__ void __launch_bounds__(256, MINB) k_transport(Ctx C, Bank in, const uint32_t *nIn, Bank out,
-                                                          uint32_t *nOut, CensusBank cen, uint32_t *nCen, uint32_t K,
-                                                          DevStats *st) {
-    __shared__ BlockStats bs;
+__device__ __forceinline__ void block_stats_zero(BlockStats &bs) {
     if (threadIdx.x == 0) bs = BlockStats{0, 0, 0, 0, 0, 0.0, 0.0, 0.0};
     __syncthreads();
-    const uint32_t n = *nIn;
+}
+
+// One warp's share of the step statistics: reduced over the warp with shuffles,
+// then one shared atomic per quantity.  Every lane of the warp calls it.
+__device__ __forceinline__ void warp_stats(BlockStats &bs, uint32_t segs, uint32_t rw, double dep, int outcome,
+                                           double w) {
     const unsigned lane = threadIdx.x & 31;
-    for (uint32_t base = blockIdx.x * blockDim.x; base < n; base += gridDim.x * blockDim.x) {
-        const uint32_t idx = base + threadIdx.x;
-        const bool active = idx < n;
-        Track T;
-        PartReg &p = T.p;
-        uint32_t pid = 0, draw = 0;
-        int outcome = OUT_CONTINUE;
-        if (active) {
-            load_part(in, idx, p);
-            pid = in.pid[idx];
-            draw = in.draw[idx];
-            track_begin(C, T);
-            PhiloxRng rng;
-            rng.init(C.seedLo, C.seedHi, TAG_TRANSPORT, C.step, pid, draw);
-            AtomicTally tal{C.eint, C.eradAvg, 0.0};
-            uint32_t s = 0, rw = 0;
-            for (; s < K;) {
-                if (C.perCellCounters) atomicAdd(C.segs + p.cell, 1u);
-                ++s;
-                const uint32_t cell0 = p.cell;
-                PhysOut o = physics_step(C, T, rng, tal);
-                if (o.errCode) {
-                    raise_error(C, o.errCode, cell0, pid);
-                    outcome = OUT_ERROR;
-                    break;
-                }
-                rw += o.usedRW;
-                outcome = manager_handle(C, T, o);
-                if (outcome != OUT_CONTINUE) {
-                    if (outcome == OUT_ERROR) raise_error(C, STORM_DERR_NOT_ON_BOUNDARY, cell0, pid);
-                    break;
-                }
-            }
-            draw = rng.draw;
-            atomicAdd(&bs.segments, static_cast<unsigned long long>(s));
-            if (rw) atomicAdd(&bs.rwSteps, static_cast<unsigned long long>(rw));
-            if (tal.depSum != 0.0) atomicAdd(&bs.eDeposited, tal.depSum);
-            if (outcome == OUT_ESCAPE) { atomicAdd(&bs.escaped, 1ull); atomicAdd(&bs.eEscaped, p.w); }
-            else if (outcome == OUT_CUTOFF) { atomicAdd(&bs.cutoff, 1ull); }
-            else if (outcome == OUT_CENSUS) { atomicAdd(&bs.census, 1ull); atomicAdd(&bs.eCensusPre, p.w); }
-        }
-        const bool keep = active && outcome == OUT_CONTINUE;
-        const bool cens = active && outcome == OUT_CENSUS;
-        const unsigned mK = __ballot_sync(FULL, keep), mC = __ballot_sync(FULL, cens);
-        uint32_t bK = 0, bC = 0;
-        if (lane == 0) {
-            if (mK) bK = atomicAdd(nOut, __popc(mK));
-            if (mC) bC = atomicAdd(nCen, __popc(mC));
-        }
-        bK = __shfl_sync(FULL, bK, 0);
-        bC = __shfl_sync(FULL, bC, 0);
-        const unsigned lt = lanemask_lt();
-        if (keep) store_part(out, bK + __popc(mK & lt), p, pid, draw);
-        if (cens) census_store64(cen, bC + __popc(mC & lt), p, pid, draw);
+    const uint32_t s = warp_sum(segs);
+    const unsigned mE = __ballot_sync(FULL, outcome == OUT_ESCAPE);
+    const unsigned mX = __ballot_sync(FULL, outcome == OUT_CUTOFF);
+    const unsigned mC = __ballot_sync(FULL, outcome == OUT_CENSUS);
+    const uint32_t r = __any_sync(FULL, rw != 0) ? warp_sum(rw) : 0u;
+    const double d = __any_sync(FULL, dep != 0.0) ? warp_sum(dep) : 0.0;
+    const double eE = mE ? warp_sum(outcome == OUT_ESCAPE ? w : 0.0) : 0.0;
+    const double eC = mC ? warp_sum(outcome == OUT_CENSUS ? w : 0.0) : 0.0;
+    if (lane == 0) {
+        if (s) atomicAdd(&bs.segments, static_cast<unsigned long long>(s));
+        if (r) atomicAdd(&bs.rwSteps, static_cast<unsigned long long>(r));
+        if (d != 0.0) atomicAdd(&bs.eDeposited, d);
+        if (mE) { atomicAdd(&bs.escaped, static_cast<unsigned long long>(__popc(mE))); atomicAdd(&bs.eEscaped, eE); }
+        if (mX) atomicAdd(&bs.cutoff, static_cast<unsigned long long>(__popc(mX)));
+        if (mC) { atomicAdd(&bs.census, static_cast<unsigned long long>(__popc(mC))); atomicAdd(&bs.eCensusPre, eC); }
     }
+}
+
+__device__ __forceinline__ void block_stats_flush(const BlockStats &bs, DevStats *st) {
     __syncthreads();
     if (threadIdx.x == 0) {
         if (bs.segments) atomicAdd(&st->segments, bs.segments);
@@ -743,85 +703,16 @@ __global__ void __launch_bounds__(256, MINB) k_transport(Ctx C, Bank in, const u
     }
 }
 
-// The same bank visit in the FP32-tracking form.
-template <int MINB>
-__global__ void __launch_bounds__(256, MINB) k_transport32(Ctx C, Bank in, const uint32_t *nIn, Bank out,
-                                                            uint32_t *nOut, CensusBank cen, uint32_t *nCen, uint32_t K,
-                                                            DevStats *st) {
-    __shared__ BlockStats bs;
-    if (threadIdx.x == 0) bs = BlockStats{0, 0, 0, 0, 0, 0.0, 0.0, 0.0};
-    __syncthreads();
-    const uint32_t n = *nIn;
-    const unsigned lane = threadIdx.x & 31;
-    for (uint32_t base = blockIdx.x * blockDim.x; base < n; base += gridDim.x * blockDim.x) {
-        const uint32_t idx = base + threadIdx.x;
-        const bool active = idx < n;
-        Track32 T;
-        uint32_t pid = 0, draw = 0;
-        int outcome = OUT_CONTINUE;
-        if (active) {
-            load32(in, idx, T);
-            cell_ijk(C, T.cell, T.i, T.j, T.k);
-            pid = in.pid[idx];
-            draw = in.draw[idx];
-            PhiloxRng rng;
-            rng.init(C.seedLo, C.seedHi, TAG_TRANSPORT, C.step, pid, draw);
-            AtomicTally tal{C.eint, C.eradAvg, 0.0};
-            uint32_t s = 0, rw = 0;
-            for (; s < K;) {
-                if (C.perCellCounters) atomicAdd(C.segs + T.cell, 1u);
-                ++s;
-                const uint32_t cell0 = T.cell;
-                int usedRW = 0, err = 0;
-                outcome = segment32(C, T, rng, tal, usedRW, err);
-                rw += usedRW;
-                if (outcome != OUT_CONTINUE) {
-                    if (outcome == OUT_ERROR) raise_error(C, err ? err : STORM_DERR_NOT_ON_BOUNDARY, cell0, pid);
-                    break;
-                }
-            }
-            draw = rng.draw;
-            atomicAdd(&bs.segments, static_cast<unsigned long long>(s));
-            if (rw) atomicAdd(&bs.rwSteps, static_cast<unsigned long long>(rw));
-            if (tal.depSum != 0.0) atomicAdd(&bs.eDeposited, tal.depSum);
-            if (outcome == OUT_ESCAPE) { atomicAdd(&bs.escaped, 1ull); atomicAdd(&bs.eEscaped, T.w); }
-            else if (outcome == OUT_CUTOFF) { atomicAdd(&bs.cutoff, 1ull); }
-            else if (outcome == OUT_CENSUS) { atomicAdd(&bs.census, 1ull); atomicAdd(&bs.eCensusPre, T.w); }
-        }
-        const bool keep = active && outcome == OUT_CONTINUE;
-        const bool cens = active && outcome == OUT_CENSUS;
-        const unsigned mK = __ballot_sync(FULL, keep), mC = __ballot_sync(FULL, cens);
-        uint32_t bK = 0, bC = 0;
-        if (lane == 0) {
-            if (mK) bK = atomicAdd(nOut, __popc(mK));
-            if (mC) bC = atomicAdd(nCen, __popc(mC));
-        }
-        bK = __shfl_sync(FULL, bK, 0);
-        bC = __shfl_sync(FULL, bC, 0);
-        const unsigned lt = lanemask_lt();
-        if (keep) store32(out, bK + __popc(mK & lt), T, pid, draw);
-        if (cens) census_store32(cen, bC + __popc(mC & lt), T, pid, draw);
-    }
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        if (bs.segments) atomicAdd(&st->segments, bs.segments);
-        if (bs.rwSteps) atomicAdd(&st->rwSteps, bs.rwSteps);
-        if (bs.escaped) atomicAdd(&st->escaped, bs.escaped);
-        if (bs.cutoff) atomicAdd(&st->cutoff, bs.cutoff);
-        if (bs.census) atomicAdd(&st->census, bs.census);
-        if (bs.eDeposited != 0.0) atomicAdd(&st->eDeposited, bs.eDeposited);
-        if (bs.eEscaped != 0.0) atomicAdd(&st->eEscaped, bs.eEscaped);
-        if (bs.eCensusPre != 0.0) atomicAdd(&st->eCensusPre, bs.eCensusPre);
-    }
-}
-
-// ------------------------------------------------------------------ persistent transport
-// Both forms behind one interface for the persistent kernel.
+// The two particle forms behind one interface: the FP64 form (global FP64
+// coordinates, the reference's arithmetic) and the FP32-tracking form.
 struct Form64 {
     using T = Track;
     static __device__ __forceinline__ void load(const Ctx &C, const Bank &b, uint32_t q, T &t) {
         load_part(b, q, t.p);
         track_begin(C, t);
+    }
+    static __device__ __forceinline__ void keep(const Bank &b, uint32_t q, const T &t, uint32_t pid, uint32_t draw) {
+        store_part(b, q, t.p, pid, draw);
     }
     static __device__ __forceinline__ void store(const CensusBank &b, uint32_t q, const T &t, uint32_t pid,
                                                  uint32_t draw) {
@@ -845,6 +736,9 @@ struct Form32 {
         load32(b, q, t);
         cell_ijk(C, t.cell, t.i, t.j, t.k);
     }
+    static __device__ __forceinline__ void keep(const Bank &b, uint32_t q, const T &t, uint32_t pid, uint32_t draw) {
+        store32(b, q, t, pid, draw);
+    }
     static __device__ __forceinline__ void store(const CensusBank &b, uint32_t q, const T &t, uint32_t pid,
                                                  uint32_t draw) {
         census_store32(b, q, t, pid, draw);
@@ -859,6 +753,83 @@ struct Form32 {
     static __device__ __forceinline__ double weight(const T &t) { return t.w; }
 };
 
+// One bank visit of the HandleAll loop (manager/MonteCarloManagerSerial.hpp:267-383):
+// every active particle runs up to K segments in registers; survivors are
+// compacted into the next bank and census particles appended to the census bank
+// (warp ballot + one atomic per warp).  Step statistics are reduced per warp.
+template <class F>
+__device__ __forceinline__ void visit_bank(const Ctx &C, const Bank &in, uint32_t n, const Bank &out, uint32_t *nOut,
+                                           const CensusBank &cen, uint32_t *nCen, uint32_t K, BlockStats &bs) {
+    const unsigned lane = threadIdx.x & 31;
+    for (uint32_t base = blockIdx.x * blockDim.x; base < n; base += gridDim.x * blockDim.x) {
+        const uint32_t idx = base + threadIdx.x;
+        const bool active = idx < n;
+        typename F::T t;
+        uint32_t pid = 0, draw = 0, s = 0, rw = 0;
+        double dep = 0.0, w = 0.0;
+        int outcome = OUT_CONTINUE;
+        if (active) {
+            F::load(C, in, idx, t);
+            pid = in.pid[idx];
+            PhiloxRng rng;
+            rng.init(C.seedLo, C.seedHi, TAG_TRANSPORT, C.step, pid, in.draw[idx]);
+            SegmentTally tal;
+            tal.init(C.eint, C.eradAvg, C.perCellCounters ? C.segs : nullptr);
+            while (s < K) {
+                const uint32_t cell0 = F::cell(t);
+                tal.enter(cell0);
+                ++s;
+                int usedRW = 0, err = 0;
+                outcome = F::seg(C, t, rng, tal, usedRW, err);
+                rw += usedRW;
+                if (outcome != OUT_CONTINUE) {
+                    if (outcome == OUT_ERROR) raise_error(C, err, cell0, pid);
+                    break;
+                }
+            }
+            dep = tal.depSum;
+            draw = rng.draw;
+            w = F::weight(t);
+        }
+        warp_stats(bs, s, rw, dep, outcome, w);
+        const bool keep = active && outcome == OUT_CONTINUE;
+        const bool cens = active && outcome == OUT_CENSUS;
+        const unsigned mK = __ballot_sync(FULL, keep), mC = __ballot_sync(FULL, cens);
+        uint32_t bK = 0, bC = 0;
+        if (lane == 0) {
+            if (mK) bK = atomicAdd(nOut, __popc(mK));
+            if (mC) bC = atomicAdd(nCen, __popc(mC));
+        }
+        bK = __shfl_sync(FULL, bK, 0);
+        bC = __shfl_sync(FULL, bC, 0);
+        const unsigned lt = lanemask_lt();
+        if (keep) F::keep(out, bK + __popc(mK & lt), t, pid, draw);
+        if (cens) F::store(cen, bC + __popc(mC & lt), t, pid, draw);
+    }
+}
+
+template <int MINB>
+__global__ void __launch_bounds__(256, MINB) k_transport(Ctx C, Bank in, const uint32_t *nIn, Bank out,
+                                                          uint32_t *nOut, CensusBank cen, uint32_t *nCen, uint32_t K,
+                                                          DevStats *st) {
+    __shared__ BlockStats bs;
+    block_stats_zero(bs);
+    visit_bank<Form64>(C, in, *nIn, out, nOut, cen, nCen, K, bs);
+    block_stats_flush(bs, st);
+}
+
+// The same bank visit in the FP32-tracking form.
+template <int MINB>
+__global__ void __launch_bounds__(256, MINB) k_transport32(Ctx C, Bank in, const uint32_t *nIn, Bank out,
+                                                            uint32_t *nOut, CensusBank cen, uint32_t *nCen, uint32_t K,
+                                                            DevStats *st) {
+    __shared__ BlockStats bs;
+    block_stats_zero(bs);
+    visit_bank<Form32>(C, in, *nIn, out, nOut, cen, nCen, K, bs);
+    block_stats_flush(bs, st);
+}
+
+// ------------------------------------------------------------------ persistent transport
 // The whole HandleAll loop in one launch.  Every lane holds one history; a lane
 // whose particle reaches census, escapes or is cut off writes it out and takes
 // the next unstarted particle (one atomic per warp for the lanes that need
@@ -869,8 +840,7 @@ __global__ void __launch_bounds__(256, MINB) k_transport_refill(Ctx C, Bank in, 
                                                                  uint32_t *nCen, uint32_t burst, uint32_t maxSegs,
                                                                  DevStats *st) {
     __shared__ BlockStats bs;
-    if (threadIdx.x == 0) bs = BlockStats{0, 0, 0, 0, 0, 0.0, 0.0, 0.0};
-    __syncthreads();
+    block_stats_zero(bs);
     const unsigned lane = threadIdx.x & 31;
     const unsigned lt = lanemask_lt();
     typename F::T t;
@@ -878,8 +848,6 @@ __global__ void __launch_bounds__(256, MINB) k_transport_refill(Ctx C, Bank in, 
     uint32_t pid = 0, segsThis = 0;
     bool has = false;
     bool exhausted = false;   // warp-uniform: the counter has passed n, stop adding to it
-    double dep = 0.0;
-    unsigned long long segs = 0, rws = 0;
     for (;;) {
         // refill the empty lanes from the unstarted particles
         const unsigned need = exhausted ? 0u : __ballot_sync(FULL, !has);
@@ -901,11 +869,14 @@ __global__ void __launch_bounds__(256, MINB) k_transport_refill(Ctx C, Bank in, 
         }
         if (!__any_sync(FULL, has)) break;
         int outcome = OUT_CONTINUE;
+        uint32_t segs = 0, rws = 0;
+        double dep = 0.0, w = 0.0;
         if (has) {
-            AtomicTally tal{C.eint, C.eradAvg, 0.0};
+            SegmentTally tal;
+            tal.init(C.eint, C.eradAvg, C.perCellCounters ? C.segs : nullptr);
             for (uint32_t b = 0; b < burst; ++b) {
                 const uint32_t cell0 = F::cell(t);
-                if (C.perCellCounters) atomicAdd(C.segs + cell0, 1u);
+                tal.enter(cell0);
                 ++segs;
                 int usedRW = 0, err = 0;
                 outcome = F::seg(C, t, rng, tal, usedRW, err);
@@ -920,11 +891,10 @@ __global__ void __launch_bounds__(256, MINB) k_transport_refill(Ctx C, Bank in, 
                     break;
                 }
             }
-            dep += tal.depSum;
-            if (outcome == OUT_ESCAPE) { atomicAdd(&bs.escaped, 1ull); atomicAdd(&bs.eEscaped, F::weight(t)); }
-            else if (outcome == OUT_CUTOFF) { atomicAdd(&bs.cutoff, 1ull); }
-            else if (outcome == OUT_CENSUS) { atomicAdd(&bs.census, 1ull); atomicAdd(&bs.eCensusPre, F::weight(t)); }
+            dep = tal.depSum;
+            w = F::weight(t);
         }
+        warp_stats(bs, segs, rws, dep, has ? outcome : OUT_CONTINUE, w);
         const bool cens = has && outcome == OUT_CENSUS;
         const unsigned mC = __ballot_sync(FULL, cens);
         if (mC) {
@@ -935,20 +905,7 @@ __global__ void __launch_bounds__(256, MINB) k_transport_refill(Ctx C, Bank in, 
         }
         if (has && outcome != OUT_CONTINUE) has = false;
     }
-    atomicAdd(&bs.segments, segs);
-    if (rws) atomicAdd(&bs.rwSteps, rws);
-    if (dep != 0.0) atomicAdd(&bs.eDeposited, dep);
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        if (bs.segments) atomicAdd(&st->segments, bs.segments);
-        if (bs.rwSteps) atomicAdd(&st->rwSteps, bs.rwSteps);
-        if (bs.escaped) atomicAdd(&st->escaped, bs.escaped);
-        if (bs.cutoff) atomicAdd(&st->cutoff, bs.cutoff);
-        if (bs.census) atomicAdd(&st->census, bs.census);
-        if (bs.eDeposited != 0.0) atomicAdd(&st->eDeposited, bs.eDeposited);
-        if (bs.eEscaped != 0.0) atomicAdd(&st->eEscaped, bs.eEscaped);
-        if (bs.eCensusPre != 0.0) atomicAdd(&st->eCensusPre, bs.eCensusPre);
-    }
+    block_stats_flush(bs, st);
 }
 
 // ------------------------------------------------------------------ comb

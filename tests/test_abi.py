@@ -89,3 +89,25 @@ def test_create_without_device_fails_loudly():
         pytest.skip("a GPU is visible")
     rc, _ = _create(problems.gray_slab().to_desc())
     assert rc == 7   # STORM_ERR_NO_DEVICE: no CPU fallback
+
+
+def test_dropin_header_compiles_and_fails_loudly_without_device():
+    """MonteCarloManagerCUDA compiled against the reference's types (built
+    where the reference sources exist): it loads, and constructing it without a
+    GPU throws the reference's StormError instead of falling back to the CPU."""
+    path = os.path.join(ROOT, "oracle", "_ref", "libstormdropin.so")
+    if not os.path.exists(path):
+        pytest.skip("drop-in harness not built")
+    import torch
+    if torch.cuda.is_available():
+        pytest.skip("a GPU is visible")
+    L = C.CDLL(path)
+    for s in ("dropin_create", "dropin_step", "dropin_destroy", "dropin_ref", "dropin_get_cells"):
+        assert hasattr(L, s), s
+    L.dropin_create.restype = C.c_void_p
+    L.dropin_create.argtypes = [C.POINTER(A.StormProblemDesc), C.c_int, C.c_char_p, C.c_size_t]
+    desc = problems.gray_slab().to_desc()
+    err = C.create_string_buffer(512)
+    assert not L.dropin_create(C.byref(desc), 0, err, 512)
+    msg = err.value.decode()
+    assert "MonteCarloManagerCUDA" in msg and "storm_cuda_create" in msg, msg
