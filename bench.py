@@ -50,7 +50,7 @@ def parse():
     ap.add_argument("--min-blocks", type=int, default=0, help="transport occupancy variant (1-4)")
     ap.add_argument("--waves", type=int, default=4)
     ap.add_argument("--refill", type=int, default=-1, help="1 persistent refill kernel, 0 bank visits")
-    ap.add_argument("--burst", type=int, default=4)
+    ap.add_argument("--burst", type=int, default=8)
     return ap.parse_args()
 
 
@@ -254,16 +254,41 @@ def run_form(args, precision, seed, local, dist, timed=True):
     return out
 
 
-def roofline(res, bytes_per_segment):
+def transport_kernel(args, fp32):
+    """Name of the transport kernel the run launches (refill is the engine default)."""
+    form = "Form32" if fp32 else "Form64"
+    if args.refill != 0:
+        return f"k_transport_refill<{form}>"
+    return "k_transport32" if fp32 else "k_transport"
+
+
+def measured_traffic(kernel):
+    """DRAM bytes per segment of `kernel` from the committed ncu summary, or None."""
+    path = os.path.join(ROOT, "profiles", "transport_traffic.json")
+    if not os.path.exists(path):
+        return None, None
+    entry = json.load(open(path)).get(kernel)
+    if not entry:
+        return None, None
+    return entry["dram_bytes_per_segment"], entry["capture"]
+
+
+def roofline(res, bytes_per_segment, kernel):
     peak, src = _peak()
     tt = res["transport"]
     mean_ms = tt["kernel_ms"] / max(tt["launches"], 1)
-    bytes_per_launch = bytes_per_segment * tt["segments"] / max(tt["launches"], 1)
+    segs_per_launch = tt["segments"] / max(tt["launches"], 1)
+    bytes_per_launch = bytes_per_segment * segs_per_launch
     achieved = bytes_per_launch / (mean_ms / 1000.0) / 1e9
-    return {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-            "traffic": None, "kernel": "k_transport32" if bytes_per_segment == BYTES_PER_SEGMENT_FP32 else "k_transport",
-            "bytes_per_segment": bytes_per_segment, "mean_launch_ms": mean_ms, "launches": tt["launches"],
-            "peak_source": src, "note": "peak = measured copy bandwidth (" + src + ")"}
+    per_seg, capture = measured_traffic(kernel)
+    traffic = per_seg * segs_per_launch if per_seg is not None else None
+    out = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+           "traffic": traffic, "kernel": kernel, "bytes_per_segment": bytes_per_segment,
+           "mean_launch_ms": mean_ms, "launches": tt["launches"], "segments_per_launch": segs_per_launch,
+           "peak_source": src, "note": "peak = measured copy bandwidth (" + src + ")"}
+    if capture:
+        out["traffic_source"] = capture
+    return out
 
 
 def e2e_run(args, eng, p, dist):
@@ -369,12 +394,12 @@ def run_storm(args, ws, rank, local, dist):
                                                  "form": "FP32 cell-local tracking, FP64 time/weights/tallies"},
             "latency_ms": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99))},
             "segments_per_step": f32["segments"] / args.steps,
-            "roofline": roofline(f32, BYTES_PER_SEGMENT_FP32),
+            "roofline": roofline(f32, BYTES_PER_SEGMENT_FP32, transport_kernel(args, True)),
             "fp64": {"value": v64, "ms_per_step": ms64 / args.steps, "dtype": "f64",
                      "latency_ms": {"p50": float(np.percentile(f64["step_ms"], 50)),
                                     "p99": float(np.percentile(f64["step_ms"], 99))},
                      "segments_per_step": f64["segments"] / args.steps,
-                     "roofline": roofline(f64, BYTES_PER_SEGMENT_FP64)},
+                     "roofline": roofline(f64, BYTES_PER_SEGMENT_FP64, transport_kernel(args, False))},
             "fp32_over_fp64": v32 / v64,
             "fp32_vs_fp64_deviation": dev,
             "cpu_baseline": cpu, "e2e": e2e, "clocks": ck, "gpu_launches": f32["launches"],

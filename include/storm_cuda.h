@@ -350,11 +350,11 @@ int storm_cuda_launch_count(StormHandle *h, uint64_t *launches);
  * launches and the segments they ran since the last reset. */
 int storm_cuda_set_profiling(StormHandle *h, int on);
 int storm_cuda_transport_timing(StormHandle *h, double *kernel_ms, uint64_t *launches, uint64_t *segments, int reset);
-/* Transport scheduling (autotuner hook).  refill = 0 (default): bank visits of
- * segments_per_visit segments with survivors compacted between launches.
- * refill = 1: one persistent launch in which each lane takes the next
- * unstarted particle as soon as its history ends, running `burst` segments
- * between refills. */
+/* Transport scheduling (autotuner hook).  refill = 1 (default, burst 8): one
+ * persistent launch in which each lane takes the next unstarted particle as
+ * soon as its history ends, running `burst` segments between refills.
+ * refill = 0: bank visits of segments_per_visit segments with survivors
+ * compacted between launches. */
 int storm_cuda_set_transport_mode(StormHandle *h, int refill, uint32_t burst);
 /* Transport kernel variant (autotuner hook): the occupancy target of the
  * kernel (__launch_bounds__ minimum blocks per SM, 1-4) and the grid size in

@@ -559,16 +559,18 @@ __device__ inline int segment32(const Ctx &C, Track32 &T, RNG &rng, TALLY &tal, 
     if (face < 0) { err = STORM_DERR_NO_FACE; return OUT_ERROR; }
     const float sF = __fdividef(bn, bd);
     const double c = C.clight;
+    const float4 cp = C.phys32[cell];
 
-    if (C.withRW && C.rwElig[cell]) {
+    // Random Walk only where the particle is at least cp.z from every face
+    if (fminf(fminf(hx - fabsf(T.qx), hy - fabsf(T.qy)), hz - fabsf(T.qz)) >= cp.z) {
         // the Random Walk jump in FP64 on the particle's global coordinates
         const double cx = C.xc[T.i], cy = C.yc[T.j], cz = C.zc[T.k];
         PartReg p;
         p.x = cx + static_cast<double>(T.qx); p.y = cy + static_cast<double>(T.qy); p.z = cz + static_cast<double>(T.qz);
         p.vx = static_cast<double>(T.ux) * c; p.vy = static_cast<double>(T.uy) * c; p.vz = static_cast<double>(T.uz) * c;
         p.t = T.t; p.w = T.w; p.w0 = T.w0; p.cell = cell;
-        const double4 cp = C.phys[cell];
-        int r = try_random_walk(C, p, rng, tal, cp, C.xe[T.i], C.xe[T.i + 1], C.ye[T.j], C.ye[T.j + 1], C.ze[T.k],
+        const double4 cpd = C.phys[cell];
+        int r = try_random_walk(C, p, rng, tal, cpd, C.xe[T.i], C.xe[T.i + 1], C.ye[T.j], C.ye[T.j + 1], C.ze[T.k],
                                 C.ze[T.k + 1], cx, cy, cz);
         if (r == -2) { err = STORM_DERR_RW_SHRINK; return OUT_ERROR; }
         if (r >= 0) {
@@ -585,7 +587,6 @@ __device__ inline int segment32(const Ctx &C, Track32 &T, RNG &rng, TALLY &tal, 
         }
     }
 
-    const float4 cp = C.phys32[cell];
     const float sC = cp.x * (-__logf(rng.rawf()));
     const float sL = static_cast<float>(T.t * c);
     int best = 0;

@@ -222,6 +222,39 @@ __global__ void k_begin(Bank b, uint32_t n, double dt, DevStats *st) {
     if ((threadIdx.x & 31) == 0 && e != 0.0) atomicAdd(&st->eCensusIn, e);
 }
 
+// Random Walk eligibility of a cell (precomputeRandomWalkData, radiation/RadiationIMC.hpp:982-1063,
+// with computeCellSurfaceArea :971-980 in GetCellFaces order) and the FP32
+// form's segment constants: x = 1/sigma_e (inf when none), y = sigma_a f,
+// z = the distance to the nearest face below which the Random Walk is never
+// taken (rwMinParticleOpticalDepth / sigma_T, less 1e-5 relative so FP32
+// rounding never skips a walk the FP64 test would take; inf in cells that are
+// not eligible).
+__device__ __forceinline__ void cell_rw_and_phys32(const Ctx &C, const CellArrays &A, uint32_t c, double sa, double ss,
+                                                   double f) {
+    const double sigmaT = sa + ss;
+    bool elig = false;
+    if (C.withRW) {
+        A.rwSigT[c] = sigmaT;
+        uint32_t i, j, k;
+        cell_ijk(C, c, i, j, k);
+        double dx = C.xe[i + 1] - C.xe[i], dy = C.ye[j + 1] - C.ye[j], dz = C.ze[k + 1] - C.ze[k];
+        double ax = dy * dz, ay = dz * dx, az = dx * dy;
+        double S = 0.0;
+        S += ax; S += ax; S += ay; S += ay; S += az; S += az;
+        double chord = (S > 0.0) ? 4.0 * A.vol[c] / S : 0.0;
+        elig = sigmaT * chord >= C.rwMinCell;
+        A.rwElig[c] = elig ? 1 : 0;
+    }
+    if (C.fp32) {
+        const double eventOpacity = ss + (1.0 - f) * sa;
+        const float rwReach = (elig && sigmaT > 0.0)
+                                  ? static_cast<float>(C.rwMinParticle / sigmaT * (1.0 - 1e-5))
+                                  : CUDART_INF_F;
+        A.phys32[c] = make_float4(eventOpacity > 0.0 ? static_cast<float>(1.0 / eventOpacity) : CUDART_INF_F,
+                                  static_cast<float>(sa * f), rwReach, 0.0f);
+    }
+}
+
 // ------------------------------------------------------------------ prestep
 // RadiationIMC::preStep (radiation/RadiationIMC.hpp:1618-1661) per cell, the opacity
 // plug-in (CalcPlanckOpacity / CalcScatteringOpacity) and precomputeRandomWalkData
@@ -263,23 +296,7 @@ __global__ void k_prestep(Ctx C, CellArrays A, OpacityEos M, double dt) {
         A.fleck[c] = f;
         if (f < 0.0 || f > 1.0) raise_error(C, STORM_DERR_FLECK, c, 0);
         A.phys[c] = cell_phys(sa, ss, f, sa + ss, C.clight);
-        if (C.fp32) {
-            const double eventOpacity = ss + (1.0 - f) * sa;
-            A.phys32[c] = make_float4(eventOpacity > 0.0 ? static_cast<float>(1.0 / eventOpacity) : CUDART_INF_F,
-                                      static_cast<float>(sa * f), 0.0f, 0.0f);
-        }
-        if (C.withRW) {
-            double sigmaT = sa + ss;
-            A.rwSigT[c] = sigmaT;
-            uint32_t i, j, k;
-            cell_ijk(C, c, i, j, k);
-            double dx = C.xe[i + 1] - C.xe[i], dy = C.ye[j + 1] - C.ye[j], dz = C.ze[k + 1] - C.ze[k];
-            double ax = dy * dz, ay = dz * dx, az = dx * dy;
-            double S = 0.0;   // computeCellSurfaceArea (:971-980) in GetCellFaces order
-            S += ax; S += ax; S += ay; S += ay; S += az; S += az;
-            double chord = (S > 0.0) ? 4.0 * A.vol[c] / S : 0.0;
-            A.rwElig[c] = (sigmaT * chord >= C.rwMinCell) ? 1 : 0;
-        }
+        cell_rw_and_phys32(C, A, c, sa, ss, f);
     }
 }
 
@@ -289,21 +306,7 @@ __global__ void k_rw_eligibility(Ctx C, CellArrays A) {
     for (uint32_t c = blockIdx.x * blockDim.x + threadIdx.x; c < C.ncells; c += gridDim.x * blockDim.x) {
         double sigmaT = A.sigA[c] + A.sigS[c];
         A.phys[c] = cell_phys(A.sigA[c], A.sigS[c], A.fleck[c], sigmaT, C.clight);
-        if (C.fp32) {
-            const double eventOpacity = A.sigS[c] + (1.0 - A.fleck[c]) * A.sigA[c];
-            A.phys32[c] = make_float4(eventOpacity > 0.0 ? static_cast<float>(1.0 / eventOpacity) : CUDART_INF_F,
-                                      static_cast<float>(A.sigA[c] * A.fleck[c]), 0.0f, 0.0f);
-        }
-        if (!C.withRW) continue;
-        A.rwSigT[c] = sigmaT;
-        uint32_t i, j, k;
-        cell_ijk(C, c, i, j, k);
-        double dx = C.xe[i + 1] - C.xe[i], dy = C.ye[j + 1] - C.ye[j], dz = C.ze[k + 1] - C.ze[k];
-        double ax = dy * dz, ay = dz * dx, az = dx * dy;
-        double S = 0.0;
-        S += ax; S += ax; S += ay; S += ay; S += az; S += az;
-        double chord = (S > 0.0) ? 4.0 * A.vol[c] / S : 0.0;
-        A.rwElig[c] = (sigmaT * chord >= C.rwMinCell) ? 1 : 0;
+        cell_rw_and_phys32(C, A, c, A.sigA[c], A.sigS[c], A.fleck[c]);
     }
 }
 
@@ -832,48 +835,65 @@ __global__ void __launch_bounds__(256, MINB) k_transport32(Ctx C, Bank in, const
 // ------------------------------------------------------------------ persistent transport
 // The whole HandleAll loop in one launch.  Every lane holds one history; a lane
 // whose particle reaches census, escapes or is cut off writes it out and takes
-// the next unstarted particle (one atomic per warp for the lanes that need
-// one), so lanes do not idle behind the longest history of their warp.  A
+// the next unstarted particle, so lanes do not idle behind the longest history
+// of their warp.  Each warp takes unstarted particles from the bank in chunks of
+// REFILL_CHUNK (one global atomic per chunk) and hands them to its empty lanes
+// between bursts of `burst` segments.  Per-lane totals (segments, deposits,
+// census energy) live in the lane's own shared-memory slot until the end.  A
 // history longer than maxSegs raises STORM_DERR_HISTORY_CAP and stops.
+constexpr uint32_t REFILL_CHUNK = 32;
+
 template <class F, int MINB>
 __global__ void __launch_bounds__(256, MINB) k_transport_refill(Ctx C, Bank in, uint32_t n, uint32_t *nextIdx, CensusBank cen,
                                                                  uint32_t *nCen, uint32_t burst, uint32_t maxSegs,
                                                                  DevStats *st) {
     __shared__ BlockStats bs;
+    __shared__ double sDep[256], sCen[256];
+    __shared__ uint32_t sSegs[256], sRw[256];
+    const unsigned tid = threadIdx.x;
+    sDep[tid] = 0.0; sCen[tid] = 0.0; sSegs[tid] = 0; sRw[tid] = 0;
     block_stats_zero(bs);
-    const unsigned lane = threadIdx.x & 31;
+    const unsigned lane = tid & 31;
     const unsigned lt = lanemask_lt();
     typename F::T t;
     PhiloxRng rng;
     uint32_t pid = 0, segsThis = 0;
     bool has = false;
-    bool exhausted = false;   // warp-uniform: the counter has passed n, stop adding to it
+    uint32_t cBase = 0, cLeft = 0;   // warp-uniform: this warp's chunk of unstarted particles
+    bool drained = false;            // warp-uniform: the bank counter has passed n
     for (;;) {
-        // refill the empty lanes from the unstarted particles
-        const unsigned need = exhausted ? 0u : __ballot_sync(FULL, !has);
-        if (need) {
-            uint32_t base = 0;
-            if (lane == static_cast<unsigned>(__ffs(need) - 1)) base = atomicAdd(nextIdx, __popc(need));
-            base = __shfl_sync(FULL, base, __ffs(need) - 1);
-            if (base + __popc(need) >= n) exhausted = true;
-            if (!has) {
-                const uint32_t q = base + __popc(need & lt);
-                if (q < n) {
-                    F::load(C, in, q, t);
-                    pid = in.pid[q];
-                    rng.init(C.seedLo, C.seedHi, TAG_TRANSPORT, C.step, pid, in.draw[q]);
-                    segsThis = 0;
-                    has = true;
-                }
+        unsigned need = __ballot_sync(FULL, !has);
+        while (need) {
+            if (cLeft == 0) {
+                if (drained) break;
+                uint32_t b = 0;
+                if (lane == 0) b = atomicAdd(nextIdx, REFILL_CHUNK);
+                b = __shfl_sync(FULL, b, 0);
+                if (b >= n) { drained = true; break; }
+                if (n - b <= REFILL_CHUNK) drained = true;
+                cBase = b;
+                cLeft = min(REFILL_CHUNK, n - b);
             }
+            const uint32_t take = min(static_cast<uint32_t>(__popc(need)), cLeft);
+            const uint32_t rank = __popc(need & lt);
+            if (!has && rank < take) {
+                const uint32_t q = cBase + rank;
+                F::load(C, in, q, t);
+                pid = in.pid[q];
+                rng.init(C.seedLo, C.seedHi, TAG_TRANSPORT, C.step, pid, in.draw[q]);
+                segsThis = 0;
+                has = true;
+            }
+            cBase += take;
+            cLeft -= take;
+            need = __ballot_sync(FULL, !has);
         }
         if (!__any_sync(FULL, has)) break;
         int outcome = OUT_CONTINUE;
-        uint32_t segs = 0, rws = 0;
-        double dep = 0.0, w = 0.0;
         if (has) {
             SegmentTally tal;
             tal.init(C.eint, C.eradAvg, C.perCellCounters ? C.segs : nullptr);
+            uint32_t segs = 0, rws = 0;
             for (uint32_t b = 0; b < burst; ++b) {
                 const uint32_t cell0 = F::cell(t);
                 tal.enter(cell0);
@@ -891,19 +911,34 @@ __global__ void __launch_bounds__(256, MINB) k_transport_refill(Ctx C, Bank in, 
                     break;
                 }
             }
-            dep = tal.depSum;
-            w = F::weight(t);
+            sSegs[tid] += segs;
+            if (rws) sRw[tid] += rws;
+            sDep[tid] += tal.depSum;
+            if (outcome == OUT_ESCAPE) { atomicAdd(&bs.escaped, 1ull); atomicAdd(&bs.eEscaped, F::weight(t)); }
+            else if (outcome == OUT_CUTOFF) atomicAdd(&bs.cutoff, 1ull);
+            else if (outcome == OUT_CENSUS) sCen[tid] += F::weight(t);
         }
-        warp_stats(bs, segs, rws, dep, has ? outcome : OUT_CONTINUE, w);
         const bool cens = has && outcome == OUT_CENSUS;
         const unsigned mC = __ballot_sync(FULL, cens);
         if (mC) {
             uint32_t bC = 0;
-            if (lane == static_cast<unsigned>(__ffs(mC) - 1)) bC = atomicAdd(nCen, __popc(mC));
-            bC = __shfl_sync(FULL, bC, __ffs(mC) - 1);
+            if (lane == 0) {
+                bC = atomicAdd(nCen, __popc(mC));
+                atomicAdd(&bs.census, static_cast<unsigned long long>(__popc(mC)));
+            }
+            bC = __shfl_sync(FULL, bC, 0);
             if (cens) F::store(cen, bC + __popc(mC & lt), t, pid, rng.draw);
         }
         if (has && outcome != OUT_CONTINUE) has = false;
+    }
+    // per-lane totals -> block
+    const uint32_t segs = warp_sum(sSegs[tid]), rws = warp_sum(sRw[tid]);
+    const double dep = warp_sum(sDep[tid]), eC = warp_sum(sCen[tid]);
+    if (lane == 0) {
+        if (segs) atomicAdd(&bs.segments, static_cast<unsigned long long>(segs));
+        if (rws) atomicAdd(&bs.rwSteps, static_cast<unsigned long long>(rws));
+        if (dep != 0.0) atomicAdd(&bs.eDeposited, dep);
+        if (eC != 0.0) atomicAdd(&bs.eCensusPre, eC);
     }
     block_stats_flush(bs, st);
 }

@@ -79,8 +79,8 @@ struct StormHandle {
     uint32_t step = 0;
     uint32_t K = 8, maxRounds = 4096;
     int minBlocks = 3;               // transport occupancy variant (__launch_bounds__ min blocks)
-    int refill = 0;                  // 1: persistent refill kernel, 0: bank visits of K segments
-    uint32_t burst = 4;              // refill kernel: segments between refills
+    int refill = 1;                  // 1: persistent refill kernel, 0: bank visits of K segments
+    uint32_t burst = 8;              // refill kernel: segments between refills
     int smCount = 148;
     uint32_t transportGrid = 0;      // resident blocks of the chosen variant x SMs
     uint64_t launches = 0;
