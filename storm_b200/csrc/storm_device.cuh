@@ -51,6 +51,8 @@ struct BoxFaceDev {
 struct RwTables {
     const double *tau, *logTau, *surv, *radius;
     double logMin, logMax;   // std::log(1e-8), std::log(64) as the host computes them
+    // FP32 copies for the FP32-tracking form
+    const float *logTau32, *surv32, *radius32;
 };
 
 // Everything a kernel needs, passed by value.
@@ -535,6 +537,96 @@ struct Track32 {
 
 __device__ __forceinline__ float clampf(float v, float h) { return fminf(fmaxf(v, -h), h); }
 
+// RandomWalk::sampleLeakTime / sampleRadius (radiation/RandomWalk.hpp:81-137)
+// on the FP32 copies of the tables: the same binary search and interpolations.
+__device__ inline float rw_sample_leak32(const RwTables &T, float xi) {
+    const float target = 1.0f - xi;
+    if (target >= T.surv32[0]) return __expf(T.logTau32[0]);
+    if (target <= T.surv32[RW_TABLE - 1]) return __expf(T.logTau32[RW_TABLE - 1]);
+    uint32_t first = 0, count = RW_TABLE;
+    while (count > 0) {
+        const uint32_t step = count >> 1, it = first + step;
+        if (T.surv32[it] > target) { first = it + 1; count -= step + 1; } else count = step;
+    }
+    if (first == 0) return __expf(T.logTau32[0]);
+    if (first == RW_TABLE) return __expf(T.logTau32[RW_TABLE - 1]);
+    const float S0 = T.surv32[first - 1], S1 = T.surv32[first];
+    const float frac = (S0 - target) / (S0 - S1);
+    const float l0 = T.logTau32[first - 1], l1 = T.logTau32[first];
+    return __expf(l0 + frac * (l1 - l0));
+}
+
+__device__ inline float rw_sample_radius32(const RwTables &T, float tau, float xi) {
+    const float logTau = __logf(fminf(fmaxf(tau, 1e-8f), 64.0f));
+    const float lmin = static_cast<float>(T.logMin), lmax = static_cast<float>(T.logMax);
+    const float tauPos = (logTau - lmin) / (lmax - lmin) * static_cast<float>(RW_TABLE - 1);
+    uint32_t tauIdx = static_cast<uint32_t>(fmaxf(tauPos, 0.0f));
+    if (tauIdx > RW_TABLE - 2) tauIdx = RW_TABLE - 2;
+    const float tauFrac = tauPos - static_cast<float>(tauIdx);
+    const float xiPos = fminf(fmaxf(xi, 0.0f), 1.0f) * static_cast<float>(RW_RADIUS - 1);
+    uint32_t xiIdx = static_cast<uint32_t>(xiPos);
+    if (xiIdx > RW_RADIUS - 2) xiIdx = RW_RADIUS - 2;
+    const float xiFrac = xiPos - static_cast<float>(xiIdx);
+    const float *r0p = T.radius32 + static_cast<size_t>(tauIdx) * RW_RADIUS + xiIdx;
+    const float *r1p = r0p + RW_RADIUS;
+    const float r0 = r0p[0] + xiFrac * (r0p[1] - r0p[0]);
+    const float r1 = r1p[0] + xiFrac * (r1p[1] - r1p[0]);
+    return fminf(fmaxf(r0 + tauFrac * (r1 - r0), 0.0f), 1.0f);
+}
+
+// RadiationIMC::tryRandomWalkStep (radiation/RadiationIMC.hpp:1065-1276), gray, in
+// the FP32-tracking form: cell-local FP32 geometry, FP64 time, weight and
+// tallies, the same draws in the same order as the FP64 form.  Ro is the
+// distance to the nearest face (the caller has checked Ro >= rwMinParticle /
+// sigma_T); cp.w is the diffusion coefficient c / (3 sigma_T).
+template <class RNG, class TALLY>
+__device__ inline int rw_jump32(const Ctx &C, Track32 &T, RNG &rng, TALLY &tal, const float4 &cp, float Ro, float hx,
+                                float hy, float hz, int &err) {
+    const uint32_t cell = T.cell;
+    const float tauLeak = rw_sample_leak32(C.rw, rng.rawf());
+    const double tLeak = static_cast<double>(tauLeak * (Ro * Ro) / cp.w);
+    const bool leak = tLeak <= T.t;
+    const double dt = leak ? tLeak : T.t;
+    const float tau = cp.y * static_cast<float>(dt * C.clight);
+    const double e1 = static_cast<double>(expm1f(-tau));
+    if (!C.noFeedback) tal.mat(cell, -e1 * T.w);
+    if (cp.y > 0.0f) tal.rad(cell, T.w * e1 * C.phys[cell].z);
+    T.w *= 1.0 + e1;
+    T.t -= dt;
+    if (fabs(T.w) < T.w0 * 1e-4) {
+        if (!C.noFeedback) tal.mat(cell, T.w);
+        return OUT_CUTOFF;
+    }
+    const float cosT = 2.0f * rng.rawf() - 1.0f;
+    const float sinT = sqrtf(fmaxf(0.0f, 1.0f - cosT * cosT));
+    float sphi, cphi;
+    __sincosf(6.2831853f * rng.rawf(), &sphi, &cphi);
+    const float dx = sinT * cphi, dy = sinT * sphi, dz = cosT;
+    float disp = Ro;
+    if (!leak) {
+        const float tauPos = static_cast<float>(dt) * cp.w / (Ro * Ro);
+        disp = fminf(Ro * rw_sample_radius32(C.rw, tauPos, rng.rawf()), Ro);
+    }
+    const float nudge = 1.0f - static_cast<float>(RW_NUDGE);   // toward the cell centre (local origin)
+    float lx = (T.qx + disp * dx) * nudge, ly = (T.qy + disp * dy) * nudge, lz = (T.qz + disp * dz) * nudge;
+    int guard = 0;
+    while (fabsf(lx) > hx || fabsf(ly) > hy || fabsf(lz) > hz) {
+        disp *= 0.99f;
+        lx = T.qx + disp * dx;
+        ly = T.qy + disp * dy;
+        lz = T.qz + disp * dz;
+        if (++guard > RW_SHRINK_CAP) { err = STORM_DERR_RW_SHRINK; return OUT_ERROR; }
+    }
+    T.qx = lx; T.qy = ly; T.qz = lz;
+    const float theta = 6.2831853f * rng.rawf();
+    const float cz = 2.0f * rng.rawf() - 1.0f;
+    const float sz = sqrtf(fmaxf(0.0f, 1.0f - cz * cz));
+    float st, ct;
+    __sincosf(theta, &st, &ct);
+    T.ux = sz * ct; T.uy = sz * st; T.uz = cz;
+    return leak ? OUT_CONTINUE : OUT_CENSUS;
+}
+
 // One segment plus the manager's handling, in the FP32-tracking form.  Same
 // events, same draws per event and the same FP64 tally updates as the FP64
 // form; distances, the face search and the collision distance are FP32 in the
@@ -548,6 +640,16 @@ template <class RNG, class TALLY>
 __device__ inline int segment32(const Ctx &C, Track32 &T, RNG &rng, TALLY &tal, int &usedRW, int &err) {
     const uint32_t cell = T.cell;
     const float hx = C.hx[T.i], hy = C.hy[T.j], hz = C.hz[T.k];
+    const float4 cp = C.phys32[cell];
+
+    // Random Walk only where the particle is at least cp.z = rwMinParticleOpticalDepth / sigma_T
+    // from every face (cp.z is inf in cells that are not eligible)
+    const float Ro = fminf(fminf(hx - fabsf(T.qx), hy - fabsf(T.qy)), hz - fabsf(T.qz));
+    if (Ro >= cp.z && Ro > 0.0f) {
+        usedRW = 1;
+        return rw_jump32(C, T, rng, tal, cp, Ro, hx, hy, hz, err);
+    }
+
     const float ax = fabsf(T.ux), ay = fabsf(T.uy), az = fabsf(T.uz);
     const float nxp = ax > 0.0f ? fmaxf(hx - (T.ux > 0.0f ? T.qx : -T.qx), 0.0f) : 1.0f;
     const float nyp = ay > 0.0f ? fmaxf(hy - (T.uy > 0.0f ? T.qy : -T.qy), 0.0f) : 1.0f;
@@ -559,33 +661,6 @@ __device__ inline int segment32(const Ctx &C, Track32 &T, RNG &rng, TALLY &tal, 
     if (face < 0) { err = STORM_DERR_NO_FACE; return OUT_ERROR; }
     const float sF = __fdividef(bn, bd);
     const double c = C.clight;
-    const float4 cp = C.phys32[cell];
-
-    // Random Walk only where the particle is at least cp.z from every face
-    if (fminf(fminf(hx - fabsf(T.qx), hy - fabsf(T.qy)), hz - fabsf(T.qz)) >= cp.z) {
-        // the Random Walk jump in FP64 on the particle's global coordinates
-        const double cx = C.xc[T.i], cy = C.yc[T.j], cz = C.zc[T.k];
-        PartReg p;
-        p.x = cx + static_cast<double>(T.qx); p.y = cy + static_cast<double>(T.qy); p.z = cz + static_cast<double>(T.qz);
-        p.vx = static_cast<double>(T.ux) * c; p.vy = static_cast<double>(T.uy) * c; p.vz = static_cast<double>(T.uz) * c;
-        p.t = T.t; p.w = T.w; p.w0 = T.w0; p.cell = cell;
-        const double4 cpd = C.phys[cell];
-        int r = try_random_walk(C, p, rng, tal, cpd, C.xe[T.i], C.xe[T.i + 1], C.ye[T.j], C.ye[T.j + 1], C.ze[T.k],
-                                C.ze[T.k + 1], cx, cy, cz);
-        if (r == -2) { err = STORM_DERR_RW_SHRINK; return OUT_ERROR; }
-        if (r >= 0) {
-            usedRW = 1;
-            T.t = p.t; T.w = p.w;
-            T.qx = clampf(static_cast<float>(p.x - cx), hx);
-            T.qy = clampf(static_cast<float>(p.y - cy), hy);
-            T.qz = clampf(static_cast<float>(p.z - cz), hz);
-            const double inv = C.invC;
-            T.ux = static_cast<float>(p.vx * inv); T.uy = static_cast<float>(p.vy * inv); T.uz = static_cast<float>(p.vz * inv);
-            if (r == REMOVE) return OUT_CUTOFF;
-            if (r == DONE) return OUT_CENSUS;
-            return OUT_CONTINUE;
-        }
-    }
 
     const float sC = cp.x * (-__logf(rng.rawf()));
     const float sL = static_cast<float>(T.t * c);

@@ -119,6 +119,8 @@ void launch_census_keys_pid(cudaStream_t s, const Ctx &C, const CensusBank &cen,
 void launch_gather(cudaStream_t s, const Ctx &C, const CensusBank &src, const uint32_t *idx, uint32_t n, const Bank &dst,
                    double *eradCensus, DevStats *st);
 void launch_bank_to_census(cudaStream_t s, const Ctx &C, const Bank &src, const CensusBank &dst, uint32_t n);
+void launch_count_bad_cells(cudaStream_t s, const uint32_t *cell, uint32_t n, uint32_t N, int32_t *bad);
+void launch_to_float(cudaStream_t s, const double *src, float *dst, uint32_t n);
 void launch_poststep(cudaStream_t s, const Ctx &C, const CellArrays &A, const OpacityEos &M, double dt);
 void launch_replay(cudaStream_t s, const Ctx &C, const ReplayDev &R, uint32_t n);
 void launch_rw_radius(cudaStream_t s, const double *tau, const double *surv, double *radius);

@@ -225,10 +225,9 @@ __global__ void k_begin(Bank b, uint32_t n, double dt, DevStats *st) {
 // Random Walk eligibility of a cell (precomputeRandomWalkData, radiation/RadiationIMC.hpp:982-1063,
 // with computeCellSurfaceArea :971-980 in GetCellFaces order) and the FP32
 // form's segment constants: x = 1/sigma_e (inf when none), y = sigma_a f,
-// z = the distance to the nearest face below which the Random Walk is never
-// taken (rwMinParticleOpticalDepth / sigma_T, less 1e-5 relative so FP32
-// rounding never skips a walk the FP64 test would take; inf in cells that are
-// not eligible).
+// z = rwMinParticleOpticalDepth / sigma_T, the distance to the nearest face a
+// particle needs for a Random Walk jump (inf in cells that are not eligible),
+// w = the diffusion coefficient c / (3 sigma_T).
 __device__ __forceinline__ void cell_rw_and_phys32(const Ctx &C, const CellArrays &A, uint32_t c, double sa, double ss,
                                                    double f) {
     const double sigmaT = sa + ss;
@@ -247,11 +246,11 @@ __device__ __forceinline__ void cell_rw_and_phys32(const Ctx &C, const CellArray
     }
     if (C.fp32) {
         const double eventOpacity = ss + (1.0 - f) * sa;
-        const float rwReach = (elig && sigmaT > 0.0)
-                                  ? static_cast<float>(C.rwMinParticle / sigmaT * (1.0 - 1e-5))
-                                  : CUDART_INF_F;
+        const bool rw = elig && sigmaT > 0.0;
         A.phys32[c] = make_float4(eventOpacity > 0.0 ? static_cast<float>(1.0 / eventOpacity) : CUDART_INF_F,
-                                  static_cast<float>(sa * f), rwReach, 0.0f);
+                                  static_cast<float>(sa * f),
+                                  rw ? static_cast<float>(C.rwMinParticle / sigmaT) : CUDART_INF_F,
+                                  rw ? static_cast<float>(C.clight / (3.0 * sigmaT)) : 0.0f);
     }
 }
 
@@ -1574,6 +1573,22 @@ static int refill_occ(int minBlocks) {
 }
 int refill_blocks_per_sm(int minBlocks, bool fp32) { return fp32 ? refill_occ<Form32>(minBlocks) : refill_occ<Form64>(minBlocks); }
 
+// Count (per warp) the census entries whose cell index is not a cell of the grid.
+__global__ void k_count_bad_cells(const uint32_t *cell, uint32_t n, uint32_t N, int32_t *bad) {
+    bool b = false;
+    for (uint32_t q = blockIdx.x * blockDim.x + threadIdx.x; q < n; q += gridDim.x * blockDim.x) b |= cell[q] >= N;
+    if (__any_sync(FULL, b) && (threadIdx.x & 31) == 0) atomicAdd(bad, 1);
+}
+__global__ void k_to_float(const double *src, float *dst, uint32_t n) {
+    for (uint32_t q = blockIdx.x * blockDim.x + threadIdx.x; q < n; q += gridDim.x * blockDim.x)
+        dst[q] = static_cast<float>(src[q]);
+}
+void launch_to_float(cudaStream_t s, const double *src, float *dst, uint32_t n) {
+    if (n) k_to_float<<<grid_for(n, 256, 4096), 256, 0, s>>>(src, dst, n);
+}
+void launch_count_bad_cells(cudaStream_t s, const uint32_t *cell, uint32_t n, uint32_t N, int32_t *bad) {
+    if (n) k_count_bad_cells<<<grid_for(n, 256, 4096), 256, 0, s>>>(cell, n, N, bad);
+}
 void launch_bank_to_local(cudaStream_t s, const Ctx &C, const Bank &src, const Bank &dst, uint32_t n) {
     if (n) k_bank_to_local<<<grid_for(n, 256, 8192), 256, 0, s>>>(C, src, dst, n);
 }

@@ -48,6 +48,7 @@ struct StormHandle {
     Ctx C{};
     // random walk tables
     double *rwTau = nullptr, *rwLogTau = nullptr, *rwSurv = nullptr, *rwRadius = nullptr;
+    float *rwLogTau32 = nullptr, *rwSurv32 = nullptr, *rwRadius32 = nullptr;   // FP32-tracking form
     // face sources
     uint32_t *fsCell = nullptr;
     int32_t *fsSide = nullptr;
@@ -78,7 +79,7 @@ struct StormHandle {
     uint64_t nBank = 0;              // particles in bankA after emission
     uint32_t step = 0;
     uint32_t K = 8, maxRounds = 4096;
-    int minBlocks = 3;               // transport occupancy variant (__launch_bounds__ min blocks)
+    int minBlocks = 3;               // transport occupancy variant (__launch_bounds__ min blocks); 4 for FP32
     int refill = 1;                  // 1: persistent refill kernel, 0: bank visits of K segments
     uint32_t burst = 8;              // refill kernel: segments between refills
     int smCount = 148;
@@ -328,6 +329,19 @@ int build_rw_tables(StormHandle *h) {
     launch_rw_radius(h->stream, h->rwTau, h->rwSurv, h->rwRadius);
     ++h->launches;
     CK(cudaGetLastError());
+    if (h->fp32) {
+        CK(dalloc(h, &h->rwLogTau32, RW_TABLE));
+        CK(dalloc(h, &h->rwSurv32, RW_TABLE));
+        CK(dalloc(h, &h->rwRadius32, static_cast<size_t>(RW_TABLE) * RW_RADIUS));
+        launch_to_float(h->stream, h->rwLogTau, h->rwLogTau32, RW_TABLE);
+        launch_to_float(h->stream, h->rwSurv, h->rwSurv32, RW_TABLE);
+        launch_to_float(h->stream, h->rwRadius, h->rwRadius32, RW_TABLE * RW_RADIUS);
+        h->launches += 3;
+        CK(cudaGetLastError());
+        h->C.rw.logTau32 = h->rwLogTau32;
+        h->C.rw.surv32 = h->rwSurv32;
+        h->C.rw.radius32 = h->rwRadius32;
+    }
     CK(cudaStreamSynchronize(h->stream));
     h->C.rw.tau = h->rwTau;
     h->C.rw.logTau = h->rwLogTau;
@@ -445,6 +459,9 @@ int storm_cuda_create(const StormProblemDesc *d, StormHandle **out) {
     H2D(h->xe, h->hxe.data(), d->nx + 1); H2D(h->ye, h->hye.data(), d->ny + 1); H2D(h->ze, h->hze.data(), d->nz + 1);
     H2D(h->xc, h->hxc.data(), d->nx); H2D(h->yc, h->hyc.data(), d->ny); H2D(h->zc, h->hzc.data(), d->nz);
     h->fp32 = d->precision == STORM_PRECISION_FP32_TRACK;
+    // measured on B200 at 64^3: FP32 tracking fits 64 registers without spills (4 blocks of 256
+    // per SM); the FP64 form is fastest at 80 registers (3 blocks)
+    h->minBlocks = h->fp32 ? 4 : 3;
     {
         std::vector<float> fx(d->nx), fy(d->ny), fz(d->nz);
         for (uint32_t i = 0; i < d->nx; ++i) fx[i] = static_cast<float>(0.5 * (h->hxe[i + 1] - h->hxe[i]));
@@ -575,7 +592,7 @@ int storm_cuda_destroy(StormHandle *h) {
     void *ps[] = {h->xe, h->ye, h->ze, h->xc, h->yc, h->zc, h->A.T, h->A.mass, h->A.vol, h->A.eint, h->A.ceint,
                   h->A.sigA, h->A.sigS, h->A.fleck, h->A.rwSigT, h->A.eradAvg, h->A.eradCensus, h->A.emitE,
                   h->A.rwElig, h->A.photons, h->A.phys, h->A.phys32, h->hx, h->hy, h->hz, h->segs, h->tabA, h->tabS, h->rhoF, h->rwTau, h->rwLogTau, h->rwSurv,
-                  h->rwRadius, h->fsCell, h->fsSide, h->fsOffset, h->dAmbiguous, h->offsets, h->tileSums, h->dTotalU64, h->dTotalE, h->combW, h->combWtot,
+                  h->rwRadius, h->rwLogTau32, h->rwSurv32, h->rwRadius32, h->fsCell, h->fsSide, h->fsOffset, h->dAmbiguous, h->offsets, h->tileSums, h->dTotalU64, h->dTotalE, h->combW, h->combWtot,
                   h->combStart, h->combCount, h->counts, h->dStats, h->dErr};
     for (void *p : ps)
         if (p) cudaFree(p);
@@ -937,23 +954,28 @@ int storm_cuda_set_census(StormHandle *h, const StormParticlesSoA *in) {
     const Bank &stage = h->fp32 ? h->bankB : h->bankA;   // FP32 form: stage FP64, then convert
     const double *sd[] = {in->x, in->y, in->z, in->vx, in->vy, in->vz, in->time_left, in->weight, in->initial_weight};
     double *dd[] = {stage.x, stage.y, stage.z, stage.vx, stage.vy, stage.vz, stage.t, stage.w, stage.w0};
-    if (n) {
-        if (!in->cell) return STORM_ERR_INVALID_ARG;
-        for (uint64_t q = 0; q < n; ++q)
-            if (in->cell[q] >= h->N) return STORM_ERR_INVALID_ARG;
-    }
-    for (int q = 0; q < 9; ++q) {
+    if (n && !in->cell) return STORM_ERR_INVALID_ARG;
+    for (int q = 0; q < 9; ++q)
         if (!sd[q] && n) return STORM_ERR_INVALID_ARG;
-        if (n) CK(cudaMemcpyAsync(dd[q], sd[q], n * sizeof(double), cudaMemcpyHostToDevice, h->stream));
-    }
+    h->nCensus = 0;
     if (n) {
+        for (int q = 0; q < 9; ++q)
+            CK(cudaMemcpyAsync(dd[q], sd[q], n * sizeof(double), cudaMemcpyHostToDevice, h->stream));
         CK(cudaMemcpyAsync(stage.cell, in->cell, n * sizeof(uint32_t), cudaMemcpyHostToDevice, h->stream));
+        // cell indices are checked on the device (a host loop would cost as much as the copy)
+        int32_t bad = 0;
+        CK(cudaMemsetAsync(h->dAmbiguous + 1, 0, sizeof(int32_t), h->stream));
+        launch_count_bad_cells(h->stream, stage.cell, static_cast<uint32_t>(n), h->N, h->dAmbiguous + 1);
+        ++h->launches;
+        CK(cudaMemcpyAsync(&bad, h->dAmbiguous + 1, sizeof(int32_t), cudaMemcpyDeviceToHost, h->stream));
+        CK(cudaStreamSynchronize(h->stream));
+        if (bad) return STORM_ERR_INVALID_ARG;
         if (h->fp32) {
             launch_bank_to_local(h->stream, h->C, h->bankB, h->bankA, static_cast<uint32_t>(n));
             ++h->launches;
             CK(cudaGetLastError());
+            CK(cudaStreamSynchronize(h->stream));
         }
-        CK(cudaStreamSynchronize(h->stream));
     }
     h->nCensus = n;
     return STORM_OK;

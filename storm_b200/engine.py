@@ -77,18 +77,44 @@ class Particles:
         self.id = np.zeros(n, np.uint64)
         self.n = n
 
+    @classmethod
+    def pinned(cls, capacity):
+        """A buffer in page-locked host memory (full-rate host<->device copies);
+        id is left out (None)."""
+        import torch
+        p = cls(0)
+        for f in cls.FIELDS:
+            setattr(p, f, torch.empty(capacity, dtype=torch.float64, pin_memory=True).numpy())
+        p.cell = torch.empty(capacity, dtype=torch.int32, pin_memory=True).numpy().view(np.uint32)
+        p.id = None
+        p.n = capacity
+        return p
+
+    def view(self, n):
+        """The first n particles, sharing this buffer's memory."""
+        if n > self.n:
+            raise ValueError(f"buffer holds {self.n} particles, {n} requested")
+        v = Particles(0)
+        for f in self.FIELDS:
+            setattr(v, f, getattr(self, f)[:n])
+        v.cell = self.cell[:n]
+        v.id = None if self.id is None else self.id[:n]
+        v.n = n
+        return v
+
     def soa(self):
         """Struct of pointers; every field is made contiguous first (the C side
-        reads plain arrays)."""
+        reads plain arrays).  id may be None (not read or written)."""
         for f in self.FIELDS:
             setattr(self, f, np.ascontiguousarray(getattr(self, f), dtype=np.float64))
         self.cell = np.ascontiguousarray(self.cell, dtype=np.uint32)
-        self.id = np.ascontiguousarray(self.id, dtype=np.uint64)
         s = A.StormParticlesSoA()
         for f in self.FIELDS:
             setattr(s, f, A.ptr(getattr(self, f)))
         s.cell = A.ptr(self.cell, C.c_uint32)
-        s.id = A.ptr(self.id, C.c_uint64)
+        if self.id is not None:
+            self.id = np.ascontiguousarray(self.id, dtype=np.uint64)
+            s.id = A.ptr(self.id, C.c_uint64)
         s.count = self.n
         return s
 
@@ -151,9 +177,11 @@ class Engine:
         self._check(lib().storm_cuda_census_count(self.h, C.byref(n)))
         return n.value
 
-    def census(self):
+    def census(self, out=None):
+        """The census as host particles; with `out` (e.g. Particles.pinned) the
+        census is written into its first n slots and a view of them returned."""
         n = self.census_count()
-        p = Particles(n)
+        p = Particles(n) if out is None else out.view(n)
         s = p.soa()
         cnt = C.c_uint64()
         self._check(lib().storm_cuda_get_census(self.h, C.byref(s), n, C.byref(cnt)))
@@ -168,6 +196,14 @@ class Engine:
         s = p.soa()
         self._check(lib().storm_cuda_population_control(self.h, C.byref(s)))
         return self.census()
+
+    def temperature(self, out=None):
+        """Material temperatures into `out` (or a new array)."""
+        out = np.zeros(self.n) if out is None else out
+        null = C.POINTER(C.c_double)()
+        self._check(lib().storm_cuda_get_cell_arrays(self.h, A.ptr(out), null, null, null, null, null,
+                                                      C.POINTER(C.c_uint64)()))
+        return out
 
     def cells(self):
         keys = ("temperature", "internal_energy", "erad_time_avg", "erad_census", "sigma_a", "fleck")
