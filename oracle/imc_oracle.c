@@ -71,11 +71,27 @@ static uint32_t fmix32(uint32_t h) {
     h ^= h >> 16; h *= 0x85ebca6bu; h ^= h >> 13; h *= 0xc2b2ae35u; h ^= h >> 16;
     return h;
 }
-/* Comb shuffle key: a keyed bijection of the particle index, so sorting by
- * (cell, key) is a pseudo-random permutation within each cell with no ties. */
-uint32_t orc_comb_key(uint64_t seed, uint32_t step, uint32_t pid) {
+/* Comb shuffle key: a keyed bijection of [0, 2^b) applied to the particle
+ * index (every pid of the step is below 2^b), so sorting by (cell << b | key)
+ * is a pseudo-random permutation within each cell with no ties.  Xor with the
+ * step key, then odd multiplications and xor-shifts, each invertible mod 2^b. */
+uint32_t orc_comb_key(uint64_t seed, uint32_t step, uint32_t pid, int b) {
     uint32_t k = fmix32((uint32_t)seed ^ fmix32(step * 0x9E3779B9u + (uint32_t)(seed >> 32)));
-    return fmix32(pid ^ k);
+    const uint32_t mask = b >= 32 ? 0xffffffffu : ((1u << b) - 1u);
+    uint32_t h = (pid ^ k) & mask;
+    h = (h * 0x9E3779B1u) & mask;
+    h ^= h >> ((b + 1) / 2);
+    h = (h * 0x85EBCA77u) & mask;
+    h ^= h >> ((b + 2) / 3);
+    h = (h * 0xC2B2AE3Du) & mask;
+    h ^= h >> ((b + 1) / 2);
+    return h;
+}
+/* the comb key width: the smallest b >= 1 with 2^b >= pidLimit */
+static int pid_bits(uint64_t pidLimit) {
+    int b = 1;
+    while (b < 32 && (1ull << b) < pidLimit) ++b;
+    return b;
 }
 
 typedef struct {
@@ -150,6 +166,7 @@ struct Oracle {
     StormBoxFace faces[6];
     /* banks */
     Bank census, bank;
+    uint64_t pidLimit;   /* every pid of the current census is below this */
     uint32_t step;
     StormStepStats st;
     int32_t derr;
@@ -1028,6 +1045,7 @@ int orc_phase_emit(Oracle *o, double dt) {
  * particle is stepped to census, escape or removal. */
 int orc_phase_transport(Oracle *o) {
     memset(o->segs, 0, sizeof(uint64_t) * o->N);
+    o->pidLimit = o->bank.n ? o->bank.n : 1;   /* transport pids are bank slots */
     for (uint64_t q = 0; q < o->bank.n; ++q) {
         Part p = o->bank.p[q];
         Rng r;
@@ -1097,20 +1115,21 @@ int orc_phase_comb(Oracle *o) {
     Bank in = o->census;
     Bank out = {NULL, 0, 0};
     uint64_t nz = 0;
+    const int b = pid_bits(o->pidLimit);
     KeyIdx *ki = (KeyIdx *)malloc(sizeof(KeyIdx) * (in.n ? in.n : 1));
     for (uint64_t q = 0; q < in.n; ++q) {
         const Part *p = &in.p[q];
         if (outside_box(o, v3(p->x, p->y, p->z))) { raise(o, STORM_DERR_COMB_OUTSIDE, p->cell, p->pid); break; }
         if (!isfinite(p->w) || p->w < 0.0) { raise(o, STORM_DERR_COMB_WEIGHT, p->cell, p->pid); break; }
         if (p->w == 0.0) continue;
-        ki[nz].key = ((uint64_t)p->cell << 32) | orc_comb_key(o->d.seed, o->step, p->pid);
+        ki[nz].key = ((uint64_t)p->cell << b) | orc_comb_key(o->d.seed, o->step, p->pid, b);
         ki[nz].idx = q;
         ++nz;
     }
     if (o->derr) { free(ki); return -1; }
     qsort(ki, nz, sizeof(KeyIdx), cmp_key);
     uint64_t *start = (uint64_t *)calloc(N + 1, sizeof(uint64_t));
-    for (uint64_t q = 0; q < nz; ++q) start[(ki[q].key >> 32) + 1]++;
+    for (uint64_t q = 0; q < nz; ++q) start[(ki[q].key >> b) + 1]++;
     for (uint64_t i = 0; i < N; ++i) start[i + 1] += start[i];
     double *W = (double *)calloc(N ? N : 1, sizeof(double));
     for (uint64_t i = 0; i < N; ++i) {
@@ -1253,6 +1272,7 @@ int orc_set_census(Oracle *o, const StormParticlesSoA *in) {
         p.pid = (uint32_t)q;
         bank_push(&o->census, &p);
     }
+    o->pidLimit = in->count ? in->count : 1;
     return 0;
 }
 uint64_t orc_census_count(Oracle *o) { return o->census.n; }

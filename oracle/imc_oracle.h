@@ -66,7 +66,7 @@ void orc_isotropic(const double *tape2, double clight, double *out3);
 /* Philox4x32-10 and the engine's uniform mapping */
 void orc_philox4x32_10(const uint32_t ctr[4], const uint32_t key[2], uint32_t out[4]);
 double orc_uniform(uint64_t seed, uint32_t tag, uint32_t step, uint32_t pid, uint32_t draw);
-uint32_t orc_comb_key(uint64_t seed, uint32_t step, uint32_t pid);
+uint32_t orc_comb_key(uint64_t seed, uint32_t step, uint32_t pid, int b);
 uint32_t orc_step_index(Oracle *o);
 
 #ifdef __cplusplus

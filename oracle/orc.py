@@ -58,7 +58,7 @@ def lib():
         L.orc_uniform.restype = C.c_double
         L.orc_uniform.argtypes = [C.c_uint64, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32]
         L.orc_comb_key.restype = C.c_uint32
-        L.orc_comb_key.argtypes = [C.c_uint64, C.c_uint32, C.c_uint32]
+        L.orc_comb_key.argtypes = [C.c_uint64, C.c_uint32, C.c_uint32, C.c_int]
         _lib = L
     return _lib
 

@@ -72,7 +72,8 @@ struct Ctx {
     // FP32-tracking form
     int32_t fp32;            // banks hold cell-local FP32 offsets and FP32 directions
     const float *hx, *hy, *hz;   // half widths per axis
-    const float4 *phys32;    // x = 1/sigma_e (inf when none), y = sigma_a f [1/cm]
+    const float4 *phys32;    // x = 1/sigma_e (inf when none), y = sigma_a f [1/cm], z = RW reach, w = -1/(sigma_a f c)
+    float rwDiffPerReach;    // c / (3 rwMinParticleOpticalDepth): diffusion coefficient = reach * this
     float reflNudge[6];      // 1e-6 * faceScale of each box face, capped at a quarter cell
     double invC;             // 1 / c
     // per-cell arrays
@@ -578,19 +579,20 @@ __device__ inline float rw_sample_radius32(const RwTables &T, float tau, float x
 // the FP32-tracking form: cell-local FP32 geometry, FP64 time, weight and
 // tallies, the same draws in the same order as the FP64 form.  Ro is the
 // distance to the nearest face (the caller has checked Ro >= rwMinParticle /
-// sigma_T); cp.w is the diffusion coefficient c / (3 sigma_T).
+// sigma_T); the diffusion coefficient c / (3 sigma_T) is cp.z * C.rwDiffPerReach.
 template <class RNG, class TALLY>
 __device__ inline int rw_jump32(const Ctx &C, Track32 &T, RNG &rng, TALLY &tal, const float4 &cp, float Ro, float hx,
                                 float hy, float hz, int &err) {
     const uint32_t cell = T.cell;
+    const float D = cp.z * C.rwDiffPerReach;
     const float tauLeak = rw_sample_leak32(C.rw, rng.rawf());
-    const double tLeak = static_cast<double>(tauLeak * (Ro * Ro) / cp.w);
+    const double tLeak = static_cast<double>(tauLeak * (Ro * Ro) / D);
     const bool leak = tLeak <= T.t;
     const double dt = leak ? tLeak : T.t;
     const float tau = cp.y * static_cast<float>(dt * C.clight);
     const double e1 = static_cast<double>(expm1f(-tau));
     if (!C.noFeedback) tal.mat(cell, -e1 * T.w);
-    if (cp.y > 0.0f) tal.rad(cell, T.w * e1 * C.phys[cell].z);
+    if (cp.y > 0.0f) tal.rad(cell, T.w * e1 * static_cast<double>(cp.w));
     T.w *= 1.0 + e1;
     T.t -= dt;
     if (fabs(T.w) < T.w0 * 1e-4) {
@@ -604,7 +606,7 @@ __device__ inline int rw_jump32(const Ctx &C, Track32 &T, RNG &rng, TALLY &tal, 
     const float dx = sinT * cphi, dy = sinT * sphi, dz = cosT;
     float disp = Ro;
     if (!leak) {
-        const float tauPos = static_cast<float>(dt) * cp.w / (Ro * Ro);
+        const float tauPos = static_cast<float>(dt) * D / (Ro * Ro);
         disp = fminf(Ro * rw_sample_radius32(C.rw, tauPos, rng.rawf()), Ro);
     }
     const float nudge = 1.0f - static_cast<float>(RW_NUDGE);   // toward the cell centre (local origin)
@@ -673,7 +675,7 @@ __device__ inline int segment32(const Ctx &C, Track32 &T, RNG &rng, TALLY &tal, 
     const float tau = cp.y * ds;
     const double e1 = static_cast<double>(expm1f(-tau));
     double integrated = T.w * dt;
-    if (tau >= 1e-12f) integrated = T.w * e1 * C.phys[cell].z;
+    if (tau >= 1e-12f) integrated = T.w * e1 * static_cast<double>(cp.w);
     T.qx = clampf(fmaf(T.ux, ds, T.qx), hx);
     T.qy = clampf(fmaf(T.uy, ds, T.qy), hy);
     T.qz = clampf(fmaf(T.uz, ds, T.qz), hz);

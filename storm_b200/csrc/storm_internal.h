@@ -96,20 +96,21 @@ int refill_blocks_per_sm(int minBlocks, bool fp32);
 void launch_bank_to_local(cudaStream_t s, const Ctx &C, const Bank &src, const Bank &dst, uint32_t n);
 void launch_bank_to_global(cudaStream_t s, const Ctx &C, const Bank &src, const Bank &dst, uint32_t n);
 void launch_comb_keys(cudaStream_t s, const Ctx &C, const CensusBank &cen, uint32_t n, uint64_t *keys, uint32_t *vals,
-                      uint32_t combKey);
+                      uint32_t combKey, int pidBits);
 int launch_radix_sort(cudaStream_t s, uint64_t *keys, uint32_t *vals, uint64_t *keysAlt, uint32_t *valsAlt, uint32_t n,
                       int bits, uint32_t *tileHist);
 uint32_t radix_tile_count(uint32_t n);
-void launch_comb_ranges(cudaStream_t s, const uint64_t *keys, uint32_t n, uint32_t ncells, uint32_t *start);
-void launch_comb_cell_sums(cudaStream_t s, const Ctx &C, const CensusBank &cen, const uint32_t *idx,
-                           const uint32_t *start, uint32_t ncells, double *W);
+void launch_comb_ranges(cudaStream_t s, const uint64_t *keys, uint32_t n, uint32_t ncells, uint32_t *start, int pidBits);
+void launch_sorted_weights(cudaStream_t s, const Ctx &C, const CensusBank &cen, const uint32_t *idx, uint32_t n,
+                           double *wS);
+void launch_comb_cell_sums(cudaStream_t s, const double *wS, const uint32_t *start, uint32_t ncells, double *W);
 void launch_blocked_sum(cudaStream_t s, const double *v, uint32_t n, double *out);
-void launch_comb_plan(cudaStream_t s, const Ctx &C, const CombParams &P, const CensusBank &cen, const uint32_t *idx,
-                      const uint32_t *start, const double *W, const double *Wtot, uint32_t *pCount, double *pWeight,
-                      uint64_t *cellCount, double *eradCensus, DevStats *st);
+void launch_comb_plan(cudaStream_t s, const Ctx &C, const CombParams &P, const double *wS, const uint32_t *start,
+                      const double *W, const double *Wtot, uint32_t *pCount, double *pWeight, uint64_t *cellCount,
+                      double *eradCensus, DevStats *st);
 void launch_comb_emit(cudaStream_t s, const Ctx &C, const CensusBank &cen, const uint32_t *idx, const uint64_t *sortedKeys,
-                      uint32_t nValid, const uint32_t *pCount, const double *pWeight, const uint64_t *pOffset,
-                      const Bank &out);
+                      int pidBits, uint32_t nValid, const uint32_t *pCount, const double *pWeight,
+                      const uint64_t *pOffset, const Bank &out);
 void launch_mask_count(cudaStream_t s, const uint32_t *pCount, uint32_t n, uint64_t *out);
 void launch_allocate_checked(cudaStream_t s, const Ctx &C, const CellArrays &A, const double *total,
                              uint64_t newPerCell, double rel, int32_t *ambiguous);

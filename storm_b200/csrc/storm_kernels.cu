@@ -227,7 +227,7 @@ __global__ void k_begin(Bank b, uint32_t n, double dt, DevStats *st) {
 // form's segment constants: x = 1/sigma_e (inf when none), y = sigma_a f,
 // z = rwMinParticleOpticalDepth / sigma_T, the distance to the nearest face a
 // particle needs for a Random Walk jump (inf in cells that are not eligible),
-// w = the diffusion coefficient c / (3 sigma_T).
+// w = -1 / (sigma_a f c), the factor from exp-deposit to time-integrated energy.
 __device__ __forceinline__ void cell_rw_and_phys32(const Ctx &C, const CellArrays &A, uint32_t c, double sa, double ss,
                                                    double f) {
     const double sigmaT = sa + ss;
@@ -247,10 +247,11 @@ __device__ __forceinline__ void cell_rw_and_phys32(const Ctx &C, const CellArray
     if (C.fp32) {
         const double eventOpacity = ss + (1.0 - f) * sa;
         const bool rw = elig && sigmaT > 0.0;
+        const double rate = sa * f * C.clight;
         A.phys32[c] = make_float4(eventOpacity > 0.0 ? static_cast<float>(1.0 / eventOpacity) : CUDART_INF_F,
                                   static_cast<float>(sa * f),
                                   rw ? static_cast<float>(C.rwMinParticle / sigmaT) : CUDART_INF_F,
-                                  rw ? static_cast<float>(C.clight / (3.0 * sigmaT)) : 0.0f);
+                                  rate > 0.0 ? static_cast<float>(-1.0 / rate) : 0.0f);
     }
 }
 
@@ -944,7 +945,8 @@ __global__ void __launch_bounds__(256, MINB) k_transport_refill(Ctx C, Bank in, 
 
 // ------------------------------------------------------------------ comb
 // CombPopulationControl::activate (population/CombPopulationControl.hpp:79-253).
-// Sort key = (cell << 32) | bijective hash of the particle's pid: a pseudo-random
+// Sort key = (cell << b) | keyed bijective hash of the particle's pid on b bits
+// (every pid of the step is below 2^b): a pseudo-random
 // order inside each cell (the reference sorts by id then std::shuffles) that does
 // not depend on the order particles reached census.  Zero-weight particles get
 // cell = Ncells and sort last (they are skipped, :136-137).
@@ -952,7 +954,22 @@ __device__ __forceinline__ uint32_t fmix32(uint32_t h) {
     h ^= h >> 16; h *= 0x85ebca6bu; h ^= h >> 13; h *= 0xc2b2ae35u; h ^= h >> 16;
     return h;
 }
-__global__ void k_comb_keys(Ctx C, CensusBank cen, uint32_t n, uint64_t *keys, uint32_t *vals, uint32_t combKey) {
+// A keyed bijection of [0, 2^b): xor with the key, then odd multiplications and
+// xor-shifts, each invertible modulo 2^b.  pid < 2^b, so (cell << b) | hash is a
+// total order with no ties in b + cell bits.
+__device__ __forceinline__ uint32_t comb_hash(uint32_t pid, uint32_t key, int b) {
+    const uint32_t mask = b >= 32 ? 0xffffffffu : ((1u << b) - 1u);
+    uint32_t h = (pid ^ key) & mask;
+    h = (h * 0x9E3779B1u) & mask;
+    h ^= h >> ((b + 1) / 2);
+    h = (h * 0x85EBCA77u) & mask;
+    h ^= h >> ((b + 2) / 3);
+    h = (h * 0xC2B2AE3Du) & mask;
+    h ^= h >> ((b + 1) / 2);
+    return h;
+}
+__global__ void k_comb_keys(Ctx C, CensusBank cen, uint32_t n, uint64_t *keys, uint32_t *vals, uint32_t combKey,
+                            int pidBits) {
     for (uint32_t q = blockIdx.x * blockDim.x + threadIdx.x; q < n; q += gridDim.x * blockDim.x) {
         const double w = census_w(C, cen, q);
         const uint2 cp = census_cell_pid(C, cen, q);
@@ -967,7 +984,7 @@ __global__ void k_comb_keys(Ctx C, CensusBank cen, uint32_t n, uint64_t *keys, u
         if (badWeight) raise_error(C, STORM_DERR_COMB_WEIGHT, cell, pid);
         // zero, negative and non-finite weights never reach the per-cell loops
         if (w == 0.0 || badWeight || cell >= C.ncells) cell = C.ncells;
-        keys[q] = (static_cast<uint64_t>(cell) << 32) | fmix32(pid ^ combKey);
+        keys[q] = (static_cast<uint64_t>(cell) << pidBits) | comb_hash(pid, combKey, pidBits);
         vals[q] = q;
     }
 }
@@ -1020,54 +1037,89 @@ __global__ void k_rs_scan(uint32_t *tileHist, uint32_t len) {
     }
 }
 
+// Stable scatter of one 8-bit digit.  The block ranks its tile in shared memory
+// (per-warp match_any counts, then a scan over digits), stages the tile there in
+// digit order and writes it out in runs of equal digits, so global writes are
+// coalesced within each run.
+constexpr int RS_PER_THREAD = RS_PER_WARP / 32;
+constexpr size_t RS_SMEM = static_cast<size_t>(RS_TILE) * 12 + RS_WARPS * 256 * 4 + 2 * 256 * 4;
+
 __global__ void __launch_bounds__(RS_THREADS) k_rs_scatter(const uint64_t *kin, const uint32_t *vin, uint64_t *kout,
                                                            uint32_t *vout, uint32_t n, int shift,
                                                            const uint32_t *tileOff, uint32_t ntiles) {
-    __shared__ uint32_t wc[RS_WARPS][257];
+    extern __shared__ __align__(16) unsigned char rsMem[];
+    __shared__ uint64_t scanSh[32];
+    uint64_t *sk = reinterpret_cast<uint64_t *>(rsMem);
+    uint32_t *sv = reinterpret_cast<uint32_t *>(rsMem + static_cast<size_t>(RS_TILE) * 8);
+    uint32_t(*wc)[256] = reinterpret_cast<uint32_t(*)[256]>(rsMem + static_cast<size_t>(RS_TILE) * 12);
+    uint32_t *dstart = reinterpret_cast<uint32_t *>(rsMem + static_cast<size_t>(RS_TILE) * 12 + RS_WARPS * 256 * 4);
+    uint32_t *gbase = dstart + 256;
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-    for (int d = lane; d < 257; d += 32) wc[wid][d] = 0;
+    for (int d = lane; d < 256; d += 32) wc[wid][d] = 0;
     __syncwarp();
-    const uint32_t start = blockIdx.x * RS_TILE + wid * RS_PER_WARP;
-    for (int it = 0; it < RS_PER_WARP / 32; ++it) {
-        uint32_t q = start + it * 32 + lane;
-        uint32_t d = (q < n) ? static_cast<uint32_t>((kin[q] >> shift) & 255u) : 256u;
-        unsigned m = __match_any_sync(FULL, d);
-        if ((__ffs(m) - 1) == lane) wc[wid][d] += __popc(m);
+    const uint32_t tileBase = blockIdx.x * RS_TILE;
+    const uint32_t start = tileBase + wid * RS_PER_WARP;
+    const unsigned lt = lanemask_lt();
+    uint64_t key[RS_PER_THREAD];
+    uint32_t val[RS_PER_THREAD], rank[RS_PER_THREAD];
+#pragma unroll
+    for (int it = 0; it < RS_PER_THREAD; ++it) {
+        const uint32_t q = start + it * 32 + lane;
+        key[it] = q < n ? kin[q] : 0;
+        val[it] = q < n ? vin[q] : 0;
+    }
+#pragma unroll
+    for (int it = 0; it < RS_PER_THREAD; ++it) {
+        const uint32_t q = start + it * 32 + lane;
+        const uint32_t d = q < n ? static_cast<uint32_t>((key[it] >> shift) & 255u) : 256u;
+        const unsigned m = __match_any_sync(FULL, d);
+        const uint32_t before = d < 256u ? wc[wid][d] : 0u;
+        __syncwarp();
+        rank[it] = before + __popc(m & lt);
+        if (d < 256u && (__ffs(m) - 1) == lane) wc[wid][d] = before + __popc(m);
         __syncwarp();
     }
     __syncthreads();
     {
-        const uint32_t d = threadIdx.x;   // 256 threads, one digit each
-        uint32_t run = tileOff[d * ntiles + blockIdx.x];
+        // digit d: per-warp exclusive offsets within the digit, then the digit's start in the tile
+        const uint32_t d = threadIdx.x;
+        uint32_t run = 0;
+#pragma unroll
         for (int w = 0; w < RS_WARPS; ++w) {
-            uint32_t c = wc[w][d];
+            const uint32_t c = wc[w][d];
             wc[w][d] = run;
             run += c;
         }
+        const uint64_t incl = block_scan_incl(run, scanSh);
+        dstart[d] = static_cast<uint32_t>(incl - run);
+        gbase[d] = tileOff[d * ntiles + blockIdx.x];
     }
     __syncthreads();
-    const unsigned lt = lanemask_lt();
-    for (int it = 0; it < RS_PER_WARP / 32; ++it) {
-        uint32_t q = start + it * 32 + lane;
-        const bool valid = q < n;
-        uint64_t key = valid ? kin[q] : 0;
-        uint32_t d = valid ? static_cast<uint32_t>((key >> shift) & 255u) : 256u;
-        unsigned m = __match_any_sync(FULL, d);
-        uint32_t pos = wc[wid][d] + __popc(m & lt);
-        __syncwarp();
-        if (valid) {
-            kout[pos] = key;
-            vout[pos] = vin[q];
-            if ((__ffs(m) - 1) == lane) wc[wid][d] += __popc(m);
+#pragma unroll
+    for (int it = 0; it < RS_PER_THREAD; ++it) {
+        const uint32_t q = start + it * 32 + lane;
+        if (q < n) {
+            const uint32_t d = static_cast<uint32_t>((key[it] >> shift) & 255u);
+            const uint32_t pos = dstart[d] + wc[wid][d] + rank[it];
+            sk[pos] = key[it];
+            sv[pos] = val[it];
         }
-        __syncwarp();
+    }
+    __syncthreads();
+    const uint32_t cnt = min(static_cast<uint32_t>(RS_TILE), n - tileBase);
+    for (uint32_t pos = threadIdx.x; pos < cnt; pos += RS_THREADS) {
+        const uint64_t k = sk[pos];
+        const uint32_t d = static_cast<uint32_t>((k >> shift) & 255u);
+        const uint32_t g = gbase[d] + (pos - dstart[d]);
+        kout[g] = k;
+        vout[g] = sv[pos];
     }
 }
 
-// first sorted position of each cell (lower_bound of cell << 32), cells 0..N
-__global__ void k_comb_ranges(const uint64_t *keys, uint32_t n, uint32_t ncells, uint32_t *start) {
+// first sorted position of each cell (lower_bound of cell << pidBits), cells 0..N
+__global__ void k_comb_ranges(const uint64_t *keys, uint32_t n, uint32_t ncells, uint32_t *start, int pidBits) {
     for (uint32_t c = blockIdx.x * blockDim.x + threadIdx.x; c <= ncells; c += gridDim.x * blockDim.x) {
-        const uint64_t v = static_cast<uint64_t>(c) << 32;
+        const uint64_t v = static_cast<uint64_t>(c) << pidBits;
         uint32_t first = 0, count = n;
         while (count > 0) {
             uint32_t step = count >> 1, it = first + step;
@@ -1077,12 +1129,17 @@ __global__ void k_comb_ranges(const uint64_t *keys, uint32_t n, uint32_t ncells,
     }
 }
 
+// census weights in sorted order (one gather, so the per-cell loops read contiguous memory)
+__global__ void k_sorted_weights(Ctx C, CensusBank cen, const uint32_t *idx, uint32_t n, double *wS) {
+    for (uint32_t q = blockIdx.x * blockDim.x + threadIdx.x; q < n; q += gridDim.x * blockDim.x)
+        wS[q] = census_w(C, cen, idx[q]);
+}
+
 // weights[cell] (:136-141), summed in sorted order
-__global__ void k_comb_cell_sums(Ctx C, CensusBank cen, const uint32_t *idx, const uint32_t *start, uint32_t ncells,
-                                 double *W) {
+__global__ void k_comb_cell_sums(const double *wS, const uint32_t *start, uint32_t ncells, double *W) {
     for (uint32_t c = blockIdx.x * blockDim.x + threadIdx.x; c < ncells; c += gridDim.x * blockDim.x) {
         double s = 0.0;
-        for (uint32_t q = start[c]; q < start[c + 1]; ++q) s += census_w(C, cen, idx[q]);
+        for (uint32_t q = start[c]; q < start[c + 1]; ++q) s += wS[q];
         W[c] = s;
     }
 }
@@ -1127,7 +1184,7 @@ __device__ __forceinline__ CombCell comb_cell_params(const Ctx &C, const CombPar
 // of those copies, and the cell's census radiation energy summed in output order
 // (RadiationIMC::postStep :2013-2016).  pCount bit 31 marks a particle kept as is.
 constexpr uint32_t KEEP = 0x80000000u;
-__global__ void k_comb_plan(Ctx C, CombParams P, CensusBank cen, const uint32_t *idx, const uint32_t *start, const double *W,
+__global__ void k_comb_plan(Ctx C, CombParams P, const double *wS, const uint32_t *start, const double *W,
                             const double *Wtot, uint32_t *pCount, double *pWeight, uint64_t *cellCount,
                             double *eradCensus, DevStats *st) {
     const double tot = *Wtot;
@@ -1145,7 +1202,7 @@ __global__ void k_comb_plan(Ctx C, CombParams P, CensusBank cen, const uint32_t 
             CombCell cc = comb_cell_params(C, P, c, b - a, W[c], tot);
             if (cc.mode == 0) {
                 for (uint32_t q = a; q < b; ++q) {
-                    const double w = census_w(C, cen, idx[q]);
+                    const double w = wS[q];
                     if (w > 2 * cc.w_ideal) {
                         const uint64_t ns = static_cast<uint64_t>(ceil(w / cc.w_ideal));
                         const double ws = w / static_cast<double>(ns);
@@ -1164,7 +1221,7 @@ __global__ void k_comb_plan(Ctx C, CombParams P, CensusBank cen, const uint32_t 
                 uint64_t k = 0;
                 double cum = 0;
                 for (uint32_t q = a; q < b; ++q) {
-                    const double w = census_w(C, cen, idx[q]);
+                    const double w = wS[q];
                     const uint64_t k0 = k;
                     while ((cum + w) > (static_cast<double>(k) + cc.r) * cc.e) {
                         ++k;
@@ -1188,13 +1245,14 @@ __global__ void k_comb_plan(Ctx C, CombParams P, CensusBank cen, const uint32_t 
 // One thread per sorted particle writes its copies at its output offset.
 // The exclusive prefix of the copy counts over sorted particles is the output
 // position: cells are contiguous in sorted order and the output is cell-major.
-__global__ void k_comb_emit(Ctx C, CensusBank cen, const uint32_t *idx, const uint64_t *sortedKeys, uint32_t nValid,
-                            const uint32_t *pCount, const double *pWeight, const uint64_t *pOffset, Bank out) {
+__global__ void k_comb_emit(Ctx C, CensusBank cen, const uint32_t *idx, const uint64_t *sortedKeys, int pidBits,
+                            uint32_t nValid, const uint32_t *pCount, const double *pWeight, const uint64_t *pOffset,
+                            Bank out) {
     for (uint32_t q = blockIdx.x * blockDim.x + threadIdx.x; q < nValid; q += gridDim.x * blockDim.x) {
         const uint32_t raw = pCount[q];
         const uint32_t m = raw & ~KEEP;
         if (m == 0) continue;
-        const uint32_t c = static_cast<uint32_t>(sortedKeys[q] >> 32);
+        const uint32_t c = static_cast<uint32_t>(sortedKeys[q] >> pidBits);
         if (C.fp32) {
             Track32 T;
             uint32_t pid_, draw_;
@@ -1478,12 +1536,14 @@ int transport_blocks_per_sm(int minBlocks, bool fp32) {
     return nb;
 }
 void launch_comb_keys(cudaStream_t s, const Ctx &C, const CensusBank &cen, uint32_t n, uint64_t *keys, uint32_t *vals,
-                      uint32_t combKey) {
-    k_comb_keys<<<grid_for(n, 256, 8192), 256, 0, s>>>(C, cen, n, keys, vals, combKey);
+                      uint32_t combKey, int pidBits) {
+    k_comb_keys<<<grid_for(n, 256, 8192), 256, 0, s>>>(C, cen, n, keys, vals, combKey, pidBits);
 }
 int launch_radix_sort(cudaStream_t s, uint64_t *keys, uint32_t *vals, uint64_t *keysAlt, uint32_t *valsAlt, uint32_t n,
                       int bits, uint32_t *tileHist) {
     // returns 1 when the sorted data ends in the Alt buffers
+    // the scatter stages a tile in more than the default 48 KB of shared memory (set on the current device)
+    cudaFuncSetAttribute(k_rs_scatter, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(RS_SMEM));
     const uint32_t ntiles = (n + RS_TILE - 1) / RS_TILE ? (n + RS_TILE - 1) / RS_TILE : 1;
     int passes = (bits + 7) / 8;
     uint64_t *ka = keys, *kb = keysAlt;
@@ -1496,7 +1556,7 @@ int launch_radix_sort(cudaStream_t s, uint64_t *keys, uint32_t *vals, uint64_t *
         k_scan32_tiles<<<stiles, 1024, 0, s>>>(tileHist, len, scanSums);
         k_scan_sums<<<1, 1024, 0, s>>>(scanSums, stiles, scanSums + stiles);
         k_scan32_add<<<stiles, 1024, 0, s>>>(tileHist, len, scanSums);
-        k_rs_scatter<<<ntiles, RS_THREADS, 0, s>>>(ka, va, kb, vb, n, 8 * p, tileHist, ntiles);
+        k_rs_scatter<<<ntiles, RS_THREADS, RS_SMEM, s>>>(ka, va, kb, vb, n, 8 * p, tileHist, ntiles);
         uint64_t *tk = ka; ka = kb; kb = tk;
         uint32_t *tv = va; va = vb; vb = tv;
     }
@@ -1509,27 +1569,30 @@ size_t radix_scratch_words(uint32_t n) {
     size_t stiles = (len + 1023) / 1024;
     return len + (len & 1) + 2 * (stiles + 2);
 }
-void launch_comb_ranges(cudaStream_t s, const uint64_t *keys, uint32_t n, uint32_t ncells, uint32_t *start) {
-    k_comb_ranges<<<grid_for(ncells + 1, 256, 8192), 256, 0, s>>>(keys, n, ncells, start);
+void launch_comb_ranges(cudaStream_t s, const uint64_t *keys, uint32_t n, uint32_t ncells, uint32_t *start, int pidBits) {
+    k_comb_ranges<<<grid_for(ncells + 1, 256, 8192), 256, 0, s>>>(keys, n, ncells, start, pidBits);
 }
-void launch_comb_cell_sums(cudaStream_t s, const Ctx &C, const CensusBank &cen, const uint32_t *idx,
-                           const uint32_t *start, uint32_t ncells, double *W) {
-    k_comb_cell_sums<<<grid_for(ncells, 128, 8192), 128, 0, s>>>(C, cen, idx, start, ncells, W);
+void launch_sorted_weights(cudaStream_t s, const Ctx &C, const CensusBank &cen, const uint32_t *idx, uint32_t n,
+                           double *wS) {
+    if (n) k_sorted_weights<<<grid_for(n, 256, 8192), 256, 0, s>>>(C, cen, idx, n, wS);
+}
+void launch_comb_cell_sums(cudaStream_t s, const double *wS, const uint32_t *start, uint32_t ncells, double *W) {
+    k_comb_cell_sums<<<grid_for(ncells, 128, 8192), 128, 0, s>>>(wS, start, ncells, W);
 }
 void launch_blocked_sum(cudaStream_t s, const double *v, uint32_t n, double *out) {
     k_blocked_sum<<<1, 1024, 0, s>>>(v, n, out);
 }
-void launch_comb_plan(cudaStream_t s, const Ctx &C, const CombParams &P, const CensusBank &cen, const uint32_t *idx,
-                      const uint32_t *start, const double *W, const double *Wtot, uint32_t *pCount, double *pWeight,
-                      uint64_t *cellCount, double *eradCensus, DevStats *st) {
-    k_comb_plan<<<grid_for(C.ncells, 128, 8192), 128, 0, s>>>(C, P, cen, idx, start, W, Wtot, pCount, pWeight, cellCount,
+void launch_comb_plan(cudaStream_t s, const Ctx &C, const CombParams &P, const double *wS, const uint32_t *start,
+                      const double *W, const double *Wtot, uint32_t *pCount, double *pWeight, uint64_t *cellCount,
+                      double *eradCensus, DevStats *st) {
+    k_comb_plan<<<grid_for(C.ncells, 128, 8192), 128, 0, s>>>(C, P, wS, start, W, Wtot, pCount, pWeight, cellCount,
                                                                eradCensus, st);
 }
 void launch_comb_emit(cudaStream_t s, const Ctx &C, const CensusBank &cen, const uint32_t *idx, const uint64_t *sortedKeys,
-                      uint32_t nValid, const uint32_t *pCount, const double *pWeight, const uint64_t *pOffset,
-                      const Bank &out) {
+                      int pidBits, uint32_t nValid, const uint32_t *pCount, const double *pWeight,
+                      const uint64_t *pOffset, const Bank &out) {
     if (!nValid) return;
-    k_comb_emit<<<grid_for(nValid, 256, 148 * 16), 256, 0, s>>>(C, cen, idx, sortedKeys, nValid, pCount, pWeight,
+    k_comb_emit<<<grid_for(nValid, 256, 148 * 16), 256, 0, s>>>(C, cen, idx, sortedKeys, pidBits, nValid, pCount, pWeight,
                                                                 pOffset, out);
 }
 void launch_mask_count(cudaStream_t s, const uint32_t *pCount, uint32_t n, uint64_t *out) {

@@ -77,6 +77,7 @@ struct StormHandle {
     // host state
     uint64_t nCensus = 0;            // particles at the head of bankA
     uint64_t nBank = 0;              // particles in bankA after emission
+    uint64_t pidLimit = 1;           // every pid of the current census is below this (comb key width)
     uint32_t step = 0;
     uint32_t K = 8, maxRounds = 4096;
     int minBlocks = 3;               // transport occupancy variant (__launch_bounds__ min blocks); 4 for FP32
@@ -555,6 +556,7 @@ int storm_cuda_create(const StormProblemDesc *d, StormHandle **out) {
     C.clight = d->clight; C.arad = d->arad; C.sigmaSB = d->sigma_sb; C.kevKelvin = d->kev_kelvin;
     C.rwMinParticle = d->rw_min_particle_optical_depth;
     C.rwMinCell = d->rw_min_cell_optical_depth;
+    C.rwDiffPerReach = C.rwMinParticle > 0.0 ? static_cast<float>(C.clight / (3.0 * C.rwMinParticle)) : 0.0f;
     C.seedLo = static_cast<uint32_t>(d->seed);
     C.seedHi = static_cast<uint32_t>(d->seed >> 32);
     C.step = 0;
@@ -686,6 +688,7 @@ int storm_cuda_phase_transport(StormHandle *h) {
     if (!h) return STORM_ERR_INVALID_ARG;
     refresh_ctx(h);
     const uint64_t n0 = h->nBank;
+    h->pidLimit = n0 ? n0 : 1;   // transport pids are bank slots
     CK(cudaEventRecord(h->evTransport0, h->stream));
     CK(cudaMemsetAsync(h->counts, 0, sizeof(uint32_t) * (h->maxRounds + 2), h->stream));
     if (h->desc.per_cell_segment_counters) CK(cudaMemsetAsync(h->segs, 0, sizeof(uint32_t) * h->N, h->stream));
@@ -800,6 +803,13 @@ int storm_cuda_phase_transport(StormHandle *h) {
     return STORM_OK;
 }
 
+// bits of the comb's pid hash: the smallest b >= 1 with 2^b >= pidLimit
+int pid_bits(const StormHandle *h) {
+    int b = 1;
+    while (b < 32 && (1ull << b) < h->pidLimit) ++b;
+    return b;
+}
+
 int storm_cuda_phase_comb(StormHandle *h) {
     if (!h) return STORM_ERR_INVALID_ARG;
     refresh_ctx(h);
@@ -815,7 +825,7 @@ int storm_cuda_phase_comb(StormHandle *h) {
         // NoPopulationControl (population/NoPopulationControl.hpp:25-28): the census
         // passes unchanged; order it by pid so the next step's streams are reproducible.
         launch_census_keys_pid(h->stream, h->C, h->bankC, n, h->keys, h->vals);
-        int alt = launch_radix_sort(h->stream, h->keys, h->vals, h->keysAlt, h->valsAlt, n, 32, h->tileHist);
+        int alt = launch_radix_sort(h->stream, h->keys, h->vals, h->keysAlt, h->valsAlt, n, pid_bits(h), h->tileHist);
         const uint32_t *idx = alt ? h->valsAlt : h->vals;
         launch_gather(h->stream, h->C, h->bankC, idx, n, h->bankA, h->A.eradCensus, h->dStats);
         h->launches += 2 + 3 * 4;
@@ -832,22 +842,26 @@ int storm_cuda_phase_comb(StormHandle *h) {
         };
         return fm(static_cast<uint32_t>(h->desc.seed) ^ fm(h->step * 0x9E3779B9u + static_cast<uint32_t>(h->desc.seed >> 32)));
     }();
-    launch_comb_keys(h->stream, h->C, h->bankC, n, h->keys, h->vals, combKey);
+    const int pidBits = pid_bits(h);
+    launch_comb_keys(h->stream, h->C, h->bankC, n, h->keys, h->vals, combKey, pidBits);
     int cellBits = 0;
     while ((1ull << cellBits) <= N) ++cellBits;
-    int alt = launch_radix_sort(h->stream, h->keys, h->vals, h->keysAlt, h->valsAlt, n, 32 + cellBits, h->tileHist);
+    int alt = launch_radix_sort(h->stream, h->keys, h->vals, h->keysAlt, h->valsAlt, n, pidBits + cellBits, h->tileHist);
     const uint64_t *skeys = alt ? h->keysAlt : h->keys;
     const uint32_t *idx = alt ? h->valsAlt : h->vals;
-    const int passes = (32 + cellBits + 7) / 8;
-    launch_comb_ranges(h->stream, skeys, n, N, h->combStart);
-    launch_comb_cell_sums(h->stream, h->C, h->bankC, idx, h->combStart, N, h->combW);
+    const int passes = (pidBits + cellBits + 7) / 8;
+    // census weights in sorted order; comb_plan overwrites each slot with the copies' weight
+    double *wS = h->pWeight;
+    launch_comb_ranges(h->stream, skeys, n, N, h->combStart, pidBits);
+    launch_sorted_weights(h->stream, h->C, h->bankC, idx, n, wS);
+    launch_comb_cell_sums(h->stream, wS, h->combStart, N, h->combW);
     launch_blocked_sum(h->stream, h->combW, N, h->combWtot);
     CombParams P;
     P.nmin = h->desc.comb_nmin;
     P.ntotal = static_cast<uint64_t>(static_cast<double>(static_cast<uint64_t>(N) * h->desc.comb_nmin) * h->desc.comb_factor);
-    launch_comb_plan(h->stream, h->C, P, h->bankC, idx, h->combStart, h->combW, h->combWtot, h->pCount, h->pWeight,
+    launch_comb_plan(h->stream, h->C, P, wS, h->combStart, h->combW, h->combWtot, h->pCount, h->pWeight,
                      h->combCount, h->A.eradCensus, h->dStats);
-    h->launches += 1 + 5 * passes + 4;
+    h->launches += 1 + 5 * passes + 5;
     CK(cudaGetLastError());
     uint32_t nValid = 0;
     CK(cudaMemcpyAsync(&nValid, h->combStart + N, sizeof(uint32_t), cudaMemcpyDeviceToHost, h->stream));
@@ -878,7 +892,7 @@ int storm_cuda_phase_comb(StormHandle *h) {
         CK(bank_alloc(h, h->bankA, grown));
         CK(bank_alloc(h, h->bankB, grown));
     }
-    launch_comb_emit(h->stream, h->C, h->bankC, idx, skeys, nValid, h->pCount, h->pWeight, h->pOff, h->bankA);
+    launch_comb_emit(h->stream, h->C, h->bankC, idx, skeys, pidBits, nValid, h->pCount, h->pWeight, h->pOff, h->bankA);
     ++h->launches;
     CK(cudaGetLastError());
     if (grown) {
@@ -1012,6 +1026,7 @@ int storm_cuda_population_control(StormHandle *h, const StormParticlesSoA *in) {
     CK(cudaMemsetAsync(h->dErr, 0, 4 * sizeof(int32_t), h->stream));
     h->stats = StormStepStats{};
     h->stats.census_out_pre_comb = n;
+    h->pidLimit = n ? n : 1;
     return storm_cuda_phase_comb(h);
 }
 
