@@ -243,14 +243,20 @@ def run_form(args, precision, seed, local, dist, timed=True):
     eng.transport_timing(reset=True)
     l0 = eng.launches()
     step_ms, segs = [], 0
+    phase = {"emit": 0.0, "transport": 0.0, "comb": 0.0}
     for _ in range(args.steps if timed else 0):
         st = eng.step()
         step_ms.append(st["step_ms"])
         segs += st["segments"]
+        for k in phase:
+            phase[k] += st[k + "_ms"]
     torch.cuda.synchronize()
     barrier(dist, "storm")
+    k = max(len(step_ms), 1)
+    phase = {name: v / k for name, v in phase.items()}
+    phase["other"] = sum(step_ms) / k - sum(phase.values())
     out = {"engine": eng, "problem": p, "step_ms": step_ms, "segments": segs, "launches": eng.launches() - l0,
-           "transport": eng.transport_timing(reset=True)}
+           "transport": eng.transport_timing(reset=True), "phase_ms": phase}
     return out
 
 
@@ -382,11 +388,13 @@ def run_storm(args, ws, rank, local, dist):
                                                  "form": "FP32 cell-local tracking, FP64 time/weights/tallies"},
             "latency_ms": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99))},
             "segments_per_step": f32["segments"] / args.steps,
+            "phase_ms_per_step": f32["phase_ms"],
             "roofline": roofline(f32, BYTES_PER_SEGMENT_FP32, transport_kernel(args, True)),
             "fp64": {"value": v64, "ms_per_step": ms64 / args.steps, "dtype": "f64",
                      "latency_ms": {"p50": float(np.percentile(f64["step_ms"], 50)),
                                     "p99": float(np.percentile(f64["step_ms"], 99))},
                      "segments_per_step": f64["segments"] / args.steps,
+                     "phase_ms_per_step": f64["phase_ms"],
                      "roofline": roofline(f64, BYTES_PER_SEGMENT_FP64, transport_kernel(args, False))},
             "fp32_over_fp64": v32 / v64,
             "fp32_vs_fp64_deviation": dev,

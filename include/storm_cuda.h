@@ -36,7 +36,7 @@
 extern "C" {
 #endif
 
-#define STORM_CUDA_ABI_VERSION 1
+#define STORM_CUDA_ABI_VERSION 2
 
 /* ---------------------------------------------------------------- status */
 enum StormStatus {
@@ -202,6 +202,8 @@ typedef struct StormStepStats {
     double energy_emission_debit;/* material energy removed by cell emission */
     double transport_ms;         /* device time of transport (CUDA events) */
     double step_ms;              /* device time of the whole step */
+    double emit_ms;              /* device time from step start through emission (begin, prestep, emit) */
+    double comb_ms;              /* device time of population control */
 } StormStepStats;
 
 /* Replay of single segments against a recorded uniform tape: the parity
@@ -269,6 +271,12 @@ int storm_cuda_set_census(StormHandle *h, const StormParticlesSoA *host_in);
  * must hold `capacity` entries; *count receives the census size. */
 int storm_cuda_get_census(StormHandle *h, StormParticlesSoA *host_out, uint64_t capacity, uint64_t *count);
 int storm_cuda_census_count(StormHandle *h, uint64_t *count);
+/* The transport bank after storm_cuda_phase_emit: the census followed by the
+ * step's cell and face source packets (RadiationIMC::generateParticles and the
+ * boundary's generateNewBoundaryParticles, in that order), id = the particle's
+ * stream index.  For inspecting the emission phase.  host_out = NULL returns
+ * the count alone. */
+int storm_cuda_get_bank(StormHandle *h, StormParticlesSoA *host_out, uint64_t capacity, uint64_t *count);
 /* populationControl->activate(particles) on host particles: the result becomes
  * the handle's census (CombPopulationControl::activate,
  * population/CombPopulationControl.hpp:79-253; with comb disabled the

@@ -5,7 +5,7 @@ sizes against the compiled library.
 """
 import ctypes as C
 
-ABI_VERSION = 1
+ABI_VERSION = 2
 
 STORM_OK = 0
 STATUS_NAMES = {
@@ -87,6 +87,7 @@ class StormStepStats(C.Structure):
         ("energy_census_in", C.c_double), ("energy_emitted", C.c_double), ("energy_deposited", C.c_double),
         ("energy_escaped", C.c_double), ("energy_census_pre_comb", C.c_double), ("energy_census_out", C.c_double),
         ("energy_emission_debit", C.c_double), ("transport_ms", C.c_double), ("step_ms", C.c_double),
+        ("emit_ms", C.c_double), ("comb_ms", C.c_double),
     ]
 
     def as_dict(self):

@@ -602,6 +602,71 @@ __global__ void k_emit_cells(Ctx C, CellArrays A, const uint64_t *offsets, uint6
     if ((threadIdx.x & 31) == 0 && esum != 0.0) atomicAdd(&st->eEmitted, esum);
 }
 
+// The same packets in the FP32-tracking form: the cell's 12 fan tetrahedra
+// have equal volume (a box), so the pick is floor(12 u); the point and the
+// direction are drawn in the cell's own FP32 frame with the same draws in the
+// same order (4 position, 2 direction, 1 time); time and weight stay FP64.
+__device__ __forceinline__ void local_face_vertex(int side, int v, float hx, float hy, float hz, float &x, float &y,
+                                                  float &z) {
+    // vertex v of side `side` in face_vertices' order, relative to the cell centre
+    const int axis = side >> 1;
+    const float sgn = (side & 1) ? 1.0f : -1.0f;
+    const float a = (v == 1 || v == 2) ? 1.0f : -1.0f;   // first in-plane coordinate
+    const float b = (v >= 2) ? 1.0f : -1.0f;             // second in-plane coordinate
+    if (axis == 0) { x = sgn * hx; y = a * hy; z = ((v == 2 || v == 3) ? 1.0f : -1.0f) * hz; }
+    else if (axis == 1) { x = b * hx; y = sgn * hy; z = ((v == 1 || v == 2) ? 1.0f : -1.0f) * hz; }
+    else { x = a * hx; y = ((v >= 2) ? 1.0f : -1.0f) * hy; z = sgn * hz; }
+}
+
+__global__ void k_emit_cells32(Ctx C, CellArrays A, const uint64_t *offsets, uint64_t total, Bank b,
+                               uint32_t bankBase, double dt, DevStats *st) {
+    double esum = 0.0;
+    for (uint64_t e = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; e < total; e += (uint64_t)gridDim.x * blockDim.x) {
+        uint32_t lo = 0, hi = C.ncells;   // last cell whose offset <= e
+        while (lo < hi) {
+            uint32_t mid = (lo + hi) >> 1;
+            if (offsets[mid] <= e) lo = mid + 1; else hi = mid;
+        }
+        const uint32_t c = lo - 1;
+        const uint64_t np = A.photons[c];
+        const double energyPerPhoton = A.emitE[c] * 1.0 / static_cast<double>(np);
+        PhiloxRng rng;
+        rng.init(C.seedLo, C.seedHi, TAG_CELL_EMIT, C.step, static_cast<uint32_t>(e), 0);
+        Track32 T;
+        T.cell = c;
+        cell_ijk(C, c, T.i, T.j, T.k);
+        const float hx = C.hx[T.i], hy = C.hy[T.j], hz = C.hz[T.k];
+        const int tet = min(static_cast<int>(12.0f * rng.rawf()), 11);
+        float s0 = rng.rawf(), s1 = rng.rawf(), s2 = rng.rawf(), tmp;
+        if (s0 > s1) { tmp = s0; s0 = s1; s1 = tmp; }
+        if (s1 > s2) { tmp = s1; s1 = s2; s2 = tmp; }
+        if (s0 > s1) { tmp = s0; s0 = s1; s1 = tmp; }
+        const int side = tet >> 1, tri = (tet & 1) + 1;
+        float x0, y0, z0, x1, y1, z1, x2, y2, z2;
+        local_face_vertex(side, 0, hx, hy, hz, x0, y0, z0);
+        local_face_vertex(side, tri, hx, hy, hz, x1, y1, z1);
+        local_face_vertex(side, tri + 1, hx, hy, hz, x2, y2, z2);
+        const float a0 = s0, a1 = s1 - s0, a2 = s2 - s1;   // the centre's weight 1 - s2 multiplies 0
+        T.qx = clampf(a0 * x0 + a1 * x1 + a2 * x2, hx);
+        T.qy = clampf(a0 * y0 + a1 * y1 + a2 * y2, hy);
+        T.qz = clampf(a0 * z0 + a1 * z1 + a2 * z2, hz);
+        const float theta = 6.2831853f * rng.rawf();
+        const float cz = 2.0f * rng.rawf() - 1.0f;
+        const float sz = sqrtf(fmaxf(0.0f, 1.0f - cz * cz));
+        float sth, cth;
+        __sincosf(theta, &sth, &cth);
+        T.ux = sz * cth; T.uy = sz * sth; T.uz = cz;
+        T.t = dt * rng.open();
+        T.w = energyPerPhoton;
+        T.w0 = fabs(T.w);
+        const uint32_t slot = bankBase + static_cast<uint32_t>(e);
+        store32(b, slot, T, slot, 0);
+        esum += T.w;
+    }
+    esum = warp_sum(esum);
+    if ((threadIdx.x & 31) == 0 && esum != 0.0) atomicAdd(&st->eEmitted, esum);
+}
+
 // ------------------------------------------------------------------ face emission
 // SideTemperature / TwoSidesTemperature::generateNewBoundaryParticles
 // (boundary/SideTemperature.hpp:114-163, TwoSidesTemperature.hpp:126-199) for the
@@ -1245,43 +1310,84 @@ __global__ void k_comb_plan(Ctx C, CombParams P, const double *wS, const uint32_
 // One thread per sorted particle writes its copies at its output offset.
 // The exclusive prefix of the copy counts over sorted particles is the output
 // position: cells are contiguous in sorted order and the output is cell-major.
+// Each thread takes EMIT_BATCH sorted particles per iteration and issues all
+// of their census-record gathers (read-only loads) before it writes any copy,
+// so the random reads overlap.
+constexpr int EMIT_BATCH = 2;
+
+__device__ __forceinline__ void comb_emit_fp64(const Ctx &C, PartReg &p, uint32_t c, uint32_t raw, double wNew,
+                                               uint64_t o, const Bank &out) {
+    if (!(raw & KEEP)) { p.w = wNew; p.w0 = p.w; p.t = 0; }
+    p.cell = c;
+    if (outside_box(C, p.x, p.y, p.z)) {   // :228-250
+        uint32_t i, j, k;
+        cell_ijk(C, c, i, j, k);
+        const double mx = C.xc[i], my = C.yc[j], mz = C.zc[k];
+        const double ox = p.x, oy = p.y, oz = p.z, dx = mx - ox, dy = my - oy, dz = mz - oz;
+        double t = 1e-6;
+        while (outside_box(C, p.x, p.y, p.z) && t < 1.0) {
+            p.x = ox + t * dx; p.y = oy + t * dy; p.z = oz + t * dz;
+            t *= 2;
+        }
+        if (outside_box(C, p.x, p.y, p.z)) { p.x = mx; p.y = my; p.z = mz; }
+    }
+    const uint32_t m = raw & ~KEEP;
+    for (uint32_t k = 0; k < m; ++k) store_part(out, static_cast<uint32_t>(o + k), p, static_cast<uint32_t>(o + k), 0);
+}
+
+template <bool FP32>
 __global__ void k_comb_emit(Ctx C, CensusBank cen, const uint32_t *idx, const uint64_t *sortedKeys, int pidBits,
                             uint32_t nValid, const uint32_t *pCount, const double *pWeight, const uint64_t *pOffset,
                             Bank out) {
-    for (uint32_t q = blockIdx.x * blockDim.x + threadIdx.x; q < nValid; q += gridDim.x * blockDim.x) {
-        const uint32_t raw = pCount[q];
-        const uint32_t m = raw & ~KEEP;
-        if (m == 0) continue;
-        const uint32_t c = static_cast<uint32_t>(sortedKeys[q] >> pidBits);
-        if (C.fp32) {
-            Track32 T;
-            uint32_t pid_, draw_;
-            census_load32(cen, idx[q], T, pid_, draw_);
-            if (!(raw & KEEP)) { T.w = pWeight[q]; T.w0 = T.w; T.t = 0; }
-            T.cell = c;
-            const uint64_t o = pOffset[q];
-            for (uint32_t k = 0; k < m; ++k) store32(out, static_cast<uint32_t>(o + k), T, static_cast<uint32_t>(o + k), 0);
-            continue;
+    const uint32_t stride = gridDim.x * blockDim.x;
+    constexpr int words = FP32 ? 4 : 6;
+    for (uint32_t base = blockIdx.x * blockDim.x + threadIdx.x; base < nValid; base += EMIT_BATCH * stride) {
+        uint32_t raw[EMIT_BATCH], src[EMIT_BATCH];
+        uint4 rec[EMIT_BATCH][words];
+#pragma unroll
+        for (int u = 0; u < EMIT_BATCH; ++u) {
+            const uint32_t q = base + u * stride;
+            raw[u] = q < nValid ? pCount[q] : 0u;
+            src[u] = (raw[u] & ~KEEP) ? idx[q] : 0u;
         }
-        PartReg p;
-        uint32_t pid_, draw_;
-        census_load64(cen, idx[q], p, pid_, draw_);
-        if (!(raw & KEEP)) { p.w = pWeight[q]; p.w0 = p.w; p.t = 0; }
-        p.cell = c;
-        if (outside_box(C, p.x, p.y, p.z)) {   // :228-250
-            uint32_t i, j, k;
-            cell_ijk(C, c, i, j, k);
-            const double mx = C.xc[i], my = C.yc[j], mz = C.zc[k];
-            const double ox = p.x, oy = p.y, oz = p.z, dx = mx - ox, dy = my - oy, dz = mz - oz;
-            double t = 1e-6;
-            while (outside_box(C, p.x, p.y, p.z) && t < 1.0) {
-                p.x = ox + t * dx; p.y = oy + t * dy; p.z = oz + t * dz;
-                t *= 2;
+#pragma unroll
+        for (int u = 0; u < EMIT_BATCH; ++u) {
+            if (raw[u] & ~KEEP) {
+                const uint4 *r = cen.rec + static_cast<size_t>(src[u]) * words;
+#pragma unroll
+                for (int w = 0; w < words; ++w) rec[u][w] = __ldg(r + w);
             }
-            if (outside_box(C, p.x, p.y, p.z)) { p.x = mx; p.y = my; p.z = mz; }
         }
-        const uint64_t o = pOffset[q];
-        for (uint32_t k = 0; k < m; ++k) store_part(out, static_cast<uint32_t>(o + k), p, static_cast<uint32_t>(o + k), 0);
+#pragma unroll
+        for (int u = 0; u < EMIT_BATCH; ++u) {
+            const uint32_t m = raw[u] & ~KEEP;
+            if (m == 0) continue;
+            const uint32_t q = base + u * stride;
+            const uint32_t c = static_cast<uint32_t>(sortedKeys[q] >> pidBits);
+            const uint64_t o = pOffset[q];
+            const double wNew = pWeight[q];
+            if constexpr (FP32) {
+                const uint4 a = rec[u][0], b = rec[u][1], d = rec[u][2];
+                Track32 T;
+                T.qx = __uint_as_float(a.x); T.qy = __uint_as_float(a.y); T.qz = __uint_as_float(a.z);
+                T.ux = __uint_as_float(a.w); T.uy = __uint_as_float(b.x); T.uz = __uint_as_float(b.y);
+                T.t = __longlong_as_double((static_cast<unsigned long long>(b.w) << 32) | b.z);
+                T.w = lo_double(d); T.w0 = hi_double(d);
+                if (!(raw[u] & KEEP)) { T.w = wNew; T.w0 = T.w; T.t = 0; }
+                T.cell = c;
+                for (uint32_t k = 0; k < m; ++k)
+                    store32(out, static_cast<uint32_t>(o + k), T, static_cast<uint32_t>(o + k), 0);
+            } else {
+                const uint4 a = rec[u][0], b = rec[u][1], d = rec[u][2], e = rec[u][3], f = rec[u][words - 2];
+                PartReg p;
+                p.x = lo_double(a); p.y = hi_double(a);
+                p.z = lo_double(b); p.vx = hi_double(b);
+                p.vy = lo_double(d); p.vz = hi_double(d);
+                p.t = lo_double(e); p.w = hi_double(e);
+                p.w0 = lo_double(f);
+                comb_emit_fp64(C, p, c, raw[u], wNew, o, out);
+            }
+        }
     }
 }
 
@@ -1491,7 +1597,10 @@ void launch_scan_u64(cudaStream_t s, const uint64_t *in, uint32_t n, uint64_t *o
 void launch_emit_cells(cudaStream_t s, const Ctx &C, const CellArrays &A, const uint64_t *offsets, uint64_t total,
                        const Bank &b, uint32_t bankBase, double dt, DevStats *st) {
     if (!total) return;
-    k_emit_cells<<<grid_for(total, 256, 148 * 16), 256, 0, s>>>(C, A, offsets, total, b, bankBase, dt, st);
+    if (C.fp32)
+        k_emit_cells32<<<grid_for(total, 256, 148 * 16), 256, 0, s>>>(C, A, offsets, total, b, bankBase, dt, st);
+    else
+        k_emit_cells<<<grid_for(total, 256, 148 * 16), 256, 0, s>>>(C, A, offsets, total, b, bankBase, dt, st);
 }
 void launch_emit_faces(cudaStream_t s, const Ctx &C, const FaceSources &F, uint64_t total, const Bank &b,
                        uint32_t bankBase, double dt, DevStats *st) {
@@ -1592,8 +1701,12 @@ void launch_comb_emit(cudaStream_t s, const Ctx &C, const CensusBank &cen, const
                       int pidBits, uint32_t nValid, const uint32_t *pCount, const double *pWeight,
                       const uint64_t *pOffset, const Bank &out) {
     if (!nValid) return;
-    k_comb_emit<<<grid_for(nValid, 256, 148 * 16), 256, 0, s>>>(C, cen, idx, sortedKeys, pidBits, nValid, pCount, pWeight,
-                                                                pOffset, out);
+    if (C.fp32)
+        k_comb_emit<true><<<grid_for(nValid, 256, 148 * 16), 256, 0, s>>>(C, cen, idx, sortedKeys, pidBits, nValid, pCount,
+                                                                           pWeight, pOffset, out);
+    else
+        k_comb_emit<false><<<grid_for(nValid, 256, 148 * 16), 256, 0, s>>>(C, cen, idx, sortedKeys, pidBits, nValid, pCount,
+                                                                            pWeight, pOffset, out);
 }
 void launch_mask_count(cudaStream_t s, const uint32_t *pCount, uint32_t n, uint64_t *out) {
     k_mask_count<<<grid_for(n, 256, 8192), 256, 0, s>>>(pCount, n, out);

@@ -35,6 +35,7 @@ struct StormHandle {
     int device = 0;
     cudaStream_t stream = nullptr;
     cudaEvent_t evStart = nullptr, evTransport0 = nullptr, evTransport1 = nullptr, evEnd = nullptr;
+    cudaEvent_t evAfterEmit = nullptr, evAfterComb = nullptr;
     uint32_t nx = 0, ny = 0, nz = 0, N = 0;
     std::vector<double> hxe, hye, hze, hxc, hyc, hzc;
     // device mesh + cells
@@ -90,7 +91,7 @@ struct StormHandle {
     uint64_t memBytes = 0;
     StormStepStats stats{};
     std::vector<uint64_t> lastPhotons;
-    double lastTransportMs = 0.0, lastStepMs = 0.0;
+    double lastTransportMs = 0.0, lastStepMs = 0.0, lastEmitMs = 0.0, lastCombMs = 0.0;
     // transport kernel timing
     bool profiling = false;
     std::vector<cudaEvent_t> evPool;
@@ -444,6 +445,8 @@ int storm_cuda_create(const StormProblemDesc *d, StormHandle **out) {
     cudaEventCreate(&h->evTransport0);
     cudaEventCreate(&h->evTransport1);
     cudaEventCreate(&h->evEnd);
+    cudaEventCreate(&h->evAfterEmit);
+    cudaEventCreate(&h->evAfterComb);
 
     h->hxe.assign(d->x_edges, d->x_edges + d->nx + 1);
     h->hye.assign(d->y_edges, d->y_edges + d->ny + 1);
@@ -598,7 +601,7 @@ int storm_cuda_destroy(StormHandle *h) {
                   h->combStart, h->combCount, h->counts, h->dStats, h->dErr};
     for (void *p : ps)
         if (p) cudaFree(p);
-    cudaEvent_t evs[] = {h->evStart, h->evTransport0, h->evTransport1, h->evEnd};
+    cudaEvent_t evs[] = {h->evStart, h->evTransport0, h->evTransport1, h->evEnd, h->evAfterEmit, h->evAfterComb};
     for (cudaEvent_t e : evs)
         if (e) cudaEventDestroy(e);
     for (cudaEvent_t e : h->evPool)
@@ -936,6 +939,8 @@ int storm_cuda_phase_stats(StormHandle *h, StormStepStats *s) {
     s->energy_emission_debit = d.eDebit;
     s->transport_ms = h->lastTransportMs;
     s->step_ms = h->lastStepMs;
+    s->emit_ms = h->lastEmitMs;
+    s->comb_ms = h->lastCombMs;
     return STORM_OK;
 }
 
@@ -946,14 +951,22 @@ int storm_cuda_step(StormHandle *h, double dt, StormStepStats *stats) {
     int rc = storm_cuda_phase_begin(h, dt);
     if (rc == STORM_OK) rc = storm_cuda_phase_prestep(h, dt);
     if (rc == STORM_OK) rc = storm_cuda_phase_emit(h, dt);
+    CK(cudaEventRecord(h->evAfterEmit, h->stream));
     if (rc == STORM_OK) rc = storm_cuda_phase_transport(h);
     if (rc == STORM_OK) rc = storm_cuda_phase_comb(h);
+    CK(cudaEventRecord(h->evAfterComb, h->stream));
     if (rc == STORM_OK) rc = storm_cuda_phase_poststep(h, dt);
     CK(cudaEventRecord(h->evEnd, h->stream));
     CK(cudaEventSynchronize(h->evEnd));
     float ms = 0.f;
     cudaEventElapsedTime(&ms, h->evStart, h->evEnd);
     h->lastStepMs = ms;
+    if (rc == STORM_OK) {
+        cudaEventElapsedTime(&ms, h->evStart, h->evAfterEmit);
+        h->lastEmitMs = ms;
+        cudaEventElapsedTime(&ms, h->evTransport1, h->evAfterComb);
+        h->lastCombMs = ms;
+    }
     if (stats) storm_cuda_phase_stats(h, stats);
     return rc;
 }
@@ -1055,6 +1068,39 @@ int storm_cuda_get_census(StormHandle *h, StormParticlesSoA *out, uint64_t capac
     CK(cudaStreamSynchronize(h->stream));
     if (out->id)
         for (uint64_t q = 0; q < n; ++q) out->id[q] = q;
+    out->count = n;
+    return STORM_OK;
+}
+
+int storm_cuda_get_bank(StormHandle *h, StormParticlesSoA *out, uint64_t capacity, uint64_t *count) {
+    if (!h) return STORM_ERR_INVALID_ARG;
+    if (!out) {   // size query
+        if (!count) return STORM_ERR_INVALID_ARG;
+        *count = h->nBank;
+        return STORM_OK;
+    }
+    CK(cudaSetDevice(h->device));
+    const uint64_t n = std::min<uint64_t>(h->nBank, capacity);
+    if (count) *count = h->nBank;
+    if (h->fp32 && n) {
+        launch_bank_to_global(h->stream, h->C, h->bankA, h->bankB, static_cast<uint32_t>(n));
+        ++h->launches;
+        CK(cudaGetLastError());
+    }
+    const Bank &src = h->fp32 ? h->bankB : h->bankA;
+    const double *sd[] = {src.x, src.y, src.z, src.vx, src.vy, src.vz, src.t, src.w, src.w0};
+    double *dd[] = {out->x, out->y, out->z, out->vx, out->vy, out->vz, out->time_left, out->weight, out->initial_weight};
+    for (int q = 0; q < 9; ++q)
+        if (dd[q] && n) CK(cudaMemcpyAsync(dd[q], sd[q], n * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+    if (out->cell && n) CK(cudaMemcpyAsync(out->cell, src.cell, n * sizeof(uint32_t), cudaMemcpyDeviceToHost, h->stream));
+    std::vector<uint32_t> pid;
+    if (out->id && n) {
+        pid.resize(n);
+        CK(cudaMemcpyAsync(pid.data(), src.pid, n * sizeof(uint32_t), cudaMemcpyDeviceToHost, h->stream));
+    }
+    CK(cudaStreamSynchronize(h->stream));
+    if (out->id)
+        for (uint64_t q = 0; q < n; ++q) out->id[q] = pid[q];
     out->count = n;
     return STORM_OK;
 }

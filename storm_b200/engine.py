@@ -42,6 +42,7 @@ def lib():
         L.storm_cuda_set_census.argtypes = [vp, C.POINTER(A.StormParticlesSoA)]
         L.storm_cuda_get_census.argtypes = [vp, C.POINTER(A.StormParticlesSoA), C.c_uint64, u64p]
         L.storm_cuda_census_count.argtypes = [vp, u64p]
+        L.storm_cuda_get_bank.argtypes = [vp, C.POINTER(A.StormParticlesSoA), C.c_uint64, u64p]
         L.storm_cuda_population_control.argtypes = [vp, C.POINTER(A.StormParticlesSoA)]
         L.storm_cuda_get_cell_arrays.argtypes = [vp, dp, dp, dp, dp, dp, dp, u64p]
         L.storm_cuda_set_cell_state.argtypes = [vp, dp, dp, dp]
@@ -185,6 +186,15 @@ class Engine:
         s = p.soa()
         cnt = C.c_uint64()
         self._check(lib().storm_cuda_get_census(self.h, C.byref(s), n, C.byref(cnt)))
+        return p
+
+    def bank(self):
+        """The transport bank after phase('emit'): census then source packets."""
+        cnt = C.c_uint64()
+        self._check(lib().storm_cuda_get_bank(self.h, None, 0, C.byref(cnt)))
+        p = Particles(cnt.value)
+        s = p.soa()
+        self._check(lib().storm_cuda_get_bank(self.h, C.byref(s), cnt.value, C.byref(cnt)))
         return p
 
     def set_census(self, p):

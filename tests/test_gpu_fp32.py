@@ -11,6 +11,7 @@ import pytest
 from storm_b200 import _abi as A
 from storm_b200 import problems
 from storm_b200.engine import Engine, Particles
+from storm_b200.units import UNITS
 
 pytestmark = pytest.mark.gpu
 
@@ -90,3 +91,35 @@ def test_fp32_agrees_with_fp64_within_statistics():
     assert hot.sum() > 100
     assert (z < 3.0).mean() > 0.97, (z > 3).sum()
     assert z.mean() < 1.2
+
+
+def test_fp32_emission_follows_fp64_draws():
+    """Cell and face source packets of the FP32 form: drawn in the cell's own
+    FP32 frame from the same Philox draws as the FP64 form, so each packet sits
+    where the FP64 packet sits to FP32 rounding (the tetrahedron pick may differ
+    when 12 u lands within FP32 rounding of an integer)."""
+    p = problems.step_cube(n=16, new_photons_per_cell=5, face_packets=40, comb_nmin=10)
+    dt = p.dt
+    banks = []
+    for prec in (A.PRECISION_FP64, A.PRECISION_FP32_TRACK):
+        q = problems.step_cube(n=16, new_photons_per_cell=5, face_packets=40, comb_nmin=10)
+        q.precision = prec
+        e = Engine(q)
+        for ph in ("begin", "prestep", "emit"):
+            e.phase(ph, dt)
+        banks.append(e.bank())
+        e.close()
+    b64, b32 = banks
+    assert b64.n == b32.n > 0
+    np.testing.assert_array_equal(b64.cell, b32.cell)
+    np.testing.assert_array_equal(b64.id, b32.id)
+    np.testing.assert_array_equal(b64.time_left, b32.time_left)
+    np.testing.assert_array_equal(b64.weight, b32.weight)
+    h = 0.5 / 16
+    dpos = np.max(np.abs(np.stack([b64.x - b32.x, b64.y - b32.y, b64.z - b32.z])), axis=0)
+    assert (dpos <= 1e-6 * h).mean() > 0.999, np.sort(dpos)[-5:]
+    assert (dpos <= 2 * h).all()
+    c = UNITS["clight"]
+    # 2^-23 quantisation of cos(theta) moves the direction by ~1e-7 / sin(theta)
+    ddir = np.max(np.abs(np.stack([b64.vx - b32.vx, b64.vy - b32.vy, b64.vz - b32.vz]) / c), axis=0)
+    assert (ddir <= 1e-4).mean() > 0.999, np.sort(ddir)[-5:]
