@@ -100,9 +100,12 @@ __device__ __forceinline__ void philox4x32_10(uint32_t c0, uint32_t c1, uint32_t
                                               uint32_t k1, uint32_t out[4]) {
 #pragma unroll
     for (int r = 0; r < 10; ++r) {
-        uint32_t hi0 = __umulhi(0xD2511F53u, c0), lo0 = 0xD2511F53u * c0;
-        uint32_t hi1 = __umulhi(0xCD9E8D57u, c2), lo1 = 0xCD9E8D57u * c2;
-        uint32_t n0 = hi1 ^ c1 ^ k0, n2 = hi0 ^ c3 ^ k1;
+        // one 32x32->64 multiply gives both halves of each product
+        const uint64_t p0 = static_cast<uint64_t>(0xD2511F53u) * c0;
+        const uint64_t p1 = static_cast<uint64_t>(0xCD9E8D57u) * c2;
+        const uint32_t hi0 = static_cast<uint32_t>(p0 >> 32), lo0 = static_cast<uint32_t>(p0);
+        const uint32_t hi1 = static_cast<uint32_t>(p1 >> 32), lo1 = static_cast<uint32_t>(p1);
+        const uint32_t n0 = hi1 ^ c1 ^ k0, n2 = hi0 ^ c3 ^ k1;
         c0 = n0; c1 = lo1; c2 = n2; c3 = lo0;
         k0 += 0x9E3779B9u;
         k1 += 0xBB67AE85u;
@@ -169,6 +172,34 @@ struct PhiloxRng {
         double v = raw();
         return v <= 0.0 ? DBL_MIN : (v >= 1.0 ? ONE_BELOW : v);
     }
+    __device__ __forceinline__ bool exhausted() const { return false; }
+};
+
+// The FP32-tracking form's per-particle stream: the same Philox counter
+// (block, pid, step, tag) with all four words of a block used, one 23-bit float
+// draw per word, so a collision and its isotropic re-scatter take under one
+// block.  Draws the FP64 form consumes without using (the event-type draw)
+// are not taken.  This stream is its own: the FP32 form's histories are
+// statistically independent of the FP64 form's.
+struct PhiloxRng4 {
+    uint32_t k0, k1, tag, step, pid, draw;
+    uint32_t block;
+    uint32_t w[4];
+    __device__ __forceinline__ void init(uint32_t kk0, uint32_t kk1, uint32_t t, uint32_t s, uint32_t p, uint32_t d) {
+        k0 = kk0; k1 = kk1; tag = t; step = s; pid = p; draw = d; block = 0xffffffffu;
+    }
+    __device__ __forceinline__ float rawf() {
+        const uint32_t b = draw >> 2;
+        if (b != block) {
+            philox4x32_10(b, pid, step, tag, k0, k1, w);
+            block = b;
+        }
+        const uint32_t sel = draw & 3u;
+        const uint32_t word = sel == 0 ? w[0] : (sel == 1 ? w[1] : (sel == 2 ? w[2] : w[3]));
+        ++draw;
+        return u23(word);
+    }
+    __device__ __forceinline__ void skip() {}
     __device__ __forceinline__ bool exhausted() const { return false; }
 };
 
@@ -534,6 +565,10 @@ struct Track32 {
     float qx, qy, qz, ux, uy, uz;
     double t, w, w0;
     uint32_t cell, i, j, k;
+    // the constants of cell `cc`, kept in registers while the particle stays in it
+    uint32_t cc;
+    float4 cp;
+    float hx, hy, hz;
 };
 
 __device__ __forceinline__ float clampf(float v, float h) { return fminf(fmaxf(v, -h), h); }
@@ -641,8 +676,13 @@ __device__ inline int rw_jump32(const Ctx &C, Track32 &T, RNG &rng, TALLY &tal, 
 template <class RNG, class TALLY>
 __device__ inline int segment32(const Ctx &C, Track32 &T, RNG &rng, TALLY &tal, int &usedRW, int &err) {
     const uint32_t cell = T.cell;
-    const float hx = C.hx[T.i], hy = C.hy[T.j], hz = C.hz[T.k];
-    const float4 cp = C.phys32[cell];
+    if (T.cc != cell) {   // entered another cell: load its constants once
+        T.cp = C.phys32[cell];
+        T.hx = C.hx[T.i]; T.hy = C.hy[T.j]; T.hz = C.hz[T.k];
+        T.cc = cell;
+    }
+    const float hx = T.hx, hy = T.hy, hz = T.hz;
+    const float4 cp = T.cp;
 
     // Random Walk only where the particle is at least cp.z = rwMinParticleOpticalDepth / sigma_T
     // from every face (cp.z is inf in cells that are not eligible)
@@ -688,7 +728,7 @@ __device__ inline int segment32(const Ctx &C, Track32 &T, RNG &rng, TALLY &tal, 
     }
     if (best == 2) return OUT_CENSUS;
     if (best == 1) {
-        rng.skip();
+        rng.skip();   // the event-type draw (a no-op on the FP32 form's own stream)
         const float theta = 6.2831853f * rng.rawf();
         const float cosT = 2.0f * rng.rawf() - 1.0f;
         const float sinT = sqrtf(fmaxf(0.0f, 1.0f - cosT * cosT));

@@ -775,6 +775,7 @@ __device__ __forceinline__ void block_stats_flush(const BlockStats &bs, DevStats
 // coordinates, the reference's arithmetic) and the FP32-tracking form.
 struct Form64 {
     using T = Track;
+    using Rng = PhiloxRng;
     static __device__ __forceinline__ void load(const Ctx &C, const Bank &b, uint32_t q, T &t) {
         load_part(b, q, t.p);
         track_begin(C, t);
@@ -800,9 +801,11 @@ struct Form64 {
 };
 struct Form32 {
     using T = Track32;
+    using Rng = PhiloxRng4;
     static __device__ __forceinline__ void load(const Ctx &C, const Bank &b, uint32_t q, T &t) {
         load32(b, q, t);
         cell_ijk(C, t.cell, t.i, t.j, t.k);
+        t.cc = OUTSIDE;
     }
     static __device__ __forceinline__ void keep(const Bank &b, uint32_t q, const T &t, uint32_t pid, uint32_t draw) {
         store32(b, q, t, pid, draw);
@@ -839,7 +842,7 @@ __device__ __forceinline__ void visit_bank(const Ctx &C, const Bank &in, uint32_
         if (active) {
             F::load(C, in, idx, t);
             pid = in.pid[idx];
-            PhiloxRng rng;
+            typename F::Rng rng;
             rng.init(C.seedLo, C.seedHi, TAG_TRANSPORT, C.step, pid, in.draw[idx]);
             SegmentTally tal;
             tal.init(C.eint, C.eradAvg, C.perCellCounters ? C.segs : nullptr);
@@ -921,7 +924,7 @@ __global__ void __launch_bounds__(256, MINB) k_transport_refill(Ctx C, Bank in, 
     const unsigned lane = tid & 31;
     const unsigned lt = lanemask_lt();
     typename F::T t;
-    PhiloxRng rng;
+    typename F::Rng rng;
     uint32_t pid = 0, segsThis = 0;
     bool has = false;
     uint32_t cBase = 0, cLeft = 0;   // warp-uniform: this warp's chunk of unstarted particles
