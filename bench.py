@@ -51,6 +51,9 @@ def parse():
     ap.add_argument("--waves", type=int, default=4)
     ap.add_argument("--refill", type=int, default=-1, help="1 persistent refill kernel, 0 bank visits")
     ap.add_argument("--burst", type=int, default=8)
+    ap.add_argument("--serving-requests", type=int, default=32, help="requests in the serving run (0 = skip it)")
+    ap.add_argument("--serving-slots", type=int, default=16)
+    ap.add_argument("--serving-workers", type=int, default=8)
     return ap.parse_args()
 
 
@@ -335,6 +338,49 @@ def e2e_run(args, eng, p, dist):
                     "host-side checks inside the timed region (wall clock)"}
 
 
+def serving_run(args):
+    """Many independent FP32-tracking problems (N log-uniform in [16, 48],
+    1e4-1e6 packets/step log-uniform, kappa uniform in [0.1, 1000], 5-20 steps)
+    through the serving loop, against the same requests one at a time.  The
+    concurrent run receives the requests as a Poisson stream at 4x the rate the
+    one-at-a-time server completes them."""
+    import numpy as np
+    from storm_b200 import problems
+    from storm_b200.engine import Server
+    mix = problems.serving_mix(args.serving_requests, seed=11)
+
+    def run(slots, workers, gaps):
+        srv = Server(max_active=slots, workers=workers)
+        t0 = time.perf_counter()
+        for (p, steps), gap in zip(mix, gaps):
+            if gap > 0:
+                time.sleep(gap)
+            srv.submit(p, steps, want_temperature=False)
+        srv.drain()
+        wall = time.perf_counter() - t0
+        st = srv.stats()
+        res = srv.poll()
+        srv.close()
+        ok = sum(1 for r in res if r["status"] == 0)
+        return {"segments_per_s": st["segments"] / wall, "wall_s": wall, "segments": st["segments"],
+                "step_ms_p50": st["step_ms_p50"], "step_ms_p99": st["step_ms_p99"], "completed": ok,
+                "queued_ms_max": max((r["queued_ms"] for r in res), default=0.0),
+                "peak_device_gb": st["peak_device_bytes"] / 1e9, "slots": slots, "workers": workers}
+
+    alone = run(1, 1, [0.0] * len(mix))
+    rng = np.random.default_rng(12)
+    mean_gap = alone["wall_s"] / len(mix) / 4.0
+    gaps = [0.0] + list(rng.exponential(mean_gap, len(mix) - 1))
+    mixed = run(args.serving_slots, args.serving_workers, gaps)
+    return {"requests": len(mix), "form": "fp32-track",
+            "mix": "uniform cubes, N log-uniform [16,48], packets/step log-uniform [1e4,1e6], "
+                   "kappa uniform [0.1,1000] 1/cm, 5-20 steps, seeded",
+            "one_at_a_time": alone, "concurrent": mixed,
+            "throughput_ratio": mixed["segments_per_s"] / max(alone["segments_per_s"], 1e-300),
+            "p99_step_latency_ratio": mixed["step_ms_p99"] / max(alone["step_ms_p99"], 1e-300),
+            "arrivals": f"Poisson, mean gap {mean_gap * 1e3:.2f} ms (4x the one-at-a-time completion rate)"}
+
+
 def run_storm(args, ws, rank, local, dist):
     import numpy as np
     import torch
@@ -377,6 +423,7 @@ def run_storm(args, ws, rank, local, dist):
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline(args.n, 1)
+    serving = serving_run(args) if (rank == 0 and ws == 1 and args.serving_requests > 0) else None
     if rank == 0:
         lat = sorted(f32["step_ms"])
         line = {
@@ -398,7 +445,7 @@ def run_storm(args, ws, rank, local, dist):
                      "roofline": roofline(f64, BYTES_PER_SEGMENT_FP64, transport_kernel(args, False))},
             "fp32_over_fp64": v32 / v64,
             "fp32_vs_fp64_deviation": dev,
-            "cpu_baseline": cpu, "e2e": e2e, "clocks": ck, "gpu_launches": f32["launches"],
+            "cpu_baseline": cpu, "e2e": e2e, "serving": serving, "clocks": ck, "gpu_launches": f32["launches"],
             "transport_share": f32["transport"]["kernel_ms"] / max(sum(f32["step_ms"]), 1e-9),
         }
         print(json.dumps(line), flush=True)

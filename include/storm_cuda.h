@@ -343,11 +343,69 @@ int storm_cuda_emission_allocation_noalloc(int device, const double *d_energy, u
                                            uint64_t new_photons_per_cell, uint64_t *d_photons,
                                            uint64_t *d_offsets, void *stream);
 
+/* ---------------------------------------------------------------- serving */
+
+/* Many independent problems on one GPU.  A request (descriptor, steps, dt) is
+ * admitted when a slot is free and its estimated device memory fits the HBM
+ * budget; its census and material state then stay on the device until its
+ * last step.  Worker threads advance the active problems round-robin, one time
+ * step at a time, each problem on its own stream, so the work of different
+ * problems overlaps on the GPU.  No reference counterpart (the reference runs
+ * one problem per process). */
+typedef struct StormServer StormServer;
+
+typedef struct StormServerConfig {
+    int32_t device;
+    uint32_t max_active;             /* problems on the device at once */
+    uint32_t workers;                /* host threads issuing steps (1-256) */
+    uint32_t pad_;
+    uint64_t hbm_budget_bytes;       /* admission budget (0 = 90% of free device memory) */
+} StormServerConfig;
+
+typedef struct StormRequestResult {
+    uint64_t ticket;
+    int32_t status;                  /* StormStatus of the request */
+    uint32_t steps;                  /* time steps run */
+    uint64_t segments;
+    uint64_t device_bytes;           /* device memory the problem held */
+    double queued_ms;                /* submission to admission (wall clock) */
+    double active_ms;                /* admission to completion (wall clock) */
+    double step_ms_p50, step_ms_p99, step_ms_max;   /* wall time of each step, issue to completion */
+    double device_ms;                /* summed device time of its steps */
+} StormRequestResult;
+
+typedef struct StormServerStats {
+    uint64_t submitted, completed, failed, active, queued;
+    uint64_t segments;               /* of completed requests */
+    double busy_ms;                  /* first admission to last completion (wall clock) */
+    double step_ms_p50, step_ms_p99; /* over every step of every completed request */
+    uint64_t peak_device_bytes;
+    uint64_t budget_bytes;
+} StormServerStats;
+
+int storm_server_create(const StormServerConfig *config, StormServer **out);
+/* Queue a problem.  The descriptor and its arrays are copied; temperature_out
+ * (Ncells doubles, may be NULL) receives the final material temperatures and
+ * must stay valid until the request's result has been polled. */
+int storm_server_submit(StormServer *s, const StormProblemDesc *desc, uint32_t steps, double dt,
+                        double *temperature_out, uint64_t *ticket);
+/* Results of requests finished since the last poll (up to capacity). */
+int storm_server_poll(StormServer *s, StormRequestResult *results, uint32_t capacity, uint32_t *count);
+/* Block until every submitted request has finished. */
+int storm_server_drain(StormServer *s);
+int storm_server_stats(StormServer *s, StormServerStats *out);
+/* Finishes the queued work, then stops the workers. */
+int storm_server_destroy(StormServer *s);
+
 /* ---------------------------------------------------------------- diagnostics */
 
 /* First device error word, the cell and particle it was raised for, and a message. */
 int storm_cuda_last_error(StormHandle *h, int32_t *derr, uint64_t *cell, uint64_t *particle,
                           char *msg, size_t msg_len);
+/* Device memory freed by destroyed handles is cached for reuse by later
+ * handles on the same device (cudaFree would wait for every stream on the
+ * device).  This returns the cached blocks of `device` to the driver. */
+int storm_cuda_release_cached(int device, uint64_t *bytes);
 /* Bytes of device memory the handle holds (GetHandlerMemoryBytes). */
 int storm_cuda_memory_bytes(StormHandle *h, uint64_t *bytes);
 /* Kernel launches issued by the handle since creation (for launch accounting). */

@@ -114,3 +114,28 @@ def ptr(arr, ctype=C.c_double):
     if arr is None:
         return None
     return arr.ctypes.data_as(C.POINTER(ctype))
+
+
+class StormServerConfig(C.Structure):
+    _fields_ = [("device", C.c_int32), ("max_active", C.c_uint32), ("workers", C.c_uint32), ("pad_", C.c_uint32),
+                ("hbm_budget_bytes", C.c_uint64)]
+
+
+class StormRequestResult(C.Structure):
+    _fields_ = [("ticket", C.c_uint64), ("status", C.c_int32), ("steps", C.c_uint32), ("segments", C.c_uint64),
+                ("device_bytes", C.c_uint64), ("queued_ms", C.c_double), ("active_ms", C.c_double),
+                ("step_ms_p50", C.c_double), ("step_ms_p99", C.c_double), ("step_ms_max", C.c_double),
+                ("device_ms", C.c_double)]
+
+    def as_dict(self):
+        return {name: getattr(self, name) for name, _ in self._fields_}
+
+
+class StormServerStats(C.Structure):
+    _fields_ = [("submitted", C.c_uint64), ("completed", C.c_uint64), ("failed", C.c_uint64), ("active", C.c_uint64),
+                ("queued", C.c_uint64), ("segments", C.c_uint64), ("busy_ms", C.c_double),
+                ("step_ms_p50", C.c_double), ("step_ms_p99", C.c_double), ("peak_device_bytes", C.c_uint64),
+                ("budget_bytes", C.c_uint64)]
+
+    def as_dict(self):
+        return {name: getattr(self, name) for name, _ in self._fields_}

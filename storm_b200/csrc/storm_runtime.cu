@@ -7,7 +7,10 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <map>
+#include <mutex>
 #include <string>
+#include <unordered_map>
 #include <vector>
 
 #include "storm_cuda.h"
@@ -117,17 +120,107 @@ int cuda_fail(StormHandle *h, cudaError_t e, const char *what) {
         if (e_ != cudaSuccess) return cuda_fail(h, e_, #call); \
     } while (0)
 
+// Device memory cache shared by every handle in the process.  cudaFree waits
+// for the whole device, so a handle that freed its buffers at the end of a
+// request would stall every other problem on the GPU; blocks return here
+// instead and are handed to the next allocation of about the same size
+// (at most 25% larger) on the same device.  A handle frees only after its own
+// stream is idle, so a reused block has no work in flight.  When cudaMalloc
+// runs out of memory the device's cached blocks are released and it retries.
+class DevicePool {
+public:
+    cudaError_t alloc(void **p, size_t bytes) {
+        const size_t want = round_up(bytes);
+        int dev = 0;
+        cudaGetDevice(&dev);
+        {
+            std::lock_guard<std::mutex> lk(m_);
+            auto it = free_.lower_bound({dev, want});
+            if (it != free_.end() && it->first.first == dev && it->first.second <= want + want / 4) {
+                *p = it->second;
+                live_[it->second] = it->first;
+                cached_ -= it->first.second;
+                free_.erase(it);
+                return cudaSuccess;
+            }
+        }
+        cudaError_t e = cudaMalloc(p, want);
+        if (e == cudaErrorMemoryAllocation) {
+            cudaGetLastError();
+            release(dev);
+            e = cudaMalloc(p, want);
+        }
+        if (e != cudaSuccess) return e;
+        std::lock_guard<std::mutex> lk(m_);
+        live_[*p] = {dev, want};
+        return cudaSuccess;
+    }
+    void free(void *p) {
+        if (!p) return;
+        std::lock_guard<std::mutex> lk(m_);
+        auto it = live_.find(p);
+        if (it == live_.end()) return;
+        free_.insert({it->second, p});
+        cached_ += it->second.second;
+        live_.erase(it);
+    }
+    // cudaFree every cached block of `dev`; returns the bytes released
+    size_t release(int dev) {
+        std::vector<void *> blocks;
+        size_t bytes = 0;
+        {
+            std::lock_guard<std::mutex> lk(m_);
+            for (auto it = free_.begin(); it != free_.end();) {
+                if (it->first.first == dev) {
+                    blocks.push_back(it->second);
+                    bytes += it->first.second;
+                    it = free_.erase(it);
+                } else {
+                    ++it;
+                }
+            }
+            cached_ -= bytes;
+        }
+        int prev = 0;
+        cudaGetDevice(&prev);
+        cudaSetDevice(dev);
+        for (void *b : blocks) cudaFree(b);
+        cudaSetDevice(prev);
+        return bytes;
+    }
+
+private:
+    static size_t round_up(size_t bytes) {
+        if (bytes <= (1u << 20)) {
+            size_t b = 512;
+            while (b < bytes) b <<= 1;
+            return b;
+        }
+        const size_t g = 2u << 20;
+        return (bytes + g - 1) / g * g;
+    }
+    std::mutex m_;
+    std::unordered_map<void *, std::pair<int, size_t>> live_;
+    std::multimap<std::pair<int, size_t>, void *> free_;
+    size_t cached_ = 0;
+};
+
+DevicePool &device_pool() {
+    static DevicePool pool;
+    return pool;
+}
+
 template <class T>
 cudaError_t dalloc(StormHandle *h, T **p, size_t n) {
     size_t bytes = sizeof(T) * (n ? n : 1);
-    cudaError_t e = cudaMalloc(reinterpret_cast<void **>(p), bytes);
+    cudaError_t e = device_pool().alloc(reinterpret_cast<void **>(p), bytes);
     if (e == cudaSuccess) h->memBytes += bytes;
     return e;
 }
 template <class T>
 void dfree(StormHandle *h, T *&p, size_t n) {
     if (p) {
-        cudaFree(p);
+        device_pool().free(p);
         h->memBytes -= sizeof(T) * (n ? n : 1);
         p = nullptr;
     }
@@ -312,15 +405,24 @@ double rw_survival(double tau) {
     double s = 2.0 * sum;
     return s < 0.0 ? 0.0 : (1.0 < s ? 1.0 : s);
 }
-int build_rw_tables(StormHandle *h) {
-    std::vector<double> tau(RW_TABLE), ltau(RW_TABLE), surv(RW_TABLE);
-    const double logMin = std::log(1e-8), logMax = std::log(64.0);
-    for (int i = 0; i < RW_TABLE; ++i) {
-        double frac = static_cast<double>(i) / static_cast<double>(RW_TABLE - 1);
-        tau[i] = std::exp(logMin + frac * (logMax - logMin));
-        ltau[i] = std::log(tau[i]);
-        surv[i] = rw_survival(tau[i]);
+// The host tables depend on nothing but the table sizes: computed once per process.
+struct RwHostTables {
+    std::vector<double> tau, ltau, surv;
+    RwHostTables() : tau(RW_TABLE), ltau(RW_TABLE), surv(RW_TABLE) {
+        const double logMin = std::log(1e-8), logMax = std::log(64.0);
+        for (int i = 0; i < RW_TABLE; ++i) {
+            double frac = static_cast<double>(i) / static_cast<double>(RW_TABLE - 1);
+            tau[i] = std::exp(logMin + frac * (logMax - logMin));
+            ltau[i] = std::log(tau[i]);
+            surv[i] = rw_survival(tau[i]);
+        }
     }
+};
+
+int build_rw_tables(StormHandle *h) {
+    static const RwHostTables host;   // thread-safe initialisation
+    const std::vector<double> &tau = host.tau, &ltau = host.ltau, &surv = host.surv;
+    const double logMin = std::log(1e-8), logMax = std::log(64.0);
     CK(dalloc(h, &h->rwTau, RW_TABLE));
     CK(dalloc(h, &h->rwLogTau, RW_TABLE));
     CK(dalloc(h, &h->rwSurv, RW_TABLE));
@@ -352,6 +454,14 @@ int build_rw_tables(StormHandle *h) {
     h->C.rw.logMin = logMin;
     h->C.rw.logMax = logMax;
     return STORM_OK;
+}
+
+// Small device->host read on the handle's own stream (never the legacy default
+// stream, so handles on other streams keep running).
+cudaError_t read_small(StormHandle *h, void *dst, const void *src, size_t bytes) {
+    cudaError_t e = cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, h->stream);
+    if (e != cudaSuccess) return e;
+    return cudaStreamSynchronize(h->stream);
 }
 
 int check_device_error(StormHandle *h) {
@@ -390,6 +500,15 @@ uint32_t grid_transport(uint64_t n, uint32_t resident) {
 extern "C" {
 
 int storm_cuda_abi_version(void) { return STORM_CUDA_ABI_VERSION; }
+
+int storm_cuda_release_cached(int device, uint64_t *bytes) {
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return STORM_ERR_NO_DEVICE;
+    if (device < 0 || device >= ndev) return STORM_ERR_INVALID_ARG;
+    const size_t b = device_pool().release(device);
+    if (bytes) *bytes = b;
+    return STORM_OK;
+}
 
 const char *storm_cuda_status_string(int s) {
     switch (s) {
@@ -599,8 +718,7 @@ int storm_cuda_destroy(StormHandle *h) {
                   h->A.rwElig, h->A.photons, h->A.phys, h->A.phys32, h->hx, h->hy, h->hz, h->segs, h->tabA, h->tabS, h->rhoF, h->rwTau, h->rwLogTau, h->rwSurv,
                   h->rwRadius, h->rwLogTau32, h->rwSurv32, h->rwRadius32, h->fsCell, h->fsSide, h->fsOffset, h->dAmbiguous, h->offsets, h->tileSums, h->dTotalU64, h->dTotalE, h->combW, h->combWtot,
                   h->combStart, h->combCount, h->counts, h->dStats, h->dErr};
-    for (void *p : ps)
-        if (p) cudaFree(p);
+    for (void *p : ps) device_pool().free(p);
     cudaEvent_t evs[] = {h->evStart, h->evTransport0, h->evTransport1, h->evEnd, h->evAfterEmit, h->evAfterComb};
     for (cudaEvent_t e : evs)
         if (e) cudaEventDestroy(e);
@@ -730,11 +848,11 @@ int storm_cuda_phase_transport(StormHandle *h) {
         int rc = check_device_error(h);
         if (rc != STORM_OK) return rc;
         uint32_t nc = 0;
-        CK(cudaMemcpy(&nc, nCen, sizeof(uint32_t), cudaMemcpyDeviceToHost));
+        CK(read_small(h, &nc, nCen, sizeof(uint32_t)));
         h->stats.census_out_pre_comb = nc;
         if (h->profiling) {
             DevStats d{};
-            CK(cudaMemcpy(&d, h->dStats, sizeof(d), cudaMemcpyDeviceToHost));
+            CK(read_small(h, &d, h->dStats, sizeof(d)));
             h->profSegments += d.segments;
         }
         float ms = 0.f;
@@ -778,7 +896,7 @@ int storm_cuda_phase_transport(StormHandle *h) {
             inWindow = 0;
             if (remaining == 0) done = true;
             int32_t e0 = 0;
-            CK(cudaMemcpy(&e0, h->dErr, sizeof(int32_t), cudaMemcpyDeviceToHost));
+            CK(read_small(h, &e0, h->dErr, sizeof(int32_t)));
             if (e0) break;
         }
     }
@@ -792,11 +910,11 @@ int storm_cuda_phase_transport(StormHandle *h) {
         return STORM_ERR_DEVICE;
     }
     uint32_t nc = 0;
-    CK(cudaMemcpy(&nc, nCen, sizeof(uint32_t), cudaMemcpyDeviceToHost));
+    CK(read_small(h, &nc, nCen, sizeof(uint32_t)));
     h->stats.census_out_pre_comb = nc;
     if (h->profiling) {
         DevStats d{};
-        CK(cudaMemcpy(&d, h->dStats, sizeof(d), cudaMemcpyDeviceToHost));
+        CK(read_small(h, &d, h->dStats, sizeof(d)));
         h->profSegments += d.segments;
     }
     float ms = 0.f;
@@ -881,7 +999,7 @@ int storm_cuda_phase_comb(StormHandle *h) {
     int rc = check_device_error(h);
     if (rc != STORM_OK) return rc;
     uint64_t total = 0;
-    CK(cudaMemcpy(&total, h->dTotalU64, sizeof(uint64_t), cudaMemcpyDeviceToHost));
+    CK(read_small(h, &total, h->dTotalU64, sizeof(uint64_t)));
     // The write goes to bank A, which transport has finished with.  When the
     // combed census outgrows the banks, A and B are replaced first (their
     // contents are dead); C and the comb buffers, which the write still reads,

@@ -60,6 +60,12 @@ def lib():
         L.storm_cuda_set_transport_variant.argtypes = [vp, C.c_int, C.c_int]
         L.storm_cuda_set_transport_mode.argtypes = [vp, C.c_int, C.c_uint32]
         L.storm_cuda_transport_timing.argtypes = [vp, dp, u64p, u64p, C.c_int]
+        L.storm_server_create.argtypes = [C.POINTER(A.StormServerConfig), C.POINTER(vp)]
+        L.storm_server_submit.argtypes = [vp, C.POINTER(A.StormProblemDesc), C.c_uint32, C.c_double, dp, u64p]
+        L.storm_server_poll.argtypes = [vp, C.POINTER(A.StormRequestResult), C.c_uint32, C.POINTER(C.c_uint32)]
+        L.storm_server_drain.argtypes = [vp]
+        L.storm_server_stats.argtypes = [vp, C.POINTER(A.StormServerStats)]
+        L.storm_server_destroy.argtypes = [vp]
         L.storm_cuda_status_string.restype = C.c_char_p
         L.storm_cuda_status_string.argtypes = [C.c_int]
         L.storm_cuda_abi_version.restype = C.c_int
@@ -287,3 +293,56 @@ class Engine:
 
     def set_segments_per_visit(self, k):
         self._check(lib().storm_cuda_set_segments_per_visit(self.h, k))
+
+
+class Server:
+    """Many independent problems on one GPU (storm_server_*): requests queue,
+    are admitted by slots and an HBM budget, and advance concurrently."""
+
+    def __init__(self, max_active=16, workers=8, hbm_budget_bytes=0, device=0):
+        cfg = A.StormServerConfig(device, max_active, workers, 0, hbm_budget_bytes)
+        h = C.c_void_p()
+        rc = lib().storm_server_create(C.byref(cfg), C.byref(h))
+        if rc != A.STORM_OK:
+            raise StormError(rc, lib().storm_cuda_status_string(rc).decode())
+        self.h = h
+        self._keep = {}   # ticket -> (descriptor, problem, temperature buffer)
+
+    def submit(self, problem, steps, dt=None, want_temperature=True):
+        desc = problem.to_desc()
+        T = np.zeros(problem.ncells) if want_temperature else None
+        t = C.c_uint64()
+        rc = lib().storm_server_submit(self.h, C.byref(desc), steps, problem.dt if dt is None else dt,
+                                       A.ptr(T) if T is not None else None, C.byref(t))
+        if rc != A.STORM_OK:
+            raise StormError(rc, lib().storm_cuda_status_string(rc).decode())
+        self._keep[t.value] = (desc, problem, T)
+        return t.value
+
+    def poll(self, capacity=1024):
+        buf = (A.StormRequestResult * capacity)()
+        n = C.c_uint32()
+        lib().storm_server_poll(self.h, buf, capacity, C.byref(n))
+        out = []
+        for k in range(n.value):
+            r = buf[k].as_dict()
+            keep = self._keep.pop(r["ticket"], None)
+            r["temperature"] = keep[2] if keep else None
+            out.append(r)
+        return out
+
+    def drain(self):
+        lib().storm_server_drain(self.h)
+
+    def stats(self):
+        st = A.StormServerStats()
+        lib().storm_server_stats(self.h, C.byref(st))
+        return st.as_dict()
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().storm_server_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        self.close()

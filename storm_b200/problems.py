@@ -214,3 +214,45 @@ def step_cube(n=64, new_photons_per_cell=3, face_packets=450, comb_nmin=20, comb
     p.comb_nmin, p.comb_factor = comb_nmin, comb_factor
     p.seed, p.dt, p.precision, p.name = seed, dt, precision, "step_cube"
     return p
+
+
+def uniform_cube(n=32, kappa=10.0, packets_per_step=100000, seed=42, dt=1e-11, precision=A.PRECISION_FP32_TRACK):
+    """Gray cube of one material (kappa_a uniform), hot face at x=0 (1 keV),
+    vacuum elsewhere, Random Walk where kappa*dx > 10.  Half of the packets per
+    step come from the cells, half from the hot face; the comb keeps about
+    packets_per_step in census."""
+    keV = UNITS["kev_kelvin"]
+    empty = np.zeros(1)
+    e = uniform_edges(0.0, 1.0, n)
+    p = Problem(e, e.copy(), e.copy(), empty, empty, empty)
+    _material(p, 0.01 * keV, CV_PER_VOLUME)
+    p.opacity_kind = A.OPACITY_CELL_TABLE
+    p.sigma_a = np.full(p.ncells, float(kappa))
+    p.sigma_s = np.zeros(p.ncells)
+    face = max(1, int(round(0.5 * packets_per_step / (n * n))))
+    p.faces = [BoxFace(A.FACE_ESCAPE, 1.0 * keV, face)] + [BoxFace(A.FACE_ESCAPE) for _ in range(5)]
+    p.new_photons_per_cell = max(1, int(round(0.5 * packets_per_step / p.ncells)))
+    p.with_random_walk = True
+    p.rw_min_cell_optical_depth = 20.0 / 3.0
+    p.rw_min_particle_optical_depth = 5.0
+    p.comb_enabled = True
+    p.comb_nmin, p.comb_factor = max(1, int(packets_per_step / (2 * p.ncells))), 2.0
+    p.seed, p.dt, p.precision, p.name = seed, dt, precision, "uniform_cube"
+    return p
+
+
+def serving_mix(count, n_range=(16, 48), packets_range=(1e4, 1e6), kappa_range=(0.1, 1000.0), steps_range=(5, 20),
+                seed=7, precision=A.PRECISION_FP32_TRACK):
+    """A seeded stream of independent requests: N log-uniform in n_range,
+    packets per step log-uniform in packets_range, kappa uniform in
+    kappa_range, steps uniform in steps_range.  Returns [(problem, steps)]."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for k in range(count):
+        n = int(round(np.exp(rng.uniform(np.log(n_range[0]), np.log(n_range[1])))))
+        packets = float(np.exp(rng.uniform(np.log(packets_range[0]), np.log(packets_range[1]))))
+        kappa = float(rng.uniform(*kappa_range))
+        steps = int(rng.integers(steps_range[0], steps_range[1] + 1))
+        out.append((uniform_cube(n=n, kappa=kappa, packets_per_step=packets, seed=1000 + k, precision=precision),
+                    steps))
+    return out

@@ -39,6 +39,7 @@ int main(void) {
          sizeof(StormReplayBatch), sizeof(StormBoxFace));
   printf("%zu %zu %zu %zu\n", offsetof(StormProblemDesc, faces), offsetof(StormProblemDesc, seed),
          offsetof(StormProblemDesc, device), offsetof(StormReplayBatch, used_random_walk));
+  printf("%zu %zu %zu\n", sizeof(StormServerConfig), sizeof(StormRequestResult), sizeof(StormServerStats));
   return 0;
 }
 '''
@@ -53,8 +54,9 @@ int main(void) {
     sizes = [int(x) for x in out]
     assert sizes[:5] == [C.sizeof(A.StormProblemDesc), C.sizeof(A.StormParticlesSoA), C.sizeof(A.StormStepStats),
                          C.sizeof(A.StormReplayBatch), C.sizeof(A.StormBoxFace)]
-    assert sizes[5:] == [A.StormProblemDesc.faces.offset, A.StormProblemDesc.seed.offset,
-                         A.StormProblemDesc.device.offset, A.StormReplayBatch.used_random_walk.offset]
+    assert sizes[5:9] == [A.StormProblemDesc.faces.offset, A.StormProblemDesc.seed.offset,
+                          A.StormProblemDesc.device.offset, A.StormReplayBatch.used_random_walk.offset]
+    assert sizes[9:] == [C.sizeof(A.StormServerConfig), C.sizeof(A.StormRequestResult), C.sizeof(A.StormServerStats)]
 
 
 def _create(desc):
@@ -111,3 +113,20 @@ def test_dropin_header_compiles_and_fails_loudly_without_device():
     assert not L.dropin_create(C.byref(desc), 0, err, 512)
     msg = err.value.decode()
     assert "MonteCarloManagerCUDA" in msg and "storm_cuda_create" in msg, msg
+
+
+def test_server_without_device_fails_loudly():
+    import torch
+    if torch.cuda.is_available():
+        pytest.skip("a GPU is visible")
+    cfg = A.StormServerConfig(0, 4, 2, 0, 0)
+    h = C.c_void_p()
+    assert engine.lib().storm_server_create(C.byref(cfg), C.byref(h)) == 7   # STORM_ERR_NO_DEVICE
+
+
+def test_serving_mix_is_seeded():
+    a = problems.serving_mix(8)
+    b = problems.serving_mix(8)
+    assert [(p.shape, s, p.sigma_a[0], p.new_photons_per_cell) for p, s in a] == \
+           [(p.shape, s, p.sigma_a[0], p.new_photons_per_cell) for p, s in b]
+    assert all(16 <= p.shape[0] <= 48 and 5 <= s <= 20 for p, s in a)
