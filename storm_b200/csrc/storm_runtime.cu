@@ -481,6 +481,26 @@ int check_device_error(StormHandle *h) {
     return STORM_OK;
 }
 
+// One small device->host read together with the device error word, one
+// stream synchronisation for both.
+int read_checked(StormHandle *h, void *dst, const void *src, size_t bytes) {
+    int32_t e[3] = {0, 0, 0};
+    CK(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaMemcpyAsync(e, h->dErr, sizeof(e), cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    if (e[0] != 0) {
+        h->errCode = e[0];
+        h->errCell = static_cast<uint32_t>(e[1]);
+        h->errParticle = static_cast<uint32_t>(e[2]);
+        char buf[160];
+        std::snprintf(buf, sizeof(buf), "device error %d at cell %u particle %u", e[0], static_cast<uint32_t>(e[1]),
+                      static_cast<uint32_t>(e[2]));
+        h->errMsg = buf;
+        return STORM_ERR_DEVICE;
+    }
+    return STORM_OK;
+}
+
 void refresh_ctx(StormHandle *h) {
     h->C.step = h->step;
 }
@@ -814,8 +834,8 @@ int storm_cuda_phase_transport(StormHandle *h) {
     CK(cudaMemsetAsync(h->counts, 0, sizeof(uint32_t) * (h->maxRounds + 2), h->stream));
     if (h->desc.per_cell_segment_counters) CK(cudaMemsetAsync(h->segs, 0, sizeof(uint32_t) * h->N, h->stream));
     uint32_t n32 = static_cast<uint32_t>(n0);
-    CK(cudaMemcpyAsync(h->counts, &n32, sizeof(uint32_t), cudaMemcpyHostToDevice, h->stream));
     uint32_t *nCen = h->counts + h->maxRounds + 1;
+    if (!h->refill) CK(cudaMemcpyAsync(h->counts, &n32, sizeof(uint32_t), cudaMemcpyHostToDevice, h->stream));
     if (h->refill) {
         // one launch carries every history to census, escape or cutoff
         const uint64_t maxSegs64 = static_cast<uint64_t>(h->maxRounds) * h->K;
@@ -837,7 +857,9 @@ int storm_cuda_phase_transport(StormHandle *h) {
         }
         CK(cudaGetLastError());
         CK(cudaEventRecord(h->evTransport1, h->stream));
-        CK(cudaStreamSynchronize(h->stream));
+        uint32_t nc = 0;
+        int rc = read_checked(h, &nc, nCen, sizeof(uint32_t));
+        if (rc != STORM_OK) return rc;
         if (h->profiling && n0) {
             float ms = 0.f;
             CK(cudaEventElapsedTime(&ms, h->evPool[0], h->evPool[1]));
@@ -845,10 +867,6 @@ int storm_cuda_phase_transport(StormHandle *h) {
             h->profLaunches += 1;
         }
         h->stats.rounds = n0 ? 1 : 0;
-        int rc = check_device_error(h);
-        if (rc != STORM_OK) return rc;
-        uint32_t nc = 0;
-        CK(read_small(h, &nc, nCen, sizeof(uint32_t)));
         h->stats.census_out_pre_comb = nc;
         if (h->profiling) {
             DevStats d{};
@@ -985,8 +1003,8 @@ int storm_cuda_phase_comb(StormHandle *h) {
     h->launches += 1 + 5 * passes + 5;
     CK(cudaGetLastError());
     uint32_t nValid = 0;
-    CK(cudaMemcpyAsync(&nValid, h->combStart + N, sizeof(uint32_t), cudaMemcpyDeviceToHost, h->stream));
-    CK(cudaStreamSynchronize(h->stream));
+    int rc = read_checked(h, &nValid, h->combStart + N, sizeof(uint32_t));
+    if (rc != STORM_OK) return rc;
     uint64_t *countU64 = alt ? h->keys : h->keysAlt;   // the sort's spare key buffer
     if (nValid) {
         launch_mask_count(h->stream, h->pCount, nValid, countU64);
@@ -996,8 +1014,6 @@ int storm_cuda_phase_comb(StormHandle *h) {
         CK(cudaMemsetAsync(h->dTotalU64, 0, sizeof(uint64_t), h->stream));
     }
     CK(cudaGetLastError());
-    int rc = check_device_error(h);
-    if (rc != STORM_OK) return rc;
     uint64_t total = 0;
     CK(read_small(h, &total, h->dTotalU64, sizeof(uint64_t)));
     // The write goes to bank A, which transport has finished with.  When the
@@ -1024,18 +1040,23 @@ int storm_cuda_phase_comb(StormHandle *h) {
     }
     h->nCensus = total;
     h->stats.census_out = total;
-    return check_device_error(h);
+    return STORM_OK;   // errors raised by the comb emit surface at the step's end
 }
 
-int storm_cuda_phase_poststep(StormHandle *h, double dt) {
-    if (!h) return STORM_ERR_INVALID_ARG;
+int poststep_launch(StormHandle *h, double dt) {
     refresh_ctx(h);
     launch_poststep(h->stream, h->C, h->A, h->M, dt);
     ++h->launches;
     CK(cudaGetLastError());
-    int rc = check_device_error(h);
     ++h->step;
-    return rc;
+    return STORM_OK;
+}
+
+int storm_cuda_phase_poststep(StormHandle *h, double dt) {
+    if (!h) return STORM_ERR_INVALID_ARG;
+    int rc = poststep_launch(h, dt);
+    if (rc != STORM_OK) return rc;
+    return check_device_error(h);
 }
 
 int storm_cuda_phase_stats(StormHandle *h, StormStepStats *s) {
@@ -1073,8 +1094,9 @@ int storm_cuda_step(StormHandle *h, double dt, StormStepStats *stats) {
     if (rc == STORM_OK) rc = storm_cuda_phase_transport(h);
     if (rc == STORM_OK) rc = storm_cuda_phase_comb(h);
     CK(cudaEventRecord(h->evAfterComb, h->stream));
-    if (rc == STORM_OK) rc = storm_cuda_phase_poststep(h, dt);
+    if (rc == STORM_OK) rc = poststep_launch(h, dt);
     CK(cudaEventRecord(h->evEnd, h->stream));
+    if (rc == STORM_OK) rc = check_device_error(h);   // also waits for the step's last kernel
     CK(cudaEventSynchronize(h->evEnd));
     float ms = 0.f;
     cudaEventElapsedTime(&ms, h->evStart, h->evEnd);
