@@ -36,7 +36,7 @@
 extern "C" {
 #endif
 
-#define STORM_CUDA_ABI_VERSION 2
+#define STORM_CUDA_ABI_VERSION 3
 
 /* ---------------------------------------------------------------- status */
 enum StormStatus {
@@ -64,7 +64,8 @@ enum StormDeviceError {
     STORM_DERR_HISTORY_CAP = 8,      /* a history exceeded max_rounds * segments_per_visit segments */
     STORM_DERR_BANK_OVERFLOW = 9,    /* more particles than bank capacity */
     STORM_DERR_TAPE_EXHAUSTED = 10,  /* replay: uniform tape too short */
-    STORM_DERR_COMB_TOTAL = 11       /* population/CombPopulationControl.hpp:147-153 total weight not finite */
+    STORM_DERR_COMB_TOTAL = 11,      /* population/CombPopulationControl.hpp:147-153 total weight not finite */
+    STORM_DERR_MG_SAMPLE = 12        /* utils/LinearInterpolation.hpp:22-28 "X too large" in a thermal energy draw */
 };
 
 /* ---------------------------------------------------------------- enums */
@@ -85,7 +86,13 @@ enum StormOpacityKind {
     /* sigma_a = min(kP0 * (kev_kelvin / max(T, t_floor))^alpha * rho^beta, cap)
        sigma_s = max(kR0 * f - kP0 * f, 0) with the same factors f.
        Marshak form: examples/marshak_wave/MarshakOpacity.hpp:30-46 (cap = +inf there). */
-    STORM_OPACITY_POWER_LAW = 1
+    STORM_OPACITY_POWER_LAW = 1,
+    /* Multigroup (groups >= 2): sigma_a(E, T) = sigma_a[cell] / ((kT)^q E^p) * (1 - exp(-E/kT))^s
+       with kT = k_B max(T, 1 K), E = max(frequency, group_bounds[0]), or the centre of the
+       particle's group when mg_group_constant; sigma_s[cell] elastic.  Planck mean, emission
+       spectrum and group CDF from the group centres with planck_integral weights, as
+       examples/densmore2012/DensmoreOpacity.hpp:36-56, 71-82, 146-165. */
+    STORM_OPACITY_MG_POWER = 2
 };
 
 enum StormEosKind {
@@ -166,6 +173,14 @@ typedef struct StormProblemDesc {
     uint32_t max_rounds;             /* bank visits per step before STORM_DERR_HISTORY_CAP (0 = automatic) */
     int32_t per_cell_segment_counters;   /* fill GetCellsStepsCounters() (costs one atomic per segment) */
     int32_t device;                  /* CUDA device ordinal */
+
+    /* ---- multigroup (RadiationIMC<..., NumGroups> with withMultigroupOpacity;
+     * the Random Walk becomes the PGRW of radiation/RadiationIMC.hpp:1008-1061) */
+    uint32_t groups;                 /* 0 or 1: gray; G >= 2: G groups */
+    int32_t mg_group_constant;       /* opacity at the centre of the particle's group */
+    const double *group_bounds;      /* G+1 increasing energies [erg] (energyBoundaries) */
+    double mg_p, mg_q, mg_s;         /* STORM_OPACITY_MG_POWER exponents */
+    double k_boltz;                  /* erg/K, for kT */
 } StormProblemDesc;
 
 /* Particle arrays, struct-of-arrays.  Mirrors the fields of
@@ -180,6 +195,7 @@ typedef struct StormParticlesSoA {
     uint32_t *cell;              /* cellIndex */
     uint64_t *id;                /* particle id within the step (may be NULL on input) */
     uint64_t count;
+    double *frequency;           /* photon energy [erg], multigroup problems (NULL otherwise) */
 } StormParticlesSoA;
 
 typedef struct StormStepStats {
@@ -228,6 +244,9 @@ typedef struct StormReplayBatch {
     int32_t *mgr_status;             /* 0 continue, 1 census, 2 removed (cutoff), 3 escaped */
     uint32_t *draws_used;
     int32_t *used_random_walk;
+    /* multigroup: the particle's frequency before and after (NULL for gray) */
+    const double *frequency;
+    double *phys_frequency;
 } StormReplayBatch;
 
 typedef struct StormHandle StormHandle;

@@ -191,12 +191,15 @@ class ReplayBatch:
     OUT_D = ("phys_x", "phys_y", "phys_z", "phys_vx", "phys_vy", "phys_vz", "phys_time_left", "phys_weight",
              "dep_material", "dep_erad", "mgr_x", "mgr_y", "mgr_z", "mgr_vx", "mgr_vy", "mgr_vz")
 
-    def __init__(self, before, cell, tape_offset, tape_length, tape):
+    def __init__(self, before, cell, tape_offset, tape_length, tape, frequency=None):
         n = len(cell)
         self.n = n
         self.arrays = {}
         for k, name in enumerate(self.IN):
             self.arrays[name] = np.ascontiguousarray(before[:, k])
+        if frequency is not None:   # multigroup: frequency in and out
+            self.arrays["frequency"] = np.ascontiguousarray(frequency, float)
+            self.arrays["phys_frequency"] = np.zeros(n)
         self.arrays["cell"] = np.ascontiguousarray(cell, np.uint32)
         self.arrays["tape_offset"] = np.ascontiguousarray(tape_offset, np.uint64)
         self.arrays["tape_length"] = np.ascontiguousarray(tape_length, np.uint32)

@@ -67,6 +67,8 @@ def lib():
         L.ref_record_tape_size.restype = C.c_uint64
         L.ref_record_tape_size.argtypes = [vp]
         L.ref_record_get.argtypes = [vp, u64p, u32p, dp, dp, i32p, u64p, dp, u64p, u32p, i32p, dp]
+        L.ref_record_get_frequency.argtypes = [vp, dp, dp]
+        L.ref_mg_thermal_energy.argtypes = [vp, C.c_uint64, u32p, dp, dp]
         L.ref_rw_sample.argtypes = [C.c_uint64, dp, dp, dp, dp, dp]
         L.ref_rw_functions.argtypes = [C.c_uint64, dp, dp, dp, dp]
         L.ref_sample_in_cell.argtypes = [vp, C.c_uint64, u32p, C.c_uint64, dp, dp, u32p]
@@ -90,6 +92,7 @@ class Particles:
         self.cell = np.zeros(n, dtype=np.uint32)
         self.id = np.zeros(n, dtype=np.uint64)
         self.n = n
+        self.frequency = np.zeros(n)   # photon energy (multigroup)
 
     def soa(self):
         """Struct of pointers; every field is made contiguous first (the C side
@@ -103,12 +106,15 @@ class Particles:
             setattr(s, f, A.ptr(getattr(self, f)))
         s.cell = A.ptr(self.cell, C.c_uint32)
         s.id = A.ptr(self.id, C.c_uint64)
+        if getattr(self, "frequency", None) is not None:
+            self.frequency = np.ascontiguousarray(self.frequency, dtype=np.float64)
+            s.frequency = A.ptr(self.frequency)
         s.count = self.n
         return s
 
     def take(self, idx):
         p = Particles(len(idx))
-        for f in self.FIELDS + ("cell", "id"):
+        for f in self.FIELDS + ("cell", "id", "frequency"):
             setattr(p, f, np.ascontiguousarray(getattr(self, f)[idx]))
         return p
 
@@ -194,7 +200,18 @@ class Reference:
                          A.ptr(r["after"]), A.ptr(r["status"], C.c_int32), A.ptr(r["next"], C.c_uint64),
                          A.ptr(r["tallies"]), A.ptr(r["tape_offset"], C.c_uint64),
                          A.ptr(r["tape_length"], C.c_uint32), A.ptr(r["used_rw"], C.c_int32), A.ptr(r["tape"]))
+        r["freq_before"] = np.zeros(n)
+        r["freq_after"] = np.zeros(n)
+        L.ref_record_get_frequency(self.h, A.ptr(r["freq_before"]), A.ptr(r["freq_after"]))
         return r
+
+    def thermal_energy(self, cells, xi):
+        """The opacity plug-in's GetThermalEnergy at given uniforms (multigroup)."""
+        cells = np.ascontiguousarray(cells, np.uint32)
+        xi = np.ascontiguousarray(xi, float)
+        out = np.zeros(len(xi))
+        self._check(lib().ref_mg_thermal_energy(self.h, len(xi), A.ptr(cells, C.c_uint32), A.ptr(xi), A.ptr(out)))
+        return out
 
     def sample_in_cell(self, cells, seed):
         cells = np.ascontiguousarray(cells, np.uint32)

@@ -20,6 +20,8 @@
 // so the harness opacity model keeps the address on first use.  Engine states
 // compare with ==, so the draws of one step are counted by advancing a copy
 // taken before the call, and replayed through a second copy to log the doubles.
+#include <algorithm>
+#include <array>
 #include <cassert>
 #include <chrono>
 #include <cstdint>
@@ -47,6 +49,8 @@
 #include "manager/MonteCarloManagerSerial.hpp"
 #include "utils/RandomInCell.hpp"
 #include "utils/RandomOnFace.hpp"
+#include "utils/LinearInterpolation.hpp"
+#include <planck_integral/planck_integral.hpp>
 
 #include "storm_cuda.h"
 
@@ -78,30 +82,82 @@ struct HarnessEOS {
 };
 
 // ------------------------------------------------------------------ opacity
-class HarnessOpacity : public STORM::RadiationOpacityModel<Vector3D, Grid, Cell, 1> {
+// Gray (NumGroups = 1): per-cell table or the Marshak power law.  Multigroup
+// (STORM_OPACITY_MG_POWER): sigma(E, T) = sigma0[cell] / ((kT)^q E^p) (1 - e^{-E/kT})^s
+// with the group machinery of examples/densmore2012/DensmoreOpacity.hpp:36-165
+// (Planck mean and emission spectrum from group centres weighted by
+// planck_integral, inverse-CDF sampling by LinearInterpolation).
+template <std::size_t G>
+class HarnessOpacityT : public STORM::RadiationOpacityModel<Vector3D, Grid, Cell, G> {
 public:
-    using Base = STORM::RadiationOpacityModel<Vector3D, Grid, Cell, 1>;
+    using Base = STORM::RadiationOpacityModel<Vector3D, Grid, Cell, G>;
+    using GroupArray = typename Base::GroupArray;
+    using GroupBoundaries = typename Base::GroupBoundaries;
+    using GroupCdf = std::array<double, G + 1>;
     int kind = STORM_OPACITY_CELL_TABLE;
     std::vector<double> sigA, sigS, rhoFactor;
     double kP0 = 0, kR0 = 0, alpha = 0, tFloor = 1.0, cap = 0, kevKelvin = units::kev_kelvin;
+    GroupBoundaries bounds{};
+    bool groupConstant = false;
+    double mgP = 3.0, mgQ = 0.0, mgS = 0.0, kBoltz = units::k_boltz;
     const std::vector<Cell> *cells = nullptr;
     std::mt19937_64 *captured = nullptr;
 
     double CalcPlanckOpacity(const Cell &cell) override {
         std::size_t i = index(cell);
+        if (kind == STORM_OPACITY_MG_POWER) {
+            double kT = kBoltz * std::max(cell.temperature, 1.0);
+            double weightedSum = 0, totalWeight = 0;
+            for (std::size_t g = 0; g < G; ++g) {
+                double Ec = 0.5 * (bounds[g] + bounds[g + 1]);
+                double a = bounds[g] / kT, b = bounds[g + 1] / kT;
+                double Bg = (a > 0.0 && b > a) ? planck_integral::planck_integral(a, b) : 0.0;
+                weightedSum += sigmaAt(i, Ec, kT) * Bg;
+                totalWeight += Bg;
+            }
+            return (totalWeight > 0) ? weightedSum / totalWeight : 1e-20;
+        }
         if (kind == STORM_OPACITY_CELL_TABLE) return sigA[i];
         double tf = std::pow(kevKelvin / std::max(cell.temperature, tFloor), alpha);
         double k = kP0 * tf * rf(i);
         return (cap > 0.0) ? std::min(k, cap) : k;
     }
+    double CalcAbsorptionOpacity(const Cell &cell, double frequency) override {
+        if (kind != STORM_OPACITY_MG_POWER) return CalcPlanckOpacity(cell);
+        std::size_t i = index(cell);
+        double kT = kBoltz * std::max(cell.temperature, 1.0);
+        double E;
+        if (groupConstant) {
+            std::size_t g = this->findGroup(frequency, bounds);
+            E = 0.5 * (bounds[g] + bounds[g + 1]);
+        } else {
+            E = std::max(frequency, bounds[0]);
+        }
+        return sigmaAt(i, E, kT);
+    }
     double CalcScatteringOpacity(const Cell &cell) override {
         std::size_t i = index(cell);
-        if (kind == STORM_OPACITY_CELL_TABLE) return sigS.empty() ? 0.0 : sigS[i];
+        if (kind == STORM_OPACITY_CELL_TABLE || kind == STORM_OPACITY_MG_POWER) return sigS.empty() ? 0.0 : sigS[i];
         if (!(kR0 > 0.0)) return 0.0;
         double tf = std::pow(kevKelvin / std::max(cell.temperature, tFloor), alpha);
         double kR = kR0 * tf * rf(i);
         double kP = kP0 * tf * rf(i);
         return std::max(kR - kP, 0.0);
+    }
+    double GetThermalEnergy(const Cell &cell, double random, const GroupBoundaries &boundaries) const override {
+        if (kind != STORM_OPACITY_MG_POWER) return Base::GetThermalEnergy(cell, random, boundaries);
+        GroupCdf cumulative = cumulativePlanck(cell, boundaries);
+        double total = cumulative[G];
+        if (!(total > 0.0) || !std::isfinite(total)) return Base::GetThermalEnergy(cell, random, boundaries);
+        double r = std::isfinite(random) ? std::clamp(random, 0.0, std::nextafter(1.0, 0.0)) : 0.5;
+        return STORM::LinearInterpolation(cumulative, boundaries, r * total);
+    }
+    GroupArray GetCumulativeOpacity(const Cell &cell, const GroupBoundaries &boundaries) const override {
+        if (kind != STORM_OPACITY_MG_POWER) return Base::GetCumulativeOpacity(cell, boundaries);
+        GroupArray upper{};
+        GroupCdf cumulative = cumulativePlanck(cell, boundaries);
+        for (std::size_t g = 0; g < G; ++g) upper[g] = cumulative[g + 1];
+        return upper;
     }
     Vector3D getRandomVelocity(const Cell &cell, std::mt19937_64 &rng, std::uniform_real_distribution<double> &dist) override {
         captured = &rng;
@@ -110,11 +166,32 @@ public:
     static Vector3D isotropic(std::mt19937_64 &rng, std::uniform_real_distribution<double> &dist) {
         return Base::isotropicVelocity(rng, dist);
     }
+    double sigmaAt(std::size_t i, double E, double kT) const {
+        double v = sigA[i] / (std::pow(kT, mgQ) * std::pow(E, mgP));
+        if (mgS != 0.0) v *= std::pow(-std::expm1(-E / kT), mgS);
+        return v;
+    }
 
 private:
     std::size_t index(const Cell &cell) const { return static_cast<std::size_t>(&cell - cells->data()); }
     double rf(std::size_t i) const { return rhoFactor.empty() ? 1.0 : rhoFactor[i]; }
+    GroupCdf cumulativePlanck(const Cell &cell, const GroupBoundaries &boundaries) const {
+        GroupCdf cdf{};
+        cdf[0] = 0.0;
+        std::size_t i = index(cell);
+        double kT = kBoltz * std::max(cell.temperature, 1.0);
+        for (std::size_t g = 0; g < G; ++g) {
+            double a = boundaries[g] / kT, b = boundaries[g + 1] / kT;
+            double bg = (a > 0.0 && b > a) ? planck_integral::planck_integral(a, b) : 0.0;
+            double Ec = 0.5 * (boundaries[g] + boundaries[g + 1]);
+            double sg = sigmaAt(i, Ec, kT);
+            double weight = (sg > 0.0 && std::isfinite(sg) && std::isfinite(bg)) ? sg * bg : 0.0;
+            cdf[g + 1] = cdf[g] + weight;
+        }
+        return cdf;
+    }
 };
+using HarnessOpacity = HarnessOpacityT<1>;
 
 // ------------------------------------------------------------------ boundary
 // A per-box-face boundary plug-in written against STORM's BoundaryCondition
@@ -227,23 +304,32 @@ struct Record {
     uint64_t tapeOffset;
     uint32_t tapeLength;
     int32_t usedRW;
+    double freqBefore, freqAfter;
 };
 
-using IMCBase = STORM::RadiationIMC<Vector3D, Grid, Cell, Ext, HarnessEOS, 1>;
-
-class RecordingIMC : public IMCBase {
-public:
-    using IMCBase::IMCBase;
-    HarnessOpacity *opac = nullptr;
-    std::vector<Ext> *ext = nullptr;
+struct RecordState {
     bool recording = false;
     std::size_t maxRecords = 0;
     std::vector<Record> records;
     std::vector<double> tape;
+};
+
+template <std::size_t G>
+using IMCBaseT = STORM::RadiationIMC<Vector3D, Grid, Cell, Ext, HarnessEOS, G>;
+
+template <std::size_t G>
+class RecordingIMC : public IMCBaseT<G> {
+public:
+    using Base = IMCBaseT<G>;
+    using Functionality = typename Base::Functionality;
+    using Base::Base;
+    HarnessOpacityT<G> *opac = nullptr;
+    std::vector<Ext> *ext = nullptr;
+    RecordState rs;
 
     Functionality step(MCParticle &p, std::vector<MCParticle> &add) override {
-        if (!recording || opac == nullptr || opac->captured == nullptr || records.size() >= maxRecords)
-            return IMCBase::step(p, add);
+        if (!rs.recording || opac == nullptr || opac->captured == nullptr || rs.records.size() >= rs.maxRecords)
+            return Base::step(p, add);
         Record r{};
         r.id = p.id;
         r.cell = static_cast<uint32_t>(p.cellIndex);
@@ -251,11 +337,12 @@ public:
         double b[9] = {p.location.x, p.location.y, p.location.z, p.velocity.x, p.velocity.y, p.velocity.z,
                        p.timeLeft, p.weight, p.initialWeight};
         std::memcpy(r.before, b, sizeof(b));
+        r.freqBefore = p.frequency;
         r.eradBefore = this->getEradTimeAvg()[c];
         r.ematBefore = (*ext)[c].internal_energy;
         std::mt19937_64 snap = *opac->captured;
         std::size_t rwBefore = this->getRandomWalkStepCount();
-        Functionality res = IMCBase::step(p, add);
+        Functionality res = Base::step(p, add);
         std::mt19937_64 counter = snap;
         uint32_t n = 0;
         while (!(counter == *opac->captured)) {
@@ -263,19 +350,55 @@ public:
             if (++n > 4096) throw STORM::StormError("recording: could not match the engine state");
         }
         std::uniform_real_distribution<double> dist(0.0, 1.0);
-        r.tapeOffset = tape.size();
+        r.tapeOffset = rs.tape.size();
         r.tapeLength = n;
-        for (uint32_t k = 0; k < n; ++k) tape.push_back(dist(snap));
+        for (uint32_t k = 0; k < n; ++k) rs.tape.push_back(dist(snap));
         double a[8] = {p.location.x, p.location.y, p.location.z, p.velocity.x, p.velocity.y, p.velocity.z,
                        p.timeLeft, p.weight};
         std::memcpy(r.after, a, sizeof(a));
+        r.freqAfter = p.frequency;
         r.status = static_cast<int32_t>(res.change);
         r.nextCell = res.nextCellIndex;
         r.eradAfter = this->getEradTimeAvg()[c];
         r.ematAfter = (*ext)[c].internal_energy;
         r.usedRW = this->getRandomWalkStepCount() != rwBefore;
-        records.push_back(r);
+        rs.records.push_back(r);
         return res;
+    }
+};
+
+// The RadiationIMC calls the C API needs, independent of the group count.
+struct PhysicsView {
+    virtual ~PhysicsView() = default;
+    virtual void updateGridData() = 0;
+    virtual std::vector<MCParticle> preStep(double dt) = 0;
+    virtual const std::vector<double> &eradTimeAvg() const = 0;
+    virtual const std::vector<double> &planckOpacities() const = 0;
+    virtual const std::vector<double> &factorFleck() const = 0;
+    virtual std::vector<std::size_t> lastSourcePhotonsPerCell() const = 0;
+    virtual std::size_t randomWalkStepCount() const = 0;
+    virtual RecordState &records() = 0;
+    virtual int thermalEnergy(uint64_t n, const uint32_t *cells, const double *xi, double *energy) = 0;
+};
+template <std::size_t G>
+struct PhysicsViewT : PhysicsView {
+    std::shared_ptr<RecordingIMC<G>> p;
+    explicit PhysicsViewT(std::shared_ptr<RecordingIMC<G>> q) : p(std::move(q)) {}
+    void updateGridData() override { p->updateGridData(); }
+    std::vector<MCParticle> preStep(double dt) override { return p->preStep(dt); }
+    const std::vector<double> &eradTimeAvg() const override { return p->getEradTimeAvg(); }
+    const std::vector<double> &planckOpacities() const override { return p->getPlanckOpacities(); }
+    const std::vector<double> &factorFleck() const override { return p->getFactorFleck(); }
+    std::vector<std::size_t> lastSourcePhotonsPerCell() const override {
+        const auto &v = p->getLastSourcePhotonsPerCell();
+        return std::vector<std::size_t>(v.begin(), v.end());
+    }
+    std::size_t randomWalkStepCount() const override { return p->getRandomWalkStepCount(); }
+    RecordState &records() override { return p->rs; }
+    int thermalEnergy(uint64_t n, const uint32_t *cells, const double *xi, double *energy) override {
+        typename HarnessOpacityT<G>::GroupBoundaries b = p->opac->bounds;
+        for (uint64_t k = 0; k < n; ++k) energy[k] = p->opac->GetThermalEnergy((*p->opac->cells)[cells[k]], xi[k], b);
+        return 0;
     }
 };
 
@@ -293,15 +416,57 @@ struct RefHandle {
     std::vector<Cell> cells;
     std::vector<Ext> ext;
     std::shared_ptr<HarnessEOS> eos;
-    std::shared_ptr<HarnessOpacity> opacity;
     std::shared_ptr<STORM::BoundaryCondition<Vector3D, Grid>> boundary;
     HarnessBoundary *harnessBoundary = nullptr;
-    std::shared_ptr<RecordingIMC> physics;
+    std::shared_ptr<STORM::MonteCarloPhysics<Vector3D, Grid>> physics;   // RecordingIMC<G>
+    std::unique_ptr<PhysicsView> view;
     std::shared_ptr<STORM::PopulationControl<Vector3D, Grid>> pop;
     std::unique_ptr<STORM::MonteCarloManagerSerial<Vector3D, Grid>> manager;
     std::vector<MCParticle> census;
     std::string lastError;
 };
+
+constexpr std::size_t kMGGroups = 64;
+
+// RadiationIMC<..., G> with the harness opacity plug-in built from the descriptor.
+template <std::size_t G>
+void build_physics(RefHandle &h, const StormProblemDesc *d) {
+    const std::size_t N = h.grid->GetPointNo();
+    auto opacity = std::make_shared<HarnessOpacityT<G>>();
+    auto &op = *opacity;
+    op.kind = d->opacity_kind;
+    op.cells = &h.cells;
+    if (d->opacity_kind == STORM_OPACITY_CELL_TABLE || d->opacity_kind == STORM_OPACITY_MG_POWER) {
+        op.sigA.assign(d->sigma_a, d->sigma_a + N);
+        if (d->sigma_s) op.sigS.assign(d->sigma_s, d->sigma_s + N);
+    } else {
+        op.kP0 = d->kP0; op.kR0 = d->kR0; op.alpha = d->alpha; op.tFloor = d->t_floor; op.cap = d->cap;
+        op.kevKelvin = d->kev_kelvin;
+        if (d->density_factor) op.rhoFactor.assign(d->density_factor, d->density_factor + N);
+    }
+    STORM::RadiationIMCParameters<G> p;
+    if constexpr (G > 1) {
+        for (std::size_t g = 0; g <= G; ++g) op.bounds[g] = d->group_bounds[g];
+        op.groupConstant = d->mg_group_constant != 0;
+        op.mgP = d->mg_p; op.mgQ = d->mg_q; op.mgS = d->mg_s;
+        op.kBoltz = d->k_boltz;
+        p.withMultigroupOpacity = true;
+        p.energyBoundaries = op.bounds;
+        p.energyBoundariesProvided = true;
+    }
+    p.newPhotonsPerCell = d->new_photons_per_cell;
+    p.withRandomWalk = d->with_random_walk != 0;
+    p.rwMinCellOpticalDepth = d->rw_min_cell_optical_depth;
+    p.rwMinParticleOpticalDepth = d->rw_min_particle_optical_depth;
+    p.noHydroFeedback = d->no_hydro_feedback != 0;
+    auto physics = std::make_shared<RecordingIMC<G>>(*h.grid, h.boundary, h.cells, h.ext, h.eos, opacity, p,
+                                                     STORM::DirectRadiationIMCTraits<Vector3D, Cell, Ext, G>(),
+                                                     RandomInCellPositionSampler<Vector3D, Grid>(), d->seed);
+    physics->opac = opacity.get();
+    physics->ext = &h.ext;
+    h.physics = physics;
+    h.view = std::make_unique<PhysicsViewT<G>>(physics);
+}
 
 extern "C" {
 
@@ -335,18 +500,6 @@ RefHandle *ref_create(const StormProblemDesc *d, int boundary_kind, char *err, s
         h->eos->f = d->eos_f;
         h->eos->beta = d->eos_beta;
         h->eos->mu = d->eos_mu;
-        h->opacity = std::make_shared<HarnessOpacity>();
-        auto &op = *h->opacity;
-        op.kind = d->opacity_kind;
-        op.cells = &h->cells;
-        if (d->opacity_kind == STORM_OPACITY_CELL_TABLE) {
-            op.sigA.assign(d->sigma_a, d->sigma_a + N);
-            if (d->sigma_s) op.sigS.assign(d->sigma_s, d->sigma_s + N);
-        } else {
-            op.kP0 = d->kP0; op.kR0 = d->kR0; op.alpha = d->alpha; op.tFloor = d->t_floor; op.cap = d->cap;
-            op.kevKelvin = d->kev_kelvin;
-            if (d->density_factor) op.rhoFactor.assign(d->density_factor, d->density_factor + N);
-        }
         switch (boundary_kind) {
         case 0: {
             auto b = std::make_shared<HarnessBoundary>(*h->grid);
@@ -370,17 +523,12 @@ RefHandle *ref_create(const StormProblemDesc *d, int boundary_kind, char *err, s
             break;
         default: throw STORM::StormError("unknown boundary kind");
         }
-        STORM::RadiationIMCParameters<1> p;
-        p.newPhotonsPerCell = d->new_photons_per_cell;
-        p.withRandomWalk = d->with_random_walk != 0;
-        p.rwMinCellOpticalDepth = d->rw_min_cell_optical_depth;
-        p.rwMinParticleOpticalDepth = d->rw_min_particle_optical_depth;
-        p.noHydroFeedback = d->no_hydro_feedback != 0;
-        h->physics = std::make_shared<RecordingIMC>(*h->grid, h->boundary, h->cells, h->ext, h->eos, h->opacity, p,
-                                                    STORM::DirectRadiationIMCTraits<Vector3D, Cell, Ext, 1>(),
-                                                    RandomInCellPositionSampler<Vector3D, Grid>(), d->seed);
-        h->physics->opac = h->opacity.get();
-        h->physics->ext = &h->ext;
+        if (d->groups >= 2) {
+            if (d->groups != kMGGroups) throw STORM::StormError("reference build holds multigroup for 64 groups only");
+            build_physics<kMGGroups>(*h, d);
+        } else {
+            build_physics<1>(*h, d);
+        }
         if (d->comb_enabled)
             h->pop = std::make_shared<STORM::CombPopulationControl<Vector3D, Grid>>(*h->grid, d->comb_nmin, d->comb_factor);
         else
@@ -414,7 +562,7 @@ int ref_step(RefHandle *h, double dt, RefStepOut *out) {
             uint64_t s = 0;
             for (auto c : h->manager->GetCellsStepsCounters()) s += c;
             out->segments = s;
-            out->rw_steps = h->physics->getRandomWalkStepCount();
+            out->rw_steps = h->view->randomWalkStepCount();
             out->wall_seconds = std::chrono::duration<double>(t1 - t0).count();
             out->escaped_energy = h->harnessBoundary ? h->harnessBoundary->escaped : 0.0;
         }
@@ -430,8 +578,8 @@ int ref_step(RefHandle *h, double dt, RefStepOut *out) {
 // replace the census buffer so the tests can inspect them.
 int ref_prestep_only(RefHandle *h, double dt, uint64_t *emitted) {
     try {
-        h->physics->updateGridData();
-        h->census = h->physics->preStep(dt);
+        h->view->updateGridData();
+        h->census = h->view->preStep(dt);
         if (emitted) *emitted = h->census.size();
         return 0;
     } catch (const std::exception &e) {
@@ -450,6 +598,7 @@ int ref_get_census(RefHandle *h, StormParticlesSoA *o) {
         o->time_left[k] = p.timeLeft; o->weight[k] = p.weight; o->initial_weight[k] = p.initialWeight;
         o->cell[k] = static_cast<uint32_t>(p.cellIndex);
         if (o->id) o->id[k] = p.id;
+        if (o->frequency) o->frequency[k] = p.frequency;
     }
     return 0;
 }
@@ -464,7 +613,7 @@ int ref_set_census(RefHandle *h, const StormParticlesSoA *in) {
         p.weight = in->weight[k];
         p.initialWeight = in->initial_weight[k];
         p.cellIndex = in->cell[k];
-        p.frequency = 0;
+        p.frequency = in->frequency ? in->frequency[k] : 0.0;
         p.id = in->id ? in->id[k] : std::numeric_limits<std::size_t>::max();
         h->census.push_back(p);
     }
@@ -474,9 +623,9 @@ int ref_set_census(RefHandle *h, const StormParticlesSoA *in) {
 int ref_get_cells(RefHandle *h, double *T, double *eint, double *eradAvg, double *eradCensus, double *sigA, double *fleck,
                   uint64_t *segs) {
     const std::size_t N = h->grid->GetPointNo();
-    const auto &ea = h->physics->getEradTimeAvg();
-    const auto &sa = h->physics->getPlanckOpacities();
-    const auto &ff = h->physics->getFactorFleck();
+    const auto &ea = h->view->eradTimeAvg();
+    const auto &sa = h->view->planckOpacities();
+    const auto &ff = h->view->factorFleck();
     const auto &sc = h->manager->GetCellsStepsCounters();
     for (std::size_t i = 0; i < N; ++i) {
         if (T) T[i] = h->cells[i].temperature;
@@ -491,32 +640,33 @@ int ref_get_cells(RefHandle *h, double *T, double *eint, double *eradAvg, double
 }
 
 int ref_get_emission(RefHandle *h, uint64_t *photons) {
-    const auto &v = h->physics->getLastSourcePhotonsPerCell();
+    const auto v = h->view->lastSourcePhotonsPerCell();
     for (std::size_t i = 0; i < v.size(); ++i) photons[i] = v[i];
     return 0;
 }
 
 // ---------------- recording
 int ref_record_begin(RefHandle *h, uint64_t maxRecords) {
-    h->physics->records.clear();
-    h->physics->tape.clear();
-    h->physics->maxRecords = maxRecords;
-    h->physics->recording = true;
+    RecordState &rs = h->view->records();
+    rs.records.clear();
+    rs.tape.clear();
+    rs.maxRecords = maxRecords;
+    rs.recording = true;
     return 0;
 }
 int ref_record_end(RefHandle *h) {
-    h->physics->recording = false;
+    h->view->records().recording = false;
     return 0;
 }
-uint64_t ref_record_count(RefHandle *h) { return h->physics->records.size(); }
-uint64_t ref_record_tape_size(RefHandle *h) { return h->physics->tape.size(); }
+uint64_t ref_record_count(RefHandle *h) { return h->view->records().records.size(); }
+uint64_t ref_record_tape_size(RefHandle *h) { return h->view->records().tape.size(); }
 
 // Copies the records out as parallel arrays.  before: 9n, after: 8n,
 // tallies: 4n (emat before/after, erad before/after), tape: tape_size.
 int ref_record_get(RefHandle *h, uint64_t *id, uint32_t *cell, double *before, double *after, int32_t *status,
                    uint64_t *nextCell, double *tallies, uint64_t *tapeOffset, uint32_t *tapeLength, int32_t *usedRW,
                    double *tape) {
-    const auto &R = h->physics->records;
+    const auto &R = h->view->records().records;
     for (std::size_t k = 0; k < R.size(); ++k) {
         id[k] = R[k].id;
         cell[k] = R[k].cell;
@@ -532,8 +682,29 @@ int ref_record_get(RefHandle *h, uint64_t *id, uint32_t *cell, double *before, d
         tapeLength[k] = R[k].tapeLength;
         usedRW[k] = R[k].usedRW;
     }
-    std::memcpy(tape, h->physics->tape.data(), h->physics->tape.size() * sizeof(double));
+    std::memcpy(tape, h->view->records().tape.data(), h->view->records().tape.size() * sizeof(double));
     return 0;
+}
+
+// Frequencies of the records (multigroup): before and after, n each.
+int ref_record_get_frequency(RefHandle *h, double *before, double *after) {
+    const auto &R = h->view->records().records;
+    for (std::size_t k = 0; k < R.size(); ++k) {
+        before[k] = R[k].freqBefore;
+        after[k] = R[k].freqAfter;
+    }
+    return 0;
+}
+
+// Multigroup tables the reference computes per cell: the Planck mean opacity
+// of its opacity plug-in and the thermal energy it samples at given uniforms.
+int ref_mg_thermal_energy(RefHandle *h, uint64_t n, const uint32_t *cells, const double *xi, double *energy) {
+    try {
+        return h->view->thermalEnergy(n, cells, xi, energy);
+    } catch (const std::exception &e) {
+        h->lastError = e.what();
+        return 1;
+    }
 }
 
 // ---------------- component probes
@@ -625,6 +796,7 @@ int ref_comb(RefHandle *h, const StormParticlesSoA *in, StormParticlesSoA *out, 
             p.weight = in->weight[k];
             p.initialWeight = in->initial_weight[k];
             p.cellIndex = in->cell[k];
+            p.frequency = in->frequency ? in->frequency[k] : 0.0;
             p.id = in->id ? in->id[k] : k;
             v.push_back(p);
         }
@@ -636,6 +808,7 @@ int ref_comb(RefHandle *h, const StormParticlesSoA *in, StormParticlesSoA *out, 
             out->time_left[k] = r[k].timeLeft; out->weight[k] = r[k].weight; out->initial_weight[k] = r[k].initialWeight;
             out->cell[k] = static_cast<uint32_t>(r[k].cellIndex);
             if (out->id) out->id[k] = r[k].id;
+            if (out->frequency) out->frequency[k] = r[k].frequency;
         }
         return 0;
     } catch (const std::exception &e) {

@@ -5,7 +5,7 @@ sizes against the compiled library.
 """
 import ctypes as C
 
-ABI_VERSION = 2
+ABI_VERSION = 3
 
 STORM_OK = 0
 STATUS_NAMES = {
@@ -24,6 +24,7 @@ FACE_REFLECT = 0
 FACE_ESCAPE = 1
 OPACITY_CELL_TABLE = 0
 OPACITY_POWER_LAW = 1
+OPACITY_MG_POWER = 2
 EOS_LINEAR = 0
 EOS_POWER_LAW = 1
 
@@ -67,6 +68,8 @@ class StormProblemDesc(C.Structure):
         ("seed", C.c_uint64), ("capacity", C.c_uint64),
         ("segments_per_visit", C.c_uint32), ("max_rounds", C.c_uint32),
         ("per_cell_segment_counters", C.c_int32), ("device", C.c_int32),
+        ("groups", C.c_uint32), ("mg_group_constant", C.c_int32), ("group_bounds", _dp),
+        ("mg_p", C.c_double), ("mg_q", C.c_double), ("mg_s", C.c_double), ("k_boltz", C.c_double),
     ]
 
 
@@ -75,7 +78,7 @@ class StormParticlesSoA(C.Structure):
         ("x", _dp), ("y", _dp), ("z", _dp),
         ("vx", _dp), ("vy", _dp), ("vz", _dp),
         ("time_left", _dp), ("weight", _dp), ("initial_weight", _dp),
-        ("cell", _u32p), ("id", _u64p), ("count", C.c_uint64),
+        ("cell", _u32p), ("id", _u64p), ("count", C.c_uint64), ("frequency", _dp),
     ]
 
 
@@ -106,6 +109,7 @@ class StormReplayBatch(C.Structure):
         ("dep_material", _dp), ("dep_erad", _dp),
         ("mgr_x", _dp), ("mgr_y", _dp), ("mgr_z", _dp), ("mgr_vx", _dp), ("mgr_vy", _dp), ("mgr_vz", _dp),
         ("mgr_cell", _u32p), ("mgr_status", _i32p), ("draws_used", _u32p), ("used_random_walk", _i32p),
+        ("frequency", _dp), ("phys_frequency", _dp),
     ]
 
 

@@ -84,6 +84,16 @@ struct Ctx {
     uint32_t *segs;
     RwTables rw;
     int32_t *err;            // [0] code, [1] cell lo, [2] particle lo
+    // multigroup (groups >= 2)
+    uint32_t groups;
+    int32_t mgGroupConst;    // opacity at the centre of the particle's group
+    const double *gb;        // groups + 1 bounds [erg]
+    double mgP, mgQ, mgS, kBoltz;
+    const double *T;         // cell temperatures
+    const double *sig0;      // sigma0 per cell
+    const double *mgCdf;     // per cell, groups + 1: cumulative sigma_g B_g (the emission spectrum)
+    const double4 *pgrw;     // per cell: sigmaT_bar, sigmaA_bar, D, gamma
+    const uint32_t *pgrwCut; // per cell: group cutoff (0 = no PGRW)
 };
 
 // ------------------------------------------------------------------ errors
@@ -226,6 +236,7 @@ struct TapeRng {
 // ------------------------------------------------------------------ particle in registers
 struct PartReg {
     double x, y, z, vx, vy, vz, t, w, w0;
+    double nu;       // photon energy [erg] (multigroup)
     uint32_t cell;
 };
 
@@ -320,6 +331,108 @@ struct SegmentTally {
     __device__ __forceinline__ void rad(uint32_t c, double v) { atomicAdd(erad + c, v); }
 };
 
+// ------------------------------------------------------------------ multigroup
+// planck_integral(a, b) = 15/pi^4 int_a^b x^3/(e^x - 1) dx from Clark's two
+// published series: the Bernoulli expansion below x = 0.5 and the exponential
+// tail series above; the same evaluation order as the host table build.
+constexpr double PI_NORM_PI = 3.14159265358979323846;
+__device__ __forceinline__ double pi_norm() { return 15.0 / (PI_NORM_PI * PI_NORM_PI * PI_NORM_PI * PI_NORM_PI); }
+__device__ inline double pi_small_series(double x) {
+    const double B[21] = {1.0, -0.5, 1.0 / 6.0, 0.0, -1.0 / 30.0, 0.0, 1.0 / 42.0, 0.0, -1.0 / 30.0, 0.0,
+                          5.0 / 66.0, 0.0, -691.0 / 2730.0, 0.0, 7.0 / 6.0, 0.0, -3617.0 / 510.0, 0.0,
+                          43867.0 / 798.0, 0.0, -174611.0 / 330.0};
+    double sum = 0.0, xp = x * x * x, fact = 1.0;
+#pragma unroll
+    for (int k = 0; k <= 20; ++k) {
+        if (k > 0) { fact *= k; xp *= x; }
+        if (B[k] != 0.0) sum += B[k] * xp / (fact * (k + 3));
+    }
+    return sum;
+}
+__device__ inline double pi_tail_series(double x) {
+    double sum = 0.0;
+    for (int n = 1; n < 100000; ++n) {
+        double e = exp(-n * x);
+        if (e == 0.0) break;
+        double dn = n;
+        double term = e * (x * x * x / dn + 3.0 * x * x / (dn * dn) + 6.0 * x / (dn * dn * dn) + 6.0 / (dn * dn * dn * dn));
+        sum += term;
+        if (term < 1e-18 * sum) break;
+    }
+    return sum;
+}
+__device__ inline double pi_cumulative(double x) {
+    if (!(x > 0.0)) return 0.0;
+    if (x < 0.5) return pi_norm() * pi_small_series(x);
+    return 1.0 - pi_norm() * pi_tail_series(x);
+}
+__device__ inline double planck_integral(double a, double b) {
+    if (a >= 0.5 && b >= 0.5) return pi_norm() * (pi_tail_series(a) - pi_tail_series(b));
+    return pi_cumulative(b) - pi_cumulative(a);
+}
+
+// std::clamp(nu, b_0, b_G) (RadiationIMC::clampFrequencyToBounds, radiation/RadiationIMC.hpp:869-872)
+__device__ __forceinline__ double mg_clamp(const Ctx &C, double nu) {
+    const double lo = C.gb[0], hi = C.gb[C.groups];
+    return nu < lo ? lo : (hi < nu ? hi : nu);
+}
+// RadiationOpacityModel::findGroup (radiation/RadiationOpacityModel.hpp:76-86):
+// the first g with nu < b_{g+1}, else the last group
+__device__ __forceinline__ uint32_t mg_find_group(const Ctx &C, double nu) {
+    uint32_t lo = 0, hi = C.groups - 1;   // answer in [lo, hi]
+    while (lo < hi) {
+        const uint32_t mid = (lo + hi) >> 1;
+        if (nu < C.gb[mid + 1]) hi = mid; else lo = mid + 1;
+    }
+    return lo;
+}
+// kT of the opacity model: k_B max(T, 1 K)
+__device__ __forceinline__ double mg_kT(const Ctx &C, uint32_t c) {
+    const double T = C.T[c];
+    return C.kBoltz * (T < 1.0 ? 1.0 : T);
+}
+// sigma0 / ((kT)^q E^p) (1 - e^{-E/kT})^s
+__device__ __forceinline__ double mg_sigma(const Ctx &C, uint32_t c, double E, double kT) {
+    double v = C.sig0[c] / (pow(kT, C.mgQ) * pow(E, C.mgP));
+    if (C.mgS != 0.0) v *= pow(-expm1(-E / kT), C.mgS);
+    return v;
+}
+// CalcAbsorptionOpacity(cell, frequency)
+__device__ __forceinline__ double mg_absorption(const Ctx &C, uint32_t c, double nu) {
+    const double kT = mg_kT(C, c);
+    double E;
+    if (C.mgGroupConst) {
+        const uint32_t g = mg_find_group(C, nu);
+        E = 0.5 * (C.gb[g] + C.gb[g + 1]);
+    } else {
+        E = nu < C.gb[0] ? C.gb[0] : nu;
+    }
+    return mg_sigma(C, c, E, kT);
+}
+// GetThermalEnergy (examples/densmore2012/DensmoreOpacity.hpp:71-82): the
+// inverse of the cell's cumulative sigma_g B_g by STORM::LinearInterpolation
+// (utils/LinearInterpolation.hpp:18-42); the base class's uniform draw when the
+// spectrum is empty.  Returns a negative energy where LinearInterpolation
+// throws (x beyond the table).
+__device__ inline double mg_thermal_energy(const Ctx &C, uint32_t c, double random) {
+    const uint32_t G = C.groups;
+    const double *x = C.mgCdf + static_cast<size_t>(c) * (G + 1);
+    const double *y = C.gb;
+    const double total = x[G];
+    if (!(total > 0.0) || !isfinite(total)) return y[0] + random * (y[G] - y[0]);
+    const double r = isfinite(random) ? (random < 0.0 ? 0.0 : (ONE_BELOW < random ? ONE_BELOW : random)) : 0.5;
+    const double xi = r * total;
+    // std::upper_bound: the first x > xi
+    uint32_t first = 0, count = G + 1;
+    while (count > 0) {
+        const uint32_t step = count >> 1, it = first + step;
+        if (!(xi < x[it])) { first = it + 1; count -= step + 1; } else count = step;
+    }
+    if (first == G + 1) return fabs(x[G] - xi) < 1e-12 ? y[G] : -1.0;
+    if (fabs(x[first] - xi) < 1e-12 || first == 0) return y[first];
+    return y[first] + (xi - x[first]) * (y[first - 1] - y[first]) / (x[first - 1] - x[first]);
+}
+
 // ------------------------------------------------------------------ Random Walk jump
 // RadiationIMC::tryRandomWalkStep (radiation/RadiationIMC.hpp:1065-1276), gray.
 // Returns -1 when the walk is not taken (no draws consumed), else a ParticleStatus.
@@ -335,22 +448,39 @@ __device__ inline int try_random_walk(const Ctx &C, PartReg &p, RNG &rng, TALLY 
     for (int s = 0; s < 6; ++s) Ro = (d[s] < Ro) ? d[s] : Ro;
     Ro = (Ro > 0.0) ? Ro : 0.0;
     const double c = C.clight;
-    double sigmaT = C.rwSigT[cell];
-    double Dphys = cp.w;
+    const bool pgrw = C.groups >= 2;
+    double sigmaT, sigmaAeff, Dphys, gammaRw = 1.0;
+    uint32_t cutoff = 0;
+    if (pgrw) {   // PGRW cell data (:1080-1087)
+        const double4 g4 = C.pgrw[cell];
+        sigmaT = g4.x; sigmaAeff = g4.y; Dphys = g4.z; gammaRw = g4.w;
+        cutoff = C.pgrwCut[cell];
+    } else {
+        sigmaT = C.rwSigT[cell];
+        sigmaAeff = C.sigA[cell];
+        Dphys = cp.w;
+    }
     bool doRW = (Ro > 0.0 && sigmaT > 0.0 && Dphys > 0.0 && Ro * sigmaT >= C.rwMinParticle);
+    if (doRW && pgrw && mg_clamp(C, p.nu) >= C.gb[cutoff]) doRW = false;   // (:1098-1115)
     if (!doRW) return -1;
+    const double fl = pgrw ? C.fleck[cell] : 0.0;
     double tauLeak = rw_sample_leak(C.rw, rng.open());
     double tLeak = tauLeak * Ro * Ro / Dphys;
     double tCensus = p.t;
+    double tUp = DBL_MAX;   // upscatter out of the diffusive groups (:1130-1135)
+    if (pgrw && gammaRw < 1.0 && sigmaAeff > 0.0 && fl > 0.0) {
+        double xiUp = rng.open();
+        tUp = -log(xiUp) / (c * (1.0 - fl) * sigmaAeff * (1.0 - gammaRw));
+    }
     int ev;
     double dt;
-    if (tLeak <= tCensus && tLeak <= DBL_MAX) { ev = 0; dt = tLeak; }
-    else if (tCensus <= DBL_MAX) { ev = 1; dt = tCensus; }
-    else { ev = 2; dt = DBL_MAX; }
-    const double rate = cp.y;   // sigma_a * f * c
+    if (tLeak <= tCensus && tLeak <= tUp) { ev = 0; dt = tLeak; }
+    else if (tCensus <= tUp) { ev = 1; dt = tCensus; }
+    else { ev = 2; dt = tUp; }
+    const double rate = pgrw ? sigmaAeff * fl * c : cp.y;   // sigma_a_eff * f * c
     double rwExp = expm1(-dt * rate);
     if (!C.noFeedback) tal.mat(cell, -rwExp * p.w);
-    if (rate > 0.0) tal.rad(cell, p.w * rwExp * cp.z);
+    if (rate > 0.0) tal.rad(cell, p.w * rwExp * (pgrw ? (-1.0 / rate) : cp.z));
     p.w *= 1.0 + rwExp;
     p.t -= dt;
     if (fabs(p.w) < p.w0 * 1e-4) {
@@ -399,6 +529,18 @@ __device__ inline int try_random_walk(const Ctx &C, PartReg &p, RNG &rng, TALLY 
     }
     p.x = lx; p.y = ly; p.z = lz;
     isotropic(rng, c, p.vx, p.vy, p.vz);
+    if (ev == 2) {   // upscatter: a frequency above the cutoff from the emission spectrum (:1232-1250)
+        const double *cdf = C.mgCdf + static_cast<size_t>(cell) * (C.groups + 1);
+        const double cdfAtCutoff = cdf[cutoff], cdfTotal = cdf[C.groups];
+        if (cdfTotal > cdfAtCutoff) {
+            double lo = cdfAtCutoff / cdfTotal;
+            double xi = rng.open();
+            p.nu = mg_thermal_energy(C, cell, lo + xi * (1.0 - lo));
+        } else {
+            p.nu = nextafter(C.gb[cutoff], DBL_MAX);
+        }
+        p.nu = mg_clamp(C, p.nu);
+    }
     return (ev == 1) ? DONE : NO_CELL_MOVE;
 }
 
@@ -503,7 +645,19 @@ __device__ inline PhysOut physics_step(const Ctx &C, Track &T, RNG &rng, TALLY &
     case 4: next = (k > 0) ? cell - C.nx * C.ny : OUTSIDE; break;
     default: next = (k + 1 < C.nz) ? cell + C.nx * C.ny : OUTSIDE; break;
     }
-    const double4 cp = C.phys[cell];
+    double4 cp = C.phys[cell];
+    double elastic = 0.0, eventOpacity = 0.0;
+    if (C.groups >= 2) {
+        // CalcAbsorptionOpacity at the particle's frequency (:1742-1754)
+        const double f = C.fleck[cell];
+        const double absorptionOpacity = mg_absorption(C, cell, mg_clamp(C, p.nu));
+        elastic = C.sigS[cell];
+        const double effectiveAbsorptionOpacity = (1.0 - f) * absorptionOpacity;
+        eventOpacity = elastic + effectiveAbsorptionOpacity;
+        cp.x = (eventOpacity > 0.0) ? 1.0 / eventOpacity : CUDART_INF;
+        cp.y = absorptionOpacity * f * C.clight;
+        cp.z = -1.0 / cp.y;
+    }
 
     if (C.withRW && C.rwElig[cell]) {
         int r = try_random_walk(C, p, rng, tal, cp, xl, xh, yl, yh, zl, zh, C.xc[i], C.yc[j], C.zc[k]);
@@ -548,8 +702,21 @@ __device__ inline PhysOut physics_step(const Ctx &C, Track &T, RNG &rng, TALLY &
         o.next = next;
         if (next == OUTSIDE) o.ghost = C.ncells + face_index(C, i, j, k, face);
     } else if (best == 1) {
-        rng.skip();   // event-type draw; both branches re-scatter isotropically
-        isotropic(rng, c, p.vx, p.vy, p.vz);
+        if (C.groups >= 2) {
+            // elastic or effective scatter (:1826-1852): both re-scatter
+            // isotropically; an effective scatter re-emits from the spectrum
+            const double eventRandom = rng.open() * eventOpacity;
+            const bool effective = !(eventRandom < elastic);
+            isotropic(rng, c, p.vx, p.vy, p.vz);
+            p.nu = mg_clamp(C, p.nu);
+            if (effective) {
+                p.nu = mg_thermal_energy(C, cell, rng.open());
+                if (p.nu < 0.0) { o.errCode = STORM_DERR_MG_SAMPLE; return o; }
+            }
+        } else {
+            rng.skip();   // event-type draw; both branches re-scatter isotropically
+            isotropic(rng, c, p.vx, p.vy, p.vz);
+        }
         T.speed = vnorm(p.vx, p.vy, p.vz);
         o.status = NO_CELL_MOVE;
     } else {

@@ -14,6 +14,7 @@ namespace storm {
 struct Bank {
     double *x, *y, *z, *vx, *vy, *vz, *t, *w, *w0;
     uint32_t *cell, *pid, *draw;
+    double *nu;          // photon energy, multigroup problems only (NULL otherwise)
 };
 
 // Census bank: one record of 16-byte vectors per particle (96 B in the FP64
@@ -30,10 +31,15 @@ struct CellArrays {
     uint64_t *photons;
     double4 *phys;      // per-cell segment constants (cell_phys)
     float4 *phys32;     // FP32-tracking form: 1/sigma_e, sigma_a f
+    // multigroup
+    double *mgCdf;      // per cell, groups + 1
+    double4 *pgrw;      // per cell: sigmaT_bar, sigmaA_bar, D, gamma
+    uint32_t *pgrwCut;  // per cell group cutoff
 };
 
 struct OpacityEos {
     int32_t opacityKind, eosKind;
+    // multigroup: tabA holds sigma0 per cell, tabS the elastic opacity
     const double *tabA, *tabS, *rhoF;
     double kP0, kR0, alpha, tFloor, cap;
     double cvPerMass, eosF, eosBeta, eosMu;
@@ -59,6 +65,8 @@ struct DevStats {
 
 struct ReplayDev {
     const double *in[9];
+    const double *freq;     // multigroup: frequency before (NULL = 0)
+    double *freqOut;        // multigroup: frequency after (NULL = not returned)
     const uint32_t *cell;
     const uint64_t *tapeOffset;
     const uint32_t *tapeLength;

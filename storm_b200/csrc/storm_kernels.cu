@@ -29,12 +29,14 @@ __device__ __forceinline__ void load_part(const Bank &b, uint32_t q, PartReg &p)
     p.vx = b.vx[q]; p.vy = b.vy[q]; p.vz = b.vz[q];
     p.t = b.t[q]; p.w = b.w[q]; p.w0 = b.w0[q];
     p.cell = b.cell[q];
+    p.nu = b.nu ? b.nu[q] : 0.0;
 }
 __device__ __forceinline__ void store_part(const Bank &b, uint32_t q, const PartReg &p, uint32_t pid, uint32_t draw) {
     b.x[q] = p.x; b.y[q] = p.y; b.z[q] = p.z;
     b.vx[q] = p.vx; b.vy[q] = p.vy; b.vz[q] = p.vz;
     b.t[q] = p.t; b.w[q] = p.w; b.w0[q] = p.w0;
     b.cell[q] = p.cell; b.pid[q] = pid; b.draw[q] = draw;
+    if (b.nu) b.nu[q] = p.nu;
 }
 
 // FP32-tracking banks reuse the same buffers: x,y,z hold the cell-local
@@ -108,7 +110,7 @@ __device__ __forceinline__ void copy_any(const Ctx &C, const Bank &src, uint32_t
 }
 
 // ---- census bank: array of records, gathered in random order by the comb.
-// FP64 form, 96 B: (x,y) (z,vx) (vy,vz) (t,w) (w0,[cell,pid]) ([draw,-,-,-])
+// FP64 form, 96 B: (x,y) (z,vx) (vy,vz) (t,w) (w0,[cell,pid]) ([draw,-],nu)
 // FP32 form, 64 B: (qx,qy,qz,ux) (uy,uz,t) (w,w0) (cell,pid,draw,-)
 __device__ __forceinline__ uint4 two_doubles(double a, double b) {
     const unsigned long long x = __double_as_longlong(a), y = __double_as_longlong(b);
@@ -130,7 +132,8 @@ __device__ __forceinline__ void census_store64(const CensusBank &c, uint32_t q, 
     r[3] = two_doubles(p.t, p.w);
     const unsigned long long w0 = __double_as_longlong(p.w0);
     r[4] = make_uint4(static_cast<uint32_t>(w0), static_cast<uint32_t>(w0 >> 32), p.cell, pid);
-    r[5] = make_uint4(draw, 0u, 0u, 0u);
+    const unsigned long long nu = __double_as_longlong(p.nu);
+    r[5] = make_uint4(draw, 0u, static_cast<uint32_t>(nu), static_cast<uint32_t>(nu >> 32));
 }
 __device__ __forceinline__ void census_load64(const CensusBank &c, uint32_t q, PartReg &p, uint32_t &pid,
                                               uint32_t &draw) {
@@ -142,6 +145,7 @@ __device__ __forceinline__ void census_load64(const CensusBank &c, uint32_t q, P
     p.t = lo_double(e); p.w = hi_double(e);
     p.w0 = lo_double(f);
     p.cell = f.z; pid = f.w; draw = g.x;
+    p.nu = hi_double(g);
 }
 __device__ __forceinline__ void census_store32(const CensusBank &c, uint32_t q, const Track32 &T, uint32_t pid,
                                                uint32_t draw) {
@@ -222,6 +226,17 @@ __global__ void k_begin(Bank b, uint32_t n, double dt, DevStats *st) {
     if ((threadIdx.x & 31) == 0 && e != 0.0) atomicAdd(&st->eCensusIn, e);
 }
 
+// mean chord 4V/S of a cell (computeCellSurfaceArea, radiation/RadiationIMC.hpp:971-980, GetCellFaces order)
+__device__ __forceinline__ double cell_chord(const Ctx &C, const CellArrays &A, uint32_t c) {
+    uint32_t i, j, k;
+    cell_ijk(C, c, i, j, k);
+    double dx = C.xe[i + 1] - C.xe[i], dy = C.ye[j + 1] - C.ye[j], dz = C.ze[k + 1] - C.ze[k];
+    double ax = dy * dz, ay = dz * dx, az = dx * dy;
+    double S = 0.0;
+    S += ax; S += ax; S += ay; S += ay; S += az; S += az;
+    return (S > 0.0) ? 4.0 * A.vol[c] / S : 0.0;
+}
+
 // Random Walk eligibility of a cell (precomputeRandomWalkData, radiation/RadiationIMC.hpp:982-1063,
 // with computeCellSurfaceArea :971-980 in GetCellFaces order) and the FP32
 // form's segment constants: x = 1/sigma_e (inf when none), y = sigma_a f,
@@ -233,15 +248,13 @@ __device__ __forceinline__ void cell_rw_and_phys32(const Ctx &C, const CellArray
     const double sigmaT = sa + ss;
     bool elig = false;
     if (C.withRW) {
-        A.rwSigT[c] = sigmaT;
-        uint32_t i, j, k;
-        cell_ijk(C, c, i, j, k);
-        double dx = C.xe[i + 1] - C.xe[i], dy = C.ye[j + 1] - C.ye[j], dz = C.ze[k + 1] - C.ze[k];
-        double ax = dy * dz, ay = dz * dx, az = dx * dy;
-        double S = 0.0;
-        S += ax; S += ax; S += ay; S += ay; S += az; S += az;
-        double chord = (S > 0.0) ? 4.0 * A.vol[c] / S : 0.0;
-        elig = sigmaT * chord >= C.rwMinCell;
+        if (C.groups >= 2) {   // PGRW: eligible where some groups are diffusive (tables from prestep)
+            elig = A.pgrwCut[c] > 0;
+            A.rwSigT[c] = elig ? A.pgrw[c].x : sigmaT;
+        } else {
+            A.rwSigT[c] = sigmaT;
+            elig = sigmaT * cell_chord(C, A, c) >= C.rwMinCell;
+        }
         A.rwElig[c] = elig ? 1 : 0;
     }
     if (C.fp32) {
@@ -259,11 +272,77 @@ __device__ __forceinline__ void cell_rw_and_phys32(const Ctx &C, const CellArray
 // RadiationIMC::preStep (radiation/RadiationIMC.hpp:1618-1661) per cell, the opacity
 // plug-in (CalcPlanckOpacity / CalcScatteringOpacity) and precomputeRandomWalkData
 // (:982-1006, gray branch); clears Erad_time_avg_.
+// Multigroup per-cell tables: the Planck mean opacity of the opacity plug-in
+// (examples/densmore2012/DensmoreOpacity.hpp:36-56), the cumulative emission
+// spectrum sum_g sigma_g B_g it samples from (:146-165), and the PGRW data of
+// precomputeRandomWalkData (radiation/RadiationIMC.hpp:1008-1061).  Every
+// group weight is evaluated at the group centre with planck_integral.
+__device__ inline double mg_cell_tables(const Ctx &C, const CellArrays &A, uint32_t c, double scat, double chord) {
+    const uint32_t G = C.groups;
+    const double T = C.T[c];
+    const double kT = C.kBoltz * (T < 1.0 ? 1.0 : T);   // the opacity model's kT
+    const double kTrw = C.kBoltz * T;                    // precomputeRandomWalkData's kT
+    double *cdf = A.mgCdf + static_cast<size_t>(c) * (G + 1);
+    double weightedSum = 0.0, totalWeight = 0.0, cum = 0.0;
+    double totalSigABgAll = 0.0, totalBgDiff = 0.0, sumBgSigADiff = 0.0, sumBgSigTDiff = 0.0, sumBgOverSigTDiff = 0.0;
+    uint32_t cutoff = 0;
+    bool foundNonDiffusive = false;
+    cdf[0] = 0.0;
+    for (uint32_t g = 0; g < G; ++g) {
+        const double b0 = C.gb[g], b1 = C.gb[g + 1];
+        const double Ec = 0.5 * (b0 + b1);
+        const double a = b0 / kT, b = b1 / kT;
+        const double Bg = (a > 0.0 && b > a) ? planck_integral(a, b) : 0.0;
+        const double sg = mg_sigma(C, c, Ec, kT);   // = CalcAbsorptionOpacity(cell, centre of g)
+        weightedSum += sg * Bg;
+        totalWeight += Bg;
+        const double weight = (sg > 0.0 && isfinite(sg) && isfinite(Bg)) ? sg * Bg : 0.0;
+        cum = cum + weight;
+        cdf[g + 1] = cum;
+        if (C.withRW) {
+            double Bgr;
+            if (kTrw == kT) {
+                Bgr = (a > 0.0 && b > a) ? Bg : 1.0 / static_cast<double>(G);
+            } else {
+                const double ar = b0 / kTrw, br = b1 / kTrw;
+                Bgr = (ar > 0.0 && br > ar) ? planck_integral(ar, br) : 1.0 / static_cast<double>(G);
+            }
+            const double sigT = sg + scat;
+            totalSigABgAll += sg * Bgr;
+            if (!foundNonDiffusive && sigT * chord >= C.rwMinCell) {
+                cutoff = g + 1;
+                totalBgDiff += Bgr;
+                sumBgSigADiff += Bgr * sg;
+                sumBgSigTDiff += Bgr * sigT;
+                if (sigT > 0.0) sumBgOverSigTDiff += Bgr / sigT;
+            } else {
+                foundNonDiffusive = true;
+            }
+        }
+    }
+    const double sigmaP = (totalWeight > 0.0) ? weightedSum / totalWeight : 1e-20;
+    if (C.withRW) {
+        if (cutoff > 0 && totalBgDiff > 0.0) {
+            A.pgrwCut[c] = cutoff;
+            A.pgrw[c] = make_double4(sumBgSigTDiff / totalBgDiff, sumBgSigADiff / totalBgDiff,
+                                     (C.clight / 3.0) * sumBgOverSigTDiff / totalBgDiff,
+                                     (totalSigABgAll > 0.0) ? sumBgSigADiff / totalSigABgAll : 1.0);
+        } else {
+            A.pgrwCut[c] = 0;
+            A.pgrw[c] = make_double4(0.0, 0.0, 0.0, 0.0);
+        }
+    }
+    return sigmaP;
+}
+
 __global__ void k_prestep(Ctx C, CellArrays A, OpacityEos M, double dt) {
     for (uint32_t c = blockIdx.x * blockDim.x + threadIdx.x; c < C.ncells; c += gridDim.x * blockDim.x) {
         double sa, ss;
         const double T = A.T[c];
-        if (M.opacityKind == STORM_OPACITY_CELL_TABLE) {
+        if (C.groups >= 2) {
+            ss = M.tabS ? M.tabS[c] : 0.0;
+            sa = mg_cell_tables(C, A, c, ss, C.withRW ? cell_chord(C, A, c) : 0.0);
+        } else if (M.opacityKind == STORM_OPACITY_CELL_TABLE) {
             sa = M.tabA[c];
             ss = M.tabS ? M.tabS[c] : 0.0;
         } else {
@@ -593,6 +672,11 @@ __global__ void k_emit_cells(Ctx C, CellArrays A, const uint64_t *offsets, uint6
         repair_outside(C, p.x, p.y, p.z, C.xc[i], C.yc[j], C.zc[k]);
         isotropic(rng, C.clight, p.vx, p.vy, p.vz);
         p.t = dt * rng.open();
+        p.nu = 0.0;
+        if (C.groups >= 2) {   // GetThermalEnergy (radiation/RadiationIMC.hpp:2495-2500)
+            p.nu = mg_thermal_energy(C, c, rng.open());
+            if (p.nu < 0.0) raise_error(C, STORM_DERR_MG_SAMPLE, c, static_cast<uint32_t>(e));
+        }
         p.w = energyPerPhoton;
         p.w0 = fabs(p.w);
         store_any(C, b, bankBase + static_cast<uint32_t>(e), p, bankBase + static_cast<uint32_t>(e), 0);
@@ -711,6 +795,7 @@ __global__ void k_emit_faces(Ctx C, FaceSources F, uint64_t total, Bank b, uint3
         v[(axis + 2) % 3] = one_m * stt;
         p.vx = v[0] * C.clight; p.vy = v[1] * C.clight; p.vz = v[2] * C.clight;
         p.w = energy;
+        p.nu = 0.0;   // the harness boundary plug-in leaves frequency 0 (clamped to the lowest bound where used)
         p.t = dt * rng.raw();
         p.cell = c;
         repair_outside(C, p.x, p.y, p.z, C.xc[i], C.yc[j], C.zc[k]);
@@ -1381,13 +1466,14 @@ __global__ void k_comb_emit(Ctx C, CensusBank cen, const uint32_t *idx, const ui
                 for (uint32_t k = 0; k < m; ++k)
                     store32(out, static_cast<uint32_t>(o + k), T, static_cast<uint32_t>(o + k), 0);
             } else {
-                const uint4 a = rec[u][0], b = rec[u][1], d = rec[u][2], e = rec[u][3], f = rec[u][words - 2];
+                const uint4 a = rec[u][0], b = rec[u][1], d = rec[u][2], e = rec[u][3], f = rec[u][4];
                 PartReg p;
                 p.x = lo_double(a); p.y = hi_double(a);
                 p.z = lo_double(b); p.vx = hi_double(b);
                 p.vy = lo_double(d); p.vz = hi_double(d);
                 p.t = lo_double(e); p.w = hi_double(e);
                 p.w0 = lo_double(f);
+                p.nu = hi_double(rec[u][5]);
                 comb_emit_fp64(C, p, c, raw[u], wNew, o, out);
             }
         }
@@ -1476,6 +1562,7 @@ __global__ void k_replay(Ctx C, ReplayDev R, uint32_t n) {
         p.vx = R.in[3][q]; p.vy = R.in[4][q]; p.vz = R.in[5][q];
         p.t = R.in[6][q]; p.w = R.in[7][q]; p.w0 = R.in[8][q];
         p.cell = R.cell[q];
+        p.nu = R.freq ? R.freq[q] : 0.0;
         track_begin(C, T);
         TapeRng rng{R.tape + R.tapeOffset[q], R.tapeLength[q], 0, false};
         LocalTally tal{0.0, 0.0};
@@ -1483,6 +1570,7 @@ __global__ void k_replay(Ctx C, ReplayDev R, uint32_t n) {
         R.phys[0][q] = p.x; R.phys[1][q] = p.y; R.phys[2][q] = p.z;
         R.phys[3][q] = p.vx; R.phys[4][q] = p.vy; R.phys[5][q] = p.vz;
         R.phys[6][q] = p.t; R.phys[7][q] = p.w;
+        if (R.freqOut) R.freqOut[q] = p.nu;
         R.physStatus[q] = o.errCode ? -1 : o.status;
         R.physNext[q] = (o.status == CELL_MOVE && !o.errCode) ? (o.next != OUTSIDE ? o.next : o.ghost) : OUTSIDE;
         R.dep[0][q] = tal.mat_;

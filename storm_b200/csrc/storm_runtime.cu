@@ -53,6 +53,7 @@ struct StormHandle {
     // random walk tables
     double *rwTau = nullptr, *rwLogTau = nullptr, *rwSurv = nullptr, *rwRadius = nullptr;
     float *rwLogTau32 = nullptr, *rwSurv32 = nullptr, *rwRadius32 = nullptr;   // FP32-tracking form
+    double *gb = nullptr;            // multigroup bounds
     // face sources
     uint32_t *fsCell = nullptr;
     int32_t *fsSide = nullptr;
@@ -232,6 +233,10 @@ cudaError_t bank_alloc(StormHandle *h, Bank &b, size_t n) {
         cudaError_t e = dalloc(h, q, n);
         if (e != cudaSuccess) return e;
     }
+    if (h->desc.groups >= 2) {
+        cudaError_t e = dalloc(h, &b.nu, n);
+        if (e != cudaSuccess) return e;
+    }
     uint32_t **u[] = {&b.cell, &b.pid, &b.draw};
     for (uint32_t **q : u) {
         cudaError_t e = dalloc(h, q, n);
@@ -240,7 +245,7 @@ cudaError_t bank_alloc(StormHandle *h, Bank &b, size_t n) {
     return cudaSuccess;
 }
 void bank_free(StormHandle *h, Bank &b, size_t n) {
-    double **d[] = {&b.x, &b.y, &b.z, &b.vx, &b.vy, &b.vz, &b.t, &b.w, &b.w0};
+    double **d[] = {&b.x, &b.y, &b.z, &b.vx, &b.vy, &b.vz, &b.t, &b.w, &b.w0, &b.nu};
     for (double **q : d) dfree(h, *q, n);
     uint32_t **u[] = {&b.cell, &b.pid, &b.draw};
     for (uint32_t **q : u) dfree(h, *q, n);
@@ -257,6 +262,10 @@ cudaError_t bank_copy(cudaStream_t s, const Bank &dst, const Bank &src, size_t n
     uint32_t *du[] = {dst.cell, dst.pid, dst.draw};
     for (int q = 0; q < 3; ++q) {
         cudaError_t e = cudaMemcpyAsync(du[q], su[q], n * sizeof(uint32_t), cudaMemcpyDeviceToDevice, s);
+        if (e != cudaSuccess) return e;
+    }
+    if (src.nu && dst.nu) {
+        cudaError_t e = cudaMemcpyAsync(dst.nu, src.nu, n * sizeof(double), cudaMemcpyDeviceToDevice, s);
         if (e != cudaSuccess) return e;
     }
     return cudaSuccess;
@@ -551,9 +560,19 @@ int storm_cuda_create(const StormProblemDesc *d, StormHandle **out) {
     if (d->nx == 0 || d->ny == 0 || d->nz == 0 || !d->x_edges || !d->y_edges || !d->z_edges) return STORM_ERR_INVALID_ARG;
     if (!d->temperature || !d->mass || !d->internal_energy) return STORM_ERR_INVALID_ARG;
     if (d->new_photons_per_cell == 0) return STORM_ERR_INVALID_ARG;   // RadiationIMC.hpp:584-588
-    if (d->opacity_kind == STORM_OPACITY_CELL_TABLE && !d->sigma_a) return STORM_ERR_INVALID_ARG;
-    if (d->opacity_kind != STORM_OPACITY_CELL_TABLE && d->opacity_kind != STORM_OPACITY_POWER_LAW)
+    if ((d->opacity_kind == STORM_OPACITY_CELL_TABLE || d->opacity_kind == STORM_OPACITY_MG_POWER) && !d->sigma_a)
+        return STORM_ERR_INVALID_ARG;
+    if (d->opacity_kind != STORM_OPACITY_CELL_TABLE && d->opacity_kind != STORM_OPACITY_POWER_LAW &&
+        d->opacity_kind != STORM_OPACITY_MG_POWER)
         return STORM_ERR_UNSUPPORTED;
+    const bool mg = d->groups >= 2;
+    if (mg != (d->opacity_kind == STORM_OPACITY_MG_POWER)) return STORM_ERR_INVALID_ARG;
+    if (mg) {   // energyBoundaries must increase (radiation/RadiationIMC.hpp:667-676)
+        if (!d->group_bounds || !(d->k_boltz > 0.0) || d->groups > 4096) return STORM_ERR_INVALID_ARG;
+        for (uint32_t g = 0; g < d->groups; ++g)
+            if (!(d->group_bounds[g + 1] > d->group_bounds[g])) return STORM_ERR_INVALID_ARG;
+        if (d->precision != STORM_PRECISION_FP64) return STORM_ERR_UNSUPPORTED;
+    }
     if (d->eos_kind != STORM_EOS_LINEAR && d->eos_kind != STORM_EOS_POWER_LAW) return STORM_ERR_UNSUPPORTED;
     if (d->precision != STORM_PRECISION_FP64 && d->precision != STORM_PRECISION_FP32_TRACK) return STORM_ERR_UNSUPPORTED;
     uint64_t N64 = static_cast<uint64_t>(d->nx) * d->ny * d->nz;
@@ -645,7 +664,7 @@ int storm_cuda_create(const StormProblemDesc *d, StormHandle **out) {
     OpacityEos &M = h->M;
     M.opacityKind = d->opacity_kind;
     M.eosKind = d->eos_kind;
-    if (d->opacity_kind == STORM_OPACITY_CELL_TABLE) {
+    if (d->opacity_kind == STORM_OPACITY_CELL_TABLE || d->opacity_kind == STORM_OPACITY_MG_POWER) {
         ALLOC(h->tabA, N);
         H2D(h->tabA, d->sigma_a, N);
         if (d->sigma_s) {
@@ -691,6 +710,23 @@ int storm_cuda_create(const StormProblemDesc *d, StormHandle **out) {
     C.Y0 = h->hye.front(); C.Y1 = h->hye.back();
     C.Z0 = h->hze.front(); C.Z1 = h->hze.back();
     box_faces(h);
+    if (mg) {
+        const uint32_t G = d->groups;
+        ALLOC(h->gb, G + 1);
+        H2D(h->gb, d->group_bounds, G + 1);
+        ALLOC(A.mgCdf, static_cast<size_t>(N) * (G + 1));
+        ALLOC(A.pgrw, N);
+        ALLOC(A.pgrwCut, N);
+        if (cudaMemset(A.pgrwCut, 0, N * sizeof(uint32_t)) != cudaSuccess) return fail(STORM_ERR_CUDA);
+        C.groups = G;
+        C.mgGroupConst = d->mg_group_constant;
+        C.gb = h->gb;
+        C.mgP = d->mg_p; C.mgQ = d->mg_q; C.mgS = d->mg_s;
+        C.kBoltz = d->k_boltz;
+        C.sig0 = h->tabA;
+        C.mgCdf = A.mgCdf; C.pgrw = A.pgrw; C.pgrwCut = A.pgrwCut;
+    }
+    C.T = A.T;
     C.escapeNoCheck = d->escape_without_check;
     C.withRW = d->with_random_walk;
     C.noFeedback = d->no_hydro_feedback;
@@ -737,7 +773,8 @@ int storm_cuda_destroy(StormHandle *h) {
                   h->A.sigA, h->A.sigS, h->A.fleck, h->A.rwSigT, h->A.eradAvg, h->A.eradCensus, h->A.emitE,
                   h->A.rwElig, h->A.photons, h->A.phys, h->A.phys32, h->hx, h->hy, h->hz, h->segs, h->tabA, h->tabS, h->rhoF, h->rwTau, h->rwLogTau, h->rwSurv,
                   h->rwRadius, h->rwLogTau32, h->rwSurv32, h->rwRadius32, h->fsCell, h->fsSide, h->fsOffset, h->dAmbiguous, h->offsets, h->tileSums, h->dTotalU64, h->dTotalE, h->combW, h->combWtot,
-                  h->combStart, h->combCount, h->counts, h->dStats, h->dErr};
+                  h->combStart, h->combCount, h->counts, h->dStats, h->dErr, h->gb, h->A.mgCdf, h->A.pgrw,
+                  h->A.pgrwCut};
     for (void *p : ps) device_pool().free(p);
     cudaEvent_t evs[] = {h->evStart, h->evTransport0, h->evTransport1, h->evEnd, h->evAfterEmit, h->evAfterComb};
     for (cudaEvent_t e : evs)
@@ -1129,6 +1166,10 @@ int storm_cuda_set_census(StormHandle *h, const StormParticlesSoA *in) {
         for (int q = 0; q < 9; ++q)
             CK(cudaMemcpyAsync(dd[q], sd[q], n * sizeof(double), cudaMemcpyHostToDevice, h->stream));
         CK(cudaMemcpyAsync(stage.cell, in->cell, n * sizeof(uint32_t), cudaMemcpyHostToDevice, h->stream));
+        if (stage.nu) {
+            if (in->frequency) CK(cudaMemcpyAsync(stage.nu, in->frequency, n * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+            else CK(cudaMemsetAsync(stage.nu, 0, n * sizeof(double), h->stream));
+        }
         // cell indices are checked on the device (a host loop would cost as much as the copy)
         int32_t bad = 0;
         CK(cudaMemsetAsync(h->dAmbiguous + 1, 0, sizeof(int32_t), h->stream));
@@ -1169,6 +1210,10 @@ int storm_cuda_population_control(StormHandle *h, const StormParticlesSoA *in) {
         for (uint64_t q = 0; q < n; ++q) pid[q] = static_cast<uint32_t>(q);
         CK(cudaMemcpyAsync(stage.cell, in->cell, n * sizeof(uint32_t), cudaMemcpyHostToDevice, h->stream));
         CK(cudaMemcpyAsync(stage.pid, pid.data(), n * sizeof(uint32_t), cudaMemcpyHostToDevice, h->stream));
+        if (stage.nu) {
+            if (in->frequency) CK(cudaMemcpyAsync(stage.nu, in->frequency, n * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+            else CK(cudaMemsetAsync(stage.nu, 0, n * sizeof(double), h->stream));
+        }
         CK(cudaMemsetAsync(stage.draw, 0, n * sizeof(uint32_t), h->stream));
         launch_bank_to_census(h->stream, h->C, h->bankB, h->bankC, static_cast<uint32_t>(n));
         ++h->launches;
@@ -1205,6 +1250,10 @@ int storm_cuda_get_census(StormHandle *h, StormParticlesSoA *out, uint64_t capac
     for (int q = 0; q < 9; ++q)
         if (dd[q] && n) CK(cudaMemcpyAsync(dd[q], sd[q], n * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
     if (out->cell && n) CK(cudaMemcpyAsync(out->cell, src.cell, n * sizeof(uint32_t), cudaMemcpyDeviceToHost, h->stream));
+    if (out->frequency && n) {
+        if (src.nu) CK(cudaMemcpyAsync(out->frequency, src.nu, n * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+        else std::memset(out->frequency, 0, n * sizeof(double));
+    }
     CK(cudaStreamSynchronize(h->stream));
     if (out->id)
         for (uint64_t q = 0; q < n; ++q) out->id[q] = q;
@@ -1233,6 +1282,10 @@ int storm_cuda_get_bank(StormHandle *h, StormParticlesSoA *out, uint64_t capacit
     for (int q = 0; q < 9; ++q)
         if (dd[q] && n) CK(cudaMemcpyAsync(dd[q], sd[q], n * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
     if (out->cell && n) CK(cudaMemcpyAsync(out->cell, src.cell, n * sizeof(uint32_t), cudaMemcpyDeviceToHost, h->stream));
+    if (out->frequency && n) {
+        if (src.nu) CK(cudaMemcpyAsync(out->frequency, src.nu, n * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+        else std::memset(out->frequency, 0, n * sizeof(double));
+    }
     std::vector<uint32_t> pid;
     if (out->id && n) {
         pid.resize(n);
@@ -1331,6 +1384,8 @@ int storm_cuda_replay_segments(StormHandle *h, StormReplayBatch *b) {
     ReplayDev R{};
     const double *ins[9] = {b->x, b->y, b->z, b->vx, b->vy, b->vz, b->time_left, b->weight, b->initial_weight};
     for (int q = 0; q < 9; ++q) R.in[q] = static_cast<const double *>(up(ins[q], n * sizeof(double)));
+    R.freq = b->frequency ? static_cast<const double *>(up(b->frequency, n * sizeof(double))) : nullptr;
+    R.freqOut = b->phys_frequency ? static_cast<double *>(up(nullptr, n * sizeof(double))) : nullptr;
     R.cell = static_cast<const uint32_t *>(up(b->cell, n * sizeof(uint32_t)));
     R.tapeOffset = static_cast<const uint64_t *>(up(b->tape_offset, n * sizeof(uint64_t)));
     R.tapeLength = static_cast<const uint32_t *>(up(b->tape_length, n * sizeof(uint32_t)));
@@ -1368,6 +1423,7 @@ int storm_cuda_replay_segments(StormHandle *h, StormReplayBatch *b) {
         cudaMemcpy(b->mgr_status, R.mgrStatus, n * sizeof(int32_t), cudaMemcpyDeviceToHost);
         cudaMemcpy(b->draws_used, R.draws, n * sizeof(uint32_t), cudaMemcpyDeviceToHost);
         cudaMemcpy(b->used_random_walk, R.usedRW, n * sizeof(int32_t), cudaMemcpyDeviceToHost);
+        if (b->phys_frequency) cudaMemcpy(b->phys_frequency, R.freqOut, n * sizeof(double), cudaMemcpyDeviceToHost);
     }
     for (void *p : owned)
         if (p) cudaFree(p);

@@ -83,6 +83,7 @@ class Particles:
         self.cell = np.zeros(n, np.uint32)
         self.id = np.zeros(n, np.uint64)
         self.n = n
+        self.frequency = np.zeros(n)   # photon energy (multigroup)
 
     @classmethod
     def pinned(cls, capacity):
@@ -94,6 +95,7 @@ class Particles:
             setattr(p, f, torch.empty(capacity, dtype=torch.float64, pin_memory=True).numpy())
         p.cell = torch.empty(capacity, dtype=torch.int32, pin_memory=True).numpy().view(np.uint32)
         p.id = None
+        p.frequency = None
         p.n = capacity
         return p
 
@@ -106,6 +108,7 @@ class Particles:
             setattr(v, f, getattr(self, f)[:n])
         v.cell = self.cell[:n]
         v.id = None if self.id is None else self.id[:n]
+        v.frequency = None if getattr(self, "frequency", None) is None else self.frequency[:n]
         v.n = n
         return v
 
@@ -122,6 +125,9 @@ class Particles:
         if self.id is not None:
             self.id = np.ascontiguousarray(self.id, dtype=np.uint64)
             s.id = A.ptr(self.id, C.c_uint64)
+        if getattr(self, "frequency", None) is not None:
+            self.frequency = np.ascontiguousarray(self.frequency, dtype=np.float64)
+            s.frequency = A.ptr(self.frequency)
         s.count = self.n
         return s
 

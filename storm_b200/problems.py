@@ -67,6 +67,13 @@ class Problem:
     device: int = 0
     dt: float = 1e-11
     name: str = "problem"
+    # multigroup (groups >= 2): STORM_OPACITY_MG_POWER with sigma_a = sigma0 per cell
+    groups: int = 0
+    group_bounds: np.ndarray = None
+    mg_group_constant: bool = False
+    mg_p: float = 3.0
+    mg_q: float = 0.0
+    mg_s: float = 0.0
 
     @property
     def shape(self):
@@ -145,6 +152,11 @@ class Problem:
         d.max_rounds = self.max_rounds
         d.per_cell_segment_counters = int(self.per_cell_segment_counters)
         d.device = self.device
+        d.groups = self.groups
+        d.mg_group_constant = int(self.mg_group_constant)
+        d.group_bounds = arr(self.group_bounds)
+        d.mg_p, d.mg_q, d.mg_s = self.mg_p, self.mg_q, self.mg_s
+        d.k_boltz = UNITS["k_boltz"]
         d._keep = keep
         return d
 
@@ -256,3 +268,41 @@ def serving_mix(count, n_range=(16, 48), packets_range=(1e4, 1e6), kappa_range=(
         out.append((uniform_cube(n=n, kappa=kappa, packets_per_step=packets, seed=1000 + k, precision=precision),
                     steps))
     return out
+
+
+def mg_cube(n=16, groups=64, kappa0=100.0, new_photons_per_cell=4, comb_nmin=4, seed=42, dt=1e-11,
+            precision=A.PRECISION_FP64, T_range_kev=(0.01, 0.1), with_random_walk=True, face_source=False,
+            group_constant=True):
+    """Multigroup gray-material cube: `groups` log-spaced groups over
+    [0.01, 100] keV, kappa_g = kappa0 nu_g^-3 (1 - exp(-nu_g/T)) (nu_g the group
+    centre in keV), initial T uniform in T_range_kev per cell (seeded), cell
+    emission sampled from the Planck-weighted opacity spectrum; vacuum faces
+    (optionally a 1 keV source on x=0)."""
+    keV = UNITS["kev_kelvin"]
+    kev_erg = UNITS["kev"]
+    empty = np.zeros(1)
+    e = uniform_edges(0.0, 1.0, n)
+    p = Problem(e, e.copy(), e.copy(), empty, empty, empty)
+    rng = np.random.default_rng(seed + 17)
+    T0 = rng.uniform(T_range_kev[0], T_range_kev[1], p.ncells) * keV
+    _material(p, 1.0, CV_PER_VOLUME)
+    p.temperature = T0
+    p.internal_energy = CV_PER_VOLUME * T0 * p.volumes()
+    p.cell_internal_energy = p.internal_energy.copy()
+    p.opacity_kind = A.OPACITY_MG_POWER
+    p.sigma_a = np.full(p.ncells, kappa0 * kev_erg ** 3)     # kappa0 (E/keV)^-3
+    p.sigma_s = np.zeros(p.ncells)
+    p.groups = groups
+    p.group_bounds = np.exp(np.linspace(np.log(0.01), np.log(100.0), groups + 1)) * kev_erg
+    p.mg_group_constant = group_constant
+    p.mg_p, p.mg_q, p.mg_s = 3.0, 0.0, 1.0
+    p.faces = [BoxFace(A.FACE_ESCAPE, 1.0 * keV if face_source else 0.0, 50 if face_source else 0)] + \
+              [BoxFace(A.FACE_ESCAPE) for _ in range(5)]
+    p.new_photons_per_cell = new_photons_per_cell
+    p.with_random_walk = with_random_walk
+    p.rw_min_cell_optical_depth = 20.0 / 3.0
+    p.rw_min_particle_optical_depth = 5.0
+    p.comb_enabled = True
+    p.comb_nmin, p.comb_factor = comb_nmin, 2.0
+    p.seed, p.dt, p.precision, p.name = seed, dt, precision, "mg_cube"
+    return p

@@ -14,6 +14,9 @@ Fixtures (numpy .npz):
                       RandomPointOnFace outputs with the draws each consumed
   allocation_slab.npz photon counts per cell (getLastSourcePhotonsPerCell) and the
                       cell temperatures they were allocated from, several steps
+  replay_mg.npz       recorded calls on a 6^3 multigroup cube (64 groups, PGRW)
+                      with frequencies and the step's starting temperatures
+  replay_mg_thin.npz  the same, optically thinner, opacity continuous in frequency
 """
 import os
 import sys
@@ -27,11 +30,12 @@ from oracle import ref  # noqa: E402
 from storm_b200 import problems  # noqa: E402
 
 
-def record(problem, warm_steps, max_records, take):
+def record(problem, warm_steps, max_records, take, mg=False):
     r = ref.Reference(problem)
     for _ in range(warm_steps):
         r.step()
     c = r.cells()     # tables of the last step; the recorded step recomputes them
+    T_start = c["temperature"]
     r.record_begin(max_records)
     r.step()
     r.record_end()
@@ -44,6 +48,8 @@ def record(problem, warm_steps, max_records, take):
     special = (rec["status"] == 1) & (rec["next"] >= problem.ncells)
     special |= rec["used_rw"] == 1
     special |= rec["status"] == 3
+    if mg:   # every frequency change (effective scatters, PGRW upscatters)
+        special |= rec["freq_before"] != rec["freq_after"]
     sub = idx[(idx % max(1, n // take) == 0) | special]
     if len(sub) > 3 * take:
         sub = sub[np.linspace(0, len(sub) - 1, 3 * take).astype(int)]
@@ -58,10 +64,13 @@ def record(problem, warm_steps, max_records, take):
         if k + 1 < n and rec["id"][k + 1] == rec["id"][k]:
             nxt_before[q] = rec["before"][k + 1][:6]
             nxt_cell[q] = rec["cell"][k + 1]
-    return dict(before=rec["before"][sub], after=rec["after"][sub], status=rec["status"][sub],
-                next=rec["next"][sub].astype(np.int64), tallies=rec["tallies"][sub], cell=rec["cell"][sub],
-                used_rw=rec["used_rw"][sub], tape=tape, tape_offset=new_off, tape_length=tape_len,
-                next_before=nxt_before, next_cell=nxt_cell, sigma_a=c["sigma_a"], fleck=c["fleck"])
+    out = dict(before=rec["before"][sub], after=rec["after"][sub], status=rec["status"][sub],
+               next=rec["next"][sub].astype(np.int64), tallies=rec["tallies"][sub], cell=rec["cell"][sub],
+               used_rw=rec["used_rw"][sub], tape=tape, tape_offset=new_off, tape_length=tape_len,
+               next_before=nxt_before, next_cell=nxt_cell, sigma_a=c["sigma_a"], fleck=c["fleck"])
+    if mg:   # frequencies, and the temperatures the recorded step built its tables from
+        out.update(freq_before=rec["freq_before"][sub], freq_after=rec["freq_after"][sub], T_start=T_start)
+    return out
 
 
 def main():
@@ -70,6 +79,14 @@ def main():
 
     cube = problems.step_cube(n=8, new_photons_per_cell=3, face_packets=40, comb_nmin=20)
     np.savez_compressed(os.path.join(HERE, "replay_cube_rw.npz"), **record(cube, 1, 400000, 1500))
+
+    # multigroup: 64 groups, PGRW, group-constant kappa0 nu^-3 (1 - e^{-nu/T}) (replay_mg.npz)
+    mg = problems.mg_cube(n=6, groups=64, new_photons_per_cell=3, comb_nmin=3, seed=5)
+    np.savez_compressed(os.path.join(HERE, "replay_mg.npz"), **record(mg, 1, 400000, 1500, mg=True))
+    # optically thinner, opacity continuous in frequency: collisions, effective scatters, face crossings
+    mgt = problems.mg_cube(n=6, groups=64, kappa0=1.0, new_photons_per_cell=3, comb_nmin=3, seed=6,
+                           group_constant=False)
+    np.savez_compressed(os.path.join(HERE, "replay_mg_thin.npz"), **record(mgt, 1, 400000, 1500, mg=True))
 
     rng = np.random.default_rng(7)
     xi_leak = np.concatenate([rng.random(3000), [1e-300, 1e-12, 0.5, 1 - 1e-12, np.nextafter(1, 0)]])

@@ -34,7 +34,7 @@ def _replay(engine, oracle_lib, g):
     return b
 
 
-def _check_replay(b, g, ncells, near_tie_allowance=0.001):
+def _check_replay(b, g, ncells, near_tie_allowance=0.001, time_rel=0.0):
     n = len(g["cell"])
     st_ok = b["phys_status"] == g["status"]
     # a status flip is only acceptable on a near tie of two event times
@@ -51,6 +51,9 @@ def _check_replay(b, g, ncells, near_tie_allowance=0.001):
             # w *= 1 + expm1(-tau): for large tau the sum cancels, so an ulp of
             # CUDA's expm1 is an ulp of the segment's starting weight
             atol = 8e-16 * np.abs(g["before"][ok, 7])
+        elif k == 6:
+            # timeLeft - dt cancels when the event time is close to census
+            atol = time_rel * np.abs(g["before"][ok, 6]) + 1e-300
         else:
             atol = 1e-300
         good = close(b[nm][ok], g["after"][ok, k], atol=atol)
