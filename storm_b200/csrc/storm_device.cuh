@@ -94,6 +94,8 @@ struct Ctx {
     const double *mgCdf;     // per cell, groups + 1: cumulative sigma_g B_g (the emission spectrum)
     const double4 *pgrw;     // per cell: sigmaT_bar, sigmaA_bar, D, gamma
     const uint32_t *pgrwCut; // per cell: group cutoff (0 = no PGRW)
+    const float *gb32;       // FP32-tracking form: bounds and group centres as floats
+    const float *gc32;
 };
 
 // ------------------------------------------------------------------ errors
@@ -736,6 +738,8 @@ struct Track32 {
     uint32_t cc;
     float4 cp;
     float hx, hy, hz;
+    // multigroup: photon energy, and the cell's kT and sigma0 (cached with cp)
+    float nu, kT, s0;
 };
 
 __device__ __forceinline__ float clampf(float v, float h) { return fminf(fmaxf(v, -h), h); }
@@ -782,19 +786,43 @@ __device__ inline float rw_sample_radius32(const RwTables &T, float tau, float x
 // tallies, the same draws in the same order as the FP64 form.  Ro is the
 // distance to the nearest face (the caller has checked Ro >= rwMinParticle /
 // sigma_T); the diffusion coefficient c / (3 sigma_T) is cp.z * C.rwDiffPerReach.
-template <class RNG, class TALLY>
+template <bool MG, class RNG, class TALLY>
 __device__ inline int rw_jump32(const Ctx &C, Track32 &T, RNG &rng, TALLY &tal, const float4 &cp, float Ro, float hx,
                                 float hy, float hz, int &err) {
     const uint32_t cell = T.cell;
-    const float D = cp.z * C.rwDiffPerReach;
+    // gray: D = c / (3 sigma_T) from the reach; multigroup: the PGRW cell data
+    float D, sigAf;
+    double fl = 0.0, sigmaA = 0.0, gammaRw = 1.0;
+    if (MG) {
+        const double4 g4 = C.pgrw[cell];
+        D = cp.w;
+        fl = cp.y;
+        sigmaA = g4.y;
+        gammaRw = g4.w;
+        sigAf = static_cast<float>(sigmaA * fl);
+    } else {
+        D = cp.z * C.rwDiffPerReach;
+        sigAf = cp.y;
+    }
     const float tauLeak = rw_sample_leak32(C.rw, rng.rawf());
     const double tLeak = static_cast<double>(tauLeak * (Ro * Ro) / D);
-    const bool leak = tLeak <= T.t;
-    const double dt = leak ? tLeak : T.t;
-    const float tau = cp.y * static_cast<float>(dt * C.clight);
+    double tUp = DBL_MAX;
+    if (MG && gammaRw < 1.0 && sigmaA > 0.0 && fl > 0.0) {   // PGRW upscatter (radiation/RadiationIMC.hpp:1130-1135)
+        const float xiUp = rng.rawf();
+        tUp = -static_cast<double>(__logf(xiUp)) / (C.clight * (1.0 - fl) * sigmaA * (1.0 - gammaRw));
+    }
+    int ev;
+    double dt;
+    if (tLeak <= T.t && tLeak <= tUp) { ev = 0; dt = tLeak; }
+    else if (T.t <= tUp) { ev = 1; dt = T.t; }
+    else { ev = 2; dt = tUp; }
+    const float tau = sigAf * static_cast<float>(dt * C.clight);
     const double e1 = static_cast<double>(expm1f(-tau));
     if (!C.noFeedback) tal.mat(cell, -e1 * T.w);
-    if (cp.y > 0.0f) tal.rad(cell, T.w * e1 * static_cast<double>(cp.w));
+    if (sigAf > 0.0f) {
+        const double invRate = MG ? -1.0 / (static_cast<double>(sigAf) * C.clight) : static_cast<double>(cp.w);
+        tal.rad(cell, T.w * e1 * invRate);
+    }
     T.w *= 1.0 + e1;
     T.t -= dt;
     if (fabs(T.w) < T.w0 * 1e-4) {
@@ -807,7 +835,7 @@ __device__ inline int rw_jump32(const Ctx &C, Track32 &T, RNG &rng, TALLY &tal, 
     __sincosf(6.2831853f * rng.rawf(), &sphi, &cphi);
     const float dx = sinT * cphi, dy = sinT * sphi, dz = cosT;
     float disp = Ro;
-    if (!leak) {
+    if (ev != 0) {
         const float tauPos = static_cast<float>(dt) * D / (Ro * Ro);
         disp = fminf(Ro * rw_sample_radius32(C.rw, tauPos, rng.rawf()), Ro);
     }
@@ -828,7 +856,38 @@ __device__ inline int rw_jump32(const Ctx &C, Track32 &T, RNG &rng, TALLY &tal, 
     float st, ct;
     __sincosf(theta, &st, &ct);
     T.ux = sz * ct; T.uy = sz * st; T.uz = cz;
-    return leak ? OUT_CONTINUE : OUT_CENSUS;
+    if (MG && ev == 2) {   // upscatter: a frequency above the cutoff (:1232-1250)
+        const uint32_t cutoff = C.pgrwCut[cell];
+        const double *cdf = C.mgCdf + static_cast<size_t>(cell) * (C.groups + 1);
+        const double cdfAtCutoff = cdf[cutoff], cdfTotal = cdf[C.groups];
+        double nu;
+        if (cdfTotal > cdfAtCutoff) {
+            const double lo = cdfAtCutoff / cdfTotal;
+            nu = mg_thermal_energy(C, cell, lo + static_cast<double>(rng.rawf()) * (1.0 - lo));
+        } else {
+            nu = nextafter(C.gb[cutoff], DBL_MAX);
+        }
+        T.nu = static_cast<float>(mg_clamp(C, nu));
+    }
+    return ev == 1 ? OUT_CENSUS : OUT_CONTINUE;
+}
+
+// Multigroup absorption opacity in FP32 from the cell's cached kT and sigma0.
+__device__ __forceinline__ float mg_absorption32(const Ctx &C, const Track32 &T, float nu) {
+    float E;
+    if (C.mgGroupConst) {
+        uint32_t lo = 0, hi = C.groups - 1;
+        while (lo < hi) {
+            const uint32_t mid = (lo + hi) >> 1;
+            if (nu < C.gb32[mid + 1]) hi = mid; else lo = mid + 1;
+        }
+        E = C.gc32[lo];
+    } else {
+        E = fmaxf(nu, C.gb32[0]);
+    }
+    float v = T.s0 / (__powf(T.kT, static_cast<float>(C.mgQ)) * __powf(E, static_cast<float>(C.mgP)));
+    if (C.mgS != 0.0) v *= __powf(-expm1f(-E / T.kT), static_cast<float>(C.mgS));
+    return v;
 }
 
 // One segment plus the manager's handling, in the FP32-tracking form.  Same
@@ -840,23 +899,45 @@ __device__ inline int rw_jump32(const Ctx &C, Track32 &T, RNG &rng, TALLY &tal, 
 // at speed |u_a|; the nearest exit is found by cross-multiplied comparisons
 // (n_a |u_b| < n_b |u_a|, first smallest wins, an axis with u_a = 0 never
 // wins) and only the winner is divided.
-template <class RNG, class TALLY>
+template <bool MG, class RNG, class TALLY>
 __device__ inline int segment32(const Ctx &C, Track32 &T, RNG &rng, TALLY &tal, int &usedRW, int &err) {
     const uint32_t cell = T.cell;
     if (T.cc != cell) {   // entered another cell: load its constants once
         T.cp = C.phys32[cell];
         T.hx = C.hx[T.i]; T.hy = C.hy[T.j]; T.hz = C.hz[T.k];
         T.cc = cell;
+        if (MG) {
+            T.kT = static_cast<float>(mg_kT(C, cell));
+            T.s0 = static_cast<float>(C.sig0[cell]);
+        }
     }
     const float hx = T.hx, hy = T.hy, hz = T.hz;
     const float4 cp = T.cp;
+    if (MG) T.nu = fminf(fmaxf(T.nu, C.gb32[0]), C.gb32[C.groups]);   // clampFrequencyToBounds
 
     // Random Walk only where the particle is at least cp.z = rwMinParticleOpticalDepth / sigma_T
-    // from every face (cp.z is inf in cells that are not eligible)
+    // from every face (cp.z is inf in cells that are not eligible); in a multigroup
+    // problem only below the cell's PGRW group cutoff
     const float Ro = fminf(fminf(hx - fabsf(T.qx), hy - fabsf(T.qy)), hz - fabsf(T.qz));
-    if (Ro >= cp.z && Ro > 0.0f) {
+    if (Ro >= cp.z && Ro > 0.0f && (!MG || static_cast<double>(T.nu) < C.gb[C.pgrwCut[cell]])) {
         usedRW = 1;
-        return rw_jump32(C, T, rng, tal, cp, Ro, hx, hy, hz, err);
+        return rw_jump32<MG>(C, T, rng, tal, cp, Ro, hx, hy, hz, err);
+    }
+    // gray: the cell constants; multigroup: the opacity at the particle's frequency
+    float invSigE, sigAf, sigE = 0.0f, elastic = 0.0f;
+    double invRate;
+    if (MG) {
+        const float sigA = mg_absorption32(C, T, T.nu);
+        const float f = cp.y;
+        elastic = cp.x;
+        sigE = elastic + (1.0f - f) * sigA;
+        invSigE = sigE > 0.0f ? 1.0f / sigE : CUDART_INF_F;
+        sigAf = sigA * f;
+        invRate = -1.0 / (static_cast<double>(sigAf) * C.clight);
+    } else {
+        invSigE = cp.x;
+        sigAf = cp.y;
+        invRate = static_cast<double>(cp.w);
     }
 
     const float ax = fabsf(T.ux), ay = fabsf(T.uy), az = fabsf(T.uz);
@@ -871,7 +952,7 @@ __device__ inline int segment32(const Ctx &C, Track32 &T, RNG &rng, TALLY &tal, 
     const float sF = __fdividef(bn, bd);
     const double c = C.clight;
 
-    const float sC = cp.x * (-__logf(rng.rawf()));
+    const float sC = invSigE * (-__logf(rng.rawf()));
     const float sL = static_cast<float>(T.t * c);
     int best = 0;
     float ds = sF;
@@ -879,10 +960,10 @@ __device__ inline int segment32(const Ctx &C, Track32 &T, RNG &rng, TALLY &tal, 
     if (sL < ds) { best = 2; ds = sL; }
     const double dt = (best == 2) ? T.t : static_cast<double>(ds) * C.invC;
     T.t -= dt;
-    const float tau = cp.y * ds;
+    const float tau = sigAf * ds;
     const double e1 = static_cast<double>(expm1f(-tau));
     double integrated = T.w * dt;
-    if (tau >= 1e-12f) integrated = T.w * e1 * static_cast<double>(cp.w);
+    if (tau >= 1e-12f) integrated = T.w * e1 * invRate;
     T.qx = clampf(fmaf(T.ux, ds, T.qx), hx);
     T.qy = clampf(fmaf(T.uy, ds, T.qy), hy);
     T.qz = clampf(fmaf(T.uz, ds, T.qz), hz);
@@ -895,13 +976,20 @@ __device__ inline int segment32(const Ctx &C, Track32 &T, RNG &rng, TALLY &tal, 
     }
     if (best == 2) return OUT_CENSUS;
     if (best == 1) {
-        rng.skip();   // the event-type draw (a no-op on the FP32 form's own stream)
+        bool effective = false;
+        if (MG) effective = !(rng.rawf() * sigE < elastic);   // elastic or effective scatter
+        else rng.skip();   // the event-type draw (a no-op on the FP32 form's own stream)
         const float theta = 6.2831853f * rng.rawf();
         const float cosT = 2.0f * rng.rawf() - 1.0f;
         const float sinT = sqrtf(fmaxf(0.0f, 1.0f - cosT * cosT));
         float st, ct;
         __sincosf(theta, &st, &ct);
         T.ux = sinT * ct; T.uy = sinT * st; T.uz = cosT;
+        if (MG && effective) {   // re-emission from the cell's spectrum
+            const double nu = mg_thermal_energy(C, cell, static_cast<double>(rng.rawf()));
+            if (nu < 0.0) { err = STORM_DERR_MG_SAMPLE; return OUT_ERROR; }
+            T.nu = static_cast<float>(nu);
+        }
         return OUT_CONTINUE;
     }
     // face crossing

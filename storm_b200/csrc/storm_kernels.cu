@@ -61,6 +61,9 @@ __device__ __forceinline__ void store32(const Bank &b, uint32_t q, const Track32
     b.t[q] = T.t; b.w[q] = T.w; b.w0[q] = T.w0;
     b.cell[q] = T.cell; b.pid[q] = pid; b.draw[q] = draw;
 }
+// multigroup FP32 banks keep the frequency as a float in the first half of nu
+__device__ __forceinline__ float load_nu32(const Bank &b, uint32_t q) { return reinterpret_cast<const float *>(b.nu)[q]; }
+__device__ __forceinline__ void store_nu32(const Bank &b, uint32_t q, float nu) { reinterpret_cast<float *>(b.nu)[q] = nu; }
 // global FP64 particle -> FP32-tracking particle of its cell
 __device__ __forceinline__ void to_local(const Ctx &C, const PartReg &p, Track32 &T) {
     cell_ijk(C, p.cell, T.i, T.j, T.k);
@@ -72,6 +75,7 @@ __device__ __forceinline__ void to_local(const Ctx &C, const PartReg &p, Track32
     const double inv = sp > 0.0 ? 1.0 / sp : 0.0;
     T.ux = static_cast<float>(p.vx * inv); T.uy = static_cast<float>(p.vy * inv); T.uz = static_cast<float>(p.vz * inv);
     T.t = p.t; T.w = p.w; T.w0 = p.w0;
+    T.nu = static_cast<float>(p.nu);
 }
 __device__ __forceinline__ void to_global(const Ctx &C, const Track32 &T, PartReg &p) {
     uint32_t i, j, k;
@@ -83,6 +87,7 @@ __device__ __forceinline__ void to_global(const Ctx &C, const Track32 &T, PartRe
     p.vy = static_cast<double>(T.uy) * C.clight;
     p.vz = static_cast<double>(T.uz) * C.clight;
     p.t = T.t; p.w = T.w; p.w0 = T.w0; p.cell = T.cell;
+    p.nu = static_cast<double>(T.nu);
 }
 // store an FP64 particle in the bank's layout
 __device__ __forceinline__ void store_any(const Ctx &C, const Bank &b, uint32_t q, const PartReg &p, uint32_t pid,
@@ -91,6 +96,7 @@ __device__ __forceinline__ void store_any(const Ctx &C, const Bank &b, uint32_t 
         Track32 T;
         to_local(C, p, T);
         store32(b, q, T, pid, draw);
+        if (b.nu) store_nu32(b, q, T.nu);
     } else {
         store_part(b, q, p, pid, draw);
     }
@@ -156,6 +162,12 @@ __device__ __forceinline__ void census_store32(const CensusBank &c, uint32_t q, 
     r[2] = two_doubles(T.w, T.w0);
     r[3] = make_uint4(T.cell, pid, draw, 0u);
 }
+// the same record with the frequency (multigroup) in its last word
+__device__ __forceinline__ void census_store32_mg(const CensusBank &c, uint32_t q, const Track32 &T, uint32_t pid,
+                                                  uint32_t draw) {
+    census_store32(c, q, T, pid, draw);
+    reinterpret_cast<uint32_t *>(c.rec + static_cast<size_t>(q) * 4 + 3)[3] = __float_as_uint(T.nu);
+}
 __device__ __forceinline__ void census_load32(const CensusBank &c, uint32_t q, Track32 &T, uint32_t &pid,
                                               uint32_t &draw) {
     const uint4 *r = c.rec + static_cast<size_t>(q) * 4;
@@ -165,6 +177,7 @@ __device__ __forceinline__ void census_load32(const CensusBank &c, uint32_t q, T
     T.t = __longlong_as_double((static_cast<unsigned long long>(b.w) << 32) | b.z);
     T.w = lo_double(d); T.w0 = hi_double(d);
     T.cell = e.x; pid = e.y; draw = e.z;
+    T.nu = __uint_as_float(e.w);
 }
 // weight, cell and pid of census record q
 __device__ __forceinline__ double census_w(const Ctx &C, const CensusBank &c, uint32_t q) {
@@ -184,6 +197,7 @@ __global__ void k_bank_to_local(Ctx C, Bank src, Bank dst, uint32_t n) {
         Track32 T;
         to_local(C, p, T);
         store32(dst, q, T, src.pid[q], src.draw[q]);
+        if (dst.nu) store_nu32(dst, q, T.nu);
     }
 }
 __global__ void k_bank_to_census(Ctx C, Bank src, CensusBank dst, uint32_t n) {
@@ -193,7 +207,8 @@ __global__ void k_bank_to_census(Ctx C, Bank src, CensusBank dst, uint32_t n) {
         if (C.fp32) {
             Track32 T;
             to_local(C, p, T);
-            census_store32(dst, q, T, src.pid[q], src.draw[q]);
+            if (C.groups >= 2) census_store32_mg(dst, q, T, src.pid[q], src.draw[q]);
+            else census_store32(dst, q, T, src.pid[q], src.draw[q]);
         } else {
             census_store64(dst, q, p, src.pid[q], src.draw[q]);
         }
@@ -203,6 +218,7 @@ __global__ void k_bank_to_global(Ctx C, Bank src, Bank dst, uint32_t n) {
     for (uint32_t q = blockIdx.x * blockDim.x + threadIdx.x; q < n; q += gridDim.x * blockDim.x) {
         Track32 T;
         load32(src, q, T);
+        T.nu = src.nu ? load_nu32(src, q) : 0.0f;
         PartReg p;
         to_global(C, T, p);
         store_part(dst, q, p, src.pid[q], src.draw[q]);
@@ -257,7 +273,14 @@ __device__ __forceinline__ void cell_rw_and_phys32(const Ctx &C, const CellArray
         }
         A.rwElig[c] = elig ? 1 : 0;
     }
-    if (C.fp32) {
+    if (C.fp32 && C.groups >= 2) {
+        // multigroup: x = elastic opacity, y = Fleck factor, z = PGRW reach, w = PGRW D
+        const double4 g4 = A.pgrw[c];
+        const bool rw = elig && g4.x > 0.0;
+        A.phys32[c] = make_float4(static_cast<float>(ss), static_cast<float>(f),
+                                  rw ? static_cast<float>(C.rwMinParticle / g4.x) : CUDART_INF_F,
+                                  rw ? static_cast<float>(g4.z) : 0.0f);
+    } else if (C.fp32) {
         const double eventOpacity = ss + (1.0 - f) * sa;
         const bool rw = elig && sigmaT > 0.0;
         const double rate = sa * f * C.clight;
@@ -745,6 +768,11 @@ __global__ void k_emit_cells32(Ctx C, CellArrays A, const uint64_t *offsets, uin
         T.w0 = fabs(T.w);
         const uint32_t slot = bankBase + static_cast<uint32_t>(e);
         store32(b, slot, T, slot, 0);
+        if (C.groups >= 2) {   // GetThermalEnergy (radiation/RadiationIMC.hpp:2495-2500)
+            const double nu = mg_thermal_energy(C, c, rng.open());
+            if (nu < 0.0) raise_error(C, STORM_DERR_MG_SAMPLE, c, static_cast<uint32_t>(e));
+            store_nu32(b, slot, static_cast<float>(nu));
+        }
         esum += T.w;
     }
     esum = warp_sum(esum);
@@ -901,7 +929,34 @@ struct Form32 {
     }
     template <class RNG, class TALLY>
     static __device__ __forceinline__ int seg(const Ctx &C, T &t, RNG &rng, TALLY &tal, int &usedRW, int &err) {
-        int m = segment32(C, t, rng, tal, usedRW, err);
+        int m = segment32<false>(C, t, rng, tal, usedRW, err);
+        if (m == OUT_ERROR && !err) err = STORM_DERR_NOT_ON_BOUNDARY;
+        return m;
+    }
+    static __device__ __forceinline__ uint32_t cell(const T &t) { return t.cell; }
+    static __device__ __forceinline__ double weight(const T &t) { return t.w; }
+};
+// The FP32-tracking form of a multigroup problem: the frequency rides along.
+struct Form32MG {
+    using T = Track32;
+    using Rng = PhiloxRng4;
+    static __device__ __forceinline__ void load(const Ctx &C, const Bank &b, uint32_t q, T &t) {
+        load32(b, q, t);
+        t.nu = load_nu32(b, q);
+        cell_ijk(C, t.cell, t.i, t.j, t.k);
+        t.cc = OUTSIDE;
+    }
+    static __device__ __forceinline__ void keep(const Bank &b, uint32_t q, const T &t, uint32_t pid, uint32_t draw) {
+        store32(b, q, t, pid, draw);
+        store_nu32(b, q, t.nu);
+    }
+    static __device__ __forceinline__ void store(const CensusBank &b, uint32_t q, const T &t, uint32_t pid,
+                                                 uint32_t draw) {
+        census_store32_mg(b, q, t, pid, draw);
+    }
+    template <class RNG, class TALLY>
+    static __device__ __forceinline__ int seg(const Ctx &C, T &t, RNG &rng, TALLY &tal, int &usedRW, int &err) {
+        int m = segment32<true>(C, t, rng, tal, usedRW, err);
         if (m == OUT_ERROR && !err) err = STORM_DERR_NOT_ON_BOUNDARY;
         return m;
     }
@@ -1463,8 +1518,11 @@ __global__ void k_comb_emit(Ctx C, CensusBank cen, const uint32_t *idx, const ui
                 T.w = lo_double(d); T.w0 = hi_double(d);
                 if (!(raw[u] & KEEP)) { T.w = wNew; T.w0 = T.w; T.t = 0; }
                 T.cell = c;
-                for (uint32_t k = 0; k < m; ++k)
+                const float nu = __uint_as_float(rec[u][3].w);
+                for (uint32_t k = 0; k < m; ++k) {
                     store32(out, static_cast<uint32_t>(o + k), T, static_cast<uint32_t>(o + k), 0);
+                    if (out.nu) store_nu32(out, static_cast<uint32_t>(o + k), nu);
+                }
             } else {
                 const uint4 a = rec[u][0], b = rec[u][1], d = rec[u][2], e = rec[u][3], f = rec[u][4];
                 PartReg p;
@@ -1503,6 +1561,7 @@ __global__ void k_gather(Ctx C, CensusBank src, const uint32_t *idx, uint32_t n,
             Track32 T;
             census_load32(src, sq, T, pid_, draw_);
             store32(dst, q, T, q, 0);
+            if (dst.nu) store_nu32(dst, q, T.nu);
             w = T.w; cell = T.cell;
         } else {
             PartReg p;
@@ -1824,7 +1883,8 @@ static void refill_launch(cudaStream_t s, uint32_t grid, int minBlocks, const Ct
 void launch_transport_refill(cudaStream_t s, uint32_t grid, int minBlocks, const Ctx &C, const Bank &in, uint32_t n,
                              uint32_t *nextIdx, const CensusBank &cen, uint32_t *nCen, uint32_t burst, uint32_t maxSegs,
                              DevStats *st) {
-    if (C.fp32) refill_launch<Form32>(s, grid, minBlocks, C, in, n, nextIdx, cen, nCen, burst, maxSegs, st);
+    if (C.fp32 && C.groups >= 2) refill_launch<Form32MG>(s, grid, minBlocks, C, in, n, nextIdx, cen, nCen, burst, maxSegs, st);
+    else if (C.fp32) refill_launch<Form32>(s, grid, minBlocks, C, in, n, nextIdx, cen, nCen, burst, maxSegs, st);
     else refill_launch<Form64>(s, grid, minBlocks, C, in, n, nextIdx, cen, nCen, burst, maxSegs, st);
 }
 template <class F>

@@ -54,6 +54,7 @@ struct StormHandle {
     double *rwTau = nullptr, *rwLogTau = nullptr, *rwSurv = nullptr, *rwRadius = nullptr;
     float *rwLogTau32 = nullptr, *rwSurv32 = nullptr, *rwRadius32 = nullptr;   // FP32-tracking form
     double *gb = nullptr;            // multigroup bounds
+    float *gb32 = nullptr, *gc32 = nullptr;   // multigroup bounds and centres, FP32-tracking form
     // face sources
     uint32_t *fsCell = nullptr;
     int32_t *fsSide = nullptr;
@@ -571,7 +572,6 @@ int storm_cuda_create(const StormProblemDesc *d, StormHandle **out) {
         if (!d->group_bounds || !(d->k_boltz > 0.0) || d->groups > 4096) return STORM_ERR_INVALID_ARG;
         for (uint32_t g = 0; g < d->groups; ++g)
             if (!(d->group_bounds[g + 1] > d->group_bounds[g])) return STORM_ERR_INVALID_ARG;
-        if (d->precision != STORM_PRECISION_FP64) return STORM_ERR_UNSUPPORTED;
     }
     if (d->eos_kind != STORM_EOS_LINEAR && d->eos_kind != STORM_EOS_POWER_LAW) return STORM_ERR_UNSUPPORTED;
     if (d->precision != STORM_PRECISION_FP64 && d->precision != STORM_PRECISION_FP32_TRACK) return STORM_ERR_UNSUPPORTED;
@@ -725,6 +725,16 @@ int storm_cuda_create(const StormProblemDesc *d, StormHandle **out) {
         C.kBoltz = d->k_boltz;
         C.sig0 = h->tabA;
         C.mgCdf = A.mgCdf; C.pgrw = A.pgrw; C.pgrwCut = A.pgrwCut;
+        if (h->fp32) {
+            std::vector<float> b32(G + 1), c32(G);
+            for (uint32_t g = 0; g <= G; ++g) b32[g] = static_cast<float>(d->group_bounds[g]);
+            for (uint32_t g = 0; g < G; ++g) c32[g] = static_cast<float>(0.5 * (d->group_bounds[g] + d->group_bounds[g + 1]));
+            ALLOC(h->gb32, G + 1);
+            ALLOC(h->gc32, G);
+            H2D(h->gb32, b32.data(), G + 1);
+            H2D(h->gc32, c32.data(), G);
+            C.gb32 = h->gb32; C.gc32 = h->gc32;
+        }
     }
     C.T = A.T;
     C.escapeNoCheck = d->escape_without_check;
@@ -774,7 +784,7 @@ int storm_cuda_destroy(StormHandle *h) {
                   h->A.rwElig, h->A.photons, h->A.phys, h->A.phys32, h->hx, h->hy, h->hz, h->segs, h->tabA, h->tabS, h->rhoF, h->rwTau, h->rwLogTau, h->rwSurv,
                   h->rwRadius, h->rwLogTau32, h->rwSurv32, h->rwRadius32, h->fsCell, h->fsSide, h->fsOffset, h->dAmbiguous, h->offsets, h->tileSums, h->dTotalU64, h->dTotalE, h->combW, h->combWtot,
                   h->combStart, h->combCount, h->counts, h->dStats, h->dErr, h->gb, h->A.mgCdf, h->A.pgrw,
-                  h->A.pgrwCut};
+                  h->A.pgrwCut, h->gb32, h->gc32};
     for (void *p : ps) device_pool().free(p);
     cudaEvent_t evs[] = {h->evStart, h->evTransport0, h->evTransport1, h->evEnd, h->evAfterEmit, h->evAfterComb};
     for (cudaEvent_t e : evs)
@@ -872,8 +882,10 @@ int storm_cuda_phase_transport(StormHandle *h) {
     if (h->desc.per_cell_segment_counters) CK(cudaMemsetAsync(h->segs, 0, sizeof(uint32_t) * h->N, h->stream));
     uint32_t n32 = static_cast<uint32_t>(n0);
     uint32_t *nCen = h->counts + h->maxRounds + 1;
-    if (!h->refill) CK(cudaMemcpyAsync(h->counts, &n32, sizeof(uint32_t), cudaMemcpyHostToDevice, h->stream));
-    if (h->refill) {
+    // the multigroup FP32 form runs only in the refill kernel
+    const bool refill = h->refill || (h->fp32 && h->desc.groups >= 2);
+    if (!refill) CK(cudaMemcpyAsync(h->counts, &n32, sizeof(uint32_t), cudaMemcpyHostToDevice, h->stream));
+    if (refill) {
         // one launch carries every history to census, escape or cutoff
         const uint64_t maxSegs64 = static_cast<uint64_t>(h->maxRounds) * h->K;
         const uint32_t maxSegs = static_cast<uint32_t>(std::min<uint64_t>(maxSegs64, 0xffffffffull));

@@ -103,3 +103,31 @@ def test_mg_steps_statistics_vs_reference(ref_lib):
     se = np.sqrt(a.var(0, ddof=1) / len(a) + b.var(0, ddof=1) / len(b))
     z = np.abs(ma - mb) / np.maximum(se, 1e-9 * ma)
     assert (z < 4).mean() > 0.95, np.sort(z)[-10:]
+
+
+def test_mg_fp32_tracking_conserves_and_agrees_with_fp64():
+    """The FP32-tracking form of a multigroup problem: energy conserved per step
+    and temperatures within the seed-to-seed scatter of the FP64 form."""
+    from storm_b200 import _abi as A
+
+    def run(precision, seeds):
+        out = []
+        for s in seeds:
+            p = problems.mg_cube(n=8, groups=64, kappa0=1.0, new_photons_per_cell=6, comb_nmin=6, seed=s,
+                                 precision=precision)
+            e = Engine(p)
+            for _ in range(4):
+                st = e.step()
+                assert _balance(st) < 1e-10
+            c = e.census()
+            assert (c.frequency >= p.group_bounds[0] * (1 - 1e-6)).all()
+            assert (c.frequency <= p.group_bounds[-1] * (1 + 1e-6)).all()
+            out.append(e.cells()["temperature"])
+            e.close()
+        return np.array(out)
+    a = run(A.PRECISION_FP32_TRACK, range(30, 38))
+    b = run(A.PRECISION_FP64, range(70, 78))
+    ma, mb = a.mean(0), b.mean(0)
+    se = np.sqrt(a.var(0, ddof=1) / len(a) + b.var(0, ddof=1) / len(b))
+    z = np.abs(ma - mb) / np.maximum(se, 1e-9 * ma)
+    assert (z < 4).mean() > 0.95, np.sort(z)[-10:]
