@@ -51,6 +51,8 @@ def parse():
     ap.add_argument("--waves", type=int, default=4)
     ap.add_argument("--refill", type=int, default=-1, help="1 persistent refill kernel, 0 bank visits")
     ap.add_argument("--burst", type=int, default=8)
+    ap.add_argument("--mg-steps", type=int, default=5, help="timed steps of the multigroup run (0 = skip it)")
+    ap.add_argument("--mg-n", type=int, default=128)
     ap.add_argument("--serving-requests", type=int, default=32, help="requests in the serving run (0 = skip it)")
     ap.add_argument("--serving-slots", type=int, default=12)
     ap.add_argument("--serving-workers", type=int, default=6)
@@ -338,6 +340,45 @@ def e2e_run(args, eng, p, dist):
                     "host-side checks inside the timed region (wall clock)"}
 
 
+def mg_run(args):
+    """The multigroup configuration: a 128^3 unit cube, 64 groups log-spaced over
+    [0.01, 100] keV, kappa_g = 100 nu_g^-3 (1 - exp(-nu_g/T)) cm^-1, initial T
+    uniform in [0.01, 0.1] keV per cell (seeded), cell emission from the
+    Planck-weighted opacity spectrum (about 4e7 packets per step at 2 packets
+    per cell), comb Nmin=12 factor=2, PGRW.  Both forms on the same problem;
+    device-timed steps after 2 warm-up steps."""
+    import numpy as np
+    from storm_b200 import _abi as A
+    from storm_b200 import problems
+    from storm_b200.engine import Engine
+    out = {"workload": f"mg_cube {args.mg_n}^3, 64 groups [0.01,100] keV, kappa0=100 nu^-3 (1-exp(-nu/T)), "
+                       "T0 U[0.01,0.1] keV, 2 photons/cell base allocation, comb Nmin=12 factor=2, PGRW",
+           "steps": args.mg_steps}
+    temps = {}
+    for name, prec in (("fp32", A.PRECISION_FP32_TRACK), ("fp64", A.PRECISION_FP64)):
+        p = problems.mg_cube(n=args.mg_n, groups=64, kappa0=100.0, new_photons_per_cell=2, comb_nmin=12, seed=3,
+                             precision=prec)
+        p.per_cell_segment_counters = False
+        e = Engine(p)
+        for _ in range(2):
+            e.step()
+        segs, ms, lat = 0, 0.0, []
+        for _ in range(args.mg_steps):
+            st = e.step()
+            segs += st["segments"]
+            ms += st["step_ms"]
+            lat.append(st["step_ms"])
+        out[name] = {"segments_per_s": segs / (ms / 1e3), "ms_per_step": ms / args.mg_steps,
+                     "segments_per_step": segs / args.mg_steps, "emitted_per_step": st["emitted_cells"],
+                     "census_per_step": st["census_out"], "step_ms_p99": float(np.percentile(lat, 99)),
+                     "device_gb": e.memory_bytes() / 1e9}
+        temps[name] = e.cells()["temperature"]
+        e.close()
+    out["fp32_over_fp64"] = out["fp32"]["segments_per_s"] / out["fp64"]["segments_per_s"]
+    out["mean_relative_temperature_difference"] = float(np.mean(np.abs(temps["fp32"] - temps["fp64"]) / temps["fp64"]))
+    return out
+
+
 def serving_run(args):
     """Many independent FP32-tracking problems (N log-uniform in [16, 48],
     1e4-1e6 packets/step log-uniform, kappa uniform in [0.1, 1000], 5-20 steps)
@@ -426,6 +467,7 @@ def run_storm(args, ws, rank, local, dist):
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline(args.n, 1)
     serving = serving_run(args) if (rank == 0 and ws == 1 and args.serving_requests > 0) else None
+    multigroup = mg_run(args) if (rank == 0 and ws == 1 and args.mg_steps > 0) else None
     if rank == 0:
         lat = sorted(f32["step_ms"])
         line = {
@@ -447,7 +489,8 @@ def run_storm(args, ws, rank, local, dist):
                      "roofline": roofline(f64, BYTES_PER_SEGMENT_FP64, transport_kernel(args, False))},
             "fp32_over_fp64": v32 / v64,
             "fp32_vs_fp64_deviation": dev,
-            "cpu_baseline": cpu, "e2e": e2e, "serving": serving, "clocks": ck, "gpu_launches": f32["launches"],
+            "cpu_baseline": cpu, "e2e": e2e, "serving": serving, "multigroup": multigroup, "clocks": ck,
+            "gpu_launches": f32["launches"],
             "transport_share": f32["transport"]["kernel_ms"] / max(sum(f32["step_ms"]), 1e-9),
         }
         print(json.dumps(line), flush=True)

@@ -50,6 +50,7 @@ def lib():
         L.ref_create.restype = vp
         L.ref_create.argtypes = [C.POINTER(A.StormProblemDesc), C.c_int, C.c_char_p, C.c_size_t]
         L.ref_destroy.argtypes = [vp]
+        L.ref_set_face_temperature.argtypes = [vp, C.c_int, C.c_double]
         L.ref_last_error.restype = C.c_char_p
         L.ref_last_error.argtypes = [vp]
         L.ref_step.argtypes = [vp, C.c_double, C.POINTER(RefStepOut)]
@@ -142,6 +143,9 @@ class Reference:
     def _check(self, rc):
         if rc != 0:
             raise RuntimeError("reference error: " + lib().ref_last_error(self.h).decode())
+
+    def set_face_temperature(self, face, T):
+        self._check(lib().ref_set_face_temperature(self.h, face, T))
 
     def step(self, dt=None):
         out = RefStepOut()

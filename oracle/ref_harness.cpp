@@ -200,12 +200,18 @@ using HarnessOpacity = HarnessOpacityT<1>;
 // faces with a source temperature emit Planck surface packets like
 // SideTemperature::generateNewBoundaryParticles (boundary/SideTemperature.hpp:114-163),
 // including TwoSidesTemperature's outside-box repair (boundary/TwoSidesTemperature.hpp:178-189).
+// With group bounds set (multigroup problems) each packet's frequency follows
+// DensmoreBoundary::generateNewBoundaryParticles
+// (examples/densmore2012/DensmoreBoundary.hpp:99-109, 128-139): a group from the
+// face's cumulative Planck integrals, then a uniform energy inside it.
 class HarnessBoundary : public STORM::BoundaryCondition<Vector3D, Grid> {
 public:
     StormBoxFace faces[6];
     bool escapeNoCheck = false;
     double sigmaSB = units::sigma_sb, clight = units::clight;
     double escaped = 0.0;
+    std::vector<double> bounds;   // groups + 1 energies [erg]; empty for gray problems
+    double kBoltz = units::k_boltz;
     std::mt19937_64 re{0};
 
     explicit HarnessBoundary(const Grid &g) : STORM::BoundaryCondition<Vector3D, Grid>(g) { std::memset(faces, 0, sizeof(faces)); }
@@ -257,6 +263,16 @@ public:
                 const std::size_t Np = faces[bf].packets_per_face;
                 const double T4 = boost::math::pow<4>(faces[bf].source_temperature);
                 double energyToProduce = sigmaSB * T4 * this->grid.GetArea(faceIdx) * fullDt / Np;
+                const std::size_t G = bounds.empty() ? 0 : bounds.size() - 1;
+                std::vector<double> cdf(G + 1, 0.0);
+                if (G) {
+                    const double kT = kBoltz * faces[bf].source_temperature;
+                    for (std::size_t g = 0; g < G; ++g) {
+                        double a = bounds[g] / kT, b = bounds[g + 1] / kT;
+                        double bg = (a > 0.0 && b > a) ? planck_integral::planck_integral(a, b) : 0.0;
+                        cdf[g + 1] = cdf[g] + bg;
+                    }
+                }
                 for (std::size_t j = 0; j < Np; ++j) {
                     out.emplace_back();
                     MCParticle &p = out.back();
@@ -271,6 +287,17 @@ public:
                     p.velocity = Vector3D(v[0], v[1], v[2]);
                     p.velocity *= clight;
                     p.frequency = 0;
+                    if (G) {
+                        const double total = cdf[G];
+                        if (total > 0.0) {
+                            double r = unif(re) * total;
+                            std::size_t g = 0;
+                            while (g + 1 < G && cdf[g + 1] < r) ++g;
+                            p.frequency = bounds[g] + unif(re) * (bounds[g + 1] - bounds[g]);
+                        } else {
+                            p.frequency = 0.5 * (bounds[0] + bounds[G]);
+                        }
+                    }
                     p.weight = energyToProduce;
                     p.initialWeight = p.weight;
                     p.timeLeft = fullDt * unif(re);
@@ -426,7 +453,9 @@ struct RefHandle {
     std::string lastError;
 };
 
-constexpr std::size_t kMGGroups = 64;
+// Multigroup instantiations of RadiationIMC held by this build: 30 groups (the
+// Densmore 2012 benchmark) and 64 groups (the 128^3 multigroup cube).
+constexpr std::size_t kMGGroupsA = 30, kMGGroupsB = 64;
 
 // RadiationIMC<..., G> with the harness opacity plug-in built from the descriptor.
 template <std::size_t G>
@@ -507,6 +536,10 @@ RefHandle *ref_create(const StormProblemDesc *d, int boundary_kind, char *err, s
             b->escapeNoCheck = d->escape_without_check != 0;
             b->sigmaSB = d->sigma_sb;
             b->clight = d->clight;
+            if (d->groups >= 2) {
+                b->bounds.assign(d->group_bounds, d->group_bounds + d->groups + 1);
+                b->kBoltz = d->k_boltz;
+            }
             h->harnessBoundary = b.get();
             h->boundary = b;
             break;
@@ -524,8 +557,9 @@ RefHandle *ref_create(const StormProblemDesc *d, int boundary_kind, char *err, s
         default: throw STORM::StormError("unknown boundary kind");
         }
         if (d->groups >= 2) {
-            if (d->groups != kMGGroups) throw STORM::StormError("reference build holds multigroup for 64 groups only");
-            build_physics<kMGGroups>(*h, d);
+            if (d->groups == kMGGroupsA) build_physics<kMGGroupsA>(*h, d);
+            else if (d->groups == kMGGroupsB) build_physics<kMGGroupsB>(*h, d);
+            else throw STORM::StormError("reference build holds multigroup for 30 and 64 groups only");
         } else {
             build_physics<1>(*h, d);
         }
@@ -542,6 +576,14 @@ RefHandle *ref_create(const StormProblemDesc *d, int boundary_kind, char *err, s
 }
 
 void ref_destroy(RefHandle *h) { delete h; }
+
+// The per-face descriptor boundary's SetTemperature (MarshakBoundary.hpp:33,
+// DensmoreBoundary.hpp:42): a new source temperature for box face `face`.
+int ref_set_face_temperature(RefHandle *h, int face, double T) {
+    if (!h->harnessBoundary || face < 0 || face > 5) return -1;
+    h->harnessBoundary->faces[face].source_temperature = T;
+    return 0;
+}
 
 const char *ref_last_error(RefHandle *h) { return h->lastError.c_str(); }
 

@@ -28,6 +28,7 @@ constexpr uint32_t OUTSIDE = 0xffffffffu;
 constexpr double EPSILON_FACE = 1e-12;       // particle/Particle.hpp:17
 constexpr double MONTECARLO_EPS = 1e-8;      // manager/MonteCarloConfig.hpp:11
 constexpr double RW_NUDGE = 1e-6;            // radiation/RadiationIMC.hpp:1211
+constexpr float ENTRY32 = 1.0f - 0x1p-21f;    // FP32 form: entry offset / half width after a cell change
 constexpr double RW_PI = 3.14159265358979323846;
 constexpr double TWO_PI_ISO = 6.283185307179586476925286766559;   // radiation/RadiationOpacityModel.hpp:143
 constexpr double ONE_BELOW = 0x1.fffffffffffffp-1;                  // std::nextafter(1.0, 0.0)
@@ -96,6 +97,7 @@ struct Ctx {
     const uint32_t *pgrwCut; // per cell: group cutoff (0 = no PGRW)
     const float *gb32;       // FP32-tracking form: bounds and group centres as floats
     const float *gc32;
+    const double *faceCdf;   // per box face, groups + 1: cumulative B_g at the face's source temperature
 };
 
 // ------------------------------------------------------------------ errors
@@ -1004,13 +1006,20 @@ __device__ inline int segment32(const Ctx &C, Track32 &T, RNG &rng, TALLY &tal, 
     default: inside = T.k + 1 < C.nz; break;
     }
     if (inside) {
+        // The serial manager nudges a particle that changed cells 1e-8 of the
+        // way to the new cell's centre (MonteCarloManagerSerial.hpp:323-327),
+        // which an FP32 offset cannot hold.  The particle enters ENTRY32 of
+        // the half width from the centre instead: at least 4 ulps inside the
+        // face, so a cell whose mean free path is below the offset's
+        // resolution still sees a nonzero distance to the face (Random Walk
+        // eligible) rather than a particle pinned to the face.
         switch (face) {
-        case 0: --T.i; T.cell -= 1; T.qx = C.hx[T.i]; break;
-        case 1: ++T.i; T.cell += 1; T.qx = -C.hx[T.i]; break;
-        case 2: --T.j; T.cell -= C.nx; T.qy = C.hy[T.j]; break;
-        case 3: ++T.j; T.cell += C.nx; T.qy = -C.hy[T.j]; break;
-        case 4: --T.k; T.cell -= C.nx * C.ny; T.qz = C.hz[T.k]; break;
-        default: ++T.k; T.cell += C.nx * C.ny; T.qz = -C.hz[T.k]; break;
+        case 0: --T.i; T.cell -= 1; T.qx = C.hx[T.i] * ENTRY32; break;
+        case 1: ++T.i; T.cell += 1; T.qx = -C.hx[T.i] * ENTRY32; break;
+        case 2: --T.j; T.cell -= C.nx; T.qy = C.hy[T.j] * ENTRY32; break;
+        case 3: ++T.j; T.cell += C.nx; T.qy = -C.hy[T.j] * ENTRY32; break;
+        case 4: --T.k; T.cell -= C.nx * C.ny; T.qz = C.hz[T.k] * ENTRY32; break;
+        default: ++T.k; T.cell += C.nx * C.ny; T.qz = -C.hz[T.k] * ENTRY32; break;
         }
         return OUT_CONTINUE;
     }

@@ -64,13 +64,16 @@ __device__ __forceinline__ void store32(const Bank &b, uint32_t q, const Track32
 // multigroup FP32 banks keep the frequency as a float in the first half of nu
 __device__ __forceinline__ float load_nu32(const Bank &b, uint32_t q) { return reinterpret_cast<const float *>(b.nu)[q]; }
 __device__ __forceinline__ void store_nu32(const Bank &b, uint32_t q, float nu) { reinterpret_cast<float *>(b.nu)[q] = nu; }
-// global FP64 particle -> FP32-tracking particle of its cell
+// global FP64 particle -> FP32-tracking particle of its cell.  Offsets are held
+// ENTRY32 of the half width inside the cell, as on a cell change: a packet
+// born on a face (boundary sources) then starts a few ulps inside it, where
+// the FP64 form resolves its first sub-ulp flights.
 __device__ __forceinline__ void to_local(const Ctx &C, const PartReg &p, Track32 &T) {
     cell_ijk(C, p.cell, T.i, T.j, T.k);
     T.cell = p.cell;
-    T.qx = clampf(static_cast<float>(p.x - C.xc[T.i]), C.hx[T.i]);
-    T.qy = clampf(static_cast<float>(p.y - C.yc[T.j]), C.hy[T.j]);
-    T.qz = clampf(static_cast<float>(p.z - C.zc[T.k]), C.hz[T.k]);
+    T.qx = clampf(static_cast<float>(p.x - C.xc[T.i]), C.hx[T.i] * ENTRY32);
+    T.qy = clampf(static_cast<float>(p.y - C.yc[T.j]), C.hy[T.j] * ENTRY32);
+    T.qz = clampf(static_cast<float>(p.z - C.zc[T.k]), C.hz[T.k] * ENTRY32);
     const double sp = vnorm(p.vx, p.vy, p.vz);
     const double inv = sp > 0.0 ? 1.0 / sp : 0.0;
     T.ux = static_cast<float>(p.vx * inv); T.uy = static_cast<float>(p.vy * inv); T.uz = static_cast<float>(p.vz * inv);
@@ -823,8 +826,29 @@ __global__ void k_emit_faces(Ctx C, FaceSources F, uint64_t total, Bank b, uint3
         v[(axis + 2) % 3] = one_m * stt;
         p.vx = v[0] * C.clight; p.vy = v[1] * C.clight; p.vz = v[2] * C.clight;
         p.w = energy;
-        p.nu = 0.0;   // the harness boundary plug-in leaves frequency 0 (clamped to the lowest bound where used)
+        p.nu = 0.0;   // gray problems carry frequency 0
         p.t = dt * rng.raw();
+        if (C.groups >= 2) {
+            // DensmoreBoundary::generateNewBoundaryParticles
+            // (examples/densmore2012/DensmoreBoundary.hpp:128-139): the first group
+            // whose cumulative Planck integral reaches u * total (the last group
+            // when none does), then a uniform energy inside it; two draws after
+            // the time draw, so gray streams are unchanged.
+            const uint32_t G = C.groups;
+            const double *row = C.faceCdf + static_cast<size_t>(side) * (G + 1);
+            const double total = row[G];
+            if (total > 0.0) {
+                const double r = rng.raw() * total;
+                uint32_t lo = 0, hi = G - 1;
+                while (lo < hi) {
+                    const uint32_t mid = (lo + hi) >> 1;
+                    if (row[mid + 1] < r) lo = mid + 1; else hi = mid;
+                }
+                p.nu = C.gb[lo] + rng.raw() * (C.gb[lo + 1] - C.gb[lo]);
+            } else {
+                p.nu = 0.5 * (C.gb[0] + C.gb[G]);
+            }
+        }
         p.cell = c;
         repair_outside(C, p.x, p.y, p.z, C.xc[i], C.yc[j], C.zc[k]);
         p.w0 = fabs(p.w);
@@ -834,6 +858,27 @@ __global__ void k_emit_faces(Ctx C, FaceSources F, uint64_t total, Bank b, uint3
     }
     esum = warp_sum(esum);
     if ((threadIdx.x & 31) == 0 && esum != 0.0) atomicAdd(&st->eEmitted, esum);
+}
+
+// The Planck spectrum of each box face over the groups, cumulative
+// planck_integral(b_g / kT, b_{g+1} / kT) at kT = k_B T_face, as
+// DensmoreBoundary builds it (examples/densmore2012/DensmoreBoundary.hpp:99-109).
+// One thread per face; rebuilt only when a face temperature changes.
+__global__ void k_face_spectra(Ctx C, double *cdf) {
+    const int f = threadIdx.x;
+    if (f >= 6) return;
+    const uint32_t G = C.groups;
+    double *row = cdf + static_cast<size_t>(f) * (G + 1);
+    const double kT = C.kBoltz * C.sourceT[f];
+    double acc = 0.0;
+    row[0] = 0.0;
+    for (uint32_t g = 0; g < G; ++g) {
+        if (kT > 0.0) {
+            const double a = C.gb[g] / kT, b = C.gb[g + 1] / kT;
+            acc += (a > 0.0 && b > a) ? planck_integral(a, b) : 0.0;
+        }
+        row[g + 1] = acc;
+    }
 }
 
 // ------------------------------------------------------------------ transport
@@ -1757,6 +1802,7 @@ void launch_emit_faces(cudaStream_t s, const Ctx &C, const FaceSources &F, uint6
     if (!total) return;
     k_emit_faces<<<grid_for(total, 256, 148 * 16), 256, 0, s>>>(C, F, total, b, bankBase, dt, st);
 }
+void launch_face_spectra(cudaStream_t s, const Ctx &C, double *cdf) { k_face_spectra<<<1, 32, 0, s>>>(C, cdf); }
 void launch_transport(cudaStream_t s, uint32_t grid, const Ctx &C, const Bank &in, const uint32_t *nIn, const Bank &out,
                       uint32_t *nOut, const CensusBank &cen, uint32_t *nCen, uint32_t K, DevStats *st, int minBlocks) {
     if (C.fp32) {

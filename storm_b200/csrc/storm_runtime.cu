@@ -55,6 +55,8 @@ struct StormHandle {
     float *rwLogTau32 = nullptr, *rwSurv32 = nullptr, *rwRadius32 = nullptr;   // FP32-tracking form
     double *gb = nullptr;            // multigroup bounds
     float *gb32 = nullptr, *gc32 = nullptr;   // multigroup bounds and centres, FP32-tracking form
+    double *faceCdf = nullptr;                // multigroup: 6 x (groups + 1) face Planck spectra
+    double faceCdfT[6] = {-1, -1, -1, -1, -1, -1};   // face temperatures the spectra were built for
     // face sources
     uint32_t *fsCell = nullptr;
     int32_t *fsSide = nullptr;
@@ -717,6 +719,7 @@ int storm_cuda_create(const StormProblemDesc *d, StormHandle **out) {
         ALLOC(A.mgCdf, static_cast<size_t>(N) * (G + 1));
         ALLOC(A.pgrw, N);
         ALLOC(A.pgrwCut, N);
+        ALLOC(h->faceCdf, 6 * (static_cast<size_t>(G) + 1));
         if (cudaMemset(A.pgrwCut, 0, N * sizeof(uint32_t)) != cudaSuccess) return fail(STORM_ERR_CUDA);
         C.groups = G;
         C.mgGroupConst = d->mg_group_constant;
@@ -725,6 +728,7 @@ int storm_cuda_create(const StormProblemDesc *d, StormHandle **out) {
         C.kBoltz = d->k_boltz;
         C.sig0 = h->tabA;
         C.mgCdf = A.mgCdf; C.pgrw = A.pgrw; C.pgrwCut = A.pgrwCut;
+        C.faceCdf = h->faceCdf;
         if (h->fp32) {
             std::vector<float> b32(G + 1), c32(G);
             for (uint32_t g = 0; g <= G; ++g) b32[g] = static_cast<float>(d->group_bounds[g]);
@@ -784,7 +788,7 @@ int storm_cuda_destroy(StormHandle *h) {
                   h->A.rwElig, h->A.photons, h->A.phys, h->A.phys32, h->hx, h->hy, h->hz, h->segs, h->tabA, h->tabS, h->rhoF, h->rwTau, h->rwLogTau, h->rwSurv,
                   h->rwRadius, h->rwLogTau32, h->rwSurv32, h->rwRadius32, h->fsCell, h->fsSide, h->fsOffset, h->dAmbiguous, h->offsets, h->tileSums, h->dTotalU64, h->dTotalE, h->combW, h->combWtot,
                   h->combStart, h->combCount, h->counts, h->dStats, h->dErr, h->gb, h->A.mgCdf, h->A.pgrw,
-                  h->A.pgrwCut, h->gb32, h->gc32};
+                  h->A.pgrwCut, h->gb32, h->gc32, h->faceCdf};
     for (void *p : ps) device_pool().free(p);
     cudaEvent_t evs[] = {h->evStart, h->evTransport0, h->evTransport1, h->evEnd, h->evAfterEmit, h->evAfterComb};
     for (cudaEvent_t e : evs)
@@ -863,6 +867,11 @@ int storm_cuda_phase_emit(StormHandle *h, double dt) {
     if (rc != STORM_OK) return rc;
     launch_emit_cells(h->stream, h->C, h->A, h->offsets, ne, h->bankA, static_cast<uint32_t>(h->nCensus), dt, h->dStats);
     FaceSources F{h->fsCell, h->fsSide, h->fsOffset, h->fsCount};
+    if (nf && h->C.groups >= 2 && std::memcmp(h->faceCdfT, h->C.sourceT, sizeof(h->faceCdfT)) != 0) {
+        launch_face_spectra(h->stream, h->C, h->faceCdf);
+        ++h->launches;
+        std::memcpy(h->faceCdfT, h->C.sourceT, sizeof(h->faceCdfT));
+    }
     launch_emit_faces(h->stream, h->C, F, nf, h->bankA, static_cast<uint32_t>(h->nCensus + ne), dt, h->dStats);
     h->launches += (ne ? 1 : 0) + (nf ? 1 : 0);
     CK(cudaGetLastError());

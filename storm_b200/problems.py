@@ -306,3 +306,140 @@ def mg_cube(n=16, groups=64, kappa0=100.0, new_photons_per_cell=4, comb_nmin=4, 
     p.comb_nmin, p.comb_factor = comb_nmin, 2.0
     p.seed, p.dt, p.precision, p.name = seed, dt, precision, "mg_cube"
     return p
+
+
+# ---------------------------------------------------------------- the reference's benchmark problems
+
+# Krief & McClarren (2024) Marshak waves 1-4 as the reference states them
+# (examples/marshak_wave/MarshakCommon.hpp:48-113): power-law opacity
+# kappa = kappa0 (keV / T)^alpha rho^betaRho (Planck kappaP0, total kappaR0),
+# EOS e_vol = f T^beta rho^(1 - mu), bath T(t) = coeff (t / ns)^exponent keV.
+MARSHAK_PARAMS = {
+    1: dict(length=0.2, x_offset=0.0, kP0=0.1, kR0=100.0, alpha=3.0, beta_rho=0.0, f_keV=6.860085e14, eos_beta=4.0,
+            eos_mu=0.0, bath_coeff=1.008038, bath_exp=1.0 / 3.0, initial_dt=1e-15),
+    2: dict(length=0.2, x_offset=0.0, kP0=100.0, kR0=100.0, alpha=3.0, beta_rho=0.0, f_keV=6.860085e14, eos_beta=4.0,
+            eos_mu=0.0, bath_coeff=1.014565, bath_exp=1.0 / 3.0, initial_dt=1e-15),
+    3: dict(length=1.0, x_offset=0.0, kP0=0.1, kR0=40.0, alpha=1.5, beta_rho=1.2, f_keV=1e14, eos_beta=3.4,
+            eos_mu=0.14, bath_coeff=1.0470478, bath_exp=86.0 / 57.0, initial_dt=1e-15),
+    4: dict(length=1.0, x_offset=1e-5, kP0=0.001, kR0=2.0, alpha=4.5, beta_rho=1.9, f_keV=1e14, eos_beta=6.0,
+            eos_mu=0.3, bath_coeff=1.01008116, bath_exp=14.0 / 139.0, initial_dt=1e-17),
+}
+MARSHAK_FINAL_TIME = 1e-9
+
+
+def marshak_density(problem, x):
+    """ComputeDensity (MarshakCommon.hpp:115-124)."""
+    x = np.asarray(x, dtype=np.float64)
+    if problem == 3:
+        return np.power(np.maximum(x, 1e-30), 20.0 / 19.0)
+    if problem == 4:
+        return np.power(np.maximum(x, 1e-30), -40.0 / 139.0)
+    return np.ones_like(x)
+
+
+def marshak_bath_temperature(problem, t):
+    """BathTemperature (MarshakCommon.hpp:141-145), in K."""
+    q = MARSHAK_PARAMS[problem]
+    t_ns = max(t, 1e-20) * 1e9
+    return q["bath_coeff"] * t_ns ** q["bath_exp"] * UNITS["kev_kelvin"]
+
+
+def marshak4_edges(x_offset, x_max):
+    """BuildMarshak4MeshEdges (MarshakCommon.hpp:249-263): 512 cells, the first
+    7e-5 cm wide, each 1.0096903847403653 times the last, the last edge x_max."""
+    edges = np.empty(513)
+    edges[0] = x_offset
+    width = 7.0e-5
+    for i in range(512):
+        edges[i + 1] = x_max if i + 1 == 512 else edges[i] + width
+        width *= 1.0096903847403653
+    return edges
+
+
+def marshak_wave(problem=1, nx=256, new_photons_per_cell=15, boundary_per_face=100, seed=42,
+                 precision=A.PRECISION_FP64):
+    """Marshak wave `problem` (1-4) as RunMarshakWave sets it up
+    (MarshakCommon.hpp:265-320): an nx x 1 x 1 slab (problem 4: the fixed
+    512-cell graded mesh), T0 = 1 eV, the bath on x=0 (packets that reach it
+    escape), the other faces reflecting, Random Walk on with its default
+    thresholds, comb (15, 6).  The time loop and the bath updates are
+    `benchmarks.run_marshak_wave`."""
+    q = MARSHAK_PARAMS[problem]
+    keV = UNITS["kev_kelvin"]
+    x_max = q["x_offset"] + q["length"]
+    if problem == 4:
+        xe = marshak4_edges(q["x_offset"], x_max)
+        dy = x_max / (len(xe) - 1)
+    else:
+        dy = x_max / nx
+        xe = uniform_edges(0.0, x_max, nx)
+    empty = np.zeros(1)
+    p = Problem(xe, uniform_edges(0.0, dy, 1), uniform_edges(0.0, dy, 1), empty, empty, empty)
+    xc, _, _ = p.cell_centers()
+    rho = marshak_density(problem, xc)
+    vol = p.volumes()
+    f = q["f_keV"] / keV ** q["eos_beta"]
+    T0 = 1e-3 * keV
+    p.temperature = np.full(p.ncells, T0)
+    p.internal_energy = f * T0 ** q["eos_beta"] * np.power(rho, 1.0 - q["eos_mu"]) * vol
+    p.cell_internal_energy = p.internal_energy.copy()
+    p.mass = rho * vol
+    p.eos_kind = A.EOS_POWER_LAW
+    p.eos_f, p.eos_beta, p.eos_mu = f, q["eos_beta"], q["eos_mu"]
+    p.opacity_kind = A.OPACITY_POWER_LAW
+    p.kP0, p.kR0, p.alpha, p.t_floor, p.cap = q["kP0"], q["kR0"], q["alpha"], 1.0, 0.0
+    p.density_factor = np.power(rho, q["beta_rho"]) if q["beta_rho"] != 0.0 else None
+    p.faces = [BoxFace(A.FACE_ESCAPE, marshak_bath_temperature(problem, q["initial_dt"]), boundary_per_face)] + \
+              [BoxFace(A.FACE_REFLECT) for _ in range(5)]
+    p.new_photons_per_cell = new_photons_per_cell
+    p.with_random_walk = True
+    p.comb_enabled = True
+    p.comb_nmin, p.comb_factor = 15, 6.0
+    p.seed, p.dt, p.precision, p.name = seed, q["initial_dt"], precision, f"marshak_wave_{problem}"
+    return p
+
+
+def densmore_group_bounds(groups=30):
+    """Group bounds of the Densmore benchmark (examples/densmore2012/main.cpp:151-158):
+    1e-4 keV times ratio^g, ratio = (100 keV / 1e-4 keV)^(1/groups), built by
+    repeated multiplication as there."""
+    kev = UNITS["kev"]
+    e_min, e_max = kev * 1e-4, kev * 1e2
+    ratio = (e_max / e_min) ** (1.0 / groups)
+    b = np.empty(groups + 1)
+    b[0] = e_min
+    for g in range(groups):
+        b[g + 1] = b[g] * ratio
+    return b
+
+
+def densmore2012(nx=512, new_photons_per_cell=16, boundary_per_face=100, seed=42, precision=A.PRECISION_FP64):
+    """Densmore et al. (2012) Fig. 4, as examples/densmore2012/main.cpp:128-208
+    sets it up: x in [0, 3] cm (nx x 1 x 1), sigma(E) = sigma0 / (sqrt(kT) E^3)
+    with sigma0 = 10 keV^3.5/cm below x = 2 and 1000 keV^3.5/cm above, 30
+    groups, cv = 1e15 erg/cm^3/keV, T0 = 1 eV, a 1 keV Planck source on x=0
+    (packets that reach it escape), reflecting elsewhere, Random Walk with its
+    default thresholds, comb (200, 5), dt = 5e-12 s (200 steps to 1 ns)."""
+    keV = UNITS["kev_kelvin"]
+    kev = UNITS["kev"]
+    length = 3.0
+    dy = length / nx
+    empty = np.zeros(1)
+    p = Problem(uniform_edges(0.0, length, nx), uniform_edges(0.0, dy, 1), uniform_edges(0.0, dy, 1),
+                empty, empty, empty)
+    _material(p, keV / 1000.0, CV_PER_VOLUME)
+    xc, _, _ = p.cell_centers()
+    p.opacity_kind = A.OPACITY_MG_POWER
+    p.sigma_a = np.where(xc < 2.0, 10.0 * kev ** 3.5, 1000.0 * kev ** 3.5)
+    p.sigma_s = np.zeros(p.ncells)
+    p.groups = 30
+    p.group_bounds = densmore_group_bounds(30)
+    p.mg_group_constant = False
+    p.mg_p, p.mg_q, p.mg_s = 3.0, 0.5, 0.0
+    p.faces = [BoxFace(A.FACE_ESCAPE, keV, boundary_per_face)] + [BoxFace(A.FACE_REFLECT) for _ in range(5)]
+    p.new_photons_per_cell = new_photons_per_cell
+    p.with_random_walk = True
+    p.comb_enabled = True
+    p.comb_nmin, p.comb_factor = 200, 5.0
+    p.seed, p.dt, p.precision, p.name = seed, 5e-12, precision, "densmore2012"
+    return p

@@ -1,0 +1,96 @@
+"""The reference's full-run benchmarks on the GPU, against the curves the
+reference ships and the gates its regression suite applies
+(regression_tests/lib/regression_checks.sh:73-118):
+
+* Marshak waves 1-4 (gray, power-law opacity and EOS, time-dependent bath):
+  gas-temperature relative L1 against the diffusion profile below 0.10;
+* Densmore et al. 2012 Fig. 4 (30 groups, multigroup Planck face source):
+  gas-temperature L1 against the digitised Milagro curve below 0.10 keV;
+
+in both arithmetic forms, at the examples' default sizes.  Also the face
+source's frequency spectrum against planck_integral, and a short multigroup
+face-driven run against the reference's serial path.
+"""
+import numpy as np
+import pytest
+
+from conftest import golden
+from storm_b200 import _abi as A
+from storm_b200 import benchmarks as B
+from storm_b200 import problems as P
+from storm_b200.engine import Engine
+from storm_b200.units import UNITS
+
+pytestmark = pytest.mark.gpu
+
+FORMS = {"fp64": A.PRECISION_FP64, "fp32": A.PRECISION_FP32_TRACK}
+
+
+@pytest.mark.parametrize("form", sorted(FORMS))
+@pytest.mark.parametrize("problem", [1, 2, 3, 4])
+def test_marshak_wave_against_diffusion_reference(problem, form):
+    res = B.run_marshak_wave(Engine, problem, precision=FORMS[form])
+    l1 = B.marshak_l1(res["x"], res["t_gas"], golden("reference_curves.npz")[f"marshak_wave_{problem}"])
+    print(f"marshak_wave_{problem} {form}: TGAS_REL_L1 = {l1:.4e} over {res['steps']} steps")
+    assert 0.0 <= l1 < 0.10
+
+
+@pytest.mark.parametrize("form", sorted(FORMS))
+def test_densmore2012_against_milagro_curve(form):
+    res = B.run_densmore2012(Engine, precision=FORMS[form])
+    l1 = B.densmore_l1(res["x"], res["t_gas"], golden("reference_curves.npz")["densmore2012"])
+    print(f"densmore2012 {form}: DENSMORE2012_TGAS_L1 = {l1:.4e} keV")
+    assert 0.0 <= l1 < 0.10
+
+
+def test_mg_face_source_spectrum(ref_lib):
+    """Face packets of a multigroup problem: group occupation follows the
+    Planck integrals at the face temperature (chi-square), energies are
+    uniform inside each group."""
+    p = P.densmore2012(nx=8, new_photons_per_cell=1, boundary_per_face=200000)
+    e = Engine(p)
+    e.phase("begin", p.dt)
+    e.phase("prestep", p.dt)
+    e.phase("emit", p.dt)
+    b = e.bank()
+    nf = 200000
+    nu = b.frequency[-nf:]
+    gb = p.group_bounds
+    kT = UNITS["k_boltz"] * p.faces[0].source_temperature
+    prob = np.array([ref_lib.planck_integral(gb[g] / kT, gb[g + 1] / kT) for g in range(p.groups)])
+    prob /= prob.sum()
+    g = np.searchsorted(gb, nu, side="right") - 1
+    assert (g >= 0).all() and (g < p.groups).all()
+    counts = np.bincount(g, minlength=p.groups)
+    expect = nf * prob
+    big = expect > 20
+    chi2 = (((counts - expect) ** 2)[big] / expect[big]).sum()
+    assert chi2 < big.sum() + 6 * np.sqrt(2 * big.sum()), chi2
+    assert counts[~big].sum() < 200
+    frac = (nu - gb[g]) / (gb[g + 1] - gb[g])
+    hist = np.histogram(frac, bins=10, range=(0, 1))[0]
+    assert np.abs(hist - nf / 10).max() < 6 * np.sqrt(nf / 10)
+    e.close()
+
+
+def test_mg_face_driven_steps_vs_reference(ref_lib):
+    """Fifteen steps of a small Densmore slab (30 groups, face source, PGRW) on
+    independent seeds: the GPU and the reference's serial path agree within
+    the seed-to-seed scatter, cell by cell."""
+    def run(make, seeds):
+        out = []
+        for s in seeds:
+            p = P.densmore2012(nx=24, new_photons_per_cell=6, boundary_per_face=200, seed=s)
+            p.comb_nmin = 20
+            m = make(p)
+            for _ in range(15):
+                m.step(p.dt)
+            out.append(m.cells()["temperature"])
+            m.close()
+        return np.array(out)
+    a = run(Engine, range(40, 48))
+    b = run(ref_lib.Reference, range(80, 88))
+    ma, mb = a.mean(0), b.mean(0)
+    se = np.sqrt(a.var(0, ddof=1) / len(a) + b.var(0, ddof=1) / len(b))
+    z = np.abs(ma - mb) / np.maximum(se, 1e-9 * ma)
+    assert (z < 4).mean() > 0.95, np.sort(z)[-10:]
