@@ -98,6 +98,9 @@ struct Ctx {
     const float *gb32;       // FP32-tracking form: bounds and group centres as floats
     const float *gc32;
     const double *faceCdf;   // per box face, groups + 1: cumulative B_g at the face's source temperature
+    const double *mgEp;      // per group: E_g^p at the group centre (host pow, the opacity model's value)
+    const float *mgEp32;     // the same as floats, FP32-tracking form
+    double *mgKTq;           // per cell: (kT)^q, written by the prestep
 };
 
 // ------------------------------------------------------------------ errors
@@ -338,7 +341,11 @@ struct SegmentTally {
 // ------------------------------------------------------------------ multigroup
 // planck_integral(a, b) = 15/pi^4 int_a^b x^3/(e^x - 1) dx from Clark's two
 // published series: the Bernoulli expansion below x = 0.5 and the exponential
-// tail series above; the same evaluation order as the host table build.
+// tail series sum_n e^{-n x} (x^3/n + 3x^2/n^2 + 6x/n^3 + 6/n^4) above, with the
+// host table build's switch point and stopping rule.  On the device the tail's
+// exponentials come by recurrence, e^{-(n+1)x} = e^{-nx} e^{-x}, and each term
+// takes one division; both change the sum by about n ulps (n < 100 terms
+// where x >= 0.5), far inside the 1e-12 the tables are held to.
 constexpr double PI_NORM_PI = 3.14159265358979323846;
 __device__ __forceinline__ double pi_norm() { return 15.0 / (PI_NORM_PI * PI_NORM_PI * PI_NORM_PI * PI_NORM_PI); }
 __device__ inline double pi_small_series(double x) {
@@ -354,26 +361,42 @@ __device__ inline double pi_small_series(double x) {
     return sum;
 }
 __device__ inline double pi_tail_series(double x) {
-    double sum = 0.0;
-    for (int n = 1; n < 100000; ++n) {
-        double e = exp(-n * x);
-        if (e == 0.0) break;
-        double dn = n;
-        double term = e * (x * x * x / dn + 3.0 * x * x / (dn * dn) + 6.0 * x / (dn * dn * dn) + 6.0 / (dn * dn * dn * dn));
+    const double e1 = exp(-x);
+    const double x2 = x * x, x3 = x2 * x;
+    double sum = 0.0, e = e1;
+    for (int n = 1; n < 100000 && e != 0.0; ++n) {
+        const double dn = n;
+        const double d2 = dn * dn;
+        const double term = e * ((((x3 * dn + 3.0 * x2) * dn + 6.0 * x) * dn + 6.0) / (d2 * d2));
         sum += term;
         if (term < 1e-18 * sum) break;
+        e *= e1;
     }
     return sum;
 }
-__device__ inline double pi_cumulative(double x) {
-    if (!(x > 0.0)) return 0.0;
-    if (x < 0.5) return pi_norm() * pi_small_series(x);
-    return 1.0 - pi_norm() * pi_tail_series(x);
+// One group bound's share of planck_integral: the tail sum where x >= 0.5 and
+// the cumulative 15/pi^4 int_0^x.  A table over G groups evaluates each of its
+// G + 1 bounds once instead of twice.
+struct PiBound {
+    double x, tail, cum;
+};
+__device__ inline PiBound pi_bound(double x) {
+    PiBound r{x, 0.0, 0.0};
+    if (!(x > 0.0)) return r;
+    if (x < 0.5) {
+        r.cum = pi_norm() * pi_small_series(x);
+    } else {
+        r.tail = pi_tail_series(x);
+        r.cum = 1.0 - pi_norm() * r.tail;
+    }
+    return r;
 }
-__device__ inline double planck_integral(double a, double b) {
-    if (a >= 0.5 && b >= 0.5) return pi_norm() * (pi_tail_series(a) - pi_tail_series(b));
-    return pi_cumulative(b) - pi_cumulative(a);
+// planck_integral(a, b) from its two bounds (a > 0, b > a)
+__device__ __forceinline__ double pi_between(const PiBound &a, const PiBound &b) {
+    if (a.x >= 0.5 && b.x >= 0.5) return pi_norm() * (a.tail - b.tail);
+    return b.cum - a.cum;
 }
+__device__ inline double planck_integral(double a, double b) { return pi_between(pi_bound(a), pi_bound(b)); }
 
 // std::clamp(nu, b_0, b_G) (RadiationIMC::clampFrequencyToBounds, radiation/RadiationIMC.hpp:869-872)
 __device__ __forceinline__ double mg_clamp(const Ctx &C, double nu) {
@@ -395,23 +418,27 @@ __device__ __forceinline__ double mg_kT(const Ctx &C, uint32_t c) {
     const double T = C.T[c];
     return C.kBoltz * (T < 1.0 ? 1.0 : T);
 }
-// sigma0 / ((kT)^q E^p) (1 - e^{-E/kT})^s
-__device__ __forceinline__ double mg_sigma(const Ctx &C, uint32_t c, double E, double kT) {
-    double v = C.sig0[c] / (pow(kT, C.mgQ) * pow(E, C.mgP));
-    if (C.mgS != 0.0) v *= pow(-expm1(-E / kT), C.mgS);
+// (1 - e^{-E/kT})^s
+__device__ __forceinline__ double mg_stim(const Ctx &C, double E, double kT) {
+    const double x = -expm1(-E / kT);
+    return C.mgS == 1.0 ? x : pow(x, C.mgS);
+}
+// sigma0 / ((kT)^q E^p) (1 - e^{-E/kT})^s with (kT)^q = kTq and E^p = Ep given
+__device__ __forceinline__ double mg_sigma(const Ctx &C, uint32_t c, double E, double kT, double kTq, double Ep) {
+    double v = C.sig0[c] / (kTq * Ep);
+    if (C.mgS != 0.0) v *= mg_stim(C, E, kT);
     return v;
 }
-// CalcAbsorptionOpacity(cell, frequency)
+// CalcAbsorptionOpacity(cell, frequency); (kT)^q comes from the cell's prestep
+// value, E^p from the per-group table when the opacity is taken at the group centre
 __device__ __forceinline__ double mg_absorption(const Ctx &C, uint32_t c, double nu) {
     const double kT = mg_kT(C, c);
-    double E;
     if (C.mgGroupConst) {
         const uint32_t g = mg_find_group(C, nu);
-        E = 0.5 * (C.gb[g] + C.gb[g + 1]);
-    } else {
-        E = nu < C.gb[0] ? C.gb[0] : nu;
+        return mg_sigma(C, c, 0.5 * (C.gb[g] + C.gb[g + 1]), kT, C.mgKTq[c], C.mgEp[g]);
     }
-    return mg_sigma(C, c, E, kT);
+    const double E = nu < C.gb[0] ? C.gb[0] : nu;
+    return mg_sigma(C, c, E, kT, C.mgKTq[c], pow(E, C.mgP));
 }
 // GetThermalEnergy (examples/densmore2012/DensmoreOpacity.hpp:71-82): the
 // inverse of the cell's cumulative sigma_g B_g by STORM::LinearInterpolation
@@ -874,9 +901,10 @@ __device__ inline int rw_jump32(const Ctx &C, Track32 &T, RNG &rng, TALLY &tal, 
     return ev == 1 ? OUT_CENSUS : OUT_CONTINUE;
 }
 
-// Multigroup absorption opacity in FP32 from the cell's cached kT and sigma0.
+// Multigroup absorption opacity in FP32 from the cell's cached kT and
+// sigma0 / (kT)^q: at the group centre E_g^p comes from the per-group table.
 __device__ __forceinline__ float mg_absorption32(const Ctx &C, const Track32 &T, float nu) {
-    float E;
+    float E, v;
     if (C.mgGroupConst) {
         uint32_t lo = 0, hi = C.groups - 1;
         while (lo < hi) {
@@ -884,11 +912,15 @@ __device__ __forceinline__ float mg_absorption32(const Ctx &C, const Track32 &T,
             if (nu < C.gb32[mid + 1]) hi = mid; else lo = mid + 1;
         }
         E = C.gc32[lo];
+        v = T.s0 / C.mgEp32[lo];
     } else {
         E = fmaxf(nu, C.gb32[0]);
+        v = T.s0 / __powf(E, static_cast<float>(C.mgP));
     }
-    float v = T.s0 / (__powf(T.kT, static_cast<float>(C.mgQ)) * __powf(E, static_cast<float>(C.mgP)));
-    if (C.mgS != 0.0) v *= __powf(-expm1f(-E / T.kT), static_cast<float>(C.mgS));
+    if (C.mgS != 0.0) {
+        const float x = -expm1f(-E / T.kT);
+        v *= (C.mgS == 1.0) ? x : __powf(x, static_cast<float>(C.mgS));
+    }
     return v;
 }
 
@@ -910,7 +942,7 @@ __device__ inline int segment32(const Ctx &C, Track32 &T, RNG &rng, TALLY &tal, 
         T.cc = cell;
         if (MG) {
             T.kT = static_cast<float>(mg_kT(C, cell));
-            T.s0 = static_cast<float>(C.sig0[cell]);
+            T.s0 = static_cast<float>(C.sig0[cell] / C.mgKTq[cell]);   // sigma0 / (kT)^q
         }
     }
     const float hx = T.hx, hy = T.hy, hz = T.hz;

@@ -314,12 +314,17 @@ __device__ inline double mg_cell_tables(const Ctx &C, const CellArrays &A, uint3
     uint32_t cutoff = 0;
     bool foundNonDiffusive = false;
     cdf[0] = 0.0;
+    const double kTq = pow(kT, C.mgQ);   // the same in every group
+    C.mgKTq[c] = kTq;
+    PiBound lo = pi_bound(C.gb[0] / kT);
     for (uint32_t g = 0; g < G; ++g) {
         const double b0 = C.gb[g], b1 = C.gb[g + 1];
         const double Ec = 0.5 * (b0 + b1);
-        const double a = b0 / kT, b = b1 / kT;
-        const double Bg = (a > 0.0 && b > a) ? planck_integral(a, b) : 0.0;
-        const double sg = mg_sigma(C, c, Ec, kT);   // = CalcAbsorptionOpacity(cell, centre of g)
+        const PiBound hi = pi_bound(b1 / kT);
+        const double a = lo.x, b = hi.x;   // b0 / kT, b1 / kT
+        const double Bg = (a > 0.0 && b > a) ? pi_between(lo, hi) : 0.0;
+        lo = hi;
+        const double sg = mg_sigma(C, c, Ec, kT, kTq, C.mgEp[g]);   // = CalcAbsorptionOpacity(cell, centre of g)
         weightedSum += sg * Bg;
         totalWeight += Bg;
         const double weight = (sg > 0.0 && isfinite(sg) && isfinite(Bg)) ? sg * Bg : 0.0;

@@ -56,6 +56,8 @@ struct StormHandle {
     double *gb = nullptr;            // multigroup bounds
     float *gb32 = nullptr, *gc32 = nullptr;   // multigroup bounds and centres, FP32-tracking form
     double *faceCdf = nullptr;                // multigroup: 6 x (groups + 1) face Planck spectra
+    double *mgEp = nullptr, *mgKTq = nullptr; // multigroup: E_g^p per group, (kT)^q per cell
+    float *mgEp32 = nullptr;
     double faceCdfT[6] = {-1, -1, -1, -1, -1, -1};   // face temperatures the spectra were built for
     // face sources
     uint32_t *fsCell = nullptr;
@@ -720,6 +722,21 @@ int storm_cuda_create(const StormProblemDesc *d, StormHandle **out) {
         ALLOC(A.pgrw, N);
         ALLOC(A.pgrwCut, N);
         ALLOC(h->faceCdf, 6 * (static_cast<size_t>(G) + 1));
+        ALLOC(h->mgKTq, N);
+        {
+            // E^p at each group centre with the host's pow, as the opacity
+            // model evaluates CalcAbsorptionOpacity there
+            std::vector<double> ep(G);
+            std::vector<float> ep32(G);
+            for (uint32_t g = 0; g < G; ++g) {
+                ep[g] = std::pow(0.5 * (d->group_bounds[g] + d->group_bounds[g + 1]), d->mg_p);
+                ep32[g] = static_cast<float>(ep[g]);
+            }
+            ALLOC(h->mgEp, G);
+            ALLOC(h->mgEp32, G);
+            H2D(h->mgEp, ep.data(), G);
+            H2D(h->mgEp32, ep32.data(), G);
+        }
         if (cudaMemset(A.pgrwCut, 0, N * sizeof(uint32_t)) != cudaSuccess) return fail(STORM_ERR_CUDA);
         C.groups = G;
         C.mgGroupConst = d->mg_group_constant;
@@ -729,6 +746,7 @@ int storm_cuda_create(const StormProblemDesc *d, StormHandle **out) {
         C.sig0 = h->tabA;
         C.mgCdf = A.mgCdf; C.pgrw = A.pgrw; C.pgrwCut = A.pgrwCut;
         C.faceCdf = h->faceCdf;
+        C.mgEp = h->mgEp; C.mgEp32 = h->mgEp32; C.mgKTq = h->mgKTq;
         if (h->fp32) {
             std::vector<float> b32(G + 1), c32(G);
             for (uint32_t g = 0; g <= G; ++g) b32[g] = static_cast<float>(d->group_bounds[g]);
@@ -788,7 +806,7 @@ int storm_cuda_destroy(StormHandle *h) {
                   h->A.rwElig, h->A.photons, h->A.phys, h->A.phys32, h->hx, h->hy, h->hz, h->segs, h->tabA, h->tabS, h->rhoF, h->rwTau, h->rwLogTau, h->rwSurv,
                   h->rwRadius, h->rwLogTau32, h->rwSurv32, h->rwRadius32, h->fsCell, h->fsSide, h->fsOffset, h->dAmbiguous, h->offsets, h->tileSums, h->dTotalU64, h->dTotalE, h->combW, h->combWtot,
                   h->combStart, h->combCount, h->counts, h->dStats, h->dErr, h->gb, h->A.mgCdf, h->A.pgrw,
-                  h->A.pgrwCut, h->gb32, h->gc32, h->faceCdf};
+                  h->A.pgrwCut, h->gb32, h->gc32, h->faceCdf, h->mgEp, h->mgEp32, h->mgKTq};
     for (void *p : ps) device_pool().free(p);
     cudaEvent_t evs[] = {h->evStart, h->evTransport0, h->evTransport1, h->evEnd, h->evAfterEmit, h->evAfterComb};
     for (cudaEvent_t e : evs)
