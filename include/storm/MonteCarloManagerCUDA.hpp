@@ -14,8 +14,10 @@
 // What the plug-ins keep private -- the opacity and EOS models, a boundary's
 // temperatures, the comb's Nmin / factor, the RNG seed, and the cell vectors
 // RadiationIMC holds by reference -- is handed over in a CudaIMCBinding.
-// bind_parameters() copies the public RadiationIMCParameters.  An unsupported
-// plug-in is rejected with StormError; there is no CPU fallback.
+// bind_parameters() copies the public RadiationIMCParameters, the group energy
+// boundaries of a multigroup RadiationIMC included; census frequencies travel
+// with the particles.  An unsupported plug-in is rejected with StormError;
+// there is no CPU fallback.
 //
 // Include after the reference headers (Particle, MonteCarloPhysics,
 // PopulationControl, BoundaryCondition, MonteCarloConfig, RadiationCell).
@@ -50,13 +52,19 @@ struct CudaIMCBinding {
     std::function<double(std::size_t)> scatteringOpacity;   // CELL_TABLE: sigma_s of cell i (empty = 0)
     double kP0 = 0, kR0 = 0, alpha = 0, beta = 0, tFloor = 1.0, cap = 0;
     std::vector<double> densityFactor;                        // POWER_LAW: rho^beta per cell
+    // MG_POWER (RadiationIMC<..., NumGroups> with withMultigroupOpacity):
+    // sigma(E, T) = sigma0 / ((kT)^q E^p) (1 - e^{-E/kT})^s, kT = kBoltz max(T, 1 K)
+    std::function<double(std::size_t)> sigma0;              // sigma0 of cell i
+    std::vector<double> groupBounds;                          // NumGroups + 1 energies (bind_parameters copies them)
+    double mgP = 3.0, mgQ = 0.0, mgS = 0.0, kBoltz = 0.0;
+    bool mgGroupConstant = false;                             // opacity at the centre of the particle's group
     // EOS plug-in
     int eosKind = STORM_EOS_LINEAR;
     double cvPerMass = 1.0, eosF = 1.0, eosBeta = 1.0, eosMu = 0.0;
     // boundary plug-in as per-box-face actions, GetBoxFaces() order
     std::array<StormBoxFace, 6> faces{};
     bool escapeWithoutCheck = false;
-    // RadiationIMCParameters<1> (copy with bind_parameters)
+    // RadiationIMCParameters<NumGroups> (copy with bind_parameters)
     std::size_t newPhotonsPerCell = 1;
     bool withRandomWalk = false, noHydroFeedback = false;
     double rwMinCellOpticalDepth = 25.0, rwMinParticleOpticalDepth = 5.0;
@@ -79,12 +87,20 @@ struct CudaIMCBinding {
         noHydroFeedback = p.noHydroFeedback;
         rwMinCellOpticalDepth = p.rwMinCellOpticalDepth;
         rwMinParticleOpticalDepth = p.rwMinParticleOpticalDepth;
-        if (p.withHydro || p.withMultigroupOpacity || p.withDDMC || p.MMC || p.withCompton) {
+        if (p.withHydro || p.withDDMC || p.MMC || p.withCompton) {
             StormError eo("MonteCarloManagerCUDA: RadiationIMC option not supported on the device path");
             eo.addEntry("withHydro", p.withHydro);
-            eo.addEntry("withMultigroupOpacity", p.withMultigroupOpacity);
             eo.addEntry("withDDMC", p.withDDMC);
+            eo.addEntry("MMC", p.MMC);
+            eo.addEntry("withCompton", p.withCompton);
             throw eo;
+        }
+        groupBounds.clear();
+        if (p.withMultigroupOpacity) {
+            if (!p.energyBoundariesProvided || p.energyBoundaries.size() < 3)
+                throw StormError("MonteCarloManagerCUDA: multigroup opacity needs the group energy boundaries");
+            groupBounds.assign(p.energyBoundaries.begin(), p.energyBoundaries.end());
+            opacityKind = STORM_OPACITY_MG_POWER;
         }
     }
 };
@@ -255,6 +271,23 @@ private:
             }
             d.sigma_a = sa.data();
             d.sigma_s = ss.data();
+        } else if (binding_.opacityKind == STORM_OPACITY_MG_POWER) {
+            if (!binding_.sigma0 || binding_.groupBounds.size() < 3 || !(binding_.kBoltz > 0.0))
+                throw StormError("MonteCarloManagerCUDA: MG_POWER opacity needs sigma0, the group bounds and kBoltz");
+            sa.resize(N);
+            ss.assign(N, 0.0);
+            for (std::size_t i = 0; i < N; ++i) {
+                sa[i] = binding_.sigma0(i);
+                if (binding_.scatteringOpacity) ss[i] = binding_.scatteringOpacity(i);
+            }
+            d.sigma_a = sa.data();
+            d.sigma_s = ss.data();
+            d.groups = static_cast<std::uint32_t>(binding_.groupBounds.size() - 1);
+            d.group_bounds = binding_.groupBounds.data();
+            d.mg_p = binding_.mgP; d.mg_q = binding_.mgQ; d.mg_s = binding_.mgS;
+            d.mg_group_constant = binding_.mgGroupConstant;
+            d.k_boltz = binding_.kBoltz;
+            multigroup_ = true;
         }
         d.kP0 = binding_.kP0; d.kR0 = binding_.kR0; d.alpha = binding_.alpha; d.beta = binding_.beta;
         d.t_floor = binding_.tFloor;
@@ -300,7 +333,7 @@ private:
 
     void upload_census(const std::vector<MCParticle> &ps) {
         const std::size_t n = ps.size();
-        std::vector<double> x(n), y(n), z(n), vx(n), vy(n), vz(n), t(n), w(n), w0(n);
+        std::vector<double> x(n), y(n), z(n), vx(n), vy(n), vz(n), t(n), w(n), w0(n), nu(multigroup_ ? n : 0);
         std::vector<std::uint32_t> cell(n);
         for (std::size_t q = 0; q < n; ++q) {
             const MCParticle &p = ps[q];
@@ -308,20 +341,21 @@ private:
             vx[q] = p.velocity.x; vy[q] = p.velocity.y; vz[q] = p.velocity.z;
             t[q] = p.timeLeft; w[q] = p.weight; w0[q] = p.initialWeight;
             cell[q] = static_cast<std::uint32_t>(p.cellIndex);
+            if (multigroup_) nu[q] = p.frequency;
         }
         StormParticlesSoA s{x.data(), y.data(), z.data(), vx.data(), vy.data(), vz.data(), t.data(), w.data(),
-                            w0.data(), cell.data(), nullptr, n};
+                            w0.data(), cell.data(), nullptr, n, multigroup_ ? nu.data() : nullptr};
         cuda_detail::check(storm_cuda_set_census(h_, &s), h_, "set_census");
     }
 
     std::vector<MCParticle> download_census() {
         std::uint64_t n = 0;
         cuda_detail::check(storm_cuda_census_count(h_, &n), h_, "census_count");
-        std::vector<double> x(n), y(n), z(n), vx(n), vy(n), vz(n), t(n), w(n), w0(n);
+        std::vector<double> x(n), y(n), z(n), vx(n), vy(n), vz(n), t(n), w(n), w0(n), nu(multigroup_ ? n : 0);
         std::vector<std::uint32_t> cell(n);
         std::vector<std::uint64_t> id(n);
         StormParticlesSoA s{x.data(), y.data(), z.data(), vx.data(), vy.data(), vz.data(), t.data(), w.data(),
-                            w0.data(), cell.data(), id.data(), n};
+                            w0.data(), cell.data(), id.data(), n, multigroup_ ? nu.data() : nullptr};
         std::uint64_t got = 0;
         cuda_detail::check(storm_cuda_get_census(h_, &s, n, &got), h_, "get_census");
         std::vector<MCParticle> out(n);
@@ -331,7 +365,7 @@ private:
             p.velocity = T(vx[q], vy[q], vz[q]);
             p.timeLeft = t[q]; p.weight = w[q]; p.initialWeight = w0[q];
             p.cellIndex = cell[q];
-            p.frequency = 0;
+            p.frequency = multigroup_ ? nu[q] : 0.0;
             p.id = std::numeric_limits<std::size_t>::max();   // ids are reassigned at the next step, as comb copies are
         }
         return out;
@@ -365,6 +399,7 @@ private:
     MonteCarloConfig config_;
     StormHandle *h_ = nullptr;
     std::size_t N_ = 0;
+    bool multigroup_ = false;
     std::vector<std::size_t> cellsStepsCounters_;
     std::vector<double> hostT_, hostE_, hostCE_, eradAvg_, sigmaA_, fleck_;
     std::size_t startParticleCount_ = 0, initialParticleCount_ = 0, preStepParticleCount_ = 0, endParticleCount_ = 0;

@@ -16,6 +16,23 @@ struct DropinHandle {
     std::string lastError;
 };
 
+// RadiationIMCParameters<G> as ref_create builds them, through bind_parameters
+template <std::size_t G>
+void bind_imc(STORM::CudaIMCBinding<Cell, Ext> &b, const StormProblemDesc *d) {
+    STORM::RadiationIMCParameters<G> p;
+    p.newPhotonsPerCell = d->new_photons_per_cell;
+    p.withRandomWalk = d->with_random_walk != 0;
+    p.rwMinCellOpticalDepth = d->rw_min_cell_optical_depth;
+    p.rwMinParticleOpticalDepth = d->rw_min_particle_optical_depth;
+    p.noHydroFeedback = d->no_hydro_feedback != 0;
+    if constexpr (G > 1) {
+        p.withMultigroupOpacity = true;
+        for (std::size_t g = 0; g <= G; ++g) p.energyBoundaries[g] = d->group_bounds[g];
+        p.energyBoundariesProvided = true;
+    }
+    b.bind_parameters(p);
+}
+
 extern "C" {
 
 DropinHandle *dropin_create(const StormProblemDesc *d, int precision, char *err, size_t errlen) {
@@ -29,11 +46,18 @@ DropinHandle *dropin_create(const StormProblemDesc *d, int precision, char *err,
         b.cells = &ref->cells;
         b.extensives = &ref->ext;
         b.opacityKind = d->opacity_kind;
-        if (d->opacity_kind == STORM_OPACITY_CELL_TABLE) {
+        if (d->opacity_kind == STORM_OPACITY_CELL_TABLE || d->opacity_kind == STORM_OPACITY_MG_POWER) {
             h->sigA.assign(d->sigma_a, d->sigma_a + N);
             h->sigS = d->sigma_s ? std::vector<double>(d->sigma_s, d->sigma_s + N) : std::vector<double>(N, 0.0);
             const std::vector<double> *sa = &h->sigA, *ss = &h->sigS;
-            b.planckOpacity = [sa](std::size_t i) { return (*sa)[i]; };
+            if (d->opacity_kind == STORM_OPACITY_MG_POWER) {
+                b.sigma0 = [sa](std::size_t i) { return (*sa)[i]; };
+                b.mgP = d->mg_p; b.mgQ = d->mg_q; b.mgS = d->mg_s;
+                b.mgGroupConstant = d->mg_group_constant != 0;
+                b.kBoltz = d->k_boltz;
+            } else {
+                b.planckOpacity = [sa](std::size_t i) { return (*sa)[i]; };
+            }
             b.scatteringOpacity = [ss](std::size_t i) { return (*ss)[i]; };
         } else {
             b.kP0 = d->kP0; b.kR0 = d->kR0; b.alpha = d->alpha; b.beta = d->beta; b.tFloor = d->t_floor;
@@ -45,13 +69,9 @@ DropinHandle *dropin_create(const StormProblemDesc *d, int precision, char *err,
         b.eosF = d->eos_f; b.eosBeta = d->eos_beta; b.eosMu = d->eos_mu;
         for (int f = 0; f < 6; ++f) b.faces[f] = d->faces[f];
         b.escapeWithoutCheck = d->escape_without_check != 0;
-        STORM::RadiationIMCParameters<1> p;
-        p.newPhotonsPerCell = d->new_photons_per_cell;
-        p.withRandomWalk = d->with_random_walk != 0;
-        p.rwMinCellOpticalDepth = d->rw_min_cell_optical_depth;
-        p.rwMinParticleOpticalDepth = d->rw_min_particle_optical_depth;
-        p.noHydroFeedback = d->no_hydro_feedback != 0;
-        b.bind_parameters(p);
+        if (d->groups == kMGGroupsA) bind_imc<kMGGroupsA>(b, d);
+        else if (d->groups == kMGGroupsB) bind_imc<kMGGroupsB>(b, d);
+        else bind_imc<1>(b, d);
         b.combEnabled = d->comb_enabled != 0;
         b.combNmin = d->comb_nmin;
         b.combFactor = d->comb_factor;

@@ -9,6 +9,8 @@ cells, RadiationIMC, comb and boundary objects (oracle/_ref/libstormdropin.so).
 * test_dropin_vs_serial_manager: the drop-in and the reference's serial manager
   on the same problem, different random streams: temperatures agree within
   the seed-to-seed scatter; energy bookkeeping of the drop-in closes.
+Both run gray problems and a 30-group multigroup problem (RadiationIMC<..., 30>,
+census frequencies carried through the template).
 """
 import ctypes as C
 import os
@@ -100,13 +102,16 @@ def _close(a, b, rel, atol=1e-300):
     return np.abs(a - b) <= rel * np.maximum(np.abs(a), np.abs(b)) + atol
 
 
-@pytest.mark.parametrize("kind", ["slab", "cube"])
+@pytest.mark.parametrize("kind", ["slab", "cube", "multigroup"])
 def test_dropin_matches_engine(kind):
     L = _lib()
     if kind == "slab":
         p = problems.gray_slab(new_photons_per_cell=5, face_packets=2000, comb_nmin=50)
-    else:
+    elif kind == "cube":
         p = problems.step_cube(n=12, new_photons_per_cell=3, face_packets=60, comb_nmin=10)
+    else:   # RadiationIMC<..., 30> with multigroup opacity and a Planck face source
+        p = problems.densmore2012(nx=16, new_photons_per_cell=4, boundary_per_face=50)
+        p.comb_nmin = 10
     d = DropIn(L, p)
     e = Engine(p)
     try:
@@ -131,7 +136,10 @@ def test_dropin_matches_engine(kind):
             pd, pe = d.census(), e.census()
             assert pd.n == pe.n
             np.testing.assert_array_equal(pd.cell, pe.cell)
-            for f in ("x", "y", "z", "vx", "vy", "vz", "time_left", "weight", "initial_weight") if pd.n else ():
+            fields = ["x", "y", "z", "vx", "vy", "vz", "time_left", "weight", "initial_weight"]
+            if p.groups:
+                fields.append("frequency")
+            for f in fields if pd.n else ():
                 ok = _close(getattr(pd, f), getattr(pe, f), 1e-12, atol=1e-15 if f in "xyz" else 1e-300)
                 assert ok.mean() > 0.999, (s, f, (~ok).sum())
     finally:
@@ -139,16 +147,24 @@ def test_dropin_matches_engine(kind):
         e.close()
 
 
-def test_dropin_vs_serial_manager():
+@pytest.mark.parametrize("kind", ["cube", "multigroup"])
+def test_dropin_vs_serial_manager(kind):
     L = _lib()
     from oracle import ref
+
+    def make_problem(s):
+        if kind == "cube":
+            return problems.step_cube(n=8, new_photons_per_cell=4, face_packets=80, comb_nmin=20, seed=s)
+        p = problems.densmore2012(nx=24, new_photons_per_cell=6, boundary_per_face=200, seed=s)
+        p.comb_nmin = 20
+        return p
 
     def run(make, seeds):
         out = []
         for s in seeds:
-            p = problems.step_cube(n=8, new_photons_per_cell=4, face_packets=80, comb_nmin=20, seed=s)
+            p = make_problem(s)
             m = make(p)
-            for _ in range(4):
+            for _ in range(4 if kind == "cube" else 12):
                 m.step()
             out.append(m.cells()["temperature"])
             m.close()
