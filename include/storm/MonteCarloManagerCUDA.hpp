@@ -68,6 +68,8 @@ struct CudaIMCBinding {
     std::size_t newPhotonsPerCell = 1;
     bool withRandomWalk = false, noHydroFeedback = false;
     double rwMinCellOpticalDepth = 25.0, rwMinParticleOpticalDepth = 5.0;
+    bool withDDMC = false, ddmcUseMultigroupPGRW = false;
+    double ddmcMinCellOpticalDepth = 15.0, ddmcMinParticleOpticalDepth = 5.0;
     // CombPopulationControl(grid, Nmin, factor)
     bool combEnabled = true;
     std::size_t combNmin = 20;
@@ -87,10 +89,13 @@ struct CudaIMCBinding {
         noHydroFeedback = p.noHydroFeedback;
         rwMinCellOpticalDepth = p.rwMinCellOpticalDepth;
         rwMinParticleOpticalDepth = p.rwMinParticleOpticalDepth;
-        if (p.withHydro || p.withDDMC || p.MMC || p.withCompton) {
+        withDDMC = p.withDDMC;
+        ddmcUseMultigroupPGRW = p.ddmcUseMultigroupPGRW;
+        ddmcMinCellOpticalDepth = p.ddmcMinCellOpticalDepth;
+        ddmcMinParticleOpticalDepth = p.ddmcMinParticleOpticalDepth;
+        if (p.withHydro || p.MMC || p.withCompton) {
             StormError eo("MonteCarloManagerCUDA: RadiationIMC option not supported on the device path");
             eo.addEntry("withHydro", p.withHydro);
-            eo.addEntry("withDDMC", p.withDDMC);
             eo.addEntry("MMC", p.MMC);
             eo.addEntry("withCompton", p.withCompton);
             throw eo;
@@ -303,6 +308,10 @@ private:
         d.no_hydro_feedback = binding_.noHydroFeedback;
         d.rw_min_cell_optical_depth = binding_.rwMinCellOpticalDepth;
         d.rw_min_particle_optical_depth = binding_.rwMinParticleOpticalDepth;
+        d.with_ddmc = binding_.withDDMC;
+        d.ddmc_use_multigroup_pgrw = binding_.ddmcUseMultigroupPGRW;
+        d.ddmc_min_cell_optical_depth = binding_.ddmcMinCellOpticalDepth;
+        d.ddmc_min_particle_optical_depth = binding_.ddmcMinParticleOpticalDepth;
         d.comb_enabled = binding_.combEnabled;
         d.comb_nmin = binding_.combNmin;
         d.comb_factor = binding_.combFactor;

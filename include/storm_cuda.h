@@ -36,7 +36,7 @@
 extern "C" {
 #endif
 
-#define STORM_CUDA_ABI_VERSION 3
+#define STORM_CUDA_ABI_VERSION 4
 
 /* ---------------------------------------------------------------- status */
 enum StormStatus {
@@ -181,6 +181,14 @@ typedef struct StormProblemDesc {
     const double *group_bounds;      /* G+1 increasing energies [erg] (energyBoundaries) */
     double mg_p, mg_q, mg_s;         /* STORM_OPACITY_MG_POWER exponents */
     double k_boltz;                  /* erg/K, for kT */
+
+    /* ---- DDMC-style leakage in optically thick cells (RadiationIMCParameters
+     * withDDMC, ddmcMinCellOpticalDepth, ddmcMinParticleOpticalDepth,
+     * ddmcUseMultigroupPGRW; radiation/RadiationIMC.hpp:1282-1612) */
+    int32_t with_ddmc;
+    int32_t ddmc_use_multigroup_pgrw;
+    double ddmc_min_cell_optical_depth;      /* reference default 15 */
+    double ddmc_min_particle_optical_depth;  /* reference default 5 */
 } StormProblemDesc;
 
 /* Particle arrays, struct-of-arrays.  Mirrors the fields of

@@ -369,6 +369,7 @@ public:
         r.ematBefore = (*ext)[c].internal_energy;
         std::mt19937_64 snap = *opac->captured;
         std::size_t rwBefore = this->getRandomWalkStepCount();
+        std::size_t ddmcBefore = this->getDDMCStepCount();
         Functionality res = Base::step(p, add);
         std::mt19937_64 counter = snap;
         uint32_t n = 0;
@@ -388,7 +389,8 @@ public:
         r.nextCell = res.nextCellIndex;
         r.eradAfter = this->getEradTimeAvg()[c];
         r.ematAfter = (*ext)[c].internal_energy;
-        r.usedRW = this->getRandomWalkStepCount() != rwBefore;
+        // 1: a Random Walk jump, 2: a DDMC step (tryDDMCStep took the segment)
+        r.usedRW = (this->getRandomWalkStepCount() != rwBefore) ? 1 : (this->getDDMCStepCount() != ddmcBefore ? 2 : 0);
         rs.records.push_back(r);
         return res;
     }
@@ -488,6 +490,10 @@ void build_physics(RefHandle &h, const StormProblemDesc *d) {
     p.rwMinCellOpticalDepth = d->rw_min_cell_optical_depth;
     p.rwMinParticleOpticalDepth = d->rw_min_particle_optical_depth;
     p.noHydroFeedback = d->no_hydro_feedback != 0;
+    p.withDDMC = d->with_ddmc != 0;
+    p.ddmcUseMultigroupPGRW = d->ddmc_use_multigroup_pgrw != 0;
+    p.ddmcMinCellOpticalDepth = d->ddmc_min_cell_optical_depth;
+    p.ddmcMinParticleOpticalDepth = d->ddmc_min_particle_optical_depth;
     auto physics = std::make_shared<RecordingIMC<G>>(*h.grid, h.boundary, h.cells, h.ext, h.eos, opacity, p,
                                                      STORM::DirectRadiationIMCTraits<Vector3D, Cell, Ext, G>(),
                                                      RandomInCellPositionSampler<Vector3D, Grid>(), d->seed);

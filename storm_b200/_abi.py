@@ -5,7 +5,7 @@ sizes against the compiled library.
 """
 import ctypes as C
 
-ABI_VERSION = 3
+ABI_VERSION = 4
 
 STORM_OK = 0
 STATUS_NAMES = {
@@ -70,6 +70,8 @@ class StormProblemDesc(C.Structure):
         ("per_cell_segment_counters", C.c_int32), ("device", C.c_int32),
         ("groups", C.c_uint32), ("mg_group_constant", C.c_int32), ("group_bounds", _dp),
         ("mg_p", C.c_double), ("mg_q", C.c_double), ("mg_s", C.c_double), ("k_boltz", C.c_double),
+        ("with_ddmc", C.c_int32), ("ddmc_use_multigroup_pgrw", C.c_int32),
+        ("ddmc_min_cell_optical_depth", C.c_double), ("ddmc_min_particle_optical_depth", C.c_double),
     ]
 
 

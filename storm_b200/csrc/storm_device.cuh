@@ -101,6 +101,16 @@ struct Ctx {
     const double *mgEp;      // per group: E_g^p at the group centre (host pow, the opacity model's value)
     const float *mgEp32;     // the same as floats, FP32-tracking form
     double *mgKTq;           // per cell: (kT)^q, written by the prestep
+    // DDMC-style leakage (RadiationIMCParameters::withDDMC)
+    int32_t withDDMC;
+    int32_t ddmcPgrw;        // ddmcUseMultigroupPGRW with a multigroup opacity
+    double ddmcMinParticle, ddmcMinCell;
+    double4 *ddmc;           // per cell: sigma_T, sigma_A, eligible (1/0), D  (prestep)
+    double *ddmcTot;         // per cell: total leak rate [1/s], 0 where not eligible
+    double *ddmcRate;        // per cell x 6 faces in GetCellFaces order: leak rate, 0 where none
+    uint32_t *ddmcCut;       // per cell: group cutoff (multigroup PGRW form)
+    float4 *ddmc32;          // FP32 form, 3 per cell: (reach, 1/total, sigma_A f c, frequency bound),
+                             // (cumulative face fractions 0-3), (fractions 4-5, last leak face, 0)
 };
 
 // ------------------------------------------------------------------ errors
@@ -576,6 +586,109 @@ __device__ inline int try_random_walk(const Ctx &C, PartReg &p, RNG &rng, TALLY 
 }
 
 // ------------------------------------------------------------------ physics step
+// RadiationIMC::tryDDMCStep (radiation/RadiationIMC.hpp:1416-1612) on a
+// Cartesian cell.  Returns -1 when the step is not taken (no draws consumed),
+// else the ParticleStatus; a leak sets face and next.  precomputeDDMCData sets
+// gamma = 1 in both of its branches, so the upscatter rate is always zero and
+// every event that is not census leaks through a face.
+template <class RNG, class TALLY>
+__device__ inline int try_ddmc(const Ctx &C, PartReg &p, RNG &rng, TALLY &tal, double xl, double xh, double yl,
+                               double yh, double zl, double zh, int &face, uint32_t &next) {
+    const uint32_t cell = p.cell;
+    const double total = C.ddmcTot[cell];
+    if (!(total > 0.0)) return -1;
+    const double4 dd = C.ddmc[cell];   // sigma_T, sigma_A, -, D
+    double d[6] = {p.x - xl, xh - p.x, p.y - yl, yh - p.y, p.z - zl, zh - p.z};
+    double Ro = DBL_MAX;
+#pragma unroll
+    for (int s = 0; s < 6; ++s) Ro = (d[s] < Ro) ? d[s] : Ro;
+    Ro = (Ro > 0.0) ? Ro : 0.0;
+    if (Ro * dd.x < C.ddmcMinParticle) return -1;
+    if (C.ddmcPgrw) {
+        const uint32_t cut = C.ddmcCut[cell];
+        if (cut == 0 || cut > C.groups) return -1;
+        if (mg_clamp(C, p.nu) >= C.gb[cut]) return -1;
+    }
+    const double f = C.fleck[cell];
+    const double eventRate = total;
+    const double tEvent = -log(rng.open()) / eventRate;
+    const double tCensus = p.t;
+    const double dt = (tCensus < tEvent) ? tCensus : tEvent;   // std::min(tEvent, tCensus)
+    const bool censusEvent = (tCensus <= tEvent);
+    const double absRate = dd.y * f * C.clight;
+    const double oldWeight = p.w;
+    const double expFactor = expm1(-dt * absRate);
+    if (!C.noFeedback) tal.mat(cell, -expFactor * oldWeight);
+    const double integrated = (absRate > 0.0) ? oldWeight * expFactor * (-1.0 / absRate) : oldWeight * dt;
+    tal.rad(cell, integrated);
+    p.w *= 1.0 + expFactor;
+    p.t -= dt;
+    if (fabs(p.w) < p.w0 * 1e-3) {
+        if (!C.noFeedback) tal.mat(cell, p.w);
+        return REMOVE;
+    }
+    if (censusEvent) return DONE;
+    const double eventPick = rng.open() * eventRate;
+    if (!(eventPick <= total)) return DONE;   // the upscatter branch; unreachable with a zero upscatter rate
+    // the leak face: subtract the face rates in GetCellFaces order
+    double facePick = rng.open() * total;
+    const double *rates = C.ddmcRate + static_cast<size_t>(cell) * 6;
+    int chosen = -1, last = -1;
+#pragma unroll
+    for (int s = 0; s < 6; ++s) {
+        const double r = rates[s];
+        if (!(r > 0.0) || chosen >= 0) continue;
+        last = s;
+        facePick -= r;
+        if (facePick <= 0.0) chosen = s;
+    }
+    if (chosen < 0) chosen = last;
+    if (chosen < 0) return DONE;
+    uint32_t i, j, k;
+    cell_ijk(C, cell, i, j, k);
+    const int axis = chosen >> 1, hi = chosen & 1;
+    // FaceCM: the face plane's coordinate, the cell's centre along the other axes
+    double fc[3] = {C.xc[i], C.yc[j], C.zc[k]};
+    fc[axis] = (axis == 0) ? (hi ? xh : xl) : (axis == 1 ? (hi ? yh : yl) : (hi ? zh : zl));
+    // Normal(face) is the +axis unit vector; flipped to point at the neighbour
+    double n[3] = {axis == 0 ? 1.0 : 0.0, axis == 1 ? 1.0 : 0.0, axis == 2 ? 1.0 : 0.0};
+    if (!hi) { n[0] = n[0] * (-1.0); n[1] = n[1] * (-1.0); n[2] = n[2] * (-1.0); }
+    const double PI_D = 3.14159265358979323846;
+    const double u4 = rng.open();
+    const double xiMu = (u4 < 1.0) ? u4 : 1.0;   // std::min(1.0, u)
+    const double mu = sqrt(xiMu);
+    const double phiLeak = 2.0 * PI_D * rng.open();
+    const double st2 = 1.0 - mu * mu;
+    const double sinTheta = sqrt(st2 > 0.0 ? st2 : 0.0);
+    double h[3] = {0.0, 0.0, 0.0};
+    if (fabs(n[0]) < 0.9) h[0] = 1.0; else h[1] = 1.0;
+    const double hn = h[0] * n[0] + h[1] * n[1] + h[2] * n[2];
+    double e1[3] = {h[0] - n[0] * hn, h[1] - n[1] * hn, h[2] - n[2] * hn};
+    const double e1m = sqrt(e1[0] * e1[0] + e1[1] * e1[1] + e1[2] * e1[2]);
+    if (e1m > 0.0) { e1[0] = e1[0] / e1m; e1[1] = e1[1] / e1m; e1[2] = e1[2] / e1m; }
+    double e2[3] = {n[1] * e1[2] - n[2] * e1[1], n[2] * e1[0] - n[0] * e1[2], n[0] * e1[1] - n[1] * e1[0]};
+    const double e2m = sqrt(e2[0] * e2[0] + e2[1] * e2[1] + e2[2] * e2[2]);
+    if (e2m > 0.0) { e2[0] = e2[0] / e2m; e2[1] = e2[1] / e2m; e2[2] = e2[2] / e2m; }
+    const double a1 = sinTheta * cos(phiLeak), a2 = sinTheta * sin(phiLeak);
+    double dir[3];
+#pragma unroll
+    for (int q = 0; q < 3; ++q) dir[q] = (n[q] * mu + e1[q] * a1) + e2[q] * a2;
+    const double dm = sqrt(dir[0] * dir[0] + dir[1] * dir[1] + dir[2] * dir[2]);
+    if (dm > 0.0) { dir[0] = dir[0] / dm; dir[1] = dir[1] / dm; dir[2] = dir[2] / dm; }
+    p.x = fc[0]; p.y = fc[1]; p.z = fc[2];
+    p.vx = dir[0] * C.clight; p.vy = dir[1] * C.clight; p.vz = dir[2] * C.clight;
+    face = chosen;
+    switch (chosen) {
+    case 0: next = cell - 1; break;
+    case 1: next = cell + 1; break;
+    case 2: next = cell - C.nx; break;
+    case 3: next = cell + C.nx; break;
+    case 4: next = cell - C.nx * C.ny; break;
+    default: next = cell + C.nx * C.ny; break;
+    }
+    return CELL_MOVE;
+}
+
 struct PhysOut {
     int status;        // ParticleStatus or -1 error code in errCode
     int face;          // crossed side (GetCellFaces order) for CELL_MOVE
@@ -697,6 +810,21 @@ __device__ inline PhysOut physics_step(const Ctx &C, Track &T, RNG &rng, TALLY &
             o.status = r;
             o.usedRW = 1;
             T.speed = vnorm(p.vx, p.vy, p.vz);
+            return o;
+        }
+    }
+    if (C.withDDMC) {
+        int dface = -1;
+        uint32_t dnext = OUTSIDE;
+        const int r = try_ddmc(C, p, rng, tal, xl, xh, yl, yh, zl, zh, dface, dnext);
+        if (r >= 0) {
+            o.status = r;
+            o.usedRW = 2;
+            if (r == CELL_MOVE) {
+                o.face = dface;
+                o.next = dnext;
+                T.speed = vnorm(p.vx, p.vy, p.vz);
+            }
             return o;
         }
     }
@@ -901,6 +1029,61 @@ __device__ inline int rw_jump32(const Ctx &C, Track32 &T, RNG &rng, TALLY &tal, 
     return ev == 1 ? OUT_CENSUS : OUT_CONTINUE;
 }
 
+// tryDDMCStep (radiation/RadiationIMC.hpp:1416-1612) in the FP32-tracking form:
+// the event time from the cell's total leak rate, attenuation at sigma_A f c
+// with FP64 weight, time and tallies, then census, cutoff or a leak through a
+// face picked by the cumulative face fractions.  A leaking particle enters
+// the neighbour at the centre of the shared face (ENTRY32 inside it) with a
+// cosine-law direction about the face normal.  The caller has checked the
+// particle's distance to the faces against the cell's DDMC depth.
+template <class RNG, class TALLY>
+__device__ inline int ddmc_jump32(const Ctx &C, Track32 &T, RNG &rng, TALLY &tal, const float4 &da) {
+    const uint32_t cell = T.cell;
+    const double tEvent = static_cast<double>(-__logf(rng.rawf()) * da.y);
+    const bool census = T.t <= tEvent;
+    const double dt = census ? T.t : tEvent;
+    const float tau = da.z * static_cast<float>(dt);
+    const double e1 = static_cast<double>(expm1f(-tau));
+    if (!C.noFeedback) tal.mat(cell, -e1 * T.w);
+    tal.rad(cell, da.z > 0.0f ? T.w * e1 * (-1.0 / static_cast<double>(da.z)) : T.w * dt);
+    T.w *= 1.0 + e1;
+    T.t -= dt;
+    if (fabs(T.w) < T.w0 * 1e-3) {
+        if (!C.noFeedback) tal.mat(cell, T.w);
+        return OUT_CUTOFF;
+    }
+    if (census) return OUT_CENSUS;
+    const float4 c0 = C.ddmc32[3 * static_cast<size_t>(cell) + 1], c1 = C.ddmc32[3 * static_cast<size_t>(cell) + 2];
+    const float u = rng.rawf();
+    int s = static_cast<int>(c1.z);   // the last face with a leak rate
+    if (u <= c0.x) s = 0;
+    else if (u <= c0.y) s = 1;
+    else if (u <= c0.z) s = 2;
+    else if (u <= c0.w) s = 3;
+    else if (u <= c1.x) s = 4;
+    else if (u <= c1.y) s = 5;
+    if (s < 0) return OUT_CENSUS;
+    const float mu = sqrtf(rng.rawf());
+    const float phi = 6.2831853f * rng.rawf();
+    const float st = sqrtf(fmaxf(0.0f, 1.0f - mu * mu));
+    float sp, cph;
+    __sincosf(phi, &sp, &cph);
+    const float sg = (s & 1) ? 1.0f : -1.0f;
+    switch (s) {
+    case 0: --T.i; T.cell -= 1; T.qx = C.hx[T.i] * ENTRY32; break;
+    case 1: ++T.i; T.cell += 1; T.qx = -C.hx[T.i] * ENTRY32; break;
+    case 2: --T.j; T.cell -= C.nx; T.qy = C.hy[T.j] * ENTRY32; break;
+    case 3: ++T.j; T.cell += C.nx; T.qy = -C.hy[T.j] * ENTRY32; break;
+    case 4: --T.k; T.cell -= C.nx * C.ny; T.qz = C.hz[T.k] * ENTRY32; break;
+    default: ++T.k; T.cell += C.nx * C.ny; T.qz = -C.hz[T.k] * ENTRY32; break;
+    }
+    const int axis = s >> 1;
+    if (axis == 0) { T.qy = 0.0f; T.qz = 0.0f; T.ux = sg * mu; T.uy = st * cph; T.uz = st * sp; }
+    else if (axis == 1) { T.qz = 0.0f; T.qx = 0.0f; T.uy = sg * mu; T.uz = st * cph; T.ux = st * sp; }
+    else { T.qx = 0.0f; T.qy = 0.0f; T.uz = sg * mu; T.ux = st * cph; T.uy = st * sp; }
+    return OUT_CONTINUE;
+}
+
 // Multigroup absorption opacity in FP32 from the cell's cached kT and
 // sigma0 / (kT)^q: at the group centre E_g^p comes from the per-group table.
 __device__ __forceinline__ float mg_absorption32(const Ctx &C, const Track32 &T, float nu) {
@@ -956,6 +1139,10 @@ __device__ inline int segment32(const Ctx &C, Track32 &T, RNG &rng, TALLY &tal, 
     if (Ro >= cp.z && Ro > 0.0f && (!MG || static_cast<double>(T.nu) < C.gb[C.pgrwCut[cell]])) {
         usedRW = 1;
         return rw_jump32<MG>(C, T, rng, tal, cp, Ro, hx, hy, hz, err);
+    }
+    if (C.withDDMC) {   // DDMC after a Random Walk that was not taken (:1723-1738)
+        const float4 da = C.ddmc32[3 * static_cast<size_t>(cell)];   // depth reach, 1/total, sigma_A f c, nu bound
+        if (Ro >= da.x && Ro > 0.0f && (!MG || T.nu < da.w)) return ddmc_jump32(C, T, rng, tal, da);
     }
     // gray: the cell constants; multigroup: the opacity at the particle's frequency
     float invSigE, sigAf, sigE = 0.0f, elastic = 0.0f;

@@ -92,6 +92,7 @@ void launch_emission_debit(cudaStream_t s, const Ctx &C, const CellArrays &A, De
 void launch_scan_u64(cudaStream_t s, const uint64_t *in, uint32_t n, uint64_t *out, uint64_t *tileSums, uint64_t *total);
 void launch_emit_cells(cudaStream_t s, const Ctx &C, const CellArrays &A, const uint64_t *offsets, uint64_t total,
                        const Bank &b, uint32_t bankBase, double dt, DevStats *st);
+void launch_ddmc_rates(cudaStream_t s, const Ctx &C, const CellArrays &A);
 void launch_face_spectra(cudaStream_t s, const Ctx &C, double *cdf);
 void launch_emit_faces(cudaStream_t s, const Ctx &C, const FaceSources &F, uint64_t total, const Bank &b,
                        uint32_t bankBase, double dt, DevStats *st);

@@ -366,6 +366,60 @@ __device__ inline double mg_cell_tables(const Ctx &C, const CellArrays &A, uint3
     return sigmaP;
 }
 
+// precomputeDDMCData, first loop (radiation/RadiationIMC.hpp:1283-1353): the
+// cell's DDMC opacities and diffusion coefficient.  Gray (and multigroup without
+// ddmcUseMultigroupPGRW): sigma_A = the Planck opacity, sigma_T = sigma_A +
+// sigma_s, D = c / (3 sigma_T), eligible where sigma_T 4V/S >= the cell depth.
+// The multigroup PGRW form averages the diffusive groups (those below the first
+// group with sigma_T,g 4V/S under the cell depth) with equal weights 1/G.
+__device__ inline void ddmc_cell_data(const Ctx &C, const CellArrays &A, uint32_t c, double sa, double ss) {
+    const double chord = cell_chord(C, A, c);
+    double sigmaA = 0.0, sigmaT = 0.0, D = 0.0, eligible = 0.0;
+    uint32_t cutoff = 0;
+    if (chord > 0.0) {
+        if (C.ddmcPgrw) {
+            const double T = C.T[c];
+            if (C.kBoltz * T > 0.0) {
+                const uint32_t G = C.groups;
+                const double kT = mg_kT(C, c);
+                const double kTq = C.mgKTq[c];
+                const double Bg = 1.0 / static_cast<double>(G);
+                double totalBgDiff = 0.0, sumA = 0.0, sumT = 0.0, sumOver = 0.0;
+                bool foundNonDiffusive = false;
+                for (uint32_t g = 0; g < G; ++g) {
+                    const double Ec = 0.5 * (C.gb[g] + C.gb[g + 1]);
+                    const double sigA = mg_sigma(C, c, Ec, kT, kTq, C.mgEp[g]);
+                    const double sigT = sigA + ss;
+                    if (!foundNonDiffusive && sigT * chord >= C.ddmcMinCell) {
+                        cutoff = g + 1;
+                        totalBgDiff += Bg;
+                        sumA += Bg * sigA;
+                        sumT += Bg * sigT;
+                        if (sigT > 0.0) sumOver += Bg / sigT;
+                    } else {
+                        foundNonDiffusive = true;
+                    }
+                }
+                if (cutoff > 0 && totalBgDiff > 0.0) {
+                    sigmaA = sumA / totalBgDiff;
+                    sigmaT = sumT / totalBgDiff;
+                    D = (C.clight / 3.0) * sumOver / totalBgDiff;
+                    eligible = (sigmaT > 0.0 && D > 0.0) ? 1.0 : 0.0;
+                } else {
+                    cutoff = 0;
+                }
+            }
+        } else {
+            sigmaA = sa;
+            sigmaT = sigmaA + ss;
+            D = (sigmaT > 0.0) ? C.clight / (3.0 * sigmaT) : 0.0;
+            eligible = (sigmaT * chord >= C.ddmcMinCell && D > 0.0) ? 1.0 : 0.0;
+        }
+    }
+    C.ddmc[c] = make_double4(sigmaT, sigmaA, eligible, D);
+    if (C.ddmcCut) C.ddmcCut[c] = cutoff;
+}
+
 __global__ void k_prestep(Ctx C, CellArrays A, OpacityEos M, double dt) {
     for (uint32_t c = blockIdx.x * blockDim.x + threadIdx.x; c < C.ncells; c += gridDim.x * blockDim.x) {
         double sa, ss;
@@ -407,6 +461,88 @@ __global__ void k_prestep(Ctx C, CellArrays A, OpacityEos M, double dt) {
         if (f < 0.0 || f > 1.0) raise_error(C, STORM_DERR_FLECK, c, 0);
         A.phys[c] = cell_phys(sa, ss, f, sa + ss, C.clight);
         cell_rw_and_phys32(C, A, c, sa, ss, f);
+        if (C.withDDMC) ddmc_cell_data(C, A, c, sa, ss);
+    }
+}
+
+// precomputeDDMCData, second loop (radiation/RadiationIMC.hpp:1355-1413): the
+// leak rate through each face to a neighbour inside the box,
+// D_face A / (V d) with D_face the harmonic mean of the two cells' D (the
+// cell's own D where the neighbour has none) and d the distance from the cell
+// centre to the face; cells whose rates sum to zero are not eligible.  The
+// FP32 form's per-cell copy holds the particle depth it needs, 1/total, the
+// absorption rate sigma_A f c, the PGRW frequency bound and the cumulative
+// face fractions.
+__global__ void k_ddmc_rates(Ctx C, CellArrays A) {
+    for (uint32_t c = blockIdx.x * blockDim.x + threadIdx.x; c < C.ncells; c += gridDim.x * blockDim.x) {
+        const double4 dd = C.ddmc[c];
+        double rates[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+        double total = 0.0;
+        uint32_t i, j, k;
+        cell_ijk(C, c, i, j, k);
+        if (dd.z > 0.0) {
+            const double dx = C.xe[i + 1] - C.xe[i], dy = C.ye[j + 1] - C.ye[j], dz = C.ze[k + 1] - C.ze[k];
+            const double volume = (dx * dy) * dz;
+            const double D1 = dd.w;
+#pragma unroll
+            for (int s = 0; s < 6; ++s) {
+                uint32_t next;
+                bool inside;
+                double faceDistance, area;
+                switch (s) {
+                case 0: inside = i > 0; next = c - 1; faceDistance = fabs(C.xe[i] - C.xc[i]); area = dy * dz; break;
+                case 1: inside = i + 1 < C.nx; next = c + 1; faceDistance = fabs(C.xe[i + 1] - C.xc[i]); area = dy * dz; break;
+                case 2: inside = j > 0; next = c - C.nx; faceDistance = fabs(C.ye[j] - C.yc[j]); area = dz * dx; break;
+                case 3: inside = j + 1 < C.ny; next = c + C.nx; faceDistance = fabs(C.ye[j + 1] - C.yc[j]); area = dz * dx; break;
+                case 4: inside = k > 0; next = c - C.nx * C.ny; faceDistance = fabs(C.ze[k] - C.zc[k]); area = dx * dy; break;
+                default: inside = k + 1 < C.nz; next = c + C.nx * C.ny; faceDistance = fabs(C.ze[k + 1] - C.zc[k]); area = dx * dy; break;
+                }
+                if (!inside || !(faceDistance > 0.0)) continue;
+                double diffusionFace = D1;
+                const double D2 = C.ddmc[next].w;
+                if (D2 > 0.0) diffusionFace = (D1 > 0.0 && D2 > 0.0) ? (2.0 * D1 * D2 / (D1 + D2)) : (D1 < D2 ? D2 : D1);
+                const double rate = diffusionFace * area / (volume * faceDistance);
+                if (rate > 0.0 && isfinite(rate)) {
+                    rates[s] = rate;
+                    total += rate;
+                }
+            }
+            if (!(total > 0.0)) {
+                total = 0.0;
+                for (int s = 0; s < 6; ++s) rates[s] = 0.0;
+            }
+        }
+        C.ddmcTot[c] = total;
+        double *out = C.ddmcRate + static_cast<size_t>(c) * 6;
+        for (int s = 0; s < 6; ++s) out[s] = rates[s];
+        if (C.fp32) {
+            float4 *o32 = C.ddmc32 + static_cast<size_t>(c) * 3;
+            if (total > 0.0) {
+                float bound = CUDART_INF_F;
+                float reach = static_cast<float>(C.ddmcMinParticle / dd.x);
+                if (C.ddmcPgrw) {
+                    const uint32_t cut = C.ddmcCut[c];
+                    if (cut == 0 || cut > C.groups) reach = CUDART_INF_F;
+                    else bound = C.gb32[cut];
+                }
+                float cum[6];
+                double acc = 0.0;
+                int last = -1;
+                for (int s = 0; s < 6; ++s) {
+                    acc += rates[s];
+                    cum[s] = static_cast<float>(acc / total);
+                    if (rates[s] > 0.0) last = s;
+                }
+                o32[0] = make_float4(reach, static_cast<float>(1.0 / total),
+                                     static_cast<float>(dd.y * A.fleck[c] * C.clight), bound);
+                o32[1] = make_float4(cum[0], cum[1], cum[2], cum[3]);
+                o32[2] = make_float4(cum[4], cum[5], static_cast<float>(last), 0.0f);
+            } else {
+                o32[0] = make_float4(CUDART_INF_F, 0.0f, 0.0f, 0.0f);
+                o32[1] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+                o32[2] = make_float4(0.0f, 0.0f, -1.0f, 0.0f);
+            }
+        }
     }
 }
 
@@ -954,7 +1090,7 @@ struct Form64 {
     static __device__ __forceinline__ int seg(const Ctx &C, T &t, RNG &rng, TALLY &tal, int &usedRW, int &err) {
         PhysOut o = physics_step(C, t, rng, tal);
         if (o.errCode) { err = o.errCode; return OUT_ERROR; }
-        usedRW = o.usedRW;
+        usedRW = o.usedRW == 1;   // Random Walk jumps (2 marks a DDMC step)
         int m = manager_handle(C, t, o);
         if (m == OUT_ERROR) err = STORM_DERR_NOT_ON_BOUNDARY;
         return m;
@@ -1768,6 +1904,9 @@ void launch_begin(cudaStream_t s, const Bank &b, uint32_t n, double dt, DevStats
 }
 void launch_prestep(cudaStream_t s, const Ctx &C, const CellArrays &A, const OpacityEos &M, double dt) {
     k_prestep<<<grid_for(C.ncells, 256, 8192), 256, 0, s>>>(C, A, M, dt);
+}
+void launch_ddmc_rates(cudaStream_t s, const Ctx &C, const CellArrays &A) {
+    k_ddmc_rates<<<grid_for(C.ncells, 256, 8192), 256, 0, s>>>(C, A);
 }
 void launch_rw_eligibility(cudaStream_t s, const Ctx &C, const CellArrays &A) {
     k_rw_eligibility<<<grid_for(C.ncells, 256, 8192), 256, 0, s>>>(C, A);

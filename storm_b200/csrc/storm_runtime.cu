@@ -57,6 +57,10 @@ struct StormHandle {
     float *gb32 = nullptr, *gc32 = nullptr;   // multigroup bounds and centres, FP32-tracking form
     double *faceCdf = nullptr;                // multigroup: 6 x (groups + 1) face Planck spectra
     double *mgEp = nullptr, *mgKTq = nullptr; // multigroup: E_g^p per group, (kT)^q per cell
+    double4 *ddmc = nullptr;                  // DDMC per-cell data, leak rates, FP32 copy
+    double *ddmcTot = nullptr, *ddmcRate = nullptr;
+    uint32_t *ddmcCut = nullptr;
+    float4 *ddmc32 = nullptr;
     float *mgEp32 = nullptr;
     double faceCdfT[6] = {-1, -1, -1, -1, -1, -1};   // face temperatures the spectra were built for
     // face sources
@@ -577,6 +581,10 @@ int storm_cuda_create(const StormProblemDesc *d, StormHandle **out) {
         for (uint32_t g = 0; g < d->groups; ++g)
             if (!(d->group_bounds[g + 1] > d->group_bounds[g])) return STORM_ERR_INVALID_ARG;
     }
+    if (d->with_ddmc && !(d->ddmc_min_cell_optical_depth >= 0.0 && d->ddmc_min_particle_optical_depth >= 0.0 &&
+                          std::isfinite(d->ddmc_min_cell_optical_depth) &&
+                          std::isfinite(d->ddmc_min_particle_optical_depth)))
+        return STORM_ERR_INVALID_ARG;
     if (d->eos_kind != STORM_EOS_LINEAR && d->eos_kind != STORM_EOS_POWER_LAW) return STORM_ERR_UNSUPPORTED;
     if (d->precision != STORM_PRECISION_FP64 && d->precision != STORM_PRECISION_FP32_TRACK) return STORM_ERR_UNSUPPORTED;
     uint64_t N64 = static_cast<uint64_t>(d->nx) * d->ny * d->nz;
@@ -766,6 +774,19 @@ int storm_cuda_create(const StormProblemDesc *d, StormHandle **out) {
     C.clight = d->clight; C.arad = d->arad; C.sigmaSB = d->sigma_sb; C.kevKelvin = d->kev_kelvin;
     C.rwMinParticle = d->rw_min_particle_optical_depth;
     C.rwMinCell = d->rw_min_cell_optical_depth;
+    if (d->with_ddmc) {
+        C.withDDMC = 1;
+        C.ddmcPgrw = (d->ddmc_use_multigroup_pgrw && mg) ? 1 : 0;
+        C.ddmcMinParticle = d->ddmc_min_particle_optical_depth;
+        C.ddmcMinCell = d->ddmc_min_cell_optical_depth;
+        ALLOC(h->ddmc, N);
+        ALLOC(h->ddmcTot, N);
+        ALLOC(h->ddmcRate, 6 * static_cast<size_t>(N));
+        if (C.ddmcPgrw) ALLOC(h->ddmcCut, N);
+        if (h->fp32) ALLOC(h->ddmc32, 3 * static_cast<size_t>(N));
+        C.ddmc = h->ddmc; C.ddmcTot = h->ddmcTot; C.ddmcRate = h->ddmcRate; C.ddmcCut = h->ddmcCut;
+        C.ddmc32 = h->ddmc32;
+    }
     C.rwDiffPerReach = C.rwMinParticle > 0.0 ? static_cast<float>(C.clight / (3.0 * C.rwMinParticle)) : 0.0f;
     C.seedLo = static_cast<uint32_t>(d->seed);
     C.seedHi = static_cast<uint32_t>(d->seed >> 32);
@@ -806,7 +827,8 @@ int storm_cuda_destroy(StormHandle *h) {
                   h->A.rwElig, h->A.photons, h->A.phys, h->A.phys32, h->hx, h->hy, h->hz, h->segs, h->tabA, h->tabS, h->rhoF, h->rwTau, h->rwLogTau, h->rwSurv,
                   h->rwRadius, h->rwLogTau32, h->rwSurv32, h->rwRadius32, h->fsCell, h->fsSide, h->fsOffset, h->dAmbiguous, h->offsets, h->tileSums, h->dTotalU64, h->dTotalE, h->combW, h->combWtot,
                   h->combStart, h->combCount, h->counts, h->dStats, h->dErr, h->gb, h->A.mgCdf, h->A.pgrw,
-                  h->A.pgrwCut, h->gb32, h->gc32, h->faceCdf, h->mgEp, h->mgEp32, h->mgKTq};
+                  h->A.pgrwCut, h->gb32, h->gc32, h->faceCdf, h->mgEp, h->mgEp32, h->mgKTq, h->ddmc, h->ddmcTot,
+                  h->ddmcRate, h->ddmcCut, h->ddmc32};
     for (void *p : ps) device_pool().free(p);
     cudaEvent_t evs[] = {h->evStart, h->evTransport0, h->evTransport1, h->evEnd, h->evAfterEmit, h->evAfterComb};
     for (cudaEvent_t e : evs)
@@ -841,6 +863,10 @@ int storm_cuda_phase_prestep(StormHandle *h, double dt) {
     refresh_ctx(h);
     launch_prestep(h->stream, h->C, h->A, h->M, dt);
     ++h->launches;
+    if (h->C.withDDMC) {
+        launch_ddmc_rates(h->stream, h->C, h->A);
+        ++h->launches;
+    }
     CK(cudaGetLastError());
     return STORM_OK;
 }

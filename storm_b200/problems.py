@@ -74,6 +74,11 @@ class Problem:
     mg_p: float = 3.0
     mg_q: float = 0.0
     mg_s: float = 0.0
+    # DDMC-style leakage (RadiationIMCParameters defaults)
+    with_ddmc: bool = False
+    ddmc_use_multigroup_pgrw: bool = False
+    ddmc_min_cell_optical_depth: float = 15.0
+    ddmc_min_particle_optical_depth: float = 5.0
 
     @property
     def shape(self):
@@ -157,6 +162,10 @@ class Problem:
         d.group_bounds = arr(self.group_bounds)
         d.mg_p, d.mg_q, d.mg_s = self.mg_p, self.mg_q, self.mg_s
         d.k_boltz = UNITS["k_boltz"]
+        d.with_ddmc = int(self.with_ddmc)
+        d.ddmc_use_multigroup_pgrw = int(self.ddmc_use_multigroup_pgrw)
+        d.ddmc_min_cell_optical_depth = self.ddmc_min_cell_optical_depth
+        d.ddmc_min_particle_optical_depth = self.ddmc_min_particle_optical_depth
         d._keep = keep
         return d
 
@@ -442,4 +451,27 @@ def densmore2012(nx=512, new_photons_per_cell=16, boundary_per_face=100, seed=42
     p.comb_enabled = True
     p.comb_nmin, p.comb_factor = 200, 5.0
     p.seed, p.dt, p.precision, p.name = seed, 5e-12, precision, "densmore2012"
+    return p
+
+
+def ddmc_cube(n=8, new_photons_per_cell=3, face_packets=40, comb_nmin=20, seed=42, dt=1e-10,
+              precision=A.PRECISION_FP64, with_random_walk=False, rw_min_particle_optical_depth=5.0,
+              sigma_a_thick=1.0, sigma_s_thick=1000.0):
+    """A step cube with DDMC-style leakage on (withDDMC, the reference's
+    default depths 15 and 5): sigma_a = 1, no scattering for x < 0.5; a
+    scattering-dominated half (sigma_a_thick, sigma_s_thick) for x >= 0.5 that
+    is DDMC eligible, so that particles there diffuse between cells by face
+    leaks rather than being absorbed in place.  1 keV source on x=0, vacuum
+    elsewhere, T0 = 0.01 keV.  With Random Walk also on, a particle deep enough
+    for a Random Walk jump takes it first and DDMC covers the depths between
+    the two particle thresholds."""
+    p = step_cube(n=n, new_photons_per_cell=new_photons_per_cell, face_packets=face_packets, comb_nmin=comb_nmin,
+                  seed=seed, dt=dt, precision=precision, with_random_walk=with_random_walk)
+    xc, _, _ = p.cell_centers()
+    thick = xc >= 0.5
+    p.sigma_a = np.where(thick, sigma_a_thick, 1.0)
+    p.sigma_s = np.where(thick, sigma_s_thick, 0.0)
+    p.with_ddmc = True
+    p.rw_min_particle_optical_depth = rw_min_particle_optical_depth
+    p.name = "ddmc_cube"
     return p

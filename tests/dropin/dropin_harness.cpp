@@ -25,6 +25,10 @@ void bind_imc(STORM::CudaIMCBinding<Cell, Ext> &b, const StormProblemDesc *d) {
     p.rwMinCellOpticalDepth = d->rw_min_cell_optical_depth;
     p.rwMinParticleOpticalDepth = d->rw_min_particle_optical_depth;
     p.noHydroFeedback = d->no_hydro_feedback != 0;
+    p.withDDMC = d->with_ddmc != 0;
+    p.ddmcUseMultigroupPGRW = d->ddmc_use_multigroup_pgrw != 0;
+    p.ddmcMinCellOpticalDepth = d->ddmc_min_cell_optical_depth;
+    p.ddmcMinParticleOpticalDepth = d->ddmc_min_particle_optical_depth;
     if constexpr (G > 1) {
         p.withMultigroupOpacity = true;
         for (std::size_t g = 0; g <= G; ++g) p.energyBoundaries[g] = d->group_bounds[g];

@@ -17,6 +17,13 @@ Fixtures (numpy .npz):
   replay_mg.npz       recorded calls on a 6^3 multigroup cube (64 groups, PGRW)
                       with frequencies and the step's starting temperatures
   replay_mg_thin.npz  the same, optically thinner, opacity continuous in frequency
+  replay_ddmc.npz     recorded calls on an 8^3 step cube with DDMC leakage (withDDMC)
+                      and the step's starting temperatures
+  replay_ddmc_rw.npz  the same with Random Walk on (particle depth 20): Random Walk
+                      jumps where deep enough, DDMC steps between depths 5 and 20
+  replay_ddmc_mg.npz  a 64-group cube with DDMC in its multigroup PGRW form
+
+    python tests/golden/make_golden.py ddmc     # only the DDMC fixtures
 """
 import os
 import sys
@@ -46,7 +53,7 @@ def record(problem, warm_steps, max_records, take, mg=False):
     # boundary interactions and Random Walk jumps
     idx = np.arange(n)
     special = (rec["status"] == 1) & (rec["next"] >= problem.ncells)
-    special |= rec["used_rw"] == 1
+    special |= rec["used_rw"] != 0   # Random Walk jumps and DDMC steps
     special |= rec["status"] == 3
     if mg:   # every frequency change (effective scatters, PGRW upscatters)
         special |= rec["freq_before"] != rec["freq_after"]
@@ -70,7 +77,23 @@ def record(problem, warm_steps, max_records, take, mg=False):
                next_before=nxt_before, next_cell=nxt_cell, sigma_a=c["sigma_a"], fleck=c["fleck"])
     if mg:   # frequencies, and the temperatures the recorded step built its tables from
         out.update(freq_before=rec["freq_before"][sub], freq_after=rec["freq_after"][sub], T_start=T_start)
+    if problem.with_ddmc:
+        out.update(T_start=T_start)
     return out
+
+
+def make_ddmc():
+    gray = problems.ddmc_cube(n=8, new_photons_per_cell=3, face_packets=40, comb_nmin=20, seed=11)
+    np.savez_compressed(os.path.join(HERE, "replay_ddmc.npz"), **record(gray, 1, 400000, 1500))
+    mixed = problems.ddmc_cube(n=8, new_photons_per_cell=3, face_packets=40, comb_nmin=20, seed=12,
+                               with_random_walk=True, rw_min_particle_optical_depth=20.0)
+    np.savez_compressed(os.path.join(HERE, "replay_ddmc_rw.npz"), **record(mixed, 1, 400000, 1500))
+    mg = problems.mg_cube(n=6, groups=64, kappa0=1e-4, new_photons_per_cell=3, comb_nmin=3, seed=13, dt=1e-10,
+                          with_random_walk=False)
+    mg.sigma_s = np.full(mg.ncells, 1000.0)
+    mg.with_ddmc = True
+    mg.ddmc_use_multigroup_pgrw = True
+    np.savez_compressed(os.path.join(HERE, "replay_ddmc_mg.npz"), **record(mg, 1, 400000, 1500, mg=True))
 
 
 def main():
@@ -132,4 +155,8 @@ def main():
 
 
 if __name__ == "__main__":
-    main()
+    if sys.argv[1:] == ["ddmc"]:
+        make_ddmc()
+    else:
+        main()
+        make_ddmc()
