@@ -70,10 +70,17 @@ struct CudaIMCBinding {
     double rwMinCellOpticalDepth = 25.0, rwMinParticleOpticalDepth = 5.0;
     bool withDDMC = false, ddmcUseMultigroupPGRW = false;
     double ddmcMinCellOpticalDepth = 15.0, ddmcMinParticleOpticalDepth = 5.0;
-    // CombPopulationControl(grid, Nmin, factor)
+    // CombPopulationControl(grid, Nmin, factor), or StratifiedCombPopulationControl(grid,
+    // groupCount, classifier, Nmin, factor, minParticlesPerGroup) with the classifier
+    // given as frequency bin edges (groupCount + 1; empty with groupCount equal to the
+    // number of energy groups: one bin per group)
     bool combEnabled = true;
     std::size_t combNmin = 20;
     double combFactor = 2.0;
+    int combKind = STORM_COMB_PLAIN;
+    std::uint32_t stratBins = 1;
+    std::vector<double> stratBounds;
+    std::size_t stratMinPerBin = 2;
     // constants the caller's physics uses (units::*)
     double clight = 0, arad = 0, sigmaSB = 0, kevKelvin = 0;
     // engine
@@ -315,6 +322,10 @@ private:
         d.comb_enabled = binding_.combEnabled;
         d.comb_nmin = binding_.combNmin;
         d.comb_factor = binding_.combFactor;
+        d.comb_kind = binding_.combKind;
+        d.strat_bins = binding_.stratBins;
+        d.strat_bounds = binding_.stratBounds.empty() ? nullptr : binding_.stratBounds.data();
+        d.strat_min_per_bin = binding_.stratMinPerBin;
         d.clight = binding_.clight; d.arad = binding_.arad; d.sigma_sb = binding_.sigmaSB; d.kev_kelvin = binding_.kevKelvin;
         d.seed = binding_.seed;
         // MonteCarloConfig sizes the serial manager's buffer; here it seeds the bank capacity

@@ -36,7 +36,7 @@
 extern "C" {
 #endif
 
-#define STORM_CUDA_ABI_VERSION 4
+#define STORM_CUDA_ABI_VERSION 5
 
 /* ---------------------------------------------------------------- status */
 enum StormStatus {
@@ -189,7 +189,26 @@ typedef struct StormProblemDesc {
     int32_t ddmc_use_multigroup_pgrw;
     double ddmc_min_cell_optical_depth;      /* reference default 15 */
     double ddmc_min_particle_optical_depth;  /* reference default 5 */
+
+    /* ---- population control: CombPopulationControl (0) or
+     * StratifiedCombPopulationControl (1, population/CombPopulationControl.hpp:35-511)
+     * with the particle classifier lowered to frequency bins: bin g holds
+     * frequencies below strat_bounds[g + 1] (the last bin everything above),
+     * RadiationOpacityModel::findGroup's rule.  comb_nmin and comb_factor are
+     * its Nmin and totalParticlesFactor. */
+    int32_t comb_kind;               /* StormCombKind */
+    uint32_t strat_bins;             /* groupCount, 1..STORM_STRAT_MAX_BINS */
+    const double *strat_bounds;      /* strat_bins + 1 increasing frequencies [erg]; NULL: one bin (gray), or the
+                                        problem's group_bounds when strat_bins equals groups */
+    uint64_t strat_min_per_bin;      /* minParticlesPerGroup (reference default 2) */
 } StormProblemDesc;
+
+#define STORM_STRAT_MAX_BINS 64
+
+enum StormCombKind {
+    STORM_COMB_PLAIN = 0,            /* CombPopulationControl (population/CombPopulationControl.hpp:79-253) */
+    STORM_COMB_STRATIFIED = 1        /* StratifiedCombPopulationControl (population/CombPopulationControl.hpp:255-511) */
+};
 
 /* Particle arrays, struct-of-arrays.  Mirrors the fields of
  * Particle<T,Grid> (particle/Particle.hpp:67-85) that the gray path uses.

@@ -569,7 +569,22 @@ RefHandle *ref_create(const StormProblemDesc *d, int boundary_kind, char *err, s
         } else {
             build_physics<1>(*h, d);
         }
-        if (d->comb_enabled)
+        if (d->comb_enabled && d->comb_kind == STORM_COMB_STRATIFIED) {
+            // the classifier as the engine lowers it: frequency bins by findGroup's rule
+            std::vector<double> edges;
+            const std::size_t B = d->strat_bins;
+            if (B > 1) {
+                const double *sb = d->strat_bounds ? d->strat_bounds : d->group_bounds;
+                edges.assign(sb, sb + B + 1);
+            }
+            auto classifier = [edges, B](const MCParticle &p) -> std::size_t {
+                for (std::size_t g = 0; g + 1 < B; ++g)
+                    if (p.frequency < edges[g + 1]) return g;
+                return B - 1;
+            };
+            h->pop = std::make_shared<STORM::StratifiedCombPopulationControl<Vector3D, Grid>>(
+                *h->grid, B, classifier, d->comb_nmin, d->comb_factor, d->strat_min_per_bin);
+        } else if (d->comb_enabled)
             h->pop = std::make_shared<STORM::CombPopulationControl<Vector3D, Grid>>(*h->grid, d->comb_nmin, d->comb_factor);
         else
             h->pop = std::make_shared<STORM::NoPopulationControl<Vector3D, Grid>>(*h->grid);
@@ -832,7 +847,8 @@ int ref_point_on_face(RefHandle *h, uint64_t n, const uint64_t *faces, double *p
     return 0;
 }
 
-// CombPopulationControl::activate on a given particle list (invariant tests).
+// The population control's activate (CombPopulationControl or
+// StratifiedCombPopulationControl) on a given particle list (invariant tests).
 int ref_comb(RefHandle *h, const StormParticlesSoA *in, StormParticlesSoA *out, uint64_t *outCount) {
     try {
         std::vector<MCParticle> v;

@@ -5,7 +5,7 @@ sizes against the compiled library.
 """
 import ctypes as C
 
-ABI_VERSION = 4
+ABI_VERSION = 5
 
 STORM_OK = 0
 STATUS_NAMES = {
@@ -25,6 +25,9 @@ FACE_ESCAPE = 1
 OPACITY_CELL_TABLE = 0
 OPACITY_POWER_LAW = 1
 OPACITY_MG_POWER = 2
+COMB_PLAIN = 0
+COMB_STRATIFIED = 1
+STRAT_MAX_BINS = 64
 EOS_LINEAR = 0
 EOS_POWER_LAW = 1
 
@@ -72,6 +75,8 @@ class StormProblemDesc(C.Structure):
         ("mg_p", C.c_double), ("mg_q", C.c_double), ("mg_s", C.c_double), ("k_boltz", C.c_double),
         ("with_ddmc", C.c_int32), ("ddmc_use_multigroup_pgrw", C.c_int32),
         ("ddmc_min_cell_optical_depth", C.c_double), ("ddmc_min_particle_optical_depth", C.c_double),
+        ("comb_kind", C.c_int32), ("strat_bins", C.c_uint32), ("strat_bounds", _dp),
+        ("strat_min_per_bin", C.c_uint64),
     ]
 
 

@@ -58,6 +58,13 @@ struct CombParams {
     uint64_t ntotal, nmin;
 };
 
+// StratifiedCombPopulationControl: frequency bins of the particle classifier
+struct StratParams {
+    uint32_t bins;
+    const double *bounds;    // bins + 1 edges (device), NULL when bins == 1
+    uint64_t minPerBin;
+};
+
 struct DevStats {
     unsigned long long segments, rwSteps, escaped, cutoff, census;
     double eCensusIn, eEmitted, eDeposited, eEscaped, eCensusPre, eCensusOut, eDebit;
@@ -93,6 +100,13 @@ void launch_scan_u64(cudaStream_t s, const uint64_t *in, uint32_t n, uint64_t *o
 void launch_emit_cells(cudaStream_t s, const Ctx &C, const CellArrays &A, const uint64_t *offsets, uint64_t total,
                        const Bank &b, uint32_t bankBase, double dt, DevStats *st);
 void launch_ddmc_rates(cudaStream_t s, const Ctx &C, const CellArrays &A);
+void launch_strat_keys(cudaStream_t s, const Ctx &C, const CensusBank &cen, uint32_t n, uint64_t *keys, uint32_t *vals,
+                       uint32_t combKey, int pidBits, const StratParams &S);
+void launch_strat_sums(cudaStream_t s, const double *wS, const uint32_t *start, uint32_t ncells, uint32_t bins,
+                       double *binW, double *cellW);
+void launch_strat_plan(cudaStream_t s, const Ctx &C, const CombParams &P, const StratParams &S, const double *wS,
+                       const uint32_t *start, const double *binW, const double *cellW, const double *Wtot,
+                       uint32_t *pCount, double *pWeight, uint64_t *cellCount, double *eradCensus, DevStats *st);
 void launch_face_spectra(cudaStream_t s, const Ctx &C, double *cdf);
 void launch_emit_faces(cudaStream_t s, const Ctx &C, const FaceSources &F, uint64_t total, const Bank &b,
                        uint32_t bankBase, double dt, DevStats *st);
@@ -119,7 +133,7 @@ void launch_comb_plan(cudaStream_t s, const Ctx &C, const CombParams &P, const d
                       const double *W, const double *Wtot, uint32_t *pCount, double *pWeight, uint64_t *cellCount,
                       double *eradCensus, DevStats *st);
 void launch_comb_emit(cudaStream_t s, const Ctx &C, const CensusBank &cen, const uint32_t *idx, const uint64_t *sortedKeys,
-                      int pidBits, uint32_t nValid, const uint32_t *pCount, const double *pWeight,
+                      int pidBits, uint32_t bins, uint32_t nValid, const uint32_t *pCount, const double *pWeight,
                       const uint64_t *pOffset, const Bank &out);
 void launch_mask_count(cudaStream_t s, const uint32_t *pCount, uint32_t n, uint64_t *out);
 void launch_allocate_checked(cudaStream_t s, const Ctx &C, const CellArrays &A, const double *total,

@@ -1666,8 +1666,8 @@ __device__ __forceinline__ void comb_emit_fp64(const Ctx &C, PartReg &p, uint32_
 
 template <bool FP32>
 __global__ void k_comb_emit(Ctx C, CensusBank cen, const uint32_t *idx, const uint64_t *sortedKeys, int pidBits,
-                            uint32_t nValid, const uint32_t *pCount, const double *pWeight, const uint64_t *pOffset,
-                            Bank out) {
+                            uint32_t bins, uint32_t nValid, const uint32_t *pCount, const double *pWeight,
+                            const uint64_t *pOffset, Bank out) {
     const uint32_t stride = gridDim.x * blockDim.x;
     constexpr int words = FP32 ? 4 : 6;
     for (uint32_t base = blockIdx.x * blockDim.x + threadIdx.x; base < nValid; base += EMIT_BATCH * stride) {
@@ -1692,7 +1692,7 @@ __global__ void k_comb_emit(Ctx C, CensusBank cen, const uint32_t *idx, const ui
             const uint32_t m = raw[u] & ~KEEP;
             if (m == 0) continue;
             const uint32_t q = base + u * stride;
-            const uint32_t c = static_cast<uint32_t>(sortedKeys[q] >> pidBits);
+            const uint32_t c = static_cast<uint32_t>((sortedKeys[q] >> pidBits) / bins);   // (cell, bin) keys
             const uint64_t o = pOffset[q];
             const double wNew = pWeight[q];
             if constexpr (FP32) {
@@ -1722,6 +1722,191 @@ __global__ void k_comb_emit(Ctx C, CensusBank cen, const uint32_t *idx, const ui
             }
         }
     }
+}
+
+// ------------------------------------------------------------------ stratified comb
+// StratifiedCombPopulationControl::activate (population/CombPopulationControl.hpp:255-511)
+// with its classifier lowered to frequency bins.  The census is sorted by
+// (cell, bin, keyed hash of pid), so each (cell, bin) is one contiguous run in
+// a pseudo-random order (the reference's sort by id and shuffle); per cell the
+// bin targets follow the reference's allocation, and each bin is kept, split
+// or combed like appendCombBin.
+
+// the census particle's photon energy
+__device__ __forceinline__ double census_nu(const Ctx &C, const CensusBank &c, uint32_t q) {
+    if (C.fp32) return static_cast<double>(__uint_as_float(c.rec[static_cast<size_t>(q) * 4 + 3].w));
+    return hi_double(c.rec[static_cast<size_t>(q) * 6 + 5]);
+}
+// the bin of frequency nu: the first g with nu < bounds[g + 1], else the last
+// (RadiationOpacityModel::findGroup's rule, radiation/RadiationOpacityModel.hpp:76-86)
+__device__ __forceinline__ uint32_t strat_bin(const StratParams &S, double nu) {
+    if (S.bins <= 1) return 0;
+    uint32_t lo = 0, hi = S.bins - 1;
+    while (lo < hi) {
+        const uint32_t mid = (lo + hi) >> 1;
+        if (nu < S.bounds[mid + 1]) hi = mid; else lo = mid + 1;
+    }
+    return lo;
+}
+
+__global__ void k_strat_keys(Ctx C, CensusBank cen, uint32_t n, uint64_t *keys, uint32_t *vals, uint32_t combKey,
+                             int pidBits, StratParams S) {
+    for (uint32_t q = blockIdx.x * blockDim.x + threadIdx.x; q < n; q += gridDim.x * blockDim.x) {
+        const double w = census_w(C, cen, q);
+        const uint2 cp = census_cell_pid(C, cen, q);
+        const uint32_t pid = cp.y;
+        uint32_t cell = cp.x;
+        if (!C.fp32) {   // :288-295
+            const uint4 a = cen.rec[static_cast<size_t>(q) * 6], b = cen.rec[static_cast<size_t>(q) * 6 + 1];
+            if (outside_box(C, lo_double(a), hi_double(a), lo_double(b))) raise_error(C, STORM_DERR_COMB_OUTSIDE, cell, pid);
+        }
+        const bool badWeight = !isfinite(w) || w < 0.0;   // :296-309
+        if (badWeight) raise_error(C, STORM_DERR_COMB_WEIGHT, cell, pid);
+        uint64_t cb;
+        if (w == 0.0 || badWeight || cell >= C.ncells) cb = static_cast<uint64_t>(C.ncells) * S.bins;   // :310-311
+        else cb = static_cast<uint64_t>(cell) * S.bins + strat_bin(S, census_nu(C, cen, q));
+        keys[q] = (cb << pidBits) | comb_hash(pid, combKey, pidBits);
+        vals[q] = q;
+    }
+}
+
+// binWeights[cell][g] and cellWeights[cell] (:326-328), summed in sorted order
+__global__ void k_strat_sums(const double *wS, const uint32_t *start, uint32_t ncells, uint32_t bins, double *binW,
+                             double *cellW) {
+    for (uint32_t c = blockIdx.x * blockDim.x + threadIdx.x; c < ncells; c += gridDim.x * blockDim.x) {
+        double cs = 0.0;
+        for (uint32_t g = 0; g < bins; ++g) {
+            const size_t cb = static_cast<size_t>(c) * bins + g;
+            double s = 0.0;
+            for (uint32_t q = start[cb]; q < start[cb + 1]; ++q) s += wS[q];
+            binW[cb] = s;
+            cs += s;
+        }
+        cellW[c] = cs;
+    }
+}
+
+// Per cell (:416-488): the cell's target, each bin's share of it, then each
+// bin as appendCombBin (:347-413) writes it: copy counts and weights of the
+// sorted particles (bit 31 of the count: kept as is) and the census energy.
+__global__ void k_strat_plan(Ctx C, CombParams P, StratParams S, const double *wS, const uint32_t *start,
+                             const double *binW, const double *cellW, const double *Wtot, uint32_t *pCount,
+                             double *pWeight, uint64_t *cellCount, double *eradCensus, DevStats *st) {
+    const double tot = *Wtot;
+    if (!isfinite(tot)) {
+        if (blockIdx.x == 0 && threadIdx.x == 0) raise_error(C, STORM_DERR_COMB_TOTAL, 0, 0);
+    }
+    const uint32_t B = S.bins;
+    double eOut = 0.0;
+    for (uint32_t c = blockIdx.x * blockDim.x + threadIdx.x; c < C.ncells; c += gridDim.x * blockDim.x) {
+        const size_t base = static_cast<size_t>(c) * B;
+        const uint32_t a0 = start[base], aEnd = start[base + B];
+        const double cw = cellW[c];
+        double ecell = 0.0;
+        uint64_t m = 0;
+        if (tot == 0.0 || !isfinite(tot) || !(cw > 0.0) || a0 == aEnd) {
+            for (uint32_t q = a0; q < aEnd; ++q) pCount[q] = 0;
+        } else {
+            const uint64_t share = static_cast<uint64_t>(static_cast<double>(P.ntotal) * cw / tot);
+            const uint64_t lo = share > P.nmin ? share : P.nmin;
+            const uint64_t cellTarget = (P.nmin * 20 < lo) ? P.nmin * 20 : lo;
+            uint8_t act[STORM_STRAT_MAX_BINS];
+            uint64_t target[STORM_STRAT_MAX_BINS];
+            double frac[STORM_STRAT_MAX_BINS];
+            uint32_t nAct = 0;
+            for (uint32_t g = 0; g < B; ++g) {
+                target[g] = 0;
+                frac[g] = 0.0;
+                if (start[base + g + 1] > start[base + g]) act[nAct++] = static_cast<uint8_t>(g);
+            }
+            uint64_t allocated = 0;
+            if (static_cast<uint64_t>(nAct) * S.minPerBin <= cellTarget) {
+                for (uint32_t a = 0; a < nAct; ++a) { target[act[a]] = S.minPerBin; allocated += S.minPerBin; }
+            } else {
+                // heaviest bins first (ties keep ascending bin order)
+                for (uint32_t a = 1; a < nAct; ++a) {
+                    const uint8_t g = act[a];
+                    uint32_t b = a;
+                    while (b > 0 && binW[base + act[b - 1]] < binW[base + g]) { act[b] = act[b - 1]; --b; }
+                    act[b] = g;
+                }
+                const uint64_t prot = nAct < cellTarget ? nAct : cellTarget;
+                for (uint64_t a = 0; a < prot; ++a) { target[act[a]] = 1; ++allocated; }
+            }
+            const uint64_t remaining = cellTarget > allocated ? cellTarget - allocated : 0;
+            uint64_t prop = 0;
+            for (uint32_t a = 0; a < nAct; ++a) {
+                const uint32_t g = act[a];
+                if (target[g] == 0) continue;
+                const double exact = static_cast<double>(remaining) * binW[base + g] / cw;
+                const uint64_t extra = static_cast<uint64_t>(floor(exact));
+                target[g] += extra;
+                prop += extra;
+                frac[g] = exact - static_cast<double>(extra);
+            }
+            while (prop < remaining) {
+                uint32_t best = B;
+                double bf = -1.0;
+                for (uint32_t a = 0; a < nAct; ++a) {
+                    const uint32_t g = act[a];
+                    if (target[g] > 0 && frac[g] > bf) { best = g; bf = frac[g]; }
+                }
+                if (best == B) break;
+                ++target[best];
+                frac[best] = 0.0;
+                ++prop;
+            }
+            for (uint32_t g = 0; g < B; ++g) {
+                const uint32_t a = start[base + g], b = start[base + g + 1];
+                const double bw = binW[base + g];
+                const uint64_t tg = target[g];
+                if (a == b) continue;
+                if (tg == 0 || !(bw > 0.0)) {   // a bin without a target loses its particles (:349-350)
+                    for (uint32_t q = a; q < b; ++q) pCount[q] = 0;
+                } else if (static_cast<uint64_t>(b - a) <= tg) {
+                    const double ideal = bw / static_cast<double>(tg);
+                    for (uint32_t q = a; q < b; ++q) {
+                        const double w = wS[q];
+                        if (w > 2.0 * ideal) {
+                            const uint64_t ns = static_cast<uint64_t>(ceil(w / ideal));
+                            const double ws = w / static_cast<double>(ns);
+                            for (uint64_t k = 0; k < ns; ++k) ecell += ws;
+                            pCount[q] = static_cast<uint32_t>(ns);
+                            pWeight[q] = ws;
+                            m += ns;
+                        } else {
+                            ecell += w;
+                            pCount[q] = 1u | KEEP;
+                            pWeight[q] = w;
+                            m += 1;
+                        }
+                    }
+                } else {
+                    const double newWeight = bw / static_cast<double>(tg);
+                    const double r = stream_uniform(C.seedLo, C.seedHi, TAG_COMB, C.step, c, 1 + g);
+                    uint64_t k = 0;
+                    double cum = 0.0;
+                    for (uint32_t q = a; q < b; ++q) {
+                        const double w = wS[q];
+                        const uint64_t k0 = k;
+                        while ((cum + w) > (static_cast<double>(k) + r) * newWeight && k < tg) {
+                            ++k;
+                            ecell += newWeight;
+                        }
+                        cum += w;
+                        pCount[q] = static_cast<uint32_t>(k - k0);
+                        pWeight[q] = newWeight;
+                    }
+                    m += k;
+                }
+            }
+        }
+        cellCount[c] = m;
+        eradCensus[c] = ecell;
+        eOut += ecell;
+    }
+    eOut = warp_sum(eOut);
+    if ((threadIdx.x & 31) == 0 && eOut != 0.0) atomicAdd(&st->eCensusOut, eOut);
 }
 
 __global__ void k_mask_count(const uint32_t *pCount, uint32_t n, uint64_t *out) {
@@ -1947,6 +2132,20 @@ void launch_emit_faces(cudaStream_t s, const Ctx &C, const FaceSources &F, uint6
     k_emit_faces<<<grid_for(total, 256, 148 * 16), 256, 0, s>>>(C, F, total, b, bankBase, dt, st);
 }
 void launch_face_spectra(cudaStream_t s, const Ctx &C, double *cdf) { k_face_spectra<<<1, 32, 0, s>>>(C, cdf); }
+void launch_strat_keys(cudaStream_t s, const Ctx &C, const CensusBank &cen, uint32_t n, uint64_t *keys, uint32_t *vals,
+                       uint32_t combKey, int pidBits, const StratParams &S) {
+    k_strat_keys<<<grid_for(n, 256, 148 * 16), 256, 0, s>>>(C, cen, n, keys, vals, combKey, pidBits, S);
+}
+void launch_strat_sums(cudaStream_t s, const double *wS, const uint32_t *start, uint32_t ncells, uint32_t bins,
+                       double *binW, double *cellW) {
+    k_strat_sums<<<grid_for(ncells, 256, 8192), 256, 0, s>>>(wS, start, ncells, bins, binW, cellW);
+}
+void launch_strat_plan(cudaStream_t s, const Ctx &C, const CombParams &P, const StratParams &S, const double *wS,
+                       const uint32_t *start, const double *binW, const double *cellW, const double *Wtot,
+                       uint32_t *pCount, double *pWeight, uint64_t *cellCount, double *eradCensus, DevStats *st) {
+    k_strat_plan<<<grid_for(C.ncells, 128, 8192), 128, 0, s>>>(C, P, S, wS, start, binW, cellW, Wtot, pCount, pWeight,
+                                                             cellCount, eradCensus, st);
+}
 void launch_transport(cudaStream_t s, uint32_t grid, const Ctx &C, const Bank &in, const uint32_t *nIn, const Bank &out,
                       uint32_t *nOut, const CensusBank &cen, uint32_t *nCen, uint32_t K, DevStats *st, int minBlocks) {
     if (C.fp32) {
@@ -2038,14 +2237,14 @@ void launch_comb_plan(cudaStream_t s, const Ctx &C, const CombParams &P, const d
                                                                eradCensus, st);
 }
 void launch_comb_emit(cudaStream_t s, const Ctx &C, const CensusBank &cen, const uint32_t *idx, const uint64_t *sortedKeys,
-                      int pidBits, uint32_t nValid, const uint32_t *pCount, const double *pWeight,
+                      int pidBits, uint32_t bins, uint32_t nValid, const uint32_t *pCount, const double *pWeight,
                       const uint64_t *pOffset, const Bank &out) {
     if (!nValid) return;
     if (C.fp32)
-        k_comb_emit<true><<<grid_for(nValid, 256, 148 * 16), 256, 0, s>>>(C, cen, idx, sortedKeys, pidBits, nValid, pCount,
+        k_comb_emit<true><<<grid_for(nValid, 256, 148 * 16), 256, 0, s>>>(C, cen, idx, sortedKeys, pidBits, bins, nValid, pCount,
                                                                            pWeight, pOffset, out);
     else
-        k_comb_emit<false><<<grid_for(nValid, 256, 148 * 16), 256, 0, s>>>(C, cen, idx, sortedKeys, pidBits, nValid, pCount,
+        k_comb_emit<false><<<grid_for(nValid, 256, 148 * 16), 256, 0, s>>>(C, cen, idx, sortedKeys, pidBits, bins, nValid, pCount,
                                                                             pWeight, pOffset, out);
 }
 void launch_mask_count(cudaStream_t s, const uint32_t *pCount, uint32_t n, uint64_t *out) {

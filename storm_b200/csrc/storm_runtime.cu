@@ -61,6 +61,9 @@ struct StormHandle {
     double *ddmcTot = nullptr, *ddmcRate = nullptr;
     uint32_t *ddmcCut = nullptr;
     float4 *ddmc32 = nullptr;
+    StratParams strat{1, nullptr, 2};         // stratified comb: bins, device bounds, minParticlesPerGroup
+    double *stratBounds = nullptr, *stratBinW = nullptr;
+    uint32_t *stratStart = nullptr;
     float *mgEp32 = nullptr;
     double faceCdfT[6] = {-1, -1, -1, -1, -1, -1};   // face temperatures the spectra were built for
     // face sources
@@ -581,6 +584,15 @@ int storm_cuda_create(const StormProblemDesc *d, StormHandle **out) {
         for (uint32_t g = 0; g < d->groups; ++g)
             if (!(d->group_bounds[g + 1] > d->group_bounds[g])) return STORM_ERR_INVALID_ARG;
     }
+    if (d->comb_kind != STORM_COMB_PLAIN && d->comb_kind != STORM_COMB_STRATIFIED) return STORM_ERR_INVALID_ARG;
+    if (d->comb_kind == STORM_COMB_STRATIFIED) {
+        if (d->strat_bins < 1 || d->strat_bins > STORM_STRAT_MAX_BINS) return STORM_ERR_INVALID_ARG;
+        if (d->strat_bins > 1 && !d->strat_bounds && !(mg && d->groups == d->strat_bins)) return STORM_ERR_INVALID_ARG;
+        const double *sb = d->strat_bounds ? d->strat_bounds : d->group_bounds;
+        if (d->strat_bins > 1)
+            for (uint32_t g = 0; g < d->strat_bins; ++g)
+                if (!(sb[g + 1] > sb[g])) return STORM_ERR_INVALID_ARG;
+    }
     if (d->with_ddmc && !(d->ddmc_min_cell_optical_depth >= 0.0 && d->ddmc_min_particle_optical_depth >= 0.0 &&
                           std::isfinite(d->ddmc_min_cell_optical_depth) &&
                           std::isfinite(d->ddmc_min_particle_optical_depth)))
@@ -699,6 +711,18 @@ int storm_cuda_create(const StormProblemDesc *d, StormHandle **out) {
     ALLOC(h->combW, N);
     ALLOC(h->combWtot, 2);
     ALLOC(h->combStart, N + 2);
+    if (d->comb_kind == STORM_COMB_STRATIFIED) {
+        const uint32_t B = d->strat_bins;
+        h->strat.bins = B;
+        h->strat.minPerBin = d->strat_min_per_bin;
+        ALLOC(h->stratStart, static_cast<size_t>(N) * B + 2);
+        ALLOC(h->stratBinW, static_cast<size_t>(N) * B);
+        if (B > 1) {
+            ALLOC(h->stratBounds, B + 1);
+            H2D(h->stratBounds, d->strat_bounds ? d->strat_bounds : d->group_bounds, B + 1);
+            h->strat.bounds = h->stratBounds;
+        }
+    }
     ALLOC(h->combCount, N + 1);
     h->maxRounds = d->max_rounds ? d->max_rounds : 16384;
     ALLOC(h->counts, h->maxRounds + 2);
@@ -828,7 +852,7 @@ int storm_cuda_destroy(StormHandle *h) {
                   h->rwRadius, h->rwLogTau32, h->rwSurv32, h->rwRadius32, h->fsCell, h->fsSide, h->fsOffset, h->dAmbiguous, h->offsets, h->tileSums, h->dTotalU64, h->dTotalE, h->combW, h->combWtot,
                   h->combStart, h->combCount, h->counts, h->dStats, h->dErr, h->gb, h->A.mgCdf, h->A.pgrw,
                   h->A.pgrwCut, h->gb32, h->gc32, h->faceCdf, h->mgEp, h->mgEp32, h->mgKTq, h->ddmc, h->ddmcTot,
-                  h->ddmcRate, h->ddmcCut, h->ddmc32};
+                  h->ddmcRate, h->ddmcCut, h->ddmc32, h->stratBounds, h->stratBinW, h->stratStart};
     for (void *p : ps) device_pool().free(p);
     cudaEvent_t evs[] = {h->evStart, h->evTransport0, h->evTransport1, h->evEnd, h->evAfterEmit, h->evAfterComb};
     for (cudaEvent_t e : evs)
@@ -1084,28 +1108,39 @@ int storm_cuda_phase_comb(StormHandle *h) {
         return fm(static_cast<uint32_t>(h->desc.seed) ^ fm(h->step * 0x9E3779B9u + static_cast<uint32_t>(h->desc.seed >> 32)));
     }();
     const int pidBits = pid_bits(h);
-    launch_comb_keys(h->stream, h->C, h->bankC, n, h->keys, h->vals, combKey, pidBits);
+    // StratifiedCombPopulationControl sorts by (cell, bin): runs are per (cell, bin)
+    const bool strat = h->desc.comb_kind == STORM_COMB_STRATIFIED;
+    const uint32_t B = strat ? h->strat.bins : 1u;
+    const uint64_t nRuns = static_cast<uint64_t>(N) * B;
+    uint32_t *start = strat ? h->stratStart : h->combStart;
+    if (strat) launch_strat_keys(h->stream, h->C, h->bankC, n, h->keys, h->vals, combKey, pidBits, h->strat);
+    else launch_comb_keys(h->stream, h->C, h->bankC, n, h->keys, h->vals, combKey, pidBits);
     int cellBits = 0;
-    while ((1ull << cellBits) <= N) ++cellBits;
+    while ((1ull << cellBits) <= nRuns) ++cellBits;
     int alt = launch_radix_sort(h->stream, h->keys, h->vals, h->keysAlt, h->valsAlt, n, pidBits + cellBits, h->tileHist);
     const uint64_t *skeys = alt ? h->keysAlt : h->keys;
     const uint32_t *idx = alt ? h->valsAlt : h->vals;
     const int passes = (pidBits + cellBits + 7) / 8;
-    // census weights in sorted order; comb_plan overwrites each slot with the copies' weight
+    // census weights in sorted order; the plan overwrites each slot with the copies' weight
     double *wS = h->pWeight;
-    launch_comb_ranges(h->stream, skeys, n, N, h->combStart, pidBits);
+    launch_comb_ranges(h->stream, skeys, n, static_cast<uint32_t>(nRuns), start, pidBits);
     launch_sorted_weights(h->stream, h->C, h->bankC, idx, n, wS);
-    launch_comb_cell_sums(h->stream, wS, h->combStart, N, h->combW);
+    if (strat) launch_strat_sums(h->stream, wS, start, N, B, h->stratBinW, h->combW);
+    else launch_comb_cell_sums(h->stream, wS, start, N, h->combW);
     launch_blocked_sum(h->stream, h->combW, N, h->combWtot);
     CombParams P;
     P.nmin = h->desc.comb_nmin;
     P.ntotal = static_cast<uint64_t>(static_cast<double>(static_cast<uint64_t>(N) * h->desc.comb_nmin) * h->desc.comb_factor);
-    launch_comb_plan(h->stream, h->C, P, wS, h->combStart, h->combW, h->combWtot, h->pCount, h->pWeight,
-                     h->combCount, h->A.eradCensus, h->dStats);
+    if (strat)
+        launch_strat_plan(h->stream, h->C, P, h->strat, wS, start, h->stratBinW, h->combW, h->combWtot, h->pCount,
+                          h->pWeight, h->combCount, h->A.eradCensus, h->dStats);
+    else
+        launch_comb_plan(h->stream, h->C, P, wS, start, h->combW, h->combWtot, h->pCount, h->pWeight,
+                         h->combCount, h->A.eradCensus, h->dStats);
     h->launches += 1 + 5 * passes + 5;
     CK(cudaGetLastError());
     uint32_t nValid = 0;
-    int rc = read_checked(h, &nValid, h->combStart + N, sizeof(uint32_t));
+    int rc = read_checked(h, &nValid, start + nRuns, sizeof(uint32_t));
     if (rc != STORM_OK) return rc;
     uint64_t *countU64 = alt ? h->keys : h->keysAlt;   // the sort's spare key buffer
     if (nValid) {
@@ -1131,7 +1166,8 @@ int storm_cuda_phase_comb(StormHandle *h) {
         CK(bank_alloc(h, h->bankA, grown));
         CK(bank_alloc(h, h->bankB, grown));
     }
-    launch_comb_emit(h->stream, h->C, h->bankC, idx, skeys, pidBits, nValid, h->pCount, h->pWeight, h->pOff, h->bankA);
+    launch_comb_emit(h->stream, h->C, h->bankC, idx, skeys, pidBits, B, nValid, h->pCount, h->pWeight, h->pOff,
+                     h->bankA);
     ++h->launches;
     CK(cudaGetLastError());
     if (grown) {

@@ -79,6 +79,11 @@ class Problem:
     ddmc_use_multigroup_pgrw: bool = False
     ddmc_min_cell_optical_depth: float = 15.0
     ddmc_min_particle_optical_depth: float = 5.0
+    # population control: CombPopulationControl, or StratifiedCombPopulationControl with frequency bins
+    comb_kind: int = A.COMB_PLAIN
+    strat_bins: int = 1
+    strat_bounds: np.ndarray = None
+    strat_min_per_bin: int = 2
 
     @property
     def shape(self):
@@ -166,6 +171,10 @@ class Problem:
         d.ddmc_use_multigroup_pgrw = int(self.ddmc_use_multigroup_pgrw)
         d.ddmc_min_cell_optical_depth = self.ddmc_min_cell_optical_depth
         d.ddmc_min_particle_optical_depth = self.ddmc_min_particle_optical_depth
+        d.comb_kind = self.comb_kind
+        d.strat_bins = self.strat_bins
+        d.strat_bounds = arr(self.strat_bounds)
+        d.strat_min_per_bin = self.strat_min_per_bin
         d._keep = keep
         return d
 
@@ -474,4 +483,20 @@ def ddmc_cube(n=8, new_photons_per_cell=3, face_packets=40, comb_nmin=20, seed=4
     p.with_ddmc = True
     p.rw_min_particle_optical_depth = rw_min_particle_optical_depth
     p.name = "ddmc_cube"
+    return p
+
+
+def strat_cube(n=4, groups=30, bins=6, comb_nmin=4, comb_factor=2.0, min_per_bin=2, new_photons_per_cell=6, seed=42,
+               precision=A.PRECISION_FP64):
+    """A small multigroup cube whose population control is
+    StratifiedCombPopulationControl with `bins` frequency bins, every
+    (groups / bins)-th group bound an edge."""
+    p = mg_cube(n=n, groups=groups, kappa0=1.0, new_photons_per_cell=new_photons_per_cell, comb_nmin=comb_nmin,
+                seed=seed, precision=precision, group_constant=False)
+    p.comb_factor = comb_factor
+    p.comb_kind = A.COMB_STRATIFIED
+    p.strat_bins = bins
+    p.strat_bounds = p.group_bounds[::groups // bins].copy()
+    p.strat_min_per_bin = min_per_bin
+    p.name = "strat_cube"
     return p

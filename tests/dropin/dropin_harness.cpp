@@ -79,6 +79,10 @@ DropinHandle *dropin_create(const StormProblemDesc *d, int precision, char *err,
         b.combEnabled = d->comb_enabled != 0;
         b.combNmin = d->comb_nmin;
         b.combFactor = d->comb_factor;
+        b.combKind = d->comb_kind;
+        b.stratBins = d->strat_bins;
+        if (d->strat_bounds) b.stratBounds.assign(d->strat_bounds, d->strat_bounds + d->strat_bins + 1);
+        b.stratMinPerBin = d->strat_min_per_bin;
         b.clight = d->clight; b.arad = d->arad; b.sigmaSB = d->sigma_sb; b.kevKelvin = d->kev_kelvin;
         b.seed = d->seed;
         b.precision = precision;

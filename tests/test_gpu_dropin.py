@@ -102,16 +102,20 @@ def _close(a, b, rel, atol=1e-300):
     return np.abs(a - b) <= rel * np.maximum(np.abs(a), np.abs(b)) + atol
 
 
-@pytest.mark.parametrize("kind", ["slab", "cube", "multigroup"])
+@pytest.mark.parametrize("kind", ["slab", "cube", "multigroup", "stratified", "ddmc"])
 def test_dropin_matches_engine(kind):
     L = _lib()
     if kind == "slab":
         p = problems.gray_slab(new_photons_per_cell=5, face_packets=2000, comb_nmin=50)
     elif kind == "cube":
         p = problems.step_cube(n=12, new_photons_per_cell=3, face_packets=60, comb_nmin=10)
-    else:   # RadiationIMC<..., 30> with multigroup opacity and a Planck face source
+    elif kind == "multigroup":   # RadiationIMC<..., 30> with multigroup opacity and a Planck face source
         p = problems.densmore2012(nx=16, new_photons_per_cell=4, boundary_per_face=50)
         p.comb_nmin = 10
+    elif kind == "stratified":   # StratifiedCombPopulationControl with frequency bins
+        p = problems.strat_cube(n=4)
+    else:   # DDMC leakage in the thick half
+        p = problems.ddmc_cube(n=8, new_photons_per_cell=3, face_packets=40, comb_nmin=10)
     d = DropIn(L, p)
     e = Engine(p)
     try:
