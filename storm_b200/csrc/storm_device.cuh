@@ -477,7 +477,7 @@ __device__ inline double mg_thermal_energy(const Ctx &C, uint32_t c, double rand
 // ------------------------------------------------------------------ Random Walk jump
 // RadiationIMC::tryRandomWalkStep (radiation/RadiationIMC.hpp:1065-1276), gray.
 // Returns -1 when the walk is not taken (no draws consumed), else a ParticleStatus.
-template <class RNG, class TALLY>
+template <bool MGP, class RNG, class TALLY>
 __device__ inline int try_random_walk(const Ctx &C, PartReg &p, RNG &rng, TALLY &tal, const double4 &cp, double xl,
                                       double xh, double yl, double yh, double zl, double zh, double cx, double cy,
                                       double cz) {
@@ -489,7 +489,7 @@ __device__ inline int try_random_walk(const Ctx &C, PartReg &p, RNG &rng, TALLY 
     for (int s = 0; s < 6; ++s) Ro = (d[s] < Ro) ? d[s] : Ro;
     Ro = (Ro > 0.0) ? Ro : 0.0;
     const double c = C.clight;
-    const bool pgrw = C.groups >= 2;
+    const bool pgrw = MGP && C.groups >= 2;
     double sigmaT, sigmaAeff, Dphys, gammaRw = 1.0;
     uint32_t cutoff = 0;
     if (pgrw) {   // PGRW cell data (:1080-1087)
@@ -750,7 +750,10 @@ __device__ __forceinline__ void track_begin(const Ctx &C, Track &T) {
 // |n_a| |v_b| with |n_b| |v_a| (no division), and only the winner's exit time
 // is divided out: that time is bit-identical to the reference's; the choice of
 // face can differ only when two exit times agree to within rounding.
-template <class RNG, class TALLY>
+//
+// FULL compiles the multigroup and DDMC branches in; the gray FP64 transport
+// without DDMC runs the lean instantiation, which needs fewer registers.
+template <bool FULL, class RNG, class TALLY>
 __device__ inline PhysOut physics_step(const Ctx &C, Track &T, RNG &rng, TALLY &tal) {
     PartReg &p = T.p;
     PhysOut o;
@@ -791,7 +794,7 @@ __device__ inline PhysOut physics_step(const Ctx &C, Track &T, RNG &rng, TALLY &
     }
     double4 cp = C.phys[cell];
     double elastic = 0.0, eventOpacity = 0.0;
-    if (C.groups >= 2) {
+    if (FULL && C.groups >= 2) {
         // CalcAbsorptionOpacity at the particle's frequency (:1742-1754)
         const double f = C.fleck[cell];
         const double absorptionOpacity = mg_absorption(C, cell, mg_clamp(C, p.nu));
@@ -804,7 +807,7 @@ __device__ inline PhysOut physics_step(const Ctx &C, Track &T, RNG &rng, TALLY &
     }
 
     if (C.withRW && C.rwElig[cell]) {
-        int r = try_random_walk(C, p, rng, tal, cp, xl, xh, yl, yh, zl, zh, C.xc[i], C.yc[j], C.zc[k]);
+        int r = try_random_walk<FULL>(C, p, rng, tal, cp, xl, xh, yl, yh, zl, zh, C.xc[i], C.yc[j], C.zc[k]);
         if (r == -2) { o.errCode = STORM_DERR_RW_SHRINK; return o; }
         if (r >= 0) {
             o.status = r;
@@ -813,7 +816,7 @@ __device__ inline PhysOut physics_step(const Ctx &C, Track &T, RNG &rng, TALLY &
             return o;
         }
     }
-    if (C.withDDMC) {
+    if (FULL && C.withDDMC) {
         int dface = -1;
         uint32_t dnext = OUTSIDE;
         const int r = try_ddmc(C, p, rng, tal, xl, xh, yl, yh, zl, zh, dface, dnext);
@@ -861,7 +864,7 @@ __device__ inline PhysOut physics_step(const Ctx &C, Track &T, RNG &rng, TALLY &
         o.next = next;
         if (next == OUTSIDE) o.ghost = C.ncells + face_index(C, i, j, k, face);
     } else if (best == 1) {
-        if (C.groups >= 2) {
+        if (FULL && C.groups >= 2) {
             // elastic or effective scatter (:1826-1852): both re-scatter
             // isotropically; an effective scatter re-emits from the spectrum
             const double eventRandom = rng.open() * eventOpacity;

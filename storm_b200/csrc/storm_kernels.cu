@@ -1072,7 +1072,10 @@ __device__ __forceinline__ void block_stats_flush(const BlockStats &bs, DevStats
 
 // The two particle forms behind one interface: the FP64 form (global FP64
 // coordinates, the reference's arithmetic) and the FP32-tracking form.
-struct Form64 {
+// Form64T<false> is the gray FP64 form without DDMC; Form64T<true> adds the
+// multigroup and DDMC branches.
+template <bool FULL>
+struct Form64T {
     using T = Track;
     using Rng = PhiloxRng;
     static __device__ __forceinline__ void load(const Ctx &C, const Bank &b, uint32_t q, T &t) {
@@ -1088,7 +1091,7 @@ struct Form64 {
     }
     template <class RNG, class TALLY>
     static __device__ __forceinline__ int seg(const Ctx &C, T &t, RNG &rng, TALLY &tal, int &usedRW, int &err) {
-        PhysOut o = physics_step(C, t, rng, tal);
+        PhysOut o = physics_step<FULL>(C, t, rng, tal);
         if (o.errCode) { err = o.errCode; return OUT_ERROR; }
         usedRW = o.usedRW == 1;   // Random Walk jumps (2 marks a DDMC step)
         int m = manager_handle(C, t, o);
@@ -1098,6 +1101,8 @@ struct Form64 {
     static __device__ __forceinline__ uint32_t cell(const T &t) { return t.p.cell; }
     static __device__ __forceinline__ double weight(const T &t) { return t.p.w; }
 };
+using Form64 = Form64T<false>;
+using Form64Full = Form64T<true>;
 struct Form32 {
     using T = Track32;
     using Rng = PhiloxRng4;
@@ -1211,7 +1216,7 @@ __global__ void __launch_bounds__(256, MINB) k_transport(Ctx C, Bank in, const u
                                                           DevStats *st) {
     __shared__ BlockStats bs;
     block_stats_zero(bs);
-    visit_bank<Form64>(C, in, *nIn, out, nOut, cen, nCen, K, bs);
+    visit_bank<Form64Full>(C, in, *nIn, out, nOut, cen, nCen, K, bs);
     block_stats_flush(bs, st);
 }
 
@@ -1996,7 +2001,7 @@ __global__ void k_replay(Ctx C, ReplayDev R, uint32_t n) {
         track_begin(C, T);
         TapeRng rng{R.tape + R.tapeOffset[q], R.tapeLength[q], 0, false};
         LocalTally tal{0.0, 0.0};
-        PhysOut o = physics_step(C, T, rng, tal);
+        PhysOut o = physics_step<true>(C, T, rng, tal);
         R.phys[0][q] = p.x; R.phys[1][q] = p.y; R.phys[2][q] = p.z;
         R.phys[3][q] = p.vx; R.phys[4][q] = p.vy; R.phys[5][q] = p.vz;
         R.phys[6][q] = p.t; R.phys[7][q] = p.w;
@@ -2274,6 +2279,7 @@ void launch_transport_refill(cudaStream_t s, uint32_t grid, int minBlocks, const
                              DevStats *st) {
     if (C.fp32 && C.groups >= 2) refill_launch<Form32MG>(s, grid, minBlocks, C, in, n, nextIdx, cen, nCen, burst, maxSegs, st);
     else if (C.fp32) refill_launch<Form32>(s, grid, minBlocks, C, in, n, nextIdx, cen, nCen, burst, maxSegs, st);
+    else if (C.groups >= 2 || C.withDDMC) refill_launch<Form64Full>(s, grid, minBlocks, C, in, n, nextIdx, cen, nCen, burst, maxSegs, st);
     else refill_launch<Form64>(s, grid, minBlocks, C, in, n, nextIdx, cen, nCen, burst, maxSegs, st);
 }
 template <class F>
