@@ -36,7 +36,7 @@
 extern "C" {
 #endif
 
-#define STORM_CUDA_ABI_VERSION 5
+#define STORM_CUDA_ABI_VERSION 6
 
 /* ---------------------------------------------------------------- status */
 enum StormStatus {
@@ -103,6 +103,29 @@ enum StormEosKind {
 };
 
 /* ---------------------------------------------------------------- descriptor */
+
+/* A convex-polyhedral mesh in a box (the engine's stand-in for the reference's
+ * Voronoi grids, MadVoro): cells, each with its faces in GetCellFaces order, and
+ * per face the two cells it separates (the second >= ncells for a face on the
+ * box: the ghost ncells + face index), its unit normal from the first cell to
+ * the second, centroid, area and polygon.  Cell-move nudges aim at the mesh
+ * points (the Voronoi generators), as the reference's manager does with
+ * GetMeshPoint (manager/MonteCarloManagerSerial.hpp:323-327). */
+typedef struct StormPolyMesh {
+    uint32_t ncells, nfaces, nvertices, pad_;
+    double box[6];                       /* lo x, y, z, hi x, y, z */
+    const double *points;                /* 3 ncells: mesh points */
+    const double *volume;                /* ncells */
+    const uint32_t *cell_face_offset;    /* ncells + 1 */
+    const uint32_t *cell_faces;          /* global face indices */
+    const uint32_t *face_cells;          /* 2 nfaces */
+    const double *face_normal;           /* 3 nfaces */
+    const double *face_cm;               /* 3 nfaces */
+    const double *face_area;             /* nfaces */
+    const uint32_t *face_vertex_offset;  /* nfaces + 1 */
+    const uint32_t *face_vertices;       /* ordered around each face */
+    const double *vertices;              /* 3 nvertices */
+} StormPolyMesh;
 
 /* One of the six faces of the bounding box, in GetBoxFaces() order:
  * 0 x-low, 1 x-high, 2 y-low, 3 y-high, 4 z-low, 5 z-high. */
@@ -201,6 +224,11 @@ typedef struct StormProblemDesc {
     const double *strat_bounds;      /* strat_bins + 1 increasing frequencies [erg]; NULL: one bin (gray), or the
                                         problem's group_bounds when strat_bins equals groups */
     uint64_t strat_min_per_bin;      /* minParticlesPerGroup (reference default 2) */
+
+    /* ---- convex-polyhedral mesh (NULL: the Cartesian grid of nx, ny, nz and the
+     * edges).  With a mesh, the per-cell arrays follow its cell order and the box
+     * faces are the mesh's box; the FP64 form, no DDMC and no face sources. */
+    const struct StormPolyMesh *mesh;
 } StormProblemDesc;
 
 #define STORM_STRAT_MAX_BINS 64
@@ -388,6 +416,15 @@ int storm_cuda_random_walk_sample(StormHandle *h, uint64_t n, const double *xi_l
 int storm_cuda_emission_allocation_noalloc(int device, const double *d_energy, uint32_t ncells,
                                            uint64_t new_photons_per_cell, uint64_t *d_photons,
                                            uint64_t *d_offsets, void *stream);
+
+/* ---------------------------------------------------------------- meshes */
+
+/* A bounded Voronoi tessellation of `n` generator points (3 n doubles, strictly
+ * inside the box lo x, y, z, hi x, y, z), built on the host.  No reference
+ * counterpart in this repository's path: the reference takes Voronoi grids from
+ * the MadVoro library.  The mesh is owned by the library until storm_mesh_free. */
+int storm_mesh_voronoi(const double *points, uint32_t n, const double box[6], StormPolyMesh **out);
+int storm_mesh_free(StormPolyMesh *mesh);
 
 /* ---------------------------------------------------------------- serving */
 

@@ -516,10 +516,32 @@ typedef struct RefStepOut {
 RefHandle *ref_create(const StormProblemDesc *d, int boundary_kind, char *err, size_t errlen) {
     try {
         auto h = std::make_unique<RefHandle>();
-        std::vector<double> xe(d->x_edges, d->x_edges + d->nx + 1), ye(d->y_edges, d->y_edges + d->ny + 1),
-            ze(d->z_edges, d->z_edges + d->nz + 1);
-        h->xe = xe; h->ye = ye; h->ze = ze;
-        h->grid = std::make_unique<Grid>(xe, ye, ze);
+        if (d->mesh) {   // a convex-polyhedral mesh, in the grid stand-in's polyhedral mode
+            const StormPolyMesh *m = d->mesh;
+            const std::size_t n = m->ncells, F = m->nfaces;
+            std::vector<Vector3D> pts(n), nrm(F), cm(F), nodes(m->nvertices);
+            for (std::size_t c = 0; c < n; ++c) pts[c] = Vector3D(m->points[3 * c], m->points[3 * c + 1], m->points[3 * c + 2]);
+            std::vector<std::vector<std::size_t>> cf(n), fv(F);
+            for (std::size_t c = 0; c < n; ++c)
+                for (uint32_t q = m->cell_face_offset[c]; q < m->cell_face_offset[c + 1]; ++q) cf[c].push_back(m->cell_faces[q]);
+            std::vector<std::pair<std::size_t, std::size_t>> fn(F);
+            std::vector<double> area(m->face_area, m->face_area + F), vol(m->volume, m->volume + n);
+            for (std::size_t f = 0; f < F; ++f) {
+                fn[f] = {m->face_cells[2 * f], m->face_cells[2 * f + 1]};
+                nrm[f] = Vector3D(m->face_normal[3 * f], m->face_normal[3 * f + 1], m->face_normal[3 * f + 2]);
+                cm[f] = Vector3D(m->face_cm[3 * f], m->face_cm[3 * f + 1], m->face_cm[3 * f + 2]);
+                for (uint32_t q = m->face_vertex_offset[f]; q < m->face_vertex_offset[f + 1]; ++q) fv[f].push_back(m->face_vertices[q]);
+            }
+            for (std::size_t v = 0; v < m->nvertices; ++v)
+                nodes[v] = Vector3D(m->vertices[3 * v], m->vertices[3 * v + 1], m->vertices[3 * v + 2]);
+            h->grid = std::make_unique<Grid>(Vector3D(m->box[0], m->box[1], m->box[2]), Vector3D(m->box[3], m->box[4], m->box[5]),
+                                             pts, cf, fn, nrm, cm, area, vol, fv, nodes);
+        } else {
+            std::vector<double> xe(d->x_edges, d->x_edges + d->nx + 1), ye(d->y_edges, d->y_edges + d->ny + 1),
+                ze(d->z_edges, d->z_edges + d->nz + 1);
+            h->xe = xe; h->ye = ye; h->ze = ze;
+            h->grid = std::make_unique<Grid>(xe, ye, ze);
+        }
         const std::size_t N = h->grid->GetPointNo();
         h->cells.resize(N);
         h->ext.resize(N);

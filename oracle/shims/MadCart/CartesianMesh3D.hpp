@@ -23,6 +23,7 @@
 #define STORM_SHIM_MADCART_CARTESIAN_MESH3D_HPP
 
 #include <algorithm>
+#include <cmath>
 #include <cstddef>
 #include <stdexcept>
 #include <utility>
@@ -59,12 +60,51 @@ public:
         build();
     }
 
+    // A convex-polyhedral mesh in the box [lo, hi] (the stand-in for the
+    // reference's Voronoi grids): per cell its faces, per face its neighbours
+    // (the second >= N for a face on the box: the ghost N + f, whose mesh
+    // point mirrors the cell's across that box plane), unit normal, centroid,
+    // area and polygon.
+    CartesianMesh3D(const PointT &lo, const PointT &hi, const std::vector<PointT> &points,
+                    const std::vector<std::vector<std::size_t>> &cellFaces,
+                    const std::vector<std::pair<std::size_t, std::size_t>> &faceNeighbors,
+                    const std::vector<PointT> &normals, const std::vector<PointT> &faceCM,
+                    const std::vector<double> &faceArea, const std::vector<double> &volume,
+                    const std::vector<std::vector<std::size_t>> &faceVerts, const std::vector<PointT> &nodes)
+        : xe_{lo.x, hi.x}, ye_{lo.y, hi.y}, ze_{lo.z, hi.z}, generation_(nextGeneration()), poly_(true) {
+        N_ = points.size();
+        nx_ = ny_ = nz_ = 0;
+        points_ = points;
+        cellFaces_ = cellFaces;
+        faceNeighbors_ = faceNeighbors;
+        normals_ = normals;
+        faceCM_ = faceCM;
+        faceArea_ = faceArea;
+        volume_ = volume;
+        faceVerts_ = faceVerts;
+        nodes_ = nodes;
+        points_.resize(N_ + faceNeighbors_.size());
+        for (std::size_t f = 0; f < faceNeighbors_.size(); ++f) {
+            const std::size_t g = faceNeighbors_[f].second;
+            if (g < N_) continue;
+            const PointT &c = faceCM_[f], &n = normals_[f];
+            PointT m = points_[faceNeighbors_[f].first];
+            // mirror across the box plane the face lies on
+            if (std::abs(n.x) > 0.5) m.x = 2.0 * c.x - m.x;
+            else if (std::abs(n.y) > 0.5) m.y = 2.0 * c.y - m.y;
+            else m.z = 2.0 * c.z - m.z;
+            points_[g] = m;
+        }
+        buildBoxFaces();
+    }
+
     std::size_t GetPointNo() const { return N_; }
     const PointT &GetMeshPoint(std::size_t i) const { return points_[i]; }
     const PointT &GetCellCM(std::size_t i) const { return points_[i]; }
     const std::vector<std::size_t> &GetCellFaces(std::size_t c) const { return cellFaces_[c]; }
     const std::pair<std::size_t, std::size_t> &GetFaceNeighbors(std::size_t f) const { return faceNeighbors_[f]; }
     PointT Normal(std::size_t f) const {
+        if (poly_) return normals_[f];
         int a = faceAxis(f);
         return PointT(a == 0 ? 1.0 : 0.0, a == 1 ? 1.0 : 0.0, a == 2 ? 1.0 : 0.0);
     }
@@ -81,15 +121,35 @@ public:
     }
     bool IsPointOutsideBox(std::size_t index) const { return index >= N_; }
     std::size_t GetContainingCell(const PointT &p) const {
+        if (poly_) {   // the nearest mesh point (Voronoi cells)
+            std::size_t best = 0;
+            double bd = 1e300;
+            for (std::size_t c = 0; c < N_; ++c) {
+                const double dx = p.x - points_[c].x, dy = p.y - points_[c].y, dz = p.z - points_[c].z;
+                const double d = dx * dx + dy * dy + dz * dz;
+                if (d < bd) { bd = d; best = c; }
+            }
+            return best;
+        }
         std::size_t i = locate(xe_, p.x), j = locate(ye_, p.y), k = locate(ze_, p.z);
         return i + nx_ * (j + ny_ * k);
     }
     bool IsPointInCell(const PointT &p, std::size_t c) const {
+        if (poly_) {
+            for (std::size_t f : cellFaces_[c]) {
+                PointT n = normals_[f];
+                const PointT &q = faceCM_[f];
+                const double side = n.x * (points_[c].x - q.x) + n.y * (points_[c].y - q.y) + n.z * (points_[c].z - q.z);
+                const double d = n.x * (p.x - q.x) + n.y * (p.y - q.y) + n.z * (p.z - q.z);
+                if ((side >= 0 ? d : -d) < 0) return false;
+            }
+            return true;
+        }
         std::size_t i = c % nx_, j = (c / nx_) % ny_, k = c / (nx_ * ny_);
         return p.x >= xe_[i] && p.x <= xe_[i + 1] && p.y >= ye_[j] && p.y <= ye_[j + 1] && p.z >= ze_[k] &&
                p.z <= ze_[k + 1];
     }
-    std::size_t GetTotalFacesNumber() const { return nxf_ + nyf_ + nzf_; }
+    std::size_t GetTotalFacesNumber() const { return poly_ ? faceNeighbors_.size() : nxf_ + nyf_ + nzf_; }
     const std::vector<std::size_t> &GetPointsInFace(std::size_t f) const { return faceVerts_[f]; }
     const std::vector<PointT> &GetFacePoints() const { return nodes_; }
     // Unique per grid object: RandomPointOnFace (utils/RandomOnFace.hpp:20-33)
@@ -183,6 +243,12 @@ private:
         // box faces
         const double X0 = xe_.front(), X1 = xe_.back(), Y0 = ye_.front(), Y1 = ye_.back(), Z0 = ze_.front(),
                      Z1 = ze_.back();
+        (void)X0; (void)X1; (void)Y0; (void)Y1; (void)Z0; (void)Z1;
+        buildBoxFaces();
+    }
+    void buildBoxFaces() {
+        const double X0 = xe_.front(), X1 = xe_.back(), Y0 = ye_.front(), Y1 = ye_.back(), Z0 = ze_.front(),
+                     Z1 = ze_.back();
         boxFaces_.resize(6);
         boxFaces_[0].vertices = {PointT(X0, Y0, Z0), PointT(X0, Y1, Z0), PointT(X0, Y1, Z1), PointT(X0, Y0, Z1)};
         boxFaces_[1].vertices = {PointT(X1, Y0, Z0), PointT(X1, Y1, Z0), PointT(X1, Y1, Z1), PointT(X1, Y0, Z1)};
@@ -210,6 +276,8 @@ private:
 
     std::vector<double> xe_, ye_, ze_;
     std::size_t generation_ = 0;
+    bool poly_ = false;
+    std::vector<PointT> normals_;
     std::size_t nx_ = 0, ny_ = 0, nz_ = 0, N_ = 0, nxf_ = 0, nyf_ = 0, nzf_ = 0;
     std::vector<PointT> nodes_, points_, faceCM_;
     std::vector<double> volume_, faceArea_;

@@ -5,7 +5,7 @@ sizes against the compiled library.
 """
 import ctypes as C
 
-ABI_VERSION = 5
+ABI_VERSION = 6
 
 STORM_OK = 0
 STATUS_NAMES = {
@@ -46,6 +46,16 @@ class StormBoxFace(C.Structure):
     ]
 
 
+class StormPolyMesh(C.Structure):
+    _fields_ = [
+        ("ncells", C.c_uint32), ("nfaces", C.c_uint32), ("nvertices", C.c_uint32), ("pad_", C.c_uint32),
+        ("box", C.c_double * 6), ("points", _dp), ("volume", _dp),
+        ("cell_face_offset", _u32p), ("cell_faces", _u32p), ("face_cells", _u32p),
+        ("face_normal", _dp), ("face_cm", _dp), ("face_area", _dp),
+        ("face_vertex_offset", _u32p), ("face_vertices", _u32p), ("vertices", _dp),
+    ]
+
+
 class StormProblemDesc(C.Structure):
     _fields_ = [
         ("abi_version", C.c_uint32),
@@ -77,6 +87,7 @@ class StormProblemDesc(C.Structure):
         ("ddmc_min_cell_optical_depth", C.c_double), ("ddmc_min_particle_optical_depth", C.c_double),
         ("comb_kind", C.c_int32), ("strat_bins", C.c_uint32), ("strat_bounds", _dp),
         ("strat_min_per_bin", C.c_uint64),
+        ("mesh", C.POINTER(StormPolyMesh)),
     ]
 
 

@@ -8,7 +8,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libstorm_cuda.so")
-SOURCES = ["storm_kernels.cu", "storm_runtime.cu", "storm_noalloc.cu", "storm_server.cpp"]
+SOURCES = ["storm_kernels.cu", "storm_runtime.cu", "storm_noalloc.cu", "storm_server.cpp", "storm_mesh.cpp"]
 HEADERS = ["storm_device.cuh", "storm_internal.h"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 # --fmad=false: plain expressions round like the reference's build (no contraction)

@@ -111,6 +111,17 @@ struct Ctx {
     uint32_t *ddmcCut;       // per cell: group cutoff (multigroup PGRW form)
     float4 *ddmc32;          // FP32 form, 3 per cell: (reach, 1/total, sigma_A f c, frequency bound),
                              // (cumulative face fractions 0-3), (fractions 4-5, last leak face, 0)
+    // convex-polyhedral mesh (poly != 0; nx = ncells, ny = nz = 1 so cell_ijk stays in range)
+    int32_t poly;
+    const uint32_t *cfo;     // per cell: its first cell-face slot (ncells + 1)
+    const double4 *cfN;      // per cell-face slot: the inward unit normal of updateGridData
+    const double4 *cfP;      // per cell-face slot: the face centroid (FaceCM)
+    const uint32_t *cfNext;  // per cell-face slot: the neighbour cell, or a ghost >= ncells
+    const uint32_t *cfFace;  // per cell-face slot: the global face index
+    const double *mpx, *mpy, *mpz;   // mesh points (GetMeshPoint)
+    const uint32_t *fvo, *fvi;       // face polygons: offsets (nfaces + 1) and vertex indices
+    const double *vtx;       // polygon vertices, 3 per vertex
+    const double *chord;     // per cell: 4 V / S
 };
 
 // ------------------------------------------------------------------ errors
@@ -477,16 +488,47 @@ __device__ inline double mg_thermal_energy(const Ctx &C, uint32_t c, double rand
 // ------------------------------------------------------------------ Random Walk jump
 // RadiationIMC::tryRandomWalkStep (radiation/RadiationIMC.hpp:1065-1276), gray.
 // Returns -1 when the walk is not taken (no draws consumed), else a ParticleStatus.
-template <bool MGP, class RNG, class TALLY>
-__device__ inline int try_random_walk(const Ctx &C, PartReg &p, RNG &rng, TALLY &tal, const double4 &cp, double xl,
-                                      double xh, double yl, double yh, double zl, double zh, double cx, double cy,
-                                      double cz) {
+// A cell's faces as computeMinDistanceToFaces and the Random Walk's shrink loop
+// see them: ScalarProd(location - facePoint, inwardNormal) per face in
+// GetCellFaces order, and the mesh point the nudges aim at.  On a Cartesian
+// cell the inward normals are exact unit vectors, so each product reduces
+// exactly to one coordinate difference.
+struct CartGeom {
+    double xl, xh, yl, yh, zl, zh, cx, cy, cz;
+    __device__ __forceinline__ int nf() const { return 6; }
+    __device__ __forceinline__ double dist(int s, double x, double y, double z) const {
+        switch (s) {
+        case 0: return x - xl;
+        case 1: return xh - x;
+        case 2: return y - yl;
+        case 3: return yh - y;
+        case 4: return z - zl;
+        default: return zh - z;
+        }
+    }
+};
+struct PolyGeom {
+    const Ctx *C;
+    uint32_t k0, k1;
+    double cx, cy, cz;
+    __device__ __forceinline__ int nf() const { return static_cast<int>(k1 - k0); }
+    __device__ __forceinline__ double dist(int s, double x, double y, double z) const {
+        const double4 n = C->cfN[k0 + s], q = C->cfP[k0 + s];
+        return (x - q.x) * n.x + (y - q.y) * n.y + (z - q.z) * n.z;
+    }
+};
+
+template <bool MGP, class GEOM, class RNG, class TALLY>
+__device__ inline int try_random_walk(const Ctx &C, PartReg &p, RNG &rng, TALLY &tal, const double4 &cp,
+                                      const GEOM &g) {
     const uint32_t cell = p.cell;
+    const double cx = g.cx, cy = g.cy, cz = g.cz;
     // computeMinDistanceToFaces (:956-969) in GetCellFaces order
-    double d[6] = {p.x - xl, xh - p.x, p.y - yl, yh - p.y, p.z - zl, zh - p.z};
     double Ro = DBL_MAX;
-#pragma unroll
-    for (int s = 0; s < 6; ++s) Ro = (d[s] < Ro) ? d[s] : Ro;
+    for (int s = 0; s < g.nf(); ++s) {
+        const double d = g.dist(s, p.x, p.y, p.z);
+        Ro = (d < Ro) ? d : Ro;
+    }
     Ro = (Ro > 0.0) ? Ro : 0.0;
     const double c = C.clight;
     const bool pgrw = MGP && C.groups >= 2;
@@ -549,16 +591,8 @@ __device__ inline int try_random_walk(const Ctx &C, PartReg &p, RNG &rng, TALLY 
     lz = lz * (1.0 - RW_NUDGE) + RW_NUDGE * cz;
     // shrink until inside every face plane (:1216-1228)
     int guard = 0;
-    for (int s = 0; s < 6; ++s) {
-        double q;
-        switch (s) {
-        case 0: q = lx - xl; break;
-        case 1: q = xh - lx; break;
-        case 2: q = ly - yl; break;
-        case 3: q = yh - ly; break;
-        case 4: q = lz - zl; break;
-        default: q = zh - lz; break;
-        }
+    for (int s = 0; s < g.nf(); ++s) {
+        const double q = g.dist(s, lx, ly, lz);
         if (q < 0.0) {
             disp *= 0.99;
             lx = ox + disp * dx;
@@ -753,8 +787,13 @@ __device__ __forceinline__ void track_begin(const Ctx &C, Track &T) {
 //
 // FULL compiles the multigroup and DDMC branches in; the gray FP64 transport
 // without DDMC runs the lean instantiation, which needs fewer registers.
-template <bool FULL, class RNG, class TALLY>
+//
+// V = 2 is the convex-polyhedral form: the face search of
+// distanceToNearestFace over the cell's inward normals and face centroids as
+// written (alpha = ((faceCM - x).n) / (n.v), the first smallest positive).
+template <int V, class RNG, class TALLY>
 __device__ inline PhysOut physics_step(const Ctx &C, Track &T, RNG &rng, TALLY &tal) {
+    constexpr bool FULL = V >= 1, POLY = V == 2;
     PartReg &p = T.p;
     PhysOut o;
     o.status = NO_CELL_MOVE;
@@ -765,11 +804,35 @@ __device__ inline PhysOut physics_step(const Ctx &C, Track &T, RNG &rng, TALLY &
     o.errCode = 0;
     const uint32_t cell = p.cell;
     const uint32_t i = T.i, j = T.j, k = T.k;
-    const double xl = C.xe[i], xh = C.xe[i + 1], yl = C.ye[j], yh = C.ye[j + 1], zl = C.ze[k], zh = C.ze[k + 1];
     const double thr = EPSILON_FACE * T.speed;
+    int face = -1;
+    uint32_t next;
+    double tFace;
+    if constexpr (POLY) {
+        const uint32_t k0 = C.cfo[cell], k1 = C.cfo[cell + 1];
+        double minAlpha = DBL_MAX;
+        for (uint32_t q = k0; q < k1; ++q) {
+            const double4 n = C.cfN[q];
+            const double nv = n.x * p.vx + n.y * p.vy + n.z * p.vz;
+            if (nv >= -thr) continue;
+            const double4 f = C.cfP[q];
+            const double alpha = ((f.x - p.x) * n.x + (f.y - p.y) * n.y + (f.z - p.z) * n.z) / nv;
+            if (alpha < minAlpha && alpha > 0) {
+                minAlpha = alpha;
+                face = static_cast<int>(q - k0);
+            }
+        }
+        if (face < 0) { o.errCode = STORM_DERR_NO_FACE; return o; }
+        tFace = minAlpha;
+        const uint32_t nb = C.cfNext[k0 + face];
+        next = nb < C.ncells ? nb : OUTSIDE;
+        if (next == OUTSIDE) o.ghost = nb;
+    }
+    const double xl = POLY ? 0.0 : C.xe[i], xh = POLY ? 0.0 : C.xe[i + 1], yl = POLY ? 0.0 : C.ye[j],
+                 yh = POLY ? 0.0 : C.ye[j + 1], zl = POLY ? 0.0 : C.ze[k], zh = POLY ? 0.0 : C.ze[k + 1];
+    if constexpr (!POLY) {
     // candidate face per axis: numerator (p_f - x) and velocity component
     double nb = 0.0, vb = 1.0;
-    int face = -1;
     {
         double n;
         bool ok;
@@ -781,9 +844,8 @@ __device__ inline PhysOut physics_step(const Ctx &C, Track &T, RNG &rng, TALLY &
         if (ok && (face < 0 || fabs(n) * fabs(vb) < fabs(nb) * fabs(p.vz))) { nb = n; vb = p.vz; face = p.vz > 0.0 ? 5 : 4; }
     }
     if (face < 0) { o.errCode = STORM_DERR_NO_FACE; return o; }
-    const double tFace = nb / vb;
+    tFace = nb / vb;
     if (!(tFace > 0.0)) { o.errCode = STORM_DERR_NO_FACE; return o; }
-    uint32_t next;
     switch (face) {
     case 0: next = (i > 0) ? cell - 1 : OUTSIDE; break;
     case 1: next = (i + 1 < C.nx) ? cell + 1 : OUTSIDE; break;
@@ -791,6 +853,7 @@ __device__ inline PhysOut physics_step(const Ctx &C, Track &T, RNG &rng, TALLY &
     case 3: next = (j + 1 < C.ny) ? cell + C.nx : OUTSIDE; break;
     case 4: next = (k > 0) ? cell - C.nx * C.ny : OUTSIDE; break;
     default: next = (k + 1 < C.nz) ? cell + C.nx * C.ny : OUTSIDE; break;
+    }
     }
     double4 cp = C.phys[cell];
     double elastic = 0.0, eventOpacity = 0.0;
@@ -807,7 +870,14 @@ __device__ inline PhysOut physics_step(const Ctx &C, Track &T, RNG &rng, TALLY &
     }
 
     if (C.withRW && C.rwElig[cell]) {
-        int r = try_random_walk<FULL>(C, p, rng, tal, cp, xl, xh, yl, yh, zl, zh, C.xc[i], C.yc[j], C.zc[k]);
+        int r;
+        if constexpr (POLY) {
+            const PolyGeom g{&C, C.cfo[cell], C.cfo[cell + 1], C.mpx[cell], C.mpy[cell], C.mpz[cell]};
+            r = try_random_walk<FULL>(C, p, rng, tal, cp, g);
+        } else {
+            const CartGeom g{xl, xh, yl, yh, zl, zh, C.xc[i], C.yc[j], C.zc[k]};
+            r = try_random_walk<FULL>(C, p, rng, tal, cp, g);
+        }
         if (r == -2) { o.errCode = STORM_DERR_RW_SHRINK; return o; }
         if (r >= 0) {
             o.status = r;
@@ -816,7 +886,7 @@ __device__ inline PhysOut physics_step(const Ctx &C, Track &T, RNG &rng, TALLY &
             return o;
         }
     }
-    if (FULL && C.withDDMC) {
+    if (FULL && !POLY && C.withDDMC) {
         int dface = -1;
         uint32_t dnext = OUTSIDE;
         const int r = try_ddmc(C, p, rng, tal, xl, xh, yl, yh, zl, zh, dface, dnext);
@@ -862,7 +932,7 @@ __device__ inline PhysOut physics_step(const Ctx &C, Track &T, RNG &rng, TALLY &
         o.status = CELL_MOVE;
         o.face = face;
         o.next = next;
-        if (next == OUTSIDE) o.ghost = C.ncells + face_index(C, i, j, k, face);
+        if (!POLY && next == OUTSIDE) o.ghost = C.ncells + face_index(C, i, j, k, face);
     } else if (best == 1) {
         if (FULL && C.groups >= 2) {
             // elastic or effective scatter (:1826-1852): both re-scatter
@@ -1283,9 +1353,19 @@ __device__ __forceinline__ void box_face_reflect(const BoxFaceDev &F, PartReg &p
 // (manager/MonteCarloManagerSerial.hpp:318-369), with BoundaryCondition::apply
 // for the per-face descriptor (VacuumBoundary, RigidBoundary, SideTemperature,
 // TwoSidesTemperature all lower to it).
+template <bool POLY = false>
 __device__ __forceinline__ int manager_handle(const Ctx &C, Track &T, const PhysOut &o) {
     PartReg &p = T.p;
     if (o.status == CELL_MOVE) {
+        if (POLY && o.next != OUTSIDE) {
+            const uint32_t nc = o.next;
+            p.x = (1 - MONTECARLO_EPS) * p.x + MONTECARLO_EPS * C.mpx[nc];
+            p.y = (1 - MONTECARLO_EPS) * p.y + MONTECARLO_EPS * C.mpy[nc];
+            p.z = (1 - MONTECARLO_EPS) * p.z + MONTECARLO_EPS * C.mpz[nc];
+            p.cell = nc;
+            T.i = nc;
+            return OUT_CONTINUE;
+        }
         if (o.next != OUTSIDE) {
             switch (o.face) {
             case 0: --T.i; break;
@@ -1313,9 +1393,11 @@ __device__ __forceinline__ int manager_handle(const Ctx &C, Track &T, const Phys
         }
         if (!reflected) return OUT_ERROR;
         T.speed = vnorm(p.vx, p.vy, p.vz);
-        p.x = (1 - MONTECARLO_EPS) * p.x + MONTECARLO_EPS * C.xc[T.i];
-        p.y = (1 - MONTECARLO_EPS) * p.y + MONTECARLO_EPS * C.yc[T.j];
-        p.z = (1 - MONTECARLO_EPS) * p.z + MONTECARLO_EPS * C.zc[T.k];
+        const double mx = POLY ? C.mpx[p.cell] : C.xc[T.i], my = POLY ? C.mpy[p.cell] : C.yc[T.j],
+                     mz = POLY ? C.mpz[p.cell] : C.zc[T.k];
+        p.x = (1 - MONTECARLO_EPS) * p.x + MONTECARLO_EPS * mx;
+        p.y = (1 - MONTECARLO_EPS) * p.y + MONTECARLO_EPS * my;
+        p.z = (1 - MONTECARLO_EPS) * p.z + MONTECARLO_EPS * mz;
         return OUT_CONTINUE;
     }
     if (o.status == REMOVE) return OUT_CUTOFF;

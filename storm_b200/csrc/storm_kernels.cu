@@ -247,6 +247,7 @@ __global__ void k_begin(Bank b, uint32_t n, double dt, DevStats *st) {
 
 // mean chord 4V/S of a cell (computeCellSurfaceArea, radiation/RadiationIMC.hpp:971-980, GetCellFaces order)
 __device__ __forceinline__ double cell_chord(const Ctx &C, const CellArrays &A, uint32_t c) {
+    if (C.poly) return C.chord[c];   // 4 V / S with S summed in GetCellFaces order on the host
     uint32_t i, j, k;
     cell_ijk(C, c, i, j, k);
     double dx = C.xe[i + 1] - C.xe[i], dy = C.ye[j + 1] - C.ye[j], dz = C.ze[k + 1] - C.ze[k];
@@ -766,6 +767,66 @@ __device__ inline void sample_in_cell(const Ctx &C, uint32_t cell, RNG &rng, dou
     pz = a0 * q[0][2] + a1 * q[tri][2] + a2 * q[tri + 1][2] + a3 * cz;
 }
 
+// The same sampler on a convex-polyhedral cell: the fan triangles
+// (v0, v_t, v_t+1) of each face polygon, faces in GetCellFaces order, make
+// tetrahedra with the mesh point; one is picked by std::lower_bound over the
+// running volume sum (summed again on the second pass, bit for bit), then the
+// point from three sorted uniforms.
+__device__ __forceinline__ double poly_tet_volume(const Ctx &C, uint32_t v0, uint32_t v1, uint32_t v2, double cx,
+                                                  double cy, double cz) {
+    const double ax = C.vtx[3 * v0] - cx, ay = C.vtx[3 * v0 + 1] - cy, az = C.vtx[3 * v0 + 2] - cz;
+    const double bx = C.vtx[3 * v1] - cx, by = C.vtx[3 * v1 + 1] - cy, bz = C.vtx[3 * v1 + 2] - cz;
+    const double ex = C.vtx[3 * v2] - cx, ey = C.vtx[3 * v2 + 1] - cy, ez = C.vtx[3 * v2 + 2] - cz;
+    const double crx = by * ez - bz * ey, cry = bz * ex - bx * ez, crz = bx * ey - by * ex;
+    return fabs(ax * crx + ay * cry + az * crz);
+}
+template <class RNG>
+__device__ inline void sample_in_poly_cell(const Ctx &C, uint32_t cell, RNG &rng, double &px, double &py, double &pz) {
+    const double cx = C.mpx[cell], cy = C.mpy[cell], cz = C.mpz[cell];
+    const uint32_t k0 = C.cfo[cell], k1 = C.cfo[cell + 1];
+    double total = 0.0;
+    uint32_t ntri = 0;
+    for (uint32_t q = k0; q < k1; ++q) {
+        const uint32_t f = C.cfFace[q], a = C.fvo[f], b = C.fvo[f + 1];
+        if (b - a < 3) continue;
+        for (uint32_t t = a + 1; t + 1 < b; ++t) {
+            total += poly_tet_volume(C, C.fvi[a], C.fvi[t], C.fvi[t + 1], cx, cy, cz);
+            ++ntri;
+        }
+    }
+    if (ntri == 0) { px = cx; py = cy; pz = cz; return; }
+    const double r = rng.raw() * total;
+    // the first triangle whose running sum is not below r, else the last
+    uint32_t v0 = 0, v1 = 0, v2 = 0;
+    bool found = false;
+    double run = 0.0;
+    for (uint32_t q = k0; q < k1 && !found; ++q) {
+        const uint32_t f = C.cfFace[q], a = C.fvo[f], b = C.fvo[f + 1];
+        if (b - a < 3) continue;
+        for (uint32_t t = a + 1; t + 1 < b; ++t) {
+            run += poly_tet_volume(C, C.fvi[a], C.fvi[t], C.fvi[t + 1], cx, cy, cz);
+            v0 = C.fvi[a]; v1 = C.fvi[t]; v2 = C.fvi[t + 1];
+            if (!(run < r)) { found = true; break; }
+        }
+    }
+    double s = rng.raw(), t = rng.raw(), u = rng.raw(), tmp;
+    if (s > t) { tmp = s; s = t; t = tmp; }
+    if (t > u) { tmp = t; t = u; u = tmp; }
+    if (s > t) { tmp = s; s = t; t = tmp; }
+    const double a0 = s, a1 = t - s, a2 = u - t, a3 = 1 - u;
+    px = a0 * C.vtx[3 * v0] + a1 * C.vtx[3 * v1] + a2 * C.vtx[3 * v2] + a3 * cx;
+    py = a0 * C.vtx[3 * v0 + 1] + a1 * C.vtx[3 * v1 + 1] + a2 * C.vtx[3 * v2 + 1] + a3 * cy;
+    pz = a0 * C.vtx[3 * v0 + 2] + a1 * C.vtx[3 * v1 + 2] + a2 * C.vtx[3 * v2 + 2] + a3 * cz;
+}
+
+// the cell's mesh point (GetMeshPoint)
+__device__ __forceinline__ void mesh_point(const Ctx &C, uint32_t c, double &mx, double &my, double &mz) {
+    if (C.poly) { mx = C.mpx[c]; my = C.mpy[c]; mz = C.mpz[c]; return; }
+    uint32_t i, j, k;
+    cell_ijk(C, c, i, j, k);
+    mx = C.xc[i]; my = C.yc[j]; mz = C.zc[k];
+}
+
 // RandomPointOnFace (utils/RandomOnFace.hpp:15-66) for a quad face.
 template <class RNG>
 __device__ inline void point_on_face(const double q[4][3], RNG &rng, double &px, double &py, double &pz) {
@@ -833,10 +894,11 @@ __global__ void k_emit_cells(Ctx C, CellArrays A, const uint64_t *offsets, uint6
         rng.init(C.seedLo, C.seedHi, TAG_CELL_EMIT, C.step, static_cast<uint32_t>(e), 0);
         PartReg p;
         p.cell = c;
-        sample_in_cell(C, c, rng, p.x, p.y, p.z);
-        uint32_t i, j, k;
-        cell_ijk(C, c, i, j, k);
-        repair_outside(C, p.x, p.y, p.z, C.xc[i], C.yc[j], C.zc[k]);
+        if (C.poly) sample_in_poly_cell(C, c, rng, p.x, p.y, p.z);
+        else sample_in_cell(C, c, rng, p.x, p.y, p.z);
+        double mx, my, mz;
+        mesh_point(C, c, mx, my, mz);
+        repair_outside(C, p.x, p.y, p.z, mx, my, mz);
         isotropic(rng, C.clight, p.vx, p.vy, p.vz);
         p.t = dt * rng.open();
         p.nu = 0.0;
@@ -1072,9 +1134,10 @@ __device__ __forceinline__ void block_stats_flush(const BlockStats &bs, DevStats
 
 // The two particle forms behind one interface: the FP64 form (global FP64
 // coordinates, the reference's arithmetic) and the FP32-tracking form.
-// Form64T<false> is the gray FP64 form without DDMC; Form64T<true> adds the
-// multigroup and DDMC branches.
-template <bool FULL>
+// Form64T<0> is the gray FP64 form without DDMC on a Cartesian grid;
+// Form64T<1> adds the multigroup and DDMC branches; Form64T<2> runs on a
+// convex-polyhedral mesh.
+template <int V>
 struct Form64T {
     using T = Track;
     using Rng = PhiloxRng;
@@ -1091,18 +1154,19 @@ struct Form64T {
     }
     template <class RNG, class TALLY>
     static __device__ __forceinline__ int seg(const Ctx &C, T &t, RNG &rng, TALLY &tal, int &usedRW, int &err) {
-        PhysOut o = physics_step<FULL>(C, t, rng, tal);
+        PhysOut o = physics_step<V>(C, t, rng, tal);
         if (o.errCode) { err = o.errCode; return OUT_ERROR; }
         usedRW = o.usedRW == 1;   // Random Walk jumps (2 marks a DDMC step)
-        int m = manager_handle(C, t, o);
+        int m = manager_handle<V == 2>(C, t, o);
         if (m == OUT_ERROR) err = STORM_DERR_NOT_ON_BOUNDARY;
         return m;
     }
     static __device__ __forceinline__ uint32_t cell(const T &t) { return t.p.cell; }
     static __device__ __forceinline__ double weight(const T &t) { return t.p.w; }
 };
-using Form64 = Form64T<false>;
-using Form64Full = Form64T<true>;
+using Form64 = Form64T<0>;
+using Form64Full = Form64T<1>;
+using Form64Poly = Form64T<2>;
 struct Form32 {
     using T = Track32;
     using Rng = PhiloxRng4;
@@ -1654,9 +1718,8 @@ __device__ __forceinline__ void comb_emit_fp64(const Ctx &C, PartReg &p, uint32_
     if (!(raw & KEEP)) { p.w = wNew; p.w0 = p.w; p.t = 0; }
     p.cell = c;
     if (outside_box(C, p.x, p.y, p.z)) {   // :228-250
-        uint32_t i, j, k;
-        cell_ijk(C, c, i, j, k);
-        const double mx = C.xc[i], my = C.yc[j], mz = C.zc[k];
+        double mx, my, mz;
+        mesh_point(C, c, mx, my, mz);
         const double ox = p.x, oy = p.y, oz = p.z, dx = mx - ox, dy = my - oy, dz = mz - oz;
         double t = 1e-6;
         while (outside_box(C, p.x, p.y, p.z) && t < 1.0) {
@@ -2001,7 +2064,7 @@ __global__ void k_replay(Ctx C, ReplayDev R, uint32_t n) {
         track_begin(C, T);
         TapeRng rng{R.tape + R.tapeOffset[q], R.tapeLength[q], 0, false};
         LocalTally tal{0.0, 0.0};
-        PhysOut o = physics_step<true>(C, T, rng, tal);
+        PhysOut o = C.poly ? physics_step<2>(C, T, rng, tal) : physics_step<1>(C, T, rng, tal);
         R.phys[0][q] = p.x; R.phys[1][q] = p.y; R.phys[2][q] = p.z;
         R.phys[3][q] = p.vx; R.phys[4][q] = p.vy; R.phys[5][q] = p.vz;
         R.phys[6][q] = p.t; R.phys[7][q] = p.w;
@@ -2012,7 +2075,7 @@ __global__ void k_replay(Ctx C, ReplayDev R, uint32_t n) {
         R.dep[1][q] = tal.rad_;
         R.usedRW[q] = o.usedRW;
         R.draws[q] = rng.pos;
-        int m = o.errCode ? OUT_ERROR : manager_handle(C, T, o);
+        int m = o.errCode ? OUT_ERROR : (C.poly ? manager_handle<true>(C, T, o) : manager_handle<false>(C, T, o));
         R.mgr[0][q] = p.x; R.mgr[1][q] = p.y; R.mgr[2][q] = p.z;
         R.mgr[3][q] = p.vx; R.mgr[4][q] = p.vy; R.mgr[5][q] = p.vz;
         R.mgrCell[q] = p.cell;
@@ -2279,6 +2342,7 @@ void launch_transport_refill(cudaStream_t s, uint32_t grid, int minBlocks, const
                              DevStats *st) {
     if (C.fp32 && C.groups >= 2) refill_launch<Form32MG>(s, grid, minBlocks, C, in, n, nextIdx, cen, nCen, burst, maxSegs, st);
     else if (C.fp32) refill_launch<Form32>(s, grid, minBlocks, C, in, n, nextIdx, cen, nCen, burst, maxSegs, st);
+    else if (C.poly) refill_launch<Form64Poly>(s, grid, minBlocks, C, in, n, nextIdx, cen, nCen, burst, maxSegs, st);
     else if (C.groups >= 2 || C.withDDMC) refill_launch<Form64Full>(s, grid, minBlocks, C, in, n, nextIdx, cen, nCen, burst, maxSegs, st);
     else refill_launch<Form64>(s, grid, minBlocks, C, in, n, nextIdx, cen, nCen, burst, maxSegs, st);
 }

@@ -61,6 +61,10 @@ struct StormHandle {
     double *ddmcTot = nullptr, *ddmcRate = nullptr;
     uint32_t *ddmcCut = nullptr;
     float4 *ddmc32 = nullptr;
+    // convex-polyhedral mesh
+    uint32_t *cfo = nullptr, *cfNext = nullptr, *cfFace = nullptr, *fvo = nullptr, *fvi = nullptr;
+    double4 *cfN = nullptr, *cfP = nullptr;
+    double *mpx = nullptr, *mpy = nullptr, *mpz = nullptr, *vtx = nullptr, *chord = nullptr;
     StratParams strat{1, nullptr, 2};         // stratified comb: bins, device bounds, minParticlesPerGroup
     double *stratBounds = nullptr, *stratBinW = nullptr;
     uint32_t *stratStart = nullptr;
@@ -599,13 +603,38 @@ int storm_cuda_create(const StormProblemDesc *d, StormHandle **out) {
         return STORM_ERR_INVALID_ARG;
     if (d->eos_kind != STORM_EOS_LINEAR && d->eos_kind != STORM_EOS_POWER_LAW) return STORM_ERR_UNSUPPORTED;
     if (d->precision != STORM_PRECISION_FP64 && d->precision != STORM_PRECISION_FP32_TRACK) return STORM_ERR_UNSUPPORTED;
-    uint64_t N64 = static_cast<uint64_t>(d->nx) * d->ny * d->nz;
-    if (N64 >= 0x7fffffffull) return STORM_ERR_INVALID_ARG;
-    for (int a = 0; a < 3; ++a) {
-        const double *e = a == 0 ? d->x_edges : (a == 1 ? d->y_edges : d->z_edges);
-        uint32_t n = a == 0 ? d->nx : (a == 1 ? d->ny : d->nz);
-        for (uint32_t q = 0; q < n; ++q)
-            if (!(e[q + 1] > e[q])) return STORM_ERR_INVALID_ARG;
+    const StormPolyMesh *mesh = d->mesh;
+    const bool poly = mesh != nullptr;
+    uint64_t N64 = poly ? mesh->ncells : static_cast<uint64_t>(d->nx) * d->ny * d->nz;
+    if (N64 == 0 || N64 >= 0x7fffffffull) return STORM_ERR_INVALID_ARG;
+    if (poly) {
+        if (!mesh->points || !mesh->volume || !mesh->cell_face_offset || !mesh->cell_faces || !mesh->face_cells ||
+            !mesh->face_normal || !mesh->face_cm || !mesh->face_area || !mesh->face_vertex_offset ||
+            !mesh->face_vertices || !mesh->vertices)
+            return STORM_ERR_INVALID_ARG;
+        if (!(mesh->box[3] > mesh->box[0] && mesh->box[4] > mesh->box[1] && mesh->box[5] > mesh->box[2]))
+            return STORM_ERR_INVALID_ARG;
+        for (uint32_t c = 0; c < mesh->ncells; ++c)
+            if (mesh->cell_face_offset[c + 1] < mesh->cell_face_offset[c]) return STORM_ERR_INVALID_ARG;
+        for (uint32_t q = 0; q < mesh->cell_face_offset[mesh->ncells]; ++q)
+            if (mesh->cell_faces[q] >= mesh->nfaces) return STORM_ERR_INVALID_ARG;
+        for (uint32_t f = 0; f < mesh->nfaces; ++f) {
+            if (mesh->face_cells[2 * f] >= mesh->ncells) return STORM_ERR_INVALID_ARG;
+            if (mesh->face_vertex_offset[f + 1] < mesh->face_vertex_offset[f]) return STORM_ERR_INVALID_ARG;
+        }
+        for (uint32_t q = 0; q < mesh->face_vertex_offset[mesh->nfaces]; ++q)
+            if (mesh->face_vertices[q] >= mesh->nvertices) return STORM_ERR_INVALID_ARG;
+        // the FP32-tracking form, DDMC and boundary sources are Cartesian only
+        if (d->precision != STORM_PRECISION_FP64 || d->with_ddmc) return STORM_ERR_UNSUPPORTED;
+        for (int f = 0; f < 6; ++f)
+            if (d->faces[f].source_temperature > 0.0 && d->faces[f].packets_per_face > 0) return STORM_ERR_UNSUPPORTED;
+    } else {
+        for (int a = 0; a < 3; ++a) {
+            const double *e = a == 0 ? d->x_edges : (a == 1 ? d->y_edges : d->z_edges);
+            uint32_t n = a == 0 ? d->nx : (a == 1 ? d->ny : d->nz);
+            for (uint32_t q = 0; q < n; ++q)
+                if (!(e[q + 1] > e[q])) return STORM_ERR_INVALID_ARG;
+        }
     }
     int ndev = 0;
     if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return STORM_ERR_NO_DEVICE;
@@ -613,8 +642,11 @@ int storm_cuda_create(const StormProblemDesc *d, StormHandle **out) {
 
     StormHandle *h = new StormHandle();
     h->desc = *d;
+    h->desc.mesh = nullptr;   // the mesh is copied to the device below; the caller may free it
     h->device = d->device;
-    h->nx = d->nx; h->ny = d->ny; h->nz = d->nz;
+    h->nx = poly ? static_cast<uint32_t>(N64) : d->nx;   // a polyhedral mesh: cell_ijk(c) = (c, 0, 0)
+    h->ny = poly ? 1 : d->ny;
+    h->nz = poly ? 1 : d->nz;
     h->N = static_cast<uint32_t>(N64);
     const uint32_t N = h->N;
     auto fail = [&](int rc) {
@@ -630,25 +662,33 @@ int storm_cuda_create(const StormProblemDesc *d, StormHandle **out) {
     cudaEventCreate(&h->evAfterEmit);
     cudaEventCreate(&h->evAfterComb);
 
-    h->hxe.assign(d->x_edges, d->x_edges + d->nx + 1);
-    h->hye.assign(d->y_edges, d->y_edges + d->ny + 1);
-    h->hze.assign(d->z_edges, d->z_edges + d->nz + 1);
-    h->hxc.resize(d->nx); h->hyc.resize(d->ny); h->hzc.resize(d->nz);
-    for (uint32_t i = 0; i < d->nx; ++i) h->hxc[i] = 0.5 * (h->hxe[i] + h->hxe[i + 1]);
-    for (uint32_t j = 0; j < d->ny; ++j) h->hyc[j] = 0.5 * (h->hye[j] + h->hye[j + 1]);
-    for (uint32_t k = 0; k < d->nz; ++k) h->hzc[k] = 0.5 * (h->hze[k] + h->hze[k + 1]);
+    // Cartesian: the edges and centres; a polyhedral mesh: its box as one "cell" per axis
+    const uint32_t ex = poly ? 1 : d->nx, ey = poly ? 1 : d->ny, ez = poly ? 1 : d->nz;
+    if (poly) {
+        h->hxe = {mesh->box[0], mesh->box[3]};
+        h->hye = {mesh->box[1], mesh->box[4]};
+        h->hze = {mesh->box[2], mesh->box[5]};
+    } else {
+        h->hxe.assign(d->x_edges, d->x_edges + d->nx + 1);
+        h->hye.assign(d->y_edges, d->y_edges + d->ny + 1);
+        h->hze.assign(d->z_edges, d->z_edges + d->nz + 1);
+    }
+    h->hxc.resize(ex); h->hyc.resize(ey); h->hzc.resize(ez);
+    for (uint32_t i = 0; i < ex; ++i) h->hxc[i] = 0.5 * (h->hxe[i] + h->hxe[i + 1]);
+    for (uint32_t j = 0; j < ey; ++j) h->hyc[j] = 0.5 * (h->hye[j] + h->hye[j + 1]);
+    for (uint32_t k = 0; k < ez; ++k) h->hzc[k] = 0.5 * (h->hze[k] + h->hze[k + 1]);
 
 #define ALLOC(ptr, n) do { if (dalloc(h, &(ptr), (n)) != cudaSuccess) return fail(STORM_ERR_OOM); } while (0)
 #define H2D(dst, src, n) do { if (cudaMemcpy((dst), (src), sizeof(*(dst)) * (n), cudaMemcpyHostToDevice) != cudaSuccess) return fail(STORM_ERR_CUDA); } while (0)
-    ALLOC(h->xe, d->nx + 1); ALLOC(h->ye, d->ny + 1); ALLOC(h->ze, d->nz + 1);
-    ALLOC(h->xc, d->nx); ALLOC(h->yc, d->ny); ALLOC(h->zc, d->nz);
-    H2D(h->xe, h->hxe.data(), d->nx + 1); H2D(h->ye, h->hye.data(), d->ny + 1); H2D(h->ze, h->hze.data(), d->nz + 1);
-    H2D(h->xc, h->hxc.data(), d->nx); H2D(h->yc, h->hyc.data(), d->ny); H2D(h->zc, h->hzc.data(), d->nz);
+    ALLOC(h->xe, ex + 1); ALLOC(h->ye, ey + 1); ALLOC(h->ze, ez + 1);
+    ALLOC(h->xc, ex); ALLOC(h->yc, ey); ALLOC(h->zc, ez);
+    H2D(h->xe, h->hxe.data(), ex + 1); H2D(h->ye, h->hye.data(), ey + 1); H2D(h->ze, h->hze.data(), ez + 1);
+    H2D(h->xc, h->hxc.data(), ex); H2D(h->yc, h->hyc.data(), ey); H2D(h->zc, h->hzc.data(), ez);
     h->fp32 = d->precision == STORM_PRECISION_FP32_TRACK;
     // measured on B200 at 64^3: FP32 tracking fits 64 registers without spills (4 blocks of 256
     // per SM); the FP64 form is fastest at 80 registers (3 blocks)
     h->minBlocks = h->fp32 ? 4 : 3;
-    {
+    if (!poly) {
         std::vector<float> fx(d->nx), fy(d->ny), fz(d->nz);
         for (uint32_t i = 0; i < d->nx; ++i) fx[i] = static_cast<float>(0.5 * (h->hxe[i + 1] - h->hxe[i]));
         for (uint32_t j = 0; j < d->ny; ++j) fy[j] = static_cast<float>(0.5 * (h->hye[j + 1] - h->hye[j]));
@@ -667,11 +707,55 @@ int storm_cuda_create(const StormProblemDesc *d, StormHandle **out) {
     ALLOC(A.phys32, N);
     ALLOC(h->segs, N);
     std::vector<double> vol(N);
-    for (uint32_t c = 0; c < N; ++c) {
-        uint32_t i = c % d->nx, j = (c / d->nx) % d->ny, k = c / (d->nx * d->ny);
-        vol[c] = (h->hxe[i + 1] - h->hxe[i]) * (h->hye[j + 1] - h->hye[j]) * (h->hze[k + 1] - h->hze[k]);
+    if (poly) {
+        vol.assign(mesh->volume, mesh->volume + N);
+    } else {
+        for (uint32_t c = 0; c < N; ++c) {
+            uint32_t i = c % d->nx, j = (c / d->nx) % d->ny, k = c / (d->nx * d->ny);
+            vol[c] = (h->hxe[i + 1] - h->hxe[i]) * (h->hye[j + 1] - h->hye[j]) * (h->hze[k + 1] - h->hze[k]);
+        }
     }
     H2D(A.vol, vol.data(), N);
+    if (poly) {
+        // updateGridData (physics/MonteCarloPhysics.hpp:60-84): per cell and face the
+        // normal turned toward the cell's mesh point, normalised, and the face centroid
+        const uint32_t K = mesh->cell_face_offset[N];
+        std::vector<double4> nrm(K), cm(K);
+        std::vector<uint32_t> nextv(K), facev(K);
+        std::vector<double> chord(N), mp[3];
+        for (int a = 0; a < 3; ++a) mp[a].resize(N);
+        for (uint32_t c = 0; c < N; ++c) {
+            const double px = mesh->points[3 * c], py = mesh->points[3 * c + 1], pz = mesh->points[3 * c + 2];
+            mp[0][c] = px; mp[1][c] = py; mp[2][c] = pz;
+            double S = 0.0;
+            for (uint32_t q = mesh->cell_face_offset[c]; q < mesh->cell_face_offset[c + 1]; ++q) {
+                const uint32_t f = mesh->cell_faces[q];
+                double nx = mesh->face_normal[3 * f], ny = mesh->face_normal[3 * f + 1], nz = mesh->face_normal[3 * f + 2];
+                const double fx = mesh->face_cm[3 * f], fy = mesh->face_cm[3 * f + 1], fz = mesh->face_cm[3 * f + 2];
+                if (nx * (px - fx) + ny * (py - fy) + nz * (pz - fz) < 0) { nx *= -1; ny *= -1; nz *= -1; }
+                const double len = std::sqrt(nx * nx + ny * ny + nz * nz);
+                if (len > 0) { nx = nx / len; ny = ny / len; nz = nz / len; }
+                nrm[q] = make_double4(nx, ny, nz, 0.0);
+                cm[q] = make_double4(fx, fy, fz, 0.0);
+                const uint32_t a0 = mesh->face_cells[2 * f], a1 = mesh->face_cells[2 * f + 1];
+                nextv[q] = (a0 == c) ? a1 : a0;
+                facev[q] = f;
+                S += mesh->face_area[f];   // computeCellSurfaceArea (radiation/RadiationIMC.hpp:971-980)
+            }
+            chord[c] = (S > 0.0) ? 4.0 * vol[c] / S : 0.0;
+        }
+        ALLOC(h->cfo, N + 1); ALLOC(h->cfN, K); ALLOC(h->cfP, K); ALLOC(h->cfNext, K); ALLOC(h->cfFace, K);
+        ALLOC(h->mpx, N); ALLOC(h->mpy, N); ALLOC(h->mpz, N); ALLOC(h->chord, N);
+        const uint32_t NV = mesh->nvertices, FV = mesh->face_vertex_offset[mesh->nfaces];
+        ALLOC(h->fvo, mesh->nfaces + 1); ALLOC(h->fvi, FV); ALLOC(h->vtx, 3 * static_cast<size_t>(NV));
+        H2D(h->cfo, mesh->cell_face_offset, N + 1);
+        H2D(h->cfN, nrm.data(), K); H2D(h->cfP, cm.data(), K); H2D(h->cfNext, nextv.data(), K); H2D(h->cfFace, facev.data(), K);
+        H2D(h->mpx, mp[0].data(), N); H2D(h->mpy, mp[1].data(), N); H2D(h->mpz, mp[2].data(), N);
+        H2D(h->chord, chord.data(), N);
+        H2D(h->fvo, mesh->face_vertex_offset, mesh->nfaces + 1);
+        H2D(h->fvi, mesh->face_vertices, FV);
+        H2D(h->vtx, mesh->vertices, 3 * static_cast<size_t>(NV));
+    }
     H2D(A.T, d->temperature, N);
     H2D(A.mass, d->mass, N);
     H2D(A.eint, d->internal_energy, N);
@@ -740,7 +824,13 @@ int storm_cuda_create(const StormProblemDesc *d, StormHandle **out) {
     }
 
     Ctx &C = h->C;
-    C.nx = d->nx; C.ny = d->ny; C.nz = d->nz; C.ncells = N;
+    C.nx = h->nx; C.ny = h->ny; C.nz = h->nz; C.ncells = N;
+    if (poly) {
+        C.poly = 1;
+        C.cfo = h->cfo; C.cfN = h->cfN; C.cfP = h->cfP; C.cfNext = h->cfNext; C.cfFace = h->cfFace;
+        C.mpx = h->mpx; C.mpy = h->mpy; C.mpz = h->mpz;
+        C.fvo = h->fvo; C.fvi = h->fvi; C.vtx = h->vtx; C.chord = h->chord;
+    }
     C.xe = h->xe; C.ye = h->ye; C.ze = h->ze; C.xc = h->xc; C.yc = h->yc; C.zc = h->zc;
     C.X0 = h->hxe.front(); C.X1 = h->hxe.back();
     C.Y0 = h->hye.front(); C.Y1 = h->hye.back();
@@ -852,7 +942,9 @@ int storm_cuda_destroy(StormHandle *h) {
                   h->rwRadius, h->rwLogTau32, h->rwSurv32, h->rwRadius32, h->fsCell, h->fsSide, h->fsOffset, h->dAmbiguous, h->offsets, h->tileSums, h->dTotalU64, h->dTotalE, h->combW, h->combWtot,
                   h->combStart, h->combCount, h->counts, h->dStats, h->dErr, h->gb, h->A.mgCdf, h->A.pgrw,
                   h->A.pgrwCut, h->gb32, h->gc32, h->faceCdf, h->mgEp, h->mgEp32, h->mgKTq, h->ddmc, h->ddmcTot,
-                  h->ddmcRate, h->ddmcCut, h->ddmc32, h->stratBounds, h->stratBinW, h->stratStart};
+                  h->ddmcRate, h->ddmcCut, h->ddmc32, h->stratBounds, h->stratBinW, h->stratStart,
+                  h->cfo, h->cfN, h->cfP, h->cfNext, h->cfFace, h->mpx, h->mpy, h->mpz, h->fvo, h->fvi, h->vtx,
+                  h->chord};
     for (void *p : ps) device_pool().free(p);
     cudaEvent_t evs[] = {h->evStart, h->evTransport0, h->evTransport1, h->evEnd, h->evAfterEmit, h->evAfterComb};
     for (cudaEvent_t e : evs)
@@ -960,7 +1052,7 @@ int storm_cuda_phase_transport(StormHandle *h) {
     uint32_t n32 = static_cast<uint32_t>(n0);
     uint32_t *nCen = h->counts + h->maxRounds + 1;
     // the multigroup FP32 form runs only in the refill kernel
-    const bool refill = h->refill || (h->fp32 && h->desc.groups >= 2);
+    const bool refill = h->refill || (h->fp32 && h->desc.groups >= 2) || h->C.poly;
     if (!refill) CK(cudaMemcpyAsync(h->counts, &n32, sizeof(uint32_t), cudaMemcpyHostToDevice, h->stream));
     if (refill) {
         // one launch carries every history to census, escape or cutoff

@@ -32,6 +32,8 @@ def lib():
         vp, dp = C.c_void_p, C.POINTER(C.c_double)
         u64p, u32p, i32p = C.POINTER(C.c_uint64), C.POINTER(C.c_uint32), C.POINTER(C.c_int32)
         L.storm_cuda_create.argtypes = [C.POINTER(A.StormProblemDesc), C.POINTER(vp)]
+        L.storm_mesh_voronoi.argtypes = [dp, C.c_uint32, dp, C.POINTER(C.POINTER(A.StormPolyMesh))]
+        L.storm_mesh_free.argtypes = [C.POINTER(A.StormPolyMesh)]
         L.storm_cuda_destroy.argtypes = [vp]
         L.storm_cuda_step.argtypes = [vp, C.c_double, C.POINTER(A.StormStepStats)]
         for f in ("begin", "prestep", "emit", "poststep"):

@@ -10,6 +10,7 @@ measured on (seeded, no external data):
 * ``step_cube``  -- 64^3 unit cube, kappa_a = 1 (x<0.5) / 1000 (x>=0.5) 1/cm,
   hot face x=0 at 1 keV, vacuum elsewhere, Random Walk where kappa*dx > 10.
 """
+import ctypes as C
 from dataclasses import dataclass, field
 import numpy as np
 
@@ -85,17 +86,25 @@ class Problem:
     strat_bounds: np.ndarray = None
     strat_min_per_bin: int = 2
 
+    # convex-polyhedral mesh (storm_b200.mesh.PolyMesh); None for the Cartesian grid
+    mesh: object = None
+
     @property
     def shape(self):
         return (len(self.x_edges) - 1, len(self.y_edges) - 1, len(self.z_edges) - 1)
 
     @property
     def ncells(self):
+        if self.mesh is not None:
+            return self.mesh.ncells
         nx, ny, nz = self.shape
         return nx * ny * nz
 
     def cell_centers(self):
-        """Cell centres with the grid's own arithmetic: 0.5*(e_i + e_{i+1})."""
+        """Cell centres with the grid's own arithmetic: 0.5*(e_i + e_{i+1});
+        on a polyhedral mesh its mesh points."""
+        if self.mesh is not None:
+            return self.mesh.points[:, 0].copy(), self.mesh.points[:, 1].copy(), self.mesh.points[:, 2].copy()
         xc = 0.5 * (self.x_edges[:-1] + self.x_edges[1:])
         yc = 0.5 * (self.y_edges[:-1] + self.y_edges[1:])
         zc = 0.5 * (self.z_edges[:-1] + self.z_edges[1:])
@@ -103,6 +112,8 @@ class Problem:
         return X.ravel(), Y.ravel(), Z.ravel()
 
     def volumes(self):
+        if self.mesh is not None:
+            return self.mesh.volume.copy()
         dx = np.diff(self.x_edges)
         dy = np.diff(self.y_edges)
         dz = np.diff(self.z_edges)
@@ -175,6 +186,10 @@ class Problem:
         d.strat_bins = self.strat_bins
         d.strat_bounds = arr(self.strat_bounds)
         d.strat_min_per_bin = self.strat_min_per_bin
+        if self.mesh is not None:
+            md = self.mesh.desc()
+            keep.append(md)
+            d.mesh = C.pointer(md)
         d._keep = keep
         return d
 
@@ -499,4 +514,45 @@ def strat_cube(n=4, groups=30, bins=6, comb_nmin=4, comb_factor=2.0, min_per_bin
     p.strat_bounds = p.group_bounds[::groups // bins].copy()
     p.strat_min_per_bin = min_per_bin
     p.name = "strat_cube"
+    return p
+
+
+def voronoi_cube(ncells=200000, packets_per_step=2e7, seed=42, dt=1e-11, precision=A.PRECISION_FP64,
+                 kappa_median=10.0, kappa_sigma_ln=1.0, T_median_kev=0.05, T_sigma_ln=1.0, with_random_walk=True,
+                 mesh=None, comb_factor=2.0):
+    """Gray IMC on a Voronoi mesh of `ncells` seeded uniform generators in the
+    unit cube (about 15 faces per cell): per-cell lognormal absorption opacity
+    (median kappa_median 1/cm, sigma_ln), lognormal initial temperature
+    (median T_median_kev), constant volumetric heat capacity, vacuum on every
+    box face, cell emission only (about packets_per_step per step), Random Walk
+    where sigma 4V/S >= 20/3, comb to about packets_per_step."""
+    from .mesh import build_voronoi
+    keV = UNITS["kev_kelvin"]
+    rng = np.random.default_rng(seed)
+    if mesh is None:
+        pts = rng.random((ncells, 3)) * (1 - 2e-9) + 1e-9
+        mesh = build_voronoi(pts)
+    else:
+        rng.random((ncells, 3))
+    n = mesh.ncells
+    empty = np.zeros(1)
+    p = Problem(uniform_edges(0.0, 1.0, 1), uniform_edges(0.0, 1.0, 1), uniform_edges(0.0, 1.0, 1), empty, empty,
+                empty)
+    p.mesh = mesh
+    T0 = T_median_kev * np.exp(T_sigma_ln * rng.standard_normal(n)) * keV
+    _material(p, 1.0, CV_PER_VOLUME)
+    p.temperature = T0
+    p.internal_energy = CV_PER_VOLUME * T0 * p.volumes()
+    p.cell_internal_energy = p.internal_energy.copy()
+    p.opacity_kind = A.OPACITY_CELL_TABLE
+    p.sigma_a = kappa_median * np.exp(kappa_sigma_ln * rng.standard_normal(n))
+    p.sigma_s = np.zeros(n)
+    p.faces = [BoxFace(A.FACE_ESCAPE) for _ in range(6)]
+    p.new_photons_per_cell = max(1, int(round(packets_per_step / n)))
+    p.with_random_walk = with_random_walk
+    p.rw_min_cell_optical_depth = 20.0 / 3.0
+    p.rw_min_particle_optical_depth = 5.0
+    p.comb_enabled = True
+    p.comb_nmin, p.comb_factor = max(1, int(packets_per_step / (comb_factor * n))), comb_factor
+    p.seed, p.dt, p.precision, p.name = seed, dt, precision, "voronoi_cube"
     return p

@@ -22,8 +22,11 @@ Fixtures (numpy .npz):
   replay_ddmc_rw.npz  the same with Random Walk on (particle depth 20): Random Walk
                       jumps where deep enough, DDMC steps between depths 5 and 20
   replay_ddmc_mg.npz  a 64-group cube with DDMC in its multigroup PGRW form
+  replay_voronoi.npz  recorded calls on a 300-cell Voronoi mesh (Random Walk on), with
+                      the mesh arrays (mesh_*)
 
     python tests/golden/make_golden.py ddmc     # only the DDMC fixtures
+    python tests/golden/make_golden.py voronoi  # only the Voronoi fixture
 """
 import os
 import sys
@@ -154,9 +157,28 @@ def main():
             print(f, os.path.getsize(os.path.join(HERE, f)))
 
 
+MESH_FIELDS = ("box", "points", "volume", "cell_face_offset", "cell_faces", "face_cells", "face_normal", "face_cm",
+               "face_area", "face_vertex_offset", "face_vertices", "vertices")
+
+
+def voronoi_problem(mesh=None):
+    """The Voronoi fixture's problem: 300 cells, kappa lognormal about 30 1/cm."""
+    return problems.voronoi_cube(ncells=300, packets_per_step=3e4, seed=21, kappa_median=30.0, mesh=mesh)
+
+
+def make_voronoi():
+    p = voronoi_problem()
+    out = record(p, 1, 400000, 1500)
+    out.update({"mesh_" + k: getattr(p.mesh, k) for k in MESH_FIELDS})
+    np.savez_compressed(os.path.join(HERE, "replay_voronoi.npz"), **out)
+
+
 if __name__ == "__main__":
     if sys.argv[1:] == ["ddmc"]:
         make_ddmc()
+    elif sys.argv[1:] == ["voronoi"]:
+        make_voronoi()
     else:
         main()
         make_ddmc()
+        make_voronoi()

@@ -3,11 +3,14 @@ reference ships and the gates its regression suite applies
 (regression_tests/lib/regression_checks.sh:73-118):
 
 * Marshak waves 1-4 (gray, power-law opacity and EOS, time-dependent bath):
-  gas-temperature relative L1 against the diffusion profile below 0.10;
+  gas-temperature relative L1 against the diffusion profile below 0.10 where
+  the reference's own serial run passes, within its warning level where it
+  does not;
 * Densmore et al. 2012 Fig. 4 (30 groups, multigroup Planck face source):
   gas-temperature L1 against the digitised Milagro curve below 0.10 keV;
 
-in both arithmetic forms, at the examples' default sizes.  Also the face
+in both arithmetic forms, at the examples' default sizes, and each profile
+against the reference's own serial run of the same problem.  Also the face
 source's frequency spectrum against planck_integral, and a short multigroup
 face-driven run against the reference's serial path.
 """
@@ -26,20 +29,48 @@ pytestmark = pytest.mark.gpu
 FORMS = {"fp64": A.PRECISION_FP64, "fp32": A.PRECISION_FP32_TRACK}
 
 
+def _against_reference_run(res, name, volumes):
+    """The GPU profile against the reference's own serial run of the same
+    problem (tests/golden/reference_runs.npz, tests/golden/make_reference_runs.py):
+    the volume-weighted mean gas temperature within 3 % and the heat front
+    (the first cell below half the hottest) within 3 cells."""
+    r = golden("reference_runs.npz")
+    xr, tr = r[name + "_x"], r[name + "_t_gas"]
+    np.testing.assert_allclose(res["x"], xr, rtol=0, atol=1e-12)
+    tg = res["t_gas"]
+    mean_rel = abs(np.dot(tg, volumes) - np.dot(tr, volumes)) / np.dot(tr, volumes)
+    front = lambda t: int(np.argmax(t < 0.5 * t.max())) if (t < 0.5 * t.max()).any() else len(t)
+    df = abs(front(tg) - front(tr))
+    print(f"{name}: mean T vs reference run {mean_rel:.3e}, front {front(tg)} vs {front(tr)}")
+    assert mean_rel < 0.03 and df <= 3
+    return float(r[name + "_l1"])
+
+
 @pytest.mark.parametrize("form", sorted(FORMS))
 @pytest.mark.parametrize("problem", [1, 2, 3, 4])
 def test_marshak_wave_against_diffusion_reference(problem, form):
+    """The regression suite passes a Marshak wave below a relative L1 of 0.10
+    and accepts a warning above it.  Where the reference's own serial run
+    passes, so must the GPU; where it warns (Marshak 2: the wave front is
+    steeper than a cell, and interpolating across it dominates the L1), the
+    GPU stays within a quarter of the reference's own L1."""
+    name = f"marshak_wave_{problem}"
     res = B.run_marshak_wave(Engine, problem, precision=FORMS[form])
-    l1 = B.marshak_l1(res["x"], res["t_gas"], golden("reference_curves.npz")[f"marshak_wave_{problem}"])
-    print(f"marshak_wave_{problem} {form}: TGAS_REL_L1 = {l1:.4e} over {res['steps']} steps")
-    assert 0.0 <= l1 < 0.10
+    l1 = B.marshak_l1(res["x"], res["t_gas"], golden("reference_curves.npz")[name])
+    l1_ref = _against_reference_run(res, name, P.marshak_wave(problem).volumes())
+    print(f"{name} {form}: TGAS_REL_L1 = {l1:.4e} over {res['steps']} steps (reference serial run {l1_ref:.4e})")
+    if l1_ref < 0.10:
+        assert 0.0 <= l1 < 0.10
+    else:
+        assert 0.0 <= l1 < 1.25 * l1_ref
 
 
 @pytest.mark.parametrize("form", sorted(FORMS))
 def test_densmore2012_against_milagro_curve(form):
     res = B.run_densmore2012(Engine, precision=FORMS[form])
     l1 = B.densmore_l1(res["x"], res["t_gas"], golden("reference_curves.npz")["densmore2012"])
-    print(f"densmore2012 {form}: DENSMORE2012_TGAS_L1 = {l1:.4e} keV")
+    l1_ref = _against_reference_run(res, "densmore2012", P.densmore2012().volumes())
+    print(f"densmore2012 {form}: DENSMORE2012_TGAS_L1 = {l1:.4e} keV (reference serial run {l1_ref:.4e})")
     assert 0.0 <= l1 < 0.10
 
 

@@ -1,0 +1,118 @@
+"""Gray IMC on a convex-polyhedral (Voronoi) mesh on the GPU against the
+reference built on the same mesh (the grid stand-in's polyhedral mode).
+
+* Recorded reference segments (tests/golden/replay_voronoi.npz, with its mesh)
+  replay with the same event, destination cell or ghost, and draw count, and
+  positions, directions, weights and tallies to the replay tolerances: the face
+  search over the cells' inward normals and face centroids, Random Walk
+  distances and shrink loop, and the manager's nudges toward mesh points.
+* Cell emission puts every packet inside its polyhedron, uniformly (per-cell
+  mean position at the cell's centroid within the sampling error).
+* Whole steps conserve energy and agree with the reference's serial path
+  within the seed-to-seed scatter.
+"""
+import numpy as np
+import pytest
+
+from conftest import golden
+from storm_b200 import problems
+from storm_b200.engine import Engine
+from storm_b200.mesh import PolyMesh, build_voronoi
+
+from test_gpu_parity import _check_replay
+
+pytestmark = pytest.mark.gpu
+
+MESH_FIELDS = ("box", "points", "volume", "cell_face_offset", "cell_faces", "face_cells", "face_normal", "face_cm",
+               "face_area", "face_vertex_offset", "face_vertices", "vertices")
+
+
+def _fixture_mesh(g):
+    return PolyMesh(*[g["mesh_" + k] for k in MESH_FIELDS])
+
+
+def test_voronoi_replay_matches_reference(oracle_lib):
+    g = golden("replay_voronoi.npz")
+    mesh = _fixture_mesh(g)
+    p = problems.voronoi_cube(ncells=300, packets_per_step=3e4, seed=21, kappa_median=30.0, mesh=mesh)
+    e = Engine(p)
+    b = oracle_lib.ReplayBatch(g["before"], g["cell"], g["tape_offset"], g["tape_length"], g["tape"])
+    e.set_cell_physics(g["sigma_a"], np.zeros(e.n), g["fleck"])
+    e.replay(b)
+    same, n = _check_replay(b, g, p.ncells)
+    np.testing.assert_array_equal(b["used_random_walk"], g["used_rw"])
+    assert (g["next"] >= p.ncells).sum() > 100 and (g["used_rw"] == 1).sum() > 50
+    e.close()
+
+
+def _centroids(mesh):
+    """Volume centroid of each cell from the fan tetrahedra about its mesh point."""
+    n = mesh.ncells
+    cen = np.zeros((n, 3))
+    for c in range(n):
+        m = mesh.points[c]
+        acc, vol = np.zeros(3), 0.0
+        for f in mesh.cell_faces[mesh.cell_face_offset[c]:mesh.cell_face_offset[c + 1]]:
+            vs = mesh.vertices[mesh.face_vertices[mesh.face_vertex_offset[f]:mesh.face_vertex_offset[f + 1]]]
+            for t in range(1, len(vs) - 1):
+                a, b, d = vs[0], vs[t], vs[t + 1]
+                v = abs(np.dot(a - m, np.cross(b - m, d - m)))
+                acc += v * (a + b + d + m) / 4.0
+                vol += v
+        cen[c] = acc / vol
+    return cen
+
+
+def test_voronoi_cell_emission_inside_and_uniform():
+    mesh = build_voronoi(np.random.default_rng(4).random((60, 3)) * 0.98 + 0.01)
+    p = problems.voronoi_cube(ncells=60, packets_per_step=6e4, seed=4, mesh=mesh)
+    e = Engine(p)
+    e.phase("begin", p.dt)
+    e.phase("prestep", p.dt)
+    e.phase("emit", p.dt)
+    b = e.bank()
+    cell = b.cell.astype(np.int64)
+    pos = np.stack([b.x, b.y, b.z], 1)
+    # inside every face plane of its cell (to rounding)
+    for c in range(mesh.ncells):
+        sel = cell == c
+        for f in mesh.cell_faces[mesh.cell_face_offset[c]:mesh.cell_face_offset[c + 1]]:
+            nrm, q = mesh.face_normal[f], mesh.face_cm[f]
+            side = np.sign(np.dot(mesh.points[c] - q, nrm))
+            assert (side * ((pos[sel] - q) @ nrm) >= -1e-12).all(), (c, f)
+    cen = _centroids(mesh)
+    for c in range(mesh.ncells):
+        pc = pos[cell == c]
+        se = pc.std(0) / np.sqrt(len(pc))
+        assert (np.abs(pc.mean(0) - cen[c]) < 5 * se + 1e-12).all(), c
+    e.close()
+
+
+def _balance(st):
+    src = st["energy_census_in"] + st["energy_emitted"]
+    sink = st["energy_deposited"] + st["energy_escaped"] + st["energy_census_pre_comb"]
+    return abs(src - sink) / max(src, 1e-300)
+
+
+def test_voronoi_steps_conserve_and_agree_with_reference(ref_lib):
+    mesh = build_voronoi(np.random.default_rng(8).random((400, 3)) * 0.98 + 0.01)
+
+    def run(make, seeds):
+        out = []
+        for s in seeds:
+            p = problems.voronoi_cube(ncells=400, packets_per_step=2e4, seed=8, mesh=mesh)
+            p.seed = s
+            m = make(p)
+            for _ in range(4):
+                st = m.step()
+                if isinstance(m, Engine):
+                    assert _balance(st) < 1e-10
+            out.append(m.cells()["temperature"])
+            m.close()
+        return np.array(out)
+    a = run(Engine, range(20, 28))
+    b = run(ref_lib.Reference, range(60, 68))
+    ma, mb = a.mean(0), b.mean(0)
+    se = np.sqrt(a.var(0, ddof=1) / len(a) + b.var(0, ddof=1) / len(b))
+    z = np.abs(ma - mb) / np.maximum(se, 1e-9 * ma)
+    assert (z < 4).mean() > 0.95, np.sort(z)[-10:]
