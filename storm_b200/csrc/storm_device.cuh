@@ -122,6 +122,8 @@ struct Ctx {
     const uint32_t *fvo, *fvi;       // face polygons: offsets (nfaces + 1) and vertex indices
     const double *vtx;       // polygon vertices, 3 per vertex
     const double *chord;     // per cell: 4 V / S
+    const float4 *cfN32;     // FP32 form, per cell-face slot: inward unit normal and the distance of the
+                             // cell's mesh point from the face plane, (mesh point - faceCM).n
 };
 
 // ------------------------------------------------------------------ errors
@@ -1016,7 +1018,24 @@ __device__ inline float rw_sample_radius32(const RwTables &T, float tau, float x
 // tallies, the same draws in the same order as the FP64 form.  Ro is the
 // distance to the nearest face (the caller has checked Ro >= rwMinParticle /
 // sigma_T); the diffusion coefficient c / (3 sigma_T) is cp.z * C.rwDiffPerReach.
-template <bool MG, class RNG, class TALLY>
+// distance of local point (x, y, z) from face slot k's plane, inward positive
+__device__ __forceinline__ float poly_dist32(const Ctx &C, uint32_t k, float x, float y, float z) {
+    const float4 pl = C.cfN32[k];
+    return pl.w + (x * pl.x + y * pl.y + z * pl.z);
+}
+template <bool POLY>
+__device__ __forceinline__ bool inside32(const Ctx &C, uint32_t cell, float x, float y, float z, float hx, float hy,
+                                         float hz) {
+    if constexpr (POLY) {
+        for (uint32_t k = C.cfo[cell]; k < C.cfo[cell + 1]; ++k)
+            if (poly_dist32(C, k, x, y, z) < 0.0f) return false;
+        return true;
+    } else {
+        return !(fabsf(x) > hx || fabsf(y) > hy || fabsf(z) > hz);
+    }
+}
+
+template <bool MG, bool POLY = false, class RNG, class TALLY>
 __device__ inline int rw_jump32(const Ctx &C, Track32 &T, RNG &rng, TALLY &tal, const float4 &cp, float Ro, float hx,
                                 float hy, float hz, int &err) {
     const uint32_t cell = T.cell;
@@ -1072,7 +1091,7 @@ __device__ inline int rw_jump32(const Ctx &C, Track32 &T, RNG &rng, TALLY &tal, 
     const float nudge = 1.0f - static_cast<float>(RW_NUDGE);   // toward the cell centre (local origin)
     float lx = (T.qx + disp * dx) * nudge, ly = (T.qy + disp * dy) * nudge, lz = (T.qz + disp * dz) * nudge;
     int guard = 0;
-    while (fabsf(lx) > hx || fabsf(ly) > hy || fabsf(lz) > hz) {
+    while (!inside32<POLY>(C, cell, lx, ly, lz, hx, hy, hz)) {
         disp *= 0.99f;
         lx = T.qx + disp * dx;
         ly = T.qy + disp * dy;
@@ -1189,12 +1208,18 @@ __device__ __forceinline__ float mg_absorption32(const Ctx &C, const Track32 &T,
 // at speed |u_a|; the nearest exit is found by cross-multiplied comparisons
 // (n_a |u_b| < n_b |u_a|, first smallest wins, an axis with u_a = 0 never
 // wins) and only the winner is divided.
-template <bool MG, class RNG, class TALLY>
+//
+// POLY: a convex-polyhedral cell; the offset is from the cell's mesh point and
+// each face is the plane n.q + h = 0 (n inward, h the mesh point's distance).
+// The exit is the first smallest (n.q + h) / (-n.u) over faces the direction
+// approaches; a particle that changes cells re-expresses its offset from the
+// new mesh point and is nudged 2^-21 of it toward that point.
+template <bool MG, class RNG, class TALLY, bool POLY = false>
 __device__ inline int segment32(const Ctx &C, Track32 &T, RNG &rng, TALLY &tal, int &usedRW, int &err) {
     const uint32_t cell = T.cell;
     if (T.cc != cell) {   // entered another cell: load its constants once
         T.cp = C.phys32[cell];
-        T.hx = C.hx[T.i]; T.hy = C.hy[T.j]; T.hz = C.hz[T.k];
+        if (!POLY) { T.hx = C.hx[T.i]; T.hy = C.hy[T.j]; T.hz = C.hz[T.k]; }
         T.cc = cell;
         if (MG) {
             T.kT = static_cast<float>(mg_kT(C, cell));
@@ -1208,12 +1233,18 @@ __device__ inline int segment32(const Ctx &C, Track32 &T, RNG &rng, TALLY &tal, 
     // Random Walk only where the particle is at least cp.z = rwMinParticleOpticalDepth / sigma_T
     // from every face (cp.z is inf in cells that are not eligible); in a multigroup
     // problem only below the cell's PGRW group cutoff
-    const float Ro = fminf(fminf(hx - fabsf(T.qx), hy - fabsf(T.qy)), hz - fabsf(T.qz));
+    float Ro;
+    if constexpr (POLY) {
+        Ro = FLT_MAX;
+        for (uint32_t k = C.cfo[cell]; k < C.cfo[cell + 1]; ++k) Ro = fminf(Ro, poly_dist32(C, k, T.qx, T.qy, T.qz));
+    } else {
+        Ro = fminf(fminf(hx - fabsf(T.qx), hy - fabsf(T.qy)), hz - fabsf(T.qz));
+    }
     if (Ro >= cp.z && Ro > 0.0f && (!MG || static_cast<double>(T.nu) < C.gb[C.pgrwCut[cell]])) {
         usedRW = 1;
-        return rw_jump32<MG>(C, T, rng, tal, cp, Ro, hx, hy, hz, err);
+        return rw_jump32<MG, POLY>(C, T, rng, tal, cp, Ro, hx, hy, hz, err);
     }
-    if (C.withDDMC) {   // DDMC after a Random Walk that was not taken (:1723-1738)
+    if (!POLY && C.withDDMC) {   // DDMC after a Random Walk that was not taken (:1723-1738)
         const float4 da = C.ddmc32[3 * static_cast<size_t>(cell)];   // depth reach, 1/total, sigma_A f c, nu bound
         if (Ro >= da.x && Ro > 0.0f && (!MG || T.nu < da.w)) return ddmc_jump32(C, T, rng, tal, da);
     }
@@ -1234,16 +1265,33 @@ __device__ inline int segment32(const Ctx &C, Track32 &T, RNG &rng, TALLY &tal, 
         invRate = static_cast<double>(cp.w);
     }
 
+    int face = -1;
+    float sF;
+    if constexpr (POLY) {
+        float bestS = FLT_MAX;
+        const uint32_t k0 = C.cfo[cell], k1 = C.cfo[cell + 1];
+        for (uint32_t k = k0; k < k1; ++k) {
+            const float4 pl = C.cfN32[k];
+            const float un = T.ux * pl.x + T.uy * pl.y + T.uz * pl.z;
+            if (un >= 0.0f) continue;
+            const float d = fmaxf(pl.w + (T.qx * pl.x + T.qy * pl.y + T.qz * pl.z), 0.0f);
+            const float sk = d / -un;
+            if (sk < bestS) { bestS = sk; face = static_cast<int>(k - k0); }
+        }
+        if (face < 0) { err = STORM_DERR_NO_FACE; return OUT_ERROR; }
+        sF = bestS;
+    } else {
     const float ax = fabsf(T.ux), ay = fabsf(T.uy), az = fabsf(T.uz);
     const float nxp = ax > 0.0f ? fmaxf(hx - (T.ux > 0.0f ? T.qx : -T.qx), 0.0f) : 1.0f;
     const float nyp = ay > 0.0f ? fmaxf(hy - (T.uy > 0.0f ? T.qy : -T.qy), 0.0f) : 1.0f;
     const float nzp = az > 0.0f ? fmaxf(hz - (T.uz > 0.0f ? T.qz : -T.qz), 0.0f) : 1.0f;
     float bn = nxp, bd = ax;
-    int face = ax > 0.0f ? (T.ux > 0.0f ? 1 : 0) : -1;
+    face = ax > 0.0f ? (T.ux > 0.0f ? 1 : 0) : -1;
     if (ay > 0.0f && (face < 0 || nyp * bd < bn * ay)) { bn = nyp; bd = ay; face = T.uy > 0.0f ? 3 : 2; }
     if (az > 0.0f && (face < 0 || nzp * bd < bn * az)) { bn = nzp; bd = az; face = T.uz > 0.0f ? 5 : 4; }
     if (face < 0) { err = STORM_DERR_NO_FACE; return OUT_ERROR; }
-    const float sF = __fdividef(bn, bd);
+    sF = __fdividef(bn, bd);
+    }
     const double c = C.clight;
 
     const float sC = invSigE * (-__logf(rng.rawf()));
@@ -1258,9 +1306,15 @@ __device__ inline int segment32(const Ctx &C, Track32 &T, RNG &rng, TALLY &tal, 
     const double e1 = static_cast<double>(expm1f(-tau));
     double integrated = T.w * dt;
     if (tau >= 1e-12f) integrated = T.w * e1 * invRate;
-    T.qx = clampf(fmaf(T.ux, ds, T.qx), hx);
-    T.qy = clampf(fmaf(T.uy, ds, T.qy), hy);
-    T.qz = clampf(fmaf(T.uz, ds, T.qz), hz);
+    if constexpr (POLY) {
+        T.qx = fmaf(T.ux, ds, T.qx);
+        T.qy = fmaf(T.uy, ds, T.qy);
+        T.qz = fmaf(T.uz, ds, T.qz);
+    } else {
+        T.qx = clampf(fmaf(T.ux, ds, T.qx), hx);
+        T.qy = clampf(fmaf(T.uy, ds, T.qy), hy);
+        T.qz = clampf(fmaf(T.uz, ds, T.qz), hz);
+    }
     if (!C.noFeedback) tal.mat(cell, -e1 * T.w);
     tal.rad(cell, integrated);
     T.w *= 1.0 + e1;
@@ -1287,6 +1341,35 @@ __device__ inline int segment32(const Ctx &C, Track32 &T, RNG &rng, TALLY &tal, 
         return OUT_CONTINUE;
     }
     // face crossing
+    if constexpr (POLY) {
+        const uint32_t k = C.cfo[cell] + static_cast<uint32_t>(face);
+        const uint32_t nb = C.cfNext[k];
+        if (nb < C.ncells) {
+            // the offset from the new cell's mesh point, nudged toward it
+            const float dx = static_cast<float>(C.mpx[cell] - C.mpx[nb]);
+            const float dy = static_cast<float>(C.mpy[cell] - C.mpy[nb]);
+            const float dz = static_cast<float>(C.mpz[cell] - C.mpz[nb]);
+            T.qx = (T.qx + dx) * ENTRY32;
+            T.qy = (T.qy + dy) * ENTRY32;
+            T.qz = (T.qz + dz) * ENTRY32;
+            T.cell = nb;
+            T.i = nb;
+            return OUT_CONTINUE;
+        }
+        // a box face: its axis and side from the inward normal
+        const float4 pl = C.cfN32[k];
+        const float apx = fabsf(pl.x), apy = fabsf(pl.y), apz = fabsf(pl.z);
+        const int ax = (apx >= apy && apx >= apz) ? 0 : (apy >= apz ? 1 : 2);
+        const float na = ax == 0 ? pl.x : (ax == 1 ? pl.y : pl.z);
+        const int bface = 2 * ax + (na < 0.0f ? 1 : 0);
+        if (C.escapeNoCheck || C.bf[bface].action == STORM_FACE_ESCAPE) return OUT_ESCAPE;
+        if (ax == 0) T.ux = -T.ux; else if (ax == 1) T.uy = -T.uy; else T.uz = -T.uz;
+        // back inside by the reflection nudge, measured from the face plane
+        const float d = pl.w + (T.qx * pl.x + T.qy * pl.y + T.qz * pl.z);
+        const float push = C.reflNudge[bface] - d;
+        T.qx += push * pl.x; T.qy += push * pl.y; T.qz += push * pl.z;
+        return OUT_CONTINUE;
+    }
     const int axis = face >> 1, hi = face & 1;
     bool inside;
     switch (face) {

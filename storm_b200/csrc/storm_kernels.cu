@@ -71,9 +71,15 @@ __device__ __forceinline__ void store_nu32(const Bank &b, uint32_t q, float nu) 
 __device__ __forceinline__ void to_local(const Ctx &C, const PartReg &p, Track32 &T) {
     cell_ijk(C, p.cell, T.i, T.j, T.k);
     T.cell = p.cell;
-    T.qx = clampf(static_cast<float>(p.x - C.xc[T.i]), C.hx[T.i] * ENTRY32);
-    T.qy = clampf(static_cast<float>(p.y - C.yc[T.j]), C.hy[T.j] * ENTRY32);
-    T.qz = clampf(static_cast<float>(p.z - C.zc[T.k]), C.hz[T.k] * ENTRY32);
+    if (C.poly) {   // offset from the mesh point, nudged toward it
+        T.qx = static_cast<float>(p.x - C.mpx[p.cell]) * ENTRY32;
+        T.qy = static_cast<float>(p.y - C.mpy[p.cell]) * ENTRY32;
+        T.qz = static_cast<float>(p.z - C.mpz[p.cell]) * ENTRY32;
+    } else {
+        T.qx = clampf(static_cast<float>(p.x - C.xc[T.i]), C.hx[T.i] * ENTRY32);
+        T.qy = clampf(static_cast<float>(p.y - C.yc[T.j]), C.hy[T.j] * ENTRY32);
+        T.qz = clampf(static_cast<float>(p.z - C.zc[T.k]), C.hz[T.k] * ENTRY32);
+    }
     const double sp = vnorm(p.vx, p.vy, p.vz);
     const double inv = sp > 0.0 ? 1.0 / sp : 0.0;
     T.ux = static_cast<float>(p.vx * inv); T.uy = static_cast<float>(p.vy * inv); T.uz = static_cast<float>(p.vz * inv);
@@ -83,9 +89,11 @@ __device__ __forceinline__ void to_local(const Ctx &C, const PartReg &p, Track32
 __device__ __forceinline__ void to_global(const Ctx &C, const Track32 &T, PartReg &p) {
     uint32_t i, j, k;
     cell_ijk(C, T.cell, i, j, k);
-    p.x = C.xc[i] + static_cast<double>(T.qx);
-    p.y = C.yc[j] + static_cast<double>(T.qy);
-    p.z = C.zc[k] + static_cast<double>(T.qz);
+    const double mx = C.poly ? C.mpx[T.cell] : C.xc[i], my = C.poly ? C.mpy[T.cell] : C.yc[j],
+                 mz = C.poly ? C.mpz[T.cell] : C.zc[k];
+    p.x = mx + static_cast<double>(T.qx);
+    p.y = my + static_cast<double>(T.qy);
+    p.z = mz + static_cast<double>(T.qz);
     p.vx = static_cast<double>(T.ux) * C.clight;
     p.vy = static_cast<double>(T.uy) * C.clight;
     p.vz = static_cast<double>(T.uz) * C.clight;
@@ -1167,7 +1175,8 @@ struct Form64T {
 using Form64 = Form64T<0>;
 using Form64Full = Form64T<1>;
 using Form64Poly = Form64T<2>;
-struct Form32 {
+template <bool POLY>
+struct Form32T {
     using T = Track32;
     using Rng = PhiloxRng4;
     static __device__ __forceinline__ void load(const Ctx &C, const Bank &b, uint32_t q, T &t) {
@@ -1184,13 +1193,15 @@ struct Form32 {
     }
     template <class RNG, class TALLY>
     static __device__ __forceinline__ int seg(const Ctx &C, T &t, RNG &rng, TALLY &tal, int &usedRW, int &err) {
-        int m = segment32<false>(C, t, rng, tal, usedRW, err);
+        int m = segment32<false, RNG, TALLY, POLY>(C, t, rng, tal, usedRW, err);
         if (m == OUT_ERROR && !err) err = STORM_DERR_NOT_ON_BOUNDARY;
         return m;
     }
     static __device__ __forceinline__ uint32_t cell(const T &t) { return t.cell; }
     static __device__ __forceinline__ double weight(const T &t) { return t.w; }
 };
+using Form32 = Form32T<false>;
+using Form32Poly = Form32T<true>;
 // The FP32-tracking form of a multigroup problem: the frequency rides along.
 struct Form32MG {
     using T = Track32;
@@ -2189,7 +2200,7 @@ void launch_scan_u64(cudaStream_t s, const uint64_t *in, uint32_t n, uint64_t *o
 void launch_emit_cells(cudaStream_t s, const Ctx &C, const CellArrays &A, const uint64_t *offsets, uint64_t total,
                        const Bank &b, uint32_t bankBase, double dt, DevStats *st) {
     if (!total) return;
-    if (C.fp32)
+    if (C.fp32 && !C.poly)   // polyhedral cells: the FP64 sampler, then the cell frame
         k_emit_cells32<<<grid_for(total, 256, 148 * 16), 256, 0, s>>>(C, A, offsets, total, b, bankBase, dt, st);
     else
         k_emit_cells<<<grid_for(total, 256, 148 * 16), 256, 0, s>>>(C, A, offsets, total, b, bankBase, dt, st);
@@ -2340,7 +2351,8 @@ static void refill_launch(cudaStream_t s, uint32_t grid, int minBlocks, const Ct
 void launch_transport_refill(cudaStream_t s, uint32_t grid, int minBlocks, const Ctx &C, const Bank &in, uint32_t n,
                              uint32_t *nextIdx, const CensusBank &cen, uint32_t *nCen, uint32_t burst, uint32_t maxSegs,
                              DevStats *st) {
-    if (C.fp32 && C.groups >= 2) refill_launch<Form32MG>(s, grid, minBlocks, C, in, n, nextIdx, cen, nCen, burst, maxSegs, st);
+    if (C.fp32 && C.poly) refill_launch<Form32Poly>(s, grid, minBlocks, C, in, n, nextIdx, cen, nCen, burst, maxSegs, st);
+    else if (C.fp32 && C.groups >= 2) refill_launch<Form32MG>(s, grid, minBlocks, C, in, n, nextIdx, cen, nCen, burst, maxSegs, st);
     else if (C.fp32) refill_launch<Form32>(s, grid, minBlocks, C, in, n, nextIdx, cen, nCen, burst, maxSegs, st);
     else if (C.poly) refill_launch<Form64Poly>(s, grid, minBlocks, C, in, n, nextIdx, cen, nCen, burst, maxSegs, st);
     else if (C.groups >= 2 || C.withDDMC) refill_launch<Form64Full>(s, grid, minBlocks, C, in, n, nextIdx, cen, nCen, burst, maxSegs, st);

@@ -65,6 +65,7 @@ struct StormHandle {
     uint32_t *cfo = nullptr, *cfNext = nullptr, *cfFace = nullptr, *fvo = nullptr, *fvi = nullptr;
     double4 *cfN = nullptr, *cfP = nullptr;
     double *mpx = nullptr, *mpy = nullptr, *mpz = nullptr, *vtx = nullptr, *chord = nullptr;
+    float4 *cfN32 = nullptr;
     StratParams strat{1, nullptr, 2};         // stratified comb: bins, device bounds, minParticlesPerGroup
     double *stratBounds = nullptr, *stratBinW = nullptr;
     uint32_t *stratStart = nullptr;
@@ -624,8 +625,8 @@ int storm_cuda_create(const StormProblemDesc *d, StormHandle **out) {
         }
         for (uint32_t q = 0; q < mesh->face_vertex_offset[mesh->nfaces]; ++q)
             if (mesh->face_vertices[q] >= mesh->nvertices) return STORM_ERR_INVALID_ARG;
-        // the FP32-tracking form, DDMC and boundary sources are Cartesian only
-        if (d->precision != STORM_PRECISION_FP64 || d->with_ddmc) return STORM_ERR_UNSUPPORTED;
+        // DDMC and boundary sources are Cartesian only
+        if (d->with_ddmc) return STORM_ERR_UNSUPPORTED;
         for (int f = 0; f < 6; ++f)
             if (d->faces[f].source_temperature > 0.0 && d->faces[f].packets_per_face > 0) return STORM_ERR_UNSUPPORTED;
     } else {
@@ -755,6 +756,19 @@ int storm_cuda_create(const StormProblemDesc *d, StormHandle **out) {
         H2D(h->fvo, mesh->face_vertex_offset, mesh->nfaces + 1);
         H2D(h->fvi, mesh->face_vertices, FV);
         H2D(h->vtx, mesh->vertices, 3 * static_cast<size_t>(NV));
+        if (d->precision == STORM_PRECISION_FP32_TRACK) {
+            // the FP32 form's planes: inward normal and the mesh point's distance from the plane
+            std::vector<float4> pl(K);
+            for (uint32_t c = 0; c < N; ++c)
+                for (uint32_t q = mesh->cell_face_offset[c]; q < mesh->cell_face_offset[c + 1]; ++q) {
+                    const double hq = (mp[0][c] - cm[q].x) * nrm[q].x + (mp[1][c] - cm[q].y) * nrm[q].y +
+                                      (mp[2][c] - cm[q].z) * nrm[q].z;
+                    pl[q] = make_float4(static_cast<float>(nrm[q].x), static_cast<float>(nrm[q].y),
+                                        static_cast<float>(nrm[q].z), static_cast<float>(hq));
+                }
+            ALLOC(h->cfN32, K);
+            H2D(h->cfN32, pl.data(), K);
+        }
     }
     H2D(A.T, d->temperature, N);
     H2D(A.mass, d->mass, N);
@@ -829,7 +843,7 @@ int storm_cuda_create(const StormProblemDesc *d, StormHandle **out) {
         C.poly = 1;
         C.cfo = h->cfo; C.cfN = h->cfN; C.cfP = h->cfP; C.cfNext = h->cfNext; C.cfFace = h->cfFace;
         C.mpx = h->mpx; C.mpy = h->mpy; C.mpz = h->mpz;
-        C.fvo = h->fvo; C.fvi = h->fvi; C.vtx = h->vtx; C.chord = h->chord;
+        C.fvo = h->fvo; C.fvi = h->fvi; C.vtx = h->vtx; C.chord = h->chord; C.cfN32 = h->cfN32;
     }
     C.xe = h->xe; C.ye = h->ye; C.ze = h->ze; C.xc = h->xc; C.yc = h->yc; C.zc = h->zc;
     C.X0 = h->hxe.front(); C.X1 = h->hxe.back();
@@ -944,7 +958,7 @@ int storm_cuda_destroy(StormHandle *h) {
                   h->A.pgrwCut, h->gb32, h->gc32, h->faceCdf, h->mgEp, h->mgEp32, h->mgKTq, h->ddmc, h->ddmcTot,
                   h->ddmcRate, h->ddmcCut, h->ddmc32, h->stratBounds, h->stratBinW, h->stratStart,
                   h->cfo, h->cfN, h->cfP, h->cfNext, h->cfFace, h->mpx, h->mpy, h->mpz, h->fvo, h->fvi, h->vtx,
-                  h->chord};
+                  h->chord, h->cfN32};
     for (void *p : ps) device_pool().free(p);
     cudaEvent_t evs[] = {h->evStart, h->evTransport0, h->evTransport1, h->evEnd, h->evAfterEmit, h->evAfterComb};
     for (cudaEvent_t e : evs)

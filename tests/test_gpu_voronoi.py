@@ -116,3 +116,39 @@ def test_voronoi_steps_conserve_and_agree_with_reference(ref_lib):
     se = np.sqrt(a.var(0, ddof=1) / len(a) + b.var(0, ddof=1) / len(b))
     z = np.abs(ma - mb) / np.maximum(se, 1e-9 * ma)
     assert (z < 4).mean() > 0.95, np.sort(z)[-10:]
+
+
+def test_voronoi_fp32_tracking_agrees_with_fp64():
+    """The FP32-tracking form on polyhedral cells (offsets from the mesh point,
+    face planes n.q + h = 0 in FP32): energy conserved per step, the census
+    inside its cells, temperatures within the seed-to-seed scatter of the FP64
+    form."""
+    from storm_b200 import _abi as A
+    mesh = build_voronoi(np.random.default_rng(9).random((400, 3)) * 0.98 + 0.01)
+
+    def run(precision, seeds):
+        out = []
+        for s in seeds:
+            p = problems.voronoi_cube(ncells=400, packets_per_step=2e4, seed=9, mesh=mesh, precision=precision)
+            p.seed = s
+            e = Engine(p)
+            for _ in range(4):
+                assert _balance(e.step()) < 1e-10
+            c = e.census()
+            pos = np.stack([c.x, c.y, c.z], 1)
+            cell = c.cell.astype(np.int64)
+            for q in np.random.default_rng(s).choice(len(cell), 300, replace=False):
+                k = cell[q]
+                for f in mesh.cell_faces[mesh.cell_face_offset[k]:mesh.cell_face_offset[k + 1]]:
+                    nrm, fc = mesh.face_normal[f], mesh.face_cm[f]
+                    side = np.sign(np.dot(mesh.points[k] - fc, nrm))
+                    assert side * np.dot(pos[q] - fc, nrm) >= -1e-7, (k, f)
+            out.append(e.cells()["temperature"])
+            e.close()
+        return np.array(out)
+    a = run(A.PRECISION_FP32_TRACK, range(30, 38))
+    b = run(A.PRECISION_FP64, range(70, 78))
+    ma, mb = a.mean(0), b.mean(0)
+    se = np.sqrt(a.var(0, ddof=1) / len(a) + b.var(0, ddof=1) / len(b))
+    z = np.abs(ma - mb) / np.maximum(se, 1e-9 * ma)
+    assert (z < 4).mean() > 0.95, np.sort(z)[-10:]
