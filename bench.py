@@ -52,6 +52,8 @@ def parse():
     ap.add_argument("--refill", type=int, default=-1, help="1 persistent refill kernel, 0 bank visits")
     ap.add_argument("--burst", type=int, default=8)
     ap.add_argument("--mg-steps", type=int, default=5, help="timed steps of the multigroup run (0 = skip it)")
+    ap.add_argument("--voronoi-steps", type=int, default=5, help="timed steps of the Voronoi-mesh run (0 = skip it)")
+    ap.add_argument("--voronoi-cells", type=int, default=200000)
     ap.add_argument("--mg-n", type=int, default=128)
     ap.add_argument("--serving-requests", type=int, default=32, help="requests in the serving run (0 = skip it)")
     ap.add_argument("--serving-slots", type=int, default=12)
@@ -379,6 +381,49 @@ def mg_run(args):
     return out
 
 
+def voronoi_run(args):
+    """Gray IMC on a Voronoi mesh of 2e5 seeded uniform generators in the unit
+    cube (about 15 faces per cell; the engine's own builder), per-cell
+    lognormal opacity (median 10 1/cm, sigma_ln 1), lognormal initial
+    temperature (median 0.05 keV), about 2e7 packets per step, Random Walk.
+    Both forms on the same mesh; device-timed steps after 2 warm-up steps."""
+    import numpy as np
+    from storm_b200 import _abi as A
+    from storm_b200 import problems
+    from storm_b200.engine import Engine
+    from storm_b200.mesh import build_voronoi
+    t0 = time.perf_counter()
+    mesh = build_voronoi(np.random.default_rng(5).random((args.voronoi_cells, 3)) * (1 - 2e-9) + 1e-9)
+    build_s = time.perf_counter() - t0
+    out = {"workload": f"Voronoi mesh of {args.voronoi_cells} cells in the unit cube "
+                       f"({mesh.cell_faces.size / mesh.ncells:.1f} faces/cell), kappa lognormal median 10 1/cm "
+                       "sigma_ln 1, T0 lognormal median 0.05 keV, ~2e7 packets/step, vacuum box, RW",
+           "steps": args.voronoi_steps, "mesh_build_s": build_s}
+    temps = {}
+    for name, prec in (("fp32", A.PRECISION_FP32_TRACK), ("fp64", A.PRECISION_FP64)):
+        p = problems.voronoi_cube(ncells=args.voronoi_cells, packets_per_step=2e7, seed=5, mesh=mesh,
+                                  precision=prec)
+        p.per_cell_segment_counters = False
+        e = Engine(p)
+        for _ in range(2):
+            e.step()
+        segs, ms, lat = 0, 0.0, []
+        for _ in range(args.voronoi_steps):
+            st = e.step()
+            segs += st["segments"]
+            ms += st["step_ms"]
+            lat.append(st["step_ms"])
+        out[name] = {"segments_per_s": segs / (ms / 1e3), "ms_per_step": ms / args.voronoi_steps,
+                     "segments_per_step": segs / args.voronoi_steps, "emitted_per_step": st["emitted_cells"],
+                     "census_per_step": st["census_out"], "step_ms_p99": float(np.percentile(lat, 99)),
+                     "device_gb": e.memory_bytes() / 1e9}
+        temps[name] = e.cells()["temperature"]
+        e.close()
+    out["fp32_over_fp64"] = out["fp32"]["segments_per_s"] / out["fp64"]["segments_per_s"]
+    out["mean_relative_temperature_difference"] = float(np.mean(np.abs(temps["fp32"] - temps["fp64"]) / temps["fp64"]))
+    return out
+
+
 def serving_run(args):
     """Many independent FP32-tracking problems (N log-uniform in [16, 48],
     1e4-1e6 packets/step log-uniform, kappa uniform in [0.1, 1000], 5-20 steps)
@@ -468,6 +513,7 @@ def run_storm(args, ws, rank, local, dist):
         cpu = cpu_baseline(args.n, 1)
     serving = serving_run(args) if (rank == 0 and ws == 1 and args.serving_requests > 0) else None
     multigroup = mg_run(args) if (rank == 0 and ws == 1 and args.mg_steps > 0) else None
+    voronoi = voronoi_run(args) if (rank == 0 and ws == 1 and args.voronoi_steps > 0) else None
     if rank == 0:
         lat = sorted(f32["step_ms"])
         line = {
@@ -489,7 +535,7 @@ def run_storm(args, ws, rank, local, dist):
                      "roofline": roofline(f64, BYTES_PER_SEGMENT_FP64, transport_kernel(args, False))},
             "fp32_over_fp64": v32 / v64,
             "fp32_vs_fp64_deviation": dev,
-            "cpu_baseline": cpu, "e2e": e2e, "serving": serving, "multigroup": multigroup, "clocks": ck,
+            "cpu_baseline": cpu, "e2e": e2e, "serving": serving, "multigroup": multigroup, "voronoi": voronoi, "clocks": ck,
             "gpu_launches": f32["launches"],
             "transport_share": f32["transport"]["kernel_ms"] / max(sum(f32["step_ms"]), 1e-9),
         }

@@ -12,7 +12,7 @@ SOURCES = ["storm_kernels.cu", "storm_runtime.cu", "storm_noalloc.cu", "storm_se
 HEADERS = ["storm_device.cuh", "storm_internal.h"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 # --fmad=false: plain expressions round like the reference's build (no contraction)
-FLAGS = ["-O3", "-lineinfo", "--fmad=false", "-std=c++17", "-Xcompiler", "-fPIC,-O2", "-shared"]
+FLAGS = ["-O3", "-lineinfo", "--fmad=false", "-std=c++17", "-Xcompiler", "-fPIC,-O2", "-shared", "-lpthread"]
 
 
 def _stale():

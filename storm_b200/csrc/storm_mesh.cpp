@@ -21,6 +21,7 @@
 #include <cstring>
 #include <map>
 #include <new>
+#include <thread>
 #include <utility>
 #include <vector>
 
@@ -171,7 +172,8 @@ extern "C" int storm_mesh_voronoi(const double *points, uint32_t n, const double
     const double binW = std::min(ext.x / bx, std::min(ext.y / by, ext.z / bz));
 
     std::vector<std::vector<PFace>> cells(n);
-    for (uint32_t i = 0; i < n; ++i) {
+    // cells are independent: host threads take interleaved indices
+    auto buildCell = [&](uint32_t i) {
         std::vector<PFace> c;
         // the box: faces x-low, x-high, y-low, y-high, z-low, z-high (GetBoxFaces order)
         const V3 v[8] = {{lo.x, lo.y, lo.z}, {hi.x, lo.y, lo.z}, {hi.x, hi.y, lo.z}, {lo.x, hi.y, lo.z},
@@ -223,6 +225,16 @@ extern "C" int storm_mesh_voronoi(const double *points, uint32_t n, const double
             ++ring;
         }
         cells[i].swap(c);
+    };
+    {
+        unsigned nt = std::max(1u, std::min(32u, std::thread::hardware_concurrency()));
+        if (n < 4096) nt = 1;
+        std::vector<std::thread> pool;
+        for (unsigned t = 0; t < nt; ++t)
+            pool.emplace_back([&, t] {
+                for (uint32_t i = t; i < n; i += nt) buildCell(i);
+            });
+        for (auto &th : pool) th.join();
     }
 
     // global faces

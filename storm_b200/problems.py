@@ -548,7 +548,10 @@ def voronoi_cube(ncells=200000, packets_per_step=2e7, seed=42, dt=1e-11, precisi
     p.sigma_a = kappa_median * np.exp(kappa_sigma_ln * rng.standard_normal(n))
     p.sigma_s = np.zeros(n)
     p.faces = [BoxFace(A.FACE_ESCAPE) for _ in range(6)]
-    p.new_photons_per_cell = max(1, int(round(packets_per_step / n)))
+    # the allocation floors each cell at newPhotonsPerCell and gives hot cells up
+    # to 20 times it; with these lognormal temperatures the total is about 3.1
+    # times the floor, so the floor is a third of the per-cell mean
+    p.new_photons_per_cell = max(1, int(round(packets_per_step / (3.1 * n))))
     p.with_random_walk = with_random_walk
     p.rw_min_cell_optical_depth = 20.0 / 3.0
     p.rw_min_particle_optical_depth = 5.0
