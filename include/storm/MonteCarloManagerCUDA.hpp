@@ -172,6 +172,64 @@ std::array<std::vector<double>, 3> rectilinear_edges(const Grid &grid) {
     return e;
 }
 
+// A grid that is not rectilinear (a Voronoi grid) lowered through the reference
+// Grid API into the engine's convex-polyhedral mesh: per cell its faces in
+// GetCellFaces order; per face the real cell first, its neighbour (ghost
+// indices >= N kept as they are), Normal, FaceCM, GetArea and the polygon of
+// GetPointsInFace over GetFacePoints; mesh points GetMeshPoint; volumes GetVolume.
+struct PolyMeshArrays {
+    StormPolyMesh mesh{};
+    std::vector<double> points, volume, normal, cm, area, vertices;
+    std::vector<std::uint32_t> cellFaceOffset, cellFaces, faceCells, faceVertexOffset, faceVertices;
+};
+
+template <typename Grid>
+void lower_polyhedral(const Grid &grid, PolyMeshArrays &m) {
+    const std::size_t N = grid.GetPointNo();
+    const std::size_t F = grid.GetTotalFacesNumber();
+    const auto box = grid.GetBoxCoordinates();
+    m.points.resize(3 * N);
+    m.volume.resize(N);
+    m.cellFaceOffset.assign(1, 0);
+    for (std::size_t c = 0; c < N; ++c) {
+        const auto p = grid.GetMeshPoint(c);
+        m.points[3 * c] = p.x; m.points[3 * c + 1] = p.y; m.points[3 * c + 2] = p.z;
+        m.volume[c] = grid.GetVolume(c);
+        for (const std::size_t &f : grid.GetCellFaces(c)) m.cellFaces.push_back(static_cast<std::uint32_t>(f));
+        m.cellFaceOffset.push_back(static_cast<std::uint32_t>(m.cellFaces.size()));
+    }
+    const auto &nodes = grid.GetFacePoints();
+    m.vertices.resize(3 * nodes.size());
+    for (std::size_t v = 0; v < nodes.size(); ++v) {
+        m.vertices[3 * v] = nodes[v].x; m.vertices[3 * v + 1] = nodes[v].y; m.vertices[3 * v + 2] = nodes[v].z;
+    }
+    m.faceVertexOffset.assign(1, 0);
+    for (std::size_t f = 0; f < F; ++f) {
+        auto nb = grid.GetFaceNeighbors(f);
+        if (nb.first >= N) std::swap(nb.first, nb.second);
+        m.faceCells.push_back(static_cast<std::uint32_t>(nb.first));
+        m.faceCells.push_back(static_cast<std::uint32_t>(nb.second < N ? nb.second : N + f));
+        const auto n = grid.Normal(f);
+        const auto q = grid.FaceCM(f);
+        m.normal.insert(m.normal.end(), {n.x, n.y, n.z});
+        m.cm.insert(m.cm.end(), {q.x, q.y, q.z});
+        m.area.push_back(grid.GetArea(f));
+        for (const std::size_t &v : grid.GetPointsInFace(f)) m.faceVertices.push_back(static_cast<std::uint32_t>(v));
+        m.faceVertexOffset.push_back(static_cast<std::uint32_t>(m.faceVertices.size()));
+    }
+    StormPolyMesh &d = m.mesh;
+    d.ncells = static_cast<std::uint32_t>(N);
+    d.nfaces = static_cast<std::uint32_t>(F);
+    d.nvertices = static_cast<std::uint32_t>(nodes.size());
+    d.box[0] = box.first.x; d.box[1] = box.first.y; d.box[2] = box.first.z;
+    d.box[3] = box.second.x; d.box[4] = box.second.y; d.box[5] = box.second.z;
+    d.points = m.points.data(); d.volume = m.volume.data();
+    d.cell_face_offset = m.cellFaceOffset.data(); d.cell_faces = m.cellFaces.data(); d.face_cells = m.faceCells.data();
+    d.face_normal = m.normal.data(); d.face_cm = m.cm.data(); d.face_area = m.area.data();
+    d.face_vertex_offset = m.faceVertexOffset.data(); d.face_vertices = m.faceVertices.data();
+    d.vertices = m.vertices.data();
+}
+
 }  // namespace cuda_detail
 
 template <typename T, typename Grid, typename CellT = RadiationCell, typename ExtensivesT = SimpleExtensives>
@@ -246,7 +304,17 @@ public:
 
 private:
     void create() {
-        auto edges = cuda_detail::rectilinear_edges(grid_);
+        // a rectilinear Cartesian grid runs on the engine's Cartesian path; any
+        // other grid (Voronoi) is lowered to its convex-polyhedral mesh
+        std::array<std::vector<double>, 3> edges;
+        bool rectilinear = true;
+        try {
+            edges = cuda_detail::rectilinear_edges(grid_);
+        } catch (const StormError &) {
+            rectilinear = false;
+            cuda_detail::lower_polyhedral(grid_, poly_);
+            for (auto &e : edges) e = {0.0, 1.0};
+        }
         const std::size_t N = grid_.GetPointNo();
         auto &cells = *binding_.cells;
         auto &ext = *binding_.extensives;
@@ -333,6 +401,7 @@ private:
         d.segments_per_visit = binding_.segmentsPerVisit;
         d.per_cell_segment_counters = 1;
         d.device = binding_.device;
+        if (!rectilinear) d.mesh = &poly_.mesh;
         cuda_detail::check(storm_cuda_create(&d, &h_), nullptr, "storm_cuda_create");
         N_ = N;
         cellsStepsCounters_.assign(N, 0);
@@ -420,6 +489,7 @@ private:
     StormHandle *h_ = nullptr;
     std::size_t N_ = 0;
     bool multigroup_ = false;
+    cuda_detail::PolyMeshArrays poly_;
     std::vector<std::size_t> cellsStepsCounters_;
     std::vector<double> hostT_, hostE_, hostCE_, eradAvg_, sigmaA_, fleck_;
     std::size_t startParticleCount_ = 0, initialParticleCount_ = 0, preStepParticleCount_ = 0, endParticleCount_ = 0;

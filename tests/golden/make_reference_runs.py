@@ -45,7 +45,12 @@ def run_one(name):
 
 def main(names):
     ctx = mp.get_context("spawn")
-    out = {}
+    path = os.path.join(HERE, "reference_runs.npz")
+    # problems not rerun keep their earlier results
+    out = dict(np.load(path)) if os.path.exists(path) else {}
+    for name in names:
+        for k in [k for k in out if k.startswith(name + "_")]:
+            del out[k]
     with ctx.Pool(len(names), maxtasksperchild=1) as pool:
         for name, res, l1, wall in pool.imap_unordered(run_one, names):
             print(f"{name}: L1 {l1:.4e}, {res['steps']} steps, {wall:.0f} s", flush=True)
@@ -53,7 +58,7 @@ def main(names):
                 out[f"{name}_{k}"] = res[k]
             out[f"{name}_l1"] = np.float64(l1)
             out[f"{name}_wall"] = np.float64(wall)
-    np.savez_compressed(os.path.join(HERE, "reference_runs.npz"), **out)
+    np.savez_compressed(path, **out)
 
 
 if __name__ == "__main__":

@@ -102,7 +102,7 @@ def _close(a, b, rel, atol=1e-300):
     return np.abs(a - b) <= rel * np.maximum(np.abs(a), np.abs(b)) + atol
 
 
-@pytest.mark.parametrize("kind", ["slab", "cube", "multigroup", "stratified", "ddmc"])
+@pytest.mark.parametrize("kind", ["slab", "cube", "multigroup", "stratified", "ddmc", "voronoi"])
 def test_dropin_matches_engine(kind):
     L = _lib()
     if kind == "slab":
@@ -114,6 +114,8 @@ def test_dropin_matches_engine(kind):
         p.comb_nmin = 10
     elif kind == "stratified":   # StratifiedCombPopulationControl with frequency bins
         p = problems.strat_cube(n=4)
+    elif kind == "voronoi":   # a Voronoi grid, lowered by the template through the Grid API
+        p = problems.voronoi_cube(ncells=200, packets_per_step=1e4, seed=3)
     else:   # DDMC leakage in the thick half
         p = problems.ddmc_cube(n=8, new_photons_per_cell=3, face_packets=40, comb_nmin=10)
     d = DropIn(L, p)
