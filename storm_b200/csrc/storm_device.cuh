@@ -813,6 +813,7 @@ __device__ inline PhysOut physics_step(const Ctx &C, Track &T, RNG &rng, TALLY &
     if constexpr (POLY) {
         const uint32_t k0 = C.cfo[cell], k1 = C.cfo[cell + 1];
         double minAlpha = DBL_MAX;
+#pragma unroll 4
         for (uint32_t q = k0; q < k1; ++q) {
             const double4 n = C.cfN[q];
             const double nv = n.x * p.vx + n.y * p.vy + n.z * p.vz;
@@ -1235,8 +1236,12 @@ __device__ inline int segment32(const Ctx &C, Track32 &T, RNG &rng, TALLY &tal, 
     // problem only below the cell's PGRW group cutoff
     float Ro;
     if constexpr (POLY) {
-        Ro = FLT_MAX;
-        for (uint32_t k = C.cfo[cell]; k < C.cfo[cell + 1]; ++k) Ro = fminf(Ro, poly_dist32(C, k, T.qx, T.qy, T.qz));
+        Ro = 0.0f;   // only Random Walk cells (finite reach) need the distance to the faces
+        if (cp.z < CUDART_INF_F) {
+            Ro = FLT_MAX;
+#pragma unroll 4
+            for (uint32_t k = C.cfo[cell]; k < C.cfo[cell + 1]; ++k) Ro = fminf(Ro, poly_dist32(C, k, T.qx, T.qy, T.qz));
+        }
     } else {
         Ro = fminf(fminf(hx - fabsf(T.qx), hy - fabsf(T.qy)), hz - fabsf(T.qz));
     }
@@ -1270,6 +1275,7 @@ __device__ inline int segment32(const Ctx &C, Track32 &T, RNG &rng, TALLY &tal, 
     if constexpr (POLY) {
         float bestS = FLT_MAX;
         const uint32_t k0 = C.cfo[cell], k1 = C.cfo[cell + 1];
+#pragma unroll 4
         for (uint32_t k = k0; k < k1; ++k) {
             const float4 pl = C.cfN32[k];
             const float un = T.ux * pl.x + T.uy * pl.y + T.uz * pl.z;
