@@ -54,6 +54,7 @@ def parse():
     ap.add_argument("--mg-steps", type=int, default=5, help="timed steps of the multigroup run (0 = skip it)")
     ap.add_argument("--voronoi-steps", type=int, default=5, help="timed steps of the Voronoi-mesh run (0 = skip it)")
     ap.add_argument("--voronoi-cells", type=int, default=200000)
+    ap.add_argument("--voronoi-packets", type=float, default=2e7, help="packets per step of the Voronoi-mesh run")
     ap.add_argument("--mg-n", type=int, default=128)
     ap.add_argument("--serving-requests", type=int, default=32, help="requests in the serving run (0 = skip it)")
     ap.add_argument("--serving-slots", type=int, default=12)
@@ -397,11 +398,12 @@ def voronoi_run(args):
     build_s = time.perf_counter() - t0
     out = {"workload": f"Voronoi mesh of {args.voronoi_cells} cells in the unit cube "
                        f"({mesh.cell_faces.size / mesh.ncells:.1f} faces/cell), kappa lognormal median 10 1/cm "
-                       "sigma_ln 1, T0 lognormal median 0.05 keV, ~2e7 packets/step, vacuum box, RW",
+                       f"sigma_ln 1, T0 lognormal median 0.05 keV, ~{args.voronoi_packets:.0e} packets/step, "
+                       "vacuum box, RW",
            "steps": args.voronoi_steps, "mesh_build_s": build_s}
     temps = {}
     for name, prec in (("fp32", A.PRECISION_FP32_TRACK), ("fp64", A.PRECISION_FP64)):
-        p = problems.voronoi_cube(ncells=args.voronoi_cells, packets_per_step=2e7, seed=5, mesh=mesh,
+        p = problems.voronoi_cube(ncells=args.voronoi_cells, packets_per_step=args.voronoi_packets, seed=5, mesh=mesh,
                                   precision=prec)
         p.per_cell_segment_counters = False
         e = Engine(p)
