@@ -417,6 +417,19 @@ int storm_cuda_emission_allocation_noalloc(int device, const double *d_energy, u
                                            uint64_t new_photons_per_cell, uint64_t *d_photons,
                                            uint64_t *d_offsets, void *stream);
 
+/* ---------------------------------------------------------------- checkpoints */
+
+/* The state one step hands the next -- the census bank in the handle's own
+ * layout, every cell's temperature and internal energies, the face source
+ * temperatures and the step counter that keys the random streams -- copied
+ * to a host buffer of storm_cuda_checkpoint_size bytes, and back into a handle
+ * created from the same problem (same cells, precision and groups), after
+ * which the following steps repeat those of the original run.  No reference
+ * counterpart: the reference's managers keep no restartable state. */
+int storm_cuda_checkpoint_size(StormHandle *h, uint64_t *bytes);
+int storm_cuda_checkpoint_save(StormHandle *h, void *buffer, uint64_t bytes);
+int storm_cuda_checkpoint_load(StormHandle *h, const void *buffer, uint64_t bytes);
+
 /* ---------------------------------------------------------------- meshes */
 
 /* A bounded Voronoi tessellation of `n` generator points (3 n doubles, strictly

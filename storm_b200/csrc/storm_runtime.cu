@@ -1551,6 +1551,125 @@ int storm_cuda_set_cell_physics(StormHandle *h, const double *sigA, const double
     return STORM_OK;
 }
 
+// ---------------------------------------------------------------- checkpoints
+// A checkpoint is the state one step hands the next: the census bank as it
+// sits on the device (either form's layout, byte for byte), the material state
+// of every cell, the face source temperatures and the step counter that keys
+// the random streams.  Loaded into a handle created from the same problem, the
+// following steps repeat those of the run it was taken from.
+namespace {
+struct CheckpointHeader {
+    char magic[8];               // "STORMCK1"
+    uint32_t abi, precision, groups, ncells;
+    uint64_t nCensus, step;
+    double faceT[6];
+};
+constexpr size_t kBankArrays = 9;   // x y z vx vy vz t w w0 (8 bytes per particle each)
+size_t checkpoint_bytes(const StormHandle *h, uint64_t n) {
+    const size_t perParticle = kBankArrays * 8 + 3 * 4 + (h->C.groups >= 2 ? 8 : 0);
+    return sizeof(CheckpointHeader) + n * perParticle + 3 * static_cast<size_t>(h->N) * 8;
+}
+}  // namespace
+
+int storm_cuda_checkpoint_size(StormHandle *h, uint64_t *bytes) {
+    if (!h || !bytes) return STORM_ERR_INVALID_ARG;
+    *bytes = checkpoint_bytes(h, h->nCensus);
+    return STORM_OK;
+}
+
+int storm_cuda_checkpoint_save(StormHandle *h, void *buffer, uint64_t bytes) {
+    if (!h || !buffer) return STORM_ERR_INVALID_ARG;
+    const uint64_t n = h->nCensus;
+    if (bytes < checkpoint_bytes(h, n)) return STORM_ERR_INVALID_ARG;
+    CK(cudaSetDevice(h->device));
+    char *out = static_cast<char *>(buffer);
+    CheckpointHeader hd{};
+    std::memcpy(hd.magic, "STORMCK1", 8);
+    hd.abi = STORM_CUDA_ABI_VERSION;
+    hd.precision = static_cast<uint32_t>(h->desc.precision);
+    hd.groups = h->C.groups;
+    hd.ncells = h->N;
+    hd.nCensus = n;
+    hd.step = h->step;
+    for (int f = 0; f < 6; ++f) hd.faceT[f] = h->C.sourceT[f];
+    std::memcpy(out, &hd, sizeof(hd));
+    out += sizeof(hd);
+    const Bank &b = h->bankA;
+    double *arrs[kBankArrays] = {b.x, b.y, b.z, b.vx, b.vy, b.vz, b.t, b.w, b.w0};
+    for (double *a : arrs) {
+        if (n) CK(cudaMemcpyAsync(out, a, n * 8, cudaMemcpyDeviceToHost, h->stream));
+        out += n * 8;
+    }
+    uint32_t *ia[3] = {b.cell, b.pid, b.draw};
+    for (uint32_t *a : ia) {
+        if (n) CK(cudaMemcpyAsync(out, a, n * 4, cudaMemcpyDeviceToHost, h->stream));
+        out += n * 4;
+    }
+    if (h->C.groups >= 2) {
+        if (n) CK(cudaMemcpyAsync(out, b.nu, n * 8, cudaMemcpyDeviceToHost, h->stream));
+        out += n * 8;
+    }
+    const double *cells[3] = {h->A.T, h->A.eint, h->A.ceint};
+    for (const double *a : cells) {
+        CK(cudaMemcpyAsync(out, a, static_cast<size_t>(h->N) * 8, cudaMemcpyDeviceToHost, h->stream));
+        out += static_cast<size_t>(h->N) * 8;
+    }
+    CK(cudaStreamSynchronize(h->stream));
+    return STORM_OK;
+}
+
+int storm_cuda_checkpoint_load(StormHandle *h, const void *buffer, uint64_t bytes) {
+    if (!h || !buffer || bytes < sizeof(CheckpointHeader)) return STORM_ERR_INVALID_ARG;
+    CheckpointHeader hd;
+    std::memcpy(&hd, buffer, sizeof(hd));
+    if (std::memcmp(hd.magic, "STORMCK1", 8) != 0 || hd.abi != STORM_CUDA_ABI_VERSION ||
+        hd.precision != static_cast<uint32_t>(h->desc.precision) || hd.groups != h->C.groups || hd.ncells != h->N)
+        return STORM_ERR_INVALID_ARG;
+    const uint64_t n = hd.nCensus;
+    if (bytes < checkpoint_bytes(h, n)) return STORM_ERR_INVALID_ARG;
+    CK(cudaSetDevice(h->device));
+    int rc = ensure_capacity(h, n, 0);
+    if (rc != STORM_OK) return rc;
+    const char *in = static_cast<const char *>(buffer) + sizeof(hd);
+    const Bank &b = h->bankA;
+    double *arrs[kBankArrays] = {b.x, b.y, b.z, b.vx, b.vy, b.vz, b.t, b.w, b.w0};
+    for (double *a : arrs) {
+        if (n) CK(cudaMemcpyAsync(a, in, n * 8, cudaMemcpyHostToDevice, h->stream));
+        in += n * 8;
+    }
+    uint32_t *ia[3] = {b.cell, b.pid, b.draw};
+    for (uint32_t *a : ia) {
+        if (n) CK(cudaMemcpyAsync(a, in, n * 4, cudaMemcpyHostToDevice, h->stream));
+        in += n * 4;
+    }
+    if (h->C.groups >= 2) {
+        if (n) CK(cudaMemcpyAsync(b.nu, in, n * 8, cudaMemcpyHostToDevice, h->stream));
+        in += n * 8;
+    }
+    double *cells[3] = {h->A.T, h->A.eint, h->A.ceint};
+    for (double *a : cells) {
+        CK(cudaMemcpyAsync(a, in, static_cast<size_t>(h->N) * 8, cudaMemcpyHostToDevice, h->stream));
+        in += static_cast<size_t>(h->N) * 8;
+    }
+    CK(cudaStreamSynchronize(h->stream));
+    // the census must name cells of this grid
+    if (n) {
+        CK(cudaMemsetAsync(h->dAmbiguous + 1, 0, sizeof(int32_t), h->stream));
+        launch_count_bad_cells(h->stream, b.cell, static_cast<uint32_t>(n), h->N, h->dAmbiguous + 1);
+        int32_t nb = 0;
+        CK(cudaMemcpyAsync(&nb, h->dAmbiguous + 1, sizeof(int32_t), cudaMemcpyDeviceToHost, h->stream));
+        CK(cudaStreamSynchronize(h->stream));
+        if (nb) return STORM_ERR_INVALID_ARG;
+    }
+    h->nCensus = n;
+    h->step = static_cast<uint32_t>(hd.step);
+    for (int f = 0; f < 6; ++f) {
+        rc = storm_cuda_set_face_temperature(h, f, hd.faceT[f]);
+        if (rc != STORM_OK) return rc;
+    }
+    return STORM_OK;
+}
+
 int storm_cuda_set_face_temperature(StormHandle *h, int face, double T) {
     if (!h || face < 0 || face > 5 || !(T >= 0.0)) return STORM_ERR_INVALID_ARG;
     CK(cudaSetDevice(h->device));

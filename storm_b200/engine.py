@@ -34,6 +34,9 @@ def lib():
         L.storm_cuda_create.argtypes = [C.POINTER(A.StormProblemDesc), C.POINTER(vp)]
         L.storm_mesh_voronoi.argtypes = [dp, C.c_uint32, dp, C.POINTER(C.POINTER(A.StormPolyMesh))]
         L.storm_mesh_free.argtypes = [C.POINTER(A.StormPolyMesh)]
+        L.storm_cuda_checkpoint_size.argtypes = [vp, u64p]
+        L.storm_cuda_checkpoint_save.argtypes = [vp, C.c_void_p, C.c_uint64]
+        L.storm_cuda_checkpoint_load.argtypes = [vp, C.c_void_p, C.c_uint64]
         L.storm_cuda_destroy.argtypes = [vp]
         L.storm_cuda_step.argtypes = [vp, C.c_double, C.POINTER(A.StormStepStats)]
         for f in ("begin", "prestep", "emit", "poststep"):
@@ -245,6 +248,20 @@ class Engine:
     def set_cell_physics(self, sigma_a=None, sigma_s=None, fleck=None):
         arr = [None if a is None else np.ascontiguousarray(a, float) for a in (sigma_a, sigma_s, fleck)]
         self._check(lib().storm_cuda_set_cell_physics(self.h, *[A.ptr(a) for a in arr]))
+
+    def checkpoint(self):
+        """The handle's step-to-step state (census bank, cell state, face
+        temperatures, step counter) as bytes."""
+        n = C.c_uint64()
+        self._check(lib().storm_cuda_checkpoint_size(self.h, C.byref(n)))
+        buf = np.empty(n.value, np.uint8)
+        self._check(lib().storm_cuda_checkpoint_save(self.h, buf.ctypes.data, n.value))
+        return buf.tobytes()
+
+    def restore(self, blob):
+        """Load a checkpoint taken from a handle of the same problem."""
+        buf = np.frombuffer(blob, np.uint8)
+        self._check(lib().storm_cuda_checkpoint_load(self.h, buf.ctypes.data, len(buf)))
 
     def set_face_temperature(self, face, T):
         self._check(lib().storm_cuda_set_face_temperature(self.h, face, T))
