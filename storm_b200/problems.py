@@ -446,7 +446,8 @@ def densmore_group_bounds(groups=30):
     return b
 
 
-def densmore2012(nx=512, new_photons_per_cell=16, boundary_per_face=100, seed=42, precision=A.PRECISION_FP64):
+def densmore2012(nx=512, new_photons_per_cell=16, boundary_per_face=100, seed=42, precision=A.PRECISION_FP64,
+                 comb_nmin=200):
     """Densmore et al. (2012) Fig. 4, as examples/densmore2012/main.cpp:128-208
     sets it up: x in [0, 3] cm (nx x 1 x 1), sigma(E) = sigma0 / (sqrt(kT) E^3)
     with sigma0 = 10 keV^3.5/cm below x = 2 and 1000 keV^3.5/cm above, 30
@@ -473,7 +474,7 @@ def densmore2012(nx=512, new_photons_per_cell=16, boundary_per_face=100, seed=42
     p.new_photons_per_cell = new_photons_per_cell
     p.with_random_walk = True
     p.comb_enabled = True
-    p.comb_nmin, p.comb_factor = 200, 5.0
+    p.comb_nmin, p.comb_factor = comb_nmin, 5.0
     p.seed, p.dt, p.precision, p.name = seed, 5e-12, precision, "densmore2012"
     return p
 
