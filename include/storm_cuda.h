@@ -502,6 +502,9 @@ int storm_cuda_last_error(StormHandle *h, int32_t *derr, uint64_t *cell, uint64_
  * handles on the same device (cudaFree would wait for every stream on the
  * device).  This returns the cached blocks of `device` to the driver. */
 int storm_cuda_release_cached(int device, uint64_t *bytes);
+/* The cache's cudaMalloc and cudaFree calls since the library loaded, and the
+ * bytes it holds cached and handed out, over all devices. */
+int storm_cuda_pool_counters(uint64_t *mallocs, uint64_t *frees, uint64_t *cached_bytes, uint64_t *live_bytes);
 /* Bytes of device memory the handle holds (GetHandlerMemoryBytes). */
 int storm_cuda_memory_bytes(StormHandle *h, uint64_t *bytes);
 /* Kernel launches issued by the handle since creation (for launch accounting). */

@@ -50,9 +50,8 @@ struct StormHandle {
     uint32_t *segs = nullptr;
     OpacityEos M{};
     Ctx C{};
-    // random walk tables
+    // random walk tables (shared by every handle on the device, not owned)
     double *rwTau = nullptr, *rwLogTau = nullptr, *rwSurv = nullptr, *rwRadius = nullptr;
-    float *rwLogTau32 = nullptr, *rwSurv32 = nullptr, *rwRadius32 = nullptr;   // FP32-tracking form
     double *gb = nullptr;            // multigroup bounds
     float *gb32 = nullptr, *gc32 = nullptr;   // multigroup bounds and centres, FP32-tracking form
     double *faceCdf = nullptr;                // multigroup: 6 x (groups + 1) face Planck spectra
@@ -171,6 +170,7 @@ public:
         if (e != cudaSuccess) return e;
         std::lock_guard<std::mutex> lk(m_);
         live_[*p] = {dev, want};
+        ++mallocs_;
         return cudaSuccess;
     }
     void free(void *p) {
@@ -198,6 +198,7 @@ public:
                 }
             }
             cached_ -= bytes;
+            frees_ += blocks.size();
         }
         int prev = 0;
         cudaGetDevice(&prev);
@@ -205,6 +206,17 @@ public:
         for (void *b : blocks) cudaFree(b);
         cudaSetDevice(prev);
         return bytes;
+    }
+
+    // cudaMalloc and cudaFree calls so far, and the bytes cached and live on all devices
+    void counters(uint64_t *mallocs, uint64_t *frees, uint64_t *cached, uint64_t *live) {
+        std::lock_guard<std::mutex> lk(m_);
+        *mallocs = mallocs_;
+        *frees = frees_;
+        *cached = cached_;
+        uint64_t l = 0;
+        for (const auto &kv : live_) l += kv.second.second;
+        *live = l;
     }
 
 private:
@@ -221,11 +233,47 @@ private:
     std::unordered_map<void *, std::pair<int, size_t>> live_;
     std::multimap<std::pair<int, size_t>, void *> free_;
     size_t cached_ = 0;
+    uint64_t mallocs_ = 0, frees_ = 0;
 };
 
 DevicePool &device_pool() {
     static DevicePool pool;
     return pool;
+}
+
+// A handle's stream and its six timing events outlive the handle: destroy
+// returns them, idle, to a per-device cache and the next create takes them
+// from there instead of creating new ones.
+struct StreamSet {
+    cudaStream_t stream = nullptr;
+    cudaEvent_t ev[6] = {};
+};
+std::mutex &stream_cache_mutex() {
+    static std::mutex m;
+    return m;
+}
+std::multimap<int, StreamSet> &stream_cache() {
+    static std::multimap<int, StreamSet> c;
+    return c;
+}
+bool take_stream_set(int dev, StreamSet &out) {
+    {
+        std::lock_guard<std::mutex> lk(stream_cache_mutex());
+        auto it = stream_cache().find(dev);
+        if (it != stream_cache().end()) {
+            out = it->second;
+            stream_cache().erase(it);
+            return true;
+        }
+    }
+    if (cudaStreamCreateWithFlags(&out.stream, cudaStreamNonBlocking) != cudaSuccess) return false;
+    for (cudaEvent_t &e : out.ev)
+        if (cudaEventCreate(&e) != cudaSuccess) return false;
+    return true;
+}
+void return_stream_set(int dev, const StreamSet &s) {
+    std::lock_guard<std::mutex> lk(stream_cache_mutex());
+    stream_cache().emplace(dev, s);
 }
 
 template <class T>
@@ -409,10 +457,12 @@ int build_face_sources(StormHandle *h) {
     CK(dalloc(h, &h->fsSide, side.size()));
     CK(dalloc(h, &h->fsOffset, off.size()));
     if (!cell.empty()) {
-        CK(cudaMemcpy(h->fsCell, cell.data(), cell.size() * sizeof(uint32_t), cudaMemcpyHostToDevice));
-        CK(cudaMemcpy(h->fsSide, side.data(), side.size() * sizeof(int32_t), cudaMemcpyHostToDevice));
+        CK(cudaMemcpyAsync(h->fsCell, cell.data(), cell.size() * sizeof(uint32_t), cudaMemcpyHostToDevice, h->stream));
+        CK(cudaMemcpyAsync(h->fsSide, side.data(), side.size() * sizeof(int32_t), cudaMemcpyHostToDevice, h->stream));
     }
-    CK(cudaMemcpy(h->fsOffset, off.data(), off.size() * sizeof(uint64_t), cudaMemcpyHostToDevice));
+    CK(cudaMemcpyAsync(h->fsOffset, off.data(), off.size() * sizeof(uint64_t), cudaMemcpyHostToDevice, h->stream));
+    // the host vectors go out of scope here
+    CK(cudaStreamSynchronize(h->stream));
     return STORM_OK;
 }
 
@@ -445,38 +495,65 @@ struct RwHostTables {
     }
 };
 
+// The device tables depend on nothing but constants: built once per device by
+// the first handle created there and shared, read-only, by every later handle
+// (never freed).  Building them per handle cost a table kernel and a stream
+// synchronisation in every storm_cuda_create.
+struct RwDeviceTables {
+    double *tau = nullptr, *logTau = nullptr, *surv = nullptr, *radius = nullptr;
+    float *logTau32 = nullptr, *surv32 = nullptr, *radius32 = nullptr;
+};
+std::mutex &rw_tables_mutex() {
+    static std::mutex m;
+    return m;
+}
+std::map<int, RwDeviceTables> &rw_tables_by_device() {
+    static std::map<int, RwDeviceTables> t;
+    return t;
+}
+
 int build_rw_tables(StormHandle *h) {
     static const RwHostTables host;   // thread-safe initialisation
-    const std::vector<double> &tau = host.tau, &ltau = host.ltau, &surv = host.surv;
     const double logMin = std::log(1e-8), logMax = std::log(64.0);
-    CK(dalloc(h, &h->rwTau, RW_TABLE));
-    CK(dalloc(h, &h->rwLogTau, RW_TABLE));
-    CK(dalloc(h, &h->rwSurv, RW_TABLE));
-    CK(dalloc(h, &h->rwRadius, static_cast<size_t>(RW_TABLE) * RW_RADIUS));
-    CK(cudaMemcpy(h->rwTau, tau.data(), RW_TABLE * sizeof(double), cudaMemcpyHostToDevice));
-    CK(cudaMemcpy(h->rwLogTau, ltau.data(), RW_TABLE * sizeof(double), cudaMemcpyHostToDevice));
-    CK(cudaMemcpy(h->rwSurv, surv.data(), RW_TABLE * sizeof(double), cudaMemcpyHostToDevice));
-    launch_rw_radius(h->stream, h->rwTau, h->rwSurv, h->rwRadius);
-    ++h->launches;
-    CK(cudaGetLastError());
-    if (h->fp32) {
-        CK(dalloc(h, &h->rwLogTau32, RW_TABLE));
-        CK(dalloc(h, &h->rwSurv32, RW_TABLE));
-        CK(dalloc(h, &h->rwRadius32, static_cast<size_t>(RW_TABLE) * RW_RADIUS));
-        launch_to_float(h->stream, h->rwLogTau, h->rwLogTau32, RW_TABLE);
-        launch_to_float(h->stream, h->rwSurv, h->rwSurv32, RW_TABLE);
-        launch_to_float(h->stream, h->rwRadius, h->rwRadius32, RW_TABLE * RW_RADIUS);
-        h->launches += 3;
+    std::lock_guard<std::mutex> lk(rw_tables_mutex());
+    auto &all = rw_tables_by_device();
+    auto it = all.find(h->device);
+    if (it == all.end()) {
+        RwDeviceTables t;
+        const size_t R = static_cast<size_t>(RW_TABLE) * RW_RADIUS;
+        CK(cudaMalloc(&t.tau, RW_TABLE * sizeof(double)));
+        CK(cudaMalloc(&t.logTau, RW_TABLE * sizeof(double)));
+        CK(cudaMalloc(&t.surv, RW_TABLE * sizeof(double)));
+        CK(cudaMalloc(&t.radius, R * sizeof(double)));
+        CK(cudaMalloc(&t.logTau32, RW_TABLE * sizeof(float)));
+        CK(cudaMalloc(&t.surv32, RW_TABLE * sizeof(float)));
+        CK(cudaMalloc(&t.radius32, R * sizeof(float)));
+        CK(cudaMemcpyAsync(t.tau, host.tau.data(), RW_TABLE * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+        CK(cudaMemcpyAsync(t.logTau, host.ltau.data(), RW_TABLE * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+        CK(cudaMemcpyAsync(t.surv, host.surv.data(), RW_TABLE * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+        launch_rw_radius(h->stream, t.tau, t.surv, t.radius);
+        launch_to_float(h->stream, t.logTau, t.logTau32, RW_TABLE);
+        launch_to_float(h->stream, t.surv, t.surv32, RW_TABLE);
+        launch_to_float(h->stream, t.radius, t.radius32, RW_TABLE * RW_RADIUS);
+        h->launches += 4;
         CK(cudaGetLastError());
-        h->C.rw.logTau32 = h->rwLogTau32;
-        h->C.rw.surv32 = h->rwSurv32;
-        h->C.rw.radius32 = h->rwRadius32;
+        CK(cudaStreamSynchronize(h->stream));   // complete before any other handle reads them
+        it = all.emplace(h->device, t).first;
     }
-    CK(cudaStreamSynchronize(h->stream));
-    h->C.rw.tau = h->rwTau;
-    h->C.rw.logTau = h->rwLogTau;
-    h->C.rw.surv = h->rwSurv;
-    h->C.rw.radius = h->rwRadius;
+    const RwDeviceTables &t = it->second;
+    h->rwTau = t.tau;
+    h->rwLogTau = t.logTau;
+    h->rwSurv = t.surv;
+    h->rwRadius = t.radius;
+    h->C.rw.tau = t.tau;
+    h->C.rw.logTau = t.logTau;
+    h->C.rw.surv = t.surv;
+    h->C.rw.radius = t.radius;
+    if (h->fp32) {
+        h->C.rw.logTau32 = t.logTau32;
+        h->C.rw.surv32 = t.surv32;
+        h->C.rw.radius32 = t.radius32;
+    }
     h->C.rw.logMin = logMin;
     h->C.rw.logMax = logMax;
     return STORM_OK;
@@ -553,6 +630,12 @@ int storm_cuda_release_cached(int device, uint64_t *bytes) {
     if (device < 0 || device >= ndev) return STORM_ERR_INVALID_ARG;
     const size_t b = device_pool().release(device);
     if (bytes) *bytes = b;
+    return STORM_OK;
+}
+
+int storm_cuda_pool_counters(uint64_t *mallocs, uint64_t *frees, uint64_t *cached_bytes, uint64_t *live_bytes) {
+    if (!mallocs || !frees || !cached_bytes || !live_bytes) return STORM_ERR_INVALID_ARG;
+    device_pool().counters(mallocs, frees, cached_bytes, live_bytes);
     return STORM_OK;
 }
 
@@ -655,13 +738,14 @@ int storm_cuda_create(const StormProblemDesc *d, StormHandle **out) {
         return rc;
     };
     if (cudaSetDevice(h->device) != cudaSuccess) return fail(STORM_ERR_CUDA);
-    if (cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking) != cudaSuccess) return fail(STORM_ERR_CUDA);
-    cudaEventCreate(&h->evStart);
-    cudaEventCreate(&h->evTransport0);
-    cudaEventCreate(&h->evTransport1);
-    cudaEventCreate(&h->evEnd);
-    cudaEventCreate(&h->evAfterEmit);
-    cudaEventCreate(&h->evAfterComb);
+    {
+        StreamSet ss;
+        const bool ok = take_stream_set(h->device, ss);
+        h->stream = ss.stream;
+        h->evStart = ss.ev[0]; h->evTransport0 = ss.ev[1]; h->evTransport1 = ss.ev[2];
+        h->evEnd = ss.ev[3]; h->evAfterEmit = ss.ev[4]; h->evAfterComb = ss.ev[5];
+        if (!ok) return fail(STORM_ERR_CUDA);
+    }
 
     // Cartesian: the edges and centres; a polyhedral mesh: its box as one "cell" per axis
     const uint32_t ex = poly ? 1 : d->nx, ey = poly ? 1 : d->ny, ez = poly ? 1 : d->nz;
@@ -680,7 +764,12 @@ int storm_cuda_create(const StormProblemDesc *d, StormHandle **out) {
     for (uint32_t k = 0; k < ez; ++k) h->hzc[k] = 0.5 * (h->hze[k] + h->hze[k + 1]);
 
 #define ALLOC(ptr, n) do { if (dalloc(h, &(ptr), (n)) != cudaSuccess) return fail(STORM_ERR_OOM); } while (0)
-#define H2D(dst, src, n) do { if (cudaMemcpy((dst), (src), sizeof(*(dst)) * (n), cudaMemcpyHostToDevice) != cudaSuccess) return fail(STORM_ERR_CUDA); } while (0)
+// Every create-time transfer is ordered on the handle's own stream: the legacy
+// default stream is not ordered with it (it is created non-blocking).  Pageable
+// sources are staged before cudaMemcpyAsync returns; create ends with one
+// synchronisation of the stream.
+#define H2D(dst, src, n) do { if (cudaMemcpyAsync((dst), (src), sizeof(*(dst)) * (n), cudaMemcpyHostToDevice, h->stream) != cudaSuccess) return fail(STORM_ERR_CUDA); } while (0)
+#define ZERO(ptr, bytes) do { if (cudaMemsetAsync((ptr), 0, (bytes), h->stream) != cudaSuccess) return fail(STORM_ERR_CUDA); } while (0)
     ALLOC(h->xe, ex + 1); ALLOC(h->ye, ey + 1); ALLOC(h->ze, ez + 1);
     ALLOC(h->xc, ex); ALLOC(h->yc, ey); ALLOC(h->zc, ez);
     H2D(h->xe, h->hxe.data(), ex + 1); H2D(h->ye, h->hye.data(), ey + 1); H2D(h->ze, h->hze.data(), ez + 1);
@@ -774,12 +863,12 @@ int storm_cuda_create(const StormProblemDesc *d, StormHandle **out) {
     H2D(A.mass, d->mass, N);
     H2D(A.eint, d->internal_energy, N);
     H2D(A.ceint, d->cell_internal_energy ? d->cell_internal_energy : d->internal_energy, N);
-    if (cudaMemset(A.eradAvg, 0, N * sizeof(double)) != cudaSuccess) return fail(STORM_ERR_CUDA);
-    if (cudaMemset(A.eradCensus, 0, N * sizeof(double)) != cudaSuccess) return fail(STORM_ERR_CUDA);
-    if (cudaMemset(A.sigS, 0, N * sizeof(double)) != cudaSuccess) return fail(STORM_ERR_CUDA);
-    if (cudaMemset(A.rwElig, 0, N) != cudaSuccess) return fail(STORM_ERR_CUDA);
-    if (cudaMemset(A.photons, 0, N * sizeof(uint64_t)) != cudaSuccess) return fail(STORM_ERR_CUDA);
-    if (cudaMemset(h->segs, 0, N * sizeof(uint32_t)) != cudaSuccess) return fail(STORM_ERR_CUDA);
+    ZERO(A.eradAvg, N * sizeof(double));
+    ZERO(A.eradCensus, N * sizeof(double));
+    ZERO(A.sigS, N * sizeof(double));
+    ZERO(A.rwElig, N);
+    ZERO(A.photons, N * sizeof(uint64_t));
+    ZERO(h->segs, N * sizeof(uint32_t));
     std::vector<double> ones(N, 1.0);
     H2D(A.fleck, ones.data(), N);
 
@@ -827,14 +916,16 @@ int storm_cuda_create(const StormProblemDesc *d, StormHandle **out) {
     ALLOC(h->dStats, 1);
     ALLOC(h->dAmbiguous, 2);
     ALLOC(h->dErr, 4);
-    if (cudaMemset(h->dErr, 0, 4 * sizeof(int32_t)) != cudaSuccess) return fail(STORM_ERR_CUDA);
+    ZERO(h->dErr, 4 * sizeof(int32_t));
     h->K = d->segments_per_visit ? d->segments_per_visit : 16;
     {
-        cudaDeviceProp prop{};
-        cudaGetDeviceProperties(&prop, h->device);
+        // one attribute (cudaGetDeviceProperties queries them all and can take milliseconds)
+        int sms = 0;
+        if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, h->device) != cudaSuccess || sms <= 0)
+            return fail(STORM_ERR_CUDA);
         int nb = transport_blocks_per_sm(h->minBlocks, h->fp32);
-        h->transportGrid = static_cast<uint32_t>(prop.multiProcessorCount) * static_cast<uint32_t>(nb > 0 ? nb : 1) * 4;
-        h->smCount = prop.multiProcessorCount;
+        h->transportGrid = static_cast<uint32_t>(sms) * static_cast<uint32_t>(nb > 0 ? nb : 1) * 4;
+        h->smCount = sms;
     }
 
     Ctx &C = h->C;
@@ -873,7 +964,7 @@ int storm_cuda_create(const StormProblemDesc *d, StormHandle **out) {
             H2D(h->mgEp, ep.data(), G);
             H2D(h->mgEp32, ep32.data(), G);
         }
-        if (cudaMemset(A.pgrwCut, 0, N * sizeof(uint32_t)) != cudaSuccess) return fail(STORM_ERR_CUDA);
+        ZERO(A.pgrwCut, N * sizeof(uint32_t));
         C.groups = G;
         C.mgGroupConst = d->mg_group_constant;
         C.gb = h->gb;
@@ -937,8 +1028,10 @@ int storm_cuda_create(const StormProblemDesc *d, StormHandle **out) {
     h->desc.x_edges = h->desc.y_edges = h->desc.z_edges = nullptr;
     h->desc.temperature = h->desc.mass = h->desc.internal_energy = h->desc.cell_internal_energy = nullptr;
     h->desc.sigma_a = h->desc.sigma_s = h->desc.density_factor = nullptr;
+    if (cudaStreamSynchronize(h->stream) != cudaSuccess) return fail(STORM_ERR_CUDA);
 #undef ALLOC
 #undef H2D
+#undef ZERO
     *out = h;
     return STORM_OK;
 }
@@ -946,14 +1039,14 @@ int storm_cuda_create(const StormProblemDesc *d, StormHandle **out) {
 int storm_cuda_destroy(StormHandle *h) {
     if (!h) return STORM_OK;
     cudaSetDevice(h->device);
-    if (h->stream) cudaStreamSynchronize(h->stream);
+    const bool idle = !h->stream || cudaStreamSynchronize(h->stream) == cudaSuccess;
     bank_free(h, h->bankA, h->cap);
     bank_free(h, h->bankB, h->cap);
     free_rest(h, h->cap);
     void *ps[] = {h->xe, h->ye, h->ze, h->xc, h->yc, h->zc, h->A.T, h->A.mass, h->A.vol, h->A.eint, h->A.ceint,
                   h->A.sigA, h->A.sigS, h->A.fleck, h->A.rwSigT, h->A.eradAvg, h->A.eradCensus, h->A.emitE,
-                  h->A.rwElig, h->A.photons, h->A.phys, h->A.phys32, h->hx, h->hy, h->hz, h->segs, h->tabA, h->tabS, h->rhoF, h->rwTau, h->rwLogTau, h->rwSurv,
-                  h->rwRadius, h->rwLogTau32, h->rwSurv32, h->rwRadius32, h->fsCell, h->fsSide, h->fsOffset, h->dAmbiguous, h->offsets, h->tileSums, h->dTotalU64, h->dTotalE, h->combW, h->combWtot,
+                  h->A.rwElig, h->A.photons, h->A.phys, h->A.phys32, h->hx, h->hy, h->hz, h->segs, h->tabA, h->tabS, h->rhoF,
+                  h->fsCell, h->fsSide, h->fsOffset, h->dAmbiguous, h->offsets, h->tileSums, h->dTotalU64, h->dTotalE, h->combW, h->combWtot,
                   h->combStart, h->combCount, h->counts, h->dStats, h->dErr, h->gb, h->A.mgCdf, h->A.pgrw,
                   h->A.pgrwCut, h->gb32, h->gc32, h->faceCdf, h->mgEp, h->mgEp32, h->mgKTq, h->ddmc, h->ddmcTot,
                   h->ddmcRate, h->ddmcCut, h->ddmc32, h->stratBounds, h->stratBinW, h->stratStart,
@@ -961,11 +1054,20 @@ int storm_cuda_destroy(StormHandle *h) {
                   h->chord, h->cfN32};
     for (void *p : ps) device_pool().free(p);
     cudaEvent_t evs[] = {h->evStart, h->evTransport0, h->evTransport1, h->evEnd, h->evAfterEmit, h->evAfterComb};
-    for (cudaEvent_t e : evs)
-        if (e) cudaEventDestroy(e);
+    bool complete = h->stream != nullptr;
+    for (cudaEvent_t e : evs) complete = complete && e;
+    if (idle && complete) {
+        StreamSet ss;
+        ss.stream = h->stream;
+        for (int q = 0; q < 6; ++q) ss.ev[q] = evs[q];
+        return_stream_set(h->device, ss);
+    } else {
+        for (cudaEvent_t e : evs)
+            if (e) cudaEventDestroy(e);
+        if (h->stream) cudaStreamDestroy(h->stream);
+    }
     for (cudaEvent_t e : h->evPool)
         if (e) cudaEventDestroy(e);
-    if (h->stream) cudaStreamDestroy(h->stream);
     delete h;
     return STORM_OK;
 }
@@ -1704,7 +1806,8 @@ int storm_cuda_replay_segments(StormHandle *h, StormReplayBatch *b) {
         void *p = nullptr;
         if (cudaMalloc(&p, bytes ? bytes : 8) != cudaSuccess) return nullptr;
         owned.push_back(p);
-        if (src && bytes) cudaMemcpy(p, src, bytes, cudaMemcpyHostToDevice);
+        // ordered on the handle's stream, before the replay kernel that reads it
+        if (src && bytes) cudaMemcpyAsync(p, src, bytes, cudaMemcpyHostToDevice, h->stream);
         return p;
     };
     ReplayDev R{};
@@ -1775,9 +1878,9 @@ int storm_cuda_random_walk_sample(StormHandle *h, uint64_t n, const double *xiLe
     CK(cudaStreamSynchronize(h->stream));
     double *d[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
     for (int q = 0; q < 5; ++q) CK(cudaMalloc(&d[q], n * sizeof(double)));
-    if (xiLeak) CK(cudaMemcpy(d[0], xiLeak, n * sizeof(double), cudaMemcpyHostToDevice));
-    if (tau) CK(cudaMemcpy(d[1], tau, n * sizeof(double), cudaMemcpyHostToDevice));
-    if (xiRad) CK(cudaMemcpy(d[2], xiRad, n * sizeof(double), cudaMemcpyHostToDevice));
+    if (xiLeak) CK(cudaMemcpyAsync(d[0], xiLeak, n * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+    if (tau) CK(cudaMemcpyAsync(d[1], tau, n * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+    if (xiRad) CK(cudaMemcpyAsync(d[2], xiRad, n * sizeof(double), cudaMemcpyHostToDevice, h->stream));
     launch_rw_sample(h->stream, h->C.rw, static_cast<uint32_t>(n), xiLeak ? d[0] : nullptr, tau ? d[1] : nullptr,
                      xiRad ? d[2] : nullptr, d[3], d[4]);
     ++h->launches;

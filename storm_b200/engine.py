@@ -65,6 +65,8 @@ def lib():
         L.storm_cuda_set_transport_variant.argtypes = [vp, C.c_int, C.c_int]
         L.storm_cuda_set_transport_mode.argtypes = [vp, C.c_int, C.c_uint32]
         L.storm_cuda_transport_timing.argtypes = [vp, dp, u64p, u64p, C.c_int]
+        L.storm_cuda_release_cached.argtypes = [C.c_int, u64p]
+        L.storm_cuda_pool_counters.argtypes = [u64p, u64p, u64p, u64p]
         L.storm_server_create.argtypes = [C.POINTER(A.StormServerConfig), C.POINTER(vp)]
         L.storm_server_submit.argtypes = [vp, C.POINTER(A.StormProblemDesc), C.c_uint32, C.c_double, dp, u64p]
         L.storm_server_poll.argtypes = [vp, C.POINTER(A.StormRequestResult), C.c_uint32, C.POINTER(C.c_uint32)]
@@ -76,6 +78,23 @@ def lib():
         L.storm_cuda_abi_version.restype = C.c_int
         _lib = L
     return _lib
+
+
+def pool_counters():
+    """The device memory cache's counters: cudaMalloc and cudaFree calls since
+    the library loaded, bytes cached and bytes handed out."""
+    v = [C.c_uint64() for _ in range(4)]
+    lib().storm_cuda_pool_counters(*[C.byref(x) for x in v])
+    return dict(zip(("mallocs", "frees", "cached_bytes", "live_bytes"), (x.value for x in v)))
+
+
+def release_cached(device=0):
+    """Return the device memory cache's blocks on `device` to the driver; the bytes released."""
+    b = C.c_uint64()
+    rc = lib().storm_cuda_release_cached(device, C.byref(b))
+    if rc != A.STORM_OK:
+        raise StormError(rc, lib().storm_cuda_status_string(rc).decode())
+    return b.value
 
 
 class Particles:
