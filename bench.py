@@ -57,8 +57,8 @@ def parse():
     ap.add_argument("--voronoi-packets", type=float, default=2e7, help="packets per step of the Voronoi-mesh run")
     ap.add_argument("--mg-n", type=int, default=128)
     ap.add_argument("--serving-requests", type=int, default=32, help="requests in the serving run (0 = skip it)")
-    ap.add_argument("--serving-slots", type=int, default=12)
-    ap.add_argument("--serving-workers", type=int, default=6)
+    ap.add_argument("--serving-slots", type=int, default=6)
+    ap.add_argument("--serving-workers", type=int, default=3)
     return ap.parse_args()
 
 
@@ -432,7 +432,9 @@ def serving_run(args):
     through the serving loop, against the same requests one at a time.  The
     concurrent run receives the requests as a Poisson stream at 4x the rate the
     one-at-a-time server completes them.  One untimed pass first fills the
-    engine's device memory cache, as a long-running server's would be."""
+    engine's device memory cache, as a long-running server's would be.  Both
+    arms run three times, alternating; each reports its median run (by wall
+    time) and the ratios are taken between the medians."""
     import numpy as np
     from storm_b200 import problems
     from storm_b200.engine import Server
@@ -456,12 +458,22 @@ def serving_run(args):
                 "queued_ms_max": max((r["queued_ms"] for r in res), default=0.0),
                 "peak_device_gb": st["peak_device_bytes"] / 1e9, "slots": slots, "workers": workers}
 
+    def median_run(runs):
+        runs = sorted(runs, key=lambda r: r["wall_s"])
+        out = dict(runs[len(runs) // 2])
+        out["wall_s_runs"] = [round(r["wall_s"], 4) for r in runs]
+        return out
+
     run(args.serving_slots, args.serving_workers, [0.0] * len(mix))   # warm the device memory cache
-    alone = run(1, 1, [0.0] * len(mix))
+    alone_runs = [run(1, 1, [0.0] * len(mix))]
     rng = np.random.default_rng(12)
-    mean_gap = alone["wall_s"] / len(mix) / 4.0
+    mean_gap = alone_runs[0]["wall_s"] / len(mix) / 4.0
     gaps = [0.0] + list(rng.exponential(mean_gap, len(mix) - 1))
-    mixed = run(args.serving_slots, args.serving_workers, gaps)
+    mixed_runs = [run(args.serving_slots, args.serving_workers, gaps)]
+    for _ in range(2):
+        alone_runs.append(run(1, 1, [0.0] * len(mix)))
+        mixed_runs.append(run(args.serving_slots, args.serving_workers, gaps))
+    alone, mixed = median_run(alone_runs), median_run(mixed_runs)
     return {"requests": len(mix), "form": "fp32-track",
             "mix": "uniform cubes, N log-uniform [16,48], packets/step log-uniform [1e4,1e6], "
                    "kappa uniform [0.1,1000] 1/cm, 5-20 steps, seeded",

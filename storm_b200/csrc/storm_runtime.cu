@@ -9,6 +9,7 @@
 #include <cstring>
 #include <map>
 #include <mutex>
+#include <set>
 #include <string>
 #include <unordered_map>
 #include <vector>
@@ -86,6 +87,7 @@ struct StormHandle {
     uint32_t *pCount = nullptr;      // comb: copies per sorted particle
     double *pWeight = nullptr;       // comb: weight of those copies
     uint64_t *pOff = nullptr, *pTiles = nullptr;   // comb: output positions, scan tile sums
+    size_t restBytes = 0;            // the block holding bankC.rec through pTiles
     int32_t *dAmbiguous = nullptr;
     // scratch
     uint64_t *offsets = nullptr, *tileSums = nullptr, *dTotalU64 = nullptr;
@@ -142,11 +144,16 @@ int cuda_fail(StormHandle *h, cudaError_t e, const char *what) {
 // request would stall every other problem on the GPU; blocks return here
 // instead and are handed to the next allocation of about the same size
 // (at most 25% larger) on the same device.  A handle frees only after its own
-// stream is idle, so a reused block has no work in flight.  When cudaMalloc
-// runs out of memory the device's cached blocks are released and it retries.
+// stream is idle, so a reused block has no work in flight.
+// A miss allocates stream-ordered (cudaMallocAsync on the asking handle's
+// stream, from the device's default pool with its release threshold raised so
+// it keeps what it maps): plain cudaMalloc, called while other handles'
+// kernels ran, was measured to stall for up to hundreds of milliseconds.  When
+// the allocation runs out of memory the device's cached blocks are released
+// and it retries.
 class DevicePool {
 public:
-    cudaError_t alloc(void **p, size_t bytes) {
+    cudaError_t alloc(void **p, size_t bytes, cudaStream_t stream) {
         const size_t want = round_up(bytes);
         int dev = 0;
         cudaGetDevice(&dev);
@@ -161,11 +168,12 @@ public:
                 return cudaSuccess;
             }
         }
-        cudaError_t e = cudaMalloc(p, want);
+        keep_mapped(dev);
+        cudaError_t e = cudaMallocAsync(p, want, stream);
         if (e == cudaErrorMemoryAllocation) {
             cudaGetLastError();
             release(dev);
-            e = cudaMalloc(p, want);
+            e = cudaMallocAsync(p, want, stream);
         }
         if (e != cudaSuccess) return e;
         std::lock_guard<std::mutex> lk(m_);
@@ -220,6 +228,18 @@ public:
     }
 
 private:
+    // the default pool of `dev` keeps the memory it has mapped (its release
+    // threshold is 0 by default, which returns memory at every synchronisation)
+    void keep_mapped(int dev) {
+        std::lock_guard<std::mutex> lk(m_);
+        if (pools_.count(dev)) return;
+        cudaMemPool_t mp;
+        if (cudaDeviceGetDefaultMemPool(&mp, dev) == cudaSuccess) {
+            uint64_t threshold = ~0ull;
+            cudaMemPoolSetAttribute(mp, cudaMemPoolAttrReleaseThreshold, &threshold);
+        }
+        pools_.insert(dev);
+    }
     static size_t round_up(size_t bytes) {
         if (bytes <= (1u << 20)) {
             size_t b = 512;
@@ -234,6 +254,7 @@ private:
     std::multimap<std::pair<int, size_t>, void *> free_;
     size_t cached_ = 0;
     uint64_t mallocs_ = 0, frees_ = 0;
+    std::set<int> pools_;
 };
 
 DevicePool &device_pool() {
@@ -279,7 +300,7 @@ void return_stream_set(int dev, const StreamSet &s) {
 template <class T>
 cudaError_t dalloc(StormHandle *h, T **p, size_t n) {
     size_t bytes = sizeof(T) * (n ? n : 1);
-    cudaError_t e = device_pool().alloc(reinterpret_cast<void **>(p), bytes);
+    cudaError_t e = device_pool().alloc(reinterpret_cast<void **>(p), bytes, h->stream);
     if (e == cudaSuccess) h->memBytes += bytes;
     return e;
 }
@@ -292,28 +313,40 @@ void dfree(StormHandle *h, T *&p, size_t n) {
     }
 }
 
+// A bank's fields live in one device block (one allocation instead of twelve),
+// each field on a 256-byte boundary; b.x is the block's start.
+size_t align256(size_t bytes) { return (bytes + 255) / 256 * 256; }
+size_t bank_bytes(const StormHandle *h, size_t n) {
+    const size_t d = align256(n * sizeof(double)), u = align256(n * sizeof(uint32_t));
+    return (h->desc.groups >= 2 ? 10 : 9) * d + 3 * u;
+}
 cudaError_t bank_alloc(StormHandle *h, Bank &b, size_t n) {
-    double **d[] = {&b.x, &b.y, &b.z, &b.vx, &b.vy, &b.vz, &b.t, &b.w, &b.w0};
-    for (double **q : d) {
-        cudaError_t e = dalloc(h, q, n);
-        if (e != cudaSuccess) return e;
+    unsigned char *base = nullptr;
+    cudaError_t e = dalloc(h, &base, bank_bytes(h, n));
+    if (e != cudaSuccess) return e;
+    const size_t d = align256(n * sizeof(double)), u = align256(n * sizeof(uint32_t));
+    size_t off = 0;
+    double **dd[] = {&b.x, &b.y, &b.z, &b.vx, &b.vy, &b.vz, &b.t, &b.w, &b.w0};
+    for (double **q : dd) {
+        *q = reinterpret_cast<double *>(base + off);
+        off += d;
     }
+    b.nu = nullptr;
     if (h->desc.groups >= 2) {
-        cudaError_t e = dalloc(h, &b.nu, n);
-        if (e != cudaSuccess) return e;
+        b.nu = reinterpret_cast<double *>(base + off);
+        off += d;
     }
-    uint32_t **u[] = {&b.cell, &b.pid, &b.draw};
-    for (uint32_t **q : u) {
-        cudaError_t e = dalloc(h, q, n);
-        if (e != cudaSuccess) return e;
+    uint32_t **uu[] = {&b.cell, &b.pid, &b.draw};
+    for (uint32_t **q : uu) {
+        *q = reinterpret_cast<uint32_t *>(base + off);
+        off += u;
     }
     return cudaSuccess;
 }
 void bank_free(StormHandle *h, Bank &b, size_t n) {
-    double **d[] = {&b.x, &b.y, &b.z, &b.vx, &b.vy, &b.vz, &b.t, &b.w, &b.w0, &b.nu};
-    for (double **q : d) dfree(h, *q, n);
-    uint32_t **u[] = {&b.cell, &b.pid, &b.draw};
-    for (uint32_t **q : u) dfree(h, *q, n);
+    unsigned char *base = reinterpret_cast<unsigned char *>(b.x);
+    dfree(h, base, bank_bytes(h, n));
+    b = Bank{};
 }
 cudaError_t bank_copy(cudaStream_t s, const Bank &dst, const Bank &src, size_t n) {
     if (!n) return cudaSuccess;
@@ -339,29 +372,43 @@ cudaError_t bank_copy(cudaStream_t s, const Bank &dst, const Bank &src, size_t n
 // Buffers sized by particle capacity, other than the transport banks A and B.
 size_t census_words(const StormHandle *h) { return h->fp32 ? 4 : 6; }   // uint4 per record
 
+// The census records and the comb's sort and plan buffers: one device block,
+// each array on a 256-byte boundary, the census records first.
 cudaError_t alloc_rest(StormHandle *h, size_t nc) {
-    cudaError_t e;
-    if ((e = dalloc(h, &h->bankC.rec, nc * census_words(h))) != cudaSuccess) return e;
-    if ((e = dalloc(h, &h->keys, nc)) != cudaSuccess) return e;
-    if ((e = dalloc(h, &h->keysAlt, nc)) != cudaSuccess) return e;
-    if ((e = dalloc(h, &h->vals, nc)) != cudaSuccess) return e;
-    if ((e = dalloc(h, &h->valsAlt, nc)) != cudaSuccess) return e;
     h->tileHistLen = radix_scratch_words(static_cast<uint32_t>(nc));
-    if ((e = dalloc(h, &h->tileHist, h->tileHistLen)) != cudaSuccess) return e;
-    if ((e = dalloc(h, &h->pCount, nc)) != cudaSuccess) return e;
-    if ((e = dalloc(h, &h->pWeight, nc)) != cudaSuccess) return e;
-    if ((e = dalloc(h, &h->pOff, nc + 1)) != cudaSuccess) return e;
-    return dalloc(h, &h->pTiles, nc / 1024 + 4);
+    void **ptrs[] = {reinterpret_cast<void **>(&h->bankC.rec), reinterpret_cast<void **>(&h->keys),
+                     reinterpret_cast<void **>(&h->keysAlt), reinterpret_cast<void **>(&h->vals),
+                     reinterpret_cast<void **>(&h->valsAlt), reinterpret_cast<void **>(&h->tileHist),
+                     reinterpret_cast<void **>(&h->pCount), reinterpret_cast<void **>(&h->pWeight),
+                     reinterpret_cast<void **>(&h->pOff), reinterpret_cast<void **>(&h->pTiles)};
+    const size_t bytes[] = {nc * census_words(h) * sizeof(uint4), nc * sizeof(uint64_t), nc * sizeof(uint64_t),
+                            nc * sizeof(uint32_t), nc * sizeof(uint32_t), h->tileHistLen * sizeof(*h->tileHist),
+                            nc * sizeof(uint32_t), nc * sizeof(double), (nc + 1) * sizeof(uint64_t),
+                            (nc / 1024 + 4) * sizeof(uint64_t)};
+    size_t total = 0;
+    for (size_t b : bytes) total += align256(b);
+    unsigned char *base = nullptr;
+    cudaError_t e = dalloc(h, &base, total);
+    if (e != cudaSuccess) return e;
+    h->restBytes = total;
+    size_t off = 0;
+    for (int q = 0; q < 10; ++q) {
+        *ptrs[q] = base + off;
+        off += align256(bytes[q]);
+    }
+    return cudaSuccess;
 }
-void free_rest(StormHandle *h, size_t nc) {
-    dfree(h, h->bankC.rec, nc * census_words(h));
-    dfree(h, h->keys, nc); dfree(h, h->keysAlt, nc);
-    dfree(h, h->vals, nc); dfree(h, h->valsAlt, nc);
-    dfree(h, h->tileHist, h->tileHistLen);
-    dfree(h, h->pCount, nc);
-    dfree(h, h->pWeight, nc);
-    dfree(h, h->pOff, nc + 1);
-    dfree(h, h->pTiles, nc / 1024 + 4);
+void free_rest(StormHandle *h, size_t) {
+    unsigned char *base = reinterpret_cast<unsigned char *>(h->bankC.rec);
+    dfree(h, base, h->restBytes);
+    h->restBytes = 0;
+    h->bankC.rec = nullptr;
+    h->keys = h->keysAlt = nullptr;
+    h->vals = h->valsAlt = nullptr;
+    h->tileHist = nullptr;
+    h->pCount = nullptr;
+    h->pWeight = nullptr;
+    h->pOff = h->pTiles = nullptr;
 }
 
 // (Re)allocate every per-particle buffer for capacity n, keeping the first
