@@ -1590,6 +1590,165 @@ __global__ void __launch_bounds__(RS_THREADS) k_rs_scatter(const uint64_t *kin, 
     }
 }
 
+// ------------------------------------------------------------------ bucket sort of the comb keys
+// The comb's keys are (run << pidBits) | hash, the hash a keyed bijection of
+// the pid, so the keys of one run are distinct and their sorted order is
+// unique.  Instead of an LSD radix sort over all run and pid bits, the keys are
+// counted per run, placed in their run's range in arrival order (atomics), and
+// each run is then sorted on its own in shared memory (bitonic).  The result
+// is the radix sort's.  A run longer than BUCKET_BLOCK_MAX keys raises a flag,
+// and the caller falls back to the radix sort.
+
+constexpr uint32_t BUCKET_WARP_MAX = 512;     // runs up to this length: one warp, 4 KB of shared memory
+constexpr uint32_t BUCKET_BLOCK_MAX = 8192;   // longer runs up to this length: one block of 256, 64 KB
+constexpr int BUCKET_WARPS = 8;
+
+// keys of run nRuns (zero weight, outside the mesh) and any run index beyond it share the last bucket
+__device__ __forceinline__ uint32_t bucket_run(uint64_t key, int pidBits, uint32_t nRuns) {
+    const uint64_t r = key >> pidBits;
+    return r < nRuns ? static_cast<uint32_t>(r) : nRuns;
+}
+
+// count[r] += keys in run r, r in [0, nRuns]; lanes of a warp with equal runs add once
+__global__ void k_bucket_count(const uint64_t *keys, uint32_t n, int pidBits, uint32_t nRuns, uint32_t *count) {
+    const unsigned lane = threadIdx.x & 31;
+    for (uint32_t base = blockIdx.x * blockDim.x; base < n; base += gridDim.x * blockDim.x) {
+        const uint32_t q = base + threadIdx.x;
+        const bool ok = q < n;
+        const uint32_t run = ok ? bucket_run(keys[q], pidBits, nRuns) : 0xFFFFFFFFu;
+        const unsigned m = __match_any_sync(FULL, run);
+        if (ok && static_cast<unsigned>(__ffs(m) - 1) == lane) atomicAdd(&count[run], static_cast<uint32_t>(__popc(m)));
+    }
+}
+
+// (key, q) to the next free slot of its run's range: cursor[r] starts at the run's first position
+__global__ void k_bucket_place(const uint64_t *keys, uint32_t n, int pidBits, uint32_t nRuns, uint32_t *cursor,
+                               uint64_t *outKeys, uint32_t *outVals) {
+    const unsigned lane = threadIdx.x & 31;
+    const unsigned lt = lanemask_lt();
+    for (uint32_t base = blockIdx.x * blockDim.x; base < n; base += gridDim.x * blockDim.x) {
+        const uint32_t q = base + threadIdx.x;
+        const bool ok = q < n;
+        const uint64_t k = ok ? keys[q] : 0ull;
+        const uint32_t run = ok ? bucket_run(k, pidBits, nRuns) : 0xFFFFFFFFu;
+        const unsigned m = __match_any_sync(FULL, run);
+        const int leader = __ffs(m) - 1;
+        uint32_t b = 0;
+        if (ok && static_cast<int>(lane) == leader) b = atomicAdd(&cursor[run], static_cast<uint32_t>(__popc(m)));
+        b = __shfl_sync(FULL, b, leader);
+        if (ok) {
+            const uint32_t slot = b + static_cast<uint32_t>(__popc(m & lt));
+            outKeys[slot] = k;
+            outVals[slot] = q;
+        }
+    }
+}
+
+// Ascending bitonic sort of s[0, P), P a power of two >= 2, by `threads`
+// threads numbered t; `sync` orders the stages.  Each stage's pairs (i, i ^ j)
+// are disjoint, and only the lower index of a pair touches it.
+template <class Sync>
+__device__ __forceinline__ void bitonic_sort(uint64_t *s, uint32_t P, uint32_t t, uint32_t threads, Sync sync) {
+    for (uint32_t k = 2; k <= P; k <<= 1)
+        for (uint32_t j = k >> 1; j > 0; j >>= 1) {
+            for (uint32_t i = t; i < P; i += threads) {
+                const uint32_t l = i ^ j;
+                if (l > i) {
+                    const uint64_t a = s[i], c = s[l];
+                    if ((a > c) == ((i & k) == 0)) {
+                        s[i] = c;
+                        s[l] = a;
+                    }
+                }
+            }
+            sync();
+        }
+}
+
+struct WarpSync {
+    __device__ void operator()() const { __syncwarp(); }
+};
+struct BlockSync {
+    __device__ void operator()() const { __syncthreads(); }
+};
+
+// Within a run the key's run bits are fixed, so (hash << 32) | q orders the
+// pairs by key; q < 2^32 - 1 and hash < 2^32 keep ~0 above every pair (padding).
+__device__ __forceinline__ uint64_t bucket_pack(uint64_t key, uint32_t q, uint64_t hashMask) {
+    return ((key & hashMask) << 32) | q;
+}
+
+// Runs 0..nRuns-1 of (keys, vals), each sorted in place by key: one warp per
+// run of up to BUCKET_WARP_MAX keys; longer runs are listed for k_bucket_sort_long.
+__global__ void __launch_bounds__(32 * BUCKET_WARPS) k_bucket_sort_runs(uint64_t *keys, uint32_t *vals,
+                                                                        const uint32_t *start, uint32_t nRuns,
+                                                                        int pidBits, uint32_t *longRuns,
+                                                                        uint32_t *nLong, uint32_t longCap) {
+    __shared__ uint64_t sm[BUCKET_WARPS][BUCKET_WARP_MAX];
+    const uint32_t lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    uint64_t *sw = sm[wid];
+    const uint64_t hashMask = (1ull << pidBits) - 1ull;   // pidBits <= 32
+    const uint32_t warps = gridDim.x * BUCKET_WARPS;
+    for (uint32_t r = blockIdx.x * BUCKET_WARPS + wid; r < nRuns; r += warps) {
+        const uint32_t b = start[r], len = start[r + 1] - b;
+        if (len < 2) continue;
+        if (len > BUCKET_WARP_MAX) {
+            if (lane == 0) {
+                const uint32_t slot = atomicAdd(nLong, 1u);
+                if (slot < longCap) longRuns[slot] = r;
+            }
+            continue;
+        }
+        uint32_t P = 32;
+        while (P < len) P <<= 1;
+        for (uint32_t i = lane; i < P; i += 32) sw[i] = i < len ? bucket_pack(keys[b + i], vals[b + i], hashMask) : ~0ull;
+        __syncwarp();
+        bitonic_sort(sw, P, lane, 32u, WarpSync{});
+        for (uint32_t i = lane; i < len; i += 32) {
+            const uint64_t v = sw[i];
+            keys[b + i] = (static_cast<uint64_t>(r) << pidBits) | (v >> 32);
+            vals[b + i] = static_cast<uint32_t>(v);
+        }
+        __syncwarp();
+    }
+}
+
+// The listed runs, one block each (dynamic shared memory: BUCKET_BLOCK_MAX words).
+// A run longer than BUCKET_BLOCK_MAX, or more listed runs than longCap, sets *tooLong.
+__global__ void __launch_bounds__(256) k_bucket_sort_long(uint64_t *keys, uint32_t *vals, const uint32_t *start,
+                                                          int pidBits, const uint32_t *longRuns,
+                                                          const uint32_t *nLong, uint32_t longCap,
+                                                          uint32_t *tooLong) {
+    extern __shared__ __align__(16) unsigned char bucketMem[];
+    uint64_t *sb = reinterpret_cast<uint64_t *>(bucketMem);
+    const uint32_t listed = *nLong;
+    if (listed > longCap) {
+        if (blockIdx.x == 0 && threadIdx.x == 0) *tooLong = 1u;
+        return;
+    }
+    const uint64_t hashMask = (1ull << pidBits) - 1ull;
+    for (uint32_t e = blockIdx.x; e < listed; e += gridDim.x) {
+        const uint32_t r = longRuns[e];
+        const uint32_t b = start[r], len = start[r + 1] - b;
+        if (len > BUCKET_BLOCK_MAX) {
+            if (threadIdx.x == 0) *tooLong = 1u;
+            continue;
+        }
+        uint32_t P = 32;
+        while (P < len) P <<= 1;
+        for (uint32_t i = threadIdx.x; i < P; i += blockDim.x)
+            sb[i] = i < len ? bucket_pack(keys[b + i], vals[b + i], hashMask) : ~0ull;
+        __syncthreads();
+        bitonic_sort(sb, P, threadIdx.x, blockDim.x, BlockSync{});
+        for (uint32_t i = threadIdx.x; i < len; i += blockDim.x) {
+            const uint64_t v = sb[i];
+            keys[b + i] = (static_cast<uint64_t>(r) << pidBits) | (v >> 32);
+            vals[b + i] = static_cast<uint32_t>(v);
+        }
+        __syncthreads();
+    }
+}
+
 // first sorted position of each cell (lower_bound of cell << pidBits), cells 0..N
 __global__ void k_comb_ranges(const uint64_t *keys, uint32_t n, uint32_t ncells, uint32_t *start, int pidBits) {
     for (uint32_t c = blockIdx.x * blockDim.x + threadIdx.x; c <= ncells; c += gridDim.x * blockDim.x) {
@@ -2289,6 +2448,35 @@ int launch_radix_sort(cudaStream_t s, uint64_t *keys, uint32_t *vals, uint64_t *
     }
     return passes & 1;
 }
+// Bucket sort of the comb keys (see k_bucket_count).  `start` receives the
+// first position of every run 0..nRuns (start[nRuns]: the first key outside
+// every run); `cursor` is scratch of nRuns + 1 words and `scanSums` of
+// bucket_scan_words(nRuns + 1).  The sorted pairs end in (outKeys, outVals).
+// Long runs are listed in longRuns (longCap entries); flags[0] counts them and
+// flags[1] is set when a run is too long for this sort (then nothing is sorted
+// and the caller falls back to launch_radix_sort).
+void launch_bucket_sort(cudaStream_t s, const uint64_t *keys, uint32_t n, int pidBits, uint32_t nRuns, uint32_t *start,
+                        uint32_t *cursor, uint64_t *scanSums, uint64_t *outKeys, uint32_t *outVals,
+                        uint32_t *longRuns, uint32_t longCap, uint32_t *flags) {
+    const uint32_t len = nRuns + 1;
+    cudaMemsetAsync(start, 0, sizeof(uint32_t) * len, s);
+    cudaMemsetAsync(flags, 0, 2 * sizeof(uint32_t), s);
+    k_bucket_count<<<grid_for(n, 256, 148 * 16), 256, 0, s>>>(keys, n, pidBits, nRuns, start);
+    const uint32_t stiles = (len + 1023) / 1024;
+    k_scan32_tiles<<<stiles, 1024, 0, s>>>(start, len, scanSums);
+    k_scan_sums<<<1, 1024, 0, s>>>(scanSums, stiles, scanSums + stiles);
+    k_scan32_add<<<stiles, 1024, 0, s>>>(start, len, scanSums);
+    cudaMemcpyAsync(cursor, start, sizeof(uint32_t) * len, cudaMemcpyDeviceToDevice, s);
+    k_bucket_place<<<grid_for(n, 256, 148 * 16), 256, 0, s>>>(keys, n, pidBits, nRuns, cursor, outKeys, outVals);
+    k_bucket_sort_runs<<<grid_for(nRuns, BUCKET_WARPS, 148 * 32), 32 * BUCKET_WARPS, 0, s>>>(
+        outKeys, outVals, start, nRuns, pidBits, longRuns, flags, longCap);
+    const size_t smem = sizeof(uint64_t) * BUCKET_BLOCK_MAX;
+    cudaFuncSetAttribute(k_bucket_sort_long, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
+    k_bucket_sort_long<<<148, 256, smem, s>>>(outKeys, outVals, start, pidBits, longRuns, flags, longCap, flags + 1);
+}
+size_t bucket_scan_words(uint32_t len) { return (len + 1023) / 1024 + 2; }
+uint32_t bucket_long_capacity(uint32_t n) { return n / (BUCKET_WARP_MAX + 1) + 1; }
+
 uint32_t radix_tile_count(uint32_t n) { return (n + RS_TILE - 1) / RS_TILE ? (n + RS_TILE - 1) / RS_TILE : 1; }
 // 32-bit words the radix sort needs for its tile histogram and the scan's tile sums
 size_t radix_scratch_words(uint32_t n) {

@@ -88,6 +88,11 @@ struct StormHandle {
     double *pWeight = nullptr;       // comb: weight of those copies
     uint64_t *pOff = nullptr, *pTiles = nullptr;   // comb: output positions, scan tile sums
     size_t restBytes = 0;            // the block holding bankC.rec through pTiles
+    // comb bucket sort scratch, grown on demand: run cursors and scan sums for
+    // runLen runs, the list of long runs, and its two flags
+    uint32_t *runCursor = nullptr, *longRuns = nullptr, *bucketFlags = nullptr;
+    uint64_t *runScan = nullptr;
+    size_t runLen = 0, longCap = 0;
     int32_t *dAmbiguous = nullptr;
     // scratch
     uint64_t *offsets = nullptr, *tileSums = nullptr, *dTotalU64 = nullptr;
@@ -1097,6 +1102,7 @@ int storm_cuda_destroy(StormHandle *h) {
                   h->combStart, h->combCount, h->counts, h->dStats, h->dErr, h->gb, h->A.mgCdf, h->A.pgrw,
                   h->A.pgrwCut, h->gb32, h->gc32, h->faceCdf, h->mgEp, h->mgEp32, h->mgKTq, h->ddmc, h->ddmcTot,
                   h->ddmcRate, h->ddmcCut, h->ddmc32, h->stratBounds, h->stratBinW, h->stratStart,
+                  h->runCursor, h->runScan, h->longRuns, h->bucketFlags,
                   h->cfo, h->cfN, h->cfP, h->cfNext, h->cfFace, h->mpx, h->mpy, h->mpz, h->fvo, h->fvi, h->vtx,
                   h->chord, h->cfN32};
     for (void *p : ps) device_pool().free(p);
@@ -1372,13 +1378,54 @@ int storm_cuda_phase_comb(StormHandle *h) {
     else launch_comb_keys(h->stream, h->C, h->bankC, n, h->keys, h->vals, combKey, pidBits);
     int cellBits = 0;
     while ((1ull << cellBits) <= nRuns) ++cellBits;
-    int alt = launch_radix_sort(h->stream, h->keys, h->vals, h->keysAlt, h->valsAlt, n, pidBits + cellBits, h->tileHist);
-    const uint64_t *skeys = alt ? h->keysAlt : h->keys;
-    const uint32_t *idx = alt ? h->valsAlt : h->vals;
-    const int passes = (pidBits + cellBits + 7) / 8;
+    // The bucket sort (per-run counting sort, then each run sorted in shared
+    // memory) and the radix sort give the same order; the radix sort is the
+    // fallback for runs too long for the bucket sort.
+    const uint64_t *skeys = nullptr;
+    const uint32_t *idx = nullptr;
+    uint32_t nValid = 0;
+    bool haveValid = false;
+    if (nRuns + 1 < 0xFFFFFFF0ull) {
+        const size_t len = nRuns + 1;
+        if (len > h->runLen) {
+            dfree(h, h->runCursor, h->runLen);
+            dfree(h, h->runScan, bucket_scan_words(static_cast<uint32_t>(h->runLen)));
+            CK(dalloc(h, &h->runCursor, len));
+            CK(dalloc(h, &h->runScan, bucket_scan_words(static_cast<uint32_t>(len))));
+            h->runLen = len;
+        }
+        const size_t longNeed = bucket_long_capacity(n);
+        if (longNeed > h->longCap) {
+            dfree(h, h->longRuns, h->longCap);
+            CK(dalloc(h, &h->longRuns, longNeed));
+            h->longCap = longNeed;
+        }
+        if (!h->bucketFlags) CK(dalloc(h, &h->bucketFlags, 2));
+        launch_bucket_sort(h->stream, h->keys, n, pidBits, static_cast<uint32_t>(nRuns), start, h->runCursor,
+                           h->runScan, h->keysAlt, h->valsAlt, h->longRuns, static_cast<uint32_t>(h->longCap),
+                           h->bucketFlags);
+        h->launches += 7;
+        CK(cudaGetLastError());
+        uint32_t flags[2] = {0, 0};
+        CK(cudaMemcpyAsync(flags, h->bucketFlags, sizeof(flags), cudaMemcpyDeviceToHost, h->stream));
+        int rc = read_checked(h, &nValid, start + nRuns, sizeof(uint32_t));
+        if (rc != STORM_OK) return rc;
+        if (flags[1] == 0) {
+            skeys = h->keysAlt;
+            idx = h->valsAlt;
+            haveValid = true;
+        }
+    }
+    if (!haveValid) {
+        const int alt = launch_radix_sort(h->stream, h->keys, h->vals, h->keysAlt, h->valsAlt, n, pidBits + cellBits,
+                                          h->tileHist);
+        skeys = alt ? h->keysAlt : h->keys;
+        idx = alt ? h->valsAlt : h->vals;
+        launch_comb_ranges(h->stream, skeys, n, static_cast<uint32_t>(nRuns), start, pidBits);
+        h->launches += 5 * ((pidBits + cellBits + 7) / 8) + 1;
+    }
     // census weights in sorted order; the plan overwrites each slot with the copies' weight
     double *wS = h->pWeight;
-    launch_comb_ranges(h->stream, skeys, n, static_cast<uint32_t>(nRuns), start, pidBits);
     launch_sorted_weights(h->stream, h->C, h->bankC, idx, n, wS);
     if (strat) launch_strat_sums(h->stream, wS, start, N, B, h->stratBinW, h->combW);
     else launch_comb_cell_sums(h->stream, wS, start, N, h->combW);
@@ -1392,12 +1439,13 @@ int storm_cuda_phase_comb(StormHandle *h) {
     else
         launch_comb_plan(h->stream, h->C, P, wS, start, h->combW, h->combWtot, h->pCount, h->pWeight,
                          h->combCount, h->A.eradCensus, h->dStats);
-    h->launches += 1 + 5 * passes + 5;
+    h->launches += 1 + 4;
     CK(cudaGetLastError());
-    uint32_t nValid = 0;
-    int rc = read_checked(h, &nValid, start + nRuns, sizeof(uint32_t));
-    if (rc != STORM_OK) return rc;
-    uint64_t *countU64 = alt ? h->keys : h->keysAlt;   // the sort's spare key buffer
+    if (!haveValid) {
+        int rc = read_checked(h, &nValid, start + nRuns, sizeof(uint32_t));
+        if (rc != STORM_OK) return rc;
+    }
+    uint64_t *countU64 = skeys == h->keysAlt ? h->keys : h->keysAlt;   // the sort's spare key buffer
     if (nValid) {
         launch_mask_count(h->stream, h->pCount, nValid, countU64);
         launch_scan_u64(h->stream, countU64, nValid, h->pOff, h->pTiles, h->dTotalU64);

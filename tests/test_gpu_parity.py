@@ -203,6 +203,34 @@ def test_comb_matches_oracle(oracle_lib):
                                rtol=1e-15)
 
 
+@pytest.mark.parametrize("crowd", [(600, 2000, 5000), (9000,)])
+def test_comb_crowded_cells_match_oracle(oracle_lib, crowd):
+    """Cells far above the mean population: runs of 513-8192 census particles
+    are sorted by a block each, and a run above 8192 sends the whole comb to
+    the radix-sort path.  Both give the oracle's particles in its order."""
+    from test_oracle import synthetic_census
+    from oracle import ref
+    p = problems.gray_slab(new_photons_per_cell=5, face_packets=2000, comb_nmin=8, comb_factor=1.5)
+    n = 3000 + sum(crowd)
+    pre = synthetic_census(p, n, 7, ref.Particles)
+    at = 3000
+    for c, k in zip((5, 40, 77), crowd):
+        pre.cell[at:at + k] = c
+        at += k
+    xc, yc, zc = p.cell_centers()
+    pre.x, pre.y, pre.z = xc[pre.cell].copy(), yc[pre.cell].copy(), zc[pre.cell].copy()
+    e = Engine(p)
+    post = e.population_control(pre)
+    o = oracle_lib.Oracle(p)
+    o.set_census(pre)
+    o.phase("comb")
+    oc = o.census()
+    assert post.n == oc.n
+    np.testing.assert_array_equal(post.cell, oc.cell)
+    for f in ("x", "y", "z", "vx", "vy", "vz", "weight", "initial_weight"):
+        np.testing.assert_array_equal(getattr(post, f), getattr(oc, f), err_msg=f)
+
+
 def test_step_cube_statistics_vs_oracle(oracle_lib):
     """Several steps of the step-opacity cube on different seeds: GPU and
     oracle temperatures agree within the seed-to-seed scatter."""
