@@ -1599,7 +1599,7 @@ __global__ void __launch_bounds__(RS_THREADS) k_rs_scatter(const uint64_t *kin, 
 // is the radix sort's.  A run longer than BUCKET_BLOCK_MAX keys raises a flag,
 // and the caller falls back to the radix sort.
 
-constexpr uint32_t BUCKET_WARP_MAX = 512;     // runs up to this length: one warp, 4 KB of shared memory
+constexpr uint32_t BUCKET_WARP_MAX = 512;     // runs up to this length: one warp, in registers
 constexpr uint32_t BUCKET_BLOCK_MAX = 8192;   // longer runs up to this length: one block of 256, 64 KB
 constexpr int BUCKET_WARPS = 8;
 
@@ -1678,38 +1678,87 @@ __device__ __forceinline__ uint64_t bucket_pack(uint64_t key, uint32_t q, uint64
     return ((key & hashMask) << 32) | q;
 }
 
+// Ascending bitonic sort of 32 * E values held by a warp in registers, value
+// e of lane l at index 32 e + l: stages with a distance of 32 or more pair a
+// lane's own values, shorter ones pair lanes through shuffles.
+template <int E>
+__device__ __forceinline__ void warp_bitonic(uint64_t (&v)[E], uint32_t lane) {
+    constexpr uint32_t P = 32u * E;
+#pragma unroll
+    for (uint32_t k = 2; k <= P; k <<= 1) {
+#pragma unroll
+        for (uint32_t j = k >> 1; j > 0; j >>= 1) {
+            if (j >= 32) {
+                const int d = static_cast<int>(j >> 5);
+#pragma unroll
+                for (int e = 0; e < E; ++e) {
+                    const int f = e ^ d;
+                    if (f > e) {
+                        const bool up = ((static_cast<uint32_t>(e) * 32u + lane) & k) == 0;
+                        const uint64_t a = v[e], b = v[f];
+                        if ((a > b) == up) {
+                            v[e] = b;
+                            v[f] = a;
+                        }
+                    }
+                }
+            } else {
+                const bool lower = (lane & j) == 0;
+#pragma unroll
+                for (int e = 0; e < E; ++e) {
+                    const uint64_t p = __shfl_xor_sync(FULL, static_cast<unsigned long long>(v[e]), static_cast<int>(j));
+                    const bool up = ((static_cast<uint32_t>(e) * 32u + lane) & k) == 0;
+                    const uint64_t lo = v[e] < p ? v[e] : p, hi = v[e] < p ? p : v[e];
+                    v[e] = lower == up ? lo : hi;
+                }
+            }
+        }
+    }
+}
+
+// One run [b, b + len) with len <= 32 E, sorted by one warp in registers.
+template <int E>
+__device__ __forceinline__ void warp_sort_run(uint64_t *keys, uint32_t *vals, uint32_t b, uint32_t len, uint32_t r,
+                                              int pidBits, uint64_t hashMask, uint32_t lane) {
+    uint64_t v[E];
+#pragma unroll
+    for (int e = 0; e < E; ++e) {
+        const uint32_t i = static_cast<uint32_t>(e) * 32u + lane;
+        v[e] = i < len ? bucket_pack(keys[b + i], vals[b + i], hashMask) : ~0ull;
+    }
+    warp_bitonic<E>(v, lane);
+#pragma unroll
+    for (int e = 0; e < E; ++e) {
+        const uint32_t i = static_cast<uint32_t>(e) * 32u + lane;
+        if (i < len) {
+            keys[b + i] = (static_cast<uint64_t>(r) << pidBits) | (v[e] >> 32);
+            vals[b + i] = static_cast<uint32_t>(v[e]);
+        }
+    }
+}
+
 // Runs 0..nRuns-1 of (keys, vals), each sorted in place by key: one warp per
-// run of up to BUCKET_WARP_MAX keys; longer runs are listed for k_bucket_sort_long.
+// run of up to BUCKET_WARP_MAX keys, in registers; longer runs are listed for
+// k_bucket_sort_long.
 __global__ void __launch_bounds__(32 * BUCKET_WARPS) k_bucket_sort_runs(uint64_t *keys, uint32_t *vals,
                                                                         const uint32_t *start, uint32_t nRuns,
                                                                         int pidBits, uint32_t *longRuns,
                                                                         uint32_t *nLong, uint32_t longCap) {
-    __shared__ uint64_t sm[BUCKET_WARPS][BUCKET_WARP_MAX];
     const uint32_t lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-    uint64_t *sw = sm[wid];
     const uint64_t hashMask = (1ull << pidBits) - 1ull;   // pidBits <= 32
     const uint32_t warps = gridDim.x * BUCKET_WARPS;
     for (uint32_t r = blockIdx.x * BUCKET_WARPS + wid; r < nRuns; r += warps) {
         const uint32_t b = start[r], len = start[r + 1] - b;
         if (len < 2) continue;
-        if (len > BUCKET_WARP_MAX) {
-            if (lane == 0) {
-                const uint32_t slot = atomicAdd(nLong, 1u);
-                if (slot < longCap) longRuns[slot] = r;
-            }
-            continue;
+        if (len <= 32) warp_sort_run<1>(keys, vals, b, len, r, pidBits, hashMask, lane);
+        else if (len <= 64) warp_sort_run<2>(keys, vals, b, len, r, pidBits, hashMask, lane);
+        else if (len <= 128) warp_sort_run<4>(keys, vals, b, len, r, pidBits, hashMask, lane);
+        else if (len <= 256) warp_sort_run<8>(keys, vals, b, len, r, pidBits, hashMask, lane);
+        else if (len <= BUCKET_WARP_MAX) warp_sort_run<16>(keys, vals, b, len, r, pidBits, hashMask, lane);
+        else if (lane == 0) {
+            const uint32_t slot = atomicAdd(nLong, 1u);
+            if (slot < longCap) longRuns[slot] = r;
         }
-        uint32_t P = 32;
-        while (P < len) P <<= 1;
-        for (uint32_t i = lane; i < P; i += 32) sw[i] = i < len ? bucket_pack(keys[b + i], vals[b + i], hashMask) : ~0ull;
-        __syncwarp();
-        bitonic_sort(sw, P, lane, 32u, WarpSync{});
-        for (uint32_t i = lane; i < len; i += 32) {
-            const uint64_t v = sw[i];
-            keys[b + i] = (static_cast<uint64_t>(r) << pidBits) | (v >> 32);
-            vals[b + i] = static_cast<uint32_t>(v);
-        }
-        __syncwarp();
     }
 }
 
