@@ -1932,8 +1932,9 @@ __global__ void k_comb_plan(Ctx C, CombParams P, const double *wS, const uint32_
 // so the random reads overlap.
 constexpr int EMIT_BATCH = 2;
 
-__device__ __forceinline__ void comb_emit_fp64(const Ctx &C, PartReg &p, uint32_t c, uint32_t raw, double wNew,
-                                               uint64_t o, const Bank &out) {
+// The copy of a census particle the comb writes (FP64 form): the new weight
+// unless kept, and a position outside the box pulled toward the cell centre.
+__device__ __forceinline__ void comb_copy_fp64(const Ctx &C, PartReg &p, uint32_t c, uint32_t raw, double wNew) {
     if (!(raw & KEEP)) { p.w = wNew; p.w0 = p.w; p.t = 0; }
     p.cell = c;
     if (outside_box(C, p.x, p.y, p.z)) {   // :228-250
@@ -1947,6 +1948,10 @@ __device__ __forceinline__ void comb_emit_fp64(const Ctx &C, PartReg &p, uint32_
         }
         if (outside_box(C, p.x, p.y, p.z)) { p.x = mx; p.y = my; p.z = mz; }
     }
+}
+__device__ __forceinline__ void comb_emit_fp64(const Ctx &C, PartReg &p, uint32_t c, uint32_t raw, double wNew,
+                                               uint64_t o, const Bank &out) {
+    comb_copy_fp64(C, p, c, raw, wNew);
     const uint32_t m = raw & ~KEEP;
     for (uint32_t k = 0; k < m; ++k) store_part(out, static_cast<uint32_t>(o + k), p, static_cast<uint32_t>(o + k), 0);
 }
@@ -2006,6 +2011,145 @@ __global__ void k_comb_emit(Ctx C, CensusBank cen, const uint32_t *idx, const ui
                 p.w0 = lo_double(f);
                 p.nu = hi_double(rec[u][5]);
                 comb_emit_fp64(C, p, c, raw[u], wNew, o, out);
+            }
+        }
+    }
+}
+
+// Output-driven form of the same write: one thread per output slot o, whose
+// source is the sorted particle src[o].  Every lane writes one particle, so
+// the bank writes are contiguous and no lane idles on a dropped particle.
+// src[o] comes from marking each particle with copies at its first slot and a
+// running maximum over the slots (the sources increase with the slots).
+__global__ void k_emit_src_mark(const uint32_t *pCount, const uint64_t *pOffset, uint32_t nValid, uint32_t *src) {
+    for (uint32_t q = blockIdx.x * blockDim.x + threadIdx.x; q < nValid; q += gridDim.x * blockDim.x)
+        if (pCount[q] & ~KEEP) src[pOffset[q]] = q;
+}
+
+// inclusive running maximum of v[0, n) in tiles of 1024 (the tile's maximum to tileMax)
+__global__ void __launch_bounds__(1024) k_max_tiles(uint32_t *v, uint32_t n, uint32_t *tileMax) {
+    __shared__ uint32_t wmax[32];
+    const uint32_t lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    const uint32_t q = blockIdx.x * 1024u + threadIdx.x;
+    uint32_t x = q < n ? v[q] : 0u;
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+        const uint32_t y = __shfl_up_sync(FULL, x, d);
+        if (static_cast<int>(lane) >= d) x = max(x, y);
+    }
+    if (lane == 31) wmax[wid] = x;
+    __syncthreads();
+    if (wid == 0) {
+        uint32_t w = wmax[lane];
+#pragma unroll
+        for (int d = 1; d < 32; d <<= 1) {
+            const uint32_t y = __shfl_up_sync(FULL, w, d);
+            if (static_cast<int>(lane) >= d) w = max(w, y);
+        }
+        wmax[lane] = w;
+    }
+    __syncthreads();
+    if (wid > 0) x = max(x, wmax[wid - 1]);
+    if (q < n) v[q] = x;
+    if (threadIdx.x == 1023) tileMax[blockIdx.x] = x;
+}
+// tileMax[t] <- maximum of tiles 0..t-1 (0 for t = 0), one block
+__global__ void __launch_bounds__(1024) k_max_tile_prefix(uint32_t *tileMax, uint32_t ntiles) {
+    __shared__ uint32_t wmax[32];
+    __shared__ uint32_t carryS;
+    const uint32_t lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    uint32_t carry = 0;
+    for (uint32_t base = 0; base < ntiles; base += 1024u) {
+        const uint32_t q = base + threadIdx.x;
+        uint32_t x = q < ntiles ? tileMax[q] : 0u;
+#pragma unroll
+        for (int d = 1; d < 32; d <<= 1) {
+            const uint32_t y = __shfl_up_sync(FULL, x, d);
+            if (static_cast<int>(lane) >= d) x = max(x, y);
+        }
+        if (lane == 31) wmax[wid] = x;
+        __syncthreads();
+        if (wid == 0) {
+            uint32_t w = wmax[lane];
+#pragma unroll
+            for (int d = 1; d < 32; d <<= 1) {
+                const uint32_t y = __shfl_up_sync(FULL, w, d);
+                if (static_cast<int>(lane) >= d) w = max(w, y);
+            }
+            wmax[lane] = w;
+        }
+        __syncthreads();
+        if (wid > 0) x = max(x, wmax[wid - 1]);
+        const uint32_t incl = max(x, carry);
+        // exclusive: the inclusive maximum of the previous entry
+        uint32_t prev = __shfl_up_sync(FULL, incl, 1);
+        if (lane == 0) prev = wid > 0 ? max(wmax[wid - 1], carry) : carry;
+        if (q < ntiles) tileMax[q] = prev;
+        if (threadIdx.x == 1023) carryS = incl;
+        __syncthreads();
+        carry = carryS;
+        __syncthreads();
+    }
+}
+__global__ void __launch_bounds__(1024) k_max_apply(uint32_t *v, uint32_t n, const uint32_t *tileMax) {
+    const uint32_t q = blockIdx.x * 1024u + threadIdx.x;
+    if (q < n) v[q] = max(v[q], tileMax[blockIdx.x]);
+}
+
+template <bool FP32>
+__global__ void k_comb_emit_out(Ctx C, CensusBank cen, const uint32_t *idx, const uint64_t *sortedKeys, int pidBits,
+                                uint32_t bins, uint32_t total, const uint32_t *src, const uint32_t *pCount,
+                                const double *pWeight, Bank out) {
+    constexpr int words = FP32 ? 4 : 6;
+    const uint32_t stride = gridDim.x * blockDim.x;
+    for (uint32_t base = blockIdx.x * blockDim.x + threadIdx.x; base < total; base += EMIT_BATCH * stride) {
+        uint32_t qs[EMIT_BATCH], raw[EMIT_BATCH];
+        uint4 rec[EMIT_BATCH][words];
+#pragma unroll
+        for (int u = 0; u < EMIT_BATCH; ++u) {
+            const uint32_t o = base + u * stride;
+            qs[u] = o < total ? src[o] : 0u;
+        }
+#pragma unroll
+        for (int u = 0; u < EMIT_BATCH; ++u) {
+            const uint32_t o = base + u * stride;
+            raw[u] = 0u;
+            if (o < total) {
+                raw[u] = pCount[qs[u]];
+                const uint4 *r = cen.rec + static_cast<size_t>(idx[qs[u]]) * words;
+#pragma unroll
+                for (int w = 0; w < words; ++w) rec[u][w] = __ldg(r + w);
+            }
+        }
+#pragma unroll
+        for (int u = 0; u < EMIT_BATCH; ++u) {
+            const uint32_t o = base + u * stride;
+            if (o >= total) continue;
+            const uint32_t q = qs[u];
+            const uint32_t c = static_cast<uint32_t>((sortedKeys[q] >> pidBits) / bins);   // (cell, bin) keys
+            const double wNew = pWeight[q];
+            if constexpr (FP32) {
+                const uint4 a = rec[u][0], b = rec[u][1], d = rec[u][2];
+                Track32 T;
+                T.qx = __uint_as_float(a.x); T.qy = __uint_as_float(a.y); T.qz = __uint_as_float(a.z);
+                T.ux = __uint_as_float(a.w); T.uy = __uint_as_float(b.x); T.uz = __uint_as_float(b.y);
+                T.t = __longlong_as_double((static_cast<unsigned long long>(b.w) << 32) | b.z);
+                T.w = lo_double(d); T.w0 = hi_double(d);
+                if (!(raw[u] & KEEP)) { T.w = wNew; T.w0 = T.w; T.t = 0; }
+                T.cell = c;
+                store32(out, o, T, o, 0);
+                if (out.nu) store_nu32(out, o, __uint_as_float(rec[u][3].w));
+            } else {
+                const uint4 a = rec[u][0], b = rec[u][1], d = rec[u][2], e = rec[u][3], f = rec[u][4];
+                PartReg p;
+                p.x = lo_double(a); p.y = hi_double(a);
+                p.z = lo_double(b); p.vx = hi_double(b);
+                p.vy = lo_double(d); p.vz = hi_double(d);
+                p.t = lo_double(e); p.w = hi_double(e);
+                p.w0 = lo_double(f);
+                p.nu = hi_double(rec[u][5]);
+                comb_copy_fp64(C, p, c, raw[u], wNew);
+                store_part(out, o, p, o, 0);
             }
         }
     }
@@ -2562,6 +2706,26 @@ void launch_comb_emit(cudaStream_t s, const Ctx &C, const CensusBank &cen, const
     else
         k_comb_emit<false><<<grid_for(nValid, 256, 148 * 16), 256, 0, s>>>(C, cen, idx, sortedKeys, pidBits, bins, nValid, pCount,
                                                                             pWeight, pOffset, out);
+}
+// The same write, output-driven (k_comb_emit_out).  src: scratch of `total`
+// words; tileMax: scratch of total / 1024 + 1 words.
+void launch_comb_emit_out(cudaStream_t s, const Ctx &C, const CensusBank &cen, const uint32_t *idx,
+                          const uint64_t *sortedKeys, int pidBits, uint32_t bins, uint32_t nValid, uint32_t total,
+                          const uint32_t *pCount, const double *pWeight, const uint64_t *pOffset, uint32_t *src,
+                          uint32_t *tileMax, const Bank &out) {
+    if (!nValid || !total) return;
+    cudaMemsetAsync(src, 0, sizeof(uint32_t) * total, s);
+    k_emit_src_mark<<<grid_for(nValid, 256, 148 * 16), 256, 0, s>>>(pCount, pOffset, nValid, src);
+    const uint32_t tiles = (total + 1023) / 1024;
+    k_max_tiles<<<tiles, 1024, 0, s>>>(src, total, tileMax);
+    k_max_tile_prefix<<<1, 1024, 0, s>>>(tileMax, tiles);
+    k_max_apply<<<tiles, 1024, 0, s>>>(src, total, tileMax);
+    if (C.fp32)
+        k_comb_emit_out<true><<<grid_for(total, 256, 148 * 16), 256, 0, s>>>(C, cen, idx, sortedKeys, pidBits, bins, total,
+                                                                             src, pCount, pWeight, out);
+    else
+        k_comb_emit_out<false><<<grid_for(total, 256, 148 * 16), 256, 0, s>>>(C, cen, idx, sortedKeys, pidBits, bins,
+                                                                              total, src, pCount, pWeight, out);
 }
 void launch_mask_count(cudaStream_t s, const uint32_t *pCount, uint32_t n, uint64_t *out) {
     k_mask_count<<<grid_for(n, 256, 8192), 256, 0, s>>>(pCount, n, out);

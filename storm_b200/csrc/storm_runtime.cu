@@ -1469,9 +1469,17 @@ int storm_cuda_phase_comb(StormHandle *h) {
         CK(bank_alloc(h, h->bankA, grown));
         CK(bank_alloc(h, h->bankB, grown));
     }
-    launch_comb_emit(h->stream, h->C, h->bankC, idx, skeys, pidBits, B, nValid, h->pCount, h->pWeight, h->pOff,
-                     h->bankA);
-    ++h->launches;
+    if (grown) {
+        // the output-driven write needs `total` words of scratch, which only the grown buffers have
+        launch_comb_emit(h->stream, h->C, h->bankC, idx, skeys, pidBits, B, nValid, h->pCount, h->pWeight, h->pOff,
+                         h->bankA);
+        ++h->launches;
+    } else {
+        uint32_t *src = idx == h->valsAlt ? h->vals : h->valsAlt;   // the sort's spare value buffer
+        launch_comb_emit_out(h->stream, h->C, h->bankC, idx, skeys, pidBits, B, nValid, static_cast<uint32_t>(total),
+                             h->pCount, h->pWeight, h->pOff, src, reinterpret_cast<uint32_t *>(h->pTiles), h->bankA);
+        h->launches += nValid && total ? 5 : 0;
+    }
     CK(cudaGetLastError());
     if (grown) {
         CK(cudaStreamSynchronize(h->stream));
