@@ -125,9 +125,11 @@ int launch_radix_sort(cudaStream_t s, uint64_t *keys, uint32_t *vals, uint64_t *
                       int bits, uint32_t *tileHist);
 uint32_t radix_tile_count(uint32_t n);
 void launch_comb_ranges(cudaStream_t s, const uint64_t *keys, uint32_t n, uint32_t ncells, uint32_t *start, int pidBits);
-void launch_bucket_sort(cudaStream_t s, const uint64_t *keys, uint32_t n, int pidBits, uint32_t nRuns, uint32_t *start,
-                        uint32_t *cursor, uint64_t *scanSums, uint64_t *outKeys, uint32_t *outVals,
-                        uint32_t *longRuns, uint32_t longCap, uint32_t *flags);
+void launch_bucket_sort(cudaStream_t s, const Ctx &C, const CensusBank &cen, const uint64_t *keys, uint32_t n,
+                        int pidBits, uint32_t nRuns, uint32_t *start, uint32_t *cursor, uint64_t *scanSums,
+                        uint64_t *outKeys, uint32_t *outVals, double *wS, uint32_t *longRuns, uint32_t longCap,
+                        uint32_t *flags);
+void launch_mask_count_upto(cudaStream_t s, const uint32_t *pCount, uint32_t n, const uint32_t *nValid, uint64_t *out);
 size_t bucket_scan_words(uint32_t len);
 uint32_t bucket_long_capacity(uint32_t n);
 void launch_sorted_weights(cudaStream_t s, const Ctx &C, const CensusBank &cen, const uint32_t *idx, uint32_t n,

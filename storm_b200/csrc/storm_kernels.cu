@@ -1599,7 +1599,7 @@ __global__ void __launch_bounds__(RS_THREADS) k_rs_scatter(const uint64_t *kin, 
 // is the radix sort's.  A run longer than BUCKET_BLOCK_MAX keys raises a flag,
 // and the caller falls back to the radix sort.
 
-constexpr uint32_t BUCKET_WARP_MAX = 512;     // runs up to this length: one warp, in registers
+constexpr uint32_t BUCKET_WARP_MAX = 512;     // runs up to this length: one warp (registers, then 4 KB of shared memory)
 constexpr uint32_t BUCKET_BLOCK_MAX = 8192;   // longer runs up to this length: one block of 256, 64 KB
 constexpr int BUCKET_WARPS = 8;
 
@@ -1716,10 +1716,12 @@ __device__ __forceinline__ void warp_bitonic(uint64_t (&v)[E], uint32_t lane) {
     }
 }
 
-// One run [b, b + len) with len <= 32 E, sorted by one warp in registers.
+// One run [b, b + len) with len <= 32 E, sorted by one warp in registers; the
+// census weight of each sorted particle goes to wS.
 template <int E>
-__device__ __forceinline__ void warp_sort_run(uint64_t *keys, uint32_t *vals, uint32_t b, uint32_t len, uint32_t r,
-                                              int pidBits, uint64_t hashMask, uint32_t lane) {
+__device__ __forceinline__ void warp_sort_run(const Ctx &C, const CensusBank &cen, uint64_t *keys, uint32_t *vals,
+                                              double *wS, uint32_t b, uint32_t len, uint32_t r, int pidBits,
+                                              uint64_t hashMask, uint32_t lane) {
     uint64_t v[E];
 #pragma unroll
     for (int e = 0; e < E; ++e) {
@@ -1731,31 +1733,56 @@ __device__ __forceinline__ void warp_sort_run(uint64_t *keys, uint32_t *vals, ui
     for (int e = 0; e < E; ++e) {
         const uint32_t i = static_cast<uint32_t>(e) * 32u + lane;
         if (i < len) {
+            const uint32_t q = static_cast<uint32_t>(v[e]);
             keys[b + i] = (static_cast<uint64_t>(r) << pidBits) | (v[e] >> 32);
-            vals[b + i] = static_cast<uint32_t>(v[e]);
+            vals[b + i] = q;
+            wS[b + i] = census_w(C, cen, q);
         }
     }
 }
 
-// Runs 0..nRuns-1 of (keys, vals), each sorted in place by key: one warp per
-// run of up to BUCKET_WARP_MAX keys, in registers; longer runs are listed for
-// k_bucket_sort_long.
-__global__ void __launch_bounds__(32 * BUCKET_WARPS) k_bucket_sort_runs(uint64_t *keys, uint32_t *vals,
+// Runs 0..nRuns-1 of (keys, vals), each sorted in place by key, with the census
+// weights in sorted order to wS.  One warp per run of up to BUCKET_WARP_MAX
+// keys: in registers up to 128 (fully unrolled networks; larger ones would not
+// fit the instruction cache), in the warp's shared memory above.  Longer runs
+// are listed for k_bucket_sort_long.
+__global__ void __launch_bounds__(32 * BUCKET_WARPS) k_bucket_sort_runs(Ctx C, CensusBank cen, uint64_t *keys,
+                                                                        uint32_t *vals, double *wS,
                                                                         const uint32_t *start, uint32_t nRuns,
                                                                         int pidBits, uint32_t *longRuns,
                                                                         uint32_t *nLong, uint32_t longCap) {
+    __shared__ uint64_t sm[BUCKET_WARPS][BUCKET_WARP_MAX];
     const uint32_t lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    uint64_t *sw = sm[wid];
     const uint64_t hashMask = (1ull << pidBits) - 1ull;   // pidBits <= 32
     const uint32_t warps = gridDim.x * BUCKET_WARPS;
     for (uint32_t r = blockIdx.x * BUCKET_WARPS + wid; r < nRuns; r += warps) {
         const uint32_t b = start[r], len = start[r + 1] - b;
-        if (len < 2) continue;
-        if (len <= 32) warp_sort_run<1>(keys, vals, b, len, r, pidBits, hashMask, lane);
-        else if (len <= 64) warp_sort_run<2>(keys, vals, b, len, r, pidBits, hashMask, lane);
-        else if (len <= 128) warp_sort_run<4>(keys, vals, b, len, r, pidBits, hashMask, lane);
-        else if (len <= 256) warp_sort_run<8>(keys, vals, b, len, r, pidBits, hashMask, lane);
-        else if (len <= BUCKET_WARP_MAX) warp_sort_run<16>(keys, vals, b, len, r, pidBits, hashMask, lane);
-        else if (lane == 0) {
+        if (len == 0) continue;
+        if (len == 1) {
+            if (lane == 0) wS[b] = census_w(C, cen, vals[b]);
+        } else if (len <= 32) {
+            warp_sort_run<1>(C, cen, keys, vals, wS, b, len, r, pidBits, hashMask, lane);
+        } else if (len <= 64) {
+            warp_sort_run<2>(C, cen, keys, vals, wS, b, len, r, pidBits, hashMask, lane);
+        } else if (len <= 128) {
+            warp_sort_run<4>(C, cen, keys, vals, wS, b, len, r, pidBits, hashMask, lane);
+        } else if (len <= BUCKET_WARP_MAX) {
+            uint32_t P = 256;
+            while (P < len) P <<= 1;
+            for (uint32_t i = lane; i < P; i += 32)
+                sw[i] = i < len ? bucket_pack(keys[b + i], vals[b + i], hashMask) : ~0ull;
+            __syncwarp();
+            bitonic_sort(sw, P, lane, 32u, WarpSync{});
+            for (uint32_t i = lane; i < len; i += 32) {
+                const uint64_t v = sw[i];
+                const uint32_t q = static_cast<uint32_t>(v);
+                keys[b + i] = (static_cast<uint64_t>(r) << pidBits) | (v >> 32);
+                vals[b + i] = q;
+                wS[b + i] = census_w(C, cen, q);
+            }
+            __syncwarp();
+        } else if (lane == 0) {
             const uint32_t slot = atomicAdd(nLong, 1u);
             if (slot < longCap) longRuns[slot] = r;
         }
@@ -1764,10 +1791,10 @@ __global__ void __launch_bounds__(32 * BUCKET_WARPS) k_bucket_sort_runs(uint64_t
 
 // The listed runs, one block each (dynamic shared memory: BUCKET_BLOCK_MAX words).
 // A run longer than BUCKET_BLOCK_MAX, or more listed runs than longCap, sets *tooLong.
-__global__ void __launch_bounds__(256) k_bucket_sort_long(uint64_t *keys, uint32_t *vals, const uint32_t *start,
-                                                          int pidBits, const uint32_t *longRuns,
-                                                          const uint32_t *nLong, uint32_t longCap,
-                                                          uint32_t *tooLong) {
+__global__ void __launch_bounds__(256) k_bucket_sort_long(Ctx C, CensusBank cen, uint64_t *keys, uint32_t *vals,
+                                                          double *wS, const uint32_t *start, int pidBits,
+                                                          const uint32_t *longRuns, const uint32_t *nLong,
+                                                          uint32_t longCap, uint32_t *tooLong) {
     extern __shared__ __align__(16) unsigned char bucketMem[];
     uint64_t *sb = reinterpret_cast<uint64_t *>(bucketMem);
     const uint32_t listed = *nLong;
@@ -1791,8 +1818,10 @@ __global__ void __launch_bounds__(256) k_bucket_sort_long(uint64_t *keys, uint32
         bitonic_sort(sb, P, threadIdx.x, blockDim.x, BlockSync{});
         for (uint32_t i = threadIdx.x; i < len; i += blockDim.x) {
             const uint64_t v = sb[i];
+            const uint32_t q = static_cast<uint32_t>(v);
             keys[b + i] = (static_cast<uint64_t>(r) << pidBits) | (v >> 32);
-            vals[b + i] = static_cast<uint32_t>(v);
+            vals[b + i] = q;
+            wS[b + i] = census_w(C, cen, q);
         }
         __syncthreads();
     }
@@ -2344,6 +2373,12 @@ __global__ void k_mask_count(const uint32_t *pCount, uint32_t n, uint64_t *out) 
     for (uint32_t q = blockIdx.x * blockDim.x + threadIdx.x; q < n; q += gridDim.x * blockDim.x)
         out[q] = pCount[q] & ~KEEP;
 }
+// the same over n slots of which the first *nValid are particles (zero beyond)
+__global__ void k_mask_count_upto(const uint32_t *pCount, uint32_t n, const uint32_t *nValid, uint64_t *out) {
+    const uint32_t v = *nValid;
+    for (uint32_t q = blockIdx.x * blockDim.x + threadIdx.x; q < n; q += gridDim.x * blockDim.x)
+        out[q] = q < v ? (pCount[q] & ~KEEP) : 0ull;
+}
 
 // census kept as is (no population control): order by pid for a deterministic bank
 __global__ void k_census_keys_pid(Ctx C, CensusBank cen, uint32_t n, uint64_t *keys, uint32_t *vals) {
@@ -2644,13 +2679,15 @@ int launch_radix_sort(cudaStream_t s, uint64_t *keys, uint32_t *vals, uint64_t *
 // Bucket sort of the comb keys (see k_bucket_count).  `start` receives the
 // first position of every run 0..nRuns (start[nRuns]: the first key outside
 // every run); `cursor` is scratch of nRuns + 1 words and `scanSums` of
-// bucket_scan_words(nRuns + 1).  The sorted pairs end in (outKeys, outVals).
+// bucket_scan_words(nRuns + 1).  The sorted pairs end in (outKeys, outVals)
+// and the census weights in sorted order in wS (positions below start[nRuns]).
 // Long runs are listed in longRuns (longCap entries); flags[0] counts them and
 // flags[1] is set when a run is too long for this sort (then nothing is sorted
 // and the caller falls back to launch_radix_sort).
-void launch_bucket_sort(cudaStream_t s, const uint64_t *keys, uint32_t n, int pidBits, uint32_t nRuns, uint32_t *start,
-                        uint32_t *cursor, uint64_t *scanSums, uint64_t *outKeys, uint32_t *outVals,
-                        uint32_t *longRuns, uint32_t longCap, uint32_t *flags) {
+void launch_bucket_sort(cudaStream_t s, const Ctx &C, const CensusBank &cen, const uint64_t *keys, uint32_t n,
+                        int pidBits, uint32_t nRuns, uint32_t *start, uint32_t *cursor, uint64_t *scanSums,
+                        uint64_t *outKeys, uint32_t *outVals, double *wS, uint32_t *longRuns, uint32_t longCap,
+                        uint32_t *flags) {
     const uint32_t len = nRuns + 1;
     cudaMemsetAsync(start, 0, sizeof(uint32_t) * len, s);
     cudaMemsetAsync(flags, 0, 2 * sizeof(uint32_t), s);
@@ -2662,10 +2699,11 @@ void launch_bucket_sort(cudaStream_t s, const uint64_t *keys, uint32_t n, int pi
     cudaMemcpyAsync(cursor, start, sizeof(uint32_t) * len, cudaMemcpyDeviceToDevice, s);
     k_bucket_place<<<grid_for(n, 256, 148 * 16), 256, 0, s>>>(keys, n, pidBits, nRuns, cursor, outKeys, outVals);
     k_bucket_sort_runs<<<grid_for(nRuns, BUCKET_WARPS, 148 * 32), 32 * BUCKET_WARPS, 0, s>>>(
-        outKeys, outVals, start, nRuns, pidBits, longRuns, flags, longCap);
+        C, cen, outKeys, outVals, wS, start, nRuns, pidBits, longRuns, flags, longCap);
     const size_t smem = sizeof(uint64_t) * BUCKET_BLOCK_MAX;
     cudaFuncSetAttribute(k_bucket_sort_long, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
-    k_bucket_sort_long<<<148, 256, smem, s>>>(outKeys, outVals, start, pidBits, longRuns, flags, longCap, flags + 1);
+    k_bucket_sort_long<<<148, 256, smem, s>>>(C, cen, outKeys, outVals, wS, start, pidBits, longRuns, flags, longCap,
+                                              flags + 1);
 }
 size_t bucket_scan_words(uint32_t len) { return (len + 1023) / 1024 + 2; }
 uint32_t bucket_long_capacity(uint32_t n) { return n / (BUCKET_WARP_MAX + 1) + 1; }
@@ -2729,6 +2767,9 @@ void launch_comb_emit_out(cudaStream_t s, const Ctx &C, const CensusBank &cen, c
 }
 void launch_mask_count(cudaStream_t s, const uint32_t *pCount, uint32_t n, uint64_t *out) {
     k_mask_count<<<grid_for(n, 256, 8192), 256, 0, s>>>(pCount, n, out);
+}
+void launch_mask_count_upto(cudaStream_t s, const uint32_t *pCount, uint32_t n, const uint32_t *nValid, uint64_t *out) {
+    k_mask_count_upto<<<grid_for(n, 256, 8192), 256, 0, s>>>(pCount, n, nValid, out);
 }
 void launch_census_keys_pid(cudaStream_t s, const Ctx &C, const CensusBank &cen, uint32_t n, uint64_t *keys,
                             uint32_t *vals) {

@@ -40,6 +40,7 @@ struct StormHandle {
     cudaStream_t stream = nullptr;
     cudaEvent_t evStart = nullptr, evTransport0 = nullptr, evTransport1 = nullptr, evEnd = nullptr;
     cudaEvent_t evAfterEmit = nullptr, evAfterComb = nullptr;
+    unsigned char *pinned = nullptr;   // the stream set's page-locked readback buffer (kPinnedBytes)
     uint32_t nx = 0, ny = 0, nz = 0, N = 0;
     std::vector<double> hxe, hye, hze, hxc, hyc, hzc;
     // device mesh + cells
@@ -270,9 +271,11 @@ DevicePool &device_pool() {
 // A handle's stream and its six timing events outlive the handle: destroy
 // returns them, idle, to a per-device cache and the next create takes them
 // from there instead of creating new ones.
+constexpr size_t kPinnedBytes = 4096;   // page-locked staging for small readbacks, per stream set
 struct StreamSet {
     cudaStream_t stream = nullptr;
     cudaEvent_t ev[6] = {};
+    unsigned char *pinned = nullptr;    // kPinnedBytes, or null (readbacks then go to pageable memory)
 };
 std::mutex &stream_cache_mutex() {
     static std::mutex m;
@@ -295,6 +298,9 @@ bool take_stream_set(int dev, StreamSet &out) {
     if (cudaStreamCreateWithFlags(&out.stream, cudaStreamNonBlocking) != cudaSuccess) return false;
     for (cudaEvent_t &e : out.ev)
         if (cudaEventCreate(&e) != cudaSuccess) return false;
+    void *p = nullptr;
+    if (cudaMallocHost(&p, kPinnedBytes) == cudaSuccess) out.pinned = static_cast<unsigned char *>(p);
+    else cudaGetLastError();
     return true;
 }
 void return_stream_set(int dev, const StreamSet &s) {
@@ -611,18 +617,60 @@ int build_rw_tables(StormHandle *h) {
     return STORM_OK;
 }
 
-// Small device->host read on the handle's own stream (never the legacy default
-// stream, so handles on other streams keep running).
+// Small device->host reads on the handle's own stream (never the legacy
+// default stream, so handles on other streams keep running), staged through
+// the stream set's page-locked buffer: a copy into pageable memory would
+// itself wait for the stream, so several reads would drain it several times;
+// staged, they complete with one synchronisation.
+struct Readback {
+    void *dst;
+    const void *src;
+    size_t bytes;
+};
+constexpr int kMaxReadbacks = 6;
+int raise_from_word(StormHandle *h, const int32_t *e);
+// With `check`, the device error word is read as well and a raised error is returned.
+int read_many(StormHandle *h, const Readback *r, int n, bool check) {
+    int32_t e[3] = {0, 0, 0};
+    size_t need = 16;
+    for (int q = 0; q < n; ++q) need += (r[q].bytes + 15) / 16 * 16;
+    if (h->pinned && n <= kMaxReadbacks && need <= kPinnedBytes) {
+        size_t off[kMaxReadbacks + 1];
+        size_t o = 0;
+        for (int q = 0; q < n; ++q) {
+            off[q] = o;
+            CK(cudaMemcpyAsync(h->pinned + o, r[q].src, r[q].bytes, cudaMemcpyDeviceToHost, h->stream));
+            o += (r[q].bytes + 15) / 16 * 16;
+        }
+        if (check) CK(cudaMemcpyAsync(h->pinned + o, h->dErr, sizeof(e), cudaMemcpyDeviceToHost, h->stream));
+        CK(cudaStreamSynchronize(h->stream));
+        for (int q = 0; q < n; ++q) std::memcpy(r[q].dst, h->pinned + off[q], r[q].bytes);
+        if (check) std::memcpy(e, h->pinned + o, sizeof(e));
+    } else {
+        for (int q = 0; q < n; ++q)
+            CK(cudaMemcpyAsync(r[q].dst, r[q].src, r[q].bytes, cudaMemcpyDeviceToHost, h->stream));
+        if (check) CK(cudaMemcpyAsync(e, h->dErr, sizeof(e), cudaMemcpyDeviceToHost, h->stream));
+        CK(cudaStreamSynchronize(h->stream));
+    }
+    return check ? raise_from_word(h, e) : STORM_OK;
+}
+
 cudaError_t read_small(StormHandle *h, void *dst, const void *src, size_t bytes) {
+    if (h->pinned && bytes <= kPinnedBytes) {
+        cudaError_t e = cudaMemcpyAsync(h->pinned, src, bytes, cudaMemcpyDeviceToHost, h->stream);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+        if (e == cudaSuccess) std::memcpy(dst, h->pinned, bytes);
+        return e;
+    }
     cudaError_t e = cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, h->stream);
     if (e != cudaSuccess) return e;
     return cudaStreamSynchronize(h->stream);
 }
 
-int check_device_error(StormHandle *h) {
-    int32_t e[3] = {0, 0, 0};
-    CK(cudaMemcpyAsync(e, h->dErr, sizeof(e), cudaMemcpyDeviceToHost, h->stream));
-    CK(cudaStreamSynchronize(h->stream));
+int check_device_error(StormHandle *h) { return read_many(h, nullptr, 0, true); }
+
+// STORM_ERR_DEVICE with the handle's error fields set when the device error word is raised
+int raise_from_word(StormHandle *h, const int32_t *e) {
     if (e[0] != 0) {
         h->errCode = e[0];
         h->errCell = static_cast<uint32_t>(e[1]);
@@ -639,21 +687,8 @@ int check_device_error(StormHandle *h) {
 // One small device->host read together with the device error word, one
 // stream synchronisation for both.
 int read_checked(StormHandle *h, void *dst, const void *src, size_t bytes) {
-    int32_t e[3] = {0, 0, 0};
-    CK(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, h->stream));
-    CK(cudaMemcpyAsync(e, h->dErr, sizeof(e), cudaMemcpyDeviceToHost, h->stream));
-    CK(cudaStreamSynchronize(h->stream));
-    if (e[0] != 0) {
-        h->errCode = e[0];
-        h->errCell = static_cast<uint32_t>(e[1]);
-        h->errParticle = static_cast<uint32_t>(e[2]);
-        char buf[160];
-        std::snprintf(buf, sizeof(buf), "device error %d at cell %u particle %u", e[0], static_cast<uint32_t>(e[1]),
-                      static_cast<uint32_t>(e[2]));
-        h->errMsg = buf;
-        return STORM_ERR_DEVICE;
-    }
-    return STORM_OK;
+    const Readback r{dst, src, bytes};
+    return read_many(h, &r, 1, true);
 }
 
 void refresh_ctx(StormHandle *h) {
@@ -796,6 +831,7 @@ int storm_cuda_create(const StormProblemDesc *d, StormHandle **out) {
         h->stream = ss.stream;
         h->evStart = ss.ev[0]; h->evTransport0 = ss.ev[1]; h->evTransport1 = ss.ev[2];
         h->evEnd = ss.ev[3]; h->evAfterEmit = ss.ev[4]; h->evAfterComb = ss.ev[5];
+        h->pinned = ss.pinned;
         if (!ok) return fail(STORM_ERR_CUDA);
     }
 
@@ -1113,11 +1149,13 @@ int storm_cuda_destroy(StormHandle *h) {
         StreamSet ss;
         ss.stream = h->stream;
         for (int q = 0; q < 6; ++q) ss.ev[q] = evs[q];
+        ss.pinned = h->pinned;
         return_stream_set(h->device, ss);
     } else {
         for (cudaEvent_t e : evs)
             if (e) cudaEventDestroy(e);
         if (h->stream) cudaStreamDestroy(h->stream);
+        if (h->pinned) cudaFreeHost(h->pinned);
     }
     for (cudaEvent_t e : h->evPool)
         if (e) cudaEventDestroy(e);
@@ -1174,9 +1212,11 @@ int storm_cuda_phase_emit(StormHandle *h, double dt) {
     h->launches += 6;
     CK(cudaGetLastError());
     struct { uint64_t total; int32_t amb; } back{};
-    CK(cudaMemcpyAsync(&back.total, h->dTotalU64, sizeof(uint64_t), cudaMemcpyDeviceToHost, h->stream));
-    CK(cudaMemcpyAsync(&back.amb, h->dAmbiguous, sizeof(int32_t), cudaMemcpyDeviceToHost, h->stream));
-    CK(cudaStreamSynchronize(h->stream));
+    {
+        const Readback r[2] = {{&back.total, h->dTotalU64, sizeof(uint64_t)}, {&back.amb, h->dAmbiguous, sizeof(int32_t)}};
+        const int rc = read_many(h, r, 2, false);
+        if (rc != STORM_OK) return rc;
+    }
     if (back.amb) {
         launch_sequential_sum(h->stream, h->A.emitE, N, h->dTotalE);
         launch_allocate(h->stream, h->C, h->A, h->dTotalE, h->desc.new_photons_per_cell);
@@ -1184,8 +1224,7 @@ int storm_cuda_phase_emit(StormHandle *h, double dt) {
         h->launches += 5;
         ++h->exactSums;
         CK(cudaGetLastError());
-        CK(cudaMemcpyAsync(&back.total, h->dTotalU64, sizeof(uint64_t), cudaMemcpyDeviceToHost, h->stream));
-        CK(cudaStreamSynchronize(h->stream));
+        CK(read_small(h, &back.total, h->dTotalU64, sizeof(uint64_t)));
     }
     launch_emission_debit(h->stream, h->C, h->A, h->dStats);
     ++h->launches;
@@ -1378,13 +1417,45 @@ int storm_cuda_phase_comb(StormHandle *h) {
     else launch_comb_keys(h->stream, h->C, h->bankC, n, h->keys, h->vals, combKey, pidBits);
     int cellBits = 0;
     while ((1ull << cellBits) <= nRuns) ++cellBits;
-    // The bucket sort (per-run counting sort, then each run sorted in shared
-    // memory) and the radix sort give the same order; the radix sort is the
-    // fallback for runs too long for the bucket sort.
+    // The bucket sort (per-run counting sort, then each run sorted on its own)
+    // and the radix sort give the same order; the radix sort is the fallback
+    // for runs too long for the bucket sort.  The plan and the scan of the copy
+    // counts run on the bucket sort's result before the host learns whether it
+    // succeeded: one synchronisation reads the flag, the particle count and the
+    // output total together, and only a failed bucket sort repeats the work.
     const uint64_t *skeys = nullptr;
     const uint32_t *idx = nullptr;
-    uint32_t nValid = 0;
-    bool haveValid = false;
+    double *wS = h->pWeight;   // census weights in sorted order; the plan overwrites each slot with the copies' weight
+    CombParams P;
+    P.nmin = h->desc.comb_nmin;
+    P.ntotal = static_cast<uint64_t>(static_cast<double>(static_cast<uint64_t>(N) * h->desc.comb_nmin) * h->desc.comb_factor);
+    auto radix_sort = [&]() {
+        const int alt = launch_radix_sort(h->stream, h->keys, h->vals, h->keysAlt, h->valsAlt, n, pidBits + cellBits,
+                                          h->tileHist);
+        skeys = alt ? h->keysAlt : h->keys;
+        idx = alt ? h->valsAlt : h->vals;
+        launch_comb_ranges(h->stream, skeys, n, static_cast<uint32_t>(nRuns), start, pidBits);
+        launch_sorted_weights(h->stream, h->C, h->bankC, idx, n, wS);
+        h->launches += 5 * ((pidBits + cellBits + 7) / 8) + 2;
+    };
+    // per-cell sums, the plan, and the copy counts scanned over n slots (the
+    // first start[nRuns] are particles, the rest count zero)
+    auto plan_and_scan = [&]() {
+        if (strat) launch_strat_sums(h->stream, wS, start, N, B, h->stratBinW, h->combW);
+        else launch_comb_cell_sums(h->stream, wS, start, N, h->combW);
+        launch_blocked_sum(h->stream, h->combW, N, h->combWtot);
+        if (strat)
+            launch_strat_plan(h->stream, h->C, P, h->strat, wS, start, h->stratBinW, h->combW, h->combWtot, h->pCount,
+                              h->pWeight, h->combCount, h->A.eradCensus, h->dStats);
+        else
+            launch_comb_plan(h->stream, h->C, P, wS, start, h->combW, h->combWtot, h->pCount, h->pWeight,
+                             h->combCount, h->A.eradCensus, h->dStats);
+        uint64_t *countU64 = skeys == h->keysAlt ? h->keys : h->keysAlt;   // the sort's spare key buffer
+        launch_mask_count_upto(h->stream, h->pCount, n, start + nRuns, countU64);
+        launch_scan_u64(h->stream, countU64, n, h->pOff, h->pTiles, h->dTotalU64);
+        h->launches += 4 + 3;
+    };
+    bool bucket = false;
     if (nRuns + 1 < 0xFFFFFFF0ull) {
         const size_t len = nRuns + 1;
         if (len > h->runLen) {
@@ -1401,61 +1472,42 @@ int storm_cuda_phase_comb(StormHandle *h) {
             h->longCap = longNeed;
         }
         if (!h->bucketFlags) CK(dalloc(h, &h->bucketFlags, 2));
-        launch_bucket_sort(h->stream, h->keys, n, pidBits, static_cast<uint32_t>(nRuns), start, h->runCursor,
-                           h->runScan, h->keysAlt, h->valsAlt, h->longRuns, static_cast<uint32_t>(h->longCap),
-                           h->bucketFlags);
+        launch_bucket_sort(h->stream, h->C, h->bankC, h->keys, n, pidBits, static_cast<uint32_t>(nRuns), start,
+                           h->runCursor, h->runScan, h->keysAlt, h->valsAlt, wS, h->longRuns,
+                           static_cast<uint32_t>(h->longCap), h->bucketFlags);
         h->launches += 7;
-        CK(cudaGetLastError());
-        uint32_t flags[2] = {0, 0};
-        CK(cudaMemcpyAsync(flags, h->bucketFlags, sizeof(flags), cudaMemcpyDeviceToHost, h->stream));
-        int rc = read_checked(h, &nValid, start + nRuns, sizeof(uint32_t));
-        if (rc != STORM_OK) return rc;
-        if (flags[1] == 0) {
-            skeys = h->keysAlt;
-            idx = h->valsAlt;
-            haveValid = true;
-        }
-    }
-    if (!haveValid) {
-        const int alt = launch_radix_sort(h->stream, h->keys, h->vals, h->keysAlt, h->valsAlt, n, pidBits + cellBits,
-                                          h->tileHist);
-        skeys = alt ? h->keysAlt : h->keys;
-        idx = alt ? h->valsAlt : h->vals;
-        launch_comb_ranges(h->stream, skeys, n, static_cast<uint32_t>(nRuns), start, pidBits);
-        h->launches += 5 * ((pidBits + cellBits + 7) / 8) + 1;
-    }
-    // census weights in sorted order; the plan overwrites each slot with the copies' weight
-    double *wS = h->pWeight;
-    launch_sorted_weights(h->stream, h->C, h->bankC, idx, n, wS);
-    if (strat) launch_strat_sums(h->stream, wS, start, N, B, h->stratBinW, h->combW);
-    else launch_comb_cell_sums(h->stream, wS, start, N, h->combW);
-    launch_blocked_sum(h->stream, h->combW, N, h->combWtot);
-    CombParams P;
-    P.nmin = h->desc.comb_nmin;
-    P.ntotal = static_cast<uint64_t>(static_cast<double>(static_cast<uint64_t>(N) * h->desc.comb_nmin) * h->desc.comb_factor);
-    if (strat)
-        launch_strat_plan(h->stream, h->C, P, h->strat, wS, start, h->stratBinW, h->combW, h->combWtot, h->pCount,
-                          h->pWeight, h->combCount, h->A.eradCensus, h->dStats);
-    else
-        launch_comb_plan(h->stream, h->C, P, wS, start, h->combW, h->combWtot, h->pCount, h->pWeight,
-                         h->combCount, h->A.eradCensus, h->dStats);
-    h->launches += 1 + 4;
-    CK(cudaGetLastError());
-    if (!haveValid) {
-        int rc = read_checked(h, &nValid, start + nRuns, sizeof(uint32_t));
-        if (rc != STORM_OK) return rc;
-    }
-    uint64_t *countU64 = skeys == h->keysAlt ? h->keys : h->keysAlt;   // the sort's spare key buffer
-    if (nValid) {
-        launch_mask_count(h->stream, h->pCount, nValid, countU64);
-        launch_scan_u64(h->stream, countU64, nValid, h->pOff, h->pTiles, h->dTotalU64);
-        h->launches += 4;
+        skeys = h->keysAlt;
+        idx = h->valsAlt;
+        bucket = true;
     } else {
-        CK(cudaMemsetAsync(h->dTotalU64, 0, sizeof(uint64_t), h->stream));
+        radix_sort();
     }
+    plan_and_scan();
     CK(cudaGetLastError());
+    uint32_t flags[2] = {0, 0};
+    uint32_t nValid = 0;
     uint64_t total = 0;
-    CK(read_small(h, &total, h->dTotalU64, sizeof(uint64_t)));
+    {
+        const Readback r[3] = {{&nValid, start + nRuns, sizeof(uint32_t)}, {&total, h->dTotalU64, sizeof(uint64_t)},
+                               {flags, h->bucketFlags, sizeof(flags)}};
+        const int rc = read_many(h, r, bucket ? 3 : 2, true);
+        if (rc != STORM_OK) return rc;
+    }
+    if (bucket && flags[1]) {
+        // a run too long for the bucket sort: sort by radix and plan again (the
+        // plan adds the census energy to the step statistics, so that restarts)
+        CK(cudaMemsetAsync(&h->dStats->eCensusOut, 0, sizeof(double), h->stream));
+        // the keys again: the first plan's copy counts went to their buffer
+        if (strat) launch_strat_keys(h->stream, h->C, h->bankC, n, h->keys, h->vals, combKey, pidBits, h->strat);
+        else launch_comb_keys(h->stream, h->C, h->bankC, n, h->keys, h->vals, combKey, pidBits);
+        ++h->launches;
+        radix_sort();
+        plan_and_scan();
+        CK(cudaGetLastError());
+        const Readback r[2] = {{&nValid, start + nRuns, sizeof(uint32_t)}, {&total, h->dTotalU64, sizeof(uint64_t)}};
+        const int rc = read_many(h, r, 2, true);
+        if (rc != STORM_OK) return rc;
+    }
     // The write goes to bank A, which transport has finished with.  When the
     // combed census outgrows the banks, A and B are replaced first (their
     // contents are dead); C and the comb buffers, which the write still reads,
@@ -1511,8 +1563,7 @@ int storm_cuda_phase_poststep(StormHandle *h, double dt) {
 int storm_cuda_phase_stats(StormHandle *h, StormStepStats *s) {
     if (!h || !s) return STORM_ERR_INVALID_ARG;
     DevStats d{};
-    CK(cudaMemcpyAsync(&d, h->dStats, sizeof(d), cudaMemcpyDeviceToHost, h->stream));
-    CK(cudaStreamSynchronize(h->stream));
+    CK(read_small(h, &d, h->dStats, sizeof(d)));
     *s = h->stats;
     s->segments = d.segments;
     s->rw_steps = d.rwSteps;
