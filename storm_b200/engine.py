@@ -343,7 +343,7 @@ class Server:
     """Many independent problems on one GPU (storm_server_*): requests queue,
     are admitted by slots and an HBM budget, and advance concurrently."""
 
-    def __init__(self, max_active=16, workers=8, hbm_budget_bytes=0, device=0):
+    def __init__(self, max_active=6, workers=3, hbm_budget_bytes=0, device=0):
         cfg = A.StormServerConfig(device, max_active, workers, 0, hbm_budget_bytes)
         h = C.c_void_p()
         rc = lib().storm_server_create(C.byref(cfg), C.byref(h))
