@@ -146,7 +146,6 @@ void launch_comb_emit_out(cudaStream_t s, const Ctx &C, const CensusBank &cen, c
                           const uint64_t *sortedKeys, int pidBits, uint32_t bins, uint32_t nValid, uint32_t total,
                           const uint32_t *pCount, const double *pWeight, const uint64_t *pOffset, uint32_t *src,
                           uint32_t *tileMax, const Bank &out);
-void launch_mask_count(cudaStream_t s, const uint32_t *pCount, uint32_t n, uint64_t *out);
 void launch_allocate_checked(cudaStream_t s, const Ctx &C, const CellArrays &A, const double *total,
                              uint64_t newPerCell, double rel, int32_t *ambiguous);
 size_t radix_scratch_words(uint32_t n);

@@ -2369,11 +2369,7 @@ __global__ void k_strat_plan(Ctx C, CombParams P, StratParams S, const double *w
     if ((threadIdx.x & 31) == 0 && eOut != 0.0) atomicAdd(&st->eCensusOut, eOut);
 }
 
-__global__ void k_mask_count(const uint32_t *pCount, uint32_t n, uint64_t *out) {
-    for (uint32_t q = blockIdx.x * blockDim.x + threadIdx.x; q < n; q += gridDim.x * blockDim.x)
-        out[q] = pCount[q] & ~KEEP;
-}
-// the same over n slots of which the first *nValid are particles (zero beyond)
+// copies per sorted slot, over n slots of which the first *nValid are particles (zero beyond)
 __global__ void k_mask_count_upto(const uint32_t *pCount, uint32_t n, const uint32_t *nValid, uint64_t *out) {
     const uint32_t v = *nValid;
     for (uint32_t q = blockIdx.x * blockDim.x + threadIdx.x; q < n; q += gridDim.x * blockDim.x)
@@ -2764,9 +2760,6 @@ void launch_comb_emit_out(cudaStream_t s, const Ctx &C, const CensusBank &cen, c
     else
         k_comb_emit_out<false><<<grid_for(total, 256, 148 * 16), 256, 0, s>>>(C, cen, idx, sortedKeys, pidBits, bins,
                                                                               total, src, pCount, pWeight, out);
-}
-void launch_mask_count(cudaStream_t s, const uint32_t *pCount, uint32_t n, uint64_t *out) {
-    k_mask_count<<<grid_for(n, 256, 8192), 256, 0, s>>>(pCount, n, out);
 }
 void launch_mask_count_upto(cudaStream_t s, const uint32_t *pCount, uint32_t n, const uint32_t *nValid, uint64_t *out) {
     k_mask_count_upto<<<grid_for(n, 256, 8192), 256, 0, s>>>(pCount, n, nValid, out);
