@@ -1009,9 +1009,10 @@ int storm_cuda_create(const StormProblemDesc *d, StormHandle **out) {
     // Segments between refills of the persistent transport kernel, measured on
     // B200: multigroup histories are short (about 3.6 segments at 128^3 x 64
     // groups), and lanes idle to the end of a burst once theirs ends, so
-    // multigroup problems refill after 2 segments (FP32 +23%, FP64 +53% over
-    // 8); polyhedral meshes after 4 (+3%); gray Cartesian grids after 8.
-    h->burst = mg ? 2u : (poly ? 4u : 8u);
+    // multigroup problems refill after every segment (against 8: FP32 +23%,
+    // FP64 +53% at 2 and a further +28% at 1); polyhedral meshes after 4 (+3%
+    // over 8); gray Cartesian grids after 8 (4, 6, 12 and 16 were not faster).
+    h->burst = mg ? 1u : (poly ? 4u : 8u);
     {
         // one attribute (cudaGetDeviceProperties queries them all and can take milliseconds)
         int sms = 0;
