@@ -54,3 +54,22 @@ def test_admission_respects_slots_and_budget():
     assert st["peak_device_bytes"] <= st["budget_bytes"] == 1 << 30
     # with two slots, later requests waited in the queue
     assert max(r["queued_ms"] for r in res) > 0.0
+
+
+def test_reused_streams_and_memory_give_the_same_result():
+    """A handle created on streams, events, page-locked buffers and device
+    memory that earlier handles of other sizes used (and released) runs its
+    problem exactly as the first handle did, and a repeated request of a size
+    the cache holds makes no new device allocation."""
+    from storm_b200.engine import pool_counters
+    p = problems.uniform_cube(n=12, kappa=50.0, packets_per_step=2e4, seed=21)
+    T0, segs0 = _alone(p, 3)
+    for q, _ in problems.serving_mix(4, n_range=(8, 20), packets_range=(2e3, 3e4), steps_range=(1, 2), seed=9):
+        _alone(q, 1)
+    before = pool_counters()
+    T1, segs1 = _alone(p, 3)
+    after = pool_counters()
+    np.testing.assert_allclose(T1, T0, rtol=1e-9)
+    assert abs(segs1 - segs0) <= 1e-6 * segs0 + 2
+    assert after["mallocs"] == before["mallocs"]
+    assert after["live_bytes"] == before["live_bytes"]
