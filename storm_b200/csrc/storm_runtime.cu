@@ -9,7 +9,6 @@
 #include <cstring>
 #include <map>
 #include <mutex>
-#include <set>
 #include <string>
 #include <unordered_map>
 #include <vector>
@@ -151,12 +150,13 @@ int cuda_fail(StormHandle *h, cudaError_t e, const char *what) {
 // instead and are handed to the next allocation of about the same size
 // (at most 25% larger) on the same device.  A handle frees only after its own
 // stream is idle, so a reused block has no work in flight.
-// A miss allocates stream-ordered (cudaMallocAsync on the asking handle's
-// stream, from the device's default pool with its release threshold raised so
-// it keeps what it maps): plain cudaMalloc, called while other handles'
-// kernels ran, was measured to stall for up to hundreds of milliseconds.  When
-// the allocation runs out of memory the device's cached blocks are released
-// and it retries.
+// A miss allocates stream-ordered (cudaMallocFromPoolAsync on the asking
+// handle's stream, from the engine's own memory pool on the device, which
+// keeps what it maps): plain cudaMalloc, called while other handles' kernels
+// ran, was measured to stall for up to hundreds of milliseconds.  The device's
+// default pool, which other code in the process may use, is left as it is.
+// When the allocation runs out of memory the device's cached blocks are
+// released and it retries.
 class DevicePool {
 public:
     cudaError_t alloc(void **p, size_t bytes, cudaStream_t stream) {
@@ -174,12 +174,12 @@ public:
                 return cudaSuccess;
             }
         }
-        keep_mapped(dev);
-        cudaError_t e = cudaMallocAsync(p, want, stream);
+        cudaMemPool_t mp = engine_pool(dev);
+        cudaError_t e = mp ? cudaMallocFromPoolAsync(p, want, mp, stream) : cudaMalloc(p, want);
         if (e == cudaErrorMemoryAllocation) {
             cudaGetLastError();
             release(dev);
-            e = cudaMallocAsync(p, want, stream);
+            e = mp ? cudaMallocFromPoolAsync(p, want, mp, stream) : cudaMalloc(p, want);
         }
         if (e != cudaSuccess) return e;
         std::lock_guard<std::mutex> lk(m_);
@@ -234,17 +234,28 @@ public:
     }
 
 private:
-    // the default pool of `dev` keeps the memory it has mapped (its release
-    // threshold is 0 by default, which returns memory at every synchronisation)
-    void keep_mapped(int dev) {
+    // The engine's memory pool on `dev`, created on first use with a release
+    // threshold above any size, so it keeps the memory it has mapped (the
+    // default threshold, 0, returns memory at every synchronisation); null if
+    // the device cannot make one (then plain cudaMalloc).
+    cudaMemPool_t engine_pool(int dev) {
         std::lock_guard<std::mutex> lk(m_);
-        if (pools_.count(dev)) return;
-        cudaMemPool_t mp;
-        if (cudaDeviceGetDefaultMemPool(&mp, dev) == cudaSuccess) {
+        auto it = pools_.find(dev);
+        if (it != pools_.end()) return it->second;
+        cudaMemPool_t mp = nullptr;
+        cudaMemPoolProps props{};
+        props.allocType = cudaMemAllocationTypePinned;
+        props.location.type = cudaMemLocationTypeDevice;
+        props.location.id = dev;
+        if (cudaMemPoolCreate(&mp, &props) == cudaSuccess) {
             uint64_t threshold = ~0ull;
             cudaMemPoolSetAttribute(mp, cudaMemPoolAttrReleaseThreshold, &threshold);
+        } else {
+            cudaGetLastError();
+            mp = nullptr;
         }
-        pools_.insert(dev);
+        pools_.emplace(dev, mp);
+        return mp;
     }
     static size_t round_up(size_t bytes) {
         if (bytes <= (1u << 20)) {
@@ -260,7 +271,7 @@ private:
     std::multimap<std::pair<int, size_t>, void *> free_;
     size_t cached_ = 0;
     uint64_t mallocs_ = 0, frees_ = 0;
-    std::set<int> pools_;
+    std::map<int, cudaMemPool_t> pools_;
 };
 
 DevicePool &device_pool() {

@@ -73,3 +73,17 @@ def test_reused_streams_and_memory_give_the_same_result():
     assert abs(segs1 - segs0) <= 1e-6 * segs0 + 2
     assert after["mallocs"] == before["mallocs"]
     assert after["live_bytes"] == before["live_bytes"]
+
+
+def test_release_cached_returns_the_cache():
+    """storm_cuda_release_cached hands the cached device blocks back to the
+    driver; a later handle allocates afresh and still runs."""
+    from storm_b200.engine import pool_counters, release_cached
+    p = problems.uniform_cube(n=10, kappa=5.0, packets_per_step=1e4, seed=4)
+    T0, _ = _alone(p, 2)
+    released = release_cached(0)
+    c = pool_counters()
+    assert released > 0 and c["cached_bytes"] == 0 and c["live_bytes"] == 0
+    T1, _ = _alone(p, 2)
+    np.testing.assert_allclose(T1, T0, rtol=1e-9)
+    assert pool_counters()["mallocs"] > c["mallocs"]
