@@ -515,12 +515,23 @@ int storm_cuda_launch_count(StormHandle *h, uint64_t *launches);
  * launches and the segments they ran since the last reset. */
 int storm_cuda_set_profiling(StormHandle *h, int on);
 int storm_cuda_transport_timing(StormHandle *h, double *kernel_ms, uint64_t *launches, uint64_t *segments, int reset);
-/* Transport scheduling (autotuner hook).  refill = 1 (default, burst 8): one
+/* Transport scheduling (autotuner hook).  refill = 1 (default): one
  * persistent launch in which each lane takes the next unstarted particle as
- * soon as its history ends, running `burst` segments between refills.
+ * soon as its history ends, running `burst` segments between refills (default
+ * 1 for multigroup problems, 4 on polyhedral meshes, 8 otherwise).
  * refill = 0: bank visits of segments_per_visit segments with survivors
  * compacted between launches. */
 int storm_cuda_set_transport_mode(StormHandle *h, int refill, uint32_t burst);
+/* Online tuning of the refill burst: the next 10 * steps_per_candidate calls
+ * of storm_cuda_step run the bursts 1, 2, 4, 8, 16 and back (16, 8, 4, 2, 1),
+ * steps_per_candidate steps each, and the burst with the most segments per
+ * millisecond of transport is kept.  The burst changes no result (each
+ * history's random stream is keyed by its particle), only the order of the
+ * FP64 tally sums.  steps_per_candidate = 0 stops a tuning in progress and
+ * keeps the current burst. */
+int storm_cuda_autotune_transport(StormHandle *h, uint32_t steps_per_candidate);
+/* The burst in use, and whether a tuning is in progress (1) or not (0). */
+int storm_cuda_transport_burst(StormHandle *h, uint32_t *burst, int *tuning);
 /* Transport kernel variant (autotuner hook): the occupancy target of the
  * kernel (__launch_bounds__ minimum blocks per SM, 1-4) and the grid size in
  * waves of resident blocks. */

@@ -111,6 +111,13 @@ struct StormHandle {
     int minBlocks = 3;               // transport occupancy variant (__launch_bounds__ min blocks); 4 for FP32
     int refill = 1;                  // 1: persistent refill kernel, 0: bank visits of K segments
     uint32_t burst = 8;              // refill kernel: segments between refills
+    // online burst tuning (storm_cuda_autotune_transport): step k of the
+    // palindromic schedule runs kTuneBursts[order(k)]
+    struct {
+        uint32_t perCandidate = 0, step = 0;   // perCandidate 0: not tuning
+        uint64_t segments[5] = {};
+        double ms[5] = {};
+    } tune;
     int smCount = 148;
     uint32_t transportGrid = 0;      // resident blocks of the chosen variant x SMs
     uint64_t launches = 0;
@@ -714,6 +721,11 @@ uint32_t grid_transport(uint64_t n, uint32_t resident) {
     if (g < 1) g = 1;
     return static_cast<uint32_t>(g < cap ? g : cap);
 }
+
+// refill bursts tried by storm_cuda_autotune_transport, and the candidate of schedule phase p
+constexpr uint32_t kTuneBursts[5] = {1, 2, 4, 8, 16};
+constexpr uint32_t kTunePhases = 10;   // 1 2 4 8 16 16 8 4 2 1: a linear drift over the steps cancels
+uint32_t tune_candidate(uint32_t phase) { return phase < 5 ? phase : 9 - phase; }
 
 }  // namespace
 
@@ -1625,6 +1637,30 @@ int storm_cuda_step(StormHandle *h, double dt, StormStepStats *stats) {
         cudaEventElapsedTime(&ms, h->evTransport1, h->evAfterComb);
         h->lastCombMs = ms;
     }
+    if (rc == STORM_OK && h->tune.perCandidate) {
+        // credit this step to the burst it ran with, then move along the schedule
+        DevStats d{};
+        CK(read_small(h, &d, h->dStats, sizeof(d)));
+        const uint32_t c = tune_candidate(h->tune.step / h->tune.perCandidate);
+        h->tune.segments[c] += d.segments;
+        h->tune.ms[c] += h->lastTransportMs;
+        ++h->tune.step;
+        if (h->tune.step >= kTunePhases * h->tune.perCandidate) {
+            uint32_t best = h->burst;
+            double bestRate = -1.0;
+            for (uint32_t q = 0; q < 5; ++q) {
+                const double rate = h->tune.ms[q] > 0.0 ? static_cast<double>(h->tune.segments[q]) / h->tune.ms[q] : 0.0;
+                if (rate > bestRate) {
+                    bestRate = rate;
+                    best = kTuneBursts[q];
+                }
+            }
+            h->burst = best;
+            h->tune = {};
+        } else {
+            h->burst = kTuneBursts[tune_candidate(h->tune.step / h->tune.perCandidate)];
+        }
+    }
     if (stats) storm_cuda_phase_stats(h, stats);
     return rc;
 }
@@ -2102,6 +2138,23 @@ int storm_cuda_transport_timing(StormHandle *h, double *ms, uint64_t *launches, 
         h->profLaunches = 0;
         h->profSegments = 0;
     }
+    return STORM_OK;
+}
+
+int storm_cuda_autotune_transport(StormHandle *h, uint32_t steps_per_candidate) {
+    if (!h || steps_per_candidate > 1000) return STORM_ERR_INVALID_ARG;
+    h->tune = {};
+    if (steps_per_candidate == 0) return STORM_OK;
+    h->refill = true;
+    h->tune.perCandidate = steps_per_candidate;
+    h->burst = kTuneBursts[tune_candidate(0)];
+    return STORM_OK;
+}
+
+int storm_cuda_transport_burst(StormHandle *h, uint32_t *burst, int *tuning) {
+    if (!h || !burst || !tuning) return STORM_ERR_INVALID_ARG;
+    *burst = h->burst;
+    *tuning = h->tune.perCandidate ? 1 : 0;
     return STORM_OK;
 }
 

@@ -64,6 +64,8 @@ def lib():
         L.storm_cuda_set_profiling.argtypes = [vp, C.c_int]
         L.storm_cuda_set_transport_variant.argtypes = [vp, C.c_int, C.c_int]
         L.storm_cuda_set_transport_mode.argtypes = [vp, C.c_int, C.c_uint32]
+        L.storm_cuda_autotune_transport.argtypes = [vp, C.c_uint32]
+        L.storm_cuda_transport_burst.argtypes = [vp, u32p, C.POINTER(C.c_int)]
         L.storm_cuda_transport_timing.argtypes = [vp, dp, u64p, u64p, C.c_int]
         L.storm_cuda_release_cached.argtypes = [C.c_int, u64p]
         L.storm_cuda_pool_counters.argtypes = [u64p, u64p, u64p, u64p]
@@ -334,6 +336,17 @@ class Engine:
 
     def set_transport_mode(self, refill=True, burst=4):
         self._check(lib().storm_cuda_set_transport_mode(self.h, int(refill), burst))
+
+    def autotune_transport(self, steps_per_candidate=1):
+        """Tune the refill burst over the next 10 * steps_per_candidate steps
+        (storm_cuda_autotune_transport); 0 stops a tuning in progress."""
+        self._check(lib().storm_cuda_autotune_transport(self.h, steps_per_candidate))
+
+    def transport_burst(self):
+        """(burst in use, tuning in progress)."""
+        b, t = C.c_uint32(), C.c_int()
+        self._check(lib().storm_cuda_transport_burst(self.h, C.byref(b), C.byref(t)))
+        return b.value, bool(t.value)
 
     def set_segments_per_visit(self, k):
         self._check(lib().storm_cuda_set_segments_per_visit(self.h, k))
