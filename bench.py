@@ -514,9 +514,16 @@ def run_storm(args, ws, rank, local, dist):
         # gives rms z <= 1 (= 1 if its histories were independent of the FP64 run's)
         sigma_diff = np.sqrt(np.mean((T64 - T64b)[hot] ** 2))
         z = (T32 - T64)[hot] / sigma_diff
+        # the same statistics for the two FP64 runs: sigma_diff is one number for
+        # all cells, so cells whose own scatter is wider (the wave front) sit in
+        # the tail of both; the FP32 form's tail is read against this one
+        zc = (T64b - T64)[hot] / sigma_diff
         dev = {"quantity": "per-cell material temperature after warm-up + timed steps",
                "rms_z": float(np.sqrt(np.mean(z ** 2))), "mean_z": float(np.mean(z)),
                "max_abs_z": float(np.max(np.abs(z))),
+               "frac_abs_z_above_3": float(np.mean(np.abs(z) > 3.0)),
+               "fp64_pair_max_abs_z": float(np.max(np.abs(zc))),
+               "fp64_pair_frac_abs_z_above_3": float(np.mean(np.abs(zc) > 3.0)),
                "z": "(T_fp32 - T_fp64) / sigma_diff per hot cell (T > 2 T_min)",
                "sigma_diff": "rms of T_fp64(seed) - T_fp64(seed + 1000) over the same cells",
                "cells": int(hot.sum())}
