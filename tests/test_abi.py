@@ -124,6 +124,26 @@ def test_server_without_device_fails_loudly():
     assert engine.lib().storm_server_create(C.byref(cfg), C.byref(h)) == 7   # STORM_ERR_NO_DEVICE
 
 
+def test_memory_cache_calls_without_device():
+    """The device memory cache's counters read without a GPU (nothing allocated);
+    releasing it needs a device and says so."""
+    import torch
+    if torch.cuda.is_available():
+        pytest.skip("a GPU is visible")
+    c = engine.pool_counters()
+    assert set(c) == {"mallocs", "frees", "cached_bytes", "live_bytes"}
+    assert all(isinstance(v, int) and v >= 0 for v in c.values())
+    with pytest.raises(engine.StormError):
+        engine.release_cached(0)
+
+
+def test_tuning_calls_reject_a_null_handle():
+    L = engine.lib()
+    b, t = C.c_uint32(), C.c_int()
+    assert L.storm_cuda_autotune_transport(None, 1) == 1   # STORM_ERR_INVALID_ARG
+    assert L.storm_cuda_transport_burst(None, C.byref(b), C.byref(t)) == 1
+
+
 def test_serving_mix_is_seeded():
     a = problems.serving_mix(8)
     b = problems.serving_mix(8)
