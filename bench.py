@@ -45,6 +45,7 @@ def parse():
     ap.add_argument("--impl", default="storm", choices=["storm", "reference"])
     ap.add_argument("--n", type=int, default=64, help="cells per axis")
     ap.add_argument("--e2e-steps", type=int, default=3)
+    ap.add_argument("--dev-seeds", type=int, default=8, help="seeds per form of the FP32-vs-FP64 deviation study")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--segments-per-visit", type=int, default=0)
     ap.add_argument("--min-blocks", type=int, default=0, help="transport occupancy variant (1-4)")
@@ -71,10 +72,12 @@ def workload(n=64, seed=42):
 
 
 def workload_config(n):
+    """The workload both arms report (identical dicts): what each arm computes
+    it in, and on how many processes, is stated outside `config`."""
     return {"workload": f"step_cube {n}^3 gray IMC, kappa_a=1|1000 1/cm, RW kappa*dx>10, dt=1e-11 s, "
                         f"3 photons/cell + 450/face source, comb Nmin=20 factor=2",
             "cells": n ** 3, "packets_per_step": "~1e7", "census_per_step": "~1e7",
-            "l2": "inputs larger than L2 (particle bank ~1 GB)", "precision": "fp64"}
+            "l2": "inputs larger than L2 (particle bank ~1 GB)"}
 
 
 # ---------------------------------------------------------------------- clocks
@@ -168,22 +171,23 @@ def barrier(dist, impl):
 
 # ---------------------------------------------------------------------- CPU baseline
 def _ref_worker(q):
-    """One bounded sample of the workload on the reference's serial path:
-    3 time steps of the same 64^3 cube at 1 photon per cell (2.7e6 packets/step)
-    and 30 per boundary face; the last 2 steps are timed."""
-    seed, steps, use_ref, n = q
+    """One bounded sample of the bench's own workload (the same cube, packet
+    densities and comb as `workload`) on the reference's serial path: `steps`
+    IMC steps from the initial state, the last `timed` of them timed (the
+    manager's own step wall time)."""
+    seed, steps, timed, use_ref, n = q
     sys.path.insert(0, ROOT)
-    from storm_b200 import problems
-    p = problems.step_cube(n=n, new_photons_per_cell=1, face_packets=30, comb_nmin=2, comb_factor=2.0, seed=seed)
+    p = workload(n, seed=seed)
     if use_ref:
         from oracle import ref
         m = ref.Reference(p)
         segs, wall = 0, 0.0
         for s in range(steps):
             o = m.step()
-            if s > 0:
+            if s >= steps - timed:
                 segs += o["segments"]
                 wall += o["wall_seconds"]
+        m.close()
         return segs, wall
     from oracle import orc
     m = orc.Oracle(p)
@@ -192,30 +196,35 @@ def _ref_worker(q):
         t = time.perf_counter()
         st = m.step()
         dt = time.perf_counter() - t
-        if s > 0:
+        if s >= steps - timed:
             segs += st["segments"]
             wall += dt
     return segs, wall
 
 
-def cpu_baseline(n, cores, steps=3):
+def cpu_baseline(n, cores, steps=1, timed=1):
+    """The reference's serial path on `cores` independent processes (one core
+    each), each running `steps` IMC steps of the bench's workload and timing the
+    last `timed`.  Rate = all processes' segments / the slowest process's time."""
     from oracle import ref, orc
     use_ref = ref.available()
     if not use_ref and not os.path.exists(orc.LIB_PATH):
         subprocess.run(["make", "-C", os.path.join(ROOT, "oracle"), "oracle"], check=True, capture_output=True)
     import multiprocessing as mp
     ctx = mp.get_context("spawn")
-    jobs = [(1000 + k, steps, use_ref, n) for k in range(cores)]
+    jobs = [(1000 + k, steps, timed, use_ref, n) for k in range(cores)]
     if cores == 1:
         res = [_ref_worker(jobs[0])]
     else:
-        with ctx.Pool(cores) as pool:
+        with ctx.Pool(cores, maxtasksperchild=1) as pool:
             res = pool.map(_ref_worker, jobs)
     segs = sum(r[0] for r in res)
     wall = max(r[1] for r in res)
+    which = "IMC step 1 (from the initial state)" if steps == 1 else \
+        f"IMC step{'s' if timed > 1 else ''} {steps - timed + 1}-{steps} after {steps - timed} untimed"
     return {"value": segs / wall, "unit": UNIT, "cores": cores, "kind": "reference" if use_ref else "port",
-            "sample": f"{cores} process(es) x {steps - 1} timed IMC steps of the {n}^3 cube at 1 photon/cell "
-                      f"(2.7e6 packets/step), 30/face, comb Nmin=2; {segs} segments in {wall:.1f} s"}
+            "sample": f"{cores} process(es), one core each, {which} of the bench workload ({workload_config(n)['workload']}); "
+                      f"{segs} segments in {wall:.1f} s"}
 
 
 # ---------------------------------------------------------------------- storm arm
@@ -502,48 +511,37 @@ def run_storm(args, ws, rank, local, dist):
 
     v32, ms32 = rate(f32)
     v64, ms64 = rate(f64)
-    # FP32 vs FP64 on the same Philox streams, against the seed-to-seed scatter of the FP64 form
-    dev = None
-    if rank == 0:
-        T32 = f32["engine"].cells()["temperature"]
-        T64 = f64["engine"].cells()["temperature"]
-        other = run_form(args, A.PRECISION_FP64, seed + 1000, local, None, timed=True)
-        T64b = other["engine"].cells()["temperature"]
-        hot = T64 > 2.0 * T64.min()
-        # sigma of a difference of two independent runs: an unbiased FP32 form
-        # gives rms z <= 1 (= 1 if its histories were independent of the FP64 run's)
-        sigma_diff = np.sqrt(np.mean((T64 - T64b)[hot] ** 2))
-        z = (T32 - T64)[hot] / sigma_diff
-        # the same statistics for the two FP64 runs: sigma_diff is one number for
-        # all cells, so cells whose own scatter is wider (the wave front) sit in
-        # the tail of both; the FP32 form's tail is read against this one
-        zc = (T64b - T64)[hot] / sigma_diff
-        dev = {"quantity": "per-cell material temperature after warm-up + timed steps",
-               "rms_z": float(np.sqrt(np.mean(z ** 2))), "mean_z": float(np.mean(z)),
-               "max_abs_z": float(np.max(np.abs(z))),
-               "frac_abs_z_above_3": float(np.mean(np.abs(z) > 3.0)),
-               "fp64_pair_max_abs_z": float(np.max(np.abs(zc))),
-               "fp64_pair_frac_abs_z_above_3": float(np.mean(np.abs(zc) > 3.0)),
-               "z": "(T_fp32 - T_fp64) / sigma_diff per hot cell (T > 2 T_min)",
-               "sigma_diff": "rms of T_fp64(seed) - T_fp64(seed + 1000) over the same cells",
-               "cells": int(hot.sum())}
-        other["engine"].close()
-    e2e = e2e_run(args, f32["engine"], f32["problem"], dist) if args.e2e_steps > 0 else None
+    f32["engine"].close()
+    f64["engine"].close()
+    dev = deviation_study(args, local) if (rank == 0 and args.dev_seeds > 1) else None
+    e2e = None
+    if args.e2e_steps > 0:
+        from storm_b200.engine import Engine
+        p = workload(args.n, seed=seed)
+        p.device, p.precision, p.per_cell_segment_counters = local, A.PRECISION_FP32_TRACK, False
+        eng = Engine(p)
+        for _ in range(args.warmup):
+            eng.step()
+        e2e = e2e_run(args, eng, p, dist)
+        eng.close()
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
-        cpu = cpu_baseline(args.n, 1)
+        cpu = cpu_baseline(args.n, 1, steps=1, timed=1)
     serving = serving_run(args) if (rank == 0 and ws == 1 and args.serving_requests > 0) else None
     multigroup = mg_run(args) if (rank == 0 and ws == 1 and args.mg_steps > 0) else None
     voronoi = voronoi_run(args) if (rank == 0 and ws == 1 and args.voronoi_steps > 0) else None
     if rank == 0:
         lat = sorted(f32["step_ms"])
         line = {
-            "metric": METRIC, "value": v32, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
+            "metric": METRIC, "value": v32, "fp64_value": v64, "fp32_over_fp64": v32 / v64, "unit": UNIT,
+            "n_gpus": ws, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms32 / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32-track/f64-tally",
+            "form": "value: FP32 cell-local tracking with FP64 time, weights and tallies; "
+                    "fp64_value: the all-FP64 form on the same workload",
+            "parallelism": f"{ws} independent problem(s), one per GPU",
             "data": "synthetic (seeded Philox streams)",
-            "config": workload_config(args.n) | {"parallelism": f"{ws} independent problem(s), one per GPU",
-                                                 "form": "FP32 cell-local tracking, FP64 time/weights/tallies"},
+            "config": workload_config(args.n),
             "latency_ms": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99))},
             "segments_per_step": f32["segments"] / args.steps,
             "phase_ms_per_step": f32["phase_ms"],
@@ -554,46 +552,95 @@ def run_storm(args, ws, rank, local, dist):
                      "segments_per_step": f64["segments"] / args.steps,
                      "phase_ms_per_step": f64["phase_ms"],
                      "roofline": roofline(f64, BYTES_PER_SEGMENT_FP64, transport_kernel(args, False))},
-            "fp32_over_fp64": v32 / v64,
             "fp32_vs_fp64_deviation": dev,
             "cpu_baseline": cpu, "e2e": e2e, "serving": serving, "multigroup": multigroup, "voronoi": voronoi, "clocks": ck,
             "gpu_launches": f32["launches"],
             "transport_share": f32["transport"]["kernel_ms"] / max(sum(f32["step_ms"]), 1e-9),
         }
         print(json.dumps(line), flush=True)
-    f32["engine"].close()
-    f64["engine"].close()
     if dist is not None:
         dist.destroy_process_group()
 
 
+def deviation_study(args, local):
+    """The FP32-tracking form's deviation from the FP64 form, in units of the
+    batch-estimated statistical error.  Both forms run the bench workload
+    (warm-up + timed step count) on the same `dev_seeds` seeds, i.e. on the
+    same Philox streams; a second FP64 batch on other seeds is the control.
+    Per cell and per quantity (material temperature, the last step's deposit,
+    time-averaged and census radiation energy) the difference of batch means is
+    a Welch z (storm_b200.batchstats); reported: the fraction of populated
+    cells within 1, 2 and 3 sigma, the largest |z| against its Bonferroni
+    bound, and the same for FP64 against FP64."""
+    import numpy as np
+    from storm_b200 import _abi as A
+    from storm_b200 import batchstats
+    from storm_b200.engine import Engine
+    steps = args.warmup + args.steps
+
+    def batch(precision, seeds):
+        out = []
+        for s in seeds:
+            p = workload(args.n, seed=s)
+            p.device, p.precision, p.per_cell_segment_counters = local, precision, False
+            e = Engine(p)
+            out.append(batchstats.run_snapshots(e, p, steps, (steps,)))
+            e.close()
+        return np.array(out)
+
+    seeds = range(42, 42 + args.dev_seeds)
+    r32 = batch(A.PRECISION_FP32_TRACK, seeds)
+    r64 = batch(A.PRECISION_FP64, seeds)
+    r64b = batch(A.PRECISION_FP64, range(1042, 1042 + args.dev_seeds))
+
+    def summary(res):
+        g = res["all"]
+        return {"tests": g["tests"], "frac_within": g["frac_within"], "max_abs_z": g["max_abs_z"],
+                "z_bound": g["z_bound"], "above_3": g["above_threshold"], "k_max": g["k_max"],
+                "mean_z": g["mean_z"], "rms_z": g["rms_z"], "totals_max_abs_z": res["totals"]["max_abs_z"],
+                "passed": res["passed"],
+                "per_quantity_frac_within_1": {q: res[q]["frac_within"]["1"] for q in batchstats.QUANTITIES}}
+    fp32 = summary(batchstats.compare(r32, r64))
+    ctrl = summary(batchstats.compare(r64b, r64))
+    return {"seeds_per_form": args.dev_seeds, "steps": steps,
+            "quantities": list(batchstats.QUANTITIES),
+            "z": "Welch z of the per-cell batch means (normal-equivalent), FP32 vs FP64 on the same seeds",
+            "fp32_vs_fp64": fp32, "fp64_vs_fp64_control": ctrl,
+            "within_1_sigma_like_fp64": bool(fp32["frac_within"]["1"] >= ctrl["frac_within"]["1"] - 0.05),
+            "statement": "FP32 differs from FP64 by no more than FP64 differs from itself over independent seeds"
+                         if fp32["passed"] else "FP32 deviates beyond the statistical error of the FP64 form"}
+
+
 # ---------------------------------------------------------------------- reference arm
+# host memory one reference process holds through IMC step 2 of the 64^3 workload
+REF_PROCESS_BYTES = 9e9
+
+
 def run_reference(args, ws, rank, dist):
+    """The reference's serial path on the bench's exact workload: one process
+    per host core (as many as host memory holds), each running the untimed IMC
+    step 1 and the timed IMC step 2 -- bounded by steps, not by packet
+    density, so that the whole arm takes a couple of minutes whatever
+    --steps / --warmup say."""
     if rank != 0:
         if dist is not None:
             dist.destroy_process_group()
         return
     cores = os.cpu_count() or 1
-    try:   # each reference process holds ~1.5 GB on the 64^3 sample
+    per_process = REF_PROCESS_BYTES * (args.n / 64.0) ** 3
+    try:
         import psutil
-        cores = max(1, min(cores, int(psutil.virtual_memory().available / 1.5e9)))
+        cores = max(1, min(cores, int(psutil.virtual_memory().available * 0.8 / per_process)))
     except ImportError:
         pass
-    from oracle import ref
-    kind = "reference" if ref.available() else "port"
-    # each bench step = one bounded sample per core (3 IMC steps, 2 timed)
-    total_steps = args.warmup + args.steps
-    res = None
-    vals = []
-    for s in range(max(1, min(total_steps, 2))):
-        res = cpu_baseline(args.n, cores)
-        if s >= (1 if total_steps > 1 else 0):
-            vals.append(res["value"])
-    value = statistics.mean(vals) if vals else res["value"]
+    res = cpu_baseline(args.n, cores, steps=2, timed=1)
+    value = res["value"]
     line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws,
             "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded std::mt19937_64 in the reference)",
-            "config": workload_config(args.n) | {"parallelism": f"{cores} independent reference processes"},
+            "form": "the reference's serial FP64 path (MonteCarloManagerSerial + RadiationIMC + CombPopulationControl)",
+            "parallelism": f"{cores} independent reference processes, one host core each",
+            "config": workload_config(args.n),
             "cpu_baseline": res | {"value": value},
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)

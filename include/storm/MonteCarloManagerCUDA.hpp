@@ -11,16 +11,30 @@
 // STORM::StormError, after reportError, like the serial manager
 // (manager/MonteCarloManagerSerial.hpp:458-462).
 //
-// What the plug-ins keep private -- the opacity and EOS models, a boundary's
-// temperatures, the comb's Nmin / factor, the RNG seed, and the cell vectors
-// RadiationIMC holds by reference -- is handed over in a CudaIMCBinding.
-// bind_parameters() copies the public RadiationIMCParameters, the group energy
-// boundaries of a multigroup RadiationIMC included; census frequencies travel
-// with the particles.  An unsupported plug-in is rejected with StormError;
-// there is no CPU fallback.
+// What the plug-ins keep private -- the opacity and EOS models, the comb's
+// Nmin / factor, the RNG seed, and the cell vectors RadiationIMC holds by
+// reference -- is handed over in a CudaIMCBinding.  bind_parameters() copies
+// the public RadiationIMCParameters, the group energy boundaries of a
+// multigroup RadiationIMC included; census frequencies travel with the
+// particles.  A table opacity (CELL_TABLE, MG_POWER's sigma0) is evaluated
+// through the binding's callbacks for every cell before every step, as
+// RadiationIMC::preStep evaluates the opacity plug-in
+// (radiation/RadiationIMC.hpp:1645).
+//
+// The four stock boundaries are recognised by type and lowered to per-box-face
+// actions without the binding: VacuumBoundary (every face escapes),
+// RigidBoundary (every face reflects), SideTemperature (x-low escapes and
+// emits, the rest reflect) and TwoSidesTemperature (both x faces escape and
+// emit, the rest reflect).  The source temperatures and packets per face of the
+// last two are private, so they are read off one batch of the boundary's own
+// packets (generateNewBoundaryParticles) at construction.  Any other boundary
+// takes its faces from the binding.  An unsupported plug-in or option is
+// rejected with StormError; there is no CPU fallback.
 //
 // Include after the reference headers (Particle, MonteCarloPhysics,
-// PopulationControl, BoundaryCondition, MonteCarloConfig, RadiationCell).
+// PopulationControl, BoundaryCondition, MonteCarloConfig, RadiationCell, and
+// the stock boundaries boundary/Vacuum.hpp, RigidBoundary.hpp,
+// SideTemperature.hpp, TwoSidesTemperature.hpp).
 #ifndef STORM_MONTE_CARLO_MANAGER_CUDA_HPP
 #define STORM_MONTE_CARLO_MANAGER_CUDA_HPP
 
@@ -100,11 +114,15 @@ struct CudaIMCBinding {
         ddmcUseMultigroupPGRW = p.ddmcUseMultigroupPGRW;
         ddmcMinCellOpticalDepth = p.ddmcMinCellOpticalDepth;
         ddmcMinParticleOpticalDepth = p.ddmcMinParticleOpticalDepth;
-        if (p.withHydro || p.MMC || p.withCompton) {
+        if (p.withHydro || p.MMC || p.withCompton || p.withEgTimeAvg || p.diffusionPressureGradient ||
+            p.postProcess.enabled) {
             StormError eo("MonteCarloManagerCUDA: RadiationIMC option not supported on the device path");
             eo.addEntry("withHydro", p.withHydro);
             eo.addEntry("MMC", p.MMC);
             eo.addEntry("withCompton", p.withCompton);
+            eo.addEntry("withEgTimeAvg", p.withEgTimeAvg);
+            eo.addEntry("diffusionPressureGradient", p.diffusionPressureGradient);
+            eo.addEntry("postProcess.enabled", p.postProcess.enabled);
             throw eo;
         }
         groupBounds.clear();
@@ -237,6 +255,18 @@ class MonteCarloManagerCUDA {
     using MCParticle = Particle<T, Grid>;
 
 public:
+    // MonteCarloManagerSerial::Tracker (manager/MonteCarloManagerSerial.hpp:46-70).
+    // The device path records no per-segment routes: a census particle with
+    // on_track set makes step() throw StormError, so the tracker stays empty.
+    class Tracker {
+    public:
+        void Reset(void) { track_.clear(); }
+        std::vector<MCParticle> GetTrackParticleRoute(std::size_t) const { return std::vector<MCParticle>(); }
+
+    private:
+        std::vector<MCParticle> track_;
+    };
+
     MonteCarloManagerCUDA(const Grid &grid, const std::shared_ptr<MonteCarloPhysics<T, Grid>> &physics,
                           const std::shared_ptr<PopulationControl<T, Grid>> &populationControl,
                           const std::shared_ptr<BoundaryCondition<T, Grid>> &boundaryCondition,
@@ -266,6 +296,11 @@ public:
             StormStepStats st{};
             cuda_detail::check(storm_cuda_step(h_, fullDt, &st), h_, "storm_cuda_step");
             download_cells();
+            {
+                std::vector<std::uint64_t> begin(N_);
+                cuda_detail::check(storm_cuda_get_beginning_counts(h_, begin.data()), h_, "get_beginning_counts");
+                beginningParticleCount_.assign(begin.begin(), begin.end());
+            }
             std::vector<MCParticle> out = download_census();
             initialParticleCount_ = st.census_in;
             preStepParticleCount_ = st.emitted_cells + st.emitted_faces;
@@ -287,6 +322,11 @@ public:
     inline std::size_t GetPreStepParticleCount(void) const { return preStepParticleCount_; }
     inline std::size_t GetEndParticleCount(void) const { return endParticleCount_; }
     inline double GetPureComputeTime(void) const { return pureComputeTime_; }
+    // particles per cell when the last step's transport began (census + emission)
+    inline const std::vector<std::size_t> &GetBeginningParticleCount(void) const { return beginningParticleCount_; }
+    inline std::vector<std::size_t> &GetBeginningParticleCount(void) { return beginningParticleCount_; }
+    inline const Tracker &getTracker(void) { return tracker_; }
+    inline void resetTracker(void) { tracker_.Reset(); }
     inline double GetWallTime(void) const { return wallTime_; }
     inline std::size_t GetHandlerMemoryBytes(void) const {
         std::uint64_t b = 0;
@@ -376,8 +416,11 @@ private:
         d.eos_kind = binding_.eosKind;
         d.cv_per_mass = binding_.cvPerMass;
         d.eos_f = binding_.eosF; d.eos_beta = binding_.eosBeta; d.eos_mu = binding_.eosMu;
-        for (int f = 0; f < 6; ++f) d.faces[f] = binding_.faces[f];
-        d.escape_without_check = binding_.escapeWithoutCheck;
+        std::array<StormBoxFace, 6> faces = binding_.faces;
+        bool escapeNoCheck = binding_.escapeWithoutCheck;
+        lower_stock_boundary(faces, escapeNoCheck);
+        for (int f = 0; f < 6; ++f) d.faces[f] = faces[f];
+        d.escape_without_check = escapeNoCheck;
         d.new_photons_per_cell = binding_.newPhotonsPerCell;
         d.with_random_walk = binding_.withRandomWalk;
         d.no_hydro_feedback = binding_.noHydroFeedback;
@@ -407,6 +450,79 @@ private:
         cellsStepsCounters_.assign(N, 0);
     }
 
+    // The stock boundaries, recognised by type (see the file comment).
+    void lower_stock_boundary(std::array<StormBoxFace, 6> &faces, bool &escapeNoCheck) {
+        BoundaryCondition<T, Grid> *b = boundary_.get();
+        const StormBoxFace escape{STORM_FACE_ESCAPE, 0, 0.0, 0}, reflect{STORM_FACE_REFLECT, 0, 0.0, 0};
+        if (dynamic_cast<VacuumBoundary<T, Grid> *>(b)) {
+            faces.fill(escape);
+            escapeNoCheck = true;   // VacuumBoundary::apply removes without a face test (boundary/Vacuum.hpp:18-22)
+            return;
+        }
+        if (dynamic_cast<RigidBoundary<T, Grid> *>(b)) {
+            faces.fill(reflect);
+            escapeNoCheck = false;
+            return;
+        }
+        const bool side = dynamic_cast<SideTemperature<T, Grid> *>(b) != nullptr;
+        const bool two = dynamic_cast<TwoSidesTemperature<T, Grid> *>(b) != nullptr;
+        if (!side && !two) return;
+        // SideTemperature::apply removes at x-low and reflects at x-high
+        // (boundary/SideTemperature.hpp:84-112); TwoSidesTemperature::apply
+        // removes at both x faces (boundary/TwoSidesTemperature.hpp:97-123);
+        // every other box face reflects.
+        faces.fill(reflect);
+        faces[0] = escape;
+        if (two) faces[1] = escape;
+        escapeNoCheck = false;
+        if (!(binding_.sigmaSB > 0.0))
+            throw StormError("MonteCarloManagerCUDA: the binding needs sigmaSB to lower a temperature boundary");
+        // Each x-low (x-high) boundary face gets Npercell packets of weight
+        // sigma_SB T^4 A dt / Npercell (:114-163, :126-199); one batch at dt = 1
+        // gives both.  Packets leave the x-low face with vx > 0.
+        const std::size_t N = grid_.GetPointNo();
+        std::size_t xFaces[2] = {0, 0};
+        std::vector<double> xArea(2 * N, 0.0);
+        for (std::size_t i = 0; i < N; ++i) {
+            const auto point = grid_.GetMeshPoint(i);
+            for (const std::size_t &f : grid_.GetCellFaces(i)) {
+                const auto nb = grid_.GetFaceNeighbors(f);
+                const std::size_t o = (nb.first == i) ? nb.second : nb.first;
+                if (!(o >= N && grid_.IsPointOutsideBox(o))) continue;
+                const auto d = grid_.GetMeshPoint(o) - point;
+                const double nx = d.x / std::sqrt(d.x * d.x + d.y * d.y + d.z * d.z);
+                if (std::fabs(nx) <= 0.99) continue;
+                const int sideIdx = nx < 0 ? 0 : 1;
+                ++xFaces[sideIdx];
+                xArea[2 * i + sideIdx] = grid_.GetArea(f);
+            }
+        }
+        const std::vector<MCParticle> probe = b->generateNewBoundaryParticles(1.0);
+        std::size_t count[2] = {0, 0};
+        double weight[2] = {-1.0, -1.0}, area[2] = {0.0, 0.0};
+        for (const MCParticle &q : probe) {
+            const int sideIdx = q.velocity.x > 0 ? 0 : 1;
+            ++count[sideIdx];
+            if (weight[sideIdx] < 0.0 && q.cellIndex < N) {
+                weight[sideIdx] = q.weight;
+                area[sideIdx] = xArea[2 * q.cellIndex + sideIdx];
+            }
+        }
+        for (int sideIdx = 0; sideIdx < (two ? 2 : 1); ++sideIdx) {
+            if (!xFaces[sideIdx] || !count[sideIdx]) continue;
+            const std::size_t perFace = count[sideIdx] / xFaces[sideIdx];
+            if (perFace * xFaces[sideIdx] != count[sideIdx] || !(area[sideIdx] > 0.0)) {
+                StormError eo("MonteCarloManagerCUDA: could not read the boundary's packets per face");
+                eo.addEntry("Packets", count[sideIdx]);
+                eo.addEntry("Boundary faces", xFaces[sideIdx]);
+                throw eo;
+            }
+            const double t4 = weight[sideIdx] * static_cast<double>(perFace) / (binding_.sigmaSB * area[sideIdx]);
+            faces[sideIdx].source_temperature = t4 > 0.0 ? std::sqrt(std::sqrt(t4)) : 0.0;
+            faces[sideIdx].packets_per_face = faces[sideIdx].source_temperature > 0.0 ? perFace : 0;
+        }
+    }
+
     void upload_cells() {
         auto &cells = *binding_.cells;
         auto &ext = *binding_.extensives;
@@ -418,10 +534,29 @@ private:
         }
         cuda_detail::check(storm_cuda_set_cell_state(h_, hostT_.data(), hostE_.data(), hostCE_.data()), h_,
                            "set_cell_state");
+        // the opacity plug-in at this step's cell state (RadiationIMC::preStep, :1645)
+        if (binding_.opacityKind == STORM_OPACITY_CELL_TABLE || binding_.opacityKind == STORM_OPACITY_MG_POWER) {
+            hostSA_.resize(N_);
+            hostSS_.assign(N_, 0.0);
+            const auto &absorption = binding_.opacityKind == STORM_OPACITY_CELL_TABLE ? binding_.planckOpacity
+                                                                                      : binding_.sigma0;
+            for (std::size_t i = 0; i < N_; ++i) {
+                hostSA_[i] = absorption(i);
+                if (binding_.scatteringOpacity) hostSS_[i] = binding_.scatteringOpacity(i);
+            }
+            cuda_detail::check(storm_cuda_set_opacity_tables(h_, hostSA_.data(), hostSS_.data()), h_,
+                               "set_opacity_tables");
+        }
     }
 
     void upload_census(const std::vector<MCParticle> &ps) {
         const std::size_t n = ps.size();
+        for (const MCParticle &p : ps)
+            if (p.on_track) {
+                StormError eo("MonteCarloManagerCUDA: particle tracking (Particle::on_track) is not available on the device path");
+                eo.addEntry("Particle id", p.id);
+                throw eo;
+            }
         std::vector<double> x(n), y(n), z(n), vx(n), vy(n), vz(n), t(n), w(n), w0(n), nu(multigroup_ ? n : 0);
         std::vector<std::uint32_t> cell(n);
         for (std::size_t q = 0; q < n; ++q) {
@@ -491,7 +626,9 @@ private:
     bool multigroup_ = false;
     cuda_detail::PolyMeshArrays poly_;
     std::vector<std::size_t> cellsStepsCounters_;
-    std::vector<double> hostT_, hostE_, hostCE_, eradAvg_, sigmaA_, fleck_;
+    std::vector<double> hostT_, hostE_, hostCE_, hostSA_, hostSS_, eradAvg_, sigmaA_, fleck_;
+    std::vector<std::size_t> beginningParticleCount_;
+    Tracker tracker_;
     std::size_t startParticleCount_ = 0, initialParticleCount_ = 0, preStepParticleCount_ = 0, endParticleCount_ = 0;
     double pureComputeTime_ = 0.0, wallTime_ = 0.0;
 };

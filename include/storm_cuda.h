@@ -372,6 +372,21 @@ int storm_cuda_set_cell_state(StormHandle *h, const double *temperature, const d
  * sigma_s, Fleck factor).  Replay parity uses the reference's own tables. */
 int storm_cuda_set_cell_physics(StormHandle *h, const double *sigma_a, const double *sigma_s,
                                 const double *fleck);
+/* Replace the per-cell opacity plug-in values the next prestep reads
+ * (STORM_OPACITY_CELL_TABLE: sigma_a and sigma_s per cell; STORM_OPACITY_MG_POWER:
+ * sigma0 and the elastic opacity per cell); either pointer may be NULL.  The
+ * reference evaluates opacity_->CalcPlanckOpacity(cell) and
+ * CalcScatteringOpacity(cell) for every cell in every RadiationIMC::preStep
+ * (radiation/RadiationIMC.hpp:1645); a caller whose opacity depends on the
+ * cell state refreshes the tables before each step.  Other opacity kinds
+ * return STORM_ERR_INVALID_ARG. */
+int storm_cuda_set_opacity_tables(StormHandle *h, const double *sigma_a, const double *sigma_s);
+/* Particles per cell when the last step's transport began (the census plus
+ * the step's emission): MonteCarloManagerSerial::GetBeginningParticleCount
+ * (manager/MonteCarloManagerSerial.hpp:81-82, filled at :419-424).  Kept only
+ * for handles created with per_cell_segment_counters; others return
+ * STORM_ERR_INVALID_ARG. */
+int storm_cuda_get_beginning_counts(StormHandle *h, uint64_t *counts);
 /* MarshakBoundary::SetTemperature / SideTemperature::SetTemperature. */
 int storm_cuda_set_face_temperature(StormHandle *h, int face, double temperature);
 
@@ -411,8 +426,13 @@ int storm_cuda_random_walk_sample(StormHandle *h, uint64_t n, const double *xi_l
  * Its scratch is one fixed array inside the library (about 128 KiB per GPU
  * that loads the library, held until exit).  The first call on a device looks
  * up that array's device address; make the first call before any stream
- * capture.  Calls whose work overlaps on the GPU share the array and race.
- * ncells above STORM_NOALLOC_MAX_CELLS returns STORM_ERR_INVALID_ARG. */
+ * capture, and do not use the entry point across a cudaDeviceReset of that
+ * device.  Calls whose work overlaps on the GPU share the array and race.
+ * The whole computation stays on the device (no host readback), including
+ * the exact left-to-right total that ambiguous floors fall back to.
+ * ncells above STORM_NOALLOC_MAX_CELLS returns STORM_ERR_INVALID_ARG; a CUDA
+ * error already pending on the calling thread is left pending and the call
+ * returns STORM_ERR_CUDA without launching. */
 int storm_cuda_emission_allocation_noalloc(int device, const double *d_energy, uint32_t ncells,
                                            uint64_t new_photons_per_cell, uint64_t *d_photons,
                                            uint64_t *d_offsets, void *stream);

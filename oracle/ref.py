@@ -76,6 +76,7 @@ def lib():
         L.ref_isotropic.argtypes = [C.c_uint64, C.c_uint64, dp, dp]
         L.ref_point_on_face.argtypes = [vp, C.c_uint64, u64p, dp, dp]
         L.ref_comb.argtypes = [vp, C.POINTER(A.StormParticlesSoA), C.POINTER(A.StormParticlesSoA), u64p]
+        L.ref_advance_face_stream.argtypes = [vp, C.c_uint64]
         L.ref_units.argtypes = [dp]
         L.ref_planck_integral.restype = C.c_double
         L.ref_planck_integral.argtypes = [C.c_double, C.c_double]
@@ -151,6 +152,11 @@ class Reference:
         out = RefStepOut()
         self._check(lib().ref_step(self.h, self.problem.dt if dt is None else dt, C.byref(out)))
         return out.as_dict()
+
+    def advance_face_stream(self, calls):
+        """Move the process-wide RandomPointOnFace stream forward by `calls`
+        points (independent face-source positions for batch runs)."""
+        self._check(lib().ref_advance_face_stream(self.h, calls))
 
     def prestep_only(self, dt=None):
         n = C.c_uint64()

@@ -564,6 +564,10 @@ RefHandle *ref_create(const StormProblemDesc *d, int boundary_kind, char *err, s
             b->escapeNoCheck = d->escape_without_check != 0;
             b->sigmaSB = d->sigma_sb;
             b->clight = d->clight;
+            // the packets' directions, times and frequencies follow the problem
+            // seed, so runs of different seeds are independent realisations
+            // (SideTemperature keeps a function-static engine seeded with 0)
+            b->re.seed(d->seed);
             if (d->groups >= 2) {
                 b->bounds.assign(d->group_bounds, d->group_bounds + d->groups + 1);
                 b->kBoltz = d->k_boltz;
@@ -865,6 +869,29 @@ int ref_point_on_face(RefHandle *h, uint64_t n, const uint64_t *faces, double *p
         tape[3 * k] = mdist(mirror);
         tape[3 * k + 1] = mdist(mirror);
         tape[3 * k + 2] = mdist(mirror);
+    }
+    return 0;
+}
+
+// The serial manager's GetBeginningParticleCount after its last ref_step.
+int ref_beginning_counts(RefHandle *h, uint64_t *counts) {
+    if (!h->manager) return 1;
+    const auto &v = h->manager->GetBeginningParticleCount();
+    for (std::size_t i = 0; i < v.size(); ++i) counts[i] = v[i];
+    return 0;
+}
+
+// RandomPointOnFace (utils/RandomOnFace.hpp:15-66) draws from a function-static
+// std::mt19937(0) shared by every handle of the process.  Batch runs of
+// different seeds each start a fresh process and move that stream forward by
+// `calls` points first, so that their face-source positions do not repeat.
+int ref_advance_face_stream(RefHandle *h, uint64_t calls) {
+    try {
+        const std::size_t face = h->grid->GetCellFaces(0)[0];
+        for (uint64_t k = 0; k < calls; ++k) (void)STORM::RandomPointOnFace<Vector3D, Grid>(*h->grid, face);
+    } catch (const std::exception &e) {
+        h->lastError = e.what();
+        return 1;
     }
     return 0;
 }

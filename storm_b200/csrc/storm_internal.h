@@ -95,6 +95,10 @@ void launch_rw_eligibility(cudaStream_t s, const Ctx &C, const CellArrays &A);
 void launch_emission_energy(cudaStream_t s, const Ctx &C, const CellArrays &A, double dt);
 void launch_sequential_sum(cudaStream_t s, const double *v, uint32_t n, double *out);
 void launch_allocate(cudaStream_t s, const Ctx &C, const CellArrays &A, const double *total, uint64_t newPerCell);
+// the same two kernels, run only where *onlyIf is nonzero (decided on the device)
+void launch_sequential_sum_if(cudaStream_t s, const double *v, uint32_t n, double *out, const int32_t *onlyIf);
+void launch_allocate_if(cudaStream_t s, const Ctx &C, const CellArrays &A, const double *total, uint64_t newPerCell,
+                        const int32_t *onlyIf);
 void launch_emission_debit(cudaStream_t s, const Ctx &C, const CellArrays &A, DevStats *st);
 void launch_scan_u64(cudaStream_t s, const uint64_t *in, uint32_t n, uint64_t *out, uint64_t *tileSums, uint64_t *total);
 void launch_emit_cells(cudaStream_t s, const Ctx &C, const CellArrays &A, const uint64_t *offsets, uint64_t total,
@@ -155,6 +159,7 @@ void launch_gather(cudaStream_t s, const Ctx &C, const CensusBank &src, const ui
                    double *eradCensus, DevStats *st);
 void launch_bank_to_census(cudaStream_t s, const Ctx &C, const Bank &src, const CensusBank &dst, uint32_t n);
 void launch_count_bad_cells(cudaStream_t s, const uint32_t *cell, uint32_t n, uint32_t N, int32_t *bad);
+void launch_cell_histogram(cudaStream_t s, const uint32_t *cell, uint32_t n, uint32_t N, uint32_t *count);
 void launch_to_float(cudaStream_t s, const double *src, float *dst, uint32_t n);
 void launch_poststep(cudaStream_t s, const Ctx &C, const CellArrays &A, const OpacityEos &M, double dt);
 void launch_replay(cudaStream_t s, const Ctx &C, const ReplayDev &R, uint32_t n);

@@ -578,7 +578,10 @@ __global__ void k_emission_energy(Ctx C, CellArrays A, double dt) {
 // localTotalEnergy += energyToCreateVec[i] (:2058-2059) in the reference's order:
 // one thread adds the cells left to right so the allocation below floors against
 // the same total, bit for bit.  A warp streams the values through shared memory.
-__global__ void k_sequential_sum(const double *v, uint32_t n, double *out) {
+// onlyIf: when not null, the kernel runs only if *onlyIf is nonzero (a device-side
+// fallback that needs no host readback).
+__global__ void k_sequential_sum(const double *v, uint32_t n, double *out, const int32_t *onlyIf) {
+    if (onlyIf && *onlyIf == 0) return;
     __shared__ double buf[1024];
     double s = 0.0;
     for (uint32_t base = 0; base < n; base += 1024) {
@@ -594,7 +597,8 @@ __global__ void k_sequential_sum(const double *v, uint32_t n, double *out) {
 }
 
 // nPhotonsVec (:2071-2087)
-__global__ void k_allocate(Ctx C, CellArrays A, const double *total, uint64_t newPerCell) {
+__global__ void k_allocate(Ctx C, CellArrays A, const double *total, uint64_t newPerCell, const int32_t *onlyIf) {
+    if (onlyIf && *onlyIf == 0) return;
     const double tot = *total;
     const uint64_t totalParticles = static_cast<uint64_t>(C.ncells) * newPerCell * 10;
     for (uint32_t c = blockIdx.x * blockDim.x + threadIdx.x; c < C.ncells; c += gridDim.x * blockDim.x) {
@@ -2562,14 +2566,21 @@ void launch_emission_energy(cudaStream_t s, const Ctx &C, const CellArrays &A, d
     k_emission_energy<<<grid_for(C.ncells, 256, 8192), 256, 0, s>>>(C, A, dt);
 }
 void launch_sequential_sum(cudaStream_t s, const double *v, uint32_t n, double *out) {
-    k_sequential_sum<<<1, 256, 0, s>>>(v, n, out);
+    k_sequential_sum<<<1, 256, 0, s>>>(v, n, out, nullptr);
+}
+void launch_sequential_sum_if(cudaStream_t s, const double *v, uint32_t n, double *out, const int32_t *onlyIf) {
+    k_sequential_sum<<<1, 256, 0, s>>>(v, n, out, onlyIf);
 }
 void launch_allocate_checked(cudaStream_t s, const Ctx &C, const CellArrays &A, const double *total,
                              uint64_t newPerCell, double rel, int32_t *ambiguous) {
     k_allocate_checked<<<grid_for(C.ncells, 256, 8192), 256, 0, s>>>(C, A, total, newPerCell, rel, ambiguous);
 }
 void launch_allocate(cudaStream_t s, const Ctx &C, const CellArrays &A, const double *total, uint64_t newPerCell) {
-    k_allocate<<<grid_for(C.ncells, 256, 8192), 256, 0, s>>>(C, A, total, newPerCell);
+    k_allocate<<<grid_for(C.ncells, 256, 8192), 256, 0, s>>>(C, A, total, newPerCell, nullptr);
+}
+void launch_allocate_if(cudaStream_t s, const Ctx &C, const CellArrays &A, const double *total, uint64_t newPerCell,
+                        const int32_t *onlyIf) {
+    k_allocate<<<grid_for(C.ncells, 256, 8192), 256, 0, s>>>(C, A, total, newPerCell, onlyIf);
 }
 void launch_emission_debit(cudaStream_t s, const Ctx &C, const CellArrays &A, DevStats *st) {
     k_emission_debit<<<grid_for(C.ncells, 256, 8192), 256, 0, s>>>(C, A, st);
@@ -2818,6 +2829,17 @@ __global__ void k_to_float(const double *src, float *dst, uint32_t n) {
 }
 void launch_to_float(cudaStream_t s, const double *src, float *dst, uint32_t n) {
     if (n) k_to_float<<<grid_for(n, 256, 4096), 256, 0, s>>>(src, dst, n);
+}
+// Particles per cell at the start of transport (MonteCarloManagerSerial's
+// beginningParticleCount_, manager/MonteCarloManagerSerial.hpp:419-424).
+__global__ void k_cell_histogram(const uint32_t *cell, uint32_t n, uint32_t N, uint32_t *count) {
+    for (uint32_t q = blockIdx.x * blockDim.x + threadIdx.x; q < n; q += gridDim.x * blockDim.x) {
+        const uint32_t c = cell[q];
+        if (c < N) atomicAdd(count + c, 1u);
+    }
+}
+void launch_cell_histogram(cudaStream_t s, const uint32_t *cell, uint32_t n, uint32_t N, uint32_t *count) {
+    if (n) k_cell_histogram<<<grid_for(n, 256, 8192), 256, 0, s>>>(cell, n, N, count);
 }
 void launch_count_bad_cells(cudaStream_t s, const uint32_t *cell, uint32_t n, uint32_t N, int32_t *bad) {
     if (n) k_count_bad_cells<<<grid_for(n, 256, 4096), 256, 0, s>>>(cell, n, N, bad);

@@ -15,8 +15,23 @@
 // address is what the kernels receive.  That set-up happens on the first call
 // for a device; make that first call before any stream capture.  Every call
 // shares the array: two calls whose work overlaps on the GPU race on it.  Each
-// call overwrites all of the scratch it reads (the energy total and every tile
-// sum), so nothing needs clearing between calls.
+// call clears the one word that must start at zero (the ambiguity flag) and
+// overwrites the rest of the scratch it reads (the energy total and every tile
+// sum) before reading it.  The cached address belongs to the device's context
+// as it was at the first call: do not use this entry point across a
+// cudaDeviceReset of that device.
+//
+// The counts floor each cell's share against the reference's left-to-right
+// total of the energies.  As in the regular path, a deterministic blocked total
+// with a rigorous error interval settles almost every call; where a floor is
+// ambiguous the kernels flag it, and two further kernels (which return at once
+// when the flag is clear) recompute the exact left-to-right total and the
+// counts, all on the device with no host readback.
+//
+// Errors: the call reports launch errors of its own kernels as STORM_ERR_CUDA.
+// If an earlier CUDA error is already pending on the calling thread, it
+// launches nothing, leaves that error pending for its owner and returns
+// STORM_ERR_CUDA.
 #include <cuda_runtime.h>
 
 #include <mutex>
@@ -29,8 +44,9 @@ using namespace storm;
 namespace {
 
 constexpr uint32_t kTiles = (STORM_NOALLOC_MAX_CELLS + 1023u) / 1024u;
-// layout in 8-byte words: [0] energy total, [1] photon total, [2, 2 + kTiles) tile sums
-constexpr size_t kScratchWords = 2 + kTiles;
+// layout in 8-byte words: [0] energy total, [1] photon total, [2] ambiguity flag
+// (an int32 in the word's first half), [3, 3 + kTiles) tile sums
+constexpr size_t kScratchWords = 3 + kTiles;
 
 static __device__ __align__(256) unsigned long long g_allocScratch[kScratchWords];
 
@@ -62,6 +78,7 @@ extern "C" int storm_cuda_emission_allocation_noalloc(int device, const double *
     int ndev = 0;
     if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return STORM_ERR_NO_DEVICE;
     if (device >= ndev) return STORM_ERR_INVALID_ARG;
+    if (cudaPeekAtLastError() != cudaSuccess) return STORM_ERR_CUDA;   // someone else's, left pending
     int previous = 0;
     if (cudaGetDevice(&previous) != cudaSuccess) return STORM_ERR_CUDA;
     if (cudaSetDevice(device) != cudaSuccess) return STORM_ERR_CUDA;
@@ -71,16 +88,23 @@ extern "C" int storm_cuda_emission_allocation_noalloc(int device, const double *
         cudaStream_t s = static_cast<cudaStream_t>(stream);
         double *energyTotal = static_cast<double *>(scratch);
         uint64_t *photonTotal = static_cast<uint64_t *>(scratch) + 1;
-        uint64_t *tileSums = static_cast<uint64_t *>(scratch) + 2;
+        int32_t *ambiguous = reinterpret_cast<int32_t *>(static_cast<uint64_t *>(scratch) + 2);
+        uint64_t *tileSums = static_cast<uint64_t *>(scratch) + 3;
         Ctx C{};
         C.ncells = ncells;
         CellArrays A{};
         A.emitE = const_cast<double *>(d_energy);
         A.photons = d_photons;
-        launch_sequential_sum(s, d_energy, ncells, energyTotal);
-        launch_allocate(s, C, A, energyTotal, new_photons_per_cell);
-        launch_scan_u64(s, d_photons, ncells, d_offsets, tileSums, photonTotal);
-        if (cudaGetLastError() != cudaSuccess) rc = STORM_ERR_CUDA;
+        const double rel = 4.0 * (static_cast<double>(ncells) + 1100.0) * 0x1p-53;   // both orders' rounding
+        if (cudaMemsetAsync(ambiguous, 0, sizeof(int32_t), s) != cudaSuccess) rc = STORM_ERR_CUDA;
+        if (rc == STORM_OK) {
+            launch_blocked_sum(s, d_energy, ncells, energyTotal);
+            launch_allocate_checked(s, C, A, energyTotal, new_photons_per_cell, rel, ambiguous);
+            launch_sequential_sum_if(s, d_energy, ncells, energyTotal, ambiguous);
+            launch_allocate_if(s, C, A, energyTotal, new_photons_per_cell, ambiguous);
+            launch_scan_u64(s, d_photons, ncells, d_offsets, tileSums, photonTotal);
+            if (cudaGetLastError() != cudaSuccess) rc = STORM_ERR_CUDA;
+        }
     }
     cudaSetDevice(previous);
     return rc;

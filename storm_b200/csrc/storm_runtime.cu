@@ -49,6 +49,7 @@ struct StormHandle {
     CellArrays A{};
     double *tabA = nullptr, *tabS = nullptr, *rhoF = nullptr;
     uint32_t *segs = nullptr;
+    uint32_t *beginCounts = nullptr;   // particles per cell when transport began (per-cell counters on)
     OpacityEos M{};
     Ctx C{};
     // random walk tables (shared by every handle on the device, not owned)
@@ -907,6 +908,7 @@ int storm_cuda_create(const StormProblemDesc *d, StormHandle **out) {
     ALLOC(A.phys, N);
     ALLOC(A.phys32, N);
     ALLOC(h->segs, N);
+    if (d->per_cell_segment_counters) ALLOC(h->beginCounts, N);
     std::vector<double> vol(N);
     if (poly) {
         vol.assign(mesh->volume, mesh->volume + N);
@@ -980,6 +982,7 @@ int storm_cuda_create(const StormProblemDesc *d, StormHandle **out) {
     ZERO(A.rwElig, N);
     ZERO(A.photons, N * sizeof(uint64_t));
     ZERO(h->segs, N * sizeof(uint32_t));
+    if (h->beginCounts) ZERO(h->beginCounts, N * sizeof(uint32_t));
     std::vector<double> ones(N, 1.0);
     H2D(A.fleck, ones.data(), N);
 
@@ -989,10 +992,11 @@ int storm_cuda_create(const StormProblemDesc *d, StormHandle **out) {
     if (d->opacity_kind == STORM_OPACITY_CELL_TABLE || d->opacity_kind == STORM_OPACITY_MG_POWER) {
         ALLOC(h->tabA, N);
         H2D(h->tabA, d->sigma_a, N);
-        if (d->sigma_s) {
-            ALLOC(h->tabS, N);
-            H2D(h->tabS, d->sigma_s, N);
-        }
+        // tabS always exists (zeros without sigma_s) so that the per-step
+        // opacity refresh (storm_cuda_set_opacity_tables) can fill it
+        ALLOC(h->tabS, N);
+        if (d->sigma_s) H2D(h->tabS, d->sigma_s, N);
+        else ZERO(h->tabS, N * sizeof(double));
     }
     if (d->density_factor) {
         ALLOC(h->rhoF, N);
@@ -1163,7 +1167,7 @@ int storm_cuda_destroy(StormHandle *h) {
     free_rest(h, h->cap);
     void *ps[] = {h->xe, h->ye, h->ze, h->xc, h->yc, h->zc, h->A.T, h->A.mass, h->A.vol, h->A.eint, h->A.ceint,
                   h->A.sigA, h->A.sigS, h->A.fleck, h->A.rwSigT, h->A.eradAvg, h->A.eradCensus, h->A.emitE,
-                  h->A.rwElig, h->A.photons, h->A.phys, h->A.phys32, h->hx, h->hy, h->hz, h->segs, h->tabA, h->tabS, h->rhoF,
+                  h->A.rwElig, h->A.photons, h->A.phys, h->A.phys32, h->hx, h->hy, h->hz, h->segs, h->beginCounts, h->tabA, h->tabS, h->rhoF,
                   h->fsCell, h->fsSide, h->fsOffset, h->dAmbiguous, h->offsets, h->tileSums, h->dTotalU64, h->dTotalE, h->combW, h->combWtot,
                   h->combStart, h->combCount, h->counts, h->dStats, h->dErr, h->gb, h->A.mgCdf, h->A.pgrw,
                   h->A.pgrwCut, h->gb32, h->gc32, h->faceCdf, h->mgEp, h->mgEp32, h->mgKTq, h->ddmc, h->ddmcTot,
@@ -1287,6 +1291,11 @@ int storm_cuda_phase_transport(StormHandle *h) {
     CK(cudaEventRecord(h->evTransport0, h->stream));
     CK(cudaMemsetAsync(h->counts, 0, sizeof(uint32_t) * (h->maxRounds + 2), h->stream));
     if (h->desc.per_cell_segment_counters) CK(cudaMemsetAsync(h->segs, 0, sizeof(uint32_t) * h->N, h->stream));
+    if (h->beginCounts) {
+        CK(cudaMemsetAsync(h->beginCounts, 0, sizeof(uint32_t) * h->N, h->stream));
+        launch_cell_histogram(h->stream, h->bankA.cell, static_cast<uint32_t>(n0), h->N, h->beginCounts);
+        if (n0) ++h->launches;
+    }
     uint32_t n32 = static_cast<uint32_t>(n0);
     uint32_t *nCen = h->counts + h->maxRounds + 1;
     // the multigroup FP32 form runs only in the refill kernel
@@ -1846,6 +1855,26 @@ int storm_cuda_set_cell_state(StormHandle *h, const double *T, const double *ein
     return STORM_OK;
 }
 
+int storm_cuda_set_opacity_tables(StormHandle *h, const double *sigA, const double *sigS) {
+    if (!h || !h->tabA) return STORM_ERR_INVALID_ARG;   // only the per-cell table opacity kinds have tables
+    CK(cudaSetDevice(h->device));
+    const size_t N = h->N;
+    if (sigA) CK(cudaMemcpyAsync(h->tabA, sigA, N * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+    if (sigS) CK(cudaMemcpyAsync(h->tabS, sigS, N * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+    CK(cudaStreamSynchronize(h->stream));   // pageable sources: the caller may reuse them on return
+    return STORM_OK;
+}
+
+int storm_cuda_get_beginning_counts(StormHandle *h, uint64_t *counts) {
+    if (!h || !counts || !h->beginCounts) return STORM_ERR_INVALID_ARG;
+    CK(cudaSetDevice(h->device));
+    std::vector<uint32_t> c32(h->N);
+    CK(cudaMemcpyAsync(c32.data(), h->beginCounts, h->N * sizeof(uint32_t), cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    for (size_t q = 0; q < h->N; ++q) counts[q] = c32[q];
+    return STORM_OK;
+}
+
 int storm_cuda_set_cell_physics(StormHandle *h, const double *sigA, const double *sigS, const double *fleck) {
     if (!h) return STORM_ERR_INVALID_ARG;
     CK(cudaSetDevice(h->device));
@@ -1875,9 +1904,9 @@ struct CheckpointHeader {
     double faceT[6];
 };
 constexpr size_t kBankArrays = 9;   // x y z vx vy vz t w w0 (8 bytes per particle each)
+size_t checkpoint_per_particle(const StormHandle *h) { return kBankArrays * 8 + 3 * 4 + (h->C.groups >= 2 ? 8 : 0); }
 size_t checkpoint_bytes(const StormHandle *h, uint64_t n) {
-    const size_t perParticle = kBankArrays * 8 + 3 * 4 + (h->C.groups >= 2 ? 8 : 0);
-    return sizeof(CheckpointHeader) + n * perParticle + 3 * static_cast<size_t>(h->N) * 8;
+    return sizeof(CheckpointHeader) + n * checkpoint_per_particle(h) + 3 * static_cast<size_t>(h->N) * 8;
 }
 }  // namespace
 
@@ -1935,8 +1964,25 @@ int storm_cuda_checkpoint_load(StormHandle *h, const void *buffer, uint64_t byte
     if (std::memcmp(hd.magic, "STORMCK1", 8) != 0 || hd.abi != STORM_CUDA_ABI_VERSION ||
         hd.precision != static_cast<uint32_t>(h->desc.precision) || hd.groups != h->C.groups || hd.ncells != h->N)
         return STORM_ERR_INVALID_ARG;
+    // Everything is validated on the host before any of the handle's state is
+    // overwritten, so a rejected checkpoint leaves the handle as it was.  The
+    // census count comes from the buffer: bound it by the bank's 32-bit indices
+    // and by the bytes actually present before sizing anything with it.
     const uint64_t n = hd.nCensus;
+    const uint64_t fixedBytes = sizeof(CheckpointHeader) + 3 * static_cast<uint64_t>(h->N) * 8;
+    if (bytes < fixedBytes || n > 0xFFFFFFFFull || n > (bytes - fixedBytes) / checkpoint_per_particle(h))
+        return STORM_ERR_INVALID_ARG;
     if (bytes < checkpoint_bytes(h, n)) return STORM_ERR_INVALID_ARG;
+    for (int f = 0; f < 6; ++f)
+        if (!(hd.faceT[f] >= 0.0)) return STORM_ERR_INVALID_ARG;
+    {   // the census must name cells of this grid
+        const char *cellBytes = static_cast<const char *>(buffer) + sizeof(hd) + kBankArrays * 8 * n;
+        for (uint64_t k = 0; k < n; ++k) {
+            uint32_t c;
+            std::memcpy(&c, cellBytes + 4 * k, sizeof(c));
+            if (c >= h->N) return STORM_ERR_INVALID_ARG;
+        }
+    }
     CK(cudaSetDevice(h->device));
     int rc = ensure_capacity(h, n, 0);
     if (rc != STORM_OK) return rc;
@@ -1962,15 +2008,6 @@ int storm_cuda_checkpoint_load(StormHandle *h, const void *buffer, uint64_t byte
         in += static_cast<size_t>(h->N) * 8;
     }
     CK(cudaStreamSynchronize(h->stream));
-    // the census must name cells of this grid
-    if (n) {
-        CK(cudaMemsetAsync(h->dAmbiguous + 1, 0, sizeof(int32_t), h->stream));
-        launch_count_bad_cells(h->stream, b.cell, static_cast<uint32_t>(n), h->N, h->dAmbiguous + 1);
-        int32_t nb = 0;
-        CK(cudaMemcpyAsync(&nb, h->dAmbiguous + 1, sizeof(int32_t), cudaMemcpyDeviceToHost, h->stream));
-        CK(cudaStreamSynchronize(h->stream));
-        if (nb) return STORM_ERR_INVALID_ARG;
-    }
     h->nCensus = n;
     h->step = static_cast<uint32_t>(hd.step);
     for (int f = 0; f < 6; ++f) {

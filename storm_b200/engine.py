@@ -52,6 +52,8 @@ def lib():
         L.storm_cuda_get_cell_arrays.argtypes = [vp, dp, dp, dp, dp, dp, dp, u64p]
         L.storm_cuda_set_cell_state.argtypes = [vp, dp, dp, dp]
         L.storm_cuda_set_cell_physics.argtypes = [vp, dp, dp, dp]
+        L.storm_cuda_set_opacity_tables.argtypes = [vp, dp, dp]
+        L.storm_cuda_get_beginning_counts.argtypes = [vp, u64p]
         L.storm_cuda_set_face_temperature.argtypes = [vp, C.c_int, C.c_double]
         L.storm_cuda_get_emission.argtypes = [vp, u64p, dp]
         L.storm_cuda_replay_segments.argtypes = [vp, C.POINTER(A.StormReplayBatch)]
@@ -269,6 +271,18 @@ class Engine:
     def set_cell_physics(self, sigma_a=None, sigma_s=None, fleck=None):
         arr = [None if a is None else np.ascontiguousarray(a, float) for a in (sigma_a, sigma_s, fleck)]
         self._check(lib().storm_cuda_set_cell_physics(self.h, *[A.ptr(a) for a in arr]))
+
+    def set_opacity_tables(self, sigma_a=None, sigma_s=None):
+        """Per-cell opacity plug-in values for the next prestep (table opacity kinds)."""
+        arr = [None if a is None else np.ascontiguousarray(a, float) for a in (sigma_a, sigma_s)]
+        self._check(lib().storm_cuda_set_opacity_tables(self.h, *[A.ptr(a) for a in arr]))
+
+    def beginning_counts(self):
+        """Particles per cell when the last step's transport began (handles with
+        per-cell counters)."""
+        out = np.zeros(self.n, np.uint64)
+        self._check(lib().storm_cuda_get_beginning_counts(self.h, A.ptr(out, C.c_uint64)))
+        return out
 
     def checkpoint(self):
         """The handle's step-to-step state (census bank, cell state, face

@@ -39,8 +39,15 @@ void bind_imc(STORM::CudaIMCBinding<Cell, Ext> &b, const StormProblemDesc *d) {
 
 extern "C" {
 
-DropinHandle *dropin_create(const StormProblemDesc *d, int precision, char *err, size_t errlen) {
-    RefHandle *ref = ref_create(d, 0, err, errlen);
+// boundary_kind as ref_create takes it (0 the per-face descriptor plug-in,
+// 1 RigidBoundary, 2 VacuumBoundary, 3 SideTemperature, 4 TwoSidesTemperature:
+// the template lowers kinds 1-4 by their type).  opacity_from_plugin: the
+// binding's planckOpacity / scatteringOpacity call the reference-side opacity
+// plug-in on the caller's cells (CalcPlanckOpacity, CalcScatteringOpacity),
+// so a temperature-dependent opacity is re-evaluated before every step.
+DropinHandle *dropin_create_plugins(const StormProblemDesc *d, int precision, int boundary_kind,
+                                    int opacity_from_plugin, char *err, size_t errlen) {
+    RefHandle *ref = ref_create(d, boundary_kind, err, errlen);
     if (!ref) return nullptr;
     auto h = std::make_unique<DropinHandle>();
     h->ref = ref;
@@ -67,6 +74,14 @@ DropinHandle *dropin_create(const StormProblemDesc *d, int precision, char *err,
             b.kP0 = d->kP0; b.kR0 = d->kR0; b.alpha = d->alpha; b.beta = d->beta; b.tFloor = d->t_floor;
             b.cap = d->cap;
             if (d->density_factor) b.densityFactor.assign(d->density_factor, d->density_factor + N);
+        }
+        if (opacity_from_plugin) {
+            if (d->groups >= 2) throw STORM::StormError("dropin_create_plugins: gray problems only");
+            auto *opac = static_cast<RecordingIMC<1> *>(ref->physics.get())->opac;
+            const std::vector<Cell> *cells = &ref->cells;
+            b.opacityKind = STORM_OPACITY_CELL_TABLE;
+            b.planckOpacity = [opac, cells](std::size_t i) { return opac->CalcPlanckOpacity((*cells)[i]); };
+            b.scatteringOpacity = [opac, cells](std::size_t i) { return opac->CalcScatteringOpacity((*cells)[i]); };
         }
         b.eosKind = d->eos_kind;
         b.cvPerMass = d->cv_per_mass;
@@ -96,6 +111,17 @@ DropinHandle *dropin_create(const StormProblemDesc *d, int precision, char *err,
         ref_destroy(ref);
         return nullptr;
     }
+}
+
+DropinHandle *dropin_create(const StormProblemDesc *d, int precision, char *err, size_t errlen) {
+    return dropin_create_plugins(d, precision, 0, 0, err, errlen);
+}
+
+// MonteCarloManagerCUDA::GetBeginningParticleCount after the last step.
+int dropin_beginning_counts(DropinHandle *h, uint64_t *counts) {
+    const auto &v = h->manager->GetBeginningParticleCount();
+    for (std::size_t i = 0; i < v.size(); ++i) counts[i] = v[i];
+    return static_cast<int>(v.size() == h->ref->grid->GetPointNo() ? 0 : 1);
 }
 
 void dropin_destroy(DropinHandle *h) {

@@ -3,7 +3,7 @@
 sources against oracle/shims).  Run in a container where the reference sources
 are present:
 
-    make -C oracle && python tests/golden/make_golden.py
+    make -C oracle all REF=<reference source tree> && python tests/golden/make_golden.py
 
 Fixtures (numpy .npz):
   replay_slab.npz     recorded RadiationIMC::step calls on the gray slab (boundary

@@ -38,4 +38,7 @@ def main(root):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    src = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("STORM_REFERENCE_SRC", "")
+    if not src:
+        sys.exit("usage: make_reference_curves.py <reference source tree> (or set STORM_REFERENCE_SRC)")
+    main(src)

@@ -5,7 +5,7 @@ reference_runs.npz.  Each problem runs in a fresh process, because
 CombPopulationControl and the boundary sources keep function-static random
 engines.  Run where the reference sources were compiled:
 
-    make -C oracle && python tests/golden/make_reference_runs.py
+    make -C oracle all REF=<reference source tree> && python tests/golden/make_reference_runs.py
 
 Arrays, per problem name (marshak_wave_1..4 at the examples' defaults: 256
 cells (512 for problem 4), 15 packets per cell, 100 per bath face, comb

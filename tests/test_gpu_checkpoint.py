@@ -56,3 +56,33 @@ def test_checkpoint_rejects_another_problem():
     with pytest.raises(StormError):
         other.restore(blob[:40])
     other.close()
+
+
+def test_rejected_checkpoint_leaves_the_handle_unchanged():
+    """A checkpoint whose census names a cell outside the grid, or whose header
+    claims more particles than the buffer holds, is refused before any of the
+    handle's state is overwritten: the handle keeps its census and cell state
+    and steps on as if nothing had been loaded."""
+    import struct
+    p = problems.step_cube(n=8, new_photons_per_cell=3, face_packets=40, comb_nmin=10)
+    a = Engine(p)
+    a.step()
+    blob = bytearray(a.checkpoint())
+    a.step()
+    T0, n0 = a.cells()["temperature"], a.census_count()
+    head = 8 + 4 * 4   # magic, abi, precision, groups, ncells
+    n = struct.unpack_from("<Q", blob, head)[0]
+    assert n > 0
+    bad_cell = bytearray(blob)
+    cell_at = 88 + 9 * 8 * n        # header (88 bytes), then nine 8-byte arrays, then the cell ids
+    struct.pack_into("<I", bad_cell, cell_at + 4 * (n // 2), p.ncells + 5)
+    huge = bytearray(blob)
+    struct.pack_into("<Q", huge, head, 1 << 62)
+    for b in (bad_cell, huge):
+        with pytest.raises(StormError):
+            a.restore(bytes(b))
+        assert a.census_count() == n0
+        np.testing.assert_array_equal(a.cells()["temperature"], T0)
+    a.step()
+    assert a.census_count() > 0
+    a.close()

@@ -1,0 +1,113 @@
+"""Full-run parity of the engine's FP64 form with the reference's serial path,
+judged against the batch-estimated statistical error.
+
+The reference's runs are committed as per-cell batch summaries
+(tests/golden/reference_batch.npz, made by make_reference_batch.py from the
+reference build over independent seeds).  The engine runs its own batch of
+seeds here.  Per recorded step and per cell, four quantities are compared:
+material temperature, energy deposited in the material during the step, the
+time-averaged radiation energy density and the radiation energy in census
+(`radiation/RadiationIMC.hpp:1887-2029`).  `storm_b200.batchstats.gate`
+states the criterion: no Welch z beyond the Bonferroni bound for the number
+of tests, at most the binomial allowance above |z| = 3, and every
+cell-summed total within its own Bonferroni bound.  A correct engine fails it
+with probability about 1e-3.
+
+The same gate applied to two disjoint halves of the engine's own seeds is the
+control: it shows what the gate sees between two batches of one solver.
+
+Workloads: the 100x1x1 gray slab at its defaults, all 100 steps; the
+step-opacity cube with Random Walk cut from 64^3 to 16^3 cells at the same
+packet densities, 20 steps.  Also Marshak wave 1: the distribution of the
+example's L1 over eight engine seeds against the reference's eight, and the
+final gas-temperature profile under the same per-cell gate.
+"""
+import json
+import os
+import sys
+
+import numpy as np
+import pytest
+
+from conftest import GOLDEN, golden
+from storm_b200 import batchstats
+from storm_b200.engine import Engine
+
+sys.path.insert(0, GOLDEN)
+import make_reference_batch as MB  # noqa: E402
+
+pytestmark = pytest.mark.gpu
+
+ENGINE_SEEDS = {"c1": range(2000, 2032), "c2r": range(2000, 2024)}
+
+
+def _engine_batch(name):
+    w = MB.WORKLOADS[name]
+    runs = []
+    for s in ENGINE_SEEDS[name]:
+        p = MB.workload(name, s)
+        e = Engine(p)
+        runs.append(batchstats.run_snapshots(e, p, w["steps"], w["snapshots"]))
+        e.close()
+    return np.array(runs)
+
+
+def _fixture(name):
+    g = golden("reference_batch.npz")
+    return {k[len(name) + 1:]: v for k, v in g.items() if k.startswith(name + "_")}
+
+
+def _report(name, res):
+    path = os.environ.get("STORM_FULLRUN_REPORT")
+    line = {"workload": name, **{k: res[k] for k in ("all", "totals", "passed")},
+            **{q: {k: res[q][k] for k in ("tests", "above_threshold", "k_max", "max_abs_z", "mean_z", "frac_within")}
+               for q in batchstats.QUANTITIES}}
+    print(json.dumps(line))
+    if path:
+        with open(path, "a") as f:
+            f.write(json.dumps(line) + "\n")
+
+
+@pytest.mark.parametrize("name", ["c1", "c2r"])
+def test_full_run_matches_reference_batch(name):
+    fx = _fixture(name)
+    runs = _engine_batch(name)
+    assert runs.shape[1:] == fx["mean"].shape
+    res = batchstats.compare(runs, fx)
+    _report(name, res)
+    assert res["all"]["tests"] > 0.5 * fx["mean"].size, res["all"]
+    assert res["passed"], res["all"] | {"totals": res["totals"]}
+    # total energy: conserved per step by both (the engine's own check is in test_gpu_parity)
+    half = len(runs) // 2
+    ctrl = batchstats.compare(runs[:half], runs[half:])
+    _report(name + " (engine seeds split in two)", ctrl)
+    assert ctrl["passed"], ctrl["all"]
+
+
+def test_marshak1_seed_distribution_matches_reference():
+    """Marshak wave 1 (7,912 steps): the example's L1 over eight engine seeds
+    against the reference's eight (Mann-Whitney U, two-sided, p > 1e-3), every
+    engine L1 under the regression gate 0.10, and the final gas-temperature
+    profile under the per-cell batch gate."""
+    from scipy import stats
+    from storm_b200 import benchmarks as B
+    g = golden("reference_batch.npz")
+    curve = golden("reference_curves.npz")["marshak_wave_1"]
+    l1, prof = [], []
+    for s in range(2000, 2008):
+        res = B.run_marshak_wave(Engine, 1, seed=s)
+        np.testing.assert_allclose(res["x"], g["marshak1_x"], rtol=0, atol=1e-12)
+        l1.append(B.marshak_l1(res["x"], res["t_gas"], curve))
+        prof.append(res["t_gas"])
+    l1 = np.array(l1)
+    ref_l1 = g["marshak1_l1"]
+    u = stats.mannwhitneyu(l1, ref_l1, alternative="two-sided")
+    a = batchstats.summarize(np.array(prof))
+    b = batchstats.summarize(g["marshak1_t_gas"])
+    z, ok = batchstats.welch_z(a, b)
+    gt = batchstats.gate(z[ok])
+    print(json.dumps({"workload": "marshak1", "engine_l1": l1.tolist(), "reference_l1": ref_l1.tolist(),
+                      "mannwhitney_p": float(u.pvalue), "profile_gate": gt}))
+    assert (l1 < 0.10).all(), l1
+    assert u.pvalue > 1e-3, (l1, ref_l1)
+    assert gt["passed"], gt

@@ -51,6 +51,48 @@ def test_noalloc_matches_engine_on_consecutive_calls():
                 assert off[-1] == photons.sum()
 
 
+def _allocation_formula(energy, new_per_cell):
+    """The reference's count per cell (radiation/RadiationIMC.hpp:2058-2087) on
+    the host: floor(E / S * N * n * 10) clamped to [n, 20 n], S the
+    left-to-right sum (np.cumsum adds in order)."""
+    total = np.cumsum(energy)[-1]
+    tp = float(len(energy) * new_per_cell * 10)
+    share = np.floor(energy / total * tp).astype(np.uint64)
+    out = np.clip(share, new_per_cell, 20 * new_per_cell).astype(np.uint64)
+    out[energy <= 0] = 0
+    return out
+
+
+@pytest.mark.parametrize("case", ["random", "uniform"])
+def test_noalloc_large_meshes_take_no_device_memory(case):
+    """More than 2^21 cells, so that the prefix sum's tile totals span several
+    chunks.  "uniform": every cell's share is an exact integer, which puts each
+    floor on the edge of the blocked total's error interval and sends the call
+    down its exact left-to-right fallback on the device.  Two calls in a row
+    give the host formula's counts, and the second changes neither torch's
+    allocation nor the device's free memory."""
+    import torch
+    n = (1 << 21) + 4099
+    rng = np.random.default_rng(7)
+    if case == "random":
+        energy = rng.lognormal(0.0, 2.0, n)
+        energy[::97] = 0.0
+    else:
+        energy = np.full(n, 0.5)
+    expect = _allocation_formula(energy, 3)
+    first = _noalloc(energy, 3)
+    torch.cuda.synchronize()
+    free0, alloc0 = torch.cuda.mem_get_info(0)[0], torch.cuda.memory_allocated(0)
+    second = _noalloc(energy, 3)
+    free1, alloc1 = torch.cuda.mem_get_info(0)[0], torch.cuda.memory_allocated(0)
+    for ph, off in (first, second):
+        np.testing.assert_array_equal(ph, expect)
+        np.testing.assert_array_equal(off[:-1], np.concatenate([[0], np.cumsum(expect)[:-1]]))
+        assert off[-1] == expect.sum()
+    # the helper's own tensors are freed before the second measurement
+    assert alloc1 == alloc0 and free1 == free0, (alloc0, alloc1, free0, free1)
+
+
 def test_noalloc_rejects_sizes_beyond_limit():
     from storm_b200.engine import lib
     f = lib().storm_cuda_emission_allocation_noalloc
