@@ -315,6 +315,38 @@ int storm_cuda_create(const StormProblemDesc *desc, StormHandle **out);
 /* Replaces ~MonteCarloManagerSerial (manager/MonteCarloManagerSerial.hpp:186-195). */
 int storm_cuda_destroy(StormHandle *h);
 
+/* ---------------------------------------------------------------- particle shards */
+
+/* One problem split over several ranks (one GPU each) by particle-id ranges.
+ * The mesh and every per-cell table are replicated; the census and each
+ * step's emission are cut into `shards` particle shards, and a rank holds the
+ * contiguous shards [shard_lo, shard_hi).  Three times per step the engine
+ * hands the exchange callback a device buffer of doubles to be summed in
+ * place over all ranks (an all-reduce, ordered on `stream`):
+ *   1. after transport: the per-cell material deposits and the time-averaged
+ *      radiation tallies (2 N values);
+ *   2. in the comb: the census weight and particle count of every
+ *      (shard, cell) run (2 S N values, each rank filling its own shards'
+ *      entries and zeros elsewhere);
+ *   3. after the comb: the census particles per shard and the census radiation
+ *      energy per cell (S + N values).
+ * This mirrors the reference's MPI reductions of the step totals
+ * (radiation/RadiationIMC.hpp:2070-2071; population/CombPopulationControl.hpp:102,
+ * 145), with the per-cell sums the shared mesh needs.  The comb keeps the
+ * census of each shard on its rank and places every shard's teeth after the
+ * weight of the lower shards in the same cell, so for a given `shards` the
+ * step's results do not depend on how the shards are spread over ranks, up
+ * to the summation order of the floating-point tallies.  A callback returning
+ * nonzero fails the step with STORM_ERR_INVALID_ARG.  The exchange may be NULL
+ * when one rank holds every shard. */
+typedef int (*StormExchangeFn)(void *user, double *values, uint64_t count, void *stream);
+
+/* Configure particle shards on a handle whose census is empty (before its first
+ * step).  shards = 1 turns sharding off.  Requires CombPopulationControl (the
+ * plain comb); other population controls return STORM_ERR_INVALID_ARG. */
+int storm_cuda_set_sharding(StormHandle *h, uint32_t shards, uint32_t shard_lo, uint32_t shard_hi,
+                            StormExchangeFn exchange, void *user);
+
 /* ---------------------------------------------------------------- the step */
 
 /* One full time step on the device-resident census: MonteCarloManagerSerial::step

@@ -167,6 +167,13 @@ struct Oracle {
     /* banks */
     Bank census, bank;
     uint64_t pidLimit;   /* every pid of the current census is below this */
+    /* particle shards (orc_set_sharding): S shards, this instance holds [shardLo, shardHi) */
+    uint32_t shards, shardLo, shardHi;
+    uint64_t *shardCensus;         /* census particles per shard after the last comb (every shard) */
+    uint64_t nCenGlobal, nCellEmitGlobal, nFaceEmitGlobal;   /* the current step's global counts */
+    double *dep;                   /* this instance's material deposits of the current step */
+    StormExchangeFn exchange;
+    void *exchangeUser;
     uint32_t step;
     StormStepStats st;
     int32_t derr;
@@ -823,7 +830,59 @@ Oracle *orc_create(const StormProblemDesc *d) {
     o->d.temperature = o->d.mass = o->d.internal_energy = o->d.cell_internal_energy = NULL;
     o->d.sigma_a = o->d.sigma_s = o->d.density_factor = NULL;
     if (d->with_random_walk) rw_build();
+    o->shards = 1; o->shardLo = 0; o->shardHi = 1;
     return o;
+}
+
+int orc_set_sharding(Oracle *o, uint32_t shards, uint32_t lo, uint32_t hi, StormExchangeFn exchange, void *user) {
+    if (!o || shards == 0 || lo >= hi || hi > shards || o->census.n || !o->d.comb_enabled ||
+        o->d.comb_kind != STORM_COMB_PLAIN)
+        return -1;
+    o->shards = shards; o->shardLo = lo; o->shardHi = hi;
+    free(o->shardCensus);
+    o->shardCensus = (uint64_t *)calloc(shards, sizeof(uint64_t));
+    free(o->dep);
+    o->dep = dup(NULL, o->N, 0);
+    o->exchange = exchange;
+    o->exchangeUser = user;
+    return 0;
+}
+
+/* the exchange: an in-place sum over every rank (identity without a callback) */
+static int exchange_sum(Oracle *o, double *v, uint64_t n) {
+    if (!o->exchange) return 0;
+    return o->exchange(o->exchangeUser, v, n, NULL) ? -1 : 0;
+}
+
+/* first index of shard s when `n` items are cut into S contiguous shards */
+static uint64_t shard_begin(uint64_t n, uint32_t s, uint32_t S) {
+    return (uint64_t)(((unsigned __int128)n * s) / S);
+}
+
+/* census particles of the shards below s (their pids start at this offset) */
+static uint64_t census_offset(const Oracle *o, uint32_t s) {
+    uint64_t off = 0;
+    for (uint32_t q = 0; q < s; ++q) off += o->shardCensus[q];
+    return off;
+}
+
+/* The shard a pid belongs to: census pids [0, nCen) by the shards' census
+ * counts, then cell packets and face packets each cut into S equal ranges. */
+static uint32_t shard_of_pid(const Oracle *o, uint64_t pid) {
+    const uint32_t S = o->shards;
+    if (pid < o->nCenGlobal) {
+        uint64_t off = 0;
+        for (uint32_t s = 0; s < S; ++s) {
+            off += o->shardCensus[s];
+            if (pid < off) return s;
+        }
+        return S - 1;
+    }
+    uint64_t e = pid - o->nCenGlobal, n = o->nCellEmitGlobal;
+    if (e >= n) { e -= n; n = o->nFaceEmitGlobal; }
+    uint32_t s = 0;
+    while (s + 1 < S && shard_begin(n, s + 1, S) <= e) ++s;
+    return s;
 }
 
 void orc_destroy(Oracle *o) {
@@ -833,6 +892,7 @@ void orc_destroy(Oracle *o) {
     for (size_t q = 0; q < sizeof(arrs) / sizeof(arrs[0]); ++q) free(arrs[q]);
     free(o->rwElig); free(o->segs); free(o->photons);
     free(o->census.p); free(o->bank.p);
+    free(o->shardCensus); free(o->dep);
     free(o);
 }
 
@@ -844,11 +904,14 @@ int orc_phase_begin(Oracle *o, double dt) {
     memset(&o->st, 0, sizeof(o->st));
     o->derr = 0;
     o->bank.n = 0;
+    /* sharded: this instance's census holds the global pids from the offset of its first shard */
+    const uint64_t pid0 = o->shards > 1 ? census_offset(o, o->shardLo) : 0;
+    o->nCenGlobal = o->shards > 1 ? census_offset(o, o->shards) : o->census.n;
     for (uint64_t q = 0; q < o->census.n; ++q) {
         Part p = o->census.p[q];
         p.t = dt;
         p.w0 = fabs(p.w);
-        p.pid = (uint32_t)q;
+        p.pid = (uint32_t)(pid0 + q);
         p.draw = 0;
         o->st.energy_census_in += p.w;
         bank_push(&o->bank, &p);
@@ -953,8 +1016,24 @@ int orc_phase_emit(Oracle *o, double dt) {
         uint64_t m = share < cap ? share : cap;
         o->photons[i] = o->emitE[i] > 0.0 ? (m > n ? m : n) : 0;
     }
+    /* packets are numbered globally: cell packet e has pid nCen + e and face
+     * packet f has pid nCen + nE + f; a sharded instance keeps the packets of
+     * its shards' ranges of each numbering */
+    uint64_t nE = 0, nF = 0;
+    for (uint64_t i = 0; i < N; ++i) nE += o->photons[i];
+    for (uint64_t i = 0; i < N; ++i) {
+        uint32_t ii, jj, kk;
+        cell_ijk(o, i, &ii, &jj, &kk);
+        for (int s = 0; s < 6; ++s)
+            if (neighbour(o, ii, jj, kk, s) >= N && o->faces[s].source_temperature > 0.0)
+                nF += o->faces[s].packets_per_face;
+    }
+    o->nCellEmitGlobal = nE;
+    o->nFaceEmitGlobal = nF;
+    const uint64_t eLo = shard_begin(nE, o->shardLo, o->shards), eHi = shard_begin(nE, o->shardHi, o->shards);
+    const uint64_t fLo = shard_begin(nF, o->shardLo, o->shards), fHi = shard_begin(nF, o->shardHi, o->shards);
+    const uint64_t pidBase = o->nCenGlobal;
     uint64_t e = 0;
-    uint32_t pidBase = (uint32_t)o->bank.n;
     for (uint64_t i = 0; i < N; ++i) {
         uint64_t np = o->photons[i];
         if (np == 0) continue;
@@ -964,6 +1043,7 @@ int orc_phase_emit(Oracle *o, double dt) {
         double energyPerPhoton = E * 1.0 / (double)np;
         V3 mc = center(o, i);
         for (uint64_t q = 0; q < np; ++q, ++e) {
+            if (e < eLo || e >= eHi) continue;
             Rng r;
             memset(&r, 0, sizeof(r));
             r.seed = o->d.seed; r.tag = TAG_CELL_EMIT; r.step = o->step; r.pid = (uint32_t)e;
@@ -978,13 +1058,13 @@ int orc_phase_emit(Oracle *o, double dt) {
             p.t = dt * rng_open(&r);
             p.w = energyPerPhoton;
             p.w0 = fabs(p.w);
-            p.pid = pidBase + (uint32_t)e;
+            p.pid = (uint32_t)(pidBase + e);
             p.draw = 0;
             o->st.energy_emitted += p.w;
             bank_push(&o->bank, &p);
         }
     }
-    o->st.emitted_cells = e;
+    o->st.emitted_cells = eHi - eLo;
     /* face sources: cells in index order, sides in GetCellFaces order */
     uint64_t fpk = 0;
     for (uint64_t i = 0; i < N; ++i) {
@@ -1009,6 +1089,7 @@ int orc_phase_emit(Oracle *o, double dt) {
             face_vertices(o, ii, jj, kk, s, q4);
             V3 mc = center(o, i);
             for (uint64_t q = 0; q < Np; ++q, ++fpk) {
+                if (fpk < fLo || fpk >= fHi) continue;
                 Rng r;
                 memset(&r, 0, sizeof(r));
                 r.seed = o->d.seed; r.tag = TAG_FACE_EMIT; r.step = o->step; r.pid = (uint32_t)fpk;
@@ -1030,14 +1111,14 @@ int orc_phase_emit(Oracle *o, double dt) {
                 p.x = loc.x; p.y = loc.y; p.z = loc.z;
                 repair_outside(o, &p, mc, 1e-8);
                 p.w0 = fabs(p.w);
-                p.pid = pidBase + (uint32_t)(e + fpk);
+                p.pid = (uint32_t)(pidBase + nE + fpk);
                 p.draw = 0;
                 o->st.energy_emitted += p.w;
                 bank_push(&o->bank, &p);
             }
         }
     }
-    o->st.emitted_faces = fpk;
+    o->st.emitted_faces = fHi - fLo;
     return 0;
 }
 
@@ -1045,7 +1126,12 @@ int orc_phase_emit(Oracle *o, double dt) {
  * particle is stepped to census, escape or removal. */
 int orc_phase_transport(Oracle *o) {
     memset(o->segs, 0, sizeof(uint64_t) * o->N);
-    o->pidLimit = o->bank.n ? o->bank.n : 1;   /* transport pids are bank slots */
+    /* every pid of the step (over all shards) is below this */
+    o->pidLimit = o->nCenGlobal + o->nCellEmitGlobal + o->nFaceEmitGlobal;
+    if (!o->pidLimit) o->pidLimit = 1;
+    const int sharded = o->shards > 1;
+    double *tally = sharded ? o->dep : o->eint;   /* sharded: deposits are summed over the ranks first */
+    if (sharded) memset(o->dep, 0, sizeof(double) * o->N);
     for (uint64_t q = 0; q < o->bank.n; ++q) {
         Part p = o->bank.p[q];
         Rng r;
@@ -1060,7 +1146,7 @@ int orc_phase_transport(Oracle *o) {
             StepOut so;
             physics_step(o, &p, &r, &so);
             if (so.error) { raise(o, so.error, cell, p.pid); break; }
-            o->eint[cell] += so.dmat;
+            tally[cell] += so.dmat;
             o->eradAvg[cell] += so.derad;
             o->st.energy_deposited += so.dmat;
             if (so.usedRW) o->st.rw_steps++;
@@ -1084,6 +1170,17 @@ int orc_phase_transport(Oracle *o) {
         if (o->derr) return -1;
     }
     o->bank.n = 0;
+    if (sharded) {   /* exchange 1: deposits and time-averaged radiation, per cell */
+        const uint64_t N = o->N;
+        double *buf = (double *)malloc(sizeof(double) * 2 * (N ? N : 1));
+        memcpy(buf, o->dep, sizeof(double) * N);
+        memcpy(buf + N, o->eradAvg, sizeof(double) * N);
+        int rc = exchange_sum(o, buf, 2 * N);
+        for (uint64_t i = 0; i < N; ++i) o->eint[i] += buf[i];
+        memcpy(o->eradAvg, buf + N, sizeof(double) * N);
+        free(buf);
+        if (rc) return -1;
+    }
     return 0;
 }
 
@@ -1110,7 +1207,10 @@ static int cmp_key(const void *a, const void *b) {
 /* CombPopulationControl::activate (population/CombPopulationControl.hpp:79-253).
  * Within a cell particles are ordered by the keyed bijection orc_comb_key
  * (the reference orders by id and std::shuffles with a function-static engine). */
+static int orc_phase_comb_sharded(Oracle *o);
+
 int orc_phase_comb(Oracle *o) {
+    if (o->shards > 1) return orc_phase_comb_sharded(o);
     const uint64_t N = o->N;
     Bank in = o->census;
     Bank out = {NULL, 0, 0};
@@ -1203,6 +1303,142 @@ int orc_phase_comb(Oracle *o) {
     return 0;
 }
 
+/* #{k >= 0 : (k + r) E < P}: the comb index a sequential walk holds once it
+ * has passed weight P (the loop condition of :203-222 with cum = P). */
+static uint64_t teeth_below(double P, double r, double E) {
+    if (!(P > 0.0)) return 0;
+    double g = P / E - r;
+    uint64_t k = g > 0.0 ? (uint64_t)ceil(g) : 0;
+    while (k > 0 && ((double)(k - 1) + r) * E >= P) --k;
+    while (((double)k + r) * E < P) ++k;
+    return k;
+}
+
+/* CombPopulationControl::activate over particle shards.  The census is sorted
+ * by (shard, cell, keyed hash of pid); each (shard, cell) run's weight and
+ * count are summed locally and exchanged, so that every rank sees every run.
+ * A cell's targets come from its global weight (the shards' run weights added
+ * in shard order) and count.  A combed cell's teeth are placed along the
+ * cell's runs in shard order: run s starts at the weight P of the runs below it
+ * and at the comb index teeth_below(P).  The new census stays with its shard,
+ * in (shard, cell) order; exchange 3 gives every rank the shards' census
+ * counts and the census energy per cell. */
+static int orc_phase_comb_sharded(Oracle *o) {
+    const uint64_t N = o->N;
+    const uint32_t S = o->shards;
+    const uint64_t R = (uint64_t)S * N;
+    Bank in = o->census;
+    Bank out = {NULL, 0, 0};
+    uint64_t nz = 0;
+    const int b = pid_bits(o->pidLimit);
+    KeyIdx *ki = (KeyIdx *)malloc(sizeof(KeyIdx) * (in.n ? in.n : 1));
+    for (uint64_t q = 0; q < in.n; ++q) {
+        const Part *p = &in.p[q];
+        if (outside_box(o, v3(p->x, p->y, p->z))) { raise(o, STORM_DERR_COMB_OUTSIDE, p->cell, p->pid); break; }
+        if (!isfinite(p->w) || p->w < 0.0) { raise(o, STORM_DERR_COMB_WEIGHT, p->cell, p->pid); break; }
+        if (p->w == 0.0) continue;
+        const uint64_t run = (uint64_t)shard_of_pid(o, p->pid) * N + p->cell;
+        ki[nz].key = (run << b) | orc_comb_key(o->d.seed, o->step, p->pid, b);
+        ki[nz].idx = q;
+        ++nz;
+    }
+    if (o->derr) { free(ki); return -1; }
+    qsort(ki, nz, sizeof(KeyIdx), cmp_key);
+    uint64_t *start = (uint64_t *)calloc(R + 1, sizeof(uint64_t));
+    for (uint64_t q = 0; q < nz; ++q) start[(ki[q].key >> b) + 1]++;
+    for (uint64_t r = 0; r < R; ++r) start[r + 1] += start[r];
+    /* exchange 2: run weights and counts */
+    double *WC = (double *)calloc(2 * R, sizeof(double));
+    for (uint64_t r = 0; r < R; ++r) {
+        double s = 0.0;
+        for (uint64_t q = start[r]; q < start[r + 1]; ++q) s += in.p[ki[q].idx].w;
+        WC[r] = s;
+        WC[R + r] = (double)(start[r + 1] - start[r]);
+    }
+    int rc = exchange_sum(o, WC, 2 * R);
+    double *Wc = (double *)calloc(N ? N : 1, sizeof(double));
+    uint64_t *cnt = (uint64_t *)calloc(N ? N : 1, sizeof(uint64_t));
+    for (uint64_t c = 0; c < N; ++c) {
+        double w = 0.0;
+        uint64_t k = 0;
+        for (uint32_t s = 0; s < S; ++s) { w += WC[(uint64_t)s * N + c]; k += (uint64_t)WC[R + (uint64_t)s * N + c]; }
+        Wc[c] = w;
+        cnt[c] = k;
+    }
+    double totalWeight = blocked_sum(Wc, N);
+    if (!isfinite(totalWeight)) raise(o, STORM_DERR_COMB_TOTAL, 0, 0);
+    double *xc = (double *)calloc(S + N, sizeof(double));   /* exchange 3: shard census counts | census energy */
+    if (!rc && !o->derr && totalWeight != 0.0) {
+        uint64_t Ntotal = (uint64_t)((double)(N * o->d.comb_nmin) * o->d.comb_factor);
+        const uint64_t Nmin = o->d.comb_nmin;
+        for (uint32_t s = o->shardLo; s < o->shardHi; ++s) {
+            for (uint64_t c = 0; c < N; ++c) {
+                const uint64_t r0 = start[(uint64_t)s * N + c], r1 = start[(uint64_t)s * N + c + 1];
+                if (r0 == r1) continue;
+                const uint64_t before = out.n;
+                uint64_t share = (uint64_t)((double)Ntotal * Wc[c] / totalWeight);
+                uint64_t lo = share > Nmin ? share : Nmin;
+                uint64_t NinCell = (Nmin * 20 < lo) ? Nmin * 20 : lo;
+                if (cnt[c] <= NinCell) {
+                    double weight_ideal = Wc[c] / (double)NinCell;
+                    for (uint64_t q = r0; q < r1; ++q) {
+                        Part p = in.p[ki[q].idx];
+                        if (p.w > 2 * weight_ideal) {
+                            uint64_t Nsplit = (uint64_t)ceil(p.w / weight_ideal);
+                            double ws = p.w / (double)Nsplit;
+                            p.w = ws; p.w0 = ws; p.cell = (uint32_t)c; p.t = 0;
+                            for (uint64_t k = 0; k < Nsplit; ++k) { bank_push(&out, &p); xc[S + c] += ws; }
+                        } else {
+                            bank_push(&out, &p);
+                            xc[S + c] += p.w;
+                        }
+                    }
+                } else {
+                    double new_energy = Wc[c] / (double)NinCell;
+                    double r = orc_uniform(o->d.seed, TAG_COMB, o->step, (uint32_t)c, 0);
+                    double cum = 0.0;
+                    for (uint32_t t = 0; t < s; ++t) cum += WC[(uint64_t)t * N + c];
+                    uint64_t comb_index = teeth_below(cum, r, new_energy);
+                    for (uint64_t q = r0; q < r1; ++q) {
+                        const Part *src = &in.p[ki[q].idx];
+                        while ((cum + src->w) > ((double)comb_index + r) * new_energy) {
+                            ++comb_index;
+                            Part p = *src;
+                            p.cell = (uint32_t)c; p.t = 0; p.w = new_energy; p.w0 = new_energy;
+                            bank_push(&out, &p);
+                            xc[S + c] += new_energy;
+                        }
+                        cum += src->w;
+                    }
+                }
+                xc[s] += (double)(out.n - before);
+            }
+        }
+    }
+    if (!rc && exchange_sum(o, xc, S + N)) rc = -1;
+    for (uint32_t s = 0; s < S; ++s) o->shardCensus[s] = (uint64_t)xc[s];
+    for (uint64_t c = 0; c < N; ++c) o->eradCensus[c] = xc[S + c];
+    /* outside-box repair of the result (:228-250) */
+    for (uint64_t q = 0; q < out.n; ++q) {
+        Part *p = &out.p[q];
+        V3 loc = v3(p->x, p->y, p->z);
+        if (!outside_box(o, loc)) continue;
+        V3 mc = center(o, p->cell), original = loc, direction = vsub(mc, original);
+        double t = 1e-6;
+        while (outside_box(o, loc) && t < 1.0) { loc = vadd(original, vscale(t, direction)); t *= 2; }
+        if (outside_box(o, loc)) loc = mc;
+        p->x = loc.x; p->y = loc.y; p->z = loc.z;
+    }
+    const uint64_t pid0 = census_offset(o, o->shardLo);
+    for (uint64_t q = 0; q < out.n; ++q) { out.p[q].id = pid0 + q; out.p[q].pid = (uint32_t)(pid0 + q); }
+    free(ki); free(start); free(WC); free(Wc); free(cnt); free(xc);
+    free(o->census.p);
+    o->census = out;
+    o->st.census_out = out.n;
+    for (uint64_t q = 0; q < out.n; ++q) o->st.energy_census_out += out.p[q].w;
+    return (rc || o->derr) ? -1 : 0;
+}
+
 /* RadiationIMC::postStep (radiation/RadiationIMC.hpp:1887-2029), gray, no hydro. */
 int orc_phase_poststep(Oracle *o, double dt) {
     const uint64_t N = o->N;
@@ -1223,8 +1459,10 @@ int orc_phase_poststep(Oracle *o, double dt) {
             o->T[i] = eos_T(o, o->mass[i] / o->vol[i], spec);
         }
     }
-    for (uint64_t i = 0; i < N; ++i) o->eradCensus[i] = 0.0;
-    for (uint64_t q = 0; q < o->census.n; ++q) o->eradCensus[o->census.p[q].cell] += o->census.p[q].w;
+    if (o->shards == 1) {   /* sharded: the comb's exchange filled it */
+        for (uint64_t i = 0; i < N; ++i) o->eradCensus[i] = 0.0;
+        for (uint64_t q = 0; q < o->census.n; ++q) o->eradCensus[o->census.p[q].cell] += o->census.p[q].w;
+    }
     o->step++;
     return o->derr ? -1 : 0;
 }

@@ -48,6 +48,10 @@ int orc_get_emission(Oracle *o, uint64_t *photons, double *energy);
 int orc_set_face_temperature(Oracle *o, int face, double T);
 int orc_last_error(Oracle *o, int32_t *derr, uint64_t *cell, uint64_t *particle);
 
+/* particle shards: the same contract as storm_cuda_set_sharding (host buffers,
+ * stream NULL) */
+int orc_set_sharding(Oracle *o, uint32_t shards, uint32_t lo, uint32_t hi, StormExchangeFn exchange, void *user);
+
 /* one segment per item, driven by the item's tape */
 int orc_replay_segments(Oracle *o, StormReplayBatch *b);
 

@@ -57,6 +57,7 @@ def lib():
         L.orc_philox4x32_10.argtypes = [u32p, u32p, u32p]
         L.orc_uniform.restype = C.c_double
         L.orc_uniform.argtypes = [C.c_uint64, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32]
+        L.orc_set_sharding.argtypes = [vp, C.c_uint32, C.c_uint32, C.c_uint32, A.ExchangeFn, vp]
         L.orc_comb_key.restype = C.c_uint32
         L.orc_comb_key.argtypes = [C.c_uint64, C.c_uint32, C.c_uint32, C.c_int]
         _lib = L
@@ -84,6 +85,23 @@ class Oracle:
             lib().orc_last_error(self.h, C.byref(d), C.byref(c), C.byref(p))
             raise RuntimeError(f"oracle {what} failed: {A.DERR_NAMES.get(d.value, d.value)} cell={c.value} "
                                f"particle={p.value}")
+
+    def set_sharding(self, shards, lo, hi, exchange=None):
+        """Hold particle shards [lo, hi) of `shards`; `exchange(values)` sums a
+        float64 numpy array in place over every rank (None: this instance holds
+        every shard)."""
+        if exchange is None:
+            cb = A.ExchangeFn()
+        else:
+            def call(user, values, count, stream):
+                try:
+                    exchange(np.ctypeslib.as_array(values, shape=(count,)))
+                    return 0
+                except Exception:   # reported to the oracle as a failed exchange
+                    return 1
+            cb = A.ExchangeFn(call)
+        self._exchange = cb
+        self._rc(lib().orc_set_sharding(self.h, shards, lo, hi, cb, None), "set_sharding")
 
     def step(self, dt=None):
         st = A.StormStepStats()

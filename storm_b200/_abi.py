@@ -131,6 +131,10 @@ class StormReplayBatch(C.Structure):
     ]
 
 
+# StormExchangeFn: int (*)(void *user, double *values, uint64_t count, void *stream)
+ExchangeFn = C.CFUNCTYPE(C.c_int, C.c_void_p, C.POINTER(C.c_double), C.c_uint64, C.c_void_p)
+
+
 def ptr(arr, ctype=C.c_double):
     """ctypes pointer to a contiguous numpy array (or None)."""
     if arr is None:

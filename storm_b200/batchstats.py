@@ -64,16 +64,21 @@ def summarize(runs):
             "nonzero": (runs != 0.0).mean(0)}
 
 
-def welch_z(a, b):
+def welch_z(a, b, floor=None):
     """Normal-equivalent z of Welch's t for mean(a) - mean(b), per entry, with
     a mask of the entries it is defined on.  a and b are `summarize` results.
     Entries where either side is zero in more than a tenth of its runs are
     masked out: there the batch mean is a handful of rare events and a
-    t-statistic means nothing."""
+    t-statistic means nothing.  So are entries whose standard error is below
+    `floor` (broadcast against the entries): there the runs differ only by
+    rounding, e.g. a cold cell that no particle reached, whose temperature
+    the two solvers round differently."""
     from scipy import stats
     va, vb = a["var"] / a["n"], b["var"] / b["n"]
     se2 = va + vb
     ok = np.isfinite(se2) & (se2 > 0) & (a["nonzero"] >= 0.9) & (b["nonzero"] >= 0.9)
+    if floor is not None:
+        ok &= se2 > np.square(floor)
     t = np.zeros_like(se2)
     df = np.ones_like(se2)
     t[ok] = (a["mean"] - b["mean"])[ok] / np.sqrt(se2[ok])
@@ -104,6 +109,11 @@ def gate(z, alpha=1e-3, threshold=3.0):
             "passed": bool(above <= k_max and max_abs <= z_bound)}
 
 
+# statistical errors below this fraction of a quantity's largest cell value
+# (per recorded step) are rounding, not sampling
+RESOLUTION = 1e-9
+
+
 def compare(runs_a, ref_b, alpha=1e-3):
     """Full comparison of engine runs (K, S, Q, ncells) against a summary of
     the other solver's runs (or its raw runs): the per-cell gate over every
@@ -111,7 +121,8 @@ def compare(runs_a, ref_b, alpha=1e-3):
     the Welch z of each cell-summed total."""
     a = summarize(runs_a)
     b = ref_b if isinstance(ref_b, dict) else summarize(ref_b)
-    z, ok = welch_z(a, b)
+    scale = np.maximum(np.abs(a["mean"]), np.abs(b["mean"])).max(axis=-1, keepdims=True)
+    z, ok = welch_z(a, b, RESOLUTION * scale)
     out = {"all": gate(z[ok], alpha)}
     for q, name in enumerate(QUANTITIES):
         out[name] = gate(z[:, q][ok[:, q]], alpha)
@@ -122,7 +133,8 @@ def compare(runs_a, ref_b, alpha=1e-3):
     else:
         tb = summarize(np.asarray(ref_b).sum(-1))
     zt, okt = welch_z(summarize(totals_a), tb)
-    bound = float(__import__("scipy").stats.norm.isf(alpha / (2.0 * max(int(okt.sum()), 1))))
+    from scipy import stats
+    bound = float(stats.norm.isf(alpha / (2.0 * max(int(okt.sum()), 1))))
     out["totals"] = {"z": zt.tolist(), "max_abs_z": float(np.max(np.abs(zt[okt]))) if okt.any() else 0.0,
                      "z_bound": bound}
     out["passed"] = bool(out["all"]["passed"] and out["totals"]["max_abs_z"] <= bound)

@@ -66,6 +66,9 @@ struct Ctx {
     int32_t withRW;
     int32_t noFeedback;
     int32_t perCellCounters;
+    // particle shards (storm_cuda_set_sharding): 1 = the whole problem on this handle
+    uint32_t shards;
+    const uint64_t *shardBounds;   // 3 (shards + 1) pid bounds: census, cell packets, face packets
     double clight, arad, sigmaSB, kevKelvin;
     double rwMinParticle, rwMinCell;
     double sourceT[6];       // source temperature of each box face [K]

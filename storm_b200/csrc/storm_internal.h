@@ -89,7 +89,7 @@ struct ReplayDev {
     int32_t *usedRW;
 };
 
-void launch_begin(cudaStream_t s, const Bank &b, uint32_t n, double dt, DevStats *st);
+void launch_begin(cudaStream_t s, const Bank &b, uint32_t n, uint32_t pidOffset, double dt, DevStats *st);
 void launch_prestep(cudaStream_t s, const Ctx &C, const CellArrays &A, const OpacityEos &M, double dt);
 void launch_rw_eligibility(cudaStream_t s, const Ctx &C, const CellArrays &A);
 void launch_emission_energy(cudaStream_t s, const Ctx &C, const CellArrays &A, double dt);
@@ -101,8 +101,8 @@ void launch_allocate_if(cudaStream_t s, const Ctx &C, const CellArrays &A, const
                         const int32_t *onlyIf);
 void launch_emission_debit(cudaStream_t s, const Ctx &C, const CellArrays &A, DevStats *st);
 void launch_scan_u64(cudaStream_t s, const uint64_t *in, uint32_t n, uint64_t *out, uint64_t *tileSums, uint64_t *total);
-void launch_emit_cells(cudaStream_t s, const Ctx &C, const CellArrays &A, const uint64_t *offsets, uint64_t total,
-                       const Bank &b, uint32_t bankBase, double dt, DevStats *st);
+void launch_emit_cells(cudaStream_t s, const Ctx &C, const CellArrays &A, const uint64_t *offsets, uint64_t eBegin,
+                       uint64_t count, const Bank &b, uint32_t bankBase, uint32_t pidBase, double dt, DevStats *st);
 void launch_ddmc_rates(cudaStream_t s, const Ctx &C, const CellArrays &A);
 void launch_strat_keys(cudaStream_t s, const Ctx &C, const CensusBank &cen, uint32_t n, uint64_t *keys, uint32_t *vals,
                        uint32_t combKey, int pidBits, const StratParams &S);
@@ -112,8 +112,8 @@ void launch_strat_plan(cudaStream_t s, const Ctx &C, const CombParams &P, const 
                        const uint32_t *start, const double *binW, const double *cellW, const double *Wtot,
                        uint32_t *pCount, double *pWeight, uint64_t *cellCount, double *eradCensus, DevStats *st);
 void launch_face_spectra(cudaStream_t s, const Ctx &C, double *cdf);
-void launch_emit_faces(cudaStream_t s, const Ctx &C, const FaceSources &F, uint64_t total, const Bank &b,
-                       uint32_t bankBase, double dt, DevStats *st);
+void launch_emit_faces(cudaStream_t s, const Ctx &C, const FaceSources &F, uint64_t fBegin, uint64_t count,
+                       const Bank &b, uint32_t bankBase, uint32_t pidBase, double dt, DevStats *st);
 void launch_transport(cudaStream_t s, uint32_t grid, const Ctx &C, const Bank &in, const uint32_t *nIn, const Bank &out,
                       uint32_t *nOut, const CensusBank &cen, uint32_t *nCen, uint32_t K, DevStats *st, int minBlocks);
 int transport_blocks_per_sm(int minBlocks, bool fp32);
@@ -160,6 +160,17 @@ void launch_gather(cudaStream_t s, const Ctx &C, const CensusBank &src, const ui
 void launch_bank_to_census(cudaStream_t s, const Ctx &C, const Bank &src, const CensusBank &dst, uint32_t n);
 void launch_count_bad_cells(cudaStream_t s, const uint32_t *cell, uint32_t n, uint32_t N, int32_t *bad);
 void launch_cell_histogram(cudaStream_t s, const uint32_t *cell, uint32_t n, uint32_t N, uint32_t *count);
+// particle shards (storm_cuda_set_sharding)
+void launch_shard_pack_runs(cudaStream_t s, const double *runW, const uint32_t *start, uint32_t nRuns, double *x);
+void launch_shard_cell_weights(cudaStream_t s, const double *x, uint32_t ncells, uint32_t shards, double *Wc);
+void launch_comb_plan_sharded(cudaStream_t s, const Ctx &C, const CombParams &P, const double *wS,
+                              const uint32_t *start, const double *x, const double *Wc, const double *Wtot,
+                              uint32_t lo, uint32_t hi, uint32_t *pCount, double *pWeight, double *eradCensus,
+                              DevStats *st);
+void launch_shard_pack_census(cudaStream_t s, const uint64_t *pOff, const uint64_t *total, const uint32_t *start,
+                              uint32_t n, uint32_t ncells, uint32_t shards, uint32_t lo, uint32_t hi,
+                              const double *eradCensus, double *x);
+void launch_add_into(cudaStream_t s, double *y, const double *x, uint32_t n);
 void launch_to_float(cudaStream_t s, const double *src, float *dst, uint32_t n);
 void launch_poststep(cudaStream_t s, const Ctx &C, const CellArrays &A, const OpacityEos &M, double dt);
 void launch_replay(cudaStream_t s, const Ctx &C, const ReplayDev &R, uint32_t n);

@@ -238,14 +238,15 @@ __global__ void k_bank_to_global(Ctx C, Bank src, Bank dst, uint32_t n) {
 
 // ------------------------------------------------------------------ step start
 // manager step() (manager/MonteCarloManagerSerial.hpp:393-405): census particles
-// get timeLeft = dt, initialWeight = |w|; they take pids 0..n-1.
-__global__ void k_begin(Bank b, uint32_t n, double dt, DevStats *st) {
+// get timeLeft = dt, initialWeight = |w|; they take pids pidOffset + 0..n-1
+// (pidOffset: the census of the shards below this handle's, 0 unsharded).
+__global__ void k_begin(Bank b, uint32_t n, uint32_t pidOffset, double dt, DevStats *st) {
     double e = 0.0;
     for (uint32_t q = blockIdx.x * blockDim.x + threadIdx.x; q < n; q += gridDim.x * blockDim.x) {
         double w = b.w[q];
         b.t[q] = dt;
         b.w0[q] = fabs(w);
-        b.pid[q] = q;
+        b.pid[q] = pidOffset + q;
         b.draw[q] = 0;
         e += w;
     }
@@ -888,11 +889,15 @@ __device__ __forceinline__ void repair_outside(const Ctx &C, double &x, double &
 // ------------------------------------------------------------------ cell emission
 // generateParticles per-photon loop (radiation/RadiationIMC.hpp:2405-2506) with
 // generateSingleParticle (:2516-2553).  Packet e of cell c draws from stream
-// (TAG_CELL_EMIT, step, e): 4 position, 2 direction, 1 time.
-__global__ void k_emit_cells(Ctx C, CellArrays A, const uint64_t *offsets, uint64_t total, Bank b, uint32_t bankBase,
-                             double dt, DevStats *st) {
+// (TAG_CELL_EMIT, step, e): 4 position, 2 direction, 1 time.  The launch makes
+// packets e in [eBegin, eBegin + count) (a particle shard's range; the whole
+// step's packets unsharded): packet e goes to bank slot bankBase + (e - eBegin)
+// with pid pidBase + e.
+__global__ void k_emit_cells(Ctx C, CellArrays A, const uint64_t *offsets, uint64_t eBegin, uint64_t count, Bank b,
+                             uint32_t bankBase, uint32_t pidBase, double dt, DevStats *st) {
     double esum = 0.0;
-    for (uint64_t e = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; e < total; e += (uint64_t)gridDim.x * blockDim.x) {
+    for (uint64_t j = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; j < count; j += (uint64_t)gridDim.x * blockDim.x) {
+        const uint64_t e = eBegin + j;
         // last cell whose offset <= e
         uint32_t lo = 0, hi = C.ncells;   // offsets has ncells + 1 entries
         while (lo < hi) {
@@ -920,7 +925,7 @@ __global__ void k_emit_cells(Ctx C, CellArrays A, const uint64_t *offsets, uint6
         }
         p.w = energyPerPhoton;
         p.w0 = fabs(p.w);
-        store_any(C, b, bankBase + static_cast<uint32_t>(e), p, bankBase + static_cast<uint32_t>(e), 0);
+        store_any(C, b, bankBase + static_cast<uint32_t>(j), p, pidBase + static_cast<uint32_t>(e), 0);
         esum += p.w;
     }
     esum = warp_sum(esum);
@@ -943,10 +948,11 @@ __device__ __forceinline__ void local_face_vertex(int side, int v, float hx, flo
     else { x = a * hx; y = ((v >= 2) ? 1.0f : -1.0f) * hy; z = sgn * hz; }
 }
 
-__global__ void k_emit_cells32(Ctx C, CellArrays A, const uint64_t *offsets, uint64_t total, Bank b,
-                               uint32_t bankBase, double dt, DevStats *st) {
+__global__ void k_emit_cells32(Ctx C, CellArrays A, const uint64_t *offsets, uint64_t eBegin, uint64_t count, Bank b,
+                               uint32_t bankBase, uint32_t pidBase, double dt, DevStats *st) {
     double esum = 0.0;
-    for (uint64_t e = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; e < total; e += (uint64_t)gridDim.x * blockDim.x) {
+    for (uint64_t j = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; j < count; j += (uint64_t)gridDim.x * blockDim.x) {
+        const uint64_t e = eBegin + j;
         uint32_t lo = 0, hi = C.ncells;   // last cell whose offset <= e
         while (lo < hi) {
             uint32_t mid = (lo + hi) >> 1;
@@ -984,8 +990,8 @@ __global__ void k_emit_cells32(Ctx C, CellArrays A, const uint64_t *offsets, uin
         T.t = dt * rng.open();
         T.w = energyPerPhoton;
         T.w0 = fabs(T.w);
-        const uint32_t slot = bankBase + static_cast<uint32_t>(e);
-        store32(b, slot, T, slot, 0);
+        const uint32_t slot = bankBase + static_cast<uint32_t>(j);
+        store32(b, slot, T, pidBase + static_cast<uint32_t>(e), 0);
         if (C.groups >= 2) {   // GetThermalEnergy (radiation/RadiationIMC.hpp:2495-2500)
             const double nu = mg_thermal_energy(C, c, rng.open());
             if (nu < 0.0) raise_error(C, STORM_DERR_MG_SAMPLE, c, static_cast<uint32_t>(e));
@@ -1002,10 +1008,12 @@ __global__ void k_emit_cells32(Ctx C, CellArrays A, const uint64_t *offsets, uin
 // (boundary/SideTemperature.hpp:114-163, TwoSidesTemperature.hpp:126-199) for the
 // per-face descriptor.  Face packet f draws from (TAG_FACE_EMIT, step, f):
 // 3 position, mu, theta, time.
-__global__ void k_emit_faces(Ctx C, FaceSources F, uint64_t total, Bank b, uint32_t bankBase, double dt,
-                             DevStats *st) {
+__global__ void k_emit_faces(Ctx C, FaceSources F, uint64_t fBegin, uint64_t count, Bank b, uint32_t bankBase,
+                             uint32_t pidBase, double dt, DevStats *st) {
     double esum = 0.0;
-    for (uint64_t f = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; f < total; f += (uint64_t)gridDim.x * blockDim.x) {
+    for (uint64_t slot = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; slot < count;
+         slot += (uint64_t)gridDim.x * blockDim.x) {
+        const uint64_t f = fBegin + slot;
         uint32_t lo = 0, hi = F.count;
         while (lo < hi) {
             uint32_t mid = (lo + hi) >> 1;
@@ -1067,8 +1075,7 @@ __global__ void k_emit_faces(Ctx C, FaceSources F, uint64_t total, Bank b, uint3
         p.cell = c;
         repair_outside(C, p.x, p.y, p.z, C.xc[i], C.yc[j], C.zc[k]);
         p.w0 = fabs(p.w);
-        const uint32_t slot = bankBase + static_cast<uint32_t>(f);
-        store_any(C, b, slot, p, slot, 0);
+        store_any(C, b, bankBase + static_cast<uint32_t>(slot), p, pidBase + static_cast<uint32_t>(f), 0);
         esum += p.w;
     }
     esum = warp_sum(esum);
@@ -1446,6 +1453,29 @@ __device__ __forceinline__ uint32_t comb_hash(uint32_t pid, uint32_t key, int b)
     h ^= h >> ((b + 1) / 2);
     return h;
 }
+// ------------------------------------------------------------------ particle shards
+// The shard a pid belongs to: census pids by the shards' census ranges, then
+// the step's cell packets and face packets, each cut into equal ranges.
+// C.shardBounds holds the three sets of S + 1 pid bounds, one after the other.
+__device__ __forceinline__ uint32_t shard_of_pid(const Ctx &C, uint32_t pid) {
+    const uint32_t S = C.shards;
+    const uint64_t *B = C.shardBounds;
+    const uint64_t p = pid;
+    const uint32_t g = p < B[S] ? 0u : (p < B[(S + 1) + S] ? 1u : 2u);
+    const uint64_t *b = B + static_cast<size_t>(g) * (S + 1);
+    uint32_t lo = 0, hi = S;   // the last shard whose first pid is <= p
+    while (hi - lo > 1) {
+        const uint32_t mid = (lo + hi) >> 1;
+        if (b[mid] <= p) lo = mid; else hi = mid;
+    }
+    return lo;
+}
+
+// The cell of a comb run: runs are (shard, cell) when sharded, else (cell, bin).
+__device__ __forceinline__ uint32_t cell_of_run(const Ctx &C, uint64_t run, uint32_t bins) {
+    return C.shards > 1 ? static_cast<uint32_t>(run % C.ncells) : static_cast<uint32_t>(run / bins);
+}
+
 __global__ void k_comb_keys(Ctx C, CensusBank cen, uint32_t n, uint64_t *keys, uint32_t *vals, uint32_t combKey,
                             int pidBits) {
     for (uint32_t q = blockIdx.x * blockDim.x + threadIdx.x; q < n; q += gridDim.x * blockDim.x) {
@@ -1462,7 +1492,12 @@ __global__ void k_comb_keys(Ctx C, CensusBank cen, uint32_t n, uint64_t *keys, u
         if (badWeight) raise_error(C, STORM_DERR_COMB_WEIGHT, cell, pid);
         // zero, negative and non-finite weights never reach the per-cell loops
         if (w == 0.0 || badWeight || cell >= C.ncells) cell = C.ncells;
-        keys[q] = (static_cast<uint64_t>(cell) << pidBits) | comb_hash(pid, combKey, pidBits);
+        // sharded: runs (shard, cell), shard-major; the excluded particles after every run
+        uint64_t run = cell;
+        if (C.shards > 1)
+            run = cell >= C.ncells ? static_cast<uint64_t>(C.ncells) * C.shards
+                                   : static_cast<uint64_t>(shard_of_pid(C, pid)) * C.ncells + cell;
+        keys[q] = (run << pidBits) | comb_hash(pid, combKey, pidBits);
         vals[q] = q;
     }
 }
@@ -1957,6 +1992,132 @@ __global__ void k_comb_plan(Ctx C, CombParams P, const double *wS, const uint32_
     if ((threadIdx.x & 31) == 0 && eOut != 0.0) atomicAdd(&st->eCensusOut, eOut);
 }
 
+// #{k >= 0 : (k + r) E < P}: the comb index a sequential walk holds once it
+// has passed weight P (the loop condition of :203-222 with cum = P).
+__device__ __forceinline__ uint64_t teeth_below(double P, double r, double E) {
+    if (!(P > 0.0)) return 0;
+    const double g = P / E - r;
+    uint64_t k = g > 0.0 ? static_cast<uint64_t>(ceil(g)) : 0;
+    while (k > 0 && (static_cast<double>(k - 1) + r) * E >= P) --k;
+    while ((static_cast<double>(k) + r) * E < P) ++k;
+    return k;
+}
+
+// Exchange 2 of a sharded comb: every (shard, cell) run's weight and particle
+// count, this handle's runs filled and the others zero, as doubles.
+__global__ void k_shard_pack_runs(const double *runW, const uint32_t *start, uint32_t nRuns, double *x) {
+    for (uint32_t r = blockIdx.x * blockDim.x + threadIdx.x; r < nRuns; r += gridDim.x * blockDim.x) {
+        x[r] = runW[r];
+        x[nRuns + r] = static_cast<double>(start[r + 1] - start[r]);
+    }
+}
+
+// A cell's global weight: its runs' weights added in shard order (every
+// handle adds the same numbers in the same order).
+__global__ void k_shard_cell_weights(const double *x, uint32_t ncells, uint32_t shards, double *Wc) {
+    for (uint32_t c = blockIdx.x * blockDim.x + threadIdx.x; c < ncells; c += gridDim.x * blockDim.x) {
+        double w = 0.0;
+        for (uint32_t sh = 0; sh < shards; ++sh) w += x[static_cast<size_t>(sh) * ncells + c];
+        Wc[c] = w;
+    }
+}
+
+// CombPopulationControl::activate's plan over particle shards.  x holds every
+// run's weight (S N) and count (S N) after exchange 2; Wc the cells' global
+// weights.  A cell's targets come from its global weight and count; a combed
+// cell's teeth run along its runs in shard order, run s starting at the
+// weight P of the runs below it and at comb index teeth_below(P).  Only this
+// handle's shards [lo, hi) hold particles here.  eradCensus gets this
+// handle's part of each cell's census energy.
+__global__ void k_comb_plan_sharded(Ctx C, CombParams P, const double *wS, const uint32_t *start, const double *x,
+                                    const double *Wc, const double *Wtot, uint32_t lo, uint32_t hi,
+                                    uint32_t *pCount, double *pWeight, double *eradCensus, DevStats *st) {
+    const double tot = *Wtot;
+    if (!isfinite(tot)) {
+        if (blockIdx.x == 0 && threadIdx.x == 0) raise_error(C, STORM_DERR_COMB_TOTAL, 0, 0);
+    }
+    const uint32_t N = C.ncells, S = C.shards;
+    const size_t R = static_cast<size_t>(S) * N;
+    double eOut = 0.0;
+    for (uint32_t c = blockIdx.x * blockDim.x + threadIdx.x; c < N; c += gridDim.x * blockDim.x) {
+        uint64_t cnt = 0;
+        for (uint32_t sh = 0; sh < S; ++sh) cnt += static_cast<uint64_t>(x[R + static_cast<size_t>(sh) * N + c]);
+        double ecell = 0.0;
+        const bool none = tot == 0.0 || !isfinite(tot) || cnt == 0;
+        const CombCell cc = none ? CombCell{} : comb_cell_params(C, P, c, static_cast<uint32_t>(cnt), Wc[c], tot);
+        double below = 0.0;   // weight of this cell's runs in the shards before sh
+        for (uint32_t sh = 0; sh < hi; ++sh) {
+            const size_t run = static_cast<size_t>(sh) * N + c;
+            if (sh < lo) {
+                below += x[run];
+                continue;
+            }
+            const uint32_t a = start[run], b = start[run + 1];
+            if (none) {
+                for (uint32_t q = a; q < b; ++q) pCount[q] = 0;
+            } else if (cc.mode == 0) {
+                for (uint32_t q = a; q < b; ++q) {
+                    const double w = wS[q];
+                    if (w > 2 * cc.w_ideal) {
+                        const uint64_t ns = static_cast<uint64_t>(ceil(w / cc.w_ideal));
+                        const double ws = w / static_cast<double>(ns);
+                        for (uint64_t k = 0; k < ns; ++k) ecell += ws;
+                        pCount[q] = static_cast<uint32_t>(ns);
+                        pWeight[q] = ws;
+                    } else {
+                        ecell += w;
+                        pCount[q] = 1u | KEEP;
+                        pWeight[q] = w;
+                    }
+                }
+            } else {
+                double cum = below;
+                uint64_t k = teeth_below(cum, cc.r, cc.e);
+                for (uint32_t q = a; q < b; ++q) {
+                    const double w = wS[q];
+                    const uint64_t k0 = k;
+                    while ((cum + w) > (static_cast<double>(k) + cc.r) * cc.e) {
+                        ++k;
+                        ecell += cc.e;
+                    }
+                    cum += w;
+                    pCount[q] = static_cast<uint32_t>(k - k0);
+                    pWeight[q] = cc.e;
+                }
+            }
+            below += x[run];
+        }
+        eradCensus[c] = ecell;
+        eOut += ecell;
+    }
+    eOut = warp_sum(eOut);
+    if ((threadIdx.x & 31) == 0 && eOut != 0.0) atomicAdd(&st->eCensusOut, eOut);
+}
+
+// Exchange 3 of a sharded comb: this handle's census particles per shard (the
+// copies its runs of shard s produce: the exclusive scan of the copy counts at
+// the shard's run boundaries) and its part of each cell's census energy.
+__global__ void k_shard_pack_census(const uint64_t *pOff, const uint64_t *total, const uint32_t *start, uint32_t n,
+                                    uint32_t ncells, uint32_t shards, uint32_t lo, uint32_t hi,
+                                    const double *eradCensus, double *x) {
+    const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t < shards) {
+        double v = 0.0;
+        if (t >= lo && t < hi) {
+            const uint32_t a = start[static_cast<size_t>(t) * ncells], b = start[static_cast<size_t>(t + 1) * ncells];
+            const uint64_t oa = a < n ? pOff[a] : *total, ob = b < n ? pOff[b] : *total;
+            v = static_cast<double>(ob - oa);
+        }
+        x[t] = v;
+    }
+    for (uint32_t c = t; c < ncells; c += gridDim.x * blockDim.x) x[shards + c] = eradCensus[c];
+}
+
+// y[i] += x[i]
+__global__ void k_add_into(double *y, const double *x, uint32_t n) {
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) y[i] += x[i];
+}
+
 // One thread per sorted particle writes its copies at its output offset.
 // The exclusive prefix of the copy counts over sorted particles is the output
 // position: cells are contiguous in sorted order and the output is cell-major.
@@ -2017,7 +2178,7 @@ __global__ void k_comb_emit(Ctx C, CensusBank cen, const uint32_t *idx, const ui
             const uint32_t m = raw[u] & ~KEEP;
             if (m == 0) continue;
             const uint32_t q = base + u * stride;
-            const uint32_t c = static_cast<uint32_t>((sortedKeys[q] >> pidBits) / bins);   // (cell, bin) keys
+            const uint32_t c = cell_of_run(C, sortedKeys[q] >> pidBits, bins);
             const uint64_t o = pOffset[q];
             const double wNew = pWeight[q];
             if constexpr (FP32) {
@@ -2159,7 +2320,7 @@ __global__ void k_comb_emit_out(Ctx C, CensusBank cen, const uint32_t *idx, cons
             const uint32_t o = base + u * stride;
             if (o >= total) continue;
             const uint32_t q = qs[u];
-            const uint32_t c = static_cast<uint32_t>((sortedKeys[q] >> pidBits) / bins);   // (cell, bin) keys
+            const uint32_t c = cell_of_run(C, sortedKeys[q] >> pidBits, bins);
             const double wNew = pWeight[q];
             if constexpr (FP32) {
                 const uint4 a = rec[u][0], b = rec[u][1], d = rec[u][2];
@@ -2550,8 +2711,8 @@ static inline uint32_t grid_for(uint64_t n, uint32_t block, uint32_t cap) {
     return static_cast<uint32_t>(g < cap ? g : cap);
 }
 
-void launch_begin(cudaStream_t s, const Bank &b, uint32_t n, double dt, DevStats *st) {
-    k_begin<<<grid_for(n, 256, 4096), 256, 0, s>>>(b, n, dt, st);
+void launch_begin(cudaStream_t s, const Bank &b, uint32_t n, uint32_t pidOffset, double dt, DevStats *st) {
+    k_begin<<<grid_for(n, 256, 4096), 256, 0, s>>>(b, n, pidOffset, dt, st);
 }
 void launch_prestep(cudaStream_t s, const Ctx &C, const CellArrays &A, const OpacityEos &M, double dt) {
     k_prestep<<<grid_for(C.ncells, 256, 8192), 256, 0, s>>>(C, A, M, dt);
@@ -2591,18 +2752,20 @@ void launch_scan_u64(cudaStream_t s, const uint64_t *in, uint32_t n, uint64_t *o
     k_scan_sums<<<1, 1024, 0, s>>>(tileSums, tiles, total);
     k_scan_add<<<tiles, 1024, 0, s>>>(out, n, tileSums, total);
 }
-void launch_emit_cells(cudaStream_t s, const Ctx &C, const CellArrays &A, const uint64_t *offsets, uint64_t total,
-                       const Bank &b, uint32_t bankBase, double dt, DevStats *st) {
-    if (!total) return;
+void launch_emit_cells(cudaStream_t s, const Ctx &C, const CellArrays &A, const uint64_t *offsets, uint64_t eBegin,
+                       uint64_t count, const Bank &b, uint32_t bankBase, uint32_t pidBase, double dt, DevStats *st) {
+    if (!count) return;
     if (C.fp32 && !C.poly)   // polyhedral cells: the FP64 sampler, then the cell frame
-        k_emit_cells32<<<grid_for(total, 256, 148 * 16), 256, 0, s>>>(C, A, offsets, total, b, bankBase, dt, st);
+        k_emit_cells32<<<grid_for(count, 256, 148 * 16), 256, 0, s>>>(C, A, offsets, eBegin, count, b, bankBase,
+                                                                      pidBase, dt, st);
     else
-        k_emit_cells<<<grid_for(total, 256, 148 * 16), 256, 0, s>>>(C, A, offsets, total, b, bankBase, dt, st);
+        k_emit_cells<<<grid_for(count, 256, 148 * 16), 256, 0, s>>>(C, A, offsets, eBegin, count, b, bankBase, pidBase,
+                                                                    dt, st);
 }
-void launch_emit_faces(cudaStream_t s, const Ctx &C, const FaceSources &F, uint64_t total, const Bank &b,
-                       uint32_t bankBase, double dt, DevStats *st) {
-    if (!total) return;
-    k_emit_faces<<<grid_for(total, 256, 148 * 16), 256, 0, s>>>(C, F, total, b, bankBase, dt, st);
+void launch_emit_faces(cudaStream_t s, const Ctx &C, const FaceSources &F, uint64_t fBegin, uint64_t count,
+                       const Bank &b, uint32_t bankBase, uint32_t pidBase, double dt, DevStats *st) {
+    if (!count) return;
+    k_emit_faces<<<grid_for(count, 256, 148 * 16), 256, 0, s>>>(C, F, fBegin, count, b, bankBase, pidBase, dt, st);
 }
 void launch_face_spectra(cudaStream_t s, const Ctx &C, double *cdf) { k_face_spectra<<<1, 32, 0, s>>>(C, cdf); }
 void launch_strat_keys(cudaStream_t s, const Ctx &C, const CensusBank &cen, uint32_t n, uint64_t *keys, uint32_t *vals,
@@ -2840,6 +3003,29 @@ __global__ void k_cell_histogram(const uint32_t *cell, uint32_t n, uint32_t N, u
 }
 void launch_cell_histogram(cudaStream_t s, const uint32_t *cell, uint32_t n, uint32_t N, uint32_t *count) {
     if (n) k_cell_histogram<<<grid_for(n, 256, 8192), 256, 0, s>>>(cell, n, N, count);
+}
+void launch_shard_pack_runs(cudaStream_t s, const double *runW, const uint32_t *start, uint32_t nRuns, double *x) {
+    k_shard_pack_runs<<<grid_for(nRuns, 256, 8192), 256, 0, s>>>(runW, start, nRuns, x);
+}
+void launch_shard_cell_weights(cudaStream_t s, const double *x, uint32_t ncells, uint32_t shards, double *Wc) {
+    k_shard_cell_weights<<<grid_for(ncells, 256, 8192), 256, 0, s>>>(x, ncells, shards, Wc);
+}
+void launch_comb_plan_sharded(cudaStream_t s, const Ctx &C, const CombParams &P, const double *wS,
+                              const uint32_t *start, const double *x, const double *Wc, const double *Wtot,
+                              uint32_t lo, uint32_t hi, uint32_t *pCount, double *pWeight, double *eradCensus,
+                              DevStats *st) {
+    k_comb_plan_sharded<<<grid_for(C.ncells, 128, 8192), 128, 0, s>>>(C, P, wS, start, x, Wc, Wtot, lo, hi, pCount,
+                                                                      pWeight, eradCensus, st);
+}
+void launch_shard_pack_census(cudaStream_t s, const uint64_t *pOff, const uint64_t *total, const uint32_t *start,
+                              uint32_t n, uint32_t ncells, uint32_t shards, uint32_t lo, uint32_t hi,
+                              const double *eradCensus, double *x) {
+    const uint32_t m = ncells > shards ? ncells : shards;
+    k_shard_pack_census<<<grid_for(m, 256, 8192), 256, 0, s>>>(pOff, total, start, n, ncells, shards, lo, hi,
+                                                                eradCensus, x);
+}
+void launch_add_into(cudaStream_t s, double *y, const double *x, uint32_t n) {
+    if (n) k_add_into<<<grid_for(n, 256, 8192), 256, 0, s>>>(y, x, n);
 }
 void launch_count_bad_cells(cudaStream_t s, const uint32_t *cell, uint32_t n, uint32_t N, int32_t *bad) {
     if (n) k_count_bad_cells<<<grid_for(n, 256, 4096), 256, 0, s>>>(cell, n, N, bad);

@@ -107,6 +107,18 @@ struct StormHandle {
     uint64_t nCensus = 0;            // particles at the head of bankA
     uint64_t nBank = 0;              // particles in bankA after emission
     uint64_t pidLimit = 1;           // every pid of the current census is below this (comb key width)
+    // particle shards (storm_cuda_set_sharding): this handle holds shards [shardLo, shardHi) of `shards`
+    uint32_t shards = 1, shardLo = 0, shardHi = 1;
+    StormExchangeFn exchange = nullptr;
+    void *exchangeUser = nullptr;
+    std::vector<uint64_t> shardCensus;   // census particles per shard after the last comb (every shard)
+    uint64_t nCenGlobal = 0, nCellEmitGlobal = 0, nFaceEmitGlobal = 0;   // this step's global counts
+    double *dep = nullptr;           // this handle's material deposits of the step (N)
+    double *xbuf = nullptr;          // exchange buffer (max(2 N, 2 S N, S + N) doubles)
+    double *shardWc = nullptr;       // cells' global census weights (N)
+    double *shardRunW = nullptr;     // run weights (S N)
+    uint32_t *shardStart = nullptr;  // run starts (S N + 2)
+    uint64_t *shardBounds = nullptr; // 3 (S + 1) pid bounds (Ctx::shardBounds)
     uint32_t step = 0;
     uint32_t K = 8, maxRounds = 4096;
     int minBlocks = 3;               // transport occupancy variant (__launch_bounds__ min blocks); 4 for FP32
@@ -1112,6 +1124,8 @@ int storm_cuda_create(const StormProblemDesc *d, StormHandle **out) {
     C.withRW = d->with_random_walk;
     C.noFeedback = d->no_hydro_feedback;
     C.perCellCounters = d->per_cell_segment_counters;
+    C.shards = 1;
+    C.shardBounds = nullptr;
     C.clight = d->clight; C.arad = d->arad; C.sigmaSB = d->sigma_sb; C.kevKelvin = d->kev_kelvin;
     C.rwMinParticle = d->rw_min_particle_optical_depth;
     C.rwMinCell = d->rw_min_cell_optical_depth;
@@ -1174,7 +1188,7 @@ int storm_cuda_destroy(StormHandle *h) {
                   h->ddmcRate, h->ddmcCut, h->ddmc32, h->stratBounds, h->stratBinW, h->stratStart,
                   h->runCursor, h->runScan, h->longRuns, h->bucketFlags,
                   h->cfo, h->cfN, h->cfP, h->cfNext, h->cfFace, h->mpx, h->mpy, h->mpz, h->fvo, h->fvi, h->vtx,
-                  h->chord, h->cfN32};
+                  h->chord, h->cfN32, h->dep, h->xbuf, h->shardWc, h->shardRunW, h->shardStart, h->shardBounds};
     for (void *p : ps) device_pool().free(p);
     cudaEvent_t evs[] = {h->evStart, h->evTransport0, h->evTransport1, h->evEnd, h->evAfterEmit, h->evAfterComb};
     bool complete = h->stream != nullptr;
@@ -1206,8 +1220,20 @@ int storm_cuda_phase_begin(StormHandle *h, double dt) {
     CK(cudaMemsetAsync(h->dErr, 0, 4 * sizeof(int32_t), h->stream));
     refresh_ctx(h);
     h->stats.census_in = h->nCensus;
+    // sharded: this handle's census carries the global pids that follow the lower shards' census
+    uint64_t pid0 = 0;
+    if (h->shards > 1) {
+        h->nCenGlobal = 0;
+        for (uint32_t q = 0; q < h->shards; ++q) {
+            if (q == h->shardLo) pid0 = h->nCenGlobal;
+            h->nCenGlobal += h->shardCensus[q];
+        }
+    } else {
+        h->nCenGlobal = h->nCensus;
+    }
     if (h->nCensus) {
-        launch_begin(h->stream, h->bankA, static_cast<uint32_t>(h->nCensus), dt, h->dStats);
+        launch_begin(h->stream, h->bankA, static_cast<uint32_t>(h->nCensus), static_cast<uint32_t>(pid0), dt,
+                     h->dStats);
         ++h->launches;
     }
     h->nBank = h->nCensus;
@@ -1262,24 +1288,80 @@ int storm_cuda_phase_emit(StormHandle *h, double dt) {
     }
     launch_emission_debit(h->stream, h->C, h->A, h->dStats);
     ++h->launches;
-    uint64_t ne = back.total;
+    // The step's packets are numbered over the whole problem: cell packet e has
+    // pid nCen + e, face packet f pid nCen + nE + f.  A sharded handle makes
+    // its shards' share of each numbering (equal contiguous ranges per shard).
+    const uint64_t ne = back.total;
     const uint64_t nf = h->fsTotal;
-    const uint64_t total = h->nCensus + ne + nf;
+    h->nCellEmitGlobal = ne;
+    h->nFaceEmitGlobal = nf;
+    const uint32_t S = h->shards;
+    auto cut = [S](uint64_t n, uint32_t sh) {
+        return static_cast<uint64_t>((static_cast<unsigned __int128>(n) * sh) / S);
+    };
+    const uint64_t eLo = cut(ne, h->shardLo), eHi = cut(ne, h->shardHi);
+    const uint64_t fLo = cut(nf, h->shardLo), fHi = cut(nf, h->shardHi);
+    const uint64_t total = h->nCensus + (eHi - eLo) + (fHi - fLo);
+    if (h->nCenGlobal + ne + nf > 0xFFFFFFFFull) return STORM_ERR_CAPACITY;   // pids are 32-bit
     int rc = ensure_capacity(h, total, h->nCensus);
     if (rc != STORM_OK) return rc;
-    launch_emit_cells(h->stream, h->C, h->A, h->offsets, ne, h->bankA, static_cast<uint32_t>(h->nCensus), dt, h->dStats);
+    if (S > 1) {   // the shards' pid bounds: census, cell packets, face packets
+        std::vector<uint64_t> bnd(3 * static_cast<size_t>(S + 1));
+        uint64_t off = 0;
+        for (uint32_t q = 0; q <= S; ++q) {
+            bnd[q] = off;
+            if (q < S) off += h->shardCensus[q];
+            bnd[(S + 1) + q] = h->nCenGlobal + cut(ne, q);
+            bnd[2 * (S + 1) + q] = h->nCenGlobal + ne + cut(nf, q);
+        }
+        CK(cudaMemcpyAsync(h->shardBounds, bnd.data(), bnd.size() * sizeof(uint64_t), cudaMemcpyHostToDevice,
+                           h->stream));
+        CK(cudaStreamSynchronize(h->stream));   // bnd is pageable and goes out of scope
+    }
+    launch_emit_cells(h->stream, h->C, h->A, h->offsets, eLo, eHi - eLo, h->bankA, static_cast<uint32_t>(h->nCensus),
+                      static_cast<uint32_t>(h->nCenGlobal), dt, h->dStats);
     FaceSources F{h->fsCell, h->fsSide, h->fsOffset, h->fsCount};
     if (nf && h->C.groups >= 2 && std::memcmp(h->faceCdfT, h->C.sourceT, sizeof(h->faceCdfT)) != 0) {
         launch_face_spectra(h->stream, h->C, h->faceCdf);
         ++h->launches;
         std::memcpy(h->faceCdfT, h->C.sourceT, sizeof(h->faceCdfT));
     }
-    launch_emit_faces(h->stream, h->C, F, nf, h->bankA, static_cast<uint32_t>(h->nCensus + ne), dt, h->dStats);
-    h->launches += (ne ? 1 : 0) + (nf ? 1 : 0);
+    launch_emit_faces(h->stream, h->C, F, fLo, fHi - fLo, h->bankA,
+                      static_cast<uint32_t>(h->nCensus + (eHi - eLo)), static_cast<uint32_t>(h->nCenGlobal + ne), dt,
+                      h->dStats);
+    h->launches += (eHi > eLo ? 1 : 0) + (fHi > fLo ? 1 : 0);
     CK(cudaGetLastError());
-    h->stats.emitted_cells = ne;
-    h->stats.emitted_faces = nf;
+    h->stats.emitted_cells = eHi - eLo;
+    h->stats.emitted_faces = fHi - fLo;
     h->nBank = total;
+    return STORM_OK;
+}
+
+// Hand `count` doubles of the handle's exchange buffer to the exchange
+// callback (an in-place sum over the ranks, ordered on the handle's stream).
+static int exchange_sum(StormHandle *h, uint64_t count) {
+    if (!h->exchange) return STORM_OK;   // one handle holds every shard
+    if (h->exchange(h->exchangeUser, h->xbuf, count, h->stream) != 0) {
+        h->errMsg = "the particle-shard exchange callback failed";
+        return STORM_ERR_INVALID_ARG;
+    }
+    return STORM_OK;
+}
+
+// Exchange 1 of a sharded step: the per-cell deposits and time-averaged
+// radiation tallies summed over the ranks; the deposits then join the
+// material energy.
+static int exchange_tallies(StormHandle *h) {
+    const size_t N = h->N;
+    h->C.eint = h->A.eint;
+    CK(cudaMemcpyAsync(h->xbuf, h->dep, N * sizeof(double), cudaMemcpyDeviceToDevice, h->stream));
+    CK(cudaMemcpyAsync(h->xbuf + N, h->A.eradAvg, N * sizeof(double), cudaMemcpyDeviceToDevice, h->stream));
+    int rc = exchange_sum(h, 2 * N);
+    if (rc != STORM_OK) return rc;
+    launch_add_into(h->stream, h->A.eint, h->xbuf, static_cast<uint32_t>(N));
+    CK(cudaMemcpyAsync(h->A.eradAvg, h->xbuf + N, N * sizeof(double), cudaMemcpyDeviceToDevice, h->stream));
+    ++h->launches;
+    CK(cudaGetLastError());
     return STORM_OK;
 }
 
@@ -1287,7 +1369,14 @@ int storm_cuda_phase_transport(StormHandle *h) {
     if (!h) return STORM_ERR_INVALID_ARG;
     refresh_ctx(h);
     const uint64_t n0 = h->nBank;
-    h->pidLimit = n0 ? n0 : 1;   // transport pids are bank slots
+    // every pid of the step, over all shards, is below this
+    h->pidLimit = h->nCenGlobal + h->nCellEmitGlobal + h->nFaceEmitGlobal;
+    if (h->pidLimit == 0) h->pidLimit = 1;
+    const bool sharded = h->shards > 1;
+    if (sharded) {   // deposits go to a zeroed array first; exchange 1 sums them over the ranks
+        CK(cudaMemsetAsync(h->dep, 0, sizeof(double) * h->N, h->stream));
+        h->C.eint = h->dep;
+    }
     CK(cudaEventRecord(h->evTransport0, h->stream));
     CK(cudaMemsetAsync(h->counts, 0, sizeof(uint32_t) * (h->maxRounds + 2), h->stream));
     if (h->desc.per_cell_segment_counters) CK(cudaMemsetAsync(h->segs, 0, sizeof(uint32_t) * h->N, h->stream));
@@ -1342,7 +1431,7 @@ int storm_cuda_phase_transport(StormHandle *h) {
         cudaEventElapsedTime(&ms, h->evTransport0, h->evTransport1);
         h->lastTransportMs = ms;
         h->nBank = 0;
-        return STORM_OK;
+        return sharded ? exchange_tallies(h) : STORM_OK;
     }
     const uint32_t grid = grid_transport(n0, h->transportGrid);
     uint32_t r = 0;
@@ -1404,7 +1493,7 @@ int storm_cuda_phase_transport(StormHandle *h) {
     cudaEventElapsedTime(&ms, h->evTransport0, h->evTransport1);
     h->lastTransportMs = ms;
     h->nBank = 0;
-    return STORM_OK;
+    return sharded ? exchange_tallies(h) : STORM_OK;
 }
 
 // bits of the comb's pid hash: the smallest b >= 1 with 2^b >= pidLimit
@@ -1414,9 +1503,155 @@ int pid_bits(const StormHandle *h) {
     return b;
 }
 
+// CombPopulationControl::activate over particle shards (storm_cuda_set_sharding).
+// The census is sorted by (shard, cell, keyed hash of pid); the (shard, cell)
+// runs' weights and counts go through exchange 2, so that the plan sees every
+// cell's global weight and count and each run's offset along its cell; the
+// new census stays in (shard, cell) order, and exchange 3 gives every rank the
+// shards' census counts and the cells' census energy.  Every rank makes both
+// exchanges exactly once per step, whatever its own census holds.
+static int comb_sharded(StormHandle *h) {
+    const uint32_t n = static_cast<uint32_t>(h->stats.census_out_pre_comb);
+    const uint32_t N = h->N, S = h->shards;
+    const uint64_t R = static_cast<uint64_t>(S) * N;
+    CK(cudaMemsetAsync(h->A.eradCensus, 0, sizeof(double) * N, h->stream));
+    const uint32_t combKey = [&] {
+        auto fm = [](uint32_t x) {
+            x ^= x >> 16; x *= 0x85ebca6bu; x ^= x >> 13; x *= 0xc2b2ae35u; x ^= x >> 16;
+            return x;
+        };
+        return fm(static_cast<uint32_t>(h->desc.seed) ^ fm(h->step * 0x9E3779B9u + static_cast<uint32_t>(h->desc.seed >> 32)));
+    }();
+    const int pidBits = pid_bits(h);
+    int runBits = 0;
+    while ((1ull << runBits) <= R) ++runBits;
+    if (pidBits + runBits > 64) return STORM_ERR_CAPACITY;
+    uint32_t *start = h->shardStart;
+    const uint64_t *skeys = h->keysAlt;
+    const uint32_t *idx = h->valsAlt;
+    double *wS = h->pWeight;
+    CombParams P;
+    P.nmin = h->desc.comb_nmin;
+    P.ntotal = static_cast<uint64_t>(static_cast<double>(static_cast<uint64_t>(N) * h->desc.comb_nmin) * h->desc.comb_factor);
+    if (n == 0) {
+        CK(cudaMemsetAsync(start, 0, sizeof(uint32_t) * (R + 1), h->stream));
+        CK(cudaMemsetAsync(h->dTotalU64, 0, sizeof(uint64_t), h->stream));
+    } else {
+        launch_comb_keys(h->stream, h->C, h->bankC, n, h->keys, h->vals, combKey, pidBits);
+        ++h->launches;
+        bool sorted = false;
+        if (R + 1 < 0xFFFFFFF0ull) {   // the per-run bucket sort; its flag is read before the exchanges
+            const size_t len = R + 1;
+            if (len > h->runLen) {
+                dfree(h, h->runCursor, h->runLen);
+                dfree(h, h->runScan, bucket_scan_words(static_cast<uint32_t>(h->runLen)));
+                CK(dalloc(h, &h->runCursor, len));
+                CK(dalloc(h, &h->runScan, bucket_scan_words(static_cast<uint32_t>(len))));
+                h->runLen = len;
+            }
+            const size_t longNeed = bucket_long_capacity(n);
+            if (longNeed > h->longCap) {
+                dfree(h, h->longRuns, h->longCap);
+                CK(dalloc(h, &h->longRuns, longNeed));
+                h->longCap = longNeed;
+            }
+            if (!h->bucketFlags) CK(dalloc(h, &h->bucketFlags, 2));
+            launch_bucket_sort(h->stream, h->C, h->bankC, h->keys, n, pidBits, static_cast<uint32_t>(R), start,
+                               h->runCursor, h->runScan, h->keysAlt, h->valsAlt, wS, h->longRuns,
+                               static_cast<uint32_t>(h->longCap), h->bucketFlags);
+            h->launches += 7;
+            uint32_t flags[2] = {0, 0};
+            const Readback r[1] = {{flags, h->bucketFlags, sizeof(flags)}};
+            const int rc = read_many(h, r, 1, true);
+            if (rc != STORM_OK) return rc;
+            sorted = flags[1] == 0;
+            if (!sorted) {   // the keys again: the bucket sort consumed them
+                launch_comb_keys(h->stream, h->C, h->bankC, n, h->keys, h->vals, combKey, pidBits);
+                ++h->launches;
+            }
+        }
+        if (!sorted) {
+            const int alt = launch_radix_sort(h->stream, h->keys, h->vals, h->keysAlt, h->valsAlt, n,
+                                              pidBits + runBits, h->tileHist);
+            skeys = alt ? h->keysAlt : h->keys;
+            idx = alt ? h->valsAlt : h->vals;
+            launch_comb_ranges(h->stream, skeys, n, static_cast<uint32_t>(R), start, pidBits);
+            launch_sorted_weights(h->stream, h->C, h->bankC, idx, n, wS);
+            h->launches += 5 * ((pidBits + runBits + 7) / 8) + 2;
+        }
+    }
+    // exchange 2: run weights and counts
+    launch_comb_cell_sums(h->stream, wS, start, static_cast<uint32_t>(R), h->shardRunW);
+    launch_shard_pack_runs(h->stream, h->shardRunW, start, static_cast<uint32_t>(R), h->xbuf);
+    h->launches += 2;
+    CK(cudaGetLastError());
+    int rc = exchange_sum(h, 2 * R);
+    if (rc != STORM_OK) return rc;
+    launch_shard_cell_weights(h->stream, h->xbuf, N, S, h->shardWc);
+    launch_blocked_sum(h->stream, h->shardWc, N, h->combWtot);
+    launch_comb_plan_sharded(h->stream, h->C, P, wS, start, h->xbuf, h->shardWc, h->combWtot, h->shardLo,
+                             h->shardHi, h->pCount, h->pWeight, h->A.eradCensus, h->dStats);
+    h->launches += 3;
+    if (n) {
+        uint64_t *countU64 = skeys == h->keysAlt ? h->keys : h->keysAlt;   // the sort's spare key buffer
+        launch_mask_count_upto(h->stream, h->pCount, n, start + R, countU64);
+        launch_scan_u64(h->stream, countU64, n, h->pOff, h->pTiles, h->dTotalU64);
+        h->launches += 4;
+    }
+    // exchange 3: census particles per shard and census energy per cell
+    launch_shard_pack_census(h->stream, h->pOff, h->dTotalU64, start, n, N, S, h->shardLo, h->shardHi,
+                             h->A.eradCensus, h->xbuf);
+    ++h->launches;
+    CK(cudaGetLastError());
+    rc = exchange_sum(h, static_cast<uint64_t>(S) + N);
+    if (rc != STORM_OK) return rc;
+    CK(cudaMemcpyAsync(h->A.eradCensus, h->xbuf + S, N * sizeof(double), cudaMemcpyDeviceToDevice, h->stream));
+    std::vector<double> counts(S);
+    uint32_t nValid = 0;
+    uint64_t total = 0;
+    {
+        const Readback r[3] = {{counts.data(), h->xbuf, S * sizeof(double)}, {&nValid, start + R, sizeof(uint32_t)},
+                               {&total, h->dTotalU64, sizeof(uint64_t)}};
+        rc = read_many(h, r, 3, true);
+        if (rc != STORM_OK) return rc;
+    }
+    for (uint32_t q = 0; q < S; ++q) h->shardCensus[q] = static_cast<uint64_t>(counts[q]);
+    if (n == 0) nValid = 0;
+    size_t grown = 0;
+    if (total > h->cap) {
+        if (total > 0xF0000000ull) return STORM_ERR_CAPACITY;
+        grown = total + total / 4;
+        bank_free(h, h->bankA, h->cap);
+        bank_free(h, h->bankB, h->cap);
+        CK(bank_alloc(h, h->bankA, grown));
+        CK(bank_alloc(h, h->bankB, grown));
+    }
+    if (grown) {
+        launch_comb_emit(h->stream, h->C, h->bankC, idx, skeys, pidBits, 1, nValid, h->pCount, h->pWeight, h->pOff,
+                         h->bankA);
+        ++h->launches;
+    } else if (total) {
+        uint32_t *src = idx == h->valsAlt ? h->vals : h->valsAlt;   // the sort's spare value buffer
+        launch_comb_emit_out(h->stream, h->C, h->bankC, idx, skeys, pidBits, 1, nValid, static_cast<uint32_t>(total),
+                             h->pCount, h->pWeight, h->pOff, src, reinterpret_cast<uint32_t *>(h->pTiles), h->bankA);
+        h->launches += nValid ? 5 : 0;
+    }
+    CK(cudaGetLastError());
+    if (grown) {
+        CK(cudaStreamSynchronize(h->stream));
+        free_rest(h, h->cap);
+        CK(alloc_rest(h, grown));
+        h->cap = grown;
+    }
+    h->nCensus = total;
+    h->stats.census_out = total;
+    return STORM_OK;
+}
+
 int storm_cuda_phase_comb(StormHandle *h) {
     if (!h) return STORM_ERR_INVALID_ARG;
     refresh_ctx(h);
+    if (h->shards > 1) return comb_sharded(h);
     const uint32_t n = static_cast<uint32_t>(h->stats.census_out_pre_comb);
     const uint32_t N = h->N;
     CK(cudaMemsetAsync(h->A.eradCensus, 0, sizeof(double) * N, h->stream));
@@ -1622,6 +1857,34 @@ int storm_cuda_phase_stats(StormHandle *h, StormStepStats *s) {
     return STORM_OK;
 }
 
+int storm_cuda_set_sharding(StormHandle *h, uint32_t shards, uint32_t lo, uint32_t hi, StormExchangeFn exchange,
+                            void *user) {
+    // once per handle, before its first census
+    if (!h || shards == 0 || lo >= hi || hi > shards || h->nCensus != 0 || h->dep) return STORM_ERR_INVALID_ARG;
+    if (shards > 1 && (!h->desc.comb_enabled || h->desc.comb_kind != STORM_COMB_PLAIN)) return STORM_ERR_INVALID_ARG;
+    CK(cudaSetDevice(h->device));
+    h->shards = shards;
+    h->shardLo = lo;
+    h->shardHi = hi;
+    h->exchange = exchange;
+    h->exchangeUser = user;
+    h->shardCensus.assign(shards, 0);
+    h->C.shards = shards;
+    h->C.shardBounds = nullptr;
+    if (shards > 1) {
+        const size_t N = h->N, R = static_cast<size_t>(shards) * N;
+        const size_t xb = std::max({2 * N, 2 * R, static_cast<size_t>(shards) + N});
+        CK(dalloc(h, &h->dep, N));
+        CK(dalloc(h, &h->xbuf, xb));
+        CK(dalloc(h, &h->shardWc, N));
+        CK(dalloc(h, &h->shardRunW, R));
+        CK(dalloc(h, &h->shardStart, R + 2));
+        CK(dalloc(h, &h->shardBounds, 3 * (static_cast<size_t>(shards) + 1)));
+        h->C.shardBounds = h->shardBounds;
+    }
+    return STORM_OK;
+}
+
 int storm_cuda_step(StormHandle *h, double dt, StormStepStats *stats) {
     if (!h) return STORM_ERR_INVALID_ARG;
     CK(cudaSetDevice(h->device));
@@ -1677,6 +1940,7 @@ int storm_cuda_step(StormHandle *h, double dt, StormStepStats *stats) {
 // ---------------------------------------------------------------- state in/out
 int storm_cuda_set_census(StormHandle *h, const StormParticlesSoA *in) {
     if (!h || !in) return STORM_ERR_INVALID_ARG;
+    if (h->shards > 1 && in->count) return STORM_ERR_INVALID_ARG;   // a sharded census is the comb's own
     CK(cudaSetDevice(h->device));
     const uint64_t n = in->count;
     int rc = ensure_capacity(h, n, 0);
@@ -1917,6 +2181,7 @@ int storm_cuda_checkpoint_size(StormHandle *h, uint64_t *bytes) {
 }
 
 int storm_cuda_checkpoint_save(StormHandle *h, void *buffer, uint64_t bytes) {
+    if (h && h->shards > 1) return STORM_ERR_INVALID_ARG;   // a shard's census is not a problem's
     if (!h || !buffer) return STORM_ERR_INVALID_ARG;
     const uint64_t n = h->nCensus;
     if (bytes < checkpoint_bytes(h, n)) return STORM_ERR_INVALID_ARG;
@@ -1958,7 +2223,7 @@ int storm_cuda_checkpoint_save(StormHandle *h, void *buffer, uint64_t bytes) {
 }
 
 int storm_cuda_checkpoint_load(StormHandle *h, const void *buffer, uint64_t bytes) {
-    if (!h || !buffer || bytes < sizeof(CheckpointHeader)) return STORM_ERR_INVALID_ARG;
+    if (!h || !buffer || bytes < sizeof(CheckpointHeader) || h->shards > 1) return STORM_ERR_INVALID_ARG;
     CheckpointHeader hd;
     std::memcpy(&hd, buffer, sizeof(hd));
     if (std::memcmp(hd.magic, "STORMCK1", 8) != 0 || hd.abi != STORM_CUDA_ABI_VERSION ||

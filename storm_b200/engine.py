@@ -53,6 +53,7 @@ def lib():
         L.storm_cuda_set_cell_state.argtypes = [vp, dp, dp, dp]
         L.storm_cuda_set_cell_physics.argtypes = [vp, dp, dp, dp]
         L.storm_cuda_set_opacity_tables.argtypes = [vp, dp, dp]
+        L.storm_cuda_set_sharding.argtypes = [vp, C.c_uint32, C.c_uint32, C.c_uint32, A.ExchangeFn, vp]
         L.storm_cuda_get_beginning_counts.argtypes = [vp, u64p]
         L.storm_cuda_set_face_temperature.argtypes = [vp, C.c_int, C.c_double]
         L.storm_cuda_get_emission.argtypes = [vp, u64p, dp]
@@ -192,6 +193,28 @@ class Engine:
             lib().storm_cuda_last_error(hh, C.byref(derr), C.byref(cell), C.byref(part), msg, 512)
         raise StormError(rc, msg.value.decode() or lib().storm_cuda_status_string(rc).decode(), derr.value,
                          cell.value, part.value)
+
+    # ---------------------------------------------------------------- shards
+    def set_sharding(self, shards, lo, hi, exchange=None):
+        """Hold particle shards [lo, hi) of `shards` (storm_cuda_set_sharding).
+        `exchange(ptr, count, stream)` sums `count` float64 values at device
+        address `ptr` in place over every rank, ordered on the CUDA stream
+        `stream`; None when this handle holds every shard.  See
+        `torch_exchange` for the NCCL one."""
+        if exchange is None:
+            cb = A.ExchangeFn()
+        else:
+            def call(user, values, count, stream):
+                try:
+                    exchange(C.cast(values, C.c_void_p).value, int(count), stream or 0)
+                    return 0
+                except Exception:   # the engine fails the step with STORM_ERR_INVALID_ARG
+                    import traceback
+                    traceback.print_exc()
+                    return 1
+            cb = A.ExchangeFn(call)
+        self._exchange = cb   # the callback must outlive the handle's steps
+        self._check(lib().storm_cuda_set_sharding(self.h, shards, lo, hi, cb, None))
 
     # ---------------------------------------------------------------- step
     def step(self, dt=None):
@@ -364,6 +387,34 @@ class Engine:
 
     def set_segments_per_visit(self, k):
         self._check(lib().storm_cuda_set_segments_per_visit(self.h, k))
+
+
+def device_array(ptr, count, device=None):
+    """A torch float64 tensor over `count` doubles of device memory at `ptr`
+    (no copy), through the CUDA array interface."""
+    import torch
+
+    class _Buf:
+        pass
+    b = _Buf()
+    b.__cuda_array_interface__ = {"shape": (count,), "typestr": "<f8", "data": (ptr, False), "version": 3,
+                                  "strides": None, "stream": None}
+    return torch.as_tensor(b, device=device if device is not None else torch.device("cuda",
+                                                                                      torch.cuda.current_device()))
+
+
+def torch_exchange(group=None):
+    """The exchange of a sharded engine over torch.distributed: an in-place
+    sum all-reduce (NCCL across GPUs) of the engine's buffer, ordered on the
+    engine's stream."""
+    import torch
+    import torch.distributed as dist
+
+    def exchange(ptr, count, stream):
+        t = device_array(ptr, count)
+        with torch.cuda.stream(torch.cuda.ExternalStream(stream)):
+            dist.all_reduce(t, op=dist.ReduceOp.SUM, group=group)
+    return exchange
 
 
 class Server:
