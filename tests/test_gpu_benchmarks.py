@@ -125,20 +125,11 @@ def test_mg_face_driven_steps_vs_reference(ref_lib):
     """Fifteen steps of a small Densmore slab (30 groups, face source, PGRW) on
     independent seeds: the GPU and the reference's serial path agree within
     the seed-to-seed scatter, cell by cell."""
-    def run(make, seeds):
-        out = []
-        for s in seeds:
-            p = P.densmore2012(nx=24, new_photons_per_cell=6, boundary_per_face=200, seed=s)
-            p.comb_nmin = 20
-            m = make(p)
-            for _ in range(15):
-                m.step(p.dt)
-            out.append(m.cells()["temperature"])
-            m.close()
-        return np.array(out)
-    a = run(Engine, range(40, 48))
-    b = run(ref_lib.Reference, range(80, 88))
-    ma, mb = a.mean(0), b.mean(0)
-    se = np.sqrt(a.var(0, ddof=1) / len(a) + b.var(0, ddof=1) / len(b))
-    z = np.abs(ma - mb) / np.maximum(se, 1e-9 * ma)
-    assert (z < 4).mean() > 0.95, np.sort(z)[-10:]
+    from batchcheck import assert_agree, run_batch
+
+    def prob(s):
+        p = P.densmore2012(nx=24, new_photons_per_cell=6, boundary_per_face=200, seed=s)
+        p.comb_nmin = 20
+        return p
+    assert_agree(run_batch(Engine, prob, range(40, 52), 15), run_batch(ref_lib.Reference, prob, range(80, 92), 15),
+                 "Densmore slab 24 cells, 30 groups: engine vs reference")

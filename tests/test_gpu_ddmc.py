@@ -85,39 +85,22 @@ def test_ddmc_energy_conservation(precision):
         e.close()
 
 
-def _scatter_test(a, b):
-    ma, mb = a.mean(0), b.mean(0)
-    se = np.sqrt(a.var(0, ddof=1) / len(a) + b.var(0, ddof=1) / len(b))
-    z = np.abs(ma - mb) / np.maximum(se, 1e-9 * ma)
-    assert (z < 4).mean() > 0.95, np.sort(z)[-10:]
-
-
 def test_ddmc_steps_statistics_vs_reference(ref_lib):
     """Four steps of a DDMC cube on independent seeds: the GPU and the
-    reference's serial path agree cell by cell within the seed-to-seed scatter."""
-    def run(make, seeds):
-        out = []
-        for s in seeds:
-            p = problems.ddmc_cube(n=8, new_photons_per_cell=4, face_packets=80, comb_nmin=20, seed=s)
-            m = make(p)
-            for _ in range(4):
-                m.step()
-            out.append(m.cells()["temperature"])
-            m.close()
-        return np.array(out)
-    _scatter_test(run(Engine, range(20, 28)), run(ref_lib.Reference, range(60, 68)))
+    reference's serial path agree cell by cell under the batch gate."""
+    from batchcheck import assert_agree, run_batch
+
+    def prob(s):
+        return problems.ddmc_cube(n=8, new_photons_per_cell=4, face_packets=80, comb_nmin=20, seed=s)
+    assert_agree(run_batch(Engine, prob, range(20, 36), 4), run_batch(ref_lib.Reference, prob, range(60, 76), 4),
+                 "DDMC cube 8^3: engine vs reference")
 
 
 def test_ddmc_fp32_tracking_agrees_with_fp64():
-    def run(precision, seeds):
-        out = []
-        for s in seeds:
-            p = problems.ddmc_cube(n=10, new_photons_per_cell=4, face_packets=80, comb_nmin=20, seed=s,
-                                   precision=precision)
-            e = Engine(p)
-            for _ in range(4):
-                e.step()
-            out.append(e.cells()["temperature"])
-            e.close()
-        return np.array(out)
-    _scatter_test(run(A.PRECISION_FP32_TRACK, range(30, 38)), run(A.PRECISION_FP64, range(70, 78)))
+    from batchcheck import assert_agree, run_batch
+
+    def prob(precision):
+        return lambda s: problems.ddmc_cube(n=10, new_photons_per_cell=4, face_packets=80, comb_nmin=20, seed=s,
+                                            precision=precision)
+    assert_agree(run_batch(Engine, prob(A.PRECISION_FP32_TRACK), range(30, 46), 4),
+                 run_batch(Engine, prob(A.PRECISION_FP64), range(70, 86), 4), "DDMC cube 10^3: FP32 vs FP64")

@@ -86,23 +86,13 @@ def test_mg_energy_conservation():
 
 def test_mg_steps_statistics_vs_reference(ref_lib):
     """Four steps of a small multigroup cube on independent seeds: the GPU and
-    the reference's serial path agree within the seed-to-seed scatter."""
-    def run(make, seeds):
-        out = []
-        for s in seeds:
-            p = problems.mg_cube(n=6, groups=64, kappa0=1.0, new_photons_per_cell=6, comb_nmin=6, seed=s)
-            m = make(p)
-            for _ in range(4):
-                m.step()
-            out.append(m.cells()["temperature"])
-            m.close()
-        return np.array(out)
-    a = run(Engine, range(20, 28))
-    b = run(ref_lib.Reference, range(60, 68))
-    ma, mb = a.mean(0), b.mean(0)
-    se = np.sqrt(a.var(0, ddof=1) / len(a) + b.var(0, ddof=1) / len(b))
-    z = np.abs(ma - mb) / np.maximum(se, 1e-9 * ma)
-    assert (z < 4).mean() > 0.95, np.sort(z)[-10:]
+    the reference's serial path agree cell by cell under the batch gate."""
+    from batchcheck import assert_agree, run_batch
+
+    def prob(s):
+        return problems.mg_cube(n=6, groups=64, kappa0=1.0, new_photons_per_cell=6, comb_nmin=6, seed=s)
+    assert_agree(run_batch(Engine, prob, range(20, 36), 4), run_batch(ref_lib.Reference, prob, range(60, 76), 4),
+                 "multigroup cube 6^3 x 64: engine vs reference")
 
 
 def test_mg_fp32_tracking_conserves_and_agrees_with_fp64():
@@ -110,24 +100,17 @@ def test_mg_fp32_tracking_conserves_and_agrees_with_fp64():
     and temperatures within the seed-to-seed scatter of the FP64 form."""
     from storm_b200 import _abi as A
 
-    def run(precision, seeds):
-        out = []
-        for s in seeds:
-            p = problems.mg_cube(n=8, groups=64, kappa0=1.0, new_photons_per_cell=6, comb_nmin=6, seed=s,
-                                 precision=precision)
-            e = Engine(p)
-            for _ in range(4):
-                st = e.step()
-                assert _balance(st) < 1e-10
-            c = e.census()
-            assert (c.frequency >= p.group_bounds[0] * (1 - 1e-6)).all()
-            assert (c.frequency <= p.group_bounds[-1] * (1 + 1e-6)).all()
-            out.append(e.cells()["temperature"])
-            e.close()
-        return np.array(out)
-    a = run(A.PRECISION_FP32_TRACK, range(30, 38))
-    b = run(A.PRECISION_FP64, range(70, 78))
-    ma, mb = a.mean(0), b.mean(0)
-    se = np.sqrt(a.var(0, ddof=1) / len(a) + b.var(0, ddof=1) / len(b))
-    z = np.abs(ma - mb) / np.maximum(se, 1e-9 * ma)
-    assert (z < 4).mean() > 0.95, np.sort(z)[-10:]
+    from batchcheck import assert_agree, run_batch
+
+    def prob(precision):
+        return lambda s: problems.mg_cube(n=8, groups=64, kappa0=1.0, new_photons_per_cell=6, comb_nmin=6, seed=s,
+                                          precision=precision)
+
+    def check(e, st):
+        assert _balance(st) < 1e-10
+        c = e.census()
+        g = e.problem.group_bounds
+        assert (c.frequency >= g[0] * (1 - 1e-6)).all() and (c.frequency <= g[-1] * (1 + 1e-6)).all()
+    a = run_batch(Engine, prob(A.PRECISION_FP32_TRACK), range(30, 46), 4, check)
+    b = run_batch(Engine, prob(A.PRECISION_FP64), range(70, 86), 4, check)
+    assert_agree(a, b, "multigroup cube 8^3 x 64: FP32 vs FP64")

@@ -232,24 +232,14 @@ def test_comb_crowded_cells_match_oracle(oracle_lib, crowd):
 
 
 def test_step_cube_statistics_vs_oracle(oracle_lib):
-    """Several steps of the step-opacity cube on different seeds: GPU and
-    oracle temperatures agree within the seed-to-seed scatter."""
-    def run(make, seeds):
-        out = []
-        for s in seeds:
-            p = problems.step_cube(n=8, new_photons_per_cell=4, face_packets=80, comb_nmin=20, seed=s)
-            m = make(p)
-            for _ in range(4):
-                m.step()
-            out.append(m.cells()["temperature"])
-        return np.array(out)
-    a = run(Engine, range(10, 16))
-    b = run(oracle_lib.Oracle, range(50, 56))
-    ma, mb = a.mean(0), b.mean(0)
-    se = np.sqrt(a.var(0, ddof=1) / len(a) + b.var(0, ddof=1) / len(b))
-    hot = ma > 1.5 * a.min()
-    z = np.abs(ma - mb)[hot] / np.maximum(se[hot], 1e-9 * ma[hot])
-    assert (z < 4).mean() > 0.95
+    """Several steps of the step-opacity cube on independent seeds: GPU and
+    oracle agree cell by cell under the batch gate."""
+    from batchcheck import assert_agree, run_batch
+
+    def prob(s):
+        return problems.step_cube(n=8, new_photons_per_cell=4, face_packets=80, comb_nmin=20, seed=s)
+    assert_agree(run_batch(Engine, prob, range(10, 26), 4), run_batch(oracle_lib.Oracle, prob, range(50, 66), 4),
+                 "step cube 8^3: engine vs oracle")
 
 
 def test_errors_are_reported():

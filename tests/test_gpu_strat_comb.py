@@ -57,21 +57,13 @@ def _balance(st):
 
 
 def test_stratified_comb_steps_vs_reference(ref_lib):
-    def run(make, seeds):
-        out = []
-        for s in seeds:
-            p = problems.strat_cube(n=5, seed=s, comb_nmin=6)
-            m = make(p)
-            for _ in range(4):
-                st = m.step()
-                if isinstance(m, Engine):
-                    assert _balance(st) < 1e-10
-            out.append(m.cells()["temperature"])
-            m.close()
-        return np.array(out)
-    a = run(Engine, range(20, 28))
-    b = run(ref_lib.Reference, range(60, 68))
-    ma, mb = a.mean(0), b.mean(0)
-    se = np.sqrt(a.var(0, ddof=1) / len(a) + b.var(0, ddof=1) / len(b))
-    z = np.abs(ma - mb) / np.maximum(se, 1e-9 * ma)
-    assert (z < 4).mean() > 0.95, np.sort(z)[-10:]
+    from batchcheck import assert_agree, run_batch
+
+    def check(m, st):
+        if isinstance(m, Engine):
+            assert _balance(st) < 1e-10
+
+    def prob(s):
+        return problems.strat_cube(n=5, seed=s, comb_nmin=6)
+    assert_agree(run_batch(Engine, prob, range(20, 36), 4, check), run_batch(ref_lib.Reference, prob, range(60, 76), 4),
+                 "stratified comb cube 5^3: engine vs reference")

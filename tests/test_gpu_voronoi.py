@@ -97,25 +97,18 @@ def _balance(st):
 def test_voronoi_steps_conserve_and_agree_with_reference(ref_lib):
     mesh = build_voronoi(np.random.default_rng(8).random((400, 3)) * 0.98 + 0.01)
 
-    def run(make, seeds):
-        out = []
-        for s in seeds:
-            p = problems.voronoi_cube(ncells=400, packets_per_step=2e4, seed=8, mesh=mesh)
-            p.seed = s
-            m = make(p)
-            for _ in range(4):
-                st = m.step()
-                if isinstance(m, Engine):
-                    assert _balance(st) < 1e-10
-            out.append(m.cells()["temperature"])
-            m.close()
-        return np.array(out)
-    a = run(Engine, range(20, 28))
-    b = run(ref_lib.Reference, range(60, 68))
-    ma, mb = a.mean(0), b.mean(0)
-    se = np.sqrt(a.var(0, ddof=1) / len(a) + b.var(0, ddof=1) / len(b))
-    z = np.abs(ma - mb) / np.maximum(se, 1e-9 * ma)
-    assert (z < 4).mean() > 0.95, np.sort(z)[-10:]
+    from batchcheck import assert_agree, run_batch
+
+    def prob(s):
+        p = problems.voronoi_cube(ncells=400, packets_per_step=2e4, seed=8, mesh=mesh)
+        p.seed = s
+        return p
+
+    def check(m, st):
+        if isinstance(m, Engine):
+            assert _balance(st) < 1e-10
+    assert_agree(run_batch(Engine, prob, range(20, 36), 4, check),
+                 run_batch(ref_lib.Reference, prob, range(60, 76), 4), "Voronoi 400 cells: engine vs reference")
 
 
 def test_voronoi_fp32_tracking_agrees_with_fp64():
@@ -126,29 +119,29 @@ def test_voronoi_fp32_tracking_agrees_with_fp64():
     from storm_b200 import _abi as A
     mesh = build_voronoi(np.random.default_rng(9).random((400, 3)) * 0.98 + 0.01)
 
-    def run(precision, seeds):
-        out = []
-        for s in seeds:
+    from batchcheck import assert_agree, run_batch
+
+    def prob(precision):
+        def make(s):
             p = problems.voronoi_cube(ncells=400, packets_per_step=2e4, seed=9, mesh=mesh, precision=precision)
             p.seed = s
-            e = Engine(p)
-            for _ in range(4):
-                assert _balance(e.step()) < 1e-10
-            c = e.census()
-            pos = np.stack([c.x, c.y, c.z], 1)
-            cell = c.cell.astype(np.int64)
-            for q in np.random.default_rng(s).choice(len(cell), 300, replace=False):
-                k = cell[q]
-                for f in mesh.cell_faces[mesh.cell_face_offset[k]:mesh.cell_face_offset[k + 1]]:
-                    nrm, fc = mesh.face_normal[f], mesh.face_cm[f]
-                    side = np.sign(np.dot(mesh.points[k] - fc, nrm))
-                    assert side * np.dot(pos[q] - fc, nrm) >= -1e-7, (k, f)
-            out.append(e.cells()["temperature"])
-            e.close()
-        return np.array(out)
-    a = run(A.PRECISION_FP32_TRACK, range(30, 38))
-    b = run(A.PRECISION_FP64, range(70, 78))
-    ma, mb = a.mean(0), b.mean(0)
-    se = np.sqrt(a.var(0, ddof=1) / len(a) + b.var(0, ddof=1) / len(b))
-    z = np.abs(ma - mb) / np.maximum(se, 1e-9 * ma)
-    assert (z < 4).mean() > 0.95, np.sort(z)[-10:]
+            return p
+        return make
+    steps_seen = []
+
+    def check(e, st):
+        assert _balance(st) < 1e-10
+        steps_seen.append(1)
+        if len(steps_seen) % 4:
+            return
+        c = e.census()   # after each run's last step: a sample of the census lies inside its cells
+        pos = np.stack([c.x, c.y, c.z], 1)
+        cell = c.cell.astype(np.int64)
+        for q in np.random.default_rng(len(steps_seen)).choice(len(cell), 300, replace=False):
+            k = cell[q]
+            for f in mesh.cell_faces[mesh.cell_face_offset[k]:mesh.cell_face_offset[k + 1]]:
+                nrm, fc = mesh.face_normal[f], mesh.face_cm[f]
+                side = np.sign(np.dot(mesh.points[k] - fc, nrm))
+                assert side * np.dot(pos[q] - fc, nrm) >= -1e-7, (k, f)
+    assert_agree(run_batch(Engine, prob(A.PRECISION_FP32_TRACK), range(30, 46), 4, check),
+                 run_batch(Engine, prob(A.PRECISION_FP64), range(70, 86), 4, check), "Voronoi 400 cells: FP32 vs FP64")

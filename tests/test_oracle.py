@@ -225,21 +225,11 @@ def test_comb_invariants_reference_and_oracle(oracle_lib, ref_lib):
 
 def test_oracle_matches_reference_statistically(oracle_lib, ref_lib):
     """Full time steps: the oracle (Philox streams) and the reference (its own
-    mt19937_64 streams) agree on per-cell material temperature within 3 sigma of
-    the seed-to-seed scatter."""
-    def runs(kind, seeds, steps=4):
-        out = []
-        for s in seeds:
-            p = problems.gray_slab(new_photons_per_cell=5, face_packets=3000, comb_nmin=50, seed=s)
-            m = ref_lib.Reference(p) if kind == "ref" else oracle_lib.Oracle(p)
-            for _ in range(steps):
-                m.step()
-            out.append(m.cells()["temperature"][:20])
-        return np.array(out)
-    a = runs("ref", range(100, 108))
-    b = runs("orc", range(200, 208))
-    ma, mb = a.mean(0), b.mean(0)
-    se = np.sqrt(a.var(0, ddof=1) / len(a) + b.var(0, ddof=1) / len(b))
-    hot = ma > 0.01 * ma.max()
-    z = np.abs(ma - mb)[hot] / np.maximum(se[hot], 1e-12 * ma[hot])
-    assert (z < 4.0).mean() > 0.95, z
+    mt19937_64 streams) agree cell by cell under the batch gate (per-cell Welch
+    z of temperature, deposit and radiation energies, storm_b200.batchstats)."""
+    from batchcheck import assert_agree, run_batch
+
+    def prob(s):
+        return problems.gray_slab(new_photons_per_cell=5, face_packets=3000, comb_nmin=50, seed=s)
+    assert_agree(run_batch(ref_lib.Reference, prob, range(100, 116), 4),
+                 run_batch(oracle_lib.Oracle, prob, range(200, 216), 4), "slab: reference vs oracle")
