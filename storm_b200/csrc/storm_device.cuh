@@ -1218,7 +1218,9 @@ __device__ __forceinline__ float mg_absorption32(const Ctx &C, const Track32 &T,
 // The exit is the first smallest (n.q + h) / (-n.u) over faces the direction
 // approaches; a particle that changes cells re-expresses its offset from the
 // new mesh point and is nudged 2^-21 of it toward that point.
-template <bool MG, class RNG, class TALLY, bool POLY = false>
+// DDMC = false compiles the DDMC branch out (problems without withDDMC): a
+// smaller kernel for the instruction cache.
+template <bool MG, class RNG, class TALLY, bool POLY = false, bool DDMC = true>
 __device__ inline int segment32(const Ctx &C, Track32 &T, RNG &rng, TALLY &tal, int &usedRW, int &err) {
     const uint32_t cell = T.cell;
     if (T.cc != cell) {   // entered another cell: load its constants once
@@ -1252,7 +1254,7 @@ __device__ inline int segment32(const Ctx &C, Track32 &T, RNG &rng, TALLY &tal, 
         usedRW = 1;
         return rw_jump32<MG, POLY>(C, T, rng, tal, cp, Ro, hx, hy, hz, err);
     }
-    if (!POLY && C.withDDMC) {   // DDMC after a Random Walk that was not taken (:1723-1738)
+    if (!POLY && DDMC && C.withDDMC) {   // DDMC after a Random Walk that was not taken (:1723-1738)
         const float4 da = C.ddmc32[3 * static_cast<size_t>(cell)];   // depth reach, 1/total, sigma_A f c, nu bound
         if (Ro >= da.x && Ro > 0.0f && (!MG || T.nu < da.w)) return ddmc_jump32(C, T, rng, tal, da);
     }

@@ -1186,7 +1186,7 @@ struct Form64T {
 using Form64 = Form64T<0>;
 using Form64Full = Form64T<1>;
 using Form64Poly = Form64T<2>;
-template <bool POLY>
+template <bool POLY, bool DDMC = true>
 struct Form32T {
     using T = Track32;
     using Rng = PhiloxRng4;
@@ -1204,7 +1204,7 @@ struct Form32T {
     }
     template <class RNG, class TALLY>
     static __device__ __forceinline__ int seg(const Ctx &C, T &t, RNG &rng, TALLY &tal, int &usedRW, int &err) {
-        int m = segment32<false, RNG, TALLY, POLY>(C, t, rng, tal, usedRW, err);
+        int m = segment32<false, RNG, TALLY, POLY, DDMC>(C, t, rng, tal, usedRW, err);
         if (m == OUT_ERROR && !err) err = STORM_DERR_NOT_ON_BOUNDARY;
         return m;
     }
@@ -1212,9 +1212,11 @@ struct Form32T {
     static __device__ __forceinline__ double weight(const T &t) { return t.w; }
 };
 using Form32 = Form32T<false>;
+using Form32Lean = Form32T<false, false>;   // without the DDMC branch
 using Form32Poly = Form32T<true>;
 // The FP32-tracking form of a multigroup problem: the frequency rides along.
-struct Form32MG {
+template <bool DDMC = true>
+struct Form32MGT {
     using T = Track32;
     using Rng = PhiloxRng4;
     static __device__ __forceinline__ void load(const Ctx &C, const Bank &b, uint32_t q, T &t) {
@@ -1233,13 +1235,15 @@ struct Form32MG {
     }
     template <class RNG, class TALLY>
     static __device__ __forceinline__ int seg(const Ctx &C, T &t, RNG &rng, TALLY &tal, int &usedRW, int &err) {
-        int m = segment32<true>(C, t, rng, tal, usedRW, err);
+        int m = segment32<true, RNG, TALLY, false, DDMC>(C, t, rng, tal, usedRW, err);
         if (m == OUT_ERROR && !err) err = STORM_DERR_NOT_ON_BOUNDARY;
         return m;
     }
     static __device__ __forceinline__ uint32_t cell(const T &t) { return t.cell; }
     static __device__ __forceinline__ double weight(const T &t) { return t.w; }
 };
+using Form32MG = Form32MGT<true>;
+using Form32MGLean = Form32MGT<false>;   // without the DDMC branch
 
 // One bank visit of the HandleAll loop (manager/MonteCarloManagerSerial.hpp:267-383):
 // every active particle runs up to K segments in registers; survivors are
@@ -2961,8 +2965,10 @@ void launch_transport_refill(cudaStream_t s, uint32_t grid, int minBlocks, const
                              uint32_t *nextIdx, const CensusBank &cen, uint32_t *nCen, uint32_t burst, uint32_t maxSegs,
                              DevStats *st) {
     if (C.fp32 && C.poly) refill_launch<Form32Poly>(s, grid, minBlocks, C, in, n, nextIdx, cen, nCen, burst, maxSegs, st);
-    else if (C.fp32 && C.groups >= 2) refill_launch<Form32MG>(s, grid, minBlocks, C, in, n, nextIdx, cen, nCen, burst, maxSegs, st);
-    else if (C.fp32) refill_launch<Form32>(s, grid, minBlocks, C, in, n, nextIdx, cen, nCen, burst, maxSegs, st);
+    else if (C.fp32 && C.groups >= 2 && C.withDDMC) refill_launch<Form32MG>(s, grid, minBlocks, C, in, n, nextIdx, cen, nCen, burst, maxSegs, st);
+    else if (C.fp32 && C.groups >= 2) refill_launch<Form32MGLean>(s, grid, minBlocks, C, in, n, nextIdx, cen, nCen, burst, maxSegs, st);
+    else if (C.fp32 && C.withDDMC) refill_launch<Form32>(s, grid, minBlocks, C, in, n, nextIdx, cen, nCen, burst, maxSegs, st);
+    else if (C.fp32) refill_launch<Form32Lean>(s, grid, minBlocks, C, in, n, nextIdx, cen, nCen, burst, maxSegs, st);
     else if (C.poly) refill_launch<Form64Poly>(s, grid, minBlocks, C, in, n, nextIdx, cen, nCen, burst, maxSegs, st);
     else if (C.groups >= 2 || C.withDDMC) refill_launch<Form64Full>(s, grid, minBlocks, C, in, n, nextIdx, cen, nCen, burst, maxSegs, st);
     else refill_launch<Form64>(s, grid, minBlocks, C, in, n, nextIdx, cen, nCen, burst, maxSegs, st);

@@ -63,16 +63,9 @@ def test_marshak_wave_against_diffusion_reference(problem, form):
     l1 = B.marshak_l1(res["x"], res["t_gas"], curve)
     l1_ref = _against_reference_run(res, name, P.marshak_wave(problem).volumes())
     print(f"{name} {form}: TGAS_REL_L1 = {l1:.4e} over {res['steps']} steps (reference serial run {l1_ref:.4e})")
+    # one realization against the regression gate; the distribution of Marshak
+    # 1's L1 over seeds is compared with the reference's own in test_gpu_fullrun
     gate = 0.10 if l1_ref < 0.10 else 2.0 * l1_ref
-    if not l1 < gate:
-        # One realization's L1 scatters widely: Marshak 1 gave 0.019-0.054 over
-        # seeds 42-44 and 0.101 in one run of seed 42 (the FP64 tally sums are
-        # atomic, their order varies from run to run, and over 7,912 steps the
-        # histories part); the reference's own runs gave 0.026-0.059 over seeds
-        # 42-46.  An independent realization (the next seed) must then meet it.
-        res = B.run_marshak_wave(Engine, problem, precision=FORMS[form], seed=43)
-        l1 = B.marshak_l1(res["x"], res["t_gas"], curve)
-        print(f"{name} {form}: second realization TGAS_REL_L1 = {l1:.4e}")
     assert 0.0 <= l1 < gate
 
 
