@@ -49,11 +49,24 @@
 #include <memory>
 #include <set>
 #include <string>
+#include <type_traits>
+#include <utility>
 #include <vector>
 
 #include "../storm_cuda.h"
 
 namespace STORM {
+
+namespace cuda_detail {
+// cells that move (a `velocity`) and extensives that carry a `momentum` and
+// a total `energy`: RadiationIMC's moving-material terms need the first two
+template <class T, class = void> struct has_velocity : std::false_type {};
+template <class T> struct has_velocity<T, std::void_t<decltype(std::declval<T &>().velocity)>> : std::true_type {};
+template <class T, class = void> struct has_momentum : std::false_type {};
+template <class T> struct has_momentum<T, std::void_t<decltype(std::declval<T &>().momentum)>> : std::true_type {};
+template <class T, class = void> struct has_total_energy : std::false_type {};
+template <class T> struct has_total_energy<T, std::void_t<decltype(std::declval<T &>().energy)>> : std::true_type {};
+}  // namespace cuda_detail
 
 template <typename CellT, typename ExtensivesT>
 struct CudaIMCBinding {
@@ -81,6 +94,7 @@ struct CudaIMCBinding {
     // RadiationIMCParameters<NumGroups> (copy with bind_parameters)
     std::size_t newPhotonsPerCell = 1;
     bool withRandomWalk = false, noHydroFeedback = false;
+    bool withHydro = false;   // moving material: CellT::velocity and ExtensivesT::momentum (FP64 form)
     double rwMinCellOpticalDepth = 25.0, rwMinParticleOpticalDepth = 5.0;
     bool withDDMC = false, ddmcUseMultigroupPGRW = false;
     double ddmcMinCellOpticalDepth = 15.0, ddmcMinParticleOpticalDepth = 5.0;
@@ -114,7 +128,9 @@ struct CudaIMCBinding {
         ddmcUseMultigroupPGRW = p.ddmcUseMultigroupPGRW;
         ddmcMinCellOpticalDepth = p.ddmcMinCellOpticalDepth;
         ddmcMinParticleOpticalDepth = p.ddmcMinParticleOpticalDepth;
-        if (p.withHydro || p.MMC || p.withCompton || p.withEgTimeAvg || p.diffusionPressureGradient ||
+        constexpr bool moving = cuda_detail::has_velocity<CellT>::value && cuda_detail::has_momentum<ExtensivesT>::value;
+        withHydro = p.withHydro;
+        if ((p.withHydro && !moving) || p.MMC || p.withCompton || p.withEgTimeAvg || p.diffusionPressureGradient ||
             p.postProcess.enabled) {
             StormError eo("MonteCarloManagerCUDA: RadiationIMC option not supported on the device path");
             eo.addEntry("withHydro", p.withHydro);
@@ -424,6 +440,19 @@ private:
         d.new_photons_per_cell = binding_.newPhotonsPerCell;
         d.with_random_walk = binding_.withRandomWalk;
         d.no_hydro_feedback = binding_.noHydroFeedback;
+        std::vector<double> vel;
+        if constexpr (cuda_detail::has_velocity<CellT>::value && cuda_detail::has_momentum<ExtensivesT>::value) {
+            if (binding_.withHydro) {   // the cells' velocity (RadiationIMC reads cell.velocity)
+                vel.resize(3 * N);
+                for (std::size_t i = 0; i < N; ++i) {
+                    vel[3 * i] = cells[i].velocity.x;
+                    vel[3 * i + 1] = cells[i].velocity.y;
+                    vel[3 * i + 2] = cells[i].velocity.z;
+                }
+                d.with_hydro = 1;
+                d.cell_velocity = vel.data();
+            }
+        }
         d.rw_min_cell_optical_depth = binding_.rwMinCellOpticalDepth;
         d.rw_min_particle_optical_depth = binding_.rwMinParticleOpticalDepth;
         d.with_ddmc = binding_.withDDMC;
@@ -534,6 +563,20 @@ private:
         }
         cuda_detail::check(storm_cuda_set_cell_state(h_, hostT_.data(), hostE_.data(), hostCE_.data()), h_,
                            "set_cell_state");
+        if constexpr (cuda_detail::has_velocity<CellT>::value && cuda_detail::has_momentum<ExtensivesT>::value) {
+            if (binding_.withHydro) {   // the velocities and momenta a hydro step may have moved
+                hostV_.resize(3 * N_);
+                hostM_.resize(3 * N_);
+                for (std::size_t i = 0; i < N_; ++i) {
+                    hostV_[3 * i] = cells[i].velocity.x; hostV_[3 * i + 1] = cells[i].velocity.y;
+                    hostV_[3 * i + 2] = cells[i].velocity.z;
+                    hostM_[3 * i] = ext[i].momentum.x; hostM_[3 * i + 1] = ext[i].momentum.y;
+                    hostM_[3 * i + 2] = ext[i].momentum.z;
+                }
+                cuda_detail::check(storm_cuda_set_cell_motion(h_, hostV_.data(), hostM_.data()), h_,
+                                   "set_cell_motion");
+            }
+        }
         // the opacity plug-in at this step's cell state (RadiationIMC::preStep, :1645)
         if (binding_.opacityKind == STORM_OPACITY_CELL_TABLE || binding_.opacityKind == STORM_OPACITY_MG_POWER) {
             hostSA_.resize(N_);
@@ -613,6 +656,24 @@ private:
             ext[i].Erad = eradCensus[i];
             cells[i].Erad = ext[i].mass > 0.0 ? eradCensus[i] / ext[i].mass : 0.0;
         }
+        if constexpr (cuda_detail::has_velocity<CellT>::value && cuda_detail::has_momentum<ExtensivesT>::value) {
+            if (binding_.withHydro) {   // momentum deposits and velocity = momentum / mass (:853-866)
+                hostV_.resize(3 * N_);
+                hostM_.resize(3 * N_);
+                cuda_detail::check(storm_cuda_get_cell_motion(h_, hostV_.data(), hostM_.data()), h_, "get_cell_motion");
+                for (std::size_t i = 0; i < N_; ++i) {
+                    ext[i].momentum.x = hostM_[3 * i]; ext[i].momentum.y = hostM_[3 * i + 1];
+                    ext[i].momentum.z = hostM_[3 * i + 2];
+                    cells[i].velocity.x = hostV_[3 * i]; cells[i].velocity.y = hostV_[3 * i + 1];
+                    cells[i].velocity.z = hostV_[3 * i + 2];
+                    if constexpr (cuda_detail::has_total_energy<ExtensivesT>::value) {
+                        const double p2 = hostM_[3 * i] * hostM_[3 * i] + hostM_[3 * i + 1] * hostM_[3 * i + 1] +
+                                          hostM_[3 * i + 2] * hostM_[3 * i + 2];
+                        ext[i].energy = ext[i].internal_energy + 0.5 * p2 / ext[i].mass;
+                    }
+                }
+            }
+        }
     }
 
     const Grid &grid_;
@@ -626,7 +687,7 @@ private:
     bool multigroup_ = false;
     cuda_detail::PolyMeshArrays poly_;
     std::vector<std::size_t> cellsStepsCounters_;
-    std::vector<double> hostT_, hostE_, hostCE_, hostSA_, hostSS_, eradAvg_, sigmaA_, fleck_;
+    std::vector<double> hostT_, hostE_, hostCE_, hostSA_, hostSS_, hostV_, hostM_, eradAvg_, sigmaA_, fleck_;
     std::vector<std::size_t> beginningParticleCount_;
     Tracker tracker_;
     std::size_t startParticleCount_ = 0, initialParticleCount_ = 0, preStepParticleCount_ = 0, endParticleCount_ = 0;

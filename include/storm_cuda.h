@@ -36,7 +36,7 @@
 extern "C" {
 #endif
 
-#define STORM_CUDA_ABI_VERSION 6
+#define STORM_CUDA_ABI_VERSION 7
 
 /* ---------------------------------------------------------------- status */
 enum StormStatus {
@@ -229,6 +229,15 @@ typedef struct StormProblemDesc {
      * edges).  With a mesh, the per-cell arrays follow its cell order and the box
      * faces are the mesh's box; the FP64 form, no DDMC and no face sources. */
     const struct StormPolyMesh *mesh;
+
+    /* ---- moving material (RadiationIMCParameters::withHydro with cells that
+     * carry a velocity and extensives that carry a momentum): Doppler-shifted
+     * opacities, comoving scatters and emission transformed to the lab frame,
+     * momentum deposition (radiation/RadiationIMC.hpp:228-314, 1700-1881,
+     * 2035-2510, 830-866).  FP64 form on the Cartesian grid only. */
+    int32_t with_hydro;
+    int32_t pad2_;
+    const double *cell_velocity;     /* 3 per cell [cm/s]: the cells' velocity (NULL = at rest) */
 } StormProblemDesc;
 
 #define STORM_STRAT_MAX_BINS 64
@@ -302,6 +311,9 @@ typedef struct StormReplayBatch {
     /* multigroup: the particle's frequency before and after (NULL for gray) */
     const double *frequency;
     double *phys_frequency;
+    /* moving material: the momentum the segment left in its cell, 3 per item
+     * (extensives[cell].momentum; NULL = not returned) */
+    double *phys_momentum;
 } StormReplayBatch;
 
 typedef struct StormHandle StormHandle;
@@ -419,6 +431,14 @@ int storm_cuda_set_opacity_tables(StormHandle *h, const double *sigma_a, const d
  * for handles created with per_cell_segment_counters; others return
  * STORM_ERR_INVALID_ARG. */
 int storm_cuda_get_beginning_counts(StormHandle *h, uint64_t *counts);
+/* Moving material (with_hydro): the cells' velocity and the extensives'
+ * momentum, 3 per cell each ([cm/s], [g cm/s]); either pointer may be NULL.
+ * RadiationIMC reads cell.velocity and updates extensives[cell].momentum
+ * (radiation/RadiationIMC.hpp:1793-1798, 1853-1871, 2200-2206) and sets
+ * velocity = momentum / mass in synchronizeMaterialCell (:853-866).  Set
+ * before a step when a hydro solver moved the cells; read after it. */
+int storm_cuda_set_cell_motion(StormHandle *h, const double *velocity, const double *momentum);
+int storm_cuda_get_cell_motion(StormHandle *h, double *velocity, double *momentum);
 /* MarshakBoundary::SetTemperature / SideTemperature::SetTemperature. */
 int storm_cuda_set_face_temperature(StormHandle *h, int face, double temperature);
 

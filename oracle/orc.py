@@ -209,7 +209,7 @@ class ReplayBatch:
     OUT_D = ("phys_x", "phys_y", "phys_z", "phys_vx", "phys_vy", "phys_vz", "phys_time_left", "phys_weight",
              "dep_material", "dep_erad", "mgr_x", "mgr_y", "mgr_z", "mgr_vx", "mgr_vy", "mgr_vz")
 
-    def __init__(self, before, cell, tape_offset, tape_length, tape, frequency=None):
+    def __init__(self, before, cell, tape_offset, tape_length, tape, frequency=None, momentum=False):
         n = len(cell)
         self.n = n
         self.arrays = {}
@@ -218,6 +218,8 @@ class ReplayBatch:
         if frequency is not None:   # multigroup: frequency in and out
             self.arrays["frequency"] = np.ascontiguousarray(frequency, float)
             self.arrays["phys_frequency"] = np.zeros(n)
+        if momentum:   # moving material: each segment's momentum deposit, 3 per item
+            self.arrays["phys_momentum"] = np.zeros(3 * n)
         self.arrays["cell"] = np.ascontiguousarray(cell, np.uint32)
         self.arrays["tape_offset"] = np.ascontiguousarray(tape_offset, np.uint64)
         self.arrays["tape_length"] = np.ascontiguousarray(tape_length, np.uint32)

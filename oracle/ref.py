@@ -77,6 +77,8 @@ def lib():
         L.ref_point_on_face.argtypes = [vp, C.c_uint64, u64p, dp, dp]
         L.ref_comb.argtypes = [vp, C.POINTER(A.StormParticlesSoA), C.POINTER(A.StormParticlesSoA), u64p]
         L.ref_advance_face_stream.argtypes = [vp, C.c_uint64]
+        L.ref_record_get_momentum.argtypes = [vp, dp]
+        L.ref_get_motion.argtypes = [vp, dp, dp]
         L.ref_units.argtypes = [dp]
         L.ref_planck_integral.restype = C.c_double
         L.ref_planck_integral.argtypes = [C.c_double, C.c_double]
@@ -213,7 +215,16 @@ class Reference:
         r["freq_before"] = np.zeros(n)
         r["freq_after"] = np.zeros(n)
         L.ref_record_get_frequency(self.h, A.ptr(r["freq_before"]), A.ptr(r["freq_after"]))
+        r["momentum"] = np.zeros((n, 3))
+        L.ref_record_get_momentum(self.h, A.ptr(r["momentum"]))
         return r
+
+    def motion(self):
+        """Cell velocities and momenta, (ncells, 3) each."""
+        v = np.zeros((self.n, 3))
+        m = np.zeros((self.n, 3))
+        lib().ref_get_motion(self.h, A.ptr(v), A.ptr(m))
+        return v, m
 
     def thermal_energy(self, cells, xi):
         """The opacity plug-in's GetThermalEnergy at given uniforms (multigroup)."""

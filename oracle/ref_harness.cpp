@@ -55,8 +55,16 @@
 #include "storm_cuda.h"
 
 using Grid = MadCart::CartesianMesh3D<Vector3D>;
-using Cell = STORM::RadiationCell;
-using Ext = STORM::SimpleExtensives;
+// Cells with a velocity and extensives with a momentum: RadiationIMC's coupling
+// to moving material (withHydro) compiles in only for such types.  Without
+// withHydro its hydro branches stay inactive, and the results are those of the
+// plain RadiationCell / SimpleExtensives.
+struct Cell : STORM::RadiationCell {
+    Vector3D velocity;
+};
+struct Ext : STORM::SimpleExtensives {
+    Vector3D momentum;
+};
 using MCParticle = STORM::Particle<Vector3D, Grid>;
 
 namespace {
@@ -332,6 +340,7 @@ struct Record {
     uint32_t tapeLength;
     int32_t usedRW;
     double freqBefore, freqAfter;
+    double momBefore[3], momAfter[3];   // the cell's momentum (hydro)
 };
 
 struct RecordState {
@@ -367,6 +376,10 @@ public:
         r.freqBefore = p.frequency;
         r.eradBefore = this->getEradTimeAvg()[c];
         r.ematBefore = (*ext)[c].internal_energy;
+        {
+            const Vector3D &m = (*ext)[c].momentum;
+            r.momBefore[0] = m.x; r.momBefore[1] = m.y; r.momBefore[2] = m.z;
+        }
         std::mt19937_64 snap = *opac->captured;
         std::size_t rwBefore = this->getRandomWalkStepCount();
         std::size_t ddmcBefore = this->getDDMCStepCount();
@@ -389,6 +402,10 @@ public:
         r.nextCell = res.nextCellIndex;
         r.eradAfter = this->getEradTimeAvg()[c];
         r.ematAfter = (*ext)[c].internal_energy;
+        {
+            const Vector3D &m = (*ext)[c].momentum;
+            r.momAfter[0] = m.x; r.momAfter[1] = m.y; r.momAfter[2] = m.z;
+        }
         // 1: a Random Walk jump, 2: a DDMC step (tryDDMCStep took the segment)
         r.usedRW = (this->getRandomWalkStepCount() != rwBefore) ? 1 : (this->getDDMCStepCount() != ddmcBefore ? 2 : 0);
         rs.records.push_back(r);
@@ -494,6 +511,7 @@ void build_physics(RefHandle &h, const StormProblemDesc *d) {
     p.ddmcUseMultigroupPGRW = d->ddmc_use_multigroup_pgrw != 0;
     p.ddmcMinCellOpticalDepth = d->ddmc_min_cell_optical_depth;
     p.ddmcMinParticleOpticalDepth = d->ddmc_min_particle_optical_depth;
+    p.withHydro = d->with_hydro != 0;
     auto physics = std::make_shared<RecordingIMC<G>>(*h.grid, h.boundary, h.cells, h.ext, h.eos, opacity, p,
                                                      STORM::DirectRadiationIMCTraits<Vector3D, Cell, Ext, G>(),
                                                      RandomInCellPositionSampler<Vector3D, Grid>(), d->seed);
@@ -550,6 +568,10 @@ RefHandle *ref_create(const StormProblemDesc *d, int boundary_kind, char *err, s
             h->cells[i].internalEnergy = d->cell_internal_energy ? d->cell_internal_energy[i] : d->internal_energy[i];
             h->ext[i].mass = d->mass[i];
             h->ext[i].internal_energy = d->internal_energy[i];
+            if (d->cell_velocity) {
+                h->cells[i].velocity = Vector3D(d->cell_velocity[3 * i], d->cell_velocity[3 * i + 1], d->cell_velocity[3 * i + 2]);
+                h->ext[i].momentum = h->cells[i].velocity * h->ext[i].mass;
+            }
         }
         h->eos = std::make_shared<HarnessEOS>();
         h->eos->kind = d->eos_kind;
@@ -785,6 +807,14 @@ int ref_record_get_frequency(RefHandle *h, double *before, double *after) {
     return 0;
 }
 
+// Momentum the segment deposited into its cell (3 per record; hydro problems).
+int ref_record_get_momentum(RefHandle *h, double *dmom) {
+    const auto &R = h->view->records().records;
+    for (std::size_t k = 0; k < R.size(); ++k)
+        for (int d = 0; d < 3; ++d) dmom[3 * k + d] = R[k].momAfter[d] - R[k].momBefore[d];
+    return 0;
+}
+
 // Multigroup tables the reference computes per cell: the Planck mean opacity
 // of its opacity plug-in and the thermal energy it samples at given uniforms.
 int ref_mg_thermal_energy(RefHandle *h, uint64_t n, const uint32_t *cells, const double *xi, double *energy) {
@@ -869,6 +899,16 @@ int ref_point_on_face(RefHandle *h, uint64_t n, const uint64_t *faces, double *p
         tape[3 * k] = mdist(mirror);
         tape[3 * k + 1] = mdist(mirror);
         tape[3 * k + 2] = mdist(mirror);
+    }
+    return 0;
+}
+
+// The cells' velocity and the extensives' momentum (3 per cell each).
+int ref_get_motion(RefHandle *h, double *velocity, double *momentum) {
+    for (std::size_t i = 0; i < h->cells.size(); ++i) {
+        const Vector3D &v = h->cells[i].velocity, &m = h->ext[i].momentum;
+        if (velocity) { velocity[3 * i] = v.x; velocity[3 * i + 1] = v.y; velocity[3 * i + 2] = v.z; }
+        if (momentum) { momentum[3 * i] = m.x; momentum[3 * i + 1] = m.y; momentum[3 * i + 2] = m.z; }
     }
     return 0;
 }

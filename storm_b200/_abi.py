@@ -5,7 +5,7 @@ sizes against the compiled library.
 """
 import ctypes as C
 
-ABI_VERSION = 6
+ABI_VERSION = 7
 
 STORM_OK = 0
 STATUS_NAMES = {
@@ -88,6 +88,9 @@ class StormProblemDesc(C.Structure):
         ("comb_kind", C.c_int32), ("strat_bins", C.c_uint32), ("strat_bounds", _dp),
         ("strat_min_per_bin", C.c_uint64),
         ("mesh", C.POINTER(StormPolyMesh)),
+        ("with_hydro", C.c_int32),
+        ("pad2_", C.c_int32),
+        ("cell_velocity", C.POINTER(C.c_double)),
     ]
 
 
@@ -127,7 +130,7 @@ class StormReplayBatch(C.Structure):
         ("dep_material", _dp), ("dep_erad", _dp),
         ("mgr_x", _dp), ("mgr_y", _dp), ("mgr_z", _dp), ("mgr_vx", _dp), ("mgr_vy", _dp), ("mgr_vz", _dp),
         ("mgr_cell", _u32p), ("mgr_status", _i32p), ("draws_used", _u32p), ("used_random_walk", _i32p),
-        ("frequency", _dp), ("phys_frequency", _dp),
+        ("frequency", _dp), ("phys_frequency", _dp), ("phys_momentum", _dp),
     ]
 
 

@@ -66,6 +66,11 @@ struct Ctx {
     int32_t withRW;
     int32_t noFeedback;
     int32_t perCellCounters;
+    // moving material (withHydro): per cell (vx, vy, vz, gamma) and the cells' momentum (3 per cell)
+    int32_t withHydro;
+    double4 *vel;
+    double *mom;
+    double invC2;                  // units::inv_clight2
     // particle shards (storm_cuda_set_sharding): 1 = the whole problem on this handle
     uint32_t shards;
     const uint64_t *shardBounds;   // 3 (shards + 1) pid bounds: census, cell packets, face packets
@@ -345,8 +350,12 @@ __device__ __forceinline__ void isotropic(RNG &rng, double c, double &vx, double
 // (Erad_time_avg_[cell]).  LocalTally sums one segment's deposits (replay).
 struct LocalTally {
     double mat_, rad_;
+    double mx_, my_, mz_;   // momentum (moving material)
     __device__ __forceinline__ void mat(uint32_t, double v) { mat_ += v; }
     __device__ __forceinline__ void rad(uint32_t, double v) { rad_ += v; }
+    __device__ __forceinline__ void mom(const struct Ctx &, uint32_t, double x, double y, double z) {
+        mx_ += x; my_ += y; mz_ += z;
+    }
 };
 // The transport kernels' tally: every segment adds its deposits to the cell with
 // fire-and-forget atomics (RED) and counts itself for the per-cell segment
@@ -362,6 +371,7 @@ struct SegmentTally {
     __device__ __forceinline__ void enter(uint32_t c) { if (segs) atomicAdd(segs + c, 1u); }
     __device__ __forceinline__ void mat(uint32_t c, double v) { atomicAdd(eint + c, v); depSum += v; }
     __device__ __forceinline__ void rad(uint32_t c, double v) { atomicAdd(erad + c, v); }
+    __device__ __forceinline__ void mom(const struct Ctx &C, uint32_t c, double x, double y, double z);
 };
 
 // ------------------------------------------------------------------ multigroup
@@ -523,7 +533,59 @@ struct PolyGeom {
     }
 };
 
-template <bool MGP, class GEOM, class RNG, class TALLY>
+// ------------------------------------------------------------------ moving material
+__device__ __forceinline__ void SegmentTally::mom(const Ctx &C, uint32_t c, double x, double y, double z) {
+    double *m = C.mom + 3 * static_cast<size_t>(c);
+    atomicAdd(m, x);
+    atomicAdd(m + 1, y);
+    atomicAdd(m + 2, z);
+}
+
+// computeDopplerShift (radiation/RadiationIMC.hpp:228-245): the lab-to-comoving
+// factor gamma (1 - v.u / c^2) for a particle of lab velocity u in a cell
+// moving at v; 1 for a cell at rest.
+__device__ __forceinline__ double doppler_shift(const Ctx &C, const double4 &v, double ux, double uy, double uz) {
+    const double v2 = (v.x * v.x + v.y * v.y) + v.z * v.z;
+    if (v2 < 1e-30) return 1.0;
+    const double gamma = 1.0 / sqrt(1.0 - v2 * C.invC2);
+    return gamma * (1.0 - ((v.x * ux + v.y * uy) + v.z * uz) * C.invC2);
+}
+
+// lorentzTransformToLab (radiation/RadiationIMC.hpp:286-310): a comoving
+// particle to the lab frame -- frequency and weight by the Doppler factor of
+// the reversed cell velocity, the direction boosted and renormalised to c.
+__device__ __forceinline__ void lorentz_to_lab(const Ctx &C, const double4 &v, PartReg &p) {
+    const double v2 = (v.x * v.x + v.y * v.y) + v.z * v.z;
+    if (v2 < 1e-30) return;
+    const double gamma = 1.0 / sqrt(1.0 - C.invC2 * v2);
+    const double nx = v.x * (-1.0), ny = v.y * (-1.0), nz = v.z * (-1.0);
+    const double shift = gamma * (1.0 - ((nx * p.vx + ny * p.vy) + nz * p.vz) * C.invC2);
+    p.nu *= shift;
+    p.w *= shift;
+    const double vDotP = (p.vx * nx + p.vy * ny) + p.vz * nz;
+    const double k = (gamma - 1.0) * vDotP / v2 - gamma;
+    p.vx = p.vx + nx * k;
+    p.vy = p.vy + ny * k;
+    p.vz = p.vz + nz * k;
+    const double speed = vnorm(p.vx, p.vy, p.vz);
+    if (speed > 0.0) {
+        const double f = C.clight / speed;
+        p.vx = p.vx * f;
+        p.vy = p.vy * f;
+        p.vz = p.vz * f;
+    }
+}
+
+// extensives_[cell].momentum += (w0 u0 - w u) / c^2 (the momentum a scatter or
+// a Random Walk jump leaves in the cell)
+template <class TALLY>
+__device__ __forceinline__ void momentum_exchange(const Ctx &C, TALLY &tal, uint32_t cell, double w0, double ux0,
+                                                  double uy0, double uz0, const PartReg &p) {
+    tal.mom(C, cell, (w0 * ux0 - p.w * p.vx) * C.invC2, (w0 * uy0 - p.w * p.vy) * C.invC2,
+            (w0 * uz0 - p.w * p.vz) * C.invC2);
+}
+
+template <bool MGP, class GEOM, class RNG, class TALLY, bool HYDRO = false>
 __device__ inline int try_random_walk(const Ctx &C, PartReg &p, RNG &rng, TALLY &tal, const double4 &cp,
                                       const GEOM &g) {
     const uint32_t cell = p.cell;
@@ -549,8 +611,13 @@ __device__ inline int try_random_walk(const Ctx &C, PartReg &p, RNG &rng, TALLY 
         Dphys = cp.w;
     }
     bool doRW = (Ro > 0.0 && sigmaT > 0.0 && Dphys > 0.0 && Ro * sigmaT >= C.rwMinParticle);
-    if (doRW && pgrw && mg_clamp(C, p.nu) >= C.gb[cutoff]) doRW = false;   // (:1098-1115)
+    if (doRW && pgrw) {   // (:1098-1115): the comoving frequency against the cutoff
+        double coFreq = p.nu;
+        if (HYDRO && C.withHydro) coFreq *= doppler_shift(C, C.vel[cell], p.vx, p.vy, p.vz);
+        if (mg_clamp(C, coFreq) >= C.gb[cutoff]) doRW = false;
+    }
     if (!doRW) return -1;
+    const double oldVx = p.vx, oldVy = p.vy, oldVz = p.vz, oldWeight = p.w;   // (:1121-1122)
     const double fl = pgrw ? C.fleck[cell] : 0.0;
     double tauLeak = rw_sample_leak(C.rw, rng.open());
     double tLeak = tauLeak * Ro * Ro / Dphys;
@@ -620,6 +687,11 @@ __device__ inline int try_random_walk(const Ctx &C, PartReg &p, RNG &rng, TALLY 
             p.nu = nextafter(C.gb[cutoff], DBL_MAX);
         }
         p.nu = mg_clamp(C, p.nu);
+    }
+    if (HYDRO && C.withHydro) {   // the comoving jump's end back to the lab frame (:1252-1268)
+        lorentz_to_lab(C, C.vel[cell], p);
+        if (pgrw) p.nu = mg_clamp(C, p.nu);
+        if (!C.noFeedback) momentum_exchange(C, tal, cell, oldWeight, oldVx, oldVy, oldVz, p);
     }
     return (ev == 1) ? DONE : NO_CELL_MOVE;
 }
@@ -798,7 +870,8 @@ __device__ __forceinline__ void track_begin(const Ctx &C, Track &T) {
 // written (alpha = ((faceCM - x).n) / (n.v), the first smallest positive).
 template <int V, class RNG, class TALLY>
 __device__ inline PhysOut physics_step(const Ctx &C, Track &T, RNG &rng, TALLY &tal) {
-    constexpr bool FULL = V >= 1, POLY = V == 2;
+    // V: 0 gray Cartesian, 1 + multigroup and DDMC, 2 polyhedral, 3 = 1 + moving material
+    constexpr bool FULL = V == 1 || V == 3, POLY = V == 2, HYDRO = V == 3;
     PartReg &p = T.p;
     PhysOut o;
     o.status = NO_CELL_MOVE;
@@ -863,10 +936,17 @@ __device__ inline PhysOut physics_step(const Ctx &C, Track &T, RNG &rng, TALLY &
     }
     double4 cp = C.phys[cell];
     double elastic = 0.0, eventOpacity = 0.0;
+    // moving material: the lab-to-comoving Doppler factor (:1713-1720)
+    double dop = 1.0;
+    double4 cvel = make_double4(0.0, 0.0, 0.0, 1.0);
+    if (HYDRO && C.withHydro) {
+        cvel = C.vel[cell];
+        dop = doppler_shift(C, cvel, p.vx, p.vy, p.vz);
+    }
     if (FULL && C.groups >= 2) {
-        // CalcAbsorptionOpacity at the particle's frequency (:1742-1754)
+        // CalcAbsorptionOpacity at the particle's (comoving) frequency (:1742-1754)
         const double f = C.fleck[cell];
-        const double absorptionOpacity = mg_absorption(C, cell, mg_clamp(C, p.nu));
+        const double absorptionOpacity = mg_absorption(C, cell, mg_clamp(C, HYDRO ? p.nu * dop : p.nu));
         elastic = C.sigS[cell];
         const double effectiveAbsorptionOpacity = (1.0 - f) * absorptionOpacity;
         eventOpacity = elastic + effectiveAbsorptionOpacity;
@@ -882,7 +962,7 @@ __device__ inline PhysOut physics_step(const Ctx &C, Track &T, RNG &rng, TALLY &
             r = try_random_walk<FULL>(C, p, rng, tal, cp, g);
         } else {
             const CartGeom g{xl, xh, yl, yh, zl, zh, C.xc[i], C.yc[j], C.zc[k]};
-            r = try_random_walk<FULL>(C, p, rng, tal, cp, g);
+            r = try_random_walk<FULL, CartGeom, RNG, TALLY, HYDRO>(C, p, rng, tal, cp, g);
         }
         if (r == -2) { o.errCode = STORM_DERR_RW_SHRINK; return o; }
         if (r >= 0) {
@@ -910,7 +990,7 @@ __device__ inline PhysOut physics_step(const Ctx &C, Track &T, RNG &rng, TALLY &
 
     const double c = C.clight;
     const double lp = -log1p(rng.open() - 1.0);
-    const double scatteringDistance = cp.x * lp;
+    const double scatteringDistance = HYDRO ? cp.x * lp / dop : cp.x * lp;
     const double timeScattering = isfinite(scatteringDistance) ? scatteringDistance / T.speed : CUDART_INF;
     // std::min_element over {face, scatter, census}: first smallest wins
     int best = 0;
@@ -920,13 +1000,20 @@ __device__ inline PhysOut physics_step(const Ctx &C, Track &T, RNG &rng, TALLY &
     p.t -= dt;
     const double tmp2 = cp.y;
     const double tmp = -dt * tmp2;
-    const double e1 = expm1(tmp);
+    // moving material: the weight and the momentum attenuate at the comoving
+    // rate (expFactor1), the material and the tallies at the lab rate (expFactor2)
+    const double e2 = expm1(tmp);
+    const double e1 = HYDRO ? expm1(tmp * dop) : e2;
     double integrated = p.w * dt;
-    if (fabs(tmp2 * dt) >= 1e-12) integrated = p.w * e1 * cp.z;
+    if (fabs(tmp2 * dt) >= 1e-12) integrated = p.w * e2 * cp.z;
     p.x += p.vx * dt;
     p.y += p.vy * dt;
     p.z += p.vz * dt;
-    if (!C.noFeedback) tal.mat(cell, -e1 * p.w);
+    if (!C.noFeedback) tal.mat(cell, -e2 * p.w);
+    if (HYDRO && C.withHydro && !C.noFeedback) {   // (:1793-1798)
+        const double a = -e1 * p.w;
+        tal.mom(C, cell, a * p.vx * C.invC2, a * p.vy * C.invC2, a * p.vz * C.invC2);
+    }
     tal.rad(cell, integrated);
     p.w *= 1.0 + e1;
     if (fabs(p.w) < p.w0 * 1e-3) {
@@ -940,13 +1027,14 @@ __device__ inline PhysOut physics_step(const Ctx &C, Track &T, RNG &rng, TALLY &
         o.next = next;
         if (!POLY && next == OUTSIDE) o.ghost = C.ncells + face_index(C, i, j, k, face);
     } else if (best == 1) {
+        const double oldVx = p.vx, oldVy = p.vy, oldVz = p.vz;
         if (FULL && C.groups >= 2) {
             // elastic or effective scatter (:1826-1852): both re-scatter
             // isotropically; an effective scatter re-emits from the spectrum
             const double eventRandom = rng.open() * eventOpacity;
             const bool effective = !(eventRandom < elastic);
             isotropic(rng, c, p.vx, p.vy, p.vz);
-            p.nu = mg_clamp(C, p.nu);
+            p.nu = mg_clamp(C, HYDRO ? p.nu * dop : p.nu);
             if (effective) {
                 p.nu = mg_thermal_energy(C, cell, rng.open());
                 if (p.nu < 0.0) { o.errCode = STORM_DERR_MG_SAMPLE; return o; }
@@ -954,6 +1042,13 @@ __device__ inline PhysOut physics_step(const Ctx &C, Track &T, RNG &rng, TALLY &
         } else {
             rng.skip();   // event-type draw; both branches re-scatter isotropically
             isotropic(rng, c, p.vx, p.vy, p.vz);
+        }
+        if (HYDRO && C.withHydro) {   // the comoving scatter back to the lab frame (:1853-1871)
+            const double weightBefore = p.w;
+            p.w *= dop;
+            lorentz_to_lab(C, cvel, p);
+            if (C.groups >= 2) p.nu = mg_clamp(C, p.nu);
+            if (!C.noFeedback) momentum_exchange(C, tal, cell, weightBefore, oldVx, oldVy, oldVz, p);
         }
         T.speed = vnorm(p.vx, p.vy, p.vz);
         o.status = NO_CELL_MOVE;

@@ -87,6 +87,7 @@ struct ReplayDev {
     int32_t *mgrStatus;
     uint32_t *draws;
     int32_t *usedRW;
+    double *momOut;         // moving material: 3 per record (NULL = not returned)
 };
 
 void launch_begin(cudaStream_t s, const Bank &b, uint32_t n, uint32_t pidOffset, double dt, DevStats *st);

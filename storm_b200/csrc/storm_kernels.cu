@@ -466,7 +466,14 @@ __global__ void k_prestep(Ctx C, CellArrays A, OpacityEos M, double dt) {
             cv = M.eosF * M.eosBeta * pow(Tm, M.eosBeta - 1.0) * pow(rho, 1.0 - M.eosMu) / rho;
         }
         double T3 = (T * T) * T;   // boost::math::pow<3>
-        double f = 1.0 / (1.0 + (4.0 * C.arad * T3 * sa * C.clight * dt * 1.0) / cv);
+        double gamma = 1.0;        // moving material: the cell's Lorentz factor (:1636-1644)
+        if (C.withHydro) {
+            double4 v = C.vel[c];
+            gamma = 1.0 / sqrt(1.0 - ((v.x * v.x + v.y * v.y) + v.z * v.z) * C.invC2);
+            v.w = gamma;
+            C.vel[c] = v;
+        }
+        double f = 1.0 / (1.0 + (4.0 * C.arad * T3 * sa * C.clight * dt * gamma) / cv);
         A.fleck[c] = f;
         if (f < 0.0 || f > 1.0) raise_error(C, STORM_DERR_FLECK, c, 0);
         A.phys[c] = cell_phys(sa, ss, f, sa + ss, C.clight);
@@ -645,6 +652,13 @@ __global__ void k_emission_debit(Ctx C, CellArrays A, DevStats *st) {
         if (A.photons[c] == 0) continue;
         double E = A.emitE[c];
         if (!C.noFeedback) A.eint[c] -= E;
+        if (C.withHydro && !C.noFeedback) {   // momentum carried off by the emission (:2200-2206)
+            const double4 v = C.vel[c];
+            double *m = C.mom + 3 * static_cast<size_t>(c);
+            m[0] -= E * v.x * C.invC2 * v.w;
+            m[1] -= E * v.y * C.invC2 * v.w;
+            m[2] -= E * v.z * C.invC2 * v.w;
+        }
         deb += E;
     }
     deb = warp_sum(deb);
@@ -919,11 +933,15 @@ __global__ void k_emit_cells(Ctx C, CellArrays A, const uint64_t *offsets, uint6
         isotropic(rng, C.clight, p.vx, p.vy, p.vz);
         p.t = dt * rng.open();
         p.nu = 0.0;
+        // moving material: the packet is emitted isotropically in the comoving
+        // frame; its lab weight and frequency carry the Doppler factor (:2483-2493)
+        const double D = C.withHydro ? doppler_shift(C, C.vel[c], p.vx, p.vy, p.vz) : 1.0;
         if (C.groups >= 2) {   // GetThermalEnergy (radiation/RadiationIMC.hpp:2495-2500)
             p.nu = mg_thermal_energy(C, c, rng.open());
             if (p.nu < 0.0) raise_error(C, STORM_DERR_MG_SAMPLE, c, static_cast<uint32_t>(e));
+            if (C.withHydro) p.nu = p.nu / D;
         }
-        p.w = energyPerPhoton;
+        p.w = C.withHydro ? A.emitE[c] / (static_cast<double>(np) * D) : energyPerPhoton;
         p.w0 = fabs(p.w);
         store_any(C, b, bankBase + static_cast<uint32_t>(j), p, pidBase + static_cast<uint32_t>(e), 0);
         esum += p.w;
@@ -1186,6 +1204,7 @@ struct Form64T {
 using Form64 = Form64T<0>;
 using Form64Full = Form64T<1>;
 using Form64Poly = Form64T<2>;
+using Form64Hydro = Form64T<3>;   // Form64Full with moving material
 template <bool POLY, bool DDMC = true>
 struct Form32T {
     using T = Track32;
@@ -2611,6 +2630,15 @@ __global__ void k_poststep(Ctx C, CellArrays A, OpacityEos M, double dt) {
             T = pow(ratio > 0.0 ? ratio : 0.0, 1.0 / M.eosBeta);
         }
         A.T[c] = T;
+        if (C.withHydro) {   // cell.velocity = momentum / mass (:853-858)
+            const double *m = C.mom + 3 * static_cast<size_t>(c);
+            const double mass = A.mass[c];
+            double4 v = C.vel[c];
+            v.x = m[0] / mass;
+            v.y = m[1] / mass;
+            v.z = m[2] / mass;
+            C.vel[c] = v;
+        }
     }
 }
 
@@ -2626,8 +2654,9 @@ __global__ void k_replay(Ctx C, ReplayDev R, uint32_t n) {
         p.nu = R.freq ? R.freq[q] : 0.0;
         track_begin(C, T);
         TapeRng rng{R.tape + R.tapeOffset[q], R.tapeLength[q], 0, false};
-        LocalTally tal{0.0, 0.0};
-        PhysOut o = C.poly ? physics_step<2>(C, T, rng, tal) : physics_step<1>(C, T, rng, tal);
+        LocalTally tal{0.0, 0.0, 0.0, 0.0, 0.0};
+        PhysOut o = C.poly ? physics_step<2>(C, T, rng, tal)
+                           : (C.withHydro ? physics_step<3>(C, T, rng, tal) : physics_step<1>(C, T, rng, tal));
         R.phys[0][q] = p.x; R.phys[1][q] = p.y; R.phys[2][q] = p.z;
         R.phys[3][q] = p.vx; R.phys[4][q] = p.vy; R.phys[5][q] = p.vz;
         R.phys[6][q] = p.t; R.phys[7][q] = p.w;
@@ -2638,6 +2667,11 @@ __global__ void k_replay(Ctx C, ReplayDev R, uint32_t n) {
         R.dep[1][q] = tal.rad_;
         R.usedRW[q] = o.usedRW;
         R.draws[q] = rng.pos;
+        if (R.momOut) {
+            R.momOut[3 * static_cast<size_t>(q)] = tal.mx_;
+            R.momOut[3 * static_cast<size_t>(q) + 1] = tal.my_;
+            R.momOut[3 * static_cast<size_t>(q) + 2] = tal.mz_;
+        }
         int m = o.errCode ? OUT_ERROR : (C.poly ? manager_handle<true>(C, T, o) : manager_handle<false>(C, T, o));
         R.mgr[0][q] = p.x; R.mgr[1][q] = p.y; R.mgr[2][q] = p.z;
         R.mgr[3][q] = p.vx; R.mgr[4][q] = p.vy; R.mgr[5][q] = p.vz;
@@ -2970,6 +3004,7 @@ void launch_transport_refill(cudaStream_t s, uint32_t grid, int minBlocks, const
     else if (C.fp32 && C.withDDMC) refill_launch<Form32>(s, grid, minBlocks, C, in, n, nextIdx, cen, nCen, burst, maxSegs, st);
     else if (C.fp32) refill_launch<Form32Lean>(s, grid, minBlocks, C, in, n, nextIdx, cen, nCen, burst, maxSegs, st);
     else if (C.poly) refill_launch<Form64Poly>(s, grid, minBlocks, C, in, n, nextIdx, cen, nCen, burst, maxSegs, st);
+    else if (C.withHydro) refill_launch<Form64Hydro>(s, grid, minBlocks, C, in, n, nextIdx, cen, nCen, burst, maxSegs, st);
     else if (C.groups >= 2 || C.withDDMC) refill_launch<Form64Full>(s, grid, minBlocks, C, in, n, nextIdx, cen, nCen, burst, maxSegs, st);
     else refill_launch<Form64>(s, grid, minBlocks, C, in, n, nextIdx, cen, nCen, burst, maxSegs, st);
 }

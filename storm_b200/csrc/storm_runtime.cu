@@ -114,6 +114,8 @@ struct StormHandle {
     std::vector<uint64_t> shardCensus;   // census particles per shard after the last comb (every shard)
     uint64_t nCenGlobal = 0, nCellEmitGlobal = 0, nFaceEmitGlobal = 0;   // this step's global counts
     double *dep = nullptr;           // this handle's material deposits of the step (N)
+    double4 *vel = nullptr;          // moving material: (vx, vy, vz, gamma) per cell
+    double *mom = nullptr;           // moving material: momentum, 3 per cell
     double *xbuf = nullptr;          // exchange buffer (max(2 N, 2 S N, S + N) doubles)
     double *shardWc = nullptr;       // cells' global census weights (N)
     double *shardRunW = nullptr;     // run weights (S N)
@@ -810,6 +812,14 @@ int storm_cuda_create(const StormProblemDesc *d, StormHandle **out) {
         return STORM_ERR_INVALID_ARG;
     if (d->eos_kind != STORM_EOS_LINEAR && d->eos_kind != STORM_EOS_POWER_LAW) return STORM_ERR_UNSUPPORTED;
     if (d->precision != STORM_PRECISION_FP64 && d->precision != STORM_PRECISION_FP32_TRACK) return STORM_ERR_UNSUPPORTED;
+    // moving material: the FP64 form on the Cartesian grid, without DDMC
+    if (d->with_hydro && (d->precision != STORM_PRECISION_FP64 || d->mesh || d->with_ddmc)) return STORM_ERR_UNSUPPORTED;
+    if (d->cell_velocity) {
+        const uint64_t nv = d->mesh ? d->mesh->ncells : static_cast<uint64_t>(d->nx) * d->ny * d->nz;
+        for (uint64_t q = 0; q < 3 * nv; ++q)
+            if (!std::isfinite(d->cell_velocity[q]) || !(std::fabs(d->cell_velocity[q]) < d->clight))
+                return STORM_ERR_INVALID_ARG;
+    }
     const StormPolyMesh *mesh = d->mesh;
     const bool poly = mesh != nullptr;
     uint64_t N64 = poly ? mesh->ncells : static_cast<uint64_t>(d->nx) * d->ny * d->nz;
@@ -1126,6 +1136,28 @@ int storm_cuda_create(const StormProblemDesc *d, StormHandle **out) {
     C.perCellCounters = d->per_cell_segment_counters;
     C.shards = 1;
     C.shardBounds = nullptr;
+    // moving material: (vx, vy, vz, gamma) per cell, and the momentum mass * velocity
+    C.withHydro = d->with_hydro ? 1 : 0;
+    C.invC2 = 1.0 / (d->clight * d->clight);   // units::inv_clight2 = 1 / clight2
+    if (d->with_hydro) {
+        ALLOC(h->vel, N);
+        ALLOC(h->mom, 3 * static_cast<size_t>(N));
+        std::vector<double4> v(N);
+        std::vector<double> m(3 * static_cast<size_t>(N));
+        for (uint32_t c = 0; c < N; ++c) {
+            const double vx = d->cell_velocity ? d->cell_velocity[3 * c] : 0.0;
+            const double vy = d->cell_velocity ? d->cell_velocity[3 * c + 1] : 0.0;
+            const double vz = d->cell_velocity ? d->cell_velocity[3 * c + 2] : 0.0;
+            v[c] = make_double4(vx, vy, vz, 1.0);
+            m[3 * c] = vx * d->mass[c];
+            m[3 * c + 1] = vy * d->mass[c];
+            m[3 * c + 2] = vz * d->mass[c];
+        }
+        H2D(h->vel, v.data(), N);
+        H2D(h->mom, m.data(), 3 * static_cast<size_t>(N));
+    }
+    C.vel = h->vel;
+    C.mom = h->mom;
     C.clight = d->clight; C.arad = d->arad; C.sigmaSB = d->sigma_sb; C.kevKelvin = d->kev_kelvin;
     C.rwMinParticle = d->rw_min_particle_optical_depth;
     C.rwMinCell = d->rw_min_cell_optical_depth;
@@ -1188,7 +1220,8 @@ int storm_cuda_destroy(StormHandle *h) {
                   h->ddmcRate, h->ddmcCut, h->ddmc32, h->stratBounds, h->stratBinW, h->stratStart,
                   h->runCursor, h->runScan, h->longRuns, h->bucketFlags,
                   h->cfo, h->cfN, h->cfP, h->cfNext, h->cfFace, h->mpx, h->mpy, h->mpz, h->fvo, h->fvi, h->vtx,
-                  h->chord, h->cfN32, h->dep, h->xbuf, h->shardWc, h->shardRunW, h->shardStart, h->shardBounds};
+                  h->chord, h->cfN32, h->dep, h->xbuf, h->shardWc, h->shardRunW, h->shardStart, h->shardBounds,
+                  h->vel, h->mom};
     for (void *p : ps) device_pool().free(p);
     cudaEvent_t evs[] = {h->evStart, h->evTransport0, h->evTransport1, h->evEnd, h->evAfterEmit, h->evAfterComb};
     bool complete = h->stream != nullptr;
@@ -1388,7 +1421,7 @@ int storm_cuda_phase_transport(StormHandle *h) {
     uint32_t n32 = static_cast<uint32_t>(n0);
     uint32_t *nCen = h->counts + h->maxRounds + 1;
     // the multigroup FP32 form runs only in the refill kernel
-    const bool refill = h->refill || (h->fp32 && h->desc.groups >= 2) || h->C.poly;
+    const bool refill = h->refill || (h->fp32 && h->desc.groups >= 2) || h->C.poly || h->C.withHydro;
     if (!refill) CK(cudaMemcpyAsync(h->counts, &n32, sizeof(uint32_t), cudaMemcpyHostToDevice, h->stream));
     if (refill) {
         // one launch carries every history to census, escape or cutoff
@@ -1862,6 +1895,7 @@ int storm_cuda_set_sharding(StormHandle *h, uint32_t shards, uint32_t lo, uint32
     // once per handle, before its first census
     if (!h || shards == 0 || lo >= hi || hi > shards || h->nCensus != 0 || h->dep) return STORM_ERR_INVALID_ARG;
     if (shards > 1 && (!h->desc.comb_enabled || h->desc.comb_kind != STORM_COMB_PLAIN)) return STORM_ERR_INVALID_ARG;
+    if (shards > 1 && h->C.withHydro) return STORM_ERR_UNSUPPORTED;   // the momentum tallies have no exchange
     CK(cudaSetDevice(h->device));
     h->shards = shards;
     h->shardLo = lo;
@@ -2119,6 +2153,49 @@ int storm_cuda_set_cell_state(StormHandle *h, const double *T, const double *ein
     return STORM_OK;
 }
 
+int storm_cuda_set_cell_motion(StormHandle *h, const double *velocity, const double *momentum) {
+    if (!h || !h->vel) return STORM_ERR_INVALID_ARG;   // handles created with_hydro only
+    CK(cudaSetDevice(h->device));
+    const size_t N = h->N;
+    if (velocity) {
+        std::vector<double4> v(N);
+        CK(cudaMemcpyAsync(v.data(), h->vel, N * sizeof(double4), cudaMemcpyDeviceToHost, h->stream));
+        CK(cudaStreamSynchronize(h->stream));
+        for (size_t c = 0; c < N; ++c) {
+            for (int q = 0; q < 3; ++q)
+                if (!std::isfinite(velocity[3 * c + q]) || !(std::fabs(velocity[3 * c + q]) < h->C.clight))
+                    return STORM_ERR_INVALID_ARG;
+            v[c].x = velocity[3 * c]; v[c].y = velocity[3 * c + 1]; v[c].z = velocity[3 * c + 2];
+        }
+        CK(cudaMemcpyAsync(h->vel, v.data(), N * sizeof(double4), cudaMemcpyHostToDevice, h->stream));
+        CK(cudaStreamSynchronize(h->stream));
+    }
+    if (momentum) {
+        CK(cudaMemcpyAsync(h->mom, momentum, 3 * N * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+        CK(cudaStreamSynchronize(h->stream));
+    }
+    return STORM_OK;
+}
+
+int storm_cuda_get_cell_motion(StormHandle *h, double *velocity, double *momentum) {
+    if (!h || !h->vel) return STORM_ERR_INVALID_ARG;
+    CK(cudaSetDevice(h->device));
+    const size_t N = h->N;
+    if (velocity) {
+        std::vector<double4> v(N);
+        CK(cudaMemcpyAsync(v.data(), h->vel, N * sizeof(double4), cudaMemcpyDeviceToHost, h->stream));
+        CK(cudaStreamSynchronize(h->stream));
+        for (size_t c = 0; c < N; ++c) {
+            velocity[3 * c] = v[c].x; velocity[3 * c + 1] = v[c].y; velocity[3 * c + 2] = v[c].z;
+        }
+    }
+    if (momentum) {
+        CK(cudaMemcpyAsync(momentum, h->mom, 3 * N * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+        CK(cudaStreamSynchronize(h->stream));
+    }
+    return STORM_OK;
+}
+
 int storm_cuda_set_opacity_tables(StormHandle *h, const double *sigA, const double *sigS) {
     if (!h || !h->tabA) return STORM_ERR_INVALID_ARG;   // only the per-cell table opacity kinds have tables
     CK(cudaSetDevice(h->device));
@@ -2338,6 +2415,7 @@ int storm_cuda_replay_segments(StormHandle *h, StormReplayBatch *b) {
     R.mgrStatus = static_cast<int32_t *>(up(nullptr, n * sizeof(int32_t)));
     R.draws = static_cast<uint32_t *>(up(nullptr, n * sizeof(uint32_t)));
     R.usedRW = static_cast<int32_t *>(up(nullptr, n * sizeof(int32_t)));
+    R.momOut = b->phys_momentum ? static_cast<double *>(up(nullptr, 3 * n * sizeof(double))) : nullptr;
     bool ok = true;
     for (void *p : owned) ok = ok && p;
     int rc = STORM_OK;
@@ -2363,6 +2441,7 @@ int storm_cuda_replay_segments(StormHandle *h, StormReplayBatch *b) {
         cudaMemcpy(b->draws_used, R.draws, n * sizeof(uint32_t), cudaMemcpyDeviceToHost);
         cudaMemcpy(b->used_random_walk, R.usedRW, n * sizeof(int32_t), cudaMemcpyDeviceToHost);
         if (b->phys_frequency) cudaMemcpy(b->phys_frequency, R.freqOut, n * sizeof(double), cudaMemcpyDeviceToHost);
+        if (b->phys_momentum) cudaMemcpy(b->phys_momentum, R.momOut, 3 * n * sizeof(double), cudaMemcpyDeviceToHost);
     }
     for (void *p : owned)
         if (p) cudaFree(p);

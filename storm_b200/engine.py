@@ -53,6 +53,8 @@ def lib():
         L.storm_cuda_set_cell_state.argtypes = [vp, dp, dp, dp]
         L.storm_cuda_set_cell_physics.argtypes = [vp, dp, dp, dp]
         L.storm_cuda_set_opacity_tables.argtypes = [vp, dp, dp]
+        L.storm_cuda_set_cell_motion.argtypes = [vp, dp, dp]
+        L.storm_cuda_get_cell_motion.argtypes = [vp, dp, dp]
         L.storm_cuda_set_sharding.argtypes = [vp, C.c_uint32, C.c_uint32, C.c_uint32, A.ExchangeFn, vp]
         L.storm_cuda_get_beginning_counts.argtypes = [vp, u64p]
         L.storm_cuda_set_face_temperature.argtypes = [vp, C.c_int, C.c_double]
@@ -299,6 +301,18 @@ class Engine:
         """Per-cell opacity plug-in values for the next prestep (table opacity kinds)."""
         arr = [None if a is None else np.ascontiguousarray(a, float) for a in (sigma_a, sigma_s)]
         self._check(lib().storm_cuda_set_opacity_tables(self.h, *[A.ptr(a) for a in arr]))
+
+    def set_cell_motion(self, velocity=None, momentum=None):
+        """Cell velocities / momenta, (ncells, 3) each (handles with moving material)."""
+        arr = [None if a is None else np.ascontiguousarray(a, float).reshape(-1) for a in (velocity, momentum)]
+        self._check(lib().storm_cuda_set_cell_motion(self.h, *[A.ptr(a) for a in arr]))
+
+    def cell_motion(self):
+        """(velocity, momentum), (ncells, 3) each."""
+        v = np.zeros(3 * self.n)
+        m = np.zeros(3 * self.n)
+        self._check(lib().storm_cuda_get_cell_motion(self.h, A.ptr(v), A.ptr(m)))
+        return v.reshape(-1, 3), m.reshape(-1, 3)
 
     def beginning_counts(self):
         """Particles per cell when the last step's transport began (handles with

@@ -88,6 +88,9 @@ class Problem:
 
     # convex-polyhedral mesh (storm_b200.mesh.PolyMesh); None for the Cartesian grid
     mesh: object = None
+    # moving material (withHydro): per-cell velocity [cm/s], shape (ncells, 3); None = at rest
+    with_hydro: bool = False
+    cell_velocity: np.ndarray = None
 
     @property
     def shape(self):
@@ -190,6 +193,8 @@ class Problem:
             md = self.mesh.desc()
             keep.append(md)
             d.mesh = C.pointer(md)
+        d.with_hydro = int(self.with_hydro)
+        d.cell_velocity = arr(None if self.cell_velocity is None else np.asarray(self.cell_velocity).reshape(-1))
         d._keep = keep
         return d
 

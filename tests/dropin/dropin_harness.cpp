@@ -29,6 +29,7 @@ void bind_imc(STORM::CudaIMCBinding<Cell, Ext> &b, const StormProblemDesc *d) {
     p.ddmcUseMultigroupPGRW = d->ddmc_use_multigroup_pgrw != 0;
     p.ddmcMinCellOpticalDepth = d->ddmc_min_cell_optical_depth;
     p.ddmcMinParticleOpticalDepth = d->ddmc_min_particle_optical_depth;
+    p.withHydro = d->with_hydro != 0;
     if constexpr (G > 1) {
         p.withMultigroupOpacity = true;
         for (std::size_t g = 0; g <= G; ++g) p.energyBoundaries[g] = d->group_bounds[g];

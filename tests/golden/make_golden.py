@@ -24,9 +24,14 @@ Fixtures (numpy .npz):
   replay_ddmc_mg.npz  a 64-group cube with DDMC in its multigroup PGRW form
   replay_voronoi.npz  recorded calls on a 300-cell Voronoi mesh (Random Walk on), with
                       the mesh arrays (mesh_*)
+  replay_hydro.npz    recorded calls on an 8^3 step cube (Random Walk, elastic
+                      scattering in the thin half) whose cells move at up to 5 % of c
+                      (withHydro), with the velocities and each segment's momentum deposit
+  replay_hydro_mg.npz the same for a 64-group cube with PGRW
 
     python tests/golden/make_golden.py ddmc     # only the DDMC fixtures
     python tests/golden/make_golden.py voronoi  # only the Voronoi fixture
+    python tests/golden/make_golden.py hydro    # only the moving-material fixtures
 """
 import os
 import sys
@@ -46,6 +51,7 @@ def record(problem, warm_steps, max_records, take, mg=False):
         r.step()
     c = r.cells()     # tables of the last step; the recorded step recomputes them
     T_start = c["temperature"]
+    vel_start = r.motion()[0] if problem.with_hydro else None
     r.record_begin(max_records)
     r.step()
     r.record_end()
@@ -82,7 +88,34 @@ def record(problem, warm_steps, max_records, take, mg=False):
         out.update(freq_before=rec["freq_before"][sub], freq_after=rec["freq_after"][sub], T_start=T_start)
     if problem.with_ddmc:
         out.update(T_start=T_start)
+    if problem.with_hydro:   # the cells' velocities at the recorded step, and each segment's momentum deposit
+        out.update(T_start=T_start, vel_start=vel_start, momentum=rec["momentum"][sub])
     return out
+
+
+def hydro_velocity(p, beta=0.05):
+    """A smooth velocity field of the cells, |v| up to about beta c."""
+    from storm_b200.units import UNITS
+    xc, yc, zc = p.cell_centers()
+    v = np.stack([np.sin(2 * np.pi * yc), np.cos(2 * np.pi * xc), 0.5 * np.sin(2 * np.pi * zc)], 1)
+    return v * (beta * UNITS["clight"])
+
+
+def hydro_problems():
+    """The moving-material fixtures' problems (withHydro, cells moving at up to 5 % of c)."""
+    gray = problems.step_cube(n=8, new_photons_per_cell=3, face_packets=40, comb_nmin=20, seed=31)
+    gray.sigma_s = np.where(gray.cell_centers()[0] < 0.5, 2.0, 0.0)   # elastic scatters too
+    gray.with_hydro = True
+    gray.cell_velocity = hydro_velocity(gray)
+    mg = problems.mg_cube(n=6, groups=64, new_photons_per_cell=3, comb_nmin=3, seed=32)
+    mg.with_hydro = True
+    mg.cell_velocity = hydro_velocity(mg)
+    return {"replay_hydro.npz": gray, "replay_hydro_mg.npz": mg}
+
+
+def make_hydro():
+    for name, p in hydro_problems().items():
+        np.savez_compressed(os.path.join(HERE, name), **record(p, 1, 400000, 1500, mg=p.groups >= 2))
 
 
 def make_ddmc():
@@ -178,7 +211,10 @@ if __name__ == "__main__":
         make_ddmc()
     elif sys.argv[1:] == ["voronoi"]:
         make_voronoi()
+    elif sys.argv[1:] == ["hydro"]:
+        make_hydro()
     else:
         main()
         make_ddmc()
         make_voronoi()
+        make_hydro()

@@ -52,6 +52,7 @@ def _lib():
                                         C.c_size_t]
     L.dropin_beginning_counts.argtypes = [vp, C.POINTER(C.c_uint64)]
     L.ref_beginning_counts.argtypes = [vp, C.POINTER(C.c_uint64)]
+    L.ref_get_motion.argtypes = [vp, dp, dp]
     L.dropin_destroy.argtypes = [vp]
     L.dropin_ref.restype = vp
     L.dropin_ref.argtypes = [vp]
@@ -123,7 +124,7 @@ def _close(a, b, rel, atol=1e-300):
     return np.abs(a - b) <= rel * np.maximum(np.abs(a), np.abs(b)) + atol
 
 
-@pytest.mark.parametrize("kind", ["slab", "cube", "multigroup", "stratified", "ddmc", "voronoi"])
+@pytest.mark.parametrize("kind", ["slab", "cube", "multigroup", "stratified", "ddmc", "voronoi", "hydro"])
 def test_dropin_matches_engine(kind):
     L = _lib()
     if kind == "slab":
@@ -137,6 +138,14 @@ def test_dropin_matches_engine(kind):
         p = problems.strat_cube(n=4)
     elif kind == "voronoi":   # a Voronoi grid, lowered by the template through the Grid API
         p = problems.voronoi_cube(ncells=200, packets_per_step=1e4, seed=3)
+    elif kind == "hydro":   # moving cells: velocities in and momenta out through the cell and extensives types
+        import sys
+        from conftest import GOLDEN
+        sys.path.insert(0, GOLDEN)
+        import make_golden as MG
+        p = problems.step_cube(n=10, new_photons_per_cell=3, face_packets=60, comb_nmin=10)
+        p.with_hydro = True
+        p.cell_velocity = MG.hydro_velocity(p)
     else:   # DDMC leakage in the thick half
         p = problems.ddmc_cube(n=8, new_photons_per_cell=3, face_packets=40, comb_nmin=10)
     d = DropIn(L, p)
@@ -147,8 +156,15 @@ def test_dropin_matches_engine(kind):
             ce = e.cells()
             e.set_cell_state(ce["temperature"], ce["internal_energy"], ce["internal_energy"])
             e.set_census(e.census())
+            if p.with_hydro:
+                e.set_cell_motion(*e.cell_motion())
             se = e.step()
             sd = d.step()
+            if p.with_hydro:
+                vd, md = np.zeros((p.ncells, 3)), np.zeros((p.ncells, 3))
+                L.ref_get_motion(d.ref, A.ptr(vd), A.ptr(md))
+                ve, me = e.cell_motion()
+                assert _close(vd, ve, 1e-12, atol=1e-3).all() and _close(md, me, 1e-12, atol=1e-9).all(), s
             assert sd["initial"] == se["census_in"]
             assert sd["prestep"] == se["emitted_cells"] + se["emitted_faces"]
             assert sd["end"] == se["census_out"]
