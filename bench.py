@@ -278,8 +278,10 @@ def run_form(args, precision, seed, local, dist, timed=True):
 
 
 def transport_kernel(args, fp32):
-    """Name of the transport kernel the run launches (refill is the engine default)."""
-    form = "Form32" if fp32 else "Form64"
+    """Name of the transport kernel the run launches (refill is the engine default;
+    the gray FP32 form without the DDMC branch, Form32T<false, false>, for this
+    workload)."""
+    form = "Form32Lean" if fp32 else "Form64"
     if args.refill != 0:
         return f"k_transport_refill<{form}>"
     return "k_transport32" if fp32 else "k_transport"
@@ -296,7 +298,21 @@ def measured_traffic(kernel):
     return entry["dram_bytes_per_segment"], entry["capture"]
 
 
-def roofline(res, bytes_per_segment, kernel):
+def measured_issue(kernel):
+    """Warp instructions and thread instructions per segment of `kernel` from
+    the committed ncu summary, or None."""
+    path = os.path.join(ROOT, "profiles", "transport_issue.json")
+    if not os.path.exists(path):
+        return None
+    return json.load(open(path)).get(kernel)
+
+
+def roofline(res, bytes_per_segment, kernel, sm_mhz=None):
+    """The HBM roofline of the transport kernel by the fixed per-segment byte
+    convention, with the measured DRAM traffic beside it, and a second,
+    issue-based fraction: warp instructions per segment (ncu) x segments/s
+    against 148 SMs x 4 schedulers x the SM clock sampled in the timed region,
+    with the active lanes per warp instruction."""
     peak, src = _peak()
     tt = res["transport"]
     mean_ms = tt["kernel_ms"] / max(tt["launches"], 1)
@@ -311,6 +327,18 @@ def roofline(res, bytes_per_segment, kernel):
            "peak_source": src, "note": "peak = measured copy bandwidth (" + src + ")"}
     if capture:
         out["traffic_source"] = capture
+    if per_seg is not None:
+        out["dram_frac"] = traffic / (mean_ms / 1000.0) / 1e9 / peak   # measured bytes against the peak
+    iss = measured_issue(kernel)
+    if iss:
+        clock = (sm_mhz or 1965.0) * 1e6
+        seg_rate = segs_per_launch / (mean_ms / 1000.0)
+        inst_rate = iss["warp_inst_per_segment"] * seg_rate
+        out["issue"] = {"warp_inst_per_segment": iss["warp_inst_per_segment"],
+                        "achieved_inst_per_s": inst_rate, "peak_inst_per_s": 148 * 4 * clock,
+                        "frac": inst_rate / (148 * 4 * clock),
+                        "lanes_active_per_inst": iss["thread_inst_per_segment"] / iss["warp_inst_per_segment"],
+                        "sm_mhz": clock / 1e6, "source": iss["capture"]}
     return out
 
 
@@ -545,13 +573,15 @@ def run_storm(args, ws, rank, local, dist):
             "latency_ms": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99))},
             "segments_per_step": f32["segments"] / args.steps,
             "phase_ms_per_step": f32["phase_ms"],
-            "roofline": roofline(f32, BYTES_PER_SEGMENT_FP32, transport_kernel(args, True)),
+            "roofline": roofline(f32, BYTES_PER_SEGMENT_FP32, transport_kernel(args, True),
+                                 ck["sm_mhz"] if ck else None),
             "fp64": {"value": v64, "ms_per_step": ms64 / args.steps, "dtype": "f64",
                      "latency_ms": {"p50": float(np.percentile(f64["step_ms"], 50)),
                                     "p99": float(np.percentile(f64["step_ms"], 99))},
                      "segments_per_step": f64["segments"] / args.steps,
                      "phase_ms_per_step": f64["phase_ms"],
-                     "roofline": roofline(f64, BYTES_PER_SEGMENT_FP64, transport_kernel(args, False))},
+                     "roofline": roofline(f64, BYTES_PER_SEGMENT_FP64, transport_kernel(args, False),
+                                          ck["sm_mhz"] if ck else None)},
             "fp32_vs_fp64_deviation": dev,
             "cpu_baseline": cpu, "e2e": e2e, "serving": serving, "multigroup": multigroup, "voronoi": voronoi, "clocks": ck,
             "gpu_launches": f32["launches"],

@@ -52,6 +52,9 @@ struct FaceSources {
     const int32_t *side;
     const uint64_t *offset;
     uint32_t count;
+    // polyhedral meshes: the boundary face's index and its area (NULL on the Cartesian grid)
+    const uint32_t *face;
+    const double *area;
 };
 
 struct CombParams {

@@ -879,6 +879,42 @@ __device__ inline void point_on_face(const double q[4][3], RNG &rng, double &px,
     pz = a0 * q[0][2] + r1 * q[idx + 1][2] + r2 * q[idx + 2][2];
 }
 
+// RandomPointOnFace (utils/RandomOnFace.hpp:15-66) for polygon f of a
+// polyhedral mesh: the fan triangles (v0, v_t, v_t+1) picked by area (the
+// first whose cumulative area reaches u * total), then a folded barycentric
+// point.  The cumulative areas are recomputed on the second pass with the same
+// operations, so the pick sees the same numbers the total came from.
+template <class RNG>
+__device__ inline void point_on_polygon(const Ctx &C, uint32_t f, RNG &rng, double &px, double &py, double &pz) {
+    const uint32_t a = C.fvo[f], nv = C.fvo[f + 1] - a;
+    const double *v0 = C.vtx + 3 * static_cast<size_t>(C.fvi[a]);
+    auto tri_area = [&](uint32_t t) {
+        const double *v1 = C.vtx + 3 * static_cast<size_t>(C.fvi[a + t]);
+        const double *v2 = C.vtx + 3 * static_cast<size_t>(C.fvi[a + t + 1]);
+        const double ux = v1[0] - v0[0], uy = v1[1] - v0[1], uz = v1[2] - v0[2];
+        const double vx = v2[0] - v0[0], vy = v2[1] - v0[1], vz = v2[2] - v0[2];
+        const double cx = uy * vz - uz * vy, cy = uz * vx - ux * vz, cz = ux * vy - uy * vx;
+        return sqrt(cx * cx + cy * cy + cz * cz);
+    };
+    double total = 0.0;
+    for (uint32_t t = 1; t + 1 < nv; ++t) total += tri_area(t);
+    const double r = rng.raw() * total;
+    uint32_t idx = nv - 3;   // the last triangle when rounding leaves r above every cumulative area
+    double cum = 0.0;
+    for (uint32_t t = 1; t + 1 < nv; ++t) {
+        cum += tri_area(t);
+        if (!(cum < r)) { idx = t - 1; break; }
+    }
+    double r1 = rng.raw(), r2 = rng.raw();
+    if (r1 + r2 > 1) { r1 = 1 - r1; r2 = 1 - r2; }
+    const double a0 = 1 - r1 - r2;
+    const double *v1 = C.vtx + 3 * static_cast<size_t>(C.fvi[a + idx + 1]);
+    const double *v2 = C.vtx + 3 * static_cast<size_t>(C.fvi[a + idx + 2]);
+    px = a0 * v0[0] + r1 * v1[0] + r2 * v2[0];
+    py = a0 * v0[1] + r1 * v1[1] + r2 * v2[1];
+    pz = a0 * v0[2] + r1 * v1[2] + r2 * v2[2];
+}
+
 __device__ __forceinline__ bool outside_box(const Ctx &C, double x, double y, double z) {
     return x < C.X0 || x > C.X1 || y < C.Y0 || y > C.Y1 || z < C.Z0 || z > C.Z1;
 }
@@ -1047,15 +1083,24 @@ __global__ void k_emit_faces(Ctx C, FaceSources F, uint64_t fBegin, uint64_t cou
         const double T4 = (Tf * Tf) * (Tf * Tf);
         uint32_t i, j, k;
         cell_ijk(C, c, i, j, k);
-        const double dx = C.xe[i + 1] - C.xe[i], dy = C.ye[j + 1] - C.ye[j], dz = C.ze[k + 1] - C.ze[k];
-        const double area = axis == 0 ? dy * dz : (axis == 1 ? dz * dx : dx * dy);
+        double area;   // Grid::GetArea
+        if (C.poly) {
+            area = F.area[q];
+        } else {
+            const double dx = C.xe[i + 1] - C.xe[i], dy = C.ye[j + 1] - C.ye[j], dz = C.ze[k + 1] - C.ze[k];
+            area = axis == 0 ? dy * dz : (axis == 1 ? dz * dx : dx * dy);
+        }
         const double energy = C.sigmaSB * T4 * area * dt / static_cast<double>(Np);
         PhiloxRng rng;
         rng.init(C.seedLo, C.seedHi, TAG_FACE_EMIT, C.step, static_cast<uint32_t>(f), 0);
-        double qv[4][3];
-        face_vertices(C, i, j, k, side, qv);
         PartReg p;
-        point_on_face(qv, rng, p.x, p.y, p.z);
+        if (C.poly) {
+            point_on_polygon(C, F.face[q], rng, p.x, p.y, p.z);
+        } else {
+            double qv[4][3];
+            face_vertices(C, i, j, k, side, qv);
+            point_on_face(qv, rng, p.x, p.y, p.z);
+        }
         const double mu = sqrt(rng.raw());
         double v[3];
         v[axis] = sgn * mu;
@@ -1091,7 +1136,9 @@ __global__ void k_emit_faces(Ctx C, FaceSources F, uint64_t fBegin, uint64_t cou
             }
         }
         p.cell = c;
-        repair_outside(C, p.x, p.y, p.z, C.xc[i], C.yc[j], C.zc[k]);
+        double mx, my, mz;
+        mesh_point(C, c, mx, my, mz);
+        repair_outside(C, p.x, p.y, p.z, mx, my, mz);
         p.w0 = fabs(p.w);
         store_any(C, b, bankBase + static_cast<uint32_t>(slot), p, pidBase + static_cast<uint32_t>(f), 0);
         esum += p.w;

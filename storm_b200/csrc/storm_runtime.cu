@@ -78,6 +78,11 @@ struct StormHandle {
     uint64_t *fsOffset = nullptr;
     uint32_t fsCount = 0;
     uint64_t fsTotal = 0;
+    uint32_t *fsFace = nullptr;      // polyhedral meshes: the source faces' indices and areas
+    double *fsArea = nullptr;
+    // polyhedral meshes: every cell face on the box, in cell and GetCellFaces order
+    struct PolyBoundaryFace { uint32_t cell, face; int32_t side; double area; };
+    std::vector<PolyBoundaryFace> polyBoundary;
     // banks
     size_t cap = 0;
     Bank bankA{}, bankB{};
@@ -523,11 +528,22 @@ void box_faces(StormHandle *h) {
 // Boundary cell-faces with a source, cells in index order and sides in
 // GetCellFaces order (the order generateNewBoundaryParticles visits them).
 int build_face_sources(StormHandle *h) {
-    std::vector<uint32_t> cell;
+    std::vector<uint32_t> cell, face;
     std::vector<int32_t> side;
+    std::vector<double> area;
     std::vector<uint64_t> off(1, 0);
     const uint32_t nx = h->nx, ny = h->ny, nz = h->nz;
-    for (uint32_t c = 0; c < h->N; ++c) {
+    // a polyhedral mesh: its box faces in cell and GetCellFaces order
+    for (const auto &b : h->polyBoundary) {
+        const StormBoxFace &bf = h->desc.faces[b.side];
+        if (!(bf.source_temperature > 0.0) || bf.packets_per_face == 0) continue;
+        cell.push_back(b.cell);
+        side.push_back(b.side);
+        face.push_back(b.face);
+        area.push_back(b.area);
+        off.push_back(off.back() + bf.packets_per_face);
+    }
+    for (uint32_t c = 0; c < (h->C.poly ? 0u : h->N); ++c) {
         uint32_t i = c % nx, j = (c / nx) % ny, k = c / (nx * ny);
         bool bnd[6] = {i == 0, i + 1 == nx, j == 0, j + 1 == ny, k == 0, k + 1 == nz};
         for (int s = 0; s < 6; ++s) {
@@ -542,14 +558,24 @@ int build_face_sources(StormHandle *h) {
     dfree(h, h->fsCell, h->fsCount);
     dfree(h, h->fsSide, h->fsCount);
     dfree(h, h->fsOffset, h->fsCount + 1);
+    dfree(h, h->fsFace, h->fsCount);
+    dfree(h, h->fsArea, h->fsCount);
     h->fsCount = static_cast<uint32_t>(cell.size());
     h->fsTotal = off.back();
     CK(dalloc(h, &h->fsCell, cell.size()));
     CK(dalloc(h, &h->fsSide, side.size()));
     CK(dalloc(h, &h->fsOffset, off.size()));
+    CK(dalloc(h, &h->fsFace, cell.size()));
+    CK(dalloc(h, &h->fsArea, cell.size()));
     if (!cell.empty()) {
         CK(cudaMemcpyAsync(h->fsCell, cell.data(), cell.size() * sizeof(uint32_t), cudaMemcpyHostToDevice, h->stream));
         CK(cudaMemcpyAsync(h->fsSide, side.data(), side.size() * sizeof(int32_t), cudaMemcpyHostToDevice, h->stream));
+        if (!face.empty()) {
+            CK(cudaMemcpyAsync(h->fsFace, face.data(), face.size() * sizeof(uint32_t), cudaMemcpyHostToDevice,
+                               h->stream));
+            CK(cudaMemcpyAsync(h->fsArea, area.data(), area.size() * sizeof(double), cudaMemcpyHostToDevice,
+                               h->stream));
+        }
     }
     CK(cudaMemcpyAsync(h->fsOffset, off.data(), off.size() * sizeof(uint64_t), cudaMemcpyHostToDevice, h->stream));
     // the host vectors go out of scope here
@@ -841,10 +867,8 @@ int storm_cuda_create(const StormProblemDesc *d, StormHandle **out) {
         }
         for (uint32_t q = 0; q < mesh->face_vertex_offset[mesh->nfaces]; ++q)
             if (mesh->face_vertices[q] >= mesh->nvertices) return STORM_ERR_INVALID_ARG;
-        // DDMC and boundary sources are Cartesian only
+        // DDMC is Cartesian only
         if (d->with_ddmc) return STORM_ERR_UNSUPPORTED;
-        for (int f = 0; f < 6; ++f)
-            if (d->faces[f].source_temperature > 0.0 && d->faces[f].packets_per_face > 0) return STORM_ERR_UNSUPPORTED;
     } else {
         for (int a = 0; a < 3; ++a) {
             const double *e = a == 0 ? d->x_edges : (a == 1 ? d->y_edges : d->z_edges);
@@ -966,6 +990,16 @@ int storm_cuda_create(const StormProblemDesc *d, StormHandle **out) {
                 nextv[q] = (a0 == c) ? a1 : a0;
                 facev[q] = f;
                 S += mesh->face_area[f];   // computeCellSurfaceArea (radiation/RadiationIMC.hpp:971-980)
+                if (nextv[q] >= N) {   // a face on the box: its side from the outward normal (-inward),
+                                       // as the boundary plug-ins classify it (boundary/SideTemperature.hpp:126-131)
+                    const double o[3] = {-nx, -ny, -nz};
+                    int side = -1;
+                    for (int a = 0; a < 3 && side < 0; ++a) {
+                        if (o[a] < -0.99) side = 2 * a;
+                        else if (o[a] > 0.99) side = 2 * a + 1;
+                    }
+                    if (side >= 0) h->polyBoundary.push_back({c, f, side, mesh->face_area[f]});
+                }
             }
             chord[c] = (S > 0.0) ? 4.0 * vol[c] / S : 0.0;
         }
@@ -1214,7 +1248,7 @@ int storm_cuda_destroy(StormHandle *h) {
     void *ps[] = {h->xe, h->ye, h->ze, h->xc, h->yc, h->zc, h->A.T, h->A.mass, h->A.vol, h->A.eint, h->A.ceint,
                   h->A.sigA, h->A.sigS, h->A.fleck, h->A.rwSigT, h->A.eradAvg, h->A.eradCensus, h->A.emitE,
                   h->A.rwElig, h->A.photons, h->A.phys, h->A.phys32, h->hx, h->hy, h->hz, h->segs, h->beginCounts, h->tabA, h->tabS, h->rhoF,
-                  h->fsCell, h->fsSide, h->fsOffset, h->dAmbiguous, h->offsets, h->tileSums, h->dTotalU64, h->dTotalE, h->combW, h->combWtot,
+                  h->fsCell, h->fsSide, h->fsOffset, h->fsFace, h->fsArea, h->dAmbiguous, h->offsets, h->tileSums, h->dTotalU64, h->dTotalE, h->combW, h->combWtot,
                   h->combStart, h->combCount, h->counts, h->dStats, h->dErr, h->gb, h->A.mgCdf, h->A.pgrw,
                   h->A.pgrwCut, h->gb32, h->gc32, h->faceCdf, h->mgEp, h->mgEp32, h->mgKTq, h->ddmc, h->ddmcTot,
                   h->ddmcRate, h->ddmcCut, h->ddmc32, h->stratBounds, h->stratBinW, h->stratStart,
@@ -1353,7 +1387,8 @@ int storm_cuda_phase_emit(StormHandle *h, double dt) {
     }
     launch_emit_cells(h->stream, h->C, h->A, h->offsets, eLo, eHi - eLo, h->bankA, static_cast<uint32_t>(h->nCensus),
                       static_cast<uint32_t>(h->nCenGlobal), dt, h->dStats);
-    FaceSources F{h->fsCell, h->fsSide, h->fsOffset, h->fsCount};
+    FaceSources F{h->fsCell, h->fsSide, h->fsOffset, h->fsCount, h->C.poly ? h->fsFace : nullptr,
+                  h->C.poly ? h->fsArea : nullptr};
     if (nf && h->C.groups >= 2 && std::memcmp(h->faceCdfT, h->C.sourceT, sizeof(h->faceCdfT)) != 0) {
         launch_face_spectra(h->stream, h->C, h->faceCdf);
         ++h->launches;

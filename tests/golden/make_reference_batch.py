@@ -23,7 +23,7 @@ Workloads (storm_b200.problems):
        source packets per step), 20 steps, recorded after steps 1, 10, 20;
        24 seeds
   marshak1  Marshak wave 1 (examples/marshak_wave) at the example's defaults,
-       7,912 steps to 1 ns with the bath updated before each step; 8 seeds
+       7,912 steps to 1 ns with the bath updated before each step; 24 seeds
 Arrays per workload <w>: batchstats.summary_for_fixture of the runs
 (<w>_mean, <w>_var, <w>_n, <w>_nonzero, <w>_total_*), <w>_snapshots,
 <w>_seeds and <w>_wall (seconds per run).  For marshak1 instead: the final
@@ -57,7 +57,7 @@ def workload(name, seed):
 WORKLOADS = {
     "c1": dict(steps=100, snapshots=(1, 5, 20, 50, 100), seeds=list(range(1000, 1032))),
     "c2r": dict(steps=20, snapshots=(1, 10, 20), seeds=list(range(1000, 1024))),
-    "marshak1": dict(seeds=list(range(1000, 1008))),
+    "marshak1": dict(seeds=list(range(1000, 1024))),
 }
 
 

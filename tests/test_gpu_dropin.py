@@ -279,7 +279,7 @@ def test_dropin_slab_with_plugin_opacity_matches_reference_batch():
     fx = {k[3:]: v for k, v in g.items() if k.startswith("c1_")}
     res = batchstats.compare(np.array(runs), fx)
     print(json.dumps({"workload": "c1 through MonteCarloManagerCUDA", "all": res["all"], "totals": res["totals"]}))
-    assert res["all"]["tests"] > 0.5 * fx["mean"].size
+    assert res["all"]["tests"] > 0.1 * fx["mean"].size   # cold cells carry no sampling noise
     assert res["passed"], res["all"] | {"totals": res["totals"]}
 
 

@@ -145,3 +145,57 @@ def test_voronoi_fp32_tracking_agrees_with_fp64():
                 assert side * np.dot(pos[q] - fc, nrm) >= -1e-7, (k, f)
     assert_agree(run_batch(Engine, prob(A.PRECISION_FP32_TRACK), range(30, 46), 4, check),
                  run_batch(Engine, prob(A.PRECISION_FP64), range(70, 86), 4, check), "Voronoi 400 cells: FP32 vs FP64")
+
+
+def _face_source_problem(mesh, seed, precision=None):
+    from storm_b200 import _abi as A
+    from storm_b200.units import UNITS
+    p = problems.voronoi_cube(ncells=mesh.ncells, packets_per_step=2e4, seed=11, mesh=mesh)
+    p.seed = seed
+    p.faces[0] = problems.BoxFace(A.FACE_ESCAPE, 0.5 * UNITS["kev_kelvin"], 20)   # x-low: escape and a 0.5 keV source
+    if precision is not None:
+        p.precision = precision
+    return p
+
+
+def _x_low_faces(mesh):
+    """The mesh's faces on the x-low box plane."""
+    return [f for c in range(mesh.ncells)
+            for f in mesh.cell_faces[mesh.cell_face_offset[c]:mesh.cell_face_offset[c + 1]]
+            if mesh.face_cells[f, 1] >= mesh.ncells and abs(mesh.face_cm[f, 0] - mesh.box[0]) < 1e-12]
+
+
+def test_voronoi_face_source_matches_reference(ref_lib):
+    """A Planck source on the x-low box face of a Voronoi mesh (the boundary
+    plug-in over the mesh's polygonal box faces, RandomPointOnFace's fan
+    triangles): 20 packets per x-low face, every packet on the face plane moving
+    into the box, each with the face's share sigma T^4 A dt / N; then whole
+    steps against the reference's serial path on the same mesh under the batch
+    gate, and the FP32 form against the FP64 form."""
+    from batchcheck import assert_agree, run_batch
+    from storm_b200 import _abi as A
+    from storm_b200.units import UNITS
+    mesh = build_voronoi(np.random.default_rng(11).random((300, 3)) * 0.98 + 0.01)
+    faces = _x_low_faces(mesh)
+    nf = len(faces)
+    assert nf > 5
+    p = _face_source_problem(mesh, 5)
+    e = Engine(p)
+    for ph in ("begin", "prestep", "emit"):
+        e.phase(ph)
+    st = e.stats()
+    assert st["emitted_faces"] == 20 * nf
+    b = e.bank()
+    face = slice(b.n - 20 * nf, b.n)
+    assert np.abs(b.x[face] - mesh.box[0]).max() < 1e-12 and (b.vx[face] > 0).all()
+    T = p.faces[0].source_temperature
+    total = b.weight[face].sum()
+    area = sum(mesh.face_area[f] for f in faces)
+    assert abs(total - UNITS["sigma_sb"] * T ** 4 * area * p.dt) < 1e-10 * total
+    e.close()
+    prob = lambda s: _face_source_problem(mesh, s)   # noqa: E731
+    assert_agree(run_batch(Engine, prob, range(20, 36), 4), run_batch(ref_lib.Reference, prob, range(60, 76), 4),
+                 "Voronoi 300 cells with an x-low face source: engine vs reference")
+    prob32 = lambda s: _face_source_problem(mesh, s, A.PRECISION_FP32_TRACK)   # noqa: E731
+    assert_agree(run_batch(Engine, prob32, range(120, 136), 4), run_batch(Engine, prob, range(160, 176), 4),
+                 "Voronoi 300 cells with an x-low face source: FP32 vs FP64")
