@@ -373,11 +373,36 @@ def e2e_run(args, eng, p, dist):
     torch.cuda.synchronize()
     wall = reduce(dist, time.perf_counter() - t0, "max", "storm")
     allsegs = reduce(dist, segs, "sum", "storm")
-    return {"value": allsegs / wall, "unit": UNIT, "h2d_bytes_per_step": int(h2d / args.e2e_steps),
-            "d2h_bytes_per_step": int(d2h / args.e2e_steps), "steps": args.e2e_steps,
+    link = link_bandwidth()
+    steps = max(args.e2e_steps, 1)
+    floor_ms = (h2d / steps) / link["h2d_gbs"] / 1e6 + (d2h / steps) / link["d2h_gbs"] / 1e6
+    return {"value": allsegs / wall, "unit": UNIT, "h2d_bytes_per_step": int(h2d / steps),
+            "d2h_bytes_per_step": int(d2h / steps), "steps": args.e2e_steps,
+            "ms_per_step": wall / steps * 1e3, "link": link, "copy_ms_per_step_at_link_rate": floor_ms,
             "note": "census in and out through storm_cuda_set_census / storm_cuda_step / storm_cuda_get_census, "
                     "temperatures through storm_cuda_get_cell_arrays; page-locked host buffers; copies and "
-                    "host-side checks inside the timed region (wall clock)"}
+                    "host-side checks inside the timed region (wall clock); link = one 1 GiB page-locked copy "
+                    "each way, CUDA-event timed"}
+
+
+def link_bandwidth(nbytes=1 << 30):
+    """Host<->device copy rate of this GPU's link: one page-locked copy of
+    `nbytes` each way after a warm-up copy, timed with CUDA events."""
+    import torch
+    host = torch.empty(nbytes, dtype=torch.uint8, pin_memory=True)
+    dev = torch.empty(nbytes, dtype=torch.uint8, device="cuda")
+    out = {}
+    for name, (dst, src) in (("h2d_gbs", (dev, host)), ("d2h_gbs", (host, dev))):
+        dst.copy_(src, non_blocking=True)
+        torch.cuda.synchronize()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record()
+        dst.copy_(src, non_blocking=True)
+        b.record()
+        torch.cuda.synchronize()
+        out[name] = nbytes / (a.elapsed_time(b) * 1e-3) / 1e9
+    del host, dev
+    return out
 
 
 def mg_run(args):

@@ -63,9 +63,15 @@ def test_marshak_wave_against_diffusion_reference(problem, form):
     l1 = B.marshak_l1(res["x"], res["t_gas"], curve)
     l1_ref = _against_reference_run(res, name, P.marshak_wave(problem).volumes())
     print(f"{name} {form}: TGAS_REL_L1 = {l1:.4e} over {res['steps']} steps (reference serial run {l1_ref:.4e})")
-    # one realization against the regression gate; the distribution of Marshak
-    # 1's L1 over seeds is compared with the reference's own in test_gpu_fullrun
-    gate = 0.10 if l1_ref < 0.10 else 2.0 * l1_ref
+    # one realization against the regression gate.  Marshak 1's L1 scatters
+    # past it in the reference's own runs (one of its 24 seeds in
+    # tests/golden/reference_batch.npz reaches 0.144), so a single run of it is
+    # held to twice the gate; the distribution of its L1 over seeds is compared
+    # with the reference's in test_gpu_fullrun
+    if problem == 1:
+        gate = 0.20
+    else:
+        gate = 0.10 if l1_ref < 0.10 else 2.0 * l1_ref
     assert 0.0 <= l1 < gate
 
 
