@@ -227,7 +227,8 @@ typedef struct StormProblemDesc {
 
     /* ---- convex-polyhedral mesh (NULL: the Cartesian grid of nx, ny, nz and the
      * edges).  With a mesh, the per-cell arrays follow its cell order and the box
-     * faces are the mesh's box; the FP64 form, no DDMC and no face sources. */
+     * faces are the mesh's box; either form, with DDMC and face sources, but a
+     * gray opacity only (no groups) and no moving material. */
     const struct StormPolyMesh *mesh;
 
     /* ---- moving material (RadiationIMCParameters::withHydro with cells that

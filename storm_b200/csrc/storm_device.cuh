@@ -115,7 +115,10 @@ struct Ctx {
     double ddmcMinParticle, ddmcMinCell;
     double4 *ddmc;           // per cell: sigma_T, sigma_A, eligible (1/0), D  (prestep)
     double *ddmcTot;         // per cell: total leak rate [1/s], 0 where not eligible
-    double *ddmcRate;        // per cell x 6 faces in GetCellFaces order: leak rate, 0 where none
+    double *ddmcRate;        // per cell x 6 faces in GetCellFaces order (polyhedral: per cell-face slot):
+                             // leak rate, 0 where none
+    float *ddmcCum32;        // FP32 form on a polyhedral mesh, per cell-face slot: cumulative leak fraction
+    const double *cfA;       // polyhedral mesh, per cell-face slot: the face's area (GetArea)
     uint32_t *ddmcCut;       // per cell: group cutoff (multigroup PGRW form)
     float4 *ddmc32;          // FP32 form, 3 per cell: (reach, 1/total, sigma_A f c, frequency bound),
                              // (cumulative face fractions 0-3), (fractions 4-5, last leak face, 0)
@@ -384,26 +387,62 @@ struct SegmentTally {
 // where x >= 0.5), far inside the 1e-12 the tables are held to.
 constexpr double PI_NORM_PI = 3.14159265358979323846;
 __device__ __forceinline__ double pi_norm() { return 15.0 / (PI_NORM_PI * PI_NORM_PI * PI_NORM_PI * PI_NORM_PI); }
-__device__ inline double pi_small_series(double x) {
-    const double B[21] = {1.0, -0.5, 1.0 / 6.0, 0.0, -1.0 / 30.0, 0.0, 1.0 / 42.0, 0.0, -1.0 / 30.0, 0.0,
-                          5.0 / 66.0, 0.0, -691.0 / 2730.0, 0.0, 7.0 / 6.0, 0.0, -3617.0 / 510.0, 0.0,
-                          43867.0 / 798.0, 0.0, -174611.0 / 330.0};
-    double sum = 0.0, xp = x * x * x, fact = 1.0;
-#pragma unroll
-    for (int k = 0; k <= 20; ++k) {
-        if (k > 0) { fact *= k; xp *= x; }
-        if (B[k] != 0.0) sum += B[k] * xp / (fact * (k + 3));
+// The series' constants, folded at compile time so that the device multiplies
+// instead of dividing: the small-x coefficients B_k / (k! (k + 3)), and 1/n^j
+// (j = 1..4) for the first PI_TAIL_TABLE tail terms.  Both change the sums by
+// a few ulps, inside the tables' 1e-12.
+struct PiSmallCoef {
+    double c[21];
+    constexpr PiSmallCoef() : c() {
+        const double B[21] = {1.0, -0.5, 1.0 / 6.0, 0.0, -1.0 / 30.0, 0.0, 1.0 / 42.0, 0.0, -1.0 / 30.0, 0.0,
+                              5.0 / 66.0, 0.0, -691.0 / 2730.0, 0.0, 7.0 / 6.0, 0.0, -3617.0 / 510.0, 0.0,
+                              43867.0 / 798.0, 0.0, -174611.0 / 330.0};
+        double fact = 1.0;
+        for (int k = 0; k <= 20; ++k) {
+            if (k > 0) fact *= k;
+            c[k] = B[k] / (fact * (k + 3));
+        }
     }
-    return sum;
+};
+constexpr int PI_TAIL_TABLE = 128;
+struct PiTailInv {
+    double v[4 * PI_TAIL_TABLE];   // per n: 1/n, 1/n^2, 1/n^3, 1/n^4
+    constexpr PiTailInv() : v() {
+        for (int n = 1; n <= PI_TAIL_TABLE; ++n) {
+            const double d = n, d2 = d * d;
+            v[4 * (n - 1)] = 1.0 / d;
+            v[4 * (n - 1) + 1] = 1.0 / d2;
+            v[4 * (n - 1) + 2] = 1.0 / (d2 * d);
+            v[4 * (n - 1) + 3] = 1.0 / (d2 * d2);
+        }
+    }
+};
+static __constant__ PiSmallCoef c_piSmall = PiSmallCoef();
+static __constant__ PiTailInv c_piTail = PiTailInv();
+
+__device__ inline double pi_small_series(double x) {
+    // x^3 sum_k c_k x^k, the zero coefficients skipped, by Horner in x
+    double sum = c_piSmall.c[20];
+#pragma unroll
+    for (int k = 19; k >= 0; --k) sum = sum * x + c_piSmall.c[k];
+    return sum * (x * x * x);
 }
 __device__ inline double pi_tail_series(double x) {
     const double e1 = exp(-x);
     const double x2 = x * x, x3 = x2 * x;
+    const double a2 = 3.0 * x2, a3 = 6.0 * x;
     double sum = 0.0, e = e1;
+    // every lane of a warp takes term n at the same time, so the table read is uniform
     for (int n = 1; n < 100000 && e != 0.0; ++n) {
-        const double dn = n;
-        const double d2 = dn * dn;
-        const double term = e * ((((x3 * dn + 3.0 * x2) * dn + 6.0 * x) * dn + 6.0) / (d2 * d2));
+        double term;
+        if (n <= PI_TAIL_TABLE) {
+            const double *iv = c_piTail.v + 4 * (n - 1);
+            term = e * (((x3 * iv[0] + a2 * iv[1]) + a3 * iv[2]) + 6.0 * iv[3]);
+        } else {
+            const double dn = n;
+            const double d2 = dn * dn;
+            term = e * ((((x3 * dn + a2) * dn + a3) * dn + 6.0) / (d2 * d2));
+        }
         sum += term;
         if (term < 1e-18 * sum) break;
         e *= e1;
@@ -697,6 +736,49 @@ __device__ inline int try_random_walk(const Ctx &C, PartReg &p, RNG &rng, TALLY 
 }
 
 // ------------------------------------------------------------------ physics step
+// tryDDMCStep's leak face (radiation/RadiationIMC.hpp:1524-1540): subtract the
+// positive face rates in GetCellFaces order from u * total; the last face
+// with a rate when rounding leaves some over; -1 when no face has one.
+template <class RNG>
+__device__ __forceinline__ int ddmc_pick_face(RNG &rng, const double *rates, int nf, double total) {
+    double facePick = rng.open() * total;
+    int chosen = -1, last = -1;
+    for (int s = 0; s < nf; ++s) {
+        const double r = rates[s];
+        if (!(r > 0.0) || chosen >= 0) continue;
+        last = s;
+        facePick -= r;
+        if (facePick <= 0.0) chosen = s;
+    }
+    return chosen < 0 ? last : chosen;
+}
+// tryDDMCStep's leak direction (:1561-1589): cosine law about the unit normal n
+// (pointing at the neighbour), in the frame of a helper axis.
+template <class RNG>
+__device__ __forceinline__ void ddmc_leak_direction(RNG &rng, const double n[3], double dir[3]) {
+    const double PI_D = 3.14159265358979323846;
+    const double u4 = rng.open();
+    const double xiMu = (u4 < 1.0) ? u4 : 1.0;   // std::min(1.0, u)
+    const double mu = sqrt(xiMu);
+    const double phiLeak = 2.0 * PI_D * rng.open();
+    const double st2 = 1.0 - mu * mu;
+    const double sinTheta = sqrt(st2 > 0.0 ? st2 : 0.0);
+    double h[3] = {0.0, 0.0, 0.0};
+    if (fabs(n[0]) < 0.9) h[0] = 1.0; else h[1] = 1.0;
+    const double hn = h[0] * n[0] + h[1] * n[1] + h[2] * n[2];
+    double e1[3] = {h[0] - n[0] * hn, h[1] - n[1] * hn, h[2] - n[2] * hn};
+    const double e1m = sqrt(e1[0] * e1[0] + e1[1] * e1[1] + e1[2] * e1[2]);
+    if (e1m > 0.0) { e1[0] = e1[0] / e1m; e1[1] = e1[1] / e1m; e1[2] = e1[2] / e1m; }
+    double e2[3] = {n[1] * e1[2] - n[2] * e1[1], n[2] * e1[0] - n[0] * e1[2], n[0] * e1[1] - n[1] * e1[0]};
+    const double e2m = sqrt(e2[0] * e2[0] + e2[1] * e2[1] + e2[2] * e2[2]);
+    if (e2m > 0.0) { e2[0] = e2[0] / e2m; e2[1] = e2[1] / e2m; e2[2] = e2[2] / e2m; }
+    const double a1 = sinTheta * cos(phiLeak), a2 = sinTheta * sin(phiLeak);
+#pragma unroll
+    for (int q = 0; q < 3; ++q) dir[q] = (n[q] * mu + e1[q] * a1) + e2[q] * a2;
+    const double dm = sqrt(dir[0] * dir[0] + dir[1] * dir[1] + dir[2] * dir[2]);
+    if (dm > 0.0) { dir[0] = dir[0] / dm; dir[1] = dir[1] / dm; dir[2] = dir[2] / dm; }
+}
+
 // RadiationIMC::tryDDMCStep (radiation/RadiationIMC.hpp:1416-1612) on a
 // Cartesian cell.  Returns -1 when the step is not taken (no draws consumed),
 // else the ParticleStatus; a leak sets face and next.  precomputeDDMCData sets
@@ -742,18 +824,7 @@ __device__ inline int try_ddmc(const Ctx &C, PartReg &p, RNG &rng, TALLY &tal, d
     const double eventPick = rng.open() * eventRate;
     if (!(eventPick <= total)) return DONE;   // the upscatter branch; unreachable with a zero upscatter rate
     // the leak face: subtract the face rates in GetCellFaces order
-    double facePick = rng.open() * total;
-    const double *rates = C.ddmcRate + static_cast<size_t>(cell) * 6;
-    int chosen = -1, last = -1;
-#pragma unroll
-    for (int s = 0; s < 6; ++s) {
-        const double r = rates[s];
-        if (!(r > 0.0) || chosen >= 0) continue;
-        last = s;
-        facePick -= r;
-        if (facePick <= 0.0) chosen = s;
-    }
-    if (chosen < 0) chosen = last;
+    const int chosen = ddmc_pick_face(rng, C.ddmcRate + static_cast<size_t>(cell) * 6, 6, total);
     if (chosen < 0) return DONE;
     uint32_t i, j, k;
     cell_ijk(C, cell, i, j, k);
@@ -764,28 +835,8 @@ __device__ inline int try_ddmc(const Ctx &C, PartReg &p, RNG &rng, TALLY &tal, d
     // Normal(face) is the +axis unit vector; flipped to point at the neighbour
     double n[3] = {axis == 0 ? 1.0 : 0.0, axis == 1 ? 1.0 : 0.0, axis == 2 ? 1.0 : 0.0};
     if (!hi) { n[0] = n[0] * (-1.0); n[1] = n[1] * (-1.0); n[2] = n[2] * (-1.0); }
-    const double PI_D = 3.14159265358979323846;
-    const double u4 = rng.open();
-    const double xiMu = (u4 < 1.0) ? u4 : 1.0;   // std::min(1.0, u)
-    const double mu = sqrt(xiMu);
-    const double phiLeak = 2.0 * PI_D * rng.open();
-    const double st2 = 1.0 - mu * mu;
-    const double sinTheta = sqrt(st2 > 0.0 ? st2 : 0.0);
-    double h[3] = {0.0, 0.0, 0.0};
-    if (fabs(n[0]) < 0.9) h[0] = 1.0; else h[1] = 1.0;
-    const double hn = h[0] * n[0] + h[1] * n[1] + h[2] * n[2];
-    double e1[3] = {h[0] - n[0] * hn, h[1] - n[1] * hn, h[2] - n[2] * hn};
-    const double e1m = sqrt(e1[0] * e1[0] + e1[1] * e1[1] + e1[2] * e1[2]);
-    if (e1m > 0.0) { e1[0] = e1[0] / e1m; e1[1] = e1[1] / e1m; e1[2] = e1[2] / e1m; }
-    double e2[3] = {n[1] * e1[2] - n[2] * e1[1], n[2] * e1[0] - n[0] * e1[2], n[0] * e1[1] - n[1] * e1[0]};
-    const double e2m = sqrt(e2[0] * e2[0] + e2[1] * e2[1] + e2[2] * e2[2]);
-    if (e2m > 0.0) { e2[0] = e2[0] / e2m; e2[1] = e2[1] / e2m; e2[2] = e2[2] / e2m; }
-    const double a1 = sinTheta * cos(phiLeak), a2 = sinTheta * sin(phiLeak);
     double dir[3];
-#pragma unroll
-    for (int q = 0; q < 3; ++q) dir[q] = (n[q] * mu + e1[q] * a1) + e2[q] * a2;
-    const double dm = sqrt(dir[0] * dir[0] + dir[1] * dir[1] + dir[2] * dir[2]);
-    if (dm > 0.0) { dir[0] = dir[0] / dm; dir[1] = dir[1] / dm; dir[2] = dir[2] / dm; }
+    ddmc_leak_direction(rng, n, dir);
     p.x = fc[0]; p.y = fc[1]; p.z = fc[2];
     p.vx = dir[0] * C.clight; p.vy = dir[1] * C.clight; p.vz = dir[2] * C.clight;
     face = chosen;
@@ -797,6 +848,64 @@ __device__ inline int try_ddmc(const Ctx &C, PartReg &p, RNG &rng, TALLY &tal, d
     case 4: next = cell - C.nx * C.ny; break;
     default: next = cell + C.nx * C.ny; break;
     }
+    return CELL_MOVE;
+}
+
+// tryDDMCStep on a convex-polyhedral cell: the distances to the faces, the
+// leak face and its neighbour from the cell-face slots; the particle leaves
+// from the face centroid (FaceCM) along a cosine law about Normal(face) / |.|
+// turned toward the neighbour's mesh point.  The inward slot normal is that
+// unit normal up to its sign, so negating it and applying the same test gives
+// the reference's vector.  Gray only (polyhedral meshes take no multigroup
+// opacity).
+template <class RNG, class TALLY>
+__device__ inline int try_ddmc_poly(const Ctx &C, PartReg &p, RNG &rng, TALLY &tal, const PolyGeom &g,
+                                    uint32_t &next) {
+    const uint32_t cell = p.cell;
+    const double total = C.ddmcTot[cell];
+    if (!(total > 0.0)) return -1;
+    const double4 dd = C.ddmc[cell];   // sigma_T, sigma_A, -, D
+    double Ro = DBL_MAX;
+    for (int s = 0; s < g.nf(); ++s) {
+        const double d = g.dist(s, p.x, p.y, p.z);
+        Ro = (d < Ro) ? d : Ro;
+    }
+    Ro = (Ro > 0.0) ? Ro : 0.0;
+    if (Ro * dd.x < C.ddmcMinParticle) return -1;
+    const double f = C.fleck[cell];
+    const double eventRate = total;
+    const double tEvent = -log(rng.open()) / eventRate;
+    const double tCensus = p.t;
+    const double dt = (tCensus < tEvent) ? tCensus : tEvent;   // std::min(tEvent, tCensus)
+    const bool censusEvent = (tCensus <= tEvent);
+    const double absRate = dd.y * f * C.clight;
+    const double oldWeight = p.w;
+    const double expFactor = expm1(-dt * absRate);
+    if (!C.noFeedback) tal.mat(cell, -expFactor * oldWeight);
+    const double integrated = (absRate > 0.0) ? oldWeight * expFactor * (-1.0 / absRate) : oldWeight * dt;
+    tal.rad(cell, integrated);
+    p.w *= 1.0 + expFactor;
+    p.t -= dt;
+    if (fabs(p.w) < p.w0 * 1e-3) {
+        if (!C.noFeedback) tal.mat(cell, p.w);
+        return REMOVE;
+    }
+    if (censusEvent) return DONE;
+    const double eventPick = rng.open() * eventRate;
+    if (!(eventPick <= total)) return DONE;   // the upscatter branch; unreachable with a zero upscatter rate
+    const int chosen = ddmc_pick_face(rng, C.ddmcRate + g.k0, g.nf(), total);
+    if (chosen < 0) return DONE;
+    const uint32_t k = g.k0 + static_cast<uint32_t>(chosen);
+    const uint32_t nb = C.cfNext[k];
+    const double4 nin = C.cfN[k], fcm = C.cfP[k];
+    double n[3] = {nin.x * (-1.0), nin.y * (-1.0), nin.z * (-1.0)};
+    const double tx = C.mpx[nb] - C.mpx[cell], ty = C.mpy[nb] - C.mpy[cell], tz = C.mpz[nb] - C.mpz[cell];
+    if (n[0] * tx + n[1] * ty + n[2] * tz < 0.0) { n[0] = n[0] * (-1.0); n[1] = n[1] * (-1.0); n[2] = n[2] * (-1.0); }
+    double dir[3];
+    ddmc_leak_direction(rng, n, dir);
+    p.x = fcm.x; p.y = fcm.y; p.z = fcm.z;
+    p.vx = dir[0] * C.clight; p.vy = dir[1] * C.clight; p.vz = dir[2] * C.clight;
+    next = nb;
     return CELL_MOVE;
 }
 
@@ -972,10 +1081,16 @@ __device__ inline PhysOut physics_step(const Ctx &C, Track &T, RNG &rng, TALLY &
             return o;
         }
     }
-    if (FULL && !POLY && C.withDDMC) {
+    if ((FULL || POLY) && C.withDDMC) {
         int dface = -1;
         uint32_t dnext = OUTSIDE;
-        const int r = try_ddmc(C, p, rng, tal, xl, xh, yl, yh, zl, zh, dface, dnext);
+        int r;
+        if constexpr (POLY) {
+            const PolyGeom g{&C, C.cfo[cell], C.cfo[cell + 1], C.mpx[cell], C.mpy[cell], C.mpz[cell]};
+            r = try_ddmc_poly(C, p, rng, tal, g, dnext);
+        } else {
+            r = try_ddmc(C, p, rng, tal, xl, xh, yl, yh, zl, zh, dface, dnext);
+        }
         if (r >= 0) {
             o.status = r;
             o.usedRW = 2;
@@ -1275,6 +1390,68 @@ __device__ inline int ddmc_jump32(const Ctx &C, Track32 &T, RNG &rng, TALLY &tal
     return OUT_CONTINUE;
 }
 
+// tryDDMCStep in the FP32-tracking form on a convex-polyhedral cell: the
+// same event, attenuation and tallies as ddmc_jump32; the leak face is picked
+// by the per-slot cumulative fractions, and the particle enters the neighbour
+// at the face centroid (offset from the neighbour's mesh point, nudged
+// ENTRY32 toward it) with a cosine-law direction about the face's unit normal
+// turned toward the neighbour.
+template <class RNG, class TALLY>
+__device__ inline int ddmc_jump32_poly(const Ctx &C, Track32 &T, RNG &rng, TALLY &tal, const float4 &da) {
+    const uint32_t cell = T.cell;
+    const double tEvent = static_cast<double>(-__logf(rng.rawf()) * da.y);
+    const bool census = T.t <= tEvent;
+    const double dt = census ? T.t : tEvent;
+    const float tau = da.z * static_cast<float>(dt);
+    const double e1 = static_cast<double>(expm1f(-tau));
+    if (!C.noFeedback) tal.mat(cell, -e1 * T.w);
+    tal.rad(cell, da.z > 0.0f ? T.w * e1 * (-1.0 / static_cast<double>(da.z)) : T.w * dt);
+    T.w *= 1.0 + e1;
+    T.t -= dt;
+    if (fabs(T.w) < T.w0 * 1e-3) {
+        if (!C.noFeedback) tal.mat(cell, T.w);
+        return OUT_CUTOFF;
+    }
+    if (census) return OUT_CENSUS;
+    const uint32_t k0 = C.cfo[cell], k1 = C.cfo[cell + 1];
+    const float u = rng.rawf();
+    int last = static_cast<int>(C.ddmc32[3 * static_cast<size_t>(cell) + 2].z);   // the last slot with a leak rate
+    if (last < 0) return OUT_CENSUS;
+    uint32_t k = k0 + static_cast<uint32_t>(last);
+    for (uint32_t q = k0; q < k1; ++q)
+        if (u <= C.ddmcCum32[q]) { k = q; break; }
+    const uint32_t nb = C.cfNext[k];
+    const float4 pl = C.cfN32[k];
+    float n0 = -pl.x, n1 = -pl.y, n2 = -pl.z;   // outward: toward the neighbour
+    const float tx = static_cast<float>(C.mpx[nb] - C.mpx[cell]), ty = static_cast<float>(C.mpy[nb] - C.mpy[cell]),
+                tz = static_cast<float>(C.mpz[nb] - C.mpz[cell]);
+    if (n0 * tx + n1 * ty + n2 * tz < 0.0f) { n0 = -n0; n1 = -n1; n2 = -n2; }
+    const float mu = sqrtf(rng.rawf());
+    const float phi = 6.2831853f * rng.rawf();
+    const float st = sqrtf(fmaxf(0.0f, 1.0f - mu * mu));
+    float sp, cph;
+    __sincosf(phi, &sp, &cph);
+    float h0 = 0.0f, h1 = 0.0f;
+    if (fabsf(n0) < 0.9f) h0 = 1.0f; else h1 = 1.0f;
+    const float hn = h0 * n0 + h1 * n1;
+    float a0 = h0 - n0 * hn, a1 = h1 - n1 * hn, a2 = -n2 * hn;
+    const float am = rsqrtf(fmaxf(a0 * a0 + a1 * a1 + a2 * a2, 1e-30f));
+    a0 *= am; a1 *= am; a2 *= am;
+    const float b0 = n1 * a2 - n2 * a1, b1 = n2 * a0 - n0 * a2, b2 = n0 * a1 - n1 * a0;
+    float dx = mu * n0 + st * (cph * a0 + sp * b0);
+    float dy = mu * n1 + st * (cph * a1 + sp * b1);
+    float dz = mu * n2 + st * (cph * a2 + sp * b2);
+    const float dm = rsqrtf(fmaxf(dx * dx + dy * dy + dz * dz, 1e-30f));
+    T.ux = dx * dm; T.uy = dy * dm; T.uz = dz * dm;
+    const double4 fcm = C.cfP[k];
+    T.qx = static_cast<float>(fcm.x - C.mpx[nb]) * ENTRY32;
+    T.qy = static_cast<float>(fcm.y - C.mpy[nb]) * ENTRY32;
+    T.qz = static_cast<float>(fcm.z - C.mpz[nb]) * ENTRY32;
+    T.cell = nb;
+    T.i = nb;
+    return OUT_CONTINUE;
+}
+
 // Multigroup absorption opacity in FP32 from the cell's cached kT and
 // sigma0 / (kT)^q: at the group centre E_g^p comes from the per-group table.
 __device__ __forceinline__ float mg_absorption32(const Ctx &C, const Track32 &T, float nu) {
@@ -1336,8 +1513,10 @@ __device__ inline int segment32(const Ctx &C, Track32 &T, RNG &rng, TALLY &tal, 
     // problem only below the cell's PGRW group cutoff
     float Ro;
     if constexpr (POLY) {
-        Ro = 0.0f;   // only Random Walk cells (finite reach) need the distance to the faces
-        if (cp.z < CUDART_INF_F) {
+        // only Random Walk and DDMC cells (finite reach) need the distance to the faces
+        Ro = 0.0f;
+        const bool ddmcCell = DDMC && C.withDDMC && C.ddmc32[3 * static_cast<size_t>(cell)].x < CUDART_INF_F;
+        if (cp.z < CUDART_INF_F || ddmcCell) {
             Ro = FLT_MAX;
 #pragma unroll 4
             for (uint32_t k = C.cfo[cell]; k < C.cfo[cell + 1]; ++k) Ro = fminf(Ro, poly_dist32(C, k, T.qx, T.qy, T.qz));
@@ -1349,9 +1528,12 @@ __device__ inline int segment32(const Ctx &C, Track32 &T, RNG &rng, TALLY &tal, 
         usedRW = 1;
         return rw_jump32<MG, POLY>(C, T, rng, tal, cp, Ro, hx, hy, hz, err);
     }
-    if (!POLY && DDMC && C.withDDMC) {   // DDMC after a Random Walk that was not taken (:1723-1738)
+    if (DDMC && C.withDDMC) {   // DDMC after a Random Walk that was not taken (:1723-1738)
         const float4 da = C.ddmc32[3 * static_cast<size_t>(cell)];   // depth reach, 1/total, sigma_A f c, nu bound
-        if (Ro >= da.x && Ro > 0.0f && (!MG || T.nu < da.w)) return ddmc_jump32(C, T, rng, tal, da);
+        if (Ro >= da.x && Ro > 0.0f && (!MG || T.nu < da.w)) {
+            if constexpr (POLY) return ddmc_jump32_poly(C, T, rng, tal, da);
+            else return ddmc_jump32(C, T, rng, tal, da);
+        }
     }
     // gray: the cell constants; multigroup: the opacity at the particle's frequency
     float invSigE, sigAf, sigE = 0.0f, elastic = 0.0f;

@@ -490,9 +490,75 @@ __global__ void k_prestep(Ctx C, CellArrays A, OpacityEos M, double dt) {
 // FP32 form's per-cell copy holds the particle depth it needs, 1/total, the
 // absorption rate sigma_A f c, the PGRW frequency bound and the cumulative
 // face fractions.
+// precomputeDDMCData's second loop on a convex-polyhedral cell
+// (radiation/RadiationIMC.hpp:1355-1413): per cell-face slot, GetCellFaces
+// order, faces on the box excluded; the face distance from the face centroid
+// along the unit normal (the inward slot normal, the same up to its sign), or
+// half the distance to the neighbour's mesh point where that is zero.  The
+// FP32 form's header holds what the Cartesian one holds, with the last slot
+// that has a rate; the cumulative face fractions go per slot.
+__device__ inline void ddmc_rates_poly(const Ctx &C, const CellArrays &A, uint32_t c, const double4 &dd) {
+    const uint32_t k0 = C.cfo[c], k1 = C.cfo[c + 1];
+    double total = 0.0;
+    if (dd.z > 0.0) {
+        const double volume = A.vol[c];
+        const double D1 = dd.w;
+        const double mx = C.mpx[c], my = C.mpy[c], mz = C.mpz[c];
+        for (uint32_t k = k0; k < k1; ++k) {
+            double rate = 0.0;
+            const uint32_t nb = C.cfNext[k];
+            if (nb < C.ncells) {
+                const double4 n = C.cfN[k], q = C.cfP[k];
+                double faceDistance = fabs((q.x - mx) * n.x + (q.y - my) * n.y + (q.z - mz) * n.z);
+                if (!(faceDistance > 0.0))
+                    faceDistance = 0.5 * fabs((C.mpx[nb] - mx) * n.x + (C.mpy[nb] - my) * n.y + (C.mpz[nb] - mz) * n.z);
+                if (faceDistance > 0.0) {
+                    double diffusionFace = D1;
+                    const double D2 = C.ddmc[nb].w;
+                    if (D2 > 0.0)
+                        diffusionFace = (D1 > 0.0 && D2 > 0.0) ? (2.0 * D1 * D2 / (D1 + D2)) : (D1 < D2 ? D2 : D1);
+                    const double r = diffusionFace * C.cfA[k] / (volume * faceDistance);
+                    if (r > 0.0 && isfinite(r)) rate = r;
+                }
+            }
+            C.ddmcRate[k] = rate;
+            total += rate;
+        }
+    }
+    if (!(total > 0.0)) {
+        total = 0.0;
+        for (uint32_t k = k0; k < k1; ++k) C.ddmcRate[k] = 0.0;
+    }
+    C.ddmcTot[c] = total;
+    if (C.fp32) {
+        float4 *o32 = C.ddmc32 + static_cast<size_t>(c) * 3;
+        if (total > 0.0) {
+            double acc = 0.0;
+            int last = -1;
+            for (uint32_t k = k0; k < k1; ++k) {
+                acc += C.ddmcRate[k];
+                C.ddmcCum32[k] = static_cast<float>(acc / total);
+                if (C.ddmcRate[k] > 0.0) last = static_cast<int>(k - k0);
+            }
+            o32[0] = make_float4(static_cast<float>(C.ddmcMinParticle / dd.x), static_cast<float>(1.0 / total),
+                                 static_cast<float>(dd.y * A.fleck[c] * C.clight), CUDART_INF_F);
+            o32[1] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+            o32[2] = make_float4(0.0f, 0.0f, static_cast<float>(last), 0.0f);
+        } else {
+            o32[0] = make_float4(CUDART_INF_F, 0.0f, 0.0f, 0.0f);
+            o32[1] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+            o32[2] = make_float4(0.0f, 0.0f, -1.0f, 0.0f);
+        }
+    }
+}
+
 __global__ void k_ddmc_rates(Ctx C, CellArrays A) {
     for (uint32_t c = blockIdx.x * blockDim.x + threadIdx.x; c < C.ncells; c += gridDim.x * blockDim.x) {
         const double4 dd = C.ddmc[c];
+        if (C.poly) {
+            ddmc_rates_poly(C, A, c, dd);
+            continue;
+        }
         double rates[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
         double total = 0.0;
         uint32_t i, j, k;
@@ -943,18 +1009,37 @@ __device__ __forceinline__ void repair_outside(const Ctx &C, double &x, double &
 // packets e in [eBegin, eBegin + count) (a particle shard's range; the whole
 // step's packets unsharded): packet e goes to bank slot bankBase + (e - eBegin)
 // with pid pidBase + e.
+// The cell of emitted packet e: the last cell whose offset is <= e (offsets
+// has ncells + 1 entries, offsets[ncells] the total).  The lanes of a warp
+// hold consecutive packets: the first active lane searches, the others walk
+// forward from its cell over the few cells their packets are in (a lane that
+// meets a long run of cells without packets searches the rest).
+__device__ __forceinline__ uint32_t last_offset_at_most(const uint64_t *offsets, uint32_t lo, uint32_t hi, uint64_t e) {
+    while (lo < hi) {   // the first index in [lo, hi) whose offset exceeds e
+        const uint32_t mid = (lo + hi) >> 1;
+        if (offsets[mid] <= e) lo = mid + 1; else hi = mid;
+    }
+    return lo - 1;
+}
+__device__ __forceinline__ uint32_t emission_cell(const uint64_t *offsets, uint32_t ncells, uint64_t e) {
+    const unsigned m = __activemask();
+    const int leader = __ffs(m) - 1;
+    uint32_t c = 0;
+    if (static_cast<int>(threadIdx.x & 31) == leader) c = last_offset_at_most(offsets, 0, ncells, e);
+    c = __shfl_sync(m, c, leader);   // the leader's packet is the warp's first, so its cell is at or below ours
+    for (int walk = 0; c + 1 < ncells && offsets[c + 1] <= e; ++walk) {
+        if (walk == 32) return last_offset_at_most(offsets, c + 1, ncells, e);
+        ++c;
+    }
+    return c;
+}
+
 __global__ void k_emit_cells(Ctx C, CellArrays A, const uint64_t *offsets, uint64_t eBegin, uint64_t count, Bank b,
                              uint32_t bankBase, uint32_t pidBase, double dt, DevStats *st) {
     double esum = 0.0;
     for (uint64_t j = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; j < count; j += (uint64_t)gridDim.x * blockDim.x) {
         const uint64_t e = eBegin + j;
-        // last cell whose offset <= e
-        uint32_t lo = 0, hi = C.ncells;   // offsets has ncells + 1 entries
-        while (lo < hi) {
-            uint32_t mid = (lo + hi) >> 1;
-            if (offsets[mid] <= e) lo = mid + 1; else hi = mid;
-        }
-        const uint32_t c = lo - 1;
+        const uint32_t c = emission_cell(offsets, C.ncells, e);
         const uint64_t np = A.photons[c];
         const double energyPerPhoton = A.emitE[c] * 1.0 / static_cast<double>(np);
         PhiloxRng rng;
@@ -1007,12 +1092,7 @@ __global__ void k_emit_cells32(Ctx C, CellArrays A, const uint64_t *offsets, uin
     double esum = 0.0;
     for (uint64_t j = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; j < count; j += (uint64_t)gridDim.x * blockDim.x) {
         const uint64_t e = eBegin + j;
-        uint32_t lo = 0, hi = C.ncells;   // last cell whose offset <= e
-        while (lo < hi) {
-            uint32_t mid = (lo + hi) >> 1;
-            if (offsets[mid] <= e) lo = mid + 1; else hi = mid;
-        }
-        const uint32_t c = lo - 1;
+        const uint32_t c = emission_cell(offsets, C.ncells, e);
         const uint64_t np = A.photons[c];
         const double energyPerPhoton = A.emitE[c] * 1.0 / static_cast<double>(np);
         PhiloxRng rng;

@@ -62,6 +62,8 @@ struct StormHandle {
     double *ddmcTot = nullptr, *ddmcRate = nullptr;
     uint32_t *ddmcCut = nullptr;
     float4 *ddmc32 = nullptr;
+    float *ddmcCum32 = nullptr;  // polyhedral FP32 form: cumulative leak fraction per cell-face slot
+    double *cfA = nullptr;       // polyhedral mesh: face area per cell-face slot
     // convex-polyhedral mesh
     uint32_t *cfo = nullptr, *cfNext = nullptr, *cfFace = nullptr, *fvo = nullptr, *fvi = nullptr;
     double4 *cfN = nullptr, *cfP = nullptr;
@@ -867,8 +869,8 @@ int storm_cuda_create(const StormProblemDesc *d, StormHandle **out) {
         }
         for (uint32_t q = 0; q < mesh->face_vertex_offset[mesh->nfaces]; ++q)
             if (mesh->face_vertices[q] >= mesh->nvertices) return STORM_ERR_INVALID_ARG;
-        // DDMC is Cartesian only
-        if (d->with_ddmc) return STORM_ERR_UNSUPPORTED;
+        // the polyhedral kernels are gray: no multigroup opacity
+        if (mg) return STORM_ERR_UNSUPPORTED;
     } else {
         for (int a = 0; a < 3; ++a) {
             const double *e = a == 0 ? d->x_edges : (a == 1 ? d->y_edges : d->z_edges);
@@ -970,6 +972,7 @@ int storm_cuda_create(const StormProblemDesc *d, StormHandle **out) {
         // normal turned toward the cell's mesh point, normalised, and the face centroid
         const uint32_t K = mesh->cell_face_offset[N];
         std::vector<double4> nrm(K), cm(K);
+        std::vector<double> area(K);
         std::vector<uint32_t> nextv(K), facev(K);
         std::vector<double> chord(N), mp[3];
         for (int a = 0; a < 3; ++a) mp[a].resize(N);
@@ -986,6 +989,7 @@ int storm_cuda_create(const StormProblemDesc *d, StormHandle **out) {
                 if (len > 0) { nx = nx / len; ny = ny / len; nz = nz / len; }
                 nrm[q] = make_double4(nx, ny, nz, 0.0);
                 cm[q] = make_double4(fx, fy, fz, 0.0);
+                area[q] = mesh->face_area[f];
                 const uint32_t a0 = mesh->face_cells[2 * f], a1 = mesh->face_cells[2 * f + 1];
                 nextv[q] = (a0 == c) ? a1 : a0;
                 facev[q] = f;
@@ -1009,6 +1013,8 @@ int storm_cuda_create(const StormProblemDesc *d, StormHandle **out) {
         ALLOC(h->fvo, mesh->nfaces + 1); ALLOC(h->fvi, FV); ALLOC(h->vtx, 3 * static_cast<size_t>(NV));
         H2D(h->cfo, mesh->cell_face_offset, N + 1);
         H2D(h->cfN, nrm.data(), K); H2D(h->cfP, cm.data(), K); H2D(h->cfNext, nextv.data(), K); H2D(h->cfFace, facev.data(), K);
+        ALLOC(h->cfA, K);
+        H2D(h->cfA, area.data(), K);
         H2D(h->mpx, mp[0].data(), N); H2D(h->mpy, mp[1].data(), N); H2D(h->mpz, mp[2].data(), N);
         H2D(h->chord, chord.data(), N);
         H2D(h->fvo, mesh->face_vertex_offset, mesh->nfaces + 1);
@@ -1110,7 +1116,7 @@ int storm_cuda_create(const StormProblemDesc *d, StormHandle **out) {
     C.nx = h->nx; C.ny = h->ny; C.nz = h->nz; C.ncells = N;
     if (poly) {
         C.poly = 1;
-        C.cfo = h->cfo; C.cfN = h->cfN; C.cfP = h->cfP; C.cfNext = h->cfNext; C.cfFace = h->cfFace;
+        C.cfo = h->cfo; C.cfN = h->cfN; C.cfP = h->cfP; C.cfNext = h->cfNext; C.cfFace = h->cfFace; C.cfA = h->cfA;
         C.mpx = h->mpx; C.mpy = h->mpy; C.mpz = h->mpz;
         C.fvo = h->fvo; C.fvi = h->fvi; C.vtx = h->vtx; C.chord = h->chord; C.cfN32 = h->cfN32;
     }
@@ -1202,11 +1208,15 @@ int storm_cuda_create(const StormProblemDesc *d, StormHandle **out) {
         C.ddmcMinCell = d->ddmc_min_cell_optical_depth;
         ALLOC(h->ddmc, N);
         ALLOC(h->ddmcTot, N);
-        ALLOC(h->ddmcRate, 6 * static_cast<size_t>(N));
+        // rates per face: 6 per Cartesian cell, one per cell-face slot on a polyhedral mesh
+        const size_t rateSlots = poly ? static_cast<size_t>(mesh->cell_face_offset[N]) : 6 * static_cast<size_t>(N);
+        ALLOC(h->ddmcRate, rateSlots);
         if (C.ddmcPgrw) ALLOC(h->ddmcCut, N);
         if (h->fp32) ALLOC(h->ddmc32, 3 * static_cast<size_t>(N));
+        if (h->fp32 && poly) ALLOC(h->ddmcCum32, rateSlots);
         C.ddmc = h->ddmc; C.ddmcTot = h->ddmcTot; C.ddmcRate = h->ddmcRate; C.ddmcCut = h->ddmcCut;
         C.ddmc32 = h->ddmc32;
+        C.ddmcCum32 = h->ddmcCum32;
     }
     C.rwDiffPerReach = C.rwMinParticle > 0.0 ? static_cast<float>(C.clight / (3.0 * C.rwMinParticle)) : 0.0f;
     C.seedLo = static_cast<uint32_t>(d->seed);
@@ -1255,7 +1265,7 @@ int storm_cuda_destroy(StormHandle *h) {
                   h->runCursor, h->runScan, h->longRuns, h->bucketFlags,
                   h->cfo, h->cfN, h->cfP, h->cfNext, h->cfFace, h->mpx, h->mpy, h->mpz, h->fvo, h->fvi, h->vtx,
                   h->chord, h->cfN32, h->dep, h->xbuf, h->shardWc, h->shardRunW, h->shardStart, h->shardBounds,
-                  h->vel, h->mom};
+                  h->vel, h->mom, h->ddmcCum32, h->cfA};
     for (void *p : ps) device_pool().free(p);
     cudaEvent_t evs[] = {h->evStart, h->evTransport0, h->evTransport1, h->evEnd, h->evAfterEmit, h->evAfterComb};
     bool complete = h->stream != nullptr;

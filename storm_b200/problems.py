@@ -507,6 +507,22 @@ def ddmc_cube(n=8, new_photons_per_cell=3, face_packets=40, comb_nmin=20, seed=4
     return p
 
 
+def voronoi_ddmc(ncells=300, packets_per_step=3e4, seed=23, dt=2e-10, precision=A.PRECISION_FP64, mesh=None,
+                 sigma_s_thick=500.0, with_random_walk=False):
+    """DDMC-style leakage (withDDMC, depths 15 and 5) on a Voronoi mesh: the
+    cells of voronoi_cube with sigma_a = 1 everywhere and an elastic opacity
+    sigma_s_thick in the cells whose generators lie at x >= 0.5, which makes
+    them DDMC eligible; cell emission only, vacuum on the box."""
+    p = voronoi_cube(ncells=ncells, packets_per_step=packets_per_step, seed=seed, dt=dt, precision=precision,
+                     with_random_walk=with_random_walk, mesh=mesh)
+    thick = p.mesh.points[:, 0] >= 0.5
+    p.sigma_a = np.ones(p.ncells)
+    p.sigma_s = np.where(thick, sigma_s_thick, 0.0)
+    p.with_ddmc = True
+    p.name = "voronoi_ddmc"
+    return p
+
+
 def strat_cube(n=4, groups=30, bins=6, comb_nmin=4, comb_factor=2.0, min_per_bin=2, new_photons_per_cell=6, seed=42,
                precision=A.PRECISION_FP64):
     """A small multigroup cube whose population control is

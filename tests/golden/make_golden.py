@@ -24,13 +24,16 @@ Fixtures (numpy .npz):
   replay_ddmc_mg.npz  a 64-group cube with DDMC in its multigroup PGRW form
   replay_voronoi.npz  recorded calls on a 300-cell Voronoi mesh (Random Walk on), with
                       the mesh arrays (mesh_*)
+  replay_voronoi_ddmc.npz  recorded calls on a 300-cell Voronoi mesh with DDMC leakage
+                      in its scattering half (problems.voronoi_ddmc), with the mesh
+                      arrays and the step's starting temperatures
   replay_hydro.npz    recorded calls on an 8^3 step cube (Random Walk, elastic
                       scattering in the thin half) whose cells move at up to 5 % of c
                       (withHydro), with the velocities and each segment's momentum deposit
   replay_hydro_mg.npz the same for a 64-group cube with PGRW
 
     python tests/golden/make_golden.py ddmc     # only the DDMC fixtures
-    python tests/golden/make_golden.py voronoi  # only the Voronoi fixture
+    python tests/golden/make_golden.py voronoi  # only the Voronoi fixtures
     python tests/golden/make_golden.py hydro    # only the moving-material fixtures
 """
 import os
@@ -206,15 +209,24 @@ def make_voronoi():
     np.savez_compressed(os.path.join(HERE, "replay_voronoi.npz"), **out)
 
 
+def make_voronoi_ddmc():
+    p = problems.voronoi_ddmc()
+    out = record(p, 1, 400000, 1500)
+    out.update({"mesh_" + k: getattr(p.mesh, k) for k in MESH_FIELDS})
+    np.savez_compressed(os.path.join(HERE, "replay_voronoi_ddmc.npz"), **out)
+
+
 if __name__ == "__main__":
     if sys.argv[1:] == ["ddmc"]:
         make_ddmc()
     elif sys.argv[1:] == ["voronoi"]:
         make_voronoi()
+        make_voronoi_ddmc()
     elif sys.argv[1:] == ["hydro"]:
         make_hydro()
     else:
         main()
         make_ddmc()
         make_voronoi()
+        make_voronoi_ddmc()
         make_hydro()

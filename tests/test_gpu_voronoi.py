@@ -10,6 +10,9 @@ reference built on the same mesh (the grid stand-in's polyhedral mode).
   mean position at the cell's centroid within the sampling error).
 * Whole steps conserve energy and agree with the reference's serial path
   within the seed-to-seed scatter.
+* DDMC-style leakage on polyhedral cells: recorded reference segments
+  (tests/golden/replay_voronoi_ddmc.npz) replay, and whole steps agree with
+  the reference and between the two forms.
 """
 import numpy as np
 import pytest
@@ -199,3 +202,54 @@ def test_voronoi_face_source_matches_reference(ref_lib):
     prob32 = lambda s: _face_source_problem(mesh, s, A.PRECISION_FP32_TRACK)   # noqa: E731
     assert_agree(run_batch(Engine, prob32, range(120, 136), 4), run_batch(Engine, prob, range(160, 176), 4),
                  "Voronoi 300 cells with an x-low face source: FP32 vs FP64")
+
+
+def _ddmc_problem(mesh, seed, precision=None):
+    from storm_b200 import _abi as A
+    p = problems.voronoi_ddmc(ncells=mesh.ncells, packets_per_step=2e4, mesh=mesh,
+                              precision=A.PRECISION_FP64 if precision is None else precision)
+    p.seed = seed
+    return p
+
+
+def test_voronoi_ddmc_replay_matches_reference(oracle_lib):
+    """DDMC on polyhedral cells (radiation/RadiationIMC.hpp:1282-1612):
+    recorded reference segments on a 300-cell Voronoi mesh whose scattering
+    half is DDMC eligible (tests/golden/replay_voronoi_ddmc.npz) replay with
+    the same event, destination cell and draw count, the same DDMC choice, and
+    positions (the leak face's centroid), directions (the cosine law about the
+    face normal turned toward the neighbour), weights and tallies to the
+    replay tolerances."""
+    g = golden("replay_voronoi_ddmc.npz")
+    mesh = _fixture_mesh(g)
+    p = problems.voronoi_ddmc(mesh=mesh)
+    e = Engine(p)
+    e.set_cell_state(g["T_start"], None, None)
+    e.phase("prestep", p.dt)
+    b = oracle_lib.ReplayBatch(g["before"], g["cell"], g["tape_offset"], g["tape_length"], g["tape"])
+    e.replay(b)
+    _check_replay(b, g, p.ncells, time_rel=1e-13)
+    np.testing.assert_array_equal(b["used_random_walk"], g["used_rw"])
+    ddmc = g["used_rw"] == 2
+    leaks = ddmc & (g["status"] == 1)
+    assert leaks.sum() > 500 and (ddmc & (g["status"] == 2)).sum() > 200
+    assert len(set(g["next"][leaks].tolist())) > 50   # leaks into many different neighbours
+    e.close()
+
+
+def test_voronoi_ddmc_steps_agree_with_reference(ref_lib):
+    """Whole steps with DDMC on a Voronoi mesh: energy conserved per step in
+    both forms; the engine against the reference's serial path and the FP32
+    form against the FP64 form under the batch gate."""
+    from storm_b200 import _abi as A
+    from batchcheck import assert_agree, run_batch
+    mesh = build_voronoi(np.random.default_rng(12).random((300, 3)) * 0.98 + 0.01)
+
+    def check(m, st):
+        if isinstance(m, Engine):
+            assert _balance(st) < 1e-10
+    fp64 = run_batch(Engine, lambda s: _ddmc_problem(mesh, s), range(20, 36), 4, check)
+    assert_agree(fp64, run_batch(ref_lib.Reference, lambda s: _ddmc_problem(mesh, s), range(60, 76), 4),
+                 "Voronoi DDMC 300 cells: engine vs reference")
+    assert_agree(run_batch(Engine, lambda s: _ddmc_problem(mesh, s, A.PRECISION_FP32_TRACK), range(40, 56), 4, check),
+                 fp64, "Voronoi DDMC 300 cells: FP32 vs FP64")
