@@ -621,7 +621,24 @@ struct RwHostTables {
 struct RwDeviceTables {
     double *tau = nullptr, *logTau = nullptr, *surv = nullptr, *radius = nullptr;
     float *logTau32 = nullptr, *surv32 = nullptr, *radius32 = nullptr;
+    uint16_t *leakStart = nullptr, *leakStart32 = nullptr;
 };
+// Per bucket b of the survival value, [b, b + 1) / RW_LEAK_BUCKETS: the number
+// of table entries above (b + 1) / RW_LEAK_BUCKETS, from which the samplers
+// walk forward (the table is non-increasing).  `T` is double for the FP64
+// form's table and float for the FP32 copy (the same rounding as the device's).
+template <class T>
+std::vector<uint16_t> leak_buckets(const std::vector<double> &surv) {
+    std::vector<uint16_t> start(RW_LEAK_BUCKETS);
+    uint32_t above = 0;
+    for (int b = RW_LEAK_BUCKETS - 1; b >= 0; --b) {
+        const T top = static_cast<T>(b + 1) / static_cast<T>(RW_LEAK_BUCKETS);
+        above = 0;
+        while (above < static_cast<uint32_t>(RW_TABLE) && static_cast<T>(surv[above]) > top) ++above;
+        start[b] = static_cast<uint16_t>(above);
+    }
+    return start;
+}
 std::mutex &rw_tables_mutex() {
     static std::mutex m;
     return m;
@@ -650,6 +667,15 @@ int build_rw_tables(StormHandle *h) {
         CK(cudaMemcpyAsync(t.tau, host.tau.data(), RW_TABLE * sizeof(double), cudaMemcpyHostToDevice, h->stream));
         CK(cudaMemcpyAsync(t.logTau, host.ltau.data(), RW_TABLE * sizeof(double), cudaMemcpyHostToDevice, h->stream));
         CK(cudaMemcpyAsync(t.surv, host.surv.data(), RW_TABLE * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+        {
+            static const std::vector<uint16_t> ls = leak_buckets<double>(host.surv), ls32 = leak_buckets<float>(host.surv);
+            CK(cudaMalloc(&t.leakStart, RW_LEAK_BUCKETS * sizeof(uint16_t)));
+            CK(cudaMalloc(&t.leakStart32, RW_LEAK_BUCKETS * sizeof(uint16_t)));
+            CK(cudaMemcpyAsync(t.leakStart, ls.data(), RW_LEAK_BUCKETS * sizeof(uint16_t), cudaMemcpyHostToDevice,
+                               h->stream));
+            CK(cudaMemcpyAsync(t.leakStart32, ls32.data(), RW_LEAK_BUCKETS * sizeof(uint16_t), cudaMemcpyHostToDevice,
+                               h->stream));
+        }
         launch_rw_radius(h->stream, t.tau, t.surv, t.radius);
         launch_to_float(h->stream, t.logTau, t.logTau32, RW_TABLE);
         launch_to_float(h->stream, t.surv, t.surv32, RW_TABLE);
@@ -668,10 +694,12 @@ int build_rw_tables(StormHandle *h) {
     h->C.rw.logTau = t.logTau;
     h->C.rw.surv = t.surv;
     h->C.rw.radius = t.radius;
+    h->C.rw.leakStart = t.leakStart;
     if (h->fp32) {
         h->C.rw.logTau32 = t.logTau32;
         h->C.rw.surv32 = t.surv32;
         h->C.rw.radius32 = t.radius32;
+        h->C.rw.leakStart32 = t.leakStart32;
     }
     h->C.rw.logMin = logMin;
     h->C.rw.logMax = logMax;
