@@ -1300,7 +1300,9 @@ __device__ __forceinline__ void block_stats_flush(const BlockStats &bs, DevStats
 // coordinates, the reference's arithmetic) and the FP32-tracking form.
 // Form64T<0> is the gray FP64 form without DDMC on a Cartesian grid;
 // Form64T<1> adds the multigroup and DDMC branches; Form64T<2> runs on a
-// convex-polyhedral mesh.
+// convex-polyhedral mesh; Form64T<4> is Form64T<1> without the DDMC branch
+// (multigroup problems without withDDMC: less code for the instruction cache,
+// whose misses bound the multigroup kernels).
 template <int V>
 struct Form64T {
     using T = Track;
@@ -1332,6 +1334,7 @@ using Form64 = Form64T<0>;
 using Form64Full = Form64T<1>;
 using Form64Poly = Form64T<2>;
 using Form64Hydro = Form64T<3>;   // Form64Full with moving material
+using Form64MG = Form64T<4>;      // Form64Full without the DDMC branch
 template <bool POLY, bool DDMC = true>
 struct Form32T {
     using T = Track32;
@@ -3132,6 +3135,7 @@ void launch_transport_refill(cudaStream_t s, uint32_t grid, int minBlocks, const
     else if (C.fp32) refill_launch<Form32Lean>(s, grid, minBlocks, C, in, n, nextIdx, cen, nCen, burst, maxSegs, st);
     else if (C.poly) refill_launch<Form64Poly>(s, grid, minBlocks, C, in, n, nextIdx, cen, nCen, burst, maxSegs, st);
     else if (C.withHydro) refill_launch<Form64Hydro>(s, grid, minBlocks, C, in, n, nextIdx, cen, nCen, burst, maxSegs, st);
+    else if (C.groups >= 2 && !C.withDDMC) refill_launch<Form64MG>(s, grid, minBlocks, C, in, n, nextIdx, cen, nCen, burst, maxSegs, st);
     else if (C.groups >= 2 || C.withDDMC) refill_launch<Form64Full>(s, grid, minBlocks, C, in, n, nextIdx, cen, nCen, burst, maxSegs, st);
     else refill_launch<Form64>(s, grid, minBlocks, C, in, n, nextIdx, cen, nCen, burst, maxSegs, st);
 }
