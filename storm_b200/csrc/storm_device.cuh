@@ -1340,14 +1340,10 @@ __device__ inline int rw_jump32(const Ctx &C, Track32 &T, RNG &rng, TALLY &tal, 
         const uint32_t cutoff = C.pgrwCut[cell];
         const double *cdf = C.mgCdf + static_cast<size_t>(cell) * (C.groups + 1);
         const double cdfAtCutoff = cdf[cutoff], cdfTotal = cdf[C.groups];
-        double nu;
-        if (cdfTotal > cdfAtCutoff) {
-            const double lo = cdfAtCutoff / cdfTotal;
-            nu = mg_thermal_energy(C, cell, lo + static_cast<double>(rng.rawf()) * (1.0 - lo));
-        } else {
-            nu = nextafter(C.gb[cutoff], DBL_MAX);
-        }
-        T.nu = static_cast<float>(mg_clamp(C, nu));
+        if (cdfTotal > cdfAtCutoff)   // sampled at the start of the next segment (segment32)
+            T.nu = -1.0f - static_cast<float>(cdfAtCutoff / cdfTotal);
+        else
+            T.nu = static_cast<float>(mg_clamp(C, nextafter(C.gb[cutoff], DBL_MAX)));
     }
     return ev == 1 ? OUT_CENSUS : OUT_CONTINUE;
 }
@@ -1523,7 +1519,19 @@ __device__ inline int segment32(const Ctx &C, Track32 &T, RNG &rng, TALLY &tal, 
     }
     const float hx = T.hx, hy = T.hy, hz = T.hz;
     const float4 cp = T.cp;
-    if (MG) T.nu = fminf(fmaxf(T.nu, C.gb32[0]), C.gb32[C.groups]);   // clampFrequencyToBounds
+    if (MG) {
+        // A re-emission from the cell's spectrum that the previous segment
+        // (an effective scatter, or a PGRW upscatter that draws above the
+        // cutoff's cumulative fraction lo) left pending as nu = -(1 + lo): it
+        // is sampled here, so that the kernel holds one copy of the sampler.
+        if (T.nu < 0.0f) {
+            const double lo = static_cast<double>(-T.nu - 1.0f);
+            const double nu = mg_thermal_energy(C, cell, lo + static_cast<double>(rng.rawf()) * (1.0 - lo));
+            if (nu < 0.0) { err = STORM_DERR_MG_SAMPLE; return OUT_ERROR; }
+            T.nu = static_cast<float>(nu);
+        }
+        T.nu = fminf(fmaxf(T.nu, C.gb32[0]), C.gb32[C.groups]);   // clampFrequencyToBounds
+    }
 
     // Random Walk only where the particle is at least cp.z = rwMinParticleOpticalDepth / sigma_T
     // from every face (cp.z is inf in cells that are not eligible); in a multigroup
@@ -1638,11 +1646,7 @@ __device__ inline int segment32(const Ctx &C, Track32 &T, RNG &rng, TALLY &tal, 
         float st, ct;
         __sincosf(theta, &st, &ct);
         T.ux = sinT * ct; T.uy = sinT * st; T.uz = cosT;
-        if (MG && effective) {   // re-emission from the cell's spectrum
-            const double nu = mg_thermal_energy(C, cell, static_cast<double>(rng.rawf()));
-            if (nu < 0.0) { err = STORM_DERR_MG_SAMPLE; return OUT_ERROR; }
-            T.nu = static_cast<float>(nu);
-        }
+        if (MG && effective) T.nu = -1.0f;   // re-emission from the cell's spectrum, at the next segment's start
         return OUT_CONTINUE;
     }
     // face crossing
