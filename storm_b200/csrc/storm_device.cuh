@@ -998,8 +998,10 @@ __device__ __forceinline__ void track_begin(const Ctx &C, Track &T) {
 template <int V, class RNG, class TALLY>
 __device__ inline PhysOut physics_step(const Ctx &C, Track &T, RNG &rng, TALLY &tal) {
     // V: 0 gray Cartesian, 1 + multigroup and DDMC, 2 polyhedral, 3 = 1 + moving material,
-    // 4 = 1 without the DDMC branch (a smaller kernel for the instruction cache)
-    constexpr bool FULL = V == 1 || V == 3 || V == 4, POLY = V == 2, HYDRO = V == 3, DDMC = V != 4;
+    // 4 = 1 without the DDMC branch, 5 = 2 with DDMC (the variants without a
+    // branch are smaller kernels for the instruction cache)
+    constexpr bool FULL = V == 1 || V == 3 || V == 4, POLY = V == 2 || V == 5, HYDRO = V == 3,
+                   DDMC = V == 1 || V == 3 || V == 5;
     PartReg &p = T.p;
     PhysOut o;
     o.status = NO_CELL_MOVE;

@@ -1300,9 +1300,10 @@ __device__ __forceinline__ void block_stats_flush(const BlockStats &bs, DevStats
 // coordinates, the reference's arithmetic) and the FP32-tracking form.
 // Form64T<0> is the gray FP64 form without DDMC on a Cartesian grid;
 // Form64T<1> adds the multigroup and DDMC branches; Form64T<2> runs on a
-// convex-polyhedral mesh; Form64T<4> is Form64T<1> without the DDMC branch
-// (multigroup problems without withDDMC: less code for the instruction cache,
-// whose misses bound the multigroup kernels).
+// convex-polyhedral mesh and Form64T<5> is it with the DDMC branch;
+// Form64T<4> is Form64T<1> without the DDMC branch.  Problems without
+// withDDMC run the variants without it: less code for the instruction cache,
+// whose misses bound the multigroup and polyhedral kernels.
 template <int V>
 struct Form64T {
     using T = Track;
@@ -1323,7 +1324,7 @@ struct Form64T {
         PhysOut o = physics_step<V>(C, t, rng, tal);
         if (o.errCode) { err = o.errCode; return OUT_ERROR; }
         usedRW = o.usedRW == 1;   // Random Walk jumps (2 marks a DDMC step)
-        int m = manager_handle<V == 2>(C, t, o);
+        int m = manager_handle<V == 2 || V == 5>(C, t, o);
         if (m == OUT_ERROR) err = STORM_DERR_NOT_ON_BOUNDARY;
         return m;
     }
@@ -1333,6 +1334,7 @@ struct Form64T {
 using Form64 = Form64T<0>;
 using Form64Full = Form64T<1>;
 using Form64Poly = Form64T<2>;
+using Form64PolyDDMC = Form64T<5>;   // Form64Poly with the DDMC branch
 using Form64Hydro = Form64T<3>;   // Form64Full with moving material
 using Form64MG = Form64T<4>;      // Form64Full without the DDMC branch
 template <bool POLY, bool DDMC = true>
@@ -1362,7 +1364,8 @@ struct Form32T {
 };
 using Form32 = Form32T<false>;
 using Form32Lean = Form32T<false, false>;   // without the DDMC branch
-using Form32Poly = Form32T<true>;
+using Form32Poly = Form32T<true, false>;   // without the DDMC branch
+using Form32PolyDDMC = Form32T<true, true>;
 // The FP32-tracking form of a multigroup problem: the frequency rides along.
 template <bool DDMC = true>
 struct Form32MGT {
@@ -2785,7 +2788,7 @@ __global__ void k_replay(Ctx C, ReplayDev R, uint32_t n) {
         track_begin(C, T);
         TapeRng rng{R.tape + R.tapeOffset[q], R.tapeLength[q], 0, false};
         LocalTally tal{0.0, 0.0, 0.0, 0.0, 0.0};
-        PhysOut o = C.poly ? physics_step<2>(C, T, rng, tal)
+        PhysOut o = C.poly ? (C.withDDMC ? physics_step<5>(C, T, rng, tal) : physics_step<2>(C, T, rng, tal))
                            : (C.withHydro ? physics_step<3>(C, T, rng, tal) : physics_step<1>(C, T, rng, tal));
         R.phys[0][q] = p.x; R.phys[1][q] = p.y; R.phys[2][q] = p.z;
         R.phys[3][q] = p.vx; R.phys[4][q] = p.vy; R.phys[5][q] = p.vz;
@@ -3128,11 +3131,13 @@ static void refill_launch(cudaStream_t s, uint32_t grid, int minBlocks, const Ct
 void launch_transport_refill(cudaStream_t s, uint32_t grid, int minBlocks, const Ctx &C, const Bank &in, uint32_t n,
                              uint32_t *nextIdx, const CensusBank &cen, uint32_t *nCen, uint32_t burst, uint32_t maxSegs,
                              DevStats *st) {
-    if (C.fp32 && C.poly) refill_launch<Form32Poly>(s, grid, minBlocks, C, in, n, nextIdx, cen, nCen, burst, maxSegs, st);
+    if (C.fp32 && C.poly && C.withDDMC) refill_launch<Form32PolyDDMC>(s, grid, minBlocks, C, in, n, nextIdx, cen, nCen, burst, maxSegs, st);
+    else if (C.fp32 && C.poly) refill_launch<Form32Poly>(s, grid, minBlocks, C, in, n, nextIdx, cen, nCen, burst, maxSegs, st);
     else if (C.fp32 && C.groups >= 2 && C.withDDMC) refill_launch<Form32MG>(s, grid, minBlocks, C, in, n, nextIdx, cen, nCen, burst, maxSegs, st);
     else if (C.fp32 && C.groups >= 2) refill_launch<Form32MGLean>(s, grid, minBlocks, C, in, n, nextIdx, cen, nCen, burst, maxSegs, st);
     else if (C.fp32 && C.withDDMC) refill_launch<Form32>(s, grid, minBlocks, C, in, n, nextIdx, cen, nCen, burst, maxSegs, st);
     else if (C.fp32) refill_launch<Form32Lean>(s, grid, minBlocks, C, in, n, nextIdx, cen, nCen, burst, maxSegs, st);
+    else if (C.poly && C.withDDMC) refill_launch<Form64PolyDDMC>(s, grid, minBlocks, C, in, n, nextIdx, cen, nCen, burst, maxSegs, st);
     else if (C.poly) refill_launch<Form64Poly>(s, grid, minBlocks, C, in, n, nextIdx, cen, nCen, burst, maxSegs, st);
     else if (C.withHydro) refill_launch<Form64Hydro>(s, grid, minBlocks, C, in, n, nextIdx, cen, nCen, burst, maxSegs, st);
     else if (C.groups >= 2 && !C.withDDMC) refill_launch<Form64MG>(s, grid, minBlocks, C, in, n, nextIdx, cen, nCen, burst, maxSegs, st);
