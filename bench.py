@@ -354,20 +354,21 @@ def e2e_run(args, eng, p, dist):
     buf = Particles.pinned(max(2 * n, 1))
     pin_T = torch.empty(p.ncells, dtype=torch.float64, pin_memory=True).numpy()
     host = eng.census(out=buf)
-    rec = 9 * 8 + 4
+    rec_in = 7 * 8 + 4    # position, direction, weight, cell: the step sets time left and initial weight
+    rec_out = 9 * 8 + 4
     torch.cuda.synchronize()
     barrier(dist, "storm")
     t0 = time.perf_counter()
     segs, h2d, d2h = 0, 0, 0
     for _ in range(args.e2e_steps):
-        eng.set_census(host)
-        h2d += host.n * rec
+        eng.set_census(host, step_fields=False)
+        h2d += host.n * rec_in
         st = eng.step()
         segs += st["segments"]
         if eng.census_count() > buf.n:
             break
         host = eng.census(out=buf)
-        d2h += host.n * rec
+        d2h += host.n * rec_out
         eng.temperature(out=pin_T)
         d2h += p.ncells * 8
     torch.cuda.synchronize()
@@ -379,7 +380,8 @@ def e2e_run(args, eng, p, dist):
     return {"value": allsegs / wall, "unit": UNIT, "h2d_bytes_per_step": int(h2d / steps),
             "d2h_bytes_per_step": int(d2h / steps), "steps": args.e2e_steps,
             "ms_per_step": wall / steps * 1e3, "link": link, "copy_ms_per_step_at_link_rate": floor_ms,
-            "note": "census in and out through storm_cuda_set_census / storm_cuda_step / storm_cuda_get_census, "
+            "note": "census in (without time left and initial weight, which the step sets) and out through "
+                    "storm_cuda_set_census / storm_cuda_step / storm_cuda_get_census, "
                     "temperatures through storm_cuda_get_cell_arrays; page-locked host buffers; copies and "
                     "host-side checks inside the timed region (wall clock); link = one 1 GiB page-locked copy "
                     "each way, CUDA-event timed"}

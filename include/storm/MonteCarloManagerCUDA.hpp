@@ -600,18 +600,20 @@ private:
                 eo.addEntry("Particle id", p.id);
                 throw eo;
             }
-        std::vector<double> x(n), y(n), z(n), vx(n), vy(n), vz(n), t(n), w(n), w0(n), nu(multigroup_ ? n : 0);
+        // timeLeft and initialWeight are not copied: step() sets them for every
+        // census particle (manager/MonteCarloManagerSerial.hpp:391-405)
+        std::vector<double> x(n), y(n), z(n), vx(n), vy(n), vz(n), w(n), nu(multigroup_ ? n : 0);
         std::vector<std::uint32_t> cell(n);
         for (std::size_t q = 0; q < n; ++q) {
             const MCParticle &p = ps[q];
             x[q] = p.location.x; y[q] = p.location.y; z[q] = p.location.z;
             vx[q] = p.velocity.x; vy[q] = p.velocity.y; vz[q] = p.velocity.z;
-            t[q] = p.timeLeft; w[q] = p.weight; w0[q] = p.initialWeight;
+            w[q] = p.weight;
             cell[q] = static_cast<std::uint32_t>(p.cellIndex);
             if (multigroup_) nu[q] = p.frequency;
         }
-        StormParticlesSoA s{x.data(), y.data(), z.data(), vx.data(), vy.data(), vz.data(), t.data(), w.data(),
-                            w0.data(), cell.data(), nullptr, n, multigroup_ ? nu.data() : nullptr};
+        StormParticlesSoA s{x.data(), y.data(), z.data(), vx.data(), vy.data(), vz.data(), nullptr, w.data(),
+                            nullptr, cell.data(), nullptr, n, multigroup_ ? nu.data() : nullptr};
         cuda_detail::check(storm_cuda_set_census(h_, &s), h_, "set_census");
     }
 

@@ -384,7 +384,10 @@ int storm_cuda_phase_stats(StormHandle *h, StormStepStats *stats);
 /* ---------------------------------------------------------------- state in/out */
 
 /* Replace the census with host particles (the std::vector<Particle>&& argument
- * of step()).  Copies host -> device. */
+ * of step()).  Copies host -> device.  time_left and initial_weight may be
+ * NULL: the step sets them for every census particle (timeLeft = dt,
+ * initialWeight = |weight|, manager/MonteCarloManagerSerial.hpp:391-405), so a
+ * caller that only steps need not copy them; they read 0 until then. */
 int storm_cuda_set_census(StormHandle *h, const StormParticlesSoA *host_in);
 /* Copy the census (the vector step() returns) device -> host.  host_out arrays
  * must hold `capacity` entries; *count receives the census size. */

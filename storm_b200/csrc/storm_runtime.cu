@@ -2056,12 +2056,14 @@ int storm_cuda_set_census(StormHandle *h, const StormParticlesSoA *in) {
     const double *sd[] = {in->x, in->y, in->z, in->vx, in->vy, in->vz, in->time_left, in->weight, in->initial_weight};
     double *dd[] = {stage.x, stage.y, stage.z, stage.vx, stage.vy, stage.vz, stage.t, stage.w, stage.w0};
     if (n && !in->cell) return STORM_ERR_INVALID_ARG;
-    for (int q = 0; q < 9; ++q)
-        if (!sd[q] && n) return STORM_ERR_INVALID_ARG;
+    for (int q = 0; q < 9; ++q)   // time_left (6) and initial_weight (8) may be left out: the step sets them
+        if (!sd[q] && n && q != 6 && q != 8) return STORM_ERR_INVALID_ARG;
     h->nCensus = 0;
     if (n) {
-        for (int q = 0; q < 9; ++q)
-            CK(cudaMemcpyAsync(dd[q], sd[q], n * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+        for (int q = 0; q < 9; ++q) {
+            if (sd[q]) CK(cudaMemcpyAsync(dd[q], sd[q], n * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+            else CK(cudaMemsetAsync(dd[q], 0, n * sizeof(double), h->stream));
+        }
         CK(cudaMemcpyAsync(stage.cell, in->cell, n * sizeof(uint32_t), cudaMemcpyHostToDevice, h->stream));
         if (stage.nu) {
             if (in->frequency) CK(cudaMemcpyAsync(stage.nu, in->frequency, n * sizeof(double), cudaMemcpyHostToDevice, h->stream));

@@ -136,7 +136,8 @@ class Particles:
             raise ValueError(f"buffer holds {self.n} particles, {n} requested")
         v = Particles(0)
         for f in self.FIELDS:
-            setattr(v, f, getattr(self, f)[:n])
+            a = getattr(self, f)
+            setattr(v, f, None if a is None else a[:n])
         v.cell = self.cell[:n]
         v.id = None if self.id is None else self.id[:n]
         v.frequency = None if getattr(self, "frequency", None) is None else self.frequency[:n]
@@ -145,13 +146,17 @@ class Particles:
 
     def soa(self):
         """Struct of pointers; every field is made contiguous first (the C side
-        reads plain arrays).  id may be None (not read or written)."""
+        reads plain arrays).  id may be None (not read or written); so may
+        time_left and initial_weight for storm_cuda_set_census, which a step
+        sets itself."""
         for f in self.FIELDS:
-            setattr(self, f, np.ascontiguousarray(getattr(self, f), dtype=np.float64))
+            if getattr(self, f) is not None:
+                setattr(self, f, np.ascontiguousarray(getattr(self, f), dtype=np.float64))
         self.cell = np.ascontiguousarray(self.cell, dtype=np.uint32)
         s = A.StormParticlesSoA()
         for f in self.FIELDS:
-            setattr(s, f, A.ptr(getattr(self, f)))
+            if getattr(self, f) is not None:
+                setattr(s, f, A.ptr(getattr(self, f)))
         s.cell = A.ptr(self.cell, C.c_uint32)
         if self.id is not None:
             self.id = np.ascontiguousarray(self.id, dtype=np.uint64)
@@ -262,7 +267,13 @@ class Engine:
         self._check(lib().storm_cuda_get_bank(self.h, C.byref(s), cnt.value, C.byref(cnt)))
         return p
 
-    def set_census(self, p):
+    def set_census(self, p, step_fields=True):
+        """Replace the census.  step_fields=False leaves out time_left and
+        initial_weight, which the next step sets itself."""
+        if not step_fields:
+            v = p.view(p.n)
+            v.time_left = v.initial_weight = None
+            p = v
         s = p.soa()
         self._check(lib().storm_cuda_set_census(self.h, C.byref(s)))
 

@@ -13,6 +13,7 @@ import numpy as np
 import pytest
 
 from conftest import golden
+from storm_b200 import _abi as A
 from storm_b200 import problems
 from storm_b200.engine import Engine, StormError
 from storm_b200.units import UNITS
@@ -253,3 +254,26 @@ def test_errors_are_reported():
     bad.cell[:] = 10 ** 6
     with pytest.raises(StormError):
         e.set_census(bad)
+
+
+@pytest.mark.parametrize("precision", [A.PRECISION_FP64, A.PRECISION_FP32_TRACK])
+def test_census_without_step_fields_steps_the_same(precision):
+    """storm_cuda_set_census with time_left and initial_weight left out (the
+    step sets both for every census particle) steps exactly like the full
+    census: same counts, temperatures to the atomics' summation order."""
+    p = problems.step_cube(n=10, new_photons_per_cell=3, face_packets=60, comb_nmin=10, precision=precision)
+    src = Engine(p)
+    src.step()
+    census = src.census()
+    src.close()
+    full, lean = Engine(p), Engine(p)
+    full.set_census(census)
+    lean.set_census(census, step_fields=False)
+    lc = lean.census()
+    assert (lc.time_left == 0).all() and (lc.initial_weight == 0).all()
+    sf, sl = full.step(), lean.step()
+    for k in ("census_in", "emitted_cells", "census_out", "segments", "escaped", "cutoff"):
+        assert sf[k] == sl[k], k
+    assert close(full.cells()["temperature"], lean.cells()["temperature"], 1e-9).all()
+    full.close()
+    lean.close()
