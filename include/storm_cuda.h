@@ -470,9 +470,9 @@ int storm_cuda_random_walk_sample(StormHandle *h, uint64_t n, const double *xi_l
 
 /* Photon counts per cell for an emission step (the per-cell counts
  * storm_cuda_phase_emit computes and storm_cuda_get_emission returns), for
- * callers that cannot allocate device memory while they run: code recording
- * into a CUDA graph, a host framework whose allocator owns the device memory,
- * a loop with a no-allocation rule.  This entry point has no counterpart in
+ * callers that cannot allocate device memory while they run: a host
+ * framework whose allocator owns the device memory, a loop with a
+ * no-allocation rule.  This entry point has no counterpart in
  * the reference; it calls no cudaMalloc / cudaFree and no allocating library
  * routine.
  *   d_energy   per-cell emission energy (device, ncells)
@@ -481,9 +481,8 @@ int storm_cuda_random_walk_sample(StormHandle *h, uint64_t n, const double *xi_l
  *   stream     cudaStream_t to run on (NULL = the legacy default stream)
  * Its scratch is one fixed array inside the library (about 128 KiB per GPU
  * that loads the library, held until exit).  The first call on a device looks
- * up that array's device address; make the first call before any stream
- * capture, and do not use the entry point across a cudaDeviceReset of that
- * device.  Calls whose work overlaps on the GPU share the array and race.
+ * up that array's device address once; do not use the entry point across a
+ * cudaDeviceReset of that device.  Calls whose work overlaps on the GPU share the array and race.
  * The whole computation stays on the device (no host readback), including
  * the exact left-to-right total that ambiguous floors fall back to.
  * ncells above STORM_NOALLOC_MAX_CELLS returns STORM_ERR_INVALID_ARG; a CUDA

@@ -1,9 +1,8 @@
 // Emission photon allocation that allocates no device memory.
 //
-// Who needs it: callers that cannot call cudaMalloc while they run -- code that
-// records work into a CUDA graph, a host framework whose caching allocator owns
-// the device memory, or a real-time loop with a no-allocation rule -- but that
-// still want the per-cell photon counts of an emission step computed on the
+// Who needs it: callers that cannot call cudaMalloc while they run -- a host
+// framework whose caching allocator owns the device memory, or a real-time
+// loop with a no-allocation rule -- but that still want the per-cell photon counts of an emission step computed on the
 // GPU from energies already in device memory.  The regular path
 // (storm_cuda_phase_emit) keeps its scratch in buffers its handle allocates;
 // this variant keeps it in one fixed array in the library image instead.
@@ -12,8 +11,8 @@
 // this library holds it (about 128 KiB) until the process exits.  In host code
 // the symbol is only a host-side stand-in, so its device address is looked up
 // with cudaGetSymbolAddress once per device, with that device current, and the
-// address is what the kernels receive.  That set-up happens on the first call
-// for a device; make that first call before any stream capture.  Every call
+// address is what the kernels receive.  That set-up happens once, on the first
+// call for a device.  Every call
 // shares the array: two calls whose work overlaps on the GPU race on it.  Each
 // call clears the one word that must start at zero (the ambiguity flag) and
 // overwrites the rest of the scratch it reads (the energy total and every tile

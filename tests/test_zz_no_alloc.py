@@ -1,8 +1,8 @@
 """The allocation-free emission allocation (storm_cuda_emission_allocation_noalloc)
 against the regular path, through the C ABI.
 
-It is for callers that cannot allocate device memory while they run (graph
-capture, an allocator that owns the device, a no-allocation loop).  This file
+It is for callers that cannot allocate device memory while they run (an
+allocator that owns the device, a no-allocation loop).  This file
 sorts last so that a run stopping at the first failure has run everything else;
 it also passes alone in a fresh process.
 """
