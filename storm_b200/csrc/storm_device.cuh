@@ -438,17 +438,26 @@ __device__ inline double pi_tail_series(double x) {
     const double x2 = x * x, x3 = x2 * x;
     const double a2 = 3.0 * x2, a3 = 6.0 * x;
     double sum = 0.0, e = e1;
-    // every lane of a warp takes term n at the same time, so the table read is uniform
-    for (int n = 1; n < 100000 && e != 0.0; ++n) {
-        double term;
-        if (n <= PI_TAIL_TABLE) {
-            const double *iv = c_piTail.v + 4 * (n - 1);
-            term = e * (((x3 * iv[0] + a2 * iv[1]) + a3 * iv[2]) + 6.0 * iv[3]);
-        } else {
-            const double dn = n;
-            const double d2 = dn * dn;
-            term = e * ((((x3 * dn + a2) * dn + a3) * dn + 6.0) / (d2 * d2));
-        }
+    const double e1sq = e1 * e1;
+    // every lane of a warp takes term n at the same time, so the table read is
+    // uniform; terms go in pairs, whose exponentials are two independent
+    // products, and the sum adds them in order
+    int n = 1;
+    for (; n + 1 <= PI_TAIL_TABLE && e != 0.0; n += 2) {
+        const double *iv = c_piTail.v + 4 * (n - 1);
+        const double eb = e * e1;
+        const double ta = e * (((x3 * iv[0] + a2 * iv[1]) + a3 * iv[2]) + 6.0 * iv[3]);
+        const double tb = eb * (((x3 * iv[4] + a2 * iv[5]) + a3 * iv[6]) + 6.0 * iv[7]);
+        sum += ta;
+        if (ta < 1e-18 * sum) return sum;
+        sum += tb;
+        if (tb < 1e-18 * sum) return sum;
+        e *= e1sq;
+    }
+    for (; n < 100000 && e != 0.0; ++n) {
+        const double dn = n;
+        const double d2 = dn * dn;
+        const double term = e * ((((x3 * dn + a2) * dn + a3) * dn + 6.0) / (d2 * d2));
         sum += term;
         if (term < 1e-18 * sum) break;
         e *= e1;
