@@ -95,6 +95,7 @@ struct CudaIMCBinding {
     std::size_t newPhotonsPerCell = 1;
     bool withRandomWalk = false, noHydroFeedback = false;
     bool withHydro = false;   // moving material: CellT::velocity and ExtensivesT::momentum (FP64 form)
+    bool withEgTimeAvg = false;   // group time averages (multigroup problems): getEgTimeAvg()
     double rwMinCellOpticalDepth = 25.0, rwMinParticleOpticalDepth = 5.0;
     bool withDDMC = false, ddmcUseMultigroupPGRW = false;
     double ddmcMinCellOpticalDepth = 15.0, ddmcMinParticleOpticalDepth = 5.0;
@@ -130,13 +131,12 @@ struct CudaIMCBinding {
         ddmcMinParticleOpticalDepth = p.ddmcMinParticleOpticalDepth;
         constexpr bool moving = cuda_detail::has_velocity<CellT>::value && cuda_detail::has_momentum<ExtensivesT>::value;
         withHydro = p.withHydro;
-        if ((p.withHydro && !moving) || p.MMC || p.withCompton || p.withEgTimeAvg || p.diffusionPressureGradient ||
-            p.postProcess.enabled) {
+        withEgTimeAvg = p.withEgTimeAvg;
+        if ((p.withHydro && !moving) || p.MMC || p.withCompton || p.diffusionPressureGradient || p.postProcess.enabled) {
             StormError eo("MonteCarloManagerCUDA: RadiationIMC option not supported on the device path");
             eo.addEntry("withHydro", p.withHydro);
             eo.addEntry("MMC", p.MMC);
             eo.addEntry("withCompton", p.withCompton);
-            eo.addEntry("withEgTimeAvg", p.withEgTimeAvg);
             eo.addEntry("diffusionPressureGradient", p.diffusionPressureGradient);
             eo.addEntry("postProcess.enabled", p.postProcess.enabled);
             throw eo;
@@ -352,6 +352,10 @@ public:
     // Erad_time_avg_ of the last step (RadiationIMC::getEradTimeAvg, radiation/RadiationIMC.hpp:431)
     inline const std::vector<double> &getEradTimeAvg(void) const { return eradAvg_; }
     inline const std::vector<double> &getPlanckOpacities(void) const { return sigmaA_; }
+    // Eg_time_avg_ of the last step (RadiationIMC::getEgTimeAvg, radiation/RadiationIMC.hpp:433) for
+    // multigroup problems bound with withEgTimeAvg: cell-major, the groups of cell i at
+    // [i * groups, (i + 1) * groups); empty otherwise
+    inline const std::vector<double> &getEgTimeAvg(void) const { return egAvg_; }
     inline const std::vector<double> &getFactorFleck(void) const { return fleck_; }
     // the boundary's drive temperature (MarshakBoundary::SetTemperature, SideTemperature::SetTemperature)
     void SetFaceTemperature(int face, double temperature) {
@@ -455,6 +459,7 @@ private:
         }
         d.rw_min_cell_optical_depth = binding_.rwMinCellOpticalDepth;
         d.rw_min_particle_optical_depth = binding_.rwMinParticleOpticalDepth;
+        d.with_eg_time_avg = binding_.withEgTimeAvg ? 1 : 0;   // kept for multigroup problems, as in the reference
         d.with_ddmc = binding_.withDDMC;
         d.ddmc_use_multigroup_pgrw = binding_.ddmcUseMultigroupPGRW;
         d.ddmc_min_cell_optical_depth = binding_.ddmcMinCellOpticalDepth;
@@ -658,6 +663,10 @@ private:
             ext[i].Erad = eradCensus[i];
             cells[i].Erad = ext[i].mass > 0.0 ? eradCensus[i] / ext[i].mass : 0.0;
         }
+        if (binding_.withEgTimeAvg && multigroup_) {   // postStep's group time averages (:1896-1902)
+            egAvg_.resize(N_ * (binding_.groupBounds.size() - 1));
+            cuda_detail::check(storm_cuda_get_group_tallies(h_, egAvg_.data()), h_, "get_group_tallies");
+        }
         if constexpr (cuda_detail::has_velocity<CellT>::value && cuda_detail::has_momentum<ExtensivesT>::value) {
             if (binding_.withHydro) {   // momentum deposits and velocity = momentum / mass (:853-866)
                 hostV_.resize(3 * N_);
@@ -689,7 +698,7 @@ private:
     bool multigroup_ = false;
     cuda_detail::PolyMeshArrays poly_;
     std::vector<std::size_t> cellsStepsCounters_;
-    std::vector<double> hostT_, hostE_, hostCE_, hostSA_, hostSS_, hostV_, hostM_, eradAvg_, sigmaA_, fleck_;
+    std::vector<double> hostT_, hostE_, hostCE_, hostSA_, hostSS_, hostV_, hostM_, eradAvg_, sigmaA_, fleck_, egAvg_;
     std::vector<std::size_t> beginningParticleCount_;
     Tracker tracker_;
     std::size_t startParticleCount_ = 0, initialParticleCount_ = 0, preStepParticleCount_ = 0, endParticleCount_ = 0;

@@ -36,7 +36,7 @@
 extern "C" {
 #endif
 
-#define STORM_CUDA_ABI_VERSION 7
+#define STORM_CUDA_ABI_VERSION 8
 
 /* ---------------------------------------------------------------- status */
 enum StormStatus {
@@ -239,6 +239,15 @@ typedef struct StormProblemDesc {
     int32_t with_hydro;
     int32_t pad2_;
     const double *cell_velocity;     /* 3 per cell [cm/s]: the cells' velocity (NULL = at rest) */
+
+    /* ---- group time averages (RadiationIMCParameters::withEgTimeAvg): per cell
+     * and group the time-integrated radiation energy of the particles whose lab
+     * frequency is in the group, tallied with Erad_time_avg in every segment,
+     * Random Walk jump and DDMC step and divided by dt V after the step
+     * (radiation/RadiationIMC.hpp:1166-1172, 1485-1491, 1802-1808, 1896-1902).
+     * Multigroup problems only, as in the reference; not with particle shards. */
+    int32_t with_eg_time_avg;
+    int32_t pad3_;
 } StormProblemDesc;
 
 #define STORM_STRAT_MAX_BINS 64
@@ -443,6 +452,11 @@ int storm_cuda_get_beginning_counts(StormHandle *h, uint64_t *counts);
  * before a step when a hydro solver moved the cells; read after it. */
 int storm_cuda_set_cell_motion(StormHandle *h, const double *velocity, const double *momentum);
 int storm_cuda_get_cell_motion(StormHandle *h, double *velocity, double *momentum);
+/* Group time averages of the last step (with_eg_time_avg): ncells x groups
+ * doubles, cell-major (cell c, group g at c * groups + g), RadiationIMC::
+ * getEgTimeAvg (radiation/RadiationIMC.hpp:433) after postStep.  Handles
+ * created without them return STORM_ERR_INVALID_ARG. */
+int storm_cuda_get_group_tallies(StormHandle *h, double *eg_time_avg);
 /* MarshakBoundary::SetTemperature / SideTemperature::SetTemperature. */
 int storm_cuda_set_face_temperature(StormHandle *h, int face, double temperature);
 

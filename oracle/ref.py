@@ -79,6 +79,7 @@ def lib():
         L.ref_advance_face_stream.argtypes = [vp, C.c_uint64]
         L.ref_record_get_momentum.argtypes = [vp, dp]
         L.ref_get_motion.argtypes = [vp, dp, dp]
+        L.ref_get_group_tallies.argtypes = [vp, dp]
         L.ref_units.argtypes = [dp]
         L.ref_planck_integral.restype = C.c_double
         L.ref_planck_integral.argtypes = [C.c_double, C.c_double]
@@ -225,6 +226,14 @@ class Reference:
         m = np.zeros((self.n, 3))
         lib().ref_get_motion(self.h, A.ptr(v), A.ptr(m))
         return v, m
+
+    def group_tallies(self):
+        """getEgTimeAvg after the last step (withEgTimeAvg), (ncells, groups)."""
+        G = self.problem.groups
+        out = np.zeros(self.n * G)
+        if lib().ref_get_group_tallies(self.h, A.ptr(out)) != 0:
+            raise RuntimeError("group time averages not kept")
+        return out.reshape(self.n, G)
 
     def thermal_energy(self, cells, xi):
         """The opacity plug-in's GetThermalEnergy at given uniforms (multigroup)."""

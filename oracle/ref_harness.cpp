@@ -425,6 +425,7 @@ struct PhysicsView {
     virtual std::size_t randomWalkStepCount() const = 0;
     virtual RecordState &records() = 0;
     virtual int thermalEnergy(uint64_t n, const uint32_t *cells, const double *xi, double *energy) = 0;
+    virtual int groupTallies(double *out) const = 0;   // getEgTimeAvg, cell-major
 };
 template <std::size_t G>
 struct PhysicsViewT : PhysicsView {
@@ -444,6 +445,13 @@ struct PhysicsViewT : PhysicsView {
     int thermalEnergy(uint64_t n, const uint32_t *cells, const double *xi, double *energy) override {
         typename HarnessOpacityT<G>::GroupBoundaries b = p->opac->bounds;
         for (uint64_t k = 0; k < n; ++k) energy[k] = p->opac->GetThermalEnergy((*p->opac->cells)[cells[k]], xi[k], b);
+        return 0;
+    }
+    int groupTallies(double *out) const override {
+        const auto &eg = p->getEgTimeAvg();
+        if (G < 2 || eg.empty()) return 1;
+        for (std::size_t i = 0; i < eg.size(); ++i)
+            for (std::size_t g = 0; g < G; ++g) out[i * G + g] = eg[i][g];
         return 0;
     }
 };
@@ -512,6 +520,7 @@ void build_physics(RefHandle &h, const StormProblemDesc *d) {
     p.ddmcMinCellOpticalDepth = d->ddmc_min_cell_optical_depth;
     p.ddmcMinParticleOpticalDepth = d->ddmc_min_particle_optical_depth;
     p.withHydro = d->with_hydro != 0;
+    p.withEgTimeAvg = d->with_eg_time_avg != 0;
     auto physics = std::make_shared<RecordingIMC<G>>(*h.grid, h.boundary, h.cells, h.ext, h.eos, opacity, p,
                                                      STORM::DirectRadiationIMCTraits<Vector3D, Cell, Ext, G>(),
                                                      RandomInCellPositionSampler<Vector3D, Grid>(), d->seed);
@@ -912,6 +921,9 @@ int ref_get_motion(RefHandle *h, double *velocity, double *momentum) {
     }
     return 0;
 }
+
+// RadiationIMC::getEgTimeAvg after the last step (withEgTimeAvg), cells x groups.
+int ref_get_group_tallies(RefHandle *h, double *out) { return h->view ? h->view->groupTallies(out) : 1; }
 
 // The serial manager's GetBeginningParticleCount after its last ref_step.
 int ref_beginning_counts(RefHandle *h, uint64_t *counts) {

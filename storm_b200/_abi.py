@@ -5,7 +5,7 @@ sizes against the compiled library.
 """
 import ctypes as C
 
-ABI_VERSION = 7
+ABI_VERSION = 8
 
 STORM_OK = 0
 STATUS_NAMES = {
@@ -91,6 +91,8 @@ class StormProblemDesc(C.Structure):
         ("with_hydro", C.c_int32),
         ("pad2_", C.c_int32),
         ("cell_velocity", C.POINTER(C.c_double)),
+        ("with_eg_time_avg", C.c_int32),
+        ("pad3_", C.c_int32),
     ]
 
 

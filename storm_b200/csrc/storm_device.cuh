@@ -115,6 +115,7 @@ struct Ctx {
     const double *faceCdf;   // per box face, groups + 1: cumulative B_g at the face's source temperature
     const double *mgEp;      // per group: E_g^p at the group centre (host pow, the opacity model's value)
     const float *mgEp32;     // the same as floats, FP32-tracking form
+    double *egAvg;           // group time averages (withEgTimeAvg): ncells x groups, NULL when off
     double *mgKTq;           // per cell: (kT)^q, written by the prestep
     // DDMC-style leakage (RadiationIMCParameters::withDDMC)
     int32_t withDDMC;
@@ -358,6 +359,7 @@ __device__ __forceinline__ void isotropic(RNG &rng, double c, double &vx, double
 // (extensives[cell].internal_energy) and the time-integrated radiation energy
 // (Erad_time_avg_[cell]).  LocalTally sums one segment's deposits (replay).
 struct LocalTally {
+    static constexpr bool kEg = false;   // no group time averages
     double mat_, rad_;
     double mx_, my_, mz_;   // momentum (moving material)
     __device__ __forceinline__ void mat(uint32_t, double v) { mat_ += v; }
@@ -371,6 +373,7 @@ struct LocalTally {
 // counters.  (Summing a run of segments in one cell in registers first costs
 // more in register spills than it saves in atomics.)
 struct SegmentTally {
+    static constexpr bool kEg = false;   // no group time averages
     double *eint, *erad;
     uint32_t *segs;        // NULL: no per-cell counters
     double depSum;
@@ -381,6 +384,16 @@ struct SegmentTally {
     __device__ __forceinline__ void mat(uint32_t c, double v) { atomicAdd(eint + c, v); depSum += v; }
     __device__ __forceinline__ void rad(uint32_t c, double v) { atomicAdd(erad + c, v); }
     __device__ __forceinline__ void mom(const struct Ctx &C, uint32_t c, double x, double y, double z);
+};
+// The same with the group time averages (withEgTimeAvg): every Erad_time_avg
+// contribution also goes to Eg_time_avg[cell][findGroup(frequency)] with the
+// particle's lab frequency at that moment (radiation/RadiationIMC.hpp:1166-1172,
+// 1485-1491, 1802-1808).  The kernels that take it are instantiated apart, so
+// the others carry none of its code.
+struct SegmentTallyEg : SegmentTally {
+    static constexpr bool kEg = true;
+    __device__ __forceinline__ void eg(const struct Ctx &C, uint32_t c, double v, double nu);
+    __device__ __forceinline__ void eg32(const struct Ctx &C, uint32_t c, double v, float nu);
 };
 
 // ------------------------------------------------------------------ multigroup
@@ -502,6 +515,9 @@ __device__ __forceinline__ uint32_t mg_find_group(const Ctx &C, double nu) {
         if (nu < C.gb[mid + 1]) hi = mid; else lo = mid + 1;
     }
     return lo;
+}
+__device__ __forceinline__ void SegmentTallyEg::eg(const Ctx &C, uint32_t c, double v, double nu) {
+    atomicAdd(C.egAvg + static_cast<size_t>(c) * C.groups + mg_find_group(C, nu), v);
 }
 // kT of the opacity model: k_B max(T, 1 K)
 __device__ __forceinline__ double mg_kT(const Ctx &C, uint32_t c) {
@@ -700,6 +716,9 @@ __device__ inline int try_random_walk(const Ctx &C, PartReg &p, RNG &rng, TALLY 
     double rwExp = expm1(-dt * rate);
     if (!C.noFeedback) tal.mat(cell, -rwExp * p.w);
     if (rate > 0.0) tal.rad(cell, p.w * rwExp * (pgrw ? (-1.0 / rate) : cp.z));
+    if constexpr (TALLY::kEg) {
+        if (rate > 0.0) tal.eg(C, cell, p.w * rwExp * (pgrw ? (-1.0 / rate) : cp.z), p.nu);
+    }
     p.w *= 1.0 + rwExp;
     p.t -= dt;
     if (fabs(p.w) < p.w0 * 1e-4) {
@@ -841,6 +860,7 @@ __device__ inline int try_ddmc(const Ctx &C, PartReg &p, RNG &rng, TALLY &tal, d
     if (!C.noFeedback) tal.mat(cell, -expFactor * oldWeight);
     const double integrated = (absRate > 0.0) ? oldWeight * expFactor * (-1.0 / absRate) : oldWeight * dt;
     tal.rad(cell, integrated);
+    if constexpr (TALLY::kEg) tal.eg(C, cell, integrated, p.nu);
     p.w *= 1.0 + expFactor;
     p.t -= dt;
     if (fabs(p.w) < p.w0 * 1e-3) {
@@ -1160,6 +1180,7 @@ __device__ inline PhysOut physics_step(const Ctx &C, Track &T, RNG &rng, TALLY &
         tal.mom(C, cell, a * p.vx * C.invC2, a * p.vy * C.invC2, a * p.vz * C.invC2);
     }
     tal.rad(cell, integrated);
+    if constexpr (TALLY::kEg) tal.eg(C, cell, integrated, p.nu);
     p.w *= 1.0 + e1;
     if (fabs(p.w) < p.w0 * 1e-3) {
         if (!C.noFeedback) tal.mat(cell, p.w);
@@ -1313,6 +1334,7 @@ __device__ inline int rw_jump32(const Ctx &C, Track32 &T, RNG &rng, TALLY &tal, 
     if (sigAf > 0.0f) {
         const double invRate = MG ? -1.0 / (static_cast<double>(sigAf) * C.clight) : static_cast<double>(cp.w);
         tal.rad(cell, T.w * e1 * invRate);
+        if constexpr (TALLY::kEg) tal.eg32(C, cell, T.w * e1 * invRate, T.nu);
     }
     T.w *= 1.0 + e1;
     T.t -= dt;
@@ -1376,6 +1398,8 @@ __device__ inline int ddmc_jump32(const Ctx &C, Track32 &T, RNG &rng, TALLY &tal
     const double e1 = static_cast<double>(expm1f(-tau));
     if (!C.noFeedback) tal.mat(cell, -e1 * T.w);
     tal.rad(cell, da.z > 0.0f ? T.w * e1 * (-1.0 / static_cast<double>(da.z)) : T.w * dt);
+    if constexpr (TALLY::kEg)
+        tal.eg32(C, cell, da.z > 0.0f ? T.w * e1 * (-1.0 / static_cast<double>(da.z)) : T.w * dt, T.nu);
     T.w *= 1.0 + e1;
     T.t -= dt;
     if (fabs(T.w) < T.w0 * 1e-3) {
@@ -1474,6 +1498,16 @@ __device__ inline int ddmc_jump32_poly(const Ctx &C, Track32 &T, RNG &rng, TALLY
     T.cell = nb;
     T.i = nb;
     return OUT_CONTINUE;
+}
+
+// findGroup on the FP32 form's float bounds (the same rule)
+__device__ __forceinline__ void SegmentTallyEg::eg32(const Ctx &C, uint32_t c, double v, float nu) {
+    uint32_t lo = 0, hi = C.groups - 1;
+    while (lo < hi) {
+        const uint32_t mid = (lo + hi) >> 1;
+        if (nu < C.gb32[mid + 1]) hi = mid; else lo = mid + 1;
+    }
+    atomicAdd(C.egAvg + static_cast<size_t>(c) * C.groups + lo, v);
 }
 
 // Multigroup absorption opacity in FP32 from the cell's cached kT and
@@ -1641,6 +1675,7 @@ __device__ inline int segment32(const Ctx &C, Track32 &T, RNG &rng, TALLY &tal, 
     }
     if (!C.noFeedback) tal.mat(cell, -e1 * T.w);
     tal.rad(cell, integrated);
+    if constexpr (TALLY::kEg) tal.eg32(C, cell, integrated, T.nu);
     T.w *= 1.0 + e1;
     if (fabs(T.w) < T.w0 * 1e-3) {
         if (!C.noFeedback) tal.mat(cell, T.w);

@@ -3,6 +3,8 @@
 #include <cuda_runtime.h>
 #include <math_constants.h>
 
+#include <type_traits>
+
 #include "storm_device.cuh"
 #include "storm_internal.h"
 
@@ -1303,11 +1305,13 @@ __device__ __forceinline__ void block_stats_flush(const BlockStats &bs, DevStats
 // convex-polyhedral mesh and Form64T<5> is it with the DDMC branch;
 // Form64T<4> is Form64T<1> without the DDMC branch.  Problems without
 // withDDMC run the variants without it: less code for the instruction cache,
-// whose misses bound the multigroup and polyhedral kernels.
-template <int V>
+// whose misses bound the multigroup and polyhedral kernels.  EG adds the
+// group time averages (withEgTimeAvg) to the tallies.
+template <int V, bool EG = false>
 struct Form64T {
     using T = Track;
     using Rng = PhiloxRng;
+    using Tally = std::conditional_t<EG, SegmentTallyEg, SegmentTally>;
     static __device__ __forceinline__ void load(const Ctx &C, const Bank &b, uint32_t q, T &t) {
         load_part(b, q, t.p);
         track_begin(C, t);
@@ -1337,10 +1341,14 @@ using Form64Poly = Form64T<2>;
 using Form64PolyDDMC = Form64T<5>;   // Form64Poly with the DDMC branch
 using Form64Hydro = Form64T<3>;   // Form64Full with moving material
 using Form64MG = Form64T<4>;      // Form64Full without the DDMC branch
+using Form64FullEg = Form64T<1, true>;   // the multigroup forms with the group time averages
+using Form64MGEg = Form64T<4, true>;
+using Form64HydroEg = Form64T<3, true>;
 template <bool POLY, bool DDMC = true>
 struct Form32T {
     using T = Track32;
     using Rng = PhiloxRng4;
+    using Tally = SegmentTally;
     static __device__ __forceinline__ void load(const Ctx &C, const Bank &b, uint32_t q, T &t) {
         load32(b, q, t);
         cell_ijk(C, t.cell, t.i, t.j, t.k);
@@ -1367,10 +1375,11 @@ using Form32Lean = Form32T<false, false>;   // without the DDMC branch
 using Form32Poly = Form32T<true, false>;   // without the DDMC branch
 using Form32PolyDDMC = Form32T<true, true>;
 // The FP32-tracking form of a multigroup problem: the frequency rides along.
-template <bool DDMC = true>
+template <bool DDMC = true, bool EG = false>
 struct Form32MGT {
     using T = Track32;
     using Rng = PhiloxRng4;
+    using Tally = std::conditional_t<EG, SegmentTallyEg, SegmentTally>;
     static __device__ __forceinline__ void load(const Ctx &C, const Bank &b, uint32_t q, T &t) {
         load32(b, q, t);
         t.nu = load_nu32(b, q);
@@ -1396,6 +1405,8 @@ struct Form32MGT {
 };
 using Form32MG = Form32MGT<true>;
 using Form32MGLean = Form32MGT<false>;   // without the DDMC branch
+using Form32MGEg = Form32MGT<true, true>;   // with the group time averages
+using Form32MGLeanEg = Form32MGT<false, true>;
 
 // One bank visit of the HandleAll loop (manager/MonteCarloManagerSerial.hpp:267-383):
 // every active particle runs up to K segments in registers; survivors are
@@ -1532,7 +1543,7 @@ __global__ void __launch_bounds__(256, MINB) k_transport_refill(Ctx C, Bank in, 
         if (!__any_sync(FULL, has)) break;
         int outcome = OUT_CONTINUE;
         if (has) {
-            SegmentTally tal;
+            typename F::Tally tal;
             tal.init(C.eint, C.eradAvg, C.perCellCounters ? C.segs : nullptr);
             uint32_t segs = 0, rws = 0;
             for (uint32_t b = 0; b < burst; ++b) {
@@ -2735,6 +2746,11 @@ __global__ void k_gather(Ctx C, CensusBank src, const uint32_t *idx, uint32_t n,
 __global__ void k_poststep(Ctx C, CellArrays A, OpacityEos M, double dt) {
     for (uint32_t c = blockIdx.x * blockDim.x + threadIdx.x; c < C.ncells; c += gridDim.x * blockDim.x) {
         A.eradAvg[c] /= (dt * A.vol[c]);
+        if (C.egAvg) {   // postStep's group time averages (radiation/RadiationIMC.hpp:1896-1902)
+            const double norm = dt * A.vol[c];
+            double *eg = C.egAvg + static_cast<size_t>(c) * C.groups;
+            for (uint32_t g = 0; g < C.groups; ++g) eg[g] /= norm;
+        }
         if (C.noFeedback) continue;
         double E = A.eint[c];
         if (E < 0.0) {   // throwIfNegativeInternalEnergy (:771-817)
@@ -3131,6 +3147,14 @@ static void refill_launch(cudaStream_t s, uint32_t grid, int minBlocks, const Ct
 void launch_transport_refill(cudaStream_t s, uint32_t grid, int minBlocks, const Ctx &C, const Bank &in, uint32_t n,
                              uint32_t *nextIdx, const CensusBank &cen, uint32_t *nCen, uint32_t burst, uint32_t maxSegs,
                              DevStats *st) {
+    if (C.egAvg) {   // multigroup problems with the group time averages
+        if (C.fp32 && C.withDDMC) refill_launch<Form32MGEg>(s, grid, minBlocks, C, in, n, nextIdx, cen, nCen, burst, maxSegs, st);
+        else if (C.fp32) refill_launch<Form32MGLeanEg>(s, grid, minBlocks, C, in, n, nextIdx, cen, nCen, burst, maxSegs, st);
+        else if (C.withHydro) refill_launch<Form64HydroEg>(s, grid, minBlocks, C, in, n, nextIdx, cen, nCen, burst, maxSegs, st);
+        else if (C.withDDMC) refill_launch<Form64FullEg>(s, grid, minBlocks, C, in, n, nextIdx, cen, nCen, burst, maxSegs, st);
+        else refill_launch<Form64MGEg>(s, grid, minBlocks, C, in, n, nextIdx, cen, nCen, burst, maxSegs, st);
+        return;
+    }
     if (C.fp32 && C.poly && C.withDDMC) refill_launch<Form32PolyDDMC>(s, grid, minBlocks, C, in, n, nextIdx, cen, nCen, burst, maxSegs, st);
     else if (C.fp32 && C.poly) refill_launch<Form32Poly>(s, grid, minBlocks, C, in, n, nextIdx, cen, nCen, burst, maxSegs, st);
     else if (C.fp32 && C.groups >= 2 && C.withDDMC) refill_launch<Form32MG>(s, grid, minBlocks, C, in, n, nextIdx, cen, nCen, burst, maxSegs, st);

@@ -122,6 +122,7 @@ struct StormHandle {
     uint64_t nCenGlobal = 0, nCellEmitGlobal = 0, nFaceEmitGlobal = 0;   // this step's global counts
     double *dep = nullptr;           // this handle's material deposits of the step (N)
     double4 *vel = nullptr;          // moving material: (vx, vy, vz, gamma) per cell
+    double *egAvg = nullptr;         // group time averages (with_eg_time_avg): ncells x groups
     double *mom = nullptr;           // moving material: momentum, 3 per cell
     double *xbuf = nullptr;          // exchange buffer (max(2 N, 2 S N, S + N) doubles)
     double *shardWc = nullptr;       // cells' global census weights (N)
@@ -1225,6 +1226,13 @@ int storm_cuda_create(const StormProblemDesc *d, StormHandle **out) {
         H2D(h->mom, m.data(), 3 * static_cast<size_t>(N));
     }
     C.vel = h->vel;
+    // group time averages: multigroup problems only (the reference tallies them
+    // only with withMultigroupOpacity)
+    if (d->with_eg_time_avg && mg) {
+        ALLOC(h->egAvg, static_cast<size_t>(N) * d->groups);
+        ZERO(h->egAvg, static_cast<size_t>(N) * d->groups * sizeof(double));
+    }
+    C.egAvg = h->egAvg;
     C.mom = h->mom;
     C.clight = d->clight; C.arad = d->arad; C.sigmaSB = d->sigma_sb; C.kevKelvin = d->kev_kelvin;
     C.rwMinParticle = d->rw_min_particle_optical_depth;
@@ -1293,7 +1301,7 @@ int storm_cuda_destroy(StormHandle *h) {
                   h->runCursor, h->runScan, h->longRuns, h->bucketFlags,
                   h->cfo, h->cfN, h->cfP, h->cfNext, h->cfFace, h->mpx, h->mpy, h->mpz, h->fvo, h->fvi, h->vtx,
                   h->chord, h->cfN32, h->dep, h->xbuf, h->shardWc, h->shardRunW, h->shardStart, h->shardBounds,
-                  h->vel, h->mom, h->ddmcCum32, h->cfA};
+                  h->vel, h->mom, h->ddmcCum32, h->cfA, h->egAvg};
     for (void *p : ps) device_pool().free(p);
     cudaEvent_t evs[] = {h->evStart, h->evTransport0, h->evTransport1, h->evEnd, h->evAfterEmit, h->evAfterComb};
     bool complete = h->stream != nullptr;
@@ -1349,6 +1357,8 @@ int storm_cuda_phase_begin(StormHandle *h, double dt) {
 int storm_cuda_phase_prestep(StormHandle *h, double dt) {
     if (!h) return STORM_ERR_INVALID_ARG;
     refresh_ctx(h);
+    if (h->egAvg)   // preStep clears Eg_time_avg_ (radiation/RadiationIMC.hpp:1626-1630)
+        CK(cudaMemsetAsync(h->egAvg, 0, sizeof(double) * h->N * h->desc.groups, h->stream));
     launch_prestep(h->stream, h->C, h->A, h->M, dt);
     ++h->launches;
     if (h->C.withDDMC) {
@@ -1494,7 +1504,7 @@ int storm_cuda_phase_transport(StormHandle *h) {
     uint32_t n32 = static_cast<uint32_t>(n0);
     uint32_t *nCen = h->counts + h->maxRounds + 1;
     // the multigroup FP32 form runs only in the refill kernel
-    const bool refill = h->refill || (h->fp32 && h->desc.groups >= 2) || h->C.poly || h->C.withHydro;
+    const bool refill = h->refill || (h->fp32 && h->desc.groups >= 2) || h->C.poly || h->C.withHydro || h->C.egAvg;
     if (!refill) CK(cudaMemcpyAsync(h->counts, &n32, sizeof(uint32_t), cudaMemcpyHostToDevice, h->stream));
     if (refill) {
         // one launch carries every history to census, escape or cutoff
@@ -1968,7 +1978,7 @@ int storm_cuda_set_sharding(StormHandle *h, uint32_t shards, uint32_t lo, uint32
     // once per handle, before its first census
     if (!h || shards == 0 || lo >= hi || hi > shards || h->nCensus != 0 || h->dep) return STORM_ERR_INVALID_ARG;
     if (shards > 1 && (!h->desc.comb_enabled || h->desc.comb_kind != STORM_COMB_PLAIN)) return STORM_ERR_INVALID_ARG;
-    if (shards > 1 && h->C.withHydro) return STORM_ERR_UNSUPPORTED;   // the momentum tallies have no exchange
+    if (shards > 1 && (h->C.withHydro || h->C.egAvg)) return STORM_ERR_UNSUPPORTED;   // tallies without an exchange
     CK(cudaSetDevice(h->device));
     h->shards = shards;
     h->shardLo = lo;
@@ -2249,6 +2259,15 @@ int storm_cuda_set_cell_motion(StormHandle *h, const double *velocity, const dou
         CK(cudaMemcpyAsync(h->mom, momentum, 3 * N * sizeof(double), cudaMemcpyHostToDevice, h->stream));
         CK(cudaStreamSynchronize(h->stream));
     }
+    return STORM_OK;
+}
+
+int storm_cuda_get_group_tallies(StormHandle *h, double *eg_time_avg) {
+    if (!h || !eg_time_avg || !h->egAvg) return STORM_ERR_INVALID_ARG;
+    CK(cudaSetDevice(h->device));
+    CK(cudaMemcpyAsync(eg_time_avg, h->egAvg, sizeof(double) * h->N * h->desc.groups, cudaMemcpyDeviceToHost,
+                       h->stream));
+    CK(cudaStreamSynchronize(h->stream));
     return STORM_OK;
 }
 

@@ -55,6 +55,7 @@ def lib():
         L.storm_cuda_set_opacity_tables.argtypes = [vp, dp, dp]
         L.storm_cuda_set_cell_motion.argtypes = [vp, dp, dp]
         L.storm_cuda_get_cell_motion.argtypes = [vp, dp, dp]
+        L.storm_cuda_get_group_tallies.argtypes = [vp, dp]
         L.storm_cuda_set_sharding.argtypes = [vp, C.c_uint32, C.c_uint32, C.c_uint32, A.ExchangeFn, vp]
         L.storm_cuda_get_beginning_counts.argtypes = [vp, u64p]
         L.storm_cuda_set_face_temperature.argtypes = [vp, C.c_int, C.c_double]
@@ -324,6 +325,14 @@ class Engine:
         m = np.zeros(3 * self.n)
         self._check(lib().storm_cuda_get_cell_motion(self.h, A.ptr(v), A.ptr(m)))
         return v.reshape(-1, 3), m.reshape(-1, 3)
+
+    def group_tallies(self):
+        """Group time averages of the last step (problems with
+        with_eg_time_avg): (ncells, groups)."""
+        G = self.problem.groups
+        out = np.zeros(self.n * G)
+        self._check(lib().storm_cuda_get_group_tallies(self.h, A.ptr(out)))
+        return out.reshape(self.n, G)
 
     def beginning_counts(self):
         """Particles per cell when the last step's transport began (handles with

@@ -91,6 +91,8 @@ class Problem:
     # moving material (withHydro): per-cell velocity [cm/s], shape (ncells, 3); None = at rest
     with_hydro: bool = False
     cell_velocity: np.ndarray = None
+    # group time averages (withEgTimeAvg, multigroup problems): per cell and group
+    with_eg_time_avg: bool = False
 
     @property
     def shape(self):
@@ -195,6 +197,7 @@ class Problem:
             d.mesh = C.pointer(md)
         d.with_hydro = int(self.with_hydro)
         d.cell_velocity = arr(None if self.cell_velocity is None else np.asarray(self.cell_velocity).reshape(-1))
+        d.with_eg_time_avg = int(self.with_eg_time_avg)
         d._keep = keep
         return d
 

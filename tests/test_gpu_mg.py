@@ -10,6 +10,8 @@ GPU against the reference.
   weights and tallies to the replay tolerances of the gray path.
 * Whole steps agree with the reference's own serial path statistically and
   conserve energy.
+* The group time averages (withEgTimeAvg) add up to Erad_time_avg cell by
+  cell and agree with the reference's per (cell, group).
 """
 import numpy as np
 import pytest
@@ -114,3 +116,69 @@ def test_mg_fp32_tracking_conserves_and_agrees_with_fp64():
     a = run_batch(Engine, prob(A.PRECISION_FP32_TRACK), range(30, 46), 4, check)
     b = run_batch(Engine, prob(A.PRECISION_FP64), range(70, 86), 4, check)
     assert_agree(a, b, "multigroup cube 8^3 x 64: FP32 vs FP64")
+
+
+def _eg_cube(seed, precision=None, ddmc=False):
+    from storm_b200 import _abi as A
+    p = problems.mg_cube(n=6, groups=64, kappa0=1.0, new_photons_per_cell=6, comb_nmin=6, seed=seed,
+                         precision=A.PRECISION_FP64 if precision is None else precision)
+    p.with_eg_time_avg = True
+    if ddmc:
+        p.sigma_s = np.full(p.ncells, 1000.0)
+        p.with_ddmc = True
+        p.ddmc_use_multigroup_pgrw = True
+    return p
+
+
+@pytest.mark.parametrize("ddmc", [False, True])
+@pytest.mark.parametrize("fp32", [False, True])
+def test_group_time_averages_add_up_to_erad(fp32, ddmc):
+    """withEgTimeAvg (radiation/RadiationIMC.hpp:1166-1172, 1485-1491,
+    1802-1808, 1896-1902): every Erad_time_avg contribution of a segment,
+    Random Walk jump or DDMC step also goes to the particle's group, so the
+    groups of a cell add up to its Erad_time_avg (to the atomics' summation
+    order), in both forms, with and without DDMC; a handle without the option
+    has no group tallies."""
+    from storm_b200 import _abi as A
+    from storm_b200.engine import StormError
+    p = _eg_cube(7, A.PRECISION_FP32_TRACK if fp32 else A.PRECISION_FP64, ddmc)
+    e = Engine(p)
+    for _ in range(3):
+        e.step()
+        eg = e.group_tallies()
+        erad = e.cells()["erad_time_avg"]
+        assert eg.shape == (p.ncells, 64) and (eg >= 0).all()
+        assert close(eg.sum(1), erad, 1e-9).all()
+        assert (eg > 0).sum() > 0.1 * eg.size
+    e.close()
+    q = _eg_cube(7)
+    q.with_eg_time_avg = False
+    e = Engine(q)
+    e.step()
+    with pytest.raises(StormError):
+        e.group_tallies()
+    e.close()
+
+
+def test_group_time_averages_agree_with_reference(ref_lib):
+    """Three steps of the 6^3 x 64-group cube with withEgTimeAvg on
+    independent seeds: the group time average of every (cell, group), engine
+    against the reference's serial path, under the batch gate."""
+    from storm_b200 import batchstats
+
+    def run(make, seeds):
+        out = []
+        for s in seeds:
+            m = make(_eg_cube(s))
+            for _ in range(3):
+                m.step()
+            out.append(m.group_tallies().T)   # (groups, cells)
+            m.close()
+        return np.array(out)
+    a = batchstats.summarize(run(Engine, range(20, 36)))
+    b = batchstats.summarize(run(ref_lib.Reference, range(60, 76)))
+    scale = np.maximum(np.abs(a["mean"]), np.abs(b["mean"])).max(axis=-1, keepdims=True)
+    z, ok = batchstats.welch_z(a, b, batchstats.RESOLUTION * scale)
+    g = batchstats.gate(z[ok])
+    print({"label": "group time averages 6^3 x 64: engine vs reference", **g})
+    assert g["tests"] > 2000 and g["passed"], g
