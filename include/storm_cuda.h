@@ -247,7 +247,15 @@ typedef struct StormProblemDesc {
      * (radiation/RadiationIMC.hpp:1166-1172, 1485-1491, 1802-1808, 1896-1902).
      * Multigroup problems only, as in the reference; not with particle shards. */
     int32_t with_eg_time_avg;
-    int32_t pad3_;
+
+    /* ---- reproducible tallies: the material deposits and the time-integrated
+     * radiation energy of the transport are summed per cell in 120-bit fixed
+     * point with integer atomics, at a per-step scale from the step's energy
+     * budget, and folded into FP64 after transport, so that a run repeats bit
+     * for bit (FP64 atomics add in an order that varies from run to run).  Not
+     * with moving material, group time averages, particle shards or without
+     * population control (STORM_ERR_UNSUPPORTED). */
+    int32_t reproducible_tallies;
 } StormProblemDesc;
 
 #define STORM_STRAT_MAX_BINS 64

@@ -92,7 +92,7 @@ class StormProblemDesc(C.Structure):
         ("pad2_", C.c_int32),
         ("cell_velocity", C.POINTER(C.c_double)),
         ("with_eg_time_avg", C.c_int32),
-        ("pad3_", C.c_int32),
+        ("reproducible_tallies", C.c_int32),
     ]
 
 

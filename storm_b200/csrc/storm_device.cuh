@@ -116,6 +116,10 @@ struct Ctx {
     const double *mgEp;      // per group: E_g^p at the group centre (host pow, the opacity model's value)
     const float *mgEp32;     // the same as floats, FP32-tracking form
     double *egAvg;           // group time averages (withEgTimeAvg): ncells x groups, NULL when off
+    // reproducible tallies: 4 fixed-point limbs per cell for the deposits and for
+    // Erad_time_avg (NULL when off), and this step's power-of-two scales into them
+    unsigned long long *fixMat, *fixRad;
+    double fixScaleMat, fixScaleRad;
     double *mgKTq;           // per cell: (kT)^q, written by the prestep
     // DDMC-style leakage (RadiationIMCParameters::withDDMC)
     int32_t withDDMC;
@@ -396,6 +400,54 @@ struct SegmentTallyEg : SegmentTally {
     __device__ __forceinline__ void eg32(const struct Ctx &C, uint32_t c, double v, float nu);
 };
 
+// Reproducible tallies: a value x (already multiplied by a power-of-two scale,
+// |x| < 2^119) goes into four 30-bit limbs, high to low, each added with an
+// integer atomic.  Integer addition is associative, so the sums do not depend on
+// the order the segments arrive in; up to 2^33 contributions per cell fit in a
+// limb's 64 bits.  Bits below the scale's unit are dropped, the same way in
+// every run.  The limbs are split off the magnitude with exact floating-point
+// steps (each remainder is a multiple of the value's unit in the last place
+// and below the next power) and carry its sign.
+__device__ __forceinline__ void fixed_add(unsigned long long *acc, uint32_t c, double x) {
+    const double ax = fabs(x);
+    const double h3 = floor(ax * 0x1p-90);
+    const double r3 = ax - h3 * 0x1p90;
+    const double h2 = floor(r3 * 0x1p-60);
+    const double r2 = r3 - h2 * 0x1p60;
+    const double h1 = floor(r2 * 0x1p-30);
+    const double h0 = floor(r2 - h1 * 0x1p30);
+    long long l3 = static_cast<long long>(h3), l2 = static_cast<long long>(h2), l1 = static_cast<long long>(h1),
+              l0 = static_cast<long long>(h0);
+    if (x < 0.0) { l3 = -l3; l2 = -l2; l1 = -l1; l0 = -l0; }
+    unsigned long long *a = acc + 4 * static_cast<size_t>(c);
+    if (l3) atomicAdd(a + 3, static_cast<unsigned long long>(l3));
+    if (l2) atomicAdd(a + 2, static_cast<unsigned long long>(l2));
+    if (l1) atomicAdd(a + 1, static_cast<unsigned long long>(l1));
+    if (l0) atomicAdd(a, static_cast<unsigned long long>(l0));
+}
+// The value of a cell's four limbs after the carries are propagated (integer
+// arithmetic, then one fixed sequence of floating-point operations).
+__device__ __forceinline__ double fixed_value(const unsigned long long *acc, uint32_t c) {
+    const unsigned long long *a = acc + 4 * static_cast<size_t>(c);
+    long long v0 = static_cast<long long>(a[0]), v1 = static_cast<long long>(a[1]), v2 = static_cast<long long>(a[2]),
+              v3 = static_cast<long long>(a[3]);
+    long long k = v0 >> 30; v0 -= k * (1ll << 30); v1 += k;
+    k = v1 >> 30; v1 -= k * (1ll << 30); v2 += k;
+    k = v2 >> 30; v2 -= k * (1ll << 30); v3 += k;
+    return ((static_cast<double>(v3) * 0x1p90 + static_cast<double>(v2) * 0x1p60) + static_cast<double>(v1) * 0x1p30) +
+           static_cast<double>(v0);
+}
+// The transport tally with reproducible sums (kernels of their own, as for the
+// group time averages): the same calls, fixed-point limbs instead of FP64 atomics.
+struct SegmentTallyFixed : SegmentTally {
+    static constexpr bool kEg = false;
+    unsigned long long *fm, *fr;
+    double sm, sr;
+    __device__ __forceinline__ void init_fixed(const struct Ctx &C);
+    __device__ __forceinline__ void mat(uint32_t c, double v) { fixed_add(fm, c, v * sm); depSum += v; }
+    __device__ __forceinline__ void rad(uint32_t c, double v) { fixed_add(fr, c, v * sr); }
+};
+
 // ------------------------------------------------------------------ multigroup
 // planck_integral(a, b) = 15/pi^4 int_a^b x^3/(e^x - 1) dx from Clark's two
 // published series: the Bernoulli expansion below x = 0.5 and the exponential
@@ -515,6 +567,9 @@ __device__ __forceinline__ uint32_t mg_find_group(const Ctx &C, double nu) {
         if (nu < C.gb[mid + 1]) hi = mid; else lo = mid + 1;
     }
     return lo;
+}
+__device__ __forceinline__ void SegmentTallyFixed::init_fixed(const Ctx &C) {
+    fm = C.fixMat; fr = C.fixRad; sm = C.fixScaleMat; sr = C.fixScaleRad;
 }
 __device__ __forceinline__ void SegmentTallyEg::eg(const Ctx &C, uint32_t c, double v, double nu) {
     atomicAdd(C.egAvg + static_cast<size_t>(c) * C.groups + mg_find_group(C, nu), v);

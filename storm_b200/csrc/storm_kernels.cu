@@ -1305,13 +1305,14 @@ __device__ __forceinline__ void block_stats_flush(const BlockStats &bs, DevStats
 // convex-polyhedral mesh and Form64T<5> is it with the DDMC branch;
 // Form64T<4> is Form64T<1> without the DDMC branch.  Problems without
 // withDDMC run the variants without it: less code for the instruction cache,
-// whose misses bound the multigroup and polyhedral kernels.  EG adds the
-// group time averages (withEgTimeAvg) to the tallies.
-template <int V, bool EG = false>
+// whose misses bound the multigroup and polyhedral kernels.  TL is the
+// tally: SegmentTallyEg adds the group time averages (withEgTimeAvg),
+// SegmentTallyFixed sums in fixed point (reproducible tallies).
+template <int V, class TL = SegmentTally>
 struct Form64T {
     using T = Track;
     using Rng = PhiloxRng;
-    using Tally = std::conditional_t<EG, SegmentTallyEg, SegmentTally>;
+    using Tally = TL;
     static __device__ __forceinline__ void load(const Ctx &C, const Bank &b, uint32_t q, T &t) {
         load_part(b, q, t.p);
         track_begin(C, t);
@@ -1341,14 +1342,19 @@ using Form64Poly = Form64T<2>;
 using Form64PolyDDMC = Form64T<5>;   // Form64Poly with the DDMC branch
 using Form64Hydro = Form64T<3>;   // Form64Full with moving material
 using Form64MG = Form64T<4>;      // Form64Full without the DDMC branch
-using Form64FullEg = Form64T<1, true>;   // the multigroup forms with the group time averages
-using Form64MGEg = Form64T<4, true>;
-using Form64HydroEg = Form64T<3, true>;
-template <bool POLY, bool DDMC = true>
+using Form64FullEg = Form64T<1, SegmentTallyEg>;   // the multigroup forms with the group time averages
+using Form64MGEg = Form64T<4, SegmentTallyEg>;
+using Form64HydroEg = Form64T<3, SegmentTallyEg>;
+using Form64Fix = Form64T<0, SegmentTallyFixed>;   // reproducible tallies
+using Form64FullFix = Form64T<1, SegmentTallyFixed>;
+using Form64MGFix = Form64T<4, SegmentTallyFixed>;
+using Form64PolyFix = Form64T<2, SegmentTallyFixed>;
+using Form64PolyDDMCFix = Form64T<5, SegmentTallyFixed>;
+template <bool POLY, bool DDMC = true, class TL = SegmentTally>
 struct Form32T {
     using T = Track32;
     using Rng = PhiloxRng4;
-    using Tally = SegmentTally;
+    using Tally = TL;
     static __device__ __forceinline__ void load(const Ctx &C, const Bank &b, uint32_t q, T &t) {
         load32(b, q, t);
         cell_ijk(C, t.cell, t.i, t.j, t.k);
@@ -1374,12 +1380,16 @@ using Form32 = Form32T<false>;
 using Form32Lean = Form32T<false, false>;   // without the DDMC branch
 using Form32Poly = Form32T<true, false>;   // without the DDMC branch
 using Form32PolyDDMC = Form32T<true, true>;
+using Form32Fix = Form32T<false, true, SegmentTallyFixed>;   // reproducible tallies
+using Form32LeanFix = Form32T<false, false, SegmentTallyFixed>;
+using Form32PolyFix = Form32T<true, false, SegmentTallyFixed>;
+using Form32PolyDDMCFix = Form32T<true, true, SegmentTallyFixed>;
 // The FP32-tracking form of a multigroup problem: the frequency rides along.
-template <bool DDMC = true, bool EG = false>
+template <bool DDMC = true, class TL = SegmentTally>
 struct Form32MGT {
     using T = Track32;
     using Rng = PhiloxRng4;
-    using Tally = std::conditional_t<EG, SegmentTallyEg, SegmentTally>;
+    using Tally = TL;
     static __device__ __forceinline__ void load(const Ctx &C, const Bank &b, uint32_t q, T &t) {
         load32(b, q, t);
         t.nu = load_nu32(b, q);
@@ -1405,8 +1415,10 @@ struct Form32MGT {
 };
 using Form32MG = Form32MGT<true>;
 using Form32MGLean = Form32MGT<false>;   // without the DDMC branch
-using Form32MGEg = Form32MGT<true, true>;   // with the group time averages
-using Form32MGLeanEg = Form32MGT<false, true>;
+using Form32MGEg = Form32MGT<true, SegmentTallyEg>;   // with the group time averages
+using Form32MGLeanEg = Form32MGT<false, SegmentTallyEg>;
+using Form32MGFix = Form32MGT<true, SegmentTallyFixed>;   // reproducible tallies
+using Form32MGLeanFix = Form32MGT<false, SegmentTallyFixed>;
 
 // One bank visit of the HandleAll loop (manager/MonteCarloManagerSerial.hpp:267-383):
 // every active particle runs up to K segments in registers; survivors are
@@ -1545,6 +1557,7 @@ __global__ void __launch_bounds__(256, MINB) k_transport_refill(Ctx C, Bank in, 
         if (has) {
             typename F::Tally tal;
             tal.init(C.eint, C.eradAvg, C.perCellCounters ? C.segs : nullptr);
+            if constexpr (std::is_same_v<typename F::Tally, SegmentTallyFixed>) tal.init_fixed(C);
             uint32_t segs = 0, rws = 0;
             for (uint32_t b = 0; b < burst; ++b) {
                 const uint32_t cell0 = F::cell(t);
@@ -2745,6 +2758,10 @@ __global__ void k_gather(Ctx C, CensusBank src, const uint32_t *idx, uint32_t n,
 // RadiationIMC::postStep (radiation/RadiationIMC.hpp:1887-2029), gray, no hydro.
 __global__ void k_poststep(Ctx C, CellArrays A, OpacityEos M, double dt) {
     for (uint32_t c = blockIdx.x * blockDim.x + threadIdx.x; c < C.ncells; c += gridDim.x * blockDim.x) {
+        if (C.fixMat) {   // reproducible tallies: fold the fixed-point sums of the transport
+            A.eint[c] += fixed_value(C.fixMat, c) * (1.0 / C.fixScaleMat);
+            A.eradAvg[c] += fixed_value(C.fixRad, c) * (1.0 / C.fixScaleRad);
+        }
         A.eradAvg[c] /= (dt * A.vol[c]);
         if (C.egAvg) {   // postStep's group time averages (radiation/RadiationIMC.hpp:1896-1902)
             const double norm = dt * A.vol[c];
@@ -3153,6 +3170,20 @@ void launch_transport_refill(cudaStream_t s, uint32_t grid, int minBlocks, const
         else if (C.withHydro) refill_launch<Form64HydroEg>(s, grid, minBlocks, C, in, n, nextIdx, cen, nCen, burst, maxSegs, st);
         else if (C.withDDMC) refill_launch<Form64FullEg>(s, grid, minBlocks, C, in, n, nextIdx, cen, nCen, burst, maxSegs, st);
         else refill_launch<Form64MGEg>(s, grid, minBlocks, C, in, n, nextIdx, cen, nCen, burst, maxSegs, st);
+        return;
+    }
+    if (C.fixMat) {   // reproducible tallies
+        if (C.fp32 && C.poly && C.withDDMC) refill_launch<Form32PolyDDMCFix>(s, grid, minBlocks, C, in, n, nextIdx, cen, nCen, burst, maxSegs, st);
+        else if (C.fp32 && C.poly) refill_launch<Form32PolyFix>(s, grid, minBlocks, C, in, n, nextIdx, cen, nCen, burst, maxSegs, st);
+        else if (C.fp32 && C.groups >= 2 && C.withDDMC) refill_launch<Form32MGFix>(s, grid, minBlocks, C, in, n, nextIdx, cen, nCen, burst, maxSegs, st);
+        else if (C.fp32 && C.groups >= 2) refill_launch<Form32MGLeanFix>(s, grid, minBlocks, C, in, n, nextIdx, cen, nCen, burst, maxSegs, st);
+        else if (C.fp32 && C.withDDMC) refill_launch<Form32Fix>(s, grid, minBlocks, C, in, n, nextIdx, cen, nCen, burst, maxSegs, st);
+        else if (C.fp32) refill_launch<Form32LeanFix>(s, grid, minBlocks, C, in, n, nextIdx, cen, nCen, burst, maxSegs, st);
+        else if (C.poly && C.withDDMC) refill_launch<Form64PolyDDMCFix>(s, grid, minBlocks, C, in, n, nextIdx, cen, nCen, burst, maxSegs, st);
+        else if (C.poly) refill_launch<Form64PolyFix>(s, grid, minBlocks, C, in, n, nextIdx, cen, nCen, burst, maxSegs, st);
+        else if (C.groups >= 2 && !C.withDDMC) refill_launch<Form64MGFix>(s, grid, minBlocks, C, in, n, nextIdx, cen, nCen, burst, maxSegs, st);
+        else if (C.groups >= 2 || C.withDDMC) refill_launch<Form64FullFix>(s, grid, minBlocks, C, in, n, nextIdx, cen, nCen, burst, maxSegs, st);
+        else refill_launch<Form64Fix>(s, grid, minBlocks, C, in, n, nextIdx, cen, nCen, burst, maxSegs, st);
         return;
     }
     if (C.fp32 && C.poly && C.withDDMC) refill_launch<Form32PolyDDMC>(s, grid, minBlocks, C, in, n, nextIdx, cen, nCen, burst, maxSegs, st);

@@ -123,6 +123,8 @@ struct StormHandle {
     double *dep = nullptr;           // this handle's material deposits of the step (N)
     double4 *vel = nullptr;          // moving material: (vx, vy, vz, gamma) per cell
     double *egAvg = nullptr;         // group time averages (with_eg_time_avg): ncells x groups
+    unsigned long long *fixMat = nullptr, *fixRad = nullptr;   // reproducible tallies: 4 limbs per cell
+    double stepDt = 0.0;             // the dt of the step in progress (storm_cuda_phase_begin)
     double *mom = nullptr;           // moving material: momentum, 3 per cell
     double *xbuf = nullptr;          // exchange buffer (max(2 N, 2 S N, S + N) doubles)
     double *shardWc = nullptr;       // cells' global census weights (N)
@@ -871,6 +873,9 @@ int storm_cuda_create(const StormProblemDesc *d, StormHandle **out) {
     if (d->precision != STORM_PRECISION_FP64 && d->precision != STORM_PRECISION_FP32_TRACK) return STORM_ERR_UNSUPPORTED;
     // moving material: the FP64 form on the Cartesian grid, without DDMC
     if (d->with_hydro && (d->precision != STORM_PRECISION_FP64 || d->mesh || d->with_ddmc)) return STORM_ERR_UNSUPPORTED;
+    // reproducible tallies: the transport's deposit and Erad sums only
+    if (d->reproducible_tallies && (d->with_hydro || (d->with_eg_time_avg && d->groups >= 2) || !d->comb_enabled))
+        return STORM_ERR_UNSUPPORTED;
     if (d->cell_velocity) {
         const uint64_t nv = d->mesh ? d->mesh->ncells : static_cast<uint64_t>(d->nx) * d->ny * d->nz;
         for (uint64_t q = 0; q < 3 * nv; ++q)
@@ -1233,6 +1238,15 @@ int storm_cuda_create(const StormProblemDesc *d, StormHandle **out) {
         ZERO(h->egAvg, static_cast<size_t>(N) * d->groups * sizeof(double));
     }
     C.egAvg = h->egAvg;
+    if (d->reproducible_tallies) {
+        ALLOC(h->fixMat, 4 * static_cast<size_t>(N));
+        ALLOC(h->fixRad, 4 * static_cast<size_t>(N));
+        ZERO(h->fixMat, 4 * static_cast<size_t>(N) * sizeof(unsigned long long));
+        ZERO(h->fixRad, 4 * static_cast<size_t>(N) * sizeof(unsigned long long));
+    }
+    C.fixMat = h->fixMat;
+    C.fixRad = h->fixRad;
+    C.fixScaleMat = C.fixScaleRad = 1.0;
     C.mom = h->mom;
     C.clight = d->clight; C.arad = d->arad; C.sigmaSB = d->sigma_sb; C.kevKelvin = d->kev_kelvin;
     C.rwMinParticle = d->rw_min_particle_optical_depth;
@@ -1301,7 +1315,7 @@ int storm_cuda_destroy(StormHandle *h) {
                   h->runCursor, h->runScan, h->longRuns, h->bucketFlags,
                   h->cfo, h->cfN, h->cfP, h->cfNext, h->cfFace, h->mpx, h->mpy, h->mpz, h->fvo, h->fvi, h->vtx,
                   h->chord, h->cfN32, h->dep, h->xbuf, h->shardWc, h->shardRunW, h->shardStart, h->shardBounds,
-                  h->vel, h->mom, h->ddmcCum32, h->cfA, h->egAvg};
+                  h->vel, h->mom, h->ddmcCum32, h->cfA, h->egAvg, h->fixMat, h->fixRad};
     for (void *p : ps) device_pool().free(p);
     cudaEvent_t evs[] = {h->evStart, h->evTransport0, h->evTransport1, h->evEnd, h->evAfterEmit, h->evAfterComb};
     bool complete = h->stream != nullptr;
@@ -1328,6 +1342,7 @@ int storm_cuda_phase_begin(StormHandle *h, double dt) {
     if (!h || !(dt > 0.0)) return STORM_ERR_INVALID_ARG;
     CK(cudaSetDevice(h->device));
     h->errCode = 0;
+    h->stepDt = dt;
     h->stats = StormStepStats{};
     CK(cudaMemsetAsync(h->dStats, 0, sizeof(DevStats), h->stream));
     CK(cudaMemsetAsync(h->dErr, 0, 4 * sizeof(int32_t), h->stream));
@@ -1493,6 +1508,25 @@ int storm_cuda_phase_transport(StormHandle *h) {
         CK(cudaMemsetAsync(h->dep, 0, sizeof(double) * h->N, h->stream));
         h->C.eint = h->dep;
     }
+    if (h->fixMat) {
+        // reproducible tallies: the step's deposits sum to at most the energy of
+        // its particles, and its Erad contributions to that energy times dt, so
+        // scales that map 4x those bounds below 2^119 keep every partial sum in
+        // the limbs, with a unit of 2^-117 of the bound
+        DevStats d{};
+        CK(read_small(h, &d, h->dStats, sizeof(d)));
+        const double E = std::fabs(d.eCensusIn) + std::fabs(d.eEmitted);
+        auto scale = [](double bound) {
+            if (!(bound > 0.0) || !std::isfinite(bound)) return 1.0;
+            int e = 0;
+            std::frexp(bound, &e);   // bound < 2^e
+            return std::ldexp(1.0, std::min(117 - e, 1000));
+        };
+        h->C.fixScaleMat = scale(E);
+        h->C.fixScaleRad = scale(E * h->stepDt);
+        CK(cudaMemsetAsync(h->fixMat, 0, 4 * sizeof(unsigned long long) * h->N, h->stream));
+        CK(cudaMemsetAsync(h->fixRad, 0, 4 * sizeof(unsigned long long) * h->N, h->stream));
+    }
     CK(cudaEventRecord(h->evTransport0, h->stream));
     CK(cudaMemsetAsync(h->counts, 0, sizeof(uint32_t) * (h->maxRounds + 2), h->stream));
     if (h->desc.per_cell_segment_counters) CK(cudaMemsetAsync(h->segs, 0, sizeof(uint32_t) * h->N, h->stream));
@@ -1504,7 +1538,8 @@ int storm_cuda_phase_transport(StormHandle *h) {
     uint32_t n32 = static_cast<uint32_t>(n0);
     uint32_t *nCen = h->counts + h->maxRounds + 1;
     // the multigroup FP32 form runs only in the refill kernel
-    const bool refill = h->refill || (h->fp32 && h->desc.groups >= 2) || h->C.poly || h->C.withHydro || h->C.egAvg;
+    const bool refill = h->refill || (h->fp32 && h->desc.groups >= 2) || h->C.poly || h->C.withHydro || h->C.egAvg ||
+                        h->C.fixMat;
     if (!refill) CK(cudaMemcpyAsync(h->counts, &n32, sizeof(uint32_t), cudaMemcpyHostToDevice, h->stream));
     if (refill) {
         // one launch carries every history to census, escape or cutoff
@@ -1978,7 +2013,8 @@ int storm_cuda_set_sharding(StormHandle *h, uint32_t shards, uint32_t lo, uint32
     // once per handle, before its first census
     if (!h || shards == 0 || lo >= hi || hi > shards || h->nCensus != 0 || h->dep) return STORM_ERR_INVALID_ARG;
     if (shards > 1 && (!h->desc.comb_enabled || h->desc.comb_kind != STORM_COMB_PLAIN)) return STORM_ERR_INVALID_ARG;
-    if (shards > 1 && (h->C.withHydro || h->C.egAvg)) return STORM_ERR_UNSUPPORTED;   // tallies without an exchange
+    if (shards > 1 && (h->C.withHydro || h->C.egAvg || h->C.fixMat))   // tallies without an exchange
+        return STORM_ERR_UNSUPPORTED;
     CK(cudaSetDevice(h->device));
     h->shards = shards;
     h->shardLo = lo;

@@ -93,6 +93,8 @@ class Problem:
     cell_velocity: np.ndarray = None
     # group time averages (withEgTimeAvg, multigroup problems): per cell and group
     with_eg_time_avg: bool = False
+    # tallies summed in fixed point, so that runs repeat bit for bit
+    reproducible_tallies: bool = False
 
     @property
     def shape(self):
@@ -198,6 +200,7 @@ class Problem:
         d.with_hydro = int(self.with_hydro)
         d.cell_velocity = arr(None if self.cell_velocity is None else np.asarray(self.cell_velocity).reshape(-1))
         d.with_eg_time_avg = int(self.with_eg_time_avg)
+        d.reproducible_tallies = int(self.reproducible_tallies)
         d._keep = keep
         return d
 
