@@ -96,6 +96,7 @@ struct CudaIMCBinding {
     bool withRandomWalk = false, noHydroFeedback = false;
     bool withHydro = false;   // moving material: CellT::velocity and ExtensivesT::momentum (FP64 form)
     bool withEgTimeAvg = false;   // group time averages (multigroup problems): getEgTimeAvg()
+    bool reproducibleTallies = false;   // fixed-point tally sums: runs repeat bit for bit
     double rwMinCellOpticalDepth = 25.0, rwMinParticleOpticalDepth = 5.0;
     bool withDDMC = false, ddmcUseMultigroupPGRW = false;
     double ddmcMinCellOpticalDepth = 15.0, ddmcMinParticleOpticalDepth = 5.0;
@@ -460,6 +461,7 @@ private:
         d.rw_min_cell_optical_depth = binding_.rwMinCellOpticalDepth;
         d.rw_min_particle_optical_depth = binding_.rwMinParticleOpticalDepth;
         d.with_eg_time_avg = binding_.withEgTimeAvg ? 1 : 0;   // kept for multigroup problems, as in the reference
+        d.reproducible_tallies = binding_.reproducibleTallies ? 1 : 0;
         d.with_ddmc = binding_.withDDMC;
         d.ddmc_use_multigroup_pgrw = binding_.ddmcUseMultigroupPGRW;
         d.ddmc_min_cell_optical_depth = binding_.ddmcMinCellOpticalDepth;
