@@ -407,7 +407,30 @@ def link_bandwidth(nbytes=1 << 30):
     return out
 
 
-def mg_run(args):
+def mg_transport_roofline(form, segs, ms_per_step, steps, sm_mhz=None):
+    """The multigroup transport kernel against its binding ceiling: ncu's warp
+    instructions per segment (profiles/transport_issue.json) times the kernel's
+    segments/s, against 148 SMs x 4 schedulers x the SM clock, and its measured
+    DRAM bytes per segment against the copy bandwidth."""
+    kernel = "k_transport_refill<Form32MGLean>" if form == "fp32" else "k_transport_refill<Form64MG>"
+    rate = segs / steps / (ms_per_step / 1e3) if ms_per_step > 0 else 0.0
+    out = {"kernel": kernel, "kernel_ms_per_step": ms_per_step, "segments_per_s_in_kernel": rate}
+    iss = measured_issue(kernel)
+    if iss and rate:
+        clock = (sm_mhz or 1965.0) * 1e6
+        out["issue"] = {"warp_inst_per_segment": iss["warp_inst_per_segment"],
+                        "frac": iss["warp_inst_per_segment"] * rate / (148 * 4 * clock),
+                        "lanes_active_per_inst": iss["thread_inst_per_segment"] / iss["warp_inst_per_segment"],
+                        "sm_mhz": clock / 1e6, "source": iss["capture"]}
+    per_seg, capture = measured_traffic(kernel)
+    if per_seg is not None and rate:
+        peak, src = _peak()
+        out["dram"] = {"bytes_per_segment": per_seg, "achieved_gbs": per_seg * rate / 1e9,
+                       "frac": per_seg * rate / 1e9 / peak, "peak_gbs": peak, "peak_source": src, "source": capture}
+    return out
+
+
+def mg_run(args, sm_mhz=None):
     """The multigroup configuration: a 128^3 unit cube, 64 groups log-spaced over
     [0.01, 100] keV, kappa_g = 100 nu_g^-3 (1 - exp(-nu_g/T)) cm^-1, initial T
     uniform in [0.01, 0.1] keV per cell (seeded), cell emission from the
@@ -427,18 +450,21 @@ def mg_run(args):
                              precision=prec)
         p.per_cell_segment_counters = False
         e = Engine(p)
+        e.set_profiling(True)   # the transport kernel's own CUDA-event time
         for _ in range(2):
             e.step()
-        segs, ms, lat = 0, 0.0, []
+        segs, ms, tms, lat = 0, 0.0, 0.0, []
         for _ in range(args.mg_steps):
             st = e.step()
             segs += st["segments"]
             ms += st["step_ms"]
+            tms += st["transport_ms"]
             lat.append(st["step_ms"])
         out[name] = {"segments_per_s": segs / (ms / 1e3), "ms_per_step": ms / args.mg_steps,
                      "segments_per_step": segs / args.mg_steps, "emitted_per_step": st["emitted_cells"],
                      "census_per_step": st["census_out"], "step_ms_p99": float(np.percentile(lat, 99)),
-                     "device_gb": e.memory_bytes() / 1e9}
+                     "device_gb": e.memory_bytes() / 1e9,
+                     "transport": mg_transport_roofline(name, segs, tms / args.mg_steps, args.mg_steps, sm_mhz)}
         temps[name] = e.cells()["temperature"]
         e.close()
     out["fp32_over_fp64"] = out["fp32"]["segments_per_s"] / out["fp64"]["segments_per_s"]
@@ -583,7 +609,7 @@ def run_storm(args, ws, rank, local, dist):
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline(args.n, 1, steps=1, timed=1)
     serving = serving_run(args) if (rank == 0 and ws == 1 and args.serving_requests > 0) else None
-    multigroup = mg_run(args) if (rank == 0 and ws == 1 and args.mg_steps > 0) else None
+    multigroup = mg_run(args, (ck or {}).get("sm_mhz")) if (rank == 0 and ws == 1 and args.mg_steps > 0) else None
     voronoi = voronoi_run(args) if (rank == 0 and ws == 1 and args.voronoi_steps > 0) else None
     if rank == 0:
         lat = sorted(f32["step_ms"])
