@@ -407,12 +407,11 @@ def link_bandwidth(nbytes=1 << 30):
     return out
 
 
-def mg_transport_roofline(form, segs, ms_per_step, steps, sm_mhz=None):
-    """The multigroup transport kernel against its binding ceiling: ncu's warp
-    instructions per segment (profiles/transport_issue.json) times the kernel's
-    segments/s, against 148 SMs x 4 schedulers x the SM clock, and its measured
-    DRAM bytes per segment against the copy bandwidth."""
-    kernel = "k_transport_refill<Form32MGLean>" if form == "fp32" else "k_transport_refill<Form64MG>"
+def kernel_roofline(kernel, segs, ms_per_step, steps, sm_mhz=None):
+    """A transport kernel against its binding ceiling: ncu's warp instructions
+    per segment (profiles/transport_issue.json) times the kernel's segments/s,
+    against 148 SMs x 4 schedulers x the SM clock, and its measured DRAM bytes
+    per segment against the copy bandwidth."""
     rate = segs / steps / (ms_per_step / 1e3) if ms_per_step > 0 else 0.0
     out = {"kernel": kernel, "kernel_ms_per_step": ms_per_step, "segments_per_s_in_kernel": rate}
     iss = measured_issue(kernel)
@@ -464,7 +463,9 @@ def mg_run(args, sm_mhz=None):
                      "segments_per_step": segs / args.mg_steps, "emitted_per_step": st["emitted_cells"],
                      "census_per_step": st["census_out"], "step_ms_p99": float(np.percentile(lat, 99)),
                      "device_gb": e.memory_bytes() / 1e9,
-                     "transport": mg_transport_roofline(name, segs, tms / args.mg_steps, args.mg_steps, sm_mhz)}
+                     "transport": kernel_roofline("k_transport_refill<Form32MGLean>" if name == "fp32" else
+                                                  "k_transport_refill<Form64MG>", segs, tms / args.mg_steps,
+                                                  args.mg_steps, sm_mhz)}
         temps[name] = e.cells()["temperature"]
         e.close()
     out["fp32_over_fp64"] = out["fp32"]["segments_per_s"] / out["fp64"]["segments_per_s"]
@@ -472,7 +473,7 @@ def mg_run(args, sm_mhz=None):
     return out
 
 
-def voronoi_run(args):
+def voronoi_run(args, sm_mhz=None):
     """Gray IMC on a Voronoi mesh of 2e5 seeded uniform generators in the unit
     cube (about 15 faces per cell; the engine's own builder), per-cell
     lognormal opacity (median 10 1/cm, sigma_ln 1), lognormal initial
@@ -497,18 +498,23 @@ def voronoi_run(args):
                                   precision=prec)
         p.per_cell_segment_counters = False
         e = Engine(p)
+        e.set_profiling(True)   # the transport kernel's own CUDA-event time
         for _ in range(2):
             e.step()
-        segs, ms, lat = 0, 0.0, []
+        segs, ms, tms, lat = 0, 0.0, 0.0, []
         for _ in range(args.voronoi_steps):
             st = e.step()
             segs += st["segments"]
             ms += st["step_ms"]
+            tms += st["transport_ms"]
             lat.append(st["step_ms"])
         out[name] = {"segments_per_s": segs / (ms / 1e3), "ms_per_step": ms / args.voronoi_steps,
                      "segments_per_step": segs / args.voronoi_steps, "emitted_per_step": st["emitted_cells"],
                      "census_per_step": st["census_out"], "step_ms_p99": float(np.percentile(lat, 99)),
-                     "device_gb": e.memory_bytes() / 1e9}
+                     "device_gb": e.memory_bytes() / 1e9,
+                     "transport": kernel_roofline("k_transport_refill<Form32Poly>" if name == "fp32" else
+                                                  "k_transport_refill<Form64Poly>", segs,
+                                                  tms / args.voronoi_steps, args.voronoi_steps, sm_mhz)}
         temps[name] = e.cells()["temperature"]
         e.close()
     out["fp32_over_fp64"] = out["fp32"]["segments_per_s"] / out["fp64"]["segments_per_s"]
@@ -610,7 +616,7 @@ def run_storm(args, ws, rank, local, dist):
         cpu = cpu_baseline(args.n, 1, steps=1, timed=1)
     serving = serving_run(args) if (rank == 0 and ws == 1 and args.serving_requests > 0) else None
     multigroup = mg_run(args, (ck or {}).get("sm_mhz")) if (rank == 0 and ws == 1 and args.mg_steps > 0) else None
-    voronoi = voronoi_run(args) if (rank == 0 and ws == 1 and args.voronoi_steps > 0) else None
+    voronoi = voronoi_run(args, (ck or {}).get("sm_mhz")) if (rank == 0 and ws == 1 and args.voronoi_steps > 0) else None
     if rank == 0:
         lat = sorted(f32["step_ms"])
         line = {
