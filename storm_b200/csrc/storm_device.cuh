@@ -147,6 +147,12 @@ struct Ctx {
     const double *chord;     // per cell: 4 V / S
     const float4 *cfN32;     // FP32 form, per cell-face slot: inward unit normal and the distance of the
                              // cell's mesh point from the face plane, (mesh point - faceCM).n
+    // polyhedral cell emission: each cell's fan tetrahedra in the sampler's order
+    // (faces in GetCellFaces order, triangles (v0, v_t, v_t+1)) with their running
+    // volume sums, and each tetrahedron's (first, t) offsets into fvi
+    const uint32_t *tetOff;  // per cell: its first tetrahedron (ncells + 1)
+    const double *tetCum;
+    const uint2 *tetAT;
 };
 
 // ------------------------------------------------------------------ errors

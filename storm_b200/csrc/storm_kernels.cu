@@ -878,30 +878,48 @@ __device__ __forceinline__ double poly_tet_volume(const Ctx &C, uint32_t v0, uin
 template <class RNG>
 __device__ inline void sample_in_poly_cell(const Ctx &C, uint32_t cell, RNG &rng, double &px, double &py, double &pz) {
     const double cx = C.mpx[cell], cy = C.mpy[cell], cz = C.mpz[cell];
-    const uint32_t k0 = C.cfo[cell], k1 = C.cfo[cell + 1];
-    double total = 0.0;
-    uint32_t ntri = 0;
-    for (uint32_t q = k0; q < k1; ++q) {
-        const uint32_t f = C.cfFace[q], a = C.fvo[f], b = C.fvo[f + 1];
-        if (b - a < 3) continue;
-        for (uint32_t t = a + 1; t + 1 < b; ++t) {
-            total += poly_tet_volume(C, C.fvi[a], C.fvi[t], C.fvi[t + 1], cx, cy, cz);
-            ++ntri;
-        }
-    }
-    if (ntri == 0) { px = cx; py = cy; pz = cz; return; }
-    const double r = rng.raw() * total;
-    // the first triangle whose running sum is not below r, else the last
     uint32_t v0 = 0, v1 = 0, v2 = 0;
-    bool found = false;
-    double run = 0.0;
-    for (uint32_t q = k0; q < k1 && !found; ++q) {
-        const uint32_t f = C.cfFace[q], a = C.fvo[f], b = C.fvo[f + 1];
-        if (b - a < 3) continue;
-        for (uint32_t t = a + 1; t + 1 < b; ++t) {
-            run += poly_tet_volume(C, C.fvi[a], C.fvi[t], C.fvi[t + 1], cx, cy, cz);
-            v0 = C.fvi[a]; v1 = C.fvi[t]; v2 = C.fvi[t + 1];
-            if (!(run < r)) { found = true; break; }
+    if (C.tetCum) {
+        // the running sums of the mesh's tetrahedron table (k_poly_tets): the
+        // same numbers as the two passes below, looked up instead of summed
+        const uint32_t k0 = C.tetOff[cell], k1 = C.tetOff[cell + 1];
+        if (k0 == k1) { px = cx; py = cy; pz = cz; return; }
+        const double r = rng.raw() * C.tetCum[k1 - 1];
+        // the first tetrahedron whose running sum is not below r, else the last:
+        // !(sum < r) holds from some index on, since the sums never decrease and
+        // a NaN sum stays NaN
+        uint32_t lo = k0, hi = k1 - 1;
+        while (lo < hi) {
+            const uint32_t mid = (lo + hi) >> 1;
+            if (C.tetCum[mid] < r) lo = mid + 1; else hi = mid;
+        }
+        const uint2 at = C.tetAT[lo];
+        v0 = C.fvi[at.x]; v1 = C.fvi[at.y]; v2 = C.fvi[at.y + 1];
+    } else {
+        const uint32_t k0 = C.cfo[cell], k1 = C.cfo[cell + 1];
+        double total = 0.0;
+        uint32_t ntri = 0;
+        for (uint32_t q = k0; q < k1; ++q) {
+            const uint32_t f = C.cfFace[q], a = C.fvo[f], b = C.fvo[f + 1];
+            if (b - a < 3) continue;
+            for (uint32_t t = a + 1; t + 1 < b; ++t) {
+                total += poly_tet_volume(C, C.fvi[a], C.fvi[t], C.fvi[t + 1], cx, cy, cz);
+                ++ntri;
+            }
+        }
+        if (ntri == 0) { px = cx; py = cy; pz = cz; return; }
+        const double r = rng.raw() * total;
+        // the first triangle whose running sum is not below r, else the last
+        bool found = false;
+        double run = 0.0;
+        for (uint32_t q = k0; q < k1 && !found; ++q) {
+            const uint32_t f = C.cfFace[q], a = C.fvo[f], b = C.fvo[f + 1];
+            if (b - a < 3) continue;
+            for (uint32_t t = a + 1; t + 1 < b; ++t) {
+                run += poly_tet_volume(C, C.fvi[a], C.fvi[t], C.fvi[t + 1], cx, cy, cz);
+                v0 = C.fvi[a]; v1 = C.fvi[t]; v2 = C.fvi[t + 1];
+                if (!(run < r)) { found = true; break; }
+            }
         }
     }
     double s = rng.raw(), t = rng.raw(), u = rng.raw(), tmp;
@@ -912,6 +930,28 @@ __device__ inline void sample_in_poly_cell(const Ctx &C, uint32_t cell, RNG &rng
     px = a0 * C.vtx[3 * v0] + a1 * C.vtx[3 * v1] + a2 * C.vtx[3 * v2] + a3 * cx;
     py = a0 * C.vtx[3 * v0 + 1] + a1 * C.vtx[3 * v1 + 1] + a2 * C.vtx[3 * v2 + 1] + a3 * cy;
     pz = a0 * C.vtx[3 * v0 + 2] + a1 * C.vtx[3 * v1 + 2] + a2 * C.vtx[3 * v2 + 2] + a3 * cz;
+}
+
+// The table sample_in_poly_cell looks up: per cell its fan tetrahedra in the
+// sampler's order, each with the running sum of the volumes up to it, formed by
+// the sampler's own operations in its order (so equal to its sums bit for bit),
+// and its (first, t) offsets into fvi.  tetOff comes from the host.
+__global__ void k_poly_tets(Ctx C, const uint32_t *tetOff, double *tetCum, uint2 *tetAT) {
+    for (uint32_t cell = blockIdx.x * blockDim.x + threadIdx.x; cell < C.ncells; cell += gridDim.x * blockDim.x) {
+        const double cx = C.mpx[cell], cy = C.mpy[cell], cz = C.mpz[cell];
+        uint32_t o = tetOff[cell];
+        double total = 0.0;
+        for (uint32_t q = C.cfo[cell]; q < C.cfo[cell + 1]; ++q) {
+            const uint32_t f = C.cfFace[q], a = C.fvo[f], b = C.fvo[f + 1];
+            if (b - a < 3) continue;
+            for (uint32_t t = a + 1; t + 1 < b; ++t) {
+                total += poly_tet_volume(C, C.fvi[a], C.fvi[t], C.fvi[t + 1], cx, cy, cz);
+                tetCum[o] = total;
+                tetAT[o] = make_uint2(a, t);
+                ++o;
+            }
+        }
+    }
 }
 
 // the cell's mesh point (GetMeshPoint)
@@ -2965,6 +3005,9 @@ void launch_emit_cells(cudaStream_t s, const Ctx &C, const CellArrays &A, const 
     else
         k_emit_cells<<<grid_for(count, 256, 148 * 16), 256, 0, s>>>(C, A, offsets, eBegin, count, b, bankBase, pidBase,
                                                                     dt, st);
+}
+void launch_poly_tets(cudaStream_t s, const Ctx &C, const uint32_t *tetOff, double *tetCum, uint2 *tetAT) {
+    k_poly_tets<<<grid_for(C.ncells, 128, 8192), 128, 0, s>>>(C, tetOff, tetCum, tetAT);
 }
 void launch_emit_faces(cudaStream_t s, const Ctx &C, const FaceSources &F, uint64_t fBegin, uint64_t count,
                        const Bank &b, uint32_t bankBase, uint32_t pidBase, double dt, DevStats *st) {

@@ -69,6 +69,9 @@ struct StormHandle {
     double4 *cfN = nullptr, *cfP = nullptr;
     double *mpx = nullptr, *mpy = nullptr, *mpz = nullptr, *vtx = nullptr, *chord = nullptr;
     float4 *cfN32 = nullptr;
+    uint32_t *tetOff = nullptr;  // polyhedral emission: the cells' fan tetrahedra (k_poly_tets)
+    double *tetCum = nullptr;
+    uint2 *tetAT = nullptr;
     StratParams strat{1, nullptr, 2};         // stratified comb: bins, device bounds, minParticlesPerGroup
     double *stratBounds = nullptr, *stratBinW = nullptr;
     uint32_t *stratStart = nullptr;
@@ -1054,6 +1057,25 @@ int storm_cuda_create(const StormProblemDesc *d, StormHandle **out) {
         H2D(h->fvo, mesh->face_vertex_offset, mesh->nfaces + 1);
         H2D(h->fvi, mesh->face_vertices, FV);
         H2D(h->vtx, mesh->vertices, 3 * static_cast<size_t>(NV));
+        {   // the emission sampler's tetrahedron table: its offsets here, its sums on the device
+            std::vector<uint32_t> toff(static_cast<size_t>(N) + 1);
+            uint64_t nt = 0;
+            for (uint32_t c = 0; c < N; ++c) {
+                toff[c] = static_cast<uint32_t>(nt);
+                for (uint32_t q = mesh->cell_face_offset[c]; q < mesh->cell_face_offset[c + 1]; ++q) {
+                    const uint32_t nv = mesh->face_vertex_offset[facev[q] + 1] - mesh->face_vertex_offset[facev[q]];
+                    if (nv >= 3) nt += nv - 2;
+                }
+                if (nt > 0xFFFFFFFFull) break;
+            }
+            if (nt > 0 && nt <= 0xFFFFFFFFull) {   // else the sampler sums the volumes itself
+                toff[N] = static_cast<uint32_t>(nt);
+                ALLOC(h->tetOff, static_cast<size_t>(N) + 1);
+                ALLOC(h->tetCum, nt);
+                ALLOC(h->tetAT, nt);
+                H2D(h->tetOff, toff.data(), static_cast<size_t>(N) + 1);
+            }
+        }
         if (d->precision == STORM_PRECISION_FP32_TRACK) {
             // the FP32 form's planes: inward normal and the mesh point's distance from the plane
             std::vector<float4> pl(K);
@@ -1153,6 +1175,11 @@ int storm_cuda_create(const StormProblemDesc *d, StormHandle **out) {
         C.cfo = h->cfo; C.cfN = h->cfN; C.cfP = h->cfP; C.cfNext = h->cfNext; C.cfFace = h->cfFace; C.cfA = h->cfA;
         C.mpx = h->mpx; C.mpy = h->mpy; C.mpz = h->mpz;
         C.fvo = h->fvo; C.fvi = h->fvi; C.vtx = h->vtx; C.chord = h->chord; C.cfN32 = h->cfN32;
+        if (h->tetCum) {
+            launch_poly_tets(h->stream, C, h->tetOff, h->tetCum, h->tetAT);
+            if (cudaGetLastError() != cudaSuccess) return fail(STORM_ERR_CUDA);
+            C.tetOff = h->tetOff; C.tetCum = h->tetCum; C.tetAT = h->tetAT;
+        }
     }
     C.xe = h->xe; C.ye = h->ye; C.ze = h->ze; C.xc = h->xc; C.yc = h->yc; C.zc = h->zc;
     C.X0 = h->hxe.front(); C.X1 = h->hxe.back();
@@ -1315,7 +1342,8 @@ int storm_cuda_destroy(StormHandle *h) {
                   h->runCursor, h->runScan, h->longRuns, h->bucketFlags,
                   h->cfo, h->cfN, h->cfP, h->cfNext, h->cfFace, h->mpx, h->mpy, h->mpz, h->fvo, h->fvi, h->vtx,
                   h->chord, h->cfN32, h->dep, h->xbuf, h->shardWc, h->shardRunW, h->shardStart, h->shardBounds,
-                  h->vel, h->mom, h->ddmcCum32, h->cfA, h->egAvg, h->fixMat, h->fixRad};
+                  h->vel, h->mom, h->ddmcCum32, h->cfA, h->egAvg, h->fixMat, h->fixRad, h->tetOff, h->tetCum,
+                  h->tetAT};
     for (void *p : ps) device_pool().free(p);
     cudaEvent_t evs[] = {h->evStart, h->evTransport0, h->evTransport1, h->evEnd, h->evAfterEmit, h->evAfterComb};
     bool complete = h->stream != nullptr;

@@ -91,6 +91,69 @@ def test_voronoi_cell_emission_inside_and_uniform():
     e.close()
 
 
+def _two_pass_point(mesh, c, u):
+    """RandomInCellPositionSampler on polyhedral cell c (utils/RandomInCell.hpp:11-67)
+    from draws u[0..3], summing the fan tetrahedra's volumes twice as the
+    reference does: the total, then the running sum up to the picked one."""
+    cx, cy, cz = (float(v) for v in mesh.points[c])
+    V = mesh.vertices
+    tets = []
+    for f in mesh.cell_faces[mesh.cell_face_offset[c]:mesh.cell_face_offset[c + 1]]:
+        a, b = int(mesh.face_vertex_offset[f]), int(mesh.face_vertex_offset[f + 1])
+        for t in range(a + 1, b - 1):
+            tets.append((int(mesh.face_vertices[a]), int(mesh.face_vertices[t]), int(mesh.face_vertices[t + 1])))
+
+    def vol(v0, v1, v2):
+        ax, ay, az = V[v0, 0] - cx, V[v0, 1] - cy, V[v0, 2] - cz
+        bx, by, bz = V[v1, 0] - cx, V[v1, 1] - cy, V[v1, 2] - cz
+        ex, ey, ez = V[v2, 0] - cx, V[v2, 1] - cy, V[v2, 2] - cz
+        crx, cry, crz = by * ez - bz * ey, bz * ex - bx * ez, bx * ey - by * ex
+        return abs(ax * crx + ay * cry + az * crz)
+
+    total = 0.0
+    for tt in tets:
+        total += vol(*tt)
+    r = u[0] * total
+    run, pick = 0.0, tets[-1]
+    for tt in tets:
+        run += vol(*tt)
+        if not run < r:
+            pick = tt
+            break
+    s, t, w = sorted((u[1], u[2], u[3]))
+    a0, a1, a2, a3 = s, t - s, w - t, 1 - w
+    v0, v1, v2 = (V[k] for k in pick)
+    return tuple(a0 * v0[d] + a1 * v1[d] + a2 * v2[d] + a3 * (cx, cy, cz)[d] for d in range(3))
+
+
+def test_voronoi_cell_emission_matches_two_pass_sampler(oracle_lib):
+    """The device looks the picked tetrahedron up in the mesh's table of running
+    volume sums; on the same Philox draws (stream TAG_CELL_EMIT, draws 0-3) the
+    positions equal the two-pass sum's bit for bit."""
+    mesh = build_voronoi(np.random.default_rng(7).random((40, 3)) * 0.98 + 0.01)
+    p = problems.voronoi_cube(ncells=40, packets_per_step=4e3, seed=11, mesh=mesh)
+    e = Engine(p)
+    e.phase("begin", p.dt)
+    e.phase("prestep", p.dt)
+    e.phase("emit", p.dt)
+    b, st = e.bank(), e.stats()
+    e.close()
+    n0, ne = int(st["census_in"]), int(st["emitted_cells"])
+    assert n0 == 0 and ne > 1000
+    box = mesh.box
+    checked = 0
+    for j in range(ne):
+        q = n0 + j
+        pid = int(b.id[q])
+        u = [oracle_lib.uniform(p.seed, 2, 0, pid, d) for d in range(4)]
+        x, y, z = _two_pass_point(mesh, int(b.cell[q]), u)
+        if not (box[0] <= x <= box[3] and box[1] <= y <= box[4] and box[2] <= z <= box[5]):
+            continue   # moved inside by the outside-box repair
+        assert (b.x[q], b.y[q], b.z[q]) == (x, y, z), (j, pid)
+        checked += 1
+    assert checked > 0.99 * ne
+
+
 def _balance(st):
     src = st["energy_census_in"] + st["energy_emitted"]
     sink = st["energy_deposited"] + st["energy_escaped"] + st["energy_census_pre_comb"]
