@@ -109,7 +109,7 @@ void launch_emit_cells(cudaStream_t s, const Ctx &C, const CellArrays &A, const 
                        uint64_t count, const Bank &b, uint32_t bankBase, uint32_t pidBase, double dt, DevStats *st);
 void launch_ddmc_rates(cudaStream_t s, const Ctx &C, const CellArrays &A);
 void launch_strat_keys(cudaStream_t s, const Ctx &C, const CensusBank &cen, uint32_t n, uint64_t *keys, uint32_t *vals,
-                       uint32_t combKey, int pidBits, const StratParams &S);
+                       uint32_t combKey, int pidBits, const StratParams &S, double *wc = nullptr);
 void launch_strat_sums(cudaStream_t s, const double *wS, const uint32_t *start, uint32_t ncells, uint32_t bins,
                        double *binW, double *cellW);
 void launch_strat_plan(cudaStream_t s, const Ctx &C, const CombParams &P, const StratParams &S, const double *wS,
@@ -129,7 +129,7 @@ int refill_blocks_per_sm(int minBlocks, bool fp32);
 void launch_bank_to_local(cudaStream_t s, const Ctx &C, const Bank &src, const Bank &dst, uint32_t n);
 void launch_bank_to_global(cudaStream_t s, const Ctx &C, const Bank &src, const Bank &dst, uint32_t n);
 void launch_comb_keys(cudaStream_t s, const Ctx &C, const CensusBank &cen, uint32_t n, uint64_t *keys, uint32_t *vals,
-                      uint32_t combKey, int pidBits);
+                      uint32_t combKey, int pidBits, double *wc = nullptr);
 int launch_radix_sort(cudaStream_t s, uint64_t *keys, uint32_t *vals, uint64_t *keysAlt, uint32_t *valsAlt, uint32_t n,
                       int bits, uint32_t *tileHist);
 uint32_t radix_tile_count(uint32_t n);
@@ -137,7 +137,7 @@ void launch_comb_ranges(cudaStream_t s, const uint64_t *keys, uint32_t n, uint32
 void launch_bucket_sort(cudaStream_t s, const Ctx &C, const CensusBank &cen, const uint64_t *keys, uint32_t n,
                         int pidBits, uint32_t nRuns, uint32_t *start, uint32_t *cursor, uint64_t *scanSums,
                         uint64_t *outKeys, uint32_t *outVals, double *wS, uint32_t *longRuns, uint32_t longCap,
-                        uint32_t *flags);
+                        uint32_t *flags, const double *wc = nullptr);
 void launch_mask_count_upto(cudaStream_t s, const uint32_t *pCount, uint32_t n, const uint32_t *nValid, uint64_t *out);
 size_t bucket_scan_words(uint32_t len);
 uint32_t bucket_long_capacity(uint32_t n);

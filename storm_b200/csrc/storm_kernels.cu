@@ -1697,9 +1697,10 @@ __device__ __forceinline__ uint32_t cell_of_run(const Ctx &C, uint64_t run, uint
 }
 
 __global__ void k_comb_keys(Ctx C, CensusBank cen, uint32_t n, uint64_t *keys, uint32_t *vals, uint32_t combKey,
-                            int pidBits) {
+                            int pidBits, double *wc) {
     for (uint32_t q = blockIdx.x * blockDim.x + threadIdx.x; q < n; q += gridDim.x * blockDim.x) {
         const double w = census_w(C, cen, q);
+        if (wc) wc[q] = w;
         const uint2 cp = census_cell_pid(C, cen, q);
         const uint32_t pid = cp.y;
         uint32_t cell = cp.x;
@@ -1880,25 +1881,48 @@ __global__ void k_bucket_count(const uint64_t *keys, uint32_t n, int pidBits, ui
     }
 }
 
-// (key, q) to the next free slot of its run's range: cursor[r] starts at the run's first position
+// The census weight of particle q for the sorted-weight array: from the key
+// kernel's compact copy wc (8 bytes a particle, read back mostly from L2), or
+// from the particle's record when there is none.
+__device__ __forceinline__ double run_w(const Ctx &C, const CensusBank &cen, const double *wc, uint32_t q) {
+    return wc ? wc[q] : census_w(C, cen, q);
+}
+
+// (key, q) to the next free slot of its run's range: cursor[r] starts at the run's first position.
+// Each thread places PLACE_ILP keys per pass, their cursor atomics issued
+// together, so that their round trips overlap.
+constexpr int PLACE_ILP = 4;
 __global__ void k_bucket_place(const uint64_t *keys, uint32_t n, int pidBits, uint32_t nRuns, uint32_t *cursor,
                                uint64_t *outKeys, uint32_t *outVals) {
     const unsigned lane = threadIdx.x & 31;
     const unsigned lt = lanemask_lt();
-    for (uint32_t base = blockIdx.x * blockDim.x; base < n; base += gridDim.x * blockDim.x) {
-        const uint32_t q = base + threadIdx.x;
-        const bool ok = q < n;
-        const uint64_t k = ok ? keys[q] : 0ull;
-        const uint32_t run = ok ? bucket_run(k, pidBits, nRuns) : 0xFFFFFFFFu;
-        const unsigned m = __match_any_sync(FULL, run);
-        const int leader = __ffs(m) - 1;
-        uint32_t b = 0;
-        if (ok && static_cast<int>(lane) == leader) b = atomicAdd(&cursor[run], static_cast<uint32_t>(__popc(m)));
-        b = __shfl_sync(FULL, b, leader);
-        if (ok) {
-            const uint32_t slot = b + static_cast<uint32_t>(__popc(m & lt));
-            outKeys[slot] = k;
-            outVals[slot] = q;
+    const uint32_t stride = gridDim.x * blockDim.x;
+    for (uint64_t base = blockIdx.x * blockDim.x; base < n; base += static_cast<uint64_t>(PLACE_ILP) * stride) {
+        uint32_t q[PLACE_ILP], run[PLACE_ILP], b[PLACE_ILP];
+        uint64_t k[PLACE_ILP];
+        unsigned m[PLACE_ILP];
+#pragma unroll
+        for (int u = 0; u < PLACE_ILP; ++u) {
+            const uint64_t qq = base + static_cast<uint64_t>(u) * stride + threadIdx.x;
+            q[u] = static_cast<uint32_t>(qq);
+            k[u] = qq < n ? keys[qq] : 0ull;
+            run[u] = qq < n ? bucket_run(k[u], pidBits, nRuns) : 0xFFFFFFFFu;
+        }
+#pragma unroll
+        for (int u = 0; u < PLACE_ILP; ++u) {
+            m[u] = __match_any_sync(FULL, run[u]);
+            b[u] = 0;
+            if (run[u] != 0xFFFFFFFFu && static_cast<int>(lane) == __ffs(m[u]) - 1)
+                b[u] = atomicAdd(&cursor[run[u]], static_cast<uint32_t>(__popc(m[u])));
+        }
+#pragma unroll
+        for (int u = 0; u < PLACE_ILP; ++u) {
+            const uint32_t bb = __shfl_sync(FULL, b[u], __ffs(m[u]) - 1);
+            if (run[u] != 0xFFFFFFFFu) {
+                const uint32_t slot = bb + static_cast<uint32_t>(__popc(m[u] & lt));
+                outKeys[slot] = k[u];
+                outVals[slot] = q[u];
+            }
         }
     }
 }
@@ -1979,8 +2003,8 @@ __device__ __forceinline__ void warp_bitonic(uint64_t (&v)[E], uint32_t lane) {
 // census weight of each sorted particle goes to wS.
 template <int E>
 __device__ __forceinline__ void warp_sort_run(const Ctx &C, const CensusBank &cen, uint64_t *keys, uint32_t *vals,
-                                              double *wS, uint32_t b, uint32_t len, uint32_t r, int pidBits,
-                                              uint64_t hashMask, uint32_t lane) {
+                                              double *wS, const double *wc, uint32_t b, uint32_t len, uint32_t r,
+                                              int pidBits, uint64_t hashMask, uint32_t lane) {
     uint64_t v[E];
 #pragma unroll
     for (int e = 0; e < E; ++e) {
@@ -1995,7 +2019,7 @@ __device__ __forceinline__ void warp_sort_run(const Ctx &C, const CensusBank &ce
             const uint32_t q = static_cast<uint32_t>(v[e]);
             keys[b + i] = (static_cast<uint64_t>(r) << pidBits) | (v[e] >> 32);
             vals[b + i] = q;
-            wS[b + i] = census_w(C, cen, q);
+            wS[b + i] = run_w(C, cen, wc, q);
         }
     }
 }
@@ -2005,8 +2029,8 @@ __device__ __forceinline__ void warp_sort_run(const Ctx &C, const CensusBank &ce
 // keys: in registers up to 128 (fully unrolled networks; larger ones would not
 // fit the instruction cache), in the warp's shared memory above.  Longer runs
 // are listed for k_bucket_sort_long.
-__global__ void __launch_bounds__(32 * BUCKET_WARPS) k_bucket_sort_runs(Ctx C, CensusBank cen, uint64_t *keys,
-                                                                        uint32_t *vals, double *wS,
+__global__ void __launch_bounds__(32 * BUCKET_WARPS) k_bucket_sort_runs(Ctx C, CensusBank cen, const double *wc,
+                                                                        uint64_t *keys, uint32_t *vals, double *wS,
                                                                         const uint32_t *start, uint32_t nRuns,
                                                                         int pidBits, uint32_t *longRuns,
                                                                         uint32_t *nLong, uint32_t longCap) {
@@ -2019,13 +2043,13 @@ __global__ void __launch_bounds__(32 * BUCKET_WARPS) k_bucket_sort_runs(Ctx C, C
         const uint32_t b = start[r], len = start[r + 1] - b;
         if (len == 0) continue;
         if (len == 1) {
-            if (lane == 0) wS[b] = census_w(C, cen, vals[b]);
+            if (lane == 0) wS[b] = run_w(C, cen, wc, vals[b]);
         } else if (len <= 32) {
-            warp_sort_run<1>(C, cen, keys, vals, wS, b, len, r, pidBits, hashMask, lane);
+            warp_sort_run<1>(C, cen, keys, vals, wS, wc, b, len, r, pidBits, hashMask, lane);
         } else if (len <= 64) {
-            warp_sort_run<2>(C, cen, keys, vals, wS, b, len, r, pidBits, hashMask, lane);
+            warp_sort_run<2>(C, cen, keys, vals, wS, wc, b, len, r, pidBits, hashMask, lane);
         } else if (len <= 128) {
-            warp_sort_run<4>(C, cen, keys, vals, wS, b, len, r, pidBits, hashMask, lane);
+            warp_sort_run<4>(C, cen, keys, vals, wS, wc, b, len, r, pidBits, hashMask, lane);
         } else if (len <= BUCKET_WARP_MAX) {
             uint32_t P = 256;
             while (P < len) P <<= 1;
@@ -2038,7 +2062,7 @@ __global__ void __launch_bounds__(32 * BUCKET_WARPS) k_bucket_sort_runs(Ctx C, C
                 const uint32_t q = static_cast<uint32_t>(v);
                 keys[b + i] = (static_cast<uint64_t>(r) << pidBits) | (v >> 32);
                 vals[b + i] = q;
-                wS[b + i] = census_w(C, cen, q);
+                wS[b + i] = run_w(C, cen, wc, q);
             }
             __syncwarp();
         } else if (lane == 0) {
@@ -2050,7 +2074,8 @@ __global__ void __launch_bounds__(32 * BUCKET_WARPS) k_bucket_sort_runs(Ctx C, C
 
 // The listed runs, one block each (dynamic shared memory: BUCKET_BLOCK_MAX words).
 // A run longer than BUCKET_BLOCK_MAX, or more listed runs than longCap, sets *tooLong.
-__global__ void __launch_bounds__(256) k_bucket_sort_long(Ctx C, CensusBank cen, uint64_t *keys, uint32_t *vals,
+__global__ void __launch_bounds__(256) k_bucket_sort_long(Ctx C, CensusBank cen, const double *wc, uint64_t *keys,
+                                                          uint32_t *vals,
                                                           double *wS, const uint32_t *start, int pidBits,
                                                           const uint32_t *longRuns, const uint32_t *nLong,
                                                           uint32_t longCap, uint32_t *tooLong) {
@@ -2080,7 +2105,7 @@ __global__ void __launch_bounds__(256) k_bucket_sort_long(Ctx C, CensusBank cen,
             const uint32_t q = static_cast<uint32_t>(v);
             keys[b + i] = (static_cast<uint64_t>(r) << pidBits) | (v >> 32);
             vals[b + i] = q;
-            wS[b + i] = census_w(C, cen, q);
+            wS[b + i] = run_w(C, cen, wc, q);
         }
         __syncthreads();
     }
@@ -2595,9 +2620,10 @@ __device__ __forceinline__ uint32_t strat_bin(const StratParams &S, double nu) {
 }
 
 __global__ void k_strat_keys(Ctx C, CensusBank cen, uint32_t n, uint64_t *keys, uint32_t *vals, uint32_t combKey,
-                             int pidBits, StratParams S) {
+                             int pidBits, StratParams S, double *wc) {
     for (uint32_t q = blockIdx.x * blockDim.x + threadIdx.x; q < n; q += gridDim.x * blockDim.x) {
         const double w = census_w(C, cen, q);
+        if (wc) wc[q] = w;
         const uint2 cp = census_cell_pid(C, cen, q);
         const uint32_t pid = cp.y;
         uint32_t cell = cp.x;
@@ -3016,8 +3042,8 @@ void launch_emit_faces(cudaStream_t s, const Ctx &C, const FaceSources &F, uint6
 }
 void launch_face_spectra(cudaStream_t s, const Ctx &C, double *cdf) { k_face_spectra<<<1, 32, 0, s>>>(C, cdf); }
 void launch_strat_keys(cudaStream_t s, const Ctx &C, const CensusBank &cen, uint32_t n, uint64_t *keys, uint32_t *vals,
-                       uint32_t combKey, int pidBits, const StratParams &S) {
-    k_strat_keys<<<grid_for(n, 256, 148 * 16), 256, 0, s>>>(C, cen, n, keys, vals, combKey, pidBits, S);
+                       uint32_t combKey, int pidBits, const StratParams &S, double *wc) {
+    k_strat_keys<<<grid_for(n, 256, 148 * 16), 256, 0, s>>>(C, cen, n, keys, vals, combKey, pidBits, S, wc);
 }
 void launch_strat_sums(cudaStream_t s, const double *wS, const uint32_t *start, uint32_t ncells, uint32_t bins,
                        double *binW, double *cellW) {
@@ -3067,8 +3093,8 @@ int transport_blocks_per_sm(int minBlocks, bool fp32) {
     return nb;
 }
 void launch_comb_keys(cudaStream_t s, const Ctx &C, const CensusBank &cen, uint32_t n, uint64_t *keys, uint32_t *vals,
-                      uint32_t combKey, int pidBits) {
-    k_comb_keys<<<grid_for(n, 256, 8192), 256, 0, s>>>(C, cen, n, keys, vals, combKey, pidBits);
+                      uint32_t combKey, int pidBits, double *wc) {
+    k_comb_keys<<<grid_for(n, 256, 8192), 256, 0, s>>>(C, cen, n, keys, vals, combKey, pidBits, wc);
 }
 int launch_radix_sort(cudaStream_t s, uint64_t *keys, uint32_t *vals, uint64_t *keysAlt, uint32_t *valsAlt, uint32_t n,
                       int bits, uint32_t *tileHist) {
@@ -3104,7 +3130,7 @@ int launch_radix_sort(cudaStream_t s, uint64_t *keys, uint32_t *vals, uint64_t *
 void launch_bucket_sort(cudaStream_t s, const Ctx &C, const CensusBank &cen, const uint64_t *keys, uint32_t n,
                         int pidBits, uint32_t nRuns, uint32_t *start, uint32_t *cursor, uint64_t *scanSums,
                         uint64_t *outKeys, uint32_t *outVals, double *wS, uint32_t *longRuns, uint32_t longCap,
-                        uint32_t *flags) {
+                        uint32_t *flags, const double *wc) {
     const uint32_t len = nRuns + 1;
     cudaMemsetAsync(start, 0, sizeof(uint32_t) * len, s);
     cudaMemsetAsync(flags, 0, 2 * sizeof(uint32_t), s);
@@ -3116,11 +3142,11 @@ void launch_bucket_sort(cudaStream_t s, const Ctx &C, const CensusBank &cen, con
     cudaMemcpyAsync(cursor, start, sizeof(uint32_t) * len, cudaMemcpyDeviceToDevice, s);
     k_bucket_place<<<grid_for(n, 256, 148 * 16), 256, 0, s>>>(keys, n, pidBits, nRuns, cursor, outKeys, outVals);
     k_bucket_sort_runs<<<grid_for(nRuns, BUCKET_WARPS, 148 * 32), 32 * BUCKET_WARPS, 0, s>>>(
-        C, cen, outKeys, outVals, wS, start, nRuns, pidBits, longRuns, flags, longCap);
+        C, cen, wc, outKeys, outVals, wS, start, nRuns, pidBits, longRuns, flags, longCap);
     const size_t smem = sizeof(uint64_t) * BUCKET_BLOCK_MAX;
     cudaFuncSetAttribute(k_bucket_sort_long, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
-    k_bucket_sort_long<<<148, 256, smem, s>>>(C, cen, outKeys, outVals, wS, start, pidBits, longRuns, flags, longCap,
-                                              flags + 1);
+    k_bucket_sort_long<<<148, 256, smem, s>>>(C, cen, wc, outKeys, outVals, wS, start, pidBits, longRuns, flags,
+                                              longCap, flags + 1);
 }
 size_t bucket_scan_words(uint32_t len) { return (len + 1023) / 1024 + 2; }
 uint32_t bucket_long_capacity(uint32_t n) { return n / (BUCKET_WARP_MAX + 1) + 1; }

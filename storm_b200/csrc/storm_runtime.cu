@@ -1866,8 +1866,11 @@ int storm_cuda_phase_comb(StormHandle *h) {
     const uint32_t B = strat ? h->strat.bins : 1u;
     const uint64_t nRuns = static_cast<uint64_t>(N) * B;
     uint32_t *start = strat ? h->stratStart : h->combStart;
-    if (strat) launch_strat_keys(h->stream, h->C, h->bankC, n, h->keys, h->vals, combKey, pidBits, h->strat);
-    else launch_comb_keys(h->stream, h->C, h->bankC, n, h->keys, h->vals, combKey, pidBits);
+    // the key kernel's compact copy of the census weights, for the bucket sort's
+    // sorted-weight gather; the plan's output offsets take that space later
+    double *wc = reinterpret_cast<double *>(h->pOff);
+    if (strat) launch_strat_keys(h->stream, h->C, h->bankC, n, h->keys, h->vals, combKey, pidBits, h->strat, wc);
+    else launch_comb_keys(h->stream, h->C, h->bankC, n, h->keys, h->vals, combKey, pidBits, wc);
     int cellBits = 0;
     while ((1ull << cellBits) <= nRuns) ++cellBits;
     // The bucket sort (per-run counting sort, then each run sorted on its own)
@@ -1927,7 +1930,7 @@ int storm_cuda_phase_comb(StormHandle *h) {
         if (!h->bucketFlags) CK(dalloc(h, &h->bucketFlags, 2));
         launch_bucket_sort(h->stream, h->C, h->bankC, h->keys, n, pidBits, static_cast<uint32_t>(nRuns), start,
                            h->runCursor, h->runScan, h->keysAlt, h->valsAlt, wS, h->longRuns,
-                           static_cast<uint32_t>(h->longCap), h->bucketFlags);
+                           static_cast<uint32_t>(h->longCap), h->bucketFlags, wc);
         h->launches += 7;
         skeys = h->keysAlt;
         idx = h->valsAlt;
