@@ -344,47 +344,52 @@ def roofline(res, bytes_per_segment, kernel, sm_mhz=None):
 
 def e2e_run(args, eng, p, dist):
     """The same metric through the C ABI with host buffers, as a caller of the
-    drop-in runs it: before each step the census goes host->device from
-    page-locked memory, after it the new census and the material temperatures
-    come back into page-locked memory."""
+    drop-in runs it: each step takes the census from page-locked host memory
+    and returns the new census there (storm_cuda_step_host, which overlaps the
+    upload with the step's work that does not need the census), and the
+    material temperatures come back after it.  The census travels with the
+    fields a step reads (position, direction, weight, cell) both ways; time
+    left and initial weight, which every step sets for its census at its start,
+    are neither sent nor read back."""
     import torch
     from storm_b200.engine import Particles
     import numpy as np
     n = eng.census_count()
-    buf = Particles.pinned(max(2 * n, 1))
+    bufs = [Particles.pinned(max(2 * n, 1)) for _ in range(2)]
+    for b in bufs:
+        b.time_left = b.initial_weight = None
     pin_T = torch.empty(p.ncells, dtype=torch.float64, pin_memory=True).numpy()
-    host = eng.census(out=buf)
-    rec_in = 7 * 8 + 4    # position, direction, weight, cell: the step sets time left and initial weight
-    rec_out = 9 * 8 + 4
+    host = eng.census(out=bufs[0])
+    rec = 7 * 8 + 4    # position, direction, weight, cell
     torch.cuda.synchronize()
     barrier(dist, "storm")
     t0 = time.perf_counter()
-    segs, h2d, d2h = 0, 0, 0
-    for _ in range(args.e2e_steps):
-        eng.set_census(host, step_fields=False)
-        h2d += host.n * rec_in
-        st = eng.step()
-        segs += st["segments"]
-        if eng.census_count() > buf.n:
+    segs, h2d, d2h, done = 0, 0, 0, 0
+    for k in range(args.e2e_steps):
+        if eng.census_count() > bufs[0].n:
             break
-        host = eng.census(out=buf)
-        d2h += host.n * rec_out
+        st, out = eng.step_host(host, bufs[(k + 1) % 2])
+        h2d += host.n * rec
+        segs += st["segments"]
+        d2h += out.n * rec
         eng.temperature(out=pin_T)
         d2h += p.ncells * 8
+        host = out
+        done += 1
     torch.cuda.synchronize()
     wall = reduce(dist, time.perf_counter() - t0, "max", "storm")
     allsegs = reduce(dist, segs, "sum", "storm")
     link = link_bandwidth()
-    steps = max(args.e2e_steps, 1)
+    steps = max(done, 1)
     floor_ms = (h2d / steps) / link["h2d_gbs"] / 1e6 + (d2h / steps) / link["d2h_gbs"] / 1e6
     return {"value": allsegs / wall, "unit": UNIT, "h2d_bytes_per_step": int(h2d / steps),
-            "d2h_bytes_per_step": int(d2h / steps), "steps": args.e2e_steps,
+            "d2h_bytes_per_step": int(d2h / steps), "steps": done,
             "ms_per_step": wall / steps * 1e3, "link": link, "copy_ms_per_step_at_link_rate": floor_ms,
-            "note": "census in (without time left and initial weight, which the step sets) and out through "
-                    "storm_cuda_set_census / storm_cuda_step / storm_cuda_get_census, "
-                    "temperatures through storm_cuda_get_cell_arrays; page-locked host buffers; copies and "
-                    "host-side checks inside the timed region (wall clock); link = one 1 GiB page-locked copy "
-                    "each way, CUDA-event timed"}
+            "note": "census in and out through storm_cuda_step_host (upload overlapped with the prestep, the "
+                    "emission and the new packets' transport), without time left and initial weight, which "
+                    "the step sets; temperatures through storm_cuda_get_cell_arrays; page-locked host buffers; "
+                    "copies and host-side checks inside the timed region (wall clock); link = one 1 GiB "
+                    "page-locked copy each way, CUDA-event timed"}
 
 
 def link_bandwidth(nbytes=1 << 30):

@@ -407,9 +407,27 @@ int storm_cuda_phase_stats(StormHandle *h, StormStepStats *stats);
  * caller that only steps need not copy them; they read 0 until then. */
 int storm_cuda_set_census(StormHandle *h, const StormParticlesSoA *host_in);
 /* Copy the census (the vector step() returns) device -> host.  host_out arrays
- * must hold `capacity` entries; *count receives the census size. */
+ * must hold `capacity` entries; *count receives the census size.  A NULL field
+ * is not copied: a caller that hands the census back to the next step can leave
+ * out time_left and initial_weight, which that step sets again. */
 int storm_cuda_get_census(StormHandle *h, StormParticlesSoA *host_out, uint64_t capacity, uint64_t *count);
 int storm_cuda_census_count(StormHandle *h, uint64_t *count);
+/* set_census(census_in), step(dt) and get_census(census_out) in one call, as
+ * a caller that keeps its census on the host runs a step (the vector in, the
+ * vector out of MonteCarloManagerSerial::step, manager/MonteCarloManagerSerial.hpp).
+ * The upload runs on a stream of its own while the step's prestep, emission
+ * and the transport of its new packets proceed; the census joins once it is in
+ * place.  The result is the three calls' result: each particle draws from its
+ * own stream and the comb orders the census by key (FP64 tally sums can differ
+ * in their last bits, by their order).  The census's cells are checked before
+ * the step changes any cell state: a cell outside the mesh returns
+ * STORM_ERR_INVALID_ARG with the cell state unchanged and an empty census.
+ * Page-locked host arrays let the upload overlap; census_out's NULL fields are
+ * not written (as get_census).  Particle shards, moving material,
+ * reproducible tallies, the burst tuner and profiling run the three calls in
+ * turn. */
+int storm_cuda_step_host(StormHandle *h, double dt, const StormParticlesSoA *census_in, StormParticlesSoA *census_out,
+                         uint64_t out_capacity, uint64_t *out_count, StormStepStats *stats);
 /* The transport bank after storm_cuda_phase_emit: the census followed by the
  * step's cell and face source packets (RadiationIMC::generateParticles and the
  * boundary's generateNewBoundaryParticles, in that order), id = the particle's

@@ -116,6 +116,7 @@ void launch_strat_plan(cudaStream_t s, const Ctx &C, const CombParams &P, const 
                        const uint32_t *start, const double *binW, const double *cellW, const double *Wtot,
                        uint32_t *pCount, double *pWeight, uint64_t *cellCount, double *eradCensus, DevStats *st);
 void launch_face_spectra(cudaStream_t s, const Ctx &C, double *cdf);
+void launch_set_u32(cudaStream_t s, uint32_t *p, uint32_t v);
 void launch_poly_tets(cudaStream_t s, const Ctx &C, const uint32_t *tetOff, double *tetCum, uint2 *tetAT);
 void launch_emit_faces(cudaStream_t s, const Ctx &C, const FaceSources &F, uint64_t fBegin, uint64_t count,
                        const Bank &b, uint32_t bankBase, uint32_t pidBase, double dt, DevStats *st);

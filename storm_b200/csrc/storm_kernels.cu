@@ -3032,6 +3032,8 @@ void launch_emit_cells(cudaStream_t s, const Ctx &C, const CellArrays &A, const 
         k_emit_cells<<<grid_for(count, 256, 148 * 16), 256, 0, s>>>(C, A, offsets, eBegin, count, b, bankBase, pidBase,
                                                                     dt, st);
 }
+__global__ void k_set_u32(uint32_t *p, uint32_t v) { *p = v; }
+void launch_set_u32(cudaStream_t s, uint32_t *p, uint32_t v) { k_set_u32<<<1, 1, 0, s>>>(p, v); }
 void launch_poly_tets(cudaStream_t s, const Ctx &C, const uint32_t *tetOff, double *tetCum, uint2 *tetAT) {
     k_poly_tets<<<grid_for(C.ncells, 128, 8192), 128, 0, s>>>(C, tetOff, tetCum, tetAT);
 }

@@ -39,6 +39,9 @@ struct StormHandle {
     cudaStream_t stream = nullptr;
     cudaEvent_t evStart = nullptr, evTransport0 = nullptr, evTransport1 = nullptr, evEnd = nullptr;
     cudaEvent_t evAfterEmit = nullptr, evAfterComb = nullptr;
+    // storm_cuda_step_host: the census upload's own stream and its events
+    cudaStream_t copyStream = nullptr;
+    cudaEvent_t evCopyGo = nullptr, evCells = nullptr, evCensusReady = nullptr;
     unsigned char *pinned = nullptr;   // the stream set's page-locked readback buffer (kPinnedBytes)
     uint32_t nx = 0, ny = 0, nz = 0, N = 0;
     std::vector<double> hxe, hye, hze, hxc, hyc, hzc;
@@ -1328,6 +1331,7 @@ int storm_cuda_create(const StormProblemDesc *d, StormHandle **out) {
 int storm_cuda_destroy(StormHandle *h) {
     if (!h) return STORM_OK;
     cudaSetDevice(h->device);
+    if (h->copyStream) cudaStreamSynchronize(h->copyStream);   // a census upload still writing the banks
     const bool idle = !h->stream || cudaStreamSynchronize(h->stream) == cudaSuccess;
     bank_free(h, h->bankA, h->cap);
     bank_free(h, h->bankB, h->cap);
@@ -1361,6 +1365,9 @@ int storm_cuda_destroy(StormHandle *h) {
         if (h->pinned) cudaFreeHost(h->pinned);
     }
     for (cudaEvent_t e : h->evPool)
+        if (e) cudaEventDestroy(e);
+    if (h->copyStream) cudaStreamDestroy(h->copyStream);
+    for (cudaEvent_t e : {h->evCopyGo, h->evCells, h->evCensusReady})
         if (e) cudaEventDestroy(e);
     delete h;
     return STORM_OK;
@@ -1412,8 +1419,10 @@ int storm_cuda_phase_prestep(StormHandle *h, double dt) {
     return STORM_OK;
 }
 
-int storm_cuda_phase_emit(StormHandle *h, double dt) {
-    if (!h) return STORM_ERR_INVALID_ARG;
+// The emission's first half: the cells' energies and photon counts (the
+// reference's allocation, exact) and their scan; *ne gets the step's number of
+// cell packets.  Nothing of the handle's state changes but these per-cell counts.
+static int emit_count(StormHandle *h, double dt, uint64_t *ne) {
     refresh_ctx(h);
     const uint32_t N = h->N;
     // The reference floors each cell's share against its left-to-right total
@@ -1444,12 +1453,18 @@ int storm_cuda_phase_emit(StormHandle *h, double dt) {
         CK(cudaGetLastError());
         CK(read_small(h, &back.total, h->dTotalU64, sizeof(uint64_t)));
     }
+    *ne = back.total;
+    return STORM_OK;
+}
+
+// The second half: the material's emission debit and the packets, cell
+// packets after the census, face packets after those.
+static int emit_packets(StormHandle *h, double dt, uint64_t ne) {
     launch_emission_debit(h->stream, h->C, h->A, h->dStats);
     ++h->launches;
     // The step's packets are numbered over the whole problem: cell packet e has
     // pid nCen + e, face packet f pid nCen + nE + f.  A sharded handle makes
     // its shards' share of each numbering (equal contiguous ranges per shard).
-    const uint64_t ne = back.total;
     const uint64_t nf = h->fsTotal;
     h->nCellEmitGlobal = ne;
     h->nFaceEmitGlobal = nf;
@@ -1494,6 +1509,13 @@ int storm_cuda_phase_emit(StormHandle *h, double dt) {
     h->stats.emitted_faces = fHi - fLo;
     h->nBank = total;
     return STORM_OK;
+}
+
+int storm_cuda_phase_emit(StormHandle *h, double dt) {
+    if (!h) return STORM_ERR_INVALID_ARG;
+    uint64_t ne = 0;
+    const int rc = emit_count(h, dt, &ne);
+    return rc != STORM_OK ? rc : emit_packets(h, dt, ne);
 }
 
 // Hand `count` doubles of the handle's exchange buffer to the exchange
@@ -2118,6 +2140,169 @@ int storm_cuda_step(StormHandle *h, double dt, StormStepStats *stats) {
         }
     }
     if (stats) storm_cuda_phase_stats(h, stats);
+    return rc;
+}
+
+// storm_cuda_step_host: set_census, step and get_census in one call, the
+// census upload overlapped with the step's work that does not need it.  The
+// copy stream carries the census into the bank (cells first, checked on the
+// device before anything of the step changes the cell state), while the main
+// stream runs the prestep, the emission and the transport of the step's new
+// packets; the census joins with its begin and a second transport launch.
+// Each particle draws from its own stream and the comb orders the census by
+// key, so the result is the three calls' result (FP64 tally sums up to their
+// order).  Problems whose transport is not the refill kernel, particle shards,
+// moving material, reproducible tallies, the burst tuner and profiling take the
+// three calls one after another.
+static bool step_host_overlaps(const StormHandle *h) {
+    const bool refill = h->refill || (h->fp32 && h->desc.groups >= 2) || h->C.poly || h->C.egAvg;
+    return refill && h->shards == 1 && !h->C.withHydro && !h->C.fixMat && !h->tune.perCandidate && !h->profiling &&
+           h->pinned != nullptr;
+}
+
+int storm_cuda_step_host(StormHandle *h, double dt, const StormParticlesSoA *in, StormParticlesSoA *out,
+                         uint64_t out_capacity, uint64_t *out_count, StormStepStats *stats) {
+    if (!h || !in || !out || !(dt > 0.0)) return STORM_ERR_INVALID_ARG;
+    const uint64_t n = in->count;
+    if (n == 0 || !step_host_overlaps(h)) {
+        int rc = storm_cuda_set_census(h, in);
+        if (rc == STORM_OK) rc = storm_cuda_step(h, dt, stats);
+        if (rc == STORM_OK) rc = storm_cuda_get_census(h, out, out_capacity, out_count);
+        return rc;
+    }
+    const double *sd[] = {in->x, in->y, in->z, in->vx, in->vy, in->vz, in->time_left, in->weight, in->initial_weight};
+    if (!in->cell) return STORM_ERR_INVALID_ARG;
+    for (int q = 0; q < 9; ++q)
+        if (!sd[q] && q != 6 && q != 8) return STORM_ERR_INVALID_ARG;
+    if (n > 0xFFFFFFFFull) return STORM_ERR_CAPACITY;
+    CK(cudaSetDevice(h->device));
+    if (!h->copyStream) {
+        CK(cudaStreamCreateWithFlags(&h->copyStream, cudaStreamNonBlocking));
+        for (cudaEvent_t *e : {&h->evCopyGo, &h->evCells, &h->evCensusReady})
+            CK(cudaEventCreateWithFlags(e, cudaEventDisableTiming));
+    }
+    // begin (phase_begin without the census's own kernel, which waits for the census)
+    h->errCode = 0;
+    h->stepDt = dt;
+    h->stats = StormStepStats{};
+    h->nCensus = 0;
+    CK(cudaEventRecord(h->evStart, h->stream));
+    CK(cudaMemsetAsync(h->dStats, 0, sizeof(DevStats), h->stream));
+    CK(cudaMemsetAsync(h->dErr, 0, 4 * sizeof(int32_t), h->stream));
+    refresh_ctx(h);
+    int rc = storm_cuda_phase_prestep(h, dt);
+    if (rc != STORM_OK) return rc;
+    // the step's packet count, then room for census and packets together
+    uint64_t ne = 0;
+    rc = emit_count(h, dt, &ne);
+    if (rc != STORM_OK) return rc;
+    if (n + ne + h->fsTotal > 0xFFFFFFFFull) return STORM_ERR_CAPACITY;   // pids are 32-bit
+    rc = ensure_capacity(h, n + ne + h->fsTotal, 0);
+    if (rc != STORM_OK) return rc;
+    // the upload, after every earlier use of the banks on the main stream
+    const Bank &stage = h->fp32 ? h->bankB : h->bankA;   // FP32 form: stage FP64, then convert
+    double *dd[] = {stage.x, stage.y, stage.z, stage.vx, stage.vy, stage.vz, stage.t, stage.w, stage.w0};
+    int32_t *badFlag = reinterpret_cast<int32_t *>(h->pinned + kPinnedBytes - 64);
+    cudaStream_t cs = h->copyStream;
+    CK(cudaEventRecord(h->evCopyGo, h->stream));
+    CK(cudaStreamWaitEvent(cs, h->evCopyGo, 0));
+    CK(cudaMemcpyAsync(stage.cell, in->cell, n * sizeof(uint32_t), cudaMemcpyHostToDevice, cs));
+    CK(cudaMemsetAsync(h->dAmbiguous + 1, 0, sizeof(int32_t), cs));
+    launch_count_bad_cells(cs, stage.cell, static_cast<uint32_t>(n), h->N, h->dAmbiguous + 1);
+    ++h->launches;
+    CK(cudaMemcpyAsync(badFlag, h->dAmbiguous + 1, sizeof(int32_t), cudaMemcpyDeviceToHost, cs));
+    CK(cudaEventRecord(h->evCells, cs));
+    for (int q = 0; q < 9; ++q) {
+        if (sd[q]) CK(cudaMemcpyAsync(dd[q], sd[q], n * sizeof(double), cudaMemcpyHostToDevice, cs));
+        else CK(cudaMemsetAsync(dd[q], 0, n * sizeof(double), cs));
+    }
+    if (stage.nu) {
+        if (in->frequency) CK(cudaMemcpyAsync(stage.nu, in->frequency, n * sizeof(double), cudaMemcpyHostToDevice, cs));
+        else CK(cudaMemsetAsync(stage.nu, 0, n * sizeof(double), cs));
+    }
+    // nothing of the cell state changes before the census's cells are known to be in the mesh
+    CK(cudaEventSynchronize(h->evCells));
+    if (*badFlag) {
+        CK(cudaStreamSynchronize(cs));
+        return STORM_ERR_INVALID_ARG;
+    }
+    if (h->fp32) {
+        launch_bank_to_local(cs, h->C, h->bankB, h->bankA, static_cast<uint32_t>(n));
+        ++h->launches;
+    }
+    CK(cudaGetLastError());
+    CK(cudaEventRecord(h->evCensusReady, cs));
+    // the census's place in the numbering: slots and pids [0, n), packets after it
+    h->nCensus = n;
+    h->nCenGlobal = n;
+    h->stats.census_in = n;
+    rc = emit_packets(h, dt, ne);
+    if (rc != STORM_OK) {
+        cudaStreamSynchronize(cs);
+        return rc;
+    }
+    CK(cudaEventRecord(h->evAfterEmit, h->stream));
+    // transport: the packets [n, nBank), then the census [0, n) once it is in place
+    const uint64_t nb = h->nBank;
+    CK(cudaEventRecord(h->evTransport0, h->stream));
+    CK(cudaMemsetAsync(h->counts, 0, sizeof(uint32_t) * (h->maxRounds + 2), h->stream));
+    if (h->desc.per_cell_segment_counters) CK(cudaMemsetAsync(h->segs, 0, sizeof(uint32_t) * h->N, h->stream));
+    uint32_t *nCen = h->counts + h->maxRounds + 1;
+    const uint64_t maxSegs64 = static_cast<uint64_t>(h->maxRounds) * h->K;
+    const uint32_t maxSegs = static_cast<uint32_t>(std::min<uint64_t>(maxSegs64, 0xffffffffull));
+    const int nbps = refill_blocks_per_sm(h->minBlocks, h->fp32);
+    auto grid_for_range = [&](uint64_t len) {
+        uint32_t g = static_cast<uint32_t>(h->smCount) * static_cast<uint32_t>(nbps > 0 ? nbps : 1);
+        const uint32_t need = static_cast<uint32_t>((len + 255) / 256);
+        return need < g ? (need ? need : 1u) : g;
+    };
+    if (nb > n) {
+        launch_set_u32(h->stream, h->counts + 1, static_cast<uint32_t>(n));   // the refill queue starts at n
+        launch_transport_refill(h->stream, grid_for_range(nb - n), h->minBlocks, h->C, h->bankA,
+                                static_cast<uint32_t>(nb), h->counts + 1, h->bankC, nCen, h->burst, maxSegs, h->dStats);
+        h->launches += 2;
+    }
+    CK(cudaStreamWaitEvent(h->stream, h->evCensusReady, 0));
+    launch_begin(h->stream, h->bankA, static_cast<uint32_t>(n), 0u, dt, h->dStats);
+    ++h->launches;
+    if (h->beginCounts) {
+        CK(cudaMemsetAsync(h->beginCounts, 0, sizeof(uint32_t) * h->N, h->stream));
+        launch_cell_histogram(h->stream, h->bankA.cell, static_cast<uint32_t>(nb), h->N, h->beginCounts);
+        ++h->launches;
+    }
+    CK(cudaMemsetAsync(h->counts + 1, 0, sizeof(uint32_t), h->stream));
+    launch_transport_refill(h->stream, grid_for_range(n), h->minBlocks, h->C, h->bankA, static_cast<uint32_t>(n),
+                            h->counts + 1, h->bankC, nCen, h->burst, maxSegs, h->dStats);
+    ++h->launches;
+    CK(cudaGetLastError());
+    CK(cudaEventRecord(h->evTransport1, h->stream));
+    uint32_t nc = 0;
+    rc = read_checked(h, &nc, nCen, sizeof(uint32_t));
+    if (rc != STORM_OK) return rc;
+    h->stats.rounds = 1;
+    h->stats.census_out_pre_comb = nc;
+    float tms = 0.f;
+    cudaEventElapsedTime(&tms, h->evTransport0, h->evTransport1);
+    h->lastTransportMs = tms;
+    h->nBank = 0;
+    // the comb, the poststep and the new census back to the host, as storm_cuda_step does
+    rc = storm_cuda_phase_comb(h);
+    CK(cudaEventRecord(h->evAfterComb, h->stream));
+    if (rc == STORM_OK) rc = poststep_launch(h, dt);
+    CK(cudaEventRecord(h->evEnd, h->stream));
+    if (rc == STORM_OK) rc = check_device_error(h);
+    CK(cudaEventSynchronize(h->evEnd));
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, h->evStart, h->evEnd);
+    h->lastStepMs = ms;
+    if (rc == STORM_OK) {
+        cudaEventElapsedTime(&ms, h->evStart, h->evAfterEmit);
+        h->lastEmitMs = ms;
+        cudaEventElapsedTime(&ms, h->evTransport1, h->evAfterComb);
+        h->lastCombMs = ms;
+    }
+    if (stats) storm_cuda_phase_stats(h, stats);
+    if (rc == STORM_OK) rc = storm_cuda_get_census(h, out, out_capacity, out_count);
     return rc;
 }
 

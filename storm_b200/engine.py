@@ -46,6 +46,9 @@ def lib():
         L.storm_cuda_phase_stats.argtypes = [vp, C.POINTER(A.StormStepStats)]
         L.storm_cuda_set_census.argtypes = [vp, C.POINTER(A.StormParticlesSoA)]
         L.storm_cuda_get_census.argtypes = [vp, C.POINTER(A.StormParticlesSoA), C.c_uint64, u64p]
+        L.storm_cuda_step_host.argtypes = [vp, C.c_double, C.POINTER(A.StormParticlesSoA),
+                                           C.POINTER(A.StormParticlesSoA), C.c_uint64, u64p,
+                                           C.POINTER(A.StormStepStats)]
         L.storm_cuda_census_count.argtypes = [vp, u64p]
         L.storm_cuda_get_bank.argtypes = [vp, C.POINTER(A.StormParticlesSoA), C.c_uint64, u64p]
         L.storm_cuda_population_control.argtypes = [vp, C.POINTER(A.StormParticlesSoA)]
@@ -267,6 +270,28 @@ class Engine:
         s = p.soa()
         self._check(lib().storm_cuda_get_bank(self.h, C.byref(s), cnt.value, C.byref(cnt)))
         return p
+
+    def step_host(self, census, out, dt=None, step_fields=False):
+        """One step with the census on the host (storm_cuda_step_host): `census`
+        goes in, the new census comes back into `out` (e.g. Particles.pinned),
+        the upload overlapping the step's work that does not need it.  Without
+        step_fields, time_left and initial_weight are neither sent nor read
+        back (every step sets them).  Returns (stats, view of out)."""
+        if not step_fields:
+            v = census.view(census.n)
+            v.time_left = v.initial_weight = None
+            census = v
+            o = out.view(out.n)
+            o.time_left = o.initial_weight = None
+            out = o
+        sin, sout = census.soa(), out.soa()
+        st = A.StormStepStats()
+        cnt = C.c_uint64()
+        self._check(lib().storm_cuda_step_host(self.h, self.problem.dt if dt is None else dt, C.byref(sin),
+                                                C.byref(sout), out.n, C.byref(cnt), C.byref(st)))
+        if cnt.value > out.n:
+            raise ValueError(f"census of {cnt.value} particles does not fit the {out.n} of out")
+        return st.as_dict(), out.view(cnt.value)
 
     def set_census(self, p, step_fields=True):
         """Replace the census.  step_fields=False leaves out time_left and
