@@ -308,10 +308,16 @@ public:
         try {
             auto t0 = std::chrono::steady_clock::now();
             upload_cells();
-            upload_census(particleList);
+            // the census goes in with the step itself (storm_cuda_step_host: its
+            // upload overlaps the step's emission and new-packet transport); the
+            // new census comes back below with every field
+            CensusArrays in = pack_census(particleList);
             std::vector<MCParticle>().swap(particleList);
             StormStepStats st{};
-            cuda_detail::check(storm_cuda_step(h_, fullDt, &st), h_, "storm_cuda_step");
+            StormParticlesSoA none{};
+            std::uint64_t nOut = 0;
+            cuda_detail::check(storm_cuda_step_host(h_, fullDt, &in.soa, &none, 0, &nOut, &st), h_,
+                               "storm_cuda_step_host");
             download_cells();
             {
                 std::vector<std::uint64_t> begin(N_);
@@ -599,7 +605,13 @@ private:
         }
     }
 
-    void upload_census(const std::vector<MCParticle> &ps) {
+    // a census as the C ABI's arrays (the vectors own what soa points at)
+    struct CensusArrays {
+        std::vector<double> x, y, z, vx, vy, vz, w, nu;
+        std::vector<std::uint32_t> cell;
+        StormParticlesSoA soa{};
+    };
+    CensusArrays pack_census(const std::vector<MCParticle> &ps) const {
         const std::size_t n = ps.size();
         for (const MCParticle &p : ps)
             if (p.on_track) {
@@ -609,19 +621,21 @@ private:
             }
         // timeLeft and initialWeight are not copied: step() sets them for every
         // census particle (manager/MonteCarloManagerSerial.hpp:391-405)
-        std::vector<double> x(n), y(n), z(n), vx(n), vy(n), vz(n), w(n), nu(multigroup_ ? n : 0);
-        std::vector<std::uint32_t> cell(n);
+        CensusArrays a;
+        for (auto *v : {&a.x, &a.y, &a.z, &a.vx, &a.vy, &a.vz, &a.w}) v->resize(n);
+        a.nu.resize(multigroup_ ? n : 0);
+        a.cell.resize(n);
         for (std::size_t q = 0; q < n; ++q) {
             const MCParticle &p = ps[q];
-            x[q] = p.location.x; y[q] = p.location.y; z[q] = p.location.z;
-            vx[q] = p.velocity.x; vy[q] = p.velocity.y; vz[q] = p.velocity.z;
-            w[q] = p.weight;
-            cell[q] = static_cast<std::uint32_t>(p.cellIndex);
-            if (multigroup_) nu[q] = p.frequency;
+            a.x[q] = p.location.x; a.y[q] = p.location.y; a.z[q] = p.location.z;
+            a.vx[q] = p.velocity.x; a.vy[q] = p.velocity.y; a.vz[q] = p.velocity.z;
+            a.w[q] = p.weight;
+            a.cell[q] = static_cast<std::uint32_t>(p.cellIndex);
+            if (multigroup_) a.nu[q] = p.frequency;
         }
-        StormParticlesSoA s{x.data(), y.data(), z.data(), vx.data(), vy.data(), vz.data(), nullptr, w.data(),
-                            nullptr, cell.data(), nullptr, n, multigroup_ ? nu.data() : nullptr};
-        cuda_detail::check(storm_cuda_set_census(h_, &s), h_, "set_census");
+        a.soa = StormParticlesSoA{a.x.data(), a.y.data(), a.z.data(), a.vx.data(), a.vy.data(), a.vz.data(), nullptr,
+                                  a.w.data(), nullptr, a.cell.data(), nullptr, n, multigroup_ ? a.nu.data() : nullptr};
+        return a;
     }
 
     std::vector<MCParticle> download_census() {

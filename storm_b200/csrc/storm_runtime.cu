@@ -2212,26 +2212,9 @@ int storm_cuda_step_host(StormHandle *h, double dt, const StormParticlesSoA *in,
     ++h->launches;
     CK(cudaMemcpyAsync(badFlag, h->dAmbiguous + 1, sizeof(int32_t), cudaMemcpyDeviceToHost, cs));
     CK(cudaEventRecord(h->evCells, cs));
-    for (int q = 0; q < 9; ++q) {
-        if (sd[q]) CK(cudaMemcpyAsync(dd[q], sd[q], n * sizeof(double), cudaMemcpyHostToDevice, cs));
-        else CK(cudaMemsetAsync(dd[q], 0, n * sizeof(double), cs));
-    }
-    if (stage.nu) {
-        if (in->frequency) CK(cudaMemcpyAsync(stage.nu, in->frequency, n * sizeof(double), cudaMemcpyHostToDevice, cs));
-        else CK(cudaMemsetAsync(stage.nu, 0, n * sizeof(double), cs));
-    }
     // nothing of the cell state changes before the census's cells are known to be in the mesh
     CK(cudaEventSynchronize(h->evCells));
-    if (*badFlag) {
-        CK(cudaStreamSynchronize(cs));
-        return STORM_ERR_INVALID_ARG;
-    }
-    if (h->fp32) {
-        launch_bank_to_local(cs, h->C, h->bankB, h->bankA, static_cast<uint32_t>(n));
-        ++h->launches;
-    }
-    CK(cudaGetLastError());
-    CK(cudaEventRecord(h->evCensusReady, cs));
+    if (*badFlag) return STORM_ERR_INVALID_ARG;
     // the census's place in the numbering: slots and pids [0, n), packets after it
     h->nCensus = n;
     h->nCenGlobal = n;
@@ -2244,6 +2227,8 @@ int storm_cuda_step_host(StormHandle *h, double dt, const StormParticlesSoA *in,
     CK(cudaEventRecord(h->evAfterEmit, h->stream));
     // transport: the packets [n, nBank), then the census [0, n) once it is in place
     const uint64_t nb = h->nBank;
+    h->pidLimit = h->nCenGlobal + h->nCellEmitGlobal + h->nFaceEmitGlobal;   // the comb's key width
+    if (h->pidLimit == 0) h->pidLimit = 1;
     CK(cudaEventRecord(h->evTransport0, h->stream));
     CK(cudaMemsetAsync(h->counts, 0, sizeof(uint32_t) * (h->maxRounds + 2), h->stream));
     if (h->desc.per_cell_segment_counters) CK(cudaMemsetAsync(h->segs, 0, sizeof(uint32_t) * h->N, h->stream));
@@ -2262,6 +2247,22 @@ int storm_cuda_step_host(StormHandle *h, double dt, const StormParticlesSoA *in,
                                 static_cast<uint32_t>(nb), h->counts + 1, h->bankC, nCen, h->burst, maxSegs, h->dStats);
         h->launches += 2;
     }
+    // the rest of the census, behind the work above (from pageable memory the
+    // host itself copies, while the device runs that work)
+    for (int q = 0; q < 9; ++q) {
+        if (sd[q]) CK(cudaMemcpyAsync(dd[q], sd[q], n * sizeof(double), cudaMemcpyHostToDevice, cs));
+        else CK(cudaMemsetAsync(dd[q], 0, n * sizeof(double), cs));
+    }
+    if (stage.nu) {
+        if (in->frequency) CK(cudaMemcpyAsync(stage.nu, in->frequency, n * sizeof(double), cudaMemcpyHostToDevice, cs));
+        else CK(cudaMemsetAsync(stage.nu, 0, n * sizeof(double), cs));
+    }
+    if (h->fp32) {
+        launch_bank_to_local(cs, h->C, h->bankB, h->bankA, static_cast<uint32_t>(n));
+        ++h->launches;
+    }
+    CK(cudaGetLastError());
+    CK(cudaEventRecord(h->evCensusReady, cs));
     CK(cudaStreamWaitEvent(h->stream, h->evCensusReady, 0));
     launch_begin(h->stream, h->bankA, static_cast<uint32_t>(n), 0u, dt, h->dStats);
     ++h->launches;
