@@ -93,7 +93,9 @@ struct ReplayDev {
     double *momOut;         // moving material: 3 per record (NULL = not returned)
 };
 
-void launch_begin(cudaStream_t s, const Bank &b, uint32_t n, uint32_t pidOffset, double dt, DevStats *st);
+// particles [lo, n) (pids pidOffset + q)
+void launch_begin(cudaStream_t s, const Bank &b, uint32_t n, uint32_t pidOffset, double dt, DevStats *st,
+                  uint32_t lo = 0);
 void launch_prestep(cudaStream_t s, const Ctx &C, const CellArrays &A, const OpacityEos &M, double dt);
 void launch_rw_eligibility(cudaStream_t s, const Ctx &C, const CellArrays &A);
 void launch_emission_energy(cudaStream_t s, const Ctx &C, const CellArrays &A, double dt);
@@ -127,7 +129,8 @@ void launch_transport_refill(cudaStream_t s, uint32_t grid, int minBlocks, const
                              uint32_t *nextIdx, const CensusBank &cen, uint32_t *nCen, uint32_t burst, uint32_t maxSegs,
                              DevStats *st);
 int refill_blocks_per_sm(int minBlocks, bool fp32);
-void launch_bank_to_local(cudaStream_t s, const Ctx &C, const Bank &src, const Bank &dst, uint32_t n);
+void launch_bank_to_local(cudaStream_t s, const Ctx &C, const Bank &src, const Bank &dst, uint32_t n,
+                          uint32_t lo = 0);   // particles [lo, n)
 void launch_bank_to_global(cudaStream_t s, const Ctx &C, const Bank &src, const Bank &dst, uint32_t n);
 void launch_comb_keys(cudaStream_t s, const Ctx &C, const CensusBank &cen, uint32_t n, uint64_t *keys, uint32_t *vals,
                       uint32_t combKey, int pidBits, double *wc = nullptr);

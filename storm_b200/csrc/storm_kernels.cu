@@ -203,8 +203,8 @@ __device__ __forceinline__ uint2 census_cell_pid(const Ctx &C, const CensusBank 
 }
 
 // convert a bank between the FP64 (global) and FP32-tracking (local) layouts
-__global__ void k_bank_to_local(Ctx C, Bank src, Bank dst, uint32_t n) {
-    for (uint32_t q = blockIdx.x * blockDim.x + threadIdx.x; q < n; q += gridDim.x * blockDim.x) {
+__global__ void k_bank_to_local(Ctx C, Bank src, Bank dst, uint32_t lo, uint32_t n) {
+    for (uint32_t q = lo + blockIdx.x * blockDim.x + threadIdx.x; q < n; q += gridDim.x * blockDim.x) {
         PartReg p;
         load_part(src, q, p);
         Track32 T;
@@ -242,9 +242,9 @@ __global__ void k_bank_to_global(Ctx C, Bank src, Bank dst, uint32_t n) {
 // manager step() (manager/MonteCarloManagerSerial.hpp:393-405): census particles
 // get timeLeft = dt, initialWeight = |w|; they take pids pidOffset + 0..n-1
 // (pidOffset: the census of the shards below this handle's, 0 unsharded).
-__global__ void k_begin(Bank b, uint32_t n, uint32_t pidOffset, double dt, DevStats *st) {
+__global__ void k_begin(Bank b, uint32_t lo, uint32_t n, uint32_t pidOffset, double dt, DevStats *st) {
     double e = 0.0;
-    for (uint32_t q = blockIdx.x * blockDim.x + threadIdx.x; q < n; q += gridDim.x * blockDim.x) {
+    for (uint32_t q = lo + blockIdx.x * blockDim.x + threadIdx.x; q < n; q += gridDim.x * blockDim.x) {
         double w = b.w[q];
         b.t[q] = dt;
         b.w0[q] = fabs(w);
@@ -2981,8 +2981,9 @@ static inline uint32_t grid_for(uint64_t n, uint32_t block, uint32_t cap) {
     return static_cast<uint32_t>(g < cap ? g : cap);
 }
 
-void launch_begin(cudaStream_t s, const Bank &b, uint32_t n, uint32_t pidOffset, double dt, DevStats *st) {
-    k_begin<<<grid_for(n, 256, 4096), 256, 0, s>>>(b, n, pidOffset, dt, st);
+void launch_begin(cudaStream_t s, const Bank &b, uint32_t n, uint32_t pidOffset, double dt, DevStats *st,
+                  uint32_t lo) {
+    if (n > lo) k_begin<<<grid_for(n - lo, 256, 4096), 256, 0, s>>>(b, lo, n, pidOffset, dt, st);
 }
 void launch_prestep(cudaStream_t s, const Ctx &C, const CellArrays &A, const OpacityEos &M, double dt) {
     k_prestep<<<grid_for(C.ncells, 256, 8192), 256, 0, s>>>(C, A, M, dt);
@@ -3333,8 +3334,8 @@ void launch_add_into(cudaStream_t s, double *y, const double *x, uint32_t n) {
 void launch_count_bad_cells(cudaStream_t s, const uint32_t *cell, uint32_t n, uint32_t N, int32_t *bad) {
     if (n) k_count_bad_cells<<<grid_for(n, 256, 4096), 256, 0, s>>>(cell, n, N, bad);
 }
-void launch_bank_to_local(cudaStream_t s, const Ctx &C, const Bank &src, const Bank &dst, uint32_t n) {
-    if (n) k_bank_to_local<<<grid_for(n, 256, 8192), 256, 0, s>>>(C, src, dst, n);
+void launch_bank_to_local(cudaStream_t s, const Ctx &C, const Bank &src, const Bank &dst, uint32_t n, uint32_t lo) {
+    if (n > lo) k_bank_to_local<<<grid_for(n - lo, 256, 8192), 256, 0, s>>>(C, src, dst, lo, n);
 }
 void launch_bank_to_census(cudaStream_t s, const Ctx &C, const Bank &src, const CensusBank &dst, uint32_t n) {
     if (n) k_bank_to_census<<<grid_for(n, 256, 8192), 256, 0, s>>>(C, src, dst, n);

@@ -41,7 +41,8 @@ struct StormHandle {
     cudaEvent_t evAfterEmit = nullptr, evAfterComb = nullptr;
     // storm_cuda_step_host: the census upload's own stream and its events
     cudaStream_t copyStream = nullptr;
-    cudaEvent_t evCopyGo = nullptr, evCells = nullptr, evCensusReady = nullptr;
+    cudaEvent_t evCopyGo = nullptr, evCells = nullptr;
+    std::vector<cudaEvent_t> evChunks;   // one per census chunk in place
     unsigned char *pinned = nullptr;   // the stream set's page-locked readback buffer (kPinnedBytes)
     uint32_t nx = 0, ny = 0, nz = 0, N = 0;
     std::vector<double> hxe, hye, hze, hxc, hyc, hzc;
@@ -321,6 +322,10 @@ DevicePool &device_pool() {
 // returns them, idle, to a per-device cache and the next create takes them
 // from there instead of creating new ones.
 constexpr size_t kPinnedBytes = 4096;   // page-locked staging for small readbacks, per stream set
+// storm_cuda_step_host: the census upload in at most kHostChunks chunks of at
+// least kHostChunkMin particles, each transported once it is in place
+constexpr uint32_t kHostChunks = 6;
+constexpr uint64_t kHostChunkMin = 1u << 20;
 struct StreamSet {
     cudaStream_t stream = nullptr;
     cudaEvent_t ev[6] = {};
@@ -1367,7 +1372,9 @@ int storm_cuda_destroy(StormHandle *h) {
     for (cudaEvent_t e : h->evPool)
         if (e) cudaEventDestroy(e);
     if (h->copyStream) cudaStreamDestroy(h->copyStream);
-    for (cudaEvent_t e : {h->evCopyGo, h->evCells, h->evCensusReady})
+    for (cudaEvent_t e : {h->evCopyGo, h->evCells})
+        if (e) cudaEventDestroy(e);
+    for (cudaEvent_t e : h->evChunks)
         if (e) cudaEventDestroy(e);
     delete h;
     return STORM_OK;
@@ -2178,8 +2185,10 @@ int storm_cuda_step_host(StormHandle *h, double dt, const StormParticlesSoA *in,
     CK(cudaSetDevice(h->device));
     if (!h->copyStream) {
         CK(cudaStreamCreateWithFlags(&h->copyStream, cudaStreamNonBlocking));
-        for (cudaEvent_t *e : {&h->evCopyGo, &h->evCells, &h->evCensusReady})
+        for (cudaEvent_t *e : {&h->evCopyGo, &h->evCells})
             CK(cudaEventCreateWithFlags(e, cudaEventDisableTiming));
+        h->evChunks.assign(kHostChunks, nullptr);
+        for (cudaEvent_t &e : h->evChunks) CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
     }
     // begin (phase_begin without the census's own kernel, which waits for the census)
     h->errCode = 0;
@@ -2247,34 +2256,45 @@ int storm_cuda_step_host(StormHandle *h, double dt, const StormParticlesSoA *in,
                                 static_cast<uint32_t>(nb), h->counts + 1, h->bankC, nCen, h->burst, maxSegs, h->dStats);
         h->launches += 2;
     }
-    // the rest of the census, behind the work above (from pageable memory the
-    // host itself copies, while the device runs that work)
-    for (int q = 0; q < 9; ++q) {
-        if (sd[q]) CK(cudaMemcpyAsync(dd[q], sd[q], n * sizeof(double), cudaMemcpyHostToDevice, cs));
-        else CK(cudaMemsetAsync(dd[q], 0, n * sizeof(double), cs));
-    }
-    if (stage.nu) {
-        if (in->frequency) CK(cudaMemcpyAsync(stage.nu, in->frequency, n * sizeof(double), cudaMemcpyHostToDevice, cs));
-        else CK(cudaMemsetAsync(stage.nu, 0, n * sizeof(double), cs));
-    }
-    if (h->fp32) {
-        launch_bank_to_local(cs, h->C, h->bankB, h->bankA, static_cast<uint32_t>(n));
-        ++h->launches;
+    // the rest of the census behind the work above (from pageable memory the host
+    // itself copies while the device runs that work), in chunks that each join
+    // the transport as soon as they are in place
+    const uint64_t chunk = std::max<uint64_t>(kHostChunkMin, (n + kHostChunks - 1) / kHostChunks);
+    uint32_t nChunks = 0;
+    for (uint64_t lo = 0; lo < n; lo += chunk, ++nChunks) {
+        const uint64_t len = std::min<uint64_t>(chunk, n - lo);
+        for (int q = 0; q < 9; ++q) {
+            if (sd[q]) CK(cudaMemcpyAsync(dd[q] + lo, sd[q] + lo, len * sizeof(double), cudaMemcpyHostToDevice, cs));
+            else CK(cudaMemsetAsync(dd[q] + lo, 0, len * sizeof(double), cs));
+        }
+        if (stage.nu) {
+            if (in->frequency)
+                CK(cudaMemcpyAsync(stage.nu + lo, in->frequency + lo, len * sizeof(double), cudaMemcpyHostToDevice, cs));
+            else CK(cudaMemsetAsync(stage.nu + lo, 0, len * sizeof(double), cs));
+        }
+        if (h->fp32) {
+            launch_bank_to_local(cs, h->C, h->bankB, h->bankA, static_cast<uint32_t>(lo + len), static_cast<uint32_t>(lo));
+            ++h->launches;
+        }
+        CK(cudaEventRecord(h->evChunks[nChunks], cs));
     }
     CK(cudaGetLastError());
-    CK(cudaEventRecord(h->evCensusReady, cs));
-    CK(cudaStreamWaitEvent(h->stream, h->evCensusReady, 0));
-    launch_begin(h->stream, h->bankA, static_cast<uint32_t>(n), 0u, dt, h->dStats);
-    ++h->launches;
-    if (h->beginCounts) {
-        CK(cudaMemsetAsync(h->beginCounts, 0, sizeof(uint32_t) * h->N, h->stream));
-        launch_cell_histogram(h->stream, h->bankA.cell, static_cast<uint32_t>(nb), h->N, h->beginCounts);
+    for (uint32_t k = 0; k < nChunks; ++k) {
+        const uint64_t lo = k * chunk, hi = std::min<uint64_t>(n, lo + chunk);
+        CK(cudaStreamWaitEvent(h->stream, h->evChunks[k], 0));
+        launch_begin(h->stream, h->bankA, static_cast<uint32_t>(hi), 0u, dt, h->dStats, static_cast<uint32_t>(lo));
         ++h->launches;
+        if (h->beginCounts && k + 1 == nChunks) {   // every particle's cell is in place now
+            CK(cudaMemsetAsync(h->beginCounts, 0, sizeof(uint32_t) * h->N, h->stream));
+            launch_cell_histogram(h->stream, h->bankA.cell, static_cast<uint32_t>(nb), h->N, h->beginCounts);
+            ++h->launches;
+        }
+        launch_set_u32(h->stream, h->counts + 1, static_cast<uint32_t>(lo));
+        launch_transport_refill(h->stream, grid_for_range(hi - lo), h->minBlocks, h->C, h->bankA,
+                                static_cast<uint32_t>(hi), h->counts + 1, h->bankC, nCen, h->burst, maxSegs,
+                                h->dStats);
+        h->launches += 2;
     }
-    CK(cudaMemsetAsync(h->counts + 1, 0, sizeof(uint32_t), h->stream));
-    launch_transport_refill(h->stream, grid_for_range(n), h->minBlocks, h->C, h->bankA, static_cast<uint32_t>(n),
-                            h->counts + 1, h->bankC, nCen, h->burst, maxSegs, h->dStats);
-    ++h->launches;
     CK(cudaGetLastError());
     CK(cudaEventRecord(h->evTransport1, h->stream));
     uint32_t nc = 0;
