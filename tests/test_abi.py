@@ -150,3 +150,12 @@ def test_serving_mix_is_seeded():
     assert [(p.shape, s, p.sigma_a[0], p.new_photons_per_cell) for p, s in a] == \
            [(p.shape, s, p.sigma_a[0], p.new_photons_per_cell) for p, s in b]
     assert all(16 <= p.shape[0] <= 48 and 5 <= s <= 20 for p, s in a)
+
+
+def test_host_step_rejects_missing_arguments():
+    """storm_cuda_step_host checks its handle and buffers before touching a device."""
+    L = engine.lib()
+    s = A.StormParticlesSoA()
+    cnt = C.c_uint64()
+    st = A.StormStepStats()
+    assert L.storm_cuda_step_host(None, 1e-11, C.byref(s), C.byref(s), 0, C.byref(cnt), C.byref(st)) == 1
