@@ -2024,6 +2024,77 @@ __device__ __forceinline__ void warp_sort_run(const Ctx &C, const CensusBank &ce
     }
 }
 
+// The same network on 32-bit words.
+template <int E>
+__device__ __forceinline__ void warp_bitonic32(uint32_t (&v)[E], uint32_t lane) {
+    constexpr uint32_t P = 32u * E;
+#pragma unroll
+    for (uint32_t k = 2; k <= P; k <<= 1) {
+#pragma unroll
+        for (uint32_t j = k >> 1; j > 0; j >>= 1) {
+            if (j >= 32) {
+                const int d = static_cast<int>(j >> 5);
+#pragma unroll
+                for (int e = 0; e < E; ++e) {
+                    const int f = e ^ d;
+                    if (f > e) {
+                        const bool up = ((static_cast<uint32_t>(e) * 32u + lane) & k) == 0;
+                        const uint32_t a = v[e], b = v[f];
+                        if ((a > b) == up) {
+                            v[e] = b;
+                            v[f] = a;
+                        }
+                    }
+                }
+            } else {
+                const bool lower = (lane & j) == 0;
+#pragma unroll
+                for (int e = 0; e < E; ++e) {
+                    const uint32_t p = __shfl_xor_sync(FULL, v[e], static_cast<int>(j));
+                    const bool up = ((static_cast<uint32_t>(e) * 32u + lane) & k) == 0;
+                    const uint32_t lo = min(v[e], p), hi = max(v[e], p);
+                    v[e] = lower == up ? lo : hi;
+                }
+            }
+        }
+    }
+}
+
+// A run of up to 32 E keys sorted as 32-bit words (hash << L) | position, when
+// pidBits + L <= 31 (so every word is below the padding ~0): the hashes of a
+// step's pids are distinct, so this is the order by key.  Each lane then takes
+// its particle index from the lane and register that held that position.
+template <int E>
+__device__ __forceinline__ void warp_sort_run32(const Ctx &C, const CensusBank &cen, uint64_t *keys, uint32_t *vals,
+                                                double *wS, const double *wc, uint32_t b, uint32_t len, uint32_t r,
+                                                int pidBits, uint64_t hashMask, uint32_t lane) {
+    constexpr uint32_t L = E == 1 ? 5u : (E == 2 ? 6u : 7u);
+    uint32_t v[E], q0[E];
+#pragma unroll
+    for (int e = 0; e < E; ++e) {
+        const uint32_t i = static_cast<uint32_t>(e) * 32u + lane;
+        q0[e] = i < len ? vals[b + i] : 0u;
+        v[e] = i < len ? (static_cast<uint32_t>(keys[b + i] & hashMask) << L) | i : ~0u;
+    }
+    warp_bitonic32<E>(v, lane);
+#pragma unroll
+    for (int e = 0; e < E; ++e) {
+        const uint32_t i = static_cast<uint32_t>(e) * 32u + lane;
+        const uint32_t pos = v[e] & ((1u << L) - 1u);
+        uint32_t q = 0;
+#pragma unroll
+        for (int f = 0; f < E; ++f) {
+            const uint32_t t = __shfl_sync(FULL, q0[f], static_cast<int>(pos & 31u));
+            if ((pos >> 5) == static_cast<uint32_t>(f)) q = t;
+        }
+        if (i < len) {
+            keys[b + i] = (static_cast<uint64_t>(r) << pidBits) | (v[e] >> L);
+            vals[b + i] = q;
+            wS[b + i] = run_w(C, cen, wc, q);
+        }
+    }
+}
+
 // Runs 0..nRuns-1 of (keys, vals), each sorted in place by key, with the census
 // weights in sorted order to wS.  One warp per run of up to BUCKET_WARP_MAX
 // keys: in registers up to 128 (fully unrolled networks; larger ones would not
@@ -2045,11 +2116,14 @@ __global__ void __launch_bounds__(32 * BUCKET_WARPS) k_bucket_sort_runs(Ctx C, C
         if (len == 1) {
             if (lane == 0) wS[b] = run_w(C, cen, wc, vals[b]);
         } else if (len <= 32) {
-            warp_sort_run<1>(C, cen, keys, vals, wS, wc, b, len, r, pidBits, hashMask, lane);
+            if (pidBits <= 26) warp_sort_run32<1>(C, cen, keys, vals, wS, wc, b, len, r, pidBits, hashMask, lane);
+            else warp_sort_run<1>(C, cen, keys, vals, wS, wc, b, len, r, pidBits, hashMask, lane);
         } else if (len <= 64) {
-            warp_sort_run<2>(C, cen, keys, vals, wS, wc, b, len, r, pidBits, hashMask, lane);
+            if (pidBits <= 25) warp_sort_run32<2>(C, cen, keys, vals, wS, wc, b, len, r, pidBits, hashMask, lane);
+            else warp_sort_run<2>(C, cen, keys, vals, wS, wc, b, len, r, pidBits, hashMask, lane);
         } else if (len <= 128) {
-            warp_sort_run<4>(C, cen, keys, vals, wS, wc, b, len, r, pidBits, hashMask, lane);
+            if (pidBits <= 24) warp_sort_run32<4>(C, cen, keys, vals, wS, wc, b, len, r, pidBits, hashMask, lane);
+            else warp_sort_run<4>(C, cen, keys, vals, wS, wc, b, len, r, pidBits, hashMask, lane);
         } else if (len <= BUCKET_WARP_MAX) {
             uint32_t P = 256;
             while (P < len) P <<= 1;
