@@ -424,8 +424,8 @@ int storm_cuda_census_count(StormHandle *h, uint64_t *count);
  * STORM_ERR_INVALID_ARG with the cell state unchanged and an empty census.
  * Page-locked host arrays let the upload overlap; census_out's NULL fields are
  * not written (as get_census).  Particle shards, moving material,
- * reproducible tallies, the burst tuner and profiling run the three calls in
- * turn. */
+ * reproducible tallies, the burst tuner, profiling and the bank-visit
+ * transport mode run the three calls in turn. */
 int storm_cuda_step_host(StormHandle *h, double dt, const StormParticlesSoA *census_in, StormParticlesSoA *census_out,
                          uint64_t out_capacity, uint64_t *out_count, StormStepStats *stats);
 /* The transport bank after storm_cuda_phase_emit: the census followed by the
