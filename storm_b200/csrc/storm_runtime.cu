@@ -2155,7 +2155,8 @@ int storm_cuda_step(StormHandle *h, double dt, StormStepStats *stats) {
 // copy stream carries the census into the bank (cells first, checked on the
 // device before anything of the step changes the cell state), while the main
 // stream runs the prestep, the emission and the transport of the step's new
-// packets; the census joins with its begin and a second transport launch.
+// packets; the rest of the census follows in chunks, each joining with its
+// begin and a transport launch over its slots once it is in place.
 // Each particle draws from its own stream and the comb orders the census by
 // key, so the result is the three calls' result (FP64 tally sums up to their
 // order).  Problems whose transport is not the refill kernel, particle shards,
