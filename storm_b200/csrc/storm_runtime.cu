@@ -2168,16 +2168,9 @@ static bool step_host_overlaps(const StormHandle *h) {
            h->pinned != nullptr;
 }
 
-int storm_cuda_step_host(StormHandle *h, double dt, const StormParticlesSoA *in, StormParticlesSoA *out,
-                         uint64_t out_capacity, uint64_t *out_count, StormStepStats *stats) {
-    if (!h || !in || !out || !(dt > 0.0)) return STORM_ERR_INVALID_ARG;
+static int step_host_overlapped(StormHandle *h, double dt, const StormParticlesSoA *in, StormParticlesSoA *out,
+                                uint64_t out_capacity, uint64_t *out_count, StormStepStats *stats) {
     const uint64_t n = in->count;
-    if (n == 0 || !step_host_overlaps(h)) {
-        int rc = storm_cuda_set_census(h, in);
-        if (rc == STORM_OK) rc = storm_cuda_step(h, dt, stats);
-        if (rc == STORM_OK) rc = storm_cuda_get_census(h, out, out_capacity, out_count);
-        return rc;
-    }
     const double *sd[] = {in->x, in->y, in->z, in->vx, in->vy, in->vz, in->time_left, in->weight, in->initial_weight};
     if (!in->cell) return STORM_ERR_INVALID_ARG;
     for (int q = 0; q < 9; ++q)
@@ -2230,10 +2223,7 @@ int storm_cuda_step_host(StormHandle *h, double dt, const StormParticlesSoA *in,
     h->nCenGlobal = n;
     h->stats.census_in = n;
     rc = emit_packets(h, dt, ne);
-    if (rc != STORM_OK) {
-        cudaStreamSynchronize(cs);
-        return rc;
-    }
+    if (rc != STORM_OK) return rc;
     CK(cudaEventRecord(h->evAfterEmit, h->stream));
     // transport: the packets [n, nBank), then the census [0, n) once it is in place
     const uint64_t nb = h->nBank;
@@ -2325,6 +2315,21 @@ int storm_cuda_step_host(StormHandle *h, double dt, const StormParticlesSoA *in,
     }
     if (stats) storm_cuda_phase_stats(h, stats);
     if (rc == STORM_OK) rc = storm_cuda_get_census(h, out, out_capacity, out_count);
+    return rc;
+}
+
+int storm_cuda_step_host(StormHandle *h, double dt, const StormParticlesSoA *in, StormParticlesSoA *out,
+                         uint64_t out_capacity, uint64_t *out_count, StormStepStats *stats) {
+    if (!h || !in || !out || !(dt > 0.0)) return STORM_ERR_INVALID_ARG;
+    if (in->count == 0 || !step_host_overlaps(h)) {
+        int rc = storm_cuda_set_census(h, in);
+        if (rc == STORM_OK) rc = storm_cuda_step(h, dt, stats);
+        if (rc == STORM_OK) rc = storm_cuda_get_census(h, out, out_capacity, out_count);
+        return rc;
+    }
+    const int rc = step_host_overlapped(h, dt, in, out, out_capacity, out_count, stats);
+    // a call that failed part-way leaves no upload still writing the banks
+    if (rc != STORM_OK && h->copyStream) cudaStreamSynchronize(h->copyStream);
     return rc;
 }
 
